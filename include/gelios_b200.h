@@ -1,0 +1,190 @@
+/* gelios_b200 — B200-native (sm_100a) plasma time step of Gelios_2D behind a C ABI.
+ *
+ * The reference (SergeyMSU/Gelios_2D) exposes this path as member functions
+ * of its grid class Setka (Setka.h:21-235); each entry point below names the
+ * reference interface it stands in for.  The ABI carries only plain pointers,
+ * sizes and POD structs: a C++ driver that holds a reference Setka converts
+ * its Point/Cell/Gran/Rail pointers to indices (Point::number, Cell::number,
+ * All_Gran / All_Gran_copy order) and calls these functions in place of the
+ * member functions (see INTEGRATION.md for the shim).
+ *
+ * Conventions
+ *   - return 0 on success, a negative GELIOS_E_* code on error; the message
+ *     of the last error of the calling thread is gelios_last_error().
+ *   - one context per host thread; calls on one context are not re-entrant.
+ *   - device memory belongs to the context; host arrays belong to the caller
+ *     and are only read/written during the call.
+ *   - numbering: points in All_Points order, cells in All_Cells order, faces
+ *     unified as All_Gran (main, [0, n_main)) followed by All_Gran_copy
+ *     ([n_main, n_faces)); -1 stands for a null pointer.
+ *   - enum values are the reference's: Gran_type (Gran.h:8-17), Cell_type
+ *     (Cell.h:8-17), Point_type (Point.h:7-22), Rail_type (Rail.h:8-16).
+ */
+#ifndef GELIOS_B200_H
+#define GELIOS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GELIOS_ABI_VERSION 1
+
+enum {
+    GELIOS_OK = 0,
+    GELIOS_E_ARG = -1,      /* bad argument / size */
+    GELIOS_E_CUDA = -2,     /* CUDA runtime error */
+    GELIOS_E_STATE = -3,    /* call order (e.g. step before topology) */
+    GELIOS_E_NODEVICE = -4, /* no CUDA device */
+    GELIOS_E_MESH = -5,     /* topology the kernels cannot take */
+    GELIOS_E_LIMIT = -6     /* size beyond a stated maximum */
+};
+
+/* Step forms (which reference loop gelios_step replaces). */
+enum {
+    GELIOS_FORM_STATIONARY = 0, /* Setka::Go_stationary(int)                      Setka.h:177, Setka.cpp:5205-5343  */
+    GELIOS_FORM_MK2 = 1,        /* Setka::Go_5_komponent__MK2(int)                Setka.h:186, Setka.cpp:10121-10482 */
+    GELIOS_FORM_INNER_MK2 = 2   /* Setka::Go_stationary_5_komponent_inner_MK2(int) Setka.h:176, Setka.cpp:6999-7212  */
+};
+
+/* Riemann-solver precision (geometry, accumulation and the dt reduction stay FP64). */
+enum { GELIOS_PREC_FP64 = 0, GELIOS_PREC_FP32_FLUX = 1 };
+
+/* Runtime replacement of the reference's compile-time constants
+ * (Help.h:39-114, Gran.cpp:216-281, Setka.cpp:3380/5256/10129/10169,
+ * Solvers.cpp:1206).  gelios_params_reference() fills the reference values. */
+typedef struct gelios_params {
+    double gamma;        /* adiabatic index ga/ggg */
+    double kurant;       /* CFL number */
+    double chi;          /* inner-sphere wind speed (chi_real) */
+    double inner_mach;   /* inner-sphere Mach number (10) */
+    double in_ro, in_p, in_u, in_v, in_Q; /* Input BC state */
+    double extern_u_par; /* outflow clamp of Get_par (-0.1) */
+    double extern_u_tvd; /* outflow clamp of Get_par_TVD (-0.01) */
+    double R11;          /* MK2: cells with centroid radius < R11 are not updated */
+    double rad_stat;     /* Go_stationary: radial scaling below this radius (95) */
+    double R1, R111, R5, Left; /* rail geometry of Move_Setka_Calculate_2 */
+    double koef;         /* Move_surface damping (0.1) */
+    double src_rmin, src_rmax; /* radial window of the source re-interpolation */
+    double src_coef;     /* n_p_LISM_/Kn_ */
+    double a_2;          /* charge-exchange cross-section coefficient */
+    double ro_floor, p_floor; /* update clamps (1e-5, 1e-6) */
+    double dt0;          /* dt of the first step of every call (1e-8) */
+    int32_t n_inner;     /* rail points of the inner layer (20) */
+    int32_t n_outer_shock; /* (13) */
+    int32_t godunov_max_iter; /* Newton/bisection cap (1100); exceeded -> status flag, never a trap */
+    int32_t precision;   /* GELIOS_PREC_* */
+} gelios_params;
+
+/* Topology + geometry of a Setka, as flat arrays (read during the call only). */
+typedef struct gelios_mesh_view {
+    int32_t dims[8]; /* N1..M4 passed to Setka(N1..M4), zeros for grids without rails */
+    int32_t n_points;
+    const double *x, *y;           /* Point::x, y */
+    const int32_t *point_type;     /* Point::type */
+    int32_t n_cells;
+    const int32_t *cell_type;      /* Cell::type */
+    const int32_t *contour_start;  /* n_cells+1, CSR of Cell::contour */
+    const int32_t *contour;
+    const int32_t *gran_start;     /* n_cells+1, CSR of Cell::Grans (order = flux summation order) */
+    const int32_t *gran;
+    const int32_t *cell_back, *cell_next; /* Cell::Back/Next (TVD_prepare), may be NULL */
+    const double *r_istoch;        /* Cell::r_istoch, may be NULL */
+    int32_t n_faces, n_main;
+    const int32_t *face_A, *face_B, *face_type, *face_master, *face_sosed, *face_copy;
+    const int32_t *face_sosed_up, *face_sosed_down; /* may be NULL: then computed like TVD_prepare */
+    int32_t n_rails;               /* A_Rails, B_Rails, C_Rails, D_Rails concatenated */
+    const int32_t *rail_type;
+    const double *rail_s;
+    const int32_t *rail_M;         /* 4 per rail: M1..M4 */
+    const int32_t *rail_pstart, *rail_points; /* CSR of Rail::All_point */
+    const int32_t *rail_kstart, *rail_keys;   /* CSR of Rail::Key_point */
+    int32_t n_contact, n_inner_line, n_outer_line;
+    const int32_t *line_contact, *line_inner, *line_outer; /* Line_Contact/Inner/Outer (sorted by polar angle) */
+} gelios_mesh_view;
+
+typedef struct gelios_status {
+    int32_t flags;      /* bit0 Newton/bisection cap, bit1 non-positive TVD state,
+                           bit2 negative Newton pressure, bit3 broken source chain,
+                           bit4 non-finite dt */
+    int32_t steps_done;
+    int64_t n_ro_clamp; /* updates clamped to ro_floor */
+    int64_t n_p_clamp;  /* updates clamped to p_floor */
+    double dt;          /* dt computed by the last step (the one the next step would use) */
+    int32_t result_buf; /* buffer (0/1) that holds the newest state, like par[] in the reference */
+    int32_t pad_;
+} gelios_status;
+
+typedef struct gelios_ctx gelios_ctx;
+typedef struct gelios_mesh gelios_mesh;
+
+/* ---- parameters ---------------------------------------------------------- */
+void gelios_params_reference(gelios_params *out);
+const char *gelios_last_error(void);
+int gelios_abi_version(void);
+
+/* ---- native grid builders (host) -------------------------------------------
+ * Setka::Setka(N1,N2,N3,N4,M1,M2,M3,M4), Setka.cpp:19-1076: same points,
+ * cells, faces, rails and Line_* lists in the same order (bit-exact). */
+gelios_mesh *gelios_mesh_build_setka(int N1, int N2, int N3, int N4, int M1, int M2, int M3, int M4);
+/* Axisymmetric polar half-plane grid: n_theta x n_r quads, rays uniform in
+ * 0..pi, radii log-spaced r_in..r_out; Axis faces on both rays, Inner_sphere
+ * faces at r_in, Input faces on the outer arc for theta < pi/2, Extern beyond. */
+gelios_mesh *gelios_mesh_build_polar(int n_theta, int n_r, double r_in, double r_out);
+/* Setka::TVD_prepare, Setka.cpp:1294-1492: Sosed_up/Sosed_down of every face,
+ * Back/Next/r_istoch of every cell (uses the reference's colliding face numbers). */
+int gelios_mesh_tvd_prepare(gelios_mesh *m);
+/* Cells whose centroid radius is <= r_max (All_Cells_Inner, Gelios_2D.cpp:152-231). */
+int gelios_mesh_inner_cells(const gelios_mesh *m, double r_max, int32_t *out, int32_t cap);
+/* Pointers into the mesh (valid until gelios_mesh_free). */
+int gelios_mesh_get_view(const gelios_mesh *m, gelios_mesh_view *out);
+void gelios_mesh_free(gelios_mesh *m);
+
+/* ---- device context --------------------------------------------------------
+ * gelios_create: stands in for the Setka instance that owns par[0/1] and the
+ * points; it owns device buffers and one CUDA stream on `device`. */
+int gelios_create(gelios_ctx **out, const gelios_params *prm, int device);
+int gelios_set_params(gelios_ctx *ctx, const gelios_params *prm);
+void gelios_destroy(gelios_ctx *ctx);
+/* Copies the topology (and current point coordinates) to the device. */
+int gelios_upload_topology(gelios_ctx *ctx, const gelios_mesh_view *mesh);
+/* Cell::par[buf].ro/p/u/v/Q for all cells (host arrays of n_cells doubles). */
+int gelios_upload_state(gelios_ctx *ctx, int buf, const double *ro, const double *p, const double *u,
+                        const double *v, const double *Q);
+int gelios_download_state(gelios_ctx *ctx, int buf, double *ro, double *p, double *u, double *v, double *Q);
+/* Monte-Carlo moments left in Cell::par[0] by MK_start_new (Setka.cpp:12241-12449):
+ * Hn/Hu/Hv/HT are [cell*4 + sort], ku/kv/kT are per cell. */
+int gelios_upload_mc(gelios_ctx *ctx, const double *Hn, const double *Hu, const double *Hv, const double *HT,
+                     const double *ku, const double *kv, const double *kT);
+/* All_Cells_Inner for GELIOS_FORM_INNER_MK2. */
+int gelios_set_inner_cells(gelios_ctx *ctx, const int32_t *cells, int32_t n);
+/* Runs `nsteps` iterations of the chosen loop (each call restarts dt at dt0,
+ * as the reference does).  Asynchronous on the context stream unless
+ * `status` is non-NULL, in which case it synchronises and fills it. */
+int gelios_step(gelios_ctx *ctx, int form, int nsteps, gelios_status *status);
+/* Point::x,y (after motion) for all points. */
+int gelios_download_points(gelios_ctx *ctx, double *x, double *y);
+int gelios_synchronize(gelios_ctx *ctx);
+/* Device-resident pointers of the state buffers (5 x n_cells doubles each,
+ * rows ro,p,u,v,Q) for callers that keep data in HBM. */
+int gelios_state_device_ptr(gelios_ctx *ctx, int buf, double **dptr);
+/* The context's CUDA stream (cudaStream_t as void*). */
+void *gelios_stream(gelios_ctx *ctx);
+/* Kernel launches issued by the last gelios_step call. */
+int64_t gelios_last_launch_count(gelios_ctx *ctx);
+
+/* ---- per-face solvers on the device (known-answer checks) ------------------
+ * Batched HLLC_2d_Korolkov_b_s (Setka.cpp:10484-10700): in[n*16] =
+ * roL,QL,pL,v1L,v2L, roR,QR,pR,v1R,v2R, W, n1, n2, rad, metod, nul_potok;
+ * out[n*9] = time, P0..P3, PQ, Vl, Vc, Vp.  Host arrays. */
+int gelios_hllc_batch(const gelios_params *prm, int n, const double *in, double *out);
+/* Batched Godunov_Solver_Alexashov (Solvers.cpp:693-1172): in[n*15] =
+ * q1[5] (ro,p,u,v,w), q2[5], n[3], w, dist; out[n*10] = time, q[5], dsl, dsp, dsc, status. */
+int gelios_godunov_batch(const gelios_params *prm, int n, const double *in, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

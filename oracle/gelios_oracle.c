@@ -1,0 +1,1750 @@
+/* Test infrastructure only (never linked by the product): CPU restatement of
+ * the Gelios_2D plasma time step, used as the checker of the CUDA path.
+ *
+ * Every function states the reference lines it follows (paths within the
+ * SergeyMSU/Gelios_2D tree).  Operation order follows the reference so that,
+ * built without FMA contraction and given the reference's compile-time
+ * constants as parameters, results agree with the compiled reference bit for
+ * bit.  Data are structure-of-arrays indexed by the unified numbering of the
+ * mesh (cells in All_Cells order, faces = All_Gran then All_Gran_copy).
+ *
+ * Where the reference calls exit(-1) (Newton/bisection caps, non-positive
+ * TVD states) this restatement raises a status bit and carries on.
+ */
+#include "gelios_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define PI_ 3.14159265358979323846
+#define kv(x) ((x) * (x))
+
+enum { T_USUALY = 0, T_INNER_SPHERE, T_EXTERN, T_INPUT, T_AXIS, T_UPPER_WALL };
+enum { C_1 = 0, C_2, C_3, C_4, C_5, C_CENTR };
+enum { P_CONTACT = 6, P_INNER_SHOCK = 7, P_OUTER_SHOCK = 8 };
+enum { R_A = 0, R_B, R_C, R_D };
+
+typedef struct {
+    double ro, p, u, v, Q;
+} st5;
+
+typedef struct ctx {
+    go_params prm;
+    go_mesh m;
+    /* owned copies of mutable geometry */
+    double *x, *y, *x2, *y2, *Vx, *Vy;
+    int32_t *count;
+    /* state par[2], 5 fields each */
+    double *par[2][5];
+    /* MC moments */
+    double *Hn, *Hu, *Hv, *HT, *ku, *kv_, *kT;
+    int32_t *inner;
+    int32_t n_inner_cells;
+    int64_t status, n_ro_clamp, n_p_clamp, n_tvd_bad;
+    double last_dt;
+} ctx;
+
+/* ------------------------------------------------------------------ helpers */
+static double dmin(double a, double b) { return (b < a) ? b : a; } /* std::min */
+static double dmax(double a, double b) { return (a < b) ? b : a; } /* std::max */
+
+/* sign, minmod: Help.cpp:67-94 */
+static double sgn(double x) { return x > 0 ? 1.0 : (x < 0 ? -1.0 : 0.0); }
+static double minmod(double x, double y) {
+    if (sgn(x) + sgn(y) == 0) return 0.0;
+    return ((sgn(x) + sgn(y)) / 2.0) * dmin(fabs(x), fabs(y));
+}
+/* linear, 3-point minmod: Help.cpp:96-113 */
+static double linear3(double x1, double t1, double x2, double t2, double x3, double t3, double y) {
+    double d = minmod((t1 - t2) / (x1 - x2), (t2 - t3) / (x2 - x3));
+    return (d * (y - x2) + t2);
+}
+/* linear, 2-point: Help.cpp:115-120 */
+static double linear2(double x1, double t1, double x2, double t2, double y) {
+    double d = (t1 - t2) / (x1 - x2);
+    return (d * (y - x2) + t2);
+}
+/* polar_angle: Help.cpp:37-65 (RR_ in the threshold is the geometry scale) */
+static double polar_angle(double x, double y, double tiny) {
+    if (fabs(x) + fabs(y) < tiny) return 0.0;
+    if (x < 0) return atan(y / x) + 1.0 * PI_;
+    else if (x > 0 && y >= 0) return atan(y / x);
+    else if (x > 0 && y < 0) return atan(y / x) + 2.0 * PI_;
+    else if (y > 0 && x >= 0 && x <= 0) return PI_ / 2.0;
+    else if (y < 0 && x >= 0 && x <= 0) return 3.0 * PI_ / 2.0;
+    return 0.0;
+}
+/* polar_perenos: Help.cpp:3-14 */
+static void polar_perenos(double x1, double y1, double x2, double y2, double *u, double *v, double tiny) {
+    double phi1 = polar_angle(x1, y1, tiny);
+    double phi2 = polar_angle(x2, y2, tiny);
+    double fr = *u * cos(phi1) + *v * sin(phi1);
+    double ff = -*u * sin(phi1) + *v * cos(phi1);
+    *u = fr * cos(phi2) - ff * sin(phi2);
+    *v = fr * sin(phi2) + ff * cos(phi2);
+}
+/* the polar_angle threshold is 0.000001/RR_ (Help.cpp:39); RR_ = 390.222 */
+#define TINY_ANGLE (0.000001 / 390.222)
+
+/* ------------------------------------------------------------------ geometry */
+/* Cell::Get_Center / Get_Center_posle: Cell.cpp:66-111 */
+static void cell_center(const ctx *c, int k, int posle, double *ox, double *oy) {
+    const double *X = posle ? c->x2 : c->x, *Y = posle ? c->y2 : c->y;
+    int s = c->m.contour_start[k], e = c->m.contour_start[k + 1], n = e - s;
+    double A = 0.0, Gx = 0.0, Gy = 0.0;
+    for (int i = 0; i < n; i++) {
+        int a = c->m.contour[s + i];
+        int j = i + 1;
+        if (j == n) j = 0;
+        int b = c->m.contour[s + j];
+        A = A + (X[a] * Y[b] - Y[a] * X[b]);
+        Gx = Gx + (X[a] + X[b]) * (X[a] * Y[b] - Y[a] * X[b]);
+        Gy = Gy + (Y[a] + Y[b]) * (X[a] * Y[b] - Y[a] * X[b]);
+    }
+    A = A * 0.5;
+    Gx = Gx / (6.0 * A);
+    Gy = Gy / (6.0 * A);
+    *ox = Gx;
+    *oy = Gy;
+}
+/* Cell::Get_Volume / Get_Volume_posle: Cell.cpp:146-254 */
+static double cell_volume(const ctx *c, int k, int posle) {
+    const double *X = posle ? c->x2 : c->x, *Y = posle ? c->y2 : c->y;
+    int s = c->m.contour_start[k], n = c->m.contour_start[k + 1] - s;
+    const int32_t *ct = c->m.contour + s;
+    if (n == 4) {
+        double a1 = X[ct[0]] - X[ct[2]];
+        double a2 = Y[ct[0]] - Y[ct[2]];
+        double a = sqrt(kv(a1) + kv(a2));
+        double b1 = X[ct[1]] - X[ct[3]];
+        double b2 = Y[ct[1]] - Y[ct[3]];
+        double b = sqrt(kv(b1) + kv(b2));
+        a1 = a1 / a;
+        a2 = a2 / a;
+        b1 = b1 / b;
+        b2 = b2 / b;
+        double cc = a1 * b1 + a2 * b2;
+        double sn = sqrt(1 - kv(cc));
+        return 0.5 * a * b * sn;
+    }
+    double x = 0.0, y = 0.0;
+    if (!posle) {
+        cell_center(c, k, 0, &x, &y);
+    } else {
+        for (int i = 0; i < n; i++) {
+            x += X[ct[i]];
+            y += Y[ct[i]];
+        }
+        x = x / (1.0 * n);
+        y = y / (1.0 * n);
+    }
+    double S = 0.0;
+    for (int g = c->m.gran_start[k]; g < c->m.gran_start[k + 1]; g++) {
+        int f = c->m.gran[g];
+        int pa = c->m.face_A[f], pb = c->m.face_B[f];
+        double a1 = sqrt(kv(X[pa] - x) + kv(Y[pa] - y));
+        double a2 = sqrt(kv(X[pb] - x) + kv(Y[pb] - y));
+        double a3 = sqrt(kv(X[pa] - X[pb]) + kv(Y[pa] - Y[pb]));
+        double p = (a1 + a2 + a3) / 2.0;
+        S = S + sqrt(p * (p - a1) * (p - a2) * (p - a3));
+    }
+    return S;
+}
+/* Cell::Get_Volume_rotate / Get_Volume_posle_rotate: Cell.cpp:188-206, 256-275 */
+static double cell_volume_rotate(const ctx *c, int k, int posle, double angle) {
+    const double *X = posle ? c->x2 : c->x, *Y = posle ? c->y2 : c->y;
+    int s = c->m.contour_start[k], n = c->m.contour_start[k + 1] - s;
+    double A = 0.0, G = 0.0;
+    for (int i = 0; i < n; i++) {
+        int a = c->m.contour[s + i];
+        int j = i + 1;
+        if (j == n) j = 0;
+        int b = c->m.contour[s + j];
+        A = A + (X[a] * Y[b] - Y[a] * X[b]);
+        G = G + (Y[a] + Y[b]) * (X[a] * Y[b] - Y[a] * X[b]);
+    }
+    A = A * 0.5;
+    return fabs(A) * (1.0 / (6.0 * A)) * G * PI_ * angle / 180.0;
+}
+/* Gran::Get_Center(_posle), Get_normal, Get_square: Gran.cpp:159-198 */
+static void face_center(const ctx *c, int f, int posle, double *ox, double *oy) {
+    const double *X = posle ? c->x2 : c->x, *Y = posle ? c->y2 : c->y;
+    int a = c->m.face_A[f], b = c->m.face_B[f];
+    *ox = (X[a] + X[b]) / 2.0;
+    *oy = (Y[a] + Y[b]) / 2.0;
+}
+static void face_normal(const ctx *c, int f, double *n1, double *n2) {
+    int a = c->m.face_A[f], b = c->m.face_B[f];
+    double t1 = c->x[b] - c->x[a];
+    double t2 = c->y[b] - c->y[a];
+    double n = sqrt(kv(t1) + kv(t2));
+    t1 = t1 / n;
+    t2 = t2 / n;
+    *n1 = t2;
+    *n2 = -t1;
+}
+static double face_square(const ctx *c, int f) {
+    int a = c->m.face_A[f], b = c->m.face_B[f];
+    return sqrt(kv(c->x[b] - c->x[a]) + kv(c->y[b] - c->y[a]));
+}
+
+static st5 cell_state(const ctx *c, int k, int buf) {
+    st5 s;
+    s.ro = c->par[buf][0][k];
+    s.p = c->par[buf][1][k];
+    s.u = c->par[buf][2][k];
+    s.v = c->par[buf][3][k];
+    s.Q = c->par[buf][4][k];
+    return s;
+}
+
+static int cell_has_axis(const ctx *c, int k) {
+    for (int g = c->m.gran_start[k]; g < c->m.gran_start[k + 1]; g++)
+        if (c->m.face_type[c->m.gran[g]] == T_AXIS) return 1;
+    return 0;
+}
+
+/* ------------------------------------------------------------------ boundary / reconstruction */
+/* Inner_sphere BC state: Gran.cpp:234-265 (Get_par) and 520-534 (Get_par_TVD) */
+static st5 inner_sphere_state(const ctx *c, int f) {
+    const go_params *P = &c->prm;
+    double x, y;
+    face_center(c, f, 0, &x, &y);
+    double dist = sqrt(x * x + y * y);
+    double ro = 1.0 / (kv(P->chi) * dist * dist);
+    double P_E = ro * P->chi * P->chi / (P->gamma * P->inner_mach * P->inner_mach);
+    st5 s = {ro, P_E, P->chi * x / dist, P->chi * y / dist, ro};
+    return s;
+}
+static st5 input_state(const ctx *c) {
+    st5 s = {c->prm.in_ro, c->prm.in_p, c->prm.in_u, c->prm.in_v, c->prm.in_Q};
+    return s;
+}
+
+/* Gran::Get_par: Gran.cpp:205-289 */
+static st5 get_par(const ctx *c, int f, int buf) {
+    int t = c->m.face_type[f];
+    st5 s = {0, 0, 0, 0, 0};
+    if (t == T_USUALY) {
+        s = cell_state(c, c->m.face_sosed[f], buf);
+    } else if (t == T_EXTERN) {
+        s = cell_state(c, c->m.face_master[f], buf);
+        if (s.u >= 0.0) s.u = c->prm.extern_u_par;
+    } else if (t == T_UPPER_WALL) {
+        s = cell_state(c, c->m.face_master[f], buf);
+    } else if (t == T_AXIS) {
+        s = cell_state(c, c->m.face_master[f], buf);
+        s.v = -s.v;
+    } else if (t == T_INNER_SPHERE) {
+        s = inner_sphere_state(c, f);
+    } else if (t == T_INPUT) {
+        s = input_state(c);
+    }
+    return s;
+}
+
+static int is_tracked_face(const ctx *c, int f) {
+    int ta = c->m.point_type[c->m.face_A[f]], tb = c->m.point_type[c->m.face_B[f]];
+    return (ta == P_CONTACT && tb == P_CONTACT) || (ta == P_INNER_SHOCK && tb == P_INNER_SHOCK) ||
+           (ta == P_OUTER_SHOCK && tb == P_OUTER_SHOCK);
+}
+
+/* Gran::Get_par_TVD: Gran.cpp:292-559.  `io` holds the caller's incoming
+ * values (the reference writes into the caller's Parametr in place). */
+static void get_par_tvd(ctx *c, int f, int buf, st5 *io) {
+    int t = c->m.face_type[f];
+    int M = c->m.face_master[f];
+    if (t == T_USUALY) {
+        int Sd = c->m.face_sosed_down[f];
+        int So = c->m.face_sosed[f];
+        if (Sd < 0) {
+            if (cell_has_axis(c, M)) { /* Gran.cpp:308-338 */
+                double x, y, x2, y2, dist1, dist2, dist3;
+                st5 par = cell_state(c, M, buf);
+                face_center(c, f, 0, &x, &y);
+                st5 par2 = cell_state(c, M, buf);
+                st5 par1 = cell_state(c, M, buf);
+                par1.v = -par1.v;
+                st5 par3 = cell_state(c, So, buf);
+                cell_center(c, M, 0, &x2, &y2);
+                dist2 = sqrt(kv(x - x2) + kv(y - y2));
+                cell_center(c, So, 0, &x2, &y2);
+                dist3 = sqrt(kv(x - x2) + kv(y - y2));
+                cell_center(c, M, 0, &x2, &y2);
+                y2 = -y2;
+                dist1 = sqrt(kv(x - x2) + kv(y - y2));
+                par.v = linear3(-dist1, par1.v, -dist2, par2.v, dist3, par3.v, 0.0);
+                *io = par;
+            } else {
+                *io = cell_state(c, M, buf);
+            }
+            return;
+        }
+        if (is_tracked_face(c, f)) { /* Gran.cpp:345-426 */
+            double x, y, x2, y2, dist1, dist2;
+            face_center(c, f, 0, &x, &y);
+            st5 par2 = cell_state(c, M, buf);
+            st5 par1 = cell_state(c, Sd, buf);
+            cell_center(c, M, 0, &x2, &y2);
+            dist2 = sqrt(kv(x - x2) + kv(y - y2));
+            cell_center(c, Sd, 0, &x2, &y2);
+            dist1 = sqrt(kv(x - x2) + kv(y - y2));
+            io->ro = linear2(-dist1, par1.ro, -dist2, par2.ro, 0.0);
+            io->p = linear2(-dist1, par1.p, -dist2, par2.p, 0.0);
+            io->u = linear2(-dist1, par1.u, -dist2, par2.u, 0.0);
+            io->v = linear2(-dist1, par1.v, -dist2, par2.v, 0.0);
+            io->Q = linear2(-dist1, par1.Q, -dist2, par2.Q, 0.0);
+            if (io->ro <= 0.0) io->ro = par2.ro;
+            if (io->p <= 0.0) io->p = par2.p;
+            return;
+        }
+        /* Gran.cpp:427-472 */
+        double x, y, x2, y2, dist1, dist2, dist3;
+        face_center(c, f, 0, &x, &y);
+        st5 par2 = cell_state(c, M, buf);
+        st5 par1 = cell_state(c, Sd, buf);
+        st5 par3 = cell_state(c, So, buf);
+        cell_center(c, M, 0, &x2, &y2);
+        dist2 = sqrt(kv(x - x2) + kv(y - y2));
+        cell_center(c, So, 0, &x2, &y2);
+        dist3 = sqrt(kv(x - x2) + kv(y - y2));
+        cell_center(c, Sd, 0, &x2, &y2);
+        dist1 = sqrt(kv(x - x2) + kv(y - y2));
+        io->ro = linear3(-dist1, par1.ro, -dist2, par2.ro, dist3, par3.ro, 0.0);
+        io->p = linear3(-dist1, par1.p, -dist2, par2.p, dist3, par3.p, 0.0);
+        io->u = linear3(-dist1, par1.u, -dist2, par2.u, dist3, par3.u, 0.0);
+        io->v = linear3(-dist1, par1.v, -dist2, par2.v, dist3, par3.v, 0.0);
+        io->Q = linear3(-dist1, par1.Q, -dist2, par2.Q, dist3, par3.Q, 0.0);
+        if (io->ro <= 0.0 || io->p <= 0.0) { /* reference: exit(-1), Gran.cpp:444-455 */
+            c->status |= 2;
+            c->n_tvd_bad++;
+        }
+    } else if (t == T_EXTERN) {
+        *io = cell_state(c, M, buf);
+        if (io->u >= 0.0) io->u = c->prm.extern_u_tvd;
+    } else if (t == T_UPPER_WALL) {
+        *io = cell_state(c, M, buf);
+    } else if (t == T_AXIS) { /* Gran.cpp:486-519 */
+        double x, y, x2, y2, dist1, dist2;
+        int Sd = c->m.face_sosed_down[f];
+        face_center(c, f, 0, &x, &y);
+        st5 par2 = cell_state(c, M, buf);
+        st5 par1 = cell_state(c, Sd, buf);
+        cell_center(c, M, 0, &x2, &y2);
+        dist2 = sqrt(kv(x - x2) + kv(y - y2));
+        cell_center(c, Sd, 0, &x2, &y2);
+        dist1 = sqrt(kv(x - x2) + kv(y - y2));
+        *io = par2;
+        io->v = linear3(-dist1, par1.v, -dist2, par2.v, dist2, -par2.v, 0.0);
+    } else if (t == T_INNER_SPHERE) {
+        *io = inner_sphere_state(c, f);
+    } else if (t == T_INPUT) {
+        *io = input_state(c);
+    }
+}
+
+/* Gran::Get_par_TVD_radial: Gran.cpp:562-675; only ro and p are consumed by
+ * the callers (Setka.cpp:10228-10230, 10246-10248, 7083-7089).  Non-Usualy
+ * faces leave the caller's fresh Parametr untouched (zeros). */
+static void get_par_tvd_radial(const ctx *c, int f, int buf, double *oro, double *op) {
+    const double g2 = 2.0 * c->prm.gamma;
+    *oro = 0.0;
+    *op = 0.0;
+    if (c->m.face_type[f] != T_USUALY) return;
+    int M = c->m.face_master[f], So = c->m.face_sosed[f], Sd = c->m.face_sosed_down[f];
+    if (Sd < 0) {
+        if (cell_has_axis(c, M)) { /* Gran.cpp:580-626 */
+            double x, y, x2, y2, dist1, dist2, dist3;
+            face_center(c, f, 0, &x, &y);
+            double r = sqrt(kv(x) + kv(y));
+            st5 par2 = cell_state(c, M, buf);
+            st5 par1 = par2;
+            par1.v = -par1.v;
+            st5 par3 = cell_state(c, So, buf);
+            cell_center(c, M, 0, &x2, &y2);
+            double r2 = sqrt(kv(x2) + kv(y2));
+            dist2 = sqrt(kv(x - x2) + kv(y - y2));
+            cell_center(c, So, 0, &x2, &y2);
+            double r3 = sqrt(kv(x2) + kv(y2));
+            dist3 = sqrt(kv(x - x2) + kv(y - y2));
+            cell_center(c, M, 0, &x2, &y2);
+            y2 = -y2;
+            double r1 = sqrt(kv(x2) + kv(y2));
+            dist1 = sqrt(kv(x - x2) + kv(y - y2));
+            *oro = linear3(-dist1, par1.ro * kv(r1), -dist2, par2.ro * kv(r2), dist3, par3.ro * kv(r3), 0.0) / kv(r);
+            *op = linear3(-dist1, par1.p * pow(r1, g2), -dist2, par2.p * pow(r2, g2), dist3, par3.p * pow(r3, g2),
+                          0.0) /
+                  pow(r, g2);
+        } else {
+            st5 s = cell_state(c, M, buf);
+            *oro = s.ro;
+            *op = s.p;
+        }
+        return;
+    }
+    double x, y, x2, y2, dist1, dist2, dist3;
+    face_center(c, f, 0, &x, &y);
+    double r = sqrt(kv(x) + kv(y));
+    st5 par2 = cell_state(c, M, buf);
+    st5 par1 = cell_state(c, Sd, buf);
+    st5 par3 = cell_state(c, So, buf);
+    cell_center(c, M, 0, &x2, &y2);
+    double r2 = sqrt(kv(x2) + kv(y2));
+    dist2 = sqrt(kv(x - x2) + kv(y - y2));
+    cell_center(c, So, 0, &x2, &y2);
+    double r3 = sqrt(kv(x2) + kv(y2));
+    dist3 = sqrt(kv(x - x2) + kv(y - y2));
+    cell_center(c, Sd, 0, &x2, &y2);
+    double r1 = sqrt(kv(x2) + kv(y2));
+    dist1 = sqrt(kv(x - x2) + kv(y - y2));
+    *oro = linear3(-dist1, par1.ro * kv(r1), -dist2, par2.ro * kv(r2), dist3, par3.ro * kv(r3), 0.0) / kv(r);
+    *op = linear3(-dist1, par1.p * pow(r1, g2), -dist2, par2.p * pow(r2, g2), dist3, par3.p * pow(r3, g2), 0.0) /
+          pow(r, g2);
+}
+
+/* ------------------------------------------------------------------ Riemann solvers */
+/* Setka::HLLC_2d_Korolkov_b_s: Setka.cpp:10484-10700 */
+static double hllc(const go_params *prm, double ro_L, double Q_L, double p_L, double v1_L, double v2_L, double ro_R,
+                   double Q_R, double p_R, double v1_R, double v2_R, double W, double *P, double *PQ, double n1,
+                   double n2, double rad, int metod, double *Vl, double *Vc, double *Vp, int nul_potok) {
+    const double ggg = prm->gamma, g1 = prm->gamma - 1.0;
+    double t1 = n2;
+    double t2 = -n1;
+    double u1 = v1_L * n1 + v2_L * n2;
+    double v1 = v1_L * t1 + v2_L * t2;
+    double u2 = v1_R * n1 + v2_R * n2;
+    double v2 = v1_R * t1 + v2_R * t2;
+    double cL = sqrt(ggg * p_L / ro_L);
+    double cR = sqrt(ggg * p_R / ro_R);
+    double uu_L = (kv(v1_L) + kv(v2_L)) / 2.0;
+    double uu_R = (kv(v1_R) + kv(v2_R)) / 2.0;
+    double SL = dmin(u1, u2) - dmax(cL, cR);
+    double SR = dmax(u1, u2) + dmax(cL, cR);
+    *Vl = SL;
+    *Vp = SR;
+    double suR = (SR - u2);
+    double suL = (SL - u1);
+    double SM = (suR * ro_R * u2 - suL * ro_L * u1 - p_R + p_L) / (suR * ro_R - suL * ro_L);
+    *Vc = SM;
+    double UU = dmax(fabs(SL), fabs(SR));
+    double time = prm->kurant * rad / UU;
+    double FL[5], FR[5], UL[5], UR[5];
+    double e1 = p_L / g1 + ro_L * uu_L;
+    double e2 = p_R / g1 + ro_R * uu_R;
+    FL[0] = ro_L * u1;
+    FL[1] = ro_L * u1 * u1 + p_L;
+    FL[2] = ro_L * u1 * v1;
+    FL[3] = (e1 + p_L) * u1;
+    FL[4] = Q_L * u1;
+    FR[0] = ro_R * u2;
+    FR[1] = ro_R * u2 * u2 + p_R;
+    FR[2] = ro_R * u2 * v2;
+    FR[3] = (e2 + p_R) * u2;
+    FR[4] = Q_R * u2;
+    UL[0] = ro_L;
+    UL[1] = ro_L * u1;
+    UL[2] = ro_L * v1;
+    UL[3] = e1;
+    UL[4] = Q_L;
+    UR[0] = ro_R;
+    UR[1] = ro_R * u2;
+    UR[2] = ro_R * v2;
+    UR[3] = e2;
+    UR[4] = Q_R;
+    if (SL >= W) {
+        P[1] = n1 * (FL[1] - W * UL[1]) + t1 * (FL[2] - W * UL[2]);
+        P[2] = n2 * (FL[1] - W * UL[1]) + t2 * (FL[2] - W * UL[2]);
+        P[0] = FL[0] - W * UL[0];
+        P[3] = FL[3] - W * UL[3];
+        *PQ = FL[4] - W * UL[4];
+        return time;
+    }
+    if (SR <= W) {
+        P[1] = n1 * (FR[1] - W * UR[1]) + t1 * (FR[2] - W * UR[2]);
+        P[2] = n2 * (FR[1] - W * UR[1]) + t2 * (FR[2] - W * UR[2]);
+        P[0] = FR[0] - W * UR[0];
+        P[3] = FR[3] - W * UR[3];
+        *PQ = FR[4] - W * UR[4];
+        return time;
+    }
+    double ro_LL = ro_L * (SL - u1) / (SL - SM);
+    double ro_RR = ro_R * (SR - u2) / (SR - SM);
+    double Q_LL = Q_L * (SL - u1) / (SL - SM);
+    double Q_RR = Q_R * (SR - u2) / (SR - SM);
+    double UZ0 = (SR * UR[0] - SL * UL[0] + FL[0] - FR[0]) / (SR - SL);
+    double UZ1 = (SR * UR[1] - SL * UL[1] + FL[1] - FR[1]) / (SR - SL);
+    double UZ2 = (SR * UR[2] - SL * UL[2] + FL[2] - FR[2]) / (SR - SL);
+    double UZ3 = (SR * UR[3] - SL * UL[3] + FL[3] - FR[3]) / (SR - SL);
+    double UZ4 = (SR * UR[4] - SL * UL[4] + FL[4] - FR[4]) / (SR - SL);
+    if (metod == 0) {
+        double PO[5];
+        for (int i = 0; i < 5; i++) PO[i] = (SR * FL[i] - SL * FR[i] + SR * SL * (UR[i] - UL[i])) / (SR - SL);
+        P[1] = n1 * (PO[1] - W * UZ1) + t1 * (PO[2] - W * UZ2);
+        P[2] = n2 * (PO[1] - W * UZ1) + t2 * (PO[2] - W * UZ2);
+        P[0] = PO[0] - W * UZ0;
+        P[3] = PO[3] - W * UZ3;
+        *PQ = PO[4] - W * UZ4;
+        return time;
+    }
+    double suRm = suR / (SR - SM);
+    double suLm = suL / (SL - SM);
+    double ptzR = p_R + ro_R * suR * (SM - u2);
+    double ptzL = p_L + ro_L * suL * (SM - u1);
+    double ptz = (ptzR + ptzL) / 2.0;
+    double vLL, vRR;
+    if (nul_potok) {
+        vRR = UZ2 / UZ0;
+        vLL = vRR;
+    } else {
+        vLL = v1;
+        vRR = v2;
+    }
+    double ee2 = e2 * suRm + (ptz * SM - p_R * u2) / (SR - SM);
+    double ee1 = e1 * suLm + (ptz * SM - p_L * u1) / (SL - SM);
+    double ULL[5], URR[5], PO[5] = {0, 0, 0, 0, 0};
+    ULL[0] = ro_LL;
+    ULL[1] = ro_LL * SM;
+    ULL[2] = ro_LL * vLL;
+    ULL[3] = ee1;
+    ULL[4] = Q_LL;
+    URR[0] = ro_RR;
+    URR[1] = ro_RR * SM;
+    URR[2] = ro_RR * vRR;
+    URR[3] = ee2;
+    URR[4] = Q_RR;
+    if (SL < W && SM >= W) {
+        for (int i = 0; i < 5; i++) PO[i] = FL[i] + SL * ULL[i] - SL * UL[i] - W * ULL[i];
+    } else if (SR > W && SM < W) {
+        for (int i = 0; i < 5; i++) PO[i] = FR[i] + SR * URR[i] - SR * UR[i] - W * URR[i];
+    }
+    P[1] = n1 * PO[1] + t1 * PO[2];
+    P[2] = n2 * PO[1] + t2 * PO[2];
+    P[0] = PO[0];
+    P[3] = PO[3];
+    *PQ = PO[4];
+    return time;
+}
+
+/* Solvers::lev: Solvers.cpp:1307-1321 */
+static double lev(double ga, double enI, double pI, double rI, double enII, double pII, double rII, double uuu) {
+    const double g1 = ga - 1.0, g2 = ga + 1.0, gp = (g2 / ga) / 2.0, gm = (g1 / ga) / 2.0;
+    double cI = sqrt(ga * pI / rI);
+    double cII = sqrt(ga * pII / rII);
+    double fI = (uuu - pI) / (rI * cI * sqrt(gp * uuu / pI + gm));
+    double fII = 2.0 / g1 * cII * (pow((uuu / pII), gm) - 1.0);
+    double f1 = fI + fII;
+    double f2 = enI - enII;
+    (void)cI;
+    return f1 - f2;
+}
+/* Solvers::devtwo: Solvers.cpp:1231-1305 (bisection) */
+static double devtwo(double ga, double enI, double pI, double rI, double enII, double pII, double rII, int cap,
+                     int *status) {
+    const double epsil = 10e-10;
+    double kl = pI, kp = pII, kc, ksi, ksir, ksit;
+    ksi = lev(ga, enI, pI, rI, enII, pII, rII, kl);
+    ksir = lev(ga, enI, pI, rI, enII, pII, rII, kp);
+    if (fabs(ksi) <= epsil) return kl;
+    if (fabs(ksir) <= epsil) return kp;
+    int k = 0;
+    for (;;) {
+        k = k + 1;
+        if (k == cap) {
+            *status |= 1;
+            return (kl + kp) / 2.0;
+        }
+        kc = (kl + kp) / 2.0;
+        ksit = lev(ga, enI, pI, rI, enII, pII, rII, kc);
+        if (fabs(ksit) <= epsil) return kc;
+        if ((ksi * ksit) <= 0.0) {
+            kp = kc;
+            ksir = ksit;
+        } else {
+            kl = kc;
+            ksi = ksit;
+        }
+    }
+}
+/* Solvers::newton: Solvers.cpp:1174-1229 */
+static double newton(double ga, double enI, double pI, double rI, double enII, double pII, double rII, int cap,
+                     int *status) {
+    const double eps = 10e-10;
+    const double g1 = ga - 1.0, g2 = ga + 1.0, gp = (g2 / ga) / 2.0, gm = (g1 / ga) / 2.0;
+    (void)g1;
+    double fI, fIs, fII, fIIs, p;
+    double cI = sqrt(ga * pI / rI);
+    double cII = sqrt(ga * pII / rII);
+    double pn = pI * rII * cII + pII * rI * cI + (enI - enII) * rI * cI * rII * cII;
+    pn = pn / (rI * cI + rII * cII);
+    double pee = pn;
+    int kiter = 0;
+    for (;;) {
+        p = pn;
+        if (p <= 0.0) {
+            *status |= 4;
+            return p;
+        }
+        kiter = kiter + 1;
+        fI = (p - pI) / (rI * cI * sqrt(gp * p / pI + gm));
+        fIs = (ga + 1.0) * p / pI + (3.0 * ga - 1.0);
+        fIs = fIs / (4.0 * ga * rI * cI * pow((gp * p / pI + gm), (3.0 / 2.0)));
+        fII = (p - pII) / (rII * cII * sqrt(gp * p / pII + gm));
+        fIIs = (ga + 1.0) * p / pII + (3.0 * ga - 1.0);
+        fIIs = fIIs / (4.0 * ga * rII * cII * pow((gp * p / pII + gm), (3.0 / 2.0)));
+        if (kiter == cap) {
+            *status |= 1;
+            return p;
+        }
+        pn = p - (fI + fII - (enI - enII)) / (fIs + fIIs);
+        if (!(fabs(pn / pee - p / pee) >= eps)) break;
+    }
+    return pn;
+}
+
+/* Solvers::Godunov_Solver_Alexashov: Solvers.cpp:693-1172.  q1, q2 = (ro, p,
+ * u, v, w); n[3] unit normal; output qqq[5] = mass, 3 momentum, energy flux
+ * in the moving frame w. */
+static double godunov(const go_params *prm, const double *qqq1, const double *qqq2, const double *n, double *qqq,
+                      double *dsl, double *dsp, double *dsc, double w, double DIST, int *status) {
+    const double ga = prm->gamma, g1 = ga - 1.0, g2 = ga + 1.0, gm = (g1 / ga) / 2.0;
+    const double gg1 = g1, gg2 = g2, gga = ga;
+    const double eps = 10e-10, eps8 = 10e-8;
+    const int cap = prm->godunov_max_iter;
+    double al = n[0], be = n[1], ge = n[2];
+    double time = 0.0;
+    double al2 = be, be2 = -al, ge2 = 0.0;
+    double al3 = 0.0, be3 = 0.0, ge3 = 1.0;
+    double enI = al * qqq1[2] + be * qqq1[3] + ge * qqq1[4];
+    double teI2 = al2 * qqq1[2] + be2 * qqq1[3] + ge2 * qqq1[4];
+    double teI3 = al3 * qqq1[2] + be3 * qqq1[3] + ge3 * qqq1[4];
+    double enII = al * qqq2[2] + be * qqq2[3] + ge * qqq2[4];
+    double teII2 = al2 * qqq2[2] + be2 * qqq2[3] + ge2 * qqq2[4];
+    double teII3 = al3 * qqq2[2] + be3 * qqq2[3] + ge3 * qqq2[4];
+    double pI = qqq1[1], pII = qqq2[1], rI = qqq1[0], rII = qqq2[0];
+    int ipiz = 0;
+    if (pI > pII) {
+        double eno2 = enII, teo22 = teII2, teo23 = teII3, p2 = pII, r2 = rII;
+        double eno1 = enI, teo12 = teI2, teo13 = teI3, p1 = pI, r1 = rI;
+        enI = -eno2; teI2 = teo22; teI3 = teo23; pI = p2; rI = r2;
+        enII = -eno1; teII2 = teo12; teII3 = teo13; pII = p1; rII = r1;
+        w = -w;
+        ipiz = 1;
+    }
+    double cI = 0.0, cII = 0.0;
+    if (pI != 0.0) cI = sqrt(ga * pI / rI);
+    if (pII != 0.0) cII = sqrt(ga * pII / rII);
+    double a = sqrt(rI * (g2 * pII + g1 * pI) / 2.0);
+    double Uud = (pII - pI) / a;
+    double Urz = -2.0 * cII / g1 * (1.0 - pow((pI / pII), gm));
+    double Uvk = -2.0 * (cII + cI) / g1;
+    double Udf = enI - enII;
+    int il = -2, ip = -2;
+    double p = 0.0, r = 0.0, te2 = 0.0, te3 = 0.0, en = 0.0;
+    if (Udf < Uvk) {
+        il = -1; ip = -1;
+    } else if ((Udf >= Uvk) && (Udf <= Urz)) {
+        p = pI * pow(((Udf - Uvk) / (Urz - Uvk)), (1.0 / gm));
+        il = 0; ip = 0;
+    } else if ((Udf > Urz) && (Udf <= Uud)) {
+        p = devtwo(ga, enI, pI, rI, enII, pII, rII, cap, status);
+        il = 1; ip = 0;
+    } else if (Udf > Uud) {
+        p = newton(ga, enI, pI, rI, enII, pII, rII, cap, status);
+        il = 1; ip = 1;
+    }
+    if ((il == 1) && (ip == 1)) { /* TWO SHOCKS */
+        double aI = sqrt(rI * (g2 / 2.0 * p + g1 / 2.0 * pI));
+        double aII = sqrt(rII * (g2 / 2.0 * p + g1 / 2.0 * pII));
+        double u = (aI * enI + aII * enII + pI - pII) / (aI + aII);
+        double dI = enI - aI / rI;
+        double dII = enII + aII / rII;
+        *dsl = dI; *dsp = dII; *dsc = u;
+        double UU = dmax(fabs(*dsl), fabs(*dsp));
+        time = (UU > eps8) ? prm->kurant * DIST / UU : prm->kurant * DIST / eps8;
+        if (w <= dI) {
+            en = enI; p = pI; r = rI; te2 = teI2; te3 = teI3;
+        } else if ((w > dI) && (w <= u)) {
+            en = u; r = rI * aI / (aI - rI * (enI - u)); te2 = teI2; te3 = teI3;
+        } else if ((w > u) && (w < dII)) {
+            en = u; r = rII * aII / (aII + rII * (enII - u)); te2 = teII2; te3 = teII3;
+        } else if (w >= dII) {
+            en = enII; p = pII; r = rII; te2 = teII2; te3 = teII3;
+        }
+    }
+    if ((il == 1) && (ip == 0)) { /* LEFT SHOCK, RIGHT EXPANSION */
+        double aI = sqrt(rI * (g2 / 2.0 * p + g1 / 2.0 * pI));
+        double aII;
+        if (fabs(p - pII) < eps) aII = rII * cII;
+        else aII = gm * rII * cII * (1.0 - p / pII) / (1.0 - pow((p / pII), gm));
+        double u = (aI * enI + aII * enII + pI - pII) / (aI + aII);
+        double dI = enI - aI / rI;
+        double dII = enII + cII;
+        double ddII = u + cII - g1 * (enII - u) / 2.0;
+        *dsl = dI; *dsp = dII; *dsc = u;
+        double UU = dmax(fabs(*dsl), fabs(*dsp));
+        UU = dmax(UU, fabs(ddII));
+        time = (UU > eps8) ? prm->kurant * DIST / UU : prm->kurant * DIST / eps8;
+        if (w <= dI) {
+            en = enI; p = pI; r = rI; te2 = teI2; te3 = teI3;
+        }
+        if ((w > dI) && (w <= u)) {
+            en = u; r = rI * aI / (aI - rI * (enI - u)); te2 = teI2; te3 = teI3;
+        }
+        if ((w > u) && (w <= ddII)) {
+            double ce = cII - g1 / 2.0 * (enII - u);
+            en = u; r = ga * p / ce / ce; te2 = teII2; te3 = teII3;
+        }
+        if ((w > ddII) && (w < dII)) {
+            double ce = -g1 / g2 * (enII - w) + 2.0 / g2 * cII;
+            en = w - ce; p = pII * pow((ce / cII), (1.0 / gm)); r = ga * p / ce / ce; te2 = teII2; te3 = teII3;
+        }
+        if (w >= dII) {
+            en = enII; p = pII; r = rII; te2 = teII2; te3 = teII3;
+        }
+    }
+    if ((il == 0) && (ip == 0)) { /* TWO EXPANSION FANS */
+        double aI, aII;
+        if (fabs(p - pI) < eps) aI = rI * cI;
+        else aI = gm * rI * cI * (1.0 - p / pI) / (1.0 - pow((p / pI), gm));
+        if (fabs(p - pII) < eps) aII = rII * cII;
+        else aII = gm * rII * cII * (1.0 - p / pII) / (1.0 - pow((p / pII), gm));
+        double u = (aI * enI + aII * enII + pI - pII) / (aI + aII);
+        double dI = enI - cI;
+        double ddI = u - cI - g1 * (enI - u) / 2.0;
+        double dII = enII + cII;
+        double ddII = u + cII - g1 * (enII - u) / 2.0;
+        *dsl = dI; *dsp = dII; *dsc = u;
+        double UU = dmax(fabs(*dsl), fabs(*dsp));
+        UU = dmax(UU, fabs(ddII));
+        UU = dmax(UU, fabs(ddI));
+        time = (UU > eps8) ? prm->kurant * DIST / UU : prm->kurant * DIST / eps8;
+        if (w <= dI) {
+            en = enI; p = pI; r = rI; te2 = teI2; te3 = teI3;
+        }
+        if ((w > dI) && (w < ddI)) {
+            double ce = g1 / g2 * (enI - w) + 2.0 / g2 * cI;
+            en = w + ce; p = pI * pow((ce / cI), (1.0 / gm)); r = ga * p / ce / ce; te2 = teI2; te3 = teI3;
+        }
+        if ((w >= ddI) && (w <= u)) {
+            double ce = cI + g1 / 2.0 * (enI - u);
+            en = u; r = ga * p / ce / ce; te2 = teI2; te3 = teI3;
+        }
+        if ((w > u) && (w <= ddII)) {
+            double ce = cII - g1 / 2.0 * (enII - u);
+            en = u; r = ga * p / ce / ce; te2 = teII2; te3 = teII3;
+        }
+        if ((w > ddII) && (w < dII)) {
+            double ce = -g1 / g2 * (enII - w) + 2.0 / g2 * cII;
+            en = w - ce; p = pII * pow((ce / cII), (1.0 / gm)); r = ga * p / ce / ce; te2 = teII2; te3 = teII3;
+        }
+        if (w >= dII) {
+            en = enII; p = pII; r = rII; te2 = teII2; te3 = teII3;
+        }
+    }
+    if ((il == -1) && (ip == -1)) { /* VACUUM */
+        double dI = enI - cI;
+        double ddI = enI + 2.0 / gg1 * cI;
+        double dII = enII + cII;
+        double ddII = enII - 2.0 / gg1 * cII;
+        *dsl = dI; *dsp = dII; *dsc = (dI + dII) / 2.0;
+        double UU = dmax(fabs(*dsl), fabs(*dsp));
+        UU = dmax(UU, fabs(ddII));
+        UU = dmax(UU, fabs(ddI));
+        time = (UU > eps8) ? prm->kurant * DIST / UU : prm->kurant * DIST / eps8;
+        if (w <= dI) {
+            en = enI; p = pI; r = rI; te2 = teI2; te3 = teI3;
+        }
+        if ((w > dI) && (w < ddI)) {
+            double ce = gg1 / gg2 * (enI - w) + 2.0 / gg2 * cI;
+            en = w + ce; p = pI * pow((ce / cI), (1.0 / gm)); r = gga * p / ce / ce; te2 = teI2; te3 = teI3;
+        }
+        if ((w >= ddI) && (w <= ddII)) {
+            en = w; p = 0.0; r = 0.0; te2 = 0.0; te3 = 0.0;
+        }
+        if ((w > ddII) && (w < dII)) {
+            double ce = -gg1 / gg2 * (enII - w) + 2.0 / gg2 * cII;
+            en = w - ce; p = pII * pow((ce / cII), (1.0 / gm)); r = gga * p / ce / ce; te2 = teII2; te3 = teII3;
+        }
+        if (w >= dII) {
+            en = enII; p = pII; r = rII; te2 = teII2; te3 = teII3;
+        }
+    }
+    if (ipiz == 1) {
+        en = -en;
+        double dsl1 = *dsl, dsp1 = *dsp;
+        *dsl = -dsp1;
+        *dsp = -dsl1;
+        *dsc = -*dsc;
+        w = -w;
+    }
+    double uo = al * en + al2 * te2 + al3 * te3;
+    double vo = be * en + be2 * te2 + be3 * te3;
+    double wo = ge * en + ge2 * te2 + ge3 * te3;
+    double eo = p / g1 + 0.5 * r * (uo * uo + vo * vo + wo * wo);
+    en = al * uo + be * vo + ge * wo;
+    qqq[0] = (r * (en - w));
+    qqq[1] = (r * (en - w) * uo + al * p);
+    qqq[2] = (r * (en - w) * vo + be * p);
+    qqq[3] = (r * (en - w) * wo + ge * p);
+    qqq[4] = ((en - w) * eo + en * p);
+    return time;
+}
+
+/* ------------------------------------------------------------------ charge-exchange source */
+/* Cell::Get_Sourse_MK1: Cell.cpp:498-665 */
+static void source_mk1(ctx *c, int k, double u, double v, double ro, double p, double *q1, double *q2, double *q3) {
+    const go_params *P = &c->prm;
+    double xx, yy;
+    cell_center(c, k, 0, &xx, &yy);
+    double rr = sqrt(kv(xx) + kv(yy));
+    double uH[4], vH[4], roH[4], pH[4];
+    double ku = c->ku[k], kvv = c->kv_[k], kT = c->kT[k];
+    if (rr > P->src_rmin && rr < P->src_rmax && xx >= 0.0) {
+        int K_do = c->m.cell_back[k], K_posle = c->m.cell_next[k];
+        double r1, r2;
+        if (rr < c->m.r_istoch[k]) {
+            r1 = c->m.r_istoch[k];
+            while (r1 > rr) {
+                if (K_do < 0) { c->status |= 8; *q1 = *q2 = *q3 = 0.0; return; }
+                r1 = c->m.r_istoch[K_do];
+                K_do = c->m.cell_back[K_do];
+            }
+            if (K_do < 0) { c->status |= 8; *q1 = *q2 = *q3 = 0.0; return; }
+            K_do = c->m.cell_next[K_do];
+            K_posle = c->m.cell_next[K_do];
+        } else {
+            r2 = c->m.r_istoch[k];
+            while (r2 < rr) {
+                if (K_posle < 0) { c->status |= 8; *q1 = *q2 = *q3 = 0.0; return; }
+                r2 = c->m.r_istoch[K_posle];
+                K_posle = c->m.cell_next[K_posle];
+            }
+            if (K_posle < 0) { c->status |= 8; *q1 = *q2 = *q3 = 0.0; return; }
+            K_posle = c->m.cell_back[K_posle];
+            K_do = c->m.cell_back[K_posle];
+        }
+        r1 = c->m.r_istoch[K_do];
+        r2 = c->m.r_istoch[K_posle];
+        double TH[4];
+        for (int s = 0; s < 4; s++) uH[s] = linear2(r1, c->Hu[4 * K_do + s], r2, c->Hu[4 * K_posle + s], rr);
+        for (int s = 0; s < 4; s++) vH[s] = linear2(r1, c->Hv[4 * K_do + s], r2, c->Hv[4 * K_posle + s], rr);
+        for (int s = 0; s < 4; s++) roH[s] = linear2(r1, c->Hn[4 * K_do + s], r2, c->Hn[4 * K_posle + s], rr);
+        for (int s = 0; s < 4; s++) TH[s] = linear2(r1, c->HT[4 * K_do + s], r2, c->HT[4 * K_posle + s], rr);
+        ku = linear2(r1, c->ku[K_do], r2, c->ku[K_posle], rr);
+        kvv = linear2(r1, c->kv_[K_do], r2, c->kv_[K_posle], rr);
+        kT = linear2(r1, c->kT[K_do], r2, c->kT[K_posle], rr);
+        for (int s = 0; s < 4; s++) pH[s] = 0.5 * TH[s] * roH[s];
+    } else {
+        for (int s = 0; s < 4; s++) {
+            uH[s] = c->Hu[4 * k + s];
+            vH[s] = c->Hv[4 * k + s];
+            roH[s] = c->Hn[4 * k + s];
+            pH[s] = 0.5 * c->HT[4 * k + s] * c->Hn[4 * k + s];
+        }
+    }
+    for (int s = 0; s < 4; s++)
+        if (roH[s] <= 0.0) {
+            roH[s] = 0.0000001;
+            pH[s] = 0.0;
+        }
+    double UM[4], UH[4], sig[4], nu[4];
+    for (int s = 0; s < 4; s++)
+        UM[s] = sqrt(kv(u - uH[s]) + kv(v - vH[s]) + (64.0 / (9.0 * PI_)) * (p / ro + 2.0 * pH[s] / roH[s]));
+    for (int s = 0; s < 4; s++)
+        UH[s] = sqrt(kv(u - uH[s]) + kv(v - vH[s]) + (4.0 / PI_) * (p / ro + 2.0 * pH[s] / roH[s]));
+    for (int s = 0; s < 4; s++) sig[s] = kv(1.0 - P->a_2 * log(UM[s]));
+    for (int s = 0; s < 4; s++) nu[s] = ro * roH[s] * UM[s] * sig[s];
+    double Mu = P->src_coef * (nu[0] * (uH[0] - u) + nu[1] * (uH[1] - u) + nu[2] * (uH[2] - u) + nu[3] * (uH[3] - u));
+    double Mv = P->src_coef * (nu[0] * (vH[0] - v) + nu[1] * (vH[1] - v) + nu[2] * (vH[2] - v) + nu[3] * (vH[3] - v));
+    double e[4];
+    for (int s = 0; s < 4; s++)
+        e[s] = nu[s] * ((kv(uH[s]) + kv(vH[s]) - kv(u) - kv(v)) / 2.0 + (UH[s] / UM[s]) * (2.0 * pH[s] / roH[s] - p / ro));
+    double MT = P->src_coef * (e[0] + e[1] + e[2] + e[3]);
+    *q1 = Mu * ku;
+    *q2 = Mv * kvv;
+    *q3 = MT * kT;
+}
+
+/* ------------------------------------------------------------------ step forms */
+static void write_state(ctx *c, int k, int buf, double ro, double Q, double p, double u, double v) {
+    c->par[buf][0][k] = ro;
+    c->par[buf][1][k] = p;
+    c->par[buf][2][k] = u;
+    c->par[buf][3][k] = v;
+    c->par[buf][4][k] = Q;
+}
+
+/* Setka::Go_stationary: Setka.cpp:5205-5343 */
+void go_stationary(void *h, int step) {
+    ctx *c = (ctx *)h;
+    const go_params *P = &c->prm;
+    const double ggg = P->gamma, g2 = 2 * P->gamma;
+    int now1 = 1, now2 = 0;
+    double T[2];
+    T[0] = T[1] = P->dt0;
+    for (int st = 0; st < step; st++) {
+        now1 = (now1 + 1) % 2;
+        now2 = (now2 + 1) % 2;
+        double time = 10000000;
+        T[now2] = 100000000;
+        for (int k = 0; k < c->m.n_cells; k++) {
+            double Potok[5] = {0, 0, 0, 0, 0};
+            double Pf[4], PQ = 0.0;
+            st5 par1 = cell_state(c, k, now1);
+            double n1, n2, dist, x, y;
+            cell_center(c, k, 0, &x, &y);
+            double rad = sqrt(kv(x) + kv(y));
+            if (c->m.cell_type[k] == C_CENTR) continue;
+            for (int g = c->m.gran_start[k]; g < c->m.gran_start[k + 1]; g++) {
+                int f = c->m.gran[g];
+                double x2, y2;
+                double S = face_square(c, f);
+                face_center(c, f, 0, &x2, &y2);
+                dist = sqrt(kv(x - x2) + kv(y - y2));
+                st5 par11 = par1;
+                st5 par2 = get_par(c, f, now1);
+                face_normal(c, f, &n1, &n2);
+                double Vc, Vl, Vp;
+                int met = 1;
+                int ft = c->m.face_type[f];
+                if (rad < P->rad_stat && ft == T_USUALY) {
+                    double x3, y3;
+                    cell_center(c, c->m.face_sosed[f], 0, &x3, &y3);
+                    double dd = sqrt(kv(x3) + kv(y3));
+                    par11.ro = par11.ro * kv(rad) / (kv(x2) + kv(y2));
+                    par2.ro = par2.ro * kv(dd) / (kv(x2) + kv(y2));
+                    par11.p = par11.p * pow(rad / sqrt(kv(x2) + kv(y2)), g2);
+                    par2.p = par2.p * pow(dd / sqrt(kv(x2) + kv(y2)), g2);
+                    polar_perenos(x, y, x2, y2, &par11.u, &par11.v, TINY_ANGLE);
+                    polar_perenos(x3, y3, x2, y2, &par2.u, &par2.v, TINY_ANGLE);
+                } else if (ft == T_INNER_SPHERE) {
+                    par11.ro = par11.ro * kv(rad) / (kv(x2) + kv(y2));
+                    par11.p = par11.p * pow(rad / sqrt(kv(x2) + kv(y2)), g2);
+                } else if (rad < P->rad_stat && ft == T_AXIS) {
+                    polar_perenos(x, y, x2, y2, &par11.u, &par11.v, TINY_ANGLE);
+                    par11.v = 0.0;
+                    par2 = par11;
+                } else if (ft == T_AXIS) {
+                    par11.v = 0.0;
+                    par2 = par11;
+                }
+                time = dmin(time, hllc(P, par11.ro, par11.Q, par11.p, par11.u, par11.v, par2.ro, par2.Q, par2.p,
+                                       par2.u, par2.v, 0.0, Pf, &PQ, n1, n2, dist, met, &Vl, &Vc, &Vp, 0));
+                for (int q = 0; q < 4; q++) Potok[q] = Potok[q] + Pf[q] * S;
+                Potok[4] = Potok[4] + PQ * S;
+            }
+            if (time < T[now2]) T[now2] = time;
+            double ro3, p3, u3, v3, Q33;
+            double Volume = cell_volume(c, k, 0);
+            ro3 = par1.ro - T[now1] * (Potok[0] / Volume + par1.ro * par1.v / y);
+            Q33 = par1.Q - (T[now1] / Volume) * Potok[4] - T[now1] * par1.Q * par1.v / y;
+            if (ro3 <= 0) {
+                ro3 = P->ro_floor;
+                c->n_ro_clamp++;
+            }
+            u3 = (par1.ro * par1.u - T[now1] * (Potok[1] / Volume + par1.ro * par1.v * par1.u / y)) / ro3;
+            v3 = (par1.ro * par1.v - T[now1] * (Potok[2] / Volume + par1.ro * par1.v * par1.v / y)) / ro3;
+            p3 = (((par1.p / (ggg - 1) + par1.ro * (par1.u * par1.u + par1.v * par1.v) * 0.5) -
+                   T[now1] * (Potok[3] / Volume +
+                              +par1.v * (ggg * par1.p / (ggg - 1) + par1.ro * (par1.u * par1.u + par1.v * par1.v) * 0.5) / y)) -
+                  0.5 * ro3 * (u3 * u3 + v3 * v3)) *
+                 (ggg - 1);
+            if (p3 <= 0) {
+                p3 = P->p_floor;
+                c->n_p_clamp++;
+            }
+            write_state(c, k, now2, ro3, Q33, p3, u3, v3);
+        }
+    }
+    c->last_dt = T[now2];
+}
+
+/* Setka::Move_surface: Setka.cpp:3378-3844 (including its index quirks:
+ * the averaging loops of the inner and outer shocks walk Line_Contact). */
+void go_move_surface(void *h, int ii, double dt) {
+    ctx *c = (ctx *)h;
+    const go_params *P = &c->prm;
+    const double koef = P->koef, ggg = P->gamma, g2 = 2.0 * P->gamma;
+    const int nC = c->m.n_contact, nI = c->m.n_inner_line, nO = c->m.n_outer_line;
+    const int32_t *LC = c->m.line_contact, *LI = c->m.line_inner, *LO = c->m.line_outer;
+    const int32_t *fA = c->m.face_A, *fB = c->m.face_B;
+    int stt = 0;
+    if (nC > 0) { /* contact, Setka.cpp:3394-3542 */
+        for (int j = 0; j < nC; j++) {
+            int f = LC[j];
+            st5 par1 = {0, 0, 0, 0, 0}, par2 = {0, 0, 0, 0, 0};
+            get_par_tvd(c, f, ii, &par1);
+            int fc = c->m.face_copy[f];
+            get_par_tvd(c, fc, ii, &par2);
+            double n1, n2, nn[3], q1[5], q2[5], qq[5], VV, Vl, Vp;
+            face_normal(c, f, &n1, &n2);
+            nn[0] = n1; nn[1] = n2; nn[2] = 0.0;
+            q1[0] = par1.ro; q1[1] = par1.p; q1[2] = par1.u; q1[3] = par1.v; q1[4] = 0.0;
+            q2[0] = par2.ro; q2[1] = par2.p; q2[2] = par2.u; q2[3] = par2.v; q2[4] = 0.0;
+            godunov(P, q1, q2, nn, qq, &Vl, &Vp, &VV, 0.0, 0.0, &stt);
+            VV = VV * koef * 0.3;
+            int b = fB[f];
+            c->Vx[b] += VV * n1;
+            c->Vy[b] += VV * n2;
+            c->count[b]++;
+        }
+        for (int j = 0; j < nC; j++) {
+            int a = fA[LC[j]];
+            if (c->count[a] > 0) {
+                c->Vx[a] /= (1.0 * c->count[a]);
+                c->Vy[a] /= (1.0 * c->count[a]);
+            }
+        }
+        {
+            int a0 = fA[LC[0]], b0 = fB[LC[0]];
+            c->Vx[a0] = c->Vx[b0] + (c->x[b0] - c->x[a0]) / dt;
+            int a1 = fA[LC[nC - 1]], b1 = fB[LC[nC - 1]];
+            c->Vy[b1] = c->Vy[a1] + (c->y[a1] - c->y[b1]) / dt;
+        }
+    }
+    if (nI > 0) { /* inner shock, Setka.cpp:3545-3738 */
+        for (int j = 0; j < nI; j++) {
+            int f = LI[j];
+            int M = c->m.face_master[f];
+            st5 par1 = cell_state(c, M, ii);
+            double x, y, x2, y2;
+            cell_center(c, M, 0, &x, &y);
+            double radius = sqrt(kv(x) + kv(y));
+            face_center(c, f, 0, &x2, &y2);
+            double dis = sqrt(kv(x2) + kv(y2));
+            int fc = c->m.face_copy[f];
+            st5 par2 = {0, 0, 0, 0, 0};
+            get_par_tvd(c, fc, ii, &par2);
+            double n1, n2, nn[3], q1[5], q2[5], qq[5], VV, Vl, Vp;
+            face_normal(c, f, &n1, &n2);
+            par1.ro = par1.ro * kv(radius) / kv(dis);
+            par1.p = par1.p * pow(radius / dis, g2);
+            polar_perenos(x, y, x2, y2, &par1.u, &par1.v, TINY_ANGLE);
+            nn[0] = n1; nn[1] = n2; nn[2] = 0.0;
+            q1[0] = par1.ro; q1[1] = par1.p; q1[2] = par1.u; q1[3] = par1.v; q1[4] = 0.0;
+            q2[0] = par2.ro; q2[1] = par2.p; q2[2] = par2.u; q2[3] = par2.v; q2[4] = 0.0;
+            godunov(P, q1, q2, nn, qq, &Vl, &Vp, &VV, 0.0, 0.0, &stt);
+            Vl = Vl * koef * 0.1;
+            double t1 = -n2, t2 = n1;
+            int a = fA[f], b = fB[f];
+            if (fabs(par2.u * t1 + par2.v * t2) < 0.1) {
+                c->Vx[a] += Vl * n1;
+                c->Vy[a] += Vl * n2;
+                c->count[a]++;
+                c->Vx[b] += Vl * n1;
+                c->Vy[b] += Vl * n2;
+                c->count[b]++;
+            } else {
+                c->Vx[b] += Vl * n1;
+                c->Vy[b] += Vl * n2;
+                c->count[b]++;
+            }
+        }
+        for (int j = 0; j < nI; j++) { /* walks Line_Contact (Setka.cpp:3718-3731) */
+            int a = fA[LC[j]];
+            if (c->count[a] > 0) {
+                c->Vx[a] /= (1.0 * c->count[a]);
+                c->Vy[a] /= (1.0 * c->count[a]);
+            }
+        }
+        {
+            int a0 = fA[LI[0]], b0 = fB[LI[0]];
+            c->Vx[a0] = c->Vx[b0] + (c->x[b0] - c->x[a0]) / dt;
+            int a1 = fA[LI[nI - 1]], b1 = fB[LI[nI - 1]];
+            c->Vx[b1] = c->Vx[a1] + (c->x[a1] - c->x[b1]) / dt;
+        }
+    }
+    if (nO > 0) { /* outer shock, Setka.cpp:3741-3843 */
+        const int lim = P->n_outer_shock + c->m.dims[0] + c->m.dims[1] + 1;
+        for (int j = 0; j < nO; j++) {
+            if (j >= lim) continue;
+            int f = LO[j];
+            st5 par1 = {0, 0, 0, 0, 0}, par2 = {0, 0, 0, 0, 0};
+            get_par_tvd(c, f, ii, &par1);
+            int fc = c->m.face_copy[f];
+            get_par_tvd(c, fc, ii, &par2);
+            double n1, n2, nn[3], q1[5], q2[5], qq[5], VV, Vl, Vp;
+            face_normal(c, f, &n1, &n2);
+            nn[0] = n1; nn[1] = n2; nn[2] = 0.0;
+            q1[0] = par1.ro; q1[1] = par1.p; q1[2] = par1.u; q1[3] = par1.v; q1[4] = 0.0;
+            q2[0] = par2.ro; q2[1] = par2.p; q2[2] = par2.u; q2[3] = par2.v; q2[4] = 0.0;
+            godunov(P, q1, q2, nn, qq, &Vl, &Vp, &VV, 0.0, 0.0, &stt);
+            Vp = Vp * koef;
+            double t1 = -n2, t2 = n1;
+            int a = fA[f], b = fB[f];
+            if ((kv(par1.u) + kv(par1.v) + kv(0.0)) / (ggg * par1.p / par1.ro) > 1.0) {
+                c->Vx[b] += Vp * n1;
+                c->Vy[b] += Vp * n2;
+                c->count[b]++;
+            } else {
+                if (fabs(par1.u * t1 + par1.v * t2) < 0.01) {
+                    c->Vx[a] += Vp * n1;
+                    c->Vy[a] += Vp * n2;
+                    c->count[a]++;
+                    c->Vx[b] += Vp * n1;
+                    c->Vy[b] += Vp * n2;
+                    c->count[b]++;
+                } else if (par1.u * t1 + par1.v * t2 > 0) {
+                    c->Vx[b] += Vp * n1;
+                    c->Vy[b] += Vp * n2;
+                    c->count[b]++;
+                } else {
+                    c->Vx[a] += Vp * n1;
+                    c->Vy[a] += Vp * n2;
+                    c->count[a]++;
+                }
+            }
+        }
+        for (int j = 0; j < nO; j++) { /* walks Line_Contact (Setka.cpp:3829-3837) */
+            int a = fA[LC[j]];
+            if (c->count[a] > 0) {
+                c->Vx[a] /= (1.0 * c->count[a]);
+                c->Vy[a] /= (1.0 * c->count[a]);
+            }
+        }
+        {
+            int a0 = fA[LO[0]], b0 = fB[LO[0]];
+            c->Vx[a0] = c->Vx[b0] + (c->x[b0] - c->x[a0]) / dt;
+            int a1 = fA[LO[nO - 1]], b1 = fB[LO[nO - 1]];
+            c->Vy[b1] = c->Vy[a1] + (c->y[a1] - c->y[b1]) / dt;
+        }
+    }
+    if (stt) c->status |= stt;
+}
+
+/* Setka::Move_Setka_Calculate_2: Setka.cpp:4324-4759 */
+void go_move_setka2(void *h, double dt) {
+    ctx *c = (ctx *)h;
+    const go_params *P = &c->prm;
+    const int ni = P->n_inner;
+    const double R1 = P->R1, R111 = P->R111, R5 = P->R5;
+    double *X = c->x, *Y = c->y, *X2 = c->x2, *Y2 = c->y2;
+    double V, R2, R3, R4, r, x;
+    for (int q = 0; q < c->m.n_rails; q++) {
+        const int32_t *ap = c->m.rail_points + c->m.rail_pstart[q];
+        const int32_t *kp = c->m.rail_keys + c->m.rail_kstart[q];
+        const int np = c->m.rail_pstart[q + 1] - c->m.rail_pstart[q];
+        const int M1 = c->m.rail_M[4 * q], M2 = c->m.rail_M[4 * q + 1], M3 = c->m.rail_M[4 * q + 2],
+                  M4 = c->m.rail_M[4 * q + 3];
+        const double s = c->m.rail_s[q];
+        const int t = c->m.rail_type[q];
+        if (t == R_A) { /* Setka.cpp:4331-4457 */
+            for (int kk = 0; kk < 3; kk++) {
+                int K = kp[kk];
+                V = c->Vx[K] * cos(s) + c->Vy[K] * sin(s);
+                X2[K] = X[K] + dt * V * cos(s);
+                Y2[K] = Y[K] + dt * V * sin(s);
+            }
+            X2[kp[3]] = X[kp[3]];
+            Y2[kp[3]] = Y[kp[3]];
+            R2 = sqrt(kv(X2[kp[0]]) + kv(Y2[kp[0]]));
+            for (int j = 0; j < ni; j++) {
+                x = j * 1.0 / (ni);
+                r = R1 + pow(x, 1.3) * (R111 - R1);
+                X2[ap[j]] = r * cos(s);
+                Y2[ap[j]] = r * sin(s);
+            }
+            for (int j = ni; j < M1 - 1; j++) {
+                x = (j - ni) * 1.0 / (M1 - 1 - ni);
+                r = R111 + pow(x, 1.05) * (R2 - R111);
+                X2[ap[j]] = r * cos(s);
+                Y2[ap[j]] = r * sin(s);
+            }
+            R3 = sqrt(kv(X2[kp[1]]) + kv(Y2[kp[1]]));
+            for (int j = 0; j < M2 - 1; j++) {
+                r = R2 + (R3 - R2) * (j + 1) / (M2);
+                X2[ap[M1 + j]] = r * cos(s);
+                Y2[ap[M1 + j]] = r * sin(s);
+            }
+            R3 = sqrt(kv(X2[kp[1]]) + kv(Y2[kp[1]]));
+            R4 = sqrt(kv(X2[kp[2]]) + kv(Y2[kp[2]]));
+            for (int j = 0; j < M3 - 1; j++) {
+                r = R3 + (R4 - R3) * (j + 1) / (M3);
+                X2[ap[M1 + M2 + j]] = r * cos(s);
+                Y2[ap[M1 + M2 + j]] = r * sin(s);
+            }
+            R4 = sqrt(kv(X2[kp[2]]) + kv(Y2[kp[2]]));
+            for (int j = 0; j < M4; j++) {
+                x = (j + 1) * 1.0 / (M4);
+                double dd = 1.5708 / sqrt(1.0 - 1.0 / 1.76);
+                r = R4 + pow(x, 1.76 * (1.0 - kv(s / dd))) * (R5 - R4);
+                X2[ap[M1 + M2 + M3 + j]] = r * cos(s);
+                Y2[ap[M1 + M2 + M3 + j]] = r * sin(s);
+            }
+        } else if (t == R_B) { /* Setka.cpp:4467-4595 */
+            int K0 = kp[0], K1 = kp[1], K2 = kp[2], K3 = kp[3];
+            V = c->Vx[K0] * cos(s) + c->Vy[K0] * sin(s);
+            X2[K0] = X[K0] + dt * V * cos(s);
+            Y2[K0] = Y[K0] + dt * V * sin(s);
+            V = c->Vx[K1] * 0.0 + c->Vy[K1] * 1.0;
+            X2[K1] = X2[K0];
+            Y2[K1] = Y[K1] + dt * V;
+            V = c->Vx[K2] * 0.0 + c->Vy[K2] * 1.0;
+            X2[K2] = X2[K0];
+            Y2[K2] = Y[K2] + dt * V;
+            X2[K3] = X2[K0];
+            Y2[K3] = Y[K3];
+            R2 = sqrt(kv(X2[K0]) + kv(Y2[K0]));
+            for (int j = 0; j < ni; j++) {
+                x = j * 1.0 / (ni);
+                r = R1 + pow(x, 1.3) * (R111 - R1);
+                X2[ap[j]] = r * cos(s);
+                Y2[ap[j]] = r * sin(s);
+            }
+            for (int j = ni; j < M1 - 1; j++) {
+                x = (j - ni) * 1.0 / (M1 - 1 - ni);
+                r = R111 + pow(x, 1.05) * (R2 - R111);
+                X2[ap[j]] = r * cos(s);
+                Y2[ap[j]] = r * sin(s);
+            }
+            R2 = Y2[K0];
+            R3 = Y2[K1];
+            for (int j = 0; j < M2 - 1; j++) {
+                r = R2 + (R3 - R2) * (j + 1) / (M2);
+                X2[ap[M1 + j]] = X2[K0];
+                Y2[ap[M1 + j]] = r;
+            }
+            R3 = Y2[K1];
+            R4 = Y2[K2];
+            for (int j = 0; j < M3 - 1; j++) {
+                r = R3 + (R4 - R3) * (j + 1) / (M3);
+                X2[ap[M1 + M2 + j]] = X2[K0];
+                Y2[ap[M1 + M2 + j]] = r;
+            }
+            for (int j = 0; j < M4; j++) {
+                r = R4 + (R5 - R4) * (j + 1) / (M4);
+                X2[ap[M1 + M2 + M3 + j]] = X2[K0];
+                Y2[ap[M1 + M2 + M3 + j]] = r;
+            }
+        } else if (t == R_C) { /* Setka.cpp:4597-4674 */
+            int K0 = kp[0], K1 = kp[1];
+            V = c->Vx[K0] * cos(s) + c->Vy[K0] * sin(s);
+            X2[K0] = X[K0] + dt * V * cos(s);
+            Y2[K0] = Y[K0] + dt * V * sin(s);
+            X2[K1] = P->Left;
+            Y2[K1] = Y[K1];
+            R2 = sqrt(kv(X2[K0]) + kv(Y2[K0]));
+            for (int j = 0; j < ni; j++) {
+                x = j * 1.0 / (ni);
+                r = R1 + pow(x, 1.3) * (R111 - R1);
+                X2[ap[j]] = r * cos(s);
+                Y2[ap[j]] = r * sin(s);
+            }
+            for (int j = ni; j < M1 - 1; j++) {
+                x = (j - ni) * 1.0 / (M1 - 1 - ni);
+                r = R111 + pow(x, 1.05) * (R2 - R111);
+                X2[ap[j]] = r * cos(s);
+                Y2[ap[j]] = r * sin(s);
+            }
+            R2 = X2[K0];
+            R3 = X2[K1];
+            x = pow(R3 / (R2), 1.0 / (M2));
+            for (int j = M1; j < np; j++) {
+                r = R2 * pow(x, j + 1 - M1);
+                X2[ap[j]] = r;
+                Y2[ap[j]] = Y2[K0];
+            }
+        }
+    }
+    /* D rails after all C rails: Setka.cpp:4676-4758 */
+    const int sM2 = c->m.dims[5], sM3 = c->m.dims[6], sM4 = c->m.dims[7];
+    int jj = 0;
+    int prev_k2 = -1;
+    for (int q = 0; q < c->m.n_rails; q++) {
+        if (c->m.rail_type[q] != R_D) continue;
+        const int32_t *ap = c->m.rail_points + c->m.rail_pstart[q];
+        const int32_t *kp = c->m.rail_keys + c->m.rail_kstart[q];
+        const int M2 = c->m.rail_M[4 * q + 1], M3 = c->m.rail_M[4 * q + 2], M4 = c->m.rail_M[4 * q + 3];
+        int K0 = kp[0], K1 = kp[1], K2 = kp[2], K3 = kp[3];
+        V = c->Vy[K1];
+        X2[K1] = X2[K0];
+        Y2[K1] = Y[K1] + dt * V;
+        V = c->Vy[K2];
+        X2[K2] = X2[K0];
+        Y2[K2] = Y[K2] + dt * V;
+        if (jj >= P->n_outer_shock) Y2[K2] = Y2[prev_k2];
+        X2[K3] = X2[K0];
+        Y2[K3] = Y[K3];
+        R2 = Y2[K0];
+        R3 = Y2[K1];
+        for (int j = 0; j < sM2 - 1; j++) {
+            r = R2 + (R3 - R2) * (j + 1) / (M2);
+            X2[ap[j + 1]] = X2[K0];
+            Y2[ap[j + 1]] = r;
+        }
+        R3 = Y2[K1];
+        R4 = Y2[K2];
+        for (int j = 0; j < sM3 - 1; j++) {
+            r = R3 + (R4 - R3) * (j + 1) / (M3);
+            X2[ap[sM2 + j + 1]] = X2[K0];
+            Y2[ap[sM2 + j + 1]] = r;
+        }
+        for (int j = 0; j < sM4; j++) {
+            r = R4 + (R5 - R4) * (j + 1) / (M4);
+            X2[ap[sM2 + sM3 + j + 1]] = X2[K0];
+            Y2[ap[sM2 + sM3 + j + 1]] = r;
+        }
+        prev_k2 = K2;
+        jj++;
+    }
+}
+
+void go_commit_points(void *h) {
+    ctx *c = (ctx *)h;
+    for (int i = 0; i < c->m.n_points; i++) {
+        c->x[i] = c->x2[i];
+        c->y[i] = c->y2[i];
+        c->Vx[i] = 0.0;
+        c->Vy[i] = 0.0;
+        c->count[i] = 0;
+    }
+}
+
+static int face_np_flag(const ctx *c, int f) { /* Setka.cpp:10301-10324 */
+    int ta = c->m.point_type[c->m.face_A[f]], tb = c->m.point_type[c->m.face_B[f]];
+    if (ta == P_CONTACT && tb != P_CONTACT) return 1;
+    if (ta != P_CONTACT && tb == P_CONTACT) return 1;
+    if (ta == P_INNER_SHOCK && tb != P_INNER_SHOCK) return 1;
+    if (ta != P_INNER_SHOCK && tb == P_INNER_SHOCK) return 1;
+    if (ta == P_OUTER_SHOCK && tb != P_OUTER_SHOCK) return 1;
+    if (ta != P_OUTER_SHOCK && tb == P_OUTER_SHOCK) return 1;
+    return 0;
+}
+
+/* Setka::Go_5_komponent__MK2: Setka.cpp:10121-10482 */
+void go_mk2(void *h, int step) {
+    ctx *c = (ctx *)h;
+    const go_params *P = &c->prm;
+    const double ggg = P->gamma, g2 = 2 * P->gamma;
+    int now1 = 1, now2 = 0;
+    double T[2];
+    T[0] = T[1] = P->dt0;
+    for (int st = 0; st < step; st++) {
+        now1 = (now1 + 1) % 2;
+        now2 = (now2 + 1) % 2;
+        double time = 10000000;
+        T[now2] = 100000000;
+        go_move_surface(c, now1, T[now1]);
+        go_move_setka2(c, T[now1]);
+        for (int k = 0; k < c->m.n_cells; k++) {
+            double Potok[5] = {0, 0, 0, 0, 0};
+            double Pf[4], PQ = 0.0;
+            st5 par1 = cell_state(c, k, now1);
+            double n1, n2, dist, x, y;
+            cell_center(c, k, 0, &x, &y);
+            double vs1 = cell_volume(c, k, 0);
+            double vs2 = cell_volume(c, k, 1);
+            double radius = sqrt(kv(x) + kv(y));
+            if (radius < P->R11) continue;
+            double Volume = cell_volume_rotate(c, k, 0, 360.0) / (2.0 * PI_);
+            double Volume2 = cell_volume_rotate(c, k, 1, 360.0) / (2.0 * PI_);
+            double W = 0.0;
+            int np = 1;
+            const int kt = c->m.cell_type[k];
+            for (int g = c->m.gran_start[k]; g < c->m.gran_start[k + 1]; g++) {
+                int f = c->m.gran[g];
+                double x2, y2, x4, y4;
+                double S = face_square(c, f) * (c->y[c->m.face_A[f]] + c->y[c->m.face_B[f]]) * 0.5;
+                face_center(c, f, 0, &x2, &y2);
+                face_center(c, f, 1, &x4, &y4);
+                dist = sqrt(kv(x - x2) + kv(y - y2));
+                st5 par11 = par1;
+                st5 par2 = get_par(c, f, now1);
+                face_normal(c, f, &n1, &n2);
+                double Vc, Vl, Vp;
+                W = ((x4 - x2) * n1 + (y4 - y2) * n2) / T[now1];
+                int met = 0;
+                double dis = sqrt(kv(x2) + kv(y2));
+                int ft = c->m.face_type[f];
+                if (ft == T_USUALY) {
+                    int So = c->m.face_sosed[f];
+                    double x3, y3;
+                    cell_center(c, So, 0, &x3, &y3);
+                    double dd = sqrt(kv(x3) + kv(y3));
+                    if (kt == C_1) {
+                        par11.ro = par11.ro * kv(radius) / kv(dis);
+                        par11.Q = par11.Q * kv(radius) / kv(dis);
+                        par11.p = par11.p * pow(radius / dis, g2);
+                        polar_perenos(x, y, x2, y2, &par11.u, &par11.v, TINY_ANGLE);
+                        double pro, pp;
+                        get_par_tvd_radial(c, f, now1, &pro, &pp);
+                        par11.ro = pro;
+                        par11.p = pp;
+                    } else {
+                        get_par_tvd(c, f, now1, &par11);
+                    }
+                    int fc = c->m.face_copy[f];
+                    if (c->m.cell_type[So] == C_1) {
+                        par2.ro = par2.ro * kv(dd) / kv(dis);
+                        par2.Q = par2.Q * kv(dd) / kv(dis);
+                        par2.p = par2.p * pow(dd / dis, g2);
+                        polar_perenos(x3, y3, x2, y2, &par2.u, &par2.v, TINY_ANGLE);
+                        double pro, pp;
+                        get_par_tvd_radial(c, fc, now1, &pro, &pp);
+                        par2.ro = pro;
+                        par2.p = pp;
+                    } else {
+                        get_par_tvd(c, fc, now1, &par2);
+                    }
+                } else if (ft == T_INNER_SPHERE) {
+                    par11.ro = par11.ro * kv(radius) / kv(dis);
+                    par11.Q = par11.Q * kv(radius) / kv(dis);
+                    par11.p = par11.p * pow(radius / dis, g2);
+                } else if (kt == C_1 && ft == T_AXIS) {
+                    par11.ro = par11.ro * kv(radius) / kv(dis);
+                    par11.Q = par11.Q * kv(radius) / kv(dis);
+                    par11.p = par11.p * pow(radius / dis, g2);
+                    polar_perenos(x, y, x2, y2, &par11.u, &par11.v, TINY_ANGLE);
+                    par2 = par11;
+                    par2.v = -par2.v;
+                } else if (kt != C_1 && ft == T_AXIS) {
+                    get_par_tvd(c, f, now1, &par11);
+                    par2 = par11;
+                    par2.v = -par2.v;
+                }
+                np = face_np_flag(c, f);
+                int god = is_tracked_face(c, f);
+                if (god) {
+                    double Vl2, Vp2, VV, nn[3], q1[5], q2[5], qq[5];
+                    nn[0] = n1; nn[1] = n2; nn[2] = 0.0;
+                    q1[0] = par11.ro; q1[1] = par11.p; q1[2] = par11.u; q1[3] = par11.v; q1[4] = 0.0;
+                    q2[0] = par2.ro; q2[1] = par2.p; q2[2] = par2.u; q2[3] = par2.v; q2[4] = 0.0;
+                    int stt = 0;
+                    time = dmin(time, godunov(P, q1, q2, nn, qq, &Vl2, &Vp2, &VV, W, dist, &stt));
+                    c->status |= stt;
+                    Potok[0] = Potok[0] + qq[0] * S;
+                    Potok[1] = Potok[1] + qq[1] * S;
+                    Potok[2] = Potok[2] + qq[2] * S;
+                    Potok[3] = Potok[3] + qq[4] * S;
+                    time = dmin(time, hllc(P, par11.ro, par11.Q, par11.p, par11.u, par11.v, par2.ro, par2.Q, par2.p,
+                                           par2.u, par2.v, W, Pf, &PQ, n1, n2, dist, met, &Vl, &Vc, &Vp, np));
+                    Potok[4] = Potok[4] + PQ * S;
+                } else {
+                    time = dmin(time, hllc(P, par11.ro, par11.Q, par11.p, par11.u, par11.v, par2.ro, par2.Q, par2.p,
+                                           par2.u, par2.v, W, Pf, &PQ, n1, n2, dist, met, &Vl, &Vc, &Vp, np));
+                    for (int q = 0; q < 4; q++) Potok[q] = Potok[q] + Pf[q] * S;
+                    Potok[4] = Potok[4] + PQ * S;
+                }
+            }
+            if (time < T[now2]) T[now2] = time;
+            double u = par1.u, v = par1.v, ro = par1.ro, p = par1.p, Q = par1.Q;
+            double q2_1, q2_2, q3;
+            source_mk1(c, k, u, v, ro, p, &q2_1, &q2_2, &q3);
+            double ro3, Q33, u3, v3, p3;
+            if (kt != C_CENTR) {
+                ro3 = ro * Volume / Volume2 - T[now1] * (Potok[0] / Volume2);
+                Q33 = Q * Volume / Volume2 - (T[now1] / Volume2) * Potok[4];
+                if (ro3 <= 0.0) {
+                    ro3 = P->ro_floor;
+                    c->n_ro_clamp++;
+                }
+                u3 = (ro * u * Volume / Volume2 - T[now1] * (Potok[1] / Volume2 - q2_1)) / ro3;
+                v3 = (ro * v * Volume / Volume2 - T[now1] * ((Potok[2] - p * 0.5 * (vs1 + vs2)) / Volume2 - q2_2)) / ro3;
+                p3 = (((p / (ggg - 1) + ro * (u * u + v * v) * 0.5) * Volume / Volume2 -
+                       T[now1] * (Potok[3] / Volume2 - q3)) -
+                      0.5 * ro3 * (u3 * u3 + v3 * v3)) *
+                     (ggg - 1);
+                if (p3 <= 0) {
+                    p3 = P->p_floor;
+                    c->n_p_clamp++;
+                }
+                write_state(c, k, now2, ro3, Q33, p3, u3, v3);
+            } else {
+                st5 s = cell_state(c, k, now1);
+                write_state(c, k, now2, s.ro, s.Q, s.p, s.u, s.v);
+            }
+        }
+        go_commit_points(c);
+    }
+    c->last_dt = T[now2];
+}
+
+/* Setka::Go_stationary_5_komponent_inner_MK2: Setka.cpp:6999-7212 */
+void go_inner_mk2(void *h, int step) {
+    ctx *c = (ctx *)h;
+    const go_params *P = &c->prm;
+    const double ggg = P->gamma, g2 = 2.0 * P->gamma;
+    int now1 = 1, now2 = 0;
+    double T[2];
+    T[0] = T[1] = P->dt0;
+    for (int st = 0; st < step; st++) {
+        now1 = (now1 + 1) % 2;
+        now2 = (now2 + 1) % 2;
+        double time = 10000000;
+        T[now2] = 100000000;
+        for (int ic = 0; ic < c->n_inner_cells; ic++) {
+            int k = c->inner[ic];
+            const int kt = c->m.cell_type[k];
+            if (kt == C_CENTR) continue;
+            double Potok[5] = {0, 0, 0, 0, 0};
+            double Pf[4], PQ = 0.0;
+            st5 par1 = cell_state(c, k, now1);
+            double n1, n2, dist, x, y;
+            cell_center(c, k, 0, &x, &y);
+            double vs1 = cell_volume(c, k, 0);
+            double vs2 = cell_volume(c, k, 1);
+            double radius = sqrt(kv(x) + kv(y));
+            double Volume = cell_volume_rotate(c, k, 0, 360.0) / (2.0 * PI_);
+            for (int g = c->m.gran_start[k]; g < c->m.gran_start[k + 1]; g++) {
+                int f = c->m.gran[g];
+                double x2, y2;
+                double S = face_square(c, f) * (c->y[c->m.face_A[f]] + c->y[c->m.face_B[f]]) * 0.5;
+                face_center(c, f, 0, &x2, &y2);
+                dist = sqrt(kv(x - x2) + kv(y - y2));
+                st5 par11 = par1;
+                st5 par2 = get_par(c, f, now1);
+                face_normal(c, f, &n1, &n2);
+                double Vc, Vl, Vp;
+                int met = 1;
+                double dis = sqrt(kv(x2) + kv(y2));
+                int ft = c->m.face_type[f];
+                if (ft == T_USUALY) {
+                    int So = c->m.face_sosed[f];
+                    double x3, y3;
+                    cell_center(c, So, 0, &x3, &y3);
+                    double dd = sqrt(kv(x3) + kv(y3));
+                    par11.ro = par11.ro * kv(radius) / kv(dis);
+                    par2.ro = par2.ro * kv(dd) / kv(dis);
+                    par11.Q = par11.Q * kv(radius) / kv(dis);
+                    par2.Q = par2.Q * kv(dd) / kv(dis);
+                    par11.p = par11.p * pow(radius / dis, g2);
+                    par2.p = par2.p * pow(dd / dis, g2);
+                    polar_perenos(x, y, x2, y2, &par11.u, &par11.v, TINY_ANGLE);
+                    polar_perenos(x3, y3, x2, y2, &par2.u, &par2.v, TINY_ANGLE);
+                    if (kt == C_1 && c->m.cell_type[So] == C_1) {
+                        double r1, p1, r2, p2;
+                        get_par_tvd_radial(c, f, now1, &r1, &p1);
+                        get_par_tvd_radial(c, c->m.face_copy[f], now1, &r2, &p2);
+                        par11.ro = r1;
+                        par2.ro = r2;
+                        par11.p = p1;
+                        par2.p = p2;
+                    }
+                } else if (ft == T_INNER_SPHERE) {
+                    par11 = par2;
+                } else if (ft == T_AXIS) {
+                    par11.ro = par11.ro * kv(radius) / kv(dis);
+                    par11.Q = par11.Q * kv(radius) / kv(dis);
+                    par11.p = par11.p * pow(radius / dis, g2);
+                    polar_perenos(x, y, x2, y2, &par11.u, &par11.v, TINY_ANGLE);
+                    par2 = par11;
+                    par2.v = -par2.v;
+                    met = 0;
+                }
+                time = dmin(time, hllc(P, par11.ro, par11.Q, par11.p, par11.u, par11.v, par2.ro, par2.Q, par2.p,
+                                       par2.u, par2.v, 0.0, Pf, &PQ, n1, n2, dist, met, &Vl, &Vc, &Vp, 0));
+                for (int q = 0; q < 4; q++) Potok[q] = Potok[q] + Pf[q] * S;
+                Potok[4] = Potok[4] + PQ * S;
+            }
+            if (time < T[now2]) T[now2] = time;
+            double u = par1.u, v = par1.v, ro = par1.ro, p = par1.p, Q = par1.Q;
+            double q2_1, q2_2, q3;
+            source_mk1(c, k, u, v, ro, p, &q2_1, &q2_2, &q3);
+            double ro3, Q33, u3, v3, p3;
+            ro3 = ro - T[now1] * (Potok[0] / Volume);
+            Q33 = Q - (T[now1] / Volume) * Potok[4] - T[now1];
+            if (ro3 <= 0) {
+                ro3 = P->ro_floor;
+                c->n_ro_clamp++;
+            }
+            u3 = (ro * u - T[now1] * (Potok[1] / Volume - q2_1)) / ro3;
+            v3 = (ro * v - T[now1] * ((Potok[2] - p * 0.5 * (vs1 + vs2)) / Volume - q2_2)) / ro3;
+            p3 = (((p / (ggg - 1) + ro * (u * u + v * v) * 0.5) - T[now1] * (Potok[3] / Volume - q3)) -
+                  0.5 * ro3 * (u3 * u3 + v3 * v3)) *
+                 (ggg - 1);
+            if (p3 <= 0) {
+                p3 = P->p_floor;
+                c->n_p_clamp++;
+            }
+            write_state(c, k, now2, ro3, Q33, p3, u3, v3);
+        }
+    }
+    c->last_dt = T[now2];
+}
+
+/* ------------------------------------------------------------------ lifecycle */
+static void *dup(const void *src, size_t bytes) {
+    void *p = malloc(bytes ? bytes : 1);
+    if (src && bytes) memcpy(p, src, bytes);
+    else memset(p, 0, bytes ? bytes : 1);
+    return p;
+}
+
+void *go_create(const go_params *prm, const go_mesh *m) {
+    ctx *c = (ctx *)calloc(1, sizeof(ctx));
+    c->prm = *prm;
+    c->m = *m;
+    const int np = m->n_points, nc = m->n_cells, nf = m->n_faces;
+    const int nct = m->contour_start[nc], ngt = m->gran_start[nc];
+    c->m.point_type = (const int32_t *)dup(m->point_type, sizeof(int32_t) * np);
+    c->m.cell_type = (const int32_t *)dup(m->cell_type, sizeof(int32_t) * nc);
+    c->m.contour_start = (const int32_t *)dup(m->contour_start, sizeof(int32_t) * (nc + 1));
+    c->m.contour = (const int32_t *)dup(m->contour, sizeof(int32_t) * nct);
+    c->m.gran_start = (const int32_t *)dup(m->gran_start, sizeof(int32_t) * (nc + 1));
+    c->m.gran = (const int32_t *)dup(m->gran, sizeof(int32_t) * ngt);
+    c->m.cell_back = (const int32_t *)dup(m->cell_back, sizeof(int32_t) * nc);
+    c->m.cell_next = (const int32_t *)dup(m->cell_next, sizeof(int32_t) * nc);
+    c->m.r_istoch = (const double *)dup(m->r_istoch, sizeof(double) * nc);
+    c->m.face_A = (const int32_t *)dup(m->face_A, sizeof(int32_t) * nf);
+    c->m.face_B = (const int32_t *)dup(m->face_B, sizeof(int32_t) * nf);
+    c->m.face_type = (const int32_t *)dup(m->face_type, sizeof(int32_t) * nf);
+    c->m.face_master = (const int32_t *)dup(m->face_master, sizeof(int32_t) * nf);
+    c->m.face_sosed = (const int32_t *)dup(m->face_sosed, sizeof(int32_t) * nf);
+    c->m.face_copy = (const int32_t *)dup(m->face_copy, sizeof(int32_t) * nf);
+    c->m.face_sosed_up = (const int32_t *)dup(m->face_sosed_up, sizeof(int32_t) * nf);
+    c->m.face_sosed_down = (const int32_t *)dup(m->face_sosed_down, sizeof(int32_t) * nf);
+    const int nr = m->n_rails;
+    c->m.rail_type = (const int32_t *)dup(m->rail_type, sizeof(int32_t) * nr);
+    c->m.rail_s = (const double *)dup(m->rail_s, sizeof(double) * nr);
+    c->m.rail_M = (const int32_t *)dup(m->rail_M, sizeof(int32_t) * 4 * nr);
+    c->m.rail_pstart = (const int32_t *)dup(m->rail_pstart, sizeof(int32_t) * (nr + 1));
+    c->m.rail_kstart = (const int32_t *)dup(m->rail_kstart, sizeof(int32_t) * (nr + 1));
+    c->m.rail_points = (const int32_t *)dup(m->rail_points, sizeof(int32_t) * (nr ? m->rail_pstart[nr] : 0));
+    c->m.rail_keys = (const int32_t *)dup(m->rail_keys, sizeof(int32_t) * (nr ? m->rail_kstart[nr] : 0));
+    c->m.line_contact = (const int32_t *)dup(m->line_contact, sizeof(int32_t) * m->n_contact);
+    c->m.line_inner = (const int32_t *)dup(m->line_inner, sizeof(int32_t) * m->n_inner_line);
+    c->m.line_outer = (const int32_t *)dup(m->line_outer, sizeof(int32_t) * m->n_outer_line);
+    c->x = (double *)dup(m->x, sizeof(double) * np);
+    c->y = (double *)dup(m->y, sizeof(double) * np);
+    c->x2 = (double *)dup(m->x, sizeof(double) * np);
+    c->y2 = (double *)dup(m->y, sizeof(double) * np);
+    c->Vx = (double *)dup(NULL, sizeof(double) * np);
+    c->Vy = (double *)dup(NULL, sizeof(double) * np);
+    c->count = (int32_t *)dup(NULL, sizeof(int32_t) * np);
+    for (int b = 0; b < 2; b++)
+        for (int q = 0; q < 5; q++) c->par[b][q] = (double *)dup(NULL, sizeof(double) * nc);
+    c->Hn = (double *)dup(NULL, sizeof(double) * 4 * nc);
+    c->Hu = (double *)dup(NULL, sizeof(double) * 4 * nc);
+    c->Hv = (double *)dup(NULL, sizeof(double) * 4 * nc);
+    c->HT = (double *)dup(NULL, sizeof(double) * 4 * nc);
+    c->ku = (double *)dup(NULL, sizeof(double) * nc);
+    c->kv_ = (double *)dup(NULL, sizeof(double) * nc);
+    c->kT = (double *)dup(NULL, sizeof(double) * nc);
+    c->inner = (int32_t *)dup(NULL, sizeof(int32_t));
+    return c;
+}
+
+void go_destroy(void *h) {
+    ctx *c = (ctx *)h;
+    if (!c) return;
+    free((void *)c->m.point_type); free((void *)c->m.cell_type); free((void *)c->m.contour_start);
+    free((void *)c->m.contour); free((void *)c->m.gran_start); free((void *)c->m.gran);
+    free((void *)c->m.cell_back); free((void *)c->m.cell_next); free((void *)c->m.r_istoch);
+    free((void *)c->m.face_A); free((void *)c->m.face_B); free((void *)c->m.face_type);
+    free((void *)c->m.face_master); free((void *)c->m.face_sosed); free((void *)c->m.face_copy);
+    free((void *)c->m.face_sosed_up); free((void *)c->m.face_sosed_down);
+    free((void *)c->m.rail_type); free((void *)c->m.rail_s); free((void *)c->m.rail_M);
+    free((void *)c->m.rail_pstart); free((void *)c->m.rail_kstart); free((void *)c->m.rail_points);
+    free((void *)c->m.rail_keys); free((void *)c->m.line_contact); free((void *)c->m.line_inner);
+    free((void *)c->m.line_outer);
+    free(c->x); free(c->y); free(c->x2); free(c->y2); free(c->Vx); free(c->Vy); free(c->count);
+    for (int b = 0; b < 2; b++)
+        for (int q = 0; q < 5; q++) free(c->par[b][q]);
+    free(c->Hn); free(c->Hu); free(c->Hv); free(c->HT); free(c->ku); free(c->kv_); free(c->kT);
+    free(c->inner);
+    free(c);
+}
+
+void go_set_state(void *h, int buf, const double *ro, const double *p, const double *u, const double *v,
+                  const double *Q) {
+    ctx *c = (ctx *)h;
+    size_t n = sizeof(double) * c->m.n_cells;
+    memcpy(c->par[buf][0], ro, n);
+    memcpy(c->par[buf][1], p, n);
+    memcpy(c->par[buf][2], u, n);
+    memcpy(c->par[buf][3], v, n);
+    memcpy(c->par[buf][4], Q, n);
+}
+
+void go_get_state(void *h, int buf, double *ro, double *p, double *u, double *v, double *Q) {
+    ctx *c = (ctx *)h;
+    size_t n = sizeof(double) * c->m.n_cells;
+    memcpy(ro, c->par[buf][0], n);
+    memcpy(p, c->par[buf][1], n);
+    memcpy(u, c->par[buf][2], n);
+    memcpy(v, c->par[buf][3], n);
+    memcpy(Q, c->par[buf][4], n);
+}
+
+void go_set_mc(void *h, const double *Hn, const double *Hu, const double *Hv, const double *HT, const double *ku,
+               const double *kv, const double *kT) {
+    ctx *c = (ctx *)h;
+    size_t n = sizeof(double) * c->m.n_cells;
+    memcpy(c->Hn, Hn, 4 * n);
+    memcpy(c->Hu, Hu, 4 * n);
+    memcpy(c->Hv, Hv, 4 * n);
+    memcpy(c->HT, HT, 4 * n);
+    memcpy(c->ku, ku, n);
+    memcpy(c->kv_, kv, n);
+    memcpy(c->kT, kT, n);
+}
+
+void go_set_inner_list(void *h, const int32_t *cells, int32_t n) {
+    ctx *c = (ctx *)h;
+    free(c->inner);
+    c->inner = (int32_t *)dup(cells, sizeof(int32_t) * (n > 0 ? n : 1));
+    c->n_inner_cells = n;
+}
+
+void go_get_points(void *h, double *x, double *y, double *x2, double *y2, double *Vx, double *Vy, int32_t *count) {
+    ctx *c = (ctx *)h;
+    size_t n = sizeof(double) * c->m.n_points;
+    memcpy(x, c->x, n);
+    memcpy(y, c->y, n);
+    memcpy(x2, c->x2, n);
+    memcpy(y2, c->y2, n);
+    memcpy(Vx, c->Vx, n);
+    memcpy(Vy, c->Vy, n);
+    memcpy(count, c->count, sizeof(int32_t) * c->m.n_points);
+}
+
+void go_status(void *h, int64_t *out4) {
+    ctx *c = (ctx *)h;
+    out4[0] = c->status;
+    out4[1] = c->n_ro_clamp;
+    out4[2] = c->n_p_clamp;
+    out4[3] = c->n_tvd_bad;
+}
+
+double go_last_dt(void *h) { return ((ctx *)h)->last_dt; }
+
+double go_hllc(const go_params *prm, const double *L5, const double *R5, double W, double *P4, double *PQ, double n1,
+               double n2, double rad, int metod, double *VlVcVp, int nul_potok) {
+    return hllc(prm, L5[0], L5[1], L5[2], L5[3], L5[4], R5[0], R5[1], R5[2], R5[3], R5[4], W, P4, PQ, n1, n2, rad,
+                metod, &VlVcVp[0], &VlVcVp[1], &VlVcVp[2], nul_potok);
+}
+
+double go_godunov(const go_params *prm, const double *q1, const double *q2, const double *n3, double *q5,
+                  double *dsl_dsp_dsc, double w, double dist, int *status) {
+    return godunov(prm, q1, q2, n3, q5, &dsl_dsp_dsc[0], &dsl_dsp_dsc[1], &dsl_dsp_dsc[2], w, dist, status);
+}
+
+void go_face_par(void *h, int f, int which, int buf, double *out5) {
+    ctx *c = (ctx *)h;
+    st5 s = {0, 0, 0, 0, 0};
+    if (which == 0) {
+        s = get_par(c, f, buf);
+    } else if (which == 1) {
+        int M = c->m.face_master[f];
+        if (M >= 0) s = cell_state(c, M, buf);
+        get_par_tvd(c, f, buf, &s);
+    } else {
+        get_par_tvd_radial(c, f, buf, &s.ro, &s.p);
+    }
+    out5[0] = s.ro; out5[1] = s.p; out5[2] = s.u; out5[3] = s.v; out5[4] = s.Q;
+}
+
+void go_cell_geom(void *h, int k, double *out) {
+    ctx *c = (ctx *)h;
+    cell_center(c, k, 0, &out[0], &out[1]);
+    cell_center(c, k, 1, &out[2], &out[3]);
+    out[4] = cell_volume(c, k, 0);
+    out[5] = cell_volume(c, k, 1);
+    out[6] = cell_volume_rotate(c, k, 0, 360.0) / (2.0 * PI_);
+    out[7] = cell_volume_rotate(c, k, 1, 360.0) / (2.0 * PI_);
+}
+
+void go_source_mk1(void *h, int k, double u, double v, double ro, double p, double *q3) {
+    source_mk1((ctx *)h, k, u, v, ro, p, &q3[0], &q3[1], &q3[2]);
+}
