@@ -1,0 +1,345 @@
+"""Benchmark of the Gelios_2D plasma time step on B200 (cell-updates/s).
+
+One "step" = one call of the moving-grid time step (the Go_5_komponent__MK2
+form: surface tracking, rail motion, per-face HLL/exact-Godunov fluxes with
+TVD reconstruction, charge-exchange source from Monte-Carlo moments,
+conservative ALE update, CFL reduction) over the whole grid, inputs resident
+in HBM.  Default workload: the reference's rail grid Setka(200,100,50,100,
+100,100,150,150) (~200k cells, ~400 rays x ~500 radial cells), the
+reference's initial field and seeded Monte-Carlo moments.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload mk2_200k|mk2_1m|plain]
+
+N>1 runs N independent replicas (one process per GPU, torchrun); value is
+the whole-job rate, the time is the max over ranks.  --impl reference times
+the reference's own CPU step (compiled from its sources, all host threads)
+on the same grid and prints its line; under torchrun only rank 0 does.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "cell-updates/s"
+WORKLOADS = {
+    "mk2_200k": ("moving-grid plasma step (Go_5_komponent__MK2 form) on Setka(200,100,50,100,100,100,150,150)",
+                 "mk2", (200, 100, 50, 100, 100, 100, 150, 150)),
+    "mk2_1m": ("moving-grid plasma step (Go_5_komponent__MK2 form) on Setka(480,240,100,220,200,200,300,300)",
+               "mk2", (480, 240, 100, 220, 200, 200, 300, 300)),
+    "plain": ("plain single-fluid step (Go_stationary form), polar 180x120, r=1..600", "plain", None),
+}
+# Algorithmic bytes per cell update (each datum moved once per step):
+#   MK2 form: 8*(2*5) state + 8*19 Monte-Carlo moments + 16*(1+1) points (x,y,x2,y2)
+#             + 8 written point coordinate + 4*4 neighbour indices = 288 B
+#   plain form: 8*(2*5) + 16 points + 4*4 indices = 112 B
+BYTES_PER_CELL = {"mk2": 288, "plain": 112}
+
+
+def _env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def build_workload(name: str):
+    import gelios_2d_b200 as g
+    from gelios_2d_b200 import _native as N
+    from gelios_2d_b200 import workloads as W
+
+    desc, form, dims = WORKLOADS[name]
+    if form == "mk2":
+        mesh = g.Mesh.setka(*dims)
+        params = N.reference_params()
+        st0 = W.init_conditions_reference(mesh)
+        mc = W.mc_fields(mesh, seed=9)
+        counted = W.counted_cells_mk2(mesh, params)
+    else:
+        mesh = W.plain_mesh()
+        params = W.plain_params()
+        st0 = W.plain_initial(mesh, params, seed=2024)
+        mc = None
+        counted = W.counted_cells_stationary(mesh)
+    return desc, form, dims, mesh, params, st0, mc, counted
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock / power / throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(workload: str):
+    """DRAM bytes per launch of the cell kernel from the committed ncu summary."""
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        return d.get(workload)
+    except Exception:
+        return None
+
+
+def cpu_reference_rate(mesh, params, st0, mc, counted, form, budget_s=12.0, max_steps=200, threads=None):
+    """The reference's own step (compiled from its sources, all host threads)
+    on the same grid: cell-updates/s over a bounded number of steps."""
+    from oracle import ref
+
+    threads = threads or os.cpu_count() or 1
+    ref.set_threads(threads, fast=True)
+    S = ref.RefSetka.from_mesh(mesh, fast=True)
+    S.tvd_prepare()
+    S.set_state(0, st0)
+    S.set_state(1, st0)
+    if mc is not None:
+        S.set_mc(*mc)
+    run = S.go_mk2 if form == "mk2" else S.go_stationary
+    # keep the reference's printf diagnostics off our stdout
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    try:
+        t0 = time.perf_counter()
+        run(1)
+        one = time.perf_counter() - t0
+        steps = int(max(1, min(max_steps, budget_s / max(one, 1e-6))))
+        t0 = time.perf_counter()
+        run(steps)
+        el = time.perf_counter() - t0
+    finally:
+        os.dup2(saved, 1)
+        os.close(devnull)
+        os.close(saved)
+    return counted * steps / el, steps, threads, el
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mk2_200k", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32flux"])
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = _env_int("RANK", 0)
+    world = _env_int("WORLD_SIZE", 1)
+    local = _env_int("LOCAL_RANK", 0)
+
+    desc, form, dims, mesh, params, st0, mc, counted = build_workload(args.workload)
+    config = {"workload": desc, "cells": int(mesh.n_cells), "cells_updated_per_step": int(counted),
+              "faces": int(mesh.n_faces), "points": int(mesh.n_points),
+              "l2": "flushed between timed steps (256 MiB write)" if args.workload != "mk2_1m" else
+                    "inputs larger than L2", "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        rate, steps, threads, el = cpu_reference_rate(mesh, params, st0, mc, counted, form)
+        line = {"metric": METRIC, "value": rate, "unit": "cell-updates/s", "impl": "reference",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1000.0 * el / steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "config": config,
+                "cpu_baseline": {"value": rate, "unit": "cell-updates/s", "cores": threads, "kind": "reference",
+                                 "sample": f"{steps} steps of the reference step on the full grid ({el:.1f} s)"},
+                "e2e": {"value": rate, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+
+    import gelios_2d_b200 as g
+    from gelios_2d_b200 import _native as N
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist_mod.init_process_group("nccl", timeout=timedelta(seconds=120))
+        dist = dist_mod
+    device = local
+    torch.cuda.set_device(device)
+    if args.precision == "fp32flux":
+        params = params.copy(precision=N.PREC_FP32_FLUX)
+    S = g.Setka(mesh, params, device=device)
+    S.set_par(0, st0)
+    S.set_par(1, st0)
+    if mc is not None:
+        S.set_mc(*mc)
+    fcode = N.FORM_MK2 if form == "mk2" else N.FORM_STATIONARY
+    stream = torch.cuda.ExternalStream(S.stream_handle(), device=device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")
+    do_flush = args.workload != "mk2_1m"
+    steps_per_call = 1 if do_flush else 10
+
+    def one(timed_events=None):
+        if do_flush:
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+        if timed_events is not None:
+            timed_events[0].record(stream)
+        S.step_async(fcode, steps_per_call)
+        if timed_events is not None:
+            timed_events[1].record(stream)
+        return S.launches()
+
+    for _ in range(args.warmup):
+        one()
+    S.synchronize()
+
+    sampler = ClockSampler(device)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    sampler.start()
+    S.set_phase_timing(True)
+    S.phase_times(reset=True)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches = 0
+    for k in range(args.steps):
+        launches += one(evs[k])
+    S.synchronize()
+    torch.cuda.synchronize(device)
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    phases = S.phase_times(reset=True)
+    S.set_phase_timing(False)
+    total_ms = sum(a.elapsed_time(b) for a, b in evs)
+    if dist:
+        t = torch.tensor([total_ms], device=f"cuda:{device}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    n_steps_total = args.steps * steps_per_call
+    value = world * counted * n_steps_total / (total_ms / 1000.0)
+
+    # end to end through the public API with pinned host buffers
+    host_in = torch.from_numpy(np.ascontiguousarray(st0)).pin_memory().numpy()
+    host_out = torch.empty(st0.shape, dtype=torch.float64).pin_memory().numpy()
+    e2e_steps = max(3, min(args.steps, 20))
+    S.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        S.set_par(0, host_in)
+        S.step_async(fcode, 1)
+        res = S.par(1)
+        host_out[...] = res
+    e2e_s = time.perf_counter() - t0
+    e2e_value = world * counted * e2e_steps / e2e_s
+    if dist:
+        t = torch.tensor([e2e_s], device=f"cuda:{device}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_value = world * counted * e2e_steps / float(t.item())
+
+    # roofline of the dominant kernel (the cell update)
+    cell_ms, cell_launch = phases["cells"]
+    avg_s = (cell_ms / max(cell_launch, 1)) / 1000.0
+    bpc = BYTES_PER_CELL[form]
+    achieved = bpc * counted / avg_s / 1e9 if avg_s > 0 else None
+    peak, peak_kind = measured_peaks()
+    traffic = ncu_traffic(args.workload)
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / n_steps_total, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64 (fp32 flux)",
+        "data": "synthetic (seeded initial field and Monte-Carlo moments)", "config": config,
+        "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": int(st0.nbytes),
+                "d2h_bytes_per_step": int(st0.nbytes)},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "kernel": f"{form}_cell_kernel", "bytes_per_cell": bpc,
+                     "avg_launch_us": avg_s * 1e6, "peak_kind": f"{peak_kind} hbm_gbs"},
+        "phases_ms": {k: v[0] for k, v in phases.items()},
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            rate, steps, threads, el = cpu_reference_rate(mesh, params, st0, mc, counted, form)
+            line["cpu_baseline"] = {"value": rate, "unit": "cell-updates/s", "cores": threads, "kind": "reference",
+                                    "sample": f"{steps} steps of the reference step on the full grid ({el:.1f} s)"}
+        except Exception as e:  # the reference library must be prebuilt
+            line["cpu_baseline"] = {"value": None, "unit": "cell-updates/s", "cores": 0, "kind": "reference",
+                                    "sample": f"unavailable: {e}"}
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,676 @@
+// C ABI of gelios_b200: the device context that stands in for a reference
+// Setka during its time loops (Setka.h:176-186).  Host code only; kernels are
+// in step_kernels.cu.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/gelios_b200.h"
+#include "physics.cuh"
+#include "step_kernels.cuh"
+
+namespace gelios {
+void set_error(const std::string& msg);
+gelios_mesh* mesh_from_view(const gelios_mesh_view* v);
+}  // namespace gelios
+
+using namespace gelios;
+
+namespace {
+
+#define GELIOS_CUDA_TRY(expr)                                                              \
+    do {                                                                                   \
+        cudaError_t e_ = (expr);                                                           \
+        if (e_ != cudaSuccess) {                                                           \
+            set_error(std::string(#expr) + ": " + cudaGetErrorString(e_));                 \
+            return GELIOS_E_CUDA;                                                          \
+        }                                                                                  \
+    } while (0)
+
+// A device allocation owned by the context.
+struct DBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~DBuf() {
+        if (p) cudaFree(p);
+    }
+    int alloc(size_t n) {
+        if (p) {
+            cudaFree(p);
+            p = nullptr;
+        }
+        bytes = n;
+        if (n == 0) n = 16;
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e != cudaSuccess) {
+            set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+            p = nullptr;
+            return GELIOS_E_CUDA;
+        }
+        return GELIOS_OK;
+    }
+    template <typename T>
+    T* as() const {
+        return static_cast<T*>(p);
+    }
+};
+
+template <typename T>
+int upload(DBuf& b, const T* src, size_t n, cudaStream_t s) {
+    int rc = b.alloc(n * sizeof(T));
+    if (rc) return rc;
+    if (n && src) {
+        cudaError_t e = cudaMemcpyAsync(b.p, src, n * sizeof(T), cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) {
+            set_error(std::string("cudaMemcpyAsync: ") + cudaGetErrorString(e));
+            return GELIOS_E_CUDA;
+        }
+    } else if (n) {
+        cudaMemsetAsync(b.p, 0, n * sizeof(T), s);
+    }
+    return GELIOS_OK;
+}
+
+}  // namespace
+
+struct gelios_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    gelios_params prm{};
+    bool have_mesh = false;
+    DevMesh d;
+    // topology / geometry
+    DBuf X, Y, X2, Y2, Vx, Vy, cnt, ptype, cstart, contour, gstart, cflags, sA, sB, snb, ssd, ssd2, sinfo;
+    DBuf fA, fB, ftype, fmaster, fsosed, fcopy, fsdown;
+    DBuf rtype, rM, rpstart, rpts, rkstart, rkeys, rs;
+    DBuf lc, li, lo;
+    DBuf Hn, Hu, Hv, HT, ku, kv, kT, r_istoch, cback, cnext;
+    // state par[2] x 5 fields, centroids [2], scratch
+    DBuf state[2];
+    DBuf cen[2];
+    DBuf words;    // T[2] (double), dt_acc (u64), counters[2] (u64), status (int)
+    DBuf surface;  // Move_surface per-face speeds
+    DBuf inner;
+    int n_inner = 0;
+    int64_t launches = 0;
+    // phase timing
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+    size_t ev_used = 0;
+    double phase_ms[5] = {0, 0, 0, 0, 0};
+    int64_t phase_launch[5] = {0, 0, 0, 0, 0};
+    cudaEvent_t event() {
+        if (ev_used == ev_pool.size()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            ev_pool.push_back(e);
+        }
+        return ev_pool[ev_used++];
+    }
+    // records the start of a phase; returns the event (or nullptr if timing is off)
+    cudaEvent_t phase_begin() {
+        if (!timing) return nullptr;
+        cudaEvent_t e = event();
+        cudaEventRecord(e, stream);
+        return e;
+    }
+    void phase_end(int phase, cudaEvent_t begin, int n_launch) {
+        phase_launch[phase] += n_launch;
+        if (!timing || !begin) return;
+        cudaEvent_t e = event();
+        cudaEventRecord(e, stream);
+        pending.push_back({phase, {begin, e}});
+    }
+    void collect() {
+        if (pending.empty()) return;
+        cudaStreamSynchronize(stream);
+        for (auto& p : pending) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, p.second.first, p.second.second);
+            phase_ms[p.first] += ms;
+        }
+        pending.clear();
+        ev_used = 0;
+    }
+    ~gelios_ctx() {
+        for (auto e : ev_pool) cudaEventDestroy(e);
+    }
+
+    double* T() const { return words.as<double>(); }
+    unsigned long long* acc() const { return reinterpret_cast<unsigned long long*>(words.as<char>() + 16); }
+    unsigned long long* counters() const { return reinterpret_cast<unsigned long long*>(words.as<char>() + 24); }
+    int* status() const { return reinterpret_cast<int*>(words.as<char>() + 40); }
+    double* field(int buf, int k) const { return state[buf].as<double>() + static_cast<size_t>(k) * d.n_cells; }
+};
+
+extern "C" void gelios_params_reference(gelios_params* o) {
+    if (!o) return;
+    const double RR = 390.222;
+    std::memset(o, 0, sizeof(*o));
+    o->gamma = 5.0 / 3.0;
+    o->kurant = 0.1;
+    o->chi = 36.1275;
+    o->inner_mach = 10.0;
+    o->in_ro = 1.0;
+    o->in_p = 1.0;
+    o->in_u = -2.54338;
+    o->in_v = 0.0;
+    o->in_Q = 100.0;
+    o->extern_u_par = -0.1;
+    o->extern_u_tvd = -0.01;
+    o->R11 = 38.0 / RR;
+    o->rad_stat = 95.0;
+    o->R1 = 1.0 / RR;
+    o->R111 = 50.0 / RR;
+    o->R5 = 2200.0 / RR;
+    o->Left = -1500.0 / RR;
+    o->koef = 0.1;
+    o->src_rmin = 10.0 / RR;
+    o->src_rmax = 1500.0 / RR;
+    o->src_coef = 3.0 / 6.0;
+    o->a_2 = 0.1307345665;
+    o->ro_floor = 0.00001;
+    o->p_floor = 0.000001;
+    o->dt0 = 0.00000001;
+    o->n_inner = 20;
+    o->n_outer_shock = 13;
+    o->godunov_max_iter = 1100;
+    o->precision = GELIOS_PREC_FP64;
+}
+
+extern "C" int gelios_create(gelios_ctx** out, const gelios_params* prm, int device) {
+    if (!out || !prm) {
+        set_error("gelios_create: null argument");
+        return GELIOS_E_ARG;
+    }
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        set_error("gelios_create: no CUDA device");
+        return GELIOS_E_NODEVICE;
+    }
+    if (device < 0 || device >= ndev) {
+        set_error("gelios_create: device index out of range");
+        return GELIOS_E_ARG;
+    }
+    GELIOS_CUDA_TRY(cudaSetDevice(device));
+    auto ctx = std::make_unique<gelios_ctx>();
+    ctx->device = device;
+    ctx->prm = *prm;
+    GELIOS_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    if (ctx->words.alloc(64)) return GELIOS_E_CUDA;
+    GELIOS_CUDA_TRY(cudaMemsetAsync(ctx->words.p, 0, 64, ctx->stream));
+    *out = ctx.release();
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_set_params(gelios_ctx* ctx, const gelios_params* prm) {
+    if (!ctx || !prm) return GELIOS_E_ARG;
+    ctx->prm = *prm;
+    return GELIOS_OK;
+}
+
+extern "C" void gelios_destroy(gelios_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaStreamDestroy(ctx->stream);
+    }
+    delete ctx;
+}
+
+extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v) {
+    if (!ctx || !v) return GELIOS_E_ARG;
+    if (v->n_points <= 0 || v->n_cells <= 0 || v->n_faces <= 0 || !v->x || !v->y || !v->point_type ||
+        !v->cell_type || !v->contour_start || !v->contour || !v->gran_start || !v->gran || !v->face_A || !v->face_B ||
+        !v->face_type || !v->face_master || !v->face_sosed || !v->face_copy) {
+        set_error("gelios_upload_topology: incomplete mesh view");
+        return GELIOS_E_ARG;
+    }
+    GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    const int np = v->n_points, nc = v->n_cells, nf = v->n_faces;
+    // TVD_prepare outputs: taken from the caller or computed here
+    std::unique_ptr<gelios_mesh, void (*)(gelios_mesh*)> tmp(nullptr, gelios_mesh_free);
+    const int32_t *fsdown = v->face_sosed_down, *cback = v->cell_back, *cnext = v->cell_next;
+    const double* r_istoch = v->r_istoch;
+    if (!fsdown || !cback || !cnext || !r_istoch) {
+        tmp.reset(mesh_from_view(v));
+        int rc = gelios_mesh_tvd_prepare(tmp.get());
+        if (rc) return rc;
+        gelios_mesh_view tv;
+        gelios_mesh_get_view(tmp.get(), &tv);
+        if (!fsdown) fsdown = tv.face_sosed_down;
+        if (!cback) cback = tv.cell_back;
+        if (!cnext) cnext = tv.cell_next;
+        if (!r_istoch) r_istoch = tv.r_istoch;
+    }
+    const int ng = v->gran_start[nc];
+    // per-slot arrays and per-cell flags
+    std::vector<int32_t> sA(ng), sB(ng), snb(ng), ssd(ng), ssd2(ng);
+    std::vector<uint32_t> sinfo(ng), cflags(nc, 0u);
+    for (int c = 0; c < nc; c++) {
+        if (v->cell_type[c] == C_1) cflags[c] |= CF_C1;
+        if (v->cell_type[c] == C_CENTR) cflags[c] |= CF_CENTR;
+        for (int g = v->gran_start[c]; g < v->gran_start[c + 1]; g++) {
+            const int f = v->gran[g];
+            if (f < 0 || f >= nf) {
+                set_error("gelios_upload_topology: face index out of range");
+                return GELIOS_E_MESH;
+            }
+            if (v->face_master[f] != c) {
+                set_error("gelios_upload_topology: a face in Cell::Grans is not mastered by that cell");
+                return GELIOS_E_MESH;
+            }
+            const int ft = v->face_type[f];
+            if (ft == G_AXIS) cflags[c] |= CF_AXIS;
+            sA[g] = v->face_A[f];
+            sB[g] = v->face_B[f];
+            snb[g] = v->face_sosed[f];
+            ssd[g] = fsdown[f];
+            const int fc = v->face_copy[f];
+            ssd2[g] = fc >= 0 ? fsdown[fc] : -1;
+            if (ft == G_USUALY && (snb[g] < 0 || fc < 0)) {
+                set_error("gelios_upload_topology: interior face without neighbour or twin");
+                return GELIOS_E_MESH;
+            }
+            const int ta = v->point_type[sA[g]], tb = v->point_type[sB[g]];
+            uint32_t info = static_cast<uint32_t>(ft) & SI_TYPE_MASK;
+            const bool god = (ta == P_CONTACT && tb == P_CONTACT) || (ta == P_INNER_SHOCK && tb == P_INNER_SHOCK) ||
+                             (ta == P_OUTER_SHOCK && tb == P_OUTER_SHOCK);
+            bool npf = false;
+            if (ta == P_CONTACT && tb != P_CONTACT) npf = true;
+            else if (ta != P_CONTACT && tb == P_CONTACT) npf = true;
+            else if (ta == P_INNER_SHOCK && tb != P_INNER_SHOCK) npf = true;
+            else if (ta != P_INNER_SHOCK && tb == P_INNER_SHOCK) npf = true;
+            else if (ta == P_OUTER_SHOCK && tb != P_OUTER_SHOCK) npf = true;
+            else if (ta != P_OUTER_SHOCK && tb == P_OUTER_SHOCK) npf = true;
+            if (god) info |= SI_GOD;
+            if (npf) info |= SI_NP;
+            sinfo[g] = info;
+        }
+    }
+    // rails must come grouped A, B, C, D (the export order of the reference lists)
+    int na = 0, nb = 0, ncr = 0, nd = 0;
+    for (int r = 0; r < v->n_rails; r++) {
+        const int t = v->rail_type[r];
+        const int expect_min = (nb + ncr + nd) ? ((ncr + nd) ? ((nd) ? 3 : 2) : 1) : 0;
+        if (t < expect_min || t > 3) {
+            set_error("gelios_upload_topology: rails must be ordered A, B, C, D");
+            return GELIOS_E_MESH;
+        }
+        const int nk = v->rail_kstart[r + 1] - v->rail_kstart[r];
+        if ((t != 2 && nk < 4) || (t == 2 && nk < 2)) {
+            set_error("gelios_upload_topology: rail without its key points");
+            return GELIOS_E_MESH;
+        }
+        (t == 0 ? na : t == 1 ? nb : t == 2 ? ncr : nd)++;
+    }
+    int rc = 0;
+    rc |= upload(ctx->X, v->x, np, s);
+    rc |= upload(ctx->Y, v->y, np, s);
+    rc |= upload(ctx->X2, v->x, np, s);
+    rc |= upload(ctx->Y2, v->y, np, s);
+    rc |= upload<double>(ctx->Vx, nullptr, np, s);
+    rc |= upload<double>(ctx->Vy, nullptr, np, s);
+    rc |= upload<int32_t>(ctx->cnt, nullptr, np, s);
+    rc |= upload(ctx->ptype, v->point_type, np, s);
+    rc |= upload(ctx->cstart, v->contour_start, nc + 1, s);
+    rc |= upload(ctx->contour, v->contour, v->contour_start[nc], s);
+    rc |= upload(ctx->gstart, v->gran_start, nc + 1, s);
+    rc |= upload(ctx->cflags, cflags.data(), nc, s);
+    rc |= upload(ctx->sA, sA.data(), ng, s);
+    rc |= upload(ctx->sB, sB.data(), ng, s);
+    rc |= upload(ctx->snb, snb.data(), ng, s);
+    rc |= upload(ctx->ssd, ssd.data(), ng, s);
+    rc |= upload(ctx->ssd2, ssd2.data(), ng, s);
+    rc |= upload(ctx->sinfo, sinfo.data(), ng, s);
+    rc |= upload(ctx->fA, v->face_A, nf, s);
+    rc |= upload(ctx->fB, v->face_B, nf, s);
+    rc |= upload(ctx->ftype, v->face_type, nf, s);
+    rc |= upload(ctx->fmaster, v->face_master, nf, s);
+    rc |= upload(ctx->fsosed, v->face_sosed, nf, s);
+    rc |= upload(ctx->fcopy, v->face_copy, nf, s);
+    rc |= upload(ctx->fsdown, fsdown, nf, s);
+    const int nr = v->n_rails;
+    if (nr > 0) {
+        rc |= upload(ctx->rtype, v->rail_type, nr, s);
+        rc |= upload(ctx->rM, v->rail_M, 4 * nr, s);
+        rc |= upload(ctx->rpstart, v->rail_pstart, nr + 1, s);
+        rc |= upload(ctx->rpts, v->rail_points, v->rail_pstart[nr], s);
+        rc |= upload(ctx->rkstart, v->rail_kstart, nr + 1, s);
+        rc |= upload(ctx->rkeys, v->rail_keys, v->rail_kstart[nr], s);
+        rc |= upload(ctx->rs, v->rail_s, nr, s);
+    }
+    rc |= upload(ctx->lc, v->line_contact, v->n_contact, s);
+    rc |= upload(ctx->li, v->line_inner, v->n_inner_line, s);
+    rc |= upload(ctx->lo, v->line_outer, v->n_outer_line, s);
+    rc |= upload<double>(ctx->Hn, nullptr, 4 * static_cast<size_t>(nc), s);
+    rc |= upload<double>(ctx->Hu, nullptr, 4 * static_cast<size_t>(nc), s);
+    rc |= upload<double>(ctx->Hv, nullptr, 4 * static_cast<size_t>(nc), s);
+    rc |= upload<double>(ctx->HT, nullptr, 4 * static_cast<size_t>(nc), s);
+    rc |= upload<double>(ctx->ku, nullptr, nc, s);
+    rc |= upload<double>(ctx->kv, nullptr, nc, s);
+    rc |= upload<double>(ctx->kT, nullptr, nc, s);
+    rc |= upload(ctx->r_istoch, r_istoch, nc, s);
+    rc |= upload(ctx->cback, cback, nc, s);
+    rc |= upload(ctx->cnext, cnext, nc, s);
+    rc |= upload<double>(ctx->state[0], nullptr, 5 * static_cast<size_t>(nc), s);
+    rc |= upload<double>(ctx->state[1], nullptr, 5 * static_cast<size_t>(nc), s);
+    rc |= upload<double>(ctx->cen[0], nullptr, 2 * static_cast<size_t>(nc), s);
+    rc |= upload<double>(ctx->cen[1], nullptr, 2 * static_cast<size_t>(nc), s);
+    rc |= upload<double>(ctx->surface, nullptr,
+                         static_cast<size_t>(v->n_contact) + 2 * v->n_inner_line + 2 * v->n_outer_line + 1, s);
+    if (rc) return GELIOS_E_CUDA;
+    GELIOS_CUDA_TRY(cudaStreamSynchronize(s));
+    DevMesh& d = ctx->d;
+    d = DevMesh();
+    d.n_points = np;
+    d.n_cells = nc;
+    d.n_faces = nf;
+    d.n_main = v->n_main;
+    std::memcpy(d.dims, v->dims, sizeof(d.dims));
+    d.X = ctx->X.as<double>();
+    d.Y = ctx->Y.as<double>();
+    d.X2 = ctx->X2.as<double>();
+    d.Y2 = ctx->Y2.as<double>();
+    d.Vx = ctx->Vx.as<double>();
+    d.Vy = ctx->Vy.as<double>();
+    d.cnt = ctx->cnt.as<int>();
+    d.ptype = ctx->ptype.as<int32_t>();
+    d.cstart = ctx->cstart.as<int32_t>();
+    d.contour = ctx->contour.as<int32_t>();
+    d.gstart = ctx->gstart.as<int32_t>();
+    d.cflags = ctx->cflags.as<uint32_t>();
+    d.sA = ctx->sA.as<int32_t>();
+    d.sB = ctx->sB.as<int32_t>();
+    d.snb = ctx->snb.as<int32_t>();
+    d.ssd = ctx->ssd.as<int32_t>();
+    d.ssd2 = ctx->ssd2.as<int32_t>();
+    d.sinfo = ctx->sinfo.as<uint32_t>();
+    d.fA = ctx->fA.as<int32_t>();
+    d.fB = ctx->fB.as<int32_t>();
+    d.ftype = ctx->ftype.as<int32_t>();
+    d.fmaster = ctx->fmaster.as<int32_t>();
+    d.fsosed = ctx->fsosed.as<int32_t>();
+    d.fcopy = ctx->fcopy.as<int32_t>();
+    d.fsdown = ctx->fsdown.as<int32_t>();
+    d.rtype = ctx->rtype.as<int32_t>();
+    d.rM = ctx->rM.as<int32_t>();
+    d.rpstart = ctx->rpstart.as<int32_t>();
+    d.rpts = ctx->rpts.as<int32_t>();
+    d.rkstart = ctx->rkstart.as<int32_t>();
+    d.rkeys = ctx->rkeys.as<int32_t>();
+    d.rs = ctx->rs.as<double>();
+    d.n_rail_a = na;
+    d.n_rail_b = nb;
+    d.n_rail_c = ncr;
+    d.n_rail_d = nd;
+    d.lc = ctx->lc.as<int32_t>();
+    d.li = ctx->li.as<int32_t>();
+    d.lo = ctx->lo.as<int32_t>();
+    d.n_lc = v->n_contact;
+    d.n_li = v->n_inner_line;
+    d.n_lo = v->n_outer_line;
+    d.Hn = ctx->Hn.as<double>();
+    d.Hu = ctx->Hu.as<double>();
+    d.Hv = ctx->Hv.as<double>();
+    d.HT = ctx->HT.as<double>();
+    d.ku = ctx->ku.as<double>();
+    d.kv = ctx->kv.as<double>();
+    d.kT = ctx->kT.as<double>();
+    d.r_istoch = ctx->r_istoch.as<double>();
+    d.cback = ctx->cback.as<int32_t>();
+    d.cnext = ctx->cnext.as<int32_t>();
+    ctx->have_mesh = true;
+    ctx->n_inner = 0;
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_upload_state(gelios_ctx* ctx, int buf, const double* ro, const double* p, const double* u,
+                                   const double* v, const double* Q) {
+    if (!ctx || buf < 0 || buf > 1 || !ro || !p || !u || !v || !Q) return GELIOS_E_ARG;
+    if (!ctx->have_mesh) {
+        set_error("gelios_upload_state: no topology");
+        return GELIOS_E_STATE;
+    }
+    GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
+    const size_t n = sizeof(double) * ctx->d.n_cells;
+    const double* src[5] = {ro, p, u, v, Q};
+    for (int k = 0; k < 5; k++)
+        GELIOS_CUDA_TRY(cudaMemcpyAsync(ctx->field(buf, k), src[k], n, cudaMemcpyHostToDevice, ctx->stream));
+    GELIOS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_download_state(gelios_ctx* ctx, int buf, double* ro, double* p, double* u, double* v,
+                                     double* Q) {
+    if (!ctx || buf < 0 || buf > 1 || !ro || !p || !u || !v || !Q) return GELIOS_E_ARG;
+    if (!ctx->have_mesh) return GELIOS_E_STATE;
+    GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
+    const size_t n = sizeof(double) * ctx->d.n_cells;
+    double* dst[5] = {ro, p, u, v, Q};
+    for (int k = 0; k < 5; k++)
+        GELIOS_CUDA_TRY(cudaMemcpyAsync(dst[k], ctx->field(buf, k), n, cudaMemcpyDeviceToHost, ctx->stream));
+    GELIOS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_upload_mc(gelios_ctx* ctx, const double* Hn, const double* Hu, const double* Hv,
+                                const double* HT, const double* ku, const double* kv, const double* kT) {
+    if (!ctx || !Hn || !Hu || !Hv || !HT || !ku || !kv || !kT) return GELIOS_E_ARG;
+    if (!ctx->have_mesh) return GELIOS_E_STATE;
+    GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
+    const size_t n = sizeof(double) * ctx->d.n_cells;
+    cudaStream_t s = ctx->stream;
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(ctx->Hn.p, Hn, 4 * n, cudaMemcpyHostToDevice, s));
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(ctx->Hu.p, Hu, 4 * n, cudaMemcpyHostToDevice, s));
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(ctx->Hv.p, Hv, 4 * n, cudaMemcpyHostToDevice, s));
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(ctx->HT.p, HT, 4 * n, cudaMemcpyHostToDevice, s));
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(ctx->ku.p, ku, n, cudaMemcpyHostToDevice, s));
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(ctx->kv.p, kv, n, cudaMemcpyHostToDevice, s));
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(ctx->kT.p, kT, n, cudaMemcpyHostToDevice, s));
+    GELIOS_CUDA_TRY(cudaStreamSynchronize(s));
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_set_inner_cells(gelios_ctx* ctx, const int32_t* cells, int32_t n) {
+    if (!ctx || n < 0 || (n > 0 && !cells)) return GELIOS_E_ARG;
+    if (!ctx->have_mesh) return GELIOS_E_STATE;
+    for (int i = 0; i < n; i++)
+        if (cells[i] < 0 || cells[i] >= ctx->d.n_cells) {
+            set_error("gelios_set_inner_cells: cell index out of range");
+            return GELIOS_E_ARG;
+        }
+    GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
+    if (upload(ctx->inner, cells, n, ctx->stream)) return GELIOS_E_CUDA;
+    GELIOS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    ctx->n_inner = n;
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status* status) {
+    if (!ctx || nsteps < 0) return GELIOS_E_ARG;
+    if (form != GELIOS_FORM_STATIONARY && form != GELIOS_FORM_MK2 && form != GELIOS_FORM_INNER_MK2) {
+        set_error("gelios_step: unknown form");
+        return GELIOS_E_ARG;
+    }
+    if (!ctx->have_mesh) {
+        set_error("gelios_step: no topology uploaded");
+        return GELIOS_E_STATE;
+    }
+    const DevMesh& d = ctx->d;
+    if (form == GELIOS_FORM_MK2 && (d.n_rail_a + d.n_rail_b + d.n_rail_c + d.n_rail_d == 0 || d.n_lc == 0)) {
+        set_error("gelios_step: the moving-grid form needs rails and tracked lines");
+        return GELIOS_E_MESH;
+    }
+    GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    const gelios_params& P = ctx->prm;
+    // T[0] = T[1] = dt0, accumulator = +inf, counters = 0, status = 0
+    struct Words {
+        double T[2];
+        unsigned long long acc;
+        unsigned long long counters[2];
+        int status;
+        int pad[5];
+    } w{};
+    static_assert(sizeof(Words) == 64, "device word layout");
+    w.T[0] = w.T[1] = P.dt0;
+    w.acc = 0x7ff0000000000000ULL;
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(ctx->words.p, &w, sizeof(w), cudaMemcpyHostToDevice, s));
+    int64_t launches = 0;
+    double* cen0 = ctx->cen[0].as<double>();
+    double* cen1 = ctx->cen[1].as<double>();
+    if (ctx->ev_used > 4096) ctx->collect();
+    {
+        cudaEvent_t e0 = ctx->phase_begin();
+        launch_centroid(d, d.X, d.Y, cen0, cen0 + d.n_cells, s);
+        ctx->phase_end(0, e0, 1);
+    }
+    launches++;
+    for (int st = 0; st < nsteps; st++) {
+        const int cur = st & 1, nxt = cur ^ 1;
+        StepBuffers b;
+        for (int k = 0; k < 5; k++) {
+            b.cur[k] = ctx->field(cur, k);
+            b.nxt[k] = ctx->field(nxt, k);
+        }
+        b.dt_cur = ctx->T() + cur;
+        b.dt_next = ctx->T() + nxt;
+        b.dt_acc = ctx->acc();
+        b.counters = ctx->counters();
+        b.status = ctx->status();
+        if (form == GELIOS_FORM_MK2) {
+            double* cc = (st & 1) ? cen1 : cen0;
+            double* cn = (st & 1) ? cen0 : cen1;
+            b.cx = cc;
+            b.cy = cc + d.n_cells;
+            b.cx_next = cn;
+            b.cy_next = cn + d.n_cells;
+            cudaEvent_t e1 = ctx->phase_begin();
+            const int nm = launch_motion(d, P, b, ctx->surface.as<double>(), s);
+            ctx->phase_end(2, e1, nm);  // Move_surface + rails (surface is 1 of them)
+            cudaEvent_t e3 = ctx->phase_begin();
+            launch_mk2_cells(d, P, b, s);
+            ctx->phase_end(3, e3, 1);
+            cudaEvent_t e4 = ctx->phase_begin();
+            launch_commit(d, b, s);
+            ctx->phase_end(4, e4, 1);
+            launches += nm + 2;
+        } else {
+            b.cx = cen0;
+            b.cy = cen0 + d.n_cells;
+            cudaEvent_t e3 = ctx->phase_begin();
+            if (form == GELIOS_FORM_STATIONARY) launch_stationary(d, P, b, s);
+            else launch_inner(d, P, b, ctx->inner.as<int32_t>(), ctx->n_inner, s);
+            ctx->phase_end(3, e3, 1);
+            cudaEvent_t e4 = ctx->phase_begin();
+            launch_dt_finalize(b, s);
+            ctx->phase_end(4, e4, 1);
+            launches += 2;
+        }
+    }
+    GELIOS_CUDA_TRY(cudaGetLastError());
+    ctx->launches = launches;
+    if (status) {
+        Words r{};
+        GELIOS_CUDA_TRY(cudaMemcpyAsync(&r, ctx->words.p, sizeof(r), cudaMemcpyDeviceToHost, s));
+        GELIOS_CUDA_TRY(cudaStreamSynchronize(s));
+        std::memset(status, 0, sizeof(*status));
+        status->flags = r.status;
+        status->steps_done = nsteps;
+        status->n_ro_clamp = static_cast<int64_t>(r.counters[0]);
+        status->n_p_clamp = static_cast<int64_t>(r.counters[1]);
+        status->result_buf = nsteps & 1;
+        status->dt = r.T[nsteps & 1];
+        if (!(status->dt == status->dt)) status->flags |= ST_DT_BAD;
+    }
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_download_points(gelios_ctx* ctx, double* x, double* y) {
+    if (!ctx || !x || !y) return GELIOS_E_ARG;
+    if (!ctx->have_mesh) return GELIOS_E_STATE;
+    GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
+    const size_t n = sizeof(double) * ctx->d.n_points;
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(x, ctx->X.p, n, cudaMemcpyDeviceToHost, ctx->stream));
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(y, ctx->Y.p, n, cudaMemcpyDeviceToHost, ctx->stream));
+    GELIOS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_synchronize(gelios_ctx* ctx) {
+    if (!ctx) return GELIOS_E_ARG;
+    GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
+    GELIOS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_state_device_ptr(gelios_ctx* ctx, int buf, double** dptr) {
+    if (!ctx || buf < 0 || buf > 1 || !dptr) return GELIOS_E_ARG;
+    if (!ctx->have_mesh) return GELIOS_E_STATE;
+    *dptr = ctx->state[buf].as<double>();
+    return GELIOS_OK;
+}
+
+extern "C" void* gelios_stream(gelios_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+extern "C" int64_t gelios_last_launch_count(gelios_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+extern "C" int gelios_set_phase_timing(gelios_ctx* ctx, int enabled) {
+    if (!ctx) return GELIOS_E_ARG;
+    GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
+    ctx->collect();
+    ctx->timing = enabled != 0;
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_phase_times(gelios_ctx* ctx, double* ms, int64_t* launches, int reset) {
+    if (!ctx) return GELIOS_E_ARG;
+    GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
+    ctx->collect();
+    for (int k = 0; k < 5; k++) {
+        if (ms) ms[k] = ctx->phase_ms[k];
+        if (launches) launches[k] = ctx->phase_launch[k];
+        if (reset) {
+            ctx->phase_ms[k] = 0.0;
+            ctx->phase_launch[k] = 0;
+        }
+    }
+    return GELIOS_OK;
+}
+
+namespace {
+int run_batch(const gelios_params* prm, int n, const double* in, int in_w, double* out, int out_w, bool godunov) {
+    if (!prm || n < 0 || (n > 0 && (!in || !out))) return GELIOS_E_ARG;
+    if (n == 0) return GELIOS_OK;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        set_error("no CUDA device");
+        return GELIOS_E_NODEVICE;
+    }
+    DBuf din, dout;
+    if (din.alloc(sizeof(double) * in_w * n) || dout.alloc(sizeof(double) * out_w * n)) return GELIOS_E_CUDA;
+    GELIOS_CUDA_TRY(cudaMemcpy(din.p, in, sizeof(double) * in_w * n, cudaMemcpyHostToDevice));
+    if (godunov) launch_godunov_batch(*prm, n, din.as<double>(), dout.as<double>(), 0);
+    else launch_hllc_batch(*prm, n, din.as<double>(), dout.as<double>(), 0);
+    GELIOS_CUDA_TRY(cudaGetLastError());
+    GELIOS_CUDA_TRY(cudaMemcpy(out, dout.p, sizeof(double) * out_w * n, cudaMemcpyDeviceToHost));
+    return GELIOS_OK;
+}
+}  // namespace
+
+extern "C" int gelios_hllc_batch(const gelios_params* prm, int n, const double* in, double* out) {
+    return run_batch(prm, n, in, 16, out, 9, false);
+}
+
+extern "C" int gelios_godunov_batch(const gelios_params* prm, int n, const double* in, double* out) {
+    return run_batch(prm, n, in, 15, out, 10, true);
+}

@@ -322,6 +322,52 @@ void finalize(Builder& B, gelios_mesh& m, const std::vector<Rail*>& rails) {
 
 }  // namespace
 
+namespace gelios {
+// Owned copy of a caller's mesh view (used when the caller leaves the
+// TVD_prepare outputs empty).
+gelios_mesh* mesh_from_view(const gelios_mesh_view* v) {
+    auto* m = new gelios_mesh();
+    std::memcpy(m->dims, v->dims, sizeof(m->dims));
+    const int np = v->n_points, nc = v->n_cells, nf = v->n_faces, nr = v->n_rails;
+    m->x.assign(v->x, v->x + np);
+    m->y.assign(v->y, v->y + np);
+    m->ptype.assign(v->point_type, v->point_type + np);
+    m->ctype.assign(v->cell_type, v->cell_type + nc);
+    m->cstart.assign(v->contour_start, v->contour_start + nc + 1);
+    m->contour.assign(v->contour, v->contour + m->cstart[nc]);
+    m->gstart.assign(v->gran_start, v->gran_start + nc + 1);
+    m->gran.assign(v->gran, v->gran + m->gstart[nc]);
+    m->cback.assign(nc, -1);
+    m->cnext.assign(nc, -1);
+    m->r_istoch.assign(nc, 0.0);
+    m->n_main = v->n_main;
+    m->fA.assign(v->face_A, v->face_A + nf);
+    m->fB.assign(v->face_B, v->face_B + nf);
+    m->ftype.assign(v->face_type, v->face_type + nf);
+    m->fmaster.assign(v->face_master, v->face_master + nf);
+    m->fsosed.assign(v->face_sosed, v->face_sosed + nf);
+    m->fcopy.assign(v->face_copy, v->face_copy + nf);
+    m->fsup.assign(nf, -1);
+    m->fsdown.assign(nf, -1);
+    if (nr > 0) {
+        m->rtype.assign(v->rail_type, v->rail_type + nr);
+        m->rs.assign(v->rail_s, v->rail_s + nr);
+        m->rM.assign(v->rail_M, v->rail_M + 4 * nr);
+        m->rpstart.assign(v->rail_pstart, v->rail_pstart + nr + 1);
+        m->rpts.assign(v->rail_points, v->rail_points + m->rpstart[nr]);
+        m->rkstart.assign(v->rail_kstart, v->rail_kstart + nr + 1);
+        m->rkeys.assign(v->rail_keys, v->rail_keys + m->rkstart[nr]);
+    } else {
+        m->rpstart.assign(1, 0);
+        m->rkstart.assign(1, 0);
+    }
+    if (v->n_contact) m->lcontact.assign(v->line_contact, v->line_contact + v->n_contact);
+    if (v->n_inner_line) m->linner.assign(v->line_inner, v->line_inner + v->n_inner_line);
+    if (v->n_outer_line) m->louter.assign(v->line_outer, v->line_outer + v->n_outer_line);
+    return m;
+}
+}  // namespace gelios
+
 extern "C" gelios_mesh* gelios_mesh_build_setka(int N1, int N2, int N3, int N4, int M1, int M2, int M3, int M4) {
     if (N1 < 1 || N2 < 1 || N3 < 1 || N4 < 2 || M1 < 1 || M2 < 1 || M3 < 1 || M4 < 1) {
         gelios::set_error("gelios_mesh_build_setka: dimensions out of range");
@@ -934,3 +980,22 @@ extern "C" int gelios_mesh_get_view(const gelios_mesh* m, gelios_mesh_view* v) {
 }
 
 extern "C" void gelios_mesh_free(gelios_mesh* m) { delete m; }
+
+extern "C" int gelios_tvd_prepare_view(const gelios_mesh_view* v, int32_t* sosed_up, int32_t* sosed_down,
+                                       int32_t* back, int32_t* next, double* r_istoch) {
+    if (!v || v->n_cells <= 0 || v->n_faces <= 0) {
+        gelios::set_error("gelios_tvd_prepare_view: empty view");
+        return GELIOS_E_ARG;
+    }
+    gelios_mesh* m = gelios::mesh_from_view(v);
+    const int rc = gelios_mesh_tvd_prepare(m);
+    if (rc == GELIOS_OK) {
+        if (sosed_up) std::copy(m->fsup.begin(), m->fsup.end(), sosed_up);
+        if (sosed_down) std::copy(m->fsdown.begin(), m->fsdown.end(), sosed_down);
+        if (back) std::copy(m->cback.begin(), m->cback.end(), back);
+        if (next) std::copy(m->cnext.begin(), m->cnext.end(), next);
+        if (r_istoch) std::copy(m->r_istoch.begin(), m->r_istoch.end(), r_istoch);
+    }
+    delete m;
+    return rc;
+}

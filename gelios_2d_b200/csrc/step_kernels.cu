@@ -1,0 +1,1351 @@
+// sm_100a kernels of the Gelios_2D plasma time step.
+//
+// One time step of Setka::Go_5_komponent__MK2 (Setka.cpp:10121-10482) is
+//   surface_kernel   Move_surface (Setka.cpp:3378-3844): tracked-face exact
+//                    Godunov speeds, one CTA, reference accumulation order
+//   rail_*_kernel    Move_Setka_Calculate_2 (Setka.cpp:4324-4759): one CTA per
+//                    rail, A+B rails, then C rails, then D rails (the
+//                    reference's sequence; C_Rails[0] shares points with the
+//                    last B rail and overwrites them)
+//   mk2_cell_kernel  per-cell flux accumulation in Grans order, charge-exchange
+//                    source, conservative ALE update, next-step centroid,
+//                    block-min of the CFL candidates
+//   commit_kernel    x = x2, V = 0, count = 0; dt of the next step
+// Go_stationary (Setka.cpp:5205-5343) and
+// Go_stationary_5_komponent_inner_MK2 (Setka.cpp:6999-7212) are
+// stationary_cell_kernel / inner_cell_kernel + dt_finalize_kernel.
+//
+// Owner-computes: a thread owns a cell and sums its faces in the reference's
+// Grans order, so no floating-point atomics are needed and results are
+// deterministic run to run.  The CFL minimum is exact under any order
+// (atomicMin on the bit pattern of non-negative doubles).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "physics.cuh"
+#include "step_kernels.cuh"
+
+namespace gelios {
+
+// ------------------------------------------------------------------ helpers
+__device__ __forceinline__ St5 load_state(const double* const* st, int c) {
+    St5 s;
+    s.ro = st[0][c];
+    s.p = st[1][c];
+    s.u = st[2][c];
+    s.v = st[3][c];
+    s.Q = st[4][c];
+    return s;
+}
+
+// Cell::Get_Center (Cell.cpp:66-88) on coordinates X, Y.
+__device__ __forceinline__ void centroid(const int32_t* contour, int n, const double* X, const double* Y, double& ox,
+                                         double& oy) {
+    double A = 0.0, Gx = 0.0, Gy = 0.0;
+    int a = contour[0];
+    double xa = X[a], ya = Y[a];
+    const double x0 = xa, y0 = ya;
+    for (int i = 0; i < n; i++) {
+        double xb, yb;
+        if (i + 1 == n) {
+            xb = x0;
+            yb = y0;
+        } else {
+            const int b = contour[i + 1];
+            xb = X[b];
+            yb = Y[b];
+        }
+        const double cr = xa * yb - ya * xb;
+        A = A + cr;
+        Gx = Gx + (xa + xb) * cr;
+        Gy = Gy + (ya + yb) * cr;
+        xa = xb;
+        ya = yb;
+    }
+    A = A * 0.5;
+    ox = Gx / (6.0 * A);
+    oy = Gy / (6.0 * A);
+}
+
+// Cell::Get_Volume_rotate(360)/(2 pi) (Cell.cpp:188-206) on X, Y.
+__device__ __forceinline__ double volume_rotate(const int32_t* contour, int n, const double* X, const double* Y) {
+    double A = 0.0, G = 0.0;
+    int a = contour[0];
+    double xa = X[a], ya = Y[a];
+    const double x0 = xa, y0 = ya;
+    for (int i = 0; i < n; i++) {
+        double xb, yb;
+        if (i + 1 == n) {
+            xb = x0;
+            yb = y0;
+        } else {
+            const int b = contour[i + 1];
+            xb = X[b];
+            yb = Y[b];
+        }
+        const double cr = xa * yb - ya * xb;
+        A = A + cr;
+        G = G + (ya + yb) * cr;
+        xa = xb;
+        ya = yb;
+    }
+    A = A * 0.5;
+    return fabs(A) * (1.0 / (6.0 * A)) * G * kPi * 360.0 / 180.0 / (2.0 * kPi);
+}
+
+// Cell::Get_Volume / Get_Volume_posle (Cell.cpp:146-186, 208-254).
+// posle selects the arithmetic-mean centre of the non-quad branch.
+__device__ double area(const int32_t* contour, int n, const int32_t* sA, const int32_t* sB, int g0, int g1,
+                       const double* X, const double* Y, bool posle) {
+    if (n == 4) {
+        const int p0 = contour[0], p1 = contour[1], p2 = contour[2], p3 = contour[3];
+        double a1 = X[p0] - X[p2];
+        double a2 = Y[p0] - Y[p2];
+        const double a = sqrt(sq(a1) + sq(a2));
+        double b1 = X[p1] - X[p3];
+        double b2 = Y[p1] - Y[p3];
+        const double b = sqrt(sq(b1) + sq(b2));
+        a1 = a1 / a;
+        a2 = a2 / a;
+        b1 = b1 / b;
+        b2 = b2 / b;
+        const double c = a1 * b1 + a2 * b2;
+        const double s = sqrt(1 - sq(c));
+        return 0.5 * a * b * s;
+    }
+    double x = 0.0, y = 0.0;
+    if (!posle) {
+        centroid(contour, n, X, Y, x, y);
+    } else {
+        for (int i = 0; i < n; i++) {
+            x += X[contour[i]];
+            y += Y[contour[i]];
+        }
+        x = x / (1.0 * n);
+        y = y / (1.0 * n);
+    }
+    double S = 0.0;
+    for (int g = g0; g < g1; g++) {
+        const int pa = sA[g], pb = sB[g];
+        const double a1 = sqrt(sq(X[pa] - x) + sq(Y[pa] - y));
+        const double a2 = sqrt(sq(X[pb] - x) + sq(Y[pb] - y));
+        const double a3 = sqrt(sq(X[pa] - X[pb]) + sq(Y[pa] - Y[pb]));
+        const double p = (a1 + a2 + a3) / 2.0;
+        S = S + sqrt(p * (p - a1) * (p - a2) * (p - a3));
+    }
+    return S;
+}
+
+// Inner_sphere BC state (Gran.cpp:234-265, 520-534) at face centre (x, y).
+__device__ __forceinline__ St5 inner_sphere_state(const gelios_params& P, double x, double y) {
+    const double dist = sqrt(x * x + y * y);
+    const double ro = 1.0 / (sq(P.chi) * dist * dist);
+    const double P_E = ro * P.chi * P.chi / (P.gamma * P.inner_mach * P.inner_mach);
+    St5 s;
+    s.ro = ro;
+    s.p = P_E;
+    s.u = P.chi * x / dist;
+    s.v = P.chi * y / dist;
+    s.Q = ro;
+    return s;
+}
+__device__ __forceinline__ St5 input_state(const gelios_params& P) {
+    St5 s;
+    s.ro = P.in_ro;
+    s.p = P.in_p;
+    s.u = P.in_u;
+    s.v = P.in_v;
+    s.Q = P.in_Q;
+    return s;
+}
+
+// Gran::Get_par (Gran.cpp:205-289) for a face of the owning cell `own`.
+__device__ __forceinline__ St5 get_par(const gelios_params& P, int ft, const St5& own, const double* const* st,
+                                       int nb, double fx, double fy) {
+    St5 s = own;
+    if (ft == G_USUALY) {
+        s = load_state(st, nb);
+    } else if (ft == G_EXTERN) {
+        if (s.u >= 0.0) s.u = P.extern_u_par;
+    } else if (ft == G_AXIS) {
+        s.v = -s.v;
+    } else if (ft == G_INNER_SPHERE) {
+        s = inner_sphere_state(P, fx, fy);
+    } else if (ft == G_INPUT) {
+        s = input_state(P);
+    }
+    return s;
+}
+
+// Gran::Get_par_TVD (Gran.cpp:292-473) of a Usualy face seen from Master M
+// (state Ms, centre Mx,My) with Sosed So and Sosed_down Sd.
+__device__ St5 tvd_usualy(const double* const* st, const double* cx, const double* cy, double fx, double fy,
+                          const St5& Ms, double Mx, double My, int So, int Sd, bool m_has_axis, bool tracked,
+                          int* status) {
+    if (Sd < 0) {
+        St5 par = Ms;
+        if (m_has_axis) {  // Gran.cpp:308-338
+            const St5 par3 = load_state(st, So);
+            const double dist2 = sqrt(sq(fx - Mx) + sq(fy - My));
+            const double dist3 = sqrt(sq(fx - cx[So]) + sq(fy - cy[So]));
+            const double dist1 = sqrt(sq(fx - Mx) + sq(fy - (-My)));
+            par.v = linear3(-dist1, -Ms.v, -dist2, Ms.v, dist3, par3.v, 0.0);
+        }
+        return par;
+    }
+    const St5 par1 = load_state(st, Sd);
+    const double dist2 = sqrt(sq(fx - Mx) + sq(fy - My));
+    if (tracked) {  // Gran.cpp:345-426
+        const double dist1 = sqrt(sq(fx - cx[Sd]) + sq(fy - cy[Sd]));
+        St5 o;
+        o.ro = linear2(-dist1, par1.ro, -dist2, Ms.ro, 0.0);
+        o.p = linear2(-dist1, par1.p, -dist2, Ms.p, 0.0);
+        o.u = linear2(-dist1, par1.u, -dist2, Ms.u, 0.0);
+        o.v = linear2(-dist1, par1.v, -dist2, Ms.v, 0.0);
+        o.Q = linear2(-dist1, par1.Q, -dist2, Ms.Q, 0.0);
+        if (o.ro <= 0.0) o.ro = Ms.ro;
+        if (o.p <= 0.0) o.p = Ms.p;
+        return o;
+    }
+    const St5 par3 = load_state(st, So);
+    const double dist3 = sqrt(sq(fx - cx[So]) + sq(fy - cy[So]));
+    const double dist1 = sqrt(sq(fx - cx[Sd]) + sq(fy - cy[Sd]));
+    St5 o;
+    o.ro = linear3(-dist1, par1.ro, -dist2, Ms.ro, dist3, par3.ro, 0.0);
+    o.p = linear3(-dist1, par1.p, -dist2, Ms.p, dist3, par3.p, 0.0);
+    o.u = linear3(-dist1, par1.u, -dist2, Ms.u, dist3, par3.u, 0.0);
+    o.v = linear3(-dist1, par1.v, -dist2, Ms.v, dist3, par3.v, 0.0);
+    o.Q = linear3(-dist1, par1.Q, -dist2, Ms.Q, dist3, par3.Q, 0.0);
+    if (o.ro <= 0.0 || o.p <= 0.0) *status |= ST_TVD_BAD;  // the reference exits (Gran.cpp:444-455)
+    return o;
+}
+
+// Gran::Get_par_TVD of an Axis face (Gran.cpp:486-519).
+__device__ __forceinline__ St5 tvd_axis(const double* const* st, const double* cx, const double* cy, double fx,
+                                        double fy, const St5& Ms, double Mx, double My, int Sd) {
+    St5 o = Ms;
+    if (Sd < 0) return o;  // no TVD partner: the upload rejects such a grid for the MK2 form
+    const St5 par1 = load_state(st, Sd);
+    const double dist2 = sqrt(sq(fx - Mx) + sq(fy - My));
+    const double dist1 = sqrt(sq(fx - cx[Sd]) + sq(fy - cy[Sd]));
+    o.v = linear3(-dist1, par1.v, -dist2, Ms.v, dist2, -Ms.v, 0.0);
+    return o;
+}
+
+// Gran::Get_par_TVD_radial (Gran.cpp:562-675), ro and p only (the callers
+// use no other field).
+__device__ void tvd_radial(const double* const* st, const double* cx, const double* cy, double fx, double fy,
+                           const St5& Ms, double Mx, double My, int So, int Sd, bool m_has_axis, double g2,
+                           double& oro, double& op) {
+    const double r = sqrt(sq(fx) + sq(fy));
+    if (Sd < 0) {
+        if (!m_has_axis) {
+            oro = Ms.ro;
+            op = Ms.p;
+            return;
+        }
+        const St5 par3 = load_state(st, So);
+        const double r2 = sqrt(sq(Mx) + sq(My));
+        const double dist2 = sqrt(sq(fx - Mx) + sq(fy - My));
+        const double sx = cx[So], sy = cy[So];
+        const double r3 = sqrt(sq(sx) + sq(sy));
+        const double dist3 = sqrt(sq(fx - sx) + sq(fy - sy));
+        const double r1 = sqrt(sq(Mx) + sq(-My));
+        const double dist1 = sqrt(sq(fx - Mx) + sq(fy - (-My)));
+        oro = linear3(-dist1, Ms.ro * sq(r1), -dist2, Ms.ro * sq(r2), dist3, par3.ro * sq(r3), 0.0) / sq(r);
+        op = linear3(-dist1, Ms.p * pow2g(r1, g2), -dist2, Ms.p * pow2g(r2, g2), dist3, par3.p * pow2g(r3, g2), 0.0) /
+             pow2g(r, g2);
+        return;
+    }
+    const St5 par1 = load_state(st, Sd);
+    const St5 par3 = load_state(st, So);
+    const double r2 = sqrt(sq(Mx) + sq(My));
+    const double dist2 = sqrt(sq(fx - Mx) + sq(fy - My));
+    const double sx = cx[So], sy = cy[So];
+    const double r3 = sqrt(sq(sx) + sq(sy));
+    const double dist3 = sqrt(sq(fx - sx) + sq(fy - sy));
+    const double dx = cx[Sd], dy = cy[Sd];
+    const double r1 = sqrt(sq(dx) + sq(dy));
+    const double dist1 = sqrt(sq(fx - dx) + sq(fy - dy));
+    oro = linear3(-dist1, par1.ro * sq(r1), -dist2, Ms.ro * sq(r2), dist3, par3.ro * sq(r3), 0.0) / sq(r);
+    op = linear3(-dist1, par1.p * pow2g(r1, g2), -dist2, Ms.p * pow2g(r2, g2), dist3, par3.p * pow2g(r3, g2), 0.0) /
+         pow2g(r, g2);
+}
+
+// Cell::Get_Sourse_MK1 (Cell.cpp:498-665).
+__device__ void source_mk1(const DevMesh& d, const gelios_params& P, int k, double xx, double yy, double u, double v,
+                           double ro, double p, double& q1, double& q2, double& q3, int* status) {
+    const double rr = sqrt(sq(xx) + sq(yy));
+    double uH[4], vH[4], roH[4], pH[4];
+    double ku = d.ku[k], kvv = d.kv[k], kT = d.kT[k];
+    if (rr > P.src_rmin && rr < P.src_rmax && xx >= 0.0) {
+        int K_do = d.cback[k], K_posle = d.cnext[k];
+        const double ri = d.r_istoch[k];
+        if (rr < ri) {
+            double r1 = ri;
+            int guard = 0;
+            while (r1 > rr) {
+                if (K_do < 0 || ++guard > d.n_cells) {
+                    *status |= ST_CHAIN;
+                    q1 = q2 = q3 = 0.0;
+                    return;
+                }
+                r1 = d.r_istoch[K_do];
+                K_do = d.cback[K_do];
+            }
+            if (K_do < 0) {
+                *status |= ST_CHAIN;
+                q1 = q2 = q3 = 0.0;
+                return;
+            }
+            K_do = d.cnext[K_do];
+            K_posle = K_do >= 0 ? d.cnext[K_do] : -1;
+        } else {
+            double r2 = ri;
+            int guard = 0;
+            while (r2 < rr) {
+                if (K_posle < 0 || ++guard > d.n_cells) {
+                    *status |= ST_CHAIN;
+                    q1 = q2 = q3 = 0.0;
+                    return;
+                }
+                r2 = d.r_istoch[K_posle];
+                K_posle = d.cnext[K_posle];
+            }
+            if (K_posle < 0) {
+                *status |= ST_CHAIN;
+                q1 = q2 = q3 = 0.0;
+                return;
+            }
+            K_posle = d.cback[K_posle];
+            K_do = K_posle >= 0 ? d.cback[K_posle] : -1;
+        }
+        if (K_do < 0 || K_posle < 0) {
+            *status |= ST_CHAIN;
+            q1 = q2 = q3 = 0.0;
+            return;
+        }
+        const double r1 = d.r_istoch[K_do];
+        const double r2 = d.r_istoch[K_posle];
+        double TH[4];
+#pragma unroll
+        for (int s = 0; s < 4; s++) uH[s] = linear2(r1, d.Hu[4 * K_do + s], r2, d.Hu[4 * K_posle + s], rr);
+#pragma unroll
+        for (int s = 0; s < 4; s++) vH[s] = linear2(r1, d.Hv[4 * K_do + s], r2, d.Hv[4 * K_posle + s], rr);
+#pragma unroll
+        for (int s = 0; s < 4; s++) roH[s] = linear2(r1, d.Hn[4 * K_do + s], r2, d.Hn[4 * K_posle + s], rr);
+#pragma unroll
+        for (int s = 0; s < 4; s++) TH[s] = linear2(r1, d.HT[4 * K_do + s], r2, d.HT[4 * K_posle + s], rr);
+        ku = linear2(r1, d.ku[K_do], r2, d.ku[K_posle], rr);
+        kvv = linear2(r1, d.kv[K_do], r2, d.kv[K_posle], rr);
+        kT = linear2(r1, d.kT[K_do], r2, d.kT[K_posle], rr);
+#pragma unroll
+        for (int s = 0; s < 4; s++) pH[s] = 0.5 * TH[s] * roH[s];
+    } else {
+#pragma unroll
+        for (int s = 0; s < 4; s++) {
+            uH[s] = d.Hu[4 * k + s];
+            vH[s] = d.Hv[4 * k + s];
+            roH[s] = d.Hn[4 * k + s];
+            pH[s] = 0.5 * d.HT[4 * k + s] * d.Hn[4 * k + s];
+        }
+    }
+    double Mu = 0.0, Mv = 0.0, MT = 0.0;
+    double nuu[4], nuv[4], nue[4];
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+        if (roH[s] <= 0.0) {
+            roH[s] = 0.0000001;
+            pH[s] = 0.0;
+        }
+        const double UM = sqrt(sq(u - uH[s]) + sq(v - vH[s]) + (64.0 / (9.0 * kPi)) * (p / ro + 2.0 * pH[s] / roH[s]));
+        const double UH = sqrt(sq(u - uH[s]) + sq(v - vH[s]) + (4.0 / kPi) * (p / ro + 2.0 * pH[s] / roH[s]));
+        const double sig = sq(1.0 - P.a_2 * log(UM));
+        const double nu = ro * roH[s] * UM * sig;
+        nuu[s] = nu * (uH[s] - u);
+        nuv[s] = nu * (vH[s] - v);
+        nue[s] = nu * ((sq(uH[s]) + sq(vH[s]) - sq(u) - sq(v)) / 2.0 + (UH / UM) * (2.0 * pH[s] / roH[s] - p / ro));
+    }
+    Mu = P.src_coef * (nuu[0] + nuu[1] + nuu[2] + nuu[3]);
+    Mv = P.src_coef * (nuv[0] + nuv[1] + nuv[2] + nuv[3]);
+    MT = P.src_coef * (nue[0] + nue[1] + nue[2] + nue[3]);
+    q1 = Mu * ku;
+    q2 = Mv * kvv;
+    q3 = MT * kT;
+}
+
+// Block-level minimum of `t` (non-negative doubles; NaN ignored) folded into
+// the device word acc with one atomicMin per block; clamp counters likewise.
+__device__ __forceinline__ void block_reduce_commit(double t, int nro, int np_, int status, unsigned long long* acc,
+                                                    unsigned long long* counters, int* status_word) {
+    __shared__ double smin[32];
+    __shared__ int sro[32], sp[32], sst[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ot = __shfl_down_sync(0xffffffffu, t, o);
+        t = (ot < t) ? ot : t;
+        nro += __shfl_down_sync(0xffffffffu, nro, o);
+        np_ += __shfl_down_sync(0xffffffffu, np_, o);
+        status |= __shfl_down_sync(0xffffffffu, status, o);
+    }
+    if (lane == 0) {
+        smin[wid] = t;
+        sro[wid] = nro;
+        sp[wid] = np_;
+        sst[wid] = status;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        t = lane < nw ? smin[lane] : __longlong_as_double(0x7ff0000000000000LL);
+        nro = lane < nw ? sro[lane] : 0;
+        np_ = lane < nw ? sp[lane] : 0;
+        status = lane < nw ? sst[lane] : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ot = __shfl_down_sync(0xffffffffu, t, o);
+            t = (ot < t) ? ot : t;
+            nro += __shfl_down_sync(0xffffffffu, nro, o);
+            np_ += __shfl_down_sync(0xffffffffu, np_, o);
+            status |= __shfl_down_sync(0xffffffffu, status, o);
+        }
+        if (lane == 0) {
+            if (t >= 0.0 && t < __longlong_as_double(0x7ff0000000000000LL))
+                atomicMin(acc, static_cast<unsigned long long>(__double_as_longlong(t)));
+            if (nro) atomicAdd(&counters[0], static_cast<unsigned long long>(nro));
+            if (np_) atomicAdd(&counters[1], static_cast<unsigned long long>(np_));
+            if (status) atomicOr(status_word, status);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ kernels
+__global__ void centroid_kernel(DevMesh d, const double* __restrict__ X, const double* __restrict__ Y, double* cx,
+                                double* cy) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= d.n_cells) return;
+    const int s = d.cstart[c], n = d.cstart[c + 1] - s;
+    double x, y;
+    centroid(d.contour + s, n, X, Y, x, y);
+    cx[c] = x;
+    cy[c] = y;
+}
+
+// Go_stationary cell update (Setka.cpp:5225-5341).
+__global__ void __launch_bounds__(128) stationary_cell_kernel(DevMesh d, gelios_params P, StepBuffers b) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double tmin_c = __longlong_as_double(0x7ff0000000000000LL);
+    int nro = 0, npc = 0, status = 0;
+    const double* const* st = b.cur;
+    if (c < d.n_cells && !(d.cflags[c] & CF_CENTR)) {
+        const double dt = *b.dt_cur;
+        const St5 par1 = load_state(st, c);
+        const double x = b.cx[c], y = b.cy[c];
+        const double rad = sqrt(sq(x) + sq(y));
+        const double g2 = 2 * P.gamma;
+        double Pt0 = 0.0, Pt1 = 0.0, Pt2 = 0.0, Pt3 = 0.0, Pt4 = 0.0;
+        double time = 10000000.0;
+        const int g0 = d.gstart[c], g1 = d.gstart[c + 1];
+        for (int g = g0; g < g1; g++) {
+            const int A = d.sA[g], B = d.sB[g];
+            const uint32_t info = d.sinfo[g];
+            const int ft = info & SI_TYPE_MASK;
+            const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
+            const double S = sqrt(sq(xb - xa) + sq(yb - ya));
+            const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
+            const double dist = sqrt(sq(x - x2) + sq(y - y2));
+            const int nb = d.snb[g];
+            St5 par11 = par1;
+            St5 par2 = get_par(P, ft, par1, st, nb, x2, y2);
+            double t1 = xb - xa, t2 = yb - ya;
+            const double nn = sqrt(sq(t1) + sq(t2));
+            t1 = t1 / nn;
+            t2 = t2 / nn;
+            const double n1 = t2, n2 = -t1;
+            if (rad < P.rad_stat && ft == G_USUALY) {
+                const double x3 = b.cx[nb], y3 = b.cy[nb];
+                const double dd = sqrt(sq(x3) + sq(y3));
+                const double f2 = sq(x2) + sq(y2);
+                const double fr = sqrt(f2);
+                par11.ro = par11.ro * sq(rad) / f2;
+                par2.ro = par2.ro * sq(dd) / f2;
+                par11.p = par11.p * pow2g(rad / fr, g2);
+                par2.p = par2.p * pow2g(dd / fr, g2);
+                polar_perenos(x, y, x2, y2, par11.u, par11.v);
+                polar_perenos(x3, y3, x2, y2, par2.u, par2.v);
+            } else if (ft == G_INNER_SPHERE) {
+                const double f2 = sq(x2) + sq(y2);
+                par11.ro = par11.ro * sq(rad) / f2;
+                par11.p = par11.p * pow2g(rad / sqrt(f2), g2);
+            } else if (rad < P.rad_stat && ft == G_AXIS) {
+                polar_perenos(x, y, x2, y2, par11.u, par11.v);
+                par11.v = 0.0;
+                par2 = par11;
+            } else if (ft == G_AXIS) {
+                par11.v = 0.0;
+                par2 = par11;
+            }
+            FluxOut<double> F;
+            double tf;
+            if (P.precision == GELIOS_PREC_FP32_FLUX) {
+                tf = hllc_flux<float>(P.gamma, P.kurant, par11, par2, 0.0, n1, n2, dist, 1, false, F);
+            } else {
+                tf = hllc_flux<double>(P.gamma, P.kurant, par11, par2, 0.0, n1, n2, dist, 1, false, F);
+            }
+            time = dmin_ref(time, tf);
+            Pt0 = Pt0 + F.P0 * S;
+            Pt1 = Pt1 + F.P1 * S;
+            Pt2 = Pt2 + F.P2 * S;
+            Pt3 = Pt3 + F.P3 * S;
+            Pt4 = Pt4 + F.PQ * S;
+        }
+        tmin_c = time;
+        const int s0 = d.cstart[c], n = d.cstart[c + 1] - s0;
+        const double Volume = area(d.contour + s0, n, d.sA, d.sB, g0, g1, d.X, d.Y, false);
+        const double gm1 = P.gamma - 1;
+        double ro3 = par1.ro - dt * (Pt0 / Volume + par1.ro * par1.v / y);
+        const double Q33 = par1.Q - (dt / Volume) * Pt4 - dt * par1.Q * par1.v / y;
+        if (ro3 <= 0) {
+            ro3 = P.ro_floor;
+            nro = 1;
+        }
+        const double uu = par1.u * par1.u + par1.v * par1.v;
+        const double u3 = (par1.ro * par1.u - dt * (Pt1 / Volume + par1.ro * par1.v * par1.u / y)) / ro3;
+        const double v3 = (par1.ro * par1.v - dt * (Pt2 / Volume + par1.ro * par1.v * par1.v / y)) / ro3;
+        double p3 = (((par1.p / gm1 + par1.ro * uu * 0.5) -
+                      dt * (Pt3 / Volume + par1.v * (P.gamma * par1.p / gm1 + par1.ro * uu * 0.5) / y)) -
+                     0.5 * ro3 * (u3 * u3 + v3 * v3)) *
+                    gm1;
+        if (p3 <= 0) {
+            p3 = P.p_floor;
+            npc = 1;
+        }
+        b.nxt[0][c] = ro3;
+        b.nxt[1][c] = p3;
+        b.nxt[2][c] = u3;
+        b.nxt[3][c] = v3;
+        b.nxt[4][c] = Q33;
+    }
+    block_reduce_commit(tmin_c, nro, npc, status, b.dt_acc, b.counters, b.status);
+}
+
+// Go_5_komponent__MK2 cell update (Setka.cpp:10148-10470).
+template <typename TF>
+__global__ void __launch_bounds__(128) mk2_cell_kernel(DevMesh d, gelios_params P, StepBuffers b) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double tmin_c = __longlong_as_double(0x7ff0000000000000LL);
+    int nro = 0, npc = 0, status = 0;
+    const double* const* st = b.cur;
+    if (c < d.n_cells) {
+        const int s0 = d.cstart[c], n = d.cstart[c + 1] - s0;
+        const int32_t* con = d.contour + s0;
+        // centroid after the motion = centroid of the next step
+        double xn, yn;
+        centroid(con, n, d.X2, d.Y2, xn, yn);
+        b.cx_next[c] = xn;
+        b.cy_next[c] = yn;
+        const double x = b.cx[c], y = b.cy[c];
+        const double radius = sqrt(sq(x) + sq(y));
+        if (!(radius < P.R11)) {
+            const double dt = *b.dt_cur;
+            const uint32_t cf = d.cflags[c];
+            const bool own_c1 = (cf & CF_C1) != 0;
+            const int g0 = d.gstart[c], g1 = d.gstart[c + 1];
+            const double vs1 = area(con, n, d.sA, d.sB, g0, g1, d.X, d.Y, false);
+            const double vs2 = area(con, n, d.sA, d.sB, g0, g1, d.X2, d.Y2, true);
+            const double Volume = volume_rotate(con, n, d.X, d.Y);
+            const double Volume2 = volume_rotate(con, n, d.X2, d.Y2);
+            const St5 par1 = load_state(st, c);
+            const double g2 = 2 * P.gamma;
+            double Pt0 = 0.0, Pt1 = 0.0, Pt2 = 0.0, Pt3 = 0.0, Pt4 = 0.0;
+            double time = 10000000.0;
+            for (int g = g0; g < g1; g++) {
+                const int A = d.sA[g], B = d.sB[g];
+                const uint32_t info = d.sinfo[g];
+                const int ft = info & SI_TYPE_MASK;
+                const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
+                const double S = sqrt(sq(xb - xa) + sq(yb - ya)) * (ya + yb) * 0.5;
+                const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
+                const double x4 = (d.X2[A] + d.X2[B]) / 2.0, y4 = (d.Y2[A] + d.Y2[B]) / 2.0;
+                const double dist = sqrt(sq(x - x2) + sq(y - y2));
+                const int nb = d.snb[g];
+                St5 par11 = par1;
+                St5 par2 = get_par(P, ft, par1, st, nb, x2, y2);
+                double t1 = xb - xa, t2 = yb - ya;
+                const double nn = sqrt(sq(t1) + sq(t2));
+                t1 = t1 / nn;
+                t2 = t2 / nn;
+                const double n1 = t2, n2 = -t1;
+                const double W = ((x4 - x2) * n1 + (y4 - y2) * n2) / dt;
+                const double dis = sqrt(sq(x2) + sq(y2));
+                const bool tracked = (info & SI_GOD) != 0;
+                if (ft == G_USUALY) {
+                    const double x3 = b.cx[nb], y3 = b.cy[nb];
+                    const double dd = sqrt(sq(x3) + sq(y3));
+                    if (own_c1) {
+                        par11.ro = par11.ro * sq(radius) / sq(dis);
+                        par11.Q = par11.Q * sq(radius) / sq(dis);
+                        par11.p = par11.p * pow2g(radius / dis, g2);
+                        polar_perenos(x, y, x2, y2, par11.u, par11.v);
+                        tvd_radial(st, b.cx, b.cy, x2, y2, par1, x, y, nb, d.ssd[g], (cf & CF_AXIS) != 0, g2,
+                                   par11.ro, par11.p);
+                    } else {
+                        par11 = tvd_usualy(st, b.cx, b.cy, x2, y2, par1, x, y, nb, d.ssd[g], (cf & CF_AXIS) != 0,
+                                           tracked, &status);
+                    }
+                    const uint32_t nbf = d.cflags[nb];
+                    if (nbf & CF_C1) {
+                        par2.ro = par2.ro * sq(dd) / sq(dis);
+                        par2.Q = par2.Q * sq(dd) / sq(dis);
+                        par2.p = par2.p * pow2g(dd / dis, g2);
+                        polar_perenos(x3, y3, x2, y2, par2.u, par2.v);
+                        const St5 nbs = load_state(st, nb);
+                        tvd_radial(st, b.cx, b.cy, x2, y2, nbs, x3, y3, c, d.ssd2[g], (nbf & CF_AXIS) != 0, g2,
+                                   par2.ro, par2.p);
+                    } else {
+                        const St5 nbs = load_state(st, nb);
+                        par2 = tvd_usualy(st, b.cx, b.cy, x2, y2, nbs, x3, y3, c, d.ssd2[g], (nbf & CF_AXIS) != 0,
+                                          tracked, &status);
+                    }
+                } else if (ft == G_INNER_SPHERE) {
+                    par11.ro = par11.ro * sq(radius) / sq(dis);
+                    par11.Q = par11.Q * sq(radius) / sq(dis);
+                    par11.p = par11.p * pow2g(radius / dis, g2);
+                } else if (ft == G_AXIS) {
+                    if (own_c1) {
+                        par11.ro = par11.ro * sq(radius) / sq(dis);
+                        par11.Q = par11.Q * sq(radius) / sq(dis);
+                        par11.p = par11.p * pow2g(radius / dis, g2);
+                        polar_perenos(x, y, x2, y2, par11.u, par11.v);
+                    } else {
+                        par11 = tvd_axis(st, b.cx, b.cy, x2, y2, par1, x, y, d.ssd[g]);
+                    }
+                    par2 = par11;
+                    par2.v = -par2.v;
+                }
+                const bool np = (info & SI_NP) != 0;
+                FluxOut<double> F;
+                if (tracked) {
+                    double q1[5] = {par11.ro, par11.p, par11.u, par11.v, 0.0};
+                    double q2[5] = {par2.ro, par2.p, par2.u, par2.v, 0.0};
+                    double nv[3] = {n1, n2, 0.0};
+                    double qq[5], ds[3];
+                    time = dmin_ref(time, godunov_dev(P.gamma, P.kurant, q1, q2, nv, qq, ds, W, dist,
+                                                      P.godunov_max_iter, &status));
+                    Pt0 = Pt0 + qq[0] * S;
+                    Pt1 = Pt1 + qq[1] * S;
+                    Pt2 = Pt2 + qq[2] * S;
+                    Pt3 = Pt3 + qq[4] * S;
+                    time = dmin_ref(time, hllc_flux<TF>(P.gamma, P.kurant, par11, par2, W, n1, n2, dist, 0, np, F));
+                    Pt4 = Pt4 + F.PQ * S;
+                } else {
+                    time = dmin_ref(time, hllc_flux<TF>(P.gamma, P.kurant, par11, par2, W, n1, n2, dist, 0, np, F));
+                    Pt0 = Pt0 + F.P0 * S;
+                    Pt1 = Pt1 + F.P1 * S;
+                    Pt2 = Pt2 + F.P2 * S;
+                    Pt3 = Pt3 + F.P3 * S;
+                    Pt4 = Pt4 + F.PQ * S;
+                }
+            }
+            tmin_c = time;
+            double q2_1, q2_2, q3;
+            source_mk1(d, P, c, x, y, par1.u, par1.v, par1.ro, par1.p, q2_1, q2_2, q3, &status);
+            if (!(cf & CF_CENTR)) {
+                const double ro = par1.ro, u = par1.u, v = par1.v, p = par1.p, Q = par1.Q;
+                const double gm1 = P.gamma - 1;
+                double ro3 = ro * Volume / Volume2 - dt * (Pt0 / Volume2);
+                const double Q33 = Q * Volume / Volume2 - (dt / Volume2) * Pt4;
+                if (ro3 <= 0.0) {
+                    ro3 = P.ro_floor;
+                    nro = 1;
+                }
+                const double u3 = (ro * u * Volume / Volume2 - dt * (Pt1 / Volume2 - q2_1)) / ro3;
+                const double v3 = (ro * v * Volume / Volume2 - dt * ((Pt2 - p * 0.5 * (vs1 + vs2)) / Volume2 - q2_2)) / ro3;
+                double p3 = (((p / gm1 + ro * (u * u + v * v) * 0.5) * Volume / Volume2 - dt * (Pt3 / Volume2 - q3)) -
+                             0.5 * ro3 * (u3 * u3 + v3 * v3)) *
+                            gm1;
+                if (p3 <= 0) {
+                    p3 = P.p_floor;
+                    npc = 1;
+                }
+                b.nxt[0][c] = ro3;
+                b.nxt[1][c] = p3;
+                b.nxt[2][c] = u3;
+                b.nxt[3][c] = v3;
+                b.nxt[4][c] = Q33;
+            } else {
+                b.nxt[0][c] = par1.ro;
+                b.nxt[1][c] = par1.p;
+                b.nxt[2][c] = par1.u;
+                b.nxt[3][c] = par1.v;
+                b.nxt[4][c] = par1.Q;
+            }
+        }
+    }
+    block_reduce_commit(tmin_c, nro, npc, status, b.dt_acc, b.counters, b.status);
+}
+
+// Go_stationary_5_komponent_inner_MK2 cell update (Setka.cpp:7021-7210).
+template <typename TF>
+__global__ void __launch_bounds__(128) inner_cell_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                         const int32_t* __restrict__ list, int n_list) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double tmin_c = __longlong_as_double(0x7ff0000000000000LL);
+    int nro = 0, npc = 0, status = 0;
+    const double* const* st = b.cur;
+    const int c = i < n_list ? list[i] : -1;
+    if (c >= 0 && !(d.cflags[c] & CF_CENTR)) {
+        const double dt = *b.dt_cur;
+        const uint32_t cf = d.cflags[c];
+        const int s0 = d.cstart[c], n = d.cstart[c + 1] - s0;
+        const int32_t* con = d.contour + s0;
+        const int g0 = d.gstart[c], g1 = d.gstart[c + 1];
+        const St5 par1 = load_state(st, c);
+        const double x = b.cx[c], y = b.cy[c];
+        const double vs1 = area(con, n, d.sA, d.sB, g0, g1, d.X, d.Y, false);
+        const double vs2 = area(con, n, d.sA, d.sB, g0, g1, d.X2, d.Y2, true);
+        const double radius = sqrt(sq(x) + sq(y));
+        const double Volume = volume_rotate(con, n, d.X, d.Y);
+        const double g2 = 2.0 * P.gamma;
+        double Pt0 = 0.0, Pt1 = 0.0, Pt2 = 0.0, Pt3 = 0.0, Pt4 = 0.0;
+        double time = 10000000.0;
+        for (int g = g0; g < g1; g++) {
+            const int A = d.sA[g], B = d.sB[g];
+            const uint32_t info = d.sinfo[g];
+            const int ft = info & SI_TYPE_MASK;
+            const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
+            const double S = sqrt(sq(xb - xa) + sq(yb - ya)) * (ya + yb) * 0.5;
+            const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
+            const double dist = sqrt(sq(x - x2) + sq(y - y2));
+            const int nb = d.snb[g];
+            St5 par11 = par1;
+            St5 par2 = get_par(P, ft, par1, st, nb, x2, y2);
+            double t1 = xb - xa, t2 = yb - ya;
+            const double nn = sqrt(sq(t1) + sq(t2));
+            t1 = t1 / nn;
+            t2 = t2 / nn;
+            const double n1 = t2, n2 = -t1;
+            int met = 1;
+            const double dis = sqrt(sq(x2) + sq(y2));
+            if (ft == G_USUALY) {
+                const double x3 = b.cx[nb], y3 = b.cy[nb];
+                const double dd = sqrt(sq(x3) + sq(y3));
+                par11.ro = par11.ro * sq(radius) / sq(dis);
+                par2.ro = par2.ro * sq(dd) / sq(dis);
+                par11.Q = par11.Q * sq(radius) / sq(dis);
+                par2.Q = par2.Q * sq(dd) / sq(dis);
+                par11.p = par11.p * pow2g(radius / dis, g2);
+                par2.p = par2.p * pow2g(dd / dis, g2);
+                polar_perenos(x, y, x2, y2, par11.u, par11.v);
+                polar_perenos(x3, y3, x2, y2, par2.u, par2.v);
+                const uint32_t nbf = d.cflags[nb];
+                if ((cf & CF_C1) && (nbf & CF_C1)) {
+                    const St5 nbs = load_state(st, nb);
+                    tvd_radial(st, b.cx, b.cy, x2, y2, par1, x, y, nb, d.ssd[g], (cf & CF_AXIS) != 0, g2, par11.ro,
+                               par11.p);
+                    tvd_radial(st, b.cx, b.cy, x2, y2, nbs, x3, y3, c, d.ssd2[g], (nbf & CF_AXIS) != 0, g2, par2.ro,
+                               par2.p);
+                }
+            } else if (ft == G_INNER_SPHERE) {
+                par11 = par2;
+            } else if (ft == G_AXIS) {
+                par11.ro = par11.ro * sq(radius) / sq(dis);
+                par11.Q = par11.Q * sq(radius) / sq(dis);
+                par11.p = par11.p * pow2g(radius / dis, g2);
+                polar_perenos(x, y, x2, y2, par11.u, par11.v);
+                par2 = par11;
+                par2.v = -par2.v;
+                met = 0;
+            }
+            FluxOut<double> F;
+            time = dmin_ref(time, hllc_flux<TF>(P.gamma, P.kurant, par11, par2, 0.0, n1, n2, dist, met, false, F));
+            Pt0 = Pt0 + F.P0 * S;
+            Pt1 = Pt1 + F.P1 * S;
+            Pt2 = Pt2 + F.P2 * S;
+            Pt3 = Pt3 + F.P3 * S;
+            Pt4 = Pt4 + F.PQ * S;
+        }
+        tmin_c = time;
+        double q2_1, q2_2, q3;
+        source_mk1(d, P, c, x, y, par1.u, par1.v, par1.ro, par1.p, q2_1, q2_2, q3, &status);
+        const double ro = par1.ro, u = par1.u, v = par1.v, p = par1.p, Q = par1.Q;
+        const double gm1 = P.gamma - 1;
+        double ro3 = ro - dt * (Pt0 / Volume);
+        const double Q33 = Q - (dt / Volume) * Pt4 - dt;
+        if (ro3 <= 0) {
+            ro3 = P.ro_floor;
+            nro = 1;
+        }
+        const double u3 = (ro * u - dt * (Pt1 / Volume - q2_1)) / ro3;
+        const double v3 = (ro * v - dt * ((Pt2 - p * 0.5 * (vs1 + vs2)) / Volume - q2_2)) / ro3;
+        double p3 = (((p / gm1 + ro * (u * u + v * v) * 0.5) - dt * (Pt3 / Volume - q3)) - 0.5 * ro3 * (u3 * u3 + v3 * v3)) *
+                    gm1;
+        if (p3 <= 0) {
+            p3 = P.p_floor;
+            npc = 1;
+        }
+        b.nxt[0][c] = ro3;
+        b.nxt[1][c] = p3;
+        b.nxt[2][c] = u3;
+        b.nxt[3][c] = v3;
+        b.nxt[4][c] = Q33;
+    }
+    block_reduce_commit(tmin_c, nro, npc, status, b.dt_acc, b.counters, b.status);
+}
+
+// T[now2] of the reference: min(1e7, all face candidates) if any cell took
+// part, 1e8 otherwise; re-arm the accumulator.
+__global__ void dt_finalize_kernel(StepBuffers b) {
+    const unsigned long long a = *b.dt_acc;
+    double t = (a == 0x7ff0000000000000ULL) ? 100000000.0 : __longlong_as_double(static_cast<long long>(a));
+    *b.dt_next = t;
+    *b.dt_acc = 0x7ff0000000000000ULL;
+}
+
+// x = x2, y = y2, V = 0, count = 0 (Setka.cpp:10473-10480) + dt finalisation.
+__global__ void commit_kernel(DevMesh d, StepBuffers b) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        const unsigned long long a = *b.dt_acc;
+        double t = (a == 0x7ff0000000000000ULL) ? 100000000.0 : __longlong_as_double(static_cast<long long>(a));
+        *b.dt_next = t;
+        *b.dt_acc = 0x7ff0000000000000ULL;
+    }
+    if (i < d.n_points) {
+        d.X[i] = d.X2[i];
+        d.Y[i] = d.Y2[i];
+        d.Vx[i] = 0.0;
+        d.Vy[i] = 0.0;
+        d.cnt[i] = 0;
+    }
+}
+
+// ------------------------------------------------------------------ grid motion
+// Move_Setka_Calculate_2, A and B rails (Setka.cpp:4331-4595): one CTA per rail.
+__global__ void rail_ab_kernel(DevMesh d, gelios_params P, const double* __restrict__ dtp, int first_rail,
+                               int n_rails) {
+    const int q = first_rail + blockIdx.x;
+    if (blockIdx.x >= n_rails) return;
+    const double dt = *dtp;
+    const int32_t* ap = d.rpts + d.rpstart[q];
+    const int32_t* kp = d.rkeys + d.rkstart[q];
+    const int M1 = d.rM[4 * q], M2 = d.rM[4 * q + 1], M3 = d.rM[4 * q + 2], M4 = d.rM[4 * q + 3];
+    const double s = d.rs[q];
+    const int t = d.rtype[q];
+    double* X = d.X;
+    double* Y = d.Y;
+    double* X2 = d.X2;
+    double* Y2 = d.Y2;
+    __shared__ double sh[4];  // R2, R3, R4, x2 of key point 0
+    const double cs = cos(s), sn = sin(s);
+    if (threadIdx.x == 0) {
+        if (t == 0) {  // A rail
+            for (int kk = 0; kk < 3; kk++) {
+                const int K = kp[kk];
+                const double V = d.Vx[K] * cs + d.Vy[K] * sn;
+                X2[K] = X[K] + dt * V * cs;
+                Y2[K] = Y[K] + dt * V * sn;
+            }
+            X2[kp[3]] = X[kp[3]];
+            Y2[kp[3]] = Y[kp[3]];
+            sh[0] = sqrt(sq(X2[kp[0]]) + sq(Y2[kp[0]]));
+            sh[1] = sqrt(sq(X2[kp[1]]) + sq(Y2[kp[1]]));
+            sh[2] = sqrt(sq(X2[kp[2]]) + sq(Y2[kp[2]]));
+        } else {  // B rail
+            const int K0 = kp[0], K1 = kp[1], K2 = kp[2], K3 = kp[3];
+            double V = d.Vx[K0] * cs + d.Vy[K0] * sn;
+            X2[K0] = X[K0] + dt * V * cs;
+            Y2[K0] = Y[K0] + dt * V * sn;
+            V = d.Vx[K1] * 0.0 + d.Vy[K1] * 1.0;
+            X2[K1] = X2[K0];
+            Y2[K1] = Y[K1] + dt * V;
+            V = d.Vx[K2] * 0.0 + d.Vy[K2] * 1.0;
+            X2[K2] = X2[K0];
+            Y2[K2] = Y[K2] + dt * V;
+            X2[K3] = X2[K0];
+            Y2[K3] = Y[K3];
+            sh[0] = sqrt(sq(X2[K0]) + sq(Y2[K0]));
+            sh[1] = Y2[K1];
+            sh[2] = Y2[K2];
+            sh[3] = X2[K0];
+        }
+    }
+    __syncthreads();
+    const int ni = P.n_inner;
+    const double R2 = sh[0];
+    for (int j = threadIdx.x; j < M1 - 1; j += blockDim.x) {
+        double r;
+        if (j < ni) {
+            const double x = j * 1.0 / (ni);
+            r = P.R1 + pow(x, 1.3) * (P.R111 - P.R1);
+        } else {
+            const double x = (j - ni) * 1.0 / (M1 - 1 - ni);
+            r = P.R111 + pow(x, 1.05) * (R2 - P.R111);
+        }
+        X2[ap[j]] = r * cs;
+        Y2[ap[j]] = r * sn;
+    }
+    if (t == 0) {
+        const double R3 = sh[1], R4 = sh[2];
+        for (int j = threadIdx.x; j < M2 - 1; j += blockDim.x) {
+            const double r = R2 + (R3 - R2) * (j + 1) / (M2);
+            X2[ap[M1 + j]] = r * cs;
+            Y2[ap[M1 + j]] = r * sn;
+        }
+        for (int j = threadIdx.x; j < M3 - 1; j += blockDim.x) {
+            const double r = R3 + (R4 - R3) * (j + 1) / (M3);
+            X2[ap[M1 + M2 + j]] = r * cs;
+            Y2[ap[M1 + M2 + j]] = r * sn;
+        }
+        const double dd = 1.5708 / sqrt(1.0 - 1.0 / 1.76);
+        const double e = 1.76 * (1.0 - sq(s / dd));
+        for (int j = threadIdx.x; j < M4; j += blockDim.x) {
+            const double x = (j + 1) * 1.0 / (M4);
+            const double r = R4 + pow(x, e) * (P.R5 - R4);
+            X2[ap[M1 + M2 + M3 + j]] = r * cs;
+            Y2[ap[M1 + M2 + M3 + j]] = r * sn;
+        }
+    } else {
+        const double R2y = Y2[kp[0]];
+        const double R3 = sh[1], R4 = sh[2], xk = sh[3];
+        for (int j = threadIdx.x; j < M2 - 1; j += blockDim.x) {
+            X2[ap[M1 + j]] = xk;
+            Y2[ap[M1 + j]] = R2y + (R3 - R2y) * (j + 1) / (M2);
+        }
+        for (int j = threadIdx.x; j < M3 - 1; j += blockDim.x) {
+            X2[ap[M1 + M2 + j]] = xk;
+            Y2[ap[M1 + M2 + j]] = R3 + (R4 - R3) * (j + 1) / (M3);
+        }
+        for (int j = threadIdx.x; j < M4; j += blockDim.x) {
+            X2[ap[M1 + M2 + M3 + j]] = xk;
+            Y2[ap[M1 + M2 + M3 + j]] = R4 + (P.R5 - R4) * (j + 1) / (M4);
+        }
+    }
+}
+
+// C rails (Setka.cpp:4597-4674).
+__global__ void rail_c_kernel(DevMesh d, gelios_params P, const double* __restrict__ dtp, int first_rail,
+                              int n_rails) {
+    const int q = first_rail + blockIdx.x;
+    if (blockIdx.x >= n_rails) return;
+    const double dt = *dtp;
+    const int32_t* ap = d.rpts + d.rpstart[q];
+    const int np = d.rpstart[q + 1] - d.rpstart[q];
+    const int32_t* kp = d.rkeys + d.rkstart[q];
+    const int M1 = d.rM[4 * q], M2 = d.rM[4 * q + 1];
+    const double s = d.rs[q];
+    const double cs = cos(s), sn = sin(s);
+    __shared__ double sh[3];
+    if (threadIdx.x == 0) {
+        const int K0 = kp[0], K1 = kp[1];
+        const double V = d.Vx[K0] * cs + d.Vy[K0] * sn;
+        d.X2[K0] = d.X[K0] + dt * V * cs;
+        d.Y2[K0] = d.Y[K0] + dt * V * sn;
+        d.X2[K1] = P.Left;
+        d.Y2[K1] = d.Y[K1];
+        sh[0] = sqrt(sq(d.X2[K0]) + sq(d.Y2[K0]));
+        sh[1] = d.X2[K0];
+        sh[2] = d.Y2[K0];
+    }
+    __syncthreads();
+    const int ni = P.n_inner;
+    const double R2 = sh[0];
+    for (int j = threadIdx.x; j < M1 - 1; j += blockDim.x) {
+        double r;
+        if (j < ni) {
+            const double x = j * 1.0 / (ni);
+            r = P.R1 + pow(x, 1.3) * (P.R111 - P.R1);
+        } else {
+            const double x = (j - ni) * 1.0 / (M1 - 1 - ni);
+            r = P.R111 + pow(x, 1.05) * (R2 - P.R111);
+        }
+        d.X2[ap[j]] = r * cs;
+        d.Y2[ap[j]] = r * sn;
+    }
+    const double R2x = sh[1], R3x = P.Left, yk = sh[2];
+    const double x = pow(R3x / (R2x), 1.0 / (M2));
+    for (int j = M1 + threadIdx.x; j < np; j += blockDim.x) {
+        d.X2[ap[j]] = R2x * pow(x, static_cast<double>(j + 1 - M1));
+        d.Y2[ap[j]] = yk;
+    }
+}
+
+// D rails (Setka.cpp:4676-4758); rail jj >= n_outer_shock copies the outer
+// shock height of rail jj-1, i.e. of rail n_outer_shock-1.
+__global__ void rail_d_kernel(DevMesh d, gelios_params P, const double* __restrict__ dtp, int first_rail,
+                              int n_rails) {
+    const int jj = blockIdx.x;
+    if (jj >= n_rails) return;
+    const int q = first_rail + jj;
+    const double dt = *dtp;
+    const int32_t* ap = d.rpts + d.rpstart[q];
+    const int32_t* kp = d.rkeys + d.rkstart[q];
+    const int M2 = d.rM[4 * q + 1], M3 = d.rM[4 * q + 2], M4 = d.rM[4 * q + 3];
+    const int sM2 = d.dims[5], sM3 = d.dims[6], sM4 = d.dims[7];
+    __shared__ double sh[4];
+    if (threadIdx.x == 0) {
+        const int K0 = kp[0], K1 = kp[1], K2 = kp[2], K3 = kp[3];
+        double V = d.Vy[K1];
+        d.X2[K1] = d.X2[K0];
+        d.Y2[K1] = d.Y[K1] + dt * V;
+        V = d.Vy[K2];
+        d.X2[K2] = d.X2[K0];
+        if (jj >= P.n_outer_shock && P.n_outer_shock >= 1) {
+            const int qs = first_rail + P.n_outer_shock - 1;
+            const int Ks = d.rkeys[d.rkstart[qs] + 2];
+            d.Y2[K2] = d.Y[Ks] + dt * d.Vy[Ks];
+        } else {
+            d.Y2[K2] = d.Y[K2] + dt * V;
+        }
+        d.X2[K3] = d.X2[K0];
+        d.Y2[K3] = d.Y[K3];
+        sh[0] = d.Y2[K0];
+        sh[1] = d.Y2[K1];
+        sh[2] = d.Y2[K2];
+        sh[3] = d.X2[K0];
+    }
+    __syncthreads();
+    const double R2 = sh[0], R3 = sh[1], R4 = sh[2], xk = sh[3];
+    for (int j = threadIdx.x; j < sM2 - 1; j += blockDim.x) {
+        d.X2[ap[j + 1]] = xk;
+        d.Y2[ap[j + 1]] = R2 + (R3 - R2) * (j + 1) / (M2);
+    }
+    for (int j = threadIdx.x; j < sM3 - 1; j += blockDim.x) {
+        d.X2[ap[sM2 + j + 1]] = xk;
+        d.Y2[ap[sM2 + j + 1]] = R3 + (R4 - R3) * (j + 1) / (M3);
+    }
+    for (int j = threadIdx.x; j < sM4; j += blockDim.x) {
+        d.X2[ap[sM2 + sM3 + j + 1]] = xk;
+        d.Y2[ap[sM2 + sM3 + j + 1]] = R4 + (P.R5 - R4) * (j + 1) / (M4);
+    }
+}
+
+// ------------------------------------------------------------------ surface tracking
+// Get_par_TVD of a main/copy face f read through the face table.
+__device__ St5 face_tvd(const DevMesh& d, const double* const* st, const double* cx, const double* cy, int f,
+                        int* status) {
+    const int ft = d.ftype[f];
+    const int M = d.fmaster[f];
+    const int a = d.fA[f], bb = d.fB[f];
+    const double fx = (d.X[a] + d.X[bb]) / 2.0, fy = (d.Y[a] + d.Y[bb]) / 2.0;
+    const St5 Ms = load_state(st, M);
+    if (ft == G_USUALY) {
+        const int ta = d.ptype[a], tb = d.ptype[bb];
+        const bool tracked = (ta == P_CONTACT && tb == P_CONTACT) || (ta == P_INNER_SHOCK && tb == P_INNER_SHOCK) ||
+                             (ta == P_OUTER_SHOCK && tb == P_OUTER_SHOCK);
+        return tvd_usualy(st, cx, cy, fx, fy, Ms, cx[M], cy[M], d.fsosed[f], d.fsdown[f],
+                          (d.cflags[M] & CF_AXIS) != 0, tracked, status);
+    }
+    if (ft == G_AXIS) return tvd_axis(st, cx, cy, fx, fy, Ms, cx[M], cy[M], d.fsdown[f]);
+    St5 o = Ms;
+    return o;  // Extern/Upper_wall/Input/Inner faces do not occur on tracked lines
+}
+
+// Move_surface (Setka.cpp:3378-3844).  Phase 1: one thread per tracked face
+// computes its exact-Godunov wave speed (and the branch the reference takes);
+// phase 2: thread 0 replays the reference's sequential accumulation,
+// averaging loops (which walk Line_Contact in all three blocks) and end-node
+// fix-ups, so every node velocity is bit-identical to the serial code.
+__global__ void __launch_bounds__(256) surface_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                      double* __restrict__ scratch) {
+    const double dt = *b.dt_cur;
+    const double* const* st = b.cur;
+    const int nC = d.n_lc, nI = d.n_li, nO = d.n_lo;
+    double* vc = scratch;              // [nC]  contact speed VV
+    double* vi = scratch + nC;         // [nI]  inner-shock speed Vl, sign of branch
+    double* bi = vi + nI;              // [nI]  1.0 -> both nodes, 0.0 -> B only
+    double* vo = bi + nI;              // [nO]  outer-shock speed Vp
+    double* bo = vo + nO;              // [nO]  branch: 0 B only, 1 both, 2 B, 3 A
+    int status = 0;
+    const double ga = P.gamma, g2 = 2.0 * P.gamma;
+    for (int j = threadIdx.x; j < nC + nI + nO; j += blockDim.x) {
+        double nv[3], q1[5], q2[5], qq[5], ds[3];
+        if (j < nC) {
+            const int f = d.lc[j];
+            const St5 p1 = face_tvd(d, st, b.cx, b.cy, f, &status);
+            const St5 p2 = face_tvd(d, st, b.cx, b.cy, d.fcopy[f], &status);
+            const int a = d.fA[f], bb = d.fB[f];
+            double t1 = d.X[bb] - d.X[a], t2 = d.Y[bb] - d.Y[a];
+            const double n = sqrt(sq(t1) + sq(t2));
+            t1 /= n;
+            t2 /= n;
+            nv[0] = t2; nv[1] = -t1; nv[2] = 0.0;
+            q1[0] = p1.ro; q1[1] = p1.p; q1[2] = p1.u; q1[3] = p1.v; q1[4] = 0.0;
+            q2[0] = p2.ro; q2[1] = p2.p; q2[2] = p2.u; q2[3] = p2.v; q2[4] = 0.0;
+            godunov_dev(ga, P.kurant, q1, q2, nv, qq, ds, 0.0, 0.0, P.godunov_max_iter, &status);
+            vc[j] = ds[2] * P.koef * 0.3;
+        } else if (j < nC + nI) {
+            const int jj = j - nC;
+            const int f = d.li[jj];
+            const int M = d.fmaster[f];
+            St5 p1 = load_state(st, M);
+            const double x = b.cx[M], y = b.cy[M];
+            const double radius = sqrt(sq(x) + sq(y));
+            const int a = d.fA[f], bb = d.fB[f];
+            const double x2 = (d.X[a] + d.X[bb]) / 2.0, y2 = (d.Y[a] + d.Y[bb]) / 2.0;
+            const double dis = sqrt(sq(x2) + sq(y2));
+            const St5 p2 = face_tvd(d, st, b.cx, b.cy, d.fcopy[f], &status);
+            double t1 = d.X[bb] - d.X[a], t2 = d.Y[bb] - d.Y[a];
+            const double n = sqrt(sq(t1) + sq(t2));
+            t1 /= n;
+            t2 /= n;
+            const double n1 = t2, n2 = -t1;
+            p1.ro = p1.ro * sq(radius) / sq(dis);
+            p1.p = p1.p * pow2g(radius / dis, g2);
+            polar_perenos(x, y, x2, y2, p1.u, p1.v);
+            nv[0] = n1; nv[1] = n2; nv[2] = 0.0;
+            q1[0] = p1.ro; q1[1] = p1.p; q1[2] = p1.u; q1[3] = p1.v; q1[4] = 0.0;
+            q2[0] = p2.ro; q2[1] = p2.p; q2[2] = p2.u; q2[3] = p2.v; q2[4] = 0.0;
+            godunov_dev(ga, P.kurant, q1, q2, nv, qq, ds, 0.0, 0.0, P.godunov_max_iter, &status);
+            vi[jj] = ds[0] * P.koef * 0.1;
+            const double tt1 = -n2, tt2 = n1;
+            bi[jj] = (fabs(p2.u * tt1 + p2.v * tt2) < 0.1) ? 1.0 : 0.0;
+        } else {
+            const int jj = j - nC - nI;
+            const int lim = P.n_outer_shock + d.dims[0] + d.dims[1] + 1;
+            if (jj >= lim) {
+                vo[jj] = 0.0;
+                bo[jj] = -1.0;
+                continue;
+            }
+            const int f = d.lo[jj];
+            const St5 p1 = face_tvd(d, st, b.cx, b.cy, f, &status);
+            const St5 p2 = face_tvd(d, st, b.cx, b.cy, d.fcopy[f], &status);
+            const int a = d.fA[f], bb = d.fB[f];
+            double t1 = d.X[bb] - d.X[a], t2 = d.Y[bb] - d.Y[a];
+            const double n = sqrt(sq(t1) + sq(t2));
+            t1 /= n;
+            t2 /= n;
+            const double n1 = t2, n2 = -t1;
+            nv[0] = n1; nv[1] = n2; nv[2] = 0.0;
+            q1[0] = p1.ro; q1[1] = p1.p; q1[2] = p1.u; q1[3] = p1.v; q1[4] = 0.0;
+            q2[0] = p2.ro; q2[1] = p2.p; q2[2] = p2.u; q2[3] = p2.v; q2[4] = 0.0;
+            godunov_dev(ga, P.kurant, q1, q2, nv, qq, ds, 0.0, 0.0, P.godunov_max_iter, &status);
+            vo[jj] = ds[1] * P.koef;
+            const double tt1 = -n2, tt2 = n1;
+            double br;
+            if ((sq(p1.u) + sq(p1.v) + sq(0.0)) / (ga * p1.p / p1.ro) > 1.0) br = 0.0;
+            else if (fabs(p1.u * tt1 + p1.v * tt2) < 0.01) br = 1.0;
+            else if (p1.u * tt1 + p1.v * tt2 > 0) br = 2.0;
+            else br = 3.0;
+            bo[jj] = br;
+        }
+    }
+    if (status) atomicOr(b.status, status);
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    double* Vx = d.Vx;
+    double* Vy = d.Vy;
+    int* cnt = d.cnt;
+    auto nrm = [&](int f, double& n1, double& n2) {
+        const int a = d.fA[f], bb = d.fB[f];
+        double t1 = d.X[bb] - d.X[a], t2 = d.Y[bb] - d.Y[a];
+        const double n = sqrt(sq(t1) + sq(t2));
+        t1 /= n;
+        t2 /= n;
+        n1 = t2;
+        n2 = -t1;
+    };
+    if (nC > 0) {
+        for (int j = 0; j < nC; j++) {
+            const int f = d.lc[j];
+            double n1, n2;
+            nrm(f, n1, n2);
+            const int B = d.fB[f];
+            Vx[B] += vc[j] * n1;
+            Vy[B] += vc[j] * n2;
+            cnt[B]++;
+        }
+        for (int j = 0; j < nC; j++) {
+            const int A = d.fA[d.lc[j]];
+            if (cnt[A] > 0) {
+                Vx[A] /= (1.0 * cnt[A]);
+                Vy[A] /= (1.0 * cnt[A]);
+            }
+        }
+        const int a0 = d.fA[d.lc[0]], b0 = d.fB[d.lc[0]];
+        Vx[a0] = Vx[b0] + (d.X[b0] - d.X[a0]) / dt;
+        const int a1 = d.fA[d.lc[nC - 1]], b1 = d.fB[d.lc[nC - 1]];
+        Vy[b1] = Vy[a1] + (d.Y[a1] - d.Y[b1]) / dt;
+    }
+    if (nI > 0) {
+        for (int j = 0; j < nI; j++) {
+            const int f = d.li[j];
+            double n1, n2;
+            nrm(f, n1, n2);
+            const int A = d.fA[f], B = d.fB[f];
+            const double Vl = vi[j];
+            if (bi[j] != 0.0) {
+                Vx[A] += Vl * n1;
+                Vy[A] += Vl * n2;
+                cnt[A]++;
+            }
+            Vx[B] += Vl * n1;
+            Vy[B] += Vl * n2;
+            cnt[B]++;
+        }
+        // walks Line_Contact (Setka.cpp:3718-3731); past its end the reference
+        // reads out of bounds, here the walk stops at the end of the list
+        for (int j = 0; j < nI && j < nC; j++) {
+            const int A = d.fA[d.lc[j]];
+            if (cnt[A] > 0) {
+                Vx[A] /= (1.0 * cnt[A]);
+                Vy[A] /= (1.0 * cnt[A]);
+            }
+        }
+        const int a0 = d.fA[d.li[0]], b0 = d.fB[d.li[0]];
+        Vx[a0] = Vx[b0] + (d.X[b0] - d.X[a0]) / dt;
+        const int a1 = d.fA[d.li[nI - 1]], b1 = d.fB[d.li[nI - 1]];
+        Vx[b1] = Vx[a1] + (d.X[a1] - d.X[b1]) / dt;
+    }
+    if (nO > 0) {
+        for (int j = 0; j < nO; j++) {
+            const double br = bo[j];
+            if (br < 0.0) continue;
+            const int f = d.lo[j];
+            double n1, n2;
+            nrm(f, n1, n2);
+            const int A = d.fA[f], B = d.fB[f];
+            const double Vp = vo[j];
+            if (br == 0.0 || br == 2.0) {
+                Vx[B] += Vp * n1;
+                Vy[B] += Vp * n2;
+                cnt[B]++;
+            } else if (br == 1.0) {
+                Vx[A] += Vp * n1;
+                Vy[A] += Vp * n2;
+                cnt[A]++;
+                Vx[B] += Vp * n1;
+                Vy[B] += Vp * n2;
+                cnt[B]++;
+            } else {
+                Vx[A] += Vp * n1;
+                Vy[A] += Vp * n2;
+                cnt[A]++;
+            }
+        }
+        for (int j = 0; j < nO && j < nC; j++) {  // walks Line_Contact (Setka.cpp:3829-3837)
+            const int A = d.fA[d.lc[j]];
+            if (cnt[A] > 0) {
+                Vx[A] /= (1.0 * cnt[A]);
+                Vy[A] /= (1.0 * cnt[A]);
+            }
+        }
+        const int a0 = d.fA[d.lo[0]], b0 = d.fB[d.lo[0]];
+        Vx[a0] = Vx[b0] + (d.X[b0] - d.X[a0]) / dt;
+        const int a1 = d.fA[d.lo[nO - 1]], b1 = d.fB[d.lo[nO - 1]];
+        Vy[b1] = Vy[a1] + (d.Y[a1] - d.Y[b1]) / dt;
+    }
+}
+
+// ------------------------------------------------------------------ per-face batches (known-answer checks)
+__global__ void hllc_batch_kernel(gelios_params P, int n, const double* __restrict__ in, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double* a = in + 16 * i;
+    St5 L, R;
+    L.ro = a[0]; L.Q = a[1]; L.p = a[2]; L.u = a[3]; L.v = a[4];
+    R.ro = a[5]; R.Q = a[6]; R.p = a[7]; R.u = a[8]; R.v = a[9];
+    FluxOut<double> F;
+    double t;
+    if (P.precision == GELIOS_PREC_FP32_FLUX)
+        t = hllc_flux<float>(P.gamma, P.kurant, L, R, a[10], a[11], a[12], a[13], (int)a[14], a[15] != 0.0, F);
+    else
+        t = hllc_flux<double>(P.gamma, P.kurant, L, R, a[10], a[11], a[12], a[13], (int)a[14], a[15] != 0.0, F);
+    double* o = out + 9 * i;
+    o[0] = t;
+    o[1] = F.P0;
+    o[2] = F.P1;
+    o[3] = F.P2;
+    o[4] = F.P3;
+    o[5] = F.PQ;
+    // wave speeds (Vl, Vc, Vp) recomputed in FP64 for the check
+    const double n1 = a[11], n2 = a[12];
+    const double u1 = L.u * n1 + L.v * n2, u2 = R.u * n1 + R.v * n2;
+    const double cL = sqrt(P.gamma * L.p / L.ro), cR = sqrt(P.gamma * R.p / R.ro);
+    const double SL = dmin_ref(u1, u2) - dmax_ref(cL, cR);
+    const double SR = dmax_ref(u1, u2) + dmax_ref(cL, cR);
+    const double suR = SR - u2, suL = SL - u1;
+    o[6] = SL;
+    o[7] = (suR * R.ro * u2 - suL * L.ro * u1 - R.p + L.p) / (suR * R.ro - suL * L.ro);
+    o[8] = SR;
+}
+
+__global__ void godunov_batch_kernel(gelios_params P, int n, const double* __restrict__ in, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double* a = in + 15 * i;
+    double q1[5], q2[5], nv[3], qq[5], ds[3];
+    for (int k = 0; k < 5; k++) {
+        q1[k] = a[k];
+        q2[k] = a[5 + k];
+    }
+    nv[0] = a[10]; nv[1] = a[11]; nv[2] = a[12];
+    int status = 0;
+    const double t = godunov_dev(P.gamma, P.kurant, q1, q2, nv, qq, ds, a[13], a[14], P.godunov_max_iter, &status);
+    double* o = out + 10 * i;
+    o[0] = t;
+    for (int k = 0; k < 5; k++) o[1 + k] = qq[k];
+    o[6] = ds[0];
+    o[7] = ds[1];
+    o[8] = ds[2];
+    o[9] = status;
+}
+
+// ------------------------------------------------------------------ launchers
+namespace {
+inline int blocks_for(int n, int t) { return (n + t - 1) / t; }
+}
+
+void launch_centroid(const DevMesh& d, const double* X, const double* Y, double* cx, double* cy, cudaStream_t s) {
+    if (d.n_cells > 0) centroid_kernel<<<blocks_for(d.n_cells, 256), 256, 0, s>>>(d, X, Y, cx, cy);
+}
+void launch_stationary(const DevMesh& d, const gelios_params& P, const StepBuffers& b, cudaStream_t s) {
+    stationary_cell_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b);
+}
+void launch_mk2_cells(const DevMesh& d, const gelios_params& P, const StepBuffers& b, cudaStream_t s) {
+    if (P.precision == GELIOS_PREC_FP32_FLUX)
+        mk2_cell_kernel<float><<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b);
+    else
+        mk2_cell_kernel<double><<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b);
+}
+void launch_inner(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const int32_t* list, int n,
+                  cudaStream_t s) {
+    const int nb = blocks_for(n > 0 ? n : 1, 128);
+    if (P.precision == GELIOS_PREC_FP32_FLUX)
+        inner_cell_kernel<float><<<nb, 128, 0, s>>>(d, P, b, list, n);
+    else
+        inner_cell_kernel<double><<<nb, 128, 0, s>>>(d, P, b, list, n);
+}
+void launch_dt_finalize(const StepBuffers& b, cudaStream_t s) { dt_finalize_kernel<<<1, 1, 0, s>>>(b); }
+void launch_commit(const DevMesh& d, const StepBuffers& b, cudaStream_t s) {
+    commit_kernel<<<blocks_for(d.n_points > 0 ? d.n_points : 1, 256), 256, 0, s>>>(d, b);
+}
+int launch_motion(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* scratch, cudaStream_t s) {
+    int launches = 0;
+    surface_kernel<<<1, 256, 0, s>>>(d, P, b, scratch);
+    launches++;
+    if (d.n_rail_a + d.n_rail_b > 0) {
+        rail_ab_kernel<<<d.n_rail_a + d.n_rail_b, 128, 0, s>>>(d, P, b.dt_cur, 0, d.n_rail_a + d.n_rail_b);
+        launches++;
+    }
+    if (d.n_rail_c > 0) {
+        rail_c_kernel<<<d.n_rail_c, 128, 0, s>>>(d, P, b.dt_cur, d.n_rail_a + d.n_rail_b, d.n_rail_c);
+        launches++;
+    }
+    if (d.n_rail_d > 0) {
+        rail_d_kernel<<<d.n_rail_d, 128, 0, s>>>(d, P, b.dt_cur, d.n_rail_a + d.n_rail_b + d.n_rail_c, d.n_rail_d);
+        launches++;
+    }
+    return launches;
+}
+void launch_hllc_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s) {
+    hllc_batch_kernel<<<blocks_for(n, 128), 128, 0, s>>>(P, n, in, out);
+}
+void launch_godunov_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s) {
+    godunov_batch_kernel<<<blocks_for(n, 128), 128, 0, s>>>(P, n, in, out);
+}
+
+}  // namespace gelios

@@ -1,0 +1,71 @@
+// Device-side views shared by the step kernels and the context (capi.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/gelios_b200.h"
+
+namespace gelios {
+
+// Read-mostly topology + mutable point geometry, SoA, all device pointers.
+//
+// Per-cell face slots ("s*" arrays) are laid out in the reference's Grans
+// order: slot g of cell c is gstart[c] + k for its k-th face.  A slot holds
+// what the owner cell needs about the face without chasing the face table:
+//   sA/sB   end points            snb   Sosed (neighbour cell)
+//   ssd     Sosed_down of the face (TVD on the owner side)
+//   ssd2    Sosed_down of its twin (TVD on the neighbour side)
+//   sinfo   face type | SI_GOD | SI_NP
+struct DevMesh {
+    int n_points = 0, n_cells = 0, n_faces = 0, n_main = 0;
+    int dims[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double *X = nullptr, *Y = nullptr, *X2 = nullptr, *Y2 = nullptr, *Vx = nullptr, *Vy = nullptr;
+    int* cnt = nullptr;
+    const int32_t* ptype = nullptr;
+    const int32_t *cstart = nullptr, *contour = nullptr, *gstart = nullptr;
+    const uint32_t* cflags = nullptr;
+    const int32_t *sA = nullptr, *sB = nullptr, *snb = nullptr, *ssd = nullptr, *ssd2 = nullptr;
+    const uint32_t* sinfo = nullptr;
+    const int32_t *fA = nullptr, *fB = nullptr, *ftype = nullptr, *fmaster = nullptr, *fsosed = nullptr,
+                  *fcopy = nullptr, *fsdown = nullptr;
+    const int32_t *rtype = nullptr, *rM = nullptr, *rpstart = nullptr, *rpts = nullptr, *rkstart = nullptr,
+                  *rkeys = nullptr;
+    const double* rs = nullptr;
+    int n_rail_a = 0, n_rail_b = 0, n_rail_c = 0, n_rail_d = 0;
+    const int32_t *lc = nullptr, *li = nullptr, *lo = nullptr;
+    int n_lc = 0, n_li = 0, n_lo = 0;
+    const double *Hn = nullptr, *Hu = nullptr, *Hv = nullptr, *HT = nullptr, *ku = nullptr, *kv = nullptr,
+                 *kT = nullptr, *r_istoch = nullptr;
+    const int32_t *cback = nullptr, *cnext = nullptr;
+};
+
+// Buffers of one time step (double buffering of the state like par[now1] ->
+// par[now2]; centroids of the current/next point positions; dt words).
+struct StepBuffers {
+    const double* cur[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    double* nxt[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    const double* cx = nullptr;
+    const double* cy = nullptr;
+    double* cx_next = nullptr;
+    double* cy_next = nullptr;
+    const double* dt_cur = nullptr;
+    double* dt_next = nullptr;
+    unsigned long long* dt_acc = nullptr;
+    unsigned long long* counters = nullptr;  // [0] ro clamps, [1] p clamps
+    int* status = nullptr;
+};
+
+void launch_centroid(const DevMesh& d, const double* X, const double* Y, double* cx, double* cy, cudaStream_t s);
+void launch_stationary(const DevMesh& d, const gelios_params& P, const StepBuffers& b, cudaStream_t s);
+void launch_mk2_cells(const DevMesh& d, const gelios_params& P, const StepBuffers& b, cudaStream_t s);
+void launch_inner(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const int32_t* list, int n,
+                  cudaStream_t s);
+void launch_dt_finalize(const StepBuffers& b, cudaStream_t s);
+void launch_commit(const DevMesh& d, const StepBuffers& b, cudaStream_t s);
+int launch_motion(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* scratch, cudaStream_t s);
+void launch_hllc_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s);
+void launch_godunov_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s);
+
+}  // namespace gelios

@@ -1,0 +1,193 @@
+"""Host-side mirror of the reference's operator interface for the plasma step.
+
+The reference drives its time step through member functions of ``Setka``
+(Setka.h:21-235).  :class:`Setka` keeps those names and their meaning on top
+of the C ABI (include/gelios_b200.h):
+
+==========================================  =====================================
+reference (Setka.h)                          here
+==========================================  =====================================
+``Setka(N1..M4)`` (Setka.cpp:19-1076)        ``Setka.from_constructor(N1..M4)``
+``TVD_prepare()`` (Setka.cpp:1294-1492)      ``TVD_prepare()``
+``Init_conditions()`` (Setka.cpp:5149-5203)  ``Init_conditions()``
+``Cell::par[0/1]``                           ``par(buf)`` / ``set_par(buf, state)``
+``Go_stationary(int)``                       ``Go_stationary(step)``
+``Go_5_komponent__MK2(int)``                 ``Go_5_komponent__MK2(step)``
+``Go_stationary_5_komponent_inner_MK2(int)`` ``Go_stationary_5_komponent_inner_MK2(step)``
+==========================================  =====================================
+
+As in the reference, a step call restarts dt at 1e-8 and the newest state
+ends in ``par[step % 2]``; cells a loop skips keep their old values in both
+buffers.  Differences in error behaviour: where the reference calls
+``exit(-1)`` the step raises :class:`StepError` carrying the device status
+flags instead (the kernels never trap).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from .mesh import Mesh
+
+STATUS_BITS = {1: "newton/bisection iteration cap", 2: "non-positive TVD state", 4: "negative Newton pressure",
+               8: "broken source chain", 16: "non-finite dt"}
+
+
+class StepError(RuntimeError):
+    def __init__(self, status: N.GeliosStatus):
+        names = [v for k, v in STATUS_BITS.items() if status.flags & k]
+        super().__init__("device status: " + ", ".join(names))
+        self.status = status
+
+
+class Setka:
+    """A grid + state resident on one GPU, stepped by the sm_100a kernels."""
+
+    def __init__(self, mesh: Mesh, params: N.GeliosParams | None = None, device: int = 0,
+                 raise_on_status: bool = False):
+        self.mesh = mesh
+        self.params = params if params is not None else N.reference_params()
+        self.raise_on_status = raise_on_status
+        L = N.lib()
+        h = C.c_void_p()
+        N.check(L.gelios_create(C.byref(h), C.byref(self.params), int(device)), "gelios_create")
+        self._h = h
+        self._L = L
+        v, keep = mesh.view()
+        N.check(L.gelios_upload_topology(self._h, C.byref(v)), "gelios_upload_topology")
+        del keep
+        self.last_status = N.GeliosStatus()
+        self.All_Cells_Inner = np.zeros(0, np.int32)
+
+    # ------------------------------------------------------------ construction
+    @classmethod
+    def from_constructor(cls, N1, N2, N3, N4, M1, M2, M3, M4, params=None, device=0) -> "Setka":
+        return cls(Mesh.setka(N1, N2, N3, N4, M1, M2, M3, M4, tvd=True), params, device)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.gelios_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, params: N.GeliosParams):
+        self.params = params
+        N.check(self._L.gelios_set_params(self._h, C.byref(params)), "gelios_set_params")
+
+    # ------------------------------------------------------------ reference-named operations
+    def TVD_prepare(self):
+        """Setka::TVD_prepare: recompute TVD neighbours and source chains from
+        the current point positions and re-upload the topology."""
+        self.mesh.tvd_prepare()
+        v, keep = self.mesh.view()
+        st = [self.par(0), self.par(1)]
+        N.check(self._L.gelios_upload_topology(self._h, C.byref(v)), "gelios_upload_topology")
+        self.set_par(0, st[0])
+        self.set_par(1, st[1])
+
+    def Init_conditions(self):
+        """Setka::Init_conditions (Setka.cpp:5149-5203) into par[0] and par[1]."""
+        from .workloads import init_conditions_reference
+
+        st = init_conditions_reference(self.mesh)
+        self.set_par(0, st)
+        self.set_par(1, st)
+
+    def build_inner_list(self, r_max: float | None = None):
+        """All_Cells_Inner of main (Gelios_2D.cpp:152-231): centroid radius <= R111_."""
+        r = self.params.R111 if r_max is None else r_max
+        self.All_Cells_Inner = self.mesh.inner_cells(r)
+        a = np.ascontiguousarray(self.All_Cells_Inner, np.int32)
+        ptr = a.ctypes.data_as(C.POINTER(C.c_int32)) if len(a) else C.cast(None, C.POINTER(C.c_int32))
+        N.check(self._L.gelios_set_inner_cells(self._h, ptr, len(a)), "gelios_set_inner_cells")
+
+    def Go_stationary(self, step: int) -> N.GeliosStatus:
+        return self._go(N.FORM_STATIONARY, step)
+
+    def Go_5_komponent__MK2(self, step: int) -> N.GeliosStatus:
+        return self._go(N.FORM_MK2, step)
+
+    def Go_stationary_5_komponent_inner_MK2(self, step: int) -> N.GeliosStatus:
+        return self._go(N.FORM_INNER_MK2, step)
+
+    def _go(self, form: int, step: int) -> N.GeliosStatus:
+        st = N.GeliosStatus()
+        N.check(self._L.gelios_step(self._h, int(form), int(step), C.byref(st)), "gelios_step")
+        self.last_status = st
+        if self.raise_on_status and st.flags:
+            raise StepError(st)
+        return st
+
+    def step_async(self, form: int, step: int):
+        """Enqueue `step` iterations without synchronising (timing loops)."""
+        N.check(self._L.gelios_step(self._h, int(form), int(step), None), "gelios_step")
+
+    def synchronize(self):
+        N.check(self._L.gelios_synchronize(self._h), "gelios_synchronize")
+
+    # ------------------------------------------------------------ state
+    def set_par(self, buf: int, st: np.ndarray):
+        """Cell::par[buf] = rows (ro, p, u, v, Q) of st (shape (5, n_cells))."""
+        st = np.ascontiguousarray(st, np.float64)
+        rows = [np.ascontiguousarray(st[k]) for k in range(5)]
+        N.check(self._L.gelios_upload_state(self._h, int(buf), *rows), "gelios_upload_state")
+
+    def par(self, buf: int) -> np.ndarray:
+        out = [np.zeros(self.mesh.n_cells) for _ in range(5)]
+        N.check(self._L.gelios_download_state(self._h, int(buf), *out), "gelios_download_state")
+        return np.stack(out)
+
+    def set_mc(self, Hn, Hu, Hv, HT, ku, kv, kT):
+        """Monte-Carlo moments of par[0] (H_n/H_u/H_v/H_T[4], k_u/k_v/k_T)."""
+        f = lambda a: np.ascontiguousarray(a, np.float64).ravel()  # noqa: E731
+        N.check(self._L.gelios_upload_mc(self._h, f(Hn), f(Hu), f(Hv), f(HT), f(ku), f(kv), f(kT)),
+                "gelios_upload_mc")
+
+    def points(self) -> tuple[np.ndarray, np.ndarray]:
+        x = np.zeros(self.mesh.n_points)
+        y = np.zeros(self.mesh.n_points)
+        N.check(self._L.gelios_download_points(self._h, x, y), "gelios_download_points")
+        return x, y
+
+    PHASES = ("centroids", "motion", "cells", "commit_dt")
+
+    def set_phase_timing(self, on: bool):
+        N.check(self._L.gelios_set_phase_timing(self._h, int(bool(on))), "gelios_set_phase_timing")
+
+    def phase_times(self, reset: bool = True) -> dict:
+        """Per-phase device ms and launch counts accumulated while timing was on."""
+        ms = np.zeros(5)
+        ln = np.zeros(5, np.int64)
+        N.check(self._L.gelios_phase_times(self._h, ms, ln, int(bool(reset))), "gelios_phase_times")
+        names = ("centroids", "surface", "motion", "cells", "commit_dt")
+        return {names[k]: (float(ms[k]), int(ln[k])) for k in range(5)}
+
+    def launches(self) -> int:
+        return int(self._L.gelios_last_launch_count(self._h))
+
+    def stream_handle(self) -> int:
+        return int(self._L.gelios_stream(self._h) or 0)
+
+
+def hllc_batch(params: N.GeliosParams, rows: np.ndarray) -> np.ndarray:
+    """Device HLLC_2d_Korolkov_b_s over rows of 16 inputs -> rows of 9 outputs."""
+    rows = np.ascontiguousarray(rows, np.float64)
+    out = np.zeros((len(rows), 9))
+    N.check(N.lib().gelios_hllc_batch(C.byref(params), len(rows), rows.ravel(), out.ravel()), "gelios_hllc_batch")
+    return out
+
+
+def godunov_batch(params: N.GeliosParams, rows: np.ndarray) -> np.ndarray:
+    """Device Godunov_Solver_Alexashov over rows of 15 inputs -> rows of 10 outputs."""
+    rows = np.ascontiguousarray(rows, np.float64)
+    out = np.zeros((len(rows), 10))
+    N.check(N.lib().gelios_godunov_batch(C.byref(params), len(rows), rows.ravel(), out.ravel()),
+            "gelios_godunov_batch")
+    return out

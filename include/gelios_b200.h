@@ -136,6 +136,10 @@ gelios_mesh *gelios_mesh_build_polar(int n_theta, int n_r, double r_in, double r
 /* Setka::TVD_prepare, Setka.cpp:1294-1492: Sosed_up/Sosed_down of every face,
  * Back/Next/r_istoch of every cell (uses the reference's colliding face numbers). */
 int gelios_mesh_tvd_prepare(gelios_mesh *m);
+/* Setka::TVD_prepare on a caller's view: fills n_faces Sosed_up/Sosed_down
+ * and n_cells Back/Next/r_istoch (any output pointer may be NULL). */
+int gelios_tvd_prepare_view(const gelios_mesh_view *v, int32_t *sosed_up, int32_t *sosed_down, int32_t *back,
+                            int32_t *next, double *r_istoch);
 /* Cells whose centroid radius is <= r_max (All_Cells_Inner, Gelios_2D.cpp:152-231). */
 int gelios_mesh_inner_cells(const gelios_mesh *m, double r_max, int32_t *out, int32_t cap);
 /* Pointers into the mesh (valid until gelios_mesh_free). */
@@ -174,6 +178,14 @@ int gelios_state_device_ptr(gelios_ctx *ctx, int buf, double **dptr);
 void *gelios_stream(gelios_ctx *ctx);
 /* Kernel launches issued by the last gelios_step call. */
 int64_t gelios_last_launch_count(gelios_ctx *ctx);
+/* Phase timing: when enabled, gelios_step brackets each phase with CUDA
+ * events on the context stream and accumulates, per phase, the device time
+ * and the number of launches (phases: 0 centroids, 1 Move_surface,
+ * 2 rail motion, 3 cell update, 4 commit/dt).  gelios_phase_times
+ * synchronises, writes ms[5] and launches[5] accumulated since the last
+ * reset, and resets when `reset` is non-zero. */
+int gelios_set_phase_timing(gelios_ctx *ctx, int enabled);
+int gelios_phase_times(gelios_ctx *ctx, double *ms, int64_t *launches, int reset);
 
 /* ---- per-face solvers on the device (known-answer checks) ------------------
  * Batched HLLC_2d_Korolkov_b_s (Setka.cpp:10484-10700): in[n*16] =

@@ -1041,7 +1041,9 @@ void go_move_surface(void *h, int ii, double dt) {
                 c->count[b]++;
             }
         }
-        for (int j = 0; j < nI; j++) { /* walks Line_Contact (Setka.cpp:3718-3731) */
+        /* walks Line_Contact (Setka.cpp:3718-3731); the reference reads past
+         * its end when Line_Inner is longer, here the walk stops there */
+        for (int j = 0; j < nI && j < nC; j++) {
             int a = fA[LC[j]];
             if (c->count[a] > 0) {
                 c->Vx[a] /= (1.0 * c->count[a]);
@@ -1096,7 +1098,7 @@ void go_move_surface(void *h, int ii, double dt) {
                 }
             }
         }
-        for (int j = 0; j < nO; j++) { /* walks Line_Contact (Setka.cpp:3829-3837) */
+        for (int j = 0; j < nO && j < nC; j++) { /* walks Line_Contact (Setka.cpp:3829-3837) */
             int a = fA[LC[j]];
             if (c->count[a] > 0) {
                 c->Vx[a] /= (1.0 * c->count[a]);

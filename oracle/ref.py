@@ -83,8 +83,20 @@ def lib(fast: bool = False) -> C.CDLL:
     L.gref_hlld.restype = C.c_double
     L.gref_hlld.argtypes = [_f64p, _f64p, _f64p, _f64p, _f64p, C.c_double, C.c_double]
     L.gref_constants.argtypes = [_f64p]
+    L.gref_set_threads.argtypes = [C.c_int]
+    L.gref_max_threads.restype = C.c_int
+    L.gref_set_threads(1)
     _LIBS[name] = L
     return L
+
+
+def set_threads(n: int, fast: bool = False) -> None:
+    """OpenMP threads of the reference loops (1 = parity mode)."""
+    lib(fast).gref_set_threads(int(n))
+
+
+def max_threads() -> int:
+    return int(lib().gref_max_threads())
 
 
 def available() -> bool:
@@ -128,7 +140,7 @@ class RefSetka:
             i32(m["gran_start"]), i32(m["gran"]),
             int(m["n_main"]), len(m["face_A"]) - int(m["n_main"]), i32(m["face_A"]), i32(m["face_B"]),
             i32(m["face_type"]), i32(m["face_master"]), i32(m["face_sosed"]), i32(m["face_copy"]),
-            i32(m["face_main"]),
+            i32(m["face_main"] if "face_main" in m else (np.arange(len(m["face_A"])) < int(m["n_main"]))),
             nrail, i32(m["rail_type"]) if nrail else empty_i, f64(m["rail_s"]) if nrail else np.zeros(1),
             i32(m["rail_M"]) if nrail else empty_i, i32(m["rail_pstart"]), i32(m["rail_points"]) if nrail else empty_i,
             i32(m["rail_kstart"]), i32(m["rail_keys"]) if nrail else empty_i,

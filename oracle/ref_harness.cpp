@@ -15,6 +15,7 @@
 // Nothing in the product links or loads this file.
 #include "Help.h"
 
+#include <omp.h>
 #include <unistd.h>
 #include <cstdint>
 #include <cstring>
@@ -122,6 +123,11 @@ Setka* dummy() {
 }  // namespace
 
 extern "C" {
+
+// OpenMP threads of the reference loops (1 for parity runs: the reference's
+// multithreaded dt reduction is racy, Setka.cpp:10141, 10359-10393).
+void gref_set_threads(int n) { omp_set_num_threads(n > 0 ? n : 1); }
+int gref_max_threads(void) { return omp_get_num_procs(); }
 
 // ---------------------------------------------------------------- lifecycle
 void* gref_setka_new(int N1, int N2, int N3, int N4, int M1, int M2, int M3, int M4) {

@@ -1,0 +1,103 @@
+"""Generates the golden fixtures of tests/golden from the compiled reference.
+
+Run where the reference tree and oracle/_ref/libgelios_ref.so exist:
+    python tests/golden/make_golden.py
+The fixtures are the reference's own outputs (HLLC_2d_Korolkov_b_s,
+Godunov_Solver_Alexashov, and short Go_stationary / Go_5_komponent__MK2 /
+Go_stationary_5_komponent_inner_MK2 runs on Setka(4,3,3,10,23,6,7,7)), so the
+oracle stays pinned where the reference cannot be built.
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parent.parent))
+
+from oracle import ref  # noqa: E402
+from gelios_2d_b200 import workloads as W  # noqa: E402
+from gelios_2d_b200.mesh import Mesh  # noqa: E402
+
+SMALL = (4, 3, 3, 10, 23, 6, 7, 7)
+
+
+def hllc_cases(n=96, seed=11):
+    u = W.splitmix64(seed, n * 16).reshape(n, 16)
+    rows = []
+    # the smoke check of main (Gelios_2D.cpp:46-67) first
+    rows.append([2.0, 1.0, 2.0, 1.0, 0.0, 1.0, 1.0, 1.0, 0.5, 0.0, 0.0, 1.0, 0.0, 10.0, 1, 0])
+    for i in range(1, n):
+        a = u[i]
+        th = 2 * np.pi * a[11]
+        rows.append([0.1 + 2 * a[0], 50 * a[1], 0.05 + 3 * a[2], 4 * (a[3] - 0.5), 4 * (a[4] - 0.5),
+                     0.1 + 2 * a[5], 50 * a[6], 0.05 + 3 * a[7], 4 * (a[8] - 0.5), 4 * (a[9] - 0.5),
+                     (a[10] - 0.5) * 2.0 if i % 3 else 0.0, np.cos(th), np.sin(th), 0.01 + a[12],
+                     i % 2, (i // 2) % 2])
+    return np.array(rows)
+
+
+def godunov_cases(n=96, seed=13):
+    u = W.splitmix64(seed, n * 16).reshape(n, 16)
+    rows = []
+    for i in range(n):
+        a = u[i]
+        th = 2 * np.pi * a[10]
+        scale = 1.0 if i % 4 else 20.0  # strong shocks
+        rows.append([0.1 + 2 * a[0], 0.05 + 3 * a[1] * scale, 3 * (a[2] - 0.5), 3 * (a[3] - 0.5), 0.0,
+                     0.1 + 2 * a[4], 0.05 + 3 * a[5], 3 * (a[6] - 0.5) - (2.0 if i % 5 == 0 else 0.0),
+                     3 * (a[7] - 0.5), 0.0, np.cos(th), np.sin(th), 0.0,
+                     (a[8] - 0.5) if i % 2 else 0.0, 0.01 + a[9]])
+    return np.array(rows)
+
+
+def main():
+    ref.set_threads(1)
+    h = hllc_cases()
+    out = np.zeros((len(h), 9))
+    for i, r in enumerate(h):
+        t, P, PQ, v = ref.hllc(r[0:5], r[5:10], r[10], r[11], r[12], r[13], int(r[14]), bool(r[15]))
+        out[i] = [t, *P, PQ, *v]
+    np.savez_compressed(HERE / "kat_hllc.npz", inputs=h, outputs=out)
+    g = godunov_cases()
+    out = np.zeros((len(g), 9))
+    for i, r in enumerate(g):
+        t, q, d = ref.godunov(r[0:5], r[5:10], r[10:13], r[13], r[14])
+        out[i] = [t, *q, *d]
+    np.savez_compressed(HERE / "kat_godunov.npz", inputs=g, outputs=out)
+
+    # short runs on the small rail grid
+    S = ref.RefSetka.constructor(*SMALL)
+    S.tvd_prepare()
+    S.init_conditions()
+    m = Mesh.from_arrays(S.export())
+    st0 = S.get_state(0)
+    mc = W.mc_fields(m, seed=5)
+    res = {"state0": st0, "Hn": mc[0], "Hu": mc[1], "Hv": mc[2], "HT": mc[3], "ku": mc[4], "kv": mc[5], "kT": mc[6]}
+    for name, steps in (("stationary", 3), ("mk2", 4), ("inner", 3)):
+        R = ref.RefSetka.constructor(*SMALL)
+        R.tvd_prepare()
+        R.set_state(0, st0)
+        R.set_state(1, st0)
+        R.set_mc(*mc)
+        if name == "stationary":
+            R.go_stationary(steps)
+        elif name == "mk2":
+            R.go_mk2(steps)
+        else:
+            R.build_inner_list()
+            res["inner_list"] = R.inner_list()
+            R.go_inner_mk2(steps)
+        res[f"{name}_par0"] = R.get_state(0)
+        res[f"{name}_par1"] = R.get_state(1)
+        pm = R.point_motion()
+        res[f"{name}_x"] = pm["x"]
+        res[f"{name}_y"] = pm["y"]
+    np.savez_compressed(HERE / "steps_small.npz", **res)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

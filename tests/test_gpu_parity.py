@@ -1,0 +1,228 @@
+"""Parity of the sm_100a kernels with the oracle (C restatement pinned to the
+reference), called through the C ABI.
+
+Tolerances (FP64 drop-in; the north_star bar): max-norm relative error per
+primitive variable <= 1e-12 after one/two steps from a common state and
+<= 1e-9 after 1000 steps.  Point coordinates after grid motion agree to
+1e-13 relative (the rails use cos/sin/pow of libdevice vs glibc: ~1 ulp).
+The FP32-flux form is compared to the FP64 oracle with a loose bound and its
+L1/Linf errors are reported.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import gelios_2d_b200 as g
+from gelios_2d_b200 import _native as N
+from gelios_2d_b200 import workloads as W
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLD = Path(__file__).resolve().parent / "golden"
+MEDIUM = (30, 7, 11, 20, 60, 20, 40, 40)
+SMALL = (4, 3, 3, 10, 23, 6, 7, 7)
+
+
+def rel_err(a: np.ndarray, b: np.ndarray) -> float:
+    """max over variables of max|a-b| / max|b| (per row of a (5, n) state)."""
+    out = 0.0
+    for k in range(a.shape[0]):
+        s = np.max(np.abs(b[k]))
+        if s > 0:
+            out = max(out, float(np.max(np.abs(a[k] - b[k])) / s))
+    return out
+
+
+def go_params(p: N.GeliosParams) -> O.GoParams:
+    d = {n: getattr(p, n) for n, _ in O.GoParams._fields_ if n != "pad_"}
+    return O.GoParams(**d, pad_=0)
+
+
+def _pair(mesh, params, st0, mc=None):
+    dev = g.Setka(mesh, params)
+    dev.set_par(0, st0)
+    dev.set_par(1, st0)
+    ora = O.Oracle(go_params(params), mesh)
+    ora.set_state(0, st0)
+    ora.set_state(1, st0)
+    if mc is not None:
+        dev.set_mc(*mc)
+        ora.set_mc(*mc)
+    return dev, ora
+
+
+# ------------------------------------------------------------------ per-face kernels
+def test_hllc_device_vs_oracle():
+    d = np.load(GOLD / "kat_hllc.npz")
+    P = N.reference_params()
+    dev = g.hllc_batch(P, d["inputs"])
+    ref = d["outputs"]
+    # [time, P0..P3, PQ, Vl, Vc, Vp]
+    scale = np.maximum(np.abs(ref), 1e-300)
+    err = np.abs(dev - ref) / np.maximum(scale, np.max(np.abs(ref), axis=1, keepdims=True) * 1e-3)
+    assert np.max(err) <= 1e-13, np.max(err)
+
+
+def test_hllc_fp32_flux_form():
+    d = np.load(GOLD / "kat_hllc.npz")
+    P = N.reference_params(precision=N.PREC_FP32_FLUX)
+    dev = g.hllc_batch(P, d["inputs"])
+    ref = d["outputs"]
+    rows = np.max(np.abs(ref[:, 1:6]), axis=1, keepdims=True)
+    err = np.abs(dev[:, 1:6] - ref[:, 1:6]) / rows
+    assert np.max(err) <= 1e-5, np.max(err)
+
+
+def test_godunov_device_vs_oracle():
+    d = np.load(GOLD / "kat_godunov.npz")
+    P = N.reference_params()
+    dev = g.godunov_batch(P, d["inputs"])
+    ref = d["outputs"]
+    assert np.all(dev[:, 9] == 0)
+    rows = np.maximum(np.max(np.abs(ref[:, 1:6]), axis=1), 1e-300)
+    err = np.max(np.abs(dev[:, 1:6] - ref[:, 1:6]), axis=1) / rows
+    assert np.max(err) <= 1e-11, np.max(err)
+    assert np.max(np.abs(dev[:, 0] - ref[:, 0]) / np.abs(ref[:, 0])) <= 1e-11
+
+
+# ------------------------------------------------------------------ Go_stationary (plain single fluid)
+@pytest.mark.parametrize("steps", [1, 2, 10])
+def test_stationary_plain_small(steps):
+    mesh = W.plain_mesh(36, 24)
+    P = W.plain_params()
+    st0 = W.plain_initial(mesh, P, seed=3)
+    dev, ora = _pair(mesh, P, st0)
+    s = dev.Go_stationary(steps)
+    ora.stationary(steps)
+    buf = steps % 2
+    assert s.result_buf == buf
+    e = rel_err(dev.par(buf), ora.get_state(buf))
+    assert e <= 1e-12, e
+    assert abs(s.dt - ora.last_dt()) <= 1e-12 * ora.last_dt()
+    assert s.flags == 0
+
+
+def test_stationary_plain_full_1000_steps():
+    """The plain workload at full size (180 x 120), 1000 steps."""
+    mesh = W.plain_mesh()
+    P = W.plain_params()
+    st0 = W.plain_initial(mesh, P, seed=2024)
+    dev, ora = _pair(mesh, P, st0)
+    dev.Go_stationary(1000)
+    ora.stationary(1000)
+    e = rel_err(dev.par(0), ora.get_state(0))
+    assert e <= 1e-9, e
+
+
+# ------------------------------------------------------------------ Go_5_komponent__MK2 (moving grid)
+@pytest.mark.parametrize("steps", [1, 2, 12])
+def test_mk2_moving_grid(steps):
+    mesh = g.Mesh.setka(*MEDIUM)
+    P = N.reference_params()
+    st0 = W.init_conditions_reference(mesh)
+    mc = W.mc_fields(mesh, seed=9)
+    dev, ora = _pair(mesh, P, st0, mc)
+    s = dev.Go_5_komponent__MK2(steps)
+    ora.mk2(steps)
+    buf = steps % 2
+    e = rel_err(dev.par(buf), ora.get_state(buf))
+    e_other = rel_err(dev.par(1 - buf), ora.get_state(1 - buf))
+    tol = 1e-12 if steps <= 2 else 1e-10
+    assert e <= tol, e
+    assert e_other <= tol, e_other
+    x, y = dev.points()
+    pts = ora.points()
+    assert np.max(np.abs(x - pts["x"]) / np.maximum(np.abs(pts["x"]), 1e-3)) <= 1e-13
+    assert np.max(np.abs(y - pts["y"]) / np.maximum(np.abs(pts["y"]), 1e-3)) <= 1e-13
+    st = ora.status()
+    assert (s.flags & 1) == (st[0] & 1)
+
+
+def test_inner_mk2():
+    mesh = g.Mesh.setka(*MEDIUM)
+    P = N.reference_params()
+    st0 = W.init_conditions_reference(mesh)
+    mc = W.mc_fields(mesh, seed=4)
+    dev, ora = _pair(mesh, P, st0, mc)
+    dev.build_inner_list()
+    assert len(dev.All_Cells_Inner) > 0
+    ora.set_inner_list(dev.All_Cells_Inner)
+    dev.Go_stationary_5_komponent_inner_MK2(3)
+    ora.inner_mk2(3)
+    for b in (0, 1):
+        e = rel_err(dev.par(b), ora.get_state(b))
+        assert e <= 1e-12, e
+
+
+def test_mk2_golden_fixture():
+    """Device vs the reference's own output stored in tests/golden."""
+    gd = np.load(GOLD / "steps_small.npz")
+    mesh = g.Mesh.setka(*SMALL)
+    dev = g.Setka(mesh, N.reference_params())
+    dev.set_par(0, gd["state0"])
+    dev.set_par(1, gd["state0"])
+    dev.set_mc(gd["Hn"], gd["Hu"], gd["Hv"], gd["HT"], gd["ku"], gd["kv"], gd["kT"])
+    dev.Go_5_komponent__MK2(4)
+    assert rel_err(dev.par(0), gd["mk2_par0"]) <= 1e-12
+    assert rel_err(dev.par(1), gd["mk2_par1"]) <= 1e-12
+
+
+def test_deterministic_runs():
+    mesh = g.Mesh.setka(*MEDIUM)
+    P = N.reference_params()
+    st0 = W.init_conditions_reference(mesh)
+    mc = W.mc_fields(mesh, seed=9)
+    outs = []
+    for _ in range(2):
+        dev = g.Setka(mesh, P)
+        dev.set_par(0, st0)
+        dev.set_par(1, st0)
+        dev.set_mc(*mc)
+        dev.Go_5_komponent__MK2(6)
+        outs.append((dev.par(0), dev.points()))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1][0], outs[1][1][0])
+
+
+# ------------------------------------------------------------------ precision form
+def test_fp32_flux_errors():
+    mesh = W.plain_mesh(36, 24)
+    P = W.plain_params()
+    st0 = W.plain_initial(mesh, P, seed=3)
+    dev32, ora = _pair(mesh, P.copy(precision=N.PREC_FP32_FLUX), st0)
+    dev32.Go_stationary(20)
+    ora.stationary(20)
+    a, b = dev32.par(0), ora.get_state(0)
+    for k, name in enumerate(("rho", "p", "u", "v")):
+        linf = np.max(np.abs(a[k] - b[k])) / np.max(np.abs(b[k]))
+        l1 = np.sum(np.abs(a[k] - b[k])) / np.sum(np.abs(b[k]))
+        print(f"FP32-flux {name}: L1 {l1:.3e} Linf {linf:.3e}")
+        assert linf <= 1e-4
+
+
+# ------------------------------------------------------------------ failure detection (no GPU fault)
+def test_iteration_cap_reports_status_without_hanging():
+    """A Newton/bisection cap of 1 (test-only parameter) must end the solve
+    with a status flag; the reference would exit(-1) (Solvers.cpp:1206-1273)."""
+    mesh = g.Mesh.setka(*MEDIUM)
+    P = N.reference_params(godunov_max_iter=1)
+    st0 = W.init_conditions_reference(mesh)
+    dev = g.Setka(mesh, P)
+    dev.set_par(0, st0)
+    dev.set_par(1, st0)
+    s = dev.Go_5_komponent__MK2(2)
+    assert s.flags & 1
+    dev2 = g.Setka(mesh, P, raise_on_status=True)
+    dev2.set_par(0, st0)
+    dev2.set_par(1, st0)
+    with pytest.raises(g.StepError):
+        dev2.Go_5_komponent__MK2(2)
+
+
+def test_launch_count_reported():
+    mesh = W.plain_mesh(36, 24)
+    P = W.plain_params()
+    dev, _ = _pair(mesh, P, W.plain_initial(mesh, P))
+    dev.Go_stationary(5)
+    assert dev.launches() == 1 + 2 * 5

@@ -1,0 +1,137 @@
+"""The C restatement (oracle/gelios_oracle.c) is pinned to the reference.
+
+Against the live compiled reference (oracle/_ref/libgelios_ref.so, the
+unmodified reference sources) and against the golden fixtures it produced
+(tests/golden/make_golden.py), with the reference's compile-time constants as
+parameters, the restatement must agree BIT FOR BIT.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from gelios_2d_b200 import workloads as W
+from gelios_2d_b200.mesh import Mesh
+from oracle import oracle as O
+
+GOLD = Path(__file__).resolve().parent / "golden"
+SMALL = (4, 3, 3, 10, 23, 6, 7, 7)
+MEDIUM = (30, 7, 11, 20, 60, 20, 40, 40)
+
+
+def test_hllc_known_answer_from_main_smoke_check():
+    # Gelios_2D.cpp:46-67 evaluated with the compiled reference
+    t, P, PQ, _ = O.hllc(O.reference_params(), (2, 1, 2, 1, 0), (1, 1, 1, 0.5, 0), 0.0, 1.0, 0.0, 10.0, 1)
+    assert t == 0.43649167310370851
+    assert P.tolist() == [2.0169953705134338, 3.9865567562696662, 0.0, 6.0199554761660163]
+    assert PQ == 1.0084976852567169
+
+
+def test_hllc_golden_bitexact():
+    d = np.load(GOLD / "kat_hllc.npz")
+    P0 = O.reference_params()
+    for r, o in zip(d["inputs"], d["outputs"]):
+        t, P, PQ, v = O.hllc(P0, r[0:5], r[5:10], r[10], r[11], r[12], r[13], int(r[14]), bool(r[15]))
+        assert np.array_equal(np.array([t, *P, PQ, *v]), o, equal_nan=True)
+
+
+def test_godunov_golden_bitexact():
+    d = np.load(GOLD / "kat_godunov.npz")
+    P0 = O.reference_params()
+    for r, o in zip(d["inputs"], d["outputs"]):
+        t, q, ds, st = O.godunov(P0, r[0:5], r[5:10], r[10:13], r[13], r[14])
+        assert st == 0
+        assert np.array_equal(np.array([t, *q, *ds]), o, equal_nan=True)
+
+
+def _oracle_on_small(mesh_dict, g):
+    o = O.Oracle(O.reference_params(), mesh_dict)
+    o.set_state(0, g["state0"])
+    o.set_state(1, g["state0"])
+    o.set_mc(g["Hn"], g["Hu"], g["Hv"], g["HT"], g["ku"], g["kv"], g["kT"])
+    return o
+
+
+@pytest.mark.parametrize("form,steps", [("stationary", 3), ("mk2", 4), ("inner", 3)])
+def test_steps_golden_bitexact(form, steps):
+    g = np.load(GOLD / "steps_small.npz")
+    m = Mesh.setka(*SMALL)
+    o = _oracle_on_small(m, g)
+    if form == "stationary":
+        o.stationary(steps)
+    elif form == "mk2":
+        o.mk2(steps)
+    else:
+        o.set_inner_list(g["inner_list"])
+        o.inner_mk2(steps)
+    for b in (0, 1):
+        assert np.array_equal(o.get_state(b), g[f"{form}_par{b}"])
+    pts = o.points()
+    assert np.array_equal(pts["x"], g[f"{form}_x"]) and np.array_equal(pts["y"], g[f"{form}_y"])
+
+
+def test_steps_live_reference_medium(have_ref):
+    from oracle import ref
+
+    S = ref.RefSetka.constructor(*MEDIUM)
+    S.tvd_prepare()
+    S.init_conditions()
+    m = Mesh.from_arrays(S.export())
+    st0 = S.get_state(0)
+    mc = W.mc_fields(m, seed=3)
+    S.set_mc(*mc)
+    o = O.Oracle(O.reference_params(), m)
+    o.set_state(0, st0)
+    o.set_state(1, st0)
+    o.set_mc(*mc)
+    S.go_mk2(6)
+    o.mk2(6)
+    assert np.array_equal(o.get_state(0), S.get_state(0))
+    assert np.array_equal(o.get_state(1), S.get_state(1))
+    pm = S.point_motion()
+    pts = o.points()
+    assert np.array_equal(pts["x"], pm["x"]) and np.array_equal(pts["y"], pm["y"])
+    S.go_stationary(3)
+    o.stationary(3)
+    assert np.array_equal(o.get_state(1), S.get_state(1))
+
+
+def test_polar_grid_through_reference_objects(have_ref):
+    """The polar grid of the plain workload, instantiated as reference objects,
+    stepped by the reference's own Go_stationary vs the restatement."""
+    from oracle import ref
+
+    m = Mesh.polar(24, 16, 1.0, 600.0)
+    P = O.reference_params()
+    st = W.plain_initial(m, W.plain_params(), seed=1)
+    S = ref.RefSetka.from_mesh(m)
+    S.set_state(0, st)
+    S.set_state(1, st)
+    o = O.Oracle(P, m)
+    o.set_state(0, st)
+    o.set_state(1, st)
+    S.go_stationary(5)
+    o.stationary(5)
+    assert np.array_equal(o.get_state(1), S.get_state(1))
+    assert np.array_equal(o.get_state(0), S.get_state(0))
+
+
+def test_phase_level_motion(have_ref):
+    """Move_surface + Move_Setka_Calculate_2 alone (point velocities and x2/y2)."""
+    from oracle import ref
+
+    S = ref.RefSetka.constructor(*MEDIUM)
+    S.tvd_prepare()
+    S.init_conditions()
+    m = Mesh.from_arrays(S.export())
+    o = O.Oracle(O.reference_params(), m)
+    st0 = S.get_state(0)
+    o.set_state(0, st0)
+    o.set_state(1, st0)
+    S.move_surface(0, 1e-3)
+    o.move_surface(0, 1e-3)
+    S.move_setka2(1e-3)
+    o.move_setka2(1e-3)
+    a, b = S.point_motion(), o.points()
+    for k in ("Vx", "Vy", "x2", "y2", "count"):
+        assert np.array_equal(a[k], b[k]), k
