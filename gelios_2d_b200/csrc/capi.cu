@@ -87,7 +87,8 @@ struct gelios_ctx {
     DBuf X, Y, X2, Y2, Vx, Vy, cnt, ptype, cstart, contour, gstart, cflags, sA, sB, snb, ssd, ssd2, sinfo;
     DBuf fA, fB, ftype, fmaster, fsosed, fcopy, fsdown;
     DBuf rtype, rM, rpstart, rpts, rkstart, rkeys, rs;
-    DBuf lc, li, lo;
+    DBuf lc, li, lo, sp_point, sp_line, sp_inc, sp_ainc, sp_fix;
+    DBuf u_slot, u_cell, u_twin, flux;
     DBuf Hn, Hu, Hv, HT, ku, kv, kT, r_istoch, cback, cnext;
     // state par[2] x 5 fields, centroids [2], scratch
     DBuf state[2];
@@ -96,6 +97,7 @@ struct gelios_ctx {
     DBuf surface;  // Move_surface per-face speeds
     DBuf inner;
     int n_inner = 0;
+    int n_sp = 0;
     int64_t launches = 0;
     // phase timing
     bool timing = false;
@@ -312,6 +314,105 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
         }
         (t == 0 ? na : t == 1 ? nb : t == 2 ? ncr : nd)++;
     }
+    // face units: every slot of a cell except the twins of interior faces,
+    // whose flux comes from the unit of the main face (see step_kernels.cu)
+    std::vector<int32_t> u_slot, u_cell, u_twin;
+    {
+        std::vector<int32_t> slot_of_face(nf, -1);
+        for (int c = 0; c < nc; c++)
+            for (int g = v->gran_start[c]; g < v->gran_start[c + 1]; g++) slot_of_face[v->gran[g]] = g;
+        for (int c = 0; c < nc; c++)
+            for (int g = v->gran_start[c]; g < v->gran_start[c + 1]; g++) {
+                const int f = v->gran[g];
+                const bool interior = v->face_type[f] == G_USUALY;
+                if (interior && f >= v->n_main) continue;  // twin of a main face
+                int twin = -1;
+                if (interior) {
+                    twin = slot_of_face[v->face_copy[f]];
+                    if (twin < 0) {
+                        set_error("gelios_upload_topology: interior face whose twin is in no cell");
+                        return GELIOS_E_MESH;
+                    }
+                }
+                u_slot.push_back(g);
+                u_cell.push_back(c);
+                u_twin.push_back(twin);
+            }
+        // every interior twin must be covered by its main face's unit
+        std::vector<char> covered(ng, 0);
+        for (size_t u = 0; u < u_slot.size(); u++) {
+            covered[u_slot[u]] = 1;
+            if (u_twin[u] >= 0) covered[u_twin[u]] = 1;
+        }
+        for (int g = 0; g < ng; g++)
+            if (!covered[g]) {
+                set_error("gelios_upload_topology: interior copy face without its main face in a cell");
+                return GELIOS_E_MESH;
+            }
+    }
+    // surface-tracking nodes (see surface_nodes_kernel)
+    std::vector<int32_t> sp_point, sp_line, sp_inc, sp_ainc, sp_fix(12, 0);
+    {
+        std::vector<int32_t> local(np, -1);
+        const int32_t* lines[3] = {v->line_contact, v->line_inner, v->line_outer};
+        const int nl[3] = {v->n_contact, v->n_inner_line, v->n_outer_line};
+        int base = 0;
+        for (int L = 0; L < 3; L++) {
+            for (int j = 0; j < nl[L]; j++) {
+                const int f = lines[L][j];
+                if (f < 0 || f >= nf) {
+                    set_error("gelios_upload_topology: tracked-line face out of range");
+                    return GELIOS_E_MESH;
+                }
+                const int ends[2] = {v->face_A[f], v->face_B[f]};
+                for (int role = 0; role < 2; role++) {
+                    const int p = ends[role];
+                    int id = local[p];
+                    if (id < 0) {
+                        id = static_cast<int>(sp_point.size());
+                        local[p] = id;
+                        sp_point.push_back(p);
+                        sp_line.push_back(L);
+                        for (int k = 0; k < 4; k++) {
+                            sp_inc.push_back(-1);
+                            sp_ainc.push_back(-1);
+                        }
+                    } else if (sp_line[id] != L) {
+                        set_error("gelios_upload_topology: a point lies on two tracked lines");
+                        return GELIOS_E_MESH;
+                    }
+                    int k = 0;
+                    while (k < 4 && sp_inc[4 * id + k] >= 0) k++;
+                    if (k == 4) {
+                        set_error("gelios_upload_topology: tracked-line point with more than 4 faces");
+                        return GELIOS_E_MESH;
+                    }
+                    sp_inc[4 * id + k] = ((base + j) << 1) | role;
+                    if (L == 0 && role == 0) {
+                        int q = 0;
+                        while (q < 4 && sp_ainc[4 * id + q] >= 0) q++;
+                        if (q == 4) {
+                            set_error("gelios_upload_topology: contact point is the A end of more than 4 faces");
+                            return GELIOS_E_MESH;
+                        }
+                        sp_ainc[4 * id + q] = j;
+                    }
+                }
+            }
+            if (nl[L] > 0) {
+                sp_fix[4 * L + 0] = local[v->face_A[lines[L][0]]];
+                sp_fix[4 * L + 1] = local[v->face_B[lines[L][0]]];
+                sp_fix[4 * L + 2] = local[v->face_A[lines[L][nl[L] - 1]]];
+                sp_fix[4 * L + 3] = local[v->face_B[lines[L][nl[L] - 1]]];
+            }
+            base += nl[L];
+        }
+    }
+    const int n_sp = static_cast<int>(sp_point.size());
+    if (n_sp * (2 * sizeof(double) + sizeof(int)) > 200 * 1024) {
+        set_error("gelios_upload_topology: too many tracked-line points for one CTA");
+        return GELIOS_E_LIMIT;
+    }
     int rc = 0;
     rc |= upload(ctx->X, v->x, np, s);
     rc |= upload(ctx->Y, v->y, np, s);
@@ -351,6 +452,15 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     rc |= upload(ctx->lc, v->line_contact, v->n_contact, s);
     rc |= upload(ctx->li, v->line_inner, v->n_inner_line, s);
     rc |= upload(ctx->lo, v->line_outer, v->n_outer_line, s);
+    rc |= upload(ctx->u_slot, u_slot.data(), u_slot.size(), s);
+    rc |= upload(ctx->u_cell, u_cell.data(), u_cell.size(), s);
+    rc |= upload(ctx->u_twin, u_twin.data(), u_twin.size(), s);
+    rc |= upload<double>(ctx->flux, nullptr, 5 * static_cast<size_t>(ng), s);
+    rc |= upload(ctx->sp_point, sp_point.data(), sp_point.size(), s);
+    rc |= upload(ctx->sp_line, sp_line.data(), sp_line.size(), s);
+    rc |= upload(ctx->sp_inc, sp_inc.data(), sp_inc.size(), s);
+    rc |= upload(ctx->sp_ainc, sp_ainc.data(), sp_ainc.size(), s);
+    rc |= upload(ctx->sp_fix, sp_fix.data(), sp_fix.size(), s);
     rc |= upload<double>(ctx->Hn, nullptr, 4 * static_cast<size_t>(nc), s);
     rc |= upload<double>(ctx->Hu, nullptr, 4 * static_cast<size_t>(nc), s);
     rc |= upload<double>(ctx->Hv, nullptr, 4 * static_cast<size_t>(nc), s);
@@ -366,7 +476,7 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     rc |= upload<double>(ctx->cen[0], nullptr, 2 * static_cast<size_t>(nc), s);
     rc |= upload<double>(ctx->cen[1], nullptr, 2 * static_cast<size_t>(nc), s);
     rc |= upload<double>(ctx->surface, nullptr,
-                         static_cast<size_t>(v->n_contact) + 2 * v->n_inner_line + 2 * v->n_outer_line + 1, s);
+                         4 * (static_cast<size_t>(v->n_contact) + v->n_inner_line + v->n_outer_line) + 1, s);
     if (rc) return GELIOS_E_CUDA;
     GELIOS_CUDA_TRY(cudaStreamSynchronize(s));
     DevMesh& d = ctx->d;
@@ -394,6 +504,11 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     d.ssd = ctx->ssd.as<int32_t>();
     d.ssd2 = ctx->ssd2.as<int32_t>();
     d.sinfo = ctx->sinfo.as<uint32_t>();
+    d.n_slots = ng;
+    d.n_units = static_cast<int>(u_slot.size());
+    d.u_slot = ctx->u_slot.as<int32_t>();
+    d.u_cell = ctx->u_cell.as<int32_t>();
+    d.u_twin = ctx->u_twin.as<int32_t>();
     d.fA = ctx->fA.as<int32_t>();
     d.fB = ctx->fB.as<int32_t>();
     d.ftype = ctx->ftype.as<int32_t>();
@@ -418,6 +533,12 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     d.n_lc = v->n_contact;
     d.n_li = v->n_inner_line;
     d.n_lo = v->n_outer_line;
+    d.n_sp = n_sp;
+    d.sp_point = ctx->sp_point.as<int32_t>();
+    d.sp_line = ctx->sp_line.as<int32_t>();
+    d.sp_inc = ctx->sp_inc.as<int32_t>();
+    d.sp_ainc = ctx->sp_ainc.as<int32_t>();
+    d.sp_fix = ctx->sp_fix.as<int32_t>();
     d.Hn = ctx->Hn.as<double>();
     d.Hu = ctx->Hu.as<double>();
     d.Hv = ctx->Hv.as<double>();
@@ -558,23 +679,36 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             const int nm = launch_motion(d, P, b, ctx->surface.as<double>(), s);
             ctx->phase_end(2, e1, nm);  // Move_surface + rails (surface is 1 of them)
             cudaEvent_t e3 = ctx->phase_begin();
-            launch_mk2_cells(d, P, b, s);
-            ctx->phase_end(3, e3, 1);
+            launch_mk2_units(d, P, b, ctx->flux.as<double>(), s);
+            ctx->phase_end(1, e3, 1);
+            cudaEvent_t e5 = ctx->phase_begin();
+            launch_mk2_update(d, P, b, ctx->flux.as<double>(), s);
+            ctx->phase_end(3, e5, 1);
             cudaEvent_t e4 = ctx->phase_begin();
             launch_commit(d, b, s);
             ctx->phase_end(4, e4, 1);
-            launches += nm + 2;
+            launches += nm + 3;
         } else {
             b.cx = cen0;
             b.cy = cen0 + d.n_cells;
-            cudaEvent_t e3 = ctx->phase_begin();
-            if (form == GELIOS_FORM_STATIONARY) launch_stationary(d, P, b, s);
-            else launch_inner(d, P, b, ctx->inner.as<int32_t>(), ctx->n_inner, s);
-            ctx->phase_end(3, e3, 1);
+            if (form == GELIOS_FORM_STATIONARY) {
+                cudaEvent_t e1 = ctx->phase_begin();
+                launch_stationary_units(d, P, b, ctx->flux.as<double>(), s);
+                ctx->phase_end(1, e1, 1);
+                cudaEvent_t e3 = ctx->phase_begin();
+                launch_stationary_update(d, P, b, ctx->flux.as<double>(), s);
+                ctx->phase_end(3, e3, 1);
+                launches += 2;
+            } else {
+                cudaEvent_t e3 = ctx->phase_begin();
+                launch_inner(d, P, b, ctx->inner.as<int32_t>(), ctx->n_inner, s);
+                ctx->phase_end(3, e3, 1);
+                launches += 1;
+            }
             cudaEvent_t e4 = ctx->phase_begin();
             launch_dt_finalize(b, s);
             ctx->phase_end(4, e4, 1);
-            launches += 2;
+            launches += 1;
         }
     }
     GELIOS_CUDA_TRY(cudaGetLastError());

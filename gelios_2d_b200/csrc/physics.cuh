@@ -89,7 +89,8 @@ __device__ __forceinline__ double pow2g(double a, double g2) { return pow(a, g2)
 // ---------------------------------------------------------------- HLLC / HLL
 // Setka::HLLC_2d_Korolkov_b_s, Setka.cpp:10484-10700.  metod == 0 -> HLL
 // (10604-10618); otherwise HLLC with the optional tangential smoothing
-// `nul_potok` (10644-10653).  Returns kurant*rad/max(|SL|,|SR|).
+// `nul_potok` (10644-10653).  Returns UU = max(|SL|,|SR|); the reference's
+// CFL candidate is kurant*rad/UU (computed by the caller for each side).
 // T is the arithmetic type of the solver (double: drop-in; float: the
 // FP32-flux form, whose inputs/outputs stay double).
 template <typename T>
@@ -130,9 +131,10 @@ __device__ __forceinline__ double hllc_flux(double gamma, double kurant, const S
     const T suR = (SR - u2);
     const T suL = (SL - u1);
     const T SM = (suR * ro_R * u2 - suL * ro_L * u1 - p_R + p_L) / (suR * ro_R - suL * ro_L);
-    // dt candidate in FP64 (the CFL reduction stays FP64)
-    const double UU = dmax_ref(fabs((double)SL), fabs((double)SR));
-    const double time = kurant * rad / UU;
+    // wave-speed bound of the CFL candidate, FP64 (the reduction stays FP64)
+    const double time = dmax_ref(fabs((double)SL), fabs((double)SR));
+    (void)kurant;
+    (void)rad;
     const T e1 = p_L / g1 + ro_L * uu_L;
     const T e2 = p_R / g1 + ro_R * uu_R;
     const T FL0 = ro_L * u1, FL1 = ro_L * u1 * u1 + p_L, FL2 = ro_L * u1 * v1, FL3 = (e1 + p_L) * u1, FL4 = Q_L * u1;
@@ -230,7 +232,9 @@ __device__ __forceinline__ double lev_dev(double ga, double enI, double pI, doub
 }
 
 // Solvers::Godunov_Solver_Alexashov with newton/devtwo, Solvers.cpp:693-1305.
-// q = (ro, p, u, v, w); returns time; qqq[5] flux; ds[3] = dsl, dsp, dsc.
+// q = (ro, p, u, v, w); qqq[5] flux; ds[3] = dsl, dsp, dsc.  Returns the
+// wave-speed bound UU of the reference's CFL candidate kurant*DIST/UU (UU is
+// replaced by eps8 when it is not above it, Solvers.cpp:841-848).
 // The Newton and bisection loops are capped at max_iter (the reference
 // exits the program at 1100); hitting the cap raises ST_ITER_CAP.
 static __device__ __noinline__ double godunov_dev(double ga, double kurant, const double* qqq1, const double* qqq2,
@@ -349,7 +353,7 @@ static __device__ __noinline__ double godunov_dev(double ga, double kurant, cons
         const double dII = enII + aII / rII;
         dsl = dI; dsp = dII; dsc = u;
         const double UU = dmax_ref(fabs(dsl), fabs(dsp));
-        time = (UU > eps8) ? kurant * DIST / UU : kurant * DIST / eps8;
+        time = (UU > eps8) ? UU : eps8;
         if (w <= dI) {
             en = enI; p = pI; r = rI; te2 = teI2; te3 = teI3;
         } else if ((w > dI) && (w <= u)) {
@@ -372,7 +376,7 @@ static __device__ __noinline__ double godunov_dev(double ga, double kurant, cons
         dsl = dI; dsp = dII; dsc = u;
         double UU = dmax_ref(fabs(dsl), fabs(dsp));
         UU = dmax_ref(UU, fabs(ddII));
-        time = (UU > eps8) ? kurant * DIST / UU : kurant * DIST / eps8;
+        time = (UU > eps8) ? UU : eps8;
         if (w <= dI) {
             en = enI; p = pI; r = rI; te2 = teI2; te3 = teI3;
         }
@@ -406,7 +410,7 @@ static __device__ __noinline__ double godunov_dev(double ga, double kurant, cons
         double UU = dmax_ref(fabs(dsl), fabs(dsp));
         UU = dmax_ref(UU, fabs(ddII));
         UU = dmax_ref(UU, fabs(ddI));
-        time = (UU > eps8) ? kurant * DIST / UU : kurant * DIST / eps8;
+        time = (UU > eps8) ? UU : eps8;
         if (w <= dI) {
             en = enI; p = pI; r = rI; te2 = teI2; te3 = teI3;
         }
@@ -439,7 +443,7 @@ static __device__ __noinline__ double godunov_dev(double ga, double kurant, cons
         double UU = dmax_ref(fabs(dsl), fabs(dsp));
         UU = dmax_ref(UU, fabs(ddII));
         UU = dmax_ref(UU, fabs(ddI));
-        time = (UU > eps8) ? kurant * DIST / UU : kurant * DIST / eps8;
+        time = (UU > eps8) ? UU : eps8;
         if (w <= dI) {
             en = enI; p = pI; r = rI; te2 = teI2; te3 = teI3;
         }

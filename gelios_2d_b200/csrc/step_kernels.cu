@@ -1,8 +1,9 @@
 // sm_100a kernels of the Gelios_2D plasma time step.
 //
 // One time step of Setka::Go_5_komponent__MK2 (Setka.cpp:10121-10482) is
-//   surface_kernel   Move_surface (Setka.cpp:3378-3844): tracked-face exact
-//                    Godunov speeds, one CTA, reference accumulation order
+//   surface_*_kernel Move_surface (Setka.cpp:3378-3844): tracked-face exact
+//                    Godunov speeds (one thread per face), then node velocities
+//                    replayed per node in the reference's operation order
 //   rail_*_kernel    Move_Setka_Calculate_2 (Setka.cpp:4324-4759): one CTA per
 //                    rail, A+B rails, then C rails, then D rails (the
 //                    reference's sequence; C_Rails[0] shares points with the
@@ -433,75 +434,152 @@ __global__ void centroid_kernel(DevMesh d, const double* __restrict__ X, const d
     cy[c] = y;
 }
 
-// Go_stationary cell update (Setka.cpp:5225-5341).
-__global__ void __launch_bounds__(128) stationary_cell_kernel(DevMesh d, gelios_params P, StepBuffers b) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    double tmin_c = __longlong_as_double(0x7ff0000000000000LL);
-    int nro = 0, npc = 0, status = 0;
-    const double* const* st = b.cur;
-    if (c < d.n_cells && !(d.cflags[c] & CF_CENTR)) {
-        const double dt = *b.dt_cur;
-        const St5 par1 = load_state(st, c);
-        const double x = b.cx[c], y = b.cy[c];
-        const double rad = sqrt(sq(x) + sq(y));
-        const double g2 = 2 * P.gamma;
-        double Pt0 = 0.0, Pt1 = 0.0, Pt2 = 0.0, Pt3 = 0.0, Pt4 = 0.0;
-        double time = 10000000.0;
-        const int g0 = d.gstart[c], g1 = d.gstart[c + 1];
-        for (int g = g0; g < g1; g++) {
+// ------------------------------------------------------------------ face units
+// A face unit is one flux evaluation: an interior face (Usualy main face,
+// evaluated once for both sides: the reference evaluates it from each side
+// and the two results are the negatives of each other up to rounding,
+// Setka.cpp:10195-10380) or a one-sided face (boundary types, evaluated for
+// its owner only).  Each unit writes F*S into the per-slot flux buffer of the
+// owner slot (and -F*S into the twin's slot of the neighbour), and folds the
+// CFL candidates of the sides whose cell is updated this step into the dt
+// word.  The cell kernels then sum their slots in Grans order.
+
+// Go_stationary flux of one side (Setka.cpp:5244-5306): owner state `own`
+// at centre (x, y), radius rad; face end points (xa,ya)->(xb,yb) seen from the
+// owner; neighbour (for Usualy faces) state/centre.
+template <typename TF>
+__device__ __forceinline__ double stationary_side(const gelios_params& P, int ft, const St5& own, double x, double y,
+                                                  double rad, double xa, double ya, double xb, double yb,
+                                                  const St5& nbs, double x3, double y3, FluxOut<double>& F,
+                                                  double& dist) {
+    const double g2 = 2 * P.gamma;
+    const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
+    dist = sqrt(sq(x - x2) + sq(y - y2));
+    St5 par11 = own;
+    St5 par2 = own;
+    if (ft == G_USUALY) par2 = nbs;
+    else if (ft == G_EXTERN) {
+        if (par2.u >= 0.0) par2.u = P.extern_u_par;
+    } else if (ft == G_AXIS) par2.v = -par2.v;
+    else if (ft == G_INNER_SPHERE) par2 = inner_sphere_state(P, x2, y2);
+    else if (ft == G_INPUT) par2 = input_state(P);
+    double t1 = xb - xa, t2 = yb - ya;
+    const double nn = sqrt(sq(t1) + sq(t2));
+    t1 = t1 / nn;
+    t2 = t2 / nn;
+    const double n1 = t2, n2 = -t1;
+    if (rad < P.rad_stat && ft == G_USUALY) {
+        const double dd = sqrt(sq(x3) + sq(y3));
+        const double f2 = sq(x2) + sq(y2);
+        const double fr = sqrt(f2);
+        par11.ro = par11.ro * sq(rad) / f2;
+        par2.ro = par2.ro * sq(dd) / f2;
+        par11.p = par11.p * pow2g(rad / fr, g2);
+        par2.p = par2.p * pow2g(dd / fr, g2);
+        polar_perenos(x, y, x2, y2, par11.u, par11.v);
+        polar_perenos(x3, y3, x2, y2, par2.u, par2.v);
+    } else if (ft == G_INNER_SPHERE) {
+        const double f2 = sq(x2) + sq(y2);
+        par11.ro = par11.ro * sq(rad) / f2;
+        par11.p = par11.p * pow2g(rad / sqrt(f2), g2);
+    } else if (rad < P.rad_stat && ft == G_AXIS) {
+        polar_perenos(x, y, x2, y2, par11.u, par11.v);
+        par11.v = 0.0;
+        par2 = par11;
+    } else if (ft == G_AXIS) {
+        par11.v = 0.0;
+        par2 = par11;
+    }
+    return hllc_flux<TF>(P.gamma, P.kurant, par11, par2, 0.0, n1, n2, 1.0, 1, false, F);  // UU
+}
+
+template <typename TF>
+__global__ void __launch_bounds__(128) stationary_unit_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                              double* __restrict__ fl) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    double tmin_u = __longlong_as_double(0x7ff0000000000000LL);
+    const size_t ng = d.n_slots;
+    if (u < d.n_units) {
+        const int g = d.u_slot[u], K = d.u_cell[u], gt = d.u_twin[u];
+        const bool procK = !(d.cflags[K] & CF_CENTR);
+        const int nb = gt >= 0 ? d.snb[g] : -1;
+        const bool procN = nb >= 0 && !(d.cflags[nb] & CF_CENTR);
+        if (procK || procN) {
+            const int ft = d.sinfo[g] & SI_TYPE_MASK;
             const int A = d.sA[g], B = d.sB[g];
-            const uint32_t info = d.sinfo[g];
-            const int ft = info & SI_TYPE_MASK;
             const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
             const double S = sqrt(sq(xb - xa) + sq(yb - ya));
-            const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
-            const double dist = sqrt(sq(x - x2) + sq(y - y2));
-            const int nb = d.snb[g];
-            St5 par11 = par1;
-            St5 par2 = get_par(P, ft, par1, st, nb, x2, y2);
-            double t1 = xb - xa, t2 = yb - ya;
-            const double nn = sqrt(sq(t1) + sq(t2));
-            t1 = t1 / nn;
-            t2 = t2 / nn;
-            const double n1 = t2, n2 = -t1;
-            if (rad < P.rad_stat && ft == G_USUALY) {
-                const double x3 = b.cx[nb], y3 = b.cy[nb];
-                const double dd = sqrt(sq(x3) + sq(y3));
-                const double f2 = sq(x2) + sq(y2);
-                const double fr = sqrt(f2);
-                par11.ro = par11.ro * sq(rad) / f2;
-                par2.ro = par2.ro * sq(dd) / f2;
-                par11.p = par11.p * pow2g(rad / fr, g2);
-                par2.p = par2.p * pow2g(dd / fr, g2);
-                polar_perenos(x, y, x2, y2, par11.u, par11.v);
-                polar_perenos(x3, y3, x2, y2, par2.u, par2.v);
-            } else if (ft == G_INNER_SPHERE) {
-                const double f2 = sq(x2) + sq(y2);
-                par11.ro = par11.ro * sq(rad) / f2;
-                par11.p = par11.p * pow2g(rad / sqrt(f2), g2);
-            } else if (rad < P.rad_stat && ft == G_AXIS) {
-                polar_perenos(x, y, x2, y2, par11.u, par11.v);
-                par11.v = 0.0;
-                par2 = par11;
-            } else if (ft == G_AXIS) {
-                par11.v = 0.0;
-                par2 = par11;
+            const double x = b.cx[K], y = b.cy[K];
+            const double rad = sqrt(sq(x) + sq(y));
+            const St5 own = load_state(b.cur, K);
+            St5 nbs = own;
+            double x3 = 0.0, y3 = 0.0, radn = 0.0;
+            if (nb >= 0) {
+                nbs = load_state(b.cur, nb);
+                x3 = b.cx[nb];
+                y3 = b.cy[nb];
+                radn = sqrt(sq(x3) + sq(y3));
             }
             FluxOut<double> F;
-            double tf;
-            if (P.precision == GELIOS_PREC_FP32_FLUX) {
-                tf = hllc_flux<float>(P.gamma, P.kurant, par11, par2, 0.0, n1, n2, dist, 1, false, F);
-            } else {
-                tf = hllc_flux<double>(P.gamma, P.kurant, par11, par2, 0.0, n1, n2, dist, 1, false, F);
+            double dist;
+            const double UU = stationary_side<TF>(P, ft, own, x, y, rad, xa, ya, xb, yb, nbs, x3, y3, F, dist);
+            fl[0 * ng + g] = F.P0 * S;
+            fl[1 * ng + g] = F.P1 * S;
+            fl[2 * ng + g] = F.P2 * S;
+            fl[3 * ng + g] = F.P3 * S;
+            fl[4 * ng + g] = F.PQ * S;
+            if (procK) tmin_u = dmin_ref(tmin_u, P.kurant * dist / UU);
+            if (gt >= 0) {
+                // the twin's evaluation mirrors this one unless the radial
+                // scaling switches at rad_stat between the two cells
+                const bool same = (rad < P.rad_stat) == (radn < P.rad_stat);
+                if (same) {
+                    const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
+                    const double distn = sqrt(sq(x3 - x2) + sq(y3 - y2));
+                    fl[0 * ng + gt] = -(F.P0 * S);
+                    fl[1 * ng + gt] = -(F.P1 * S);
+                    fl[2 * ng + gt] = -(F.P2 * S);
+                    fl[3 * ng + gt] = -(F.P3 * S);
+                    fl[4 * ng + gt] = -(F.PQ * S);
+                    if (procN) tmin_u = dmin_ref(tmin_u, P.kurant * distn / UU);
+                } else {
+                    FluxOut<double> G;
+                    double distn;
+                    const double Un = stationary_side<TF>(P, ft, nbs, x3, y3, radn, xb, yb, xa, ya, own, x, y, G, distn);
+                    fl[0 * ng + gt] = G.P0 * S;
+                    fl[1 * ng + gt] = G.P1 * S;
+                    fl[2 * ng + gt] = G.P2 * S;
+                    fl[3 * ng + gt] = G.P3 * S;
+                    fl[4 * ng + gt] = G.PQ * S;
+                    if (procN) tmin_u = dmin_ref(tmin_u, P.kurant * distn / Un);
+                }
             }
-            time = dmin_ref(time, tf);
-            Pt0 = Pt0 + F.P0 * S;
-            Pt1 = Pt1 + F.P1 * S;
-            Pt2 = Pt2 + F.P2 * S;
-            Pt3 = Pt3 + F.P3 * S;
-            Pt4 = Pt4 + F.PQ * S;
         }
-        tmin_c = time;
+    }
+    block_reduce_commit(tmin_u, 0, 0, 0, b.dt_acc, b.counters, b.status);
+}
+
+// Go_stationary cell update (Setka.cpp:5309-5341) from the summed slots.
+__global__ void __launch_bounds__(128) stationary_update_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                                const double* __restrict__ fl) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double tmark = __longlong_as_double(0x7ff0000000000000LL);
+    int nro = 0, npc = 0;
+    const size_t ng = d.n_slots;
+    if (c < d.n_cells && !(d.cflags[c] & CF_CENTR)) {
+        tmark = 10000000.0;  // `time` starts at 1e7 in every step (Setka.cpp:5222)
+        const double dt = *b.dt_cur;
+        const St5 par1 = load_state(b.cur, c);
+        const double y = b.cy[c];
+        const int g0 = d.gstart[c], g1 = d.gstart[c + 1];
+        double Pt0 = 0.0, Pt1 = 0.0, Pt2 = 0.0, Pt3 = 0.0, Pt4 = 0.0;
+        for (int g = g0; g < g1; g++) {
+            Pt0 = Pt0 + fl[0 * ng + g];
+            Pt1 = Pt1 + fl[1 * ng + g];
+            Pt2 = Pt2 + fl[2 * ng + g];
+            Pt3 = Pt3 + fl[3 * ng + g];
+            Pt4 = Pt4 + fl[4 * ng + g];
+        }
         const int s0 = d.cstart[c], n = d.cstart[c + 1] - s0;
         const double Volume = area(d.contour + s0, n, d.sA, d.sB, g0, g1, d.X, d.Y, false);
         const double gm1 = P.gamma - 1;
@@ -528,131 +606,174 @@ __global__ void __launch_bounds__(128) stationary_cell_kernel(DevMesh d, gelios_
         b.nxt[3][c] = v3;
         b.nxt[4][c] = Q33;
     }
-    block_reduce_commit(tmin_c, nro, npc, status, b.dt_acc, b.counters, b.status);
+    block_reduce_commit(tmark, nro, npc, 0, b.dt_acc, b.counters, b.status);
 }
 
-// Go_5_komponent__MK2 cell update (Setka.cpp:10148-10470).
+// Go_5_komponent__MK2 face reconstruction of one side (Setka.cpp:10213-10276)
+// for a Usualy face: owner M (state Ms, centre Mx,My, flags mf), across the
+// face the cell So; Sd = Sosed_down of the face as seen from M.
+__device__ __forceinline__ St5 mk2_usualy_side(const double* const* st, const double* cx, const double* cy,
+                                               double fx, double fy, double dis, const St5& Ms, double Mx,
+                                               double My, uint32_t mf, int So, int Sd, bool tracked, double g2,
+                                               int* status) {
+    if (mf & CF_C1) {
+        const double radius = sqrt(sq(Mx) + sq(My));
+        St5 o = Ms;
+        o.ro = o.ro * sq(radius) / sq(dis);
+        o.Q = o.Q * sq(radius) / sq(dis);
+        o.p = o.p * pow2g(radius / dis, g2);
+        polar_perenos(Mx, My, fx, fy, o.u, o.v);
+        tvd_radial(st, cx, cy, fx, fy, Ms, Mx, My, So, Sd, (mf & CF_AXIS) != 0, g2, o.ro, o.p);
+        return o;
+    }
+    return tvd_usualy(st, cx, cy, fx, fy, Ms, Mx, My, So, Sd, (mf & CF_AXIS) != 0, tracked, status);
+}
+
 template <typename TF>
-__global__ void __launch_bounds__(128) mk2_cell_kernel(DevMesh d, gelios_params P, StepBuffers b) {
+__global__ void __launch_bounds__(128) mk2_unit_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                       double* __restrict__ fl) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    double tmin_u = __longlong_as_double(0x7ff0000000000000LL);
+    int status = 0;
+    const size_t ng = d.n_slots;
+    if (u < d.n_units) {
+        const int g = d.u_slot[u], K = d.u_cell[u], gt = d.u_twin[u];
+        const double x = b.cx[K], y = b.cy[K];
+        const bool procK = !(sqrt(sq(x) + sq(y)) < P.R11);
+        const int nb = gt >= 0 ? d.snb[g] : -1;
+        double x3 = 0.0, y3 = 0.0;
+        bool procN = false;
+        if (nb >= 0) {
+            x3 = b.cx[nb];
+            y3 = b.cy[nb];
+            procN = !(sqrt(sq(x3) + sq(y3)) < P.R11);
+        }
+        if (procK || procN) {
+            const double dt = *b.dt_cur;
+            const uint32_t info = d.sinfo[g];
+            const int ft = info & SI_TYPE_MASK;
+            const uint32_t cf = d.cflags[K];
+            const int A = d.sA[g], B = d.sB[g];
+            const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
+            const double S = sqrt(sq(xb - xa) + sq(yb - ya)) * (ya + yb) * 0.5;
+            const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
+            const double x4 = (d.X2[A] + d.X2[B]) / 2.0, y4 = (d.Y2[A] + d.Y2[B]) / 2.0;
+            const double dist = sqrt(sq(x - x2) + sq(y - y2));
+            const double g2 = 2 * P.gamma;
+            const St5 par1 = load_state(b.cur, K);
+            St5 par11 = par1;
+            St5 par2 = get_par(P, ft, par1, b.cur, nb, x2, y2);
+            double t1 = xb - xa, t2 = yb - ya;
+            const double nn = sqrt(sq(t1) + sq(t2));
+            t1 = t1 / nn;
+            t2 = t2 / nn;
+            const double n1 = t2, n2 = -t1;
+            const double W = ((x4 - x2) * n1 + (y4 - y2) * n2) / dt;
+            const double dis = sqrt(sq(x2) + sq(y2));
+            const bool tracked = (info & SI_GOD) != 0;
+            if (ft == G_USUALY) {
+                par11 = mk2_usualy_side(b.cur, b.cx, b.cy, x2, y2, dis, par1, x, y, cf, nb, d.ssd[g], tracked, g2,
+                                        &status);
+                par2 = mk2_usualy_side(b.cur, b.cx, b.cy, x2, y2, dis, par2, x3, y3, d.cflags[nb], K, d.ssd2[g],
+                                       tracked, g2, &status);
+            } else if (ft == G_INNER_SPHERE) {
+                const double radius = sqrt(sq(x) + sq(y));
+                par11.ro = par11.ro * sq(radius) / sq(dis);
+                par11.Q = par11.Q * sq(radius) / sq(dis);
+                par11.p = par11.p * pow2g(radius / dis, g2);
+            } else if (ft == G_AXIS) {
+                if (cf & CF_C1) {
+                    const double radius = sqrt(sq(x) + sq(y));
+                    par11.ro = par11.ro * sq(radius) / sq(dis);
+                    par11.Q = par11.Q * sq(radius) / sq(dis);
+                    par11.p = par11.p * pow2g(radius / dis, g2);
+                    polar_perenos(x, y, x2, y2, par11.u, par11.v);
+                } else {
+                    par11 = tvd_axis(b.cur, b.cx, b.cy, x2, y2, par1, x, y, d.ssd[g]);
+                }
+                par2 = par11;
+                par2.v = -par2.v;
+            }
+            const bool np = (info & SI_NP) != 0;
+            FluxOut<double> F;
+            const double UU = hllc_flux<TF>(P.gamma, P.kurant, par11, par2, W, n1, n2, 1.0, 0, np, F);
+            double fm0 = F.P0 * S, fm1 = F.P1 * S, fm2 = F.P2 * S, fm3 = F.P3 * S;
+            double UG = 1.0;
+            if (tracked) {
+                double q1[5] = {par11.ro, par11.p, par11.u, par11.v, 0.0};
+                double q2[5] = {par2.ro, par2.p, par2.u, par2.v, 0.0};
+                double nv[3] = {n1, n2, 0.0};
+                double qq[5], ds[3];
+                UG = godunov_dev(P.gamma, P.kurant, q1, q2, nv, qq, ds, W, 1.0, P.godunov_max_iter, &status);
+                fm0 = qq[0] * S;
+                fm1 = qq[1] * S;
+                fm2 = qq[2] * S;
+                fm3 = qq[4] * S;
+            }
+            const double fq = F.PQ * S;
+            fl[0 * ng + g] = fm0;
+            fl[1 * ng + g] = fm1;
+            fl[2 * ng + g] = fm2;
+            fl[3 * ng + g] = fm3;
+            fl[4 * ng + g] = fq;
+            if (procK) {
+                // reference order: Godunov candidate first, then HLL (Setka.cpp:10359, 10366)
+                if (tracked) tmin_u = dmin_ref(tmin_u, P.kurant * dist / UG);
+                tmin_u = dmin_ref(tmin_u, P.kurant * dist / UU);
+            }
+            if (gt >= 0) {
+                fl[0 * ng + gt] = -fm0;
+                fl[1 * ng + gt] = -fm1;
+                fl[2 * ng + gt] = -fm2;
+                fl[3 * ng + gt] = -fm3;
+                fl[4 * ng + gt] = -fq;
+                if (procN) {
+                    const double distn = sqrt(sq(x3 - x2) + sq(y3 - y2));
+                    if (tracked) tmin_u = dmin_ref(tmin_u, P.kurant * distn / UG);
+                    tmin_u = dmin_ref(tmin_u, P.kurant * distn / UU);
+                }
+            }
+        }
+    }
+    block_reduce_commit(tmin_u, 0, 0, status, b.dt_acc, b.counters, b.status);
+}
+
+// Go_5_komponent__MK2 cell update (Setka.cpp:10386-10468) from the summed
+// slots; also the centroid of the moved cell (the next step's centroid).
+__global__ void __launch_bounds__(128) mk2_update_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                         const double* __restrict__ fl) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    double tmin_c = __longlong_as_double(0x7ff0000000000000LL);
+    double tmark = __longlong_as_double(0x7ff0000000000000LL);
     int nro = 0, npc = 0, status = 0;
-    const double* const* st = b.cur;
+    const size_t ng = d.n_slots;
     if (c < d.n_cells) {
         const int s0 = d.cstart[c], n = d.cstart[c + 1] - s0;
         const int32_t* con = d.contour + s0;
-        // centroid after the motion = centroid of the next step
         double xn, yn;
         centroid(con, n, d.X2, d.Y2, xn, yn);
         b.cx_next[c] = xn;
         b.cy_next[c] = yn;
         const double x = b.cx[c], y = b.cy[c];
-        const double radius = sqrt(sq(x) + sq(y));
-        if (!(radius < P.R11)) {
+        if (!(sqrt(sq(x) + sq(y)) < P.R11)) {
+            tmark = 10000000.0;  // `time` starts at 1e7 in every step (Setka.cpp:10141)
             const double dt = *b.dt_cur;
-            const uint32_t cf = d.cflags[c];
-            const bool own_c1 = (cf & CF_C1) != 0;
             const int g0 = d.gstart[c], g1 = d.gstart[c + 1];
-            const double vs1 = area(con, n, d.sA, d.sB, g0, g1, d.X, d.Y, false);
-            const double vs2 = area(con, n, d.sA, d.sB, g0, g1, d.X2, d.Y2, true);
-            const double Volume = volume_rotate(con, n, d.X, d.Y);
-            const double Volume2 = volume_rotate(con, n, d.X2, d.Y2);
-            const St5 par1 = load_state(st, c);
-            const double g2 = 2 * P.gamma;
             double Pt0 = 0.0, Pt1 = 0.0, Pt2 = 0.0, Pt3 = 0.0, Pt4 = 0.0;
-            double time = 10000000.0;
             for (int g = g0; g < g1; g++) {
-                const int A = d.sA[g], B = d.sB[g];
-                const uint32_t info = d.sinfo[g];
-                const int ft = info & SI_TYPE_MASK;
-                const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
-                const double S = sqrt(sq(xb - xa) + sq(yb - ya)) * (ya + yb) * 0.5;
-                const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
-                const double x4 = (d.X2[A] + d.X2[B]) / 2.0, y4 = (d.Y2[A] + d.Y2[B]) / 2.0;
-                const double dist = sqrt(sq(x - x2) + sq(y - y2));
-                const int nb = d.snb[g];
-                St5 par11 = par1;
-                St5 par2 = get_par(P, ft, par1, st, nb, x2, y2);
-                double t1 = xb - xa, t2 = yb - ya;
-                const double nn = sqrt(sq(t1) + sq(t2));
-                t1 = t1 / nn;
-                t2 = t2 / nn;
-                const double n1 = t2, n2 = -t1;
-                const double W = ((x4 - x2) * n1 + (y4 - y2) * n2) / dt;
-                const double dis = sqrt(sq(x2) + sq(y2));
-                const bool tracked = (info & SI_GOD) != 0;
-                if (ft == G_USUALY) {
-                    const double x3 = b.cx[nb], y3 = b.cy[nb];
-                    const double dd = sqrt(sq(x3) + sq(y3));
-                    if (own_c1) {
-                        par11.ro = par11.ro * sq(radius) / sq(dis);
-                        par11.Q = par11.Q * sq(radius) / sq(dis);
-                        par11.p = par11.p * pow2g(radius / dis, g2);
-                        polar_perenos(x, y, x2, y2, par11.u, par11.v);
-                        tvd_radial(st, b.cx, b.cy, x2, y2, par1, x, y, nb, d.ssd[g], (cf & CF_AXIS) != 0, g2,
-                                   par11.ro, par11.p);
-                    } else {
-                        par11 = tvd_usualy(st, b.cx, b.cy, x2, y2, par1, x, y, nb, d.ssd[g], (cf & CF_AXIS) != 0,
-                                           tracked, &status);
-                    }
-                    const uint32_t nbf = d.cflags[nb];
-                    if (nbf & CF_C1) {
-                        par2.ro = par2.ro * sq(dd) / sq(dis);
-                        par2.Q = par2.Q * sq(dd) / sq(dis);
-                        par2.p = par2.p * pow2g(dd / dis, g2);
-                        polar_perenos(x3, y3, x2, y2, par2.u, par2.v);
-                        const St5 nbs = load_state(st, nb);
-                        tvd_radial(st, b.cx, b.cy, x2, y2, nbs, x3, y3, c, d.ssd2[g], (nbf & CF_AXIS) != 0, g2,
-                                   par2.ro, par2.p);
-                    } else {
-                        const St5 nbs = load_state(st, nb);
-                        par2 = tvd_usualy(st, b.cx, b.cy, x2, y2, nbs, x3, y3, c, d.ssd2[g], (nbf & CF_AXIS) != 0,
-                                          tracked, &status);
-                    }
-                } else if (ft == G_INNER_SPHERE) {
-                    par11.ro = par11.ro * sq(radius) / sq(dis);
-                    par11.Q = par11.Q * sq(radius) / sq(dis);
-                    par11.p = par11.p * pow2g(radius / dis, g2);
-                } else if (ft == G_AXIS) {
-                    if (own_c1) {
-                        par11.ro = par11.ro * sq(radius) / sq(dis);
-                        par11.Q = par11.Q * sq(radius) / sq(dis);
-                        par11.p = par11.p * pow2g(radius / dis, g2);
-                        polar_perenos(x, y, x2, y2, par11.u, par11.v);
-                    } else {
-                        par11 = tvd_axis(st, b.cx, b.cy, x2, y2, par1, x, y, d.ssd[g]);
-                    }
-                    par2 = par11;
-                    par2.v = -par2.v;
-                }
-                const bool np = (info & SI_NP) != 0;
-                FluxOut<double> F;
-                if (tracked) {
-                    double q1[5] = {par11.ro, par11.p, par11.u, par11.v, 0.0};
-                    double q2[5] = {par2.ro, par2.p, par2.u, par2.v, 0.0};
-                    double nv[3] = {n1, n2, 0.0};
-                    double qq[5], ds[3];
-                    time = dmin_ref(time, godunov_dev(P.gamma, P.kurant, q1, q2, nv, qq, ds, W, dist,
-                                                      P.godunov_max_iter, &status));
-                    Pt0 = Pt0 + qq[0] * S;
-                    Pt1 = Pt1 + qq[1] * S;
-                    Pt2 = Pt2 + qq[2] * S;
-                    Pt3 = Pt3 + qq[4] * S;
-                    time = dmin_ref(time, hllc_flux<TF>(P.gamma, P.kurant, par11, par2, W, n1, n2, dist, 0, np, F));
-                    Pt4 = Pt4 + F.PQ * S;
-                } else {
-                    time = dmin_ref(time, hllc_flux<TF>(P.gamma, P.kurant, par11, par2, W, n1, n2, dist, 0, np, F));
-                    Pt0 = Pt0 + F.P0 * S;
-                    Pt1 = Pt1 + F.P1 * S;
-                    Pt2 = Pt2 + F.P2 * S;
-                    Pt3 = Pt3 + F.P3 * S;
-                    Pt4 = Pt4 + F.PQ * S;
-                }
+                Pt0 = Pt0 + fl[0 * ng + g];
+                Pt1 = Pt1 + fl[1 * ng + g];
+                Pt2 = Pt2 + fl[2 * ng + g];
+                Pt3 = Pt3 + fl[3 * ng + g];
+                Pt4 = Pt4 + fl[4 * ng + g];
             }
-            tmin_c = time;
+            const St5 par1 = load_state(b.cur, c);
             double q2_1, q2_2, q3;
             source_mk1(d, P, c, x, y, par1.u, par1.v, par1.ro, par1.p, q2_1, q2_2, q3, &status);
-            if (!(cf & CF_CENTR)) {
+            if (!(d.cflags[c] & CF_CENTR)) {
+                const double vs1 = area(con, n, d.sA, d.sB, g0, g1, d.X, d.Y, false);
+                const double vs2 = area(con, n, d.sA, d.sB, g0, g1, d.X2, d.Y2, true);
+                const double Volume = volume_rotate(con, n, d.X, d.Y);
+                const double Volume2 = volume_rotate(con, n, d.X2, d.Y2);
                 const double ro = par1.ro, u = par1.u, v = par1.v, p = par1.p, Q = par1.Q;
                 const double gm1 = P.gamma - 1;
                 double ro3 = ro * Volume / Volume2 - dt * (Pt0 / Volume2);
@@ -662,7 +783,8 @@ __global__ void __launch_bounds__(128) mk2_cell_kernel(DevMesh d, gelios_params 
                     nro = 1;
                 }
                 const double u3 = (ro * u * Volume / Volume2 - dt * (Pt1 / Volume2 - q2_1)) / ro3;
-                const double v3 = (ro * v * Volume / Volume2 - dt * ((Pt2 - p * 0.5 * (vs1 + vs2)) / Volume2 - q2_2)) / ro3;
+                const double v3 =
+                    (ro * v * Volume / Volume2 - dt * ((Pt2 - p * 0.5 * (vs1 + vs2)) / Volume2 - q2_2)) / ro3;
                 double p3 = (((p / gm1 + ro * (u * u + v * v) * 0.5) * Volume / Volume2 - dt * (Pt3 / Volume2 - q3)) -
                              0.5 * ro3 * (u3 * u3 + v3 * v3)) *
                             gm1;
@@ -684,7 +806,7 @@ __global__ void __launch_bounds__(128) mk2_cell_kernel(DevMesh d, gelios_params 
             }
         }
     }
-    block_reduce_commit(tmin_c, nro, npc, status, b.dt_acc, b.counters, b.status);
+    block_reduce_commit(tmark, nro, npc, status, b.dt_acc, b.counters, b.status);
 }
 
 // Go_stationary_5_komponent_inner_MK2 cell update (Setka.cpp:7021-7210).
@@ -760,7 +882,8 @@ __global__ void __launch_bounds__(128) inner_cell_kernel(DevMesh d, gelios_param
                 met = 0;
             }
             FluxOut<double> F;
-            time = dmin_ref(time, hllc_flux<TF>(P.gamma, P.kurant, par11, par2, 0.0, n1, n2, dist, met, false, F));
+            time = dmin_ref(time, P.kurant * dist / hllc_flux<TF>(P.gamma, P.kurant, par11, par2, 0.0, n1, n2, dist,
+                                                                  met, false, F));
             Pt0 = Pt0 + F.P0 * S;
             Pt1 = Pt1 + F.P1 * S;
             Pt2 = Pt2 + F.P2 * S;
@@ -1043,200 +1166,187 @@ __device__ St5 face_tvd(const DevMesh& d, const double* const* st, const double*
     return o;  // Extern/Upper_wall/Input/Inner faces do not occur on tracked lines
 }
 
-// Move_surface (Setka.cpp:3378-3844).  Phase 1: one thread per tracked face
-// computes its exact-Godunov wave speed (and the branch the reference takes);
-// phase 2: thread 0 replays the reference's sequential accumulation,
-// averaging loops (which walk Line_Contact in all three blocks) and end-node
-// fix-ups, so every node velocity is bit-identical to the serial code.
-__global__ void __launch_bounds__(256) surface_kernel(DevMesh d, gelios_params P, StepBuffers b,
-                                                      double* __restrict__ scratch) {
-    const double dt = *b.dt_cur;
-    const double* const* st = b.cur;
+// Move_surface (Setka.cpp:3378-3844), part 1: one thread per tracked face
+// (contact, inner shock, outer shock) computes its exact-Godunov wave speed,
+// the face normal and the branch the reference takes.
+// scratch layout per face j of the concatenated lines (contact, inner, outer):
+//   [0] speed  [1] n1  [2] n2  [3] branch
+//   branch: contact 0 (B only); inner 0 (B only) / 1 (A and B);
+//           outer -1 (skipped) / 0 B / 1 A and B / 2 B / 3 A
+__global__ void __launch_bounds__(64) surface_faces_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                           double* __restrict__ scratch) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int nC = d.n_lc, nI = d.n_li, nO = d.n_lo;
-    double* vc = scratch;              // [nC]  contact speed VV
-    double* vi = scratch + nC;         // [nI]  inner-shock speed Vl, sign of branch
-    double* bi = vi + nI;              // [nI]  1.0 -> both nodes, 0.0 -> B only
-    double* vo = bi + nI;              // [nO]  outer-shock speed Vp
-    double* bo = vo + nO;              // [nO]  branch: 0 B only, 1 both, 2 B, 3 A
+    if (j >= nC + nI + nO) return;
+    const double* const* st = b.cur;
     int status = 0;
     const double ga = P.gamma, g2 = 2.0 * P.gamma;
-    for (int j = threadIdx.x; j < nC + nI + nO; j += blockDim.x) {
-        double nv[3], q1[5], q2[5], qq[5], ds[3];
-        if (j < nC) {
-            const int f = d.lc[j];
-            const St5 p1 = face_tvd(d, st, b.cx, b.cy, f, &status);
-            const St5 p2 = face_tvd(d, st, b.cx, b.cy, d.fcopy[f], &status);
-            const int a = d.fA[f], bb = d.fB[f];
-            double t1 = d.X[bb] - d.X[a], t2 = d.Y[bb] - d.Y[a];
-            const double n = sqrt(sq(t1) + sq(t2));
-            t1 /= n;
-            t2 /= n;
-            nv[0] = t2; nv[1] = -t1; nv[2] = 0.0;
-            q1[0] = p1.ro; q1[1] = p1.p; q1[2] = p1.u; q1[3] = p1.v; q1[4] = 0.0;
-            q2[0] = p2.ro; q2[1] = p2.p; q2[2] = p2.u; q2[3] = p2.v; q2[4] = 0.0;
-            godunov_dev(ga, P.kurant, q1, q2, nv, qq, ds, 0.0, 0.0, P.godunov_max_iter, &status);
-            vc[j] = ds[2] * P.koef * 0.3;
-        } else if (j < nC + nI) {
-            const int jj = j - nC;
-            const int f = d.li[jj];
-            const int M = d.fmaster[f];
-            St5 p1 = load_state(st, M);
-            const double x = b.cx[M], y = b.cy[M];
-            const double radius = sqrt(sq(x) + sq(y));
-            const int a = d.fA[f], bb = d.fB[f];
-            const double x2 = (d.X[a] + d.X[bb]) / 2.0, y2 = (d.Y[a] + d.Y[bb]) / 2.0;
-            const double dis = sqrt(sq(x2) + sq(y2));
-            const St5 p2 = face_tvd(d, st, b.cx, b.cy, d.fcopy[f], &status);
-            double t1 = d.X[bb] - d.X[a], t2 = d.Y[bb] - d.Y[a];
-            const double n = sqrt(sq(t1) + sq(t2));
-            t1 /= n;
-            t2 /= n;
-            const double n1 = t2, n2 = -t1;
-            p1.ro = p1.ro * sq(radius) / sq(dis);
-            p1.p = p1.p * pow2g(radius / dis, g2);
-            polar_perenos(x, y, x2, y2, p1.u, p1.v);
-            nv[0] = n1; nv[1] = n2; nv[2] = 0.0;
-            q1[0] = p1.ro; q1[1] = p1.p; q1[2] = p1.u; q1[3] = p1.v; q1[4] = 0.0;
-            q2[0] = p2.ro; q2[1] = p2.p; q2[2] = p2.u; q2[3] = p2.v; q2[4] = 0.0;
-            godunov_dev(ga, P.kurant, q1, q2, nv, qq, ds, 0.0, 0.0, P.godunov_max_iter, &status);
-            vi[jj] = ds[0] * P.koef * 0.1;
-            const double tt1 = -n2, tt2 = n1;
-            bi[jj] = (fabs(p2.u * tt1 + p2.v * tt2) < 0.1) ? 1.0 : 0.0;
+    double nv[3], q1[5], q2[5], qq[5], ds[3];
+    double* out = scratch + 4 * j;
+    int f;
+    if (j < nC) f = d.lc[j];
+    else if (j < nC + nI) f = d.li[j - nC];
+    else f = d.lo[j - nC - nI];
+    const int a = d.fA[f], bb = d.fB[f];
+    double t1 = d.X[bb] - d.X[a], t2 = d.Y[bb] - d.Y[a];
+    const double nn = sqrt(sq(t1) + sq(t2));
+    t1 /= nn;
+    t2 /= nn;
+    const double n1 = t2, n2 = -t1;
+    out[1] = n1;
+    out[2] = n2;
+    nv[0] = n1; nv[1] = n2; nv[2] = 0.0;
+    if (j < nC) {
+        const St5 p1 = face_tvd(d, st, b.cx, b.cy, f, &status);
+        const St5 p2 = face_tvd(d, st, b.cx, b.cy, d.fcopy[f], &status);
+        q1[0] = p1.ro; q1[1] = p1.p; q1[2] = p1.u; q1[3] = p1.v; q1[4] = 0.0;
+        q2[0] = p2.ro; q2[1] = p2.p; q2[2] = p2.u; q2[3] = p2.v; q2[4] = 0.0;
+        godunov_dev(ga, P.kurant, q1, q2, nv, qq, ds, 0.0, 0.0, P.godunov_max_iter, &status);
+        out[0] = ds[2] * P.koef * 0.3;
+        out[3] = 0.0;
+    } else if (j < nC + nI) {
+        const int M = d.fmaster[f];
+        St5 p1 = load_state(st, M);
+        const double x = b.cx[M], y = b.cy[M];
+        const double radius = sqrt(sq(x) + sq(y));
+        const double x2 = (d.X[a] + d.X[bb]) / 2.0, y2 = (d.Y[a] + d.Y[bb]) / 2.0;
+        const double dis = sqrt(sq(x2) + sq(y2));
+        const St5 p2 = face_tvd(d, st, b.cx, b.cy, d.fcopy[f], &status);
+        p1.ro = p1.ro * sq(radius) / sq(dis);
+        p1.p = p1.p * pow2g(radius / dis, g2);
+        polar_perenos(x, y, x2, y2, p1.u, p1.v);
+        q1[0] = p1.ro; q1[1] = p1.p; q1[2] = p1.u; q1[3] = p1.v; q1[4] = 0.0;
+        q2[0] = p2.ro; q2[1] = p2.p; q2[2] = p2.u; q2[3] = p2.v; q2[4] = 0.0;
+        godunov_dev(ga, P.kurant, q1, q2, nv, qq, ds, 0.0, 0.0, P.godunov_max_iter, &status);
+        out[0] = ds[0] * P.koef * 0.1;
+        const double tt1 = -n2, tt2 = n1;
+        out[3] = (fabs(p2.u * tt1 + p2.v * tt2) < 0.1) ? 1.0 : 0.0;
+    } else {
+        const int jj = j - nC - nI;
+        const int lim = P.n_outer_shock + d.dims[0] + d.dims[1] + 1;
+        if (jj >= lim) {
+            out[0] = 0.0;
+            out[3] = -1.0;
         } else {
-            const int jj = j - nC - nI;
-            const int lim = P.n_outer_shock + d.dims[0] + d.dims[1] + 1;
-            if (jj >= lim) {
-                vo[jj] = 0.0;
-                bo[jj] = -1.0;
-                continue;
-            }
-            const int f = d.lo[jj];
             const St5 p1 = face_tvd(d, st, b.cx, b.cy, f, &status);
             const St5 p2 = face_tvd(d, st, b.cx, b.cy, d.fcopy[f], &status);
-            const int a = d.fA[f], bb = d.fB[f];
-            double t1 = d.X[bb] - d.X[a], t2 = d.Y[bb] - d.Y[a];
-            const double n = sqrt(sq(t1) + sq(t2));
-            t1 /= n;
-            t2 /= n;
-            const double n1 = t2, n2 = -t1;
-            nv[0] = n1; nv[1] = n2; nv[2] = 0.0;
             q1[0] = p1.ro; q1[1] = p1.p; q1[2] = p1.u; q1[3] = p1.v; q1[4] = 0.0;
             q2[0] = p2.ro; q2[1] = p2.p; q2[2] = p2.u; q2[3] = p2.v; q2[4] = 0.0;
             godunov_dev(ga, P.kurant, q1, q2, nv, qq, ds, 0.0, 0.0, P.godunov_max_iter, &status);
-            vo[jj] = ds[1] * P.koef;
+            out[0] = ds[1] * P.koef;
             const double tt1 = -n2, tt2 = n1;
             double br;
             if ((sq(p1.u) + sq(p1.v) + sq(0.0)) / (ga * p1.p / p1.ro) > 1.0) br = 0.0;
             else if (fabs(p1.u * tt1 + p1.v * tt2) < 0.01) br = 1.0;
             else if (p1.u * tt1 + p1.v * tt2 > 0) br = 2.0;
             else br = 3.0;
-            bo[jj] = br;
+            out[3] = br;
         }
     }
     if (status) atomicOr(b.status, status);
+}
+
+// Move_surface, part 2: node velocities.  The reference accumulates the face
+// speeds into Point::Vx/Vy/count in one serial pass per line, then runs three
+// averaging loops that all walk Line_Contact (Setka.cpp:3522-3530, 3718-3731,
+// 3829-3837) with end-node fix-ups between them.  The three lines touch
+// disjoint point sets (P_Contact, P_Inner_shock, P_Outer_shock), so each node
+// replays, on its own, exactly the ordered operations the serial code applies
+// to it: its face incidences in line order (sp_inc), then, for contact nodes,
+// one division per averaging pass in which it is the A end of a contact face
+// (sp_ainc).  Fix-ups run on one thread between the first and the later
+// passes, as in the reference.  Every node's result is bit-identical to the
+// serial code.
+__global__ void __launch_bounds__(512) surface_nodes_kernel(DevMesh d, StepBuffers b,
+                                                            const double* __restrict__ scratch) {
+    extern __shared__ double sm[];
+    const int n = d.n_sp;
+    double* vx = sm;
+    double* vy = sm + n;
+    int* cn = reinterpret_cast<int*>(sm + 2 * n);
+    const int nC = d.n_lc, nI = d.n_li, nO = d.n_lo;
+    const double dt = *b.dt_cur;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int line = d.sp_line[i];
+        double v = 0.0, w = 0.0;
+        int c = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int e = d.sp_inc[4 * i + k];
+            if (e < 0) break;
+            const int j = e >> 1, role = e & 1;  // role 0: A end, 1: B end
+            const double* f = scratch + 4 * j;
+            const double br = f[3];
+            bool add;
+            if (line == 0) add = role == 1;
+            else if (line == 1) add = role == 1 || br != 0.0;
+            else add = (br == 1.0) || (role == 1 && (br == 0.0 || br == 2.0)) || (role == 0 && br == 3.0);
+            if (add) {
+                v += f[0] * f[1];
+                w += f[0] * f[2];
+                c++;
+            }
+        }
+        if (line == 0) {  // first averaging pass: every contact face (Setka.cpp:3522-3530)
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int j = d.sp_ainc[4 * i + k];
+                if (j < 0) break;
+                if (c > 0) {
+                    v /= (1.0 * c);
+                    w /= (1.0 * c);
+                }
+            }
+        }
+        vx[i] = v;
+        vy[i] = w;
+        cn[i] = c;
+    }
     __syncthreads();
-    if (threadIdx.x != 0) return;
-    double* Vx = d.Vx;
-    double* Vy = d.Vy;
-    int* cnt = d.cnt;
-    auto nrm = [&](int f, double& n1, double& n2) {
-        const int a = d.fA[f], bb = d.fB[f];
-        double t1 = d.X[bb] - d.X[a], t2 = d.Y[bb] - d.Y[a];
-        const double n = sqrt(sq(t1) + sq(t2));
-        t1 /= n;
-        t2 /= n;
-        n1 = t2;
-        n2 = -t1;
-    };
-    if (nC > 0) {
-        for (int j = 0; j < nC; j++) {
-            const int f = d.lc[j];
-            double n1, n2;
-            nrm(f, n1, n2);
-            const int B = d.fB[f];
-            Vx[B] += vc[j] * n1;
-            Vy[B] += vc[j] * n2;
-            cnt[B]++;
+    if (threadIdx.x == 0) {
+        const int32_t* fx = d.sp_fix;  // local ids of a0, b0, a_last, b_last per line
+        if (nC > 0) {
+            const int a0 = fx[0], b0 = fx[1], a1 = fx[2], b1 = fx[3];
+            vx[a0] = vx[b0] + (d.X[d.sp_point[b0]] - d.X[d.sp_point[a0]]) / dt;
+            vy[b1] = vy[a1] + (d.Y[d.sp_point[a1]] - d.Y[d.sp_point[b1]]) / dt;
         }
-        for (int j = 0; j < nC; j++) {
-            const int A = d.fA[d.lc[j]];
-            if (cnt[A] > 0) {
-                Vx[A] /= (1.0 * cnt[A]);
-                Vy[A] /= (1.0 * cnt[A]);
-            }
+        if (nI > 0) {
+            const int a0 = fx[4], b0 = fx[5], a1 = fx[6], b1 = fx[7];
+            vx[a0] = vx[b0] + (d.X[d.sp_point[b0]] - d.X[d.sp_point[a0]]) / dt;
+            vx[b1] = vx[a1] + (d.X[d.sp_point[a1]] - d.X[d.sp_point[b1]]) / dt;
         }
-        const int a0 = d.fA[d.lc[0]], b0 = d.fB[d.lc[0]];
-        Vx[a0] = Vx[b0] + (d.X[b0] - d.X[a0]) / dt;
-        const int a1 = d.fA[d.lc[nC - 1]], b1 = d.fB[d.lc[nC - 1]];
-        Vy[b1] = Vy[a1] + (d.Y[a1] - d.Y[b1]) / dt;
+        if (nO > 0) {
+            const int a0 = fx[8], b0 = fx[9], a1 = fx[10], b1 = fx[11];
+            vx[a0] = vx[b0] + (d.X[d.sp_point[b0]] - d.X[d.sp_point[a0]]) / dt;
+            vy[b1] = vy[a1] + (d.Y[d.sp_point[a1]] - d.Y[d.sp_point[b1]]) / dt;
+        }
     }
-    if (nI > 0) {
-        for (int j = 0; j < nI; j++) {
-            const int f = d.li[j];
-            double n1, n2;
-            nrm(f, n1, n2);
-            const int A = d.fA[f], B = d.fB[f];
-            const double Vl = vi[j];
-            if (bi[j] != 0.0) {
-                Vx[A] += Vl * n1;
-                Vy[A] += Vl * n2;
-                cnt[A]++;
-            }
-            Vx[B] += Vl * n1;
-            Vy[B] += Vl * n2;
-            cnt[B]++;
-        }
-        // walks Line_Contact (Setka.cpp:3718-3731); past its end the reference
-        // reads out of bounds, here the walk stops at the end of the list
-        for (int j = 0; j < nI && j < nC; j++) {
-            const int A = d.fA[d.lc[j]];
-            if (cnt[A] > 0) {
-                Vx[A] /= (1.0 * cnt[A]);
-                Vy[A] /= (1.0 * cnt[A]);
+    __syncthreads();
+    const int lim2 = nI > 0 ? (nI < nC ? nI : nC) : 0;
+    const int lim3 = nO > 0 ? (nO < nC ? nO : nC) : 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double v = vx[i], w = vy[i];
+        const int c = cn[i];
+        if (d.sp_line[i] == 0) {
+            // second and third passes walk Line_Contact up to the inner/outer
+            // line lengths (Setka.cpp:3718-3731, 3829-3837)
+            for (int pass = 0; pass < 2; pass++) {
+                const int lim = pass == 0 ? lim2 : lim3;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const int j = d.sp_ainc[4 * i + k];
+                    if (j < 0) break;
+                    if (j < lim && c > 0) {
+                        v /= (1.0 * c);
+                        w /= (1.0 * c);
+                    }
+                }
             }
         }
-        const int a0 = d.fA[d.li[0]], b0 = d.fB[d.li[0]];
-        Vx[a0] = Vx[b0] + (d.X[b0] - d.X[a0]) / dt;
-        const int a1 = d.fA[d.li[nI - 1]], b1 = d.fB[d.li[nI - 1]];
-        Vx[b1] = Vx[a1] + (d.X[a1] - d.X[b1]) / dt;
-    }
-    if (nO > 0) {
-        for (int j = 0; j < nO; j++) {
-            const double br = bo[j];
-            if (br < 0.0) continue;
-            const int f = d.lo[j];
-            double n1, n2;
-            nrm(f, n1, n2);
-            const int A = d.fA[f], B = d.fB[f];
-            const double Vp = vo[j];
-            if (br == 0.0 || br == 2.0) {
-                Vx[B] += Vp * n1;
-                Vy[B] += Vp * n2;
-                cnt[B]++;
-            } else if (br == 1.0) {
-                Vx[A] += Vp * n1;
-                Vy[A] += Vp * n2;
-                cnt[A]++;
-                Vx[B] += Vp * n1;
-                Vy[B] += Vp * n2;
-                cnt[B]++;
-            } else {
-                Vx[A] += Vp * n1;
-                Vy[A] += Vp * n2;
-                cnt[A]++;
-            }
-        }
-        for (int j = 0; j < nO && j < nC; j++) {  // walks Line_Contact (Setka.cpp:3829-3837)
-            const int A = d.fA[d.lc[j]];
-            if (cnt[A] > 0) {
-                Vx[A] /= (1.0 * cnt[A]);
-                Vy[A] /= (1.0 * cnt[A]);
-            }
-        }
-        const int a0 = d.fA[d.lo[0]], b0 = d.fB[d.lo[0]];
-        Vx[a0] = Vx[b0] + (d.X[b0] - d.X[a0]) / dt;
-        const int a1 = d.fA[d.lo[nO - 1]], b1 = d.fB[d.lo[nO - 1]];
-        Vy[b1] = Vy[a1] + (d.Y[a1] - d.Y[b1]) / dt;
+        const int p = d.sp_point[i];
+        d.Vx[p] = v;
+        d.Vy[p] = w;
+        d.cnt[p] = c;
     }
 }
 
@@ -1254,6 +1364,7 @@ __global__ void hllc_batch_kernel(gelios_params P, int n, const double* __restri
         t = hllc_flux<float>(P.gamma, P.kurant, L, R, a[10], a[11], a[12], a[13], (int)a[14], a[15] != 0.0, F);
     else
         t = hllc_flux<double>(P.gamma, P.kurant, L, R, a[10], a[11], a[12], a[13], (int)a[14], a[15] != 0.0, F);
+    t = P.kurant * a[13] / t;
     double* o = out + 9 * i;
     o[0] = t;
     o[1] = F.P0;
@@ -1284,7 +1395,8 @@ __global__ void godunov_batch_kernel(gelios_params P, int n, const double* __res
     }
     nv[0] = a[10]; nv[1] = a[11]; nv[2] = a[12];
     int status = 0;
-    const double t = godunov_dev(P.gamma, P.kurant, q1, q2, nv, qq, ds, a[13], a[14], P.godunov_max_iter, &status);
+    const double t = P.kurant * a[14] / godunov_dev(P.gamma, P.kurant, q1, q2, nv, qq, ds, a[13], a[14],
+                                                    P.godunov_max_iter, &status);
     double* o = out + 10 * i;
     o[0] = t;
     for (int k = 0; k < 5; k++) o[1 + k] = qq[k];
@@ -1302,14 +1414,26 @@ inline int blocks_for(int n, int t) { return (n + t - 1) / t; }
 void launch_centroid(const DevMesh& d, const double* X, const double* Y, double* cx, double* cy, cudaStream_t s) {
     if (d.n_cells > 0) centroid_kernel<<<blocks_for(d.n_cells, 256), 256, 0, s>>>(d, X, Y, cx, cy);
 }
-void launch_stationary(const DevMesh& d, const gelios_params& P, const StepBuffers& b, cudaStream_t s) {
-    stationary_cell_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b);
-}
-void launch_mk2_cells(const DevMesh& d, const gelios_params& P, const StepBuffers& b, cudaStream_t s) {
+void launch_stationary_units(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
+                             cudaStream_t s) {
     if (P.precision == GELIOS_PREC_FP32_FLUX)
-        mk2_cell_kernel<float><<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b);
+        stationary_unit_kernel<float><<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, b, fl);
     else
-        mk2_cell_kernel<double><<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b);
+        stationary_unit_kernel<double><<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, b, fl);
+}
+void launch_stationary_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
+                              cudaStream_t s) {
+    stationary_update_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, fl);
+}
+void launch_mk2_units(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl, cudaStream_t s) {
+    if (P.precision == GELIOS_PREC_FP32_FLUX)
+        mk2_unit_kernel<float><<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, b, fl);
+    else
+        mk2_unit_kernel<double><<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, b, fl);
+}
+void launch_mk2_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
+                       cudaStream_t s) {
+    mk2_update_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, fl);
 }
 void launch_inner(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const int32_t* list, int n,
                   cudaStream_t s) {
@@ -1325,8 +1449,19 @@ void launch_commit(const DevMesh& d, const StepBuffers& b, cudaStream_t s) {
 }
 int launch_motion(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* scratch, cudaStream_t s) {
     int launches = 0;
-    surface_kernel<<<1, 256, 0, s>>>(d, P, b, scratch);
-    launches++;
+    const int nf = d.n_lc + d.n_li + d.n_lo;
+    if (nf > 0) {
+        surface_faces_kernel<<<blocks_for(nf, 64), 64, 0, s>>>(d, P, b, scratch);
+        const size_t shm = static_cast<size_t>(d.n_sp) * (2 * sizeof(double) + sizeof(int));
+        static size_t shm_opted = 0;
+        if (shm > 48 * 1024 && shm > shm_opted) {
+            cudaFuncSetAttribute(surface_nodes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(shm));
+            shm_opted = shm;
+        }
+        surface_nodes_kernel<<<1, 512, shm, s>>>(d, b, scratch);
+        launches += 2;
+    }
     if (d.n_rail_a + d.n_rail_b > 0) {
         rail_ab_kernel<<<d.n_rail_a + d.n_rail_b, 128, 0, s>>>(d, P, b.dt_cur, 0, d.n_rail_a + d.n_rail_b);
         launches++;

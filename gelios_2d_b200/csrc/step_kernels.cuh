@@ -28,6 +28,10 @@ struct DevMesh {
     const uint32_t* cflags = nullptr;
     const int32_t *sA = nullptr, *sB = nullptr, *snb = nullptr, *ssd = nullptr, *ssd2 = nullptr;
     const uint32_t* sinfo = nullptr;
+    // face units (one flux evaluation each, see step_kernels.cu): owner slot,
+    // owner cell, slot of the twin face in the neighbour (-1: one-sided)
+    int n_slots = 0, n_units = 0;
+    const int32_t *u_slot = nullptr, *u_cell = nullptr, *u_twin = nullptr;
     const int32_t *fA = nullptr, *fB = nullptr, *ftype = nullptr, *fmaster = nullptr, *fsosed = nullptr,
                   *fcopy = nullptr, *fsdown = nullptr;
     const int32_t *rtype = nullptr, *rM = nullptr, *rpstart = nullptr, *rpts = nullptr, *rkstart = nullptr,
@@ -36,6 +40,14 @@ struct DevMesh {
     int n_rail_a = 0, n_rail_b = 0, n_rail_c = 0, n_rail_d = 0;
     const int32_t *lc = nullptr, *li = nullptr, *lo = nullptr;
     int n_lc = 0, n_li = 0, n_lo = 0;
+    // surface-tracking nodes (points of the three tracked lines): point id,
+    // line (0 contact, 1 inner, 2 outer), up to 4 face incidences (j << 1 |
+    // end, j in the concatenated line order, end 0 = A, 1 = B; -1 = none),
+    // up to 4 contact faces whose A end it is (-1 = none); fix-up node ids
+    // (a0, b0, a_last, b_last) per line
+    int n_sp = 0;
+    const int32_t *sp_point = nullptr, *sp_line = nullptr, *sp_inc = nullptr, *sp_ainc = nullptr,
+                  *sp_fix = nullptr;
     const double *Hn = nullptr, *Hu = nullptr, *Hv = nullptr, *HT = nullptr, *ku = nullptr, *kv = nullptr,
                  *kT = nullptr, *r_istoch = nullptr;
     const int32_t *cback = nullptr, *cnext = nullptr;
@@ -58,8 +70,13 @@ struct StepBuffers {
 };
 
 void launch_centroid(const DevMesh& d, const double* X, const double* Y, double* cx, double* cy, cudaStream_t s);
-void launch_stationary(const DevMesh& d, const gelios_params& P, const StepBuffers& b, cudaStream_t s);
-void launch_mk2_cells(const DevMesh& d, const gelios_params& P, const StepBuffers& b, cudaStream_t s);
+void launch_stationary_units(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
+                             cudaStream_t s);
+void launch_stationary_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
+                              cudaStream_t s);
+void launch_mk2_units(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl, cudaStream_t s);
+void launch_mk2_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
+                       cudaStream_t s);
 void launch_inner(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const int32_t* list, int n,
                   cudaStream_t s);
 void launch_dt_finalize(const StepBuffers& b, cudaStream_t s);

@@ -156,8 +156,6 @@ class Setka:
         N.check(self._L.gelios_download_points(self._h, x, y), "gelios_download_points")
         return x, y
 
-    PHASES = ("centroids", "motion", "cells", "commit_dt")
-
     def set_phase_timing(self, on: bool):
         N.check(self._L.gelios_set_phase_timing(self._h, int(bool(on))), "gelios_set_phase_timing")
 
@@ -166,7 +164,7 @@ class Setka:
         ms = np.zeros(5)
         ln = np.zeros(5, np.int64)
         N.check(self._L.gelios_phase_times(self._h, ms, ln, int(bool(reset))), "gelios_phase_times")
-        names = ("centroids", "surface", "motion", "cells", "commit_dt")
+        names = ("centroids", "faces", "motion", "cells", "commit_dt")
         return {names[k]: (float(ms[k]), int(ln[k])) for k in range(5)}
 
     def launches(self) -> int:

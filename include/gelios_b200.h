@@ -180,8 +180,8 @@ void *gelios_stream(gelios_ctx *ctx);
 int64_t gelios_last_launch_count(gelios_ctx *ctx);
 /* Phase timing: when enabled, gelios_step brackets each phase with CUDA
  * events on the context stream and accumulates, per phase, the device time
- * and the number of launches (phases: 0 centroids, 1 Move_surface,
- * 2 rail motion, 3 cell update, 4 commit/dt).  gelios_phase_times
+ * and the number of launches (phases: 0 centroids, 1 face fluxes,
+ * 2 surface tracking + rail motion, 3 cell update, 4 commit/dt).  gelios_phase_times
  * synchronises, writes ms[5] and launches[5] accumulated since the last
  * reset, and resets when `reset` is non-zero. */
 int gelios_set_phase_timing(gelios_ctx *ctx, int enabled);
