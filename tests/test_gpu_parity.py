@@ -225,4 +225,4 @@ def test_launch_count_reported():
     P = W.plain_params()
     dev, _ = _pair(mesh, P, W.plain_initial(mesh, P))
     dev.Go_stationary(5)
-    assert dev.launches() == 1 + 2 * 5
+    assert dev.launches() == 1 + 3 * 5  # centroids + (face units, cell update, dt) per step
