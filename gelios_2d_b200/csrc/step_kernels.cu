@@ -199,12 +199,14 @@ __device__ St5 tvd_usualy(const double* const* st, const double* cx, const doubl
     const double dist2 = sqrt(sq(fx - Mx) + sq(fy - My));
     if (tracked) {  // Gran.cpp:345-426
         const double dist1 = sqrt(sq(fx - cx[Sd]) + sq(fy - cy[Sd]));
+        // linear(-dist1, t1, -dist2, t2, 0) with one reciprocal
+        const double r = 1.0 / (-dist1 - (-dist2)), x2 = -dist2;
         St5 o;
-        o.ro = linear2(-dist1, par1.ro, -dist2, Ms.ro, 0.0);
-        o.p = linear2(-dist1, par1.p, -dist2, Ms.p, 0.0);
-        o.u = linear2(-dist1, par1.u, -dist2, Ms.u, 0.0);
-        o.v = linear2(-dist1, par1.v, -dist2, Ms.v, 0.0);
-        o.Q = linear2(-dist1, par1.Q, -dist2, Ms.Q, 0.0);
+        o.ro = (par1.ro - Ms.ro) * r * (0.0 - x2) + Ms.ro;
+        o.p = (par1.p - Ms.p) * r * (0.0 - x2) + Ms.p;
+        o.u = (par1.u - Ms.u) * r * (0.0 - x2) + Ms.u;
+        o.v = (par1.v - Ms.v) * r * (0.0 - x2) + Ms.v;
+        o.Q = (par1.Q - Ms.Q) * r * (0.0 - x2) + Ms.Q;
         if (o.ro <= 0.0) o.ro = Ms.ro;
         if (o.p <= 0.0) o.p = Ms.p;
         return o;
@@ -212,12 +214,14 @@ __device__ St5 tvd_usualy(const double* const* st, const double* cx, const doubl
     const St5 par3 = load_state(st, So);
     const double dist3 = sqrt(sq(fx - cx[So]) + sq(fy - cy[So]));
     const double dist1 = sqrt(sq(fx - cx[Sd]) + sq(fy - cy[Sd]));
+    // linear(-dist1, t1, -dist2, t2, dist3, t3, 0) for the five fields
+    const double r12 = 1.0 / (-dist1 - (-dist2)), r23 = 1.0 / (-dist2 - dist3), x2 = -dist2;
     St5 o;
-    o.ro = linear3(-dist1, par1.ro, -dist2, Ms.ro, dist3, par3.ro, 0.0);
-    o.p = linear3(-dist1, par1.p, -dist2, Ms.p, dist3, par3.p, 0.0);
-    o.u = linear3(-dist1, par1.u, -dist2, Ms.u, dist3, par3.u, 0.0);
-    o.v = linear3(-dist1, par1.v, -dist2, Ms.v, dist3, par3.v, 0.0);
-    o.Q = linear3(-dist1, par1.Q, -dist2, Ms.Q, dist3, par3.Q, 0.0);
+    o.ro = linear3r(par1.ro, Ms.ro, par3.ro, r12, r23, x2);
+    o.p = linear3r(par1.p, Ms.p, par3.p, r12, r23, x2);
+    o.u = linear3r(par1.u, Ms.u, par3.u, r12, r23, x2);
+    o.v = linear3r(par1.v, Ms.v, par3.v, r12, r23, x2);
+    o.Q = linear3r(par1.Q, Ms.Q, par3.Q, r12, r23, x2);
     if (o.ro <= 0.0 || o.p <= 0.0) *status |= ST_TVD_BAD;  // the reference exits (Gran.cpp:444-455)
     return o;
 }
@@ -329,18 +333,21 @@ __device__ void source_mk1(const DevMesh& d, const gelios_params& P, int k, doub
         }
         const double r1 = d.r_istoch[K_do];
         const double r2 = d.r_istoch[K_posle];
+        // linear(r1, t1, r2, t2, rr) for 19 fields with one reciprocal
+        const double ir = 1.0 / (r1 - r2), dr = rr - r2;
+        auto lin = [&](double t1, double t2) { return (t1 - t2) * ir * dr + t2; };
         double TH[4];
 #pragma unroll
-        for (int s = 0; s < 4; s++) uH[s] = linear2(r1, d.Hu[4 * K_do + s], r2, d.Hu[4 * K_posle + s], rr);
+        for (int s = 0; s < 4; s++) uH[s] = lin(d.Hu[4 * K_do + s], d.Hu[4 * K_posle + s]);
 #pragma unroll
-        for (int s = 0; s < 4; s++) vH[s] = linear2(r1, d.Hv[4 * K_do + s], r2, d.Hv[4 * K_posle + s], rr);
+        for (int s = 0; s < 4; s++) vH[s] = lin(d.Hv[4 * K_do + s], d.Hv[4 * K_posle + s]);
 #pragma unroll
-        for (int s = 0; s < 4; s++) roH[s] = linear2(r1, d.Hn[4 * K_do + s], r2, d.Hn[4 * K_posle + s], rr);
+        for (int s = 0; s < 4; s++) roH[s] = lin(d.Hn[4 * K_do + s], d.Hn[4 * K_posle + s]);
 #pragma unroll
-        for (int s = 0; s < 4; s++) TH[s] = linear2(r1, d.HT[4 * K_do + s], r2, d.HT[4 * K_posle + s], rr);
-        ku = linear2(r1, d.ku[K_do], r2, d.ku[K_posle], rr);
-        kvv = linear2(r1, d.kv[K_do], r2, d.kv[K_posle], rr);
-        kT = linear2(r1, d.kT[K_do], r2, d.kT[K_posle], rr);
+        for (int s = 0; s < 4; s++) TH[s] = lin(d.HT[4 * K_do + s], d.HT[4 * K_posle + s]);
+        ku = lin(d.ku[K_do], d.ku[K_posle]);
+        kvv = lin(d.kv[K_do], d.kv[K_posle]);
+        kT = lin(d.kT[K_do], d.kT[K_posle]);
 #pragma unroll
         for (int s = 0; s < 4; s++) pH[s] = 0.5 * TH[s] * roH[s];
     } else {
@@ -354,19 +361,23 @@ __device__ void source_mk1(const DevMesh& d, const gelios_params& P, int k, doub
     }
     double Mu = 0.0, Mv = 0.0, MT = 0.0;
     double nuu[4], nuv[4], nue[4];
+    const double pro = p / ro;
+    const double kin = sq(u) + sq(v);
 #pragma unroll
     for (int s = 0; s < 4; s++) {
         if (roH[s] <= 0.0) {
             roH[s] = 0.0000001;
             pH[s] = 0.0;
         }
-        const double UM = sqrt(sq(u - uH[s]) + sq(v - vH[s]) + (64.0 / (9.0 * kPi)) * (p / ro + 2.0 * pH[s] / roH[s]));
-        const double UH = sqrt(sq(u - uH[s]) + sq(v - vH[s]) + (4.0 / kPi) * (p / ro + 2.0 * pH[s] / roH[s]));
+        const double th = 2.0 * pH[s] / roH[s];
+        const double du2 = sq(u - uH[s]) + sq(v - vH[s]);
+        const double UM = sqrt(du2 + (64.0 / (9.0 * kPi)) * (pro + th));
+        const double UH = sqrt(du2 + (4.0 / kPi) * (pro + th));
         const double sig = sq(1.0 - P.a_2 * log(UM));
         const double nu = ro * roH[s] * UM * sig;
         nuu[s] = nu * (uH[s] - u);
         nuv[s] = nu * (vH[s] - v);
-        nue[s] = nu * ((sq(uH[s]) + sq(vH[s]) - sq(u) - sq(v)) / 2.0 + (UH / UM) * (2.0 * pH[s] / roH[s] - p / ro));
+        nue[s] = nu * ((sq(uH[s]) + sq(vH[s]) - kin) / 2.0 + (UH / UM) * (th - pro));
     }
     Mu = P.src_coef * (nuu[0] + nuu[1] + nuu[2] + nuu[3]);
     Mv = P.src_coef * (nuv[0] + nuv[1] + nuv[2] + nuv[3]);
@@ -776,16 +787,17 @@ __global__ void __launch_bounds__(128) mk2_update_kernel(DevMesh d, gelios_param
                 const double Volume2 = volume_rotate(con, n, d.X2, d.Y2);
                 const double ro = par1.ro, u = par1.u, v = par1.v, p = par1.p, Q = par1.Q;
                 const double gm1 = P.gamma - 1;
-                double ro3 = ro * Volume / Volume2 - dt * (Pt0 / Volume2);
-                const double Q33 = Q * Volume / Volume2 - (dt / Volume2) * Pt4;
+                const double rV2 = 1.0 / Volume2, VV = Volume * rV2;
+                double ro3 = ro * VV - dt * (Pt0 * rV2);
+                const double Q33 = Q * VV - (dt * rV2) * Pt4;
                 if (ro3 <= 0.0) {
                     ro3 = P.ro_floor;
                     nro = 1;
                 }
-                const double u3 = (ro * u * Volume / Volume2 - dt * (Pt1 / Volume2 - q2_1)) / ro3;
-                const double v3 =
-                    (ro * v * Volume / Volume2 - dt * ((Pt2 - p * 0.5 * (vs1 + vs2)) / Volume2 - q2_2)) / ro3;
-                double p3 = (((p / gm1 + ro * (u * u + v * v) * 0.5) * Volume / Volume2 - dt * (Pt3 / Volume2 - q3)) -
+                const double rro3 = 1.0 / ro3;
+                const double u3 = (ro * u * VV - dt * (Pt1 * rV2 - q2_1)) * rro3;
+                const double v3 = (ro * v * VV - dt * ((Pt2 - p * 0.5 * (vs1 + vs2)) * rV2 - q2_2)) * rro3;
+                double p3 = (((p / gm1 + ro * (u * u + v * v) * 0.5) * VV - dt * (Pt3 * rV2 - q3)) -
                              0.5 * ro3 * (u3 * u3 + v3 * v3)) *
                             gm1;
                 if (p3 <= 0) {
