@@ -78,6 +78,23 @@ class GeliosStatus(C.Structure):
                 ("n_p_clamp", C.c_int64), ("dt", C.c_double), ("result_buf", C.c_int32), ("pad_", C.c_int32)]
 
 
+_UP = C.POINTER(C.c_uint32)
+
+
+class GeliosDeviceGrid(C.Structure):
+    """gelios_device_grid: device pointers of a grid for the allocation-free step."""
+
+    _fields_ = [("n_cells", C.c_int32), ("n_slots", C.c_int32), ("n_units", C.c_int32),
+                ("x", C.c_void_p), ("y", C.c_void_p), ("contour_start", C.c_void_p), ("contour", C.c_void_p),
+                ("gran_start", C.c_void_p), ("cell_flags", C.c_void_p), ("slot_A", C.c_void_p),
+                ("slot_B", C.c_void_p), ("slot_nb", C.c_void_p), ("slot_info", C.c_void_p),
+                ("unit_slot", C.c_void_p), ("unit_cell", C.c_void_p), ("unit_twin", C.c_void_p)]
+
+
+NOALLOC_MAX_CELLS = 32768
+NOALLOC_MAX_SLOTS = 131072
+
+
 class GeliosError(RuntimeError):
     def __init__(self, code: int, where: str, msg: str):
         super().__init__(f"{where} failed with {code}: {msg}")
@@ -127,6 +144,9 @@ def lib() -> C.CDLL:
     L.gelios_last_launch_count.argtypes = [vp]
     L.gelios_set_phase_timing.argtypes = [vp, C.c_int]
     L.gelios_phase_times.argtypes = [vp, dp, np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS"), C.c_int]
+    L.gelios_stationary_step_noalloc.argtypes = [C.POINTER(GeliosParams), C.POINTER(GeliosDeviceGrid),
+                                                 C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_void_p,
+                                                 C.c_void_p, C.c_void_p]
     L.gelios_hllc_batch.argtypes = [C.POINTER(GeliosParams), C.c_int, dp, dp]
     L.gelios_godunov_batch.argtypes = [C.POINTER(GeliosParams), C.c_int, dp, dp]
     _LIB = L

@@ -196,6 +196,44 @@ int gelios_hllc_batch(const gelios_params *prm, int n, const double *in, double 
  * q1[5] (ro,p,u,v,w), q2[5], n[3], w, dist; out[n*10] = time, q[5], dsl, dsp, dsc, status. */
 int gelios_godunov_batch(const gelios_params *prm, int n, const double *in, double *out);
 
+/* ---- allocation-free plain step (no counterpart in the reference) ---------
+ * For callers that cannot call cudaMalloc when they step (their device memory
+ * is handed out up front by their own pool, or they step where the CUDA
+ * allocator must not be touched): one step of the plain single-fluid form
+ * (the same kernels as gelios_step with GELIOS_FORM_STATIONARY) on a grid
+ * and state the caller already holds in device memory.  Nothing is
+ * allocated: the step's scratch (face-slot fluxes, centroids, dt words) is
+ * one fixed file-scope device array of about 5.8 MB that every GPU loading
+ * the library holds until exit, so grids are limited to
+ * GELIOS_NOALLOC_MAX_CELLS cells and GELIOS_NOALLOC_MAX_SLOTS face slots
+ * (GELIOS_E_LIMIT beyond).  The first call on a device resolves that array's
+ * device address and should come before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU (other streams, other threads)
+ * race.  Inputs: the grid arrays below, state_in[5] (ro, p, u, v, Q per cell)
+ * and dt_in (one device double, the dt of this step); outputs: state_out[5]
+ * and dt_out (the dt the next step would use).  Runs on `stream`
+ * (cudaStream_t as void*, may be NULL) and returns without synchronising. */
+#define GELIOS_NOALLOC_MAX_CELLS 32768
+#define GELIOS_NOALLOC_MAX_SLOTS 131072
+
+typedef struct gelios_device_grid {
+    int32_t n_cells, n_slots, n_units;
+    const double *x, *y;               /* point coordinates */
+    const int32_t *contour_start;      /* n_cells+1 */
+    const int32_t *contour;
+    const int32_t *gran_start;         /* n_cells+1: face slots of cell c are gran_start[c].. */
+    const uint32_t *cell_flags;        /* bit0 has an Axis face, bit1 C_1, bit2 C_centr */
+    const int32_t *slot_A, *slot_B;    /* end points of the face in each slot */
+    const int32_t *slot_nb;            /* Sosed of the face (-1 if none) */
+    const uint32_t *slot_info;         /* Gran_type | 8 both ends tracked | 16 one end tracked */
+    const int32_t *unit_slot, *unit_cell, *unit_twin; /* flux evaluations: owner slot, owner cell,
+                                                           twin slot of an interior face or -1 */
+} gelios_device_grid;
+
+int gelios_stationary_step_noalloc(const gelios_params *prm, const gelios_device_grid *grid,
+                                   const double *const *state_in, double *const *state_out, const double *dt_in,
+                                   double *dt_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
