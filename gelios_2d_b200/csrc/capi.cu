@@ -80,6 +80,8 @@ int upload(DBuf& b, const T* src, size_t n, cudaStream_t s) {
 struct gelios_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;  // overlaps the source terms with the grid motion
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     gelios_params prm{};
     bool have_mesh = false;
     DevMesh d;
@@ -88,7 +90,7 @@ struct gelios_ctx {
     DBuf fA, fB, ftype, fmaster, fsosed, fcopy, fsdown;
     DBuf rtype, rM, rpstart, rpts, rkstart, rkeys, rs;
     DBuf lc, li, lo, sp_point, sp_line, sp_inc, sp_ainc, sp_fix;
-    DBuf u_slot, u_cell, u_twin, flux;
+    DBuf u_slot, u_cell, u_twin, flux, aux;
     DBuf Hn, Hu, Hv, HT, ku, kv, kT, r_istoch, cback, cnext;
     // state par[2] x 5 fields, centroids [2], scratch
     DBuf state[2];
@@ -205,6 +207,9 @@ extern "C" int gelios_create(gelios_ctx** out, const gelios_params* prm, int dev
     ctx->device = device;
     ctx->prm = *prm;
     GELIOS_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    GELIOS_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+    GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+    GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
     if (ctx->words.alloc(64)) return GELIOS_E_CUDA;
     GELIOS_CUDA_TRY(cudaMemsetAsync(ctx->words.p, 0, 64, ctx->stream));
     *out = ctx.release();
@@ -224,6 +229,12 @@ extern "C" void gelios_destroy(gelios_ctx* ctx) {
         cudaStreamSynchronize(ctx->stream);
         cudaStreamDestroy(ctx->stream);
     }
+    if (ctx->side) {
+        cudaStreamSynchronize(ctx->side);
+        cudaStreamDestroy(ctx->side);
+    }
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
     delete ctx;
 }
 
@@ -456,6 +467,7 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     rc |= upload(ctx->u_cell, u_cell.data(), u_cell.size(), s);
     rc |= upload(ctx->u_twin, u_twin.data(), u_twin.size(), s);
     rc |= upload<double>(ctx->flux, nullptr, 5 * static_cast<size_t>(ng), s);
+    rc |= upload<double>(ctx->aux, nullptr, 5 * static_cast<size_t>(nc), s);
     rc |= upload(ctx->sp_point, sp_point.data(), sp_point.size(), s);
     rc |= upload(ctx->sp_line, sp_line.data(), sp_line.size(), s);
     rc |= upload(ctx->sp_inc, sp_inc.data(), sp_inc.size(), s);
@@ -473,8 +485,8 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     rc |= upload(ctx->cnext, cnext, nc, s);
     rc |= upload<double>(ctx->state[0], nullptr, 5 * static_cast<size_t>(nc), s);
     rc |= upload<double>(ctx->state[1], nullptr, 5 * static_cast<size_t>(nc), s);
-    rc |= upload<double>(ctx->cen[0], nullptr, 2 * static_cast<size_t>(nc), s);
-    rc |= upload<double>(ctx->cen[1], nullptr, 2 * static_cast<size_t>(nc), s);
+    rc |= upload<double>(ctx->cen[0], nullptr, 3 * static_cast<size_t>(nc), s);
+    rc |= upload<double>(ctx->cen[1], nullptr, 3 * static_cast<size_t>(nc), s);
     rc |= upload<double>(ctx->surface, nullptr,
                          4 * (static_cast<size_t>(v->n_contact) + v->n_inner_line + v->n_outer_line) + 1, s);
     if (rc) return GELIOS_E_CUDA;
@@ -652,7 +664,7 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
     if (ctx->ev_used > 4096) ctx->collect();
     {
         cudaEvent_t e0 = ctx->phase_begin();
-        launch_centroid(d, d.X, d.Y, cen0, cen0 + d.n_cells, s);
+        launch_centroid(d, d.X, d.Y, cen0, cen0 + d.n_cells, cen0 + 2 * static_cast<size_t>(d.n_cells), P.gamma, s);
         ctx->phase_end(0, e0, 1);
     }
     launches++;
@@ -673,24 +685,33 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             double* cn = (st & 1) ? cen0 : cen1;
             b.cx = cc;
             b.cy = cc + d.n_cells;
+            b.rp = cc + 2 * static_cast<size_t>(d.n_cells);
             b.cx_next = cn;
             b.cy_next = cn + d.n_cells;
+            b.rp_next = cn + 2 * static_cast<size_t>(d.n_cells);
+            // side stream: source terms and pre-motion geometry, overlapping the motion
+            GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_fork, s));
+            GELIOS_CUDA_TRY(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
+            launch_mk2_source(d, P, b, ctx->aux.as<double>(), ctx->side);
+            GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_join, ctx->side));
             cudaEvent_t e1 = ctx->phase_begin();
             const int nm = launch_motion(d, P, b, ctx->surface.as<double>(), s);
-            ctx->phase_end(2, e1, nm);  // Move_surface + rails (surface is 1 of them)
+            ctx->phase_end(2, e1, nm);  // Move_surface + rails
             cudaEvent_t e3 = ctx->phase_begin();
             launch_mk2_units(d, P, b, ctx->flux.as<double>(), s);
             ctx->phase_end(1, e3, 1);
+            GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_join, 0));
             cudaEvent_t e5 = ctx->phase_begin();
-            launch_mk2_update(d, P, b, ctx->flux.as<double>(), s);
+            launch_mk2_update(d, P, b, ctx->flux.as<double>(), ctx->aux.as<double>(), s);
             ctx->phase_end(3, e5, 1);
             cudaEvent_t e4 = ctx->phase_begin();
             launch_commit(d, b, s);
             ctx->phase_end(4, e4, 1);
-            launches += nm + 3;
+            launches += nm + 4;
         } else {
             b.cx = cen0;
             b.cy = cen0 + d.n_cells;
+            b.rp = cen0 + 2 * static_cast<size_t>(d.n_cells);
             if (form == GELIOS_FORM_STATIONARY) {
                 cudaEvent_t e1 = ctx->phase_begin();
                 launch_stationary_units(d, P, b, ctx->flux.as<double>(), s);

@@ -31,10 +31,11 @@ using namespace gelios;
 
 namespace {
 
-// scratch layout (doubles): flux slots [5 * MAX_SLOTS], centroids [2 * MAX_CELLS],
+// scratch layout (doubles): flux slots [5 * MAX_SLOTS], centroids and
+// |centroid|^(2 gamma) [3 * MAX_CELLS],
 // then 8 doubles of dt/status words (T unused, acc, counters[2], status)
 constexpr size_t kFluxDoubles = 5ull * GELIOS_NOALLOC_MAX_SLOTS;
-constexpr size_t kCenDoubles = 2ull * GELIOS_NOALLOC_MAX_CELLS;
+constexpr size_t kCenDoubles = 3ull * GELIOS_NOALLOC_MAX_CELLS;
 constexpr size_t kWordDoubles = 8;
 constexpr size_t kScratchDoubles = kFluxDoubles + kCenDoubles + kWordDoubles;
 
@@ -135,6 +136,7 @@ extern "C" int gelios_stationary_step_noalloc(const gelios_params* prm, const ge
     }
     b.cx = cen;
     b.cy = cen + GELIOS_NOALLOC_MAX_CELLS;
+    b.rp = cen + 2 * GELIOS_NOALLOC_MAX_CELLS;
     b.dt_cur = dt_in;
     b.dt_next = dt_out;
     b.dt_acc = reinterpret_cast<unsigned long long*>(words + 8);
@@ -142,7 +144,8 @@ extern "C" int gelios_stationary_step_noalloc(const gelios_params* prm, const ge
     b.status = reinterpret_cast<int*>(words + 32);
     // the array keeps the last call's contents: re-arm the words first
     noalloc_words_init<<<1, 1, 0, s>>>(b.dt_acc, b.counters, b.status);
-    launch_centroid(d, d.X, d.Y, cen, cen + GELIOS_NOALLOC_MAX_CELLS, s);
+    launch_centroid(d, d.X, d.Y, cen, cen + GELIOS_NOALLOC_MAX_CELLS, cen + 2 * GELIOS_NOALLOC_MAX_CELLS, prm->gamma,
+                    s);
     launch_stationary_units(d, *prm, b, flux, s);
     launch_stationary_update(d, *prm, b, flux, s);
     launch_dt_finalize(b, s);

@@ -239,10 +239,12 @@ __device__ __forceinline__ St5 tvd_axis(const double* const* st, const double* c
 }
 
 // Gran::Get_par_TVD_radial (Gran.cpp:562-675), ro and p only (the callers
-// use no other field).
-__device__ void tvd_radial(const double* const* st, const double* cx, const double* cy, double fx, double fy,
-                           const St5& Ms, double Mx, double My, int So, int Sd, bool m_has_axis, double g2,
-                           double& oro, double& op) {
+// use no other field).  rp[c] = |centroid of c|^(2 gamma) is computed once
+// per cell and step; pdis = |face centre|^(2 gamma) once per face (the
+// reference evaluates pow at every use).
+__device__ void tvd_radial(const double* const* st, const double* cx, const double* cy, const double* rp, double fx,
+                           double fy, const St5& Ms, double Mx, double My, double rpM, int So, int Sd,
+                           bool m_has_axis, double pdis, double& oro, double& op) {
     const double r = sqrt(sq(fx) + sq(fy));
     if (Sd < 0) {
         if (!m_has_axis) {
@@ -256,11 +258,11 @@ __device__ void tvd_radial(const double* const* st, const double* cx, const doub
         const double sx = cx[So], sy = cy[So];
         const double r3 = sqrt(sq(sx) + sq(sy));
         const double dist3 = sqrt(sq(fx - sx) + sq(fy - sy));
-        const double r1 = sqrt(sq(Mx) + sq(-My));
         const double dist1 = sqrt(sq(fx - Mx) + sq(fy - (-My)));
-        oro = linear3(-dist1, Ms.ro * sq(r1), -dist2, Ms.ro * sq(r2), dist3, par3.ro * sq(r3), 0.0) / sq(r);
-        op = linear3(-dist1, Ms.p * pow2g(r1, g2), -dist2, Ms.p * pow2g(r2, g2), dist3, par3.p * pow2g(r3, g2), 0.0) /
-             pow2g(r, g2);
+        const double r12 = 1.0 / (-dist1 - (-dist2)), r23 = 1.0 / (-dist2 - dist3);
+        // the mirrored centre has the radius of M itself
+        oro = linear3r(Ms.ro * sq(r2), Ms.ro * sq(r2), par3.ro * sq(r3), r12, r23, -dist2) / sq(r);
+        op = linear3r(Ms.p * rpM, Ms.p * rpM, par3.p * rp[So], r12, r23, -dist2) / pdis;
         return;
     }
     const St5 par1 = load_state(st, Sd);
@@ -273,9 +275,9 @@ __device__ void tvd_radial(const double* const* st, const double* cx, const doub
     const double dx = cx[Sd], dy = cy[Sd];
     const double r1 = sqrt(sq(dx) + sq(dy));
     const double dist1 = sqrt(sq(fx - dx) + sq(fy - dy));
-    oro = linear3(-dist1, par1.ro * sq(r1), -dist2, Ms.ro * sq(r2), dist3, par3.ro * sq(r3), 0.0) / sq(r);
-    op = linear3(-dist1, par1.p * pow2g(r1, g2), -dist2, Ms.p * pow2g(r2, g2), dist3, par3.p * pow2g(r3, g2), 0.0) /
-         pow2g(r, g2);
+    const double r12 = 1.0 / (-dist1 - (-dist2)), r23 = 1.0 / (-dist2 - dist3);
+    oro = linear3r(par1.ro * sq(r1), Ms.ro * sq(r2), par3.ro * sq(r3), r12, r23, -dist2) / sq(r);
+    op = linear3r(par1.p * rp[Sd], Ms.p * rpM, par3.p * rp[So], r12, r23, -dist2) / pdis;
 }
 
 // Cell::Get_Sourse_MK1 (Cell.cpp:498-665).
@@ -435,7 +437,7 @@ __device__ __forceinline__ void block_reduce_commit(double t, int nro, int np_, 
 
 // ------------------------------------------------------------------ kernels
 __global__ void centroid_kernel(DevMesh d, const double* __restrict__ X, const double* __restrict__ Y, double* cx,
-                                double* cy) {
+                                double* cy, double* rp, double g2) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= d.n_cells) return;
     const int s = d.cstart[c], n = d.cstart[c + 1] - s;
@@ -443,6 +445,7 @@ __global__ void centroid_kernel(DevMesh d, const double* __restrict__ X, const d
     centroid(d.contour + s, n, X, Y, x, y);
     cx[c] = x;
     cy[c] = y;
+    rp[c] = pow2g(sqrt(sq(x) + sq(y)), g2);
 }
 
 // ------------------------------------------------------------------ face units
@@ -460,9 +463,9 @@ __global__ void centroid_kernel(DevMesh d, const double* __restrict__ X, const d
 // owner; neighbour (for Usualy faces) state/centre.
 template <typename TF>
 __device__ __forceinline__ double stationary_side(const gelios_params& P, int ft, const St5& own, double x, double y,
-                                                  double rad, double xa, double ya, double xb, double yb,
-                                                  const St5& nbs, double x3, double y3, FluxOut<double>& F,
-                                                  double& dist) {
+                                                  double rad, double rpo, double xa, double ya, double xb, double yb,
+                                                  const St5& nbs, double x3, double y3, double rpn,
+                                                  FluxOut<double>& F, double& dist) {
     const double g2 = 2 * P.gamma;
     const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
     dist = sqrt(sq(x - x2) + sq(y - y2));
@@ -482,17 +485,17 @@ __device__ __forceinline__ double stationary_side(const gelios_params& P, int ft
     if (rad < P.rad_stat && ft == G_USUALY) {
         const double dd = sqrt(sq(x3) + sq(y3));
         const double f2 = sq(x2) + sq(y2);
-        const double fr = sqrt(f2);
+        const double pf = pow2g(sqrt(f2), g2);  // (rad/fr)^(2g) = rad^(2g) / fr^(2g)
         par11.ro = par11.ro * sq(rad) / f2;
         par2.ro = par2.ro * sq(dd) / f2;
-        par11.p = par11.p * pow2g(rad / fr, g2);
-        par2.p = par2.p * pow2g(dd / fr, g2);
+        par11.p = par11.p * (rpo / pf);
+        par2.p = par2.p * (rpn / pf);
         polar_perenos(x, y, x2, y2, par11.u, par11.v);
         polar_perenos(x3, y3, x2, y2, par2.u, par2.v);
     } else if (ft == G_INNER_SPHERE) {
         const double f2 = sq(x2) + sq(y2);
         par11.ro = par11.ro * sq(rad) / f2;
-        par11.p = par11.p * pow2g(rad / sqrt(f2), g2);
+        par11.p = par11.p * (rpo / pow2g(sqrt(f2), g2));
     } else if (rad < P.rad_stat && ft == G_AXIS) {
         polar_perenos(x, y, x2, y2, par11.u, par11.v);
         par11.v = 0.0;
@@ -533,7 +536,9 @@ __global__ void __launch_bounds__(128) stationary_unit_kernel(DevMesh d, gelios_
             }
             FluxOut<double> F;
             double dist;
-            const double UU = stationary_side<TF>(P, ft, own, x, y, rad, xa, ya, xb, yb, nbs, x3, y3, F, dist);
+            const double rpK = b.rp[K], rpN = nb >= 0 ? b.rp[nb] : 0.0;
+            const double UU =
+                stationary_side<TF>(P, ft, own, x, y, rad, rpK, xa, ya, xb, yb, nbs, x3, y3, rpN, F, dist);
             fl[0 * ng + g] = F.P0 * S;
             fl[1 * ng + g] = F.P1 * S;
             fl[2 * ng + g] = F.P2 * S;
@@ -556,7 +561,8 @@ __global__ void __launch_bounds__(128) stationary_unit_kernel(DevMesh d, gelios_
                 } else {
                     FluxOut<double> G;
                     double distn;
-                    const double Un = stationary_side<TF>(P, ft, nbs, x3, y3, radn, xb, yb, xa, ya, own, x, y, G, distn);
+                    const double Un =
+                        stationary_side<TF>(P, ft, nbs, x3, y3, radn, rpN, xb, yb, xa, ya, own, x, y, rpK, G, distn);
                     fl[0 * ng + gt] = G.P0 * S;
                     fl[1 * ng + gt] = G.P1 * S;
                     fl[2 * ng + gt] = G.P2 * S;
@@ -624,17 +630,17 @@ __global__ void __launch_bounds__(128) stationary_update_kernel(DevMesh d, gelio
 // for a Usualy face: owner M (state Ms, centre Mx,My, flags mf), across the
 // face the cell So; Sd = Sosed_down of the face as seen from M.
 __device__ __forceinline__ St5 mk2_usualy_side(const double* const* st, const double* cx, const double* cy,
-                                               double fx, double fy, double dis, const St5& Ms, double Mx,
-                                               double My, uint32_t mf, int So, int Sd, bool tracked, double g2,
-                                               int* status) {
+                                               const double* rp, double fx, double fy, double dis, double pdis,
+                                               const St5& Ms, double Mx, double My, double rpM, uint32_t mf, int So,
+                                               int Sd, bool tracked, int* status) {
     if (mf & CF_C1) {
         const double radius = sqrt(sq(Mx) + sq(My));
         St5 o = Ms;
         o.ro = o.ro * sq(radius) / sq(dis);
         o.Q = o.Q * sq(radius) / sq(dis);
-        o.p = o.p * pow2g(radius / dis, g2);
+        o.p = o.p * (rpM / pdis);
         polar_perenos(Mx, My, fx, fy, o.u, o.v);
-        tvd_radial(st, cx, cy, fx, fy, Ms, Mx, My, So, Sd, (mf & CF_AXIS) != 0, g2, o.ro, o.p);
+        tvd_radial(st, cx, cy, rp, fx, fy, Ms, Mx, My, rpM, So, Sd, (mf & CF_AXIS) != 0, pdis, o.ro, o.p);
         return o;
     }
     return tvd_usualy(st, cx, cy, fx, fy, Ms, Mx, My, So, Sd, (mf & CF_AXIS) != 0, tracked, status);
@@ -682,22 +688,27 @@ __global__ void __launch_bounds__(128) mk2_unit_kernel(DevMesh d, gelios_params 
             const double W = ((x4 - x2) * n1 + (y4 - y2) * n2) / dt;
             const double dis = sqrt(sq(x2) + sq(y2));
             const bool tracked = (info & SI_GOD) != 0;
+            const uint32_t nbf = nb >= 0 ? d.cflags[nb] : 0u;
+            // |face centre|^(2 gamma), needed only by the radial forms
+            const bool radial = ((cf & CF_C1) && (ft == G_USUALY || ft == G_AXIS)) || ft == G_INNER_SPHERE ||
+                                (ft == G_USUALY && (nbf & CF_C1));
+            const double pdis = radial ? pow2g(dis, g2) : 1.0;
             if (ft == G_USUALY) {
-                par11 = mk2_usualy_side(b.cur, b.cx, b.cy, x2, y2, dis, par1, x, y, cf, nb, d.ssd[g], tracked, g2,
-                                        &status);
-                par2 = mk2_usualy_side(b.cur, b.cx, b.cy, x2, y2, dis, par2, x3, y3, d.cflags[nb], K, d.ssd2[g],
-                                       tracked, g2, &status);
+                par11 = mk2_usualy_side(b.cur, b.cx, b.cy, b.rp, x2, y2, dis, pdis, par1, x, y, b.rp[K], cf, nb,
+                                        d.ssd[g], tracked, &status);
+                par2 = mk2_usualy_side(b.cur, b.cx, b.cy, b.rp, x2, y2, dis, pdis, par2, x3, y3, b.rp[nb], nbf, K,
+                                       d.ssd2[g], tracked, &status);
             } else if (ft == G_INNER_SPHERE) {
                 const double radius = sqrt(sq(x) + sq(y));
                 par11.ro = par11.ro * sq(radius) / sq(dis);
                 par11.Q = par11.Q * sq(radius) / sq(dis);
-                par11.p = par11.p * pow2g(radius / dis, g2);
+                par11.p = par11.p * (b.rp[K] / pdis);
             } else if (ft == G_AXIS) {
                 if (cf & CF_C1) {
                     const double radius = sqrt(sq(x) + sq(y));
                     par11.ro = par11.ro * sq(radius) / sq(dis);
                     par11.Q = par11.Q * sq(radius) / sq(dis);
-                    par11.p = par11.p * pow2g(radius / dis, g2);
+                    par11.p = par11.p * (b.rp[K] / pdis);
                     polar_perenos(x, y, x2, y2, par11.u, par11.v);
                 } else {
                     par11 = tvd_axis(b.cur, b.cx, b.cy, x2, y2, par1, x, y, d.ssd[g]);
@@ -749,10 +760,39 @@ __global__ void __launch_bounds__(128) mk2_unit_kernel(DevMesh d, gelios_params 
     block_reduce_commit(tmin_u, 0, 0, status, b.dt_acc, b.counters, b.status);
 }
 
+// Terms of the MK2 cell update that do not depend on the fluxes or on the
+// motion: the charge-exchange source Get_Sourse_MK1 (Cell.cpp:498-665) and
+// the area / rotated volume of the cell before the motion.  Runs on a side
+// stream while surface tracking and the rails move the grid.
+// aux rows: q1, q2, q3, vs1 (Get_Volume), Volume (Get_Volume_rotate/2pi)
+__global__ void __launch_bounds__(128) mk2_source_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                         double* __restrict__ aux) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    int status = 0;
+    if (c < d.n_cells) {
+        const double x = b.cx[c], y = b.cy[c];
+        if (!(sqrt(sq(x) + sq(y)) < P.R11)) {
+            const size_t n = d.n_cells;
+            const St5 par1 = load_state(b.cur, c);
+            double q1, q2, q3;
+            source_mk1(d, P, c, x, y, par1.u, par1.v, par1.ro, par1.p, q1, q2, q3, &status);
+            aux[0 * n + c] = q1;
+            aux[1 * n + c] = q2;
+            aux[2 * n + c] = q3;
+            const int s0 = d.cstart[c], nv = d.cstart[c + 1] - s0;
+            const int32_t* con = d.contour + s0;
+            aux[3 * n + c] = area(con, nv, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X, d.Y, false);
+            aux[4 * n + c] = volume_rotate(con, nv, d.X, d.Y);
+        }
+    }
+    if (status) atomicOr(b.status, status);
+}
+
 // Go_5_komponent__MK2 cell update (Setka.cpp:10386-10468) from the summed
 // slots; also the centroid of the moved cell (the next step's centroid).
 __global__ void __launch_bounds__(128) mk2_update_kernel(DevMesh d, gelios_params P, StepBuffers b,
-                                                         const double* __restrict__ fl) {
+                                                         const double* __restrict__ fl,
+                                                         const double* __restrict__ aux) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     double tmark = __longlong_as_double(0x7ff0000000000000LL);
     int nro = 0, npc = 0, status = 0;
@@ -764,6 +804,7 @@ __global__ void __launch_bounds__(128) mk2_update_kernel(DevMesh d, gelios_param
         centroid(con, n, d.X2, d.Y2, xn, yn);
         b.cx_next[c] = xn;
         b.cy_next[c] = yn;
+        b.rp_next[c] = pow2g(sqrt(sq(xn) + sq(yn)), 2 * P.gamma);
         const double x = b.cx[c], y = b.cy[c];
         if (!(sqrt(sq(x) + sq(y)) < P.R11)) {
             tmark = 10000000.0;  // `time` starts at 1e7 in every step (Setka.cpp:10141)
@@ -778,12 +819,12 @@ __global__ void __launch_bounds__(128) mk2_update_kernel(DevMesh d, gelios_param
                 Pt4 = Pt4 + fl[4 * ng + g];
             }
             const St5 par1 = load_state(b.cur, c);
-            double q2_1, q2_2, q3;
-            source_mk1(d, P, c, x, y, par1.u, par1.v, par1.ro, par1.p, q2_1, q2_2, q3, &status);
+            const size_t nc = d.n_cells;
+            const double q2_1 = aux[0 * nc + c], q2_2 = aux[1 * nc + c], q3 = aux[2 * nc + c];
             if (!(d.cflags[c] & CF_CENTR)) {
-                const double vs1 = area(con, n, d.sA, d.sB, g0, g1, d.X, d.Y, false);
+                const double vs1 = aux[3 * nc + c];
                 const double vs2 = area(con, n, d.sA, d.sB, g0, g1, d.X2, d.Y2, true);
-                const double Volume = volume_rotate(con, n, d.X, d.Y);
+                const double Volume = aux[4 * nc + c];
                 const double Volume2 = volume_rotate(con, n, d.X2, d.Y2);
                 const double ro = par1.ro, u = par1.u, v = par1.v, p = par1.p, Q = par1.Q;
                 const double gm1 = P.gamma - 1;
@@ -870,24 +911,25 @@ __global__ void __launch_bounds__(128) inner_cell_kernel(DevMesh d, gelios_param
                 par2.ro = par2.ro * sq(dd) / sq(dis);
                 par11.Q = par11.Q * sq(radius) / sq(dis);
                 par2.Q = par2.Q * sq(dd) / sq(dis);
-                par11.p = par11.p * pow2g(radius / dis, g2);
-                par2.p = par2.p * pow2g(dd / dis, g2);
+                const double pdis = pow2g(dis, g2);
+                par11.p = par11.p * (b.rp[c] / pdis);
+                par2.p = par2.p * (b.rp[nb] / pdis);
                 polar_perenos(x, y, x2, y2, par11.u, par11.v);
                 polar_perenos(x3, y3, x2, y2, par2.u, par2.v);
                 const uint32_t nbf = d.cflags[nb];
                 if ((cf & CF_C1) && (nbf & CF_C1)) {
                     const St5 nbs = load_state(st, nb);
-                    tvd_radial(st, b.cx, b.cy, x2, y2, par1, x, y, nb, d.ssd[g], (cf & CF_AXIS) != 0, g2, par11.ro,
-                               par11.p);
-                    tvd_radial(st, b.cx, b.cy, x2, y2, nbs, x3, y3, c, d.ssd2[g], (nbf & CF_AXIS) != 0, g2, par2.ro,
-                               par2.p);
+                    tvd_radial(st, b.cx, b.cy, b.rp, x2, y2, par1, x, y, b.rp[c], nb, d.ssd[g], (cf & CF_AXIS) != 0,
+                               pdis, par11.ro, par11.p);
+                    tvd_radial(st, b.cx, b.cy, b.rp, x2, y2, nbs, x3, y3, b.rp[nb], c, d.ssd2[g],
+                               (nbf & CF_AXIS) != 0, pdis, par2.ro, par2.p);
                 }
             } else if (ft == G_INNER_SPHERE) {
                 par11 = par2;
             } else if (ft == G_AXIS) {
                 par11.ro = par11.ro * sq(radius) / sq(dis);
                 par11.Q = par11.Q * sq(radius) / sq(dis);
-                par11.p = par11.p * pow2g(radius / dis, g2);
+                par11.p = par11.p * (b.rp[c] / pow2g(dis, g2));
                 polar_perenos(x, y, x2, y2, par11.u, par11.v);
                 par2 = par11;
                 par2.v = -par2.v;
@@ -1225,7 +1267,7 @@ __global__ void __launch_bounds__(64) surface_faces_kernel(DevMesh d, gelios_par
         const double dis = sqrt(sq(x2) + sq(y2));
         const St5 p2 = face_tvd(d, st, b.cx, b.cy, d.fcopy[f], &status);
         p1.ro = p1.ro * sq(radius) / sq(dis);
-        p1.p = p1.p * pow2g(radius / dis, g2);
+        p1.p = p1.p * (b.rp[M] / pow2g(dis, g2));
         polar_perenos(x, y, x2, y2, p1.u, p1.v);
         q1[0] = p1.ro; q1[1] = p1.p; q1[2] = p1.u; q1[3] = p1.v; q1[4] = 0.0;
         q2[0] = p2.ro; q2[1] = p2.p; q2[2] = p2.u; q2[3] = p2.v; q2[4] = 0.0;
@@ -1423,8 +1465,9 @@ namespace {
 inline int blocks_for(int n, int t) { return (n + t - 1) / t; }
 }
 
-void launch_centroid(const DevMesh& d, const double* X, const double* Y, double* cx, double* cy, cudaStream_t s) {
-    if (d.n_cells > 0) centroid_kernel<<<blocks_for(d.n_cells, 256), 256, 0, s>>>(d, X, Y, cx, cy);
+void launch_centroid(const DevMesh& d, const double* X, const double* Y, double* cx, double* cy, double* rp,
+                     double gamma, cudaStream_t s) {
+    if (d.n_cells > 0) centroid_kernel<<<blocks_for(d.n_cells, 256), 256, 0, s>>>(d, X, Y, cx, cy, rp, 2 * gamma);
 }
 void launch_stationary_units(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
                              cudaStream_t s) {
@@ -1444,8 +1487,11 @@ void launch_mk2_units(const DevMesh& d, const gelios_params& P, const StepBuffer
         mk2_unit_kernel<double><<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, b, fl);
 }
 void launch_mk2_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
-                       cudaStream_t s) {
-    mk2_update_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, fl);
+                       const double* aux, cudaStream_t s) {
+    mk2_update_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, fl, aux);
+}
+void launch_mk2_source(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* aux, cudaStream_t s) {
+    mk2_source_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, aux);
 }
 void launch_inner(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const int32_t* list, int n,
                   cudaStream_t s) {

@@ -60,8 +60,10 @@ struct StepBuffers {
     double* nxt[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     const double* cx = nullptr;
     const double* cy = nullptr;
+    const double* rp = nullptr;  // |centroid|^(2 gamma) per cell
     double* cx_next = nullptr;
     double* cy_next = nullptr;
+    double* rp_next = nullptr;
     const double* dt_cur = nullptr;
     double* dt_next = nullptr;
     unsigned long long* dt_acc = nullptr;
@@ -69,14 +71,16 @@ struct StepBuffers {
     int* status = nullptr;
 };
 
-void launch_centroid(const DevMesh& d, const double* X, const double* Y, double* cx, double* cy, cudaStream_t s);
+void launch_centroid(const DevMesh& d, const double* X, const double* Y, double* cx, double* cy, double* rp,
+                     double gamma, cudaStream_t s);
 void launch_stationary_units(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
                              cudaStream_t s);
 void launch_stationary_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
                               cudaStream_t s);
 void launch_mk2_units(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl, cudaStream_t s);
 void launch_mk2_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
-                       cudaStream_t s);
+                       const double* aux, cudaStream_t s);
+void launch_mk2_source(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* aux, cudaStream_t s);
 void launch_inner(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const int32_t* list, int n,
                   cudaStream_t s);
 void launch_dt_finalize(const StepBuffers& b, cudaStream_t s);
