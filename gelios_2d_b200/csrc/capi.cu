@@ -3,6 +3,7 @@
 // in step_kernels.cu.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <memory>
@@ -90,7 +91,7 @@ struct gelios_ctx {
     DBuf fA, fB, ftype, fmaster, fsosed, fcopy, fsdown;
     DBuf rtype, rM, rpstart, rpts, rkstart, rkeys, rs;
     DBuf lc, li, lo, sp_point, sp_line, sp_inc, sp_ainc, sp_fix;
-    DBuf u_slot, u_cell, u_twin, flux, aux;
+    DBuf u_slot, u_cell, u_twin, flux, aux, rec;
     DBuf Hn, Hu, Hv, HT, ku, kv, kT, r_istoch, cback, cnext;
     // state par[2] x 5 fields, centroids [2], scratch
     DBuf state[2];
@@ -349,6 +350,34 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
                 u_cell.push_back(c);
                 u_twin.push_back(twin);
             }
+        // group units of the same kind (plain interior, interior with a C_1
+        // side, tracked, one-sided) so that warps run one code path
+        {
+            const size_t nu = u_slot.size();
+            std::vector<int> cls(nu);
+            for (size_t u = 0; u < nu; u++) {
+                const int g = u_slot[u];
+                const int f = v->gran[g];
+                const int ta = v->point_type[v->face_A[f]], tb = v->point_type[v->face_B[f]];
+                const bool tracked = (ta == P_CONTACT && tb == P_CONTACT) || (ta == P_INNER_SHOCK && tb == P_INNER_SHOCK) ||
+                                     (ta == P_OUTER_SHOCK && tb == P_OUTER_SHOCK);
+                const bool c1 = v->cell_type[u_cell[u]] == C_1 ||
+                                (u_twin[u] >= 0 && v->cell_type[v->face_sosed[f]] == C_1);
+                cls[u] = tracked ? 2 : (u_twin[u] < 0 ? 3 : (c1 ? 1 : 0));
+            }
+            std::vector<size_t> order(nu);
+            for (size_t u = 0; u < nu; u++) order[u] = u;
+            std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return cls[a] < cls[b]; });
+            std::vector<int32_t> s2(nu), c2(nu), t2(nu);
+            for (size_t k = 0; k < nu; k++) {
+                s2[k] = u_slot[order[k]];
+                c2[k] = u_cell[order[k]];
+                t2[k] = u_twin[order[k]];
+            }
+            u_slot.swap(s2);
+            u_cell.swap(c2);
+            u_twin.swap(t2);
+        }
         // every interior twin must be covered by its main face's unit
         std::vector<char> covered(ng, 0);
         for (size_t u = 0; u < u_slot.size(); u++) {
@@ -468,6 +497,7 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     rc |= upload(ctx->u_twin, u_twin.data(), u_twin.size(), s);
     rc |= upload<double>(ctx->flux, nullptr, 5 * static_cast<size_t>(ng), s);
     rc |= upload<double>(ctx->aux, nullptr, 5 * static_cast<size_t>(nc), s);
+    rc |= upload<double>(ctx->rec, nullptr, 10 * u_slot.size(), s);
     rc |= upload(ctx->sp_point, sp_point.data(), sp_point.size(), s);
     rc |= upload(ctx->sp_line, sp_line.data(), sp_line.size(), s);
     rc |= upload(ctx->sp_inc, sp_inc.data(), sp_inc.size(), s);
@@ -693,21 +723,22 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_fork, s));
             GELIOS_CUDA_TRY(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
             launch_mk2_source(d, P, b, ctx->aux.as<double>(), ctx->side);
+            launch_mk2_recon(d, P, b, ctx->rec.as<double>(), ctx->side);
             GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_join, ctx->side));
             cudaEvent_t e1 = ctx->phase_begin();
             const int nm = launch_motion(d, P, b, ctx->surface.as<double>(), s);
             ctx->phase_end(2, e1, nm);  // Move_surface + rails
-            cudaEvent_t e3 = ctx->phase_begin();
-            launch_mk2_units(d, P, b, ctx->flux.as<double>(), s);
-            ctx->phase_end(1, e3, 1);
             GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_join, 0));
+            cudaEvent_t e3 = ctx->phase_begin();
+            launch_mk2_flux(d, P, b, ctx->rec.as<double>(), ctx->flux.as<double>(), s);
+            ctx->phase_end(1, e3, 1);
             cudaEvent_t e5 = ctx->phase_begin();
             launch_mk2_update(d, P, b, ctx->flux.as<double>(), ctx->aux.as<double>(), s);
             ctx->phase_end(3, e5, 1);
             cudaEvent_t e4 = ctx->phase_begin();
             launch_commit(d, b, s);
             ctx->phase_end(4, e4, 1);
-            launches += nm + 4;
+            launches += nm + 5;
         } else {
             b.cx = cen0;
             b.cy = cen0 + d.n_cells;

@@ -4,10 +4,9 @@
 //   surface_*_kernel Move_surface (Setka.cpp:3378-3844): tracked-face exact
 //                    Godunov speeds (one thread per face), then node velocities
 //                    replayed per node in the reference's operation order
-//   rail_*_kernel    Move_Setka_Calculate_2 (Setka.cpp:4324-4759): one CTA per
-//                    rail, A+B rails, then C rails, then D rails (the
-//                    reference's sequence; C_Rails[0] shares points with the
-//                    last B rail and overwrites them)
+//   rails_kernel     Move_Setka_Calculate_2 (Setka.cpp:4324-4759): one CTA per
+//                    rail; the points C_Rails[0] shares with the last B rail
+//                    and with the D rails keep the reference's pass order
 //   mk2_cell_kernel  per-cell flux accumulation in Grans order, charge-exchange
 //                    source, conservative ALE update, next-step centroid,
 //                    block-min of the CFL candidates
@@ -646,13 +645,19 @@ __device__ __forceinline__ St5 mk2_usualy_side(const double* const* st, const do
     return tvd_usualy(st, cx, cy, fx, fy, Ms, Mx, My, So, Sd, (mf & CF_AXIS) != 0, tracked, status);
 }
 
-template <typename TF>
-__global__ void __launch_bounds__(128) mk2_unit_kernel(DevMesh d, gelios_params P, StepBuffers b,
-                                                       double* __restrict__ fl) {
+// The MK2 face units in two kernels:
+//  * mk2_recon_kernel: the two reconstructed face states of every unit
+//    (Setka.cpp:10204-10276: TVD / radial TVD / boundary states).  They use
+//    the points before the motion only, so this kernel runs on the side
+//    stream while surface tracking and the rails move the grid;
+//  * mk2_flux_kernel: face speed W from the moved points, HLL / HLLC, exact
+//    Godunov on tracked faces (Setka.cpp:10198-10209, 10335-10380), slot
+//    fluxes and CFL candidates.
+// rec rows: ro, p, u, v, Q of the owner side, then of the other side.
+__global__ void __launch_bounds__(128) mk2_recon_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                        double* __restrict__ rec) {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
-    double tmin_u = __longlong_as_double(0x7ff0000000000000LL);
     int status = 0;
-    const size_t ng = d.n_slots;
     if (u < d.n_units) {
         const int g = d.u_slot[u], K = d.u_cell[u], gt = d.u_twin[u];
         const double x = b.cx[K], y = b.cy[K];
@@ -666,30 +671,19 @@ __global__ void __launch_bounds__(128) mk2_unit_kernel(DevMesh d, gelios_params 
             procN = !(sqrt(sq(x3) + sq(y3)) < P.R11);
         }
         if (procK || procN) {
-            const double dt = *b.dt_cur;
             const uint32_t info = d.sinfo[g];
             const int ft = info & SI_TYPE_MASK;
             const uint32_t cf = d.cflags[K];
             const int A = d.sA[g], B = d.sB[g];
             const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
-            const double S = sqrt(sq(xb - xa) + sq(yb - ya)) * (ya + yb) * 0.5;
             const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
-            const double x4 = (d.X2[A] + d.X2[B]) / 2.0, y4 = (d.Y2[A] + d.Y2[B]) / 2.0;
-            const double dist = sqrt(sq(x - x2) + sq(y - y2));
             const double g2 = 2 * P.gamma;
             const St5 par1 = load_state(b.cur, K);
             St5 par11 = par1;
             St5 par2 = get_par(P, ft, par1, b.cur, nb, x2, y2);
-            double t1 = xb - xa, t2 = yb - ya;
-            const double nn = sqrt(sq(t1) + sq(t2));
-            t1 = t1 / nn;
-            t2 = t2 / nn;
-            const double n1 = t2, n2 = -t1;
-            const double W = ((x4 - x2) * n1 + (y4 - y2) * n2) / dt;
             const double dis = sqrt(sq(x2) + sq(y2));
             const bool tracked = (info & SI_GOD) != 0;
             const uint32_t nbf = nb >= 0 ? d.cflags[nb] : 0u;
-            // |face centre|^(2 gamma), needed only by the radial forms
             const bool radial = ((cf & CF_C1) && (ft == G_USUALY || ft == G_AXIS)) || ft == G_INNER_SPHERE ||
                                 (ft == G_USUALY && (nbf & CF_C1));
             const double pdis = radial ? pow2g(dis, g2) : 1.0;
@@ -716,6 +710,69 @@ __global__ void __launch_bounds__(128) mk2_unit_kernel(DevMesh d, gelios_params 
                 par2 = par11;
                 par2.v = -par2.v;
             }
+            const size_t n = d.n_units;
+            rec[0 * n + u] = par11.ro;
+            rec[1 * n + u] = par11.p;
+            rec[2 * n + u] = par11.u;
+            rec[3 * n + u] = par11.v;
+            rec[4 * n + u] = par11.Q;
+            rec[5 * n + u] = par2.ro;
+            rec[6 * n + u] = par2.p;
+            rec[7 * n + u] = par2.u;
+            rec[8 * n + u] = par2.v;
+            rec[9 * n + u] = par2.Q;
+        }
+    }
+    if (status) atomicOr(b.status, status);
+}
+
+template <typename TF>
+__global__ void __launch_bounds__(128) mk2_flux_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                       const double* __restrict__ rec, double* __restrict__ fl) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    double tmin_u = __longlong_as_double(0x7ff0000000000000LL);
+    int status = 0;
+    const size_t ng = d.n_slots;
+    if (u < d.n_units) {
+        const int g = d.u_slot[u], K = d.u_cell[u], gt = d.u_twin[u];
+        const double x = b.cx[K], y = b.cy[K];
+        const bool procK = !(sqrt(sq(x) + sq(y)) < P.R11);
+        const int nb = gt >= 0 ? d.snb[g] : -1;
+        double x3 = 0.0, y3 = 0.0;
+        bool procN = false;
+        if (nb >= 0) {
+            x3 = b.cx[nb];
+            y3 = b.cy[nb];
+            procN = !(sqrt(sq(x3) + sq(y3)) < P.R11);
+        }
+        if (procK || procN) {
+            const double dt = *b.dt_cur;
+            const uint32_t info = d.sinfo[g];
+            const int A = d.sA[g], B = d.sB[g];
+            const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
+            const double S = sqrt(sq(xb - xa) + sq(yb - ya)) * (ya + yb) * 0.5;
+            const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
+            const double x4 = (d.X2[A] + d.X2[B]) / 2.0, y4 = (d.Y2[A] + d.Y2[B]) / 2.0;
+            const double dist = sqrt(sq(x - x2) + sq(y - y2));
+            double t1 = xb - xa, t2 = yb - ya;
+            const double nn = sqrt(sq(t1) + sq(t2));
+            t1 = t1 / nn;
+            t2 = t2 / nn;
+            const double n1 = t2, n2 = -t1;
+            const double W = ((x4 - x2) * n1 + (y4 - y2) * n2) / dt;
+            const size_t n = d.n_units;
+            St5 par11, par2;
+            par11.ro = rec[0 * n + u];
+            par11.p = rec[1 * n + u];
+            par11.u = rec[2 * n + u];
+            par11.v = rec[3 * n + u];
+            par11.Q = rec[4 * n + u];
+            par2.ro = rec[5 * n + u];
+            par2.p = rec[6 * n + u];
+            par2.u = rec[7 * n + u];
+            par2.v = rec[8 * n + u];
+            par2.Q = rec[9 * n + u];
+            const bool tracked = (info & SI_GOD) != 0;
             const bool np = (info & SI_NP) != 0;
             FluxOut<double> F;
             const double UU = hllc_flux<TF>(P.gamma, P.kurant, par11, par2, W, n1, n2, 1.0, 0, np, F);
@@ -1000,202 +1057,195 @@ __global__ void commit_kernel(DevMesh d, StepBuffers b) {
 }
 
 // ------------------------------------------------------------------ grid motion
-// Move_Setka_Calculate_2, A and B rails (Setka.cpp:4331-4595): one CTA per rail.
-__global__ void rail_ab_kernel(DevMesh d, gelios_params P, const double* __restrict__ dtp, int first_rail,
-                               int n_rails) {
-    const int q = first_rail + blockIdx.x;
-    if (blockIdx.x >= n_rails) return;
-    const double dt = *dtp;
-    const int32_t* ap = d.rpts + d.rpstart[q];
-    const int32_t* kp = d.rkeys + d.rkstart[q];
-    const int M1 = d.rM[4 * q], M2 = d.rM[4 * q + 1], M3 = d.rM[4 * q + 2], M4 = d.rM[4 * q + 3];
-    const double s = d.rs[q];
-    const int t = d.rtype[q];
-    double* X = d.X;
-    double* Y = d.Y;
-    double* X2 = d.X2;
-    double* Y2 = d.Y2;
-    __shared__ double sh[4];  // R2, R3, R4, x2 of key point 0
-    const double cs = cos(s), sn = sin(s);
-    if (threadIdx.x == 0) {
-        if (t == 0) {  // A rail
-            for (int kk = 0; kk < 3; kk++) {
-                const int K = kp[kk];
-                const double V = d.Vx[K] * cs + d.Vy[K] * sn;
-                X2[K] = X[K] + dt * V * cs;
-                Y2[K] = Y[K] + dt * V * sn;
-            }
-            X2[kp[3]] = X[kp[3]];
-            Y2[kp[3]] = Y[kp[3]];
-            sh[0] = sqrt(sq(X2[kp[0]]) + sq(Y2[kp[0]]));
-            sh[1] = sqrt(sq(X2[kp[1]]) + sq(Y2[kp[1]]));
-            sh[2] = sqrt(sq(X2[kp[2]]) + sq(Y2[kp[2]]));
-        } else {  // B rail
-            const int K0 = kp[0], K1 = kp[1], K2 = kp[2], K3 = kp[3];
-            double V = d.Vx[K0] * cs + d.Vy[K0] * sn;
-            X2[K0] = X[K0] + dt * V * cs;
-            Y2[K0] = Y[K0] + dt * V * sn;
-            V = d.Vx[K1] * 0.0 + d.Vy[K1] * 1.0;
-            X2[K1] = X2[K0];
-            Y2[K1] = Y[K1] + dt * V;
-            V = d.Vx[K2] * 0.0 + d.Vy[K2] * 1.0;
-            X2[K2] = X2[K0];
-            Y2[K2] = Y[K2] + dt * V;
-            X2[K3] = X2[K0];
-            Y2[K3] = Y[K3];
-            sh[0] = sqrt(sq(X2[K0]) + sq(Y2[K0]));
-            sh[1] = Y2[K1];
-            sh[2] = Y2[K2];
-            sh[3] = X2[K0];
-        }
-    }
-    __syncthreads();
-    const int ni = P.n_inner;
-    const double R2 = sh[0];
-    for (int j = threadIdx.x; j < M1 - 1; j += blockDim.x) {
-        double r;
-        if (j < ni) {
-            const double x = j * 1.0 / (ni);
-            r = P.R1 + pow(x, 1.3) * (P.R111 - P.R1);
-        } else {
-            const double x = (j - ni) * 1.0 / (M1 - 1 - ni);
-            r = P.R111 + pow(x, 1.05) * (R2 - P.R111);
-        }
-        X2[ap[j]] = r * cs;
-        Y2[ap[j]] = r * sn;
-    }
-    if (t == 0) {
-        const double R3 = sh[1], R4 = sh[2];
-        for (int j = threadIdx.x; j < M2 - 1; j += blockDim.x) {
-            const double r = R2 + (R3 - R2) * (j + 1) / (M2);
-            X2[ap[M1 + j]] = r * cs;
-            Y2[ap[M1 + j]] = r * sn;
-        }
-        for (int j = threadIdx.x; j < M3 - 1; j += blockDim.x) {
-            const double r = R3 + (R4 - R3) * (j + 1) / (M3);
-            X2[ap[M1 + M2 + j]] = r * cs;
-            Y2[ap[M1 + M2 + j]] = r * sn;
-        }
-        const double dd = 1.5708 / sqrt(1.0 - 1.0 / 1.76);
-        const double e = 1.76 * (1.0 - sq(s / dd));
-        for (int j = threadIdx.x; j < M4; j += blockDim.x) {
-            const double x = (j + 1) * 1.0 / (M4);
-            const double r = R4 + pow(x, e) * (P.R5 - R4);
-            X2[ap[M1 + M2 + M3 + j]] = r * cs;
-            Y2[ap[M1 + M2 + M3 + j]] = r * sn;
-        }
-    } else {
-        const double R2y = Y2[kp[0]];
-        const double R3 = sh[1], R4 = sh[2], xk = sh[3];
-        for (int j = threadIdx.x; j < M2 - 1; j += blockDim.x) {
-            X2[ap[M1 + j]] = xk;
-            Y2[ap[M1 + j]] = R2y + (R3 - R2y) * (j + 1) / (M2);
-        }
-        for (int j = threadIdx.x; j < M3 - 1; j += blockDim.x) {
-            X2[ap[M1 + M2 + j]] = xk;
-            Y2[ap[M1 + M2 + j]] = R3 + (R4 - R3) * (j + 1) / (M3);
-        }
-        for (int j = threadIdx.x; j < M4; j += blockDim.x) {
-            X2[ap[M1 + M2 + M3 + j]] = xk;
-            Y2[ap[M1 + M2 + M3 + j]] = R4 + (P.R5 - R4) * (j + 1) / (M4);
-        }
-    }
+// Move_Setka_Calculate_2 (Setka.cpp:4324-4759) in one launch, one CTA per
+// rail.  The reference moves the A rails, then the B rails, then the C rails,
+// then the D rails, and two of them share points:
+//  * C_Rails[0] starts with the first M1 points of the last B rail and
+//    overwrites them (with its own angle), so the last B rail leaves those
+//    points to C_Rails[0] and uses its own value of its key point 0 for the
+//    points above it, as the reference's B pass does;
+//  * the first point of every D rail is a point of C_Rails[0]; the D block
+//    recomputes that point's new position from C_Rails[0]'s key point with
+//    the same operations (bit-identical to reading it back).
+__device__ __forceinline__ void c0_key(const DevMesh& d, int q, double dt, double& x2, double& y2) {
+    const int K0 = d.rkeys[d.rkstart[q]];
+    const double s = d.rs[q], cs = cos(s), sn = sin(s);
+    const double V = d.Vx[K0] * cs + d.Vy[K0] * sn;
+    x2 = d.X[K0] + dt * V * cs;
+    y2 = d.Y[K0] + dt * V * sn;
 }
 
-// C rails (Setka.cpp:4597-4674).
-__global__ void rail_c_kernel(DevMesh d, gelios_params P, const double* __restrict__ dtp, int first_rail,
-                              int n_rails) {
-    const int q = first_rail + blockIdx.x;
-    if (blockIdx.x >= n_rails) return;
+__global__ void __launch_bounds__(128) rails_kernel(DevMesh d, gelios_params P, const double* __restrict__ dtp) {
+    const int q = blockIdx.x;
     const double dt = *dtp;
     const int32_t* ap = d.rpts + d.rpstart[q];
     const int np = d.rpstart[q + 1] - d.rpstart[q];
     const int32_t* kp = d.rkeys + d.rkstart[q];
-    const int M1 = d.rM[4 * q], M2 = d.rM[4 * q + 1];
-    const double s = d.rs[q];
-    const double cs = cos(s), sn = sin(s);
-    __shared__ double sh[3];
-    if (threadIdx.x == 0) {
-        const int K0 = kp[0], K1 = kp[1];
-        const double V = d.Vx[K0] * cs + d.Vy[K0] * sn;
-        d.X2[K0] = d.X[K0] + dt * V * cs;
-        d.Y2[K0] = d.Y[K0] + dt * V * sn;
-        d.X2[K1] = P.Left;
-        d.Y2[K1] = d.Y[K1];
-        sh[0] = sqrt(sq(d.X2[K0]) + sq(d.Y2[K0]));
-        sh[1] = d.X2[K0];
-        sh[2] = d.Y2[K0];
-    }
-    __syncthreads();
+    const int M1 = d.rM[4 * q], M2 = d.rM[4 * q + 1], M3 = d.rM[4 * q + 2], M4 = d.rM[4 * q + 3];
+    const int t = d.rtype[q];
+    const int first_c = d.n_rail_a + d.n_rail_b, first_d = first_c + d.n_rail_c;
+    // the last B rail hands its first M1 points to C_Rails[0]
+    const bool handoff = (t == 1) && (q == first_c - 1) && d.n_rail_c > 0;
+    double* X2 = d.X2;
+    double* Y2 = d.Y2;
+    const double* X = d.X;
+    const double* Y = d.Y;
+    __shared__ double sh[6];
     const int ni = P.n_inner;
-    const double R2 = sh[0];
-    for (int j = threadIdx.x; j < M1 - 1; j += blockDim.x) {
-        double r;
-        if (j < ni) {
-            const double x = j * 1.0 / (ni);
-            r = P.R1 + pow(x, 1.3) * (P.R111 - P.R1);
-        } else {
-            const double x = (j - ni) * 1.0 / (M1 - 1 - ni);
-            r = P.R111 + pow(x, 1.05) * (R2 - P.R111);
+    if (t == 0 || t == 1 || t == 2) {
+        const double s = d.rs[q];
+        const double cs = cos(s), sn = sin(s);
+        if (threadIdx.x == 0) {
+            if (t == 0) {  // A rail, Setka.cpp:4331-4356
+                for (int kk = 0; kk < 3; kk++) {
+                    const int K = kp[kk];
+                    const double V = d.Vx[K] * cs + d.Vy[K] * sn;
+                    X2[K] = X[K] + dt * V * cs;
+                    Y2[K] = Y[K] + dt * V * sn;
+                }
+                X2[kp[3]] = X[kp[3]];
+                Y2[kp[3]] = Y[kp[3]];
+                sh[0] = sqrt(sq(X2[kp[0]]) + sq(Y2[kp[0]]));
+                sh[1] = sqrt(sq(X2[kp[1]]) + sq(Y2[kp[1]]));
+                sh[2] = sqrt(sq(X2[kp[2]]) + sq(Y2[kp[2]]));
+            } else if (t == 1) {  // B rail, Setka.cpp:4469-4502
+                const int K0 = kp[0], K1 = kp[1], K2 = kp[2], K3 = kp[3];
+                double V = d.Vx[K0] * cs + d.Vy[K0] * sn;
+                const double x0 = X[K0] + dt * V * cs, y0 = Y[K0] + dt * V * sn;
+                if (!handoff) {
+                    X2[K0] = x0;
+                    Y2[K0] = y0;
+                }
+                V = d.Vx[K1] * 0.0 + d.Vy[K1] * 1.0;
+                X2[K1] = x0;
+                Y2[K1] = Y[K1] + dt * V;
+                V = d.Vx[K2] * 0.0 + d.Vy[K2] * 1.0;
+                X2[K2] = x0;
+                Y2[K2] = Y[K2] + dt * V;
+                X2[K3] = x0;
+                Y2[K3] = Y[K3];
+                sh[0] = sqrt(sq(x0) + sq(y0));
+                sh[1] = Y2[K1];
+                sh[2] = Y2[K2];
+                sh[3] = x0;
+                sh[4] = y0;
+            } else {  // C rail, Setka.cpp:4603-4614
+                const int K0 = kp[0], K1 = kp[1];
+                const double V = d.Vx[K0] * cs + d.Vy[K0] * sn;
+                X2[K0] = X[K0] + dt * V * cs;
+                Y2[K0] = Y[K0] + dt * V * sn;
+                X2[K1] = P.Left;
+                Y2[K1] = Y[K1];
+                sh[0] = sqrt(sq(X2[K0]) + sq(Y2[K0]));
+                sh[3] = X2[K0];
+                sh[4] = Y2[K0];
+            }
         }
-        d.X2[ap[j]] = r * cs;
-        d.Y2[ap[j]] = r * sn;
+        __syncthreads();
+        const double R2 = sh[0];
+        if (!handoff) {  // inner layer, Setka.cpp:4390-4406 (and 4532-4548, 4644-4660)
+            for (int j = threadIdx.x; j < M1 - 1; j += blockDim.x) {
+                double r;
+                if (j < ni) {
+                    const double x = j * 1.0 / (ni);
+                    r = P.R1 + pow(x, 1.3) * (P.R111 - P.R1);
+                } else {
+                    const double x = (j - ni) * 1.0 / (M1 - 1 - ni);
+                    r = P.R111 + pow(x, 1.05) * (R2 - P.R111);
+                }
+                X2[ap[j]] = r * cs;
+                Y2[ap[j]] = r * sn;
+            }
+        }
+        if (t == 0) {  // Setka.cpp:4411-4456
+            const double R3 = sh[1], R4 = sh[2];
+            for (int j = threadIdx.x; j < M2 - 1; j += blockDim.x) {
+                const double r = R2 + (R3 - R2) * (j + 1) / (M2);
+                X2[ap[M1 + j]] = r * cs;
+                Y2[ap[M1 + j]] = r * sn;
+            }
+            for (int j = threadIdx.x; j < M3 - 1; j += blockDim.x) {
+                const double r = R3 + (R4 - R3) * (j + 1) / (M3);
+                X2[ap[M1 + M2 + j]] = r * cs;
+                Y2[ap[M1 + M2 + j]] = r * sn;
+            }
+            const double dd = 1.5708 / sqrt(1.0 - 1.0 / 1.76);
+            const double e = 1.76 * (1.0 - sq(s / dd));
+            for (int j = threadIdx.x; j < M4; j += blockDim.x) {
+                const double x = (j + 1) * 1.0 / (M4);
+                const double r = R4 + pow(x, e) * (P.R5 - R4);
+                X2[ap[M1 + M2 + M3 + j]] = r * cs;
+                Y2[ap[M1 + M2 + M3 + j]] = r * sn;
+            }
+        } else if (t == 1) {  // Setka.cpp:4552-4593
+            const double R2y = sh[4], R3 = sh[1], R4 = sh[2], xk = sh[3];
+            for (int j = threadIdx.x; j < M2 - 1; j += blockDim.x) {
+                X2[ap[M1 + j]] = xk;
+                Y2[ap[M1 + j]] = R2y + (R3 - R2y) * (j + 1) / (M2);
+            }
+            for (int j = threadIdx.x; j < M3 - 1; j += blockDim.x) {
+                X2[ap[M1 + M2 + j]] = xk;
+                Y2[ap[M1 + M2 + j]] = R3 + (R4 - R3) * (j + 1) / (M3);
+            }
+            for (int j = threadIdx.x; j < M4; j += blockDim.x) {
+                X2[ap[M1 + M2 + M3 + j]] = xk;
+                Y2[ap[M1 + M2 + M3 + j]] = R4 + (P.R5 - R4) * (j + 1) / (M4);
+            }
+        } else {  // Setka.cpp:4662-4673
+            const double R2x = sh[3], yk = sh[4];
+            const double x = pow(P.Left / (R2x), 1.0 / (M2));
+            for (int j = M1 + threadIdx.x; j < np; j += blockDim.x) {
+                X2[ap[j]] = R2x * pow(x, static_cast<double>(j + 1 - M1));
+                Y2[ap[j]] = yk;
+            }
+        }
+        return;
     }
-    const double R2x = sh[1], R3x = P.Left, yk = sh[2];
-    const double x = pow(R3x / (R2x), 1.0 / (M2));
-    for (int j = M1 + threadIdx.x; j < np; j += blockDim.x) {
-        d.X2[ap[j]] = R2x * pow(x, static_cast<double>(j + 1 - M1));
-        d.Y2[ap[j]] = yk;
-    }
-}
-
-// D rails (Setka.cpp:4676-4758); rail jj >= n_outer_shock copies the outer
-// shock height of rail jj-1, i.e. of rail n_outer_shock-1.
-__global__ void rail_d_kernel(DevMesh d, gelios_params P, const double* __restrict__ dtp, int first_rail,
-                              int n_rails) {
-    const int jj = blockIdx.x;
-    if (jj >= n_rails) return;
-    const int q = first_rail + jj;
-    const double dt = *dtp;
-    const int32_t* ap = d.rpts + d.rpstart[q];
-    const int32_t* kp = d.rkeys + d.rkstart[q];
-    const int M2 = d.rM[4 * q + 1], M3 = d.rM[4 * q + 2], M4 = d.rM[4 * q + 3];
+    // D rail, Setka.cpp:4676-4758
+    const int jj = q - first_d;
     const int sM2 = d.dims[5], sM3 = d.dims[6], sM4 = d.dims[7];
-    __shared__ double sh[4];
     if (threadIdx.x == 0) {
-        const int K0 = kp[0], K1 = kp[1], K2 = kp[2], K3 = kp[3];
+        const int K1 = kp[1], K2 = kp[2], K3 = kp[3];
+        // key point 0 = point M1 + jj of C_Rails[0], as the C pass moves it
+        double c0x, c0y;
+        c0_key(d, first_c, dt, c0x, c0y);
+        const int Mc1 = d.rM[4 * first_c], Mc2 = d.rM[4 * first_c + 1];
+        const int j = Mc1 + jj;
+        const double xr = pow(P.Left / (c0x), 1.0 / (Mc2));
+        const double x0 = c0x * pow(xr, static_cast<double>(j + 1 - Mc1));
+        const double y0 = c0y;
         double V = d.Vy[K1];
-        d.X2[K1] = d.X2[K0];
-        d.Y2[K1] = d.Y[K1] + dt * V;
+        X2[K1] = x0;
+        Y2[K1] = Y[K1] + dt * V;
         V = d.Vy[K2];
-        d.X2[K2] = d.X2[K0];
+        X2[K2] = x0;
         if (jj >= P.n_outer_shock && P.n_outer_shock >= 1) {
-            const int qs = first_rail + P.n_outer_shock - 1;
+            const int qs = first_d + P.n_outer_shock - 1;
             const int Ks = d.rkeys[d.rkstart[qs] + 2];
-            d.Y2[K2] = d.Y[Ks] + dt * d.Vy[Ks];
+            Y2[K2] = Y[Ks] + dt * d.Vy[Ks];
         } else {
-            d.Y2[K2] = d.Y[K2] + dt * V;
+            Y2[K2] = Y[K2] + dt * V;
         }
-        d.X2[K3] = d.X2[K0];
-        d.Y2[K3] = d.Y[K3];
-        sh[0] = d.Y2[K0];
-        sh[1] = d.Y2[K1];
-        sh[2] = d.Y2[K2];
-        sh[3] = d.X2[K0];
+        X2[K3] = x0;
+        Y2[K3] = Y[K3];
+        sh[0] = y0;
+        sh[1] = Y2[K1];
+        sh[2] = Y2[K2];
+        sh[3] = x0;
     }
     __syncthreads();
     const double R2 = sh[0], R3 = sh[1], R4 = sh[2], xk = sh[3];
     for (int j = threadIdx.x; j < sM2 - 1; j += blockDim.x) {
-        d.X2[ap[j + 1]] = xk;
-        d.Y2[ap[j + 1]] = R2 + (R3 - R2) * (j + 1) / (M2);
+        X2[ap[j + 1]] = xk;
+        Y2[ap[j + 1]] = R2 + (R3 - R2) * (j + 1) / (M2);
     }
     for (int j = threadIdx.x; j < sM3 - 1; j += blockDim.x) {
-        d.X2[ap[sM2 + j + 1]] = xk;
-        d.Y2[ap[sM2 + j + 1]] = R3 + (R4 - R3) * (j + 1) / (M3);
+        X2[ap[sM2 + j + 1]] = xk;
+        Y2[ap[sM2 + j + 1]] = R3 + (R4 - R3) * (j + 1) / (M3);
     }
     for (int j = threadIdx.x; j < sM4; j += blockDim.x) {
-        d.X2[ap[sM2 + sM3 + j + 1]] = xk;
-        d.Y2[ap[sM2 + sM3 + j + 1]] = R4 + (P.R5 - R4) * (j + 1) / (M4);
+        X2[ap[sM2 + sM3 + j + 1]] = xk;
+        Y2[ap[sM2 + sM3 + j + 1]] = R4 + (P.R5 - R4) * (j + 1) / (M4);
     }
 }
 
@@ -1480,11 +1530,15 @@ void launch_stationary_update(const DevMesh& d, const gelios_params& P, const St
                               cudaStream_t s) {
     stationary_update_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, fl);
 }
-void launch_mk2_units(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl, cudaStream_t s) {
+void launch_mk2_recon(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* rec, cudaStream_t s) {
+    mk2_recon_kernel<<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, b, rec);
+}
+void launch_mk2_flux(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec, double* fl,
+                     cudaStream_t s) {
     if (P.precision == GELIOS_PREC_FP32_FLUX)
-        mk2_unit_kernel<float><<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, b, fl);
+        mk2_flux_kernel<float><<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, b, rec, fl);
     else
-        mk2_unit_kernel<double><<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, b, fl);
+        mk2_flux_kernel<double><<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, b, rec, fl);
 }
 void launch_mk2_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
                        const double* aux, cudaStream_t s) {
@@ -1520,16 +1574,9 @@ int launch_motion(const DevMesh& d, const gelios_params& P, const StepBuffers& b
         surface_nodes_kernel<<<1, 512, shm, s>>>(d, b, scratch);
         launches += 2;
     }
-    if (d.n_rail_a + d.n_rail_b > 0) {
-        rail_ab_kernel<<<d.n_rail_a + d.n_rail_b, 128, 0, s>>>(d, P, b.dt_cur, 0, d.n_rail_a + d.n_rail_b);
-        launches++;
-    }
-    if (d.n_rail_c > 0) {
-        rail_c_kernel<<<d.n_rail_c, 128, 0, s>>>(d, P, b.dt_cur, d.n_rail_a + d.n_rail_b, d.n_rail_c);
-        launches++;
-    }
-    if (d.n_rail_d > 0) {
-        rail_d_kernel<<<d.n_rail_d, 128, 0, s>>>(d, P, b.dt_cur, d.n_rail_a + d.n_rail_b + d.n_rail_c, d.n_rail_d);
+    const int nr = d.n_rail_a + d.n_rail_b + d.n_rail_c + d.n_rail_d;
+    if (nr > 0) {
+        rails_kernel<<<nr, 128, 0, s>>>(d, P, b.dt_cur);
         launches++;
     }
     return launches;

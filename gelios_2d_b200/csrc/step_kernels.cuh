@@ -77,7 +77,9 @@ void launch_stationary_units(const DevMesh& d, const gelios_params& P, const Ste
                              cudaStream_t s);
 void launch_stationary_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
                               cudaStream_t s);
-void launch_mk2_units(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl, cudaStream_t s);
+void launch_mk2_recon(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* rec, cudaStream_t s);
+void launch_mk2_flux(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec, double* fl,
+                     cudaStream_t s);
 void launch_mk2_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
                        const double* aux, cudaStream_t s);
 void launch_mk2_source(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* aux, cudaStream_t s);
