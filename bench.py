@@ -295,8 +295,7 @@ def main():
     for _ in range(e2e_steps):
         S.set_par(0, host_in)
         S.step_async(fcode, 1)
-        res = S.par(1)
-        host_out[...] = res
+        S.par(1, out=host_out)
     e2e_s = time.perf_counter() - t0
     e2e_value = world * counted * e2e_steps / e2e_s
     if dist:

@@ -101,6 +101,7 @@ struct gelios_ctx {
     DBuf inner;
     int n_inner = 0;
     int n_sp = 0;
+    bool cen_valid = false;  // cen[0] holds the centroids of the current points
     int64_t launches = 0;
     // phase timing
     bool timing = false;
@@ -220,6 +221,7 @@ extern "C" int gelios_create(gelios_ctx** out, const gelios_params* prm, int dev
 extern "C" int gelios_set_params(gelios_ctx* ctx, const gelios_params* prm) {
     if (!ctx || !prm) return GELIOS_E_ARG;
     ctx->prm = *prm;
+    ctx->cen_valid = false;  // the cached |centroid|^(2 gamma) depends on gamma
     return GELIOS_OK;
 }
 
@@ -329,6 +331,7 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     // face units: every slot of a cell except the twins of interior faces,
     // whose flux comes from the unit of the main face (see step_kernels.cu)
     std::vector<int32_t> u_slot, u_cell, u_twin;
+    int u_tr0 = 0, u_tr1 = 0;
     {
         std::vector<int32_t> slot_of_face(nf, -1);
         for (int c = 0; c < nc; c++)
@@ -377,6 +380,10 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
             u_slot.swap(s2);
             u_cell.swap(c2);
             u_twin.swap(t2);
+            u_tr0 = 0;
+            while (u_tr0 < static_cast<int>(nu) && cls[order[u_tr0]] < 2) u_tr0++;
+            u_tr1 = u_tr0;
+            while (u_tr1 < static_cast<int>(nu) && cls[order[u_tr1]] == 2) u_tr1++;
         }
         // every interior twin must be covered by its main face's unit
         std::vector<char> covered(ng, 0);
@@ -551,6 +558,8 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     d.u_slot = ctx->u_slot.as<int32_t>();
     d.u_cell = ctx->u_cell.as<int32_t>();
     d.u_twin = ctx->u_twin.as<int32_t>();
+    d.u_tr0 = u_tr0;
+    d.u_tr1 = u_tr1;
     d.fA = ctx->fA.as<int32_t>();
     d.fB = ctx->fB.as<int32_t>();
     d.ftype = ctx->ftype.as<int32_t>();
@@ -593,6 +602,7 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     d.cnext = ctx->cnext.as<int32_t>();
     ctx->have_mesh = true;
     ctx->n_inner = 0;
+    ctx->cen_valid = false;
     return GELIOS_OK;
 }
 
@@ -692,12 +702,12 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
     double* cen0 = ctx->cen[0].as<double>();
     double* cen1 = ctx->cen[1].as<double>();
     if (ctx->ev_used > 4096) ctx->collect();
-    {
+    if (!ctx->cen_valid) {
         cudaEvent_t e0 = ctx->phase_begin();
         launch_centroid(d, d.X, d.Y, cen0, cen0 + d.n_cells, cen0 + 2 * static_cast<size_t>(d.n_cells), P.gamma, s);
         ctx->phase_end(0, e0, 1);
+        launches++;
     }
-    launches++;
     for (int st = 0; st < nsteps; st++) {
         const int cur = st & 1, nxt = cur ^ 1;
         StepBuffers b;
@@ -730,15 +740,15 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             ctx->phase_end(2, e1, nm);  // Move_surface + rails
             GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_join, 0));
             cudaEvent_t e3 = ctx->phase_begin();
-            launch_mk2_flux(d, P, b, ctx->rec.as<double>(), ctx->flux.as<double>(), s);
-            ctx->phase_end(1, e3, 1);
+            const int nfl = launch_mk2_flux(d, P, b, ctx->rec.as<double>(), ctx->flux.as<double>(), s);
+            ctx->phase_end(1, e3, nfl);
             cudaEvent_t e5 = ctx->phase_begin();
             launch_mk2_update(d, P, b, ctx->flux.as<double>(), ctx->aux.as<double>(), s);
             ctx->phase_end(3, e5, 1);
             cudaEvent_t e4 = ctx->phase_begin();
             launch_commit(d, b, s);
             ctx->phase_end(4, e4, 1);
-            launches += nm + 5;
+            launches += nm + 4 + nfl;
         } else {
             b.cx = cen0;
             b.cy = cen0 + d.n_cells;
@@ -765,6 +775,10 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
     }
     GELIOS_CUDA_TRY(cudaGetLastError());
     ctx->launches = launches;
+    // centroids of the current points: after an odd number of moving-grid
+    // steps they sit in the second buffer; swap so cen[0] holds them
+    if (form == GELIOS_FORM_MK2 && (nsteps & 1)) std::swap(ctx->cen[0].p, ctx->cen[1].p);
+    ctx->cen_valid = true;
     if (status) {
         Words r{};
         GELIOS_CUDA_TRY(cudaMemcpyAsync(&r, ctx->words.p, sizeof(r), cudaMemcpyDeviceToHost, s));

@@ -726,14 +726,19 @@ __global__ void __launch_bounds__(128) mk2_recon_kernel(DevMesh d, gelios_params
     if (status) atomicOr(b.status, status);
 }
 
-template <typename TF>
+// Units are grouped by kind with the tracked ones in [u_tr0, u_tr1): the
+// kernel without the exact Godunov solver covers the rest (index i is
+// remapped around the tracked range), a second launch covers that range.
+template <typename TF, bool TRACKED>
 __global__ void __launch_bounds__(128) mk2_flux_kernel(DevMesh d, gelios_params P, StepBuffers b,
-                                                       const double* __restrict__ rec, double* __restrict__ fl) {
-    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+                                                       const double* __restrict__ rec, double* __restrict__ fl,
+                                                       int n_launch) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double tmin_u = __longlong_as_double(0x7ff0000000000000LL);
     int status = 0;
     const size_t ng = d.n_slots;
-    if (u < d.n_units) {
+    const int u = TRACKED ? d.u_tr0 + i : (i < d.u_tr0 ? i : i + (d.u_tr1 - d.u_tr0));
+    if (i < n_launch) {
         const int g = d.u_slot[u], K = d.u_cell[u], gt = d.u_twin[u];
         const double x = b.cx[K], y = b.cy[K];
         const bool procK = !(sqrt(sq(x) + sq(y)) < P.R11);
@@ -772,13 +777,13 @@ __global__ void __launch_bounds__(128) mk2_flux_kernel(DevMesh d, gelios_params 
             par2.u = rec[7 * n + u];
             par2.v = rec[8 * n + u];
             par2.Q = rec[9 * n + u];
-            const bool tracked = (info & SI_GOD) != 0;
+            const bool tracked = TRACKED;
             const bool np = (info & SI_NP) != 0;
             FluxOut<double> F;
             const double UU = hllc_flux<TF>(P.gamma, P.kurant, par11, par2, W, n1, n2, 1.0, 0, np, F);
             double fm0 = F.P0 * S, fm1 = F.P1 * S, fm2 = F.P2 * S, fm3 = F.P3 * S;
             double UG = 1.0;
-            if (tracked) {
+            if (TRACKED) {
                 double q1[5] = {par11.ro, par11.p, par11.u, par11.v, 0.0};
                 double q2[5] = {par2.ro, par2.p, par2.u, par2.v, 0.0};
                 double nv[3] = {n1, n2, 0.0};
@@ -1533,12 +1538,25 @@ void launch_stationary_update(const DevMesh& d, const gelios_params& P, const St
 void launch_mk2_recon(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* rec, cudaStream_t s) {
     mk2_recon_kernel<<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, b, rec);
 }
-void launch_mk2_flux(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec, double* fl,
-                     cudaStream_t s) {
-    if (P.precision == GELIOS_PREC_FP32_FLUX)
-        mk2_flux_kernel<float><<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, b, rec, fl);
-    else
-        mk2_flux_kernel<double><<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, b, rec, fl);
+int launch_mk2_flux(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec, double* fl,
+                    cudaStream_t s) {
+    const int nt = d.u_tr1 - d.u_tr0, nr = d.n_units - nt;
+    int launches = 0;
+    if (nr > 0) {
+        if (P.precision == GELIOS_PREC_FP32_FLUX)
+            mk2_flux_kernel<float, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, b, rec, fl, nr);
+        else
+            mk2_flux_kernel<double, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, b, rec, fl, nr);
+        launches++;
+    }
+    if (nt > 0) {
+        if (P.precision == GELIOS_PREC_FP32_FLUX)
+            mk2_flux_kernel<float, true><<<blocks_for(nt, 128), 128, 0, s>>>(d, P, b, rec, fl, nt);
+        else
+            mk2_flux_kernel<double, true><<<blocks_for(nt, 128), 128, 0, s>>>(d, P, b, rec, fl, nt);
+        launches++;
+    }
+    return launches;
 }
 void launch_mk2_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
                        const double* aux, cudaStream_t s) {

@@ -31,6 +31,7 @@ struct DevMesh {
     // face units (one flux evaluation each, see step_kernels.cu): owner slot,
     // owner cell, slot of the twin face in the neighbour (-1: one-sided)
     int n_slots = 0, n_units = 0;
+    int u_tr0 = 0, u_tr1 = 0;  // range of the tracked-face units (grouped together)
     const int32_t *u_slot = nullptr, *u_cell = nullptr, *u_twin = nullptr;
     const int32_t *fA = nullptr, *fB = nullptr, *ftype = nullptr, *fmaster = nullptr, *fsosed = nullptr,
                   *fcopy = nullptr, *fsdown = nullptr;
@@ -78,8 +79,8 @@ void launch_stationary_units(const DevMesh& d, const gelios_params& P, const Ste
 void launch_stationary_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
                               cudaStream_t s);
 void launch_mk2_recon(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* rec, cudaStream_t s);
-void launch_mk2_flux(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec, double* fl,
-                     cudaStream_t s);
+int launch_mk2_flux(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec, double* fl,
+                    cudaStream_t s);
 void launch_mk2_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
                        const double* aux, cudaStream_t s);
 void launch_mk2_source(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* aux, cudaStream_t s);

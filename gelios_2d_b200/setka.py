@@ -139,10 +139,14 @@ class Setka:
         rows = [np.ascontiguousarray(st[k]) for k in range(5)]
         N.check(self._L.gelios_upload_state(self._h, int(buf), *rows), "gelios_upload_state")
 
-    def par(self, buf: int) -> np.ndarray:
-        out = [np.zeros(self.mesh.n_cells) for _ in range(5)]
-        N.check(self._L.gelios_download_state(self._h, int(buf), *out), "gelios_download_state")
-        return np.stack(out)
+    def par(self, buf: int, out: np.ndarray | None = None) -> np.ndarray:
+        """Cell::par[buf] as rows (ro, p, u, v, Q); written into `out`
+        (shape (5, n_cells), C-contiguous, e.g. pinned host memory) if given."""
+        if out is None:
+            out = np.zeros((5, self.mesh.n_cells))
+        rows = [out[k] for k in range(5)]
+        N.check(self._L.gelios_download_state(self._h, int(buf), *rows), "gelios_download_state")
+        return out
 
     def set_mc(self, Hn, Hu, Hv, HT, ku, kv, kT):
         """Monte-Carlo moments of par[0] (H_n/H_u/H_v/H_T[4], k_u/k_v/k_T)."""
