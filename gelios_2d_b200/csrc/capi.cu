@@ -82,7 +82,7 @@ struct gelios_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;  // overlaps the source terms with the grid motion
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_recon = nullptr, ev_rails = nullptr;
     gelios_params prm{};
     bool have_mesh = false;
     DevMesh d;
@@ -91,7 +91,7 @@ struct gelios_ctx {
     DBuf fA, fB, ftype, fmaster, fsosed, fcopy, fsdown;
     DBuf rtype, rM, rpstart, rpts, rkstart, rkeys, rs;
     DBuf lc, li, lo, sp_point, sp_line, sp_inc, sp_ainc, sp_fix;
-    DBuf u_slot, u_cell, u_twin, flux, aux, rec;
+    DBuf u_slot, u_cell, u_twin, flux, aux, rec, src_lo;
     DBuf Hn, Hu, Hv, HT, ku, kv, kT, r_istoch, cback, cnext;
     // state par[2] x 5 fields, centroids [2], scratch
     DBuf state[2];
@@ -212,6 +212,8 @@ extern "C" int gelios_create(gelios_ctx** out, const gelios_params* prm, int dev
     GELIOS_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
     GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
     GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+    GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_recon, cudaEventDisableTiming));
+    GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_rails, cudaEventDisableTiming));
     if (ctx->words.alloc(64)) return GELIOS_E_CUDA;
     GELIOS_CUDA_TRY(cudaMemsetAsync(ctx->words.p, 0, 64, ctx->stream));
     *out = ctx.release();
@@ -238,6 +240,8 @@ extern "C" void gelios_destroy(gelios_ctx* ctx) {
     }
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+    if (ctx->ev_recon) cudaEventDestroy(ctx->ev_recon);
+    if (ctx->ev_rails) cudaEventDestroy(ctx->ev_rails);
     delete ctx;
 }
 
@@ -520,6 +524,18 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     rc |= upload(ctx->r_istoch, r_istoch, nc, s);
     rc |= upload(ctx->cback, cback, nc, s);
     rc |= upload(ctx->cnext, cnext, nc, s);
+    // the bracket cache of the source interpolation needs doubly linked
+    // chains with strictly increasing r_istoch along Next
+    bool chains_ok = true;
+    for (int c = 0; c < nc && chains_ok; c++) {
+        const int nx = cnext[c], bk = cback[c];
+        if (nx >= 0 && (cback[nx] != c || !(r_istoch[nx] > r_istoch[c]))) chains_ok = false;
+        if (bk >= 0 && (cnext[bk] != c || !(r_istoch[bk] < r_istoch[c]))) chains_ok = false;
+    }
+    {
+        std::vector<int32_t> minus1(nc, -1);
+        rc |= upload(ctx->src_lo, minus1.data(), nc, s);
+    }
     rc |= upload<double>(ctx->state[0], nullptr, 5 * static_cast<size_t>(nc), s);
     rc |= upload<double>(ctx->state[1], nullptr, 5 * static_cast<size_t>(nc), s);
     rc |= upload<double>(ctx->cen[0], nullptr, 3 * static_cast<size_t>(nc), s);
@@ -600,6 +616,8 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     d.r_istoch = ctx->r_istoch.as<double>();
     d.cback = ctx->cback.as<int32_t>();
     d.cnext = ctx->cnext.as<int32_t>();
+    d.src_lo = chains_ok ? ctx->src_lo.as<int32_t>() : nullptr;
+    d.src_lo_out = chains_ok ? ctx->src_lo.as<int32_t>() : nullptr;
     ctx->have_mesh = true;
     ctx->n_inner = 0;
     ctx->cen_valid = false;
@@ -729,18 +747,28 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             b.cx_next = cn;
             b.cy_next = cn + d.n_cells;
             b.rp_next = cn + 2 * static_cast<size_t>(d.n_cells);
-            // side stream: source terms and pre-motion geometry, overlapping the motion
+            // Two streams per step.
+            //   side: face reconstructions, source terms (both independent of
+            //         the motion), then the tracked-face fluxes once the rails
+            //         have moved;
+            //   main: surface tracking + rails, the other face fluxes, then
+            //         the cell update and the commit.
+            cudaStream_t sd = ctx->side;
             GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_fork, s));
-            GELIOS_CUDA_TRY(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
-            launch_mk2_source(d, P, b, ctx->aux.as<double>(), ctx->side);
-            launch_mk2_recon(d, P, b, ctx->rec.as<double>(), ctx->side);
-            GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_join, ctx->side));
+            GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_fork, 0));
+            launch_mk2_recon(d, P, b, ctx->rec.as<double>(), sd);
+            GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_recon, sd));
+            launch_mk2_source(d, P, b, ctx->aux.as<double>(), sd);
             cudaEvent_t e1 = ctx->phase_begin();
             const int nm = launch_motion(d, P, b, ctx->surface.as<double>(), s);
             ctx->phase_end(2, e1, nm);  // Move_surface + rails
-            GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_join, 0));
+            GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_rails, s));
+            GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_rails, 0));
+            const int nft = launch_mk2_flux_tracked(d, P, b, ctx->rec.as<double>(), ctx->flux.as<double>(), sd);
+            GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_join, sd));
+            GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_recon, 0));
             cudaEvent_t e3 = ctx->phase_begin();
-            const int nfl = launch_mk2_flux(d, P, b, ctx->rec.as<double>(), ctx->flux.as<double>(), s);
+            const int nfl = launch_mk2_flux_plain(d, P, b, ctx->rec.as<double>(), ctx->flux.as<double>(), s) + nft;
             ctx->phase_end(1, e3, nfl);
             cudaEvent_t e5 = ctx->phase_begin();
             launch_mk2_update(d, P, b, ctx->flux.as<double>(), ctx->aux.as<double>(), s);

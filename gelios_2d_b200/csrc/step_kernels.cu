@@ -288,7 +288,45 @@ __device__ void source_mk1(const DevMesh& d, const gelios_params& P, int k, doub
     if (rr > P.src_rmin && rr < P.src_rmax && xx >= 0.0) {
         int K_do = d.cback[k], K_posle = d.cnext[k];
         const double ri = d.r_istoch[k];
-        if (rr < ri) {
+        const int cached = d.src_lo ? d.src_lo[k] : -1;
+        if (cached >= 0) {
+            // The reference walks the radial chain from the cell itself
+            // (Cell.cpp:528-555).  Along a chain r_istoch increases strictly
+            // (checked at upload), so the bracket it finds is unique:
+            // r[lo] <= rr < r[hi] when rr < r_istoch, r[lo] < rr <= r[hi]
+            // otherwise, with hi = Next(lo).  Searching from last step's
+            // bracket finds the same pair in a step or two.
+            const bool caseA = rr < ri;
+            int lo = cached;
+            int guard = 0;
+            for (;;) {
+                const int hi = d.cnext[lo];
+                if (hi < 0 || ++guard > d.n_cells) {
+                    lo = -1;
+                    break;
+                }
+                const double rlo = d.r_istoch[lo], rhi = d.r_istoch[hi];
+                const bool below = caseA ? (rr < rlo) : !(rr > rlo);
+                const bool above = caseA ? !(rr < rhi) : (rr > rhi);
+                if (below) {
+                    lo = d.cback[lo];
+                    if (lo < 0) break;
+                } else if (above) {
+                    lo = hi;
+                } else {
+                    break;
+                }
+            }
+            // the reference dereferences Back of the lower cell (rr < r_istoch)
+            // or Next of the upper cell (otherwise); a missing link is its crash
+            if (lo < 0 || (caseA ? d.cback[lo] < 0 : d.cnext[d.cnext[lo]] < 0)) {
+                *status |= ST_CHAIN;
+                q1 = q2 = q3 = 0.0;
+                return;
+            }
+            K_do = lo;
+            K_posle = d.cnext[lo];
+        } else if (rr < ri) {
             double r1 = ri;
             int guard = 0;
             while (r1 > rr) {
@@ -332,6 +370,7 @@ __device__ void source_mk1(const DevMesh& d, const gelios_params& P, int k, doub
             q1 = q2 = q3 = 0.0;
             return;
         }
+        if (d.src_lo_out) d.src_lo_out[k] = K_do;
         const double r1 = d.r_istoch[K_do];
         const double r2 = d.r_istoch[K_posle];
         // linear(r1, t1, r2, t2, rr) for 19 fields with one reciprocal
@@ -1282,7 +1321,7 @@ __device__ St5 face_tvd(const DevMesh& d, const double* const* st, const double*
 //   [0] speed  [1] n1  [2] n2  [3] branch
 //   branch: contact 0 (B only); inner 0 (B only) / 1 (A and B);
 //           outer -1 (skipped) / 0 B / 1 A and B / 2 B / 3 A
-__global__ void __launch_bounds__(64) surface_faces_kernel(DevMesh d, gelios_params P, StepBuffers b,
+__global__ void __launch_bounds__(32) surface_faces_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                            double* __restrict__ scratch) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int nC = d.n_lc, nI = d.n_li, nO = d.n_lo;
@@ -1538,25 +1577,26 @@ void launch_stationary_update(const DevMesh& d, const gelios_params& P, const St
 void launch_mk2_recon(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* rec, cudaStream_t s) {
     mk2_recon_kernel<<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, b, rec);
 }
-int launch_mk2_flux(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec, double* fl,
-                    cudaStream_t s) {
-    const int nt = d.u_tr1 - d.u_tr0, nr = d.n_units - nt;
-    int launches = 0;
-    if (nr > 0) {
-        if (P.precision == GELIOS_PREC_FP32_FLUX)
-            mk2_flux_kernel<float, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, b, rec, fl, nr);
-        else
-            mk2_flux_kernel<double, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, b, rec, fl, nr);
-        launches++;
-    }
-    if (nt > 0) {
-        if (P.precision == GELIOS_PREC_FP32_FLUX)
-            mk2_flux_kernel<float, true><<<blocks_for(nt, 128), 128, 0, s>>>(d, P, b, rec, fl, nt);
-        else
-            mk2_flux_kernel<double, true><<<blocks_for(nt, 128), 128, 0, s>>>(d, P, b, rec, fl, nt);
-        launches++;
-    }
-    return launches;
+int launch_mk2_flux_plain(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
+                          double* fl, cudaStream_t s) {
+    const int nr = d.n_units - (d.u_tr1 - d.u_tr0);
+    if (nr <= 0) return 0;
+    if (P.precision == GELIOS_PREC_FP32_FLUX)
+        mk2_flux_kernel<float, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, b, rec, fl, nr);
+    else
+        mk2_flux_kernel<double, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, b, rec, fl, nr);
+    return 1;
+}
+int launch_mk2_flux_tracked(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
+                            double* fl, cudaStream_t s) {
+    const int nt = d.u_tr1 - d.u_tr0;
+    if (nt <= 0) return 0;
+    // few units, long serial solves: small blocks spread them over the SMs
+    if (P.precision == GELIOS_PREC_FP32_FLUX)
+        mk2_flux_kernel<float, true><<<blocks_for(nt, 32), 32, 0, s>>>(d, P, b, rec, fl, nt);
+    else
+        mk2_flux_kernel<double, true><<<blocks_for(nt, 32), 32, 0, s>>>(d, P, b, rec, fl, nt);
+    return 1;
 }
 void launch_mk2_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
                        const double* aux, cudaStream_t s) {
@@ -1581,7 +1621,7 @@ int launch_motion(const DevMesh& d, const gelios_params& P, const StepBuffers& b
     int launches = 0;
     const int nf = d.n_lc + d.n_li + d.n_lo;
     if (nf > 0) {
-        surface_faces_kernel<<<blocks_for(nf, 64), 64, 0, s>>>(d, P, b, scratch);
+        surface_faces_kernel<<<blocks_for(nf, 32), 32, 0, s>>>(d, P, b, scratch);
         const size_t shm = static_cast<size_t>(d.n_sp) * (2 * sizeof(double) + sizeof(int));
         static size_t shm_opted = 0;
         if (shm > 48 * 1024 && shm > shm_opted) {

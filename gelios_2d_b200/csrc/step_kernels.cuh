@@ -52,6 +52,10 @@ struct DevMesh {
     const double *Hn = nullptr, *Hu = nullptr, *Hv = nullptr, *HT = nullptr, *ku = nullptr, *kv = nullptr,
                  *kT = nullptr, *r_istoch = nullptr;
     const int32_t *cback = nullptr, *cnext = nullptr;
+    // bracket of the source interpolation found in the previous step (lower
+    // cell, -1 = none); used when the chains are consistent (see source_mk1)
+    const int32_t* src_lo = nullptr;
+    int32_t* src_lo_out = nullptr;
 };
 
 // Buffers of one time step (double buffering of the state like par[now1] ->
@@ -79,8 +83,10 @@ void launch_stationary_units(const DevMesh& d, const gelios_params& P, const Ste
 void launch_stationary_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
                               cudaStream_t s);
 void launch_mk2_recon(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* rec, cudaStream_t s);
-int launch_mk2_flux(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec, double* fl,
-                    cudaStream_t s);
+int launch_mk2_flux_plain(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
+                          double* fl, cudaStream_t s);
+int launch_mk2_flux_tracked(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
+                            double* fl, cudaStream_t s);
 void launch_mk2_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
                        const double* aux, cudaStream_t s);
 void launch_mk2_source(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* aux, cudaStream_t s);
