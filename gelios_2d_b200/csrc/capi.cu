@@ -770,6 +770,8 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             cudaEvent_t e3 = ctx->phase_begin();
             const int nfl = launch_mk2_flux_plain(d, P, b, ctx->rec.as<double>(), ctx->flux.as<double>(), s) + nft;
             ctx->phase_end(1, e3, nfl);
+            // the update reads the source terms and the tracked-face fluxes
+            GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_join, 0));
             cudaEvent_t e5 = ctx->phase_begin();
             launch_mk2_update(d, P, b, ctx->flux.as<double>(), ctx->aux.as<double>(), s);
             ctx->phase_end(3, e5, 1);
