@@ -81,8 +81,11 @@ int upload(DBuf& b, const T* src, size_t n, cudaStream_t s) {
 struct gelios_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
-    cudaStream_t side = nullptr;  // overlaps the source terms with the grid motion
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_recon = nullptr, ev_rails = nullptr;
+    // side streams: work of the moving-grid step that does not depend on the
+    // motion runs there while the main stream moves the grid
+    cudaStream_t side = nullptr;   // face reconstructions, tracked-face star pressures
+    cudaStream_t side2 = nullptr;  // charge-exchange source terms
+    cudaEvent_t ev_fork = nullptr, ev_recon = nullptr, ev_solve = nullptr, ev_source = nullptr;
     gelios_params prm{};
     bool have_mesh = false;
     DevMesh d;
@@ -91,7 +94,7 @@ struct gelios_ctx {
     DBuf fA, fB, ftype, fmaster, fsosed, fcopy, fsdown;
     DBuf rtype, rM, rpstart, rpts, rkstart, rkeys, rs;
     DBuf lc, li, lo, sp_point, sp_line, sp_inc, sp_ainc, sp_fix;
-    DBuf u_slot, u_cell, u_twin, flux, aux, rec, src_lo;
+    DBuf u_slot, u_cell, u_twin, flux, aux, rec, pstar, src_lo;
     DBuf Hn, Hu, Hv, HT, ku, kv, kT, r_istoch, cback, cnext;
     // state par[2] x 5 fields, centroids [2], scratch
     DBuf state[2];
@@ -208,12 +211,20 @@ extern "C" int gelios_create(gelios_ctx** out, const gelios_params* prm, int dev
     auto ctx = std::make_unique<gelios_ctx>();
     ctx->device = device;
     ctx->prm = *prm;
-    GELIOS_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-    GELIOS_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+    // The main stream carries the serial chain of the moving-grid step
+    // (surface tracking -> rails -> fluxes -> update), whose kernels occupy
+    // few SMs; it gets the highest priority so that its blocks are placed
+    // first while the side streams' grid-wide kernels fill the rest.
+    int prio_least = 0, prio_greatest = 0;
+    GELIOS_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest));
+    const int prio_mid = prio_greatest < prio_least ? prio_greatest + 1 : prio_greatest;
+    GELIOS_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, prio_greatest));
+    GELIOS_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->side, cudaStreamNonBlocking, prio_mid));
+    GELIOS_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->side2, cudaStreamNonBlocking, prio_least));
     GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
-    GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
     GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_recon, cudaEventDisableTiming));
-    GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_rails, cudaEventDisableTiming));
+    GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_solve, cudaEventDisableTiming));
+    GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_source, cudaEventDisableTiming));
     if (ctx->words.alloc(64)) return GELIOS_E_CUDA;
     GELIOS_CUDA_TRY(cudaMemsetAsync(ctx->words.p, 0, 64, ctx->stream));
     *out = ctx.release();
@@ -234,14 +245,13 @@ extern "C" void gelios_destroy(gelios_ctx* ctx) {
         cudaStreamSynchronize(ctx->stream);
         cudaStreamDestroy(ctx->stream);
     }
-    if (ctx->side) {
-        cudaStreamSynchronize(ctx->side);
-        cudaStreamDestroy(ctx->side);
-    }
-    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
-    if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
-    if (ctx->ev_recon) cudaEventDestroy(ctx->ev_recon);
-    if (ctx->ev_rails) cudaEventDestroy(ctx->ev_rails);
+    for (cudaStream_t* sp : {&ctx->side, &ctx->side2})
+        if (*sp) {
+            cudaStreamSynchronize(*sp);
+            cudaStreamDestroy(*sp);
+        }
+    for (cudaEvent_t e : {ctx->ev_fork, ctx->ev_recon, ctx->ev_solve, ctx->ev_source})
+        if (e) cudaEventDestroy(e);
     delete ctx;
 }
 
@@ -509,6 +519,7 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     rc |= upload<double>(ctx->flux, nullptr, 5 * static_cast<size_t>(ng), s);
     rc |= upload<double>(ctx->aux, nullptr, 5 * static_cast<size_t>(nc), s);
     rc |= upload<double>(ctx->rec, nullptr, 10 * u_slot.size(), s);
+    rc |= upload<double>(ctx->pstar, nullptr, static_cast<size_t>(u_tr1 - u_tr0) + 1, s);
     rc |= upload(ctx->sp_point, sp_point.data(), sp_point.size(), s);
     rc |= upload(ctx->sp_line, sp_line.data(), sp_line.size(), s);
     rc |= upload(ctx->sp_inc, sp_inc.data(), sp_inc.size(), s);
@@ -747,38 +758,42 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             b.cx_next = cn;
             b.cy_next = cn + d.n_cells;
             b.rp_next = cn + 2 * static_cast<size_t>(d.n_cells);
-            // Two streams per step.
-            //   side: face reconstructions, source terms (both independent of
-            //         the motion), then the tracked-face fluxes once the rails
-            //         have moved;
-            //   main: surface tracking + rails, the other face fluxes, then
-            //         the cell update and the commit.
-            cudaStream_t sd = ctx->side;
+            // Three streams per step.
+            //   side:  face reconstructions, then the star pressures of the
+            //          tracked faces (neither depends on the motion);
+            //   side2: charge-exchange source terms and pre-motion volumes;
+            //   main:  surface tracking + rails, the face fluxes (the tracked
+            //          ones sample the pre-solved Riemann problems at the
+            //          moved face speed), the cell update, the commit.
+            cudaStream_t sd = ctx->side, sd2 = ctx->side2;
             GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_fork, s));
             GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_fork, 0));
+            GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd2, ctx->ev_fork, 0));
             launch_mk2_recon(d, P, b, ctx->rec.as<double>(), sd);
             GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_recon, sd));
-            launch_mk2_source(d, P, b, ctx->aux.as<double>(), sd);
+            const int nsv = launch_mk2_tracked_solve(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(), sd);
+            GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_solve, sd));
+            launch_mk2_source(d, P, b, ctx->aux.as<double>(), sd2);
+            GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_source, sd2));
             cudaEvent_t e1 = ctx->phase_begin();
             const int nm = launch_motion(d, P, b, ctx->surface.as<double>(), s);
             ctx->phase_end(2, e1, nm);  // Move_surface + rails
-            GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_rails, s));
-            GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_rails, 0));
-            const int nft = launch_mk2_flux_tracked(d, P, b, ctx->rec.as<double>(), ctx->flux.as<double>(), sd);
-            GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_join, sd));
             GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_recon, 0));
             cudaEvent_t e3 = ctx->phase_begin();
-            const int nfl = launch_mk2_flux_plain(d, P, b, ctx->rec.as<double>(), ctx->flux.as<double>(), s) + nft;
+            int nfl = launch_mk2_flux_plain(d, P, b, ctx->rec.as<double>(), ctx->flux.as<double>(), s);
+            GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_solve, 0));
+            nfl += launch_mk2_flux_tracked(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(),
+                                           ctx->flux.as<double>(), s);
             ctx->phase_end(1, e3, nfl);
-            // the update reads the source terms and the tracked-face fluxes
-            GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_join, 0));
+            // the update reads the source terms
+            GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_source, 0));
             cudaEvent_t e5 = ctx->phase_begin();
             launch_mk2_update(d, P, b, ctx->flux.as<double>(), ctx->aux.as<double>(), s);
             ctx->phase_end(3, e5, 1);
             cudaEvent_t e4 = ctx->phase_begin();
             launch_commit(d, b, s);
             ctx->phase_end(4, e4, 1);
-            launches += nm + 4 + nfl;
+            launches += nm + 4 + nfl + nsv;
         } else {
             b.cx = cen0;
             b.cy = cen0 + d.n_cells;

@@ -239,15 +239,135 @@ __device__ __forceinline__ double lev_dev(double ga, double enI, double pI, doub
     return (fI + fII) - (enI - enII);
 }
 
+// Solvers::devtwo (Solvers.cpp:1231-1305): bisection for the star pressure
+// between pI and pII, stopping where |lev| <= 1e-9 (cap max_iter).
+//
+// COOP = true: the 32 lanes of a warp call it with identical arguments and
+// walk the same bisection together.  Each round, lanes 0..30 evaluate lev at
+// the 31 midpoints of the next five bisection levels (lane j = node j+1 of a
+// heap-ordered binary tree, its interval derived from the round's interval by
+// the same halvings the sequential loop performs), then every lane replays
+// the five sequential decisions on the broadcast values.  The midpoints, the
+// function values and the decisions are the ones of the sequential loop, so
+// the result and the iteration count are the same; the latency is one lev
+// evaluation per five iterations instead of five.
+template <bool COOP>
+__device__ __forceinline__ double godunov_devtwo(double ga, double enI, double pI, double rI, double enII, double pII,
+                                                 double rII, int max_iter, int* status) {
+    const double epsil = 10e-10;
+    double kl = pI, kp = pII;
+    double ksi = lev_dev(ga, enI, pI, rI, enII, pII, rII, kl);
+    const double ksir0 = lev_dev(ga, enI, pI, rI, enII, pII, rII, kp);
+    if (fabs(ksi) <= epsil) return kl;
+    if (fabs(ksir0) <= epsil) return kp;
+    int k = 0;
+    if (!COOP) {
+        for (;;) {
+            k = k + 1;
+            if (k >= max_iter) {
+                *status |= ST_ITER_CAP;
+                return (kl + kp) / 2.0;
+            }
+            const double kc = (kl + kp) / 2.0;
+            const double ksit = lev_dev(ga, enI, pI, rI, enII, pII, rII, kc);
+            if (fabs(ksit) <= epsil) return kc;
+            if ((ksi * ksit) <= 0.0) {
+                kp = kc;
+            } else {
+                kl = kc;
+                ksi = ksit;
+            }
+        }
+    }
+    const int node = (threadIdx.x & 31) + 1;  // 1..32; node 32 (level 5) evaluates nothing
+    const int L = 31 - __clz(node);
+    const int idx = node - (1 << L);
+    for (;;) {
+        double a = kl, b = kp;
+        for (int l = 0; l < L; l++) {
+            const double c = (a + b) / 2.0;
+            if ((idx >> (L - 1 - l)) & 1) a = c;
+            else b = c;
+        }
+        double f = 0.0;
+        if (L < 5) f = lev_dev(ga, enI, pI, rI, enII, pII, rII, (a + b) / 2.0);
+        int nd = 1;
+        for (int l = 0; l < 5; l++) {
+            k = k + 1;
+            if (k >= max_iter) {
+                *status |= ST_ITER_CAP;
+                return (kl + kp) / 2.0;
+            }
+            const double kc = (kl + kp) / 2.0;
+            const double ksit = __shfl_sync(0xffffffffu, f, nd - 1);
+            if (fabs(ksit) <= epsil) return kc;
+            if ((ksi * ksit) <= 0.0) {
+                kp = kc;
+                nd = 2 * nd;
+            } else {
+                kl = kc;
+                ksi = ksit;
+                nd = 2 * nd + 1;
+            }
+        }
+    }
+}
+
+// Solvers::newton (Solvers.cpp:1174-1229): Newton iteration for the star
+// pressure of two shocks (cap max_iter; a non-positive iterate is returned
+// as is, like the reference, and raises ST_NEWTON_NEG).
+__device__ __forceinline__ double godunov_newton(double ga, double enI, double pI, double rI, double enII,
+                                                 double pII, double rII, int max_iter, int* status) {
+    const double gm = ((ga - 1.0) / ga) / 2.0, gp = ((ga + 1.0) / ga) / 2.0;
+    const double eps = 10e-10;
+    const double cIn = sqrt(ga * pI / rI);
+    const double cIIn = sqrt(ga * pII / rII);
+    double pn = pI * rII * cIIn + pII * rI * cIn + (enI - enII) * rI * cIn * rII * cIIn;
+    pn = pn / (rI * cIn + rII * cIIn);
+    const double pee = pn;
+    int kiter = 0;
+    for (;;) {
+        const double pp = pn;
+        if (pp <= 0.0) {
+            *status |= ST_NEWTON_NEG;
+            return pp;
+        }
+        kiter = kiter + 1;
+        // pow(z, 3/2) of the reference as z*sqrt(z)
+        const double zI = gp * pp / pI + gm, zII = gp * pp / pII + gm;
+        const double sI = sqrt(zI), sII = sqrt(zII);
+        const double fI = (pp - pI) / (rI * cIn * sI);
+        double fIs = (ga + 1.0) * pp / pI + (3.0 * ga - 1.0);
+        fIs = fIs / (4.0 * ga * rI * cIn * (zI * sI));
+        const double fII = (pp - pII) / (rII * cIIn * sII);
+        double fIIs = (ga + 1.0) * pp / pII + (3.0 * ga - 1.0);
+        fIIs = fIIs / (4.0 * ga * rII * cIIn * (zII * sII));
+        if (kiter >= max_iter) {
+            *status |= ST_ITER_CAP;
+            return pp;
+        }
+        pn = pp - (fI + fII - (enI - enII)) / (fIs + fIIs);
+        if (!(fabs(pn / pee - pp / pee) >= eps)) return pn;
+    }
+}
+
 // Solvers::Godunov_Solver_Alexashov with newton/devtwo, Solvers.cpp:693-1305.
 // q = (ro, p, u, v, w); qqq[5] flux; ds[3] = dsl, dsp, dsc.  Returns the
 // wave-speed bound UU of the reference's CFL candidate kurant*DIST/UU (UU is
 // replaced by eps8 when it is not above it, Solvers.cpp:841-848).
 // The Newton and bisection loops are capped at max_iter (the reference
 // exits the program at 1100); hitting the cap raises ST_ITER_CAP.
+//
+// The star pressure of the two iterative branches does not depend on the
+// face speed w: p_out (if given) receives the pressure after the branch
+// selection, and p_in (if given) replaces the iteration by that value, so a
+// caller can solve before the grid moves and sample after it.  COOP selects
+// the warp-cooperative bisection (all 32 lanes, identical arguments).
+template <bool COOP>
 static __device__ __noinline__ double godunov_dev(double ga, double kurant, const double* qqq1, const double* qqq2,
                                            const double* n, double* qqq, double* ds, double w, double DIST,
-                                           int max_iter, int* status) {
+                                           int max_iter, int* status, const double* p_in = nullptr,
+                                           double* p_out = nullptr) {
     const double g1 = ga - 1.0, g2 = ga + 1.0, gm = (g1 / ga) / 2.0, gp = (g2 / ga) / 2.0;
     const double eps = 10e-10, eps8 = 10e-8;
     const double al = n[0], be = n[1], ge = n[2];
@@ -286,76 +406,14 @@ static __device__ __noinline__ double godunov_dev(double ga, double kurant, cons
     } else if ((Udf >= Uvk) && (Udf <= Urz)) {
         p = pI * pow(((Udf - Uvk) / (Urz - Uvk)), (1.0 / gm));
         il = 0; ip = 0;
-    } else if ((Udf > Urz) && (Udf <= Uud)) {  // devtwo, Solvers.cpp:1231-1305
-        const double epsil = 10e-10;
-        double kl = pI, kp = pII, ksi, ksit;
-        ksi = lev_dev(ga, enI, pI, rI, enII, pII, rII, kl);
-        const double ksir0 = lev_dev(ga, enI, pI, rI, enII, pII, rII, kp);
-        if (fabs(ksi) <= epsil) {
-            p = kl;
-        } else if (fabs(ksir0) <= epsil) {
-            p = kp;
-        } else {
-            int k = 0;
-            for (;;) {
-                k = k + 1;
-                if (k >= max_iter) {
-                    *status |= ST_ITER_CAP;
-                    p = (kl + kp) / 2.0;
-                    break;
-                }
-                const double kc = (kl + kp) / 2.0;
-                ksit = lev_dev(ga, enI, pI, rI, enII, pII, rII, kc);
-                if (fabs(ksit) <= epsil) {
-                    p = kc;
-                    break;
-                }
-                if ((ksi * ksit) <= 0.0) {
-                    kp = kc;
-                } else {
-                    kl = kc;
-                    ksi = ksit;
-                }
-            }
-        }
+    } else if ((Udf > Urz) && (Udf <= Uud)) {  // devtwo
+        p = p_in ? *p_in : godunov_devtwo<COOP>(ga, enI, pI, rI, enII, pII, rII, max_iter, status);
         il = 1; ip = 0;
-    } else if (Udf > Uud) {  // newton, Solvers.cpp:1174-1229
-        const double cIn = sqrt(ga * pI / rI);
-        const double cIIn = sqrt(ga * pII / rII);
-        double pn = pI * rII * cIIn + pII * rI * cIn + (enI - enII) * rI * cIn * rII * cIIn;
-        pn = pn / (rI * cIn + rII * cIIn);
-        const double pee = pn;
-        int kiter = 0;
-        for (;;) {
-            double pp = pn;
-            if (pp <= 0.0) {
-                *status |= ST_NEWTON_NEG;
-                p = pp;
-                break;
-            }
-            kiter = kiter + 1;
-            // pow(z, 3/2) of the reference as z*sqrt(z)
-            const double zI = gp * pp / pI + gm, zII = gp * pp / pII + gm;
-            const double sI = sqrt(zI), sII = sqrt(zII);
-            const double fI = (pp - pI) / (rI * cIn * sI);
-            double fIs = (ga + 1.0) * pp / pI + (3.0 * ga - 1.0);
-            fIs = fIs / (4.0 * ga * rI * cIn * (zI * sI));
-            const double fII = (pp - pII) / (rII * cIIn * sII);
-            double fIIs = (ga + 1.0) * pp / pII + (3.0 * ga - 1.0);
-            fIIs = fIIs / (4.0 * ga * rII * cIIn * (zII * sII));
-            if (kiter >= max_iter) {
-                *status |= ST_ITER_CAP;
-                p = pp;
-                break;
-            }
-            pn = pp - (fI + fII - (enI - enII)) / (fIs + fIIs);
-            if (!(fabs(pn / pee - pp / pee) >= eps)) {
-                p = pn;
-                break;
-            }
-        }
+    } else if (Udf > Uud) {  // newton
+        p = p_in ? *p_in : godunov_newton(ga, enI, pI, rI, enII, pII, rII, max_iter, status);
         il = 1; ip = 1;
     }
+    if (p_out) *p_out = p;
     if ((il == 1) && (ip == 1)) {  // two shocks
         const double aI = sqrt(rI * (g2 / 2.0 * p + g1 / 2.0 * pI));
         const double aII = sqrt(rII * (g2 / 2.0 * p + g1 / 2.0 * pII));

@@ -279,152 +279,175 @@ __device__ void tvd_radial(const double* const* st, const double* cx, const doub
     op = linear3r(par1.p * rp[Sd], Ms.p * rpM, par3.p * rp[So], r12, r23, -dist2) / pdis;
 }
 
-// Cell::Get_Sourse_MK1 (Cell.cpp:498-665).
+// Get_Sourse_MK1 (Cell.cpp:528-555): the pair of cells of k's radial chain
+// whose r_istoch bracket the centroid radius rr (K_posle = Next(K_do)).
+// Returns false (and raises ST_CHAIN) where the reference would follow a
+// missing Back/Next link.
+__device__ bool source_bracket(const DevMesh& d, int k, double rr, int& K_do, int& K_posle, int* status) {
+    K_do = d.cback[k];
+    K_posle = d.cnext[k];
+    const double ri = d.r_istoch[k];
+    const int cached = d.src_lo ? d.src_lo[k] : -1;
+    if (cached >= 0) {
+        // The reference walks the radial chain from the cell itself.  Along
+        // a chain r_istoch increases strictly (checked at upload), so the
+        // bracket it finds is unique: r[lo] <= rr < r[hi] when rr <
+        // r_istoch, r[lo] < rr <= r[hi] otherwise, with hi = Next(lo).
+        // Searching from last step's bracket finds the same pair in a step
+        // or two.
+        const bool caseA = rr < ri;
+        int lo = cached;
+        int guard = 0;
+        for (;;) {
+            const int hi = d.cnext[lo];
+            if (hi < 0 || ++guard > d.n_cells) {
+                lo = -1;
+                break;
+            }
+            const double rlo = d.r_istoch[lo], rhi = d.r_istoch[hi];
+            const bool below = caseA ? (rr < rlo) : !(rr > rlo);
+            const bool above = caseA ? !(rr < rhi) : (rr > rhi);
+            if (below) {
+                lo = d.cback[lo];
+                if (lo < 0) break;
+            } else if (above) {
+                lo = hi;
+            } else {
+                break;
+            }
+        }
+        // the reference dereferences Back of the lower cell (rr < r_istoch)
+        // or Next of the upper cell (otherwise); a missing link is its crash
+        if (lo < 0 || (caseA ? d.cback[lo] < 0 : d.cnext[d.cnext[lo]] < 0)) {
+            *status |= ST_CHAIN;
+            return false;
+        }
+        K_do = lo;
+        K_posle = d.cnext[lo];
+    } else if (rr < ri) {
+        double r1 = ri;
+        int guard = 0;
+        while (r1 > rr) {
+            if (K_do < 0 || ++guard > d.n_cells) {
+                *status |= ST_CHAIN;
+                return false;
+            }
+            r1 = d.r_istoch[K_do];
+            K_do = d.cback[K_do];
+        }
+        if (K_do < 0) {
+            *status |= ST_CHAIN;
+            return false;
+        }
+        K_do = d.cnext[K_do];
+        K_posle = K_do >= 0 ? d.cnext[K_do] : -1;
+    } else {
+        double r2 = ri;
+        int guard = 0;
+        while (r2 < rr) {
+            if (K_posle < 0 || ++guard > d.n_cells) {
+                *status |= ST_CHAIN;
+                return false;
+            }
+            r2 = d.r_istoch[K_posle];
+            K_posle = d.cnext[K_posle];
+        }
+        if (K_posle < 0) {
+            *status |= ST_CHAIN;
+            return false;
+        }
+        K_posle = d.cback[K_posle];
+        K_do = K_posle >= 0 ? d.cback[K_posle] : -1;
+    }
+    if (K_do < 0 || K_posle < 0) {
+        *status |= ST_CHAIN;
+        return false;
+    }
+    return true;
+}
+
+// Monte-Carlo moments of species s seen by cell k (Cell.cpp:528-589): radial
+// interpolation between the chain cells K_do and K_posle inside the source
+// region, the cell's own moments outside it.  Also the k_u, k_v, k_T factors.
+struct SrcMoments {
+    double uH, vH, roH, pH, ku, kv, kT;
+};
+__device__ __forceinline__ SrcMoments source_moments(const DevMesh& d, int k, int s, bool interp, int K_do, int K_posle,
+                                                     double rr) {
+    SrcMoments m;
+    if (interp) {
+        const double r1 = d.r_istoch[K_do];
+        const double r2 = d.r_istoch[K_posle];
+        // linear(r1, t1, r2, t2, rr) with one reciprocal for all fields
+        const double ir = 1.0 / (r1 - r2), dr = rr - r2;
+        auto lin = [&](double t1, double t2) { return (t1 - t2) * ir * dr + t2; };
+        m.uH = lin(d.Hu[4 * K_do + s], d.Hu[4 * K_posle + s]);
+        m.vH = lin(d.Hv[4 * K_do + s], d.Hv[4 * K_posle + s]);
+        m.roH = lin(d.Hn[4 * K_do + s], d.Hn[4 * K_posle + s]);
+        const double TH = lin(d.HT[4 * K_do + s], d.HT[4 * K_posle + s]);
+        m.ku = lin(d.ku[K_do], d.ku[K_posle]);
+        m.kv = lin(d.kv[K_do], d.kv[K_posle]);
+        m.kT = lin(d.kT[K_do], d.kT[K_posle]);
+        m.pH = 0.5 * TH * m.roH;
+    } else {
+        m.uH = d.Hu[4 * k + s];
+        m.vH = d.Hv[4 * k + s];
+        m.roH = d.Hn[4 * k + s];
+        m.pH = 0.5 * d.HT[4 * k + s] * d.Hn[4 * k + s];
+        m.ku = d.ku[k];
+        m.kv = d.kv[k];
+        m.kT = d.kT[k];
+    }
+    return m;
+}
+
+// Charge-exchange momentum / energy exchange rates of one species
+// (Cell.cpp:590-660): nu_u, nu_v, nu_e before the sum over species.
+__device__ __forceinline__ void source_rates(const gelios_params& P, SrcMoments m, double u, double v, double ro,
+                                             double pro, double kin, double& nuu, double& nuv, double& nue) {
+    if (m.roH <= 0.0) {
+        m.roH = 0.0000001;
+        m.pH = 0.0;
+    }
+    const double th = 2.0 * m.pH / m.roH;
+    const double du2 = sq(u - m.uH) + sq(v - m.vH);
+    const double UM = sqrt(du2 + (64.0 / (9.0 * kPi)) * (pro + th));
+    const double UH = sqrt(du2 + (4.0 / kPi) * (pro + th));
+    const double sig = sq(1.0 - P.a_2 * log(UM));
+    const double nu = ro * m.roH * UM * sig;
+    nuu = nu * (m.uH - u);
+    nuv = nu * (m.vH - v);
+    nue = nu * ((sq(m.uH) + sq(m.vH) - kin) / 2.0 + (UH / UM) * (th - pro));
+}
+
+// Cell::Get_Sourse_MK1 (Cell.cpp:498-665), one thread per cell.
 __device__ void source_mk1(const DevMesh& d, const gelios_params& P, int k, double xx, double yy, double u, double v,
                            double ro, double p, double& q1, double& q2, double& q3, int* status) {
     const double rr = sqrt(sq(xx) + sq(yy));
-    double uH[4], vH[4], roH[4], pH[4];
-    double ku = d.ku[k], kvv = d.kv[k], kT = d.kT[k];
-    if (rr > P.src_rmin && rr < P.src_rmax && xx >= 0.0) {
-        int K_do = d.cback[k], K_posle = d.cnext[k];
-        const double ri = d.r_istoch[k];
-        const int cached = d.src_lo ? d.src_lo[k] : -1;
-        if (cached >= 0) {
-            // The reference walks the radial chain from the cell itself
-            // (Cell.cpp:528-555).  Along a chain r_istoch increases strictly
-            // (checked at upload), so the bracket it finds is unique:
-            // r[lo] <= rr < r[hi] when rr < r_istoch, r[lo] < rr <= r[hi]
-            // otherwise, with hi = Next(lo).  Searching from last step's
-            // bracket finds the same pair in a step or two.
-            const bool caseA = rr < ri;
-            int lo = cached;
-            int guard = 0;
-            for (;;) {
-                const int hi = d.cnext[lo];
-                if (hi < 0 || ++guard > d.n_cells) {
-                    lo = -1;
-                    break;
-                }
-                const double rlo = d.r_istoch[lo], rhi = d.r_istoch[hi];
-                const bool below = caseA ? (rr < rlo) : !(rr > rlo);
-                const bool above = caseA ? !(rr < rhi) : (rr > rhi);
-                if (below) {
-                    lo = d.cback[lo];
-                    if (lo < 0) break;
-                } else if (above) {
-                    lo = hi;
-                } else {
-                    break;
-                }
-            }
-            // the reference dereferences Back of the lower cell (rr < r_istoch)
-            // or Next of the upper cell (otherwise); a missing link is its crash
-            if (lo < 0 || (caseA ? d.cback[lo] < 0 : d.cnext[d.cnext[lo]] < 0)) {
-                *status |= ST_CHAIN;
-                q1 = q2 = q3 = 0.0;
-                return;
-            }
-            K_do = lo;
-            K_posle = d.cnext[lo];
-        } else if (rr < ri) {
-            double r1 = ri;
-            int guard = 0;
-            while (r1 > rr) {
-                if (K_do < 0 || ++guard > d.n_cells) {
-                    *status |= ST_CHAIN;
-                    q1 = q2 = q3 = 0.0;
-                    return;
-                }
-                r1 = d.r_istoch[K_do];
-                K_do = d.cback[K_do];
-            }
-            if (K_do < 0) {
-                *status |= ST_CHAIN;
-                q1 = q2 = q3 = 0.0;
-                return;
-            }
-            K_do = d.cnext[K_do];
-            K_posle = K_do >= 0 ? d.cnext[K_do] : -1;
-        } else {
-            double r2 = ri;
-            int guard = 0;
-            while (r2 < rr) {
-                if (K_posle < 0 || ++guard > d.n_cells) {
-                    *status |= ST_CHAIN;
-                    q1 = q2 = q3 = 0.0;
-                    return;
-                }
-                r2 = d.r_istoch[K_posle];
-                K_posle = d.cnext[K_posle];
-            }
-            if (K_posle < 0) {
-                *status |= ST_CHAIN;
-                q1 = q2 = q3 = 0.0;
-                return;
-            }
-            K_posle = d.cback[K_posle];
-            K_do = K_posle >= 0 ? d.cback[K_posle] : -1;
-        }
-        if (K_do < 0 || K_posle < 0) {
-            *status |= ST_CHAIN;
+    const bool interp = rr > P.src_rmin && rr < P.src_rmax && xx >= 0.0;
+    int K_do = -1, K_posle = -1;
+    if (interp) {
+        if (!source_bracket(d, k, rr, K_do, K_posle, status)) {
             q1 = q2 = q3 = 0.0;
             return;
         }
         if (d.src_lo_out) d.src_lo_out[k] = K_do;
-        const double r1 = d.r_istoch[K_do];
-        const double r2 = d.r_istoch[K_posle];
-        // linear(r1, t1, r2, t2, rr) for 19 fields with one reciprocal
-        const double ir = 1.0 / (r1 - r2), dr = rr - r2;
-        auto lin = [&](double t1, double t2) { return (t1 - t2) * ir * dr + t2; };
-        double TH[4];
-#pragma unroll
-        for (int s = 0; s < 4; s++) uH[s] = lin(d.Hu[4 * K_do + s], d.Hu[4 * K_posle + s]);
-#pragma unroll
-        for (int s = 0; s < 4; s++) vH[s] = lin(d.Hv[4 * K_do + s], d.Hv[4 * K_posle + s]);
-#pragma unroll
-        for (int s = 0; s < 4; s++) roH[s] = lin(d.Hn[4 * K_do + s], d.Hn[4 * K_posle + s]);
-#pragma unroll
-        for (int s = 0; s < 4; s++) TH[s] = lin(d.HT[4 * K_do + s], d.HT[4 * K_posle + s]);
-        ku = lin(d.ku[K_do], d.ku[K_posle]);
-        kvv = lin(d.kv[K_do], d.kv[K_posle]);
-        kT = lin(d.kT[K_do], d.kT[K_posle]);
-#pragma unroll
-        for (int s = 0; s < 4; s++) pH[s] = 0.5 * TH[s] * roH[s];
-    } else {
-#pragma unroll
-        for (int s = 0; s < 4; s++) {
-            uH[s] = d.Hu[4 * k + s];
-            vH[s] = d.Hv[4 * k + s];
-            roH[s] = d.Hn[4 * k + s];
-            pH[s] = 0.5 * d.HT[4 * k + s] * d.Hn[4 * k + s];
-        }
     }
-    double Mu = 0.0, Mv = 0.0, MT = 0.0;
-    double nuu[4], nuv[4], nue[4];
     const double pro = p / ro;
     const double kin = sq(u) + sq(v);
+    double nuu[4], nuv[4], nue[4];
+    SrcMoments m;
 #pragma unroll
     for (int s = 0; s < 4; s++) {
-        if (roH[s] <= 0.0) {
-            roH[s] = 0.0000001;
-            pH[s] = 0.0;
-        }
-        const double th = 2.0 * pH[s] / roH[s];
-        const double du2 = sq(u - uH[s]) + sq(v - vH[s]);
-        const double UM = sqrt(du2 + (64.0 / (9.0 * kPi)) * (pro + th));
-        const double UH = sqrt(du2 + (4.0 / kPi) * (pro + th));
-        const double sig = sq(1.0 - P.a_2 * log(UM));
-        const double nu = ro * roH[s] * UM * sig;
-        nuu[s] = nu * (uH[s] - u);
-        nuv[s] = nu * (vH[s] - v);
-        nue[s] = nu * ((sq(uH[s]) + sq(vH[s]) - kin) / 2.0 + (UH / UM) * (th - pro));
+        m = source_moments(d, k, s, interp, K_do, K_posle, rr);
+        source_rates(P, m, u, v, ro, pro, kin, nuu[s], nuv[s], nue[s]);
     }
-    Mu = P.src_coef * (nuu[0] + nuu[1] + nuu[2] + nuu[3]);
-    Mv = P.src_coef * (nuv[0] + nuv[1] + nuv[2] + nuv[3]);
-    MT = P.src_coef * (nue[0] + nue[1] + nue[2] + nue[3]);
-    q1 = Mu * ku;
-    q2 = Mv * kvv;
-    q3 = MT * kT;
+    const double Mu = P.src_coef * (nuu[0] + nuu[1] + nuu[2] + nuu[3]);
+    const double Mv = P.src_coef * (nuv[0] + nuv[1] + nuv[2] + nuv[3]);
+    const double MT = P.src_coef * (nue[0] + nue[1] + nue[2] + nue[3]);
+    q1 = Mu * m.ku;
+    q2 = Mv * m.kv;
+    q3 = MT * m.kT;
 }
 
 // Block-level minimum of `t` (non-negative doubles; NaN ignored) folded into
@@ -771,7 +794,7 @@ __global__ void __launch_bounds__(128) mk2_recon_kernel(DevMesh d, gelios_params
 template <typename TF, bool TRACKED>
 __global__ void __launch_bounds__(128) mk2_flux_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                        const double* __restrict__ rec, double* __restrict__ fl,
-                                                       int n_launch) {
+                                                       const double* __restrict__ pstar, int n_launch) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double tmin_u = __longlong_as_double(0x7ff0000000000000LL);
     int status = 0;
@@ -827,7 +850,9 @@ __global__ void __launch_bounds__(128) mk2_flux_kernel(DevMesh d, gelios_params 
                 double q2[5] = {par2.ro, par2.p, par2.u, par2.v, 0.0};
                 double nv[3] = {n1, n2, 0.0};
                 double qq[5], ds[3];
-                UG = godunov_dev(P.gamma, P.kurant, q1, q2, nv, qq, ds, W, 1.0, P.godunov_max_iter, &status);
+                // star pressure from mk2_tracked_solve_kernel (solved before the motion)
+                UG = godunov_dev<false>(P.gamma, P.kurant, q1, q2, nv, qq, ds, W, 1.0, P.godunov_max_iter, &status,
+                                        pstar + i);
                 fm0 = qq[0] * S;
                 fm1 = qq[1] * S;
                 fm2 = qq[2] * S;
@@ -861,6 +886,44 @@ __global__ void __launch_bounds__(128) mk2_flux_kernel(DevMesh d, gelios_params 
     block_reduce_commit(tmin_u, 0, 0, status, b.dt_acc, b.counters, b.status);
 }
 
+// Star pressure of the exact Godunov problem of every tracked-face unit
+// (Solvers.cpp:1174-1305).  It depends on the reconstructed states and on
+// the face normal before the motion, not on the face speed, so it runs on a
+// side stream while the grid moves; mk2_flux_kernel<TRACKED> samples the
+// solution at the face speed afterwards.  One warp per unit (warp-cooperative
+// bisection); pstar[i] belongs to unit u_tr0 + i.
+__global__ void __launch_bounds__(64) mk2_tracked_solve_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                               const double* __restrict__ rec,
+                                                               double* __restrict__ pstar) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= d.u_tr1 - d.u_tr0) return;
+    const int u = d.u_tr0 + i;
+    int status = 0;
+    const int g = d.u_slot[u], K = d.u_cell[u], gt = d.u_twin[u];
+    const double x = b.cx[K], y = b.cy[K];
+    const bool procK = !(sqrt(sq(x) + sq(y)) < P.R11);
+    bool procN = false;
+    const int nb = gt >= 0 ? d.snb[g] : -1;
+    if (nb >= 0) procN = !(sqrt(sq(b.cx[nb]) + sq(b.cy[nb])) < P.R11);
+    if (!(procK || procN)) return;
+    const int A = d.sA[g], B = d.sB[g];
+    const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
+    double t1 = xb - xa, t2 = yb - ya;
+    const double nn = sqrt(sq(t1) + sq(t2));
+    t1 = t1 / nn;
+    t2 = t2 / nn;
+    const size_t n = d.n_units;
+    double q1[5] = {rec[0 * n + u], rec[1 * n + u], rec[2 * n + u], rec[3 * n + u], 0.0};
+    double q2[5] = {rec[5 * n + u], rec[6 * n + u], rec[7 * n + u], rec[8 * n + u], 0.0};
+    double nv[3] = {t2, -t1, 0.0};
+    double qq[5], ds[3], p = 0.0;
+    godunov_dev<true>(P.gamma, P.kurant, q1, q2, nv, qq, ds, 0.0, 1.0, P.godunov_max_iter, &status, nullptr, &p);
+    if ((threadIdx.x & 31) == 0) {
+        pstar[i] = p;
+        if (status) atomicOr(b.status, status);
+    }
+}
+
 // Terms of the MK2 cell update that do not depend on the fluxes or on the
 // motion: the charge-exchange source Get_Sourse_MK1 (Cell.cpp:498-665) and
 // the area / rotated volume of the cell before the motion.  Runs on a side
@@ -868,30 +931,67 @@ __global__ void __launch_bounds__(128) mk2_flux_kernel(DevMesh d, gelios_params 
 // aux rows: q1, q2, q3, vs1 (Get_Volume), Volume (Get_Volume_rotate/2pi)
 __global__ void __launch_bounds__(128) mk2_source_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                          double* __restrict__ aux) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    // four lanes per cell, one hydrogen species per lane; the four rates
+    // are summed on the cell's first lane in the reference's order
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = t >> 2, sp = t & 3;
     int status = 0;
+    bool proc = false, ok = false;
+    double nuu = 0.0, nuv = 0.0, nue = 0.0;
+    SrcMoments m{};
+    double x = 0.0, y = 0.0;
     if (c < d.n_cells) {
-        const double x = b.cx[c], y = b.cy[c];
-        if (!(sqrt(sq(x) + sq(y)) < P.R11)) {
-            const size_t n = d.n_cells;
+        x = b.cx[c];
+        y = b.cy[c];
+        proc = !(sqrt(sq(x) + sq(y)) < P.R11);
+        if (proc) {
             const St5 par1 = load_state(b.cur, c);
-            double q1, q2, q3;
-            source_mk1(d, P, c, x, y, par1.u, par1.v, par1.ro, par1.p, q1, q2, q3, &status);
-            aux[0 * n + c] = q1;
-            aux[1 * n + c] = q2;
-            aux[2 * n + c] = q3;
-            const int s0 = d.cstart[c], nv = d.cstart[c + 1] - s0;
-            const int32_t* con = d.contour + s0;
-            aux[3 * n + c] = area(con, nv, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X, d.Y, false);
-            aux[4 * n + c] = volume_rotate(con, nv, d.X, d.Y);
+            const double rr = sqrt(sq(x) + sq(y));
+            const bool interp = rr > P.src_rmin && rr < P.src_rmax && x >= 0.0;
+            int K_do = -1, K_posle = -1;
+            ok = !interp || source_bracket(d, c, rr, K_do, K_posle, &status);
+            if (ok) {
+                if (interp && sp == 0 && d.src_lo_out) d.src_lo_out[c] = K_do;
+                m = source_moments(d, c, sp, interp, K_do, K_posle, rr);
+                source_rates(P, m, par1.u, par1.v, par1.ro, par1.p / par1.ro, sq(par1.u) + sq(par1.v), nuu, nuv,
+                             nue);
+            }
         }
+    }
+    const unsigned full = 0xffffffffu;
+    const int q0 = (threadIdx.x & 31) & ~3;
+    double su[3], sv[3], se[3];
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        su[j] = __shfl_sync(full, nuu, q0 + 1 + j);
+        sv[j] = __shfl_sync(full, nuv, q0 + 1 + j);
+        se[j] = __shfl_sync(full, nue, q0 + 1 + j);
+    }
+    if (proc && sp == 0) {
+        const size_t n = d.n_cells;
+        double q1 = 0.0, q2 = 0.0, q3 = 0.0;
+        if (ok) {
+            const double Mu = P.src_coef * (nuu + su[0] + su[1] + su[2]);
+            const double Mv = P.src_coef * (nuv + sv[0] + sv[1] + sv[2]);
+            const double MT = P.src_coef * (nue + se[0] + se[1] + se[2]);
+            q1 = Mu * m.ku;
+            q2 = Mv * m.kv;
+            q3 = MT * m.kT;
+        }
+        aux[0 * n + c] = q1;
+        aux[1 * n + c] = q2;
+        aux[2 * n + c] = q3;
+        const int s0 = d.cstart[c], nv = d.cstart[c + 1] - s0;
+        const int32_t* con = d.contour + s0;
+        aux[3 * n + c] = area(con, nv, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X, d.Y, false);
+        aux[4 * n + c] = volume_rotate(con, nv, d.X, d.Y);
     }
     if (status) atomicOr(b.status, status);
 }
 
 // Go_5_komponent__MK2 cell update (Setka.cpp:10386-10468) from the summed
 // slots; also the centroid of the moved cell (the next step's centroid).
-__global__ void __launch_bounds__(128) mk2_update_kernel(DevMesh d, gelios_params P, StepBuffers b,
+__global__ void __launch_bounds__(128, 6) mk2_update_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                          const double* __restrict__ fl,
                                                          const double* __restrict__ aux) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1321,16 +1421,18 @@ __device__ St5 face_tvd(const DevMesh& d, const double* const* st, const double*
 //   [0] speed  [1] n1  [2] n2  [3] branch
 //   branch: contact 0 (B only); inner 0 (B only) / 1 (A and B);
 //           outer -1 (skipped) / 0 B / 1 A and B / 2 B / 3 A
-__global__ void __launch_bounds__(32) surface_faces_kernel(DevMesh d, gelios_params P, StepBuffers b,
+// One warp per face: the lanes hold identical copies of the face's data, the
+// exact solver runs warp-cooperatively, lane 0 writes.
+__global__ void __launch_bounds__(64) surface_faces_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                            double* __restrict__ scratch) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     const int nC = d.n_lc, nI = d.n_li, nO = d.n_lo;
     if (j >= nC + nI + nO) return;
     const double* const* st = b.cur;
     int status = 0;
     const double ga = P.gamma, g2 = 2.0 * P.gamma;
     double nv[3], q1[5], q2[5], qq[5], ds[3];
-    double* out = scratch + 4 * j;
     int f;
     if (j < nC) f = d.lc[j];
     else if (j < nC + nI) f = d.li[j - nC];
@@ -1341,17 +1443,29 @@ __global__ void __launch_bounds__(32) surface_faces_kernel(DevMesh d, gelios_par
     t1 /= nn;
     t2 /= nn;
     const double n1 = t2, n2 = -t1;
-    out[1] = n1;
-    out[2] = n2;
     nv[0] = n1; nv[1] = n2; nv[2] = 0.0;
+    double o0 = 0.0, o3 = 0.0;
+    // TVD states of the face (even lanes) and of its twin (odd lanes),
+    // exchanged between lane pairs
+    auto tvd_pair = [&](St5& pf, St5& pc) {
+        const St5 mine = face_tvd(d, st, b.cx, b.cy, (lane & 1) ? d.fcopy[f] : f, &status);
+        St5 other;
+        other.ro = __shfl_xor_sync(0xffffffffu, mine.ro, 1);
+        other.p = __shfl_xor_sync(0xffffffffu, mine.p, 1);
+        other.u = __shfl_xor_sync(0xffffffffu, mine.u, 1);
+        other.v = __shfl_xor_sync(0xffffffffu, mine.v, 1);
+        other.Q = __shfl_xor_sync(0xffffffffu, mine.Q, 1);
+        pf = (lane & 1) ? other : mine;
+        pc = (lane & 1) ? mine : other;
+    };
     if (j < nC) {
-        const St5 p1 = face_tvd(d, st, b.cx, b.cy, f, &status);
-        const St5 p2 = face_tvd(d, st, b.cx, b.cy, d.fcopy[f], &status);
+        St5 p1, p2;
+        tvd_pair(p1, p2);
         q1[0] = p1.ro; q1[1] = p1.p; q1[2] = p1.u; q1[3] = p1.v; q1[4] = 0.0;
         q2[0] = p2.ro; q2[1] = p2.p; q2[2] = p2.u; q2[3] = p2.v; q2[4] = 0.0;
-        godunov_dev(ga, P.kurant, q1, q2, nv, qq, ds, 0.0, 0.0, P.godunov_max_iter, &status);
-        out[0] = ds[2] * P.koef * 0.3;
-        out[3] = 0.0;
+        godunov_dev<true>(ga, P.kurant, q1, q2, nv, qq, ds, 0.0, 0.0, P.godunov_max_iter, &status);
+        o0 = ds[2] * P.koef * 0.3;
+        o3 = 0.0;
     } else if (j < nC + nI) {
         const int M = d.fmaster[f];
         St5 p1 = load_state(st, M);
@@ -1365,33 +1479,41 @@ __global__ void __launch_bounds__(32) surface_faces_kernel(DevMesh d, gelios_par
         polar_perenos(x, y, x2, y2, p1.u, p1.v);
         q1[0] = p1.ro; q1[1] = p1.p; q1[2] = p1.u; q1[3] = p1.v; q1[4] = 0.0;
         q2[0] = p2.ro; q2[1] = p2.p; q2[2] = p2.u; q2[3] = p2.v; q2[4] = 0.0;
-        godunov_dev(ga, P.kurant, q1, q2, nv, qq, ds, 0.0, 0.0, P.godunov_max_iter, &status);
-        out[0] = ds[0] * P.koef * 0.1;
+        godunov_dev<true>(ga, P.kurant, q1, q2, nv, qq, ds, 0.0, 0.0, P.godunov_max_iter, &status);
+        o0 = ds[0] * P.koef * 0.1;
         const double tt1 = -n2, tt2 = n1;
-        out[3] = (fabs(p2.u * tt1 + p2.v * tt2) < 0.1) ? 1.0 : 0.0;
+        o3 = (fabs(p2.u * tt1 + p2.v * tt2) < 0.1) ? 1.0 : 0.0;
     } else {
         const int jj = j - nC - nI;
         const int lim = P.n_outer_shock + d.dims[0] + d.dims[1] + 1;
         if (jj >= lim) {
-            out[0] = 0.0;
-            out[3] = -1.0;
+            o0 = 0.0;
+            o3 = -1.0;
         } else {
-            const St5 p1 = face_tvd(d, st, b.cx, b.cy, f, &status);
-            const St5 p2 = face_tvd(d, st, b.cx, b.cy, d.fcopy[f], &status);
+            St5 p1, p2;
+            tvd_pair(p1, p2);
             q1[0] = p1.ro; q1[1] = p1.p; q1[2] = p1.u; q1[3] = p1.v; q1[4] = 0.0;
             q2[0] = p2.ro; q2[1] = p2.p; q2[2] = p2.u; q2[3] = p2.v; q2[4] = 0.0;
-            godunov_dev(ga, P.kurant, q1, q2, nv, qq, ds, 0.0, 0.0, P.godunov_max_iter, &status);
-            out[0] = ds[1] * P.koef;
+            godunov_dev<true>(ga, P.kurant, q1, q2, nv, qq, ds, 0.0, 0.0, P.godunov_max_iter, &status);
+            o0 = ds[1] * P.koef;
             const double tt1 = -n2, tt2 = n1;
             double br;
             if ((sq(p1.u) + sq(p1.v) + sq(0.0)) / (ga * p1.p / p1.ro) > 1.0) br = 0.0;
             else if (fabs(p1.u * tt1 + p1.v * tt2) < 0.01) br = 1.0;
             else if (p1.u * tt1 + p1.v * tt2 > 0) br = 2.0;
             else br = 3.0;
-            out[3] = br;
+            o3 = br;
         }
     }
-    if (status) atomicOr(b.status, status);
+    status = static_cast<int>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(status)));
+    if (lane == 0) {
+        double* out = scratch + 4 * j;
+        out[0] = o0;
+        out[1] = n1;
+        out[2] = n2;
+        out[3] = o3;
+        if (status) atomicOr(b.status, status);
+    }
 }
 
 // Move_surface, part 2: node velocities.  The reference accumulates the face
@@ -1532,8 +1654,9 @@ __global__ void hllc_batch_kernel(gelios_params P, int n, const double* __restri
     o[8] = SR;
 }
 
+// One warp per problem (the warp-cooperative solver of the step kernels).
 __global__ void godunov_batch_kernel(gelios_params P, int n, const double* __restrict__ in, double* __restrict__ out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= n) return;
     const double* a = in + 15 * i;
     double q1[5], q2[5], nv[3], qq[5], ds[3];
@@ -1543,8 +1666,9 @@ __global__ void godunov_batch_kernel(gelios_params P, int n, const double* __res
     }
     nv[0] = a[10]; nv[1] = a[11]; nv[2] = a[12];
     int status = 0;
-    const double t = P.kurant * a[14] / godunov_dev(P.gamma, P.kurant, q1, q2, nv, qq, ds, a[13], a[14],
-                                                    P.godunov_max_iter, &status);
+    const double t = P.kurant * a[14] / godunov_dev<true>(P.gamma, P.kurant, q1, q2, nv, qq, ds, a[13], a[14],
+                                                          P.godunov_max_iter, &status);
+    if ((threadIdx.x & 31) != 0) return;
     double* o = out + 10 * i;
     o[0] = t;
     for (int k = 0; k < 5; k++) o[1 + k] = qq[k];
@@ -1582,20 +1706,26 @@ int launch_mk2_flux_plain(const DevMesh& d, const gelios_params& P, const StepBu
     const int nr = d.n_units - (d.u_tr1 - d.u_tr0);
     if (nr <= 0) return 0;
     if (P.precision == GELIOS_PREC_FP32_FLUX)
-        mk2_flux_kernel<float, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, b, rec, fl, nr);
+        mk2_flux_kernel<float, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, b, rec, fl, nullptr, nr);
     else
-        mk2_flux_kernel<double, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, b, rec, fl, nr);
+        mk2_flux_kernel<double, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, b, rec, fl, nullptr, nr);
+    return 1;
+}
+int launch_mk2_tracked_solve(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
+                             double* pstar, cudaStream_t s) {
+    const int nt = d.u_tr1 - d.u_tr0;
+    if (nt <= 0) return 0;
+    mk2_tracked_solve_kernel<<<blocks_for(nt, 2), 64, 0, s>>>(d, P, b, rec, pstar);
     return 1;
 }
 int launch_mk2_flux_tracked(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
-                            double* fl, cudaStream_t s) {
+                            const double* pstar, double* fl, cudaStream_t s) {
     const int nt = d.u_tr1 - d.u_tr0;
     if (nt <= 0) return 0;
-    // few units, long serial solves: small blocks spread them over the SMs
     if (P.precision == GELIOS_PREC_FP32_FLUX)
-        mk2_flux_kernel<float, true><<<blocks_for(nt, 32), 32, 0, s>>>(d, P, b, rec, fl, nt);
+        mk2_flux_kernel<float, true><<<blocks_for(nt, 32), 32, 0, s>>>(d, P, b, rec, fl, pstar, nt);
     else
-        mk2_flux_kernel<double, true><<<blocks_for(nt, 32), 32, 0, s>>>(d, P, b, rec, fl, nt);
+        mk2_flux_kernel<double, true><<<blocks_for(nt, 32), 32, 0, s>>>(d, P, b, rec, fl, pstar, nt);
     return 1;
 }
 void launch_mk2_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
@@ -1603,7 +1733,7 @@ void launch_mk2_update(const DevMesh& d, const gelios_params& P, const StepBuffe
     mk2_update_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, fl, aux);
 }
 void launch_mk2_source(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* aux, cudaStream_t s) {
-    mk2_source_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, aux);
+    mk2_source_kernel<<<blocks_for(4 * d.n_cells, 128), 128, 0, s>>>(d, P, b, aux);
 }
 void launch_inner(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const int32_t* list, int n,
                   cudaStream_t s) {
@@ -1621,7 +1751,7 @@ int launch_motion(const DevMesh& d, const gelios_params& P, const StepBuffers& b
     int launches = 0;
     const int nf = d.n_lc + d.n_li + d.n_lo;
     if (nf > 0) {
-        surface_faces_kernel<<<blocks_for(nf, 32), 32, 0, s>>>(d, P, b, scratch);
+        surface_faces_kernel<<<blocks_for(nf, 2), 64, 0, s>>>(d, P, b, scratch);
         const size_t shm = static_cast<size_t>(d.n_sp) * (2 * sizeof(double) + sizeof(int));
         static size_t shm_opted = 0;
         if (shm > 48 * 1024 && shm > shm_opted) {
@@ -1643,7 +1773,7 @@ void launch_hllc_batch(const gelios_params& P, int n, const double* in, double* 
     hllc_batch_kernel<<<blocks_for(n, 128), 128, 0, s>>>(P, n, in, out);
 }
 void launch_godunov_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s) {
-    godunov_batch_kernel<<<blocks_for(n, 128), 128, 0, s>>>(P, n, in, out);
+    godunov_batch_kernel<<<blocks_for(n, 2), 64, 0, s>>>(P, n, in, out);
 }
 
 }  // namespace gelios

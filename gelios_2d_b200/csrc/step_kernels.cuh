@@ -85,8 +85,10 @@ void launch_stationary_update(const DevMesh& d, const gelios_params& P, const St
 void launch_mk2_recon(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* rec, cudaStream_t s);
 int launch_mk2_flux_plain(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
                           double* fl, cudaStream_t s);
+int launch_mk2_tracked_solve(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
+                             double* pstar, cudaStream_t s);
 int launch_mk2_flux_tracked(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
-                            double* fl, cudaStream_t s);
+                            const double* pstar, double* fl, cudaStream_t s);
 void launch_mk2_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
                        const double* aux, cudaStream_t s);
 void launch_mk2_source(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* aux, cudaStream_t s);
