@@ -85,15 +85,16 @@ struct gelios_ctx {
     // motion runs there while the main stream moves the grid
     cudaStream_t side = nullptr;   // face reconstructions, tracked-face star pressures
     cudaStream_t side2 = nullptr;  // charge-exchange source terms
-    cudaEvent_t ev_fork = nullptr, ev_recon = nullptr, ev_solve = nullptr, ev_source = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_recon = nullptr, ev_rails = nullptr, ev_tracked = nullptr,
+                ev_source = nullptr;
     gelios_params prm{};
     bool have_mesh = false;
     DevMesh d;
     // topology / geometry
-    DBuf X, Y, X2, Y2, Vx, Vy, cnt, ptype, cstart, contour, gstart, cflags, sA, sB, snb, ssd, ssd2, sinfo;
+    DBuf X, Y, X2, Y2, ptype, cstart, contour, gstart, cflags, sA, sB, snb, ssd, ssd2, sinfo;
     DBuf fA, fB, ftype, fmaster, fsosed, fcopy, fsdown;
     DBuf rtype, rM, rpstart, rpts, rkstart, rkeys, rs;
-    DBuf lc, li, lo, sp_point, sp_line, sp_inc, sp_ainc, sp_fix;
+    DBuf lc, li, lo, sp_point, sp_line, sp_inc, sp_ainc, sp_fix, sp_of_point;
     DBuf u_slot, u_cell, u_twin, flux, aux, rec, pstar, src_lo;
     DBuf Hn, Hu, Hv, HT, ku, kv, kT, r_istoch, cback, cnext;
     // state par[2] x 5 fields, centroids [2], scratch
@@ -223,7 +224,8 @@ extern "C" int gelios_create(gelios_ctx** out, const gelios_params* prm, int dev
     GELIOS_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->side2, cudaStreamNonBlocking, prio_least));
     GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
     GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_recon, cudaEventDisableTiming));
-    GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_solve, cudaEventDisableTiming));
+    GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_rails, cudaEventDisableTiming));
+    GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_tracked, cudaEventDisableTiming));
     GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_source, cudaEventDisableTiming));
     if (ctx->words.alloc(64)) return GELIOS_E_CUDA;
     GELIOS_CUDA_TRY(cudaMemsetAsync(ctx->words.p, 0, 64, ctx->stream));
@@ -250,7 +252,7 @@ extern "C" void gelios_destroy(gelios_ctx* ctx) {
             cudaStreamSynchronize(*sp);
             cudaStreamDestroy(*sp);
         }
-    for (cudaEvent_t e : {ctx->ev_fork, ctx->ev_recon, ctx->ev_solve, ctx->ev_source})
+    for (cudaEvent_t e : {ctx->ev_fork, ctx->ev_recon, ctx->ev_rails, ctx->ev_tracked, ctx->ev_source})
         if (e) cudaEventDestroy(e);
     delete ctx;
 }
@@ -411,10 +413,10 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
                 return GELIOS_E_MESH;
             }
     }
-    // surface-tracking nodes (see surface_nodes_kernel)
+    // surface-tracking nodes (see point_velocity)
     std::vector<int32_t> sp_point, sp_line, sp_inc, sp_ainc, sp_fix(12, 0);
+    std::vector<int32_t> local(np, -1);
     {
-        std::vector<int32_t> local(np, -1);
         const int32_t* lines[3] = {v->line_contact, v->line_inner, v->line_outer};
         const int nl[3] = {v->n_contact, v->n_inner_line, v->n_outer_line};
         int base = 0;
@@ -470,18 +472,11 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
         }
     }
     const int n_sp = static_cast<int>(sp_point.size());
-    if (n_sp * (2 * sizeof(double) + sizeof(int)) > 200 * 1024) {
-        set_error("gelios_upload_topology: too many tracked-line points for one CTA");
-        return GELIOS_E_LIMIT;
-    }
     int rc = 0;
     rc |= upload(ctx->X, v->x, np, s);
     rc |= upload(ctx->Y, v->y, np, s);
     rc |= upload(ctx->X2, v->x, np, s);
     rc |= upload(ctx->Y2, v->y, np, s);
-    rc |= upload<double>(ctx->Vx, nullptr, np, s);
-    rc |= upload<double>(ctx->Vy, nullptr, np, s);
-    rc |= upload<int32_t>(ctx->cnt, nullptr, np, s);
     rc |= upload(ctx->ptype, v->point_type, np, s);
     rc |= upload(ctx->cstart, v->contour_start, nc + 1, s);
     rc |= upload(ctx->contour, v->contour, v->contour_start[nc], s);
@@ -525,6 +520,7 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     rc |= upload(ctx->sp_inc, sp_inc.data(), sp_inc.size(), s);
     rc |= upload(ctx->sp_ainc, sp_ainc.data(), sp_ainc.size(), s);
     rc |= upload(ctx->sp_fix, sp_fix.data(), sp_fix.size(), s);
+    rc |= upload(ctx->sp_of_point, local.data(), local.size(), s);
     rc |= upload<double>(ctx->Hn, nullptr, 4 * static_cast<size_t>(nc), s);
     rc |= upload<double>(ctx->Hu, nullptr, 4 * static_cast<size_t>(nc), s);
     rc |= upload<double>(ctx->Hv, nullptr, 4 * static_cast<size_t>(nc), s);
@@ -566,9 +562,6 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     d.Y = ctx->Y.as<double>();
     d.X2 = ctx->X2.as<double>();
     d.Y2 = ctx->Y2.as<double>();
-    d.Vx = ctx->Vx.as<double>();
-    d.Vy = ctx->Vy.as<double>();
-    d.cnt = ctx->cnt.as<int>();
     d.ptype = ctx->ptype.as<int32_t>();
     d.cstart = ctx->cstart.as<int32_t>();
     d.contour = ctx->contour.as<int32_t>();
@@ -617,6 +610,7 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     d.sp_inc = ctx->sp_inc.as<int32_t>();
     d.sp_ainc = ctx->sp_ainc.as<int32_t>();
     d.sp_fix = ctx->sp_fix.as<int32_t>();
+    d.sp_of_point = ctx->sp_of_point.as<int32_t>();
     d.Hn = ctx->Hn.as<double>();
     d.Hu = ctx->Hu.as<double>();
     d.Hv = ctx->Hv.as<double>();
@@ -759,12 +753,13 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             b.cy_next = cn + d.n_cells;
             b.rp_next = cn + 2 * static_cast<size_t>(d.n_cells);
             // Three streams per step.
-            //   side:  face reconstructions, then the star pressures of the
-            //          tracked faces (neither depends on the motion);
+            //   side:  face reconstructions, the star pressures of the tracked
+            //          faces (neither depends on the motion), then, once the
+            //          rails have moved, the tracked-face fluxes (sampling of
+            //          the solved Riemann problems at the face speed);
             //   side2: charge-exchange source terms and pre-motion volumes;
-            //   main:  surface tracking + rails, the face fluxes (the tracked
-            //          ones sample the pre-solved Riemann problems at the
-            //          moved face speed), the cell update, the commit.
+            //   main:  surface tracking + rails, the other face fluxes, the
+            //          cell update, the commit.
             cudaStream_t sd = ctx->side, sd2 = ctx->side2;
             GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_fork, s));
             GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_fork, 0));
@@ -772,20 +767,22 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             launch_mk2_recon(d, P, b, ctx->rec.as<double>(), sd);
             GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_recon, sd));
             const int nsv = launch_mk2_tracked_solve(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(), sd);
-            GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_solve, sd));
             launch_mk2_source(d, P, b, ctx->aux.as<double>(), sd2);
             GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_source, sd2));
             cudaEvent_t e1 = ctx->phase_begin();
             const int nm = launch_motion(d, P, b, ctx->surface.as<double>(), s);
             ctx->phase_end(2, e1, nm);  // Move_surface + rails
+            GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_rails, s));
+            GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_rails, 0));
+            const int nft = launch_mk2_flux_tracked(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(),
+                                                    ctx->flux.as<double>(), sd);
+            GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_tracked, sd));
             GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_recon, 0));
             cudaEvent_t e3 = ctx->phase_begin();
-            int nfl = launch_mk2_flux_plain(d, P, b, ctx->rec.as<double>(), ctx->flux.as<double>(), s);
-            GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_solve, 0));
-            nfl += launch_mk2_flux_tracked(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(),
-                                           ctx->flux.as<double>(), s);
+            const int nfl = launch_mk2_flux_plain(d, P, b, ctx->rec.as<double>(), ctx->flux.as<double>(), s) + nft;
             ctx->phase_end(1, e3, nfl);
-            // the update reads the source terms
+            // the update reads the tracked-face fluxes and the source terms
+            GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_tracked, 0));
             GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_source, 0));
             cudaEvent_t e5 = ctx->phase_begin();
             launch_mk2_update(d, P, b, ctx->flux.as<double>(), ctx->aux.as<double>(), s);

@@ -1,16 +1,23 @@
 // sm_100a kernels of the Gelios_2D plasma time step.
 //
-// One time step of Setka::Go_5_komponent__MK2 (Setka.cpp:10121-10482) is
-//   surface_*_kernel Move_surface (Setka.cpp:3378-3844): tracked-face exact
-//                    Godunov speeds (one thread per face), then node velocities
-//                    replayed per node in the reference's operation order
-//   rails_kernel     Move_Setka_Calculate_2 (Setka.cpp:4324-4759): one CTA per
-//                    rail; the points C_Rails[0] shares with the last B rail
-//                    and with the D rails keep the reference's pass order
-//   mk2_cell_kernel  per-cell flux accumulation in Grans order, charge-exchange
-//                    source, conservative ALE update, next-step centroid,
-//                    block-min of the CFL candidates
-//   commit_kernel    x = x2, V = 0, count = 0; dt of the next step
+// One time step of Setka::Go_5_komponent__MK2 (Setka.cpp:10121-10482) is,
+// on three streams:
+//   mk2_recon_kernel          TVD states of every face unit (pre-motion)
+//   mk2_tracked_solve_kernel  star pressures of the tracked faces' exact
+//                             Riemann problems (warp per face)
+//   mk2_source_kernel         charge-exchange source (Get_Sourse_MK1), four
+//                             lanes per cell; pre-motion areas and volumes
+//   surface_faces_kernel      Move_surface (Setka.cpp:3378-3844): exact
+//                             Godunov speeds of the tracked faces (warp per
+//                             face)
+//   rails_kernel              node velocities of the key points, then
+//                             Move_Setka_Calculate_2 (Setka.cpp:4324-4759):
+//                             one CTA per rail
+//   mk2_flux_kernel           face speed from the moved points, HLL fluxes;
+//                             tracked faces sample their Riemann solution
+//   mk2_update_kernel         per-cell flux sums in Grans order, conservative
+//                             ALE update, next-step centroid, CFL block-min
+//   commit_kernel             x = x2; dt of the next step
 // Go_stationary (Setka.cpp:5205-5343) and
 // Go_stationary_5_komponent_inner_MK2 (Setka.cpp:6999-7212) are
 // stationary_cell_kernel / inner_cell_kernel + dt_finalize_kernel.
@@ -1182,7 +1189,8 @@ __global__ void dt_finalize_kernel(StepBuffers b) {
     *b.dt_acc = 0x7ff0000000000000ULL;
 }
 
-// x = x2, y = y2, V = 0, count = 0 (Setka.cpp:10473-10480) + dt finalisation.
+// x = x2, y = y2 (Setka.cpp:10473-10480; the zeroed V and count are never
+// stored, see point_velocity) + dt finalisation.
 __global__ void commit_kernel(DevMesh d, StepBuffers b) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
@@ -1194,9 +1202,131 @@ __global__ void commit_kernel(DevMesh d, StepBuffers b) {
     if (i < d.n_points) {
         d.X[i] = d.X2[i];
         d.Y[i] = d.Y2[i];
-        d.Vx[i] = 0.0;
-        d.Vy[i] = 0.0;
-        d.cnt[i] = 0;
+    }
+}
+
+// ------------------------------------------------------------------ node velocities
+// Move_surface, part 2 (Setka.cpp:3522-3535, 3718-3736, 3829-3842): the
+// velocity of a tracked-surface node.  The reference accumulates the face
+// speeds into Point::Vx/Vy/count in one serial pass per line, runs three
+// averaging loops that all walk Line_Contact, and fixes up the end nodes of
+// each line in between.  The three lines touch disjoint point sets, so the
+// value of one node depends only on its own face incidences (sp_inc, in line
+// order), on the averaging passes in which it is the A end of a contact face
+// (sp_ainc), and, for the end nodes, on the first-pass values of the other
+// end nodes of its line.  point_velocity replays exactly those operations for
+// one point, so the rails can evaluate their key points directly from the
+// per-face speeds (bit-identical to the serial passes).
+__device__ __forceinline__ void node_pass1(const DevMesh& d, const double* __restrict__ scratch, int i, double& v,
+                                           double& w, int& c) {
+    const int line = d.sp_line[i];
+    v = 0.0;
+    w = 0.0;
+    c = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int e = d.sp_inc[4 * i + k];
+        if (e < 0) break;
+        const int j = e >> 1, role = e & 1;  // role 0: A end, 1: B end
+        const double* f = scratch + 4 * j;
+        const double br = f[3];
+        bool add;
+        if (line == 0) add = role == 1;
+        else if (line == 1) add = role == 1 || br != 0.0;
+        else add = (br == 1.0) || (role == 1 && (br == 0.0 || br == 2.0)) || (role == 0 && br == 3.0);
+        if (add) {
+            v += f[0] * f[1];
+            w += f[0] * f[2];
+            c++;
+        }
+    }
+    if (line == 0) {  // first averaging pass: every contact face (Setka.cpp:3522-3530)
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int j = d.sp_ainc[4 * i + k];
+            if (j < 0) break;
+            if (c > 0) {
+                v /= (1.0 * c);
+                w /= (1.0 * c);
+            }
+        }
+    }
+}
+
+// Vx, Vy of point p after Move_surface (0 for points off the tracked lines:
+// every step starts from zero velocities, Setka.cpp:10473-10480).
+__device__ void point_velocity(const DevMesh& d, const double* __restrict__ scratch, double dt, int p, double& vx,
+                               double& vy) {
+    const int i = d.sp_of_point[p];
+    vx = 0.0;
+    vy = 0.0;
+    if (i < 0) return;
+    int c;
+    node_pass1(d, scratch, i, vx, vy, c);
+    const int line = d.sp_line[i];
+    const int32_t* fx = d.sp_fix + 4 * line;  // a0, b0 (first face), a_last, b_last
+    if (i == fx[0] || i == fx[3]) {
+        // replay the end-node fix-ups of this line in the reference's order
+        // on local copies of the four end nodes (aliases kept in sync)
+        int id[4];
+        double lx[4], ly[4];
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            id[m] = fx[m];
+            int cm;
+            node_pass1(d, scratch, id[m], lx[m], ly[m], cm);
+        }
+        auto setx = [&](int node, double val) {
+#pragma unroll
+            for (int m = 0; m < 4; m++)
+                if (id[m] == node) lx[m] = val;
+        };
+        auto sety = [&](int node, double val) {
+#pragma unroll
+            for (int m = 0; m < 4; m++)
+                if (id[m] == node) ly[m] = val;
+        };
+        const double* X = d.X;
+        const double* Y = d.Y;
+        const int pa0 = d.sp_point[id[0]], pb0 = d.sp_point[id[1]], pa1 = d.sp_point[id[2]], pb1 = d.sp_point[id[3]];
+        // fx[0]: vx[a0] = vx[b0] + (X[b0] - X[a0]) / dt on every line
+        setx(id[0], lx[1] + (X[pb0] - X[pa0]) / dt);
+        if (line == 1) {
+            // inner shock: vx[b1] = vx[a1] + (X[a1] - X[b1]) / dt (Setka.cpp:3733-3736)
+            double a1x = lx[2];
+#pragma unroll
+            for (int m = 0; m < 4; m++)
+                if (id[m] == id[2]) a1x = lx[m];
+            setx(id[3], a1x + (X[pa1] - X[pb1]) / dt);
+        } else {
+            // contact / outer shock: vy[b1] = vy[a1] + (Y[a1] - Y[b1]) / dt
+            sety(id[3], ly[2] + (Y[pa1] - Y[pb1]) / dt);
+        }
+#pragma unroll
+        for (int m = 0; m < 4; m++)
+            if (id[m] == i) {
+                vx = lx[m];
+                vy = ly[m];
+            }
+    }
+    if (line == 0) {
+        // second and third passes walk Line_Contact up to the inner/outer
+        // line lengths (Setka.cpp:3718-3731, 3829-3837)
+        const int nC = d.n_lc, nI = d.n_li, nO = d.n_lo;
+        const int lim2 = nI > 0 ? (nI < nC ? nI : nC) : 0;
+        const int lim3 = nO > 0 ? (nO < nC ? nO : nC) : 0;
+        for (int pass = 0; pass < 2; pass++) {
+            const int lim = pass == 0 ? lim2 : lim3;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int j = d.sp_ainc[4 * i + k];
+                if (j < 0) break;
+                if (j < lim && c > 0) {
+                    vx /= (1.0 * c);
+                    vy /= (1.0 * c);
+                }
+            }
+        }
     }
 }
 
@@ -1211,15 +1341,17 @@ __global__ void commit_kernel(DevMesh d, StepBuffers b) {
 //  * the first point of every D rail is a point of C_Rails[0]; the D block
 //    recomputes that point's new position from C_Rails[0]'s key point with
 //    the same operations (bit-identical to reading it back).
-__device__ __forceinline__ void c0_key(const DevMesh& d, int q, double dt, double& x2, double& y2) {
+__device__ __forceinline__ void c0_key(const DevMesh& d, int q, double dt, double vx, double vy, double& x2,
+                                       double& y2) {
     const int K0 = d.rkeys[d.rkstart[q]];
     const double s = d.rs[q], cs = cos(s), sn = sin(s);
-    const double V = d.Vx[K0] * cs + d.Vy[K0] * sn;
+    const double V = vx * cs + vy * sn;
     x2 = d.X[K0] + dt * V * cs;
     y2 = d.Y[K0] + dt * V * sn;
 }
 
-__global__ void __launch_bounds__(128) rails_kernel(DevMesh d, gelios_params P, const double* __restrict__ dtp) {
+__global__ void __launch_bounds__(128) rails_kernel(DevMesh d, gelios_params P, const double* __restrict__ dtp,
+                                                    const double* __restrict__ scratch) {
     const int q = blockIdx.x;
     const double dt = *dtp;
     const int32_t* ap = d.rpts + d.rpstart[q];
@@ -1236,6 +1368,27 @@ __global__ void __launch_bounds__(128) rails_kernel(DevMesh d, gelios_params P, 
     const double* Y = d.Y;
     __shared__ double sh[6];
     const int ni = P.n_inner;
+    // velocities of the key points this rail reads, one thread each
+    __shared__ double kvx[4], kvy[4];
+    if (threadIdx.x < 4) {
+        int pt = -1;
+        const int k = threadIdx.x;
+        if (t == 0 || t == 1) {
+            if (k < 3) pt = kp[k];
+        } else if (t == 2) {
+            if (k == 0) pt = kp[0];
+        } else {
+            if (k == 0) pt = d.rkeys[d.rkstart[first_c]];  // key point 0 of C_Rails[0]
+            else if (k < 3) pt = kp[k];
+            else if (q - first_d >= P.n_outer_shock && P.n_outer_shock >= 1)
+                pt = d.rkeys[d.rkstart[first_d + P.n_outer_shock - 1] + 2];
+        }
+        double vx = 0.0, vy = 0.0;
+        if (pt >= 0) point_velocity(d, scratch, dt, pt, vx, vy);
+        kvx[k] = vx;
+        kvy[k] = vy;
+    }
+    __syncthreads();
     if (t == 0 || t == 1 || t == 2) {
         const double s = d.rs[q];
         const double cs = cos(s), sn = sin(s);
@@ -1243,7 +1396,7 @@ __global__ void __launch_bounds__(128) rails_kernel(DevMesh d, gelios_params P, 
             if (t == 0) {  // A rail, Setka.cpp:4331-4356
                 for (int kk = 0; kk < 3; kk++) {
                     const int K = kp[kk];
-                    const double V = d.Vx[K] * cs + d.Vy[K] * sn;
+                    const double V = kvx[kk] * cs + kvy[kk] * sn;
                     X2[K] = X[K] + dt * V * cs;
                     Y2[K] = Y[K] + dt * V * sn;
                 }
@@ -1254,16 +1407,16 @@ __global__ void __launch_bounds__(128) rails_kernel(DevMesh d, gelios_params P, 
                 sh[2] = sqrt(sq(X2[kp[2]]) + sq(Y2[kp[2]]));
             } else if (t == 1) {  // B rail, Setka.cpp:4469-4502
                 const int K0 = kp[0], K1 = kp[1], K2 = kp[2], K3 = kp[3];
-                double V = d.Vx[K0] * cs + d.Vy[K0] * sn;
+                double V = kvx[0] * cs + kvy[0] * sn;
                 const double x0 = X[K0] + dt * V * cs, y0 = Y[K0] + dt * V * sn;
                 if (!handoff) {
                     X2[K0] = x0;
                     Y2[K0] = y0;
                 }
-                V = d.Vx[K1] * 0.0 + d.Vy[K1] * 1.0;
+                V = kvx[1] * 0.0 + kvy[1] * 1.0;
                 X2[K1] = x0;
                 Y2[K1] = Y[K1] + dt * V;
-                V = d.Vx[K2] * 0.0 + d.Vy[K2] * 1.0;
+                V = kvx[2] * 0.0 + kvy[2] * 1.0;
                 X2[K2] = x0;
                 Y2[K2] = Y[K2] + dt * V;
                 X2[K3] = x0;
@@ -1275,7 +1428,7 @@ __global__ void __launch_bounds__(128) rails_kernel(DevMesh d, gelios_params P, 
                 sh[4] = y0;
             } else {  // C rail, Setka.cpp:4603-4614
                 const int K0 = kp[0], K1 = kp[1];
-                const double V = d.Vx[K0] * cs + d.Vy[K0] * sn;
+                const double V = kvx[0] * cs + kvy[0] * sn;
                 X2[K0] = X[K0] + dt * V * cs;
                 Y2[K0] = Y[K0] + dt * V * sn;
                 X2[K1] = P.Left;
@@ -1352,21 +1505,21 @@ __global__ void __launch_bounds__(128) rails_kernel(DevMesh d, gelios_params P, 
         const int K1 = kp[1], K2 = kp[2], K3 = kp[3];
         // key point 0 = point M1 + jj of C_Rails[0], as the C pass moves it
         double c0x, c0y;
-        c0_key(d, first_c, dt, c0x, c0y);
+        c0_key(d, first_c, dt, kvx[0], kvy[0], c0x, c0y);
         const int Mc1 = d.rM[4 * first_c], Mc2 = d.rM[4 * first_c + 1];
         const int j = Mc1 + jj;
         const double xr = pow(P.Left / (c0x), 1.0 / (Mc2));
         const double x0 = c0x * pow(xr, static_cast<double>(j + 1 - Mc1));
         const double y0 = c0y;
-        double V = d.Vy[K1];
+        double V = kvy[1];
         X2[K1] = x0;
         Y2[K1] = Y[K1] + dt * V;
-        V = d.Vy[K2];
+        V = kvy[2];
         X2[K2] = x0;
         if (jj >= P.n_outer_shock && P.n_outer_shock >= 1) {
             const int qs = first_d + P.n_outer_shock - 1;
             const int Ks = d.rkeys[d.rkstart[qs] + 2];
-            Y2[K2] = Y[Ks] + dt * d.Vy[Ks];
+            Y2[K2] = Y[Ks] + dt * kvy[3];
         } else {
             Y2[K2] = Y[K2] + dt * V;
         }
@@ -1516,110 +1669,6 @@ __global__ void __launch_bounds__(64) surface_faces_kernel(DevMesh d, gelios_par
     }
 }
 
-// Move_surface, part 2: node velocities.  The reference accumulates the face
-// speeds into Point::Vx/Vy/count in one serial pass per line, then runs three
-// averaging loops that all walk Line_Contact (Setka.cpp:3522-3530, 3718-3731,
-// 3829-3837) with end-node fix-ups between them.  The three lines touch
-// disjoint point sets (P_Contact, P_Inner_shock, P_Outer_shock), so each node
-// replays, on its own, exactly the ordered operations the serial code applies
-// to it: its face incidences in line order (sp_inc), then, for contact nodes,
-// one division per averaging pass in which it is the A end of a contact face
-// (sp_ainc).  Fix-ups run on one thread between the first and the later
-// passes, as in the reference.  Every node's result is bit-identical to the
-// serial code.
-__global__ void __launch_bounds__(512) surface_nodes_kernel(DevMesh d, StepBuffers b,
-                                                            const double* __restrict__ scratch) {
-    extern __shared__ double sm[];
-    const int n = d.n_sp;
-    double* vx = sm;
-    double* vy = sm + n;
-    int* cn = reinterpret_cast<int*>(sm + 2 * n);
-    const int nC = d.n_lc, nI = d.n_li, nO = d.n_lo;
-    const double dt = *b.dt_cur;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const int line = d.sp_line[i];
-        double v = 0.0, w = 0.0;
-        int c = 0;
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const int e = d.sp_inc[4 * i + k];
-            if (e < 0) break;
-            const int j = e >> 1, role = e & 1;  // role 0: A end, 1: B end
-            const double* f = scratch + 4 * j;
-            const double br = f[3];
-            bool add;
-            if (line == 0) add = role == 1;
-            else if (line == 1) add = role == 1 || br != 0.0;
-            else add = (br == 1.0) || (role == 1 && (br == 0.0 || br == 2.0)) || (role == 0 && br == 3.0);
-            if (add) {
-                v += f[0] * f[1];
-                w += f[0] * f[2];
-                c++;
-            }
-        }
-        if (line == 0) {  // first averaging pass: every contact face (Setka.cpp:3522-3530)
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const int j = d.sp_ainc[4 * i + k];
-                if (j < 0) break;
-                if (c > 0) {
-                    v /= (1.0 * c);
-                    w /= (1.0 * c);
-                }
-            }
-        }
-        vx[i] = v;
-        vy[i] = w;
-        cn[i] = c;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const int32_t* fx = d.sp_fix;  // local ids of a0, b0, a_last, b_last per line
-        if (nC > 0) {
-            const int a0 = fx[0], b0 = fx[1], a1 = fx[2], b1 = fx[3];
-            vx[a0] = vx[b0] + (d.X[d.sp_point[b0]] - d.X[d.sp_point[a0]]) / dt;
-            vy[b1] = vy[a1] + (d.Y[d.sp_point[a1]] - d.Y[d.sp_point[b1]]) / dt;
-        }
-        if (nI > 0) {
-            const int a0 = fx[4], b0 = fx[5], a1 = fx[6], b1 = fx[7];
-            vx[a0] = vx[b0] + (d.X[d.sp_point[b0]] - d.X[d.sp_point[a0]]) / dt;
-            vx[b1] = vx[a1] + (d.X[d.sp_point[a1]] - d.X[d.sp_point[b1]]) / dt;
-        }
-        if (nO > 0) {
-            const int a0 = fx[8], b0 = fx[9], a1 = fx[10], b1 = fx[11];
-            vx[a0] = vx[b0] + (d.X[d.sp_point[b0]] - d.X[d.sp_point[a0]]) / dt;
-            vy[b1] = vy[a1] + (d.Y[d.sp_point[a1]] - d.Y[d.sp_point[b1]]) / dt;
-        }
-    }
-    __syncthreads();
-    const int lim2 = nI > 0 ? (nI < nC ? nI : nC) : 0;
-    const int lim3 = nO > 0 ? (nO < nC ? nO : nC) : 0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        double v = vx[i], w = vy[i];
-        const int c = cn[i];
-        if (d.sp_line[i] == 0) {
-            // second and third passes walk Line_Contact up to the inner/outer
-            // line lengths (Setka.cpp:3718-3731, 3829-3837)
-            for (int pass = 0; pass < 2; pass++) {
-                const int lim = pass == 0 ? lim2 : lim3;
-#pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const int j = d.sp_ainc[4 * i + k];
-                    if (j < 0) break;
-                    if (j < lim && c > 0) {
-                        v /= (1.0 * c);
-                        w /= (1.0 * c);
-                    }
-                }
-            }
-        }
-        const int p = d.sp_point[i];
-        d.Vx[p] = v;
-        d.Vy[p] = w;
-        d.cnt[p] = c;
-    }
-}
-
 // ------------------------------------------------------------------ per-face batches (known-answer checks)
 __global__ void hllc_batch_kernel(gelios_params P, int n, const double* __restrict__ in, double* __restrict__ out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1752,19 +1801,11 @@ int launch_motion(const DevMesh& d, const gelios_params& P, const StepBuffers& b
     const int nf = d.n_lc + d.n_li + d.n_lo;
     if (nf > 0) {
         surface_faces_kernel<<<blocks_for(nf, 2), 64, 0, s>>>(d, P, b, scratch);
-        const size_t shm = static_cast<size_t>(d.n_sp) * (2 * sizeof(double) + sizeof(int));
-        static size_t shm_opted = 0;
-        if (shm > 48 * 1024 && shm > shm_opted) {
-            cudaFuncSetAttribute(surface_nodes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(shm));
-            shm_opted = shm;
-        }
-        surface_nodes_kernel<<<1, 512, shm, s>>>(d, b, scratch);
-        launches += 2;
+        launches += 1;
     }
     const int nr = d.n_rail_a + d.n_rail_b + d.n_rail_c + d.n_rail_d;
     if (nr > 0) {
-        rails_kernel<<<nr, 128, 0, s>>>(d, P, b.dt_cur);
+        rails_kernel<<<nr, 128, 0, s>>>(d, P, b.dt_cur, scratch);
         launches++;
     }
     return launches;

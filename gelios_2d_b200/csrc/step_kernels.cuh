@@ -21,8 +21,7 @@ namespace gelios {
 struct DevMesh {
     int n_points = 0, n_cells = 0, n_faces = 0, n_main = 0;
     int dims[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    double *X = nullptr, *Y = nullptr, *X2 = nullptr, *Y2 = nullptr, *Vx = nullptr, *Vy = nullptr;
-    int* cnt = nullptr;
+    double *X = nullptr, *Y = nullptr, *X2 = nullptr, *Y2 = nullptr;
     const int32_t* ptype = nullptr;
     const int32_t *cstart = nullptr, *contour = nullptr, *gstart = nullptr;
     const uint32_t* cflags = nullptr;
@@ -49,6 +48,7 @@ struct DevMesh {
     int n_sp = 0;
     const int32_t *sp_point = nullptr, *sp_line = nullptr, *sp_inc = nullptr, *sp_ainc = nullptr,
                   *sp_fix = nullptr;
+    const int32_t* sp_of_point = nullptr;  // tracked-surface node of each point, -1 if none
     const double *Hn = nullptr, *Hu = nullptr, *Hv = nullptr, *HT = nullptr, *ku = nullptr, *kv = nullptr,
                  *kT = nullptr, *r_istoch = nullptr;
     const int32_t *cback = nullptr, *cnext = nullptr;
