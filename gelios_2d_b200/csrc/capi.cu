@@ -95,7 +95,7 @@ struct gelios_ctx {
     DBuf fA, fB, ftype, fmaster, fsosed, fcopy, fsdown;
     DBuf rtype, rM, rpstart, rpts, rkstart, rkeys, rs;
     DBuf lc, li, lo, sp_point, sp_line, sp_inc, sp_ainc, sp_fix, sp_of_point;
-    DBuf u_slot, u_cell, u_twin, flux, aux, rec, pstar, src_lo;
+    DBuf u_slot, u_cell, u_twin, u_A, u_B, u_info, flux, aux, rec, pstar, src_lo;
     DBuf Hn, Hu, Hv, HT, ku, kv, kT, r_istoch, cback, cnext;
     // state par[2] x 5 fields, centroids [2], scratch
     DBuf state[2];
@@ -106,6 +106,23 @@ struct gelios_ctx {
     int n_inner = 0;
     int n_sp = 0;
     bool cen_valid = false;  // cen[0] holds the centroids of the current points
+    // Instantiated graphs of one moving-grid step, keyed by the buffers the
+    // step reads (state parity and centroid buffer); dropped whenever the
+    // topology or the parameters change.
+    struct StepGraph {
+        int parity = -1;
+        const void* cen = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        int launches = 0;
+    };
+    StepGraph graphs[4];
+    bool graphs_off = false;  // capture failed once: launch directly
+    void drop_graphs() {
+        for (auto& g : graphs) {
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+            g = StepGraph{};
+        }
+    }
     int64_t launches = 0;
     // phase timing
     bool timing = false;
@@ -130,8 +147,8 @@ struct gelios_ctx {
         return e;
     }
     void phase_end(int phase, cudaEvent_t begin, int n_launch) {
-        phase_launch[phase] += n_launch;
         if (!timing || !begin) return;
+        phase_launch[phase] += n_launch;
         cudaEvent_t e = event();
         cudaEventRecord(e, stream);
         pending.push_back({phase, {begin, e}});
@@ -148,6 +165,7 @@ struct gelios_ctx {
         ev_used = 0;
     }
     ~gelios_ctx() {
+        drop_graphs();
         for (auto e : ev_pool) cudaEventDestroy(e);
     }
 
@@ -237,6 +255,7 @@ extern "C" int gelios_set_params(gelios_ctx* ctx, const gelios_params* prm) {
     if (!ctx || !prm) return GELIOS_E_ARG;
     ctx->prm = *prm;
     ctx->cen_valid = false;  // the cached |centroid|^(2 gamma) depends on gamma
+    ctx->drop_graphs();      // the parameters are kernel arguments
     return GELIOS_OK;
 }
 
@@ -259,6 +278,7 @@ extern "C" void gelios_destroy(gelios_ctx* ctx) {
 
 extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v) {
     if (!ctx || !v) return GELIOS_E_ARG;
+    ctx->drop_graphs();  // they hold the buffers about to be replaced
     if (v->n_points <= 0 || v->n_cells <= 0 || v->n_faces <= 0 || !v->x || !v->y || !v->point_type ||
         !v->cell_type || !v->contour_start || !v->contour || !v->gran_start || !v->gran || !v->face_A || !v->face_B ||
         !v->face_type || !v->face_master || !v->face_sosed || !v->face_copy) {
@@ -509,11 +529,25 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     rc |= upload(ctx->li, v->line_inner, v->n_inner_line, s);
     rc |= upload(ctx->lo, v->line_outer, v->n_outer_line, s);
     rc |= upload(ctx->u_slot, u_slot.data(), u_slot.size(), s);
+    {
+        // end points and slot info of each unit's face (unit-major copies)
+        const size_t nu = u_slot.size();
+        std::vector<int32_t> uA(nu), uB(nu);
+        std::vector<uint32_t> ui(nu);
+        for (size_t u = 0; u < nu; u++) {
+            uA[u] = sA[u_slot[u]];
+            uB[u] = sB[u_slot[u]];
+            ui[u] = sinfo[u_slot[u]];
+        }
+        rc |= upload(ctx->u_A, uA.data(), nu, s);
+        rc |= upload(ctx->u_B, uB.data(), nu, s);
+        rc |= upload(ctx->u_info, ui.data(), nu, s);
+    }
     rc |= upload(ctx->u_cell, u_cell.data(), u_cell.size(), s);
     rc |= upload(ctx->u_twin, u_twin.data(), u_twin.size(), s);
     rc |= upload<double>(ctx->flux, nullptr, 5 * static_cast<size_t>(ng), s);
     rc |= upload<double>(ctx->aux, nullptr, 5 * static_cast<size_t>(nc), s);
-    rc |= upload<double>(ctx->rec, nullptr, 10 * u_slot.size(), s);
+    rc |= upload<double>(ctx->rec, nullptr, static_cast<size_t>(kRecRows) * u_slot.size(), s);
     rc |= upload<double>(ctx->pstar, nullptr, static_cast<size_t>(u_tr1 - u_tr0) + 1, s);
     rc |= upload(ctx->sp_point, sp_point.data(), sp_point.size(), s);
     rc |= upload(ctx->sp_line, sp_line.data(), sp_line.size(), s);
@@ -576,6 +610,9 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     d.n_slots = ng;
     d.n_units = static_cast<int>(u_slot.size());
     d.u_slot = ctx->u_slot.as<int32_t>();
+    d.u_A = ctx->u_A.as<int32_t>();
+    d.u_B = ctx->u_B.as<int32_t>();
+    d.u_info = ctx->u_info.as<uint32_t>();
     d.u_cell = ctx->u_cell.as<int32_t>();
     d.u_twin = ctx->u_twin.as<int32_t>();
     d.u_tr0 = u_tr0;
@@ -626,6 +663,7 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     ctx->have_mesh = true;
     ctx->n_inner = 0;
     ctx->cen_valid = false;
+    ctx->drop_graphs();
     return GELIOS_OK;
 }
 
@@ -691,6 +729,102 @@ extern "C" int gelios_set_inner_cells(gelios_ctx* ctx, const int32_t* cells, int
     return GELIOS_OK;
 }
 
+namespace {
+
+// Enqueues one moving-grid step on the context's streams; returns the
+// number of kernels launched, or a negative error code.
+int enqueue_mk2(gelios_ctx* ctx, const StepBuffers& b) {
+    const DevMesh& d = ctx->d;
+    const gelios_params& P = ctx->prm;
+    cudaStream_t s = ctx->stream;
+    // Three streams per step.
+    //   side:  face reconstructions, the star pressures of the tracked
+    //          faces (neither depends on the motion), then, once the
+    //          rails have moved, the tracked-face fluxes (sampling of
+    //          the solved Riemann problems at the face speed);
+    //   side2: charge-exchange source terms and pre-motion volumes;
+    //   main:  surface tracking + rails, the other face fluxes, the
+    //          cell update, the commit.
+    cudaStream_t sd = ctx->side, sd2 = ctx->side2;
+    GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_fork, s));
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_fork, 0));
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd2, ctx->ev_fork, 0));
+    launch_mk2_recon(d, P, b, ctx->rec.as<double>(), sd);
+    GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_recon, sd));
+    const int nsv = launch_mk2_tracked_solve(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(), sd);
+    launch_mk2_source(d, P, b, ctx->aux.as<double>(), sd2);
+    GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_source, sd2));
+    cudaEvent_t e1 = ctx->phase_begin();
+    const int nm = launch_motion(d, P, b, ctx->surface.as<double>(), s);
+    ctx->phase_end(2, e1, nm);  // Move_surface + rails
+    GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_rails, s));
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_rails, 0));
+    const int nft = launch_mk2_flux_tracked(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(),
+                                            ctx->flux.as<double>(), sd);
+    GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_tracked, sd));
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_recon, 0));
+    cudaEvent_t e3 = ctx->phase_begin();
+    const int nfl = launch_mk2_flux_plain(d, P, b, ctx->rec.as<double>(), ctx->flux.as<double>(), s) + nft;
+    ctx->phase_end(1, e3, nfl);
+    // the update reads the tracked-face fluxes and the source terms
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_tracked, 0));
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_source, 0));
+    cudaEvent_t e5 = ctx->phase_begin();
+    launch_mk2_update(d, P, b, ctx->flux.as<double>(), ctx->aux.as<double>(), s);
+    ctx->phase_end(3, e5, 1);
+    cudaEvent_t e4 = ctx->phase_begin();
+    launch_commit(d, b, s);
+    ctx->phase_end(4, e4, 1);
+    GELIOS_CUDA_TRY(cudaGetLastError());
+    return nm + 4 + nfl + nsv;
+}
+
+// One moving-grid step: replays the instantiated graph of this step's
+// buffers (captured on first use), or launches directly while phase timing
+// is on or if capture is unavailable.  Returns the kernel count or a
+// negative error code.
+int step_mk2(gelios_ctx* ctx, const StepBuffers& b) {
+    if (ctx->timing || ctx->graphs_off) return enqueue_mk2(ctx, b);
+    const int parity = b.cur[0] == ctx->field(0, 0) ? 0 : 1;
+    for (auto& g : ctx->graphs)
+        if (g.exec && g.parity == parity && g.cen == b.cx) {
+            GELIOS_CUDA_TRY(cudaGraphLaunch(g.exec, ctx->stream));
+            return g.launches;
+        }
+    cudaStream_t s = ctx->stream;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        ctx->graphs_off = true;
+        return enqueue_mk2(ctx, b);
+    }
+    const int n = enqueue_mk2(ctx, b);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s, &graph);
+    cudaGraphExec_t exec = nullptr;
+    if (n < 0 || e != cudaSuccess || !graph || cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        ctx->graphs_off = true;
+        return enqueue_mk2(ctx, b);
+    }
+    cudaGraphDestroy(graph);
+    gelios_ctx::StepGraph* slot = &ctx->graphs[0];
+    for (auto& g : ctx->graphs)
+        if (!g.exec) {
+            slot = &g;
+            break;
+        }
+    if (slot->exec) cudaGraphExecDestroy(slot->exec);
+    slot->parity = parity;
+    slot->cen = b.cx;
+    slot->exec = exec;
+    slot->launches = n;
+    GELIOS_CUDA_TRY(cudaGraphLaunch(exec, s));
+    return n;
+}
+
+}  // namespace
+
 extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status* status) {
     if (!ctx || nsteps < 0) return GELIOS_E_ARG;
     if (form != GELIOS_FORM_STATIONARY && form != GELIOS_FORM_MK2 && form != GELIOS_FORM_INNER_MK2) {
@@ -752,45 +886,9 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             b.cx_next = cn;
             b.cy_next = cn + d.n_cells;
             b.rp_next = cn + 2 * static_cast<size_t>(d.n_cells);
-            // Three streams per step.
-            //   side:  face reconstructions, the star pressures of the tracked
-            //          faces (neither depends on the motion), then, once the
-            //          rails have moved, the tracked-face fluxes (sampling of
-            //          the solved Riemann problems at the face speed);
-            //   side2: charge-exchange source terms and pre-motion volumes;
-            //   main:  surface tracking + rails, the other face fluxes, the
-            //          cell update, the commit.
-            cudaStream_t sd = ctx->side, sd2 = ctx->side2;
-            GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_fork, s));
-            GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_fork, 0));
-            GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd2, ctx->ev_fork, 0));
-            launch_mk2_recon(d, P, b, ctx->rec.as<double>(), sd);
-            GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_recon, sd));
-            const int nsv = launch_mk2_tracked_solve(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(), sd);
-            launch_mk2_source(d, P, b, ctx->aux.as<double>(), sd2);
-            GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_source, sd2));
-            cudaEvent_t e1 = ctx->phase_begin();
-            const int nm = launch_motion(d, P, b, ctx->surface.as<double>(), s);
-            ctx->phase_end(2, e1, nm);  // Move_surface + rails
-            GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_rails, s));
-            GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_rails, 0));
-            const int nft = launch_mk2_flux_tracked(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(),
-                                                    ctx->flux.as<double>(), sd);
-            GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_tracked, sd));
-            GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_recon, 0));
-            cudaEvent_t e3 = ctx->phase_begin();
-            const int nfl = launch_mk2_flux_plain(d, P, b, ctx->rec.as<double>(), ctx->flux.as<double>(), s) + nft;
-            ctx->phase_end(1, e3, nfl);
-            // the update reads the tracked-face fluxes and the source terms
-            GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_tracked, 0));
-            GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_source, 0));
-            cudaEvent_t e5 = ctx->phase_begin();
-            launch_mk2_update(d, P, b, ctx->flux.as<double>(), ctx->aux.as<double>(), s);
-            ctx->phase_end(3, e5, 1);
-            cudaEvent_t e4 = ctx->phase_begin();
-            launch_commit(d, b, s);
-            ctx->phase_end(4, e4, 1);
-            launches += nm + 4 + nfl + nsv;
+            const int n = step_mk2(ctx, b);
+            if (n < 0) return n;
+            launches += n;
         } else {
             b.cx = cen0;
             b.cy = cen0 + d.n_cells;

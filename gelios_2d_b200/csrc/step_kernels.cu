@@ -723,11 +723,16 @@ __device__ __forceinline__ St5 mk2_usualy_side(const double* const* st, const do
 //    Godunov on tracked faces (Setka.cpp:10198-10209, 10335-10380), slot
 //    fluxes and CFL candidates.
 // rec rows: ro, p, u, v, Q of the owner side, then of the other side.
+// LANES = 2: two lanes per unit; on interior faces lane 0 reconstructs the
+// owner side and lane 1 the other side.  LANES = 1: one thread does both.
+template <int LANES>
 __global__ void __launch_bounds__(128) mk2_recon_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                         double* __restrict__ rec) {
-    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int u = t / LANES, side = LANES == 2 ? (t & 1) : 0;
     int status = 0;
     if (u < d.n_units) {
+        const size_t n = d.n_units;
         const int g = d.u_slot[u], K = d.u_cell[u], gt = d.u_twin[u];
         const double x = b.cx[K], y = b.cy[K];
         const bool procK = !(sqrt(sq(x) + sq(y)) < P.R11);
@@ -739,13 +744,26 @@ __global__ void __launch_bounds__(128) mk2_recon_kernel(DevMesh d, gelios_params
             y3 = b.cy[nb];
             procN = !(sqrt(sq(x3) + sq(y3)) < P.R11);
         }
+        const int A = d.u_A[u], B = d.u_B[u];
+        const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
+        const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
+        if (side == 0) {
+            double t1 = xb - xa, t2 = yb - ya;
+            const double nn = sqrt(sq(t1) + sq(t2));
+            t1 = t1 / nn;
+            t2 = t2 / nn;
+            rec[10 * n + u] = t2;
+            rec[11 * n + u] = -t1;
+            rec[12 * n + u] = sqrt(sq(xb - xa) + sq(yb - ya)) * (ya + yb) * 0.5;
+            rec[13 * n + u] = x2;
+            rec[14 * n + u] = y2;
+            rec[15 * n + u] = procK ? sqrt(sq(x - x2) + sq(y - y2)) : -1.0;
+            rec[16 * n + u] = procN ? sqrt(sq(x3 - x2) + sq(y3 - y2)) : -1.0;
+        }
         if (procK || procN) {
             const uint32_t info = d.sinfo[g];
             const int ft = info & SI_TYPE_MASK;
             const uint32_t cf = d.cflags[K];
-            const int A = d.sA[g], B = d.sB[g];
-            const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
-            const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
             const double g2 = 2 * P.gamma;
             const St5 par1 = load_state(b.cur, K);
             St5 par11 = par1;
@@ -757,39 +775,48 @@ __global__ void __launch_bounds__(128) mk2_recon_kernel(DevMesh d, gelios_params
                                 (ft == G_USUALY && (nbf & CF_C1));
             const double pdis = radial ? pow2g(dis, g2) : 1.0;
             if (ft == G_USUALY) {
-                par11 = mk2_usualy_side(b.cur, b.cx, b.cy, b.rp, x2, y2, dis, pdis, par1, x, y, b.rp[K], cf, nb,
-                                        d.ssd[g], tracked, &status);
-                par2 = mk2_usualy_side(b.cur, b.cx, b.cy, b.rp, x2, y2, dis, pdis, par2, x3, y3, b.rp[nb], nbf, K,
-                                       d.ssd2[g], tracked, &status);
-            } else if (ft == G_INNER_SPHERE) {
-                const double radius = sqrt(sq(x) + sq(y));
-                par11.ro = par11.ro * sq(radius) / sq(dis);
-                par11.Q = par11.Q * sq(radius) / sq(dis);
-                par11.p = par11.p * (b.rp[K] / pdis);
-            } else if (ft == G_AXIS) {
-                if (cf & CF_C1) {
+                for (int sd = side; sd < 2; sd += LANES) {
+                    const bool s1 = sd == 1;
+                    const St5 r = mk2_usualy_side(b.cur, b.cx, b.cy, b.rp, x2, y2, dis, pdis, s1 ? par2 : par1,
+                                                  s1 ? x3 : x, s1 ? y3 : y, b.rp[s1 ? nb : K], s1 ? nbf : cf,
+                                                  s1 ? K : nb, s1 ? d.ssd2[g] : d.ssd[g], tracked, &status);
+                    const int r0 = s1 ? 5 : 0;
+                    rec[(r0 + 0) * n + u] = r.ro;
+                    rec[(r0 + 1) * n + u] = r.p;
+                    rec[(r0 + 2) * n + u] = r.u;
+                    rec[(r0 + 3) * n + u] = r.v;
+                    rec[(r0 + 4) * n + u] = r.Q;
+                }
+            } else if (side == 0) {
+                if (ft == G_INNER_SPHERE) {
                     const double radius = sqrt(sq(x) + sq(y));
                     par11.ro = par11.ro * sq(radius) / sq(dis);
                     par11.Q = par11.Q * sq(radius) / sq(dis);
                     par11.p = par11.p * (b.rp[K] / pdis);
-                    polar_perenos(x, y, x2, y2, par11.u, par11.v);
-                } else {
-                    par11 = tvd_axis(b.cur, b.cx, b.cy, x2, y2, par1, x, y, d.ssd[g]);
+                } else if (ft == G_AXIS) {
+                    if (cf & CF_C1) {
+                        const double radius = sqrt(sq(x) + sq(y));
+                        par11.ro = par11.ro * sq(radius) / sq(dis);
+                        par11.Q = par11.Q * sq(radius) / sq(dis);
+                        par11.p = par11.p * (b.rp[K] / pdis);
+                        polar_perenos(x, y, x2, y2, par11.u, par11.v);
+                    } else {
+                        par11 = tvd_axis(b.cur, b.cx, b.cy, x2, y2, par1, x, y, d.ssd[g]);
+                    }
+                    par2 = par11;
+                    par2.v = -par2.v;
                 }
-                par2 = par11;
-                par2.v = -par2.v;
+                rec[0 * n + u] = par11.ro;
+                rec[1 * n + u] = par11.p;
+                rec[2 * n + u] = par11.u;
+                rec[3 * n + u] = par11.v;
+                rec[4 * n + u] = par11.Q;
+                rec[5 * n + u] = par2.ro;
+                rec[6 * n + u] = par2.p;
+                rec[7 * n + u] = par2.u;
+                rec[8 * n + u] = par2.v;
+                rec[9 * n + u] = par2.Q;
             }
-            const size_t n = d.n_units;
-            rec[0 * n + u] = par11.ro;
-            rec[1 * n + u] = par11.p;
-            rec[2 * n + u] = par11.u;
-            rec[3 * n + u] = par11.v;
-            rec[4 * n + u] = par11.Q;
-            rec[5 * n + u] = par2.ro;
-            rec[6 * n + u] = par2.p;
-            rec[7 * n + u] = par2.u;
-            rec[8 * n + u] = par2.v;
-            rec[9 * n + u] = par2.Q;
         }
     }
     if (status) atomicOr(b.status, status);
@@ -808,33 +835,17 @@ __global__ void __launch_bounds__(128) mk2_flux_kernel(DevMesh d, gelios_params 
     const size_t ng = d.n_slots;
     const int u = TRACKED ? d.u_tr0 + i : (i < d.u_tr0 ? i : i + (d.u_tr1 - d.u_tr0));
     if (i < n_launch) {
-        const int g = d.u_slot[u], K = d.u_cell[u], gt = d.u_twin[u];
-        const double x = b.cx[K], y = b.cy[K];
-        const bool procK = !(sqrt(sq(x) + sq(y)) < P.R11);
-        const int nb = gt >= 0 ? d.snb[g] : -1;
-        double x3 = 0.0, y3 = 0.0;
-        bool procN = false;
-        if (nb >= 0) {
-            x3 = b.cx[nb];
-            y3 = b.cy[nb];
-            procN = !(sqrt(sq(x3) + sq(y3)) < P.R11);
-        }
+        const size_t n = d.n_units;
+        const double dist = rec[15 * n + u], distn = rec[16 * n + u];
+        const bool procK = !(dist < 0.0), procN = !(distn < 0.0);
         if (procK || procN) {
             const double dt = *b.dt_cur;
-            const uint32_t info = d.sinfo[g];
-            const int A = d.sA[g], B = d.sB[g];
-            const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
-            const double S = sqrt(sq(xb - xa) + sq(yb - ya)) * (ya + yb) * 0.5;
-            const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
+            const uint32_t info = d.u_info[u];
+            const int A = d.u_A[u], B = d.u_B[u];
+            const double n1 = rec[10 * n + u], n2 = rec[11 * n + u];
+            const double S = rec[12 * n + u], x2 = rec[13 * n + u], y2 = rec[14 * n + u];
             const double x4 = (d.X2[A] + d.X2[B]) / 2.0, y4 = (d.Y2[A] + d.Y2[B]) / 2.0;
-            const double dist = sqrt(sq(x - x2) + sq(y - y2));
-            double t1 = xb - xa, t2 = yb - ya;
-            const double nn = sqrt(sq(t1) + sq(t2));
-            t1 = t1 / nn;
-            t2 = t2 / nn;
-            const double n1 = t2, n2 = -t1;
             const double W = ((x4 - x2) * n1 + (y4 - y2) * n2) / dt;
-            const size_t n = d.n_units;
             St5 par11, par2;
             par11.ro = rec[0 * n + u];
             par11.p = rec[1 * n + u];
@@ -846,6 +857,7 @@ __global__ void __launch_bounds__(128) mk2_flux_kernel(DevMesh d, gelios_params 
             par2.u = rec[7 * n + u];
             par2.v = rec[8 * n + u];
             par2.Q = rec[9 * n + u];
+            const int g = d.u_slot[u], gt = d.u_twin[u];
             const bool tracked = TRACKED;
             const bool np = (info & SI_NP) != 0;
             FluxOut<double> F;
@@ -883,7 +895,6 @@ __global__ void __launch_bounds__(128) mk2_flux_kernel(DevMesh d, gelios_params 
                 fl[3 * ng + gt] = -fm3;
                 fl[4 * ng + gt] = -fq;
                 if (procN) {
-                    const double distn = sqrt(sq(x3 - x2) + sq(y3 - y2));
                     if (tracked) tmin_u = dmin_ref(tmin_u, P.kurant * distn / UG);
                     tmin_u = dmin_ref(tmin_u, P.kurant * distn / UU);
                 }
@@ -906,23 +917,12 @@ __global__ void __launch_bounds__(64) mk2_tracked_solve_kernel(DevMesh d, gelios
     if (i >= d.u_tr1 - d.u_tr0) return;
     const int u = d.u_tr0 + i;
     int status = 0;
-    const int g = d.u_slot[u], K = d.u_cell[u], gt = d.u_twin[u];
-    const double x = b.cx[K], y = b.cy[K];
-    const bool procK = !(sqrt(sq(x) + sq(y)) < P.R11);
-    bool procN = false;
-    const int nb = gt >= 0 ? d.snb[g] : -1;
-    if (nb >= 0) procN = !(sqrt(sq(b.cx[nb]) + sq(b.cy[nb])) < P.R11);
-    if (!(procK || procN)) return;
-    const int A = d.sA[g], B = d.sB[g];
-    const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
-    double t1 = xb - xa, t2 = yb - ya;
-    const double nn = sqrt(sq(t1) + sq(t2));
-    t1 = t1 / nn;
-    t2 = t2 / nn;
     const size_t n = d.n_units;
+    // a unit with neither side updated has no flux (rows 15 and 16)
+    if (rec[15 * n + u] < 0.0 && rec[16 * n + u] < 0.0) return;
     double q1[5] = {rec[0 * n + u], rec[1 * n + u], rec[2 * n + u], rec[3 * n + u], 0.0};
     double q2[5] = {rec[5 * n + u], rec[6 * n + u], rec[7 * n + u], rec[8 * n + u], 0.0};
-    double nv[3] = {t2, -t1, 0.0};
+    double nv[3] = {rec[10 * n + u], rec[11 * n + u], 0.0};
     double qq[5], ds[3], p = 0.0;
     godunov_dev<true>(P.gamma, P.kurant, q1, q2, nv, qq, ds, 0.0, 1.0, P.godunov_max_iter, &status, nullptr, &p);
     if ((threadIdx.x & 31) == 0) {
@@ -1748,7 +1748,8 @@ void launch_stationary_update(const DevMesh& d, const gelios_params& P, const St
     stationary_update_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, fl);
 }
 void launch_mk2_recon(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* rec, cudaStream_t s) {
-    mk2_recon_kernel<<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, b, rec);
+    constexpr int kLanes = 1;
+    mk2_recon_kernel<kLanes><<<blocks_for(kLanes * d.n_units, 128), 128, 0, s>>>(d, P, b, rec);
 }
 int launch_mk2_flux_plain(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
                           double* fl, cudaStream_t s) {

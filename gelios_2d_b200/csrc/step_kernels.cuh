@@ -32,6 +32,8 @@ struct DevMesh {
     int n_slots = 0, n_units = 0;
     int u_tr0 = 0, u_tr1 = 0;  // range of the tracked-face units (grouped together)
     const int32_t *u_slot = nullptr, *u_cell = nullptr, *u_twin = nullptr;
+    const int32_t *u_A = nullptr, *u_B = nullptr;  // end points of the unit's face
+    const uint32_t* u_info = nullptr;              // slot info of the unit's face
     const int32_t *fA = nullptr, *fB = nullptr, *ftype = nullptr, *fmaster = nullptr, *fsosed = nullptr,
                   *fcopy = nullptr, *fsdown = nullptr;
     const int32_t *rtype = nullptr, *rM = nullptr, *rpstart = nullptr, *rpts = nullptr, *rkstart = nullptr,
@@ -60,6 +62,18 @@ struct DevMesh {
 
 // Buffers of one time step (double buffering of the state like par[now1] ->
 // par[now2]; centroids of the current/next point positions; dt words).
+// Rows of the per-unit reconstruction array of the moving-grid step
+// (unit-major, n_units doubles per row), written before the grid moves:
+//   0-4   owner side TVD state ro, p, u, v, Q
+//   5-9   other side TVD state
+//   10,11 face normal n1, n2 (pre-motion points)
+//   12    S = |AB| * (yA + yB) / 2
+//   13,14 face centre x2, y2 (pre-motion)
+//   15    distance owner centroid - face centre, -1 if the owner is skipped
+//   16    distance other centroid - face centre, -1 if skipped or no twin
+// A unit with rows 15 and 16 both negative has no flux this step.
+constexpr int kRecRows = 17;
+
 struct StepBuffers {
     const double* cur[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     double* nxt[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};

@@ -168,6 +168,51 @@ def test_mk2_golden_fixture():
     assert rel_err(dev.par(1), gd["mk2_par1"]) <= 1e-12
 
 
+def test_mk2_repeated_single_step_calls():
+    """Each call restarts from par[0] on the moved grid (Setka.cpp:10126-10140);
+    repeated one-step calls replay the captured step graph."""
+    mesh = g.Mesh.setka(*MEDIUM)
+    P = N.reference_params()
+    st0 = W.init_conditions_reference(mesh)
+    mc = W.mc_fields(mesh, seed=9)
+    dev, ora = _pair(mesh, P, st0, mc)
+    for _ in range(3):
+        dev.Go_5_komponent__MK2(1)
+        ora.mk2(1)
+        assert rel_err(dev.par(1), ora.get_state(1)) <= 1e-12
+    x, y = dev.points()
+    pts = ora.points()
+    assert np.max(np.abs(x - pts["x"]) / np.maximum(np.abs(pts["x"]), 1e-3)) <= 1e-13
+
+
+def test_mk2_graph_matches_direct_launches():
+    """The captured step (graph replay) against the same kernels launched
+    directly (phase timing on), bit for bit, across parameter changes and
+    odd/even step counts."""
+    mesh = g.Mesh.setka(*MEDIUM)
+    P = N.reference_params()
+    P2 = P.copy(kurant=0.07)
+    st0 = W.init_conditions_reference(mesh)
+    mc = W.mc_fields(mesh, seed=9)
+    runs = []
+    for direct in (False, True):
+        dev = g.Setka(mesh, P)
+        dev.set_par(0, st0)
+        dev.set_par(1, st0)
+        dev.set_mc(*mc)
+        dev.set_phase_timing(direct)
+        dev.Go_5_komponent__MK2(1)
+        dev.Go_5_komponent__MK2(1)
+        dev.set_params(P2)
+        dev.Go_5_komponent__MK2(2)
+        s = dev.Go_5_komponent__MK2(3)
+        runs.append((dev.par(0), dev.par(1), dev.points(), s.dt))
+    a, b = runs
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    assert np.array_equal(a[2][0], b[2][0]) and np.array_equal(a[2][1], b[2][1])
+    assert a[3] == b[3]
+
+
 def test_deterministic_runs():
     mesh = g.Mesh.setka(*MEDIUM)
     P = N.reference_params()
