@@ -203,7 +203,7 @@ int gelios_godunov_batch(const gelios_params *prm, int n, const double *in, doub
  * (the same kernels as gelios_step with GELIOS_FORM_STATIONARY) on a grid
  * and state the caller already holds in device memory.  Nothing is
  * allocated: the step's scratch (face-slot fluxes, centroids, dt words) is
- * one fixed file-scope device array of about 5.8 MB that every GPU loading
+ * one fixed file-scope device array of about 6.0 MB that every GPU loading
  * the library holds until exit, so grids are limited to
  * GELIOS_NOALLOC_MAX_CELLS cells and GELIOS_NOALLOC_MAX_SLOTS face slots
  * (GELIOS_E_LIMIT beyond).  The first call on a device resolves that array's
