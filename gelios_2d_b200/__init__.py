@@ -7,7 +7,7 @@ and a thin Python mirror of the reference's Setka operator interface.
 from . import _native
 from ._native import GeliosParams, GeliosStatus, reference_params
 from .mesh import Mesh
-from .setka import Setka, StepError, godunov_batch, hllc_batch
+from .setka import Setka, StepError, godunov_batch, hllc_batch, hlld_batch, hlldq_batch
 
 __all__ = ["GeliosParams", "GeliosStatus", "Mesh", "Setka", "StepError", "godunov_batch", "hllc_batch",
-           "reference_params", "_native"]
+           "hlld_batch", "hlldq_batch", "reference_params", "_native"]

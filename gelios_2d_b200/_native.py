@@ -149,6 +149,8 @@ def lib() -> C.CDLL:
                                                  C.c_void_p, C.c_void_p]
     L.gelios_hllc_batch.argtypes = [C.POINTER(GeliosParams), C.c_int, dp, dp]
     L.gelios_godunov_batch.argtypes = [C.POINTER(GeliosParams), C.c_int, dp, dp]
+    L.gelios_hlldq_batch.argtypes = [C.POINTER(GeliosParams), C.c_int, dp, dp]
+    L.gelios_hlld_batch.argtypes = [C.POINTER(GeliosParams), C.c_int, dp, dp]
     _LIB = L
     return L
 

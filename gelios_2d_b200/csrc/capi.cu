@@ -988,7 +988,8 @@ extern "C" int gelios_phase_times(gelios_ctx* ctx, double* ms, int64_t* launches
 }
 
 namespace {
-int run_batch(const gelios_params* prm, int n, const double* in, int in_w, double* out, int out_w, bool godunov) {
+enum BatchKind { B_HLLC, B_GODUNOV, B_HLLDQ, B_HLLD };
+int run_batch(const gelios_params* prm, int n, const double* in, int in_w, double* out, int out_w, BatchKind kind) {
     if (!prm || n < 0 || (n > 0 && (!in || !out))) return GELIOS_E_ARG;
     if (n == 0) return GELIOS_OK;
     int ndev = 0;
@@ -999,8 +1000,12 @@ int run_batch(const gelios_params* prm, int n, const double* in, int in_w, doubl
     DBuf din, dout;
     if (din.alloc(sizeof(double) * in_w * n) || dout.alloc(sizeof(double) * out_w * n)) return GELIOS_E_CUDA;
     GELIOS_CUDA_TRY(cudaMemcpy(din.p, in, sizeof(double) * in_w * n, cudaMemcpyHostToDevice));
-    if (godunov) launch_godunov_batch(*prm, n, din.as<double>(), dout.as<double>(), 0);
-    else launch_hllc_batch(*prm, n, din.as<double>(), dout.as<double>(), 0);
+    switch (kind) {
+        case B_HLLC: launch_hllc_batch(*prm, n, din.as<double>(), dout.as<double>(), 0); break;
+        case B_GODUNOV: launch_godunov_batch(*prm, n, din.as<double>(), dout.as<double>(), 0); break;
+        case B_HLLDQ: launch_hlldq_batch(*prm, n, din.as<double>(), dout.as<double>(), 0); break;
+        case B_HLLD: launch_hlld_batch(*prm, n, din.as<double>(), dout.as<double>(), 0); break;
+    }
     GELIOS_CUDA_TRY(cudaGetLastError());
     GELIOS_CUDA_TRY(cudaMemcpy(out, dout.p, sizeof(double) * out_w * n, cudaMemcpyDeviceToHost));
     return GELIOS_OK;
@@ -1008,9 +1013,17 @@ int run_batch(const gelios_params* prm, int n, const double* in, int in_w, doubl
 }  // namespace
 
 extern "C" int gelios_hllc_batch(const gelios_params* prm, int n, const double* in, double* out) {
-    return run_batch(prm, n, in, 16, out, 9, false);
+    return run_batch(prm, n, in, 16, out, 9, B_HLLC);
 }
 
 extern "C" int gelios_godunov_batch(const gelios_params* prm, int n, const double* in, double* out) {
-    return run_batch(prm, n, in, 15, out, 10, true);
+    return run_batch(prm, n, in, 15, out, 10, B_GODUNOV);
+}
+
+extern "C" int gelios_hlldq_batch(const gelios_params* prm, int n, const double* in, double* out) {
+    return run_batch(prm, n, in, 23, out, 10, B_HLLDQ);
+}
+
+extern "C" int gelios_hlld_batch(const gelios_params* prm, int n, const double* in, double* out) {
+    return run_batch(prm, n, in, 21, out, 13, B_HLLD);
 }

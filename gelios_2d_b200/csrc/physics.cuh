@@ -30,7 +30,7 @@ enum : uint32_t {
 // Cell flag bits.
 enum : uint32_t { CF_AXIS = 1u, CF_C1 = 2u, CF_CENTR = 4u };
 // Status flag bits (gelios_status::flags).
-enum : int { ST_ITER_CAP = 1, ST_TVD_BAD = 2, ST_NEWTON_NEG = 4, ST_CHAIN = 8, ST_DT_BAD = 16 };
+enum : int { ST_ITER_CAP = 1, ST_TVD_BAD = 2, ST_NEWTON_NEG = 4, ST_CHAIN = 8, ST_DT_BAD = 16, ST_WAVE_ORDER = 32 };
 
 struct St5 {
     double ro, p, u, v, Q;
@@ -552,6 +552,352 @@ static __device__ __noinline__ double godunov_dev(double ga, double kurant, cons
     ds[0] = dsl;
     ds[1] = dsp;
     ds[2] = dsc;
+    return time;
+}
+
+// ---------------------------------------------------------------- MHD fluxes
+// Magnetic fields enter these solvers in Gaussian units and are scaled by
+// 1/sqrt(4 pi) inside (Solvers.h:12, Solvers.cpp:115-127, 1648-1654).
+__device__ __forceinline__ double spi4_dev() { return sqrt(4.0 * kPi); }
+
+// Solvers::HLLDQ_Korolkov (Solvers.cpp:1642-2185).  L, R = (ro, Q, p, v1,
+// v2, v3, Bx, By, Bz); the normal must be a coordinate axis (the tangent
+// pair is picked from its sign and direction).  metod 2: HLLC-type MHD
+// flux, metod 3: HLLD.  Pout[8] = mass, momentum x3, B flux x3, energy (the
+// reference's final reordering), *PQ = flux of Q.  Returns kurant*rad/max|S|.
+// Other metods leave Pout and *PQ untouched, as the reference does.
+__device__ inline double hlldq_korolkov(double ga, double kurant, const double* L, const double* R, double n1,
+                                        double n2, double n3, double rad, int metod, double* Pout, double* PQ) {
+    const double spi4 = spi4_dev();
+    const double g1 = ga - 1.0;
+    const double ro_L = L[0], Q_L = L[1], p_L = L[2], v1_L = L[3], v2_L = L[4], v3_L = L[5];
+    const double ro_R = R[0], Q_R = R[1], p_R = R[2], v1_R = R[3], v2_R = R[4], v3_R = R[5];
+    const double bx_L = L[6] / spi4, by_L = L[7] / spi4, bz_L = L[8] / spi4;
+    const double bx_R = R[6] / spi4, by_R = R[7] / spi4, bz_R = R[8] / spi4;
+    double t1 = 0.0, t2 = 0.0, t3 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;
+    if (n1 > 0.1) {
+        t2 = 1.0; m3 = 1.0;
+    } else if (n2 > 0.1) {
+        t3 = 1.0; m1 = 1.0;
+    } else if (n3 > 0.1) {
+        t1 = 1.0; m2 = 1.0;
+    } else if (n1 < -0.1) {
+        t3 = -1.0; m2 = -1.0;
+    } else if (n2 < -0.1) {
+        t1 = -1.0; m3 = -1.0;
+    } else if (n3 < -0.1) {
+        t1 = -1.0; m2 = -1.0;
+    }
+    const double u1 = v1_L * n1 + v2_L * n2 + v3_L * n3;
+    const double v1 = v1_L * t1 + v2_L * t2 + v3_L * t3;
+    const double w1 = v1_L * m1 + v2_L * m2 + v3_L * m3;
+    const double u2 = v1_R * n1 + v2_R * n2 + v3_R * n3;
+    const double v2 = v1_R * t1 + v2_R * t2 + v3_R * t3;
+    const double w2 = v1_R * m1 + v2_R * m2 + v3_R * m3;
+    const double bn1 = bx_L * n1 + by_L * n2 + bz_L * n3;
+    const double bt1 = bx_L * t1 + by_L * t2 + bz_L * t3;
+    const double bm1 = bx_L * m1 + by_L * m2 + bz_L * m3;
+    const double bn2 = bx_R * n1 + by_R * n2 + bz_R * n3;
+    const double bt2 = bx_R * t1 + by_R * t2 + bz_R * t3;
+    const double bm2 = bx_R * m1 + by_R * m2 + bz_R * m3;
+    const double bb_L = sq(bx_L) + sq(by_L) + sq(bz_L);
+    const double bb_R = sq(bx_R) + sq(by_R) + sq(bz_R);
+    const double uu_L = (sq(v1_L) + sq(v2_L) + sq(v3_L)) / 2.0;
+    const double uu_R = (sq(v1_R) + sq(v2_R) + sq(v3_R)) / 2.0;
+    const double cfL = sqrt((ga * p_L + bb_L + sqrt(sq(ga * p_L + bb_L) - 4.0 * ga * p_L * sq(bn1))) / (2.0 * ro_L));
+    const double cfR = sqrt((ga * p_R + bb_R + sqrt(sq(ga * p_R + bb_R) - 4.0 * ga * p_R * sq(bn2))) / (2.0 * ro_R));
+    const double SL = dmin_ref(u1, u2) - dmax_ref(cfL, cfR);
+    const double SR = dmax_ref(u1, u2) + dmax_ref(cfL, cfR);
+    const double pTL = p_L + bb_L / 2.0;
+    const double pTR = p_R + bb_R / 2.0;
+    const double suR = SR - u2, suL = SL - u1;
+    const double SM = (suR * ro_R * u2 - suL * ro_L * u1 - pTR + pTL) / (suR * ro_R - suL * ro_L);
+    const double PTT = (suR * ro_R * pTL - suL * ro_L * pTR + ro_L * ro_R * suR * suL * (u2 - u1)) /
+                       (suR * ro_R - suL * ro_L);
+    const double UU = dmax_ref(fabs(SL), fabs(SR));
+    const double time = kurant * rad / UU;
+    if (metod != 2 && metod != 3) return time;
+    const double e1 = p_L / g1 + ro_L * uu_L + bb_L / 2.0;
+    const double e2 = p_R / g1 + ro_R * uu_R + bb_R / 2.0;
+    const double FL[9] = {ro_L * u1,
+                          ro_L * u1 * u1 + pTL - sq(bn1),
+                          ro_L * u1 * v1 - bn1 * bt1,
+                          ro_L * u1 * w1 - bn1 * bm1,
+                          (e1 + pTL) * u1 - bn1 * (u1 * bn1 + v1 * bt1 + w1 * bm1),
+                          0.0,
+                          u1 * bt1 - v1 * bn1,
+                          u1 * bm1 - w1 * bn1,
+                          Q_L * u1};
+    const double FR[9] = {ro_R * u2,
+                          ro_R * u2 * u2 + pTR - sq(bn2),
+                          ro_R * u2 * v2 - bn2 * bt2,
+                          ro_R * u2 * w2 - bn2 * bm2,
+                          (e2 + pTR) * u2 - bn2 * (u2 * bn2 + v2 * bt2 + w2 * bm2),
+                          0.0,
+                          u2 * bt2 - v2 * bn2,
+                          u2 * bm2 - w2 * bn2,
+                          Q_R * u2};
+    const double UL[9] = {ro_L, ro_L * u1, ro_L * v1, ro_L * w1, e1, bn1, bt1, bm1, Q_L};
+    const double UR[9] = {ro_R, ro_R * u2, ro_R * v2, ro_R * w2, e2, bn2, bt2, bm2, Q_R};
+    const double bn = (SR * UR[5] - SL * UL[5] + FL[5] - FR[5]) / (SR - SL);
+    const double bt = (SR * UR[6] - SL * UL[6] + FL[6] - FR[6]) / (SR - SL);
+    const double bm = (SR * UR[7] - SL * UL[7] + FL[7] - FR[7]) / (SR - SL);
+    const double bbn = bn * bn;
+    const double ro_LL = ro_L * (SL - u1) / (SL - SM);
+    const double ro_RR = ro_R * (SR - u2) / (SR - SM);
+    const double Q_LL = Q_L * (SL - u1) / (SL - SM);
+    const double Q_RR = Q_R * (SR - u2) / (SR - SM);
+    double PO[9];
+    if (metod == 2) {  // HLLC + MHD (Solvers.cpp:1817-1973)
+        const double sbv1 = u1 * bn1 + v1 * bt1 + w1 * bm1;
+        const double sbv2 = u2 * bn2 + v2 * bt2 + w2 * bm2;
+        const double UZ0 = (SR * UR[0] - SL * UL[0] + FL[0] - FR[0]) / (SR - SL);
+        const double UZ1 = (SR * UR[1] - SL * UL[1] + FL[1] - FR[1]) / (SR - SL);
+        const double UZ2 = (SR * UR[2] - SL * UL[2] + FL[2] - FR[2]) / (SR - SL);
+        const double UZ3 = (SR * UR[3] - SL * UL[3] + FL[3] - FR[3]) / (SR - SL);
+        const double suRm = suR / (SR - SM);
+        const double suLm = suL / (SL - SM);
+        const double ptzR = pTR + ro_R * suR * (SM - u2);
+        const double ptzL = pTL + ro_L * suL * (SM - u1);
+        const double ptz = (ptzR + ptzL) / 2.0;
+        const double vRR = UZ2 / UZ0, wRR = UZ3 / UZ0;
+        const double vLL = vRR, wLL = wRR;
+        const double btt2 = bt, bmm2 = bm, btt1 = btt2, bmm1 = bmm2;
+        const double sbvz = (bn * UZ1 + bt * UZ2 + bm * UZ3) / UZ0;
+        const double ee2 = e2 * suRm + (ptz * SM - pTR * u2 + bn * (sbv2 - sbvz)) / (SR - SM);
+        const double ee1 = e1 * suLm + (ptz * SM - pTL * u1 + bn * (sbv1 - sbvz)) / (SL - SM);
+        const double ULL[9] = {ro_LL, ro_LL * SM, ro_LL * vLL, ro_LL * wLL, ee1, bn, btt1, bmm1, Q_LL};
+        const double URR[9] = {ro_RR, ro_RR * SM, ro_RR * vRR, ro_RR * wRR, ee2, bn, btt2, bmm2, Q_RR};
+        for (int i = 0; i < 9; i++) PO[i] = 0.0;
+        if (SL >= 0.0) {
+            for (int i = 0; i < 9; i++) PO[i] = FL[i];
+        } else if (SL < 0.0 && SM >= 0.0) {
+            for (int i = 0; i < 9; i++) PO[i] = FL[i] + SL * ULL[i] - SL * UL[i];
+        } else if (SR > 0.0 && SM < 0.0) {
+            for (int i = 0; i < 9; i++) PO[i] = FR[i] + SR * URR[i] - SR * UR[i];
+        } else if (SR <= 0.0) {
+            for (int i = 0; i < 9; i++) PO[i] = FR[i];
+        }
+    } else {  // HLLD (Solvers.cpp:1975-2180)
+        const double ttL = ro_L * suL * (SL - SM) - bbn;
+        const double ttR = ro_R * suR * (SR - SM) - bbn;
+        double vLL, wLL, vRR, wRR, btt1, bmm1, btt2, bmm2;
+        if (fabs(ttL) >= 0.000001) {
+            vLL = v1 - bn * bt1 * (SM - u1) / ttL;
+            wLL = w1 - bn * bm1 * (SM - u1) / ttL;
+            btt1 = bt1 * (ro_L * suL * suL - bbn) / ttL;
+            bmm1 = bm1 * (ro_L * suL * suL - bbn) / ttL;
+        } else {
+            vLL = v1; wLL = w1; btt1 = 0.0; bmm1 = 0.0;
+        }
+        if (fabs(ttR) >= 0.000001) {
+            vRR = v2 - bn * bt2 * (SM - u2) / ttR;
+            wRR = w2 - bn * bm2 * (SM - u2) / ttR;
+            btt2 = bt2 * (ro_R * suR * suR - bbn) / ttR;
+            bmm2 = bm2 * (ro_R * suR * suR - bbn) / ttR;
+        } else {
+            vRR = v2; wRR = w2; btt2 = 0.0; bmm2 = 0.0;
+        }
+        const double eLL = (e1 * suL + PTT * SM - pTL * u1 +
+                            bn * ((u1 * bn1 + v1 * bt1 + w1 * bm1) - (SM * bn + vLL * btt1 + wLL * bmm1))) /
+                           (SL - SM);
+        const double eRR = (e2 * suR + PTT * SM - pTR * u2 +
+                            bn * ((u2 * bn2 + v2 * bt2 + w2 * bm2) - (SM * bn + vRR * btt2 + wRR * bmm2))) /
+                           (SR - SM);
+        const double sqrtroLL = sqrt(ro_LL), sqrtroRR = sqrt(ro_RR);
+        double SLL = SM - fabs(bn) / sqrtroLL;
+        double SRR = SM + fabs(bn) / sqrtroRR;
+        double idbn;
+        if (fabs(bn) > 0.001) {
+            idbn = 1.0 * sgn(bn);
+        } else {
+            idbn = 0.0;
+            SLL = SM;
+            SRR = SM;
+        }
+        const double vLLL = (sqrtroLL * vLL + sqrtroRR * vRR + idbn * (btt2 - btt1)) / (sqrtroLL + sqrtroRR);
+        const double wLLL = (sqrtroLL * wLL + sqrtroRR * wRR + idbn * (bmm2 - bmm1)) / (sqrtroLL + sqrtroRR);
+        const double bttt = (sqrtroLL * btt2 + sqrtroRR * btt1 + idbn * sqrtroLL * sqrtroRR * (vRR - vLL)) /
+                            (sqrtroLL + sqrtroRR);
+        const double bmmm = (sqrtroLL * bmm2 + sqrtroRR * bmm1 + idbn * sqrtroLL * sqrtroRR * (wRR - wLL)) /
+                            (sqrtroLL + sqrtroRR);
+        const double eLLL = eLL - idbn * sqrtroLL * ((SM * bn + vLL * btt1 + wLL * bmm1) -
+                                                     (SM * bn + vLLL * bttt + wLLL * bmmm));
+        const double eRRR = eRR + idbn * sqrtroRR * ((SM * bn + vRR * btt2 + wRR * bmm2) -
+                                                     (SM * bn + vLLL * bttt + wLLL * bmmm));
+        const double ULL[9] = {ro_LL, ro_LL * SM, ro_LL * vLL, ro_LL * wLL, eLL, bn, btt1, bmm1, Q_LL};
+        const double URR[9] = {ro_RR, ro_RR * SM, ro_RR * vRR, ro_RR * wRR, eRR, bn, btt2, bmm2, Q_RR};
+        const double ULLL[9] = {ro_LL, ro_LL * SM, ro_LL * vLLL, ro_LL * wLLL, eLLL, bn, bttt, bmmm, Q_LL};
+        const double URRR[9] = {ro_RR, ro_RR * SM, ro_RR * vLLL, ro_RR * wLLL, eRRR, bn, bttt, bmmm, Q_RR};
+        for (int i = 0; i < 9; i++) PO[i] = 0.0;
+        if (SL >= 0.0) {
+            for (int i = 0; i < 9; i++) PO[i] = FL[i];
+        } else if (SL < 0.0 && SLL >= 0.0) {
+            for (int i = 0; i < 9; i++) PO[i] = FL[i] + SL * ULL[i] - SL * UL[i];
+        } else if (SLL <= 0.0 && SM >= 0.0) {
+            for (int i = 0; i < 9; i++) PO[i] = FL[i] + SLL * ULLL[i] - (SLL - SL) * ULL[i] - SL * UL[i];
+        } else if (SM < 0.0 && SRR > 0.0) {
+            for (int i = 0; i < 9; i++) PO[i] = FR[i] + SRR * URRR[i] - (SRR - SR) * URR[i] - SR * UR[i];
+        } else if (SR > 0.0 && SRR <= 0.0) {
+            for (int i = 0; i < 9; i++) PO[i] = FR[i] + SR * URR[i] - SR * UR[i];
+        } else if (SR <= 0.0) {
+            for (int i = 0; i < 9; i++) PO[i] = FR[i];
+        }
+    }
+    const double SN = dmax_ref(fabs(SL), fabs(SR));
+    PO[5] = -SN * (bn2 - bn1);
+    // back to (x, y, z), then the reference's reordering: B fluxes before energy
+    Pout[0] = PO[0];
+    Pout[1] = n1 * PO[1] + t1 * PO[2] + m1 * PO[3];
+    Pout[2] = n2 * PO[1] + t2 * PO[2] + m2 * PO[3];
+    Pout[3] = n3 * PO[1] + t3 * PO[2] + m3 * PO[3];
+    Pout[4] = spi4 * (n1 * PO[5] + t1 * PO[6] + m1 * PO[7]);
+    Pout[5] = spi4 * (n2 * PO[5] + t2 * PO[6] + m2 * PO[7]);
+    Pout[6] = spi4 * (n3 * PO[5] + t3 * PO[6] + m3 * PO[7]);
+    Pout[7] = PO[4];
+    *PQ = PO[8];
+    return time;
+}
+
+// Solvers::HLLD_Solver_Alexashov (Solvers.cpp:92-691).  q = (ro, p, u, v, w,
+// bx, by, bz) in the (x, y, z) frame, n a unit normal (any direction: the
+// frame is built from the mean field), face speed w.  The reference fixes
+// n_state = 1 (Solvers.cpp:95), so the flux it returns is the HLL flux of
+// the MHD system in the moving frame (Solvers.cpp:313-374); its n_state = 3
+// branch is unreachable and is not restated.  q_out[8] = mass, momentum x3,
+// B flux x3, energy; ds = dsl, dsp, dsc.  Where the reference exits
+// (SR <= SL, or SM outside (SL, SR): Solvers.cpp:244-271) ST_WAVE_ORDER is
+// raised instead.  Returns kurant*DIST/max(|dsl|, |dsp|).
+__device__ inline double hlld_alexashov(double ga, double kurant, const double* qqq1, const double* qqq2,
+                                        const double* n, double* qqq, double* ds, double wv, double DIST,
+                                        int* status) {
+    const double spi4 = spi4_dev();
+    const double eps = 10e-10;
+    const double g1 = ga - 1.0;
+    const double r1 = qqq1[0], u1 = qqq1[2], v1 = qqq1[3], w1 = qqq1[4], p1 = qqq1[1];
+    const double bx1 = qqq1[5] / spi4, by1 = qqq1[6] / spi4, bz1 = qqq1[7] / spi4;
+    const double r2 = qqq2[0], u2 = qqq2[2], v2 = qqq2[3], w2 = qqq2[4], p2 = qqq2[1];
+    const double bx2 = qqq2[5] / spi4, by2 = qqq2[6] / spi4, bz2 = qqq2[7] / spi4;
+    const double abx = (bx2 + bx1) / 2.0, aby = (by2 + by1) / 2.0, abz = (bz2 + bz1) / 2.0;
+    const double bk = abx * n[0] + aby * n[1] + abz * n[2];
+    const double b2 = sq(abx) + sq(aby) + sq(abz);
+    double d = b2 - sq(bk);
+    double aco[3][3];
+    aco[0][0] = n[0];
+    aco[1][0] = n[1];
+    aco[2][0] = n[2];
+    if (d > eps) {
+        d = sqrt(d);
+        aco[0][1] = (abx - bk * n[0]) / d;
+        aco[1][1] = (aby - bk * n[1]) / d;
+        aco[2][1] = (abz - bk * n[2]) / d;
+        aco[0][2] = (aby * n[2] - abz * n[1]) / d;
+        aco[1][2] = (abz * n[0] - abx * n[2]) / d;
+        aco[2][2] = (abx * n[1] - aby * n[0]) / d;
+    } else {
+        double aix, aiy, aiz;
+        if ((fabs(n[0]) < fabs(n[1])) && (fabs(n[0]) < fabs(n[2]))) {
+            aix = 1.0; aiy = 0.0; aiz = 0.0;
+        } else if (fabs(n[1]) < fabs(n[2])) {
+            aix = 0.0; aiy = 1.0; aiz = 0.0;
+        } else {
+            aix = 0.0; aiy = 0.0; aiz = 1.0;
+        }
+        const double aik = aix * n[0] + aiy * n[1] + aiz * n[2];
+        d = sqrt(1.0 - sq(aik));
+        aco[0][1] = (aix - aik * n[0]) / d;
+        aco[1][1] = (aiy - aik * n[1]) / d;
+        aco[2][1] = (aiz - aik * n[2]) / d;
+        aco[0][2] = (aiy * n[2] - aiz * n[1]) / d;
+        aco[1][2] = (aiz * n[0] - aix * n[2]) / d;
+        aco[2][2] = (aix * n[1] - aiy * n[0]) / d;
+    }
+    double vL[3], vR[3], bL[3], bR[3];
+    for (int i = 0; i < 3; i++) {
+        vL[i] = aco[0][i] * u1 + aco[1][i] * v1 + aco[2][i] * w1;
+        vR[i] = aco[0][i] * u2 + aco[1][i] * v2 + aco[2][i] * w2;
+        bL[i] = aco[0][i] * bx1 + aco[1][i] * by1 + aco[2][i] * bz1;
+        bR[i] = aco[0][i] * bx2 + aco[1][i] * by2 + aco[2][i] * bz2;
+    }
+    const double aaL = bL[0] / sqrt(r1);
+    const double b2L = sq(bL[0]) + sq(bL[1]) + sq(bL[2]);
+    const double b21 = b2L / r1;
+    const double cL = sqrt(ga * p1 / r1);
+    double qp = sqrt(b21 + cL * (cL + 2.0 * aaL));
+    double qm = sqrt(b21 + cL * (cL - 2.0 * aaL));
+    const double cfL = (qp + qm) / 2.0;
+    const double ptL = p1 + b2L / 2.0;
+    const double aaR = bR[0] / sqrt(r2);
+    const double b2R = sq(bR[0]) + sq(bR[1]) + sq(bR[2]);
+    const double b22 = b2R / r2;
+    const double cR = sqrt(ga * p2 / r2);
+    qp = sqrt(b22 + cR * (cR + 2.0 * aaR));
+    qm = sqrt(b22 + cR * (cR - 2.0 * aaR));
+    const double cfR = (qp + qm) / 2.0;
+    const double ptR = p2 + b2R / 2.0;
+    const double SL = dmin_ref((vL[0] - cfL), (vR[0] - cfR));
+    const double SR = dmax_ref((vL[0] + cfL), (vR[0] + cfR));
+    const double suR = SR - vR[0], suL = SL - vL[0];
+    const double SM = (suR * r2 * vR[0] - ptR + ptL - suL * r1 * vL[0]) / (suR * r2 - suL * r1);
+    if (SR <= SL || SM >= SR || SM <= SL) *status |= ST_WAVE_ORDER;
+    ds[0] = SL;
+    ds[1] = SR;
+    ds[2] = SM;
+    const double UU = dmax_ref(fabs(SL), fabs(SR));
+    const double time = kurant * DIST / UU;
+    const double upt1 = (sq(u1) + sq(v1) + sq(w1)) / 2.0;
+    const double sbv1 = u1 * bx1 + v1 * by1 + w1 * bz1;
+    const double upt2 = (sq(u2) + sq(v2) + sq(w2)) / 2.0;
+    const double sbv2 = u2 * bx2 + v2 * by2 + w2 * bz2;
+    const double e1 = p1 / g1 + r1 * upt1 + b2L / 2.0;
+    const double e2 = p2 / g1 + r2 * upt2 + b2R / 2.0;
+    const double FL[8] = {r1 * vL[0],
+                          r1 * vL[0] * vL[0] + ptL - sq(bL[0]),
+                          r1 * vL[0] * vL[1] - bL[0] * bL[1],
+                          r1 * vL[0] * vL[2] - bL[0] * bL[2],
+                          (e1 + ptL) * vL[0] - bL[0] * sbv1,
+                          0.0,
+                          vL[0] * bL[1] - vL[1] * bL[0],
+                          vL[0] * bL[2] - vL[2] * bL[0]};
+    const double FR[8] = {r2 * vR[0],
+                          r2 * vR[0] * vR[0] + ptR - sq(bR[0]),
+                          r2 * vR[0] * vR[1] - bR[0] * bR[1],
+                          r2 * vR[0] * vR[2] - bR[0] * bR[2],
+                          (e2 + ptR) * vR[0] - bR[0] * sbv2,
+                          0.0,
+                          vR[0] * bR[1] - vR[1] * bR[0],
+                          vR[0] * bR[2] - vR[2] * bR[0]};
+    const double UL[8] = {r1, r1 * vL[0], r1 * vL[1], r1 * vL[2], e1, bL[0], bL[1], bL[2]};
+    const double UR[8] = {r2, r2 * vR[0], r2 * vR[1], r2 * vR[2], e2, bR[0], bR[1], bR[2]};
+    double UZ[8], dq[8], FW[8];
+    for (int ik = 0; ik < 8; ik++) {
+        UZ[ik] = (SR * UR[ik] - SL * UL[ik] + FL[ik] - FR[ik]) / (SR - SL);
+        dq[ik] = UR[ik] - UL[ik];
+        FW[ik] = 0.0;
+    }
+    double TL = SL, TR = SR;
+    if (SL > wv) {
+        TL = 0.0;
+        for (int ik = 0; ik < 8; ik++) FW[ik] = wv * UL[ik];
+    }
+    if ((SL <= wv) && (wv <= SR))
+        for (int ik = 0; ik < 8; ik++) FW[ik] = wv * UZ[ik];
+    if (SR < wv) {
+        TR = 0.0;
+        for (int ik = 0; ik < 8; ik++) FW[ik] = wv * UR[ik];
+    }
+    const double a = TR * TL, b = TR - TL;
+    double qv[3], qb[3];
+    const double q0 = (TR * FL[0] - TL * FR[0] + a * dq[0]) / b - FW[0];
+    const double q4 = (TR * FL[4] - TL * FR[4] + a * dq[4]) / b - FW[4];
+    for (int ik = 1; ik < 4; ik++) qv[ik - 1] = (TR * FL[ik] - TL * FR[ik] + a * dq[ik]) / b - FW[ik];
+    for (int ik = 5; ik < 8; ik++) qb[ik - 5] = (TR * FL[ik] - TL * FR[ik] + a * dq[ik]) / b - FW[ik];
+    qqq[0] = q0;
+    for (int i = 0; i < 3; i++) {
+        qqq[i + 1] = aco[i][0] * qv[0] + aco[i][1] * qv[1] + aco[i][2] * qv[2];
+        qqq[i + 4] = spi4 * (aco[i][0] * qb[0] + aco[i][1] * qb[1] + aco[i][2] * qb[2]);
+    }
+    qqq[7] = q4;
     return time;
 }
 

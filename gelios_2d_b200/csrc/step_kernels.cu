@@ -1727,6 +1727,51 @@ __global__ void godunov_batch_kernel(gelios_params P, int n, const double* __res
     o[9] = status;
 }
 
+// HLLDQ_Korolkov batch: in[23] = L[9], R[9], n[3], rad, metod; out[10] =
+// time, P[8], PQ.
+__global__ void hlldq_batch_kernel(gelios_params P, int n, const double* __restrict__ in, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double* a = in + 23 * i;
+    double L[9], R[9], Po[8], PQ = 0.0;
+    for (int k = 0; k < 9; k++) {
+        L[k] = a[k];
+        R[k] = a[9 + k];
+    }
+    for (int k = 0; k < 8; k++) Po[k] = 0.0;
+    const double t = hlldq_korolkov(P.gamma, P.kurant, L, R, a[18], a[19], a[20], a[21], static_cast<int>(a[22]),
+                                    Po, &PQ);
+    double* o = out + 10 * i;
+    o[0] = t;
+    for (int k = 0; k < 8; k++) o[1 + k] = Po[k];
+    o[9] = PQ;
+}
+
+// HLLD_Solver_Alexashov batch: in[21] = q1[8], q2[8], n[3], w, dist; out[13]
+// = time, q[8], dsl, dsp, dsc, status.
+__global__ void hlld_batch_kernel(gelios_params P, int n, const double* __restrict__ in, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double* a = in + 21 * i;
+    double q1[8], q2[8], nv[3], q[8], ds[3];
+    for (int k = 0; k < 8; k++) {
+        q1[k] = a[k];
+        q2[k] = a[8 + k];
+    }
+    nv[0] = a[16];
+    nv[1] = a[17];
+    nv[2] = a[18];
+    int status = 0;
+    const double t = hlld_alexashov(P.gamma, P.kurant, q1, q2, nv, q, ds, a[19], a[20], &status);
+    double* o = out + 13 * i;
+    o[0] = t;
+    for (int k = 0; k < 8; k++) o[1 + k] = q[k];
+    o[9] = ds[0];
+    o[10] = ds[1];
+    o[11] = ds[2];
+    o[12] = status;
+}
+
 // ------------------------------------------------------------------ launchers
 namespace {
 inline int blocks_for(int n, int t) { return (n + t - 1) / t; }
@@ -1813,6 +1858,12 @@ int launch_motion(const DevMesh& d, const gelios_params& P, const StepBuffers& b
 }
 void launch_hllc_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s) {
     hllc_batch_kernel<<<blocks_for(n, 128), 128, 0, s>>>(P, n, in, out);
+}
+void launch_hlldq_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s) {
+    hlldq_batch_kernel<<<blocks_for(n, 128), 128, 0, s>>>(P, n, in, out);
+}
+void launch_hlld_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s) {
+    hlld_batch_kernel<<<blocks_for(n, 128), 128, 0, s>>>(P, n, in, out);
 }
 void launch_godunov_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s) {
     godunov_batch_kernel<<<blocks_for(n, 2), 64, 0, s>>>(P, n, in, out);

@@ -112,6 +112,8 @@ void launch_dt_finalize(const StepBuffers& b, cudaStream_t s);
 void launch_commit(const DevMesh& d, const StepBuffers& b, cudaStream_t s);
 int launch_motion(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* scratch, cudaStream_t s);
 void launch_hllc_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s);
+void launch_hlldq_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s);
+void launch_hlld_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s);
 void launch_godunov_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s);
 
 }  // namespace gelios

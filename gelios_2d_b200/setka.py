@@ -193,3 +193,24 @@ def godunov_batch(params: N.GeliosParams, rows: np.ndarray) -> np.ndarray:
     N.check(N.lib().gelios_godunov_batch(C.byref(params), len(rows), rows.ravel(), out.ravel()),
             "gelios_godunov_batch")
     return out
+
+
+def hlldq_batch(params: N.GeliosParams, rows: np.ndarray) -> np.ndarray:
+    """Device HLLDQ_Korolkov (Solvers.cpp:1642-2185) over rows of 23 inputs
+    (L[9], R[9], n[3], rad, metod) -> rows of 10 outputs (time, P[8], PQ)."""
+    rows = np.ascontiguousarray(rows, np.float64)
+    out = np.zeros((len(rows), 10))
+    N.check(N.lib().gelios_hlldq_batch(C.byref(params), len(rows), rows.ravel(), out.ravel()),
+            "gelios_hlldq_batch")
+    return out
+
+
+def hlld_batch(params: N.GeliosParams, rows: np.ndarray) -> np.ndarray:
+    """Device HLLD_Solver_Alexashov (Solvers.cpp:92-691) over rows of 21
+    inputs (q1[8], q2[8], n[3], w, dist) -> rows of 13 outputs (time, q[8],
+    dsl, dsp, dsc, status)."""
+    rows = np.ascontiguousarray(rows, np.float64)
+    out = np.zeros((len(rows), 13))
+    N.check(N.lib().gelios_hlld_batch(C.byref(params), len(rows), rows.ravel(), out.ravel()),
+            "gelios_hlld_batch")
+    return out

@@ -105,10 +105,13 @@ typedef struct gelios_mesh_view {
     const int32_t *line_contact, *line_inner, *line_outer; /* Line_Contact/Inner/Outer (sorted by polar angle) */
 } gelios_mesh_view;
 
+#define GELIOS_STATUS_WAVE_ORDER 32
+
 typedef struct gelios_status {
     int32_t flags;      /* bit0 Newton/bisection cap, bit1 non-positive TVD state,
                            bit2 negative Newton pressure, bit3 broken source chain,
-                           bit4 non-finite dt */
+                           bit4 non-finite dt, bit5 MHD wave speeds out of order
+                           (GELIOS_STATUS_WAVE_ORDER) */
     int32_t steps_done;
     int64_t n_ro_clamp; /* updates clamped to ro_floor */
     int64_t n_p_clamp;  /* updates clamped to p_floor */
@@ -195,6 +198,17 @@ int gelios_hllc_batch(const gelios_params *prm, int n, const double *in, double 
 /* Batched Godunov_Solver_Alexashov (Solvers.cpp:693-1172): in[n*15] =
  * q1[5] (ro,p,u,v,w), q2[5], n[3], w, dist; out[n*10] = time, q[5], dsl, dsp, dsc, status. */
 int gelios_godunov_batch(const gelios_params *prm, int n, const double *in, double *out);
+/* Batched Solvers::HLLDQ_Korolkov (Solvers.cpp:1642-2185), MHD flux with the
+ * normal along a coordinate axis: in[n*23] = L[9], R[9] with states (ro, Q,
+ * p, v1, v2, v3, Bx, By, Bz), n1, n2, n3, rad, metod (2: HLLC-type, 3:
+ * HLLD); out[n*10] = time, P[8] (mass, momentum x3, B x3, energy), PQ. */
+int gelios_hlldq_batch(const gelios_params *prm, int n, const double *in, double *out);
+/* Batched Solvers::HLLD_Solver_Alexashov (Solvers.cpp:92-691): in[n*21] =
+ * q1[8], q2[8] with q = (ro, p, u, v, w, bx, by, bz), n[3] (unit, any
+ * direction), w (face speed), dist; out[n*13] = time, q[8] (mass, momentum
+ * x3, B x3, energy), dsl, dsp, dsc, status (GELIOS_STATUS_WAVE_ORDER where
+ * the reference exits). */
+int gelios_hlld_batch(const gelios_params *prm, int n, const double *in, double *out);
 
 /* ---- allocation-free plain step (no counterpart in the reference) ---------
  * For callers that cannot call cudaMalloc when they step (their device memory

@@ -88,6 +88,10 @@ double go_hllc(const go_params *prm, const double *L5, const double *R5, double 
                double n1, double n2, double rad, int metod, double *VlVcVp, int nul_potok);
 double go_godunov(const go_params *prm, const double *q1, const double *q2, const double *n3, double *q5,
                   double *dsl_dsp_dsc, double w, double dist, int *status);
+double go_hlldq(const go_params *prm, const double *L9, const double *R9, double *P8, double *PQ, const double *n3,
+                double rad, int metod);
+double go_hlld(const go_params *prm, const double *q1, const double *q2, const double *n3, double *q8,
+               double *dsl_dsp_dsc, double w, double dist, int *status);
 void go_face_par(void *h, int f, int which, int buf, double *out5);
 void go_cell_geom(void *h, int c, double *out8);
 void go_source_mk1(void *h, int c, double u, double v, double ro, double p, double *q3);

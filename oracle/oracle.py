@@ -97,6 +97,11 @@ def lib() -> C.CDLL:
     L.go_godunov.restype = C.c_double
     L.go_godunov.argtypes = [C.POINTER(GoParams), f64p, f64p, f64p, f64p, f64p, C.c_double, C.c_double,
                              C.POINTER(C.c_int)]
+    L.go_hlldq.restype = C.c_double
+    L.go_hlldq.argtypes = [C.POINTER(GoParams), f64p, f64p, f64p, f64p, f64p, C.c_double, C.c_int]
+    L.go_hlld.restype = C.c_double
+    L.go_hlld.argtypes = [C.POINTER(GoParams), f64p, f64p, f64p, f64p, f64p, C.c_double, C.c_double,
+                          C.POINTER(C.c_int)]
     L.go_face_par.argtypes = [vp, C.c_int, C.c_int, C.c_int, f64p]
     L.go_cell_geom.argtypes = [vp, C.c_int, f64p]
     L.go_source_mk1.argtypes = [vp, C.c_int] + [C.c_double] * 4 + [f64p]
@@ -253,4 +258,25 @@ def godunov(params: GoParams, q1, q2, n, w=0.0, dist=0.0):
     st = C.c_int(0)
     t = lib().go_godunov(C.byref(params), np.asarray(q1, np.float64), np.asarray(q2, np.float64),
                          np.asarray(n, np.float64), q, d, float(w), float(dist), C.byref(st))
+    return t, q, d, st.value
+
+
+def hlldq(params: GoParams, L_state, R_state, n, rad, metod):
+    """HLLDQ_Korolkov (Solvers.cpp:1642-2185); states (ro, Q, p, v1, v2, v3,
+    Bx, By, Bz), n a coordinate axis.  Returns (time, P[8], PQ)."""
+    P = np.zeros(8)
+    PQ = np.zeros(1)
+    t = lib().go_hlldq(C.byref(params), np.asarray(L_state, np.float64), np.asarray(R_state, np.float64), P, PQ,
+                       np.asarray(n, np.float64), float(rad), int(metod))
+    return t, P, PQ[0]
+
+
+def hlld(params: GoParams, q1, q2, n, w=0.0, dist=0.0):
+    """HLLD_Solver_Alexashov (Solvers.cpp:92-691); q = (ro, p, u, v, w, bx,
+    by, bz).  Returns (time, q[8], (dsl, dsp, dsc), status)."""
+    q = np.zeros(8)
+    d = np.zeros(3)
+    st = C.c_int(0)
+    t = lib().go_hlld(C.byref(params), np.asarray(q1, np.float64), np.asarray(q2, np.float64),
+                      np.asarray(n, np.float64), q, d, float(w), float(dist), C.byref(st))
     return t, q, d, st.value

@@ -305,3 +305,14 @@ def hlldq(L_state, R_state, n, rad, metod):
     t = lib().gref_hlldq(np.asarray(L_state, np.float64), np.asarray(R_state, np.float64), P, PQ,
                          np.asarray(n, np.float64), float(rad), int(metod))
     return t, P, PQ[0]
+
+
+def hlld(q1, q2, n, w=0.0, dist=0.0):
+    """HLLD_Solver_Alexashov (Solvers.cpp:92-691); q = (ro, p, u, v, w, bx, by, bz).
+    The reference exits the process where its wave speeds are out of order:
+    screen inputs with the oracle's status first."""
+    q = np.zeros(8)
+    d = np.zeros(3)
+    t = lib().gref_hlld(np.asarray(q1, np.float64), np.asarray(q2, np.float64), np.asarray(n, np.float64), q, d,
+                        float(w), float(dist))
+    return t, q, d

@@ -1,9 +1,10 @@
 """Generates the golden fixtures of tests/golden from the compiled reference.
 
 Run where the reference tree and oracle/_ref/libgelios_ref.so exist:
-    python tests/golden/make_golden.py
-The fixtures are the reference's own outputs (HLLC_2d_Korolkov_b_s,
-Godunov_Solver_Alexashov, and short Go_stationary / Go_5_komponent__MK2 /
+    python tests/golden/make_golden.py [faces] [steps] [mhd]
+(no argument: all).  The fixtures are the reference's own outputs
+(HLLC_2d_Korolkov_b_s, Godunov_Solver_Alexashov, HLLDQ_Korolkov,
+HLLD_Solver_Alexashov, and short Go_stationary / Go_5_komponent__MK2 /
 Go_stationary_5_komponent_inner_MK2 runs on Setka(4,3,3,10,23,6,7,7)), so the
 oracle stays pinned where the reference cannot be built.
 """
@@ -53,8 +54,89 @@ def godunov_cases(n=96, seed=13):
     return np.array(rows)
 
 
-def main():
+AXES = [(1.0, 0.0, 0.0), (0.0, 1.0, 0.0), (0.0, 0.0, 1.0), (-1.0, 0.0, 0.0), (0.0, -1.0, 0.0), (0.0, 0.0, -1.0)]
+
+
+def mhd_state(a, with_q):
+    """(ro, [Q,] p, v1, v2, v3, Bx, By, Bz) from 8 or 9 uniforms."""
+    ro = 0.1 + 2 * a[0]
+    p = 0.05 + 3 * a[1]
+    v = [3 * (a[2] - 0.5), 3 * (a[3] - 0.5), 3 * (a[4] - 0.5)]
+    b = [2 * (a[5] - 0.5), 2 * (a[6] - 0.5), 2 * (a[7] - 0.5)]
+    return [ro, 100 * a[8], p, *v, *b] if with_q else [ro, p, *v, *b]
+
+
+def hlldq_cases(n=120, seed=17):
+    """Rows of 23: L[9], R[9], n[3] (a coordinate axis), rad, metod (2 or 3)."""
+    u = W.splitmix64(seed, n * 20).reshape(n, 20)
+    rows = []
+    for i in range(n):
+        a = u[i]
+        L = mhd_state(a[0:9], True)
+        R = mhd_state(a[9:18], True)
+        if i % 7 == 0:  # weak normal field (the HLLD degenerate branch)
+            L[6 + i % 3] = 1e-5
+            R[6 + i % 3] = -1e-5
+        rows.append([*L, *R, *AXES[i % 6], 0.01 + a[18], 2 + (i // 6) % 2])
+    return np.array(rows)
+
+
+def hlld_cases(n=120, seed=19):
+    """Rows of 21: q1[8], q2[8], n[3] (unit), w, dist; only inputs whose wave
+    speeds are ordered (the reference exits the process otherwise)."""
+    from oracle import oracle as O
+
+    prm = O.reference_params()
+    u = W.splitmix64(seed, 4 * n * 22).reshape(4 * n, 22)
+    rows = []
+    for i in range(4 * n):
+        a = u[i]
+        q1 = mhd_state(a[0:8], False)
+        q2 = mhd_state(a[8:16], False)
+        if i % 5 == 0:
+            nv = np.array(AXES[i % 6])
+        else:
+            nv = np.array([a[16] - 0.5, a[17] - 0.5, a[18] - 0.5])
+            nv /= np.linalg.norm(nv)
+        w = (a[19] - 0.5) * (4.0 if i % 3 == 0 else 0.5)
+        if i % 11 == 0:  # field along the normal (the d <= eps frame branch)
+            q1[5:8] = list(0.5 * nv)
+            q2[5:8] = list(0.5 * nv)
+        row = [*q1, *q2, *nv, w, 0.01 + a[20]]
+        if O.hlld(prm, row[0:8], row[8:16], row[16:19], row[19], row[20])[3] == 0:
+            rows.append(row)
+        if len(rows) == n:
+            break
+    return np.array(rows)
+
+
+def write_mhd():
+    h = hlldq_cases()
+    out = np.zeros((len(h), 10))
+    for i, r in enumerate(h):
+        t, P, PQ = ref.hlldq(r[0:9], r[9:18], r[18:21], r[21], int(r[22]))
+        out[i] = [t, *P, PQ]
+    np.savez_compressed(HERE / "kat_hlldq.npz", inputs=h, outputs=out)
+    g = hlld_cases()
+    out = np.zeros((len(g), 12))
+    for i, r in enumerate(g):
+        t, q, d = ref.hlld(r[0:8], r[8:16], r[16:19], r[19], r[20])
+        out[i] = [t, *q, *d]
+    np.savez_compressed(HERE / "kat_hlld.npz", inputs=g, outputs=out)
+
+
+def main(parts):
     ref.set_threads(1)
+    if "mhd" in parts:
+        write_mhd()
+    if "faces" in parts:
+        write_faces()
+    if "steps" in parts:
+        write_steps()
+    print("golden fixtures written to", HERE)
+
+
+def write_faces():
     h = hllc_cases()
     out = np.zeros((len(h), 9))
     for i, r in enumerate(h):
@@ -68,6 +150,8 @@ def main():
         out[i] = [t, *q, *d]
     np.savez_compressed(HERE / "kat_godunov.npz", inputs=g, outputs=out)
 
+
+def write_steps():
     # short runs on the small rail grid
     S = ref.RefSetka.constructor(*SMALL)
     S.tvd_prepare()
@@ -96,8 +180,7 @@ def main():
         res[f"{name}_x"] = pm["x"]
         res[f"{name}_y"] = pm["y"]
     np.savez_compressed(HERE / "steps_small.npz", **res)
-    print("golden fixtures written to", HERE)
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or ["faces", "steps", "mhd"])

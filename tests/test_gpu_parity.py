@@ -86,6 +86,30 @@ def test_godunov_device_vs_oracle():
     assert np.max(np.abs(dev[:, 0] - ref[:, 0]) / np.abs(ref[:, 0])) <= 1e-11
 
 
+def test_hlldq_device_vs_reference_vectors():
+    d = np.load(GOLD / "kat_hlldq.npz")
+    P = N.reference_params()
+    dev = g.hlldq_batch(P, d["inputs"])
+    ref = d["outputs"]
+    scale = np.maximum(np.max(np.abs(ref[:, 1:10]), axis=1), 1e-300)
+    err = np.max(np.abs(dev[:, 1:10] - ref[:, 1:10]), axis=1) / scale
+    assert np.max(err) <= 1e-12, np.max(err)
+    assert np.max(np.abs(dev[:, 0] - ref[:, 0]) / np.abs(ref[:, 0])) <= 1e-13
+
+
+def test_hlld_device_vs_reference_vectors():
+    d = np.load(GOLD / "kat_hlld.npz")
+    P = N.reference_params()
+    dev = g.hlld_batch(P, d["inputs"])
+    ref = d["outputs"]
+    assert np.all(dev[:, 12] == 0)
+    scale = np.maximum(np.max(np.abs(ref[:, 1:9]), axis=1), 1e-300)
+    err = np.max(np.abs(dev[:, 1:9] - ref[:, 1:9]), axis=1) / scale
+    assert np.max(err) <= 1e-12, np.max(err)
+    assert np.max(np.abs(dev[:, 9:12] - ref[:, 9:12]) / np.maximum(np.abs(ref[:, 9:12]), 1e-300)) <= 1e-13
+    assert np.max(np.abs(dev[:, 0] - ref[:, 0]) / np.abs(ref[:, 0])) <= 1e-13
+
+
 # ------------------------------------------------------------------ Go_stationary (plain single fluid)
 @pytest.mark.parametrize("steps", [1, 2, 10])
 def test_stationary_plain_small(steps):

@@ -44,6 +44,36 @@ def test_godunov_golden_bitexact():
         assert np.array_equal(np.array([t, *q, *ds]), o, equal_nan=True)
 
 
+def test_hlldq_golden_bitexact():
+    """HLLDQ_Korolkov (Solvers.cpp:1642-2185), metods 2 and 3, six axis normals."""
+    d = np.load(GOLD / "kat_hlldq.npz")
+    P0 = O.reference_params()
+    assert set(d["inputs"][:, 22].astype(int)) == {2, 3}
+    for r, o in zip(d["inputs"], d["outputs"]):
+        t, P, PQ = O.hlldq(P0, r[0:9], r[9:18], r[18:21], r[21], int(r[22]))
+        assert np.array_equal(np.array([t, *P, PQ]), o, equal_nan=True)
+
+
+def test_hlld_golden_bitexact():
+    """HLLD_Solver_Alexashov (Solvers.cpp:92-691) with face speed, any normal."""
+    d = np.load(GOLD / "kat_hlld.npz")
+    P0 = O.reference_params()
+    for r, o in zip(d["inputs"], d["outputs"]):
+        t, q, ds, st = O.hlld(P0, r[0:8], r[8:16], r[16:19], r[19], r[20])
+        assert st == 0
+        assert np.array_equal(np.array([t, *q, *ds]), o, equal_nan=True)
+
+
+def test_hlld_reports_wave_order_instead_of_exiting():
+    """Where the reference exits (SR <= SL, Solvers.cpp:244-249) the oracle
+    raises the status bit and returns: two equal states without pressure and
+    field have no fast speed, so SL == SR (planted on the CPU)."""
+    P0 = O.reference_params()
+    q = [1.0, 0.0, 0.5, 0.0, 0.0, 0.0, 0.0, 0.0]
+    _, _, _, st = O.hlld(P0, q, q, [1.0, 0.0, 0.0], 0.0, 1.0)
+    assert st & 32
+
+
 def _oracle_on_small(mesh_dict, g):
     o = O.Oracle(O.reference_params(), mesh_dict)
     o.set_state(0, g["state0"])
