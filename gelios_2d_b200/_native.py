@@ -123,6 +123,7 @@ def lib() -> C.CDLL:
     L.gelios_mesh_build_polar.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double]
     L.gelios_mesh_tvd_prepare.argtypes = [vp]
     L.gelios_tvd_prepare_view.argtypes = [C.POINTER(GeliosMeshView), ip, ip, ip, ip, dp]
+    L.gelios_tvd_prepare_view_numbered.argtypes = [C.POINTER(GeliosMeshView), C.c_int, ip, ip, ip, ip, dp]
     L.gelios_mesh_inner_cells.argtypes = [vp, C.c_double, C.POINTER(C.c_int32), C.c_int32]
     L.gelios_mesh_get_view.argtypes = [vp, C.POINTER(GeliosMeshView)]
     L.gelios_mesh_free.argtypes = [vp]

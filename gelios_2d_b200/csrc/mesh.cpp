@@ -71,6 +71,10 @@ struct gelios_mesh {
     std::vector<int32_t> rtype, rM, rpstart, rpts, rkstart, rkeys;
     std::vector<double> rs;
     std::vector<int32_t> lcontact, linner, louter;
+    // Gran::number as TVD_prepare sees it: 0 = the constructor's numbering
+    // (All_Gran and All_Gran_copy each from 0, so numbers collide), 1 = the
+    // unique numbering Download_Setka_ALL_ALPHA_2_0 gives (Setka.cpp:3213-3224)
+    int32_t unique_face_numbers = 0;
 };
 
 namespace {
@@ -808,7 +812,8 @@ extern "C" int gelios_mesh_tvd_prepare(gelios_mesh* m) {
     const int nf = static_cast<int>(m->fA.size());
     const int nm = m->n_main;
     const int ncell = static_cast<int>(m->ctype.size());
-    auto number = [&](int f) { return f < nm ? f : f - nm; };  // Gran::number (colliding lists)
+    const bool uniq = m->unique_face_numbers != 0;
+    auto number = [&](int f) { return (uniq || f < nm) ? f : f - nm; };  // Gran::number
     auto cell_center = [&](int k, double& ox, double& oy) {  // Cell::Get_Center, Cell.cpp:66-88
         const int s = m->cstart[k], e = m->cstart[k + 1], n = e - s;
         double A = 0.0, Gx = 0.0, Gy = 0.0;
@@ -981,13 +986,15 @@ extern "C" int gelios_mesh_get_view(const gelios_mesh* m, gelios_mesh_view* v) {
 
 extern "C" void gelios_mesh_free(gelios_mesh* m) { delete m; }
 
-extern "C" int gelios_tvd_prepare_view(const gelios_mesh_view* v, int32_t* sosed_up, int32_t* sosed_down,
-                                       int32_t* back, int32_t* next, double* r_istoch) {
+extern "C" int gelios_tvd_prepare_view_numbered(const gelios_mesh_view* v, int unique_face_numbers,
+                                                int32_t* sosed_up, int32_t* sosed_down, int32_t* back,
+                                                int32_t* next, double* r_istoch) {
     if (!v || v->n_cells <= 0 || v->n_faces <= 0) {
         gelios::set_error("gelios_tvd_prepare_view: empty view");
         return GELIOS_E_ARG;
     }
     gelios_mesh* m = gelios::mesh_from_view(v);
+    m->unique_face_numbers = unique_face_numbers ? 1 : 0;
     const int rc = gelios_mesh_tvd_prepare(m);
     if (rc == GELIOS_OK) {
         if (sosed_up) std::copy(m->fsup.begin(), m->fsup.end(), sosed_up);
@@ -998,4 +1005,9 @@ extern "C" int gelios_tvd_prepare_view(const gelios_mesh_view* v, int32_t* sosed
     }
     delete m;
     return rc;
+}
+
+extern "C" int gelios_tvd_prepare_view(const gelios_mesh_view* v, int32_t* sosed_up, int32_t* sosed_down,
+                                       int32_t* back, int32_t* next, double* r_istoch) {
+    return gelios_tvd_prepare_view_numbered(v, 0, sosed_up, sosed_down, back, next, r_istoch);
 }

@@ -186,7 +186,11 @@ class Mesh(dict):
         back = np.zeros(nc, np.int32)
         nxt = np.zeros(nc, np.int32)
         ri = np.zeros(nc)
-        N.check(N.lib().gelios_tvd_prepare_view(C.byref(v), up, down, back, nxt, ri), "gelios_tvd_prepare_view")
+        # a grid loaded from a checkpoint carries the loader's unique face
+        # numbers (see gelios_tvd_prepare_view_numbered)
+        uniq = 1 if self.get("face_numbering") == "unique" else 0
+        N.check(N.lib().gelios_tvd_prepare_view_numbered(C.byref(v), uniq, up, down, back, nxt, ri),
+                "gelios_tvd_prepare_view_numbered")
         self.update(face_sosed_up=up, face_sosed_down=down, cell_back=back, cell_next=nxt, r_istoch=ri)
         return self
 

@@ -14,6 +14,8 @@ reference (Setka.h)                          here
 ``Go_stationary(int)``                       ``Go_stationary(step)``
 ``Go_5_komponent__MK2(int)``                 ``Go_5_komponent__MK2(step)``
 ``Go_stationary_5_komponent_inner_MK2(int)`` ``Go_stationary_5_komponent_inner_MK2(step)``
+``Save_Setka_ALL_ALPHA(string)``             ``Save_Setka_ALL_ALPHA(name)``
+``Download_Setka_ALL_ALPHA_2_0(string)``     ``Setka.Download_Setka_ALL_ALPHA_2_0(name)``
 ==========================================  =====================================
 
 As in the reference, a step call restarts dt at 1e-8 and the newest state
@@ -32,7 +34,7 @@ from . import _native as N
 from .mesh import Mesh
 
 STATUS_BITS = {1: "newton/bisection iteration cap", 2: "non-positive TVD state", 4: "negative Newton pressure",
-               8: "broken source chain", 16: "non-finite dt"}
+               8: "broken source chain", 16: "non-finite dt", 32: "MHD wave speeds out of order"}
 
 
 class StepError(RuntimeError):
@@ -65,6 +67,32 @@ class Setka:
     @classmethod
     def from_constructor(cls, N1, N2, N3, N4, M1, M2, M3, M4, params=None, device=0) -> "Setka":
         return cls(Mesh.setka(N1, N2, N3, N4, M1, M2, M3, M4, tvd=True), params, device)
+
+    @classmethod
+    def Download_Setka_ALL_ALPHA_2_0(cls, name, params=None, device=0) -> "Setka":
+        """Setka::Download_Setka_ALL_ALPHA_2_0 (Setka.cpp:2899-3257) followed
+        by TVD_prepare: grid, par[0] (copied to par[1], as the loader does)
+        and Monte-Carlo moments from the reference's text checkpoint."""
+        from . import checkpoint
+
+        c = checkpoint.read_alpha(name)
+        S = cls(c.mesh, params, device)
+        S.set_par(0, c.par)
+        S.set_par(1, c.par)
+        S.set_mc(*c.mc)
+        S._ckpt_extra = (c.hydrogen, c.I)
+        return S
+
+    def Save_Setka_ALL_ALPHA(self, name, buf: int = 0):
+        """Setka::Save_Setka_ALL_ALPHA (Setka.cpp:2355-2574): the grid at its
+        current point positions and par[buf] (the reference saves par[0]) in
+        the reference's text format (6 significant digits)."""
+        from . import checkpoint
+
+        m = Mesh.from_arrays(dict(self.mesh))
+        m["x"], m["y"] = self.points()
+        hyd, I = getattr(self, "_ckpt_extra", (None, None))
+        checkpoint.write_alpha(name, m, self.par(buf), getattr(self, "_mc", None), hyd, I)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -151,6 +179,7 @@ class Setka:
     def set_mc(self, Hn, Hu, Hv, HT, ku, kv, kT):
         """Monte-Carlo moments of par[0] (H_n/H_u/H_v/H_T[4], k_u/k_v/k_T)."""
         f = lambda a: np.ascontiguousarray(a, np.float64).ravel()  # noqa: E731
+        self._mc = (Hn, Hu, Hv, HT, ku, kv, kT)
         N.check(self._L.gelios_upload_mc(self._h, f(Hn), f(Hu), f(Hv), f(HT), f(ku), f(kv), f(kT)),
                 "gelios_upload_mc")
 

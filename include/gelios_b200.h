@@ -143,6 +143,13 @@ int gelios_mesh_tvd_prepare(gelios_mesh *m);
  * and n_cells Back/Next/r_istoch (any output pointer may be NULL). */
 int gelios_tvd_prepare_view(const gelios_mesh_view *v, int32_t *sosed_up, int32_t *sosed_down, int32_t *back,
                             int32_t *next, double *r_istoch);
+/* The same with the face numbering chosen: unique_face_numbers = 0 for a grid
+ * built by the constructor (All_Gran and All_Gran_copy numbered from 0 each),
+ * 1 for a grid loaded by Setka::Download_Setka_ALL_ALPHA_2_0 (main faces then
+ * copies, Setka.cpp:3213-3224).  TVD_prepare compares these numbers
+ * (Setka.cpp:1328, 1383), so the two grids get different TVD neighbours. */
+int gelios_tvd_prepare_view_numbered(const gelios_mesh_view *v, int unique_face_numbers, int32_t *sosed_up,
+                                     int32_t *sosed_down, int32_t *back, int32_t *next, double *r_istoch);
 /* Cells whose centroid radius is <= r_max (All_Cells_Inner, Gelios_2D.cpp:152-231). */
 int gelios_mesh_inner_cells(const gelios_mesh *m, double r_max, int32_t *out, int32_t cap);
 /* Pointers into the mesh (valid until gelios_mesh_free). */

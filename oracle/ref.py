@@ -43,6 +43,9 @@ def lib(fast: bool = False) -> C.CDLL:
     vp = C.c_void_p
     L.gref_setka_new.restype = vp
     L.gref_setka_new.argtypes = [C.c_int] * 8
+    L.gref_save_alpha.argtypes = [vp, C.c_char_p]
+    L.gref_load_alpha.restype = vp
+    L.gref_load_alpha.argtypes = [C.c_char_p]
     L.gref_setka_from_arrays.restype = vp
     L.gref_setka_from_arrays.argtypes = [
         _i32p,
@@ -124,6 +127,18 @@ class RefSetka:
     def constructor(cls, N1, N2, N3, N4, M1, M2, M3, M4, fast=False) -> "RefSetka":
         L = lib(fast)
         return cls(L.gref_setka_new(N1, N2, N3, N4, M1, M2, M3, M4), L, (N1, N2, N3, N4, M1, M2, M3, M4))
+
+    @classmethod
+    def load_alpha(cls, path, fast=False) -> "RefSetka":
+        """Setka::Download_Setka_ALL_ALPHA_2_0 (Setka.cpp:2899-3257) into a fresh Setka."""
+        L = lib(fast)
+        with open(path) as f:
+            dims = tuple(int(t) for t in f.readline().split()[:8])
+        return cls(L.gref_load_alpha(str(path).encode()), L, dims)
+
+    def save_alpha(self, path):
+        """Setka::Save_Setka_ALL_ALPHA (Setka.cpp:2355-2574)."""
+        self.L.gref_save_alpha(self.h, str(path).encode())
 
     @classmethod
     def from_mesh(cls, m: dict, fast=False) -> "RefSetka":

@@ -140,6 +140,31 @@ void* gref_setka_new(int N1, int N2, int N3, int N4, int M1, int M2, int M3, int
     return h;
 }
 
+// Setka::Save_Setka_ALL_ALPHA (Setka.cpp:2355-2574) of a grid to a text file.
+void gref_save_alpha(void* hv, const char* path) {
+    Quiet q;
+    auto* h = static_cast<Handle*>(hv);
+    h->S->Save_Setka_ALL_ALPHA(std::string(path));
+}
+
+// A fresh Setka filled by Setka::Download_Setka_ALL_ALPHA_2_0
+// (Setka.cpp:2899-3257).  The loader leaves the source chains unset; they
+// start empty, as after the constructor.
+void* gref_load_alpha(const char* path) {
+    Quiet q;
+    auto* h = new Handle();
+    h->S = new Setka();
+    h->S->Download_Setka_ALL_ALPHA_2_0(std::string(path));
+    for (auto c : h->S->All_Cells) {
+        c->Back = nullptr;
+        c->Next = nullptr;
+        c->r_istoch = 0.0;
+        for (int k = 0; k < 5; ++k) c->Potok[k] = 0.0;
+    }
+    h->index();
+    return h;
+}
+
 // Instantiates reference objects from flat arrays (same layout as the export).
 // dims: N1..M4 of the Setka these arrays describe (used by Move_surface /
 // Move_Setka_Calculate_2), or zeros for a grid without rails.

@@ -1,7 +1,7 @@
 """Generates the golden fixtures of tests/golden from the compiled reference.
 
 Run where the reference tree and oracle/_ref/libgelios_ref.so exist:
-    python tests/golden/make_golden.py [faces] [steps] [mhd]
+    python tests/golden/make_golden.py [faces] [steps] [mhd] [checkpoint]
 (no argument: all).  The fixtures are the reference's own outputs
 (HLLC_2d_Korolkov_b_s, Godunov_Solver_Alexashov, HLLDQ_Korolkov,
 HLLD_Solver_Alexashov, and short Go_stationary / Go_5_komponent__MK2 /
@@ -125,8 +125,37 @@ def write_mhd():
     np.savez_compressed(HERE / "kat_hlld.npz", inputs=g, outputs=out)
 
 
+def write_checkpoint():
+    """Setka::Save_Setka_ALL_ALPHA of the small rail grid with the reference's
+    initial field and seeded moments, and the reference's own state after 3
+    Go_5_komponent__MK2 steps on the grid Download_Setka_ALL_ALPHA_2_0 reads
+    back from that file."""
+    S = ref.RefSetka.constructor(*SMALL)
+    S.tvd_prepare()
+    S.init_conditions()
+    m = Mesh.from_arrays(S.export())
+    S.set_mc(*W.mc_fields(m, seed=23))
+    import gzip
+    import shutil
+    import tempfile
+
+    with tempfile.TemporaryDirectory() as tmp:
+        path = Path(tmp) / "alpha_small.txt"
+        S.save_alpha(path)
+        R = ref.RefSetka.load_alpha(path)
+        with open(path, "rb") as src, gzip.GzipFile(HERE / "alpha_small.txt.gz", "wb", mtime=0) as dst:
+            shutil.copyfileobj(src, dst)
+    R.tvd_prepare()
+    R.go_mk2(3)
+    pm = R.point_motion()
+    np.savez_compressed(HERE / "steps_alpha_small.npz", par0=R.get_state(0), par1=R.get_state(1), x=pm["x"],
+                        y=pm["y"])
+
+
 def main(parts):
     ref.set_threads(1)
+    if "checkpoint" in parts:
+        write_checkpoint()
     if "mhd" in parts:
         write_mhd()
     if "faces" in parts:
@@ -183,4 +212,4 @@ def write_steps():
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or ["faces", "steps", "mhd"])
+    main(sys.argv[1:] or ["faces", "steps", "mhd", "checkpoint"])
