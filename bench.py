@@ -191,6 +191,38 @@ def cpu_reference_rate(mesh, params, st0, mc, counted, form, budget_s=12.0, max_
     return counted * steps / el, steps, threads, el
 
 
+def fp32_flux_errors(mesh, params32, st0, mc, fcode, device, counts=(1, 100, 2000)) -> dict:
+    """L1 and Linf relative errors of rho, p, u, v of the FP32-flux form
+    against the FP64 path (itself within 1e-12 per step of the reference's
+    CPU step) after 1, 100 and 2000 steps from the same initial state."""
+    import numpy as np
+
+    import gelios_2d_b200 as g
+    from gelios_2d_b200 import _native as N
+
+    params64 = params32.copy(precision=N.PREC_FP64)
+    out = {"against": "FP64 device path"}
+    for n in counts:
+        res = []
+        for prm in (params32, params64):
+            S = g.Setka(mesh, prm, device=device)
+            S.set_par(0, st0)
+            S.set_par(1, st0)
+            if mc is not None:
+                S.set_mc(*mc)
+            st = S.step(fcode, n)
+            res.append(S.par(st.result_buf))
+            S.close()
+        a, b = res
+        errs = {}
+        for k, name in enumerate(("rho", "p", "u", "v")):
+            d = np.abs(a[k] - b[k])
+            errs[name] = {"L1": float(d.sum() / max(np.abs(b[k]).sum(), 1e-300)),
+                          "Linf": float(d.max() / max(np.abs(b[k]).max(), 1e-300))}
+        out[str(n)] = errs
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -207,6 +239,8 @@ def main():
     world = _env_int("WORLD_SIZE", 1)
     local = _env_int("LOCAL_RANK", 0)
 
+    if args.impl == "reference" and rank != 0:
+        return  # the reference arm runs on rank 0 only
     desc, form, dims, mesh, params, st0, mc, counted = build_workload(args.workload)
     config = {"workload": desc, "cells": int(mesh.n_cells), "cells_updated_per_step": int(counted),
               "faces": int(mesh.n_faces), "points": int(mesh.n_points),
@@ -214,8 +248,6 @@ def main():
                     "inputs larger than L2", "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
 
     if args.impl == "reference":
-        if rank != 0:
-            return
         rate, steps, threads, el = cpu_reference_rate(mesh, params, st0, mc, counted, form)
         line = {"metric": METRIC, "value": rate, "unit": "cell-updates/s", "impl": "reference",
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -231,6 +263,7 @@ def main():
 
     import gelios_2d_b200 as g
     from gelios_2d_b200 import _native as N
+    from gelios_2d_b200.replicas import max_over_ranks, whole_job_rate
 
     dist = None
     if world > 1:
@@ -284,13 +317,9 @@ def main():
     if dist:
         dist.barrier()
     clocks = sampler.stop()
-    total_ms = sum(a.elapsed_time(b) for a, b in evs)
-    if dist:
-        t = torch.tensor([total_ms], device=f"cuda:{device}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in evs), dist, f"cuda:{device}")
     n_steps_total = args.steps * steps_per_call
-    value = world * counted * n_steps_total / (total_ms / 1000.0)
+    value = whole_job_rate(counted * n_steps_total, world, total_ms / 1000.0)
 
     # per-phase device times, from a separate untimed pass with events
     # between the phases (the timed pass replays the captured step)
@@ -312,12 +341,8 @@ def main():
         S.set_par(0, host_in)
         S.step_async(fcode, 1)
         S.par(1, out=host_out)
-    e2e_s = time.perf_counter() - t0
-    e2e_value = world * counted * e2e_steps / e2e_s
-    if dist:
-        t = torch.tensor([e2e_s], device=f"cuda:{device}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_value = world * counted * e2e_steps / float(t.item())
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{device}")
+    e2e_value = whole_job_rate(counted * e2e_steps, world, e2e_s)
 
     # roofline of the step as a whole: its kernels run concurrently on three
     # streams (one CUDA graph per step), so the unit of work the algorithmic
@@ -342,6 +367,8 @@ def main():
         "phases_ms": {k: v[0] for k, v in phases.items()},
         "clocks": clocks,
     }
+    if args.precision == "fp32flux" and rank == 0:
+        line["fp32_flux_errors"] = fp32_flux_errors(mesh, params, st0, mc, fcode, device)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             rate, steps, threads, el = cpu_reference_rate(mesh, params, st0, mc, counted, form)

@@ -153,6 +153,10 @@ class Setka:
             raise StepError(st)
         return st
 
+    def step(self, form: int, step: int) -> N.GeliosStatus:
+        """`step` iterations of the given form (N.FORM_*), synchronously."""
+        return self._go(form, step)
+
     def step_async(self, form: int, step: int):
         """Enqueue `step` iterations without synchronising (timing loops)."""
         N.check(self._L.gelios_step(self._h, int(form), int(step), None), "gelios_step")
