@@ -27,6 +27,7 @@ GELIOS_E_LIMIT = -6
 FORM_STATIONARY = 0
 FORM_MK2 = 1
 FORM_INNER_MK2 = 2
+FORM_5_KOMPONENT = 3
 PREC_FP64 = 0
 PREC_FP32_FLUX = 1
 
@@ -133,6 +134,8 @@ def lib() -> C.CDLL:
     L.gelios_upload_topology.argtypes = [vp, C.POINTER(GeliosMeshView)]
     L.gelios_upload_state.argtypes = [vp, C.c_int] + [dp] * 5
     L.gelios_download_state.argtypes = [vp, C.c_int] + [dp] * 5
+    L.gelios_upload_hydrogen.argtypes = [vp, C.c_int, dp]
+    L.gelios_download_hydrogen.argtypes = [vp, C.c_int, dp]
     L.gelios_upload_mc.argtypes = [vp] + [dp] * 7
     L.gelios_set_inner_cells.argtypes = [vp, C.POINTER(C.c_int32), C.c_int32]
     L.gelios_step.argtypes = [vp, C.c_int, C.c_int, C.POINTER(GeliosStatus)]

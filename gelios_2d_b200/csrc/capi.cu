@@ -91,7 +91,7 @@ struct gelios_ctx {
     bool have_mesh = false;
     DevMesh d;
     // topology / geometry
-    DBuf X, Y, X2, Y2, ptype, cstart, contour, gstart, cflags, sA, sB, snb, ssd, ssd2, sinfo;
+    DBuf X, Y, X2, Y2, ptype, cstart, contour, gstart, cflags, ctype, sA, sB, snb, ssd, ssd2, sinfo;
     DBuf fA, fB, ftype, fmaster, fsosed, fcopy, fsdown;
     DBuf rtype, rM, rpstart, rpts, rkstart, rkeys, rs;
     DBuf lc, li, lo, sp_point, sp_line, sp_inc, sp_ainc, sp_fix, sp_of_point;
@@ -99,6 +99,7 @@ struct gelios_ctx {
     DBuf Hn, Hu, Hv, HT, ku, kv, kT, r_istoch, cback, cnext;
     // state par[2] x 5 fields, centroids [2], scratch
     DBuf state[2];
+    DBuf hstate[2];  // hydrogen fluids H1..H4 (16 rows) of par[0/1], Go_5_komponent form
     DBuf cen[2];
     DBuf words;    // T[2] (double), dt_acc (u64), counters[2] (u64), status (int)
     DBuf surface;  // Move_surface per-face speeds
@@ -502,6 +503,9 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     rc |= upload(ctx->contour, v->contour, v->contour_start[nc], s);
     rc |= upload(ctx->gstart, v->gran_start, nc + 1, s);
     rc |= upload(ctx->cflags, cflags.data(), nc, s);
+    rc |= upload(ctx->ctype, v->cell_type, nc, s);
+    rc |= upload<double>(ctx->hstate[0], nullptr, 16 * static_cast<size_t>(nc), s);
+    rc |= upload<double>(ctx->hstate[1], nullptr, 16 * static_cast<size_t>(nc), s);
     rc |= upload(ctx->sA, sA.data(), ng, s);
     rc |= upload(ctx->sB, sB.data(), ng, s);
     rc |= upload(ctx->snb, snb.data(), ng, s);
@@ -601,6 +605,7 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     d.contour = ctx->contour.as<int32_t>();
     d.gstart = ctx->gstart.as<int32_t>();
     d.cflags = ctx->cflags.as<uint32_t>();
+    d.ctype = ctx->ctype.as<int32_t>();
     d.sA = ctx->sA.as<int32_t>();
     d.sB = ctx->sB.as<int32_t>();
     d.snb = ctx->snb.as<int32_t>();
@@ -692,6 +697,26 @@ extern "C" int gelios_download_state(gelios_ctx* ctx, int buf, double* ro, doubl
     double* dst[5] = {ro, p, u, v, Q};
     for (int k = 0; k < 5; k++)
         GELIOS_CUDA_TRY(cudaMemcpyAsync(dst[k], ctx->field(buf, k), n, cudaMemcpyDeviceToHost, ctx->stream));
+    GELIOS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_upload_hydrogen(gelios_ctx* ctx, int buf, const double* rows16) {
+    if (!ctx || buf < 0 || buf > 1 || !rows16) return GELIOS_E_ARG;
+    if (!ctx->have_mesh) return GELIOS_E_STATE;
+    GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
+    const size_t n = sizeof(double) * 16 * ctx->d.n_cells;
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(ctx->hstate[buf].p, rows16, n, cudaMemcpyHostToDevice, ctx->stream));
+    GELIOS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_download_hydrogen(gelios_ctx* ctx, int buf, double* rows16) {
+    if (!ctx || buf < 0 || buf > 1 || !rows16) return GELIOS_E_ARG;
+    if (!ctx->have_mesh) return GELIOS_E_STATE;
+    GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
+    const size_t n = sizeof(double) * 16 * ctx->d.n_cells;
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(rows16, ctx->hstate[buf].p, n, cudaMemcpyDeviceToHost, ctx->stream));
     GELIOS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return GELIOS_OK;
 }
@@ -827,7 +852,8 @@ int step_mk2(gelios_ctx* ctx, const StepBuffers& b) {
 
 extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status* status) {
     if (!ctx || nsteps < 0) return GELIOS_E_ARG;
-    if (form != GELIOS_FORM_STATIONARY && form != GELIOS_FORM_MK2 && form != GELIOS_FORM_INNER_MK2) {
+    if (form != GELIOS_FORM_STATIONARY && form != GELIOS_FORM_MK2 && form != GELIOS_FORM_INNER_MK2 &&
+        form != GELIOS_FORM_5_KOMPONENT) {
         set_error("gelios_step: unknown form");
         return GELIOS_E_ARG;
     }
@@ -836,7 +862,8 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
         return GELIOS_E_STATE;
     }
     const DevMesh& d = ctx->d;
-    if (form == GELIOS_FORM_MK2 && (d.n_rail_a + d.n_rail_b + d.n_rail_c + d.n_rail_d == 0 || d.n_lc == 0)) {
+    const bool moving = form == GELIOS_FORM_MK2 || form == GELIOS_FORM_5_KOMPONENT;
+    if (moving && (d.n_rail_a + d.n_rail_b + d.n_rail_c + d.n_rail_d == 0 || d.n_lc == 0)) {
         set_error("gelios_step: the moving-grid form needs rails and tracked lines");
         return GELIOS_E_MESH;
     }
@@ -889,6 +916,27 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             const int n = step_mk2(ctx, b);
             if (n < 0) return n;
             launches += n;
+        } else if (form == GELIOS_FORM_5_KOMPONENT) {
+            // centroids of the current points, Move_surface +
+            // Move_Setka_Calculate, the five-fluid cell update, x = x2
+            b.cx = cen0;
+            b.cy = cen0 + d.n_cells;
+            b.rp = cen0 + 2 * static_cast<size_t>(d.n_cells);
+            if (st > 0) {  // (st == 0: computed above when not cached)
+                launch_centroid(d, d.X, d.Y, cen0, cen0 + d.n_cells, cen0 + 2 * static_cast<size_t>(d.n_cells),
+                                P.gamma, s);
+                launches++;
+            }
+            cudaEvent_t e1 = ctx->phase_begin();
+            const int nm = launch_motion(d, P, b, ctx->surface.as<double>(), s, false);
+            ctx->phase_end(2, e1, nm);
+            cudaEvent_t e3 = ctx->phase_begin();
+            launch_k5_cells(d, P, b, ctx->hstate[cur].as<double>(), ctx->hstate[nxt].as<double>(), s);
+            ctx->phase_end(3, e3, 1);
+            cudaEvent_t e4 = ctx->phase_begin();
+            launch_commit(d, b, s);
+            ctx->phase_end(4, e4, 1);
+            launches += nm + 2;
         } else {
             b.cx = cen0;
             b.cy = cen0 + d.n_cells;
@@ -918,7 +966,9 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
     // centroids of the current points: after an odd number of moving-grid
     // steps they sit in the second buffer; swap so cen[0] holds them
     if (form == GELIOS_FORM_MK2 && (nsteps & 1)) std::swap(ctx->cen[0].p, ctx->cen[1].p);
-    ctx->cen_valid = true;
+    // the five-fluid form leaves the centroids of the points before its
+    // last motion in cen[0]
+    ctx->cen_valid = !(form == GELIOS_FORM_5_KOMPONENT && nsteps > 0);
     if (status) {
         Words r{};
         GELIOS_CUDA_TRY(cudaMemcpyAsync(&r, ctx->words.p, sizeof(r), cudaMemcpyDeviceToHost, s));

@@ -18,7 +18,7 @@ constexpr double kTinyAngle = 0.000001 / 390.222;  // polar_angle threshold, Hel
 
 // Gran_type / Cell_type / Point_type values of the reference.
 enum : int { G_USUALY = 0, G_INNER_SPHERE = 1, G_EXTERN = 2, G_INPUT = 3, G_AXIS = 4, G_UPPER_WALL = 5 };
-enum : int { C_1 = 0, C_CENTR = 5 };
+enum : int { C_1 = 0, C_2 = 1, C_3 = 2, C_4 = 3, C_5 = 4, C_CENTR = 5 };
 enum : int { P_CONTACT = 6, P_INNER_SHOCK = 7, P_OUTER_SHOCK = 8 };
 
 // Slot (cell face) info bits.

@@ -1350,8 +1350,12 @@ __device__ __forceinline__ void c0_key(const DevMesh& d, int q, double dt, doubl
     y2 = d.Y[K0] + dt * V * sn;
 }
 
+// copy_outer_shock: Move_Setka_Calculate_2 gives the D rails beyond
+// n_outer_shock the outer-shock key height of the last D rail before them
+// (Setka.cpp:4725-4728); Move_Setka_Calculate (Setka.cpp:4761-5147, used by
+// Go_5_komponent) is otherwise the same and moves them on their own.
 __global__ void __launch_bounds__(128) rails_kernel(DevMesh d, gelios_params P, const double* __restrict__ dtp,
-                                                    const double* __restrict__ scratch) {
+                                                    const double* __restrict__ scratch, bool copy_outer_shock) {
     const int q = blockIdx.x;
     const double dt = *dtp;
     const int32_t* ap = d.rpts + d.rpstart[q];
@@ -1380,7 +1384,7 @@ __global__ void __launch_bounds__(128) rails_kernel(DevMesh d, gelios_params P, 
         } else {
             if (k == 0) pt = d.rkeys[d.rkstart[first_c]];  // key point 0 of C_Rails[0]
             else if (k < 3) pt = kp[k];
-            else if (q - first_d >= P.n_outer_shock && P.n_outer_shock >= 1)
+            else if (copy_outer_shock && q - first_d >= P.n_outer_shock && P.n_outer_shock >= 1)
                 pt = d.rkeys[d.rkstart[first_d + P.n_outer_shock - 1] + 2];
         }
         double vx = 0.0, vy = 0.0;
@@ -1516,7 +1520,7 @@ __global__ void __launch_bounds__(128) rails_kernel(DevMesh d, gelios_params P, 
         Y2[K1] = Y[K1] + dt * V;
         V = kvy[2];
         X2[K2] = x0;
-        if (jj >= P.n_outer_shock && P.n_outer_shock >= 1) {
+        if (copy_outer_shock && jj >= P.n_outer_shock && P.n_outer_shock >= 1) {
             const int qs = first_d + P.n_outer_shock - 1;
             const int Ks = d.rkeys[d.rkstart[qs] + 2];
             Y2[K2] = Y[Ks] + dt * kvy[3];
@@ -1772,6 +1776,481 @@ __global__ void hlld_batch_kernel(gelios_params P, int n, const double* __restri
     o[12] = status;
 }
 
+// ------------------------------------------------------------------ four hydrogen fluids
+// Setka::Go_5_komponent (Setka.cpp:8269-8950): the plasma and four hydrogen
+// fluids H1..H4, each with its own HLLC flux, on the grid moved by
+// Move_surface + Move_Setka_Calculate.  The 21-field state follows the
+// member order of Parametr's aggregate initialisers (Gran.cpp:262-265):
+// ro, p, u, v, Q, then ro, p, u, v of H1..H4.  One thread per cell, faces in
+// Grans order, every face evaluated from each side as the reference does.
+struct St21 {
+    double f[21];
+};
+constexpr int kRo = 0, kP = 1, kU = 2, kV = 3, kQ = 4;
+__device__ __forceinline__ int fh(int k, int j) { return 5 + 4 * k + j; }  // hydrogen fluid k: ro, p, u, v
+constexpr double kHPow = 0.5;              // H_pow, Help.h:90
+constexpr double kNHOverKn = 1.0 / 6.0;   // n_H_LISM_ / Kn_, Help.h:60, 65
+
+__device__ __forceinline__ St21 load21(const double* const* st, const double* __restrict__ hs, size_t nc, int c) {
+    St21 s;
+#pragma unroll
+    for (int q = 0; q < 5; q++) s.f[q] = st[q][c];
+#pragma unroll
+    for (int q = 0; q < 16; q++) s.f[5 + q] = hs[q * nc + c];
+    return s;
+}
+__device__ __forceinline__ void mirror21(St21& s) {
+    s.f[kV] = -s.f[kV];
+#pragma unroll
+    for (int k = 0; k < 4; k++) s.f[fh(k, 3)] = -s.f[fh(k, 3)];
+}
+
+// Inner_sphere with the hydrogen fluids (Gran.cpp:236-265, 520-534): plasma
+// and H1 of the solar wind, H2..H4 of the master cell.
+__device__ __forceinline__ St21 inner_sphere21(const gelios_params& P, double x, double y, const St21& master) {
+    St21 s = master;
+    const St5 w = inner_sphere_state(P, x, y);
+    s.f[kRo] = w.ro;
+    s.f[kP] = w.p;
+    s.f[kU] = w.u;
+    s.f[kV] = w.v;
+    s.f[kQ] = w.Q;
+    const double dist = sqrt(x * x + y * y);
+    s.f[fh(0, 0)] = 0.0000001;
+    s.f[fh(0, 1)] = (0.0000001 * P.chi * P.chi / (P.gamma * 14.1344 * 14.1344));
+    s.f[fh(0, 2)] = P.chi * x / dist;
+    s.f[fh(0, 3)] = P.chi * y / dist;
+    return s;
+}
+// Input (Gran.cpp:267-276, 536-545): plasma and H4 of the LISM, H1..H3 of the master cell.
+__device__ __forceinline__ St21 input21(const gelios_params& P, const St21& master) {
+    St21 s = master;
+    s.f[kRo] = P.in_ro;
+    s.f[kP] = P.in_p;
+    s.f[kU] = P.in_u;
+    s.f[kV] = P.in_v;
+    s.f[kQ] = P.in_Q;
+    s.f[fh(3, 0)] = 1.0;
+    s.f[fh(3, 1)] = 0.5;
+    s.f[fh(3, 2)] = P.in_u;  // Velosity_inf
+    s.f[fh(3, 3)] = 0.0;
+    return s;
+}
+
+// Gran::Get_par with the hydrogen fluids (Gran.cpp:205-289); own = the face
+// master's state.
+__device__ St21 get_par21(const gelios_params& P, int ft, const St21& own, const double* const* st,
+                          const double* __restrict__ hs, size_t nc, int nb, double fx, double fy) {
+    switch (ft) {
+        case G_USUALY: return load21(st, hs, nc, nb);
+        case G_EXTERN: {
+            St21 s = own;
+            if (s.f[kU] >= 0.0) s.f[kU] = P.extern_u_par;
+            return s;
+        }
+        case G_AXIS: {
+            St21 s = own;
+            mirror21(s);
+            return s;
+        }
+        case G_INNER_SPHERE: return inner_sphere21(P, fx, fy, own);
+        case G_INPUT: return input21(P, own);
+        default: return own;  // Upper_wall
+    }
+}
+
+// Gran::Get_par_TVD of an Usualy face with the hydrogen fluids
+// (Gran.cpp:296-472): master M (state Ms, centroid Mx, My), Sosed So,
+// Sosed_down Sd, face centre (fx, fy).
+__device__ St21 tvd21_usualy(const double* const* st, const double* __restrict__ hs, size_t nc, const double* cx,
+                             const double* cy, double fx, double fy, const St21& Ms, double Mx, double My, int So,
+                             int Sd, bool m_has_axis, bool tracked, int* status) {
+    if (Sd < 0) {
+        St21 par = Ms;
+        if (m_has_axis) {  // Gran.cpp:308-338: mirrored master below the axis
+            const St21 par3 = load21(st, hs, nc, So);
+            const double dist2 = sqrt(sq(fx - Mx) + sq(fy - My));
+            const double dist3 = sqrt(sq(fx - cx[So]) + sq(fy - cy[So]));
+            const double dist1 = sqrt(sq(fx - Mx) + sq(fy - (-My)));
+            const int vi[5] = {kV, fh(0, 3), fh(1, 3), fh(2, 3), fh(3, 3)};
+#pragma unroll
+            for (int q = 0; q < 5; q++)
+                par.f[vi[q]] = linear3(-dist1, -Ms.f[vi[q]], -dist2, Ms.f[vi[q]], dist3, par3.f[vi[q]], 0.0);
+        }
+        return par;
+    }
+    const St21 par1 = load21(st, hs, nc, Sd);
+    const double dist2 = sqrt(sq(fx - Mx) + sq(fy - My));
+    St21 o;
+    if (tracked) {  // Gran.cpp:345-426
+        const double dist1 = sqrt(sq(fx - cx[Sd]) + sq(fy - cy[Sd]));
+        const double r = 1.0 / (-dist1 - (-dist2)), x2 = -dist2;
+#pragma unroll
+        for (int q = 0; q < 21; q++) o.f[q] = (par1.f[q] - Ms.f[q]) * r * (0.0 - x2) + Ms.f[q];
+        if (o.f[kRo] <= 0.0) o.f[kRo] = Ms.f[kRo];
+        if (o.f[kP] <= 0.0) o.f[kP] = Ms.f[kP];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (o.f[fh(k, 0)] <= 0.0) o.f[fh(k, 0)] = Ms.f[fh(k, 0)];
+            if (o.f[fh(k, 1)] <= 0.0) o.f[fh(k, 1)] = Ms.f[fh(k, 1)];
+        }
+        return o;
+    }
+    const St21 par3 = load21(st, hs, nc, So);
+    const double dist3 = sqrt(sq(fx - cx[So]) + sq(fy - cy[So]));
+    const double dist1 = sqrt(sq(fx - cx[Sd]) + sq(fy - cy[Sd]));
+    const double r12 = 1.0 / (-dist1 - (-dist2)), r23 = 1.0 / (-dist2 - dist3), x2 = -dist2;
+#pragma unroll
+    for (int q = 0; q < 21; q++) o.f[q] = linear3r(par1.f[q], Ms.f[q], par3.f[q], r12, r23, x2);
+    if (o.f[kRo] <= 0.0 || o.f[kP] <= 0.0) *status |= ST_TVD_BAD;  // the reference exits (Gran.cpp:444-455)
+    return o;
+}
+
+// Gran::Get_par_TVD of an Axis face with the hydrogen fluids (Gran.cpp:486-519).
+__device__ St21 tvd21_axis(const double* const* st, const double* __restrict__ hs, size_t nc, const double* cx,
+                           const double* cy, double fx, double fy, const St21& Ms, double Mx, double My, int Sd) {
+    St21 o = Ms;
+    if (Sd < 0) return o;
+    const St21 par1 = load21(st, hs, nc, Sd);
+    const double dist2 = sqrt(sq(fx - Mx) + sq(fy - My));
+    const double dist1 = sqrt(sq(fx - cx[Sd]) + sq(fy - cy[Sd]));
+    const int vi[5] = {kV, fh(0, 3), fh(1, 3), fh(2, 3), fh(3, 3)};
+#pragma unroll
+    for (int q = 0; q < 5; q++)
+        o.f[vi[q]] = linear3(-dist1, par1.f[vi[q]], -dist2, Ms.f[vi[q]], dist2, -Ms.f[vi[q]], 0.0);
+    return o;
+}
+
+// Gran::Get_par_TVD_radial with the H1 fields (Gran.cpp:562-675): o = ro,
+// p, p_H1, ro_H1 (the fields Go_5_komponent takes from it,
+// Setka.cpp:8342-8349).
+__device__ void tvd21_radial(const double* const* st, const double* __restrict__ hs, size_t nc, const double* cx,
+                             const double* cy, double fx, double fy, const St21& Ms, double Mx, double My, int So,
+                             int Sd, bool m_has_axis, double g2, double* o) {
+    const double r = sqrt(sq(fx) + sq(fy));
+    St21 par1, par3;
+    double r1, r2, r3, dist1, dist2, dist3;
+    if (Sd < 0) {
+        if (!m_has_axis) {
+            o[0] = Ms.f[kRo];
+            o[1] = Ms.f[kP];
+            o[2] = Ms.f[fh(0, 1)];
+            o[3] = Ms.f[fh(0, 0)];
+            return;
+        }
+        par1 = Ms;
+        mirror21(par1);
+        par3 = load21(st, hs, nc, So);
+        r2 = sqrt(sq(Mx) + sq(My));
+        dist2 = sqrt(sq(fx - Mx) + sq(fy - My));
+        r3 = sqrt(sq(cx[So]) + sq(cy[So]));
+        dist3 = sqrt(sq(fx - cx[So]) + sq(fy - cy[So]));
+        r1 = sqrt(sq(Mx) + sq(-My));
+        dist1 = sqrt(sq(fx - Mx) + sq(fy - (-My)));
+    } else {
+        par1 = load21(st, hs, nc, Sd);
+        par3 = load21(st, hs, nc, So);
+        r2 = sqrt(sq(Mx) + sq(My));
+        dist2 = sqrt(sq(fx - Mx) + sq(fy - My));
+        r3 = sqrt(sq(cx[So]) + sq(cy[So]));
+        dist3 = sqrt(sq(fx - cx[So]) + sq(fy - cy[So]));
+        r1 = sqrt(sq(cx[Sd]) + sq(cy[Sd]));
+        dist1 = sqrt(sq(fx - cx[Sd]) + sq(fy - cy[Sd]));
+    }
+    const double r12 = 1.0 / (-dist1 - (-dist2)), r23 = 1.0 / (-dist2 - dist3), x2 = -dist2;
+    o[0] = linear3r(par1.f[kRo] * sq(r1), Ms.f[kRo] * sq(r2), par3.f[kRo] * sq(r3), r12, r23, x2) / sq(r);
+    o[1] = linear3r(par1.f[kP] * pow(r1, g2), Ms.f[kP] * pow(r2, g2), par3.f[kP] * pow(r3, g2), r12, r23, x2) /
+           pow(r, g2);
+    o[2] = linear3r(par1.f[fh(0, 1)], Ms.f[fh(0, 1)], par3.f[fh(0, 1)], r12, r23, x2);
+    o[3] = linear3r(par1.f[fh(0, 0)] * pow(r1, kHPow), Ms.f[fh(0, 0)] * pow(r2, kHPow),
+                    par3.f[fh(0, 0)] * pow(r3, kHPow), r12, r23, x2) /
+           pow(r, kHPow);
+}
+
+// radial scaling of a side's state to the face centre (Setka.cpp:8337-8341)
+__device__ __forceinline__ void radial_scale21(St21& s, double rc, double dis, double g2) {
+    s.f[kRo] = s.f[kRo] * sq(rc) / sq(dis);
+    s.f[fh(0, 0)] = s.f[fh(0, 0)] * pow(rc / dis, kHPow);
+    s.f[kQ] = s.f[kQ] * sq(rc) / sq(dis);
+    s.f[kP] = s.f[kP] * pow(rc / dis, g2);
+}
+
+// conservative update of one hydrogen fluid with its sources and the
+// cylindrical terms (Setka.cpp:8808-8940)
+__device__ __forceinline__ void k5_update_h(double ga, const double* pot, double ro_H, double p_H, double u_H,
+                                            double v_H, double q1, double q21, double q22, double q3, double VV,
+                                            double rV2, double y, double dt, double ro_floor, double p_floor,
+                                            double* out, int& nro, int& npc) {
+    double ro3 = ro_H * VV - dt * (pot[0] * rV2 + ro_H * v_H / y - q1);
+    if (ro3 <= 0) {
+        ro3 = ro_floor;
+        nro++;
+    }
+    const double rro3 = 1.0 / ro3;
+    const double u3 = (ro_H * u_H * VV - dt * (pot[1] * rV2 + ro_H * v_H * u_H / y - q21)) * rro3;
+    const double v3 = (ro_H * v_H * VV - dt * (pot[2] * rV2 + ro_H * v_H * v_H / y - q22)) * rro3;
+    double p3 = (((p_H / (ga - 1) + ro_H * (u_H * u_H + v_H * v_H) * 0.5) * VV -
+                  dt * (pot[3] * rV2 + v_H * (ga * p_H / (ga - 1) + ro_H * (u_H * u_H + v_H * v_H) * 0.5) / y - q3)) -
+                 0.5 * ro3 * (u3 * u3 + v3 * v3)) *
+                (ga - 1);
+    if (p3 <= 0) {
+        p3 = p_floor;
+        npc++;
+    }
+    out[0] = ro3;
+    out[1] = p3;
+    out[2] = u3;
+    out[3] = v3;
+}
+
+__global__ void __launch_bounds__(128) k5_cell_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                      const double* __restrict__ hcur, double* __restrict__ hnxt) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double tmin = __longlong_as_double(0x7ff0000000000000LL);
+    int nro = 0, npc = 0, status = 0;
+    const size_t nc = d.n_cells;
+    if (c < d.n_cells) {
+        const double x = b.cx[c], y = b.cy[c];
+        const double radius = sqrt(sq(x) + sq(y));
+        if (!(radius < P.R11)) {
+            tmin = 10000000.0;  // `time` starts at 1e7 in every step (Setka.cpp:8286)
+            const double ga = P.gamma, g2 = 2.0 * P.gamma;
+            const double dt = *b.dt_cur;
+            const int kt = d.ctype[c];
+            const uint32_t cf = d.cflags[c];
+            const St21 par1 = load21(b.cur, hcur, nc, c);
+            const int s0 = d.cstart[c], nv = d.cstart[c + 1] - s0;
+            const int32_t* con = d.contour + s0;
+            const int g0 = d.gstart[c], g1 = d.gstart[c + 1];
+            const double Volume = area(con, nv, d.sA, d.sB, g0, g1, d.X, d.Y, false);
+            const double Volume2 = area(con, nv, d.sA, d.sB, g0, g1, d.X2, d.Y2, true);
+            double Potok[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+            double PH[4][4];
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) PH[k][j] = 0.0;
+            for (int g = g0; g < g1; g++) {
+                const uint32_t info = d.sinfo[g];
+                const int ft = info & SI_TYPE_MASK;
+                const int A = d.sA[g], B = d.sB[g], nb = d.snb[g];
+                const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
+                const double S = sqrt(sq(xb - xa) + sq(yb - ya));
+                const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
+                const double x4 = (d.X2[A] + d.X2[B]) / 2.0, y4 = (d.Y2[A] + d.Y2[B]) / 2.0;
+                const double dist = sqrt(sq(x - x2) + sq(y - y2));
+                St21 par11 = par1;
+                St21 par2 = get_par21(P, ft, par1, b.cur, hcur, nc, nb, x2, y2);
+                double t1 = xb - xa, t2 = yb - ya;
+                const double nn = sqrt(sq(t1) + sq(t2));
+                t1 = t1 / nn;
+                t2 = t2 / nn;
+                const double n1 = t2, n2 = -t1;
+                const double W = ((x4 - x2) * n1 + (y4 - y2) * n2) / dt;
+                const double dis = sqrt(sq(x2) + sq(y2));
+                const bool tracked = (info & SI_GOD) != 0;
+                if (ft == G_USUALY) {
+                    const double x3 = b.cx[nb], y3 = b.cy[nb];
+                    const double dd = sqrt(sq(x3) + sq(y3));
+                    if (kt == C_1) {
+                        radial_scale21(par11, radius, dis, g2);
+                        polar_perenos(x, y, x2, y2, par11.f[kU], par11.f[kV]);
+                        polar_perenos(x, y, x2, y2, par11.f[fh(0, 2)], par11.f[fh(0, 3)]);
+                        double o[4];
+                        tvd21_radial(b.cur, hcur, nc, b.cx, b.cy, x2, y2, par1, x, y, nb, d.ssd[g],
+                                     (cf & CF_AXIS) != 0, g2, o);
+                        par11.f[kRo] = o[0];
+                        par11.f[kP] = o[1];
+                        par11.f[fh(0, 1)] = o[2];
+                        par11.f[fh(0, 0)] = o[3];
+                    } else {
+                        par11 = tvd21_usualy(b.cur, hcur, nc, b.cx, b.cy, x2, y2, par1, x, y, nb, d.ssd[g],
+                                             (cf & CF_AXIS) != 0, tracked, &status);
+                    }
+                    const uint32_t nbf = d.cflags[nb];
+                    if (d.ctype[nb] == C_1) {
+                        const St21 parN = par2;  // the neighbour's stored state
+                        radial_scale21(par2, dd, dis, g2);
+                        polar_perenos(x3, y3, x2, y2, par2.f[kU], par2.f[kV]);
+                        polar_perenos(x3, y3, x2, y2, par2.f[fh(0, 2)], par2.f[fh(0, 3)]);
+                        double o[4];
+                        tvd21_radial(b.cur, hcur, nc, b.cx, b.cy, x2, y2, parN, x3, y3, c, d.ssd2[g],
+                                     (nbf & CF_AXIS) != 0, g2, o);
+                        par2.f[kRo] = o[0];
+                        par2.f[kP] = o[1];
+                        par2.f[fh(0, 1)] = o[2];
+                        par2.f[fh(0, 0)] = o[3];
+                    } else {
+                        par2 = tvd21_usualy(b.cur, hcur, nc, b.cx, b.cy, x2, y2, par2, x3, y3, c, d.ssd2[g],
+                                            (nbf & CF_AXIS) != 0, tracked, &status);
+                    }
+                } else if (ft == G_INNER_SPHERE) {
+                    radial_scale21(par11, radius, dis, g2);
+                } else if (kt == C_1 && ft == G_AXIS) {
+                    radial_scale21(par11, radius, dis, g2);
+                    polar_perenos(x, y, x2, y2, par11.f[kU], par11.f[kV]);
+                    polar_perenos(x, y, x2, y2, par11.f[fh(0, 2)], par11.f[fh(0, 3)]);
+                    par2 = par11;
+                    mirror21(par2);
+                } else if (kt != C_1 && ft == G_AXIS) {
+                    par11 = tvd21_axis(b.cur, hcur, nc, b.cx, b.cy, x2, y2, par1, x, y, d.ssd[g]);
+                    par2 = par11;
+                    mirror21(par2);
+                }
+                const bool np = (info & SI_NP) != 0;
+                FluxOut<double> F;
+                for (int hk = 0; hk < 4; hk++) {
+                    if (hk == 0 && kt == C_CENTR) continue;  // H1 not evolved in C_centr (Setka.cpp:8500)
+                    St5 L, R;
+                    L.ro = par11.f[fh(hk, 0)];
+                    L.p = par11.f[fh(hk, 1)];
+                    L.u = par11.f[fh(hk, 2)];
+                    L.v = par11.f[fh(hk, 3)];
+                    L.Q = par11.f[kQ];
+                    R.ro = par2.f[fh(hk, 0)];
+                    R.p = par2.f[fh(hk, 1)];
+                    R.u = par2.f[fh(hk, 2)];
+                    R.v = par2.f[fh(hk, 3)];
+                    R.Q = par2.f[kQ];
+                    const double UU = hllc_flux<double>(ga, P.kurant, L, R, W, n1, n2, 1.0, 1, false, F);
+                    tmin = dmin_ref(tmin, P.kurant * dist / UU);
+                    PH[hk][0] = PH[hk][0] + F.P0 * S;
+                    PH[hk][1] = PH[hk][1] + F.P1 * S;
+                    PH[hk][2] = PH[hk][2] + F.P2 * S;
+                    PH[hk][3] = PH[hk][3] + F.P3 * S;
+                }
+                St5 L, R;
+                L.ro = par11.f[kRo];
+                L.p = par11.f[kP];
+                L.u = par11.f[kU];
+                L.v = par11.f[kV];
+                L.Q = par11.f[kQ];
+                R.ro = par2.f[kRo];
+                R.p = par2.f[kP];
+                R.u = par2.f[kU];
+                R.v = par2.f[kV];
+                R.Q = par2.f[kQ];
+                if (tracked) {
+                    double q1[5] = {L.ro, L.p, L.u, L.v, 0.0};
+                    double q2[5] = {R.ro, R.p, R.u, R.v, 0.0};
+                    double nvv[3] = {n1, n2, 0.0};
+                    double qq[5], ds[3];
+                    const double UG = godunov_dev<false>(ga, P.kurant, q1, q2, nvv, qq, ds, W, dist,
+                                                         P.godunov_max_iter, &status);
+                    tmin = dmin_ref(tmin, P.kurant * dist / UG);
+                    Potok[0] = Potok[0] + qq[0] * S;
+                    Potok[1] = Potok[1] + qq[1] * S;
+                    Potok[2] = Potok[2] + qq[2] * S;
+                    Potok[3] = Potok[3] + qq[4] * S;
+                    const double UU = hllc_flux<double>(ga, P.kurant, L, R, W, n1, n2, 1.0, 1, np, F);
+                    tmin = dmin_ref(tmin, P.kurant * dist / UU);
+                    Potok[4] = Potok[4] + F.PQ * S;
+                } else {
+                    const double UU = hllc_flux<double>(ga, P.kurant, L, R, W, n1, n2, 1.0, 1, np, F);
+                    tmin = dmin_ref(tmin, P.kurant * dist / UU);
+                    Potok[0] = Potok[0] + F.P0 * S;
+                    Potok[1] = Potok[1] + F.P1 * S;
+                    Potok[2] = Potok[2] + F.P2 * S;
+                    Potok[3] = Potok[3] + F.P3 * S;
+                    Potok[4] = Potok[4] + F.PQ * S;
+                }
+            }
+            // multi-fluid charge exchange (Setka.cpp:8575-8660)
+            const double u = par1.f[kU], v = par1.f[kV], ro = par1.f[kRo], p = par1.f[kP], Q = par1.f[kQ];
+            double UM[4], UH[4], nu[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const double roH = par1.f[fh(k, 0)], pH = par1.f[fh(k, 1)];
+                const double uH = par1.f[fh(k, 2)], vH = par1.f[fh(k, 3)];
+                UM[k] = sqrt(sq(u - uH) + sq(v - vH) + (64.0 / (9.0 * kPi)) * (p / ro + 2.0 * pH / roH));
+                UH[k] = sqrt(sq(u - uH) + sq(v - vH) + (4.0 / kPi) * (p / ro + 2.0 * pH / roH));
+                nu[k] = ro * roH * UM[k] * sq(1.0 - P.a_2 * log(UM[k]));
+            }
+            const double cp = P.src_coef;  // n_p_LISM_ / Kn_
+            const double q2_1 = cp * (nu[0] * (par1.f[fh(0, 2)] - u) + nu[1] * (par1.f[fh(1, 2)] - u) +
+                                      nu[2] * (par1.f[fh(2, 2)] - u) + nu[3] * (par1.f[fh(3, 2)] - u));
+            const double q2_2 = cp * (nu[0] * (par1.f[fh(0, 3)] - v) + nu[1] * (par1.f[fh(1, 3)] - v) +
+                                      nu[2] * (par1.f[fh(2, 3)] - v) + nu[3] * (par1.f[fh(3, 3)] - v));
+            double e[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const double roH = par1.f[fh(k, 0)], pH = par1.f[fh(k, 1)];
+                const double uH = par1.f[fh(k, 2)], vH = par1.f[fh(k, 3)];
+                e[k] = nu[k] * ((sq(uH) + sq(vH) - sq(u) - sq(v)) / 2.0 + (UH[k] / UM[k]) * (2.0 * pH / roH - p / ro));
+            }
+            const double q3 = cp * (e[0] + e[1] + e[2] + e[3]);
+            const double rV2 = 1.0 / Volume2, VV = Volume * rV2;
+            if (kt != C_CENTR) {
+                double ro3 = ro * VV - dt * (Potok[0] * rV2 + ro * v / y);
+                const double Q33 = Q * VV - (dt * rV2) * Potok[4] - dt * Q * v / y;
+                if (ro3 <= 0.0) {
+                    ro3 = P.ro_floor;
+                    nro++;
+                }
+                const double rro3 = 1.0 / ro3;
+                const double u3 = (ro * u * VV - dt * (Potok[1] * rV2 + ro * v * u / y - q2_1)) * rro3;
+                const double v3 = (ro * v * VV - dt * (Potok[2] * rV2 + ro * v * v / y - q2_2)) * rro3;
+                double p3 = (((p / (ga - 1) + ro * (u * u + v * v) * 0.5) * VV -
+                              dt * (Potok[3] * rV2 + v * (ga * p / (ga - 1) + ro * (u * u + v * v) * 0.5) / y - q3)) -
+                             0.5 * ro3 * (u3 * u3 + v3 * v3)) *
+                            (ga - 1);
+                if (p3 <= 0) {
+                    p3 = P.p_floor;
+                    npc++;
+                }
+                b.nxt[0][c] = ro3;
+                b.nxt[1][c] = p3;
+                b.nxt[2][c] = u3;
+                b.nxt[3][c] = v3;
+                b.nxt[4][c] = Q33;
+            } else {
+#pragma unroll
+                for (int q = 0; q < 5; q++) b.nxt[q][c] = par1.f[q];
+            }
+            // hydrogen sources by cell kind (Setka.cpp:8734-8806)
+            int kk[4] = {0, 0, 0, 0};
+            if (kt == C_CENTR || kt == C_1 || kt == C_2 || kt == C_3) {
+                if (kt == C_1 || kt == C_CENTR) kk[0] = 1;
+                else kk[1] = 1;
+            } else {
+                if (kt == C_4) kk[2] = 1;
+                else kk[3] = 1;
+            }
+            const double S1 = nu[0] + nu[1] + nu[2] + nu[3];
+            double s2[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) s2[k] = nu[k] * ((sq(u) + sq(v)) / 2.0 + (UH[k] / UM[k]) * (p / ro));
+            const double S2 = s2[0] + s2[1] + s2[2] + s2[3];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const double roH = par1.f[fh(k, 0)], pH = par1.f[fh(k, 1)];
+                const double uH = par1.f[fh(k, 2)], vH = par1.f[fh(k, 3)];
+                double out[4];
+                if (k == 0 && kt == C_CENTR) {
+                    out[0] = roH;
+                    out[1] = pH;
+                    out[2] = uH;
+                    out[3] = vH;
+                } else {
+                    const double q1h = kNHOverKn * (kk[k] * S1 - nu[k]);
+                    const double q21h = kNHOverKn * (kk[k] * S1 * u - nu[k] * uH);
+                    const double q22h = kNHOverKn * (kk[k] * S1 * v - nu[k] * vH);
+                    const double q3h = kNHOverKn * (kk[k] * S2 - nu[k] * ((sq(uH) + sq(vH)) / 2.0 +
+                                                                         (UH[k] / UM[k]) * 2.0 * (pH / roH)));
+                    // floors: Setka.cpp:8817, 8829, 8859, 8871, 8893, 8905, 8927, 8939
+                    const double rf = k == 0 ? 0.0000001 : 0.000001;
+                    const double pf = k == 3 ? 0.0000001 : 0.000001;
+                    k5_update_h(ga, PH[k], roH, pH, uH, vH, q1h, q21h, q22h, q3h, VV, rV2, y, dt, rf, pf, out, nro,
+                                npc);
+                }
+#pragma unroll
+                for (int j = 0; j < 4; j++) hnxt[(4 * k + j) * nc + c] = out[j];
+            }
+        }
+    }
+    block_reduce_commit(tmin, nro, npc, status, b.dt_acc, b.counters, b.status);
+}
+
 // ------------------------------------------------------------------ launchers
 namespace {
 inline int blocks_for(int n, int t) { return (n + t - 1) / t; }
@@ -1842,7 +2321,8 @@ void launch_dt_finalize(const StepBuffers& b, cudaStream_t s) { dt_finalize_kern
 void launch_commit(const DevMesh& d, const StepBuffers& b, cudaStream_t s) {
     commit_kernel<<<blocks_for(d.n_points > 0 ? d.n_points : 1, 256), 256, 0, s>>>(d, b);
 }
-int launch_motion(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* scratch, cudaStream_t s) {
+int launch_motion(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* scratch, cudaStream_t s,
+                  bool copy_outer_shock) {
     int launches = 0;
     const int nf = d.n_lc + d.n_li + d.n_lo;
     if (nf > 0) {
@@ -1851,13 +2331,17 @@ int launch_motion(const DevMesh& d, const gelios_params& P, const StepBuffers& b
     }
     const int nr = d.n_rail_a + d.n_rail_b + d.n_rail_c + d.n_rail_d;
     if (nr > 0) {
-        rails_kernel<<<nr, 128, 0, s>>>(d, P, b.dt_cur, scratch);
+        rails_kernel<<<nr, 128, 0, s>>>(d, P, b.dt_cur, scratch, copy_outer_shock);
         launches++;
     }
     return launches;
 }
 void launch_hllc_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s) {
     hllc_batch_kernel<<<blocks_for(n, 128), 128, 0, s>>>(P, n, in, out);
+}
+void launch_k5_cells(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* hcur, double* hnxt,
+                     cudaStream_t s) {
+    k5_cell_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, hcur, hnxt);
 }
 void launch_hlldq_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s) {
     hlldq_batch_kernel<<<blocks_for(n, 128), 128, 0, s>>>(P, n, in, out);

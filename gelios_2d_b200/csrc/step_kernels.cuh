@@ -25,6 +25,7 @@ struct DevMesh {
     const int32_t* ptype = nullptr;
     const int32_t *cstart = nullptr, *contour = nullptr, *gstart = nullptr;
     const uint32_t* cflags = nullptr;
+    const int32_t* ctype = nullptr;  // Cell_type of every cell
     const int32_t *sA = nullptr, *sB = nullptr, *snb = nullptr, *ssd = nullptr, *ssd2 = nullptr;
     const uint32_t* sinfo = nullptr;
     // face units (one flux evaluation each, see step_kernels.cu): owner slot,
@@ -110,7 +111,12 @@ void launch_inner(const DevMesh& d, const gelios_params& P, const StepBuffers& b
                   cudaStream_t s);
 void launch_dt_finalize(const StepBuffers& b, cudaStream_t s);
 void launch_commit(const DevMesh& d, const StepBuffers& b, cudaStream_t s);
-int launch_motion(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* scratch, cudaStream_t s);
+int launch_motion(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* scratch, cudaStream_t s,
+                  bool copy_outer_shock = true);
+// Go_5_komponent cell kernel: hydrogen state rows (ro, p, u, v of H1..H4),
+// 16 rows of n_cells each, of the current and the next buffer.
+void launch_k5_cells(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* hcur, double* hnxt,
+                     cudaStream_t s);
 void launch_hllc_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s);
 void launch_hlldq_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s);
 void launch_hlld_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s);

@@ -14,6 +14,7 @@ reference (Setka.h)                          here
 ``Go_stationary(int)``                       ``Go_stationary(step)``
 ``Go_5_komponent__MK2(int)``                 ``Go_5_komponent__MK2(step)``
 ``Go_stationary_5_komponent_inner_MK2(int)`` ``Go_stationary_5_komponent_inner_MK2(step)``
+``Go_5_komponent(int)``                      ``Go_5_komponent(step)`` (+ ``set_hydrogen``)
 ``Save_Setka_ALL_ALPHA(string)``             ``Save_Setka_ALL_ALPHA(name)``
 ``Download_Setka_ALL_ALPHA_2_0(string)``     ``Setka.Download_Setka_ALL_ALPHA_2_0(name)``
 ==========================================  =====================================
@@ -144,6 +145,25 @@ class Setka:
 
     def Go_stationary_5_komponent_inner_MK2(self, step: int) -> N.GeliosStatus:
         return self._go(N.FORM_INNER_MK2, step)
+
+    def Go_5_komponent(self, step: int) -> N.GeliosStatus:
+        """Setka::Go_5_komponent (Setka.cpp:8269-8950): the plasma and the
+        four hydrogen fluids (set with :meth:`set_hydrogen`) on the grid
+        moved by Move_surface + Move_Setka_Calculate."""
+        return self._go(N.FORM_5_KOMPONENT, step)
+
+    def set_hydrogen(self, buf: int, h16: np.ndarray):
+        """ro, p, u, v of the hydrogen fluids H1..H4 of Cell::par[buf]
+        (shape (16, n_cells))."""
+        h16 = np.ascontiguousarray(h16, np.float64)
+        if h16.shape != (16, self.mesh.n_cells):
+            raise ValueError("hydrogen state must be (16, n_cells)")
+        N.check(self._L.gelios_upload_hydrogen(self._h, int(buf), h16.ravel()), "gelios_upload_hydrogen")
+
+    def hydrogen(self, buf: int) -> np.ndarray:
+        out = np.zeros(16 * self.mesh.n_cells)
+        N.check(self._L.gelios_download_hydrogen(self._h, int(buf), out), "gelios_download_hydrogen")
+        return out.reshape(16, self.mesh.n_cells)
 
     def _go(self, form: int, step: int) -> N.GeliosStatus:
         st = N.GeliosStatus()

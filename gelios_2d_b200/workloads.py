@@ -145,3 +145,26 @@ def counted_cells_mk2(mesh: Mesh, params: N.GeliosParams) -> int:
 def counted_cells_stationary(mesh: Mesh) -> int:
     """Cells Go_stationary updates (all but C_centr, Setka.cpp:5239)."""
     return int(np.count_nonzero(mesh["cell_type"] != 5))
+
+
+def hydrogen_fields(mesh: Mesh, seed: int = 31) -> np.ndarray:
+    """Seeded smooth state of the four hydrogen fluids H1..H4 (rows ro, p, u,
+    v of each, shape (16, n_cells)) for the four-fluid step: densities
+    A_k exp(-r/R_k)(1 + 0.1 cos(m_k theta)) + 0.02, temperatures ~ 0.5,
+    LISM-directed velocities with a small angular modulation."""
+    x, y = mesh.centroids()
+    r = np.sqrt(x * x + y * y)
+    th = np.arctan2(y, x)
+    u = splitmix64(seed, 24)
+    h = np.zeros((16, mesh.n_cells))
+    for k in range(4):
+        A = 0.05 + 0.2 * u[4 * k]
+        R = 1.0 + 3.0 * u[4 * k + 1]
+        m = 1 + int(3 * u[4 * k + 2])
+        ro = A * np.exp(-r / R) * (1.0 + 0.1 * np.cos(m * th)) + 0.02
+        T = 0.4 + 0.2 * u[4 * k + 3]
+        h[4 * k + 0] = ro
+        h[4 * k + 1] = 0.5 * ro * T * 2.0
+        h[4 * k + 2] = -2.54338 * (0.7 + 0.1 * k) * (1.0 + 0.05 * np.cos(th))
+        h[4 * k + 3] = 0.1 * np.sin(m * th) * u[16 + k]
+    return h

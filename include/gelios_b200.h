@@ -46,7 +46,8 @@ enum {
 enum {
     GELIOS_FORM_STATIONARY = 0, /* Setka::Go_stationary(int)                      Setka.h:177, Setka.cpp:5205-5343  */
     GELIOS_FORM_MK2 = 1,        /* Setka::Go_5_komponent__MK2(int)                Setka.h:186, Setka.cpp:10121-10482 */
-    GELIOS_FORM_INNER_MK2 = 2   /* Setka::Go_stationary_5_komponent_inner_MK2(int) Setka.h:176, Setka.cpp:6999-7212  */
+    GELIOS_FORM_INNER_MK2 = 2,  /* Setka::Go_stationary_5_komponent_inner_MK2(int) Setka.h:176, Setka.cpp:6999-7212  */
+    GELIOS_FORM_5_KOMPONENT = 3 /* Setka::Go_5_komponent(int): plasma + four hydrogen fluids, Setka.cpp:8269-8950 */
 };
 
 /* Riemann-solver precision (geometry, accumulation and the dt reduction stay FP64). */
@@ -168,6 +169,11 @@ int gelios_upload_topology(gelios_ctx *ctx, const gelios_mesh_view *mesh);
 int gelios_upload_state(gelios_ctx *ctx, int buf, const double *ro, const double *p, const double *u,
                         const double *v, const double *Q);
 int gelios_download_state(gelios_ctx *ctx, int buf, double *ro, double *p, double *u, double *v, double *Q);
+/* The four hydrogen fluids of Cell::par[buf] (Cell.h:27-46) for
+ * GELIOS_FORM_5_KOMPONENT: rows16 = ro_H1, p_H1, u_H1, v_H1, ..., v_H4, each
+ * n_cells long (16 * n_cells doubles). */
+int gelios_upload_hydrogen(gelios_ctx *ctx, int buf, const double *rows16);
+int gelios_download_hydrogen(gelios_ctx *ctx, int buf, double *rows16);
 /* Monte-Carlo moments left in Cell::par[0] by MK_start_new (Setka.cpp:12241-12449):
  * Hn/Hu/Hv/HT are [cell*4 + sort], ku/kv/kT are per cell. */
 int gelios_upload_mc(gelios_ctx *ctx, const double *Hn, const double *Hu, const double *Hv, const double *HT,

@@ -37,6 +37,8 @@ typedef struct ctx {
     int32_t *count;
     /* state par[2], 5 fields each */
     double *par[2][5];
+    /* hydrogen fluids of par[2]: ro, p, u, v of H1..H4 (Go_5_komponent) */
+    double *hpar[2][16];
     /* MC moments */
     double *Hn, *Hu, *Hv, *HT, *ku, *kv_, *kT;
     int32_t *inner;
@@ -1116,8 +1118,14 @@ void go_move_surface(void *h, int ii, double dt) {
 }
 
 /* Setka::Move_Setka_Calculate_2: Setka.cpp:4324-4759 */
-void go_move_setka2(void *h, double dt) {
-    ctx *c = (ctx *)h;
+/* Setka::Move_Setka_Calculate (Setka.cpp:4761-5147) equals
+ * Move_Setka_Calculate_2 except that it does not copy the outer-shock key
+ * height along the D rails beyond n_outer_shock (Setka.cpp:4725-4728). */
+static void move_setka(ctx *c, double dt, int copy_outer_shock);
+void go_move_setka2(void *h, double dt) { move_setka((ctx *)h, dt, 1); }
+void go_move_setka1(void *h, double dt) { move_setka((ctx *)h, dt, 0); }
+
+static void move_setka(ctx *c, double dt, int copy_outer_shock) {
     const go_params *P = &c->prm;
     const int ni = P->n_inner;
     const double R1 = P->R1, R111 = P->R111, R5 = P->R5;
@@ -1265,7 +1273,7 @@ void go_move_setka2(void *h, double dt) {
         V = c->Vy[K2];
         X2[K2] = X2[K0];
         Y2[K2] = Y[K2] + dt * V;
-        if (jj >= P->n_outer_shock) Y2[K2] = Y2[prev_k2];
+        if (copy_outer_shock && jj >= P->n_outer_shock) Y2[K2] = Y2[prev_k2];
         X2[K3] = X2[K0];
         Y2[K3] = Y[K3];
         R2 = Y2[K0];
@@ -1616,6 +1624,8 @@ void *go_create(const go_params *prm, const go_mesh *m) {
     c->count = (int32_t *)dup(NULL, sizeof(int32_t) * np);
     for (int b = 0; b < 2; b++)
         for (int q = 0; q < 5; q++) c->par[b][q] = (double *)dup(NULL, sizeof(double) * nc);
+    for (int b = 0; b < 2; b++)
+        for (int q = 0; q < 16; q++) c->hpar[b][q] = (double *)dup(NULL, sizeof(double) * nc);
     c->Hn = (double *)dup(NULL, sizeof(double) * 4 * nc);
     c->Hu = (double *)dup(NULL, sizeof(double) * 4 * nc);
     c->Hv = (double *)dup(NULL, sizeof(double) * 4 * nc);
@@ -1643,6 +1653,8 @@ void go_destroy(void *h) {
     free(c->x); free(c->y); free(c->x2); free(c->y2); free(c->Vx); free(c->Vy); free(c->count);
     for (int b = 0; b < 2; b++)
         for (int q = 0; q < 5; q++) free(c->par[b][q]);
+    for (int b = 0; b < 2; b++)
+        for (int q = 0; q < 16; q++) free(c->hpar[b][q]);
     free(c->Hn); free(c->Hu); free(c->Hv); free(c->HT); free(c->ku); free(c->kv_); free(c->kT);
     free(c->inner);
     free(c);
@@ -2103,4 +2115,502 @@ void go_cell_geom(void *h, int k, double *out) {
 
 void go_source_mk1(void *h, int k, double u, double v, double ro, double p, double *q3) {
     source_mk1((ctx *)h, k, u, v, ro, p, &q3[0], &q3[1], &q3[2]);
+}
+
+/* ================================================================== four hydrogen fluids
+ * Setka::Go_5_komponent (Setka.cpp:8269-8950): the plasma and the four
+ * hydrogen fluids H1..H4 of Parametr, each with its own HLLC flux per face
+ * side, on the grid moved by Move_surface + Move_Setka_Calculate.  The
+ * 21-field state is (ro, p, u, v, Q, ro_H1, p_H1, u_H1, v_H1, ..., v_H4),
+ * the member order of Parametr's aggregate initialisers (Gran.cpp:262-265). */
+enum { F_RO = 0, F_P, F_U, F_V, F_Q };
+#define FH(k, j) (5 + 4 * (k) + (j)) /* hydrogen fluid k (0..3): j = 0 ro, 1 p, 2 u, 3 v */
+#define H_POW 0.5                     /* Help.h:90 */
+#define N_H_OVER_KN (1.0 / 6.0)       /* n_H_LISM_ / Kn_, Help.h:60, 65 */
+
+typedef struct {
+    double f[21];
+} st21;
+
+static st21 cell_state21(const ctx *c, int k, int buf) {
+    st21 s;
+    for (int q = 0; q < 5; q++) s.f[q] = c->par[buf][q][k];
+    /* par rows are (ro, p, u, v, Q) */
+    for (int q = 0; q < 16; q++) s.f[5 + q] = c->hpar[buf][q][k];
+    return s;
+}
+
+static void mirror_v21(st21 *s) {
+    s->f[F_V] = -s->f[F_V];
+    for (int k = 0; k < 4; k++) s->f[FH(k, 3)] = -s->f[FH(k, 3)];
+}
+
+/* Inner_sphere state with the hydrogen fluids (Gran.cpp:236-265, 520-534):
+ * plasma and H1 from the solar wind, H2..H4 from the master cell. */
+static st21 inner_sphere21(const ctx *c, int f, int buf) {
+    const go_params *P = &c->prm;
+    st21 s = cell_state21(c, c->m.face_master[f], buf);
+    double x, y;
+    face_center(c, f, 0, &x, &y);
+    double dist = sqrt(x * x + y * y);
+    double ro = 1.0 / (kv(P->chi) * dist * dist);
+    double P_E = ro * P->chi * P->chi / (P->gamma * P->inner_mach * P->inner_mach);
+    s.f[F_RO] = ro;
+    s.f[F_P] = P_E;
+    s.f[F_U] = P->chi * x / dist;
+    s.f[F_V] = P->chi * y / dist;
+    s.f[F_Q] = ro;
+    s.f[FH(0, 0)] = 0.0000001;
+    s.f[FH(0, 1)] = (0.0000001 * P->chi * P->chi / (P->gamma * 14.1344 * 14.1344));
+    s.f[FH(0, 2)] = P->chi * x / dist;
+    s.f[FH(0, 3)] = P->chi * y / dist;
+    return s;
+}
+
+/* Input state (Gran.cpp:267-276, 536-545): plasma and H4 from the LISM,
+ * H1..H3 from the master cell. */
+static st21 input21(const ctx *c, int f, int buf) {
+    st21 s = cell_state21(c, c->m.face_master[f], buf);
+    s.f[F_RO] = c->prm.in_ro;
+    s.f[F_P] = c->prm.in_p;
+    s.f[F_U] = c->prm.in_u;
+    s.f[F_V] = c->prm.in_v;
+    s.f[F_Q] = c->prm.in_Q;
+    s.f[FH(3, 0)] = 1.0;
+    s.f[FH(3, 1)] = 0.5;
+    s.f[FH(3, 2)] = c->prm.in_u; /* Velosity_inf */
+    s.f[FH(3, 3)] = 0.0;
+    return s;
+}
+
+/* Gran::Get_par with the hydrogen fluids (Gran.cpp:205-289) */
+static st21 get_par21(const ctx *c, int f, int buf) {
+    int t = c->m.face_type[f];
+    st21 s;
+    memset(&s, 0, sizeof(s));
+    if (t == T_USUALY) {
+        s = cell_state21(c, c->m.face_sosed[f], buf);
+    } else if (t == T_EXTERN) {
+        s = cell_state21(c, c->m.face_master[f], buf);
+        if (s.f[F_U] >= 0.0) s.f[F_U] = c->prm.extern_u_par;
+    } else if (t == T_UPPER_WALL) {
+        s = cell_state21(c, c->m.face_master[f], buf);
+    } else if (t == T_AXIS) {
+        s = cell_state21(c, c->m.face_master[f], buf);
+        mirror_v21(&s);
+    } else if (t == T_INNER_SPHERE) {
+        s = inner_sphere21(c, f, buf);
+    } else if (t == T_INPUT) {
+        s = input21(c, f, buf);
+    }
+    return s;
+}
+
+/* Gran::Get_par_TVD with the hydrogen fluids (Gran.cpp:292-559) */
+static void get_par_tvd21(ctx *c, int f, int buf, st21 *io) {
+    int t = c->m.face_type[f];
+    int M = c->m.face_master[f];
+    if (t == T_USUALY) {
+        int Sd = c->m.face_sosed_down[f];
+        int So = c->m.face_sosed[f];
+        if (Sd < 0) {
+            if (cell_has_axis(c, M)) { /* Gran.cpp:308-338 */
+                double x, y, x2, y2, dist1, dist2, dist3;
+                st21 par = cell_state21(c, M, buf);
+                face_center(c, f, 0, &x, &y);
+                st21 par2 = cell_state21(c, M, buf);
+                st21 par1 = par2;
+                mirror_v21(&par1);
+                st21 par3 = cell_state21(c, So, buf);
+                cell_center(c, M, 0, &x2, &y2);
+                dist2 = sqrt(kv(x - x2) + kv(y - y2));
+                cell_center(c, So, 0, &x2, &y2);
+                dist3 = sqrt(kv(x - x2) + kv(y - y2));
+                cell_center(c, M, 0, &x2, &y2);
+                y2 = -y2;
+                dist1 = sqrt(kv(x - x2) + kv(y - y2));
+                const int vi[5] = {F_V, FH(0, 3), FH(1, 3), FH(2, 3), FH(3, 3)};
+                for (int q = 0; q < 5; q++)
+                    par.f[vi[q]] = linear3(-dist1, par1.f[vi[q]], -dist2, par2.f[vi[q]], dist3, par3.f[vi[q]], 0.0);
+                *io = par;
+            } else {
+                *io = cell_state21(c, M, buf);
+            }
+            return;
+        }
+        if (is_tracked_face(c, f)) { /* Gran.cpp:345-426 */
+            double x, y, x2, y2, dist1, dist2;
+            face_center(c, f, 0, &x, &y);
+            st21 par2 = cell_state21(c, M, buf);
+            st21 par1 = cell_state21(c, Sd, buf);
+            cell_center(c, M, 0, &x2, &y2);
+            dist2 = sqrt(kv(x - x2) + kv(y - y2));
+            cell_center(c, Sd, 0, &x2, &y2);
+            dist1 = sqrt(kv(x - x2) + kv(y - y2));
+            for (int q = 0; q < 21; q++) io->f[q] = linear2(-dist1, par1.f[q], -dist2, par2.f[q], 0.0);
+            if (io->f[F_RO] <= 0.0) io->f[F_RO] = par2.f[F_RO];
+            if (io->f[F_P] <= 0.0) io->f[F_P] = par2.f[F_P];
+            for (int k = 0; k < 4; k++) {
+                if (io->f[FH(k, 0)] <= 0.0) io->f[FH(k, 0)] = par2.f[FH(k, 0)];
+                if (io->f[FH(k, 1)] <= 0.0) io->f[FH(k, 1)] = par2.f[FH(k, 1)];
+            }
+            return;
+        }
+        /* Gran.cpp:427-472 */
+        double x, y, x2, y2, dist1, dist2, dist3;
+        face_center(c, f, 0, &x, &y);
+        st21 par2 = cell_state21(c, M, buf);
+        st21 par1 = cell_state21(c, Sd, buf);
+        st21 par3 = cell_state21(c, So, buf);
+        cell_center(c, M, 0, &x2, &y2);
+        dist2 = sqrt(kv(x - x2) + kv(y - y2));
+        cell_center(c, So, 0, &x2, &y2);
+        dist3 = sqrt(kv(x - x2) + kv(y - y2));
+        cell_center(c, Sd, 0, &x2, &y2);
+        dist1 = sqrt(kv(x - x2) + kv(y - y2));
+        for (int q = 0; q < 21; q++) io->f[q] = linear3(-dist1, par1.f[q], -dist2, par2.f[q], dist3, par3.f[q], 0.0);
+        if (io->f[F_RO] <= 0.0 || io->f[F_P] <= 0.0) { /* reference: exit(-1), Gran.cpp:444-455 */
+            c->status |= 2;
+            c->n_tvd_bad++;
+        }
+    } else if (t == T_EXTERN) {
+        *io = cell_state21(c, M, buf);
+        if (io->f[F_U] >= 0.0) io->f[F_U] = c->prm.extern_u_tvd;
+    } else if (t == T_UPPER_WALL) {
+        *io = cell_state21(c, M, buf);
+    } else if (t == T_AXIS) { /* Gran.cpp:486-519 */
+        double x, y, x2, y2, dist1, dist2;
+        int Sd = c->m.face_sosed_down[f];
+        face_center(c, f, 0, &x, &y);
+        st21 par2 = cell_state21(c, M, buf);
+        st21 par1 = cell_state21(c, Sd, buf);
+        cell_center(c, M, 0, &x2, &y2);
+        dist2 = sqrt(kv(x - x2) + kv(y - y2));
+        cell_center(c, Sd, 0, &x2, &y2);
+        dist1 = sqrt(kv(x - x2) + kv(y - y2));
+        *io = par2;
+        const int vi[5] = {F_V, FH(0, 3), FH(1, 3), FH(2, 3), FH(3, 3)};
+        for (int q = 0; q < 5; q++)
+            io->f[vi[q]] = linear3(-dist1, par1.f[vi[q]], -dist2, par2.f[vi[q]], dist2, -par2.f[vi[q]], 0.0);
+    } else if (t == T_INNER_SPHERE) {
+        *io = inner_sphere21(c, f, buf);
+    } else if (t == T_INPUT) {
+        *io = input21(c, f, buf);
+    }
+}
+
+/* Gran::Get_par_TVD_radial (Gran.cpp:562-675) with the H1 fields; the step
+ * consumes ro, p, p_H1 and ro_H1 of it (Setka.cpp:8342-8349, 8368-8375). */
+static void get_par_tvd_radial21(const ctx *c, int f, int buf, double *o) {
+    const double g2 = 2.0 * c->prm.gamma;
+    o[0] = o[1] = o[2] = o[3] = 0.0;
+    if (c->m.face_type[f] != T_USUALY) return;
+    int M = c->m.face_master[f], So = c->m.face_sosed[f], Sd = c->m.face_sosed_down[f];
+    st21 par1, par2, par3;
+    double x, y, x2, y2, dist1, dist2, dist3, r1, r2, r3;
+    face_center(c, f, 0, &x, &y);
+    double r = sqrt(kv(x) + kv(y));
+    if (Sd < 0) {
+        if (!cell_has_axis(c, M)) {
+            st21 s = cell_state21(c, M, buf);
+            o[0] = s.f[F_RO];
+            o[1] = s.f[F_P];
+            o[2] = s.f[FH(0, 1)];
+            o[3] = s.f[FH(0, 0)];
+            return;
+        }
+        /* Gran.cpp:580-626 */
+        par2 = cell_state21(c, M, buf);
+        par1 = par2;
+        mirror_v21(&par1);
+        par3 = cell_state21(c, So, buf);
+        cell_center(c, M, 0, &x2, &y2);
+        r2 = sqrt(kv(x2) + kv(y2));
+        dist2 = sqrt(kv(x - x2) + kv(y - y2));
+        cell_center(c, So, 0, &x2, &y2);
+        r3 = sqrt(kv(x2) + kv(y2));
+        dist3 = sqrt(kv(x - x2) + kv(y - y2));
+        cell_center(c, M, 0, &x2, &y2);
+        y2 = -y2;
+        r1 = sqrt(kv(x2) + kv(y2));
+        dist1 = sqrt(kv(x - x2) + kv(y - y2));
+    } else {
+        par2 = cell_state21(c, M, buf);
+        par1 = cell_state21(c, Sd, buf);
+        par3 = cell_state21(c, So, buf);
+        cell_center(c, M, 0, &x2, &y2);
+        r2 = sqrt(kv(x2) + kv(y2));
+        dist2 = sqrt(kv(x - x2) + kv(y - y2));
+        cell_center(c, So, 0, &x2, &y2);
+        r3 = sqrt(kv(x2) + kv(y2));
+        dist3 = sqrt(kv(x - x2) + kv(y - y2));
+        cell_center(c, Sd, 0, &x2, &y2);
+        r1 = sqrt(kv(x2) + kv(y2));
+        dist1 = sqrt(kv(x - x2) + kv(y - y2));
+    }
+    o[0] = linear3(-dist1, par1.f[F_RO] * kv(r1), -dist2, par2.f[F_RO] * kv(r2), dist3, par3.f[F_RO] * kv(r3), 0.0) /
+           kv(r);
+    o[1] = linear3(-dist1, par1.f[F_P] * pow(r1, g2), -dist2, par2.f[F_P] * pow(r2, g2), dist3,
+                   par3.f[F_P] * pow(r3, g2), 0.0) /
+           pow(r, g2);
+    o[2] = linear3(-dist1, par1.f[FH(0, 1)], -dist2, par2.f[FH(0, 1)], dist3, par3.f[FH(0, 1)], 0.0);
+    o[3] = linear3(-dist1, par1.f[FH(0, 0)] * pow(r1, H_POW), -dist2, par2.f[FH(0, 0)] * pow(r2, H_POW), dist3,
+                   par3.f[FH(0, 0)] * pow(r3, H_POW), 0.0) /
+           pow(r, H_POW);
+}
+
+/* radial scaling of a side's state to the face centre (Setka.cpp:8337-8341) */
+static void radial_scale21(st21 *s, double rc, double dis, double g2) {
+    s->f[F_RO] = s->f[F_RO] * kv(rc) / kv(dis);
+    s->f[FH(0, 0)] = s->f[FH(0, 0)] * pow(rc / dis, H_POW);
+    s->f[F_Q] = s->f[F_Q] * kv(rc) / kv(dis);
+    s->f[F_P] = s->f[F_P] * pow(rc / dis, g2);
+}
+
+/* conservative update of one hydrogen fluid (Setka.cpp:8808-8940) */
+static void update_h(ctx *c, int k, int buf_out, int hk, const double *pot, double ro_H, double p_H, double u_H,
+                     double v_H, double q1, double q21, double q22, double q3, double Volume, double Volume2, double y,
+                     double dt, double ro_floor, double p_floor) {
+    const double ggg = c->prm.gamma;
+    double ro3 = ro_H * Volume / Volume2 - dt * (pot[0] / Volume2 + ro_H * v_H / y - q1);
+    if (ro3 <= 0) {
+        ro3 = ro_floor;
+        c->n_ro_clamp++;
+    }
+    double u3 = (ro_H * u_H * Volume / Volume2 - dt * (pot[1] / Volume2 + ro_H * v_H * u_H / y - q21)) / ro3;
+    double v3 = (ro_H * v_H * Volume / Volume2 - dt * (pot[2] / Volume2 + ro_H * v_H * v_H / y - q22)) / ro3;
+    double p3 = (((p_H / (ggg - 1) + ro_H * (u_H * u_H + v_H * v_H) * 0.5) * Volume / Volume2 -
+                  dt * (pot[3] / Volume2 + +v_H * (ggg * p_H / (ggg - 1) + ro_H * (u_H * u_H + v_H * v_H) * 0.5) / y -
+                        q3)) -
+                 0.5 * ro3 * (u3 * u3 + v3 * v3)) *
+                (ggg - 1);
+    if (p3 <= 0) {
+        p3 = p_floor;
+        c->n_p_clamp++;
+    }
+    c->hpar[buf_out][4 * hk + 0][k] = ro3;
+    c->hpar[buf_out][4 * hk + 1][k] = p3;
+    c->hpar[buf_out][4 * hk + 2][k] = u3;
+    c->hpar[buf_out][4 * hk + 3][k] = v3;
+}
+
+void go_set_hydrogen(void *h, int buf, const double *rows16) {
+    ctx *c = (ctx *)h;
+    const int nc = c->m.n_cells;
+    for (int q = 0; q < 16; q++) memcpy(c->hpar[buf][q], rows16 + (size_t)q * nc, sizeof(double) * nc);
+}
+
+void go_get_hydrogen(void *h, int buf, double *rows16) {
+    ctx *c = (ctx *)h;
+    const int nc = c->m.n_cells;
+    for (int q = 0; q < 16; q++) memcpy(rows16 + (size_t)q * nc, c->hpar[buf][q], sizeof(double) * nc);
+}
+
+/* Setka::Go_5_komponent: Setka.cpp:8269-8950 */
+void go_5_komponent(void *h, int step) {
+    ctx *c = (ctx *)h;
+    const go_params *P = &c->prm;
+    const double ggg = P->gamma, g2 = 2 * P->gamma;
+    int now1 = 1, now2 = 0;
+    double T[2];
+    T[0] = T[1] = P->dt0;
+    for (int st = 0; st < step; st++) {
+        now1 = (now1 + 1) % 2;
+        now2 = (now2 + 1) % 2;
+        double time = 10000000;
+        T[now2] = 100000000;
+        go_move_surface(c, now1, T[now1]);
+        go_move_setka1(c, T[now1]);
+        for (int k = 0; k < c->m.n_cells; k++) {
+            double Potok[5] = {0, 0, 0, 0, 0};
+            double PH[4][4] = {{0}};
+            double Pf[4], PQ = 0.0;
+            st21 par1 = cell_state21(c, k, now1);
+            double n1, n2, dist, x, y;
+            cell_center(c, k, 0, &x, &y);
+            double radius = sqrt(kv(x) + kv(y));
+            if (radius < P->R11) continue;
+            double Volume = cell_volume(c, k, 0);
+            double Volume2 = cell_volume(c, k, 1);
+            double W = 0.0;
+            const int kt = c->m.cell_type[k];
+            for (int g = c->m.gran_start[k]; g < c->m.gran_start[k + 1]; g++) {
+                int f = c->m.gran[g];
+                double x2, y2, x4, y4;
+                double S = face_square(c, f);
+                face_center(c, f, 0, &x2, &y2);
+                face_center(c, f, 1, &x4, &y4);
+                dist = sqrt(kv(x - x2) + kv(y - y2));
+                st21 par11 = par1;
+                st21 par2 = get_par21(c, f, now1);
+                face_normal(c, f, &n1, &n2);
+                double Vc, Vl, Vp;
+                W = ((x4 - x2) * n1 + (y4 - y2) * n2) / T[now1];
+                int met = 1;
+                double dis = sqrt(kv(x2) + kv(y2));
+                int ft = c->m.face_type[f];
+                if (ft == T_USUALY) {
+                    int So = c->m.face_sosed[f];
+                    double x3, y3;
+                    cell_center(c, So, 0, &x3, &y3);
+                    double dd = sqrt(kv(x3) + kv(y3));
+                    if (kt == C_1) {
+                        radial_scale21(&par11, radius, dis, g2);
+                        polar_perenos(x, y, x2, y2, &par11.f[F_U], &par11.f[F_V], TINY_ANGLE);
+                        polar_perenos(x, y, x2, y2, &par11.f[FH(0, 2)], &par11.f[FH(0, 3)], TINY_ANGLE);
+                        double o[4];
+                        get_par_tvd_radial21(c, f, now1, o);
+                        par11.f[F_RO] = o[0];
+                        par11.f[F_P] = o[1];
+                        par11.f[FH(0, 1)] = o[2];
+                        par11.f[FH(0, 0)] = o[3];
+                    } else {
+                        get_par_tvd21(c, f, now1, &par11);
+                    }
+                    int fc = c->m.face_copy[f];
+                    if (c->m.cell_type[So] == C_1) {
+                        radial_scale21(&par2, dd, dis, g2);
+                        polar_perenos(x3, y3, x2, y2, &par2.f[F_U], &par2.f[F_V], TINY_ANGLE);
+                        polar_perenos(x3, y3, x2, y2, &par2.f[FH(0, 2)], &par2.f[FH(0, 3)], TINY_ANGLE);
+                        double o[4];
+                        get_par_tvd_radial21(c, fc, now1, o);
+                        par2.f[F_RO] = o[0];
+                        par2.f[F_P] = o[1];
+                        par2.f[FH(0, 1)] = o[2];
+                        par2.f[FH(0, 0)] = o[3];
+                    } else {
+                        get_par_tvd21(c, fc, now1, &par2);
+                    }
+                } else if (ft == T_INNER_SPHERE) {
+                    radial_scale21(&par11, radius, dis, g2);
+                } else if (kt == C_1 && ft == T_AXIS) {
+                    radial_scale21(&par11, radius, dis, g2);
+                    polar_perenos(x, y, x2, y2, &par11.f[F_U], &par11.f[F_V], TINY_ANGLE);
+                    polar_perenos(x, y, x2, y2, &par11.f[FH(0, 2)], &par11.f[FH(0, 3)], TINY_ANGLE);
+                    par2 = par11;
+                    mirror_v21(&par2);
+                } else if (kt != C_1 && ft == T_AXIS) {
+                    get_par_tvd21(c, f, now1, &par11);
+                    par2 = par11;
+                    mirror_v21(&par2);
+                }
+                int np = face_np_flag(c, f);
+                int god = is_tracked_face(c, f);
+                for (int hk = 0; hk < 4; hk++) {
+                    if (hk == 0 && kt == C_CENTR) continue;
+                    time = dmin(time, hllc(P, par11.f[FH(hk, 0)], par11.f[F_Q], par11.f[FH(hk, 1)], par11.f[FH(hk, 2)],
+                                           par11.f[FH(hk, 3)], par2.f[FH(hk, 0)], par2.f[F_Q], par2.f[FH(hk, 1)],
+                                           par2.f[FH(hk, 2)], par2.f[FH(hk, 3)], W, Pf, &PQ, n1, n2, dist, met, &Vl,
+                                           &Vc, &Vp, 0));
+                    for (int q = 0; q < 4; q++) PH[hk][q] = PH[hk][q] + Pf[q] * S;
+                }
+                if (god) {
+                    double Vl2, Vp2, VV, nn[3], q1[5], q2[5], qq[5];
+                    nn[0] = n1; nn[1] = n2; nn[2] = 0.0;
+                    q1[0] = par11.f[F_RO]; q1[1] = par11.f[F_P]; q1[2] = par11.f[F_U]; q1[3] = par11.f[F_V]; q1[4] = 0.0;
+                    q2[0] = par2.f[F_RO]; q2[1] = par2.f[F_P]; q2[2] = par2.f[F_U]; q2[3] = par2.f[F_V]; q2[4] = 0.0;
+                    int stt = 0;
+                    time = dmin(time, godunov(P, q1, q2, nn, qq, &Vl2, &Vp2, &VV, W, dist, &stt));
+                    c->status |= stt;
+                    Potok[0] = Potok[0] + qq[0] * S;
+                    Potok[1] = Potok[1] + qq[1] * S;
+                    Potok[2] = Potok[2] + qq[2] * S;
+                    Potok[3] = Potok[3] + qq[4] * S;
+                    time = dmin(time, hllc(P, par11.f[F_RO], par11.f[F_Q], par11.f[F_P], par11.f[F_U], par11.f[F_V],
+                                           par2.f[F_RO], par2.f[F_Q], par2.f[F_P], par2.f[F_U], par2.f[F_V], W, Pf,
+                                           &PQ, n1, n2, dist, met, &Vl, &Vc, &Vp, np));
+                    Potok[4] = Potok[4] + PQ * S;
+                } else {
+                    time = dmin(time, hllc(P, par11.f[F_RO], par11.f[F_Q], par11.f[F_P], par11.f[F_U], par11.f[F_V],
+                                           par2.f[F_RO], par2.f[F_Q], par2.f[F_P], par2.f[F_U], par2.f[F_V], W, Pf,
+                                           &PQ, n1, n2, dist, met, &Vl, &Vc, &Vp, np));
+                    for (int q = 0; q < 4; q++) Potok[q] = Potok[q] + Pf[q] * S;
+                    Potok[4] = Potok[4] + PQ * S;
+                }
+            }
+            if (time < T[now2]) T[now2] = time;
+            /* multi-fluid charge exchange (Setka.cpp:8575-8660) */
+            const double u = par1.f[F_U], v = par1.f[F_V], ro = par1.f[F_RO], p = par1.f[F_P], Q = par1.f[F_Q];
+            double UM[4], UH[4], nu[4], uH[4], vH[4], roH[4], pH[4];
+            for (int hk = 0; hk < 4; hk++) {
+                roH[hk] = par1.f[FH(hk, 0)];
+                pH[hk] = par1.f[FH(hk, 1)];
+                uH[hk] = par1.f[FH(hk, 2)];
+                vH[hk] = par1.f[FH(hk, 3)];
+            }
+            for (int hk = 0; hk < 4; hk++)
+                UM[hk] = sqrt(kv(u - uH[hk]) + kv(v - vH[hk]) + (64.0 / (9.0 * PI_)) * (p / ro + 2.0 * pH[hk] / roH[hk]));
+            for (int hk = 0; hk < 4; hk++)
+                UH[hk] = sqrt(kv(u - uH[hk]) + kv(v - vH[hk]) + (4.0 / PI_) * (p / ro + 2.0 * pH[hk] / roH[hk]));
+            for (int hk = 0; hk < 4; hk++) {
+                const double sigma = kv(1.0 - P->a_2 * log(UM[hk]));
+                nu[hk] = ro * roH[hk] * UM[hk] * sigma;
+            }
+            const double cp = P->src_coef; /* n_p_LISM_ / Kn_ */
+            const double q2_1 = cp * (nu[0] * (uH[0] - u) + nu[1] * (uH[1] - u) + nu[2] * (uH[2] - u) +
+                                      nu[3] * (uH[3] - u));
+            const double q2_2 = cp * (nu[0] * (vH[0] - v) + nu[1] * (vH[1] - v) + nu[2] * (vH[2] - v) +
+                                      nu[3] * (vH[3] - v));
+            double e[4];
+            for (int hk = 0; hk < 4; hk++)
+                e[hk] = nu[hk] * ((kv(uH[hk]) + kv(vH[hk]) - kv(u) - kv(v)) / 2.0 +
+                                  (UH[hk] / UM[hk]) * (2.0 * pH[hk] / roH[hk] - p / ro));
+            const double q3 = cp * (e[0] + e[1] + e[2] + e[3]);
+            const double dt = T[now1];
+            if (kt != C_CENTR) {
+                double ro3 = ro * Volume / Volume2 - dt * (Potok[0] / Volume2 + ro * v / y);
+                double Q33 = Q * Volume / Volume2 - (dt / Volume2) * Potok[4] - dt * Q * v / y;
+                if (ro3 <= 0.0) {
+                    ro3 = P->ro_floor;
+                    c->n_ro_clamp++;
+                }
+                double u3 = (ro * u * Volume / Volume2 - dt * (Potok[1] / Volume2 + ro * v * u / y - q2_1)) / ro3;
+                double v3 = (ro * v * Volume / Volume2 - dt * (Potok[2] / Volume2 + ro * v * v / y - q2_2)) / ro3;
+                double p3 = (((p / (ggg - 1) + ro * (u * u + v * v) * 0.5) * Volume / Volume2 -
+                              dt * (Potok[3] / Volume2 + +v * (ggg * p / (ggg - 1) + ro * (u * u + v * v) * 0.5) / y -
+                                    q3)) -
+                             0.5 * ro3 * (u3 * u3 + v3 * v3)) *
+                            (ggg - 1);
+                if (p3 <= 0) {
+                    p3 = P->p_floor;
+                    c->n_p_clamp++;
+                }
+                write_state(c, k, now2, ro3, Q33, p3, u3, v3);
+            } else {
+                st5 s = cell_state(c, k, now1);
+                write_state(c, k, now2, s.ro, s.Q, s.p, s.u, s.v);
+            }
+            /* sources of the hydrogen fluids (Setka.cpp:8734-8806) */
+            int kk[4] = {0, 0, 0, 0};
+            if (kt == C_CENTR || kt == C_1 || kt == C_2 || kt == C_3) {
+                if (kt == C_1 || kt == C_CENTR) kk[0] = 1;
+                else kk[1] = 1;
+            } else {
+                if (kt == C_4) kk[2] = 1;
+                else kk[3] = 1;
+            }
+            const double S1 = nu[0] + nu[1] + nu[2] + nu[3];
+            double s2[4];
+            for (int hk = 0; hk < 4; hk++) s2[hk] = nu[hk] * ((kv(u) + kv(v)) / 2.0 + (UH[hk] / UM[hk]) * (p / ro));
+            const double S2 = s2[0] + s2[1] + s2[2] + s2[3];
+            for (int hk = 0; hk < 4; hk++) {
+                const double q1h = N_H_OVER_KN * (kk[hk] * S1 - nu[hk]);
+                const double q21h = N_H_OVER_KN * (kk[hk] * S1 * u - nu[hk] * uH[hk]);
+                const double q22h = N_H_OVER_KN * (kk[hk] * S1 * v - nu[hk] * vH[hk]);
+                const double q3h = N_H_OVER_KN * (kk[hk] * S2 - nu[hk] * ((kv(uH[hk]) + kv(vH[hk])) / 2.0 +
+                                                                        (UH[hk] / UM[hk]) * 2.0 * (pH[hk] / roH[hk])));
+                if (hk == 0 && kt == C_CENTR) {
+                    for (int j = 0; j < 4; j++) c->hpar[now2][j][k] = c->hpar[now1][j][k];
+                    continue;
+                }
+                /* floors: Setka.cpp:8817, 8829, 8859, 8871, 8893, 8905, 8927, 8939 */
+                const double rf = hk == 0 ? 0.0000001 : 0.000001;
+                const double pf = hk == 3 ? 0.0000001 : 0.000001;
+                update_h(c, k, now2, hk, PH[hk], roH[hk], pH[hk], uH[hk], vH[hk], q1h, q21h, q22h, q3h, Volume,
+                         Volume2, y, dt, rf, pf);
+            }
+        }
+        go_commit_points(c);
+    }
+    c->last_dt = T[now2];
 }

@@ -61,6 +61,11 @@ typedef struct go_mesh {
 
 void *go_create(const go_params *prm, const go_mesh *mesh);
 void go_destroy(void *h);
+/* hydrogen fluids of par[buf] (Go_5_komponent): rows16 = ro, p, u, v of H1..H4 */
+void go_set_hydrogen(void *h, int buf, const double *rows16);
+void go_get_hydrogen(void *h, int buf, double *rows16);
+void go_5_komponent(void *h, int step);
+void go_move_setka1(void *h, double dt);
 void go_set_state(void *h, int buf, const double *ro, const double *p, const double *u, const double *v,
                   const double *Q);
 void go_get_state(void *h, int buf, double *ro, double *p, double *u, double *v, double *Q);

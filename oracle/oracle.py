@@ -102,6 +102,10 @@ def lib() -> C.CDLL:
     L.go_hlld.restype = C.c_double
     L.go_hlld.argtypes = [C.POINTER(GoParams), f64p, f64p, f64p, f64p, f64p, C.c_double, C.c_double,
                           C.POINTER(C.c_int)]
+    L.go_set_hydrogen.argtypes = [vp, C.c_int, f64p]
+    L.go_get_hydrogen.argtypes = [vp, C.c_int, f64p]
+    L.go_5_komponent.argtypes = [vp, C.c_int]
+    L.go_move_setka1.argtypes = [vp, C.c_double]
     L.go_face_par.argtypes = [vp, C.c_int, C.c_int, C.c_int, f64p]
     L.go_cell_geom.argtypes = [vp, C.c_int, f64p]
     L.go_source_mk1.argtypes = [vp, C.c_int] + [C.c_double] * 4 + [f64p]
@@ -211,6 +215,19 @@ class Oracle:
 
     def mk2(self, steps):
         self.L.go_mk2(self.h, int(steps))
+
+    def set_hydrogen(self, buf, h16):
+        """ro, p, u, v of H1..H4 in par[buf]; h16 of shape (16, n_cells)."""
+        self.L.go_set_hydrogen(self.h, int(buf), np.ascontiguousarray(h16, np.float64).ravel())
+
+    def get_hydrogen(self, buf) -> np.ndarray:
+        out = np.zeros(16 * self.ncell)
+        self.L.go_get_hydrogen(self.h, int(buf), out)
+        return out.reshape(16, self.ncell)
+
+    def five_komponent(self, steps):
+        """Setka::Go_5_komponent (Setka.cpp:8269-8950)."""
+        self.L.go_5_komponent(self.h, int(steps))
 
     def inner_mk2(self, steps):
         self.L.go_inner_mk2(self.h, int(steps))

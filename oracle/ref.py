@@ -43,6 +43,9 @@ def lib(fast: bool = False) -> C.CDLL:
     vp = C.c_void_p
     L.gref_setka_new.restype = vp
     L.gref_setka_new.argtypes = [C.c_int] * 8
+    L.gref_set_hydrogen.argtypes = [vp, C.c_int, _f64p]
+    L.gref_get_hydrogen.argtypes = [vp, C.c_int, _f64p]
+    L.gref_go_5_komponent.argtypes = [vp, C.c_int]
     L.gref_save_alpha.argtypes = [vp, C.c_char_p]
     L.gref_load_alpha.restype = vp
     L.gref_load_alpha.argtypes = [C.c_char_p]
@@ -264,6 +267,20 @@ class RefSetka:
     # ------------------------------------------------------------ steps
     def go_stationary(self, steps: int):
         self.L.gref_go_stationary(self.h, int(steps))
+
+    def set_hydrogen(self, buf: int, h16: np.ndarray):
+        """ro, p, u, v of H1..H4 in par[buf]; h16 of shape (16, n_cells)."""
+        self.L.gref_set_hydrogen(self.h, int(buf), np.ascontiguousarray(h16, np.float64).ravel())
+
+    def get_hydrogen(self, buf: int) -> np.ndarray:
+        n = self.counts()["n_cells"]
+        out = np.zeros(16 * n)
+        self.L.gref_get_hydrogen(self.h, int(buf), out)
+        return out.reshape(16, n)
+
+    def go_5_komponent(self, steps: int):
+        """Setka::Go_5_komponent (Setka.cpp:8269-8950)."""
+        self.L.gref_go_5_komponent(self.h, int(steps))
 
     def go_mk2(self, steps: int):
         self.L.gref_go_mk2(self.h, int(steps))

@@ -434,6 +434,35 @@ void gref_go_mk2(void* hv, int steps) {
     static_cast<Handle*>(hv)->S->Go_5_komponent__MK2(steps);
 }
 
+// Hydrogen fluids of par[buf]: rows16 = ro, p, u, v of H1..H4, each n_cells long.
+void gref_set_hydrogen(void* hv, int buf, const double* rows16) {
+    auto* h = static_cast<Handle*>(hv);
+    const size_t n = h->S->All_Cells.size();
+    for (size_t k = 0; k < n; ++k) {
+        Parametr& p = h->S->All_Cells[k]->par[buf];
+        double* f[16] = {&p.ro_H1, &p.p_H1, &p.u_H1, &p.v_H1, &p.ro_H2, &p.p_H2, &p.u_H2, &p.v_H2,
+                         &p.ro_H3, &p.p_H3, &p.u_H3, &p.v_H3, &p.ro_H4, &p.p_H4, &p.u_H4, &p.v_H4};
+        for (int q = 0; q < 16; ++q) *f[q] = rows16[q * n + k];
+    }
+}
+
+void gref_get_hydrogen(void* hv, int buf, double* rows16) {
+    auto* h = static_cast<Handle*>(hv);
+    const size_t n = h->S->All_Cells.size();
+    for (size_t k = 0; k < n; ++k) {
+        const Parametr& p = h->S->All_Cells[k]->par[buf];
+        const double f[16] = {p.ro_H1, p.p_H1, p.u_H1, p.v_H1, p.ro_H2, p.p_H2, p.u_H2, p.v_H2,
+                              p.ro_H3, p.p_H3, p.u_H3, p.v_H3, p.ro_H4, p.p_H4, p.u_H4, p.v_H4};
+        for (int q = 0; q < 16; ++q) rows16[q * n + k] = f[q];
+    }
+}
+
+// Setka::Go_5_komponent (Setka.cpp:8269-8950)
+void gref_go_5_komponent(void* hv, int steps) {
+    Quiet q;
+    static_cast<Handle*>(hv)->S->Go_5_komponent(steps);
+}
+
 void gref_go_inner_mk2(void* hv, int steps) {
     Quiet q;
     static_cast<Handle*>(hv)->S->Go_stationary_5_komponent_inner_MK2(steps);

@@ -1,7 +1,7 @@
 """Generates the golden fixtures of tests/golden from the compiled reference.
 
 Run where the reference tree and oracle/_ref/libgelios_ref.so exist:
-    python tests/golden/make_golden.py [faces] [steps] [mhd] [checkpoint]
+    python tests/golden/make_golden.py [faces] [steps] [mhd] [checkpoint] [five]
 (no argument: all).  The fixtures are the reference's own outputs
 (HLLC_2d_Korolkov_b_s, Godunov_Solver_Alexashov, HLLDQ_Korolkov,
 HLLD_Solver_Alexashov, and short Go_stationary / Go_5_komponent__MK2 /
@@ -152,8 +152,28 @@ def write_checkpoint():
                         y=pm["y"])
 
 
+def write_five_fluid():
+    """Setka::Go_5_komponent on the small rail grid: the reference's field,
+    seeded hydrogen fluids, 4 steps."""
+    S = ref.RefSetka.constructor(*SMALL)
+    S.tvd_prepare()
+    S.init_conditions()
+    m = Mesh.from_arrays(S.export())
+    st0 = S.get_state(0)
+    h0 = W.hydrogen_fields(m, seed=3)
+    S.set_hydrogen(0, h0)
+    S.set_hydrogen(1, h0)
+    S.go_5_komponent(4)
+    pm = S.point_motion()
+    np.savez_compressed(HERE / "steps_five_fluid_small.npz", state0=st0, h0=h0, par0=S.get_state(0),
+                        par1=S.get_state(1), h_par0=S.get_hydrogen(0), h_par1=S.get_hydrogen(1), x=pm["x"],
+                        y=pm["y"])
+
+
 def main(parts):
     ref.set_threads(1)
+    if "five" in parts:
+        write_five_fluid()
     if "checkpoint" in parts:
         write_checkpoint()
     if "mhd" in parts:
@@ -212,4 +232,4 @@ def write_steps():
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or ["faces", "steps", "mhd", "checkpoint"])
+    main(sys.argv[1:] or ["faces", "steps", "mhd", "checkpoint", "five"])
