@@ -40,16 +40,21 @@ WORKLOADS = {
     "mk2_1m": ("moving-grid plasma step (Go_5_komponent__MK2 form) on Setka(480,240,100,220,200,200,300,300)",
                "mk2", (480, 240, 100, 220, 200, 200, 300, 300)),
     "plain": ("plain single-fluid step (Go_stationary form), polar 180x120, r=1..600", "plain", None),
+    "k5_200k": ("plasma + four hydrogen fluids (Go_5_komponent form) on Setka(200,100,50,100,100,100,150,150)",
+                "k5", (200, 100, 50, 100, 100, 100, 150, 150)),
 }
 # Algorithmic bytes per cell update (each datum moved once per step):
 #   MK2 form: 8*(2*5) state + 8*19 Monte-Carlo moments + 16*(1+1) points (x,y,x2,y2)
 #             + 8 written point coordinate + 4*4 neighbour indices = 288 B
 #   plain form: 8*(2*5) + 16 points + 4*4 indices = 112 B
-BYTES_PER_CELL = {"mk2": 288, "plain": 112}
+#   four-fluid form: 8*(2*21) state (plasma 5 + hydrogen 16) + 16*(1+1) points
+#             + 8 written point coordinate + 4*4 neighbour indices = 392 B
+BYTES_PER_CELL = {"mk2": 288, "plain": 112, "k5": 392}
 STEP_KERNELS = {
     "mk2": "whole moving-grid step: recon, tracked_solve, source, surface_faces, rails, flux x2, update, commit "
            "(one CUDA graph, 3 streams)",
     "plain": "whole plain step: stationary_unit + stationary_update + dt_finalize",
+    "k5": "whole four-fluid step: centroid, surface_faces, rails, k5_cell, commit",
 }
 
 
@@ -71,6 +76,13 @@ def build_workload(name: str):
         params = N.reference_params()
         st0 = W.init_conditions_reference(mesh)
         mc = W.mc_fields(mesh, seed=9)
+        counted = W.counted_cells_mk2(mesh, params)
+    elif form == "k5":
+        # `mc` carries the hydrogen fluids (16, n_cells) for this form
+        mesh = g.Mesh.setka(*dims)
+        params = N.reference_params()
+        st0 = W.init_conditions_reference(mesh)
+        mc = W.hydrogen_fields(mesh, seed=3)
         counted = W.counted_cells_mk2(mesh, params)
     else:
         mesh = W.plain_mesh()
@@ -169,9 +181,12 @@ def cpu_reference_rate(mesh, params, st0, mc, counted, form, budget_s=12.0, max_
     S.tvd_prepare()
     S.set_state(0, st0)
     S.set_state(1, st0)
-    if mc is not None:
+    if form == "k5":
+        S.set_hydrogen(0, mc)
+        S.set_hydrogen(1, mc)
+    elif mc is not None:
         S.set_mc(*mc)
-    run = S.go_mk2 if form == "mk2" else S.go_stationary
+    run = {"mk2": S.go_mk2, "k5": S.go_5_komponent}.get(form, S.go_stationary)
     # keep the reference's printf diagnostics off our stdout
     saved = os.dup(1)
     devnull = os.open(os.devnull, os.O_WRONLY)
@@ -191,6 +206,18 @@ def cpu_reference_rate(mesh, params, st0, mc, counted, form, budget_s=12.0, max_
     return counted * steps / el, steps, threads, el
 
 
+def load_inputs(S, form, st0, mc):
+    """par[0] = par[1] = st0, plus the form's extra inputs: Monte-Carlo
+    moments (moving grid) or the hydrogen fluids (four-fluid form)."""
+    S.set_par(0, st0)
+    S.set_par(1, st0)
+    if form == "k5":
+        S.set_hydrogen(0, mc)
+        S.set_hydrogen(1, mc)
+    elif mc is not None:
+        S.set_mc(*mc)
+
+
 def fp32_flux_errors(mesh, params32, st0, mc, fcode, device, counts=(1, 100, 2000)) -> dict:
     """L1 and Linf relative errors of rho, p, u, v of the FP32-flux form
     against the FP64 path (itself within 1e-12 per step of the reference's
@@ -206,10 +233,7 @@ def fp32_flux_errors(mesh, params32, st0, mc, fcode, device, counts=(1, 100, 200
         res = []
         for prm in (params32, params64):
             S = g.Setka(mesh, prm, device=device)
-            S.set_par(0, st0)
-            S.set_par(1, st0)
-            if mc is not None:
-                S.set_mc(*mc)
+            load_inputs(S, "k5" if fcode == N.FORM_5_KOMPONENT else "", st0, mc)
             st = S.step(fcode, n)
             res.append(S.par(st.result_buf))
             S.close()
@@ -278,11 +302,8 @@ def main():
     if args.precision == "fp32flux":
         params = params.copy(precision=N.PREC_FP32_FLUX)
     S = g.Setka(mesh, params, device=device)
-    S.set_par(0, st0)
-    S.set_par(1, st0)
-    if mc is not None:
-        S.set_mc(*mc)
-    fcode = N.FORM_MK2 if form == "mk2" else N.FORM_STATIONARY
+    load_inputs(S, form, st0, mc)
+    fcode = {"mk2": N.FORM_MK2, "k5": N.FORM_5_KOMPONENT}.get(form, N.FORM_STATIONARY)
     stream = torch.cuda.ExternalStream(S.stream_handle(), device=device)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")
     do_flush = args.workload != "mk2_1m"
@@ -334,13 +355,21 @@ def main():
     # end to end through the public API with pinned host buffers
     host_in = torch.from_numpy(np.ascontiguousarray(st0)).pin_memory().numpy()
     host_out = torch.empty(st0.shape, dtype=torch.float64).pin_memory().numpy()
+    e2e_bytes = int(st0.nbytes)
+    if form == "k5":  # the hydrogen fluids are step inputs and outputs too
+        h_in = torch.from_numpy(np.ascontiguousarray(mc)).pin_memory().numpy()
+        e2e_bytes += int(h_in.nbytes)
     e2e_steps = max(3, min(args.steps, 20))
     S.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         S.set_par(0, host_in)
+        if form == "k5":
+            S.set_hydrogen(0, h_in)
         S.step_async(fcode, 1)
         S.par(1, out=host_out)
+        if form == "k5":
+            S.hydrogen(1)
     e2e_s = max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{device}")
     e2e_value = whole_job_rate(counted * e2e_steps, world, e2e_s)
 
@@ -357,8 +386,8 @@ def main():
         "warmup": args.warmup, "ms_per_step": total_ms / n_steps_total, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64 (fp32 flux)",
         "data": "synthetic (seeded initial field and Monte-Carlo moments)", "config": config,
-        "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": int(st0.nbytes),
-                "d2h_bytes_per_step": int(st0.nbytes)},
+        "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": e2e_bytes,
+                "d2h_bytes_per_step": e2e_bytes},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
