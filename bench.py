@@ -42,6 +42,8 @@ WORKLOADS = {
     "plain": ("plain single-fluid step (Go_stationary form), polar 180x120, r=1..600", "plain", None),
     "k5_200k": ("plasma + four hydrogen fluids (Go_5_komponent form) on Setka(200,100,50,100,100,100,150,150)",
                 "k5", (200, 100, 50, 100, 100, 100, 150, 150)),
+    "sweep16": ("16 independent moving-grid instances, Setka(200,100,50,100,100,100,150,150) scaled by "
+                "U(0.5,1.4) per instance (~50k..~400k cells each), batched on each GPU", "sweep", None),
 }
 # Algorithmic bytes per cell update (each datum moved once per step):
 #   MK2 form: 8*(2*5) state + 8*19 Monte-Carlo moments + 16*(1+1) points (x,y,x2,y2)
@@ -247,6 +249,105 @@ def fp32_flux_errors(mesh, params32, st0, mc, fcode, device, counts=(1, 100, 200
     return out
 
 
+def run_sweep(args, rank: int, world: int, local: int) -> None:
+    """The sweep workload: instances partitioned over the ranks by cell count,
+    each rank steps its instances together (one context and graph per
+    instance); value = all cells updated / the slowest rank's device time."""
+    import torch
+
+    import gelios_2d_b200 as g  # noqa: F401
+    from gelios_2d_b200 import sweep as sw
+    from gelios_2d_b200 import workloads as W
+    from gelios_2d_b200.replicas import max_over_ranks, whole_job_rate
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist_mod.init_process_group("nccl", timeout=timedelta(seconds=120))
+        dist = dist_mod
+    torch.cuda.set_device(local)
+    n_inst = 16
+    seeds = W.splitmix64(41, n_inst)
+    sizes = []  # estimated cells per instance, to partition before building
+    for i in range(n_inst):
+        f = 0.5 + 0.9 * float(seeds[i])
+        sizes.append(f * f)
+    mine = sw.partition(sizes, world)[rank]
+    inst = sw.instance_set(n_inst, seed=41, scale=(0.5, 1.4), only=mine)
+    counted = sum(W.counted_cells_mk2(m, p) for m, p, _, _ in inst)
+    cells = sum(m.n_cells for m, _, _, _ in inst)
+    B = sw.Sweep(inst, device=local)
+    streams = [torch.cuda.ExternalStream(S.stream_handle(), device=local) for S in B.items]
+    s0 = torch.cuda.current_stream(local)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    def one(ev=None):
+        flush.fill_(1.0)
+        start = torch.cuda.Event(enable_timing=True)
+        start.record(s0)
+        for st in streams:
+            st.wait_event(start)
+        B.step_async(1)
+        for st in streams:
+            e = torch.cuda.Event()
+            e.record(st)
+            s0.wait_event(e)
+        end = torch.cuda.Event(enable_timing=True)
+        end.record(s0)
+        if ev is not None:
+            ev.append((start, end))
+        return sum(S.launches() for S in B.items)
+
+    for _ in range(args.warmup):
+        one()
+    torch.cuda.synchronize(local)
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    evs, launches = [], 0
+    for _ in range(args.steps):
+        launches += one(evs)
+    torch.cuda.synchronize(local)
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    total_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in evs), dist, f"cuda:{local}")
+    counted_all = counted
+    if dist:
+        t = torch.tensor([float(counted)], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t)
+        counted_all = float(t.item())
+    value = counted_all * args.steps / (total_ms / 1000.0)
+    peak, peak_kind = measured_peaks()
+    achieved = BYTES_PER_CELL["mk2"] * counted_all / world / (total_ms / args.steps / 1000.0) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded instances: grid scale, initial field, Monte-Carlo moments)",
+        "config": {"workload": WORKLOADS["sweep16"][0], "instances": n_inst, "instances_on_rank0": len(inst),
+                   "cells_rank0": int(cells), "cells_updated_per_step": int(counted_all),
+                   "l2": "flushed between timed steps (256 MiB write)",
+                   "parallelism": f"instances partitioned over {world} GPU(s)"},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "batched moving-grid steps of all instances on a GPU",
+                     "bytes_per_cell": BYTES_PER_CELL["mk2"], "avg_launch_us": total_ms / args.steps * 1000.0,
+                     "peak_kind": f"{peak_kind} hbm_gbs (burst copy)"},
+        "clocks": clocks,
+    }
+    B.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -265,6 +366,13 @@ def main():
 
     if args.impl == "reference" and rank != 0:
         return  # the reference arm runs on rank 0 only
+    if args.workload == "sweep16":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the sweep workload has no reference arm; "
+                              "its instances are the moving-grid step timed by the default workload"}))
+            return
+        run_sweep(args, rank, world, local)
+        return
     desc, form, dims, mesh, params, st0, mc, counted = build_workload(args.workload)
     config = {"workload": desc, "cells": int(mesh.n_cells), "cells_updated_per_step": int(counted),
               "faces": int(mesh.n_faces), "points": int(mesh.n_points),

@@ -1,0 +1,126 @@
+"""Batches of independent instances: parameter sweeps over many grids.
+
+An instance is one grid with its own inflow parameters, state and
+Monte-Carlo moments; instances never exchange data and each keeps its own
+CFL dt (the reference's dt is a minimum over one grid).  A batch therefore
+runs every instance on its own context: a step enqueues the captured step
+graph of every instance (each on its own streams) before waiting for any, so
+the instances' latency-bound kernels fill the GPU together.  Across GPUs the
+instances are partitioned by cell count (greedy, largest first) and the
+results are gathered on the host: no collective on the step path.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _native as N
+from .mesh import Mesh
+from .setka import Setka
+
+
+def partition(cell_counts, n_parts: int) -> list[list[int]]:
+    """Greedy largest-first assignment of instances to ``n_parts`` GPUs by
+    cell count; returns the instance indices of every part (each part in
+    increasing index order).  The largest part is at most the mean load plus
+    the largest instance."""
+    if n_parts < 1:
+        raise ValueError("n_parts must be >= 1")
+    counts = np.asarray(cell_counts, dtype=np.int64)
+    order = sorted(range(len(counts)), key=lambda i: (-int(counts[i]), i))
+    load = [0] * n_parts
+    parts: list[list[int]] = [[] for _ in range(n_parts)]
+    for i in order:
+        p = min(range(n_parts), key=lambda q: (load[q], q))
+        parts[p].append(i)
+        load[p] += int(counts[i])
+    return [sorted(p) for p in parts]
+
+
+class Sweep:
+    """Instances stepped together on one GPU.
+
+    ``instances``: sequence of (mesh, params, state (5, n_cells), mc or None).
+    """
+
+    def __init__(self, instances, device: int = 0, form: int = N.FORM_MK2):
+        self.form = form
+        self.items: list[Setka] = []
+        for mesh, params, st0, mc in instances:
+            S = Setka(mesh, params, device)
+            S.set_par(0, st0)
+            S.set_par(1, st0)
+            if mc is not None:
+                S.set_mc(*mc)
+            self.items.append(S)
+
+    def __len__(self) -> int:
+        return len(self.items)
+
+    @property
+    def cells(self) -> list[int]:
+        return [S.mesh.n_cells for S in self.items]
+
+    def step_async(self, n: int = 1):
+        """Enqueue ``n`` steps on every instance without waiting."""
+        for S in self.items:
+            S.step_async(self.form, n)
+
+    def synchronize(self):
+        for S in self.items:
+            S.synchronize()
+
+    def step(self, n: int = 1):
+        """``n`` steps of every instance, then wait for all."""
+        self.step_async(n)
+        self.synchronize()
+
+    def par(self, i: int, buf: int) -> np.ndarray:
+        return self.items[i].par(buf)
+
+    def close(self):
+        for S in self.items:
+            S.close()
+        self.items = []
+
+
+BASE_DIMS = (200, 100, 50, 100, 100, 100, 150, 150)  # Setka(N1..M4) of ~200k cells
+MIN_DIMS = (8, 4, 3, 6, 23, 6, 7, 7)  # the constructor needs M1 > n_inner = 20
+
+
+def instance_set(n: int, seed: int = 41, scale=(0.5, 1.4), only=None) -> list[tuple]:
+    """``n`` seeded instances of the moving-grid step with uneven grids: the
+    rail grid Setka(N1..M4) of ~200k cells with every count scaled by a
+    seeded factor in ``scale`` (cells grow with its square: 0.5..1.4 gives
+    ~50k..~400k cells, the sweep configuration's range), each with the
+    reference's initial field and its own Monte-Carlo moments.  ``only``
+    builds just those instance indices (the others' seeds are unchanged)."""
+    from . import workloads as W
+
+    u = W.splitmix64(seed, n)
+    out = []
+    for i in (range(n) if only is None else only):
+        f = scale[0] + (scale[1] - scale[0]) * float(u[i])
+        dims = tuple(max(lo, int(round(b * f))) for b, lo in zip(BASE_DIMS, MIN_DIMS))
+        mesh = Mesh.setka(*dims)
+        params = N.reference_params()
+        out.append((mesh, params, W.init_conditions_reference(mesh), W.mc_fields(mesh, seed=seed + i)))
+    return out
+
+
+def gather_results(local: dict, dist=None) -> dict | None:
+    """Merge every rank's {instance index: result} on rank 0 (host-side
+    gather; None on the other ranks).  Without a process group the local
+    results are returned."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return dict(local)
+    parts = [None] * dist.get_world_size() if dist.get_rank() == 0 else None
+    dist.gather_object(local, parts, dst=0)
+    if dist.get_rank() != 0:
+        return None
+    merged: dict = {}
+    for p in parts:
+        dup = set(merged) & set(p)
+        if dup:
+            raise ValueError(f"instances reported by two ranks: {sorted(dup)}")
+        merged.update(p)
+    return merged
