@@ -81,12 +81,12 @@ int upload(DBuf& b, const T* src, size_t n, cudaStream_t s) {
 struct gelios_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
-    // side streams: work of the moving-grid step that does not depend on the
-    // motion runs there while the main stream moves the grid
-    cudaStream_t side = nullptr;   // face reconstructions, tracked-face star pressures
-    cudaStream_t side2 = nullptr;  // charge-exchange source terms
-    cudaEvent_t ev_fork = nullptr, ev_recon = nullptr, ev_rails = nullptr, ev_tracked = nullptr,
-                ev_source = nullptr;
+    // side stream: the work of the moving-grid step that does not depend on
+    // the motion runs there while the main stream moves the grid (one side
+    // stream: a second one for the source terms made the main chain slower
+    // through contention for the SMs)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_recon = nullptr, ev_rails = nullptr, ev_tracked = nullptr;
     gelios_params prm{};
     bool have_mesh = false;
     DevMesh d;
@@ -237,15 +237,12 @@ extern "C" int gelios_create(gelios_ctx** out, const gelios_params* prm, int dev
     // first while the side streams' grid-wide kernels fill the rest.
     int prio_least = 0, prio_greatest = 0;
     GELIOS_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest));
-    const int prio_mid = prio_greatest < prio_least ? prio_greatest + 1 : prio_greatest;
     GELIOS_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, prio_greatest));
-    GELIOS_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->side, cudaStreamNonBlocking, prio_mid));
-    GELIOS_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->side2, cudaStreamNonBlocking, prio_least));
+    GELIOS_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->side, cudaStreamNonBlocking, prio_least));
     GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
     GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_recon, cudaEventDisableTiming));
     GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_rails, cudaEventDisableTiming));
     GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_tracked, cudaEventDisableTiming));
-    GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_source, cudaEventDisableTiming));
     if (ctx->words.alloc(64)) return GELIOS_E_CUDA;
     GELIOS_CUDA_TRY(cudaMemsetAsync(ctx->words.p, 0, 64, ctx->stream));
     *out = ctx.release();
@@ -267,12 +264,12 @@ extern "C" void gelios_destroy(gelios_ctx* ctx) {
         cudaStreamSynchronize(ctx->stream);
         cudaStreamDestroy(ctx->stream);
     }
-    for (cudaStream_t* sp : {&ctx->side, &ctx->side2})
+    for (cudaStream_t* sp : {&ctx->side})
         if (*sp) {
             cudaStreamSynchronize(*sp);
             cudaStreamDestroy(*sp);
         }
-    for (cudaEvent_t e : {ctx->ev_fork, ctx->ev_recon, ctx->ev_rails, ctx->ev_tracked, ctx->ev_source})
+    for (cudaEvent_t e : {ctx->ev_fork, ctx->ev_recon, ctx->ev_rails, ctx->ev_tracked})
         if (e) cudaEventDestroy(e);
     delete ctx;
 }
@@ -762,23 +759,21 @@ int enqueue_mk2(gelios_ctx* ctx, const StepBuffers& b) {
     const DevMesh& d = ctx->d;
     const gelios_params& P = ctx->prm;
     cudaStream_t s = ctx->stream;
-    // Three streams per step.
-    //   side:  face reconstructions, the star pressures of the tracked
-    //          faces (neither depends on the motion), then, once the
-    //          rails have moved, the tracked-face fluxes (sampling of
-    //          the solved Riemann problems at the face speed);
-    //   side2: charge-exchange source terms and pre-motion volumes;
-    //   main:  surface tracking + rails, the other face fluxes, the
-    //          cell update, the commit.
-    cudaStream_t sd = ctx->side, sd2 = ctx->side2;
+    // Two streams per step.
+    //   side: face reconstructions, the star pressures of the tracked faces
+    //         and the charge-exchange source terms (none depends on the
+    //         motion), then, once the rails have moved, the tracked-face
+    //         fluxes (sampling of the solved Riemann problems at the face
+    //         speed);
+    //   main: surface tracking + rails, the other face fluxes, the cell
+    //         update, the commit.
+    cudaStream_t sd = ctx->side;
     GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_fork, s));
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_fork, 0));
-    GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd2, ctx->ev_fork, 0));
     launch_mk2_recon(d, P, b, ctx->rec.as<double>(), sd);
     GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_recon, sd));
     const int nsv = launch_mk2_tracked_solve(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(), sd);
-    launch_mk2_source(d, P, b, ctx->aux.as<double>(), sd2);
-    GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_source, sd2));
+    launch_mk2_source(d, P, b, ctx->aux.as<double>(), sd);
     cudaEvent_t e1 = ctx->phase_begin();
     const int nm = launch_motion(d, P, b, ctx->surface.as<double>(), s);
     ctx->phase_end(2, e1, nm);  // Move_surface + rails
@@ -793,7 +788,6 @@ int enqueue_mk2(gelios_ctx* ctx, const StepBuffers& b) {
     ctx->phase_end(1, e3, nfl);
     // the update reads the tracked-face fluxes and the source terms
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_tracked, 0));
-    GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_source, 0));
     cudaEvent_t e5 = ctx->phase_begin();
     launch_mk2_update(d, P, b, ctx->flux.as<double>(), ctx->aux.as<double>(), s);
     ctx->phase_end(3, e5, 1);
