@@ -95,7 +95,7 @@ struct gelios_ctx {
     DBuf fA, fB, ftype, fmaster, fsosed, fcopy, fsdown;
     DBuf rtype, rM, rpstart, rpts, rkstart, rkeys, rs;
     DBuf lc, li, lo, sp_point, sp_line, sp_inc, sp_ainc, sp_fix, sp_of_point;
-    DBuf u_slot, u_cell, u_twin, u_A, u_B, u_info, flux, aux, rec, pstar, src_lo;
+    DBuf u_slot, u_cell, u_twin, u_A, u_B, u_info, u_nb, u_sd, u_sd2, flux, aux, rec, pstar, src_lo;
     DBuf Hn, Hu, Hv, HT, ku, kv, kT, r_istoch, cback, cnext;
     // state par[2] x 5 fields, centroids [2], scratch
     DBuf state[2];
@@ -106,7 +106,11 @@ struct gelios_ctx {
     DBuf inner;
     int n_inner = 0;
     int n_sp = 0;
-    bool cen_valid = false;  // cen[0] holds the centroids of the current points
+    // cen[0] holds the centroids of the current points (rows cx, cy,
+    // |c|^(2 gamma), area, rotated volume); after a moving-grid call row 2
+    // holds only the CF_RP cells, which the other forms do not accept
+    bool cen_valid = false;
+    bool cen_rp_partial = false;
     // Instantiated graphs of one moving-grid step, keyed by the buffers the
     // step reads (state parity and centroid buffer); dropped whenever the
     // topology or the parameters change.
@@ -431,6 +435,24 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
                 return GELIOS_E_MESH;
             }
     }
+    // CF_RP: cells whose |centroid|^(2 gamma) a moving-grid step reads: the
+    // cells of every radially reconstructed unit (its two cells and both
+    // Sosed_down cells, see mk2_recon_kernel) and the masters of the inner
+    // shock's faces (surface_faces_kernel)
+    for (size_t u = 0; u < u_slot.size(); u++) {
+        const int g = u_slot[u], K = u_cell[u];
+        const int nbu = u_twin[u] >= 0 ? snb[g] : -1;
+        const int ft = static_cast<int>(sinfo[g] & SI_TYPE_MASK);
+        const bool radial = ((cflags[K] & CF_C1) && (ft == G_USUALY || ft == G_AXIS)) || ft == G_INNER_SPHERE ||
+                            (ft == G_USUALY && nbu >= 0 && (cflags[nbu] & CF_C1));
+        if (!radial) continue;
+        for (const int c : {K, nbu, ssd[g], ssd2[g]})
+            if (c >= 0) cflags[c] |= CF_RP;
+    }
+    for (int j = 0; j < v->n_inner_line; j++) {
+        const int f = v->line_inner[j];
+        if (f >= 0 && f < nf && v->face_master[f] >= 0) cflags[v->face_master[f]] |= CF_RP;
+    }
     // surface-tracking nodes (see point_velocity)
     std::vector<int32_t> sp_point, sp_line, sp_inc, sp_ainc, sp_fix(12, 0);
     std::vector<int32_t> local(np, -1);
@@ -531,23 +553,33 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     rc |= upload(ctx->lo, v->line_outer, v->n_outer_line, s);
     rc |= upload(ctx->u_slot, u_slot.data(), u_slot.size(), s);
     {
-        // end points and slot info of each unit's face (unit-major copies)
+        // unit-major copies of what a unit reads about its face and cells:
+        // end points, slot info with both cells' flags, neighbour and the
+        // two Sosed_down cells
         const size_t nu = u_slot.size();
-        std::vector<int32_t> uA(nu), uB(nu);
+        std::vector<int32_t> uA(nu), uB(nu), unb(nu), usd(nu), usd2(nu);
         std::vector<uint32_t> ui(nu);
         for (size_t u = 0; u < nu; u++) {
-            uA[u] = sA[u_slot[u]];
-            uB[u] = sB[u_slot[u]];
-            ui[u] = sinfo[u_slot[u]];
+            const int g = u_slot[u];
+            uA[u] = sA[g];
+            uB[u] = sB[g];
+            unb[u] = u_twin[u] >= 0 ? snb[g] : -1;
+            usd[u] = ssd[g];
+            usd2[u] = ssd2[g];
+            const uint32_t nbf = unb[u] >= 0 ? cflags[unb[u]] : 0u;
+            ui[u] = sinfo[g] | ((cflags[u_cell[u]] & 15u) << UI_CF_OWN) | ((nbf & 15u) << UI_CF_NB);
         }
         rc |= upload(ctx->u_A, uA.data(), nu, s);
         rc |= upload(ctx->u_B, uB.data(), nu, s);
         rc |= upload(ctx->u_info, ui.data(), nu, s);
+        rc |= upload(ctx->u_nb, unb.data(), nu, s);
+        rc |= upload(ctx->u_sd, usd.data(), nu, s);
+        rc |= upload(ctx->u_sd2, usd2.data(), nu, s);
     }
     rc |= upload(ctx->u_cell, u_cell.data(), u_cell.size(), s);
     rc |= upload(ctx->u_twin, u_twin.data(), u_twin.size(), s);
     rc |= upload<double>(ctx->flux, nullptr, 5 * static_cast<size_t>(ng), s);
-    rc |= upload<double>(ctx->aux, nullptr, 5 * static_cast<size_t>(nc), s);
+    rc |= upload<double>(ctx->aux, nullptr, 3 * static_cast<size_t>(nc), s);
     rc |= upload<double>(ctx->rec, nullptr, static_cast<size_t>(kRecRows) * u_slot.size(), s);
     rc |= upload<double>(ctx->pstar, nullptr, static_cast<size_t>(u_tr1 - u_tr0) + 1, s);
     rc |= upload(ctx->sp_point, sp_point.data(), sp_point.size(), s);
@@ -580,8 +612,8 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     }
     rc |= upload<double>(ctx->state[0], nullptr, 5 * static_cast<size_t>(nc), s);
     rc |= upload<double>(ctx->state[1], nullptr, 5 * static_cast<size_t>(nc), s);
-    rc |= upload<double>(ctx->cen[0], nullptr, 3 * static_cast<size_t>(nc), s);
-    rc |= upload<double>(ctx->cen[1], nullptr, 3 * static_cast<size_t>(nc), s);
+    rc |= upload<double>(ctx->cen[0], nullptr, 5 * static_cast<size_t>(nc), s);
+    rc |= upload<double>(ctx->cen[1], nullptr, 5 * static_cast<size_t>(nc), s);
     rc |= upload<double>(ctx->surface, nullptr,
                          4 * (static_cast<size_t>(v->n_contact) + v->n_inner_line + v->n_outer_line) + 1, s);
     if (rc) return GELIOS_E_CUDA;
@@ -615,6 +647,9 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     d.u_A = ctx->u_A.as<int32_t>();
     d.u_B = ctx->u_B.as<int32_t>();
     d.u_info = ctx->u_info.as<uint32_t>();
+    d.u_nb = ctx->u_nb.as<int32_t>();
+    d.u_sd = ctx->u_sd.as<int32_t>();
+    d.u_sd2 = ctx->u_sd2.as<int32_t>();
     d.u_cell = ctx->u_cell.as<int32_t>();
     d.u_twin = ctx->u_twin.as<int32_t>();
     d.u_tr0 = u_tr0;
@@ -880,11 +915,13 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
     double* cen0 = ctx->cen[0].as<double>();
     double* cen1 = ctx->cen[1].as<double>();
     if (ctx->ev_used > 4096) ctx->collect();
-    if (!ctx->cen_valid) {
+    const size_t ncz = d.n_cells;
+    if (!ctx->cen_valid || (form != GELIOS_FORM_MK2 && ctx->cen_rp_partial)) {
         cudaEvent_t e0 = ctx->phase_begin();
-        launch_centroid(d, d.X, d.Y, cen0, cen0 + d.n_cells, cen0 + 2 * static_cast<size_t>(d.n_cells), P.gamma, s);
+        launch_centroid(d, d.X, d.Y, cen0, cen0 + ncz, cen0 + 2 * ncz, P.gamma, s, cen0 + 3 * ncz, cen0 + 4 * ncz);
         ctx->phase_end(0, e0, 1);
         launches++;
+        ctx->cen_rp_partial = false;
     }
     for (int st = 0; st < nsteps; st++) {
         const int cur = st & 1, nxt = cur ^ 1;
@@ -904,9 +941,13 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             b.cx = cc;
             b.cy = cc + d.n_cells;
             b.rp = cc + 2 * static_cast<size_t>(d.n_cells);
+            b.vs = cc + 3 * ncz;
+            b.vol = cc + 4 * ncz;
             b.cx_next = cn;
             b.cy_next = cn + d.n_cells;
             b.rp_next = cn + 2 * static_cast<size_t>(d.n_cells);
+            b.vs_next = cn + 3 * ncz;
+            b.vol_next = cn + 4 * ncz;
             const int n = step_mk2(ctx, b);
             if (n < 0) return n;
             launches += n;
@@ -963,6 +1004,7 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
     // the five-fluid form leaves the centroids of the points before its
     // last motion in cen[0]
     ctx->cen_valid = !(form == GELIOS_FORM_5_KOMPONENT && nsteps > 0);
+    if (form == GELIOS_FORM_MK2 && nsteps > 0) ctx->cen_rp_partial = true;
     if (status) {
         Words r{};
         GELIOS_CUDA_TRY(cudaMemcpyAsync(&r, ctx->words.p, sizeof(r), cudaMemcpyDeviceToHost, s));

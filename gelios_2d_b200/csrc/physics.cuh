@@ -28,7 +28,12 @@ enum : uint32_t {
     SI_NP = 1u << 4,      // exactly one end point on a tracked surface (Setka.cpp:10301-10324)
 };
 // Cell flag bits.
-enum : uint32_t { CF_AXIS = 1u, CF_C1 = 2u, CF_CENTR = 4u };
+// cell flags; CF_RP marks the cells whose |centroid|^(2 gamma) a moving-grid
+// step reads (radial reconstructions, inner-shock masters)
+enum : uint32_t { CF_AXIS = 1u, CF_C1 = 2u, CF_CENTR = 4u, CF_RP = 8u };
+// unit info: slot info (SI_*) in bits 0-7, the owner's cell flags from bit
+// 8, the neighbour's from bit 12
+enum : uint32_t { UI_CF_OWN = 8u, UI_CF_NB = 12u };
 // Status flag bits (gelios_status::flags).
 enum : int { ST_ITER_CAP = 1, ST_TVD_BAD = 2, ST_NEWTON_NEG = 4, ST_CHAIN = 8, ST_DT_BAD = 16, ST_WAVE_ORDER = 32 };
 

@@ -505,7 +505,7 @@ __device__ __forceinline__ void block_reduce_commit(double t, int nro, int np_, 
 
 // ------------------------------------------------------------------ kernels
 __global__ void centroid_kernel(DevMesh d, const double* __restrict__ X, const double* __restrict__ Y, double* cx,
-                                double* cy, double* rp, double g2) {
+                                double* cy, double* rp, double g2, double* vs, double* vol) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= d.n_cells) return;
     const int s = d.cstart[c], n = d.cstart[c + 1] - s;
@@ -514,6 +514,10 @@ __global__ void centroid_kernel(DevMesh d, const double* __restrict__ X, const d
     cx[c] = x;
     cy[c] = y;
     rp[c] = pow2g(sqrt(sq(x) + sq(y)), g2);
+    if (vs) {
+        vs[c] = area(d.contour + s, n, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], X, Y, false);
+        vol[c] = volume_rotate(d.contour + s, n, X, Y);
+    }
 }
 
 // ------------------------------------------------------------------ face units
@@ -733,10 +737,10 @@ __global__ void __launch_bounds__(128) mk2_recon_kernel(DevMesh d, gelios_params
     int status = 0;
     if (u < d.n_units) {
         const size_t n = d.n_units;
-        const int g = d.u_slot[u], K = d.u_cell[u], gt = d.u_twin[u];
+        const int K = d.u_cell[u], nb = d.u_nb[u];
+        const uint32_t info = d.u_info[u];
         const double x = b.cx[K], y = b.cy[K];
         const bool procK = !(sqrt(sq(x) + sq(y)) < P.R11);
-        const int nb = gt >= 0 ? d.snb[g] : -1;
         double x3 = 0.0, y3 = 0.0;
         bool procN = false;
         if (nb >= 0) {
@@ -761,16 +765,15 @@ __global__ void __launch_bounds__(128) mk2_recon_kernel(DevMesh d, gelios_params
             rec[16 * n + u] = procN ? sqrt(sq(x3 - x2) + sq(y3 - y2)) : -1.0;
         }
         if (procK || procN) {
-            const uint32_t info = d.sinfo[g];
             const int ft = info & SI_TYPE_MASK;
-            const uint32_t cf = d.cflags[K];
+            const uint32_t cf = (info >> UI_CF_OWN) & 15u;
             const double g2 = 2 * P.gamma;
             const St5 par1 = load_state(b.cur, K);
             St5 par11 = par1;
             St5 par2 = get_par(P, ft, par1, b.cur, nb, x2, y2);
             const double dis = sqrt(sq(x2) + sq(y2));
             const bool tracked = (info & SI_GOD) != 0;
-            const uint32_t nbf = nb >= 0 ? d.cflags[nb] : 0u;
+            const uint32_t nbf = (info >> UI_CF_NB) & 15u;
             const bool radial = ((cf & CF_C1) && (ft == G_USUALY || ft == G_AXIS)) || ft == G_INNER_SPHERE ||
                                 (ft == G_USUALY && (nbf & CF_C1));
             const double pdis = radial ? pow2g(dis, g2) : 1.0;
@@ -779,7 +782,7 @@ __global__ void __launch_bounds__(128) mk2_recon_kernel(DevMesh d, gelios_params
                     const bool s1 = sd == 1;
                     const St5 r = mk2_usualy_side(b.cur, b.cx, b.cy, b.rp, x2, y2, dis, pdis, s1 ? par2 : par1,
                                                   s1 ? x3 : x, s1 ? y3 : y, b.rp[s1 ? nb : K], s1 ? nbf : cf,
-                                                  s1 ? K : nb, s1 ? d.ssd2[g] : d.ssd[g], tracked, &status);
+                                                  s1 ? K : nb, s1 ? d.u_sd2[u] : d.u_sd[u], tracked, &status);
                     const int r0 = s1 ? 5 : 0;
                     rec[(r0 + 0) * n + u] = r.ro;
                     rec[(r0 + 1) * n + u] = r.p;
@@ -801,7 +804,7 @@ __global__ void __launch_bounds__(128) mk2_recon_kernel(DevMesh d, gelios_params
                         par11.p = par11.p * (b.rp[K] / pdis);
                         polar_perenos(x, y, x2, y2, par11.u, par11.v);
                     } else {
-                        par11 = tvd_axis(b.cur, b.cx, b.cy, x2, y2, par1, x, y, d.ssd[g]);
+                        par11 = tvd_axis(b.cur, b.cx, b.cy, x2, y2, par1, x, y, d.u_sd[u]);
                     }
                     par2 = par11;
                     par2.v = -par2.v;
@@ -931,11 +934,10 @@ __global__ void __launch_bounds__(64) mk2_tracked_solve_kernel(DevMesh d, gelios
     }
 }
 
-// Terms of the MK2 cell update that do not depend on the fluxes or on the
-// motion: the charge-exchange source Get_Sourse_MK1 (Cell.cpp:498-665) and
-// the area / rotated volume of the cell before the motion.  Runs on a side
-// stream while surface tracking and the rails move the grid.
-// aux rows: q1, q2, q3, vs1 (Get_Volume), Volume (Get_Volume_rotate/2pi)
+// The term of the MK2 cell update that depends neither on the fluxes nor on
+// the motion: the charge-exchange source Get_Sourse_MK1 (Cell.cpp:498-665).
+// Runs on a side stream while surface tracking and the rails move the grid.
+// aux rows: q1, q2, q3
 __global__ void __launch_bounds__(128) mk2_source_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                          double* __restrict__ aux) {
     // four lanes per cell, one hydrogen species per lane; the four rates
@@ -988,16 +990,18 @@ __global__ void __launch_bounds__(128) mk2_source_kernel(DevMesh d, gelios_param
         aux[0 * n + c] = q1;
         aux[1 * n + c] = q2;
         aux[2 * n + c] = q3;
-        const int s0 = d.cstart[c], nv = d.cstart[c + 1] - s0;
-        const int32_t* con = d.contour + s0;
-        aux[3 * n + c] = area(con, nv, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X, d.Y, false);
-        aux[4 * n + c] = volume_rotate(con, nv, d.X, d.Y);
     }
     if (status) atomicOr(b.status, status);
 }
 
 // Go_5_komponent__MK2 cell update (Setka.cpp:10386-10468) from the summed
-// slots; also the centroid of the moved cell (the next step's centroid).
+// slots.  The area and rotated volume before the motion come from the cache
+// (b.vs, b.vol); the kernel refills the cache for the next step from the
+// moved points: centroid, and area and rotated volume of every cell but the
+// C_centr ones (the points after the commit are these moved points, bit for bit),
+// |centroid|^(2 gamma) of the cells flagged CF_RP.  For a quadrilateral
+// Get_Volume and Get_Volume_posle are the same formula; other cells get the
+// Get_Volume form for the cache.
 __global__ void __launch_bounds__(128, 6) mk2_update_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                          const double* __restrict__ fl,
                                                          const double* __restrict__ aux) {
@@ -1012,8 +1016,16 @@ __global__ void __launch_bounds__(128, 6) mk2_update_kernel(DevMesh d, gelios_pa
         centroid(con, n, d.X2, d.Y2, xn, yn);
         b.cx_next[c] = xn;
         b.cy_next[c] = yn;
-        b.rp_next[c] = pow2g(sqrt(sq(xn) + sq(yn)), 2 * P.gamma);
+        const uint32_t cfl = d.cflags[c];
+        if (cfl & CF_RP) b.rp_next[c] = pow2g(sqrt(sq(xn) + sq(yn)), 2 * P.gamma);
         const double x = b.cx[c], y = b.cy[c];
+        double vs2 = 0.0, Volume2 = 0.0;
+        if (!(cfl & CF_CENTR)) {
+            vs2 = area(con, n, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X2, d.Y2, true);
+            Volume2 = volume_rotate(con, n, d.X2, d.Y2);
+            b.vs_next[c] = n == 4 ? vs2 : area(con, n, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X2, d.Y2, false);
+            b.vol_next[c] = Volume2;
+        }
         if (!(sqrt(sq(x) + sq(y)) < P.R11)) {
             tmark = 10000000.0;  // `time` starts at 1e7 in every step (Setka.cpp:10141)
             const double dt = *b.dt_cur;
@@ -1029,11 +1041,9 @@ __global__ void __launch_bounds__(128, 6) mk2_update_kernel(DevMesh d, gelios_pa
             const St5 par1 = load_state(b.cur, c);
             const size_t nc = d.n_cells;
             const double q2_1 = aux[0 * nc + c], q2_2 = aux[1 * nc + c], q3 = aux[2 * nc + c];
-            if (!(d.cflags[c] & CF_CENTR)) {
-                const double vs1 = aux[3 * nc + c];
-                const double vs2 = area(con, n, d.sA, d.sB, g0, g1, d.X2, d.Y2, true);
-                const double Volume = aux[4 * nc + c];
-                const double Volume2 = volume_rotate(con, n, d.X2, d.Y2);
+            if (!(cfl & CF_CENTR)) {
+                const double vs1 = b.vs[c];
+                const double Volume = b.vol[c];
                 const double ro = par1.ro, u = par1.u, v = par1.v, p = par1.p, Q = par1.Q;
                 const double gm1 = P.gamma - 1;
                 const double rV2 = 1.0 / Volume2, VV = Volume * rV2;
@@ -2257,8 +2267,9 @@ inline int blocks_for(int n, int t) { return (n + t - 1) / t; }
 }
 
 void launch_centroid(const DevMesh& d, const double* X, const double* Y, double* cx, double* cy, double* rp,
-                     double gamma, cudaStream_t s) {
-    if (d.n_cells > 0) centroid_kernel<<<blocks_for(d.n_cells, 256), 256, 0, s>>>(d, X, Y, cx, cy, rp, 2 * gamma);
+                     double gamma, cudaStream_t s, double* vs, double* vol) {
+    if (d.n_cells > 0)
+        centroid_kernel<<<blocks_for(d.n_cells, 256), 256, 0, s>>>(d, X, Y, cx, cy, rp, 2 * gamma, vs, vol);
 }
 void launch_stationary_units(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
                              cudaStream_t s) {

@@ -34,7 +34,10 @@ struct DevMesh {
     int u_tr0 = 0, u_tr1 = 0;  // range of the tracked-face units (grouped together)
     const int32_t *u_slot = nullptr, *u_cell = nullptr, *u_twin = nullptr;
     const int32_t *u_A = nullptr, *u_B = nullptr;  // end points of the unit's face
-    const uint32_t* u_info = nullptr;              // slot info of the unit's face
+    // slot info of the unit's face | owner flags << UI_CF_OWN | neighbour flags << UI_CF_NB
+    const uint32_t* u_info = nullptr;
+    // neighbour cell (-1: one-sided unit), Sosed_down of the face and of its twin
+    const int32_t *u_nb = nullptr, *u_sd = nullptr, *u_sd2 = nullptr;
     const int32_t *fA = nullptr, *fB = nullptr, *ftype = nullptr, *fmaster = nullptr, *fsosed = nullptr,
                   *fcopy = nullptr, *fsdown = nullptr;
     const int32_t *rtype = nullptr, *rM = nullptr, *rpstart = nullptr, *rpts = nullptr, *rkstart = nullptr,
@@ -81,9 +84,15 @@ struct StepBuffers {
     const double* cx = nullptr;
     const double* cy = nullptr;
     const double* rp = nullptr;  // |centroid|^(2 gamma) per cell
+    // moving-grid step: area (Get_Volume) and rotated volume of every cell
+    // before the motion, cached from the previous step's update
+    const double* vs = nullptr;
+    const double* vol = nullptr;
     double* cx_next = nullptr;
     double* cy_next = nullptr;
     double* rp_next = nullptr;
+    double* vs_next = nullptr;
+    double* vol_next = nullptr;
     const double* dt_cur = nullptr;
     double* dt_next = nullptr;
     unsigned long long* dt_acc = nullptr;
@@ -91,8 +100,10 @@ struct StepBuffers {
     int* status = nullptr;
 };
 
+// Centroids and |centroid|^(2 gamma) of every cell; with vs/vol also the
+// area (Get_Volume) and the rotated volume (rows of the moving-grid cache).
 void launch_centroid(const DevMesh& d, const double* X, const double* Y, double* cx, double* cy, double* rp,
-                     double gamma, cudaStream_t s);
+                     double gamma, cudaStream_t s, double* vs = nullptr, double* vol = nullptr);
 void launch_stationary_units(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
                              cudaStream_t s);
 void launch_stationary_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
