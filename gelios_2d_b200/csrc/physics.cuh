@@ -373,7 +373,7 @@ static __device__ __noinline__ double godunov_dev(double ga, double kurant, cons
                                            const double* n, double* qqq, double* ds, double w, double DIST,
                                            int max_iter, int* status, const double* p_in = nullptr,
                                            double* p_out = nullptr) {
-    const double g1 = ga - 1.0, g2 = ga + 1.0, gm = (g1 / ga) / 2.0, gp = (g2 / ga) / 2.0;
+    const double g1 = ga - 1.0, g2 = ga + 1.0, gm = (g1 / ga) / 2.0;
     const double eps = 10e-10, eps8 = 10e-8;
     const double al = n[0], be = n[1], ge = n[2];
     double time = 0.0;

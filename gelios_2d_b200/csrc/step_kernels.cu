@@ -33,6 +33,21 @@
 #include "physics.cuh"
 #include "step_kernels.cuh"
 
+// Minimum resident blocks per SM of the grid-wide moving-grid kernels
+// (register caps: 128 threads x 65536/(128 x minBlocks) registers).
+#ifndef GELIOS_RECON_MINB
+#define GELIOS_RECON_MINB 8
+#endif
+#ifndef GELIOS_FLUX_MINB
+#define GELIOS_FLUX_MINB 8
+#endif
+#ifndef GELIOS_UPDATE_MINB
+#define GELIOS_UPDATE_MINB 6
+#endif
+#ifndef GELIOS_SOURCE_MINB
+#define GELIOS_SOURCE_MINB 1
+#endif
+
 namespace gelios {
 
 // ------------------------------------------------------------------ helpers
@@ -730,7 +745,7 @@ __device__ __forceinline__ St5 mk2_usualy_side(const double* const* st, const do
 // LANES = 2: two lanes per unit; on interior faces lane 0 reconstructs the
 // owner side and lane 1 the other side.  LANES = 1: one thread does both.
 template <int LANES>
-__global__ void __launch_bounds__(128) mk2_recon_kernel(DevMesh d, gelios_params P, StepBuffers b,
+__global__ void __launch_bounds__(128, GELIOS_RECON_MINB) mk2_recon_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                         double* __restrict__ rec) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int u = t / LANES, side = LANES == 2 ? (t & 1) : 0;
@@ -829,7 +844,7 @@ __global__ void __launch_bounds__(128) mk2_recon_kernel(DevMesh d, gelios_params
 // kernel without the exact Godunov solver covers the rest (index i is
 // remapped around the tracked range), a second launch covers that range.
 template <typename TF, bool TRACKED>
-__global__ void __launch_bounds__(128) mk2_flux_kernel(DevMesh d, gelios_params P, StepBuffers b,
+__global__ void __launch_bounds__(128, GELIOS_FLUX_MINB) mk2_flux_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                        const double* __restrict__ rec, double* __restrict__ fl,
                                                        const double* __restrict__ pstar, int n_launch) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -938,7 +953,7 @@ __global__ void __launch_bounds__(64) mk2_tracked_solve_kernel(DevMesh d, gelios
 // the motion: the charge-exchange source Get_Sourse_MK1 (Cell.cpp:498-665).
 // Runs on a side stream while surface tracking and the rails move the grid.
 // aux rows: q1, q2, q3
-__global__ void __launch_bounds__(128) mk2_source_kernel(DevMesh d, gelios_params P, StepBuffers b,
+__global__ void __launch_bounds__(128, GELIOS_SOURCE_MINB) mk2_source_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                          double* __restrict__ aux) {
     // four lanes per cell, one hydrogen species per lane; the four rates
     // are summed on the cell's first lane in the reference's order
@@ -1002,7 +1017,7 @@ __global__ void __launch_bounds__(128) mk2_source_kernel(DevMesh d, gelios_param
 // |centroid|^(2 gamma) of the cells flagged CF_RP.  For a quadrilateral
 // Get_Volume and Get_Volume_posle are the same formula; other cells get the
 // Get_Volume form for the cache.
-__global__ void __launch_bounds__(128, 6) mk2_update_kernel(DevMesh d, gelios_params P, StepBuffers b,
+__global__ void __launch_bounds__(128, GELIOS_UPDATE_MINB) mk2_update_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                          const double* __restrict__ fl,
                                                          const double* __restrict__ aux) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
