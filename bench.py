@@ -42,6 +42,12 @@ WORKLOADS = {
     "plain": ("plain single-fluid step (Go_stationary form), polar 180x120, r=1..600", "plain", None),
     "k5_200k": ("plasma + four hydrogen fluids (Go_5_komponent form) on Setka(200,100,50,100,100,100,150,150)",
                 "k5", (200, 100, 50, 100, 100, 100, 150, 150)),
+    "mhd_200k": ("ion MHD fluid (HLLD) + pickup protons (HLLC) on the moving grid Setka(200,100,50,100,100,100,"
+                 "150,150): LISM B=0.01 at 30 deg, seeded fixed charge-exchange sources", "mhd",
+                 (200, 100, 50, 100, 100, 100, 150, 150)),
+    "mhd_1m": ("ion MHD fluid (HLLD) + pickup protons (HLLC) on the moving grid Setka(480,240,100,220,200,200,300,"
+               "300): LISM B=0.01 at 30 deg, seeded fixed charge-exchange sources", "mhd",
+               (480, 240, 100, 220, 200, 200, 300, 300)),
     "sweep16": ("16 independent moving-grid instances, Setka(200,100,50,100,100,100,150,150) scaled by "
                 "U(0.5,1.4) per instance (~50k..~400k cells each), batched on each GPU", "sweep", None),
 }
@@ -51,12 +57,16 @@ WORKLOADS = {
 #   plain form: 8*(2*5) + 16 points + 4*4 indices = 112 B
 #   four-fluid form: 8*(2*21) state (plasma 5 + hydrogen 16) + 16*(1+1) points
 #             + 8 written point coordinate + 4*4 neighbour indices = 392 B
-BYTES_PER_CELL = {"mk2": 288, "plain": 112, "k5": 392}
+#   MHD + pickup form: 8*(2*13) state (ions ro, p, u, v, w, Bx, By, Bz, Q; pickup
+#             ro, p, u, v) + 8*3 fixed sources + 16*(1+1) points + 8 written point
+#             coordinate + 4*4 neighbour indices = 288 B
+BYTES_PER_CELL = {"mk2": 288, "plain": 112, "k5": 392, "mhd": 288}
 STEP_KERNELS = {
     "mk2": "whole moving-grid step: recon, tracked_solve, source, surface_faces, rails, flux x2, update, commit "
            "(one CUDA graph, 3 streams)",
     "plain": "whole plain step: stationary_unit + stationary_update + dt_finalize",
     "k5": "whole four-fluid step: centroid, surface_faces, rails, k5_cell, commit",
+    "mhd": "whole MHD + pickup step: surface_faces, rails, mhd_face, mhd_update, commit",
 }
 
 
@@ -78,6 +88,14 @@ def build_workload(name: str):
         params = N.reference_params()
         st0 = W.init_conditions_reference(mesh)
         mc = W.mc_fields(mesh, seed=9)
+        counted = W.counted_cells_mk2(mesh, params)
+    elif form == "mhd":
+        # `mc` carries (boundary data, extra rows (8, n_cells), fixed sources)
+        mesh = g.Mesh.setka(*dims)
+        params = N.reference_params()
+        st0 = W.init_conditions_reference(mesh)
+        mp = W.mhd_params()
+        mc = (mp, W.mhd_initial(mesh, st0, mp), W.mhd_sources(mesh, seed=17))
         counted = W.counted_cells_mk2(mesh, params)
     elif form == "k5":
         # `mc` carries the hydrogen fluids (16, n_cells) for this form
@@ -172,9 +190,33 @@ def ncu_traffic(workload: str):
     return float(m.group(1)) if m else None
 
 
+def cpu_oracle_mhd_rate(mesh, params, st0, mc, counted, budget_s=12.0, max_steps=200):
+    """The MHD + pickup form has no reference step: its CPU baseline is the
+    oracle's restatement (go_mhd, one thread) on the same grid and inputs."""
+    from oracle import oracle as O
+
+    go = O.GoParams(**{n: getattr(params, n) for n, _ in O.GoParams._fields_ if n != "pad_"}, pad_=0)
+    ora = O.Oracle(go, mesh)
+    for b in (0, 1):
+        ora.set_state(b, st0)
+        ora.set_mhd(b, mc[1])
+    ora.set_sources(*mc[2])
+    mp = mc[0].as_dict()
+    t0 = time.perf_counter()
+    ora.mhd(mp, 1)
+    one = time.perf_counter() - t0
+    steps = int(max(1, min(max_steps, budget_s / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    ora.mhd(mp, steps)
+    el = time.perf_counter() - t0
+    return counted * steps / el, steps, 1, el
+
+
 def cpu_reference_rate(mesh, params, st0, mc, counted, form, budget_s=12.0, max_steps=200, threads=None):
     """The reference's own step (compiled from its sources, all host threads)
     on the same grid: cell-updates/s over a bounded number of steps."""
+    if form == "mhd":
+        return cpu_oracle_mhd_rate(mesh, params, st0, mc, counted, budget_s, max_steps)
     from oracle import ref
 
     threads = threads or os.cpu_count() or 1
@@ -216,11 +258,16 @@ def load_inputs(S, form, st0, mc):
     if form == "k5":
         S.set_hydrogen(0, mc)
         S.set_hydrogen(1, mc)
+    elif form == "mhd":
+        S.set_mhd_params(mc[0])
+        S.set_mhd(0, mc[1])
+        S.set_mhd(1, mc[1])
+        S.set_sources(*mc[2])
     elif mc is not None:
         S.set_mc(*mc)
 
 
-def fp32_flux_errors(mesh, params32, st0, mc, fcode, device, counts=(1, 100, 2000)) -> dict:
+def fp32_flux_errors(mesh, params32, st0, mc, fcode, device, counts=(1, 100, 2000), form="") -> dict:
     """L1 and Linf relative errors of rho, p, u, v of the FP32-flux form
     against the FP64 path (itself within 1e-12 per step of the reference's
     CPU step) after 1, 100 and 2000 steps from the same initial state."""
@@ -235,13 +282,19 @@ def fp32_flux_errors(mesh, params32, st0, mc, fcode, device, counts=(1, 100, 200
         res = []
         for prm in (params32, params64):
             S = g.Setka(mesh, prm, device=device)
-            load_inputs(S, "k5" if fcode == N.FORM_5_KOMPONENT else "", st0, mc)
+            load_inputs(S, form, st0, mc)
             st = S.step(fcode, n)
-            res.append(S.par(st.result_buf))
+            r = S.par(st.result_buf)
+            if form == "mhd":
+                r = np.concatenate([r, S.mhd(st.result_buf)])
+            res.append(r)
             S.close()
         a, b = res
         errs = {}
-        for k, name in enumerate(("rho", "p", "u", "v")):
+        names = ("rho", "p", "u", "v") if form != "mhd" else ("rho", "p", "u", "v", None, "w", "Bx", "By", "Bz")
+        for k, name in enumerate(names):
+            if name is None:
+                continue
             d = np.abs(a[k] - b[k])
             errs[name] = {"L1": float(d.sum() / max(np.abs(b[k]).sum(), 1e-300)),
                           "Linf": float(d.max() / max(np.abs(b[k]).max(), 1e-300))}
@@ -376,17 +429,19 @@ def main():
     desc, form, dims, mesh, params, st0, mc, counted = build_workload(args.workload)
     config = {"workload": desc, "cells": int(mesh.n_cells), "cells_updated_per_step": int(counted),
               "faces": int(mesh.n_faces), "points": int(mesh.n_points),
-              "l2": "flushed between timed steps (256 MiB write)" if args.workload != "mk2_1m" else
+              "l2": "flushed between timed steps (256 MiB write)" if not args.workload.endswith("_1m") else
                     "inputs larger than L2", "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
 
+    cpu_kind = "port" if form == "mhd" else "reference"
+    cpu_what = "the oracle's restatement (no reference step exists)" if form == "mhd" else "the reference step"
     if args.impl == "reference":
         rate, steps, threads, el = cpu_reference_rate(mesh, params, st0, mc, counted, form)
         line = {"metric": METRIC, "value": rate, "unit": "cell-updates/s", "impl": "reference",
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": 1000.0 * el / steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "config": config,
-                "cpu_baseline": {"value": rate, "unit": "cell-updates/s", "cores": threads, "kind": "reference",
-                                 "sample": f"{steps} steps of the reference step on the full grid ({el:.1f} s)"},
+                "cpu_baseline": {"value": rate, "unit": "cell-updates/s", "cores": threads, "kind": cpu_kind,
+                                 "sample": f"{steps} steps of {cpu_what} on the full grid ({el:.1f} s)"},
                 "e2e": {"value": rate, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
@@ -411,10 +466,10 @@ def main():
         params = params.copy(precision=N.PREC_FP32_FLUX)
     S = g.Setka(mesh, params, device=device)
     load_inputs(S, form, st0, mc)
-    fcode = {"mk2": N.FORM_MK2, "k5": N.FORM_5_KOMPONENT}.get(form, N.FORM_STATIONARY)
+    fcode = {"mk2": N.FORM_MK2, "k5": N.FORM_5_KOMPONENT, "mhd": N.FORM_MHD_PUI}.get(form, N.FORM_STATIONARY)
     stream = torch.cuda.ExternalStream(S.stream_handle(), device=device)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")
-    do_flush = args.workload != "mk2_1m"
+    do_flush = not args.workload.endswith("_1m")
     steps_per_call = 1 if do_flush else 10
 
     def one(timed_events=None):
@@ -464,8 +519,9 @@ def main():
     host_in = torch.from_numpy(np.ascontiguousarray(st0)).pin_memory().numpy()
     host_out = torch.empty(st0.shape, dtype=torch.float64).pin_memory().numpy()
     e2e_bytes = int(st0.nbytes)
-    if form == "k5":  # the hydrogen fluids are step inputs and outputs too
-        h_in = torch.from_numpy(np.ascontiguousarray(mc)).pin_memory().numpy()
+    if form in ("k5", "mhd"):  # the hydrogen fluids / MHD extra rows are step inputs and outputs too
+        h_in = torch.from_numpy(np.ascontiguousarray(mc if form == "k5" else mc[1])).pin_memory().numpy()
+        h_out = torch.empty(h_in.shape, dtype=torch.float64).pin_memory().numpy()
         e2e_bytes += int(h_in.nbytes)
     e2e_steps = max(3, min(args.steps, 20))
     S.synchronize()
@@ -474,10 +530,14 @@ def main():
         S.set_par(0, host_in)
         if form == "k5":
             S.set_hydrogen(0, h_in)
+        elif form == "mhd":
+            S.set_mhd(0, h_in)
         S.step_async(fcode, 1)
         S.par(1, out=host_out)
         if form == "k5":
             S.hydrogen(1)
+        elif form == "mhd":
+            h_out[:] = S.mhd(1)
     e2e_s = max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{device}")
     e2e_value = whole_job_rate(counted * e2e_steps, world, e2e_s)
 
@@ -505,12 +565,12 @@ def main():
         "clocks": clocks,
     }
     if args.precision == "fp32flux" and rank == 0:
-        line["fp32_flux_errors"] = fp32_flux_errors(mesh, params, st0, mc, fcode, device)
+        line["fp32_flux_errors"] = fp32_flux_errors(mesh, params, st0, mc, fcode, device, form=form)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             rate, steps, threads, el = cpu_reference_rate(mesh, params, st0, mc, counted, form)
-            line["cpu_baseline"] = {"value": rate, "unit": "cell-updates/s", "cores": threads, "kind": "reference",
-                                    "sample": f"{steps} steps of the reference step on the full grid ({el:.1f} s)"}
+            line["cpu_baseline"] = {"value": rate, "unit": "cell-updates/s", "cores": threads, "kind": cpu_kind,
+                                    "sample": f"{steps} steps of {cpu_what} on the full grid ({el:.1f} s)"}
         except Exception as e:  # the reference library must be prebuilt
             line["cpu_baseline"] = {"value": None, "unit": "cell-updates/s", "cores": 0, "kind": "reference",
                                     "sample": f"unavailable: {e}"}

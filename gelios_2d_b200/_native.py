@@ -28,6 +28,7 @@ FORM_STATIONARY = 0
 FORM_MK2 = 1
 FORM_INNER_MK2 = 2
 FORM_5_KOMPONENT = 3
+FORM_MHD_PUI = 4
 PREC_FP64 = 0
 PREC_FP32_FLUX = 1
 
@@ -49,6 +50,16 @@ class GeliosParams(C.Structure):
         for k, v in over.items():
             setattr(p, k, v)
         return p
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class GeliosMhdParams(C.Structure):
+    """gelios_mhd_params: boundary data of the MHD + pickup-proton form."""
+
+    _fields_ = [(n, C.c_double) for n in ("lism_bx", "lism_by", "lism_bz", "inner_bphi", "pui_in_ro", "pui_in_p",
+                                          "pui_inner_ro", "pui_inner_p")]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -137,6 +148,10 @@ def lib() -> C.CDLL:
     L.gelios_upload_hydrogen.argtypes = [vp, C.c_int, dp]
     L.gelios_download_hydrogen.argtypes = [vp, C.c_int, dp]
     L.gelios_upload_mc.argtypes = [vp] + [dp] * 7
+    L.gelios_set_mhd_params.argtypes = [vp, C.POINTER(GeliosMhdParams)]
+    L.gelios_upload_mhd.argtypes = [vp, C.c_int, dp]
+    L.gelios_download_mhd.argtypes = [vp, C.c_int, dp]
+    L.gelios_upload_sources.argtypes = [vp, dp, dp, dp]
     L.gelios_set_inner_cells.argtypes = [vp, C.POINTER(C.c_int32), C.c_int32]
     L.gelios_step.argtypes = [vp, C.c_int, C.c_int, C.POINTER(GeliosStatus)]
     L.gelios_download_points.argtypes = [vp, dp, dp]

@@ -99,7 +99,12 @@ struct gelios_ctx {
     DBuf Hn, Hu, Hv, HT, ku, kv, kT, r_istoch, cback, cnext;
     // state par[2] x 5 fields, centroids [2], scratch
     DBuf state[2];
-    DBuf hstate[2];  // hydrogen fluids H1..H4 (16 rows) of par[0/1], Go_5_komponent form
+    // extra rows of par[0/1]: hydrogen fluids H1..H4 (16 rows, Go_5_komponent
+    // form) or the MHD form's w, B and pickup protons (8 rows)
+    DBuf hstate[2];
+    gelios_mhd_params mprm{};
+    DBuf src_fixed;  // MHD form: fixed charge-exchange sources (3 rows)
+    DBuf flux_mhd;   // MHD form: 13 flux rows per face slot, allocated on first use
     DBuf cen[2];
     DBuf words;    // T[2] (double), dt_acc (u64), counters[2] (u64), status (int)
     DBuf surface;  // Move_surface per-face speeds
@@ -733,6 +738,47 @@ extern "C" int gelios_download_state(gelios_ctx* ctx, int buf, double* ro, doubl
     return GELIOS_OK;
 }
 
+extern "C" int gelios_set_mhd_params(gelios_ctx* ctx, const gelios_mhd_params* mp) {
+    if (!ctx || !mp) return GELIOS_E_ARG;
+    ctx->mprm = *mp;
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_upload_mhd(gelios_ctx* ctx, int buf, const double* rows8) {
+    if (!ctx || buf < 0 || buf > 1 || !rows8) return GELIOS_E_ARG;
+    if (!ctx->have_mesh) return GELIOS_E_STATE;
+    GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
+    const size_t n = sizeof(double) * 8 * ctx->d.n_cells;
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(ctx->hstate[buf].p, rows8, n, cudaMemcpyHostToDevice, ctx->stream));
+    GELIOS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_download_mhd(gelios_ctx* ctx, int buf, double* rows8) {
+    if (!ctx || buf < 0 || buf > 1 || !rows8) return GELIOS_E_ARG;
+    if (!ctx->have_mesh) return GELIOS_E_STATE;
+    GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
+    const size_t n = sizeof(double) * 8 * ctx->d.n_cells;
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(rows8, ctx->hstate[buf].p, n, cudaMemcpyDeviceToHost, ctx->stream));
+    GELIOS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_upload_sources(gelios_ctx* ctx, const double* q1, const double* q2, const double* q3) {
+    if (!ctx || !q1 || !q2 || !q3) return GELIOS_E_ARG;
+    if (!ctx->have_mesh) return GELIOS_E_STATE;
+    GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
+    const size_t nc = ctx->d.n_cells;
+    if (ctx->src_fixed.bytes != 3 * nc * sizeof(double) && ctx->src_fixed.alloc(3 * nc * sizeof(double)))
+        return GELIOS_E_CUDA;
+    const double* q[3] = {q1, q2, q3};
+    for (int k = 0; k < 3; k++)
+        GELIOS_CUDA_TRY(cudaMemcpyAsync(ctx->src_fixed.as<double>() + k * nc, q[k], nc * sizeof(double),
+                                        cudaMemcpyHostToDevice, ctx->stream));
+    GELIOS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return GELIOS_OK;
+}
+
 extern "C" int gelios_upload_hydrogen(gelios_ctx* ctx, int buf, const double* rows16) {
     if (!ctx || buf < 0 || buf > 1 || !rows16) return GELIOS_E_ARG;
     if (!ctx->have_mesh) return GELIOS_E_STATE;
@@ -882,7 +928,7 @@ int step_mk2(gelios_ctx* ctx, const StepBuffers& b) {
 extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status* status) {
     if (!ctx || nsteps < 0) return GELIOS_E_ARG;
     if (form != GELIOS_FORM_STATIONARY && form != GELIOS_FORM_MK2 && form != GELIOS_FORM_INNER_MK2 &&
-        form != GELIOS_FORM_5_KOMPONENT) {
+        form != GELIOS_FORM_5_KOMPONENT && form != GELIOS_FORM_MHD_PUI) {
         set_error("gelios_step: unknown form");
         return GELIOS_E_ARG;
     }
@@ -891,7 +937,8 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
         return GELIOS_E_STATE;
     }
     const DevMesh& d = ctx->d;
-    const bool moving = form == GELIOS_FORM_MK2 || form == GELIOS_FORM_5_KOMPONENT;
+    const bool mhd = form == GELIOS_FORM_MHD_PUI;
+    const bool moving = form == GELIOS_FORM_MK2 || form == GELIOS_FORM_5_KOMPONENT || mhd;
     if (moving && (d.n_rail_a + d.n_rail_b + d.n_rail_c + d.n_rail_d == 0 || d.n_lc == 0)) {
         set_error("gelios_step: the moving-grid form needs rails and tracked lines");
         return GELIOS_E_MESH;
@@ -916,7 +963,16 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
     double* cen1 = ctx->cen[1].as<double>();
     if (ctx->ev_used > 4096) ctx->collect();
     const size_t ncz = d.n_cells;
-    if (!ctx->cen_valid || (form != GELIOS_FORM_MK2 && ctx->cen_rp_partial)) {
+    if (mhd) {
+        if (ctx->src_fixed.bytes != 3 * ncz * sizeof(double)) {
+            set_error("gelios_step: the MHD form needs gelios_upload_sources");
+            return GELIOS_E_STATE;
+        }
+        const size_t fb = static_cast<size_t>(kMhdFluxRows) * d.n_slots * sizeof(double);
+        if (ctx->flux_mhd.bytes != fb && ctx->flux_mhd.alloc(fb)) return GELIOS_E_CUDA;
+    }
+    const bool cached_form = form == GELIOS_FORM_MK2 || mhd;  // forms that refill the cache partially
+    if (!ctx->cen_valid || (!cached_form && ctx->cen_rp_partial)) {
         cudaEvent_t e0 = ctx->phase_begin();
         launch_centroid(d, d.X, d.Y, cen0, cen0 + ncz, cen0 + 2 * ncz, P.gamma, s, cen0 + 3 * ncz, cen0 + 4 * ncz);
         ctx->phase_end(0, e0, 1);
@@ -935,7 +991,36 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
         b.dt_acc = ctx->acc();
         b.counters = ctx->counters();
         b.status = ctx->status();
-        if (form == GELIOS_FORM_MK2) {
+        if (mhd) {
+            // moving-grid step of the MHD form on the main stream:
+            // Move_surface + rails, face units, cell update, x = x2
+            double* cc = (st & 1) ? cen1 : cen0;
+            double* cn = (st & 1) ? cen0 : cen1;
+            b.cx = cc;
+            b.cy = cc + ncz;
+            b.rp = cc + 2 * ncz;
+            b.vs = cc + 3 * ncz;
+            b.vol = cc + 4 * ncz;
+            b.cx_next = cn;
+            b.cy_next = cn + ncz;
+            b.rp_next = cn + 2 * ncz;
+            b.vs_next = cn + 3 * ncz;
+            b.vol_next = cn + 4 * ncz;
+            cudaEvent_t e1 = ctx->phase_begin();
+            const int nm = launch_motion(d, P, b, ctx->surface.as<double>(), s);
+            ctx->phase_end(2, e1, nm);
+            cudaEvent_t e3 = ctx->phase_begin();
+            launch_mhd_faces(d, P, ctx->mprm, b, ctx->hstate[cur].as<double>(), ctx->flux_mhd.as<double>(), s);
+            ctx->phase_end(1, e3, 1);
+            cudaEvent_t e5 = ctx->phase_begin();
+            launch_mhd_update(d, P, b, ctx->flux_mhd.as<double>(), ctx->src_fixed.as<double>(),
+                              ctx->hstate[cur].as<double>(), ctx->hstate[nxt].as<double>(), s);
+            ctx->phase_end(3, e5, 1);
+            cudaEvent_t e4 = ctx->phase_begin();
+            launch_commit(d, b, s);
+            ctx->phase_end(4, e4, 1);
+            launches += nm + 3;
+        } else if (form == GELIOS_FORM_MK2) {
             double* cc = (st & 1) ? cen1 : cen0;
             double* cn = (st & 1) ? cen0 : cen1;
             b.cx = cc;
@@ -1000,11 +1085,11 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
     ctx->launches = launches;
     // centroids of the current points: after an odd number of moving-grid
     // steps they sit in the second buffer; swap so cen[0] holds them
-    if (form == GELIOS_FORM_MK2 && (nsteps & 1)) std::swap(ctx->cen[0].p, ctx->cen[1].p);
+    if (cached_form && (nsteps & 1)) std::swap(ctx->cen[0].p, ctx->cen[1].p);
     // the five-fluid form leaves the centroids of the points before its
     // last motion in cen[0]
     ctx->cen_valid = !(form == GELIOS_FORM_5_KOMPONENT && nsteps > 0);
-    if (form == GELIOS_FORM_MK2 && nsteps > 0) ctx->cen_rp_partial = true;
+    if (cached_form && nsteps > 0) ctx->cen_rp_partial = true;
     if (status) {
         Words r{};
         GELIOS_CUDA_TRY(cudaMemcpyAsync(&r, ctx->words.p, sizeof(r), cudaMemcpyDeviceToHost, s));

@@ -571,8 +571,15 @@ __device__ __forceinline__ double spi4_dev() { return sqrt(4.0 * kPi); }
 // flux, metod 3: HLLD.  Pout[8] = mass, momentum x3, B flux x3, energy (the
 // reference's final reordering), *PQ = flux of Q.  Returns kurant*rad/max|S|.
 // Other metods leave Pout and *PQ untouched, as the reference does.
-__device__ inline double hlldq_korolkov(double ga, double kurant, const double* L, const double* R, double n1,
-                                        double n2, double n3, double rad, int metod, double* Pout, double* PQ) {
+//
+// MOVING = true (metod 3 only) samples the HLLD fan at the face speed W
+// instead of at 0 and returns the flux through the moving face, F - W U of
+// the region that contains W, the way HLLC_2d_Korolkov_b_s treats moving
+// faces (Setka.cpp:10604-10699); the normal-field term becomes
+// -SN (bn2 - bn1) - W bn.  With MOVING = false the code is the reference's.
+template <bool MOVING>
+__device__ inline double hlldq_impl(double ga, double kurant, const double* L, const double* R, double n1, double n2,
+                                    double n3, double rad, int metod, double* Pout, double* PQ, double W) {
     const double spi4 = spi4_dev();
     const double g1 = ga - 1.0;
     const double ro_L = L[0], Q_L = L[1], p_L = L[2], v1_L = L[3], v2_L = L[4], v3_L = L[5];
@@ -735,22 +742,36 @@ __device__ inline double hlldq_korolkov(double ga, double kurant, const double* 
         const double ULLL[9] = {ro_LL, ro_LL * SM, ro_LL * vLLL, ro_LL * wLLL, eLLL, bn, bttt, bmmm, Q_LL};
         const double URRR[9] = {ro_RR, ro_RR * SM, ro_RR * vLLL, ro_RR * wLLL, eRRR, bn, bttt, bmmm, Q_RR};
         for (int i = 0; i < 9; i++) PO[i] = 0.0;
-        if (SL >= 0.0) {
+        const double Ws = MOVING ? W : 0.0;
+        if (SL >= Ws) {
             for (int i = 0; i < 9; i++) PO[i] = FL[i];
-        } else if (SL < 0.0 && SLL >= 0.0) {
+            if (MOVING)
+                for (int i = 0; i < 9; i++) PO[i] -= W * UL[i];
+        } else if (SL < Ws && SLL >= Ws) {
             for (int i = 0; i < 9; i++) PO[i] = FL[i] + SL * ULL[i] - SL * UL[i];
-        } else if (SLL <= 0.0 && SM >= 0.0) {
+            if (MOVING)
+                for (int i = 0; i < 9; i++) PO[i] -= W * ULL[i];
+        } else if (SLL <= Ws && SM >= Ws) {
             for (int i = 0; i < 9; i++) PO[i] = FL[i] + SLL * ULLL[i] - (SLL - SL) * ULL[i] - SL * UL[i];
-        } else if (SM < 0.0 && SRR > 0.0) {
+            if (MOVING)
+                for (int i = 0; i < 9; i++) PO[i] -= W * ULLL[i];
+        } else if (SM < Ws && SRR > Ws) {
             for (int i = 0; i < 9; i++) PO[i] = FR[i] + SRR * URRR[i] - (SRR - SR) * URR[i] - SR * UR[i];
-        } else if (SR > 0.0 && SRR <= 0.0) {
+            if (MOVING)
+                for (int i = 0; i < 9; i++) PO[i] -= W * URRR[i];
+        } else if (SR > Ws && SRR <= Ws) {
             for (int i = 0; i < 9; i++) PO[i] = FR[i] + SR * URR[i] - SR * UR[i];
-        } else if (SR <= 0.0) {
+            if (MOVING)
+                for (int i = 0; i < 9; i++) PO[i] -= W * URR[i];
+        } else if (SR <= Ws) {
             for (int i = 0; i < 9; i++) PO[i] = FR[i];
+            if (MOVING)
+                for (int i = 0; i < 9; i++) PO[i] -= W * UR[i];
         }
     }
     const double SN = dmax_ref(fabs(SL), fabs(SR));
     PO[5] = -SN * (bn2 - bn1);
+    if (MOVING) PO[5] -= W * bn;
     // back to (x, y, z), then the reference's reordering: B fluxes before energy
     Pout[0] = PO[0];
     Pout[1] = n1 * PO[1] + t1 * PO[2] + m1 * PO[3];
@@ -762,6 +783,10 @@ __device__ inline double hlldq_korolkov(double ga, double kurant, const double* 
     Pout[7] = PO[4];
     *PQ = PO[8];
     return time;
+}
+__device__ inline double hlldq_korolkov(double ga, double kurant, const double* L, const double* R, double n1,
+                                        double n2, double n3, double rad, int metod, double* Pout, double* PQ) {
+    return hlldq_impl<false>(ga, kurant, L, R, n1, n2, n3, rad, metod, Pout, PQ, 0.0);
 }
 
 // Solvers::HLLD_Solver_Alexashov (Solvers.cpp:92-691).  q = (ro, p, u, v, w,

@@ -2276,6 +2276,378 @@ __global__ void __launch_bounds__(128) k5_cell_kernel(DevMesh d, gelios_params P
     block_reduce_commit(tmin, nro, npc, status, b.dt_acc, b.counters, b.status);
 }
 
+// ------------------------------------------------------------------ MHD + pickup protons
+// GELIOS_FORM_MHD_PUI (no reference step).  The ion fluid's gas-dynamic
+// rows (ro, p, u, v, Q) are the state rows of the moving-grid step, so
+// surface tracking and the rails run on them unchanged; the extra rows hold
+// the ion's w (u_phi) and B (x, y, phi) and the pickup protons' ro, p, u, v.
+enum : int { kXw = 0, kXbx, kXby, kXbz, kXro, kXp, kXu, kXv, kMhdExtra };
+constexpr int kMhdFlux = 13;  // per slot: ion mass, mom x, y, phi, energy, Bx, By, Bphi, Q; pickup mass, mom x, y, energy
+
+struct Ext8 {
+    double f[kMhdExtra];
+};
+
+__device__ __forceinline__ Ext8 load_ext(const double* __restrict__ hs, size_t nc, int c) {
+    Ext8 e;
+#pragma unroll
+    for (int k = 0; k < kMhdExtra; k++) e.f[k] = hs[k * nc + c];
+    return e;
+}
+// mirror image across the axis: radial and azimuthal components change sign
+__device__ __forceinline__ void mirror_ext(Ext8& e) {
+    e.f[kXw] = -e.f[kXw];
+    e.f[kXby] = -e.f[kXby];
+    e.f[kXbz] = -e.f[kXbz];
+    e.f[kXv] = -e.f[kXv];
+}
+
+// Gran::Get_par's boundary rules (Gran.cpp:205-289) applied to the extra
+// rows; `ion` is the ion state the same rule gave (inner sphere: the wind).
+__device__ __forceinline__ Ext8 get_par_ext(const gelios_params& P, const gelios_mhd_params& M, int ft,
+                                            const Ext8& own, const double* __restrict__ hs, size_t nc, int nb,
+                                            double fx, double fy, const St5& ion) {
+    Ext8 e = own;
+    if (ft == G_USUALY) {
+        e = load_ext(hs, nc, nb);
+    } else if (ft == G_EXTERN) {
+        if (e.f[kXu] >= 0.0) e.f[kXu] = P.extern_u_par;
+    } else if (ft == G_AXIS) {
+        mirror_ext(e);
+    } else if (ft == G_INNER_SPHERE) {
+        const double dist = sqrt(fx * fx + fy * fy);
+        e.f[kXw] = 0.0;
+        e.f[kXbx] = 0.0;
+        e.f[kXby] = 0.0;
+        e.f[kXbz] = M.inner_bphi * (P.R1 / dist) * (fy / dist);
+        e.f[kXro] = M.pui_inner_ro * ion.ro;
+        e.f[kXp] = M.pui_inner_p * ion.p;
+        e.f[kXu] = ion.u;
+        e.f[kXv] = ion.v;
+    } else if (ft == G_INPUT) {
+        e.f[kXw] = 0.0;
+        e.f[kXbx] = M.lism_bx;
+        e.f[kXby] = M.lism_by;
+        e.f[kXbz] = M.lism_bz;
+        e.f[kXro] = M.pui_in_ro;
+        e.f[kXp] = M.pui_in_p;
+        e.f[kXu] = P.in_u;
+        e.f[kXv] = P.in_v;
+    }
+    return e;
+}
+
+// Reconstruction of the extra rows at a Usualy face seen from M (values Me,
+// centre Mx,My; neighbour So, Sosed_down Sd): the minmod rule of
+// Gran::Get_par_TVD (Gran.cpp:292-473) with its stencil, two points on
+// tracked faces, first order without a Sosed_down; non-positive pickup
+// density or pressure fall back to M's value.
+__device__ Ext8 tvd_ext(const double* __restrict__ hs, size_t nc, const double* cx, const double* cy, double fx,
+                        double fy, const Ext8& Me, double Mx, double My, int So, int Sd, bool tracked) {
+    if (Sd < 0) return Me;
+    const Ext8 e1 = load_ext(hs, nc, Sd);
+    const double dist2 = sqrt(sq(fx - Mx) + sq(fy - My));
+    const double dist1 = sqrt(sq(fx - cx[Sd]) + sq(fy - cy[Sd]));
+    const double r12 = 1.0 / (-dist1 - (-dist2)), x2 = -dist2;
+    Ext8 o;
+    if (tracked) {
+#pragma unroll
+        for (int k = 0; k < kMhdExtra; k++) o.f[k] = (e1.f[k] - Me.f[k]) * r12 * (0.0 - x2) + Me.f[k];
+    } else {
+        const Ext8 e3 = load_ext(hs, nc, So);
+        const double dist3 = sqrt(sq(fx - cx[So]) + sq(fy - cy[So]));
+        const double r23 = 1.0 / (-dist2 - dist3);
+#pragma unroll
+        for (int k = 0; k < kMhdExtra; k++) o.f[k] = linear3r(e1.f[k], Me.f[k], e3.f[k], r12, r23, x2);
+    }
+    if (!(o.f[kXro] > 0.0)) o.f[kXro] = Me.f[kXro];
+    if (!(o.f[kXp] > 0.0)) o.f[kXp] = Me.f[kXp];
+    return o;
+}
+
+// Ion MHD flux through a face with unit normal (n1, n2) moving with normal
+// speed W: both states go to the face frame (normal n, tangent t = (-n2,
+// n1), phi), Solvers::HLLDQ_Korolkov's HLLD (metod 3) solves along the
+// frame's x axis with its fan sampled at W (hlldq_impl<true>: F - W U of
+// the region containing W, as HLLC_2d_Korolkov_b_s does for moving faces),
+// and the momentum and field fluxes go back to (x, y).  out: mass, mom x,
+// mom y, mom phi, energy, Bx, By, Bphi, Q.  Returns 1 / max(|SL|, |SR|).
+__device__ __forceinline__ double mhd_face_flux(double ga, const St5& iL, const Ext8& eL, const St5& iR,
+                                                const Ext8& eR, double n1, double n2, double W, double* out) {
+    const double t1 = -n2, t2 = n1;
+    double L[9], R[9];
+    L[0] = iL.ro;
+    L[1] = iL.Q;
+    L[2] = iL.p;
+    L[3] = iL.u * n1 + iL.v * n2;
+    L[4] = iL.u * t1 + iL.v * t2;
+    L[5] = eL.f[kXw];
+    L[6] = eL.f[kXbx] * n1 + eL.f[kXby] * n2;
+    L[7] = eL.f[kXbx] * t1 + eL.f[kXby] * t2;
+    L[8] = eL.f[kXbz];
+    R[0] = iR.ro;
+    R[1] = iR.Q;
+    R[2] = iR.p;
+    R[3] = iR.u * n1 + iR.v * n2;
+    R[4] = iR.u * t1 + iR.v * t2;
+    R[5] = eR.f[kXw];
+    R[6] = eR.f[kXbx] * n1 + eR.f[kXby] * n2;
+    R[7] = eR.f[kXbx] * t1 + eR.f[kXby] * t2;
+    R[8] = eR.f[kXbz];
+    double F[8], FQ;
+    const double tinv = hlldq_impl<true>(ga, 1.0, L, R, 1.0, 0.0, 0.0, 1.0, 3, F, &FQ, W);
+    out[0] = F[0];
+    out[1] = n1 * F[1] + t1 * F[2];
+    out[2] = n2 * F[1] + t2 * F[2];
+    out[3] = F[3];
+    out[4] = F[7];
+    out[5] = n1 * F[4] + t1 * F[5];
+    out[6] = n2 * F[4] + t2 * F[5];
+    out[7] = F[6];
+    out[8] = FQ;
+    return tinv;
+}
+
+// One face unit of the MHD form, after the motion: reconstructions of both
+// sides (ion rows: the moving-grid rules of Setka.cpp:10204-10276, extra
+// rows: tvd_ext / get_par_ext) on the pre-motion points, face speed from
+// the moved points, HLLD for the ions and HLLC for the pickup protons,
+// 13 flux rows times S to the owner slot and their negatives to the twin,
+// CFL candidates of both fluids.
+template <typename TF>
+__global__ void __launch_bounds__(128) mhd_face_kernel(DevMesh d, gelios_params P, gelios_mhd_params M,
+                                                       StepBuffers b, const double* __restrict__ hs,
+                                                       double* __restrict__ fl) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    double tmin_u = __longlong_as_double(0x7ff0000000000000LL);
+    int status = 0;
+    if (u < d.n_units) {
+        const size_t nc = d.n_cells, ng = d.n_slots;
+        const int K = d.u_cell[u], nb = d.u_nb[u];
+        const uint32_t info = d.u_info[u];
+        const double x = b.cx[K], y = b.cy[K];
+        const bool procK = !(sqrt(sq(x) + sq(y)) < P.R11);
+        double x3 = 0.0, y3 = 0.0;
+        bool procN = false;
+        if (nb >= 0) {
+            x3 = b.cx[nb];
+            y3 = b.cy[nb];
+            procN = !(sqrt(sq(x3) + sq(y3)) < P.R11);
+        }
+        if (procK || procN) {
+            const int A = d.u_A[u], B = d.u_B[u];
+            const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
+            const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
+            double t1 = xb - xa, t2 = yb - ya;
+            const double nn = sqrt(sq(t1) + sq(t2));
+            t1 = t1 / nn;
+            t2 = t2 / nn;
+            const double n1 = t2, n2 = -t1;
+            const double S = nn * (ya + yb) * 0.5;
+            const double x4 = (d.X2[A] + d.X2[B]) / 2.0, y4 = (d.Y2[A] + d.Y2[B]) / 2.0;
+            const double dt = *b.dt_cur;
+            const double W = ((x4 - x2) * n1 + (y4 - y2) * n2) / dt;
+            const int ft = info & SI_TYPE_MASK;
+            const uint32_t cf = (info >> UI_CF_OWN) & 15u, nbf = (info >> UI_CF_NB) & 15u;
+            const double g2 = 2 * P.gamma;
+            const St5 par1 = load_state(b.cur, K);
+            const Ext8 ex1 = load_ext(hs, nc, K);
+            St5 par11 = par1, par2 = get_par(P, ft, par1, b.cur, nb, x2, y2);
+            Ext8 e11 = ex1, e2 = get_par_ext(P, M, ft, ex1, hs, nc, nb, x2, y2, par2);
+            const double dis = sqrt(sq(x2) + sq(y2));
+            const bool tracked = (info & SI_GOD) != 0;
+            const bool radial = ((cf & CF_C1) && (ft == G_USUALY || ft == G_AXIS)) || ft == G_INNER_SPHERE ||
+                                (ft == G_USUALY && (nbf & CF_C1));
+            const double pdis = radial ? pow2g(dis, g2) : 1.0;
+            if (ft == G_USUALY) {
+                par11 = mk2_usualy_side(b.cur, b.cx, b.cy, b.rp, x2, y2, dis, pdis, par1, x, y, b.rp[K], cf, nb,
+                                        d.u_sd[u], tracked, &status);
+                par2 = mk2_usualy_side(b.cur, b.cx, b.cy, b.rp, x2, y2, dis, pdis, par2, x3, y3, b.rp[nb], nbf, K,
+                                       d.u_sd2[u], tracked, &status);
+                if (!(cf & CF_C1))
+                    e11 = tvd_ext(hs, nc, b.cx, b.cy, x2, y2, ex1, x, y, nb, d.u_sd[u], tracked);
+                if (!(nbf & CF_C1))
+                    e2 = tvd_ext(hs, nc, b.cx, b.cy, x2, y2, e2, x3, y3, K, d.u_sd2[u], tracked);
+            } else if (ft == G_INNER_SPHERE) {
+                const double radius = sqrt(sq(x) + sq(y));
+                par11.ro = par11.ro * sq(radius) / sq(dis);
+                par11.Q = par11.Q * sq(radius) / sq(dis);
+                par11.p = par11.p * (b.rp[K] / pdis);
+            } else if (ft == G_AXIS) {
+                if (cf & CF_C1) {
+                    const double radius = sqrt(sq(x) + sq(y));
+                    par11.ro = par11.ro * sq(radius) / sq(dis);
+                    par11.Q = par11.Q * sq(radius) / sq(dis);
+                    par11.p = par11.p * (b.rp[K] / pdis);
+                    polar_perenos(x, y, x2, y2, par11.u, par11.v);
+                } else {
+                    par11 = tvd_axis(b.cur, b.cx, b.cy, x2, y2, par1, x, y, d.u_sd[u]);
+                }
+                par2 = par11;
+                par2.v = -par2.v;
+            }
+            double F[kMhdFlux];
+            const double tI = mhd_face_flux(P.gamma, par11, e11, par2, e2, n1, n2, W, F);
+            St5 pL, pR;
+            pL.ro = e11.f[kXro];
+            pL.p = e11.f[kXp];
+            pL.u = e11.f[kXu];
+            pL.v = e11.f[kXv];
+            pL.Q = 0.0;
+            pR.ro = e2.f[kXro];
+            pR.p = e2.f[kXp];
+            pR.u = e2.f[kXu];
+            pR.v = e2.f[kXv];
+            pR.Q = 0.0;
+            FluxOut<double> G;
+            const double UUp = hllc_flux<TF>(P.gamma, P.kurant, pL, pR, W, n1, n2, 1.0, 1, false, G);
+            F[9] = G.P0;
+            F[10] = G.P1;
+            F[11] = G.P2;
+            F[12] = G.P3;
+            const int g = d.u_slot[u], gt = d.u_twin[u];
+#pragma unroll
+            for (int k = 0; k < kMhdFlux; k++) fl[k * ng + g] = F[k] * S;
+            if (gt >= 0) {
+#pragma unroll
+                for (int k = 0; k < kMhdFlux; k++) fl[k * ng + gt] = -(F[k] * S);
+            }
+            if (procK) {
+                const double dist = sqrt(sq(x - x2) + sq(y - y2));
+                tmin_u = dmin_ref(tmin_u, P.kurant * dist * tI);
+                tmin_u = dmin_ref(tmin_u, P.kurant * dist / UUp);
+            }
+            if (gt >= 0 && procN) {
+                const double distn = sqrt(sq(x3 - x2) + sq(y3 - y2));
+                tmin_u = dmin_ref(tmin_u, P.kurant * distn * tI);
+                tmin_u = dmin_ref(tmin_u, P.kurant * distn / UUp);
+            }
+        }
+    }
+    block_reduce_commit(tmin_u, 0, 0, status, b.dt_acc, b.counters, b.status);
+}
+
+// Cell update of the MHD form: the MK2 update (Setka.cpp:10386-10468) for
+// both fluids with their axisymmetric terms (area-weighted like the
+// reference's p (vs1 + vs2)/2) and the fixed charge-exchange sources of the
+// ion momentum and energy; refills the geometry cache like mk2_update_kernel.
+__global__ void __launch_bounds__(128) mhd_update_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                         const double* __restrict__ fl,
+                                                         const double* __restrict__ src,
+                                                         const double* __restrict__ hcur, double* __restrict__ hnxt) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double tmark = __longlong_as_double(0x7ff0000000000000LL);
+    int nro = 0, npc = 0;
+    const size_t ng = d.n_slots, nc = d.n_cells;
+    if (c < d.n_cells) {
+        const int s0 = d.cstart[c], n = d.cstart[c + 1] - s0;
+        const int32_t* con = d.contour + s0;
+        double xn, yn;
+        centroid(con, n, d.X2, d.Y2, xn, yn);
+        b.cx_next[c] = xn;
+        b.cy_next[c] = yn;
+        const uint32_t cfl = d.cflags[c];
+        if (cfl & CF_RP) b.rp_next[c] = pow2g(sqrt(sq(xn) + sq(yn)), 2 * P.gamma);
+        const double x = b.cx[c], y = b.cy[c];
+        double vs2 = 0.0, Volume2 = 0.0;
+        if (!(cfl & CF_CENTR)) {
+            vs2 = area(con, n, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X2, d.Y2, true);
+            Volume2 = volume_rotate(con, n, d.X2, d.Y2);
+            b.vs_next[c] = n == 4 ? vs2 : area(con, n, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X2, d.Y2, false);
+            b.vol_next[c] = Volume2;
+        }
+        if (!(sqrt(sq(x) + sq(y)) < P.R11)) {
+            tmark = 10000000.0;
+            const St5 par1 = load_state(b.cur, c);
+            const Ext8 e = load_ext(hcur, nc, c);
+            if (!(cfl & CF_CENTR)) {
+                const double dt = *b.dt_cur;
+                const int g0 = d.gstart[c], g1 = d.gstart[c + 1];
+                double Pt[kMhdFlux];
+#pragma unroll
+                for (int k = 0; k < kMhdFlux; k++) Pt[k] = 0.0;
+                for (int g = g0; g < g1; g++) {
+#pragma unroll
+                    for (int k = 0; k < kMhdFlux; k++) Pt[k] = Pt[k] + fl[k * ng + g];
+                }
+                const double q1 = src[c], q2 = src[nc + c], q3 = src[2 * nc + c];
+                const double vs1 = b.vs[c], Volume = b.vol[c];
+                const double gm1 = P.gamma - 1;
+                const double rV2 = 1.0 / Volume2, VV = Volume * rV2;
+                const double Am = 0.5 * (vs1 + vs2);
+                const double i4p = 1.0 / (4.0 * kPi), i8p = 1.0 / (8.0 * kPi);
+                // ions
+                const double ro = par1.ro, p = par1.p, u = par1.u, v = par1.v, Q = par1.Q;
+                const double w = e.f[kXw], bx = e.f[kXbx], by = e.f[kXby], bz = e.f[kXbz];
+                const double bb = bx * bx + by * by + bz * bz;
+                const double Sy = p + bb * i8p + ro * w * w - bz * bz * i4p;
+                const double Sphi = -(ro * v * w - by * bz * i4p);
+                const double Sbz = v * bz - w * by;
+                double ro3 = ro * VV - dt * (Pt[0] * rV2);
+                const double Q3 = Q * VV - (dt * rV2) * Pt[8];
+                if (ro3 <= 0.0) {
+                    ro3 = P.ro_floor;
+                    nro++;
+                }
+                const double rro3 = 1.0 / ro3;
+                const double u3 = (ro * u * VV - dt * (Pt[1] * rV2 - q1)) * rro3;
+                const double v3 = (ro * v * VV - dt * ((Pt[2] - Sy * Am) * rV2 - q2)) * rro3;
+                const double w3 = (ro * w * VV - dt * ((Pt[3] - Sphi * Am) * rV2)) * rro3;
+                const double E = p / gm1 + ro * (u * u + v * v + w * w) * 0.5 + bb * i8p;
+                const double E3 = E * VV - dt * (Pt[4] * rV2 - q3);
+                const double bx3 = bx * VV - dt * (Pt[5] * rV2);
+                const double by3 = by * VV - dt * (Pt[6] * rV2);
+                const double bz3 = bz * VV - dt * ((Pt[7] - Sbz * Am) * rV2);
+                double p3 = (E3 - 0.5 * ro3 * (u3 * u3 + v3 * v3 + w3 * w3) -
+                             (bx3 * bx3 + by3 * by3 + bz3 * bz3) * i8p) *
+                            gm1;
+                if (p3 <= 0) {
+                    p3 = P.p_floor;
+                    npc++;
+                }
+                // pickup protons
+                const double rp = e.f[kXro], pp = e.f[kXp], up = e.f[kXu], vp = e.f[kXv];
+                double rp3 = rp * VV - dt * (Pt[9] * rV2);
+                if (rp3 <= 0.0) {
+                    rp3 = P.ro_floor;
+                    nro++;
+                }
+                const double rrp3 = 1.0 / rp3;
+                const double up3 = (rp * up * VV - dt * (Pt[10] * rV2)) * rrp3;
+                const double vp3 = (rp * vp * VV - dt * ((Pt[11] - pp * Am) * rV2)) * rrp3;
+                const double Ep = pp / gm1 + rp * (up * up + vp * vp) * 0.5;
+                double pp3 = ((Ep * VV - dt * (Pt[12] * rV2)) - 0.5 * rp3 * (up3 * up3 + vp3 * vp3)) * gm1;
+                if (pp3 <= 0) {
+                    pp3 = P.p_floor;
+                    npc++;
+                }
+                b.nxt[0][c] = ro3;
+                b.nxt[1][c] = p3;
+                b.nxt[2][c] = u3;
+                b.nxt[3][c] = v3;
+                b.nxt[4][c] = Q3;
+                hnxt[kXw * nc + c] = w3;
+                hnxt[kXbx * nc + c] = bx3;
+                hnxt[kXby * nc + c] = by3;
+                hnxt[kXbz * nc + c] = bz3;
+                hnxt[kXro * nc + c] = rp3;
+                hnxt[kXp * nc + c] = pp3;
+                hnxt[kXu * nc + c] = up3;
+                hnxt[kXv * nc + c] = vp3;
+            } else {
+                b.nxt[0][c] = par1.ro;
+                b.nxt[1][c] = par1.p;
+                b.nxt[2][c] = par1.u;
+                b.nxt[3][c] = par1.v;
+                b.nxt[4][c] = par1.Q;
+#pragma unroll
+                for (int k = 0; k < kMhdExtra; k++) hnxt[k * nc + c] = e.f[k];
+            }
+        }
+    }
+    block_reduce_commit(tmark, nro, npc, 0, b.dt_acc, b.counters, b.status);
+}
+
 // ------------------------------------------------------------------ launchers
 namespace {
 inline int blocks_for(int n, int t) { return (n + t - 1) / t; }
@@ -2377,6 +2749,18 @@ void launch_hlld_batch(const gelios_params& P, int n, const double* in, double* 
 }
 void launch_godunov_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s) {
     godunov_batch_kernel<<<blocks_for(n, 2), 64, 0, s>>>(P, n, in, out);
+}
+void launch_mhd_faces(const DevMesh& d, const gelios_params& P, const gelios_mhd_params& M, const StepBuffers& b,
+                      const double* hcur, double* fl, cudaStream_t s) {
+    if (d.n_units <= 0) return;
+    if (P.precision == GELIOS_PREC_FP32_FLUX)
+        mhd_face_kernel<float><<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, M, b, hcur, fl);
+    else
+        mhd_face_kernel<double><<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, M, b, hcur, fl);
+}
+void launch_mhd_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
+                       const double* src, const double* hcur, double* hnxt, cudaStream_t s) {
+    mhd_update_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, fl, src, hcur, hnxt);
 }
 
 }  // namespace gelios

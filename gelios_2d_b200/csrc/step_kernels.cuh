@@ -128,6 +128,13 @@ int launch_motion(const DevMesh& d, const gelios_params& P, const StepBuffers& b
 // 16 rows of n_cells each, of the current and the next buffer.
 void launch_k5_cells(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* hcur, double* hnxt,
                      cudaStream_t s);
+// MHD + pickup-proton form: extra rows (8 x n_cells: w, Bx, By, Bz, pickup
+// ro, p, u, v), 13 flux rows per slot, fixed sources (3 x n_cells).
+constexpr int kMhdFluxRows = 13;
+void launch_mhd_faces(const DevMesh& d, const gelios_params& P, const gelios_mhd_params& M, const StepBuffers& b,
+                      const double* hcur, double* fl, cudaStream_t s);
+void launch_mhd_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
+                       const double* src, const double* hcur, double* hnxt, cudaStream_t s);
 void launch_hllc_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s);
 void launch_hlldq_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s);
 void launch_hlld_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s);

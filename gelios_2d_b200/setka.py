@@ -15,6 +15,7 @@ reference (Setka.h)                          here
 ``Go_5_komponent__MK2(int)``                 ``Go_5_komponent__MK2(step)``
 ``Go_stationary_5_komponent_inner_MK2(int)`` ``Go_stationary_5_komponent_inner_MK2(step)``
 ``Go_5_komponent(int)``                      ``Go_5_komponent(step)`` (+ ``set_hydrogen``)
+(no reference step)                          ``Go_MHD_pickup(step)`` (+ ``set_mhd``, ``set_sources``)
 ``Save_Setka_ALL_ALPHA(string)``             ``Save_Setka_ALL_ALPHA(name)``
 ``Download_Setka_ALL_ALPHA_2_0(string)``     ``Setka.Download_Setka_ALL_ALPHA_2_0(name)``
 ==========================================  =====================================
@@ -151,6 +152,38 @@ class Setka:
         four hydrogen fluids (set with :meth:`set_hydrogen`) on the grid
         moved by Move_surface + Move_Setka_Calculate."""
         return self._go(N.FORM_5_KOMPONENT, step)
+
+    def Go_MHD_pickup(self, step: int) -> N.GeliosStatus:
+        """The moving-grid step for an ion MHD fluid and pickup protons
+        (GELIOS_FORM_MHD_PUI; no reference step: same motion as
+        Go_5_komponent__MK2, HLLD ion fluxes of Solvers::HLLDQ_Korolkov in
+        the face frame, HLLC pickup fluxes).  Extra rows via :meth:`set_mhd`,
+        fixed charge-exchange sources via :meth:`set_sources`, boundary data
+        via :meth:`set_mhd_params`."""
+        return self._go(N.FORM_MHD_PUI, step)
+
+    def set_mhd_params(self, mp: "N.GeliosMhdParams"):
+        self.mhd_params = mp
+        N.check(self._L.gelios_set_mhd_params(self._h, C.byref(mp)), "gelios_set_mhd_params")
+
+    def set_mhd(self, buf: int, x8: np.ndarray):
+        """Extra rows of par[buf] for the MHD form: w, Bx, By, Bz of the ions,
+        ro, p, u, v of the pickup protons (shape (8, n_cells))."""
+        x8 = np.ascontiguousarray(x8, np.float64)
+        if x8.shape != (8, self.mesh.n_cells):
+            raise ValueError("MHD extra rows must be (8, n_cells)")
+        N.check(self._L.gelios_upload_mhd(self._h, int(buf), x8.ravel()), "gelios_upload_mhd")
+
+    def mhd(self, buf: int) -> np.ndarray:
+        out = np.zeros(8 * self.mesh.n_cells)
+        N.check(self._L.gelios_download_mhd(self._h, int(buf), out), "gelios_download_mhd")
+        return out.reshape(8, self.mesh.n_cells)
+
+    def set_sources(self, q1, q2, q3):
+        """Fixed charge-exchange sources of the ion x/y momentum and energy
+        (per unit volume, n_cells each) for the MHD form."""
+        f = lambda a: np.ascontiguousarray(a, np.float64).ravel()  # noqa: E731
+        N.check(self._L.gelios_upload_sources(self._h, f(q1), f(q2), f(q3)), "gelios_upload_sources")
 
     def set_hydrogen(self, buf: int, h16: np.ndarray):
         """ro, p, u, v of the hydrogen fluids H1..H4 of Cell::par[buf]

@@ -168,3 +168,55 @@ def hydrogen_fields(mesh: Mesh, seed: int = 31) -> np.ndarray:
         h[4 * k + 2] = -2.54338 * (0.7 + 0.1 * k) * (1.0 + 0.05 * np.cos(th))
         h[4 * k + 3] = 0.1 * np.sin(m * th) * u[16 + k]
     return h
+
+
+# ---------------------------------------------------------------- ion MHD + pickup protons
+def mhd_params(b_lism: float = 0.01, b_angle_deg: float = 30.0, inner_bphi: float = 1.0) -> N.GeliosMhdParams:
+    """Boundary data of the MHD + pickup-proton form: LISM field of magnitude
+    b_lism at b_angle_deg to the inflow (the inflow runs along -x), a toroidal
+    wind field inner_bphi * R1 sin(theta) / r at the inner sphere, pickup
+    protons at 1% of the wind density and 10% of its pressure there and a
+    trace population (1e-3) in the inflow."""
+    a = np.deg2rad(b_angle_deg)
+    mp = N.GeliosMhdParams()
+    mp.lism_bx = -b_lism * np.cos(a)
+    mp.lism_by = b_lism * np.sin(a)
+    mp.lism_bz = 0.0
+    mp.inner_bphi = inner_bphi
+    mp.pui_in_ro = 1e-3
+    mp.pui_in_p = 1e-3
+    mp.pui_inner_ro = 0.01
+    mp.pui_inner_p = 0.1
+    return mp
+
+
+def mhd_initial(mesh: Mesh, st0: np.ndarray, mp: N.GeliosMhdParams) -> np.ndarray:
+    """Extra rows of the MHD form (shape (8, n_cells)) beside the ion state
+    st0: no azimuthal velocity, the uniform LISM field everywhere (divergence
+    free), pickup protons at 1% of the ion density and 10% of its pressure,
+    moving with the ions."""
+    x8 = np.zeros((8, mesh.n_cells))
+    x8[1] = mp.lism_bx
+    x8[2] = mp.lism_by
+    x8[3] = mp.lism_bz
+    x8[4] = 0.01 * st0[0]
+    x8[5] = 0.1 * st0[1]
+    x8[6] = st0[2]
+    x8[7] = st0[3]
+    return x8
+
+
+def mhd_sources(mesh: Mesh, seed: int = 17) -> tuple:
+    """Fixed charge-exchange sources of the ion x momentum, y momentum and
+    energy: A_i exp(-r/200) (1 + 0.1 cos(k_i theta)) with r in AU (r * 390.222
+    in grid units), A_i ~ U(5e-4, 2e-3), k_i in {1, 2, 3}, seeded."""
+    x, y = mesh.centroids()
+    r = np.sqrt(x * x + y * y) * RR_
+    th = np.arctan2(y, x)
+    u = splitmix64(seed, 6)
+    out = []
+    for i in range(3):
+        A = 5e-4 + 1.5e-3 * u[2 * i]
+        k = 1 + int(3 * u[2 * i + 1])
+        out.append(A * np.exp(-r / 200.0) * (1.0 + 0.1 * np.cos(k * th)))
+    return tuple(out)

@@ -47,7 +47,8 @@ enum {
     GELIOS_FORM_STATIONARY = 0, /* Setka::Go_stationary(int)                      Setka.h:177, Setka.cpp:5205-5343  */
     GELIOS_FORM_MK2 = 1,        /* Setka::Go_5_komponent__MK2(int)                Setka.h:186, Setka.cpp:10121-10482 */
     GELIOS_FORM_INNER_MK2 = 2,  /* Setka::Go_stationary_5_komponent_inner_MK2(int) Setka.h:176, Setka.cpp:6999-7212  */
-    GELIOS_FORM_5_KOMPONENT = 3 /* Setka::Go_5_komponent(int): plasma + four hydrogen fluids, Setka.cpp:8269-8950 */
+    GELIOS_FORM_5_KOMPONENT = 3, /* Setka::Go_5_komponent(int): plasma + four hydrogen fluids, Setka.cpp:8269-8950 */
+    GELIOS_FORM_MHD_PUI = 4     /* ion MHD fluid + pickup protons on the moving grid: no reference step (see below) */
 };
 
 /* Riemann-solver precision (geometry, accumulation and the dt reduction stay FP64). */
@@ -202,6 +203,40 @@ int64_t gelios_last_launch_count(gelios_ctx *ctx);
  * reset, and resets when `reset` is non-zero. */
 int gelios_set_phase_timing(gelios_ctx *ctx, int enabled);
 int gelios_phase_times(gelios_ctx *ctx, double *ms, int64_t *launches, int reset);
+
+/* ---- MHD + pickup-proton moving-grid step ---------------------------------
+ * GELIOS_FORM_MHD_PUI has no counterpart among the reference's steps (the
+ * reference steps gas dynamics only; its MHD solvers are never called).  It
+ * is the moving-grid step of GELIOS_FORM_MK2 (same surface tracking and rail
+ * motion, Setka.cpp:3378-3844 and 4324-4759, driven by the ion fluid's
+ * gas-dynamic state) for two fluids:
+ *   - ions, ideal MHD: ro, p, u, v, Q in the state rows of gelios_upload_state
+ *     and w (u_phi), Bx, By, Bz (B_phi) in the extra rows; Gaussian units
+ *     (magnetic pressure B^2/8pi).  Face flux: HLLD of Solvers::HLLDQ_Korolkov
+ *     (Solvers.cpp:1642-2185, metod 3) in the face frame, the states shifted
+ *     by the face speed, transformed back to the moving-face flux F - W U;
+ *   - pickup protons, gas dynamics: ro, p, u, v in the extra rows; face flux
+ *     HLLC of HLLC_2d_Korolkov_b_s (Setka.cpp:10484-10700).
+ * Cell update: the MK2 update (Setka.cpp:10425-10468) extended with the
+ * axisymmetric terms of both fluids (radial momentum p_T + ro w^2 -
+ * B_phi^2/4pi, azimuthal momentum -(ro v w - B_r B_phi/4pi), B_phi (v B_phi -
+ * w B_r)) and the caller's fixed charge-exchange sources of the ion
+ * momentum and energy (gelios_upload_sources).
+ * Extra rows (gelios_upload_mhd): w, Bx, By, Bz, ro_pui, p_pui, u_pui, v_pui,
+ * each n_cells long (8 * n_cells doubles). */
+typedef struct gelios_mhd_params {
+    double lism_bx, lism_by, lism_bz; /* B of the Input boundary state */
+    double inner_bphi;               /* B_phi of the inner-sphere state at r = R1 on the equator (falls as R1 sin(theta)/r) */
+    double pui_in_ro, pui_in_p;      /* pickup protons of the Input boundary state (moving with the inflow) */
+    double pui_inner_ro, pui_inner_p; /* pickup protons of the inner-sphere state, fractions of the wind's ro and p */
+} gelios_mhd_params;
+
+int gelios_set_mhd_params(gelios_ctx *ctx, const gelios_mhd_params *mp);
+int gelios_upload_mhd(gelios_ctx *ctx, int buf, const double *rows8);
+int gelios_download_mhd(gelios_ctx *ctx, int buf, double *rows8);
+/* Fixed charge-exchange sources of the ion fluid per unit volume: x and y
+ * momentum, energy (n_cells each); read by GELIOS_FORM_MHD_PUI. */
+int gelios_upload_sources(gelios_ctx *ctx, const double *q1, const double *q2, const double *q3);
 
 /* ---- per-face solvers on the device (known-answer checks) ------------------
  * Batched HLLC_2d_Korolkov_b_s (Setka.cpp:10484-10700): in[n*16] =

@@ -41,6 +41,8 @@ typedef struct ctx {
     double *hpar[2][16];
     /* MC moments */
     double *Hn, *Hu, *Hv, *HT, *ku, *kv_, *kT;
+    /* fixed charge-exchange sources of the MHD form (ion momentum x, y, energy) */
+    double *qfix[3];
     int32_t *inner;
     int32_t n_inner_cells;
     int64_t status, n_ro_clamp, n_p_clamp, n_tvd_bad;
@@ -1634,6 +1636,7 @@ void *go_create(const go_params *prm, const go_mesh *m) {
     c->kv_ = (double *)dup(NULL, sizeof(double) * nc);
     c->kT = (double *)dup(NULL, sizeof(double) * nc);
     c->inner = (int32_t *)dup(NULL, sizeof(int32_t));
+    for (int q = 0; q < 3; q++) c->qfix[q] = (double *)dup(NULL, sizeof(double) * nc);
     return c;
 }
 
@@ -1656,6 +1659,7 @@ void go_destroy(void *h) {
     for (int b = 0; b < 2; b++)
         for (int q = 0; q < 16; q++) free(c->hpar[b][q]);
     free(c->Hn); free(c->Hu); free(c->Hv); free(c->HT); free(c->ku); free(c->kv_); free(c->kT);
+    for (int q = 0; q < 3; q++) free(c->qfix[q]);
     free(c->inner);
     free(c);
 }
@@ -1743,8 +1747,12 @@ double go_godunov(const go_params *prm, const double *q1, const double *q2, cons
 // flux, metod 3: HLLD.  Pout[8] = mass, momentum x3, B flux x3, energy (the
 // reference's final reordering), *PQ = flux of Q.  Returns kurant*rad/max|S|.
 // Other metods leave Pout and *PQ untouched, as the reference does.
+/* W: face speed at which the HLLD fan (metod 3) is sampled; the flux is then
+ * F - W U of the region containing W (the moving-face treatment of
+ * HLLC_2d_Korolkov_b_s, Setka.cpp:10604-10699).  W = 0 is the reference's
+ * HLLDQ_Korolkov exactly (pinned by the golden vectors). */
 static double hlldq(double ga, double kurant, const double* L, const double* R, double n1,
-                                        double n2, double n3, double rad, int metod, double* Pout, double* PQ) {
+                    double n2, double n3, double rad, int metod, double* Pout, double* PQ, double W) {
     const double spi4 = sqrt(4.0 * PI_);
     const double g1 = ga - 1.0;
     const double ro_L = L[0], Q_L = L[1], p_L = L[2], v1_L = L[3], v2_L = L[4], v3_L = L[5];
@@ -1907,22 +1915,22 @@ static double hlldq(double ga, double kurant, const double* L, const double* R, 
         const double ULLL[9] = {ro_LL, ro_LL * SM, ro_LL * vLLL, ro_LL * wLLL, eLLL, bn, bttt, bmmm, Q_LL};
         const double URRR[9] = {ro_RR, ro_RR * SM, ro_RR * vLLL, ro_RR * wLLL, eRRR, bn, bttt, bmmm, Q_RR};
         for (int i = 0; i < 9; i++) PO[i] = 0.0;
-        if (SL >= 0.0) {
-            for (int i = 0; i < 9; i++) PO[i] = FL[i];
-        } else if (SL < 0.0 && SLL >= 0.0) {
-            for (int i = 0; i < 9; i++) PO[i] = FL[i] + SL * ULL[i] - SL * UL[i];
-        } else if (SLL <= 0.0 && SM >= 0.0) {
-            for (int i = 0; i < 9; i++) PO[i] = FL[i] + SLL * ULLL[i] - (SLL - SL) * ULL[i] - SL * UL[i];
-        } else if (SM < 0.0 && SRR > 0.0) {
-            for (int i = 0; i < 9; i++) PO[i] = FR[i] + SRR * URRR[i] - (SRR - SR) * URR[i] - SR * UR[i];
-        } else if (SR > 0.0 && SRR <= 0.0) {
-            for (int i = 0; i < 9; i++) PO[i] = FR[i] + SR * URR[i] - SR * UR[i];
-        } else if (SR <= 0.0) {
-            for (int i = 0; i < 9; i++) PO[i] = FR[i];
+        if (SL >= W) {
+            for (int i = 0; i < 9; i++) PO[i] = FL[i] - W * UL[i];
+        } else if (SL < W && SLL >= W) {
+            for (int i = 0; i < 9; i++) PO[i] = FL[i] + SL * ULL[i] - SL * UL[i] - W * ULL[i];
+        } else if (SLL <= W && SM >= W) {
+            for (int i = 0; i < 9; i++) PO[i] = FL[i] + SLL * ULLL[i] - (SLL - SL) * ULL[i] - SL * UL[i] - W * ULLL[i];
+        } else if (SM < W && SRR > W) {
+            for (int i = 0; i < 9; i++) PO[i] = FR[i] + SRR * URRR[i] - (SRR - SR) * URR[i] - SR * UR[i] - W * URRR[i];
+        } else if (SR > W && SRR <= W) {
+            for (int i = 0; i < 9; i++) PO[i] = FR[i] + SR * URR[i] - SR * UR[i] - W * URR[i];
+        } else if (SR <= W) {
+            for (int i = 0; i < 9; i++) PO[i] = FR[i] - W * UR[i];
         }
     }
     const double SN = dmax(fabs(SL), fabs(SR));
-    PO[5] = -SN * (bn2 - bn1);
+    PO[5] = -SN * (bn2 - bn1) - W * bn;
     // back to (x, y, z), then the reference's reordering: B fluxes before energy
     Pout[0] = PO[0];
     Pout[1] = n1 * PO[1] + t1 * PO[2] + m1 * PO[3];
@@ -2080,7 +2088,7 @@ static double hlld(double ga, double kurant, const double* qqq1, const double* q
 
 double go_hlldq(const go_params *prm, const double *L9, const double *R9, double *P8, double *PQ, const double *n3,
                 double rad, int metod) {
-    return hlldq(prm->gamma, prm->kurant, L9, R9, n3[0], n3[1], n3[2], rad, metod, P8, PQ);
+    return hlldq(prm->gamma, prm->kurant, L9, R9, n3[0], n3[1], n3[2], rad, metod, P8, PQ, 0.0);
 }
 
 double go_hlld(const go_params *prm, const double *q1, const double *q2, const double *n3, double *q8,
@@ -2609,6 +2617,302 @@ void go_5_komponent(void *h, int step) {
                 update_h(c, k, now2, hk, PH[hk], roH[hk], pH[hk], uH[hk], vH[hk], q1h, q21h, q22h, q3h, Volume,
                          Volume2, y, dt, rf, pf);
             }
+        }
+        go_commit_points(c);
+    }
+    c->last_dt = T[now2];
+}
+
+/* ------------------------------------------------------------------ MHD + pickup protons
+ * The MHD form of the moving-grid step (GELIOS_FORM_MHD_PUI of the device
+ * library).  No reference step exists: this is the project's definition,
+ * assembled from the reference's parts:
+ *   - grid motion, ion reconstruction and boundary states: go_mk2 above
+ *     (Setka.cpp:10121-10482), run on the ion fluid's gas-dynamic rows;
+ *   - extra rows (w, B, pickup protons): Get_par's boundary rules and
+ *     Get_par_TVD's minmod stencil (Gran.cpp:205-473), first order in C_1
+ *     cells and without a Sosed_down;
+ *   - ion flux: hlldq (Solvers::HLLDQ_Korolkov, metod 3) in the face frame
+ *     with its fan sampled at the face speed W (F - W U of the region that
+ *     contains W, like HLLC_2d_Korolkov_b_s on moving faces);
+ *   - pickup flux: hllc (HLLC_2d_Korolkov_b_s, metod 1);
+ *   - update: the MK2 update with the axisymmetric terms of both fluids and
+ *     the fixed charge-exchange sources.
+ * Every face is evaluated from each side, as the reference's cell loops do. */
+void go_set_mhd(void *h, int buf, const double *rows8) {
+    ctx *c = (ctx *)h;
+    const int nc = c->m.n_cells;
+    for (int q = 0; q < 8; q++) memcpy(c->hpar[buf][q], rows8 + (size_t)q * nc, sizeof(double) * nc);
+}
+void go_get_mhd(void *h, int buf, double *rows8) {
+    ctx *c = (ctx *)h;
+    const int nc = c->m.n_cells;
+    for (int q = 0; q < 8; q++) memcpy(rows8 + (size_t)q * nc, c->hpar[buf][q], sizeof(double) * nc);
+}
+void go_set_sources(void *h, const double *q1, const double *q2, const double *q3) {
+    ctx *c = (ctx *)h;
+    const int nc = c->m.n_cells;
+    memcpy(c->qfix[0], q1, sizeof(double) * nc);
+    memcpy(c->qfix[1], q2, sizeof(double) * nc);
+    memcpy(c->qfix[2], q3, sizeof(double) * nc);
+}
+
+enum { X_W = 0, X_BX, X_BY, X_BZ, X_RO, X_P, X_U, X_V };
+typedef struct {
+    double f[8];
+} ext8;
+
+static ext8 cell_ext(const ctx *c, int k, int buf) {
+    ext8 e;
+    for (int q = 0; q < 8; q++) e.f[q] = c->hpar[buf][q][k];
+    return e;
+}
+
+/* boundary rule of the extra rows across face f of its master cell */
+static ext8 get_par_ext(const ctx *c, const go_mhd_params *mp, int f, int buf) {
+    const go_params *P = &c->prm;
+    const int t = c->m.face_type[f];
+    ext8 e = cell_ext(c, c->m.face_master[f], buf);
+    if (t == T_USUALY) {
+        e = cell_ext(c, c->m.face_sosed[f], buf);
+    } else if (t == T_EXTERN) {
+        if (e.f[X_U] >= 0.0) e.f[X_U] = P->extern_u_par;
+    } else if (t == T_AXIS) {
+        e.f[X_W] = -e.f[X_W];
+        e.f[X_BY] = -e.f[X_BY];
+        e.f[X_BZ] = -e.f[X_BZ];
+        e.f[X_V] = -e.f[X_V];
+    } else if (t == T_INNER_SPHERE) {
+        double x, y;
+        face_center(c, f, 0, &x, &y);
+        const double dist = sqrt(x * x + y * y);
+        const st5 wind = inner_sphere_state(c, f);
+        e.f[X_W] = 0.0;
+        e.f[X_BX] = 0.0;
+        e.f[X_BY] = 0.0;
+        e.f[X_BZ] = mp->inner_bphi * (P->R1 / dist) * (y / dist);
+        e.f[X_RO] = mp->pui_inner_ro * wind.ro;
+        e.f[X_P] = mp->pui_inner_p * wind.p;
+        e.f[X_U] = wind.u;
+        e.f[X_V] = wind.v;
+    } else if (t == T_INPUT) {
+        e.f[X_W] = 0.0;
+        e.f[X_BX] = mp->lism_bx;
+        e.f[X_BY] = mp->lism_by;
+        e.f[X_BZ] = mp->lism_bz;
+        e.f[X_RO] = mp->pui_in_ro;
+        e.f[X_P] = mp->pui_in_p;
+        e.f[X_U] = P->in_u;
+        e.f[X_V] = P->in_v;
+    }
+    return e;
+}
+
+/* Get_par_TVD's stencil (Gran.cpp:340-472) for the extra rows of a Usualy
+ * face f seen from its master */
+static ext8 get_par_tvd_ext(const ctx *c, int f, int buf) {
+    const int M = c->m.face_master[f], So = c->m.face_sosed[f], Sd = c->m.face_sosed_down[f];
+    ext8 own = cell_ext(c, M, buf);
+    if (Sd < 0) return own;
+    double x, y, x2, y2;
+    face_center(c, f, 0, &x, &y);
+    ext8 e1 = cell_ext(c, Sd, buf), o;
+    cell_center(c, M, 0, &x2, &y2);
+    const double dist2 = sqrt(kv(x - x2) + kv(y - y2));
+    cell_center(c, Sd, 0, &x2, &y2);
+    const double dist1 = sqrt(kv(x - x2) + kv(y - y2));
+    if (is_tracked_face(c, f)) {
+        for (int q = 0; q < 8; q++) o.f[q] = linear2(-dist1, e1.f[q], -dist2, own.f[q], 0.0);
+    } else {
+        ext8 e3 = cell_ext(c, So, buf);
+        cell_center(c, So, 0, &x2, &y2);
+        const double dist3 = sqrt(kv(x - x2) + kv(y - y2));
+        for (int q = 0; q < 8; q++) o.f[q] = linear3(-dist1, e1.f[q], -dist2, own.f[q], dist3, e3.f[q], 0.0);
+    }
+    if (!(o.f[X_RO] > 0.0)) o.f[X_RO] = own.f[X_RO];
+    if (!(o.f[X_P] > 0.0)) o.f[X_P] = own.f[X_P];
+    return o;
+}
+
+/* ion flux through a face (n1, n2) moving with normal speed W: hlldq in the
+ * face frame with its fan sampled at W (F - W U).  out: mass, mom x, mom y,
+ * mom phi, energy, Bx, By, Bphi, Q; returns 1/max(|SL|,|SR|) */
+static double mhd_flux(double ga, st5 iL, ext8 eL, st5 iR, ext8 eR, double n1, double n2, double W, double *out) {
+    const double t1 = -n2, t2 = n1;
+    double L[9] = {iL.ro, iL.Q, iL.p, iL.u * n1 + iL.v * n2, iL.u * t1 + iL.v * t2, eL.f[X_W],
+                   eL.f[X_BX] * n1 + eL.f[X_BY] * n2, eL.f[X_BX] * t1 + eL.f[X_BY] * t2, eL.f[X_BZ]};
+    double R[9] = {iR.ro, iR.Q, iR.p, iR.u * n1 + iR.v * n2, iR.u * t1 + iR.v * t2, eR.f[X_W],
+                   eR.f[X_BX] * n1 + eR.f[X_BY] * n2, eR.f[X_BX] * t1 + eR.f[X_BY] * t2, eR.f[X_BZ]};
+    double F[8], FQ;
+    const double tinv = hlldq(ga, 1.0, L, R, 1.0, 0.0, 0.0, 1.0, 3, F, &FQ, W);
+    out[0] = F[0];
+    out[1] = n1 * F[1] + t1 * F[2];
+    out[2] = n2 * F[1] + t2 * F[2];
+    out[3] = F[3];
+    out[4] = F[7];
+    out[5] = n1 * F[4] + t1 * F[5];
+    out[6] = n2 * F[4] + t2 * F[5];
+    out[7] = F[6];
+    out[8] = FQ;
+    return tinv;
+}
+
+void go_mhd(void *h, const go_mhd_params *mp, int step) {
+    ctx *c = (ctx *)h;
+    const go_params *P = &c->prm;
+    const double ggg = P->gamma, g2 = 2 * P->gamma;
+    const double i4p = 1.0 / (4.0 * PI_), i8p = 1.0 / (8.0 * PI_);
+    int now1 = 1, now2 = 0;
+    double T[2];
+    T[0] = T[1] = P->dt0;
+    for (int st = 0; st < step; st++) {
+        now1 = (now1 + 1) % 2;
+        now2 = (now2 + 1) % 2;
+        T[now2] = 100000000;
+        go_move_surface(c, now1, T[now1]);
+        go_move_setka2(c, T[now1]);
+        for (int k = 0; k < c->m.n_cells; k++) {
+            double time = 10000000;
+            double Pt[13];
+            for (int q = 0; q < 13; q++) Pt[q] = 0.0;
+            st5 par1 = cell_state(c, k, now1);
+            ext8 ex1 = cell_ext(c, k, now1);
+            double x, y;
+            cell_center(c, k, 0, &x, &y);
+            double vs1 = cell_volume(c, k, 0);
+            double vs2 = cell_volume(c, k, 1);
+            double radius = sqrt(kv(x) + kv(y));
+            if (radius < P->R11) continue;
+            double Volume = cell_volume_rotate(c, k, 0, 360.0) / (2.0 * PI_);
+            double Volume2 = cell_volume_rotate(c, k, 1, 360.0) / (2.0 * PI_);
+            const int kt = c->m.cell_type[k];
+            for (int g = c->m.gran_start[k]; g < c->m.gran_start[k + 1]; g++) {
+                int f = c->m.gran[g];
+                double x2, y2, x4, y4, n1, n2;
+                double S = face_square(c, f) * (c->y[c->m.face_A[f]] + c->y[c->m.face_B[f]]) * 0.5;
+                face_center(c, f, 0, &x2, &y2);
+                face_center(c, f, 1, &x4, &y4);
+                double dist = sqrt(kv(x - x2) + kv(y - y2));
+                st5 par11 = par1;
+                st5 par2 = get_par(c, f, now1);
+                ext8 e11 = ex1;
+                ext8 e2 = get_par_ext(c, mp, f, now1);
+                face_normal(c, f, &n1, &n2);
+                double W = ((x4 - x2) * n1 + (y4 - y2) * n2) / T[now1];
+                double dis = sqrt(kv(x2) + kv(y2));
+                int ft = c->m.face_type[f];
+                if (ft == T_USUALY) {
+                    int So = c->m.face_sosed[f];
+                    double x3, y3;
+                    cell_center(c, So, 0, &x3, &y3);
+                    double dd = sqrt(kv(x3) + kv(y3));
+                    if (kt == C_1) {
+                        par11.ro = par11.ro * kv(radius) / kv(dis);
+                        par11.Q = par11.Q * kv(radius) / kv(dis);
+                        par11.p = par11.p * pow(radius / dis, g2);
+                        polar_perenos(x, y, x2, y2, &par11.u, &par11.v, TINY_ANGLE);
+                        double pro, pp;
+                        get_par_tvd_radial(c, f, now1, &pro, &pp);
+                        par11.ro = pro;
+                        par11.p = pp;
+                    } else {
+                        get_par_tvd(c, f, now1, &par11);
+                        e11 = get_par_tvd_ext(c, f, now1);
+                    }
+                    int fc = c->m.face_copy[f];
+                    if (c->m.cell_type[So] == C_1) {
+                        par2.ro = par2.ro * kv(dd) / kv(dis);
+                        par2.Q = par2.Q * kv(dd) / kv(dis);
+                        par2.p = par2.p * pow(dd / dis, g2);
+                        polar_perenos(x3, y3, x2, y2, &par2.u, &par2.v, TINY_ANGLE);
+                        double pro, pp;
+                        get_par_tvd_radial(c, fc, now1, &pro, &pp);
+                        par2.ro = pro;
+                        par2.p = pp;
+                    } else {
+                        get_par_tvd(c, fc, now1, &par2);
+                        e2 = get_par_tvd_ext(c, fc, now1);
+                    }
+                } else if (ft == T_INNER_SPHERE) {
+                    par11.ro = par11.ro * kv(radius) / kv(dis);
+                    par11.Q = par11.Q * kv(radius) / kv(dis);
+                    par11.p = par11.p * pow(radius / dis, g2);
+                } else if (kt == C_1 && ft == T_AXIS) {
+                    par11.ro = par11.ro * kv(radius) / kv(dis);
+                    par11.Q = par11.Q * kv(radius) / kv(dis);
+                    par11.p = par11.p * pow(radius / dis, g2);
+                    polar_perenos(x, y, x2, y2, &par11.u, &par11.v, TINY_ANGLE);
+                    par2 = par11;
+                    par2.v = -par2.v;
+                } else if (kt != C_1 && ft == T_AXIS) {
+                    get_par_tvd(c, f, now1, &par11);
+                    par2 = par11;
+                    par2.v = -par2.v;
+                }
+                double F[9];
+                const double tI = mhd_flux(ggg, par11, e11, par2, e2, n1, n2, W, F);
+                double Gp[4], GQ, Vl, Vc, Vp;
+                const double tP = hllc(P, e11.f[X_RO], 0.0, e11.f[X_P], e11.f[X_U], e11.f[X_V], e2.f[X_RO], 0.0,
+                                       e2.f[X_P], e2.f[X_U], e2.f[X_V], W, Gp, &GQ, n1, n2, dist, 1, &Vl, &Vc, &Vp, 0);
+                time = dmin(time, P->kurant * dist * tI);
+                time = dmin(time, tP);
+                for (int q = 0; q < 9; q++) Pt[q] = Pt[q] + F[q] * S;
+                for (int q = 0; q < 4; q++) Pt[9 + q] = Pt[9 + q] + Gp[q] * S;
+            }
+            if (time < T[now2]) T[now2] = time;
+            if (kt == C_CENTR) {
+                st5 s0 = cell_state(c, k, now1);
+                write_state(c, k, now2, s0.ro, s0.Q, s0.p, s0.u, s0.v);
+                for (int q = 0; q < 8; q++) c->hpar[now2][q][k] = ex1.f[q];
+                continue;
+            }
+            const double dt = T[now1];
+            const double Am = 0.5 * (vs1 + vs2);
+            const double q1 = c->qfix[0][k], q2 = c->qfix[1][k], q3 = c->qfix[2][k];
+            const double ro = par1.ro, p = par1.p, u = par1.u, v = par1.v, Q = par1.Q;
+            const double w = ex1.f[X_W], bx = ex1.f[X_BX], by = ex1.f[X_BY], bz = ex1.f[X_BZ];
+            const double bb = bx * bx + by * by + bz * bz;
+            const double Sy = p + bb * i8p + ro * w * w - bz * bz * i4p;
+            const double Sphi = -(ro * v * w - by * bz * i4p);
+            const double Sbz = v * bz - w * by;
+            double ro3 = ro * Volume / Volume2 - dt * (Pt[0] / Volume2);
+            const double Q3 = Q * Volume / Volume2 - (dt / Volume2) * Pt[8];
+            if (ro3 <= 0.0) {
+                ro3 = P->ro_floor;
+                c->n_ro_clamp++;
+            }
+            const double u3 = (ro * u * Volume / Volume2 - dt * (Pt[1] / Volume2 - q1)) / ro3;
+            const double v3 = (ro * v * Volume / Volume2 - dt * ((Pt[2] - Sy * Am) / Volume2 - q2)) / ro3;
+            const double w3 = (ro * w * Volume / Volume2 - dt * ((Pt[3] - Sphi * Am) / Volume2)) / ro3;
+            const double E = p / (ggg - 1) + ro * (u * u + v * v + w * w) * 0.5 + bb * i8p;
+            const double E3 = E * Volume / Volume2 - dt * (Pt[4] / Volume2 - q3);
+            const double bx3 = bx * Volume / Volume2 - dt * (Pt[5] / Volume2);
+            const double by3 = by * Volume / Volume2 - dt * (Pt[6] / Volume2);
+            const double bz3 = bz * Volume / Volume2 - dt * ((Pt[7] - Sbz * Am) / Volume2);
+            double p3 = (E3 - 0.5 * ro3 * (u3 * u3 + v3 * v3 + w3 * w3) - (bx3 * bx3 + by3 * by3 + bz3 * bz3) * i8p) *
+                        (ggg - 1);
+            if (p3 <= 0) {
+                p3 = P->p_floor;
+                c->n_p_clamp++;
+            }
+            const double rp = ex1.f[X_RO], pp = ex1.f[X_P], up = ex1.f[X_U], vp = ex1.f[X_V];
+            double rp3 = rp * Volume / Volume2 - dt * (Pt[9] / Volume2);
+            if (rp3 <= 0.0) {
+                rp3 = P->ro_floor;
+                c->n_ro_clamp++;
+            }
+            const double up3 = (rp * up * Volume / Volume2 - dt * (Pt[10] / Volume2)) / rp3;
+            const double vp3 = (rp * vp * Volume / Volume2 - dt * ((Pt[11] - pp * Am) / Volume2)) / rp3;
+            const double Ep = pp / (ggg - 1) + rp * (up * up + vp * vp) * 0.5;
+            double pp3 = ((Ep * Volume / Volume2 - dt * (Pt[12] / Volume2)) - 0.5 * rp3 * (up3 * up3 + vp3 * vp3)) *
+                         (ggg - 1);
+            if (pp3 <= 0) {
+                pp3 = P->p_floor;
+                c->n_p_clamp++;
+            }
+            write_state(c, k, now2, ro3, Q3, p3, u3, v3);
+            const double outx[8] = {w3, bx3, by3, bz3, rp3, pp3, up3, vp3};
+            for (int q = 0; q < 8; q++) c->hpar[now2][q][k] = outx[q];
         }
         go_commit_points(c);
     }

@@ -88,6 +88,19 @@ void go_move_setka2(void *h, double dt);
 void go_commit_points(void *h);
 double go_last_dt(void *h);
 
+/* MHD + pickup-proton moving-grid step (no reference step exists; this is
+ * the project's own restatement, written per cell and per face from each
+ * side like the reference's loops, as the checker of the device's
+ * once-per-face units).  Same field order as gelios_mhd_params. */
+typedef struct go_mhd_params {
+    double lism_bx, lism_by, lism_bz, inner_bphi, pui_in_ro, pui_in_p, pui_inner_ro, pui_inner_p;
+} go_mhd_params;
+/* extra rows of par[buf]: w, Bx, By, Bz, ro_pui, p_pui, u_pui, v_pui */
+void go_set_mhd(void *h, int buf, const double *rows8);
+void go_get_mhd(void *h, int buf, double *rows8);
+void go_set_sources(void *h, const double *q1, const double *q2, const double *q3);
+void go_mhd(void *h, const go_mhd_params *mp, int steps);
+
 /* per-face kernels */
 double go_hllc(const go_params *prm, const double *L5, const double *R5, double W, double *P4, double *PQ,
                double n1, double n2, double rad, int metod, double *VlVcVp, int nul_potok);

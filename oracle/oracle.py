@@ -62,6 +62,13 @@ class GoMesh(C.Structure):
     ]
 
 
+class GoMhdParams(C.Structure):
+    """Mirror of ``go_mhd_params`` (same field order as gelios_mhd_params)."""
+
+    _fields_ = [(n, C.c_double) for n in ("lism_bx", "lism_by", "lism_bz", "inner_bphi", "pui_in_ro", "pui_in_p",
+                                          "pui_inner_ro", "pui_inner_p")]
+
+
 _LIB = None
 
 
@@ -109,6 +116,10 @@ def lib() -> C.CDLL:
     L.go_face_par.argtypes = [vp, C.c_int, C.c_int, C.c_int, f64p]
     L.go_cell_geom.argtypes = [vp, C.c_int, f64p]
     L.go_source_mk1.argtypes = [vp, C.c_int] + [C.c_double] * 4 + [f64p]
+    L.go_set_mhd.argtypes = [vp, C.c_int, f64p]
+    L.go_get_mhd.argtypes = [vp, C.c_int, f64p]
+    L.go_set_sources.argtypes = [vp, f64p, f64p, f64p]
+    L.go_mhd.argtypes = [vp, C.POINTER(GoMhdParams), C.c_int]
     _LIB = L
     return L
 
@@ -224,6 +235,23 @@ class Oracle:
         out = np.zeros(16 * self.ncell)
         self.L.go_get_hydrogen(self.h, int(buf), out)
         return out.reshape(16, self.ncell)
+
+    def set_mhd(self, buf, x8):
+        """Extra rows of the MHD form in par[buf]; x8 of shape (8, n_cells)."""
+        self.L.go_set_mhd(self.h, int(buf), np.ascontiguousarray(x8, np.float64).ravel())
+
+    def get_mhd(self, buf) -> np.ndarray:
+        out = np.zeros(8 * self.ncell)
+        self.L.go_get_mhd(self.h, int(buf), out)
+        return out.reshape(8, self.ncell)
+
+    def set_sources(self, q1, q2, q3):
+        f = lambda a: np.ascontiguousarray(a, np.float64).ravel()  # noqa: E731
+        self.L.go_set_sources(self.h, f(q1), f(q2), f(q3))
+
+    def mhd(self, mp: dict, steps):
+        """The MHD + pickup-proton moving-grid step (go_mhd)."""
+        self.L.go_mhd(self.h, C.byref(GoMhdParams(**mp)), int(steps))
 
     def five_komponent(self, steps):
         """Setka::Go_5_komponent (Setka.cpp:8269-8950)."""

@@ -1,0 +1,153 @@
+"""The MHD + pickup-proton moving-grid step (GELIOS_FORM_MHD_PUI).
+
+The reference has no such step: it steps gas dynamics only and never calls
+its MHD solvers.  The step is this project's assembly of the reference's
+parts (grid motion and ion reconstruction of Go_5_komponent__MK2,
+Setka.cpp:10121-10482; HLLD of Solvers::HLLDQ_Korolkov, Solvers.cpp:1642-2185,
+in the face frame; HLLC of HLLC_2d_Korolkov_b_s, Setka.cpp:10484-10700, for
+the pickup protons).  Its flux is pinned to the reference through the HLLDQ
+golden vectors (tests/test_oracle_pin.py); the step itself is checked against
+the oracle's restatement (oracle/gelios_oracle.c, go_mhd), which evaluates
+every face from each side like the reference's cell loops, while the device
+evaluates each face once and hands the negated flux to the neighbour.
+
+Tolerances: max-norm relative error per variable <= 1e-12 after one and two
+steps, <= 1e-10 after ten; point coordinates <= 1e-13.
+"""
+import numpy as np
+import pytest
+
+import gelios_2d_b200 as g
+from gelios_2d_b200 import _native as N
+from gelios_2d_b200 import workloads as W
+from oracle import oracle as O
+
+SMALL = (4, 3, 3, 10, 23, 6, 7, 7)
+MEDIUM = (30, 7, 11, 20, 60, 20, 40, 40)
+
+
+def rel_err(a, b):
+    out = 0.0
+    for k in range(a.shape[0]):
+        s = np.max(np.abs(b[k]))
+        if s > 0:
+            out = max(out, float(np.max(np.abs(a[k] - b[k])) / s))
+    return out
+
+
+def go_params(p: N.GeliosParams) -> O.GoParams:
+    return O.GoParams(**{n: getattr(p, n) for n, _ in O.GoParams._fields_ if n != "pad_"}, pad_=0)
+
+
+def setup(dims, mp=None, seed=17):
+    mesh = g.Mesh.setka(*dims)
+    P = N.reference_params()
+    mp = mp if mp is not None else W.mhd_params()
+    st0 = W.init_conditions_reference(mesh)
+    x0 = W.mhd_initial(mesh, st0, mp)
+    src = W.mhd_sources(mesh, seed=seed)
+    return mesh, P, mp, st0, x0, src
+
+
+def oracle_run(mesh, P, mp, st0, x0, src, steps):
+    ora = O.Oracle(go_params(P), mesh)
+    for b in (0, 1):
+        ora.set_state(b, st0)
+        ora.set_mhd(b, x0)
+    ora.set_sources(*src)
+    ora.mhd(mp.as_dict(), steps)
+    return ora
+
+
+def device_run(mesh, P, mp, st0, x0, src, steps):
+    dev = g.Setka(mesh, P)
+    dev.set_mhd_params(mp)
+    for b in (0, 1):
+        dev.set_par(b, st0)
+        dev.set_mhd(b, x0)
+    dev.set_sources(*src)
+    st = dev.Go_MHD_pickup(steps)
+    return dev, st
+
+
+# ------------------------------------------------------------------ CPU (oracle)
+def test_oracle_mhd_step_stays_physical():
+    mesh, P, mp, st0, x0, src = setup(SMALL)
+    ora = oracle_run(mesh, P, mp, st0, x0, src, 6)
+    b = 6 % 2
+    s, x = ora.get_state(b), ora.get_mhd(b)
+    assert np.all(np.isfinite(s)) and np.all(np.isfinite(x))
+    assert np.all(s[0] > 0) and np.all(s[1] > 0) and np.all(x[4] > 0) and np.all(x[5] > 0)
+    assert not np.array_equal(s, st0)
+
+
+def test_oracle_field_free_stays_field_free():
+    """With no field anywhere (initial, inflow and wind) and no azimuthal
+    velocity, the induction fluxes and the azimuthal terms vanish: B and w
+    stay exactly zero."""
+    mp = W.mhd_params(b_lism=0.0, inner_bphi=0.0)
+    mesh, P, mp, st0, x0, src = setup(SMALL, mp)
+    ora = oracle_run(mesh, P, mp, st0, x0, src, 4)
+    x = ora.get_mhd(0)
+    assert np.all(x[0:4] == 0.0)
+
+
+def test_oracle_pickup_fluid_decoupled_from_field():
+    """The pickup protons see the field only through the common time step:
+    two runs with different fields but the same dt history give the same
+    pickup fluid.  Checked on one step (dt = dt0 in both runs)."""
+    mesh, P, mp1, st0, x0, src = setup(SMALL)
+    mp2 = W.mhd_params(b_lism=0.02, b_angle_deg=50.0, inner_bphi=3.0)
+    x02 = W.mhd_initial(mesh, st0, mp2)
+    o1 = oracle_run(mesh, P, mp1, st0, x0, src, 1)
+    o2 = oracle_run(mesh, P, mp2, st0, x02, src, 1)
+    assert np.array_equal(o1.get_mhd(1)[4:], o2.get_mhd(1)[4:])
+    assert not np.array_equal(o1.get_mhd(1)[1:4], o2.get_mhd(1)[1:4])
+
+
+def test_mhd_entry_points_declared():
+    names = N.header_functions()
+    for f in ("gelios_set_mhd_params", "gelios_upload_mhd", "gelios_download_mhd", "gelios_upload_sources"):
+        assert f in names
+        assert hasattr(N.lib(), f)
+
+
+# ------------------------------------------------------------------ GPU parity
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims,steps,tol", [(SMALL, 1, 1e-12), (SMALL, 2, 1e-12), (MEDIUM, 2, 1e-12),
+                                            (MEDIUM, 10, 1e-10)])
+def test_mhd_device_matches_oracle(dims, steps, tol):
+    mesh, P, mp, st0, x0, src = setup(dims)
+    ora = oracle_run(mesh, P, mp, st0, x0, src, steps)
+    dev, st = device_run(mesh, P, mp, st0, x0, src, steps)
+    b = steps % 2
+    assert st.result_buf == b
+    e_ion = rel_err(dev.par(b), ora.get_state(b))
+    e_ext = rel_err(dev.mhd(b), ora.get_mhd(b))
+    assert e_ion <= tol, e_ion
+    assert e_ext <= tol, e_ext
+    x, y = dev.points()
+    po = ora.points()
+    assert np.max(np.abs(x - po["x"])) <= 1e-13 * np.max(np.abs(po["x"]))
+    assert np.max(np.abs(y - po["y"])) <= 1e-13 * np.max(np.abs(po["y"]))
+    assert abs(st.dt - ora.last_dt()) <= 1e-12 * ora.last_dt()
+
+
+@pytest.mark.gpu
+def test_mhd_device_field_free_and_deterministic():
+    mp = W.mhd_params(b_lism=0.0, inner_bphi=0.0)
+    mesh, P, mp, st0, x0, src = setup(MEDIUM, mp)
+    d1, _ = device_run(mesh, P, mp, st0, x0, src, 3)
+    d2, _ = device_run(mesh, P, mp, st0, x0, src, 3)
+    assert np.all(d1.mhd(1)[0:4] == 0.0)
+    assert np.array_equal(d1.par(1), d2.par(1)) and np.array_equal(d1.mhd(1), d2.mhd(1))
+
+
+@pytest.mark.gpu
+def test_mhd_fp32_flux_close_to_fp64():
+    mesh, P, mp, st0, x0, src = setup(MEDIUM)
+    ora = oracle_run(mesh, P, mp, st0, x0, src, 4)
+    P32 = P.copy(precision=N.PREC_FP32_FLUX)
+    dev, _ = device_run(mesh, P32, mp, st0, x0, src, 4)
+    assert rel_err(dev.par(0), ora.get_state(0)) <= 1e-4
+    assert rel_err(dev.mhd(0)[4:], ora.get_mhd(0)[4:]) <= 1e-4
