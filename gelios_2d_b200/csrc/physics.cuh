@@ -789,6 +789,161 @@ __device__ inline double hlldq_korolkov(double ga, double kurant, const double* 
     return hlldq_impl<false>(ga, kurant, L, R, n1, n2, n3, rad, metod, Pout, PQ, 0.0);
 }
 
+// hlldq_impl<true>(ga, 1, L, R, 1, 0, 0, 1, 3, Pout, PQ, W) with the normal
+// fixed to the x axis of the face frame, written for few registers: the
+// wave speeds and star quantities first, then only the fan region that
+// contains W, one component at a time.  Same arithmetic as hlldq_impl.
+// L, R = (ro, Q, p, u_n, u_t, u_phi, B_n, B_t, B_phi); Pout[8] = mass,
+// momentum n, t, phi, B n, t, phi, energy; *PQ = Q flux.  Returns 1/max|S|.
+template <typename T>
+__device__ inline double hlld_face_moving(double gad, const double* L, const double* R, double Wd, double* Pout,
+                                          double* PQ) {
+    const T spi4 = (T)spi4_dev();
+    const T ga = (T)gad, W = (T)Wd;
+    const T g1 = ga - (T)1;
+    auto sq = [](T x) { return x * x; };
+    auto sqrt = [](T x) { return tsqrt<T>(x); };
+    auto fabs = [](T x) -> T {
+        if constexpr (sizeof(T) == 8) return ::fabs(x);
+        else return fabsf(x);
+    };
+    auto dmin_ref = [](T a, T b) { return tmin<T>(a, b); };
+    auto dmax_ref = [](T a, T b) { return tmax<T>(a, b); };
+    auto sgn = [](T x) { return x > (T)0 ? (T)1 : (x < (T)0 ? (T)-1 : (T)0); };
+    const T ro_L = (T)L[0], Q_L = (T)L[1], p_L = (T)L[2], u1 = (T)L[3], v1 = (T)L[4], w1 = (T)L[5];
+    const T ro_R = (T)R[0], Q_R = (T)R[1], p_R = (T)R[2], u2 = (T)R[3], v2 = (T)R[4], w2 = (T)R[5];
+    const T bn1 = (T)L[6] / spi4, bt1 = (T)L[7] / spi4, bm1 = (T)L[8] / spi4;
+    const T bn2 = (T)R[6] / spi4, bt2 = (T)R[7] / spi4, bm2 = (T)R[8] / spi4;
+    const T bb_L = sq(bn1) + sq(bt1) + sq(bm1);
+    const T bb_R = sq(bn2) + sq(bt2) + sq(bm2);
+    const T uu_L = (sq(u1) + sq(v1) + sq(w1)) / (T)2.0;
+    const T uu_R = (sq(u2) + sq(v2) + sq(w2)) / (T)2.0;
+    const T cfL = sqrt((ga * p_L + bb_L + sqrt(sq(ga * p_L + bb_L) - (T)4.0 * ga * p_L * sq(bn1))) / ((T)2.0 * ro_L));
+    const T cfR = sqrt((ga * p_R + bb_R + sqrt(sq(ga * p_R + bb_R) - (T)4.0 * ga * p_R * sq(bn2))) / ((T)2.0 * ro_R));
+    const T SL = dmin_ref(u1, u2) - dmax_ref(cfL, cfR);
+    const T SR = dmax_ref(u1, u2) + dmax_ref(cfL, cfR);
+    const T pTL = p_L + bb_L / (T)2.0;
+    const T pTR = p_R + bb_R / (T)2.0;
+    const T suR = SR - u2, suL = SL - u1;
+    const T SM = (suR * ro_R * u2 - suL * ro_L * u1 - pTR + pTL) / (suR * ro_R - suL * ro_L);
+    const T PTT = (suR * ro_R * pTL - suL * ro_L * pTR + ro_L * ro_R * suR * suL * (u2 - u1)) /
+                       (suR * ro_R - suL * ro_L);
+    const T UU = dmax_ref(fabs(SL), fabs(SR));
+    const double time = 1.0 * 1.0 / (double)UU;
+    const T e1 = p_L / g1 + ro_L * uu_L + bb_L / (T)2.0;
+    const T e2 = p_R / g1 + ro_R * uu_R + bb_R / (T)2.0;
+    const T sbv1 = u1 * bn1 + v1 * bt1 + w1 * bm1, sbv2 = u2 * bn2 + v2 * bt2 + w2 * bm2;
+    // fluxes of the two sides (the normal-field flux is 0)
+    const T FLt = u1 * bt1 - v1 * bn1, FLm = u1 * bm1 - w1 * bn1;
+    const T FRt = u2 * bt2 - v2 * bn2, FRm = u2 * bm2 - w2 * bn2;
+    const T bn = (SR * bn2 - SL * bn1 + (T)0.0 - (T)0.0) / (SR - SL);
+    const T bbn = bn * bn;
+    const T ro_LL = ro_L * (SL - u1) / (SL - SM);
+    const T ro_RR = ro_R * (SR - u2) / (SR - SM);
+    const T Q_LL = Q_L * (SL - u1) / (SL - SM);
+    const T Q_RR = Q_R * (SR - u2) / (SR - SM);
+    const T ttL = ro_L * suL * (SL - SM) - bbn;
+    const T ttR = ro_R * suR * (SR - SM) - bbn;
+    T vLL, wLL, vRR, wRR, btt1, bmm1, btt2, bmm2;
+    if (fabs(ttL) >= (T)0.000001) {
+        vLL = v1 - bn * bt1 * (SM - u1) / ttL;
+        wLL = w1 - bn * bm1 * (SM - u1) / ttL;
+        btt1 = bt1 * (ro_L * suL * suL - bbn) / ttL;
+        bmm1 = bm1 * (ro_L * suL * suL - bbn) / ttL;
+    } else {
+        vLL = v1; wLL = w1; btt1 = (T)0.0; bmm1 = (T)0.0;
+    }
+    if (fabs(ttR) >= (T)0.000001) {
+        vRR = v2 - bn * bt2 * (SM - u2) / ttR;
+        wRR = w2 - bn * bm2 * (SM - u2) / ttR;
+        btt2 = bt2 * (ro_R * suR * suR - bbn) / ttR;
+        bmm2 = bm2 * (ro_R * suR * suR - bbn) / ttR;
+    } else {
+        vRR = v2; wRR = w2; btt2 = (T)0.0; bmm2 = (T)0.0;
+    }
+    const T eLL = (e1 * suL + PTT * SM - pTL * u1 + bn * (sbv1 - (SM * bn + vLL * btt1 + wLL * bmm1))) / (SL - SM);
+    const T eRR = (e2 * suR + PTT * SM - pTR * u2 + bn * (sbv2 - (SM * bn + vRR * btt2 + wRR * bmm2))) / (SR - SM);
+    const T sqrtroLL = sqrt(ro_LL), sqrtroRR = sqrt(ro_RR);
+    T SLL = SM - fabs(bn) / sqrtroLL;
+    T SRR = SM + fabs(bn) / sqrtroRR;
+    T idbn;
+    if (fabs(bn) > (T)0.001) {
+        idbn = (T)1.0 * sgn(bn);
+    } else {
+        idbn = (T)0.0;
+        SLL = SM;
+        SRR = SM;
+    }
+    // fan region containing W: 0 L, 1 L*, 2 L**, 3 R**, 4 R*, 5 R
+    int reg = -1;
+    if (SL >= W) reg = 0;
+    else if (SL < W && SLL >= W) reg = 1;
+    else if (SLL <= W && SM >= W) reg = 2;
+    else if (SM < W && SRR > W) reg = 3;
+    else if (SR > W && SRR <= W) reg = 4;
+    else if (SR <= W) reg = 5;
+    T PO[9];
+    for (int i = 0; i < 9; i++) PO[i] = (T)0;
+    const bool left = reg <= 2;
+    // one side's state U, flux F, single-star state U* and the double-star
+    // state U** (reg 2/3 only)
+    const T ro = left ? ro_L : ro_R, uu = left ? u1 : u2, vv = left ? v1 : v2, ww = left ? w1 : w2;
+    const T bnk = left ? bn1 : bn2, btk = left ? bt1 : bt2, bmk = left ? bm1 : bm2;
+    const T ek = left ? e1 : e2, pTk = left ? pTL : pTR, Qk = left ? Q_L : Q_R;
+    const T Sk = left ? SL : SR;
+    const T U[9] = {ro, ro * uu, ro * vv, ro * ww, ek, bnk, btk, bmk, Qk};
+    const T F[9] = {ro * uu,
+                         ro * uu * uu + pTk - sq(bnk),
+                         ro * uu * vv - bnk * btk,
+                         ro * uu * ww - bnk * bmk,
+                         (ek + pTk) * uu - bnk * (uu * bnk + vv * btk + ww * bmk),
+                         (T)0.0,
+                         left ? FLt : FRt,
+                         left ? FLm : FRm,
+                         Qk * uu};
+    if (reg < 0) {
+        // no region (non-finite speeds): zero flux, as the reference's chain of tests leaves it
+    } else if (reg == 0 || reg == 5) {
+        for (int i = 0; i < 9; i++) PO[i] = F[i] - W * U[i];
+    } else {
+        const T roS = left ? ro_LL : ro_RR, vS = left ? vLL : vRR, wS = left ? wLL : wRR;
+        const T btS = left ? btt1 : btt2, bmS = left ? bmm1 : bmm2, eS = left ? eLL : eRR;
+        const T QS = left ? Q_LL : Q_RR;
+        const T US[9] = {roS, roS * SM, roS * vS, roS * wS, eS, bn, btS, bmS, QS};
+        if (reg == 1 || reg == 4) {
+            for (int i = 0; i < 9; i++) PO[i] = F[i] + Sk * US[i] - Sk * U[i] - W * US[i];
+        } else {
+            const T vLLL = (sqrtroLL * vLL + sqrtroRR * vRR + idbn * (btt2 - btt1)) / (sqrtroLL + sqrtroRR);
+            const T wLLL = (sqrtroLL * wLL + sqrtroRR * wRR + idbn * (bmm2 - bmm1)) / (sqrtroLL + sqrtroRR);
+            const T bttt = (sqrtroLL * btt2 + sqrtroRR * btt1 + idbn * sqrtroLL * sqrtroRR * (vRR - vLL)) /
+                                (sqrtroLL + sqrtroRR);
+            const T bmmm = (sqrtroLL * bmm2 + sqrtroRR * bmm1 + idbn * sqrtroLL * sqrtroRR * (wRR - wLL)) /
+                                (sqrtroLL + sqrtroRR);
+            T eSS;
+            if (left)
+                eSS = eLL - idbn * sqrtroLL * ((SM * bn + vLL * btt1 + wLL * bmm1) - (SM * bn + vLLL * bttt + wLLL * bmmm));
+            else
+                eSS = eRR + idbn * sqrtroRR * ((SM * bn + vRR * btt2 + wRR * bmm2) - (SM * bn + vLLL * bttt + wLLL * bmmm));
+            const T USS[9] = {roS, roS * SM, roS * vLLL, roS * wLLL, eSS, bn, bttt, bmmm, QS};
+            const T SS = left ? SLL : SRR;
+            for (int i = 0; i < 9; i++) PO[i] = F[i] + SS * USS[i] - (SS - Sk) * US[i] - Sk * U[i] - W * USS[i];
+        }
+    }
+    const T SN = dmax_ref(fabs(SL), fabs(SR));
+    PO[5] = -SN * (bn2 - bn1);
+    PO[5] -= W * bn;
+    Pout[0] = (double)PO[0];
+    Pout[1] = (double)PO[1];
+    Pout[2] = (double)PO[2];
+    Pout[3] = (double)PO[3];
+    Pout[4] = (double)(spi4 * PO[5]);
+    Pout[5] = (double)(spi4 * PO[6]);
+    Pout[6] = (double)(spi4 * PO[7]);
+    Pout[7] = (double)PO[4];
+    *PQ = (double)PO[8];
+    return time;
+}
+
 // Solvers::HLLD_Solver_Alexashov (Solvers.cpp:92-691).  q = (ro, p, u, v, w,
 // bx, by, bz) in the (x, y, z) frame, n a unit normal (any direction: the
 // frame is built from the mean field), face speed w.  The reference fixes

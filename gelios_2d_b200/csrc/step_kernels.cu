@@ -2337,32 +2337,62 @@ __device__ __forceinline__ Ext8 get_par_ext(const gelios_params& P, const gelios
     return e;
 }
 
-// Reconstruction of the extra rows at a Usualy face seen from M (values Me,
-// centre Mx,My; neighbour So, Sosed_down Sd): the minmod rule of
-// Gran::Get_par_TVD (Gran.cpp:292-473) with its stencil, two points on
-// tracked faces, first order without a Sosed_down; non-positive pickup
-// density or pressure fall back to M's value.
-__device__ Ext8 tvd_ext(const double* __restrict__ hs, size_t nc, const double* cx, const double* cy, double fx,
-                        double fy, const Ext8& Me, double Mx, double My, int So, int Sd, bool tracked) {
-    if (Sd < 0) return Me;
+// All 13 rows at a Usualy face seen from M (ion Ms, extra Me, centre Mx,My,
+// flags mf), with the cell So across the face already loaded (Ss, Se,
+// centre Sx,Sy) and Sosed_down Sd: the ion rows follow mk2_usualy_side
+// (Get_par_TVD / Get_par_TVD_radial in C_1 cells), the extra rows tvd_ext's
+// rule, with the stencil distances computed once for both.
+__device__ __forceinline__ void mhd_usualy_side(const double* const* st, const double* __restrict__ hs, size_t nc,
+                                                const double* cx, const double* cy, const double* rp, double fx,
+                                                double fy, double dis, double pdis, const St5& Ms, const Ext8& Me,
+                                                double Mx, double My, double rpM, uint32_t mf, int So, const St5& Ss,
+                                                const Ext8& Se, double Sx, double Sy, int Sd, bool tracked, St5& oi,
+                                                Ext8& oe, int* status) {
+    if (mf & CF_C1) {
+        oi = mk2_usualy_side(st, cx, cy, rp, fx, fy, dis, pdis, Ms, Mx, My, rpM, mf, So, Sd, tracked, status);
+        oe = Me;
+        return;
+    }
+    oi = Ms;
+    oe = Me;
+    if (Sd < 0) {
+        if (mf & CF_AXIS) {  // Gran.cpp:308-338
+            const double dist2 = sqrt(sq(fx - Mx) + sq(fy - My));
+            const double dist3 = sqrt(sq(fx - Sx) + sq(fy - Sy));
+            const double dist1 = sqrt(sq(fx - Mx) + sq(fy - (-My)));
+            oi.v = linear3(-dist1, -Ms.v, -dist2, Ms.v, dist3, Ss.v, 0.0);
+        }
+        return;
+    }
+    const St5 s1 = load_state(st, Sd);
     const Ext8 e1 = load_ext(hs, nc, Sd);
     const double dist2 = sqrt(sq(fx - Mx) + sq(fy - My));
     const double dist1 = sqrt(sq(fx - cx[Sd]) + sq(fy - cy[Sd]));
     const double r12 = 1.0 / (-dist1 - (-dist2)), x2 = -dist2;
-    Ext8 o;
-    if (tracked) {
+    if (tracked) {  // Gran.cpp:345-426
+        oi.ro = (s1.ro - Ms.ro) * r12 * (0.0 - x2) + Ms.ro;
+        oi.p = (s1.p - Ms.p) * r12 * (0.0 - x2) + Ms.p;
+        oi.u = (s1.u - Ms.u) * r12 * (0.0 - x2) + Ms.u;
+        oi.v = (s1.v - Ms.v) * r12 * (0.0 - x2) + Ms.v;
+        oi.Q = (s1.Q - Ms.Q) * r12 * (0.0 - x2) + Ms.Q;
+        if (oi.ro <= 0.0) oi.ro = Ms.ro;
+        if (oi.p <= 0.0) oi.p = Ms.p;
 #pragma unroll
-        for (int k = 0; k < kMhdExtra; k++) o.f[k] = (e1.f[k] - Me.f[k]) * r12 * (0.0 - x2) + Me.f[k];
+        for (int k = 0; k < kMhdExtra; k++) oe.f[k] = (e1.f[k] - Me.f[k]) * r12 * (0.0 - x2) + Me.f[k];
     } else {
-        const Ext8 e3 = load_ext(hs, nc, So);
-        const double dist3 = sqrt(sq(fx - cx[So]) + sq(fy - cy[So]));
+        const double dist3 = sqrt(sq(fx - Sx) + sq(fy - Sy));
         const double r23 = 1.0 / (-dist2 - dist3);
+        oi.ro = linear3r(s1.ro, Ms.ro, Ss.ro, r12, r23, x2);
+        oi.p = linear3r(s1.p, Ms.p, Ss.p, r12, r23, x2);
+        oi.u = linear3r(s1.u, Ms.u, Ss.u, r12, r23, x2);
+        oi.v = linear3r(s1.v, Ms.v, Ss.v, r12, r23, x2);
+        oi.Q = linear3r(s1.Q, Ms.Q, Ss.Q, r12, r23, x2);
+        if (oi.ro <= 0.0 || oi.p <= 0.0) *status |= ST_TVD_BAD;  // the reference exits (Gran.cpp:444-455)
 #pragma unroll
-        for (int k = 0; k < kMhdExtra; k++) o.f[k] = linear3r(e1.f[k], Me.f[k], e3.f[k], r12, r23, x2);
+        for (int k = 0; k < kMhdExtra; k++) oe.f[k] = linear3r(e1.f[k], Me.f[k], Se.f[k], r12, r23, x2);
     }
-    if (!(o.f[kXro] > 0.0)) o.f[kXro] = Me.f[kXro];
-    if (!(o.f[kXp] > 0.0)) o.f[kXp] = Me.f[kXp];
-    return o;
+    if (!(oe.f[kXro] > 0.0)) oe.f[kXro] = Me.f[kXro];
+    if (!(oe.f[kXp] > 0.0)) oe.f[kXp] = Me.f[kXp];
 }
 
 // Ion MHD flux through a face with unit normal (n1, n2) moving with normal
@@ -2372,6 +2402,7 @@ __device__ Ext8 tvd_ext(const double* __restrict__ hs, size_t nc, const double* 
 // the region containing W, as HLLC_2d_Korolkov_b_s does for moving faces),
 // and the momentum and field fluxes go back to (x, y).  out: mass, mom x,
 // mom y, mom phi, energy, Bx, By, Bphi, Q.  Returns 1 / max(|SL|, |SR|).
+template <typename TF>
 __device__ __forceinline__ double mhd_face_flux(double ga, const St5& iL, const Ext8& eL, const St5& iR,
                                                 const Ext8& eR, double n1, double n2, double W, double* out) {
     const double t1 = -n2, t2 = n1;
@@ -2395,7 +2426,7 @@ __device__ __forceinline__ double mhd_face_flux(double ga, const St5& iL, const 
     R[7] = eR.f[kXbx] * t1 + eR.f[kXby] * t2;
     R[8] = eR.f[kXbz];
     double F[8], FQ;
-    const double tinv = hlldq_impl<true>(ga, 1.0, L, R, 1.0, 0.0, 0.0, 1.0, 3, F, &FQ, W);
+    const double tinv = hlld_face_moving<TF>(ga, L, R, W, F, &FQ);
     out[0] = F[0];
     out[1] = n1 * F[1] + t1 * F[2];
     out[2] = n2 * F[1] + t2 * F[2];
@@ -2415,7 +2446,10 @@ __device__ __forceinline__ double mhd_face_flux(double ga, const St5& iL, const 
 // 13 flux rows times S to the owner slot and their negatives to the twin,
 // CFL candidates of both fluids.
 template <typename TF>
-__global__ void __launch_bounds__(128) mhd_face_kernel(DevMesh d, gelios_params P, gelios_mhd_params M,
+#ifndef GELIOS_MHD_FACE_MINB
+#define GELIOS_MHD_FACE_MINB 3
+#endif
+__global__ void __launch_bounds__(128, GELIOS_MHD_FACE_MINB) mhd_face_kernel(DevMesh d, gelios_params P, gelios_mhd_params M,
                                                        StepBuffers b, const double* __restrict__ hs,
                                                        double* __restrict__ fl) {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2460,14 +2494,12 @@ __global__ void __launch_bounds__(128) mhd_face_kernel(DevMesh d, gelios_params 
                                 (ft == G_USUALY && (nbf & CF_C1));
             const double pdis = radial ? pow2g(dis, g2) : 1.0;
             if (ft == G_USUALY) {
-                par11 = mk2_usualy_side(b.cur, b.cx, b.cy, b.rp, x2, y2, dis, pdis, par1, x, y, b.rp[K], cf, nb,
-                                        d.u_sd[u], tracked, &status);
-                par2 = mk2_usualy_side(b.cur, b.cx, b.cy, b.rp, x2, y2, dis, pdis, par2, x3, y3, b.rp[nb], nbf, K,
-                                       d.u_sd2[u], tracked, &status);
-                if (!(cf & CF_C1))
-                    e11 = tvd_ext(hs, nc, b.cx, b.cy, x2, y2, ex1, x, y, nb, d.u_sd[u], tracked);
-                if (!(nbf & CF_C1))
-                    e2 = tvd_ext(hs, nc, b.cx, b.cy, x2, y2, e2, x3, y3, K, d.u_sd2[u], tracked);
+                const St5 sN = par2;
+                const Ext8 eN = e2;
+                mhd_usualy_side(b.cur, hs, nc, b.cx, b.cy, b.rp, x2, y2, dis, pdis, par1, ex1, x, y, b.rp[K], cf, nb,
+                                sN, eN, x3, y3, d.u_sd[u], tracked, par11, e11, &status);
+                mhd_usualy_side(b.cur, hs, nc, b.cx, b.cy, b.rp, x2, y2, dis, pdis, sN, eN, x3, y3, b.rp[nb], nbf, K,
+                                par1, ex1, x, y, d.u_sd2[u], tracked, par2, e2, &status);
             } else if (ft == G_INNER_SPHERE) {
                 const double radius = sqrt(sq(x) + sq(y));
                 par11.ro = par11.ro * sq(radius) / sq(dis);
@@ -2487,7 +2519,7 @@ __global__ void __launch_bounds__(128) mhd_face_kernel(DevMesh d, gelios_params 
                 par2.v = -par2.v;
             }
             double F[kMhdFlux];
-            const double tI = mhd_face_flux(P.gamma, par11, e11, par2, e2, n1, n2, W, F);
+            const double tI = mhd_face_flux<TF>(P.gamma, par11, e11, par2, e2, n1, n2, W, F);
             St5 pL, pR;
             pL.ro = e11.f[kXro];
             pL.p = e11.f[kXp];

@@ -192,13 +192,17 @@ def mhd_params(b_lism: float = 0.01, b_angle_deg: float = 30.0, inner_bphi: floa
 
 def mhd_initial(mesh: Mesh, st0: np.ndarray, mp: N.GeliosMhdParams) -> np.ndarray:
     """Extra rows of the MHD form (shape (8, n_cells)) beside the ion state
-    st0: no azimuthal velocity, the uniform LISM field everywhere (divergence
-    free), pickup protons at 1% of the ion density and 10% of its pressure,
-    moving with the ions."""
+    st0: no azimuthal velocity; the uniform LISM field everywhere plus the
+    wind's toroidal field inner_bphi * R1 sin(theta) / r (both divergence
+    free; cells inside R11 keep it as the inner boundary the step does not
+    update); pickup protons at 1% of the ion density and 10% of its
+    pressure, moving with the ions."""
+    x, y = mesh.centroids()
+    r2 = x * x + y * y
     x8 = np.zeros((8, mesh.n_cells))
     x8[1] = mp.lism_bx
     x8[2] = mp.lism_by
-    x8[3] = mp.lism_bz
+    x8[3] = mp.lism_bz + mp.inner_bphi * (1.0 / RR_) * y / r2
     x8[4] = 0.01 * st0[0]
     x8[5] = 0.1 * st0[1]
     x8[6] = st0[2]
