@@ -792,7 +792,8 @@ __device__ inline double hlldq_korolkov(double ga, double kurant, const double* 
 // hlldq_impl<true>(ga, 1, L, R, 1, 0, 0, 1, 3, Pout, PQ, W) with the normal
 // fixed to the x axis of the face frame, written for few registers: the
 // wave speeds and star quantities first, then only the fan region that
-// contains W, one component at a time.  Same arithmetic as hlldq_impl.
+// contains W, one component at a time.  The arithmetic of hlldq_impl, with
+// shared reciprocals in place of repeated quotients.
 // L, R = (ro, Q, p, u_n, u_t, u_phi, B_n, B_t, B_phi); Pout[8] = mass,
 // momentum n, t, phi, B n, t, phi, energy; *PQ = Q flux.  Returns 1/max|S|.
 template <typename T>
@@ -812,57 +813,62 @@ __device__ inline double hlld_face_moving(double gad, const double* L, const dou
     auto sgn = [](T x) { return x > (T)0 ? (T)1 : (x < (T)0 ? (T)-1 : (T)0); };
     const T ro_L = (T)L[0], Q_L = (T)L[1], p_L = (T)L[2], u1 = (T)L[3], v1 = (T)L[4], w1 = (T)L[5];
     const T ro_R = (T)R[0], Q_R = (T)R[1], p_R = (T)R[2], u2 = (T)R[3], v2 = (T)R[4], w2 = (T)R[5];
-    const T bn1 = (T)L[6] / spi4, bt1 = (T)L[7] / spi4, bm1 = (T)L[8] / spi4;
-    const T bn2 = (T)R[6] / spi4, bt2 = (T)R[7] / spi4, bm2 = (T)R[8] / spi4;
+    const T ispi4 = (T)1 / spi4;
+    const T bn1 = (T)L[6] * ispi4, bt1 = (T)L[7] * ispi4, bm1 = (T)L[8] * ispi4;
+    const T bn2 = (T)R[6] * ispi4, bt2 = (T)R[7] * ispi4, bm2 = (T)R[8] * ispi4;
     const T bb_L = sq(bn1) + sq(bt1) + sq(bm1);
     const T bb_R = sq(bn2) + sq(bt2) + sq(bm2);
-    const T uu_L = (sq(u1) + sq(v1) + sq(w1)) / (T)2.0;
-    const T uu_R = (sq(u2) + sq(v2) + sq(w2)) / (T)2.0;
+    const T uu_L = (sq(u1) + sq(v1) + sq(w1)) * (T)0.5;
+    const T uu_R = (sq(u2) + sq(v2) + sq(w2)) * (T)0.5;
     const T cfL = sqrt((ga * p_L + bb_L + sqrt(sq(ga * p_L + bb_L) - (T)4.0 * ga * p_L * sq(bn1))) / ((T)2.0 * ro_L));
     const T cfR = sqrt((ga * p_R + bb_R + sqrt(sq(ga * p_R + bb_R) - (T)4.0 * ga * p_R * sq(bn2))) / ((T)2.0 * ro_R));
     const T SL = dmin_ref(u1, u2) - dmax_ref(cfL, cfR);
     const T SR = dmax_ref(u1, u2) + dmax_ref(cfL, cfR);
-    const T pTL = p_L + bb_L / (T)2.0;
-    const T pTR = p_R + bb_R / (T)2.0;
+    const T pTL = p_L + bb_L * (T)0.5;
+    const T pTR = p_R + bb_R * (T)0.5;
     const T suR = SR - u2, suL = SL - u1;
-    const T SM = (suR * ro_R * u2 - suL * ro_L * u1 - pTR + pTL) / (suR * ro_R - suL * ro_L);
-    const T PTT = (suR * ro_R * pTL - suL * ro_L * pTR + ro_L * ro_R * suR * suL * (u2 - u1)) /
-                       (suR * ro_R - suL * ro_L);
+    const T rden = (T)1 / (suR * ro_R - suL * ro_L);
+    const T SM = (suR * ro_R * u2 - suL * ro_L * u1 - pTR + pTL) * rden;
+    const T PTT = (suR * ro_R * pTL - suL * ro_L * pTR + ro_L * ro_R * suR * suL * (u2 - u1)) * rden;
     const T UU = dmax_ref(fabs(SL), fabs(SR));
     const double time = 1.0 * 1.0 / (double)UU;
-    const T e1 = p_L / g1 + ro_L * uu_L + bb_L / (T)2.0;
-    const T e2 = p_R / g1 + ro_R * uu_R + bb_R / (T)2.0;
+    const T rg1 = (T)1 / g1;
+    const T e1 = p_L * rg1 + ro_L * uu_L + bb_L * (T)0.5;
+    const T e2 = p_R * rg1 + ro_R * uu_R + bb_R * (T)0.5;
     const T sbv1 = u1 * bn1 + v1 * bt1 + w1 * bm1, sbv2 = u2 * bn2 + v2 * bt2 + w2 * bm2;
     // fluxes of the two sides (the normal-field flux is 0)
     const T FLt = u1 * bt1 - v1 * bn1, FLm = u1 * bm1 - w1 * bn1;
     const T FRt = u2 * bt2 - v2 * bn2, FRm = u2 * bm2 - w2 * bn2;
     const T bn = (SR * bn2 - SL * bn1 + (T)0.0 - (T)0.0) / (SR - SL);
     const T bbn = bn * bn;
-    const T ro_LL = ro_L * (SL - u1) / (SL - SM);
-    const T ro_RR = ro_R * (SR - u2) / (SR - SM);
-    const T Q_LL = Q_L * (SL - u1) / (SL - SM);
-    const T Q_RR = Q_R * (SR - u2) / (SR - SM);
+    const T rLM = (T)1 / (SL - SM), rRM = (T)1 / (SR - SM);
+    const T ro_LL = ro_L * (SL - u1) * rLM;
+    const T ro_RR = ro_R * (SR - u2) * rRM;
+    const T Q_LL = Q_L * (SL - u1) * rLM;
+    const T Q_RR = Q_R * (SR - u2) * rRM;
     const T ttL = ro_L * suL * (SL - SM) - bbn;
     const T ttR = ro_R * suR * (SR - SM) - bbn;
     T vLL, wLL, vRR, wRR, btt1, bmm1, btt2, bmm2;
     if (fabs(ttL) >= (T)0.000001) {
-        vLL = v1 - bn * bt1 * (SM - u1) / ttL;
-        wLL = w1 - bn * bm1 * (SM - u1) / ttL;
-        btt1 = bt1 * (ro_L * suL * suL - bbn) / ttL;
-        bmm1 = bm1 * (ro_L * suL * suL - bbn) / ttL;
+        const T r = (T)1 / ttL;
+        vLL = v1 - bn * bt1 * (SM - u1) * r;
+        wLL = w1 - bn * bm1 * (SM - u1) * r;
+        btt1 = bt1 * (ro_L * suL * suL - bbn) * r;
+        bmm1 = bm1 * (ro_L * suL * suL - bbn) * r;
     } else {
         vLL = v1; wLL = w1; btt1 = (T)0.0; bmm1 = (T)0.0;
     }
     if (fabs(ttR) >= (T)0.000001) {
-        vRR = v2 - bn * bt2 * (SM - u2) / ttR;
-        wRR = w2 - bn * bm2 * (SM - u2) / ttR;
-        btt2 = bt2 * (ro_R * suR * suR - bbn) / ttR;
-        bmm2 = bm2 * (ro_R * suR * suR - bbn) / ttR;
+        const T r = (T)1 / ttR;
+        vRR = v2 - bn * bt2 * (SM - u2) * r;
+        wRR = w2 - bn * bm2 * (SM - u2) * r;
+        btt2 = bt2 * (ro_R * suR * suR - bbn) * r;
+        bmm2 = bm2 * (ro_R * suR * suR - bbn) * r;
     } else {
         vRR = v2; wRR = w2; btt2 = (T)0.0; bmm2 = (T)0.0;
     }
-    const T eLL = (e1 * suL + PTT * SM - pTL * u1 + bn * (sbv1 - (SM * bn + vLL * btt1 + wLL * bmm1))) / (SL - SM);
-    const T eRR = (e2 * suR + PTT * SM - pTR * u2 + bn * (sbv2 - (SM * bn + vRR * btt2 + wRR * bmm2))) / (SR - SM);
+    const T eLL = (e1 * suL + PTT * SM - pTL * u1 + bn * (sbv1 - (SM * bn + vLL * btt1 + wLL * bmm1))) * rLM;
+    const T eRR = (e2 * suR + PTT * SM - pTR * u2 + bn * (sbv2 - (SM * bn + vRR * btt2 + wRR * bmm2))) * rRM;
     const T sqrtroLL = sqrt(ro_LL), sqrtroRR = sqrt(ro_RR);
     T SLL = SM - fabs(bn) / sqrtroLL;
     T SRR = SM + fabs(bn) / sqrtroRR;
@@ -913,12 +919,11 @@ __device__ inline double hlld_face_moving(double gad, const double* L, const dou
         if (reg == 1 || reg == 4) {
             for (int i = 0; i < 9; i++) PO[i] = F[i] + Sk * US[i] - Sk * U[i] - W * US[i];
         } else {
-            const T vLLL = (sqrtroLL * vLL + sqrtroRR * vRR + idbn * (btt2 - btt1)) / (sqrtroLL + sqrtroRR);
-            const T wLLL = (sqrtroLL * wLL + sqrtroRR * wRR + idbn * (bmm2 - bmm1)) / (sqrtroLL + sqrtroRR);
-            const T bttt = (sqrtroLL * btt2 + sqrtroRR * btt1 + idbn * sqrtroLL * sqrtroRR * (vRR - vLL)) /
-                                (sqrtroLL + sqrtroRR);
-            const T bmmm = (sqrtroLL * bmm2 + sqrtroRR * bmm1 + idbn * sqrtroLL * sqrtroRR * (wRR - wLL)) /
-                                (sqrtroLL + sqrtroRR);
+            const T rs = (T)1 / (sqrtroLL + sqrtroRR);
+            const T vLLL = (sqrtroLL * vLL + sqrtroRR * vRR + idbn * (btt2 - btt1)) * rs;
+            const T wLLL = (sqrtroLL * wLL + sqrtroRR * wRR + idbn * (bmm2 - bmm1)) * rs;
+            const T bttt = (sqrtroLL * btt2 + sqrtroRR * btt1 + idbn * sqrtroLL * sqrtroRR * (vRR - vLL)) * rs;
+            const T bmmm = (sqrtroLL * bmm2 + sqrtroRR * bmm1 + idbn * sqrtroLL * sqrtroRR * (wRR - wLL)) * rs;
             T eSS;
             if (left)
                 eSS = eLL - idbn * sqrtroLL * ((SM * bn + vLL * btt1 + wLL * bmm1) - (SM * bn + vLLL * bttt + wLLL * bmmm));

@@ -1046,12 +1046,25 @@ __global__ void __launch_bounds__(128, GELIOS_UPDATE_MINB) mk2_update_kernel(Dev
             const double dt = *b.dt_cur;
             const int g0 = d.gstart[c], g1 = d.gstart[c + 1];
             double Pt0 = 0.0, Pt1 = 0.0, Pt2 = 0.0, Pt3 = 0.0, Pt4 = 0.0;
-            for (int g = g0; g < g1; g++) {
-                Pt0 = Pt0 + fl[0 * ng + g];
-                Pt1 = Pt1 + fl[1 * ng + g];
-                Pt2 = Pt2 + fl[2 * ng + g];
-                Pt3 = Pt3 + fl[3 * ng + g];
-                Pt4 = Pt4 + fl[4 * ng + g];
+            if (g1 - g0 == 4) {  // quadrilaterals: all slot loads in flight together
+                double a[5][4];
+#pragma unroll
+                for (int k = 0; k < 5; k++)
+#pragma unroll
+                    for (int j = 0; j < 4; j++) a[k][j] = fl[k * ng + g0 + j];
+                Pt0 = (((Pt0 + a[0][0]) + a[0][1]) + a[0][2]) + a[0][3];
+                Pt1 = (((Pt1 + a[1][0]) + a[1][1]) + a[1][2]) + a[1][3];
+                Pt2 = (((Pt2 + a[2][0]) + a[2][1]) + a[2][2]) + a[2][3];
+                Pt3 = (((Pt3 + a[3][0]) + a[3][1]) + a[3][2]) + a[3][3];
+                Pt4 = (((Pt4 + a[4][0]) + a[4][1]) + a[4][2]) + a[4][3];
+            } else {
+                for (int g = g0; g < g1; g++) {
+                    Pt0 = Pt0 + fl[0 * ng + g];
+                    Pt1 = Pt1 + fl[1 * ng + g];
+                    Pt2 = Pt2 + fl[2 * ng + g];
+                    Pt3 = Pt3 + fl[3 * ng + g];
+                    Pt4 = Pt4 + fl[4 * ng + g];
+                }
             }
             const St5 par1 = load_state(b.cur, c);
             const size_t nc = d.n_cells;
@@ -2598,9 +2611,18 @@ __global__ void __launch_bounds__(128) mhd_update_kernel(DevMesh d, gelios_param
                 double Pt[kMhdFlux];
 #pragma unroll
                 for (int k = 0; k < kMhdFlux; k++) Pt[k] = 0.0;
-                for (int g = g0; g < g1; g++) {
+                if (g1 - g0 == 4) {  // quadrilaterals: all slot loads in flight together
 #pragma unroll
-                    for (int k = 0; k < kMhdFlux; k++) Pt[k] = Pt[k] + fl[k * ng + g];
+                    for (int k = 0; k < kMhdFlux; k++) {
+                        const double* f = fl + k * ng + g0;
+                        const double a0 = f[0], a1 = f[1], a2 = f[2], a3 = f[3];
+                        Pt[k] = (((Pt[k] + a0) + a1) + a2) + a3;
+                    }
+                } else {
+                    for (int g = g0; g < g1; g++) {
+#pragma unroll
+                        for (int k = 0; k < kMhdFlux; k++) Pt[k] = Pt[k] + fl[k * ng + g];
+                    }
                 }
                 const double q1 = src[c], q2 = src[nc + c], q3 = src[2 * nc + c];
                 const double vs1 = b.vs[c], Volume = b.vol[c];
