@@ -48,6 +48,9 @@ WORKLOADS = {
     "mhd_1m": ("ion MHD fluid (HLLD) + pickup protons (HLLC) on the moving grid Setka(480,240,100,220,200,200,300,"
                "300): LISM B=0.01 at 30 deg, seeded fixed charge-exchange sources", "mhd",
                (480, 240, 100, 220, 200, 200, 300, 300)),
+    "sweep64": ("64 independent MHD + pickup-proton instances (FP32 fluxes, FP64 accumulation), Setka(200,100,50,100,"
+                "100,100,150,150) scaled by U(0.5,1.4) per instance (~50k..~400k cells, ~11M in all), seeded inflow "
+                "u~U(0.04,0.08), rho~U(0.002,0.01), Mach~U(1.5,3), |B|~U(0,0.02), angle~U(0,60 deg)", "sweep", None),
     "sweep16": ("16 independent moving-grid instances, Setka(200,100,50,100,100,100,150,150) scaled by "
                 "U(0.5,1.4) per instance (~50k..~400k cells each), batched on each GPU", "sweep", None),
 }
@@ -322,17 +325,30 @@ def run_sweep(args, rank: int, world: int, local: int) -> None:
         dist_mod.init_process_group("nccl", timeout=timedelta(seconds=120))
         dist = dist_mod
     torch.cuda.set_device(local)
-    n_inst = 16
-    seeds = W.splitmix64(41, n_inst)
+    from gelios_2d_b200 import _native as N
+
+    mhd = args.workload == "sweep64"
+    n_inst, seed = (64, 43) if mhd else (16, 41)
+    seeds = W.splitmix64(seed, n_inst)
     sizes = []  # estimated cells per instance, to partition before building
     for i in range(n_inst):
         f = 0.5 + 0.9 * float(seeds[i])
         sizes.append(f * f)
     mine = sw.partition(sizes, world)[rank]
-    inst = sw.instance_set(n_inst, seed=41, scale=(0.5, 1.4), only=mine)
+    if mhd:
+        inst = sw.instance_set_mhd(n_inst, seed=seed, scale=(0.5, 1.4), only=mine)
+        inst = [(m, p.copy(precision=N.PREC_FP32_FLUX), s, x) for m, p, s, x in inst]
+    else:
+        inst = sw.instance_set(n_inst, seed=seed, scale=(0.5, 1.4), only=mine)
     counted = sum(W.counted_cells_mk2(m, p) for m, p, _, _ in inst)
     cells = sum(m.n_cells for m, _, _, _ in inst)
-    B = sw.Sweep(inst, device=local)
+    B = sw.Sweep(inst, device=local, form=N.FORM_MHD_PUI if mhd else N.FORM_MK2)
+    tuned = None
+    if mhd:  # per-instance launch shape and enqueue order (the sweep's autotuner)
+        res = B.autotune(reps=3)
+        tuned = {}
+        for v, _ in res:
+            tuned[str(v)] = tuned.get(str(v), 0) + 1
     streams = [torch.cuda.ExternalStream(S.stream_handle(), device=local) for S in B.items]
     s0 = torch.cuda.current_stream(local)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
@@ -376,20 +392,23 @@ def run_sweep(args, rank: int, world: int, local: int) -> None:
         counted_all = float(t.item())
     value = counted_all * args.steps / (total_ms / 1000.0)
     peak, peak_kind = measured_peaks()
-    achieved = BYTES_PER_CELL["mk2"] * counted_all / world / (total_ms / args.steps / 1000.0) / 1e9
+    bpc = BYTES_PER_CELL["mhd" if mhd else "mk2"]
+    achieved = bpc * counted_all / world / (total_ms / args.steps / 1000.0) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-        "scaling": "strong", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded instances: grid scale, initial field, Monte-Carlo moments)",
-        "config": {"workload": WORKLOADS["sweep16"][0], "instances": n_inst, "instances_on_rank0": len(inst),
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64 (fp32 flux)" if mhd else "f64",
+        "data": "synthetic (seeded instances: grid scale, inflow, initial field, " +
+                ("LISM field, charge-exchange sources)" if mhd else "Monte-Carlo moments)"),
+        "config": {"workload": WORKLOADS[args.workload][0], "instances": n_inst, "instances_on_rank0": len(inst),
                    "cells_rank0": int(cells), "cells_updated_per_step": int(counted_all),
                    "l2": "flushed between timed steps (256 MiB write)",
-                   "parallelism": f"instances partitioned over {world} GPU(s)"},
+                   "parallelism": f"instances partitioned over {world} GPU(s)",
+                   "autotune_variants_rank0": tuned},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "kernel": "batched moving-grid steps of all instances on a GPU",
-                     "bytes_per_cell": BYTES_PER_CELL["mk2"], "avg_launch_us": total_ms / args.steps * 1000.0,
+                     "bytes_per_cell": bpc, "avg_launch_us": total_ms / args.steps * 1000.0,
                      "peak_kind": f"{peak_kind} hbm_gbs (burst copy)"},
         "clocks": clocks,
     }
@@ -419,7 +438,7 @@ def main():
 
     if args.impl == "reference" and rank != 0:
         return  # the reference arm runs on rank 0 only
-    if args.workload == "sweep16":
+    if args.workload in ("sweep16", "sweep64"):
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the sweep workload has no reference arm; "
                               "its instances are the moving-grid step timed by the default workload"}))
@@ -466,6 +485,10 @@ def main():
         params = params.copy(precision=N.PREC_FP32_FLUX)
     S = g.Setka(mesh, params, device=device)
     load_inputs(S, form, st0, mc)
+    tuned = None
+    if form == "mhd":  # launch shape of the face kernel picked on this grid (the library's autotuner)
+        v, tms = S.autotune(N.FORM_MHD_PUI, reps=3)
+        tuned = {"variant": v, "face_kernel_ms": tms}
     fcode = {"mk2": N.FORM_MK2, "k5": N.FORM_5_KOMPONENT, "mhd": N.FORM_MHD_PUI}.get(form, N.FORM_STATIONARY)
     stream = torch.cuda.ExternalStream(S.stream_handle(), device=device)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")
@@ -562,6 +585,7 @@ def main():
                      "kernel": STEP_KERNELS[form], "bytes_per_cell": bpc,
                      "avg_launch_us": step_s * 1e6, "peak_kind": f"{peak_kind} hbm_gbs (burst copy)"},
         "phases_ms": {k: v[0] for k, v in phases.items()},
+        "autotune": tuned,
         "clocks": clocks,
     }
     if args.precision == "fp32flux" and rank == 0:

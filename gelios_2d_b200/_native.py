@@ -152,6 +152,9 @@ def lib() -> C.CDLL:
     L.gelios_upload_mhd.argtypes = [vp, C.c_int, dp]
     L.gelios_download_mhd.argtypes = [vp, C.c_int, dp]
     L.gelios_upload_sources.argtypes = [vp, dp, dp, dp]
+    L.gelios_variant_count.argtypes = [C.c_int]
+    L.gelios_autotune.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+    L.gelios_set_variant.argtypes = [vp, C.c_int, C.c_int32]
     L.gelios_set_inner_cells.argtypes = [vp, C.POINTER(C.c_int32), C.c_int32]
     L.gelios_step.argtypes = [vp, C.c_int, C.c_int, C.POINTER(GeliosStatus)]
     L.gelios_download_points.argtypes = [vp, dp, dp]

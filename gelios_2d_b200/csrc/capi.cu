@@ -105,6 +105,7 @@ struct gelios_ctx {
     gelios_mhd_params mprm{};
     DBuf src_fixed;  // MHD form: fixed charge-exchange sources (3 rows)
     DBuf flux_mhd;   // MHD form: 13 flux rows per face slot, allocated on first use
+    int mhd_face_variant = 0;  // launch shape of the MHD face kernel (gelios_autotune)
     DBuf cen[2];
     DBuf words;    // T[2] (double), dt_acc (u64), counters[2] (u64), status (int)
     DBuf surface;  // Move_surface per-face speeds
@@ -120,12 +121,13 @@ struct gelios_ctx {
     // step reads (state parity and centroid buffer); dropped whenever the
     // topology or the parameters change.
     struct StepGraph {
+        int form = -1;
         int parity = -1;
         const void* cen = nullptr;
         cudaGraphExec_t exec = nullptr;
         int launches = 0;
     };
-    StepGraph graphs[4];
+    StepGraph graphs[8];
     bool graphs_off = false;  // capture failed once: launch directly
     void drop_graphs() {
         for (auto& g : graphs) {
@@ -741,6 +743,7 @@ extern "C" int gelios_download_state(gelios_ctx* ctx, int buf, double* ro, doubl
 extern "C" int gelios_set_mhd_params(gelios_ctx* ctx, const gelios_mhd_params* mp) {
     if (!ctx || !mp) return GELIOS_E_ARG;
     ctx->mprm = *mp;
+    ctx->drop_graphs();  // the boundary data are kernel arguments
     return GELIOS_OK;
 }
 
@@ -769,8 +772,10 @@ extern "C" int gelios_upload_sources(gelios_ctx* ctx, const double* q1, const do
     if (!ctx->have_mesh) return GELIOS_E_STATE;
     GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
     const size_t nc = ctx->d.n_cells;
-    if (ctx->src_fixed.bytes != 3 * nc * sizeof(double) && ctx->src_fixed.alloc(3 * nc * sizeof(double)))
-        return GELIOS_E_CUDA;
+    if (ctx->src_fixed.bytes != 3 * nc * sizeof(double)) {
+        ctx->drop_graphs();  // they hold the buffer about to be replaced
+        if (ctx->src_fixed.alloc(3 * nc * sizeof(double))) return GELIOS_E_CUDA;
+    }
     const double* q[3] = {q1, q2, q3};
     for (int k = 0; k < 3; k++)
         GELIOS_CUDA_TRY(cudaMemcpyAsync(ctx->src_fixed.as<double>() + k * nc, q[k], nc * sizeof(double),
@@ -879,15 +884,44 @@ int enqueue_mk2(gelios_ctx* ctx, const StepBuffers& b) {
     return nm + 4 + nfl + nsv;
 }
 
-// One moving-grid step: replays the instantiated graph of this step's
-// buffers (captured on first use), or launches directly while phase timing
-// is on or if capture is unavailable.  Returns the kernel count or a
-// negative error code.
-int step_mk2(gelios_ctx* ctx, const StepBuffers& b) {
-    if (ctx->timing || ctx->graphs_off) return enqueue_mk2(ctx, b);
+// Enqueues one step of the MHD + pickup form on the main stream: Move_surface
+// + rails, the face units, the cell update, the commit.
+int enqueue_mhd(gelios_ctx* ctx, const StepBuffers& b) {
+    const DevMesh& d = ctx->d;
+    const gelios_params& P = ctx->prm;
+    cudaStream_t s = ctx->stream;
+    const int cur = b.cur[0] == ctx->field(0, 0) ? 0 : 1, nxt = cur ^ 1;
+    cudaEvent_t e1 = ctx->phase_begin();
+    const int nm = launch_motion(d, P, b, ctx->surface.as<double>(), s);
+    ctx->phase_end(2, e1, nm);
+    cudaEvent_t e3 = ctx->phase_begin();
+    launch_mhd_faces(d, P, ctx->mprm, b, ctx->hstate[cur].as<double>(), ctx->flux_mhd.as<double>(), s,
+                     ctx->mhd_face_variant);
+    ctx->phase_end(1, e3, 1);
+    cudaEvent_t e5 = ctx->phase_begin();
+    launch_mhd_update(d, P, b, ctx->flux_mhd.as<double>(), ctx->src_fixed.as<double>(), ctx->hstate[cur].as<double>(),
+                      ctx->hstate[nxt].as<double>(), s);
+    ctx->phase_end(3, e5, 1);
+    cudaEvent_t e4 = ctx->phase_begin();
+    launch_commit(d, b, s);
+    ctx->phase_end(4, e4, 1);
+    GELIOS_CUDA_TRY(cudaGetLastError());
+    return nm + 3;
+}
+
+int enqueue_form(gelios_ctx* ctx, const StepBuffers& b, int form) {
+    return form == GELIOS_FORM_MHD_PUI ? enqueue_mhd(ctx, b) : enqueue_mk2(ctx, b);
+}
+
+// One moving-grid step (MK2 or MHD form): replays the instantiated graph of
+// this form and these buffers (captured on first use), or launches directly
+// while phase timing is on or if capture is unavailable.  Returns the kernel
+// count or a negative error code.
+int step_graph(gelios_ctx* ctx, const StepBuffers& b, int form) {
+    if (ctx->timing || ctx->graphs_off) return enqueue_form(ctx, b, form);
     const int parity = b.cur[0] == ctx->field(0, 0) ? 0 : 1;
     for (auto& g : ctx->graphs)
-        if (g.exec && g.parity == parity && g.cen == b.cx) {
+        if (g.exec && g.form == form && g.parity == parity && g.cen == b.cx) {
             GELIOS_CUDA_TRY(cudaGraphLaunch(g.exec, ctx->stream));
             return g.launches;
         }
@@ -895,9 +929,9 @@ int step_mk2(gelios_ctx* ctx, const StepBuffers& b) {
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         cudaGetLastError();
         ctx->graphs_off = true;
-        return enqueue_mk2(ctx, b);
+        return enqueue_form(ctx, b, form);
     }
-    const int n = enqueue_mk2(ctx, b);
+    const int n = enqueue_form(ctx, b, form);
     cudaGraph_t graph = nullptr;
     const cudaError_t e = cudaStreamEndCapture(s, &graph);
     cudaGraphExec_t exec = nullptr;
@@ -905,7 +939,7 @@ int step_mk2(gelios_ctx* ctx, const StepBuffers& b) {
         if (graph) cudaGraphDestroy(graph);
         cudaGetLastError();
         ctx->graphs_off = true;
-        return enqueue_mk2(ctx, b);
+        return enqueue_form(ctx, b, form);
     }
     cudaGraphDestroy(graph);
     gelios_ctx::StepGraph* slot = &ctx->graphs[0];
@@ -915,6 +949,7 @@ int step_mk2(gelios_ctx* ctx, const StepBuffers& b) {
             break;
         }
     if (slot->exec) cudaGraphExecDestroy(slot->exec);
+    slot->form = form;
     slot->parity = parity;
     slot->cen = b.cx;
     slot->exec = exec;
@@ -969,7 +1004,10 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             return GELIOS_E_STATE;
         }
         const size_t fb = static_cast<size_t>(kMhdFluxRows) * d.n_slots * sizeof(double);
-        if (ctx->flux_mhd.bytes != fb && ctx->flux_mhd.alloc(fb)) return GELIOS_E_CUDA;
+        if (ctx->flux_mhd.bytes != fb) {
+            ctx->drop_graphs();
+            if (ctx->flux_mhd.alloc(fb)) return GELIOS_E_CUDA;
+        }
     }
     const bool cached_form = form == GELIOS_FORM_MK2 || mhd;  // forms that refill the cache partially
     if (!ctx->cen_valid || (!cached_form && ctx->cen_rp_partial)) {
@@ -1006,20 +1044,9 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             b.rp_next = cn + 2 * ncz;
             b.vs_next = cn + 3 * ncz;
             b.vol_next = cn + 4 * ncz;
-            cudaEvent_t e1 = ctx->phase_begin();
-            const int nm = launch_motion(d, P, b, ctx->surface.as<double>(), s);
-            ctx->phase_end(2, e1, nm);
-            cudaEvent_t e3 = ctx->phase_begin();
-            launch_mhd_faces(d, P, ctx->mprm, b, ctx->hstate[cur].as<double>(), ctx->flux_mhd.as<double>(), s);
-            ctx->phase_end(1, e3, 1);
-            cudaEvent_t e5 = ctx->phase_begin();
-            launch_mhd_update(d, P, b, ctx->flux_mhd.as<double>(), ctx->src_fixed.as<double>(),
-                              ctx->hstate[cur].as<double>(), ctx->hstate[nxt].as<double>(), s);
-            ctx->phase_end(3, e5, 1);
-            cudaEvent_t e4 = ctx->phase_begin();
-            launch_commit(d, b, s);
-            ctx->phase_end(4, e4, 1);
-            launches += nm + 3;
+            const int n = step_graph(ctx, b, GELIOS_FORM_MHD_PUI);
+            if (n < 0) return n;
+            launches += n;
         } else if (form == GELIOS_FORM_MK2) {
             double* cc = (st & 1) ? cen1 : cen0;
             double* cn = (st & 1) ? cen0 : cen1;
@@ -1033,7 +1060,7 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             b.rp_next = cn + 2 * static_cast<size_t>(d.n_cells);
             b.vs_next = cn + 3 * ncz;
             b.vol_next = cn + 4 * ncz;
-            const int n = step_mk2(ctx, b);
+            const int n = step_graph(ctx, b, GELIOS_FORM_MK2);
             if (n < 0) return n;
             launches += n;
         } else if (form == GELIOS_FORM_5_KOMPONENT) {
@@ -1103,6 +1130,106 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
         status->dt = r.T[nsteps & 1];
         if (!(status->dt == status->dt)) status->flags |= ST_DT_BAD;
     }
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_variant_count(int form) { return form == GELIOS_FORM_MHD_PUI ? kMhdFaceVariants : 1; }
+
+extern "C" int gelios_set_variant(gelios_ctx* ctx, int form, int32_t variant) {
+    if (!ctx || variant < 0 || variant >= gelios_variant_count(form)) return GELIOS_E_ARG;
+    if (form == GELIOS_FORM_MHD_PUI) {
+        ctx->mhd_face_variant = variant;
+        ctx->drop_graphs();  // the captured steps hold the old launch shape
+    }
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_autotune(gelios_ctx* ctx, int form, int reps, int32_t* variant, double* ms) {
+    if (!ctx || reps < 1) return GELIOS_E_ARG;
+    if (form != GELIOS_FORM_MHD_PUI) {
+        if (variant) *variant = 0;
+        if (ms) *ms = 0.0;
+        return GELIOS_OK;
+    }
+    if (!ctx->have_mesh) return GELIOS_E_STATE;
+    const DevMesh& d = ctx->d;
+    GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    const size_t fb = static_cast<size_t>(kMhdFluxRows) * d.n_slots * sizeof(double);
+    if (ctx->flux_mhd.bytes != fb) {
+        ctx->drop_graphs();
+        if (ctx->flux_mhd.alloc(fb)) return GELIOS_E_CUDA;
+    }
+    // the words a step starts from (dt0, empty accumulator); reset again below
+    struct Words {
+        double T[2];
+        unsigned long long acc;
+        unsigned long long counters[2];
+        int status;
+        int pad[5];
+    } w{};
+    w.T[0] = w.T[1] = ctx->prm.dt0;
+    w.acc = 0x7ff0000000000000ULL;
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(ctx->words.p, &w, sizeof(w), cudaMemcpyHostToDevice, s));
+    const size_t nc = d.n_cells;
+    double* cen0 = ctx->cen[0].as<double>();
+    if (!ctx->cen_valid || ctx->cen_rp_partial) {
+        launch_centroid(d, d.X, d.Y, cen0, cen0 + nc, cen0 + 2 * nc, ctx->prm.gamma, s, cen0 + 3 * nc, cen0 + 4 * nc);
+        ctx->cen_valid = true;
+        ctx->cen_rp_partial = false;
+    }
+    StepBuffers b;
+    for (int k = 0; k < 5; k++) {
+        b.cur[k] = ctx->field(0, k);
+        b.nxt[k] = ctx->field(1, k);
+    }
+    b.cx = cen0;
+    b.cy = cen0 + nc;
+    b.rp = cen0 + 2 * nc;
+    b.vs = cen0 + 3 * nc;
+    b.vol = cen0 + 4 * nc;
+    b.dt_cur = ctx->T();
+    b.dt_next = ctx->T() + 1;
+    b.dt_acc = ctx->acc();
+    b.counters = ctx->counters();
+    b.status = ctx->status();
+    cudaEvent_t e0, e1;
+    GELIOS_CUDA_TRY(cudaEventCreate(&e0));
+    GELIOS_CUDA_TRY(cudaEventCreate(&e1));
+    int best = 0;
+    double best_ms = 0.0;
+    for (int v = 0; v < kMhdFaceVariants; v++) {
+        launch_mhd_faces(d, ctx->prm, ctx->mprm, b, ctx->hstate[0].as<double>(), ctx->flux_mhd.as<double>(), s, v);
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < reps; r++)
+            launch_mhd_faces(d, ctx->prm, ctx->mprm, b, ctx->hstate[0].as<double>(), ctx->flux_mhd.as<double>(), s,
+                             v);
+        cudaEventRecord(e1, s);
+        cudaError_t err = cudaEventSynchronize(e1);
+        float t = 0.f;
+        if (err == cudaSuccess) err = cudaEventElapsedTime(&t, e0, e1);
+        if (err != cudaSuccess) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            set_error(std::string("gelios_autotune: ") + cudaGetErrorString(err));
+            return GELIOS_E_CUDA;
+        }
+        const double m = static_cast<double>(t) / reps;
+        if (v == 0 || m < best_ms) {
+            best = v;
+            best_ms = m;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(ctx->words.p, &w, sizeof(w), cudaMemcpyHostToDevice, s));
+    GELIOS_CUDA_TRY(cudaStreamSynchronize(s));
+    if (best != ctx->mhd_face_variant) {
+        ctx->mhd_face_variant = best;
+        ctx->drop_graphs();
+    }
+    if (variant) *variant = best;
+    if (ms) *ms = best_ms;
     return GELIOS_OK;
 }
 

@@ -2454,15 +2454,13 @@ __device__ __forceinline__ double mhd_face_flux(double ga, const St5& iL, const 
 
 // One face unit of the MHD form, after the motion: reconstructions of both
 // sides (ion rows: the moving-grid rules of Setka.cpp:10204-10276, extra
-// rows: tvd_ext / get_par_ext) on the pre-motion points, face speed from
-// the moved points, HLLD for the ions and HLLC for the pickup protons,
+// rows: mhd_usualy_side / get_par_ext) on the pre-motion points, face speed
+// from the moved points, HLLD for the ions and HLLC for the pickup protons,
 // 13 flux rows times S to the owner slot and their negatives to the twin,
-// CFL candidates of both fluids.
-template <typename TF>
-#ifndef GELIOS_MHD_FACE_MINB
-#define GELIOS_MHD_FACE_MINB 3
-#endif
-__global__ void __launch_bounds__(128, GELIOS_MHD_FACE_MINB) mhd_face_kernel(DevMesh d, gelios_params P, gelios_mhd_params M,
+// CFL candidates of both fluids.  BLOCK x MINB: the launch shape (threads
+// per block, minimum resident blocks per SM, which caps the registers).
+template <typename TF, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) mhd_face_kernel(DevMesh d, gelios_params P, gelios_mhd_params M,
                                                        StepBuffers b, const double* __restrict__ hs,
                                                        double* __restrict__ fl) {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2804,13 +2802,33 @@ void launch_hlld_batch(const gelios_params& P, int n, const double* in, double* 
 void launch_godunov_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s) {
     godunov_batch_kernel<<<blocks_for(n, 2), 64, 0, s>>>(P, n, in, out);
 }
-void launch_mhd_faces(const DevMesh& d, const gelios_params& P, const gelios_mhd_params& M, const StepBuffers& b,
-                      const double* hcur, double* fl, cudaStream_t s) {
-    if (d.n_units <= 0) return;
+namespace {
+template <int BLOCK, int MINB>
+void mhd_faces_shape(const DevMesh& d, const gelios_params& P, const gelios_mhd_params& M, const StepBuffers& b,
+                     const double* hcur, double* fl, cudaStream_t s) {
+    const int nb = blocks_for(d.n_units, BLOCK);
     if (P.precision == GELIOS_PREC_FP32_FLUX)
-        mhd_face_kernel<float><<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, M, b, hcur, fl);
+        mhd_face_kernel<float, BLOCK, MINB><<<nb, BLOCK, 0, s>>>(d, P, M, b, hcur, fl);
     else
-        mhd_face_kernel<double><<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, M, b, hcur, fl);
+        mhd_face_kernel<double, BLOCK, MINB><<<nb, BLOCK, 0, s>>>(d, P, M, b, hcur, fl);
+}
+}  // namespace
+
+const char* mhd_face_variant_name(int v) {
+    static const char* names[kMhdFaceVariants] = {"128x3", "128x1", "128x4", "64x6", "64x3", "256x1"};
+    return (v >= 0 && v < kMhdFaceVariants) ? names[v] : "?";
+}
+void launch_mhd_faces(const DevMesh& d, const gelios_params& P, const gelios_mhd_params& M, const StepBuffers& b,
+                      const double* hcur, double* fl, cudaStream_t s, int variant) {
+    if (d.n_units <= 0) return;
+    switch (variant) {
+        case 1: mhd_faces_shape<128, 1>(d, P, M, b, hcur, fl, s); break;
+        case 2: mhd_faces_shape<128, 4>(d, P, M, b, hcur, fl, s); break;
+        case 3: mhd_faces_shape<64, 6>(d, P, M, b, hcur, fl, s); break;
+        case 4: mhd_faces_shape<64, 3>(d, P, M, b, hcur, fl, s); break;
+        case 5: mhd_faces_shape<256, 1>(d, P, M, b, hcur, fl, s); break;
+        default: mhd_faces_shape<128, 3>(d, P, M, b, hcur, fl, s); break;
+    }
 }
 void launch_mhd_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
                        const double* src, const double* hcur, double* hnxt, cudaStream_t s) {

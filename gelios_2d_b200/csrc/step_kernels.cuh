@@ -131,8 +131,13 @@ void launch_k5_cells(const DevMesh& d, const gelios_params& P, const StepBuffers
 // MHD + pickup-proton form: extra rows (8 x n_cells: w, Bx, By, Bz, pickup
 // ro, p, u, v), 13 flux rows per slot, fixed sources (3 x n_cells).
 constexpr int kMhdFluxRows = 13;
+// The face kernel has kMhdFaceVariants launch shapes (threads per block x
+// minimum blocks per SM); variant 0 is the default, gelios_autotune picks
+// the fastest for a grid.  All shapes give the same bits.
+constexpr int kMhdFaceVariants = 6;
+const char* mhd_face_variant_name(int v);
 void launch_mhd_faces(const DevMesh& d, const gelios_params& P, const gelios_mhd_params& M, const StepBuffers& b,
-                      const double* hcur, double* fl, cudaStream_t s);
+                      const double* hcur, double* fl, cudaStream_t s, int variant = 0);
 void launch_mhd_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
                        const double* src, const double* hcur, double* hnxt, cudaStream_t s);
 void launch_hllc_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s);

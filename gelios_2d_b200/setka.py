@@ -185,6 +185,18 @@ class Setka:
         f = lambda a: np.ascontiguousarray(a, np.float64).ravel()  # noqa: E731
         N.check(self._L.gelios_upload_sources(self._h, f(q1), f(q2), f(q3)), "gelios_upload_sources")
 
+    def autotune(self, form: int = N.FORM_MHD_PUI, reps: int = 5) -> tuple[int, float]:
+        """Time every launch shape of the form's dominant kernel on this grid
+        and state, keep the fastest; returns (variant, mean ms).  The state
+        and the points are not changed."""
+        v = C.c_int32()
+        ms = C.c_double()
+        N.check(self._L.gelios_autotune(self._h, int(form), int(reps), C.byref(v), C.byref(ms)), "gelios_autotune")
+        return int(v.value), float(ms.value)
+
+    def set_variant(self, form: int, variant: int):
+        N.check(self._L.gelios_set_variant(self._h, int(form), int(variant)), "gelios_set_variant")
+
     def set_hydrogen(self, buf: int, h16: np.ndarray):
         """ro, p, u, v of the hydrogen fluids H1..H4 of Cell::par[buf]
         (shape (16, n_cells))."""

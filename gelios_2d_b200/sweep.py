@@ -49,7 +49,13 @@ class Sweep:
             S = Setka(mesh, params, device)
             S.set_par(0, st0)
             S.set_par(1, st0)
-            if mc is not None:
+            if form == N.FORM_MHD_PUI:
+                mp, x0, src = mc  # boundary data, extra rows, fixed sources
+                S.set_mhd_params(mp)
+                S.set_mhd(0, x0)
+                S.set_mhd(1, x0)
+                S.set_sources(*src)
+            elif mc is not None:
                 S.set_mc(*mc)
             self.items.append(S)
 
@@ -60,10 +66,20 @@ class Sweep:
     def cells(self) -> list[int]:
         return [S.mesh.n_cells for S in self.items]
 
+    def autotune(self, reps: int = 3) -> list[tuple[int, float]]:
+        """Per-instance schedule: every instance gets the launch shape of its
+        dominant kernel that is fastest on its own grid (gelios_autotune),
+        and the batch enqueues instances in decreasing order of their tuned
+        kernel time, so the longest start first and the short ones fill in
+        behind them.  Returns (variant, ms) per instance."""
+        res = [S.autotune(self.form, reps) for S in self.items]
+        self.order = sorted(range(len(self.items)), key=lambda i: (-res[i][1], i))
+        return res
+
     def step_async(self, n: int = 1):
         """Enqueue ``n`` steps on every instance without waiting."""
-        for S in self.items:
-            S.step_async(self.form, n)
+        for i in getattr(self, "order", range(len(self.items))):
+            self.items[i].step_async(self.form, n)
 
     def synchronize(self):
         for S in self.items:
@@ -104,6 +120,51 @@ def instance_set(n: int, seed: int = 41, scale=(0.5, 1.4), only=None) -> list[tu
         mesh = Mesh.setka(*dims)
         params = N.reference_params()
         out.append((mesh, params, W.init_conditions_reference(mesh), W.mc_fields(mesh, seed=seed + i)))
+    return out
+
+
+def inflow_params(u: np.ndarray) -> dict:
+    """Inflow of one MHD sweep instance from five uniform draws: LISM speed
+    U(0.04, 0.08) and density U(0.002, 0.01) in units of the wind at 1 AU,
+    Mach U(1.5, 3), |B| U(0, 0.02), field angle to the inflow U(0, 60 deg).
+    Speeds and densities map to the grid's units through the inner-sphere
+    wind (speed chi, density 116.667 at 1 AU: Setka::Init_conditions,
+    Setka.cpp:5149-5203); the inflow runs along -x."""
+    chi, ro_wind = 36.1275, 116.667
+    g = 5.0 / 3.0
+    u_lism = 0.04 + 0.04 * float(u[0])
+    ro_lism = 0.002 + 0.008 * float(u[1])
+    mach = 1.5 + 1.5 * float(u[2])
+    ro = ro_wind * ro_lism
+    vel = chi * u_lism
+    return {"in_ro": ro, "in_u": -vel, "in_p": ro * vel * vel / (g * mach * mach),
+            "b_lism": 0.02 * float(u[3]), "b_angle_deg": 60.0 * float(u[4])}
+
+
+def instance_set_mhd(n: int, seed: int = 43, scale=(0.5, 1.4), only=None) -> list[tuple]:
+    """``n`` seeded instances of the MHD + pickup-proton step: uneven rail
+    grids as in :func:`instance_set`, each with its own inflow
+    (:func:`inflow_params`): the Input boundary state, the LISM cells of the
+    reference's initial field set to it, its LISM field, seeded fixed
+    charge-exchange sources.  Returns (mesh, params, state, (mhd params,
+    extra rows, sources)) per instance."""
+    from . import workloads as W
+
+    u = W.splitmix64(seed, n)
+    draws = W.splitmix64(seed + 1, 5 * n).reshape(n, 5)
+    out = []
+    for i in (range(n) if only is None else only):
+        f = scale[0] + (scale[1] - scale[0]) * float(u[i])
+        dims = tuple(max(lo, int(round(b * f))) for b, lo in zip(BASE_DIMS, MIN_DIMS))
+        mesh = Mesh.setka(*dims)
+        inflow = inflow_params(draws[i])
+        params = N.reference_params(in_ro=inflow["in_ro"], in_p=inflow["in_p"], in_u=inflow["in_u"])
+        st0 = W.init_conditions_reference(mesh)
+        lism = mesh["cell_type"] == 4  # C_5, the cells Init_conditions fills with the inflow state
+        st0[0][lism], st0[1][lism], st0[2][lism], st0[3][lism] = (inflow["in_ro"], inflow["in_p"],
+                                                                  inflow["in_u"], 0.0)
+        mp = W.mhd_params(b_lism=inflow["b_lism"], b_angle_deg=inflow["b_angle_deg"])
+        out.append((mesh, params, st0, (mp, W.mhd_initial(mesh, st0, mp), W.mhd_sources(mesh, seed=seed + i))))
     return out
 
 

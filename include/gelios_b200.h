@@ -238,6 +238,21 @@ int gelios_download_mhd(gelios_ctx *ctx, int buf, double *rows8);
  * momentum, energy (n_cells each); read by GELIOS_FORM_MHD_PUI. */
 int gelios_upload_sources(gelios_ctx *ctx, const double *q1, const double *q2, const double *q3);
 
+/* ---- autotuning of launch shapes (no counterpart in the reference) ---------
+ * The dominant kernel of the MHD form (its face kernel) has
+ * gelios_variant_count(form) launch shapes (threads per block x resident
+ * blocks per SM, i.e. a register cap); all give the same bits.
+ * gelios_autotune times each shape on the context's grid and current state
+ * (`reps` launches each, CUDA events on the context stream; only scratch
+ * buffers are written, the state and the points are not touched), keeps the
+ * fastest for the steps that follow and returns its index and mean time in
+ * ms (either pointer may be NULL).  gelios_set_variant picks a shape by
+ * hand (GELIOS_E_ARG outside [0, count)).  Forms without variants: count 1,
+ * autotune returns variant 0. */
+int gelios_variant_count(int form);
+int gelios_autotune(gelios_ctx *ctx, int form, int reps, int32_t *variant, double *ms);
+int gelios_set_variant(gelios_ctx *ctx, int form, int32_t variant);
+
 /* ---- per-face solvers on the device (known-answer checks) ------------------
  * Batched HLLC_2d_Korolkov_b_s (Setka.cpp:10484-10700): in[n*16] =
  * roL,QL,pL,v1L,v2L, roR,QR,pR,v1R,v2R, W, n1, n2, rad, metod, nul_potok;

@@ -165,3 +165,73 @@ def test_mhd_fp32_flux_close_to_fp64():
     dev, _ = device_run(mesh, P32, mp, st0, x0, src, 4)
     assert rel_err(dev.par(0), ora.get_state(0)) <= 1e-4
     assert ext_err(dev.mhd(0), ora.get_mhd(0), ora.get_state(0)) <= 1e-4
+
+
+@pytest.mark.gpu
+def test_mhd_graph_matches_direct_launches():
+    """The captured step graph (default) and direct launches (phase timing
+    on) give the same bits."""
+    mesh, P, mp, st0, x0, src = setup(MEDIUM)
+    d1, _ = device_run(mesh, P, mp, st0, x0, src, 5)
+    d2 = g.Setka(mesh, P)
+    d2.set_mhd_params(mp)
+    for b in (0, 1):
+        d2.set_par(b, st0)
+        d2.set_mhd(b, x0)
+    d2.set_sources(*src)
+    d2.set_phase_timing(True)
+    d2.Go_MHD_pickup(5)
+    assert np.array_equal(d1.par(1), d2.par(1)) and np.array_equal(d1.mhd(1), d2.mhd(1))
+    assert np.array_equal(d1.points()[0], d2.points()[0])
+
+
+def test_variant_counts():
+    L = N.lib()
+    assert L.gelios_variant_count(N.FORM_MHD_PUI) == 6
+    for f in (N.FORM_STATIONARY, N.FORM_MK2, N.FORM_INNER_MK2, N.FORM_5_KOMPONENT):
+        assert L.gelios_variant_count(f) == 1
+
+
+def test_sweep_inflow_draws_in_configured_ranges():
+    from gelios_2d_b200 import sweep as sw
+
+    draws = W.splitmix64(7, 5 * 200).reshape(200, 5)
+    chi, ro_wind, g_ = 36.1275, 116.667, 5.0 / 3.0
+    for d in draws:
+        f = sw.inflow_params(d)
+        u, ro = -f["in_u"] / chi, f["in_ro"] / ro_wind
+        mach = np.sqrt(f["in_ro"] * f["in_u"] ** 2 / (g_ * f["in_p"]))
+        assert 0.04 <= u <= 0.08 and 0.002 <= ro <= 0.01 and 1.5 <= mach <= 3.0 + 1e-12
+        assert 0.0 <= f["b_lism"] <= 0.02 and 0.0 <= f["b_angle_deg"] <= 60.0
+    inst = sw.instance_set_mhd(8, only=[3])
+    mesh, P, st0, (mp, x0, src) = inst[0]
+    lism = mesh["cell_type"] == 4
+    assert np.all(st0[0][lism] == P.in_ro) and np.all(st0[2][lism] == P.in_u)
+    assert x0.shape == (8, mesh.n_cells) and len(src) == 3
+
+
+@pytest.mark.gpu
+def test_mhd_launch_shapes_give_same_bits_and_autotune_keeps_state():
+    mesh, P, mp, st0, x0, src = setup(MEDIUM)
+    ref, _ = device_run(mesh, P, mp, st0, x0, src, 3)
+    n = N.lib().gelios_variant_count(N.FORM_MHD_PUI)
+
+    def fresh():
+        d = g.Setka(mesh, P)
+        d.set_mhd_params(mp)
+        for b in (0, 1):
+            d.set_par(b, st0)
+            d.set_mhd(b, x0)
+        d.set_sources(*src)
+        return d
+
+    for v in range(1, n):
+        d = fresh()
+        d.set_variant(N.FORM_MHD_PUI, v)
+        d.Go_MHD_pickup(3)
+        assert np.array_equal(d.par(1), ref.par(1)) and np.array_equal(d.mhd(1), ref.mhd(1)), v
+    d = fresh()
+    v, ms = d.autotune(N.FORM_MHD_PUI, reps=2)
+    assert 0 <= v < n and ms > 0.0
+    d.Go_MHD_pickup(3)
+    assert np.array_equal(d.par(1), ref.par(1)) and np.array_equal(d.mhd(1), ref.mhd(1))
