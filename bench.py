@@ -177,7 +177,8 @@ def measured_peaks() -> tuple[float, str]:
 
 
 PROFILE_SUMMARY = {"mk2_200k": "mk2_step_setka200k.md", "mk2_1m": "mk2_step_setka1m.md",
-                   "plain": "stationary_step_polar180x120.md"}
+                   "plain": "stationary_step_polar180x120.md", "mhd_200k": "mhd_step_setka200k.md",
+                   "mhd_1m": "mhd_step_setka1m.md"}
 
 
 def ncu_traffic(workload: str):
