@@ -153,6 +153,8 @@ def lib() -> C.CDLL:
     L.gelios_download_mhd.argtypes = [vp, C.c_int, dp]
     L.gelios_upload_sources.argtypes = [vp, dp, dp, dp]
     L.gelios_variant_count.argtypes = [C.c_int]
+    L.gelios_io_rows.argtypes = [C.c_int]
+    L.gelios_run_streamed.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
     L.gelios_autotune.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
     L.gelios_set_variant.argtypes = [vp, C.c_int, C.c_int32]
     L.gelios_set_inner_cells.argtypes = [vp, C.POINTER(C.c_int32), C.c_int32]

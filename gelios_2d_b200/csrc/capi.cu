@@ -106,6 +106,12 @@ struct gelios_ctx {
     DBuf src_fixed;  // MHD form: fixed charge-exchange sources (3 rows)
     DBuf flux_mhd;   // MHD form: 13 flux rows per face slot, allocated on first use
     int mhd_face_variant = 0;  // launch shape of the MHD face kernel (gelios_autotune)
+    // streamed host I/O (gelios_run_streamed): copy streams, staging
+    // buffers and their events, created on first use
+    cudaStream_t io_h2d = nullptr, io_d2h = nullptr;
+    DBuf io_in[2], io_out[2];
+    cudaEvent_t ev_in_ready[2] = {nullptr, nullptr}, ev_in_free[2] = {nullptr, nullptr};
+    cudaEvent_t ev_out_ready[2] = {nullptr, nullptr}, ev_out_free[2] = {nullptr, nullptr};
     DBuf cen[2];
     DBuf words;    // T[2] (double), dt_acc (u64), counters[2] (u64), status (int)
     DBuf surface;  // Move_surface per-face speeds
@@ -275,13 +281,16 @@ extern "C" void gelios_destroy(gelios_ctx* ctx) {
         cudaStreamSynchronize(ctx->stream);
         cudaStreamDestroy(ctx->stream);
     }
-    for (cudaStream_t* sp : {&ctx->side})
+    for (cudaStream_t* sp : {&ctx->side, &ctx->io_h2d, &ctx->io_d2h})
         if (*sp) {
             cudaStreamSynchronize(*sp);
             cudaStreamDestroy(*sp);
         }
     for (cudaEvent_t e : {ctx->ev_fork, ctx->ev_recon, ctx->ev_rails, ctx->ev_tracked})
         if (e) cudaEventDestroy(e);
+    for (int j = 0; j < 2; j++)
+        for (cudaEvent_t e : {ctx->ev_in_ready[j], ctx->ev_in_free[j], ctx->ev_out_ready[j], ctx->ev_out_free[j]})
+            if (e) cudaEventDestroy(e);
     delete ctx;
 }
 
@@ -1130,6 +1139,69 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
         status->dt = r.T[nsteps & 1];
         if (!(status->dt == status->dt)) status->flags |= ST_DT_BAD;
     }
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_io_rows(int form) {
+    return 5 + (form == GELIOS_FORM_5_KOMPONENT ? 16 : form == GELIOS_FORM_MHD_PUI ? 8 : 0);
+}
+
+extern "C" int gelios_run_streamed(gelios_ctx* ctx, int form, int nsteps, const double* const* host_in,
+                                   double* const* host_out) {
+    if (!ctx || nsteps < 0 || (nsteps > 0 && (!host_in || !host_out))) return GELIOS_E_ARG;
+    if (!ctx->have_mesh) return GELIOS_E_STATE;
+    for (int k = 0; k < nsteps; k++)
+        if (!host_in[k] || !host_out[k]) return GELIOS_E_ARG;
+    GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
+    const size_t nc = ctx->d.n_cells;
+    const int extra = gelios_io_rows(form) - 5;
+    const size_t bytes = static_cast<size_t>(gelios_io_rows(form)) * nc * sizeof(double);
+    if (!ctx->io_h2d) {
+        GELIOS_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->io_h2d, cudaStreamNonBlocking));
+        GELIOS_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->io_d2h, cudaStreamNonBlocking));
+        for (int j = 0; j < 2; j++)
+            for (cudaEvent_t* e : {&ctx->ev_in_ready[j], &ctx->ev_in_free[j], &ctx->ev_out_ready[j], &ctx->ev_out_free[j]})
+                GELIOS_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
+    for (int j = 0; j < 2; j++) {
+        if (ctx->io_in[j].bytes != bytes && ctx->io_in[j].alloc(bytes)) return GELIOS_E_CUDA;
+        if (ctx->io_out[j].bytes != bytes && ctx->io_out[j].alloc(bytes)) return GELIOS_E_CUDA;
+    }
+    cudaStream_t s = ctx->stream;
+    // staging buffers are free at the start: the previous call ended with a synchronisation
+    int64_t launches = 0;
+    for (int k = 0; k < nsteps; k++) {
+        const int j = k & 1;
+        double* in = ctx->io_in[j].as<double>();
+        double* out = ctx->io_out[j].as<double>();
+        // input of call k: host -> staging (after call k-2 has read this staging buffer)
+        if (k >= 2) GELIOS_CUDA_TRY(cudaStreamWaitEvent(ctx->io_h2d, ctx->ev_in_free[j], 0));
+        GELIOS_CUDA_TRY(cudaMemcpyAsync(in, host_in[k], bytes, cudaMemcpyHostToDevice, ctx->io_h2d));
+        GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_in_ready[j], ctx->io_h2d));
+        // staging -> par[0] on the step's stream, then the step
+        GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_in_ready[j], 0));
+        GELIOS_CUDA_TRY(cudaMemcpyAsync(ctx->state[0].p, in, 5 * nc * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        if (extra)
+            GELIOS_CUDA_TRY(cudaMemcpyAsync(ctx->hstate[0].p, in + 5 * nc, extra * nc * sizeof(double),
+                                            cudaMemcpyDeviceToDevice, s));
+        GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_in_free[j], s));
+        const int rc = gelios_step(ctx, form, 1, nullptr);
+        if (rc) return rc;
+        launches += ctx->launches;
+        // par[1] -> staging (after call k-2's result has left it) -> host
+        if (k >= 2) GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_out_free[j], 0));
+        GELIOS_CUDA_TRY(cudaMemcpyAsync(out, ctx->state[1].p, 5 * nc * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        if (extra)
+            GELIOS_CUDA_TRY(cudaMemcpyAsync(out + 5 * nc, ctx->hstate[1].p, extra * nc * sizeof(double),
+                                            cudaMemcpyDeviceToDevice, s));
+        GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_out_ready[j], s));
+        GELIOS_CUDA_TRY(cudaStreamWaitEvent(ctx->io_d2h, ctx->ev_out_ready[j], 0));
+        GELIOS_CUDA_TRY(cudaMemcpyAsync(host_out[k], out, bytes, cudaMemcpyDeviceToHost, ctx->io_d2h));
+        GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_out_free[j], ctx->io_d2h));
+    }
+    GELIOS_CUDA_TRY(cudaStreamSynchronize(ctx->io_d2h));
+    GELIOS_CUDA_TRY(cudaStreamSynchronize(s));
+    ctx->launches = launches;
     return GELIOS_OK;
 }
 

@@ -185,6 +185,22 @@ class Setka:
         f = lambda a: np.ascontiguousarray(a, np.float64).ravel()  # noqa: E731
         N.check(self._L.gelios_upload_sources(self._h, f(q1), f(q2), f(q3)), "gelios_upload_sources")
 
+    def run_streamed(self, form: int, host_in, host_out):
+        """len(host_in) one-step calls of `form` with host I/O overlapped with
+        the steps (gelios_run_streamed): call k reads host_in[k] into par[0]
+        and writes par[1] into host_out[k].  Blocks are C-contiguous float64
+        arrays of shape (gelios_io_rows(form), n_cells), ideally pinned."""
+        n = len(host_in)
+        if len(host_out) != n:
+            raise ValueError("host_in and host_out differ in length")
+        rows = int(self._L.gelios_io_rows(int(form)))
+        for a in list(host_in) + list(host_out):
+            if a.dtype != np.float64 or a.shape != (rows, self.mesh.n_cells) or not a.flags.c_contiguous:
+                raise ValueError(f"blocks must be C-contiguous float64 of shape ({rows}, n_cells)")
+        pin = (C.c_void_p * max(n, 1))(*[a.ctypes.data for a in host_in])
+        pout = (C.c_void_p * max(n, 1))(*[a.ctypes.data for a in host_out])
+        N.check(self._L.gelios_run_streamed(self._h, int(form), n, pin, pout), "gelios_run_streamed")
+
     def autotune(self, form: int = N.FORM_MHD_PUI, reps: int = 5) -> tuple[int, float]:
         """Time every launch shape of the form's dominant kernel on this grid
         and state, keep the fastest; returns (variant, mean ms).  The state

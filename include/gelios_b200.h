@@ -238,6 +238,22 @@ int gelios_download_mhd(gelios_ctx *ctx, int buf, double *rows8);
  * momentum, energy (n_cells each); read by GELIOS_FORM_MHD_PUI. */
 int gelios_upload_sources(gelios_ctx *ctx, const double *q1, const double *q2, const double *q3);
 
+/* ---- streamed host I/O (no counterpart in the reference) --------------------
+ * For callers that feed a fresh state from host memory every step and read
+ * every result back (a host code coupled to the step, or a driver timing
+ * the step end to end).  Runs `nsteps` one-step calls of `form`, each like
+ * gelios_step(ctx, form, 1, NULL) (dt restarts at dt0): call k copies
+ * host_in[k] into par[0], steps, and copies par[1] into host_out[k].  A host
+ * block holds gelios_io_rows(form) rows of n_cells doubles: ro, p, u, v, Q,
+ * then the form's extra rows (the 16 hydrogen rows of
+ * GELIOS_FORM_5_KOMPONENT, the 8 rows of GELIOS_FORM_MHD_PUI).  The copies
+ * of call k+1's input and of call k-1's result run on two copy streams
+ * while call k steps, through device staging buffers (two per direction,
+ * allocated on first use); host blocks should be pinned for the copies to
+ * overlap.  Returns once every result is in host memory. */
+int gelios_io_rows(int form);
+int gelios_run_streamed(gelios_ctx *ctx, int form, int nsteps, const double *const *host_in, double *const *host_out);
+
 /* ---- autotuning of launch shapes (no counterpart in the reference) ---------
  * The dominant kernel of the MHD form (its face kernel) has
  * gelios_variant_count(form) launch shapes (threads per block x resident
