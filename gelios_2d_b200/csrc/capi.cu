@@ -104,7 +104,7 @@ struct gelios_ctx {
     DBuf hstate[2];
     gelios_mhd_params mprm{};
     DBuf src_fixed;  // MHD form: fixed charge-exchange sources (3 rows)
-    DBuf flux_mhd;   // MHD form: 13 flux rows per face slot, allocated on first use
+    DBuf flux_mhd;   // multi-fluid forms: 13 (MHD) or 21 (Go_5_komponent) flux rows per face slot, on first use
     int mhd_face_variant = 0;  // launch shape of the MHD face kernel (gelios_autotune)
     // streamed host I/O (gelios_run_streamed): copy streams, staging
     // buffers and their events, created on first use
@@ -1007,18 +1007,21 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
     double* cen1 = ctx->cen[1].as<double>();
     if (ctx->ev_used > 4096) ctx->collect();
     const size_t ncz = d.n_cells;
-    if (mhd) {
-        if (ctx->src_fixed.bytes != 3 * ncz * sizeof(double)) {
-            set_error("gelios_step: the MHD form needs gelios_upload_sources");
-            return GELIOS_E_STATE;
-        }
-        const size_t fb = static_cast<size_t>(kMhdFluxRows) * d.n_slots * sizeof(double);
+    if (mhd && ctx->src_fixed.bytes != 3 * ncz * sizeof(double)) {
+        set_error("gelios_step: the MHD form needs gelios_upload_sources");
+        return GELIOS_E_STATE;
+    }
+    if (mhd || form == GELIOS_FORM_5_KOMPONENT) {
+        // wide flux slots of the multi-fluid forms (13 or 21 rows)
+        const int rows = mhd ? kMhdFluxRows : kK5FluxRows;
+        const size_t fb = static_cast<size_t>(rows) * d.n_slots * sizeof(double);
         if (ctx->flux_mhd.bytes != fb) {
             ctx->drop_graphs();
             if (ctx->flux_mhd.alloc(fb)) return GELIOS_E_CUDA;
         }
     }
-    const bool cached_form = form == GELIOS_FORM_MK2 || mhd;  // forms that refill the cache partially
+    // forms whose update refills the geometry cache (|c|^(2 gamma) only where read)
+    const bool cached_form = form == GELIOS_FORM_MK2 || mhd || form == GELIOS_FORM_5_KOMPONENT;
     if (!ctx->cen_valid || (!cached_form && ctx->cen_rp_partial)) {
         cudaEvent_t e0 = ctx->phase_begin();
         launch_centroid(d, d.X, d.Y, cen0, cen0 + ncz, cen0 + 2 * ncz, P.gamma, s, cen0 + 3 * ncz, cen0 + 4 * ncz);
@@ -1073,26 +1076,32 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             if (n < 0) return n;
             launches += n;
         } else if (form == GELIOS_FORM_5_KOMPONENT) {
-            // centroids of the current points, Move_surface +
-            // Move_Setka_Calculate, the five-fluid cell update, x = x2
-            b.cx = cen0;
-            b.cy = cen0 + d.n_cells;
-            b.rp = cen0 + 2 * static_cast<size_t>(d.n_cells);
-            if (st > 0) {  // (st == 0: computed above when not cached)
-                launch_centroid(d, d.X, d.Y, cen0, cen0 + d.n_cells, cen0 + 2 * static_cast<size_t>(d.n_cells),
-                                P.gamma, s);
-                launches++;
-            }
+            // Move_surface + Move_Setka_Calculate, the face units and the
+            // five-fluid cell update (which refills the geometry cache for
+            // the next step, like the moving-grid form), x = x2
+            double* cc = (st & 1) ? cen1 : cen0;
+            double* cn = (st & 1) ? cen0 : cen1;
+            b.cx = cc;
+            b.cy = cc + ncz;
+            b.rp = cc + 2 * ncz;
+            b.vs = cc + 3 * ncz;
+            b.vol = cc + 4 * ncz;
+            b.cx_next = cn;
+            b.cy_next = cn + ncz;
+            b.rp_next = cn + 2 * ncz;
+            b.vs_next = cn + 3 * ncz;
+            b.vol_next = cn + 4 * ncz;
             cudaEvent_t e1 = ctx->phase_begin();
             const int nm = launch_motion(d, P, b, ctx->surface.as<double>(), s, false);
             ctx->phase_end(2, e1, nm);
             cudaEvent_t e3 = ctx->phase_begin();
-            launch_k5_cells(d, P, b, ctx->hstate[cur].as<double>(), ctx->hstate[nxt].as<double>(), s);
-            ctx->phase_end(3, e3, 1);
+            launch_k5(d, P, b, ctx->hstate[cur].as<double>(), ctx->hstate[nxt].as<double>(), ctx->flux_mhd.as<double>(),
+                      s);
+            ctx->phase_end(3, e3, 2);
             cudaEvent_t e4 = ctx->phase_begin();
             launch_commit(d, b, s);
             ctx->phase_end(4, e4, 1);
-            launches += nm + 2;
+            launches += nm + 3;
         } else {
             b.cx = cen0;
             b.cy = cen0 + d.n_cells;
@@ -1122,9 +1131,7 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
     // centroids of the current points: after an odd number of moving-grid
     // steps they sit in the second buffer; swap so cen[0] holds them
     if (cached_form && (nsteps & 1)) std::swap(ctx->cen[0].p, ctx->cen[1].p);
-    // the five-fluid form leaves the centroids of the points before its
-    // last motion in cen[0]
-    ctx->cen_valid = !(form == GELIOS_FORM_5_KOMPONENT && nsteps > 0);
+    ctx->cen_valid = true;
     if (cached_form && nsteps > 0) ctx->cen_rp_partial = true;
     if (status) {
         Words r{};

@@ -2041,27 +2041,219 @@ __device__ __forceinline__ void k5_update_h(double ga, const double* pot, double
     out[3] = v3;
 }
 
-__global__ void __launch_bounds__(128) k5_cell_kernel(DevMesh d, gelios_params P, StepBuffers b,
-                                                      const double* __restrict__ hcur, double* __restrict__ hnxt) {
+// Go_5_komponent face units (the face loop of Setka.cpp:8300-8570): each
+// face once, after the motion.  Both sides' 21-field reconstructions (the
+// plasma and H1..H4; radial in C_1 cells), four hydrogen HLLC problems and
+// the plasma's HLLC (exact Godunov plus HLLC's tracer flux on tracked
+// faces); F*S to the owner slot, -F*S to the twin (the reference evaluates
+// the face from each side; the two results are negatives of each other up to
+// rounding).  Flux rows: plasma mass, mom x, mom y, energy, Q (0-4), then
+// mass, mom x, mom y, energy of H1..H4 (5-20).  CFL candidates of each
+// updated side, H1's only where that side is not C_centr (Setka.cpp:8500).
+__global__ void __launch_bounds__(128) k5_face_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                      const double* __restrict__ hcur, double* __restrict__ fl) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    double tmin = __longlong_as_double(0x7ff0000000000000LL);
+    int status = 0;
+    if (u < d.n_units) {
+        const size_t nc = d.n_cells, ng = d.n_slots;
+        const int c = d.u_cell[u], nb = d.u_nb[u];
+        const uint32_t info = d.u_info[u];
+        const uint32_t cf = (info >> UI_CF_OWN) & 15u, nbf = (info >> UI_CF_NB) & 15u;
+        const double x = b.cx[c], y = b.cy[c];
+        const double radius = sqrt(sq(x) + sq(y));
+        const bool procK = !(radius < P.R11);
+        double x3 = 0.0, y3 = 0.0;
+        bool procN = false;
+        if (nb >= 0) {
+            x3 = b.cx[nb];
+            y3 = b.cy[nb];
+            procN = !(sqrt(sq(x3) + sq(y3)) < P.R11);
+        }
+        if (procK || procN) {
+            const double ga = P.gamma, g2 = 2.0 * P.gamma;
+            const double dt = *b.dt_cur;
+            const bool kC1 = (cf & CF_C1) != 0;
+            const St21 par1 = load21(b.cur, hcur, nc, c);
+            const int ft = info & SI_TYPE_MASK;
+            const int A = d.u_A[u], B = d.u_B[u];
+            const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
+            const double S = sqrt(sq(xb - xa) + sq(yb - ya));
+            const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
+            const double x4 = (d.X2[A] + d.X2[B]) / 2.0, y4 = (d.Y2[A] + d.Y2[B]) / 2.0;
+            const double dist = sqrt(sq(x - x2) + sq(y - y2));
+            St21 par11 = par1;
+            St21 par2 = get_par21(P, ft, par1, b.cur, hcur, nc, nb, x2, y2);
+            double t1 = xb - xa, t2 = yb - ya;
+            const double nn = sqrt(sq(t1) + sq(t2));
+            t1 = t1 / nn;
+            t2 = t2 / nn;
+            const double n1 = t2, n2 = -t1;
+            const double W = ((x4 - x2) * n1 + (y4 - y2) * n2) / dt;
+            const double dis = sqrt(sq(x2) + sq(y2));
+            const bool tracked = (info & SI_GOD) != 0;
+            if (ft == G_USUALY) {
+                const double dd = sqrt(sq(x3) + sq(y3));
+                if (kC1) {
+                    radial_scale21(par11, radius, dis, g2);
+                    polar_perenos(x, y, x2, y2, par11.f[kU], par11.f[kV]);
+                    polar_perenos(x, y, x2, y2, par11.f[fh(0, 2)], par11.f[fh(0, 3)]);
+                    double o[4];
+                    tvd21_radial(b.cur, hcur, nc, b.cx, b.cy, x2, y2, par1, x, y, nb, d.u_sd[u], (cf & CF_AXIS) != 0,
+                                 g2, o);
+                    par11.f[kRo] = o[0];
+                    par11.f[kP] = o[1];
+                    par11.f[fh(0, 1)] = o[2];
+                    par11.f[fh(0, 0)] = o[3];
+                } else {
+                    par11 = tvd21_usualy(b.cur, hcur, nc, b.cx, b.cy, x2, y2, par1, x, y, nb, d.u_sd[u],
+                                         (cf & CF_AXIS) != 0, tracked, &status);
+                }
+                if (nbf & CF_C1) {
+                    const St21 parN = par2;  // the neighbour's stored state
+                    radial_scale21(par2, dd, dis, g2);
+                    polar_perenos(x3, y3, x2, y2, par2.f[kU], par2.f[kV]);
+                    polar_perenos(x3, y3, x2, y2, par2.f[fh(0, 2)], par2.f[fh(0, 3)]);
+                    double o[4];
+                    tvd21_radial(b.cur, hcur, nc, b.cx, b.cy, x2, y2, parN, x3, y3, c, d.u_sd2[u],
+                                 (nbf & CF_AXIS) != 0, g2, o);
+                    par2.f[kRo] = o[0];
+                    par2.f[kP] = o[1];
+                    par2.f[fh(0, 1)] = o[2];
+                    par2.f[fh(0, 0)] = o[3];
+                } else {
+                    par2 = tvd21_usualy(b.cur, hcur, nc, b.cx, b.cy, x2, y2, par2, x3, y3, c, d.u_sd2[u],
+                                        (nbf & CF_AXIS) != 0, tracked, &status);
+                }
+            } else if (ft == G_INNER_SPHERE) {
+                radial_scale21(par11, radius, dis, g2);
+            } else if (kC1 && ft == G_AXIS) {
+                radial_scale21(par11, radius, dis, g2);
+                polar_perenos(x, y, x2, y2, par11.f[kU], par11.f[kV]);
+                polar_perenos(x, y, x2, y2, par11.f[fh(0, 2)], par11.f[fh(0, 3)]);
+                par2 = par11;
+                mirror21(par2);
+            } else if (!kC1 && ft == G_AXIS) {
+                par11 = tvd21_axis(b.cur, hcur, nc, b.cx, b.cy, x2, y2, par1, x, y, d.u_sd[u]);
+                par2 = par11;
+                mirror21(par2);
+            }
+            const bool np = (info & SI_NP) != 0;
+            const int g = d.u_slot[u], gt = d.u_twin[u];
+            FluxOut<double> F;
+            double UUh[4];
+            for (int hk = 0; hk < 4; hk++) {
+                St5 L, R;
+                L.ro = par11.f[fh(hk, 0)];
+                L.p = par11.f[fh(hk, 1)];
+                L.u = par11.f[fh(hk, 2)];
+                L.v = par11.f[fh(hk, 3)];
+                L.Q = par11.f[kQ];
+                R.ro = par2.f[fh(hk, 0)];
+                R.p = par2.f[fh(hk, 1)];
+                R.u = par2.f[fh(hk, 2)];
+                R.v = par2.f[fh(hk, 3)];
+                R.Q = par2.f[kQ];
+                UUh[hk] = hllc_flux<double>(ga, P.kurant, L, R, W, n1, n2, 1.0, 1, false, F);
+                const double h[4] = {F.P0 * S, F.P1 * S, F.P2 * S, F.P3 * S};
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    fl[(5 + 4 * hk + j) * ng + g] = h[j];
+                    if (gt >= 0) fl[(5 + 4 * hk + j) * ng + gt] = -h[j];
+                }
+            }
+            St5 L, R;
+            L.ro = par11.f[kRo];
+            L.p = par11.f[kP];
+            L.u = par11.f[kU];
+            L.v = par11.f[kV];
+            L.Q = par11.f[kQ];
+            R.ro = par2.f[kRo];
+            R.p = par2.f[kP];
+            R.u = par2.f[kU];
+            R.v = par2.f[kV];
+            R.Q = par2.f[kQ];
+            double pl[5];
+            double UG = 0.0;
+            if (tracked) {
+                double q1[5] = {L.ro, L.p, L.u, L.v, 0.0};
+                double q2[5] = {R.ro, R.p, R.u, R.v, 0.0};
+                double nvv[3] = {n1, n2, 0.0};
+                double qq[5], ds[3];
+                UG = godunov_dev<false>(ga, P.kurant, q1, q2, nvv, qq, ds, W, dist, P.godunov_max_iter, &status);
+                pl[0] = qq[0] * S;
+                pl[1] = qq[1] * S;
+                pl[2] = qq[2] * S;
+                pl[3] = qq[4] * S;
+            }
+            const double UU = hllc_flux<double>(ga, P.kurant, L, R, W, n1, n2, 1.0, 1, np, F);
+            if (!tracked) {
+                pl[0] = F.P0 * S;
+                pl[1] = F.P1 * S;
+                pl[2] = F.P2 * S;
+                pl[3] = F.P3 * S;
+            }
+            pl[4] = F.PQ * S;
+#pragma unroll
+            for (int j = 0; j < 5; j++) {
+                fl[j * ng + g] = pl[j];
+                if (gt >= 0) fl[j * ng + gt] = -pl[j];
+            }
+            // CFL candidates in the reference's order per side (Setka.cpp:8500-8560)
+            auto side = [&](double dd, bool centr) {
+                for (int hk = 0; hk < 4; hk++)
+                    if (!(hk == 0 && centr)) tmin = dmin_ref(tmin, P.kurant * dd / UUh[hk]);
+                if (tracked) tmin = dmin_ref(tmin, P.kurant * dd / UG);
+                tmin = dmin_ref(tmin, P.kurant * dd / UU);
+            };
+            if (procK) side(dist, (cf & CF_CENTR) != 0);
+            if (gt >= 0 && procN) side(sqrt(sq(x3 - x2) + sq(y3 - y2)), (nbf & CF_CENTR) != 0);
+        }
+    }
+    block_reduce_commit(tmin, 0, 0, status, b.dt_acc, b.counters, b.status);
+}
+
+// Go_5_komponent cell update (Setka.cpp:8570-8950) from the summed face
+// slots: multi-fluid charge exchange, cylindrical 1/y terms, clamps; it also
+// refills the geometry cache for the next step.
+__global__ void __launch_bounds__(128) k5_update_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                        const double* __restrict__ fl,
+                                                        const double* __restrict__ hcur, double* __restrict__ hnxt) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     double tmin = __longlong_as_double(0x7ff0000000000000LL);
     int nro = 0, npc = 0, status = 0;
     const size_t nc = d.n_cells;
     if (c < d.n_cells) {
+        {  // the next step's geometry cache from the moved points (see mk2_update_kernel)
+            const int s0 = d.cstart[c], n = d.cstart[c + 1] - s0;
+            const int32_t* con = d.contour + s0;
+            double xn, yn;
+            centroid(con, n, d.X2, d.Y2, xn, yn);
+            b.cx_next[c] = xn;
+            b.cy_next[c] = yn;
+            const uint32_t cfl = d.cflags[c];
+            if (cfl & CF_RP) b.rp_next[c] = pow2g(sqrt(sq(xn) + sq(yn)), 2 * P.gamma);
+            if (!(cfl & CF_CENTR)) {
+                b.vs_next[c] = area(con, n, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X2, d.Y2, false);
+                b.vol_next[c] = volume_rotate(con, n, d.X2, d.Y2);
+            }
+        }
         const double x = b.cx[c], y = b.cy[c];
         const double radius = sqrt(sq(x) + sq(y));
         if (!(radius < P.R11)) {
             tmin = 10000000.0;  // `time` starts at 1e7 in every step (Setka.cpp:8286)
-            const double ga = P.gamma, g2 = 2.0 * P.gamma;
+            const double ga = P.gamma;
             const double dt = *b.dt_cur;
             const int kt = d.ctype[c];
-            const uint32_t cf = d.cflags[c];
             const St21 par1 = load21(b.cur, hcur, nc, c);
             const int s0 = d.cstart[c], nv = d.cstart[c + 1] - s0;
             const int32_t* con = d.contour + s0;
             const int g0 = d.gstart[c], g1 = d.gstart[c + 1];
             const double Volume = area(con, nv, d.sA, d.sB, g0, g1, d.X, d.Y, false);
             const double Volume2 = area(con, nv, d.sA, d.sB, g0, g1, d.X2, d.Y2, true);
+            // face fluxes summed in Grans order: plasma rows 0-4, hydrogen
+            // fluid k rows 5 + 4k .. 8 + 4k
+            const size_t ng = d.n_slots;
             double Potok[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
             double PH[4][4];
 #pragma unroll
@@ -2069,129 +2261,12 @@ __global__ void __launch_bounds__(128) k5_cell_kernel(DevMesh d, gelios_params P
 #pragma unroll
                 for (int j = 0; j < 4; j++) PH[k][j] = 0.0;
             for (int g = g0; g < g1; g++) {
-                const uint32_t info = d.sinfo[g];
-                const int ft = info & SI_TYPE_MASK;
-                const int A = d.sA[g], B = d.sB[g], nb = d.snb[g];
-                const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
-                const double S = sqrt(sq(xb - xa) + sq(yb - ya));
-                const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
-                const double x4 = (d.X2[A] + d.X2[B]) / 2.0, y4 = (d.Y2[A] + d.Y2[B]) / 2.0;
-                const double dist = sqrt(sq(x - x2) + sq(y - y2));
-                St21 par11 = par1;
-                St21 par2 = get_par21(P, ft, par1, b.cur, hcur, nc, nb, x2, y2);
-                double t1 = xb - xa, t2 = yb - ya;
-                const double nn = sqrt(sq(t1) + sq(t2));
-                t1 = t1 / nn;
-                t2 = t2 / nn;
-                const double n1 = t2, n2 = -t1;
-                const double W = ((x4 - x2) * n1 + (y4 - y2) * n2) / dt;
-                const double dis = sqrt(sq(x2) + sq(y2));
-                const bool tracked = (info & SI_GOD) != 0;
-                if (ft == G_USUALY) {
-                    const double x3 = b.cx[nb], y3 = b.cy[nb];
-                    const double dd = sqrt(sq(x3) + sq(y3));
-                    if (kt == C_1) {
-                        radial_scale21(par11, radius, dis, g2);
-                        polar_perenos(x, y, x2, y2, par11.f[kU], par11.f[kV]);
-                        polar_perenos(x, y, x2, y2, par11.f[fh(0, 2)], par11.f[fh(0, 3)]);
-                        double o[4];
-                        tvd21_radial(b.cur, hcur, nc, b.cx, b.cy, x2, y2, par1, x, y, nb, d.ssd[g],
-                                     (cf & CF_AXIS) != 0, g2, o);
-                        par11.f[kRo] = o[0];
-                        par11.f[kP] = o[1];
-                        par11.f[fh(0, 1)] = o[2];
-                        par11.f[fh(0, 0)] = o[3];
-                    } else {
-                        par11 = tvd21_usualy(b.cur, hcur, nc, b.cx, b.cy, x2, y2, par1, x, y, nb, d.ssd[g],
-                                             (cf & CF_AXIS) != 0, tracked, &status);
-                    }
-                    const uint32_t nbf = d.cflags[nb];
-                    if (d.ctype[nb] == C_1) {
-                        const St21 parN = par2;  // the neighbour's stored state
-                        radial_scale21(par2, dd, dis, g2);
-                        polar_perenos(x3, y3, x2, y2, par2.f[kU], par2.f[kV]);
-                        polar_perenos(x3, y3, x2, y2, par2.f[fh(0, 2)], par2.f[fh(0, 3)]);
-                        double o[4];
-                        tvd21_radial(b.cur, hcur, nc, b.cx, b.cy, x2, y2, parN, x3, y3, c, d.ssd2[g],
-                                     (nbf & CF_AXIS) != 0, g2, o);
-                        par2.f[kRo] = o[0];
-                        par2.f[kP] = o[1];
-                        par2.f[fh(0, 1)] = o[2];
-                        par2.f[fh(0, 0)] = o[3];
-                    } else {
-                        par2 = tvd21_usualy(b.cur, hcur, nc, b.cx, b.cy, x2, y2, par2, x3, y3, c, d.ssd2[g],
-                                            (nbf & CF_AXIS) != 0, tracked, &status);
-                    }
-                } else if (ft == G_INNER_SPHERE) {
-                    radial_scale21(par11, radius, dis, g2);
-                } else if (kt == C_1 && ft == G_AXIS) {
-                    radial_scale21(par11, radius, dis, g2);
-                    polar_perenos(x, y, x2, y2, par11.f[kU], par11.f[kV]);
-                    polar_perenos(x, y, x2, y2, par11.f[fh(0, 2)], par11.f[fh(0, 3)]);
-                    par2 = par11;
-                    mirror21(par2);
-                } else if (kt != C_1 && ft == G_AXIS) {
-                    par11 = tvd21_axis(b.cur, hcur, nc, b.cx, b.cy, x2, y2, par1, x, y, d.ssd[g]);
-                    par2 = par11;
-                    mirror21(par2);
-                }
-                const bool np = (info & SI_NP) != 0;
-                FluxOut<double> F;
-                for (int hk = 0; hk < 4; hk++) {
-                    if (hk == 0 && kt == C_CENTR) continue;  // H1 not evolved in C_centr (Setka.cpp:8500)
-                    St5 L, R;
-                    L.ro = par11.f[fh(hk, 0)];
-                    L.p = par11.f[fh(hk, 1)];
-                    L.u = par11.f[fh(hk, 2)];
-                    L.v = par11.f[fh(hk, 3)];
-                    L.Q = par11.f[kQ];
-                    R.ro = par2.f[fh(hk, 0)];
-                    R.p = par2.f[fh(hk, 1)];
-                    R.u = par2.f[fh(hk, 2)];
-                    R.v = par2.f[fh(hk, 3)];
-                    R.Q = par2.f[kQ];
-                    const double UU = hllc_flux<double>(ga, P.kurant, L, R, W, n1, n2, 1.0, 1, false, F);
-                    tmin = dmin_ref(tmin, P.kurant * dist / UU);
-                    PH[hk][0] = PH[hk][0] + F.P0 * S;
-                    PH[hk][1] = PH[hk][1] + F.P1 * S;
-                    PH[hk][2] = PH[hk][2] + F.P2 * S;
-                    PH[hk][3] = PH[hk][3] + F.P3 * S;
-                }
-                St5 L, R;
-                L.ro = par11.f[kRo];
-                L.p = par11.f[kP];
-                L.u = par11.f[kU];
-                L.v = par11.f[kV];
-                L.Q = par11.f[kQ];
-                R.ro = par2.f[kRo];
-                R.p = par2.f[kP];
-                R.u = par2.f[kU];
-                R.v = par2.f[kV];
-                R.Q = par2.f[kQ];
-                if (tracked) {
-                    double q1[5] = {L.ro, L.p, L.u, L.v, 0.0};
-                    double q2[5] = {R.ro, R.p, R.u, R.v, 0.0};
-                    double nvv[3] = {n1, n2, 0.0};
-                    double qq[5], ds[3];
-                    const double UG = godunov_dev<false>(ga, P.kurant, q1, q2, nvv, qq, ds, W, dist,
-                                                         P.godunov_max_iter, &status);
-                    tmin = dmin_ref(tmin, P.kurant * dist / UG);
-                    Potok[0] = Potok[0] + qq[0] * S;
-                    Potok[1] = Potok[1] + qq[1] * S;
-                    Potok[2] = Potok[2] + qq[2] * S;
-                    Potok[3] = Potok[3] + qq[4] * S;
-                    const double UU = hllc_flux<double>(ga, P.kurant, L, R, W, n1, n2, 1.0, 1, np, F);
-                    tmin = dmin_ref(tmin, P.kurant * dist / UU);
-                    Potok[4] = Potok[4] + F.PQ * S;
-                } else {
-                    const double UU = hllc_flux<double>(ga, P.kurant, L, R, W, n1, n2, 1.0, 1, np, F);
-                    tmin = dmin_ref(tmin, P.kurant * dist / UU);
-                    Potok[0] = Potok[0] + F.P0 * S;
-                    Potok[1] = Potok[1] + F.P1 * S;
-                    Potok[2] = Potok[2] + F.P2 * S;
-                    Potok[3] = Potok[3] + F.P3 * S;
-                    Potok[4] = Potok[4] + F.PQ * S;
-                }
+#pragma unroll
+                for (int j = 0; j < 5; j++) Potok[j] = Potok[j] + fl[j * ng + g];
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+#pragma unroll
+                    for (int j = 0; j < 4; j++) PH[k][j] = PH[k][j] + fl[(5 + 4 * k + j) * ng + g];
             }
             // multi-fluid charge exchange (Setka.cpp:8575-8660)
             const double u = par1.f[kU], v = par1.f[kV], ro = par1.f[kRo], p = par1.f[kP], Q = par1.f[kQ];
@@ -2789,9 +2864,10 @@ int launch_motion(const DevMesh& d, const gelios_params& P, const StepBuffers& b
 void launch_hllc_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s) {
     hllc_batch_kernel<<<blocks_for(n, 128), 128, 0, s>>>(P, n, in, out);
 }
-void launch_k5_cells(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* hcur, double* hnxt,
-                     cudaStream_t s) {
-    k5_cell_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, hcur, hnxt);
+void launch_k5(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* hcur, double* hnxt,
+               double* fl, cudaStream_t s) {
+    if (d.n_units > 0) k5_face_kernel<<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, b, hcur, fl);
+    k5_update_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, fl, hcur, hnxt);
 }
 void launch_hlldq_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s) {
     hlldq_batch_kernel<<<blocks_for(n, 128), 128, 0, s>>>(P, n, in, out);

@@ -124,10 +124,12 @@ void launch_dt_finalize(const StepBuffers& b, cudaStream_t s);
 void launch_commit(const DevMesh& d, const StepBuffers& b, cudaStream_t s);
 int launch_motion(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* scratch, cudaStream_t s,
                   bool copy_outer_shock = true);
-// Go_5_komponent cell kernel: hydrogen state rows (ro, p, u, v of H1..H4),
-// 16 rows of n_cells each, of the current and the next buffer.
-void launch_k5_cells(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* hcur, double* hnxt,
-                     cudaStream_t s);
+// Go_5_komponent: face units then the cell update.  Hydrogen state rows
+// (ro, p, u, v of H1..H4), 16 rows of n_cells each, of the current and the
+// next buffer; fl: kK5FluxRows flux rows per face slot.
+constexpr int kK5FluxRows = 21;
+void launch_k5(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* hcur, double* hnxt,
+               double* fl, cudaStream_t s);
 // MHD + pickup-proton form: extra rows (8 x n_cells: w, Bx, By, Bz, pickup
 // ro, p, u, v), 13 flux rows per slot, fixed sources (3 x n_cells).
 constexpr int kMhdFluxRows = 13;
