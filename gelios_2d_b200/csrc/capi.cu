@@ -135,6 +135,7 @@ struct gelios_ctx {
     };
     StepGraph graphs[8];
     bool graphs_off = false;  // capture failed once: launch directly
+    bool coop_off = false;    // the cooperative plain step could not launch once: three kernels per step
     void drop_graphs() {
         for (auto& g : graphs) {
             if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -1029,7 +1030,34 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
         launches++;
         ctx->cen_rp_partial = false;
     }
-    for (int st = 0; st < nsteps; st++) {
+    int first = 0;
+    if (form == GELIOS_FORM_STATIONARY && nsteps > 0 && !ctx->timing && !ctx->coop_off) {
+        // all steps of the plain form in one cooperative launch
+        StepBuffers bb[2];
+        for (int par = 0; par < 2; par++) {
+            StepBuffers& b = bb[par];
+            for (int k = 0; k < 5; k++) {
+                b.cur[k] = ctx->field(par, k);
+                b.nxt[k] = ctx->field(par ^ 1, k);
+            }
+            b.dt_cur = ctx->T() + par;
+            b.dt_next = ctx->T() + (par ^ 1);
+            b.dt_acc = ctx->acc();
+            b.counters = ctx->counters();
+            b.status = ctx->status();
+            b.cx = cen0;
+            b.cy = cen0 + ncz;
+            b.rp = cen0 + 2 * ncz;
+        }
+        if (launch_stationary_persistent(d, P, bb[0], bb[1], ctx->flux.as<double>(), nsteps, s) == cudaSuccess) {
+            launches += 1;
+            first = nsteps;
+        } else {
+            cudaGetLastError();
+            ctx->coop_off = true;
+        }
+    }
+    for (int st = first; st < nsteps; st++) {
         const int cur = st & 1, nxt = cur ^ 1;
         StepBuffers b;
         for (int k = 0; k < 5; k++) {

@@ -108,6 +108,10 @@ void launch_stationary_units(const DevMesh& d, const gelios_params& P, const Ste
                              cudaStream_t s);
 void launch_stationary_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
                               cudaStream_t s);
+// `nsteps` Go_stationary steps in one cooperative launch (b0: even steps,
+// b1: odd steps); returns the launch's error code.
+cudaError_t launch_stationary_persistent(const DevMesh& d, const gelios_params& P, const StepBuffers& b0,
+                                         const StepBuffers& b1, double* fl, int nsteps, cudaStream_t s);
 void launch_mk2_recon(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* rec, cudaStream_t s);
 int launch_mk2_flux_plain(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
                           double* fl, cudaStream_t s);

@@ -294,4 +294,32 @@ def test_launch_count_reported():
     P = W.plain_params()
     dev, _ = _pair(mesh, P, W.plain_initial(mesh, P))
     dev.Go_stationary(5)
-    assert dev.launches() == 1 + 3 * 5  # centroids + (face units, cell update, dt) per step
+    assert dev.launches() == 1 + 1  # centroids + one cooperative launch for all five steps
+    dev.set_phase_timing(True)
+    dev.Go_stationary(5)
+    assert dev.launches() == 3 * 5  # (face units, cell update, dt) per step; centroids cached
+
+
+@pytest.mark.parametrize("precision", [N.PREC_FP64, N.PREC_FP32_FLUX])
+def test_stationary_persistent_matches_three_kernel_steps(precision):
+    """The cooperative multi-step launch and the three kernels per step
+    (phase timing on) agree to rounding (the shared bodies are compiled into
+    two kernels, whose multiply-add contraction may differ) with the same
+    clamp counts and status."""
+    mesh = W.plain_mesh()
+    P = W.plain_params(precision=precision)
+    st0 = W.plain_initial(mesh, P, seed=9)
+    out = []
+    for direct in (False, True):
+        dev = g.Setka(mesh, P)
+        dev.set_par(0, st0)
+        dev.set_par(1, st0)
+        dev.set_phase_timing(direct)
+        st = dev.Go_stationary(25)
+        out.append((dev.par(1), st.dt, st.n_ro_clamp, st.n_p_clamp, st.flags))
+    # FP64: rounding of the last bits; FP32 fluxes: float rounding (1e-7 per
+    # operation) compounds over the 25 steps
+    tol = 1e-13 if precision == N.PREC_FP64 else 1e-4
+    assert rel_err(out[0][0], out[1][0]) <= tol
+    assert abs(out[0][1] - out[1][1]) <= tol * out[1][1]
+    assert out[0][2:] == out[1][2:]
