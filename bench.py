@@ -42,6 +42,9 @@ WORKLOADS = {
     "plain": ("plain single-fluid step (Go_stationary form), polar 180x120, r=1..600", "plain", None),
     "k5_200k": ("plasma + four hydrogen fluids (Go_5_komponent form) on Setka(200,100,50,100,100,100,150,150)",
                 "k5", (200, 100, 50, 100, 100, 100, 150, 150)),
+    "inner_200k": ("inner fixed-grid region step (Go_stationary_5_komponent_inner_MK2 form): All_Cells_Inner "
+                   "(centroid radius <= R111) of Setka(200,100,50,100,100,100,150,150)", "inner",
+                   (200, 100, 50, 100, 100, 100, 150, 150)),
     "mhd_200k": ("ion MHD fluid (HLLD) + pickup protons (HLLC) on the moving grid Setka(200,100,50,100,100,100,"
                  "150,150): LISM B=0.01 at 30 deg, seeded fixed charge-exchange sources", "mhd",
                  (200, 100, 50, 100, 100, 100, 150, 150)),
@@ -63,13 +66,16 @@ WORKLOADS = {
 #   MHD + pickup form: 8*(2*13) state (ions ro, p, u, v, w, Bx, By, Bz, Q; pickup
 #             ro, p, u, v) + 8*3 fixed sources + 16*(1+1) points + 8 written point
 #             coordinate + 4*4 neighbour indices = 288 B
-BYTES_PER_CELL = {"mk2": 288, "plain": 112, "k5": 392, "mhd": 288}
+#   inner form: 8*(2*5) state + 8*19 Monte-Carlo moments + 16 points (fixed
+#             grid) + 4*4 neighbour indices = 264 B
+BYTES_PER_CELL = {"mk2": 288, "plain": 112, "k5": 392, "mhd": 288, "inner": 264}
 STEP_KERNELS = {
     "mk2": "whole moving-grid step: recon, tracked_solve, source, surface_faces, rails, flux x2, update, commit "
            "(one CUDA graph, 3 streams)",
     "plain": "whole plain step: stationary_unit + stationary_update + dt_finalize",
     "k5": "whole four-fluid step: centroid, surface_faces, rails, k5_cell, commit",
     "mhd": "whole MHD + pickup step: surface_faces, rails, mhd_face, mhd_update, commit",
+    "inner": "whole inner-region step: inner_cell + dt_finalize",
 }
 
 
@@ -92,6 +98,13 @@ def build_workload(name: str):
         st0 = W.init_conditions_reference(mesh)
         mc = W.mc_fields(mesh, seed=9)
         counted = W.counted_cells_mk2(mesh, params)
+    elif form == "inner":
+        mesh = g.Mesh.setka(*dims)
+        params = N.reference_params()
+        st0 = W.init_conditions_reference(mesh)
+        mc = W.mc_fields(mesh, seed=9)
+        inner = mesh.inner_cells(params.R111)
+        counted = int(np.count_nonzero(mesh["cell_type"][inner] != 5))  # C_centr cells are copied
     elif form == "mhd":
         # `mc` carries (boundary data, extra rows (8, n_cells), fixed sources)
         mesh = g.Mesh.setka(*dims)
@@ -234,7 +247,9 @@ def cpu_reference_rate(mesh, params, st0, mc, counted, form, budget_s=12.0, max_
         S.set_hydrogen(1, mc)
     elif mc is not None:
         S.set_mc(*mc)
-    run = {"mk2": S.go_mk2, "k5": S.go_5_komponent}.get(form, S.go_stationary)
+    if form == "inner":
+        S.build_inner_list()
+    run = {"mk2": S.go_mk2, "k5": S.go_5_komponent, "inner": S.go_inner_mk2}.get(form, S.go_stationary)
     # keep the reference's printf diagnostics off our stdout
     saved = os.dup(1)
     devnull = os.open(os.devnull, os.O_WRONLY)
@@ -262,6 +277,9 @@ def load_inputs(S, form, st0, mc):
     if form == "k5":
         S.set_hydrogen(0, mc)
         S.set_hydrogen(1, mc)
+    elif form == "inner":
+        S.set_mc(*mc)
+        S.build_inner_list()
     elif form == "mhd":
         S.set_mhd_params(mc[0])
         S.set_mhd(0, mc[1])
@@ -450,8 +468,8 @@ def main():
     config = {"workload": desc, "cells": int(mesh.n_cells), "cells_updated_per_step": int(counted),
               "faces": int(mesh.n_faces), "points": int(mesh.n_points),
               "l2": ("inputs larger than L2" if args.workload.endswith("_1m") else
-                     "flushed (256 MiB write) before each timed call of 100 steps; the 2.4 MB state stays "
-                     "L2-resident within a call" if form == "plain" else
+                     "flushed (256 MiB write) before each timed call of 100 steps; the few-MB state stays "
+                     "L2-resident within a call" if form in ("plain", "inner") else
                      "flushed between timed steps (256 MiB write)"), "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
 
     cpu_kind = "port" if form == "mhd" else "reference"
@@ -492,7 +510,8 @@ def main():
     if form == "mhd":  # launch shape of the face kernel picked on this grid (the library's autotuner)
         v, tms = S.autotune(N.FORM_MHD_PUI, reps=3)
         tuned = {"variant": v, "face_kernel_ms": tms}
-    fcode = {"mk2": N.FORM_MK2, "k5": N.FORM_5_KOMPONENT, "mhd": N.FORM_MHD_PUI}.get(form, N.FORM_STATIONARY)
+    fcode = {"mk2": N.FORM_MK2, "k5": N.FORM_5_KOMPONENT, "mhd": N.FORM_MHD_PUI,
+             "inner": N.FORM_INNER_MK2}.get(form, N.FORM_STATIONARY)
     stream = torch.cuda.ExternalStream(S.stream_handle(), device=device)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")
     do_flush = not args.workload.endswith("_1m")
@@ -500,7 +519,7 @@ def main():
     # 100 on the plain grid, whose 2.4 MB state stays L2-resident within a
     # call as in the reference's long step loops (L2 flushed before each
     # call; the call runs all its steps in one cooperative launch); 1 else
-    steps_per_call = 10 if not do_flush else (100 if form == "plain" else 1)
+    steps_per_call = 10 if not do_flush else (100 if form in ("plain", "inner") else 1)
 
     def one(timed_events=None):
         if do_flush:
