@@ -1221,7 +1221,13 @@ extern "C" int gelios_run_streamed(gelios_ctx* ctx, int form, int nsteps, const 
                                             cudaMemcpyDeviceToDevice, s));
         GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_in_free[j], s));
         const int rc = gelios_step(ctx, form, 1, nullptr);
-        if (rc) return rc;
+        if (rc) {
+            // no copy may touch the caller's blocks after we return
+            cudaStreamSynchronize(ctx->io_h2d);
+            cudaStreamSynchronize(ctx->io_d2h);
+            cudaStreamSynchronize(s);
+            return rc;
+        }
         launches += ctx->launches;
         // par[1] -> staging (after call k-2's result has left it) -> host
         if (k >= 2) GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_out_free[j], 0));
