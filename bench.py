@@ -361,13 +361,16 @@ def run_sweep(args, rank: int, world: int, local: int) -> None:
         inst = sw.instance_set(n_inst, seed=seed, scale=(0.5, 1.4), only=mine)
     counted = sum(W.counted_cells_mk2(m, p) for m, p, _, _ in inst)
     cells = sum(m.n_cells for m, _, _, _ in inst)
+    batched = mhd and args.sweep_mode == "batched"
     B = sw.Sweep(inst, device=local, form=N.FORM_MHD_PUI if mhd else N.FORM_MK2)
     tuned = None
-    if mhd:  # per-instance launch shape and enqueue order (the sweep's autotuner)
+    if mhd and not batched:  # per-instance launch shape and enqueue order (the sweep's autotuner)
         res = B.autotune(reps=3)
         tuned = {}
         for v, _ in res:
             tuned[str(v)] = tuned.get(str(v), 0) + 1
+    if batched:  # one launch per phase over the instances of a group (gelios_batch)
+        B.enable_batch(args.sweep_groups)
     streams = [torch.cuda.ExternalStream(S.stream_handle(), device=local) for S in B.items]
     s0 = torch.cuda.current_stream(local)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
@@ -423,7 +426,9 @@ def run_sweep(args, rank: int, world: int, local: int) -> None:
                    "cells_rank0": int(cells), "cells_updated_per_step": int(counted_all),
                    "l2": "flushed between timed steps (256 MiB write)",
                    "parallelism": f"instances partitioned over {world} GPU(s)",
-                   "autotune_variants_rank0": tuned},
+                   "autotune_variants_rank0": tuned,
+                   "mode": "batched: one launch per phase over all instances, one CUDA graph per step" if batched
+                           else "one context and captured step graph per instance, enqueued together"},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "kernel": "batched moving-grid steps of all instances on a GPU",
@@ -448,6 +453,10 @@ def main():
     ap.add_argument("--workload", default="mk2_200k", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32flux"])
+    # sweep64 only: one context and captured step graph per instance, autotuned and enqueued together
+    # (default), or gelios_batch: one launch per phase over the instances of each of --sweep-groups groups
+    ap.add_argument("--sweep-mode", default="contexts", choices=["contexts", "batched"])
+    ap.add_argument("--sweep-groups", type=int, default=1)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

@@ -1346,6 +1346,234 @@ extern "C" int gelios_autotune(gelios_ctx* ctx, int form, int reps, int32_t* var
     return GELIOS_OK;
 }
 
+// ---------------------------------------------------------------- batched instances
+struct gelios_batch {
+    int device = 0;
+    std::vector<gelios_ctx*> ctxs;
+    DBuf inst, surf, rails, units, cells, points;
+    BatchTables tab;
+    std::vector<BatchInstance> host_inst;  // one descriptor per instance, rebuilt per call
+    cudaEvent_t ev = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool graphs_off = false;
+    ~gelios_batch() {
+        for (auto& g : graph)
+            if (g) cudaGraphExecDestroy(g);
+        if (ev) cudaEventDestroy(ev);
+    }
+};
+
+extern "C" int gelios_batch_create(gelios_batch** out, gelios_ctx* const* ctxs, int n) {
+    if (!out || !ctxs || n < 1) return GELIOS_E_ARG;
+    *out = nullptr;
+    auto B = std::make_unique<gelios_batch>();
+    B->device = ctxs[0] ? ctxs[0]->device : 0;
+    std::vector<int2> surf, rails, units, cells, points;
+    for (int i = 0; i < n; i++) {
+        gelios_ctx* c = ctxs[i];
+        if (!c || !c->have_mesh) {
+            set_error("gelios_batch_create: a context without topology");
+            return GELIOS_E_STATE;
+        }
+        if (c->device != B->device || c->prm.precision != ctxs[0]->prm.precision) {
+            set_error("gelios_batch_create: contexts on different devices or with different flux precisions");
+            return GELIOS_E_ARG;
+        }
+        const DevMesh& d = c->d;
+        if (d.n_rail_a + d.n_rail_b + d.n_rail_c + d.n_rail_d == 0 || d.n_lc == 0) {
+            set_error("gelios_batch_create: the moving-grid step needs rails and tracked lines");
+            return GELIOS_E_MESH;
+        }
+        if (c->src_fixed.bytes != 3 * static_cast<size_t>(d.n_cells) * sizeof(double)) {
+            set_error("gelios_batch_create: a context without gelios_upload_sources");
+            return GELIOS_E_STATE;
+        }
+        GELIOS_CUDA_TRY(cudaSetDevice(c->device));
+        const size_t fb = static_cast<size_t>(kMhdFluxRows) * d.n_slots * sizeof(double);
+        if (c->flux_mhd.bytes != fb) {
+            c->drop_graphs();
+            if (c->flux_mhd.alloc(fb)) return GELIOS_E_CUDA;
+        }
+        const int nt = d.n_lc + d.n_li + d.n_lo;
+        for (int j = 0; j < nt; j += 2) surf.push_back(make_int2(i, j));
+        const int nr = d.n_rail_a + d.n_rail_b + d.n_rail_c + d.n_rail_d;
+        for (int q = 0; q < nr; q++) rails.push_back(make_int2(i, q));
+        for (int u = 0; u < d.n_units; u += 128) units.push_back(make_int2(i, u));
+        for (int k = 0; k < d.n_cells; k += 128) cells.push_back(make_int2(i, k));
+        for (int k = 0; k < d.n_points; k += 256) points.push_back(make_int2(i, k));
+        B->ctxs.push_back(c);
+    }
+    GELIOS_CUDA_TRY(cudaSetDevice(B->device));
+    cudaStream_t s = ctxs[0]->stream;
+    int rc = 0;
+    rc |= upload(B->surf, surf.data(), surf.size(), s);
+    rc |= upload(B->rails, rails.data(), rails.size(), s);
+    rc |= upload(B->units, units.data(), units.size(), s);
+    rc |= upload(B->cells, cells.data(), cells.size(), s);
+    rc |= upload(B->points, points.data(), points.size(), s);
+    if (B->inst.alloc(static_cast<size_t>(n) * sizeof(BatchInstance))) rc |= 1;
+    if (rc) return GELIOS_E_CUDA;
+    GELIOS_CUDA_TRY(cudaStreamSynchronize(s));
+    GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&B->ev, cudaEventDisableTiming));
+    BatchTables& t = B->tab;
+    t.surf = B->surf.as<int2>();
+    t.rails = B->rails.as<int2>();
+    t.units = B->units.as<int2>();
+    t.cells = B->cells.as<int2>();
+    t.points = B->points.as<int2>();
+    t.n_surf = static_cast<int>(surf.size());
+    t.n_rails = static_cast<int>(rails.size());
+    t.n_units = static_cast<int>(units.size());
+    t.n_cells = static_cast<int>(cells.size());
+    t.n_points = static_cast<int>(points.size());
+    t.fp32 = ctxs[0]->prm.precision == GELIOS_PREC_FP32_FLUX;
+    B->host_inst.resize(static_cast<size_t>(n));
+    *out = B.release();
+    return GELIOS_OK;
+}
+
+extern "C" void gelios_batch_destroy(gelios_batch* batch) {
+    if (!batch) return;
+    cudaSetDevice(batch->device);
+    if (!batch->ctxs.empty()) cudaStreamSynchronize(batch->ctxs[0]->stream);
+    delete batch;
+}
+
+extern "C" int gelios_batch_step(gelios_batch* B, int form, int nsteps, gelios_status* statuses) {
+    if (!B || nsteps < 0) return GELIOS_E_ARG;
+    if (form != GELIOS_FORM_MHD_PUI) {
+        set_error("gelios_batch_step: only the MHD form is batched");
+        return GELIOS_E_ARG;
+    }
+    GELIOS_CUDA_TRY(cudaSetDevice(B->device));
+    const int n = static_cast<int>(B->ctxs.size());
+    cudaStream_t s = B->ctxs[0]->stream;
+    // order after each context's own pending work
+    for (int i = 1; i < n; i++) {
+        GELIOS_CUDA_TRY(cudaEventRecord(B->ev, B->ctxs[i]->stream));
+        GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, B->ev, 0));
+    }
+    struct Words {
+        double T[2];
+        unsigned long long acc;
+        unsigned long long counters[2];
+        int status;
+        int pad[5];
+    };
+    static_assert(sizeof(Words) == 64, "device word layout");
+    for (int i = 0; i < n; i++) {
+        gelios_ctx* c = B->ctxs[i];
+        const DevMesh& d = c->d;
+        Words w{};
+        w.T[0] = w.T[1] = c->prm.dt0;
+        w.acc = 0x7ff0000000000000ULL;
+        GELIOS_CUDA_TRY(cudaMemcpyAsync(c->words.p, &w, sizeof(w), cudaMemcpyHostToDevice, s));
+        const size_t nc = d.n_cells;
+        double* cen0 = c->cen[0].as<double>();
+        double* cen1 = c->cen[1].as<double>();
+        if (!c->cen_valid) {
+            launch_centroid(d, d.X, d.Y, cen0, cen0 + nc, cen0 + 2 * nc, c->prm.gamma, s, cen0 + 3 * nc, cen0 + 4 * nc);
+            c->cen_rp_partial = false;
+        }
+        {
+            BatchInstance& I = B->host_inst[i];
+            I.d = d;
+            I.P = c->prm;
+            I.M = c->mprm;
+            for (int q = 0; q < 2; q++) {  // b[q]: the buffers of a step with parity q
+                StepBuffers& b = I.b[q];
+                b = StepBuffers();
+                for (int k = 0; k < 5; k++) {
+                    b.cur[k] = c->field(q, k);
+                    b.nxt[k] = c->field(q ^ 1, k);
+                }
+                double* cc = q ? cen1 : cen0;
+                double* cn = q ? cen0 : cen1;
+                b.cx = cc;
+                b.cy = cc + nc;
+                b.rp = cc + 2 * nc;
+                b.vs = cc + 3 * nc;
+                b.vol = cc + 4 * nc;
+                b.cx_next = cn;
+                b.cy_next = cn + nc;
+                b.rp_next = cn + 2 * nc;
+                b.vs_next = cn + 3 * nc;
+                b.vol_next = cn + 4 * nc;
+                b.dt_cur = c->T() + q;
+                b.dt_next = c->T() + (q ^ 1);
+                b.dt_acc = c->acc();
+                b.counters = c->counters();
+                b.status = c->status();
+                I.hs[q] = c->hstate[q].as<double>();
+                I.hn[q] = c->hstate[q ^ 1].as<double>();
+            }
+            I.fl = c->flux_mhd.as<double>();
+            I.src = c->src_fixed.as<double>();
+            I.surface = c->surface.as<double>();
+        }
+    }
+    // the kernels index b[parity], hs[parity], hn[parity]
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(B->inst.p, B->host_inst.data(), static_cast<size_t>(n) * sizeof(BatchInstance),
+                                    cudaMemcpyHostToDevice, s));
+    B->tab.inst = B->inst.as<BatchInstance>();
+    int64_t launches = 0;
+    const int per_step = (B->tab.n_surf > 0) + (B->tab.n_rails > 0) + (B->tab.n_units > 0) + (B->tab.n_cells > 0) +
+                         (B->tab.n_points > 0);
+    for (int st = 0; st < nsteps; st++) {
+        const int par = st & 1;
+        if (!B->graphs_off && !B->graph[par]) {
+            cudaGraph_t g = nullptr;
+            if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                launch_batch_mhd_step(B->tab, par, s);
+                if (cudaStreamEndCapture(s, &g) != cudaSuccess || !g ||
+                    cudaGraphInstantiate(&B->graph[par], g, 0) != cudaSuccess) {
+                    B->graph[par] = nullptr;
+                    B->graphs_off = true;
+                }
+                if (g) cudaGraphDestroy(g);
+            } else {
+                B->graphs_off = true;
+            }
+            cudaGetLastError();
+        }
+        if (B->graph[par]) {
+            GELIOS_CUDA_TRY(cudaGraphLaunch(B->graph[par], s));
+        } else {
+            launch_batch_mhd_step(B->tab, par, s);
+        }
+        launches += per_step;
+    }
+    GELIOS_CUDA_TRY(cudaGetLastError());
+    // the contexts' own streams follow the batch
+    GELIOS_CUDA_TRY(cudaEventRecord(B->ev, s));
+    for (int i = 1; i < n; i++) GELIOS_CUDA_TRY(cudaStreamWaitEvent(B->ctxs[i]->stream, B->ev, 0));
+    for (int i = 0; i < n; i++) {
+        gelios_ctx* c = B->ctxs[i];
+        if (nsteps & 1) std::swap(c->cen[0].p, c->cen[1].p);
+        c->cen_valid = true;
+        if (nsteps > 0) c->cen_rp_partial = true;
+        c->launches = launches;
+    }
+    if (statuses) {
+        std::vector<Words> r(n);
+        for (int i = 0; i < n; i++)
+            GELIOS_CUDA_TRY(cudaMemcpyAsync(&r[i], B->ctxs[i]->words.p, sizeof(Words), cudaMemcpyDeviceToHost, s));
+        GELIOS_CUDA_TRY(cudaStreamSynchronize(s));
+        for (int i = 0; i < n; i++) {
+            gelios_status& o = statuses[i];
+            std::memset(&o, 0, sizeof(o));
+            o.flags = r[i].status;
+            o.steps_done = nsteps;
+            o.n_ro_clamp = static_cast<int64_t>(r[i].counters[0]);
+            o.n_p_clamp = static_cast<int64_t>(r[i].counters[1]);
+            o.result_buf = nsteps & 1;
+            o.dt = r[i].T[nsteps & 1];
+            if (!(o.dt == o.dt)) o.flags |= ST_DT_BAD;
+        }
+    }
+    return GELIOS_OK;
+}
+
 extern "C" int gelios_download_points(gelios_ctx* ctx, double* x, double* y) {
     if (!ctx || !x || !y) return GELIOS_E_ARG;
     if (!ctx->have_mesh) return GELIOS_E_STATE;

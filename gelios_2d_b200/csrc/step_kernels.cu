@@ -1450,9 +1450,9 @@ __device__ __forceinline__ void c0_key(const DevMesh& d, int q, double dt, doubl
 // n_outer_shock the outer-shock key height of the last D rail before them
 // (Setka.cpp:4725-4728); Move_Setka_Calculate (Setka.cpp:4761-5147, used by
 // Go_5_komponent) is otherwise the same and moves them on their own.
-__global__ void __launch_bounds__(128) rails_kernel(DevMesh d, gelios_params P, const double* __restrict__ dtp,
-                                                    const double* __restrict__ scratch, bool copy_outer_shock) {
-    const int q = blockIdx.x;
+// One rail q (the body of rails_kernel; every thread of the block calls it).
+__device__ __forceinline__ void rails_body(const DevMesh& d, const gelios_params& P, const double* __restrict__ dtp,
+                                           const double* __restrict__ scratch, bool copy_outer_shock, int q) {
     const double dt = *dtp;
     const int32_t* ap = d.rpts + d.rpstart[q];
     const int np = d.rpstart[q + 1] - d.rpstart[q];
@@ -1646,6 +1646,11 @@ __global__ void __launch_bounds__(128) rails_kernel(DevMesh d, gelios_params P, 
     }
 }
 
+__global__ void __launch_bounds__(128) rails_kernel(DevMesh d, gelios_params P, const double* __restrict__ dtp,
+                                                    const double* __restrict__ scratch, bool copy_outer_shock) {
+    rails_body(d, P, dtp, scratch, copy_outer_shock, blockIdx.x);
+}
+
 // ------------------------------------------------------------------ surface tracking
 // Get_par_TVD of a main/copy face f read through the face table.
 __device__ St5 face_tvd(const DevMesh& d, const double* const* st, const double* cx, const double* cy, int f,
@@ -1676,12 +1681,11 @@ __device__ St5 face_tvd(const DevMesh& d, const double* const* st, const double*
 //           outer -1 (skipped) / 0 B / 1 A and B / 2 B / 3 A
 // One warp per face: the lanes hold identical copies of the face's data, the
 // exact solver runs warp-cooperatively, lane 0 writes.
-__global__ void __launch_bounds__(64) surface_faces_kernel(DevMesh d, gelios_params P, StepBuffers b,
-                                                           double* __restrict__ scratch) {
-    const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    const int nC = d.n_lc, nI = d.n_li, nO = d.n_lo;
-    if (j >= nC + nI + nO) return;
+// Tracked face j of the concatenated lines, all 32 lanes of a warp (the
+// body of surface_faces_kernel).
+__device__ __forceinline__ void surface_face_body(const DevMesh& d, const gelios_params& P, const StepBuffers& b,
+                                                  double* __restrict__ scratch, int j, int lane) {
+    const int nC = d.n_lc, nI = d.n_li;
     const double* const* st = b.cur;
     int status = 0;
     const double ga = P.gamma, g2 = 2.0 * P.gamma;
@@ -1767,6 +1771,13 @@ __global__ void __launch_bounds__(64) surface_faces_kernel(DevMesh d, gelios_par
         out[3] = o3;
         if (status) atomicOr(b.status, status);
     }
+}
+
+__global__ void __launch_bounds__(64) surface_faces_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                           double* __restrict__ scratch) {
+    const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (j >= d.n_lc + d.n_li + d.n_lo) return;
+    surface_face_body(d, P, b, scratch, j, threadIdx.x & 31);
 }
 
 // ------------------------------------------------------------------ per-face batches (known-answer checks)
@@ -2592,14 +2603,12 @@ __device__ __forceinline__ double mhd_face_flux(double ga, const St5& iL, const 
 // 13 flux rows times S to the owner slot and their negatives to the twin,
 // CFL candidates of both fluids.  BLOCK x MINB: the launch shape (threads
 // per block, minimum resident blocks per SM, which caps the registers).
-template <typename TF, int BLOCK, int MINB>
-__global__ void __launch_bounds__(BLOCK, MINB) mhd_face_kernel(DevMesh d, gelios_params P, gelios_mhd_params M,
-                                                       StepBuffers b, const double* __restrict__ hs,
-                                                       double* __restrict__ fl) {
-    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+template <typename TF>
+__device__ __forceinline__ double mhd_face_body(const DevMesh& d, const gelios_params& P, const gelios_mhd_params& M,
+                                                const StepBuffers& b, const double* __restrict__ hs,
+                                                double* __restrict__ fl, int u, int& status) {
     double tmin_u = __longlong_as_double(0x7ff0000000000000LL);
-    int status = 0;
-    if (u < d.n_units) {
+    {
         const size_t nc = d.n_cells, ng = d.n_slots;
         const int K = d.u_cell[u], nb = d.u_nb[u];
         const uint32_t info = d.u_info[u];
@@ -2700,6 +2709,17 @@ __global__ void __launch_bounds__(BLOCK, MINB) mhd_face_kernel(DevMesh d, gelios
             }
         }
     }
+    return tmin_u;
+}
+
+template <typename TF, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) mhd_face_kernel(DevMesh d, gelios_params P, gelios_mhd_params M,
+                                                               StepBuffers b, const double* __restrict__ hs,
+                                                               double* __restrict__ fl) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    double tmin_u = __longlong_as_double(0x7ff0000000000000LL);
+    int status = 0;
+    if (u < d.n_units) tmin_u = mhd_face_body<TF>(d, P, M, b, hs, fl, u, status);
     block_reduce_commit(tmin_u, 0, 0, status, b.dt_acc, b.counters, b.status);
 }
 
@@ -2707,15 +2727,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) mhd_face_kernel(DevMesh d, gelios
 // both fluids with their axisymmetric terms (area-weighted like the
 // reference's p (vs1 + vs2)/2) and the fixed charge-exchange sources of the
 // ion momentum and energy; refills the geometry cache like mk2_update_kernel.
-__global__ void __launch_bounds__(128) mhd_update_kernel(DevMesh d, gelios_params P, StepBuffers b,
-                                                         const double* __restrict__ fl,
-                                                         const double* __restrict__ src,
-                                                         const double* __restrict__ hcur, double* __restrict__ hnxt) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    double tmark = __longlong_as_double(0x7ff0000000000000LL);
-    int nro = 0, npc = 0;
+__device__ __forceinline__ void mhd_update_body(const DevMesh& d, const gelios_params& P, const StepBuffers& b,
+                                                const double* __restrict__ fl, const double* __restrict__ src,
+                                                const double* __restrict__ hcur, double* __restrict__ hnxt, int c,
+                                                double& tmark, int& nro, int& npc) {
     const size_t ng = d.n_slots, nc = d.n_cells;
-    if (c < d.n_cells) {
+    {
         const int s0 = d.cstart[c], n = d.cstart[c + 1] - s0;
         const int32_t* con = d.contour + s0;
         double xn, yn;
@@ -2830,7 +2847,99 @@ __global__ void __launch_bounds__(128) mhd_update_kernel(DevMesh d, gelios_param
             }
         }
     }
+}
+
+__global__ void __launch_bounds__(128) mhd_update_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                         const double* __restrict__ fl,
+                                                         const double* __restrict__ src,
+                                                         const double* __restrict__ hcur, double* __restrict__ hnxt) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double tmark = __longlong_as_double(0x7ff0000000000000LL);
+    int nro = 0, npc = 0;
+    if (c < d.n_cells) mhd_update_body(d, P, b, fl, src, hcur, hnxt, c, tmark, nro, npc);
     block_reduce_commit(tmark, nro, npc, 0, b.dt_acc, b.counters, b.status);
+}
+
+// ------------------------------------------------------------------ batched MHD step
+// Many independent instances of the MHD + pickup step advance together: one
+// launch per phase (surface tracking, rails, face units, cell update,
+// commit) covers every instance.  A block finds its instance and first item
+// in a static table (a block never straddles two instances, so the CFL
+// block minimum goes to one instance's dt word) and copies the instance's
+// descriptor into shared memory; the per-item work is the bodies of the
+// one-instance kernels.
+#ifndef GELIOS_BATCH_SMEM_DESC
+#define GELIOS_BATCH_SMEM_DESC 0
+#endif
+#ifndef GELIOS_BATCH_FACE_MINB
+#define GELIOS_BATCH_FACE_MINB 4
+#endif
+#if GELIOS_BATCH_SMEM_DESC
+#define BATCH_INSTANCE(I, e)          \
+    __shared__ BatchInstance I;       \
+    load_instance(I, t.inst + (e).x);
+#else
+#define BATCH_INSTANCE(I, e) const BatchInstance& I = t.inst[(e).x];
+#endif
+__device__ __forceinline__ void load_instance(BatchInstance& dst, const BatchInstance* __restrict__ src) {
+    static_assert(sizeof(BatchInstance) % 16 == 0, "instance descriptor is copied as int4");
+    const int4* s4 = reinterpret_cast<const int4*>(src);
+    int4* d4 = reinterpret_cast<int4*>(&dst);
+    for (int i = threadIdx.x; i < static_cast<int>(sizeof(BatchInstance) / 16); i += blockDim.x) d4[i] = s4[i];
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(64) batch_surface_kernel(BatchTables t, int parity) {
+    const int2 e = t.surf[blockIdx.x];
+    BATCH_INSTANCE(I, e)
+    const int j = e.y + (threadIdx.x >> 5);
+    if (j >= I.d.n_lc + I.d.n_li + I.d.n_lo) return;
+    surface_face_body(I.d, I.P, I.b[parity], I.surface, j, threadIdx.x & 31);
+}
+
+__global__ void __launch_bounds__(128) batch_rails_kernel(BatchTables t, int parity) {
+    const int2 e = t.rails[blockIdx.x];
+    BATCH_INSTANCE(I, e)
+    rails_body(I.d, I.P, I.b[parity].dt_cur, I.surface, true, e.y);
+}
+
+template <typename TF>
+__global__ void __launch_bounds__(128, GELIOS_BATCH_FACE_MINB) batch_mhd_face_kernel(BatchTables t, int parity) {
+    const int2 e = t.units[blockIdx.x];
+    BATCH_INSTANCE(I, e)
+    const int u = e.y + threadIdx.x;
+    const StepBuffers& b = I.b[parity];
+    double tmin = __longlong_as_double(0x7ff0000000000000LL);
+    int status = 0;
+    if (u < I.d.n_units) tmin = mhd_face_body<TF>(I.d, I.P, I.M, b, I.hs[parity], I.fl, u, status);
+    block_reduce_commit(tmin, 0, 0, status, b.dt_acc, b.counters, b.status);
+}
+
+__global__ void __launch_bounds__(128) batch_mhd_update_kernel(BatchTables t, int parity) {
+    const int2 e = t.cells[blockIdx.x];
+    BATCH_INSTANCE(I, e)
+    const int c = e.y + threadIdx.x;
+    const StepBuffers& b = I.b[parity];
+    double tmark = __longlong_as_double(0x7ff0000000000000LL);
+    int nro = 0, npc = 0;
+    if (c < I.d.n_cells) mhd_update_body(I.d, I.P, b, I.fl, I.src, I.hs[parity], I.hn[parity], c, tmark, nro, npc);
+    block_reduce_commit(tmark, nro, npc, 0, b.dt_acc, b.counters, b.status);
+}
+
+__global__ void __launch_bounds__(256) batch_commit_kernel(BatchTables t, int parity) {
+    const int2 e = t.points[blockIdx.x];
+    BATCH_INSTANCE(I, e)
+    const StepBuffers& b = I.b[parity];
+    if (e.y == 0 && threadIdx.x == 0) {
+        const unsigned long long a = *b.dt_acc;
+        *b.dt_next = (a == 0x7ff0000000000000ULL) ? 100000000.0 : __longlong_as_double(static_cast<long long>(a));
+        *b.dt_acc = 0x7ff0000000000000ULL;
+    }
+    const int i = e.y + threadIdx.x;
+    if (i < I.d.n_points) {
+        I.d.X[i] = I.d.X2[i];
+        I.d.Y[i] = I.d.Y2[i];
+    }
 }
 
 // ------------------------------------------------------------------ launchers
@@ -2984,6 +3093,18 @@ void launch_mhd_faces(const DevMesh& d, const gelios_params& P, const gelios_mhd
         case 5: mhd_faces_shape<256, 1>(d, P, M, b, hcur, fl, s); break;
         default: mhd_faces_shape<128, 3>(d, P, M, b, hcur, fl, s); break;
     }
+}
+void launch_batch_mhd_step(const BatchTables& t, int parity, cudaStream_t s) {
+    if (t.n_surf > 0) batch_surface_kernel<<<t.n_surf, 64, 0, s>>>(t, parity);
+    if (t.n_rails > 0) batch_rails_kernel<<<t.n_rails, 128, 0, s>>>(t, parity);
+    if (t.n_units > 0) {
+        if (t.fp32)
+            batch_mhd_face_kernel<float><<<t.n_units, 128, 0, s>>>(t, parity);
+        else
+            batch_mhd_face_kernel<double><<<t.n_units, 128, 0, s>>>(t, parity);
+    }
+    if (t.n_cells > 0) batch_mhd_update_kernel<<<t.n_cells, 128, 0, s>>>(t, parity);
+    if (t.n_points > 0) batch_commit_kernel<<<t.n_points, 256, 0, s>>>(t, parity);
 }
 void launch_mhd_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
                        const double* src, const double* hcur, double* hnxt, cudaStream_t s) {

@@ -146,6 +146,34 @@ void launch_mhd_faces(const DevMesh& d, const gelios_params& P, const gelios_mhd
                       const double* hcur, double* fl, cudaStream_t s, int variant = 0);
 void launch_mhd_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
                        const double* src, const double* hcur, double* hnxt, cudaStream_t s);
+// ---- batched MHD step: many instances, one launch per phase
+// One instance as the batched kernels read it (each block copies its
+// instance into shared memory; the size is a multiple of 16 bytes).
+struct alignas(16) BatchInstance {
+    DevMesh d;
+    gelios_params P;
+    gelios_mhd_params M;
+    StepBuffers b[2];          // buffers of the even / odd steps of a call
+    const double* hs[2];       // extra rows read by the even / odd steps
+    double* hn[2];             // extra rows written by them
+    double* fl;                // 13 flux rows per face slot
+    const double* src;         // fixed charge-exchange sources
+    double* surface;           // Move_surface scratch
+};
+// Block -> (instance, first item) of every phase of a batched step.
+struct BatchTables {
+    const BatchInstance* inst = nullptr;
+    const int2* surf = nullptr;    // 64-thread blocks, two tracked faces each
+    const int2* rails = nullptr;   // one block per rail
+    const int2* units = nullptr;   // 128 face units per block
+    const int2* cells = nullptr;   // 128 cells per block
+    const int2* points = nullptr;  // 256 points per block (y == 0: the block that also finalises the dt)
+    int n_surf = 0, n_rails = 0, n_units = 0, n_cells = 0, n_points = 0;
+    int fp32 = 0;                  // the instances' flux precision (all equal)
+};
+// The five launches of one batched MHD step (parity: even / odd step of the call).
+void launch_batch_mhd_step(const BatchTables& t, int parity, cudaStream_t s);
+
 void launch_hllc_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s);
 void launch_hlldq_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s);
 void launch_hlld_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s);

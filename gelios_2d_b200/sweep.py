@@ -42,9 +42,10 @@ class Sweep:
     ``instances``: sequence of (mesh, params, state (5, n_cells), mc or None).
     """
 
-    def __init__(self, instances, device: int = 0, form: int = N.FORM_MK2):
+    def __init__(self, instances, device: int = 0, form: int = N.FORM_MK2, batched: bool = False):
         self.form = form
         self.items: list[Setka] = []
+        self._batch = None
         for mesh, params, st0, mc in instances:
             S = Setka(mesh, params, device)
             S.set_par(0, st0)
@@ -58,6 +59,41 @@ class Sweep:
             elif mc is not None:
                 S.set_mc(*mc)
             self.items.append(S)
+        if batched:
+            self.enable_batch()
+
+    def enable_batch(self, groups: int = 1):
+        """Advance the instances with one launch per phase (gelios_batch, the
+        MHD form only), in `groups` batches of about equal cell count, each
+        on its own stream so that the batches' phases overlap."""
+        import ctypes as C
+
+        if self.form != N.FORM_MHD_PUI:
+            raise ValueError("only the MHD form is batched")
+        L = N.lib()
+        parts = [p for p in partition(self.cells, max(1, min(groups, len(self.items)))) if p]
+        self._groups = parts
+        self._batch = []
+        for p in parts:
+            arr = (C.c_void_p * len(p))(*[self.items[i]._h.value for i in p])
+            h = C.c_void_p()
+            N.check(L.gelios_batch_create(C.byref(h), arr, len(p)), "gelios_batch_create")
+            self._batch.append(h)
+
+    def batch_step(self, n: int = 1, statuses: bool = False):
+        """n batched steps; with statuses=True waits and returns the
+        instances' statuses (in instance order)."""
+        L = N.lib()
+        out = [None] * len(self.items)
+        for h, p in zip(self._batch, self._groups):
+            if statuses:
+                st = (N.GeliosStatus * len(p))()
+                N.check(L.gelios_batch_step(h, self.form, int(n), st), "gelios_batch_step")
+                for k, i in enumerate(p):
+                    out[i] = st[k]
+            else:
+                N.check(L.gelios_batch_step(h, self.form, int(n), None), "gelios_batch_step")
+        return out if statuses else None
 
     def __len__(self) -> int:
         return len(self.items)
@@ -78,6 +114,9 @@ class Sweep:
 
     def step_async(self, n: int = 1):
         """Enqueue ``n`` steps on every instance without waiting."""
+        if self._batch is not None:
+            self.batch_step(n)
+            return
         for i in getattr(self, "order", range(len(self.items))):
             self.items[i].step_async(self.form, n)
 
@@ -94,6 +133,10 @@ class Sweep:
         return self.items[i].par(buf)
 
     def close(self):
+        if self._batch is not None:
+            for h in self._batch:
+                N.lib().gelios_batch_destroy(h)
+            self._batch = None
         for S in self.items:
             S.close()
         self.items = []

@@ -254,6 +254,21 @@ int gelios_upload_sources(gelios_ctx *ctx, const double *q1, const double *q2, c
 int gelios_io_rows(int form);
 int gelios_run_streamed(gelios_ctx *ctx, int form, int nsteps, const double *const *host_in, double *const *host_out);
 
+/* ---- batched instances (no counterpart in the reference) -------------------
+ * Many independent instances of GELIOS_FORM_MHD_PUI (a parameter sweep: each
+ * context its own grid, inflow, state and dt) advanced together: every
+ * phase of a step (surface tracking, rails, face units, cell update,
+ * commit) is one launch over all instances, the step a CUDA graph.  The
+ * contexts must live on one device, have their topology, MHD data and
+ * sources uploaded and one flux precision; the batch runs on the first
+ * context's stream and leaves each context's results where gelios_step
+ * would (par[nsteps % 2], points, dt).  statuses: n entries or NULL (then
+ * the call does not wait for the GPU). */
+typedef struct gelios_batch gelios_batch;
+int gelios_batch_create(gelios_batch **out, gelios_ctx *const *ctxs, int n);
+int gelios_batch_step(gelios_batch *batch, int form, int nsteps, gelios_status *statuses);
+void gelios_batch_destroy(gelios_batch *batch);
+
 /* ---- autotuning of launch shapes (no counterpart in the reference) ---------
  * The dominant kernel of the MHD form (its face kernel) has
  * gelios_variant_count(form) launch shapes (threads per block x resident

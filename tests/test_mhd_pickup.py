@@ -235,3 +235,29 @@ def test_mhd_launch_shapes_give_same_bits_and_autotune_keeps_state():
     assert 0 <= v < n and ms > 0.0
     d.Go_MHD_pickup(3)
     assert np.array_equal(d.par(1), ref.par(1)) and np.array_equal(d.mhd(1), ref.mhd(1))
+
+
+@pytest.mark.gpu
+def test_batched_instances_match_one_context_steps():
+    """gelios_batch (one launch per phase over all instances) against each
+    instance stepped on its own: same states, points and dt to rounding (the
+    bodies are compiled into other kernels)."""
+    from gelios_2d_b200 import sweep as sw
+
+    inst = sw.instance_set_mhd(3, seed=5, scale=(0.12, 0.2))
+    alone = sw.Sweep(inst, form=N.FORM_MHD_PUI)
+    together = sw.Sweep(inst, form=N.FORM_MHD_PUI, batched=True)
+    sa = [S.Go_MHD_pickup(3) for S in alone.items]
+    st = together.batch_step(3, statuses=True)
+    for i, (mesh, P, st0, extra) in enumerate(inst):
+        a, b = alone.items[i], together.items[i]
+        assert rel_err(b.par(1), a.par(1)) <= 1e-12
+        assert ext_err(b.mhd(1), a.mhd(1), a.par(1)) <= 1e-12
+        xa, ya = a.points()
+        xb, yb = b.points()
+        assert np.max(np.abs(xa - xb)) <= 1e-13 * np.max(np.abs(xa))
+        assert np.max(np.abs(ya - yb)) <= 1e-13 * np.max(np.abs(ya))
+        assert st[i].result_buf == 1 and st[i].steps_done == 3 and st[i].flags == sa[i].flags
+        assert abs(st[i].dt - sa[i].dt) <= 1e-12 * sa[i].dt
+    together.close()
+    alone.close()
