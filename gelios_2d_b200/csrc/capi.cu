@@ -128,12 +128,13 @@ struct gelios_ctx {
     // topology or the parameters change.
     struct StepGraph {
         int form = -1;
+        int first = 0;  // the first step of a call: the graph starts with the words' initialisation
         int parity = -1;
         const void* cen = nullptr;
         cudaGraphExec_t exec = nullptr;
         int launches = 0;
     };
-    StepGraph graphs[8];
+    StepGraph graphs[16];
     bool graphs_off = false;  // capture failed once: launch directly
     bool coop_off = false;    // the cooperative plain step could not launch once: three kernels per step
     void drop_graphs() {
@@ -927,11 +928,17 @@ int enqueue_form(gelios_ctx* ctx, const StepBuffers& b, int form) {
 // this form and these buffers (captured on first use), or launches directly
 // while phase timing is on or if capture is unavailable.  Returns the kernel
 // count or a negative error code.
-int step_graph(gelios_ctx* ctx, const StepBuffers& b, int form) {
-    if (ctx->timing || ctx->graphs_off) return enqueue_form(ctx, b, form);
+// first: the first step of a call, whose graph begins with the initialisation
+// of the dt / status words (one launch per step, not two).
+int step_graph(gelios_ctx* ctx, const StepBuffers& b, int form, bool first) {
+    if (ctx->timing || ctx->graphs_off) {
+        if (first) launch_words_init(ctx->words.p, ctx->prm.dt0, ctx->stream);
+        const int m = enqueue_form(ctx, b, form);
+        return m < 0 ? m : m + (first ? 1 : 0);
+    }
     const int parity = b.cur[0] == ctx->field(0, 0) ? 0 : 1;
     for (auto& g : ctx->graphs)
-        if (g.exec && g.form == form && g.parity == parity && g.cen == b.cx) {
+        if (g.exec && g.form == form && g.first == static_cast<int>(first) && g.parity == parity && g.cen == b.cx) {
             GELIOS_CUDA_TRY(cudaGraphLaunch(g.exec, ctx->stream));
             return g.launches;
         }
@@ -939,9 +946,12 @@ int step_graph(gelios_ctx* ctx, const StepBuffers& b, int form) {
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         cudaGetLastError();
         ctx->graphs_off = true;
-        return enqueue_form(ctx, b, form);
+        if (first) launch_words_init(ctx->words.p, ctx->prm.dt0, s);
+        const int m = enqueue_form(ctx, b, form);
+        return m < 0 ? m : m + (first ? 1 : 0);
     }
-    const int n = enqueue_form(ctx, b, form);
+    if (first) launch_words_init(ctx->words.p, ctx->prm.dt0, s);
+    const int n = enqueue_form(ctx, b, form) + (first ? 1 : 0);
     cudaGraph_t graph = nullptr;
     const cudaError_t e = cudaStreamEndCapture(s, &graph);
     cudaGraphExec_t exec = nullptr;
@@ -949,7 +959,9 @@ int step_graph(gelios_ctx* ctx, const StepBuffers& b, int form) {
         if (graph) cudaGraphDestroy(graph);
         cudaGetLastError();
         ctx->graphs_off = true;
-        return enqueue_form(ctx, b, form);
+        if (first) launch_words_init(ctx->words.p, ctx->prm.dt0, s);
+        const int m = enqueue_form(ctx, b, form);
+        return m < 0 ? m : m + (first ? 1 : 0);
     }
     cudaGraphDestroy(graph);
     gelios_ctx::StepGraph* slot = &ctx->graphs[0];
@@ -960,6 +972,7 @@ int step_graph(gelios_ctx* ctx, const StepBuffers& b, int form) {
         }
     if (slot->exec) cudaGraphExecDestroy(slot->exec);
     slot->form = form;
+    slot->first = first;
     slot->parity = parity;
     slot->cen = b.cx;
     slot->exec = exec;
@@ -998,12 +1011,16 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
         unsigned long long counters[2];
         int status;
         int pad[5];
-    } w{};
+    };
     static_assert(sizeof(Words) == 64, "device word layout");
-    w.T[0] = w.T[1] = P.dt0;
-    w.acc = 0x7ff0000000000000ULL;
-    GELIOS_CUDA_TRY(cudaMemcpyAsync(ctx->words.p, &w, sizeof(w), cudaMemcpyHostToDevice, s));
+    // the moving-grid and MHD forms initialise the words in their first
+    // step (inside its graph); the others here
+    const bool graph_form = form == GELIOS_FORM_MK2 || mhd;
     int64_t launches = 0;
+    if (!graph_form || nsteps == 0) {
+        launch_words_init(ctx->words.p, P.dt0, s);
+        launches = 1;
+    }
     double* cen0 = ctx->cen[0].as<double>();
     double* cen1 = ctx->cen[1].as<double>();
     if (ctx->ev_used > 4096) ctx->collect();
@@ -1084,7 +1101,7 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             b.rp_next = cn + 2 * ncz;
             b.vs_next = cn + 3 * ncz;
             b.vol_next = cn + 4 * ncz;
-            const int n = step_graph(ctx, b, GELIOS_FORM_MHD_PUI);
+            const int n = step_graph(ctx, b, GELIOS_FORM_MHD_PUI, st == 0);
             if (n < 0) return n;
             launches += n;
         } else if (form == GELIOS_FORM_MK2) {
@@ -1100,7 +1117,7 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             b.rp_next = cn + 2 * static_cast<size_t>(d.n_cells);
             b.vs_next = cn + 3 * ncz;
             b.vol_next = cn + 4 * ncz;
-            const int n = step_graph(ctx, b, GELIOS_FORM_MK2);
+            const int n = step_graph(ctx, b, GELIOS_FORM_MK2, st == 0);
             if (n < 0) return n;
             launches += n;
         } else if (form == GELIOS_FORM_5_KOMPONENT) {
@@ -1353,13 +1370,17 @@ struct gelios_batch {
     DBuf inst, surf, rails, units, cells, points;
     BatchTables tab;
     std::vector<BatchInstance> host_inst;  // one descriptor per instance, rebuilt per call
-    cudaEvent_t ev = nullptr;
+    BatchInstance* pinned = nullptr;       // staging of the descriptors' upload (pinned: the copy is asynchronous)
+    cudaEvent_t ev = nullptr, ev_table = nullptr;
+    bool table_pending = false;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool graphs_off = false;
     ~gelios_batch() {
         for (auto& g : graph)
             if (g) cudaGraphExecDestroy(g);
         if (ev) cudaEventDestroy(ev);
+        if (ev_table) cudaEventDestroy(ev_table);
+        if (pinned) cudaFreeHost(pinned);
     }
 };
 
@@ -1415,6 +1436,8 @@ extern "C" int gelios_batch_create(gelios_batch** out, gelios_ctx* const* ctxs, 
     if (rc) return GELIOS_E_CUDA;
     GELIOS_CUDA_TRY(cudaStreamSynchronize(s));
     GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&B->ev, cudaEventDisableTiming));
+    GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&B->ev_table, cudaEventDisableTiming));
+    GELIOS_CUDA_TRY(cudaMallocHost(&B->pinned, static_cast<size_t>(n) * sizeof(BatchInstance)));
     BatchTables& t = B->tab;
     t.surf = B->surf.as<int2>();
     t.rails = B->rails.as<int2>();
@@ -1464,10 +1487,6 @@ extern "C" int gelios_batch_step(gelios_batch* B, int form, int nsteps, gelios_s
     for (int i = 0; i < n; i++) {
         gelios_ctx* c = B->ctxs[i];
         const DevMesh& d = c->d;
-        Words w{};
-        w.T[0] = w.T[1] = c->prm.dt0;
-        w.acc = 0x7ff0000000000000ULL;
-        GELIOS_CUDA_TRY(cudaMemcpyAsync(c->words.p, &w, sizeof(w), cudaMemcpyHostToDevice, s));
         const size_t nc = d.n_cells;
         double* cen0 = c->cen[0].as<double>();
         double* cen1 = c->cen[1].as<double>();
@@ -1512,11 +1531,17 @@ extern "C" int gelios_batch_step(gelios_batch* B, int form, int nsteps, gelios_s
             I.surface = c->surface.as<double>();
         }
     }
-    // the kernels index b[parity], hs[parity], hn[parity]
-    GELIOS_CUDA_TRY(cudaMemcpyAsync(B->inst.p, B->host_inst.data(), static_cast<size_t>(n) * sizeof(BatchInstance),
+    // the kernels index b[parity], hs[parity], hn[parity]; the staging is
+    // reused once the previous call's upload has been read
+    if (B->table_pending) GELIOS_CUDA_TRY(cudaEventSynchronize(B->ev_table));
+    std::memcpy(B->pinned, B->host_inst.data(), static_cast<size_t>(n) * sizeof(BatchInstance));
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(B->inst.p, B->pinned, static_cast<size_t>(n) * sizeof(BatchInstance),
                                     cudaMemcpyHostToDevice, s));
+    GELIOS_CUDA_TRY(cudaEventRecord(B->ev_table, s));
+    B->table_pending = true;
     B->tab.inst = B->inst.as<BatchInstance>();
-    int64_t launches = 0;
+    launch_batch_words_init(B->tab, n, s);  // dt0, empty accumulators: every instance starts a call
+    int64_t launches = 1;
     const int per_step = (B->tab.n_surf > 0) + (B->tab.n_rails > 0) + (B->tab.n_units > 0) + (B->tab.n_cells > 0) +
                          (B->tab.n_points > 0);
     for (int st = 0; st < nsteps; st++) {

@@ -2942,6 +2942,33 @@ __global__ void __launch_bounds__(256) batch_commit_kernel(BatchTables t, int pa
     }
 }
 
+// The dt / status words a call starts from: T[0] = T[1] = dt0, an empty CFL
+// accumulator, zero clamp counters and status (layout: T[2], acc,
+// counters[2], status).  A kernel rather than a copy from host memory: a
+// copy from pageable memory would wait for the stream to drain.
+__global__ void words_init_kernel(unsigned char* w, double dt0) {
+    double* T = reinterpret_cast<double*>(w);
+    unsigned long long* u = reinterpret_cast<unsigned long long*>(w + 16);
+    T[0] = dt0;
+    T[1] = dt0;
+    u[0] = 0x7ff0000000000000ULL;
+    u[1] = 0;
+    u[2] = 0;
+    *reinterpret_cast<int*>(w + 40) = 0;
+}
+__global__ void batch_words_init_kernel(BatchTables t, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const BatchInstance& I = t.inst[i];
+    double* T = const_cast<double*>(I.b[0].dt_cur);  // T[0]; b[1].dt_cur is T[1]
+    T[0] = I.P.dt0;
+    T[1] = I.P.dt0;
+    *I.b[0].dt_acc = 0x7ff0000000000000ULL;
+    I.b[0].counters[0] = 0;
+    I.b[0].counters[1] = 0;
+    *I.b[0].status = 0;
+}
+
 // ------------------------------------------------------------------ launchers
 namespace {
 inline int blocks_for(int n, int t) { return (n + t - 1) / t; }
@@ -3093,6 +3120,12 @@ void launch_mhd_faces(const DevMesh& d, const gelios_params& P, const gelios_mhd
         case 5: mhd_faces_shape<256, 1>(d, P, M, b, hcur, fl, s); break;
         default: mhd_faces_shape<128, 3>(d, P, M, b, hcur, fl, s); break;
     }
+}
+void launch_words_init(void* words, double dt0, cudaStream_t s) {
+    words_init_kernel<<<1, 1, 0, s>>>(static_cast<unsigned char*>(words), dt0);
+}
+void launch_batch_words_init(const BatchTables& t, int n, cudaStream_t s) {
+    if (n > 0) batch_words_init_kernel<<<blocks_for(n, 128), 128, 0, s>>>(t, n);
 }
 void launch_batch_mhd_step(const BatchTables& t, int parity, cudaStream_t s) {
     if (t.n_surf > 0) batch_surface_kernel<<<t.n_surf, 64, 0, s>>>(t, parity);

@@ -171,6 +171,10 @@ struct BatchTables {
     int n_surf = 0, n_rails = 0, n_units = 0, n_cells = 0, n_points = 0;
     int fp32 = 0;                  // the instances' flux precision (all equal)
 };
+// Words a call starts from (dt0, empty accumulator, zero counters/status),
+// on the stream: for one context / for every instance of a batch.
+void launch_words_init(void* words, double dt0, cudaStream_t s);
+void launch_batch_words_init(const BatchTables& t, int n, cudaStream_t s);
 // The five launches of one batched MHD step (parity: even / odd step of the call).
 void launch_batch_mhd_step(const BatchTables& t, int parity, cudaStream_t s);
 
