@@ -324,6 +324,34 @@ def fp32_flux_errors(mesh, params32, st0, mc, fcode, device, counts=(1, 100, 200
     return out
 
 
+def time_to_residual(mesh, params, st0, mc, form, fcode, device, tol, counted, max_steps=5_000_000,
+                     check_every=10_000) -> dict:
+    """Wall time from the seeded (cold) initial field until the density's L1
+    residual per unit time, sum|ro(n+1) - ro(n)| / (dt sum|ro(n+1)|), is at
+    most tol (checked every check_every steps), and the reference CPU step's
+    time for the same number of steps, projected from a bounded sample."""
+    import gelios_2d_b200 as g
+
+    S = g.Setka(mesh, params, device=device)
+    load_inputs(S, form, st0, mc)
+    S.synchronize()
+    t0 = time.perf_counter()
+    steps, r, dt = S.run_to_residual(fcode, tol, max_steps, check_every)
+    gpu_s = time.perf_counter() - t0
+    S.close()
+    out = {"tol": tol, "definition": "sum|ro(n+1)-ro(n)| / (dt * sum|ro(n+1)|), checked every "
+                                      f"{check_every} steps", "start": "cold (the workload's seeded initial field)",
+           "reached": r <= tol, "steps": steps, "residual": r, "dt": dt, "gpu_s": gpu_s}
+    try:
+        rate, n, threads, el = cpu_reference_rate(mesh, params, st0, mc, counted, form, budget_s=10.0)
+        out["reference_cpu_s_projected"] = steps * counted / rate
+        out["reference_cpu_sample"] = f"{n} steps on {threads} host threads ({el:.1f} s)"
+    except Exception as e:  # the reference library must be prebuilt
+        out["reference_cpu_s_projected"] = None
+        out["reference_cpu_sample"] = f"unavailable: {e}"
+    return out
+
+
 def run_sweep(args, rank: int, world: int, local: int) -> None:
     """The sweep workload: instances partitioned over the ranks by cell count,
     each rank steps its instances together (one context and graph per
@@ -457,6 +485,8 @@ def main():
     # (default), or gelios_batch: one launch per phase over the instances of each of --sweep-groups groups
     ap.add_argument("--sweep-mode", default="contexts", choices=["contexts", "batched"])
     ap.add_argument("--sweep-groups", type=int, default=1)
+    # wall time to an L1 residual per unit time (cold start), reported beside the rate
+    ap.add_argument("--residual", type=float, default=None)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -619,6 +649,9 @@ def main():
     }
     if args.precision == "fp32flux" and rank == 0:
         line["fp32_flux_errors"] = fp32_flux_errors(mesh, params, st0, mc, fcode, device, form=form)
+    if args.residual is not None and rank == 0:
+        line["time_to_residual"] = time_to_residual(mesh, params, st0, mc, form, fcode, device, args.residual,
+                                                    counted)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             rate, steps, threads, el = cpu_reference_rate(mesh, params, st0, mc, counted, form)

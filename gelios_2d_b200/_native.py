@@ -154,6 +154,9 @@ def lib() -> C.CDLL:
     L.gelios_upload_sources.argtypes = [vp, dp, dp, dp]
     L.gelios_variant_count.argtypes = [C.c_int]
     L.gelios_io_rows.argtypes = [C.c_int]
+    L.gelios_residual.argtypes = [vp, C.c_int, C.POINTER(C.c_double)]
+    L.gelios_run_to_residual.argtypes = [vp, C.c_int, C.c_double, C.c_int64, C.c_int32, C.POINTER(C.c_int64),
+                                         C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.gelios_batch_create.argtypes = [C.POINTER(vp), C.POINTER(vp), C.c_int]
     L.gelios_batch_step.argtypes = [vp, C.c_int, C.c_int, C.POINTER(GeliosStatus)]
     L.gelios_batch_destroy.argtypes = [vp]

@@ -106,6 +106,7 @@ struct gelios_ctx {
     DBuf src_fixed;  // MHD form: fixed charge-exchange sources (3 rows)
     DBuf flux_mhd;   // multi-fluid forms: 13 (MHD) or 21 (Go_5_komponent) flux rows per face slot, on first use
     int mhd_face_variant = 0;  // launch shape of the MHD face kernel (gelios_autotune)
+    DBuf resid;                // residual partial sums (gelios_residual)
     // streamed host I/O (gelios_run_streamed): copy streams, staging
     // buffers and their events, created on first use
     cudaStream_t io_h2d = nullptr, io_d2h = nullptr;
@@ -1191,6 +1192,47 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
         status->dt = r.T[nsteps & 1];
         if (!(status->dt == status->dt)) status->flags |= ST_DT_BAD;
     }
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_residual(gelios_ctx* ctx, int result_buf, double* residual) {
+    if (!ctx || !residual || result_buf < 0 || result_buf > 1) return GELIOS_E_ARG;
+    if (!ctx->have_mesh) return GELIOS_E_STATE;
+    GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
+    const size_t need = kResidualScratch * sizeof(double);
+    if (ctx->resid.bytes != need && ctx->resid.alloc(need)) return GELIOS_E_CUDA;
+    cudaStream_t s = ctx->stream;
+    launch_residual(ctx->field(result_buf, 0), ctx->field(result_buf ^ 1, 0), ctx->d.n_cells, ctx->resid.as<double>(),
+                    s);
+    double r[2] = {0.0, 0.0};
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(r, ctx->resid.p, sizeof(r), cudaMemcpyDeviceToHost, s));
+    GELIOS_CUDA_TRY(cudaStreamSynchronize(s));
+    *residual = r[1] > 0.0 ? r[0] / r[1] : 0.0;
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_run_to_residual(gelios_ctx* ctx, int form, double tol, int64_t max_steps, int32_t check_every,
+                                      int64_t* steps_done, double* residual_per_time, double* dt) {
+    if (!ctx || check_every <= 0 || (check_every & 1) || max_steps < 0) return GELIOS_E_ARG;
+    int64_t done = 0;
+    double rpt = 0.0, last_dt = 0.0;
+    while (done < max_steps) {
+        const int n = static_cast<int>(std::min<int64_t>(check_every, max_steps - done) & ~1);
+        if (n <= 0) break;
+        gelios_status st{};
+        int rc = gelios_step(ctx, form, n, &st);
+        if (rc) return rc;
+        done += n;
+        double r = 0.0;
+        rc = gelios_residual(ctx, st.result_buf, &r);
+        if (rc) return rc;
+        last_dt = st.dt;
+        rpt = last_dt > 0.0 ? r / last_dt : 0.0;
+        if (rpt <= tol) break;
+    }
+    if (steps_done) *steps_done = done;
+    if (residual_per_time) *residual_per_time = rpt;
+    if (dt) *dt = last_dt;
     return GELIOS_OK;
 }
 

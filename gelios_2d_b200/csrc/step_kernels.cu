@@ -2969,6 +2969,44 @@ __global__ void batch_words_init_kernel(BatchTables t, int n) {
     *I.b[0].status = 0;
 }
 
+// ------------------------------------------------------------------ residual
+// L1 change of one state row between the two buffers: per block the sums
+// of |a - b| and |a| in a fixed order, then one block adds the partials in
+// block order (deterministic, no atomics).
+__global__ void __launch_bounds__(256) residual_partial_kernel(const double* __restrict__ a,
+                                                               const double* __restrict__ b, int n,
+                                                               double* __restrict__ part) {
+    __shared__ double sd[256], sa[256];
+    double dsum = 0.0, asum = 0.0;
+    for (int i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256) {
+        dsum += fabs(a[i] - b[i]);
+        asum += fabs(a[i]);
+    }
+    sd[threadIdx.x] = dsum;
+    sa[threadIdx.x] = asum;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            sd[threadIdx.x] += sd[threadIdx.x + o];
+            sa[threadIdx.x] += sa[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = sd[0];
+        part[2 * blockIdx.x + 1] = sa[0];
+    }
+}
+__global__ void residual_final_kernel(const double* __restrict__ part, int nb, double* __restrict__ out) {
+    double d = 0.0, s = 0.0;
+    for (int k = 0; k < nb; k++) {
+        d += part[2 * k];
+        s += part[2 * k + 1];
+    }
+    out[0] = d;
+    out[1] = s;
+}
+
 // ------------------------------------------------------------------ launchers
 namespace {
 inline int blocks_for(int n, int t) { return (n + t - 1) / t; }
@@ -3120,6 +3158,12 @@ void launch_mhd_faces(const DevMesh& d, const gelios_params& P, const gelios_mhd
         case 5: mhd_faces_shape<256, 1>(d, P, M, b, hcur, fl, s); break;
         default: mhd_faces_shape<128, 3>(d, P, M, b, hcur, fl, s); break;
     }
+}
+int launch_residual(const double* a, const double* b, int n, double* scratch, cudaStream_t s) {
+    const int nb = n > 0 ? (blocks_for(n, 256) < 296 ? blocks_for(n, 256) : 296) : 1;
+    residual_partial_kernel<<<nb, 256, 0, s>>>(a, b, n, scratch + 2);
+    residual_final_kernel<<<1, 1, 0, s>>>(scratch + 2, nb, scratch);
+    return 2;
 }
 void launch_words_init(void* words, double dt0, cudaStream_t s) {
     words_init_kernel<<<1, 1, 0, s>>>(static_cast<unsigned char*>(words), dt0);

@@ -171,6 +171,10 @@ struct BatchTables {
     int n_surf = 0, n_rails = 0, n_units = 0, n_cells = 0, n_points = 0;
     int fp32 = 0;                  // the instances' flux precision (all equal)
 };
+// sum |a - b| and sum |a| over n doubles into scratch[0], scratch[1]
+// (scratch: 2 + 2 * 296 doubles); deterministic.  Returns the launch count.
+constexpr int kResidualScratch = 2 + 2 * 296;
+int launch_residual(const double* a, const double* b, int n, double* scratch, cudaStream_t s);
 // Words a call starts from (dt0, empty accumulator, zero counters/status),
 // on the stream: for one context / for every instance of a batch.
 void launch_words_init(void* words, double dt0, cudaStream_t s);

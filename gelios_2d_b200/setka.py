@@ -185,6 +185,20 @@ class Setka:
         f = lambda a: np.ascontiguousarray(a, np.float64).ravel()  # noqa: E731
         N.check(self._L.gelios_upload_sources(self._h, f(q1), f(q2), f(q3)), "gelios_upload_sources")
 
+    def residual(self, result_buf: int) -> float:
+        """L1 residual of the density over the last step (result_buf newer)."""
+        r = C.c_double()
+        N.check(self._L.gelios_residual(self._h, int(result_buf), C.byref(r)), "gelios_residual")
+        return float(r.value)
+
+    def run_to_residual(self, form: int, tol: float, max_steps: int, check_every: int = 20000):
+        """Calls of check_every steps until residual / dt <= tol; returns
+        (steps run, residual per unit time, dt)."""
+        n, r, dt = C.c_int64(), C.c_double(), C.c_double()
+        N.check(self._L.gelios_run_to_residual(self._h, int(form), float(tol), int(max_steps), int(check_every),
+                                               C.byref(n), C.byref(r), C.byref(dt)), "gelios_run_to_residual")
+        return int(n.value), float(r.value), float(dt.value)
+
     def run_streamed(self, form: int, host_in, host_out):
         """len(host_in) one-step calls of `form` with host I/O overlapped with
         the steps (gelios_run_streamed): call k reads host_in[k] into par[0]

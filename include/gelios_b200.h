@@ -238,6 +238,18 @@ int gelios_download_mhd(gelios_ctx *ctx, int buf, double *rows8);
  * momentum, energy (n_cells each); read by GELIOS_FORM_MHD_PUI. */
 int gelios_upload_sources(gelios_ctx *ctx, const double *q1, const double *q2, const double *q3);
 
+/* ---- residual (no counterpart in the reference: it has no residual) --------
+ * gelios_residual: the L1 residual of the density over the last step,
+ * sum |ro(n+1) - ro(n)| / sum |ro(n+1)| between the two state buffers
+ * (result_buf is the newer one); deterministic device reduction.
+ * gelios_run_to_residual: calls of `check_every` (even, > 0) steps of `form`
+ * until the residual per unit time, residual / dt, is at most `tol` or
+ * `max_steps` steps ran; each call restarts dt at dt0, as gelios_step does.
+ * Returns the steps run, the last residual per unit time and the dt. */
+int gelios_residual(gelios_ctx *ctx, int result_buf, double *residual);
+int gelios_run_to_residual(gelios_ctx *ctx, int form, double tol, int64_t max_steps, int32_t check_every,
+                           int64_t *steps_done, double *residual_per_time, double *dt);
+
 /* ---- streamed host I/O (no counterpart in the reference) --------------------
  * For callers that feed a fresh state from host memory every step and read
  * every result back (a host code coupled to the step, or a driver timing

@@ -323,3 +323,20 @@ def test_stationary_persistent_matches_three_kernel_steps(precision):
     assert rel_err(out[0][0], out[1][0]) <= tol
     assert abs(out[0][1] - out[1][1]) <= tol * out[1][1]
     assert out[0][2:] == out[1][2:]
+
+
+def test_residual_matches_host_and_run_to_residual_stops():
+    mesh = W.plain_mesh(36, 24)
+    P = W.plain_params()
+    st0 = W.plain_initial(mesh, P, seed=3)
+    dev = g.Setka(mesh, P)
+    dev.set_par(0, st0)
+    dev.set_par(1, st0)
+    st = dev.Go_stationary(10)
+    a, b = dev.par(st.result_buf)[0], dev.par(1 - st.result_buf)[0]
+    ref = float(np.abs(a - b).sum() / np.abs(a).sum())
+    assert abs(dev.residual(st.result_buf) - ref) <= 1e-12 * ref
+    n, r, dt = dev.run_to_residual(N.FORM_STATIONARY, 1e300, 1000, 100)
+    assert n == 100 and r <= 1e300 and dt > 0
+    n, r, dt = dev.run_to_residual(N.FORM_STATIONARY, 0.0, 300, 100)
+    assert n == 300 and r > 0.0
