@@ -472,13 +472,62 @@ def run_sweep(args, rank: int, world: int, local: int) -> None:
         print(json.dumps(line), flush=True)
 
 
+def run_warm_start(args, rank: int) -> None:
+    """The learned warm start on the plain problem (the Go_stationary form on
+    the polar grid of --ws-grid): converged training states from the batched
+    solver, the network trained on the GPU, then held-out parameter sets
+    marched to an L1 residual per unit time of --ws-tol from the cold start,
+    the nearest training state, the network's prediction and the nearest
+    state moved by the network.  value = wall time of the batched warm
+    (network) FP64 solve of all held-out instances."""
+    if rank != 0:
+        return
+    from gelios_2d_b200 import _native as N
+    from gelios_2d_b200 import warmstart as W
+    from gelios_2d_b200.mesh import Mesh
+
+    nt, nr = (int(v) for v in args.ws_grid.split("x"))
+    mesh = Mesh.polar(nt, nr, 1.0, 600.0)
+    t0 = time.perf_counter()
+    out, _ = W.experiment(mesh, n_train=args.ws_train, n_test=args.ws_test, tol=args.ws_tol,
+                          train=dict(iters=args.ws_iters), n_serial=2, fp32_max_steps=100_000)
+    total = time.perf_counter() - t0
+    theta = [0.005, 0.06, 2.0, 1.0, 10.0]
+    params = W.inflow_params(theta)
+    st0 = W.cold_state(mesh, params)
+    counted = int(np.sum(mesh["cell_type"] != 5))
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            rate, steps, threads, el = cpu_reference_rate(mesh, params, st0, None, counted, "plain", budget_s=10.0)
+            proj = out["cold_fp64"]["steps_mean"] * counted * args.ws_test / rate
+            cpu = {"value": proj, "unit": "s", "cores": threads, "kind": "reference",
+                   "sample": f"{steps} reference Go_stationary steps on {threads} host threads ({el:.1f} s); "
+                             f"projected for cold solves of the {args.ws_test} held-out instances one after another"}
+        except Exception as e:  # the reference library must be prebuilt
+            cpu = {"value": None, "unavailable": str(e)}
+    warm = out["warm_fp64"]
+    line = {"metric": f"wall time to L1 residual {args.ws_tol:g} per unit time, {args.ws_test} held-out instances "
+                      "(batched, network warm start)",
+            "value": warm["wall_s"], "unit": "s", "n_gpus": 1, "steps": int(sum(warm["steps"])), "warmup": 0,
+            "ms_per_step": None, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 step; bf16 GEMMs with fp32 accumulation in the network",
+            "data": "synthetic (seeded inflow parameter sets, seeded initial fields)",
+            "config": {"workload": f"learned warm start, plain problem on the {nt} x {nr} polar grid",
+                       "cells": int(mesh.n_cells), "n_train": args.ws_train, "n_test": args.ws_test,
+                       "tol": args.ws_tol, "network": "7 inputs + 24 Fourier features -> 5 x 256 GELU -> 5",
+                       "l2": "state and network resident in L2 (small instances)"},
+            "warm_start": out, "wall_s_total": total, "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mk2_200k", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="mk2_200k", choices=sorted(WORKLOADS) + ["warm_start"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32flux"])
     # sweep64 only: one context and captured step graph per instance, autotuned and enqueued together
@@ -487,6 +536,12 @@ def main():
     ap.add_argument("--sweep-groups", type=int, default=1)
     # wall time to an L1 residual per unit time (cold start), reported beside the rate
     ap.add_argument("--residual", type=float, default=None)
+    # warm_start only: polar grid, training / held-out parameter sets, residual tolerance, training steps
+    ap.add_argument("--ws-grid", default="90x60")
+    ap.add_argument("--ws-train", type=int, default=256)
+    ap.add_argument("--ws-test", type=int, default=32)
+    ap.add_argument("--ws-tol", type=float, default=1e-6)
+    ap.add_argument("--ws-iters", type=int, default=16000)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -496,6 +551,13 @@ def main():
 
     if args.impl == "reference" and rank != 0:
         return  # the reference arm runs on rank 0 only
+    if args.workload == "warm_start":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no warm start; its cold "
+                              "solves are projected in this workload's cpu_baseline"}))
+            return
+        run_warm_start(args, rank)
+        return
     if args.workload in ("sweep16", "sweep64"):
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the sweep workload has no reference arm; "

@@ -160,6 +160,24 @@ def lib() -> C.CDLL:
     L.gelios_batch_create.argtypes = [C.POINTER(vp), C.POINTER(vp), C.c_int]
     L.gelios_batch_step.argtypes = [vp, C.c_int, C.c_int, C.POINTER(GeliosStatus)]
     L.gelios_batch_destroy.argtypes = [vp]
+    L.gelios_plain_batch_create.argtypes = [C.POINTER(vp), C.POINTER(vp), C.c_int]
+    L.gelios_plain_batch_step.argtypes = [vp, C.c_int, C.POINTER(GeliosStatus)]
+    L.gelios_plain_batch_run_to_residual.argtypes = [vp, C.c_double, C.c_int64, C.c_int32, C.c_void_p, C.c_void_p,
+                                                     C.c_void_p]
+    L.gelios_plain_batch_destroy.argtypes = [vp]
+    fp = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+    L.gelios_mlp_create.argtypes = [C.POINTER(vp), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+    L.gelios_mlp_destroy.argtypes = [vp]
+    L.gelios_mlp_param_count.restype = C.c_int64
+    L.gelios_mlp_param_count.argtypes = [vp]
+    L.gelios_mlp_set_params.argtypes = [vp, fp, C.c_int64]
+    L.gelios_mlp_get_params.argtypes = [vp, fp, C.c_int64]
+    L.gelios_mlp_loss_grad.argtypes = [vp, fp, fp, C.c_int, C.POINTER(C.c_double), C.c_void_p]
+    L.gelios_mlp_set_data.argtypes = [vp, fp, fp, C.c_int64]
+    L.gelios_mlp_train.argtypes = [vp, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, C.c_uint64, C.c_void_p]
+    L.gelios_mlp_predict.argtypes = [vp, fp, C.c_int64, fp]
+    L.gelios_mlp_gemm_bf16.argtypes = [C.c_int, C.c_int, C.c_int, vp, C.c_int64, C.c_int64, vp, C.c_int64,
+                                       C.c_int64, vp, C.c_int64, vp]
     L.gelios_run_streamed.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
     L.gelios_autotune.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
     L.gelios_set_variant.argtypes = [vp, C.c_int, C.c_int32]

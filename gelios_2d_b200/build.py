@@ -25,7 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # reference's x86-64 build rounds twice (<= 1 ulp per operation, inside the
 # 1e-12-per-step parity bound the tests enforce).
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=true", "-Xcompiler", "-fPIC", "-Xptxas", "-O3"]
-CUDA_SOURCES = ["step_kernels.cu", "capi.cu", "noalloc.cu"]
+CUDA_SOURCES = ["step_kernels.cu", "capi.cu", "noalloc.cu", "mlp.cu"]
 HOST_SOURCES = ["mesh.cpp", "common.cpp"]
 
 

@@ -1733,3 +1733,212 @@ extern "C" int gelios_hlldq_batch(const gelios_params* prm, int n, const double*
 extern "C" int gelios_hlld_batch(const gelios_params* prm, int n, const double* in, double* out) {
     return run_batch(prm, n, in, 21, out, 13, B_HLLD);
 }
+
+// ------------------------------------------------------------------ plain-form batch
+// Instances of the Go_stationary form that share one mesh, advanced together
+// by one cooperative launch per chunk of steps (the converged states of an
+// inflow-parameter sweep).  Each instance keeps its own context: state,
+// parameters, flux slots and dt words.
+struct gelios_plain_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<gelios_ctx*> ctxs;
+    DBuf inst, active, resid;
+    bool fp32 = false;
+    ~gelios_plain_batch() {
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+extern "C" int gelios_plain_batch_create(gelios_plain_batch** out, gelios_ctx* const* ctxs, int n) {
+    if (!out || !ctxs || n < 1) return GELIOS_E_ARG;
+    *out = nullptr;
+    auto B = std::make_unique<gelios_plain_batch>();
+    const gelios_ctx* c0 = ctxs[0];
+    if (!c0 || !c0->have_mesh) {
+        set_error("gelios_plain_batch_create: a context without topology");
+        return GELIOS_E_STATE;
+    }
+    B->device = c0->device;
+    B->fp32 = c0->prm.precision == GELIOS_PREC_FP32_FLUX;
+    for (int i = 0; i < n; i++) {
+        gelios_ctx* c = ctxs[i];
+        if (!c || !c->have_mesh) {
+            set_error("gelios_plain_batch_create: a context without topology");
+            return GELIOS_E_STATE;
+        }
+        if (c->device != B->device || (c->prm.precision == GELIOS_PREC_FP32_FLUX) != B->fp32) {
+            set_error("gelios_plain_batch_create: contexts on different devices or with different flux precisions");
+            return GELIOS_E_ARG;
+        }
+        if (c->d.n_cells != c0->d.n_cells || c->d.n_units != c0->d.n_units || c->d.n_slots != c0->d.n_slots ||
+            c->d.n_points != c0->d.n_points) {
+            set_error("gelios_plain_batch_create: the instances must share one mesh");
+            return GELIOS_E_MESH;
+        }
+        for (int j = 0; j < i; j++)
+            if (ctxs[j] == c) {
+                set_error("gelios_plain_batch_create: a context listed twice");
+                return GELIOS_E_ARG;
+            }
+        B->ctxs.push_back(c);
+    }
+    GELIOS_CUDA_TRY(cudaSetDevice(B->device));
+    GELIOS_CUDA_TRY(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
+    if (B->inst.alloc(sizeof(PlainInstance) * n) || B->active.alloc(sizeof(int) * n) ||
+        B->resid.alloc(sizeof(double) * kResidualScratch * n))
+        return GELIOS_E_CUDA;
+    *out = B.release();
+    return GELIOS_OK;
+}
+
+extern "C" void gelios_plain_batch_destroy(gelios_plain_batch* B) {
+    if (!B) return;
+    cudaSetDevice(B->device);
+    cudaStreamSynchronize(B->stream);
+    delete B;
+}
+
+namespace {
+// Centroid caches of every instance (the plain form reads cx, cy and
+// |c|^(2 gamma) of all cells), the instance descriptors (rebuilt per call:
+// parameters and buffers may have changed), then the dt words of the listed
+// instances; the contexts' streams are drained first so their earlier work
+// is ordered before the batch's.
+int plain_batch_prepare(gelios_plain_batch* B, const std::vector<int>& list) {
+    std::vector<PlainInstance> host(B->ctxs.size());
+    for (size_t i = 0; i < B->ctxs.size(); i++) {
+        gelios_ctx* c = B->ctxs[i];
+        if ((c->prm.precision == GELIOS_PREC_FP32_FLUX) != B->fp32) {
+            set_error("gelios_plain_batch: the instances' flux precisions differ");
+            return GELIOS_E_ARG;
+        }
+        GELIOS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        if (!c->cen_valid || c->cen_rp_partial) {
+            const size_t ncz = c->d.n_cells;
+            double* cen0 = c->cen[0].as<double>();
+            launch_centroid(c->d, c->d.X, c->d.Y, cen0, cen0 + ncz, cen0 + 2 * ncz, c->prm.gamma, B->stream,
+                            cen0 + 3 * ncz, cen0 + 4 * ncz);
+            c->cen_valid = true;
+            c->cen_rp_partial = false;
+        }
+        PlainInstance& I = host[i];
+        I.P = c->prm;
+        const size_t ncz = c->d.n_cells;
+        const double* cen0 = c->cen[0].as<double>();
+        for (int par = 0; par < 2; par++) {
+            StepBuffers& b = I.b[par];
+            for (int k = 0; k < 5; k++) {
+                b.cur[k] = c->field(par, k);
+                b.nxt[k] = c->field(par ^ 1, k);
+            }
+            b.dt_cur = c->T() + par;
+            b.dt_next = c->T() + (par ^ 1);
+            b.dt_acc = c->acc();
+            b.counters = c->counters();
+            b.status = c->status();
+            b.cx = cen0;
+            b.cy = cen0 + ncz;
+            b.rp = cen0 + 2 * ncz;
+        }
+        I.fl = c->flux.as<double>();
+    }
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(B->inst.p, host.data(), sizeof(PlainInstance) * host.size(), cudaMemcpyHostToDevice,
+                                    B->stream));
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(B->active.p, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice,
+                                    B->stream));
+    launch_plain_batch_words_init(B->inst.as<PlainInstance>(), B->active.as<int>(), static_cast<int>(list.size()),
+                                  B->stream);
+    GELIOS_CUDA_TRY(cudaGetLastError());
+    return GELIOS_OK;
+}
+}  // namespace
+
+extern "C" int gelios_plain_batch_step(gelios_plain_batch* B, int nsteps, gelios_status* statuses) {
+    if (!B || nsteps < 0) return GELIOS_E_ARG;
+    GELIOS_CUDA_TRY(cudaSetDevice(B->device));
+    const int n = static_cast<int>(B->ctxs.size());
+    std::vector<int> list(n);
+    for (int i = 0; i < n; i++) list[i] = i;
+    int rc = plain_batch_prepare(B, list);
+    if (rc) return rc;
+    GELIOS_CUDA_TRY(launch_stationary_batch(B->ctxs[0]->d, B->inst.as<PlainInstance>(), B->active.as<int>(), n, nsteps,
+                                            B->fp32, B->stream));
+    GELIOS_CUDA_TRY(cudaStreamSynchronize(B->stream));
+    for (int i = 0; i < n; i++) {
+        gelios_ctx* c = B->ctxs[i];
+        c->launches = 1;
+        if (!statuses) continue;
+        double T[2];
+        unsigned long long cnt[2];
+        int flags = 0;
+        GELIOS_CUDA_TRY(cudaMemcpy(T, c->T(), sizeof(T), cudaMemcpyDeviceToHost));
+        GELIOS_CUDA_TRY(cudaMemcpy(cnt, c->counters(), sizeof(cnt), cudaMemcpyDeviceToHost));
+        GELIOS_CUDA_TRY(cudaMemcpy(&flags, c->status(), sizeof(int), cudaMemcpyDeviceToHost));
+        gelios_status& o = statuses[i];
+        std::memset(&o, 0, sizeof(o));
+        o.flags = flags;
+        o.steps_done = nsteps;
+        o.n_ro_clamp = static_cast<int64_t>(cnt[0]);
+        o.n_p_clamp = static_cast<int64_t>(cnt[1]);
+        o.result_buf = nsteps & 1;
+        o.dt = T[nsteps & 1];
+        if (!(o.dt == o.dt)) o.flags |= ST_DT_BAD;
+    }
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_plain_batch_run_to_residual(gelios_plain_batch* B, double tol, int64_t max_steps,
+                                                  int32_t check_every, int64_t* steps_done,
+                                                  double* residual_per_time, double* dt) {
+    if (!B || check_every <= 0 || (check_every & 1) || max_steps < 0) return GELIOS_E_ARG;
+    GELIOS_CUDA_TRY(cudaSetDevice(B->device));
+    const int n = static_cast<int>(B->ctxs.size());
+    std::vector<int64_t> done(n, 0);
+    std::vector<double> rpt(n, 0.0), last_dt(n, 0.0);
+    std::vector<int> list(n);
+    for (int i = 0; i < n; i++) list[i] = i;
+    std::vector<double> scratch(static_cast<size_t>(kResidualScratch) * n);
+    int64_t total = 0;
+    while (!list.empty() && total < max_steps) {
+        const int chunk = static_cast<int>(std::min<int64_t>(check_every, max_steps - total) & ~1);
+        if (chunk <= 0) break;
+        int rc = plain_batch_prepare(B, list);
+        if (rc) return rc;
+        GELIOS_CUDA_TRY(launch_stationary_batch(B->ctxs[0]->d, B->inst.as<PlainInstance>(), B->active.as<int>(),
+                                                static_cast<int>(list.size()), chunk, B->fp32, B->stream));
+        for (int i : list) {
+            gelios_ctx* c = B->ctxs[i];
+            double* sc = B->resid.as<double>() + static_cast<size_t>(kResidualScratch) * i;
+            launch_residual(c->field(0, 0), c->field(1, 0), c->d.n_cells, sc, B->stream);
+        }
+        GELIOS_CUDA_TRY(cudaGetLastError());
+        GELIOS_CUDA_TRY(cudaMemcpyAsync(scratch.data(), B->resid.p, sizeof(double) * scratch.size(),
+                                        cudaMemcpyDeviceToHost, B->stream));
+        GELIOS_CUDA_TRY(cudaStreamSynchronize(B->stream));
+        total += chunk;
+        std::vector<int> keep;
+        for (int i : list) {
+            gelios_ctx* c = B->ctxs[i];
+            double T0 = 0.0;
+            int flags = 0;
+            GELIOS_CUDA_TRY(cudaMemcpy(&T0, c->T(), sizeof(double), cudaMemcpyDeviceToHost));
+            GELIOS_CUDA_TRY(cudaMemcpy(&flags, c->status(), sizeof(int), cudaMemcpyDeviceToHost));
+            const double* sc = scratch.data() + static_cast<size_t>(kResidualScratch) * i;
+            const double r = sc[1] > 0.0 ? sc[0] / sc[1] : 0.0;
+            done[i] += chunk;
+            last_dt[i] = T0;
+            rpt[i] = T0 > 0.0 ? r / T0 : 0.0;
+            // an instance whose step reported a failure stops (its residual is kept)
+            if (!(rpt[i] <= tol) && flags == 0 && rpt[i] == rpt[i]) keep.push_back(i);
+        }
+        list.swap(keep);
+    }
+    for (gelios_ctx* c : B->ctxs) c->launches = 1;
+    for (int i = 0; i < n; i++) {
+        if (steps_done) steps_done[i] = done[i];
+        if (residual_per_time) residual_per_time[i] = rpt[i];
+        if (dt) dt[i] = last_dt[i];
+    }
+    return GELIOS_OK;
+}

@@ -771,6 +771,51 @@ __global__ void __launch_bounds__(128) stationary_persistent_kernel(DevMesh d, g
     }
 }
 
+// `nsteps` Go_stationary steps of many instances in one cooperative launch.
+// The instances share the mesh (topology and geometry) and have their own
+// parameters (inflow and inner-wind states), state buffers, flux slots and
+// dt words.  Work is dealt in 128-wide tiles of one instance each, so every
+// block folds its CFL minimum into one instance's dt word; after the cell
+// phase one thread per instance turns its minimum into the next dt.  The
+// unit and cell bodies are the one-instance kernels'.  `active` lists the
+// instances advanced by this launch (the others keep their state).
+template <typename TF>
+__global__ void __launch_bounds__(128) stationary_batch_kernel(DevMesh d, const PlainInstance* __restrict__ inst,
+                                                               const int* __restrict__ active, int n_active,
+                                                               int nsteps) {
+    cg::grid_group grid = cg::this_grid();
+    const int ut = (d.n_units + 127) / 128, ct = (d.n_cells + 127) / 128;
+    for (int st = 0; st < nsteps; st++) {
+        const int par = st & 1;
+        for (int t = blockIdx.x; t < n_active * ut; t += gridDim.x) {
+            const PlainInstance& I = inst[active[t / ut]];
+            const int u = (t % ut) * 128 + threadIdx.x;
+            double tmin = __longlong_as_double(0x7ff0000000000000LL);
+            if (u < d.n_units) tmin = stationary_unit_body<TF>(d, I.P, I.b[par], I.fl, u);
+            __syncthreads();  // the previous tile's reduction has read its shared words
+            block_reduce_commit(tmin, 0, 0, 0, I.b[par].dt_acc, I.b[par].counters, I.b[par].status);
+        }
+        grid.sync();
+        for (int t = blockIdx.x; t < n_active * ct; t += gridDim.x) {
+            const PlainInstance& I = inst[active[t / ct]];
+            const int c = (t % ct) * 128 + threadIdx.x;
+            double tmark = __longlong_as_double(0x7ff0000000000000LL);
+            int nro = 0, npc = 0;
+            if (c < d.n_cells) stationary_update_body(d, I.P, I.b[par], I.fl, c, tmark, nro, npc);
+            __syncthreads();
+            block_reduce_commit(tmark, nro, npc, 0, I.b[par].dt_acc, I.b[par].counters, I.b[par].status);
+        }
+        grid.sync();
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n_active; k += gridDim.x * blockDim.x) {
+            const StepBuffers& b = inst[active[k]].b[par];
+            const unsigned long long a = *b.dt_acc;
+            *b.dt_next = (a == 0x7ff0000000000000ULL) ? 100000000.0 : __longlong_as_double(static_cast<long long>(a));
+            *b.dt_acc = 0x7ff0000000000000ULL;
+        }
+        grid.sync();
+    }
+}
+
 // Go_5_komponent__MK2 face reconstruction of one side (Setka.cpp:10213-10276)
 // for a Usualy face: owner M (state Ms, centre Mx,My, flags mf), across the
 // face the cell So; Sd = Sosed_down of the face as seen from M.
@@ -3048,6 +3093,41 @@ cudaError_t launch_stationary_persistent(const DevMesh& d, const gelios_params& 
     int n = nsteps;
     void* args[] = {&dd, &pp, &c0, &c1, &flp, &n};
     return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(128), args, 0, s);
+}
+cudaError_t launch_stationary_batch(const DevMesh& d, const PlainInstance* inst, const int* active, int n_active,
+                                    int nsteps, bool fp32, cudaStream_t s) {
+    if (n_active <= 0 || nsteps <= 0) return cudaSuccess;
+    const void* fn = fp32 ? reinterpret_cast<const void*>(&stationary_batch_kernel<float>)
+                          : reinterpret_cast<const void*>(&stationary_batch_kernel<double>);
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 128, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
+    const int64_t tiles = static_cast<int64_t>(n_active) * blocks_for(d.n_units > d.n_cells ? d.n_units : d.n_cells, 128);
+    const int grid = tiles < static_cast<int64_t>(per_sm) * sms ? static_cast<int>(tiles) : per_sm * sms;
+    DevMesh dd = d;
+    const PlainInstance* ip = inst;
+    const int* ap = active;
+    int na = n_active, n = nsteps;
+    void* args[] = {&dd, &ip, &ap, &na, &n};
+    return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(128), args, 0, s);
+}
+__global__ void plain_batch_words_init_kernel(const PlainInstance* inst, const int* active, int n) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const PlainInstance& I = inst[active[k]];
+    double* T = const_cast<double*>(I.b[0].dt_cur);  // T[0]; b[1].dt_cur is T[1]
+    T[0] = I.P.dt0;
+    T[1] = I.P.dt0;
+    *I.b[0].dt_acc = 0x7ff0000000000000ULL;
+    I.b[0].counters[0] = 0;
+    I.b[0].counters[1] = 0;
+    *I.b[0].status = 0;
+}
+void launch_plain_batch_words_init(const PlainInstance* inst, const int* active, int n, cudaStream_t s) {
+    if (n > 0) plain_batch_words_init_kernel<<<blocks_for(n, 128), 128, 0, s>>>(inst, active, n);
 }
 void launch_mk2_recon(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* rec, cudaStream_t s) {
     constexpr int kLanes = 1;

@@ -112,6 +112,18 @@ void launch_stationary_update(const DevMesh& d, const gelios_params& P, const St
 // b1: odd steps); returns the launch's error code.
 cudaError_t launch_stationary_persistent(const DevMesh& d, const gelios_params& P, const StepBuffers& b0,
                                          const StepBuffers& b1, double* fl, int nsteps, cudaStream_t s);
+// Instances of the plain form that share one mesh: parameters, the buffers
+// of even / odd steps (dt words included) and the flux slots of each.
+struct PlainInstance {
+    gelios_params P;
+    StepBuffers b[2];
+    double* fl;
+};
+// `nsteps` steps of the instances listed in `active` (device arrays) in one
+// cooperative launch; returns the launch's error code.
+cudaError_t launch_stationary_batch(const DevMesh& d, const PlainInstance* inst, const int* active, int n_active,
+                                    int nsteps, bool fp32, cudaStream_t s);
+void launch_plain_batch_words_init(const PlainInstance* inst, const int* active, int n, cudaStream_t s);
 void launch_mk2_recon(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* rec, cudaStream_t s);
 int launch_mk2_flux_plain(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
                           double* fl, cudaStream_t s);

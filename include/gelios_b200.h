@@ -281,6 +281,67 @@ int gelios_batch_create(gelios_batch **out, gelios_ctx *const *ctxs, int n);
 int gelios_batch_step(gelios_batch *batch, int form, int nsteps, gelios_status *statuses);
 void gelios_batch_destroy(gelios_batch *batch);
 
+/* ---- batched plain-form instances (no counterpart in the reference) --------
+ * Instances of GELIOS_FORM_STATIONARY that share one mesh (the contexts
+ * were given the same gelios_mesh_view) and differ in parameters (inflow
+ * and inner-wind states) and state: an inflow-parameter sweep marched to a
+ * steady state.  All listed instances advance in one cooperative launch per
+ * call (each with its own dt); results stay where gelios_step would leave
+ * them (par[nsteps % 2] of each context).  Contexts must live on one device
+ * and share one flux precision; the batch drains their streams before it
+ * runs.
+ * gelios_plain_batch_step: `nsteps` steps of every instance; statuses: n
+ * entries or NULL.
+ * gelios_plain_batch_run_to_residual: gelios_run_to_residual for every
+ * instance at once: chunks of `check_every` (even) steps, after each chunk
+ * the instances whose residual per unit time is at most `tol` (or whose
+ * step reported a failure flag) stop; the others go on until `max_steps`.
+ * Per instance (arrays of n, each may be NULL): steps run, last residual
+ * per unit time, last dt. */
+typedef struct gelios_plain_batch gelios_plain_batch;
+int gelios_plain_batch_create(gelios_plain_batch **out, gelios_ctx *const *ctxs, int n);
+int gelios_plain_batch_step(gelios_plain_batch *batch, int nsteps, gelios_status *statuses);
+int gelios_plain_batch_run_to_residual(gelios_plain_batch *batch, double tol, int64_t max_steps,
+                                       int32_t check_every, int64_t *steps_done, double *residual_per_time,
+                                       double *dt);
+void gelios_plain_batch_destroy(gelios_plain_batch *batch);
+
+/* ---- warm-start network (no counterpart in the reference) ------------------
+ * A coordinate MLP trained and evaluated on the GPU by the library's own
+ * kernels: bf16 tensor-core GEMMs with fp32 accumulation, GELU, mean squared
+ * error, Adam on fp32 master weights.  Rows of n_in raw inputs; the network
+ * input is the raw row followed by sin(2^f pi s), cos(2^f pi s), f <
+ * n_fourier, of its last two entries (the position), i.e. n_in + 4
+ * n_fourier values; then `depth` hidden layers of `width` with GELU and a
+ * linear output layer of n_out.  Parameters are one flat fp32 vector: per
+ * layer the weight [out][in] (row-major) then the bias [out].
+ * gelios_mlp_set_params also resets the Adam moments and step count.
+ * gelios_mlp_loss_grad: mean squared error of M (<= max_batch) host rows
+ * against host targets and (grad != NULL) its gradient, without an update.
+ * gelios_mlp_set_data: the training set (host rows), kept on the device.
+ * gelios_mlp_train: `iters` Adam steps on mini-batches of `batch` rows drawn
+ * from the training set by a hash of (seed, step, row); learning rate linear
+ * from 0 over `warmup` steps, then cosine from lr_max down to lr_min; the
+ * batch loss of every step into loss_hist (iters floats, may be NULL).
+ * gelios_mlp_predict: outputs of M host rows (in chunks of max_batch).
+ * gelios_mlp_gemm_bf16: the GEMM alone (device pointers; C = A . B with
+ * A[m][k] at A[m a_m + k a_k], B[k][n] at B[k b_k + n b_n], C fp32 rows of
+ * ldc; stream may be NULL), for checks. */
+typedef struct gelios_mlp gelios_mlp;
+int gelios_mlp_create(gelios_mlp **out, int device, int n_in, int n_fourier, int width, int depth, int n_out,
+                      int max_batch);
+void gelios_mlp_destroy(gelios_mlp *mlp);
+int64_t gelios_mlp_param_count(const gelios_mlp *mlp);
+int gelios_mlp_set_params(gelios_mlp *mlp, const float *params, int64_t n);
+int gelios_mlp_get_params(const gelios_mlp *mlp, float *params, int64_t n);
+int gelios_mlp_loss_grad(gelios_mlp *mlp, const float *x, const float *t, int M, double *loss, float *grad);
+int gelios_mlp_set_data(gelios_mlp *mlp, const float *x, const float *t, int64_t n_rows);
+int gelios_mlp_train(gelios_mlp *mlp, int iters, int batch, float lr_max, float lr_min, int warmup, uint64_t seed,
+                     float *loss_hist);
+int gelios_mlp_predict(gelios_mlp *mlp, const float *x, int64_t M, float *y);
+int gelios_mlp_gemm_bf16(int M, int N, int K, const void *A, int64_t a_m, int64_t a_k, const void *B, int64_t b_k,
+                         int64_t b_n, float *C, int64_t ldc, void *stream);
+
 /* ---- autotuning of launch shapes (no counterpart in the reference) ---------
  * The dominant kernel of the MHD form (its face kernel) has
  * gelios_variant_count(form) launch shapes (threads per block x resident
