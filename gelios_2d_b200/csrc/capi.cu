@@ -124,6 +124,10 @@ struct gelios_ctx {
     // holds only the CF_RP cells, which the other forms do not accept
     bool cen_valid = false;
     bool cen_rp_partial = false;
+    // |face centre|^(2 gamma) per face unit for the plain form; stale once
+    // the points move, the topology or gamma changes
+    DBuf upf;
+    bool upf_valid = false;
     // Instantiated graphs of one moving-grid step, keyed by the buffers the
     // step reads (state parity and centroid buffer); dropped whenever the
     // topology or the parameters change.
@@ -273,6 +277,7 @@ extern "C" int gelios_set_params(gelios_ctx* ctx, const gelios_params* prm) {
     if (!ctx || !prm) return GELIOS_E_ARG;
     ctx->prm = *prm;
     ctx->cen_valid = false;  // the cached |centroid|^(2 gamma) depends on gamma
+    ctx->upf_valid = false;
     ctx->drop_graphs();      // the parameters are kernel arguments
     return GELIOS_OK;
 }
@@ -598,6 +603,7 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     rc |= upload(ctx->u_cell, u_cell.data(), u_cell.size(), s);
     rc |= upload(ctx->u_twin, u_twin.data(), u_twin.size(), s);
     rc |= upload<double>(ctx->flux, nullptr, 5 * static_cast<size_t>(ng), s);
+    rc |= upload<double>(ctx->upf, nullptr, u_slot.size(), s);
     rc |= upload<double>(ctx->aux, nullptr, 3 * static_cast<size_t>(nc), s);
     rc |= upload<double>(ctx->rec, nullptr, static_cast<size_t>(kRecRows) * u_slot.size(), s);
     rc |= upload<double>(ctx->pstar, nullptr, static_cast<size_t>(u_tr1 - u_tr0) + 1, s);
@@ -719,6 +725,7 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     ctx->have_mesh = true;
     ctx->n_inner = 0;
     ctx->cen_valid = false;
+    ctx->upf_valid = false;
     ctx->drop_graphs();
     return GELIOS_OK;
 }
@@ -1048,6 +1055,11 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
         launches++;
         ctx->cen_rp_partial = false;
     }
+    if (form == GELIOS_FORM_STATIONARY && !ctx->upf_valid && nsteps > 0) {
+        launch_unit_pf(d, P.gamma, ctx->upf.as<double>(), s);
+        launches++;
+        ctx->upf_valid = true;
+    }
     int first = 0;
     if (form == GELIOS_FORM_STATIONARY && nsteps > 0 && !ctx->timing && !ctx->coop_off) {
         // all steps of the plain form in one cooperative launch
@@ -1066,6 +1078,7 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             b.cx = cen0;
             b.cy = cen0 + ncz;
             b.rp = cen0 + 2 * ncz;
+            b.upf = ctx->upf.as<double>();
         }
         if (launch_stationary_persistent(d, P, bb[0], bb[1], ctx->flux.as<double>(), nsteps, s) == cudaSuccess) {
             launches += 1;
@@ -1153,6 +1166,7 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             b.cy = cen0 + d.n_cells;
             b.rp = cen0 + 2 * static_cast<size_t>(d.n_cells);
             if (form == GELIOS_FORM_STATIONARY) {
+                b.upf = ctx->upf.as<double>();
                 cudaEvent_t e1 = ctx->phase_begin();
                 launch_stationary_units(d, P, b, ctx->flux.as<double>(), s);
                 ctx->phase_end(1, e1, 1);
@@ -1178,7 +1192,10 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
     // steps they sit in the second buffer; swap so cen[0] holds them
     if (cached_form && (nsteps & 1)) std::swap(ctx->cen[0].p, ctx->cen[1].p);
     ctx->cen_valid = true;
-    if (cached_form && nsteps > 0) ctx->cen_rp_partial = true;
+    if (cached_form && nsteps > 0) {
+        ctx->cen_rp_partial = true;
+        ctx->upf_valid = false;
+    }
     if (status) {
         Words r{};
         GELIOS_CUDA_TRY(cudaMemcpyAsync(&r, ctx->words.p, sizeof(r), cudaMemcpyDeviceToHost, s));
@@ -1618,7 +1635,10 @@ extern "C" int gelios_batch_step(gelios_batch* B, int form, int nsteps, gelios_s
         gelios_ctx* c = B->ctxs[i];
         if (nsteps & 1) std::swap(c->cen[0].p, c->cen[1].p);
         c->cen_valid = true;
-        if (nsteps > 0) c->cen_rp_partial = true;
+        if (nsteps > 0) {
+            c->cen_rp_partial = true;
+            c->upf_valid = false;
+        }
         c->launches = launches;
     }
     if (statuses) {
@@ -1822,6 +1842,10 @@ int plain_batch_prepare(gelios_plain_batch* B, const std::vector<int>& list) {
             c->cen_valid = true;
             c->cen_rp_partial = false;
         }
+        if (!c->upf_valid) {
+            launch_unit_pf(c->d, c->prm.gamma, c->upf.as<double>(), B->stream);
+            c->upf_valid = true;
+        }
         PlainInstance& I = host[i];
         I.P = c->prm;
         const size_t ncz = c->d.n_cells;
@@ -1840,6 +1864,7 @@ int plain_batch_prepare(gelios_plain_batch* B, const std::vector<int>& list) {
             b.cx = cen0;
             b.cy = cen0 + ncz;
             b.rp = cen0 + 2 * ncz;
+            b.upf = c->upf.as<double>();
         }
         I.fl = c->flux.as<double>();
     }

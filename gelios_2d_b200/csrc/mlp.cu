@@ -2,13 +2,14 @@
 // position -> a converged state of the plain step), trained and evaluated
 // on the GPU by this file's kernels.
 //
-//   gemm_bf16_kernel      C[M,N] (fp32) = A[M,K] . B[K,N] with bf16 operands
+//   gemm_tn_kernel        C[M,N] (fp32) = A[M,K] . B[N,K]^T with bf16 operands
 //                         on the tensor cores (mma.sync m16n8k16, fp32
-//                         accumulation); A and B are read through element
-//                         strides, so the one kernel serves X.W^T (forward),
-//                         dZ.W (backward, data) and dZ^T.X (backward,
-//                         weights; split over K into partial tiles that
-//                         splitk_reduce_kernel adds in a fixed order)
+//                         accumulation), both operands k-contiguous: X.W^T
+//                         (forward), dZ.(W^T)^T (backward, data) and
+//                         (dZ^T).(H^T)^T (backward, weights; split over K
+//                         into partial tiles that splitk_reduce_kernel adds
+//                         in a fixed order)
+//   transpose_bf16_kernel the transposed operands of the backward GEMMs
 //   features_kernel       network inputs: the raw inputs, then sin / cos of
 //                         2^f pi s of the last two (the cell position), bf16
 //   gather_kernel         a mini-batch of rows of the training set, drawn by
@@ -39,68 +40,107 @@ void set_error(const std::string& msg);
 
 namespace {
 
-constexpr int TM = 64, TN = 64, TK = 32, PAD = 8;
+// GEMM tiles: 128 x 128 output per block of 8 warps (2 x 4, each warp
+// 64 x 32 = 4 x 4 tiles of m16n8), K in steps of 32; operand tiles staged
+// in shared memory rows of 40 bf16 (80 bytes: the eight 16-byte rows an
+// ldmatrix reads fall in distinct bank groups).
+constexpr int BM = 128, BN = 128, BK = 32, SPITCH = BK + 8;
+constexpr int kGemmThreads = 256;
 
-__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo, __nv_bfloat16 hi) {
-    return static_cast<uint32_t>(__bfloat16_as_ushort(lo)) | (static_cast<uint32_t>(__bfloat16_as_ushort(hi)) << 16);
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+// 16-byte asynchronous copy global -> shared; bytes beyond src_bytes are zero
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+__device__ __forceinline__ void ldmatrix_x4(uint32_t (&r)[4], const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(smem_u32(p)));
 }
 
-// 64 x 64 output tile per block of 4 warps (each warp 32 x 32: 2 x 4 tiles of
-// m16n8), operands staged in shared memory as As[m][k] and Bs[n][k]; the
-// staging walks the global operand along its unit-stride dimension.
-// blockIdx.z: K slice [z kc, (z+1) kc), written to C + z c_split.
-__global__ void __launch_bounds__(128) gemm_bf16_kernel(int M, int N, int K, int kc,
-                                                       const __nv_bfloat16* __restrict__ A, int64_t a_m, int64_t a_k,
-                                                       const __nv_bfloat16* __restrict__ B, int64_t b_k, int64_t b_n,
-                                                       float* __restrict__ C, int64_t ldc, int64_t c_split) {
-    __shared__ __nv_bfloat16 As[TM][TK + PAD];
-    __shared__ __nv_bfloat16 Bs[TN][TK + PAD];
-    const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
+// Rows row0.. (of nrows) x k k0..k0+31 (of ke) of a k-contiguous operand
+// (rows of ld elements) into S[128][SPITCH]; zeros outside.  VEC: ld and the
+// base are 16-byte aligned, so whole 8-element chunks go by cp.async.
+template <bool VEC>
+__device__ __forceinline__ void load_tile(__nv_bfloat16 (*S)[SPITCH], const __nv_bfloat16* __restrict__ G, int64_t ld,
+                                          int row0, int nrows, int k0, int ke) {
+    const __nv_bfloat16 zero = __float2bfloat16(0.f);
+    for (int c = threadIdx.x; c < BM * (BK / 8); c += kGemmThreads) {
+        const int r = c >> 2, kq = (c & 3) * 8;
+        const int gr = row0 + r, gk = k0 + kq;
+        __nv_bfloat16* dst = &S[r][kq];
+        if (VEC && gr < nrows && gk + 8 <= ke) {
+            cp_async16(smem_u32(dst), G + gr * ld + gk, 16);
+        } else if (VEC && (gr >= nrows || gk >= ke)) {
+            cp_async16(smem_u32(dst), G, 0);  // zero fill, nothing read
+        } else {
+            for (int e = 0; e < 8; e++) dst[e] = (gr < nrows && gk + e < ke) ? G[gr * ld + gk + e] : zero;
+        }
+    }
+}
+
+// C[M][N] (fp32, rows of ldc) = sum_k A[m][k] B[n][k], A and B bf16 with k
+// contiguous (rows of lda / ldb).  blockIdx.z: K slice [z kc, (z+1) kc),
+// written to C + z c_split.  Two-stage cp.async pipeline, fragments by
+// ldmatrix, mma.sync m16n8k16 bf16 -> fp32.
+template <bool AV, bool BV>
+__global__ void __launch_bounds__(kGemmThreads) gemm_tn_kernel(int M, int N, int K, int kc,
+                                                             const __nv_bfloat16* __restrict__ A, int64_t lda,
+                                                             const __nv_bfloat16* __restrict__ B, int64_t ldb,
+                                                             float* __restrict__ C, int64_t ldc, int64_t c_split) {
+    __shared__ __align__(16) __nv_bfloat16 As[2][BM][SPITCH];
+    __shared__ __align__(16) __nv_bfloat16 Bs[2][BN][SPITCH];
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     const int kb = blockIdx.z * kc, ke = min(K, kb + kc);
     C += blockIdx.z * c_split;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    const int wm = (warp >> 2) * 64, wn = (warp & 3) * 32;
     const int g = lane >> 2, t = lane & 3;
-    float acc[2][4][4];
+    float acc[4][4][4];
 #pragma unroll
-    for (int i = 0; i < 2; i++)
+    for (int i = 0; i < 4; i++)
 #pragma unroll
         for (int j = 0; j < 4; j++)
 #pragma unroll
             for (int r = 0; r < 4; r++) acc[i][j][r] = 0.f;
-    const __nv_bfloat16 zero = __float2bfloat16(0.f);
-    const bool a_kfast = a_k == 1, b_kfast = b_k == 1;
-    for (int k0 = kb; k0 < ke; k0 += TK) {
-        for (int e = threadIdx.x; e < TM * TK; e += 128) {
-            const int m = a_kfast ? e / TK : e % TM, k = a_kfast ? e % TK : e / TM;
-            const int gm = m0 + m, gk = k0 + k;
-            As[m][k] = (gm < M && gk < ke) ? A[gm * a_m + gk * a_k] : zero;
+    const int nk = ke > kb ? (ke - kb + BK - 1) / BK : 0;
+    if (nk > 0) {
+        load_tile<AV>(As[0], A, lda, m0, M, kb, ke);
+        load_tile<BV>(Bs[0], B, ldb, n0, N, kb, ke);
+    }
+    cp_async_commit();
+    // lane -> row / k offset of the 8 x 8 matrices of one ldmatrix.x4
+    const int a_row = lane & 15, a_k = (lane >> 4) << 3;
+    const int b_row = (lane & 7) + ((lane >> 4) << 3), b_k = ((lane >> 3) & 1) << 3;
+    for (int it = 0; it < nk; it++) {
+        const int cur = it & 1;
+        if (it + 1 < nk) {
+            load_tile<AV>(As[cur ^ 1], A, lda, m0, M, kb + (it + 1) * BK, ke);
+            load_tile<BV>(Bs[cur ^ 1], B, ldb, n0, N, kb + (it + 1) * BK, ke);
         }
-        for (int e = threadIdx.x; e < TN * TK; e += 128) {
-            const int n = b_kfast ? e / TK : e % TN, k = b_kfast ? e % TK : e / TN;
-            const int gn = n0 + n, gk = k0 + k;
-            Bs[n][k] = (gn < N && gk < ke) ? B[gk * b_k + gn * b_n] : zero;
-        }
+        cp_async_commit();
+        cp_async_wait1();  // the stage of this iteration has landed
         __syncthreads();
 #pragma unroll
-        for (int kk = 0; kk < TK; kk += 16) {
-            uint32_t a[2][4], b[4][2];
+        for (int kk = 0; kk < BK; kk += 16) {
+            uint32_t a[4][4], b[4][2];
 #pragma unroll
-            for (int i = 0; i < 2; i++) {
-                const int r = wm + 16 * i + g;
-                a[i][0] = pack_bf16(As[r][kk + 2 * t], As[r][kk + 2 * t + 1]);
-                a[i][1] = pack_bf16(As[r + 8][kk + 2 * t], As[r + 8][kk + 2 * t + 1]);
-                a[i][2] = pack_bf16(As[r][kk + 2 * t + 8], As[r][kk + 2 * t + 9]);
-                a[i][3] = pack_bf16(As[r + 8][kk + 2 * t + 8], As[r + 8][kk + 2 * t + 9]);
+            for (int i = 0; i < 4; i++) ldmatrix_x4(a[i], &As[cur][wm + 16 * i + a_row][kk + a_k]);
+#pragma unroll
+            for (int jp = 0; jp < 2; jp++) {
+                uint32_t r[4];
+                ldmatrix_x4(r, &Bs[cur][wn + 16 * jp + b_row][kk + b_k]);
+                b[2 * jp][0] = r[0];
+                b[2 * jp][1] = r[1];
+                b[2 * jp + 1][0] = r[2];
+                b[2 * jp + 1][1] = r[3];
             }
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int c = wn + 8 * j + g;
-                b[j][0] = pack_bf16(Bs[c][kk + 2 * t], Bs[c][kk + 2 * t + 1]);
-                b[j][1] = pack_bf16(Bs[c][kk + 2 * t + 8], Bs[c][kk + 2 * t + 9]);
-            }
-#pragma unroll
-            for (int i = 0; i < 2; i++)
+            for (int i = 0; i < 4; i++)
 #pragma unroll
                 for (int j = 0; j < 4; j++)
                     asm volatile(
@@ -109,10 +149,10 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(int M, int N, int K, int
                         : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
                         : "r"(a[i][0]), "r"(a[i][1]), "r"(a[i][2]), "r"(a[i][3]), "r"(b[j][0]), "r"(b[j][1]));
         }
-        __syncthreads();
+        __syncthreads();  // the next iteration refills the other stage, then this one
     }
 #pragma unroll
-    for (int i = 0; i < 2; i++)
+    for (int i = 0; i < 4; i++)
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             const int64_t r = m0 + wm + 16 * i + g;
@@ -122,6 +162,22 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(int M, int N, int K, int
             if (r + 8 < M && c < N) C[(r + 8) * ldc + c] = acc[i][j][2];
             if (r + 8 < M && c + 1 < N) C[(r + 8) * ldc + c + 1] = acc[i][j][3];
         }
+}
+
+// out[c][r] = in[r][c] (bf16, rows of ldin -> rows of ldout), 32 x 32 tiles
+__global__ void transpose_bf16_kernel(int R, int Cc, const __nv_bfloat16* __restrict__ in, int64_t ldin,
+                                      __nv_bfloat16* __restrict__ out, int64_t ldout) {
+    __shared__ unsigned short tile[32][33];
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const int r = r0 + y, c = c0 + threadIdx.x;
+        if (r < R && c < Cc) tile[y][threadIdx.x] = __bfloat16_as_ushort(in[r * ldin + c]);
+    }
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const int c = c0 + y, r = r0 + threadIdx.x;
+        if (r < R && c < Cc) out[c * ldout + r] = __ushort_as_bfloat16(tile[threadIdx.x][y]);
+    }
 }
 
 __global__ void splitk_reduce_kernel(int64_t n, int S, const float* __restrict__ part, float* __restrict__ out) {
@@ -298,20 +354,39 @@ struct Buf {
 // of slices
 inline int split_len(int K, int splits) {
     int kc = (K + splits - 1) / splits;
-    kc = (kc + TK - 1) / TK * TK;
-    return kc > 0 ? kc : TK;
+    kc = (kc + BK - 1) / BK * BK;
+    return kc > 0 ? kc : BK;
 }
 inline int split_count(int K, int kc) { return K > 0 ? (K + kc - 1) / kc : 1; }
 
-void gemm(int M, int N, int K, const __nv_bfloat16* A, int64_t a_m, int64_t a_k, const __nv_bfloat16* B, int64_t b_k,
-          int64_t b_n, float* C, int64_t ldc, cudaStream_t s, int splits = 1, int64_t c_split = 0) {
+inline bool vec_ok(const void* p, int64_t ld) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0 && ld % 8 == 0; }
+
+// C = A . B^T with A [M][lda], B [N][ldb] (k contiguous); see gemm_tn_kernel
+void gemm(int M, int N, int K, const __nv_bfloat16* A, int64_t lda, const __nv_bfloat16* B, int64_t ldb, float* C,
+          int64_t ldc, cudaStream_t s, int splits = 1, int64_t c_split = 0) {
     if (M <= 0 || N <= 0) return;
     const int kc = split_len(K, splits);
-    dim3 grid(blocks(N, TN), blocks(M, TM), split_count(K, kc));
-    gemm_bf16_kernel<<<grid, 128, 0, s>>>(M, N, K, kc, A, a_m, a_k, B, b_k, b_n, C, ldc, c_split);
+    dim3 grid(blocks(N, BN), blocks(M, BM), split_count(K, kc));
+    const bool av = vec_ok(A, lda), bv = vec_ok(B, ldb);
+    if (av && bv)
+        gemm_tn_kernel<true, true><<<grid, kGemmThreads, 0, s>>>(M, N, K, kc, A, lda, B, ldb, C, ldc, c_split);
+    else if (av)
+        gemm_tn_kernel<true, false><<<grid, kGemmThreads, 0, s>>>(M, N, K, kc, A, lda, B, ldb, C, ldc, c_split);
+    else if (bv)
+        gemm_tn_kernel<false, true><<<grid, kGemmThreads, 0, s>>>(M, N, K, kc, A, lda, B, ldb, C, ldc, c_split);
+    else
+        gemm_tn_kernel<false, false><<<grid, kGemmThreads, 0, s>>>(M, N, K, kc, A, lda, B, ldb, C, ldc, c_split);
 }
 
-constexpr int kMaxSplit = 16;
+inline int64_t pad8(int64_t n) { return (n + 7) / 8 * 8; }
+
+void transpose(int R, int Cc, const __nv_bfloat16* in, int64_t ldin, __nv_bfloat16* out, int64_t ldout,
+               cudaStream_t s) {
+    if (R <= 0 || Cc <= 0) return;
+    transpose_bf16_kernel<<<dim3(blocks(Cc, 32), blocks(R, 32)), dim3(32, 8), 0, s>>>(R, Cc, in, ldin, out, ldout);
+}
+
+constexpr int kMaxSplit = 32;
 
 }  // namespace
 
@@ -328,6 +403,7 @@ struct gelios_mlp {
     std::vector<Buf> h;  // bf16 inputs of every layer [max_batch][din]
     std::vector<Buf> z;  // fp32 pre-activations of every hidden layer
     Buf c, y, dh, dz, dzb, tb, rowerr, part, colpart, loss, xin;
+    Buf wt, dzt, ht;  // transposes for the backward GEMMs: W_l^T, dZ^T, H_l^T
     Buf X, T;  // training set (fp32 rows)
     int64_t n_rows = 0;
     ~gelios_mlp() {
@@ -357,7 +433,7 @@ void forward(gelios_mlp* n, int M) {
     const __nv_bfloat16* wb = n->wb.as<__nv_bfloat16>();
     for (int l = 0; l < n->layers(); l++) {
         const int di = n->din[l], dO = n->dout[l];
-        gemm(M, dO, di, n->h[l].as<__nv_bfloat16>(), di, 1, wb + n->w_off[l], 1, di, n->c.as<float>(), dO, s);
+        gemm(M, dO, di, n->h[l].as<__nv_bfloat16>(), di, wb + n->w_off[l], di, n->c.as<float>(), dO, s);
         const int64_t e = static_cast<int64_t>(M) * dO;
         const bool last = l == n->layers() - 1;
         bias_act_kernel<<<blocks(e, 256), 256, 0, s>>>(
@@ -378,16 +454,21 @@ void backward(gelios_mlp* n, int M) {
                                                    n->dzb.as<__nv_bfloat16>(), 0);
     const __nv_bfloat16* wb = n->wb.as<__nv_bfloat16>();
     float* g = n->g32.as<float>();
-    int splits = (M + 511) / 512;
+    int splits = (M + 255) / 256;
     if (splits > kMaxSplit) splits = kMaxSplit;
     if (splits < 1) splits = 1;
     const int kc = split_len(M, splits), S = split_count(M, kc);
+    const int64_t Mp = pad8(M);
+    __nv_bfloat16* dzt = n->dzt.as<__nv_bfloat16>();
+    __nv_bfloat16* ht = n->ht.as<__nv_bfloat16>();
     for (int l = L - 1; l >= 0; l--) {
         const int di = n->din[l], dO = n->dout[l];
-        // dW[dO][di] = dZ^T . H_l, split over the rows of the batch
+        // dW[dO][di] = dZ^T . H_l (both transposed so k = batch row is
+        // contiguous), split over the rows of the batch
         const int64_t wn = static_cast<int64_t>(dO) * di;
-        gemm(dO, di, M, n->dzb.as<__nv_bfloat16>(), 1, dO, n->h[l].as<__nv_bfloat16>(), di, 1, n->part.as<float>(),
-             di, s, splits, wn);
+        transpose(M, dO, n->dzb.as<__nv_bfloat16>(), dO, dzt, Mp, s);
+        transpose(M, di, n->h[l].as<__nv_bfloat16>(), di, ht, Mp, s);
+        gemm(dO, di, M, dzt, Mp, ht, Mp, n->part.as<float>(), di, s, splits, wn);
         splitk_reduce_kernel<<<blocks(wn, 256), 256, 0, s>>>(wn, S, n->part.as<float>(), g + n->w_off[l]);
         // db = column sums of dZ
         const int chunks = (M + kColRows - 1) / kColRows;
@@ -396,7 +477,9 @@ void backward(gelios_mlp* n, int M) {
         col_sum_final_kernel<<<blocks(dO, 128), 128, 0, s>>>(chunks, dO, n->colpart.as<float>(), g + n->b_off[l]);
         if (l == 0) break;
         // dH_l[M][di] = dZ . W_l, then dZ_{l-1} = dH_l * GELU'(Z_{l-1})
-        gemm(M, di, dO, n->dzb.as<__nv_bfloat16>(), dO, 1, wb + n->w_off[l], di, 1, n->dh.as<float>(), di, s);
+        transpose(dO, di, wb + n->w_off[l], di, n->wt.as<__nv_bfloat16>(), pad8(dO), s);
+        gemm(M, di, dO, n->dzb.as<__nv_bfloat16>(), dO, n->wt.as<__nv_bfloat16>(), pad8(dO), n->dh.as<float>(), di,
+             s);
         const int64_t e = static_cast<int64_t>(M) * di;
         act_bwd_kernel<<<blocks(e, 256), 256, 0, s>>>(e, n->dh.as<float>(), n->z[l - 1].as<float>(),
                                                       n->dz.as<float>(), n->dzb.as<__nv_bfloat16>(), 1);
@@ -447,7 +530,8 @@ extern "C" int gelios_mlp_create(gelios_mlp** out, int device, int n_in, int n_f
          n->dz.alloc(MB * W * 4) && n->dzb.alloc(MB * W * 2) && n->tb.alloc(MB * n_out * 4) &&
          n->rowerr.alloc(MB * 4) && n->part.alloc(static_cast<size_t>(kMaxSplit) * W * W * 4) &&
          n->colpart.alloc(((MB + kColRows - 1) / kColRows) * W * 4) && n->loss.alloc(16) &&
-         n->xin.alloc(MB * n_in * 4);
+         n->xin.alloc(MB * n_in * 4) && n->wt.alloc(W * pad8(widest) * 2) &&
+         n->dzt.alloc(W * pad8(max_batch) * 2) && n->ht.alloc(W * pad8(max_batch) * 2);
     if (!ok) return cuda_fail(cudaErrorMemoryAllocation);
     MLP_TRY(cudaMemsetAsync(n->w32.p, 0, P * 4, n->stream));
     MLP_TRY(cudaMemsetAsync(n->wb.p, 0, P * 2, n->stream));
@@ -581,11 +665,12 @@ extern "C" int gelios_mlp_predict(gelios_mlp* n, const float* x, int64_t M, floa
     return GELIOS_OK;
 }
 
-extern "C" int gelios_mlp_gemm_bf16(int M, int N, int K, const void* A, int64_t a_m, int64_t a_k, const void* B,
-                                    int64_t b_k, int64_t b_n, float* C, int64_t ldc, void* stream) {
-    if (M < 0 || N < 0 || K < 0 || !A || !B || !C) return fail("gelios_mlp_gemm_bf16: bad arguments");
-    gemm(M, N, K, static_cast<const __nv_bfloat16*>(A), a_m, a_k, static_cast<const __nv_bfloat16*>(B), b_k, b_n, C,
-         ldc, static_cast<cudaStream_t>(stream));
+extern "C" int gelios_mlp_gemm_bf16(int M, int N, int K, const void* A, int64_t lda, const void* B, int64_t ldb,
+                                    float* C, int64_t ldc, void* stream) {
+    if (M < 0 || N < 0 || K < 0 || !A || !B || !C || lda < K || ldb < K || ldc < N)
+        return fail("gelios_mlp_gemm_bf16: bad arguments");
+    gemm(M, N, K, static_cast<const __nv_bfloat16*>(A), lda, static_cast<const __nv_bfloat16*>(B), ldb, C, ldc,
+         static_cast<cudaStream_t>(stream));
     MLP_TRY(cudaGetLastError());
     return GELIOS_OK;
 }

@@ -555,7 +555,7 @@ __global__ void centroid_kernel(DevMesh d, const double* __restrict__ X, const d
 template <typename TF>
 __device__ __forceinline__ double stationary_side(const gelios_params& P, int ft, const St5& own, double x, double y,
                                                   double rad, double rpo, double xa, double ya, double xb, double yb,
-                                                  const St5& nbs, double x3, double y3, double rpn,
+                                                  const St5& nbs, double x3, double y3, double rpn, double pfc,
                                                   FluxOut<double>& F, double& dist) {
     const double g2 = 2 * P.gamma;
     const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
@@ -576,7 +576,7 @@ __device__ __forceinline__ double stationary_side(const gelios_params& P, int ft
     if (rad < P.rad_stat && ft == G_USUALY) {
         const double dd = sqrt(sq(x3) + sq(y3));
         const double f2 = sq(x2) + sq(y2);
-        const double pf = pow2g(sqrt(f2), g2);  // (rad/fr)^(2g) = rad^(2g) / fr^(2g)
+        const double pf = pfc >= 0.0 ? pfc : pow2g(sqrt(f2), g2);  // (rad/fr)^(2g) = rad^(2g) / fr^(2g)
         par11.ro = par11.ro * sq(rad) / f2;
         par2.ro = par2.ro * sq(dd) / f2;
         par11.p = par11.p * (rpo / pf);
@@ -586,7 +586,7 @@ __device__ __forceinline__ double stationary_side(const gelios_params& P, int ft
     } else if (ft == G_INNER_SPHERE) {
         const double f2 = sq(x2) + sq(y2);
         par11.ro = par11.ro * sq(rad) / f2;
-        par11.p = par11.p * (rpo / pow2g(sqrt(f2), g2));
+        par11.p = par11.p * (rpo / (pfc >= 0.0 ? pfc : pow2g(sqrt(f2), g2)));
     } else if (rad < P.rad_stat && ft == G_AXIS) {
         polar_perenos(x, y, x2, y2, par11.u, par11.v);
         par11.v = 0.0;
@@ -632,8 +632,9 @@ __device__ __forceinline__ double stationary_unit_body(const DevMesh& d, const g
             FluxOut<double> F;
             double dist;
             const double rpK = b.rp[K], rpN = nb >= 0 ? b.rp[nb] : 0.0;
+            const double pfc = b.upf ? b.upf[u] : -1.0;
             const double UU =
-                stationary_side<TF>(P, ft, own, x, y, rad, rpK, xa, ya, xb, yb, nbs, x3, y3, rpN, F, dist);
+                stationary_side<TF>(P, ft, own, x, y, rad, rpK, xa, ya, xb, yb, nbs, x3, y3, rpN, pfc, F, dist);
             fl[0 * ng + g] = F.P0 * S;
             fl[1 * ng + g] = F.P1 * S;
             fl[2 * ng + g] = F.P2 * S;
@@ -657,7 +658,8 @@ __device__ __forceinline__ double stationary_unit_body(const DevMesh& d, const g
                     FluxOut<double> G;
                     double distn;
                     const double Un =
-                        stationary_side<TF>(P, ft, nbs, x3, y3, radn, rpN, xb, yb, xa, ya, own, x, y, rpK, G, distn);
+                        stationary_side<TF>(P, ft, nbs, x3, y3, radn, rpN, xb, yb, xa, ya, own, x, y, rpK, pfc, G,
+                                            distn);
                     fl[0 * ng + gt] = G.P0 * S;
                     fl[1 * ng + gt] = G.P1 * S;
                     fl[2 * ng + gt] = G.P2 * S;
@@ -3093,6 +3095,19 @@ cudaError_t launch_stationary_persistent(const DevMesh& d, const gelios_params& 
     int n = nsteps;
     void* args[] = {&dd, &pp, &c0, &c1, &flp, &n};
     return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(128), args, 0, s);
+}
+__global__ void unit_pf_kernel(DevMesh d, double g2, double* __restrict__ upf) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= d.n_units) return;
+    const int g = d.u_slot[u];
+    const int A = d.sA[g], B = d.sB[g];
+    // the face centre and its radius as stationary_side forms them
+    const double x2 = (d.X[A] + d.X[B]) / 2.0, y2 = (d.Y[A] + d.Y[B]) / 2.0;
+    const double f2 = sq(x2) + sq(y2);
+    upf[u] = pow2g(sqrt(f2), g2);
+}
+void launch_unit_pf(const DevMesh& d, double gamma, double* upf, cudaStream_t s) {
+    if (d.n_units > 0) unit_pf_kernel<<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, 2 * gamma, upf);
 }
 cudaError_t launch_stationary_batch(const DevMesh& d, const PlainInstance* inst, const int* active, int n_active,
                                     int nsteps, bool fp32, cudaStream_t s) {

@@ -93,6 +93,9 @@ struct StepBuffers {
     double* rp_next = nullptr;
     double* vs_next = nullptr;
     double* vol_next = nullptr;
+    // plain form (fixed grid): |face centre|^(2 gamma) of every face unit,
+    // or nullptr (then computed per unit)
+    const double* upf = nullptr;
     const double* dt_cur = nullptr;
     double* dt_next = nullptr;
     unsigned long long* dt_acc = nullptr;
@@ -104,6 +107,9 @@ struct StepBuffers {
 // area (Get_Volume) and the rotated volume (rows of the moving-grid cache).
 void launch_centroid(const DevMesh& d, const double* X, const double* Y, double* cx, double* cy, double* rp,
                      double gamma, cudaStream_t s, double* vs = nullptr, double* vol = nullptr);
+// |face centre|^(2 gamma) of every face unit (the plain form's radial
+// scaling of the face state; the grid of that form does not move)
+void launch_unit_pf(const DevMesh& d, double gamma, double* upf, cudaStream_t s);
 void launch_stationary_units(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
                              cudaStream_t s);
 void launch_stationary_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,

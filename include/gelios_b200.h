@@ -324,9 +324,9 @@ void gelios_plain_batch_destroy(gelios_plain_batch *batch);
  * from 0 over `warmup` steps, then cosine from lr_max down to lr_min; the
  * batch loss of every step into loss_hist (iters floats, may be NULL).
  * gelios_mlp_predict: outputs of M host rows (in chunks of max_batch).
- * gelios_mlp_gemm_bf16: the GEMM alone (device pointers; C = A . B with
- * A[m][k] at A[m a_m + k a_k], B[k][n] at B[k b_k + n b_n], C fp32 rows of
- * ldc; stream may be NULL), for checks. */
+ * gelios_mlp_gemm_bf16: the GEMM alone (device pointers; C = A . B^T with
+ * A[m][k] at A[m lda + k], B[n][k] at B[n ldb + k], C fp32 rows of ldc;
+ * stream may be NULL), for checks. */
 typedef struct gelios_mlp gelios_mlp;
 int gelios_mlp_create(gelios_mlp **out, int device, int n_in, int n_fourier, int width, int depth, int n_out,
                       int max_batch);
@@ -339,8 +339,8 @@ int gelios_mlp_set_data(gelios_mlp *mlp, const float *x, const float *t, int64_t
 int gelios_mlp_train(gelios_mlp *mlp, int iters, int batch, float lr_max, float lr_min, int warmup, uint64_t seed,
                      float *loss_hist);
 int gelios_mlp_predict(gelios_mlp *mlp, const float *x, int64_t M, float *y);
-int gelios_mlp_gemm_bf16(int M, int N, int K, const void *A, int64_t a_m, int64_t a_k, const void *B, int64_t b_k,
-                         int64_t b_n, float *C, int64_t ldc, void *stream);
+int gelios_mlp_gemm_bf16(int M, int N, int K, const void *A, int64_t lda, const void *B, int64_t ldb, float *C,
+                         int64_t ldc, void *stream);
 
 /* ---- autotuning of launch shapes (no counterpart in the reference) ---------
  * The dominant kernel of the MHD form (its face kernel) has

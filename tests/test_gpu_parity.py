@@ -294,10 +294,11 @@ def test_launch_count_reported():
     P = W.plain_params()
     dev, _ = _pair(mesh, P, W.plain_initial(mesh, P))
     dev.Go_stationary(5)
-    assert dev.launches() == 1 + 1 + 1  # words, centroids, one cooperative launch for all five steps
+    # words, centroids, face-centre radii, one cooperative launch for all five steps
+    assert dev.launches() == 1 + 1 + 1 + 1
     dev.set_phase_timing(True)
     dev.Go_stationary(5)
-    assert dev.launches() == 1 + 3 * 5  # words + (face units, cell update, dt) per step; centroids cached
+    assert dev.launches() == 1 + 3 * 5  # words + (face units, cell update, dt) per step; geometry cached
 
 
 @pytest.mark.parametrize("precision", [N.PREC_FP64, N.PREC_FP32_FLUX])

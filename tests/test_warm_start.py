@@ -85,31 +85,26 @@ def test_nearest_index_picks_the_closest_parameters():
 
 # ---------------------------------------------------------------- GPU
 @pytest.mark.gpu
-@pytest.mark.parametrize("shape", [(100, 72, 40, "nn"), (64, 64, 256, "nt"), (130, 31, 300, "tn")])
+@pytest.mark.parametrize("shape", [(100, 72, 40, 40, 40), (256, 256, 256, 256, 256), (130, 31, 300, 301, 304),
+                                   (8192, 5, 31, 31, 32), (333, 200, 1500, 1504, 1500)])
 def test_gemm_bf16_against_float64(shape):
+    """C = A . B^T for k-contiguous A [M][lda], B [N][ldb]: 16-byte staged
+    rows (ld a multiple of 8) and element-wise staged rows, ragged M, N, K
+    (K not a multiple of the 32-wide K tile or of the 8-element chunks)."""
     import torch
 
     from gelios_2d_b200 import _native as N
 
-    M, Nn, K, mode = shape
+    M, Nn, K, lda, ldb = shape
     g = torch.Generator().manual_seed(M + Nn + K)
-    A = torch.randn(M, K, generator=g).to(torch.bfloat16)
-    B = torch.randn(K, Nn, generator=g).to(torch.bfloat16)
-    ref = A.double() @ B.double()
-    # A as stored [M][K] (a_m=K, a_k=1) or transposed [K][M] (a_m=1, a_k=M); B likewise
-    if mode[0] == "n":
-        Ad, a_m, a_k = A.contiguous().cuda(), K, 1
-    else:
-        Ad, a_m, a_k = A.t().contiguous().cuda(), 1, M
-    if mode[1] == "n":
-        Bd, b_k, b_n = B.contiguous().cuda(), Nn, 1
-    else:
-        Bd, b_k, b_n = B.t().contiguous().cuda(), 1, K
-    C = torch.zeros(M, Nn, dtype=torch.float32, device="cuda")
+    A = torch.randn(M, lda, generator=g).to(torch.bfloat16)
+    B = torch.randn(Nn, ldb, generator=g).to(torch.bfloat16)
+    ref = A[:, :K].double() @ B[:, :K].double().t()
+    Ad, Bd = A.contiguous().cuda(), B.contiguous().cuda()
+    C = torch.full((M, Nn), float("nan"), dtype=torch.float32, device="cuda")
     L = N.lib()
     torch.cuda.synchronize()
-    N.check(L.gelios_mlp_gemm_bf16(M, Nn, K, Ad.data_ptr(), a_m, a_k, Bd.data_ptr(), b_k, b_n, C.data_ptr(), Nn,
-                                   None), "gemm")
+    N.check(L.gelios_mlp_gemm_bf16(M, Nn, K, Ad.data_ptr(), lda, Bd.data_ptr(), ldb, C.data_ptr(), Nn, None), "gemm")
     torch.cuda.synchronize()
     err = (C.double().cpu() - ref).abs().max().item()
     assert err <= 1e-5 * ref.abs().max().item() * max(1.0, K / 64), err
