@@ -2,13 +2,13 @@
 // position -> a converged state of the plain step), trained and evaluated
 // on the GPU by this file's kernels.
 //
-//   gemm_tn_kernel        C[M,N] (fp32) = A[M,K] . B[N,K]^T with bf16 operands
-//                         on the tensor cores (mma.sync m16n8k16, fp32
-//                         accumulation), both operands k-contiguous: X.W^T
-//                         (forward), dZ.(W^T)^T (backward, data) and
-//                         (dZ^T).(H^T)^T (backward, weights; split over K
-//                         into partial tiles that splitk_reduce_kernel adds
-//                         in a fixed order)
+//   gemm_tc_kernel        C[M,N] (fp32) = A[M,K] . B[N,K]^T with bf16 operands
+//                         on the 5th-generation tensor cores (tcgen05.mma,
+//                         fp32 accumulator in tensor memory), both operands
+//                         k-contiguous: X.W^T (forward), dZ.(W^T)^T
+//                         (backward, data) and (dZ^T).(H^T)^T (backward,
+//                         weights; split over K into partial tiles that
+//                         splitk_reduce_kernel adds in a fixed order)
 //   transpose_bf16_kernel the transposed operands of the backward GEMMs
 //   features_kernel       network inputs: the raw inputs, then sin / cos of
 //                         2^f pi s of the last two (the cell position), bf16
@@ -40,13 +40,6 @@ void set_error(const std::string& msg);
 
 namespace {
 
-// GEMM tiles: 128 x 128 output per block of 8 warps (2 x 4, each warp
-// 64 x 32 = 4 x 4 tiles of m16n8), K in steps of 32; operand tiles staged
-// in shared memory rows of 40 bf16 (80 bytes: the eight 16-byte rows an
-// ldmatrix reads fall in distinct bank groups).
-constexpr int BM = 128, BN = 128, BK = 32, SPITCH = BK + 8;
-constexpr int kGemmThreads = 256;
-
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
@@ -55,113 +48,205 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int sr
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
-__device__ __forceinline__ void ldmatrix_x4(uint32_t (&r)[4], const void* p) {
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(smem_u32(p)));
-}
+// all but the newest TC_STAGES - 1 commit groups have landed
+__device__ __forceinline__ void cp_async_wait_ring() { asm volatile("cp.async.wait_group 3;\n" ::); }
 
-// Rows row0.. (of nrows) x k k0..k0+31 (of ke) of a k-contiguous operand
-// (rows of ld elements) into S[128][SPITCH]; zeros outside.  VEC: ld and the
-// base are 16-byte aligned, so whole 8-element chunks go by cp.async.
+// ---- the GEMM on the 5th-generation tensor cores (tcgen05)
+// C[M][N] (fp32, rows of ldc) = sum_k A[m][k] B[n][k], A and B bf16 with k
+// contiguous (rows of lda / ldb); blockIdx.z: K slice [z kc, (z+1) kc),
+// written to C + z c_split.  One 128 x 128 fp32 accumulator tile per CTA
+// in tensor memory (128 lanes x 128 columns), K in stages of 64: both
+// operand tiles (128 rows x 64 bf16)
+// staged by cp.async in the canonical K-major layout without swizzle (core
+// matrices of 8 rows x 16 bytes; 16-byte K chunks 128 bytes apart, 8-row
+// groups 1024 bytes apart), a ring of four stages (the whole K of a
+// 256-wide layer in flight at once).  One thread issues four tcgen05.mma
+// (M 128, N 128, K 16) per stage and commits them to the stage's mbarrier,
+// which frees the stage for the load of the tile four steps on; the epilogue
+// reads the accumulator with tcgen05.ld (warp w: rows 32w..32w+31).  Every
+// mbarrier wait is bounded: on expiry the CTA raises `status` and goes on.
+constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 64, TC_THREADS = 128;
+constexpr int TC_TILE = TC_BM * TC_BK * 2;  // bytes of one operand tile
+constexpr int TC_STAGES = 4;
+constexpr int TC_SMEM = 2 * TC_STAGES * TC_TILE;  // A and B per stage
+constexpr uint32_t TC_LBO = 128, TC_SBO = 1024;
+// instruction descriptor of kind::f16: fp32 accumulator (bits 4-5 = 1),
+// A and B bf16 (bits 7-9, 10-12 = 1), both K-major (bits 15, 16 = 0),
+// N >> 3 in bits 17-22, M >> 4 in bits 24-28
+constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
+                              ((uint32_t)(TC_BM >> 4) << 24);
+
+// shared-memory matrix descriptor: start address >> 4 (bits 0-13), leading
+// byte offset >> 4 (16-29), stride byte offset >> 4 (32-45), version 1
+// (bits 46-47), no swizzle (bits 61-63 = 0)
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
+    return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (static_cast<uint64_t>((TC_LBO >> 4) & 0x3FFFu) << 16) |
+           (static_cast<uint64_t>((TC_SBO >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+__device__ __forceinline__ uint32_t tc_off(int r, int kc) {
+    return static_cast<uint32_t>((r >> 3) * TC_SBO + kc * TC_LBO + (r & 7) * 16);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* b, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait for the phase of the given parity; false if it did not complete
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity) {
+    for (int i = 0; i < (1 << 22); i++)
+        if (mbar_try_wait(b, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+
+// rows row0.. x k k0..k0+63 of a k-contiguous operand into a canonical tile.
+// A warp stages 8 rows x 4 chunks per pass (lane: row lane & 7, chunk
+// lane >> 3): each row's 64 bytes are read contiguously, and the 8 rows of
+// one chunk fill one 128-byte core matrix (no bank conflict); 4 warps x 8
+// passes cover 16 row groups x 2 chunk halves.
 template <bool VEC>
-__device__ __forceinline__ void load_tile(__nv_bfloat16 (*S)[SPITCH], const __nv_bfloat16* __restrict__ G, int64_t ld,
-                                          int row0, int nrows, int k0, int ke) {
+__device__ __forceinline__ void tc_load(uint8_t* tile, const __nv_bfloat16* __restrict__ G, int64_t ld, int row0,
+                                        int nrows, int k0, int ke) {
     const __nv_bfloat16 zero = __float2bfloat16(0.f);
-    for (int c = threadIdx.x; c < BM * (BK / 8); c += kGemmThreads) {
-        const int r = c >> 2, kq = (c & 3) * 8;
-        const int gr = row0 + r, gk = k0 + kq;
-        __nv_bfloat16* dst = &S[r][kq];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int pass = 0; pass < 8; pass++) {
+        const int unit = pass * 4 + warp;  // (row group, chunk half)
+        const int r = (unit >> 1) * 8 + (lane & 7), kq = (unit & 1) * 4 + (lane >> 3);
+        const int gr = row0 + r;
+        const int gk = k0 + kq * 8;
+        uint8_t* dst = tile + tc_off(r, kq);
         if (VEC && gr < nrows && gk + 8 <= ke) {
             cp_async16(smem_u32(dst), G + gr * ld + gk, 16);
         } else if (VEC && (gr >= nrows || gk >= ke)) {
-            cp_async16(smem_u32(dst), G, 0);  // zero fill, nothing read
+            cp_async16(smem_u32(dst), G, 0);
         } else {
-            for (int e = 0; e < 8; e++) dst[e] = (gr < nrows && gk + e < ke) ? G[gr * ld + gk + e] : zero;
+            __nv_bfloat16* d = reinterpret_cast<__nv_bfloat16*>(dst);
+            for (int e = 0; e < 8; e++) d[e] = (gr < nrows && gk + e < ke) ? G[gr * ld + gk + e] : zero;
         }
     }
 }
 
-// C[M][N] (fp32, rows of ldc) = sum_k A[m][k] B[n][k], A and B bf16 with k
-// contiguous (rows of lda / ldb).  blockIdx.z: K slice [z kc, (z+1) kc),
-// written to C + z c_split.  Two-stage cp.async pipeline, fragments by
-// ldmatrix, mma.sync m16n8k16 bf16 -> fp32.
 template <bool AV, bool BV>
-__global__ void __launch_bounds__(kGemmThreads) gemm_tn_kernel(int M, int N, int K, int kc,
-                                                             const __nv_bfloat16* __restrict__ A, int64_t lda,
-                                                             const __nv_bfloat16* __restrict__ B, int64_t ldb,
-                                                             float* __restrict__ C, int64_t ldc, int64_t c_split) {
-    __shared__ __align__(16) __nv_bfloat16 As[2][BM][SPITCH];
-    __shared__ __align__(16) __nv_bfloat16 Bs[2][BN][SPITCH];
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+__global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(int M, int N, int K, int kc,
+                                                           const __nv_bfloat16* __restrict__ A, int64_t lda,
+                                                           const __nv_bfloat16* __restrict__ B, int64_t ldb,
+                                                           float* __restrict__ C, int64_t ldc, int64_t c_split,
+                                                           int* __restrict__ status) {
+    extern __shared__ __align__(1024) uint8_t tc_smem[];
+    __shared__ uint64_t bars[TC_STAGES];
+    __shared__ uint32_t tmem_slot;
+    uint8_t* sA0 = tc_smem;
+    uint8_t* sB0 = tc_smem + TC_STAGES * TC_TILE;
+    const int m0 = blockIdx.y * TC_BM, n0 = blockIdx.x * TC_BN;
     const int kb = blockIdx.z * kc, ke = min(K, kb + kc);
     C += blockIdx.z * c_split;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int wm = (warp >> 2) * 64, wn = (warp & 3) * 32;
-    const int g = lane >> 2, t = lane & 3;
-    float acc[4][4][4];
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-#pragma unroll
-            for (int r = 0; r < 4; r++) acc[i][j][r] = 0.f;
-    const int nk = ke > kb ? (ke - kb + BK - 1) / BK : 0;
-    if (nk > 0) {
-        load_tile<AV>(As[0], A, lda, m0, M, kb, ke);
-        load_tile<BV>(Bs[0], B, ldb, n0, N, kb, ke);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(TC_BN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
     }
-    cp_async_commit();
-    // lane -> row / k offset of the 8 x 8 matrices of one ldmatrix.x4
-    const int a_row = lane & 15, a_k = (lane >> 4) << 3;
-    const int b_row = (lane & 7) + ((lane >> 4) << 3), b_k = ((lane >> 3) & 1) << 3;
-    for (int it = 0; it < nk; it++) {
-        const int cur = it & 1;
-        if (it + 1 < nk) {
-            load_tile<AV>(As[cur ^ 1], A, lda, m0, M, kb + (it + 1) * BK, ke);
-            load_tile<BV>(Bs[cur ^ 1], B, ldb, n0, N, kb + (it + 1) * BK, ke);
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < TC_STAGES; i++) mbar_init(&bars[i], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+    const int nk = ke > kb ? (ke - kb + TC_BK - 1) / TC_BK : 0;
+    bool ok = true;
+    // prologue: tiles 0 .. TC_STAGES-2, one commit group each
+    for (int j = 0; j < TC_STAGES - 1; j++) {
+        if (j < nk) {
+            tc_load<AV>(sA0 + j * TC_TILE, A, lda, m0, M, kb + j * TC_BK, ke);
+            tc_load<BV>(sB0 + j * TC_TILE, B, ldb, n0, N, kb + j * TC_BK, ke);
         }
         cp_async_commit();
-        cp_async_wait1();  // the stage of this iteration has landed
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < BK; kk += 16) {
-            uint32_t a[4][4], b[4][2];
-#pragma unroll
-            for (int i = 0; i < 4; i++) ldmatrix_x4(a[i], &As[cur][wm + 16 * i + a_row][kk + a_k]);
-#pragma unroll
-            for (int jp = 0; jp < 2; jp++) {
-                uint32_t r[4];
-                ldmatrix_x4(r, &Bs[cur][wn + 16 * jp + b_row][kk + b_k]);
-                b[2 * jp][0] = r[0];
-                b[2 * jp][1] = r[1];
-                b[2 * jp + 1][0] = r[2];
-                b[2 * jp + 1][1] = r[3];
-            }
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-#pragma unroll
-                for (int j = 0; j < 4; j++)
-                    asm volatile(
-                        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-                        "{%8,%9}, {%0,%1,%2,%3};\n"
-                        : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
-                        : "r"(a[i][0]), "r"(a[i][1]), "r"(a[i][2]), "r"(a[i][3]), "r"(b[j][0]), "r"(b[j][1]));
-        }
-        __syncthreads();  // the next iteration refills the other stage, then this one
     }
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int64_t r = m0 + wm + 16 * i + g;
-            const int c = n0 + wn + 8 * j + 2 * t;
-            if (r < M && c < N) C[r * ldc + c] = acc[i][j][0];
-            if (r < M && c + 1 < N) C[r * ldc + c + 1] = acc[i][j][1];
-            if (r + 8 < M && c < N) C[(r + 8) * ldc + c] = acc[i][j][2];
-            if (r + 8 < M && c + 1 < N) C[(r + 8) * ldc + c + 1] = acc[i][j][3];
+    static_assert(TC_STAGES == 4, "cp_async_wait_ring waits for TC_STAGES - 1 groups");
+    for (int it = 0; it < nk; it++) {
+        const int s = it % TC_STAGES;
+        const int nx = it + TC_STAGES - 1;  // the tile loaded now, into the stage iteration it-1 used
+        if (nx < nk) {
+            const int sx = nx % TC_STAGES;
+            if (it >= 1 && !mbar_wait(&bars[sx], ((it - 1) / TC_STAGES) & 1)) ok = false;
+            tc_load<AV>(sA0 + sx * TC_TILE, A, lda, m0, M, kb + nx * TC_BK, ke);
+            tc_load<BV>(sB0 + sx * TC_TILE, B, ldb, n0, N, kb + nx * TC_BK, ke);
         }
+        cp_async_commit();
+        cp_async_wait_ring();
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // staged bytes visible to the tensor cores
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(sA0 + s * TC_TILE), b0 = smem_u32(sB0 + s * TC_TILE);
+#pragma unroll
+            for (int k = 0; k < TC_BK / 16; k++) {
+                const uint64_t ad = tc_desc(a0 + k * 2 * TC_LBO), bd = tc_desc(b0 + k * 2 * TC_LBO);
+                const uint32_t acc = (it > 0 || k > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(tmem),
+                    "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             smem_u32(&bars[s]))
+                         : "memory");
+        }
+    }
+    if (nk > 0 && !mbar_wait(&bars[(nk - 1) % TC_STAGES], ((nk - 1) / TC_STAGES) & 1)) ok = false;
+    tc_fence_after();
+    const int64_t row = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < TC_BN; c0 += 16) {
+        uint32_t v[16];
+        if (nk > 0) {
+            const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0);
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];\n"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                  "=r"(v[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        } else {
+#pragma unroll
+            for (int j = 0; j < 16; j++) v[j] = 0u;
+        }
+        if (row < M) {
+            float* dst = C + row * ldc + n0 + c0;
+            if (n0 + c0 + 16 <= N && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+#pragma unroll
+                for (int j = 0; j < 16; j += 4)
+                    *reinterpret_cast<float4*>(dst + j) = make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]),
+                                                                      __uint_as_float(v[j + 2]), __uint_as_float(v[j + 3]));
+            } else {
+#pragma unroll
+                for (int j = 0; j < 16; j++)
+                    if (n0 + c0 + j < N) dst[j] = __uint_as_float(v[j]);
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TC_BN) : "memory");
+    }
+    if (!ok) atomicOr(status, 1);
 }
 
 // out[c][r] = in[r][c] (bf16, rows of ldin -> rows of ldout), 32 x 32 tiles
@@ -350,32 +435,59 @@ struct Buf {
     }
 };
 
-// K slice length of a split GEMM (a multiple of the K tile) and the number
-// of slices
-inline int split_len(int K, int splits) {
-    int kc = (K + splits - 1) / splits;
-    kc = (kc + BK - 1) / BK * BK;
-    return kc > 0 ? kc : BK;
-}
+// number of K slices of length kc
 inline int split_count(int K, int kc) { return K > 0 ? (K + kc - 1) / kc : 1; }
 
 inline bool vec_ok(const void* p, int64_t ld) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0 && ld % 8 == 0; }
 
-// C = A . B^T with A [M][lda], B [N][ldb] (k contiguous); see gemm_tn_kernel
+// status word of the tensor-core GEMM (bit 0: an mbarrier wait expired)
+__device__ int g_gemm_status = 0;
+
+template <bool AV, bool BV>
+void launch_tc(dim3 grid, int M, int N, int K, int kc, const __nv_bfloat16* A, int64_t lda, const __nv_bfloat16* B,
+               int64_t ldb, float* C, int64_t ldc, int64_t c_split, cudaStream_t s) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(gemm_tc_kernel<AV, BV>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+        attr = true;
+    }
+    int* st = nullptr;
+    cudaGetSymbolAddress(reinterpret_cast<void**>(&st), g_gemm_status);
+    gemm_tc_kernel<AV, BV><<<grid, TC_THREADS, TC_SMEM, s>>>(M, N, K, kc, A, lda, B, ldb, C, ldc, c_split, st);
+}
+
+// K slice of a GEMM split `splits` ways (a multiple of the K stage)
+inline int tc_split_len(int K, int splits) {
+    int kc = (K + splits - 1) / splits;
+    return kc > 0 ? (kc + TC_BK - 1) / TC_BK * TC_BK : TC_BK;
+}
+
+// C = A . B^T with A [M][lda], B [N][ldb] (k contiguous); see gemm_tc_kernel
 void gemm(int M, int N, int K, const __nv_bfloat16* A, int64_t lda, const __nv_bfloat16* B, int64_t ldb, float* C,
           int64_t ldc, cudaStream_t s, int splits = 1, int64_t c_split = 0) {
     if (M <= 0 || N <= 0) return;
-    const int kc = split_len(K, splits);
-    dim3 grid(blocks(N, BN), blocks(M, BM), split_count(K, kc));
+    const int kc = tc_split_len(K, splits);
+    dim3 grid(blocks(N, TC_BN), blocks(M, TC_BM), split_count(K, kc));
     const bool av = vec_ok(A, lda), bv = vec_ok(B, ldb);
     if (av && bv)
-        gemm_tn_kernel<true, true><<<grid, kGemmThreads, 0, s>>>(M, N, K, kc, A, lda, B, ldb, C, ldc, c_split);
+        launch_tc<true, true>(grid, M, N, K, kc, A, lda, B, ldb, C, ldc, c_split, s);
     else if (av)
-        gemm_tn_kernel<true, false><<<grid, kGemmThreads, 0, s>>>(M, N, K, kc, A, lda, B, ldb, C, ldc, c_split);
+        launch_tc<true, false>(grid, M, N, K, kc, A, lda, B, ldb, C, ldc, c_split, s);
     else if (bv)
-        gemm_tn_kernel<false, true><<<grid, kGemmThreads, 0, s>>>(M, N, K, kc, A, lda, B, ldb, C, ldc, c_split);
+        launch_tc<false, true>(grid, M, N, K, kc, A, lda, B, ldb, C, ldc, c_split, s);
     else
-        gemm_tn_kernel<false, false><<<grid, kGemmThreads, 0, s>>>(M, N, K, kc, A, lda, B, ldb, C, ldc, c_split);
+        launch_tc<false, false>(grid, M, N, K, kc, A, lda, B, ldb, C, ldc, c_split, s);
+}
+
+// reads and clears the GEMM status word (after a synchronisation)
+bool gemm_status_ok() {
+    int v = 0;
+    cudaMemcpyFromSymbol(&v, g_gemm_status, sizeof(int));
+    if (v) {
+        const int zero = 0;
+        cudaMemcpyToSymbol(g_gemm_status, &zero, sizeof(int));
+    }
+    return v == 0;
 }
 
 inline int64_t pad8(int64_t n) { return (n + 7) / 8 * 8; }
@@ -457,7 +569,7 @@ void backward(gelios_mlp* n, int M) {
     int splits = (M + 255) / 256;
     if (splits > kMaxSplit) splits = kMaxSplit;
     if (splits < 1) splits = 1;
-    const int kc = split_len(M, splits), S = split_count(M, kc);
+    const int S = split_count(M, tc_split_len(M, splits));
     const int64_t Mp = pad8(M);
     __nv_bfloat16* dzt = n->dzt.as<__nv_bfloat16>();
     __nv_bfloat16* ht = n->ht.as<__nv_bfloat16>();
@@ -590,6 +702,7 @@ extern "C" int gelios_mlp_loss_grad(gelios_mlp* n, const float* x, const float* 
     if (grad)
         MLP_TRY(cudaMemcpyAsync(grad, n->g32.p, static_cast<size_t>(n->n_params) * 4, cudaMemcpyDeviceToHost, s));
     MLP_TRY(cudaStreamSynchronize(s));
+    if (!gemm_status_ok()) return cuda_fail(cudaErrorLaunchTimeout);
     if (loss) *loss = l;
     return GELIOS_OK;
 }
@@ -643,6 +756,7 @@ extern "C" int gelios_mlp_train(gelios_mlp* n, int iters, int batch, float lr_ma
     if (loss_hist && iters > 0)
         MLP_TRY(cudaMemcpyAsync(loss_hist, hist.p, static_cast<size_t>(iters) * 4, cudaMemcpyDeviceToHost, s));
     MLP_TRY(cudaStreamSynchronize(s));
+    if (!gemm_status_ok()) return cuda_fail(cudaErrorLaunchTimeout);
     return GELIOS_OK;
 }
 
@@ -662,6 +776,7 @@ extern "C" int gelios_mlp_predict(gelios_mlp* n, const float* x, int64_t M, floa
                                 cudaMemcpyDeviceToHost, s));
     }
     MLP_TRY(cudaStreamSynchronize(s));
+    if (!gemm_status_ok()) return cuda_fail(cudaErrorLaunchTimeout);
     return GELIOS_OK;
 }
 
@@ -672,5 +787,7 @@ extern "C" int gelios_mlp_gemm_bf16(int M, int N, int K, const void* A, int64_t 
     gemm(M, N, K, static_cast<const __nv_bfloat16*>(A), lda, static_cast<const __nv_bfloat16*>(B), ldb, C, ldc,
          static_cast<cudaStream_t>(stream));
     MLP_TRY(cudaGetLastError());
+    MLP_TRY(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    if (!gemm_status_ok()) return cuda_fail(cudaErrorLaunchTimeout);
     return GELIOS_OK;
 }
