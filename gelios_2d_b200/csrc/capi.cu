@@ -1078,6 +1078,7 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             b.cx = cen0;
             b.cy = cen0 + ncz;
             b.rp = cen0 + 2 * ncz;
+            b.vs = cen0 + 3 * ncz;
             b.upf = ctx->upf.as<double>();
         }
         if (launch_stationary_persistent(d, P, bb[0], bb[1], ctx->flux.as<double>(), nsteps, s) == cudaSuccess) {
@@ -1166,6 +1167,7 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             b.cy = cen0 + d.n_cells;
             b.rp = cen0 + 2 * static_cast<size_t>(d.n_cells);
             if (form == GELIOS_FORM_STATIONARY) {
+                b.vs = cen0 + 3 * static_cast<size_t>(d.n_cells);
                 b.upf = ctx->upf.as<double>();
                 cudaEvent_t e1 = ctx->phase_begin();
                 launch_stationary_units(d, P, b, ctx->flux.as<double>(), s);
@@ -1864,6 +1866,7 @@ int plain_batch_prepare(gelios_plain_batch* B, const std::vector<int>& list) {
             b.cx = cen0;
             b.cy = cen0 + ncz;
             b.rp = cen0 + 2 * ncz;
+            b.vs = cen0 + 3 * ncz;
             b.upf = c->upf.as<double>();
         }
         I.fl = c->flux.as<double>();

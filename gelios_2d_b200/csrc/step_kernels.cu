@@ -702,8 +702,15 @@ __device__ __forceinline__ void stationary_update_body(const DevMesh& d, const g
             Pt3 = Pt3 + fl[3 * ng + g];
             Pt4 = Pt4 + fl[4 * ng + g];
         }
-        const int s0 = d.cstart[c], n = d.cstart[c + 1] - s0;
-        const double Volume = area(d.contour + s0, n, d.sA, d.sB, g0, g1, d.X, d.Y, false);
+        // the cell's area: cached with the centroids (the plain grid does not
+        // move), or computed here when no cache is given
+        double Volume;
+        if (b.vs) {
+            Volume = b.vs[c];
+        } else {
+            const int s0 = d.cstart[c], n = d.cstart[c + 1] - s0;
+            Volume = area(d.contour + s0, n, d.sA, d.sB, g0, g1, d.X, d.Y, false);
+        }
         const double gm1 = P.gamma - 1;
         double ro3 = par1.ro - dt * (Pt0 / Volume + par1.ro * par1.v / y);
         const double Q33 = par1.Q - (dt / Volume) * Pt4 - dt * par1.Q * par1.v / y;
