@@ -603,7 +603,7 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     rc |= upload(ctx->u_cell, u_cell.data(), u_cell.size(), s);
     rc |= upload(ctx->u_twin, u_twin.data(), u_twin.size(), s);
     rc |= upload<double>(ctx->flux, nullptr, 5 * static_cast<size_t>(ng), s);
-    rc |= upload<double>(ctx->upf, nullptr, u_slot.size(), s);
+    rc |= upload<double>(ctx->upf, nullptr, static_cast<size_t>(kUnitGeoRows) * u_slot.size(), s);
     rc |= upload<double>(ctx->aux, nullptr, 3 * static_cast<size_t>(nc), s);
     rc |= upload<double>(ctx->rec, nullptr, static_cast<size_t>(kRecRows) * u_slot.size(), s);
     rc |= upload<double>(ctx->pstar, nullptr, static_cast<size_t>(u_tr1 - u_tr0) + 1, s);
@@ -1056,7 +1056,7 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
         ctx->cen_rp_partial = false;
     }
     if (form == GELIOS_FORM_STATIONARY && !ctx->upf_valid && nsteps > 0) {
-        launch_unit_pf(d, P.gamma, ctx->upf.as<double>(), s);
+        launch_unit_geometry(d, P.gamma, cen0, cen0 + ncz, ctx->upf.as<double>(), s);
         launches++;
         ctx->upf_valid = true;
     }
@@ -1080,6 +1080,7 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             b.rp = cen0 + 2 * ncz;
             b.vs = cen0 + 3 * ncz;
             b.upf = ctx->upf.as<double>();
+            b.ugeo = b.upf + d.n_units;
         }
         if (launch_stationary_persistent(d, P, bb[0], bb[1], ctx->flux.as<double>(), nsteps, s) == cudaSuccess) {
             launches += 1;
@@ -1169,6 +1170,7 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             if (form == GELIOS_FORM_STATIONARY) {
                 b.vs = cen0 + 3 * static_cast<size_t>(d.n_cells);
                 b.upf = ctx->upf.as<double>();
+                b.ugeo = b.upf + d.n_units;
                 cudaEvent_t e1 = ctx->phase_begin();
                 launch_stationary_units(d, P, b, ctx->flux.as<double>(), s);
                 ctx->phase_end(1, e1, 1);
@@ -1845,7 +1847,8 @@ int plain_batch_prepare(gelios_plain_batch* B, const std::vector<int>& list) {
             c->cen_rp_partial = false;
         }
         if (!c->upf_valid) {
-            launch_unit_pf(c->d, c->prm.gamma, c->upf.as<double>(), B->stream);
+            const double* cen = c->cen[0].as<double>();
+            launch_unit_geometry(c->d, c->prm.gamma, cen, cen + c->d.n_cells, c->upf.as<double>(), B->stream);
             c->upf_valid = true;
         }
         PlainInstance& I = host[i];
@@ -1868,6 +1871,7 @@ int plain_batch_prepare(gelios_plain_batch* B, const std::vector<int>& list) {
             b.rp = cen0 + 2 * ncz;
             b.vs = cen0 + 3 * ncz;
             b.upf = c->upf.as<double>();
+            b.ugeo = b.upf + c->d.n_units;
         }
         I.fl = c->flux.as<double>();
     }

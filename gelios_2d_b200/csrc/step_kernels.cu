@@ -549,17 +549,45 @@ __global__ void centroid_kernel(DevMesh d, const double* __restrict__ X, const d
 // CFL candidates of the sides whose cell is updated this step into the dt
 // word.  The cell kernels then sum their slots in Grans order.
 
+// Geometry of a face unit as its owner sees it: face centre (x2, y2), unit
+// normal (n1, n2) for the end points in the owner's order, |centre|^2, the
+// face length S, and the distances owner centroid - face centre and
+// neighbour centroid - face centre (0 without a neighbour).  The same
+// expressions as Setka.cpp:5244-5306 (t = B - A normalised, n = (t2, -t1));
+// the twin's view has the normal negated and the two distances swapped.
+struct FaceGeo {
+    double x2, y2, n1, n2, f2, S, dist, distn;
+};
+constexpr int kFaceGeoRows = 8;
+__device__ __forceinline__ FaceGeo face_geo(double xa, double ya, double xb, double yb, double x, double y,
+                                            bool has_nb, double x3, double y3) {
+    FaceGeo f;
+    f.x2 = (xa + xb) / 2.0;
+    f.y2 = (ya + yb) / 2.0;
+    double t1 = xb - xa, t2 = yb - ya;
+    const double nn = sqrt(sq(t1) + sq(t2));
+    f.S = nn;
+    t1 = t1 / nn;
+    t2 = t2 / nn;
+    f.n1 = t2;
+    f.n2 = -t1;
+    f.f2 = sq(f.x2) + sq(f.y2);
+    f.dist = sqrt(sq(x - f.x2) + sq(y - f.y2));
+    f.distn = has_nb ? sqrt(sq(x3 - f.x2) + sq(y3 - f.y2)) : 0.0;
+    return f;
+}
+
 // Go_stationary flux of one side (Setka.cpp:5244-5306): owner state `own`
-// at centre (x, y), radius rad; face end points (xa,ya)->(xb,yb) seen from the
-// owner; neighbour (for Usualy faces) state/centre.
+// at centre (x, y), radius rad; face centre (x2, y2), normal (n1, n2) and
+// |centre|^2 f2 as seen from the owner; neighbour (for Usualy faces)
+// state, centre and radius rad_nb.  pfc: |face centre|^(2 gamma) if cached,
+// else negative.
 template <typename TF>
 __device__ __forceinline__ double stationary_side(const gelios_params& P, int ft, const St5& own, double x, double y,
-                                                  double rad, double rpo, double xa, double ya, double xb, double yb,
-                                                  const St5& nbs, double x3, double y3, double rpn, double pfc,
-                                                  FluxOut<double>& F, double& dist) {
+                                                  double rad, double rpo, double x2, double y2, double n1, double n2,
+                                                  double f2, const St5& nbs, double x3, double y3, double rad_nb,
+                                                  double rpn, double pfc, FluxOut<double>& F) {
     const double g2 = 2 * P.gamma;
-    const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
-    dist = sqrt(sq(x - x2) + sq(y - y2));
     St5 par11 = own;
     St5 par2 = own;
     if (ft == G_USUALY) par2 = nbs;
@@ -568,23 +596,15 @@ __device__ __forceinline__ double stationary_side(const gelios_params& P, int ft
     } else if (ft == G_AXIS) par2.v = -par2.v;
     else if (ft == G_INNER_SPHERE) par2 = inner_sphere_state(P, x2, y2);
     else if (ft == G_INPUT) par2 = input_state(P);
-    double t1 = xb - xa, t2 = yb - ya;
-    const double nn = sqrt(sq(t1) + sq(t2));
-    t1 = t1 / nn;
-    t2 = t2 / nn;
-    const double n1 = t2, n2 = -t1;
     if (rad < P.rad_stat && ft == G_USUALY) {
-        const double dd = sqrt(sq(x3) + sq(y3));
-        const double f2 = sq(x2) + sq(y2);
         const double pf = pfc >= 0.0 ? pfc : pow2g(sqrt(f2), g2);  // (rad/fr)^(2g) = rad^(2g) / fr^(2g)
         par11.ro = par11.ro * sq(rad) / f2;
-        par2.ro = par2.ro * sq(dd) / f2;
+        par2.ro = par2.ro * sq(rad_nb) / f2;
         par11.p = par11.p * (rpo / pf);
         par2.p = par2.p * (rpn / pf);
         polar_perenos(x, y, x2, y2, par11.u, par11.v);
         polar_perenos(x3, y3, x2, y2, par2.u, par2.v);
     } else if (ft == G_INNER_SPHERE) {
-        const double f2 = sq(x2) + sq(y2);
         par11.ro = par11.ro * sq(rad) / f2;
         par11.p = par11.p * (rpo / (pfc >= 0.0 ? pfc : pow2g(sqrt(f2), g2)));
     } else if (rad < P.rad_stat && ft == G_AXIS) {
@@ -615,9 +635,6 @@ __device__ __forceinline__ double stationary_unit_body(const DevMesh& d, const g
         const bool procN = nb >= 0 && !(d.cflags[nb] & CF_CENTR);
         if (procK || procN) {
             const int ft = d.sinfo[g] & SI_TYPE_MASK;
-            const int A = d.sA[g], B = d.sB[g];
-            const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
-            const double S = sqrt(sq(xb - xa) + sq(yb - ya));
             const double x = b.cx[K], y = b.cy[K];
             const double rad = sqrt(sq(x) + sq(y));
             const St5 own = load_state(b.cur, K);
@@ -629,43 +646,54 @@ __device__ __forceinline__ double stationary_unit_body(const DevMesh& d, const g
                 y3 = b.cy[nb];
                 radn = sqrt(sq(x3) + sq(y3));
             }
+            FaceGeo f;
+            if (b.ugeo) {
+                const size_t nu = d.n_units;
+                f.x2 = b.ugeo[u];
+                f.y2 = b.ugeo[nu + u];
+                f.n1 = b.ugeo[2 * nu + u];
+                f.n2 = b.ugeo[3 * nu + u];
+                f.f2 = b.ugeo[4 * nu + u];
+                f.S = b.ugeo[5 * nu + u];
+                f.dist = b.ugeo[6 * nu + u];
+                f.distn = b.ugeo[7 * nu + u];
+            } else {
+                const int A = d.sA[g], B = d.sB[g];
+                f = face_geo(d.X[A], d.Y[A], d.X[B], d.Y[B], x, y, nb >= 0, x3, y3);
+            }
+            const double S = f.S;
             FluxOut<double> F;
-            double dist;
             const double rpK = b.rp[K], rpN = nb >= 0 ? b.rp[nb] : 0.0;
             const double pfc = b.upf ? b.upf[u] : -1.0;
-            const double UU =
-                stationary_side<TF>(P, ft, own, x, y, rad, rpK, xa, ya, xb, yb, nbs, x3, y3, rpN, pfc, F, dist);
+            const double UU = stationary_side<TF>(P, ft, own, x, y, rad, rpK, f.x2, f.y2, f.n1, f.n2, f.f2, nbs, x3,
+                                                  y3, radn, rpN, pfc, F);
             fl[0 * ng + g] = F.P0 * S;
             fl[1 * ng + g] = F.P1 * S;
             fl[2 * ng + g] = F.P2 * S;
             fl[3 * ng + g] = F.P3 * S;
             fl[4 * ng + g] = F.PQ * S;
-            if (procK) tmin_u = dmin_ref(tmin_u, P.kurant * dist / UU);
+            if (procK) tmin_u = dmin_ref(tmin_u, P.kurant * f.dist / UU);
             if (gt >= 0) {
                 // the twin's evaluation mirrors this one unless the radial
                 // scaling switches at rad_stat between the two cells
                 const bool same = (rad < P.rad_stat) == (radn < P.rad_stat);
                 if (same) {
-                    const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
-                    const double distn = sqrt(sq(x3 - x2) + sq(y3 - y2));
                     fl[0 * ng + gt] = -(F.P0 * S);
                     fl[1 * ng + gt] = -(F.P1 * S);
                     fl[2 * ng + gt] = -(F.P2 * S);
                     fl[3 * ng + gt] = -(F.P3 * S);
                     fl[4 * ng + gt] = -(F.PQ * S);
-                    if (procN) tmin_u = dmin_ref(tmin_u, P.kurant * distn / UU);
+                    if (procN) tmin_u = dmin_ref(tmin_u, P.kurant * f.distn / UU);
                 } else {
                     FluxOut<double> G;
-                    double distn;
-                    const double Un =
-                        stationary_side<TF>(P, ft, nbs, x3, y3, radn, rpN, xb, yb, xa, ya, own, x, y, rpK, pfc, G,
-                                            distn);
+                    const double Un = stationary_side<TF>(P, ft, nbs, x3, y3, radn, rpN, f.x2, f.y2, -f.n1, -f.n2,
+                                                          f.f2, own, x, y, rad, rpK, pfc, G);
                     fl[0 * ng + gt] = G.P0 * S;
                     fl[1 * ng + gt] = G.P1 * S;
                     fl[2 * ng + gt] = G.P2 * S;
                     fl[3 * ng + gt] = G.P3 * S;
                     fl[4 * ng + gt] = G.PQ * S;
-                    if (procN) tmin_u = dmin_ref(tmin_u, P.kurant * distn / Un);
+                    if (procN) tmin_u = dmin_ref(tmin_u, P.kurant * f.distn / Un);
                 }
             }
         }
@@ -3103,18 +3131,30 @@ cudaError_t launch_stationary_persistent(const DevMesh& d, const gelios_params& 
     void* args[] = {&dd, &pp, &c0, &c1, &flp, &n};
     return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(128), args, 0, s);
 }
-__global__ void unit_pf_kernel(DevMesh d, double g2, double* __restrict__ upf) {
+__global__ void unit_geometry_kernel(DevMesh d, double g2, const double* __restrict__ cx,
+                                     const double* __restrict__ cy, double* __restrict__ upf) {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= d.n_units) return;
-    const int g = d.u_slot[u];
+    const int g = d.u_slot[u], K = d.u_cell[u];
+    const int nb = d.u_twin[u] >= 0 ? d.snb[g] : -1;
     const int A = d.sA[g], B = d.sB[g];
-    // the face centre and its radius as stationary_side forms them
-    const double x2 = (d.X[A] + d.X[B]) / 2.0, y2 = (d.Y[A] + d.Y[B]) / 2.0;
-    const double f2 = sq(x2) + sq(y2);
-    upf[u] = pow2g(sqrt(f2), g2);
+    const FaceGeo f = face_geo(d.X[A], d.Y[A], d.X[B], d.Y[B], cx[K], cy[K], nb >= 0, nb >= 0 ? cx[nb] : 0.0,
+                               nb >= 0 ? cy[nb] : 0.0);
+    const size_t nu = d.n_units;
+    upf[u] = pow2g(sqrt(f.f2), g2);
+    double* geo = upf + nu;
+    geo[u] = f.x2;
+    geo[nu + u] = f.y2;
+    geo[2 * nu + u] = f.n1;
+    geo[3 * nu + u] = f.n2;
+    geo[4 * nu + u] = f.f2;
+    geo[5 * nu + u] = f.S;
+    geo[6 * nu + u] = f.dist;
+    geo[7 * nu + u] = f.distn;
 }
-void launch_unit_pf(const DevMesh& d, double gamma, double* upf, cudaStream_t s) {
-    if (d.n_units > 0) unit_pf_kernel<<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, 2 * gamma, upf);
+void launch_unit_geometry(const DevMesh& d, double gamma, const double* cx, const double* cy, double* upf,
+                          cudaStream_t s) {
+    if (d.n_units > 0) unit_geometry_kernel<<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, 2 * gamma, cx, cy, upf);
 }
 cudaError_t launch_stationary_batch(const DevMesh& d, const PlainInstance* inst, const int* active, int n_active,
                                     int nsteps, bool fp32, cudaStream_t s) {

@@ -93,9 +93,11 @@ struct StepBuffers {
     double* rp_next = nullptr;
     double* vs_next = nullptr;
     double* vol_next = nullptr;
-    // plain form (fixed grid): |face centre|^(2 gamma) of every face unit,
-    // or nullptr (then computed per unit)
+    // plain form (fixed grid): |face centre|^(2 gamma) of every face unit and
+    // the units' face geometry (kUnitGeoRows - 1 unit-major rows, see
+    // FaceGeo in step_kernels.cu), or nullptr (then computed per unit)
     const double* upf = nullptr;
+    const double* ugeo = nullptr;
     const double* dt_cur = nullptr;
     double* dt_next = nullptr;
     unsigned long long* dt_acc = nullptr;
@@ -107,9 +109,13 @@ struct StepBuffers {
 // area (Get_Volume) and the rotated volume (rows of the moving-grid cache).
 void launch_centroid(const DevMesh& d, const double* X, const double* Y, double* cx, double* cy, double* rp,
                      double gamma, cudaStream_t s, double* vs = nullptr, double* vol = nullptr);
-// |face centre|^(2 gamma) of every face unit (the plain form's radial
-// scaling of the face state; the grid of that form does not move)
-void launch_unit_pf(const DevMesh& d, double gamma, double* upf, cudaStream_t s);
+// Per face unit of the plain form (its grid does not move): row 0
+// |face centre|^(2 gamma), rows 1-8 the face geometry as the owner sees it
+// (centre x, y, normal, |centre|^2, length, owner and neighbour centroid
+// distances); needs the centroids cx, cy.
+constexpr int kUnitGeoRows = 9;
+void launch_unit_geometry(const DevMesh& d, double gamma, const double* cx, const double* cy, double* upf,
+                          cudaStream_t s);
 void launch_stationary_units(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
                              cudaStream_t s);
 void launch_stationary_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
