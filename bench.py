@@ -72,7 +72,8 @@ BYTES_PER_CELL = {"mk2": 288, "plain": 112, "k5": 392, "mhd": 288, "inner": 264}
 STEP_KERNELS = {
     "mk2": "whole moving-grid step: recon, tracked_solve, source, surface_faces, rails, flux x2, update, commit "
            "(one CUDA graph, 3 streams)",
-    "plain": "whole plain step: stationary_unit + stationary_update + dt_finalize",
+    "plain": "whole plain step: stationary_persistent_kernel (face units, cell update, dt; all steps of a call "
+             "in one cooperative launch)",
     "k5": "whole four-fluid step: centroid, surface_faces, rails, k5_cell, commit",
     "mhd": "whole MHD + pickup step: surface_faces, rails, mhd_face, mhd_update, commit",
     "inner": "whole inner-region step: inner_cell + dt_finalize",
