@@ -446,10 +446,13 @@ __device__ int g_gemm_status = 0;
 template <bool AV, bool BV>
 void launch_tc(dim3 grid, int M, int N, int K, int kc, const __nv_bfloat16* A, int64_t lda, const __nv_bfloat16* B,
                int64_t ldb, float* C, int64_t ldc, int64_t c_split, cudaStream_t s) {
-    static bool attr = false;
-    if (!attr) {
+    // the shared-memory opt-in is a per-device attribute of the kernel
+    static bool attr[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !attr[dev]) {
         cudaFuncSetAttribute(gemm_tc_kernel<AV, BV>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
-        attr = true;
+        if (dev >= 0 && dev < 64) attr[dev] = true;
     }
     int* st = nullptr;
     cudaGetSymbolAddress(reinterpret_cast<void**>(&st), g_gemm_status);

@@ -33,3 +33,10 @@ def test_reference_arm_line_plain(have_ref):
 def test_reference_arm_sweep_is_unavailable():
     d = _run("--impl", "reference", "--workload", "sweep64", "--steps", "1")
     assert d["impl"] == "reference" and "unavailable" in d
+
+
+def test_reference_arm_warm_start_is_unavailable():
+    # the reference has no warm start: its cold solves appear as the
+    # workload's projected CPU baseline instead
+    d = _run("--impl", "reference", "--workload", "warm_start", "--steps", "1")
+    assert d["impl"] == "reference" and "unavailable" in d
