@@ -1,7 +1,7 @@
 """Parity of the sm_100a kernels with the oracle (C restatement pinned to the
 reference), called through the C ABI.
 
-Tolerances (FP64 drop-in; the north_star bar): max-norm relative error per
+Tolerances (FP64 drop-in): max-norm relative error per
 primitive variable <= 1e-12 after one/two steps from a common state and
 <= 1e-9 after 1000 steps.  Point coordinates after grid motion agree to
 1e-13 relative (the rails use cos/sin/pow of libdevice vs glibc: ~1 ulp).
