@@ -4,17 +4,21 @@ One "step" = one call of the moving-grid time step (the Go_5_komponent__MK2
 form: surface tracking, rail motion, per-face HLL/exact-Godunov fluxes with
 TVD reconstruction, charge-exchange source from Monte-Carlo moments,
 conservative ALE update, CFL reduction) over the whole grid, inputs resident
-in HBM.  Default workload: the reference's rail grid Setka(200,100,50,100,
-100,100,150,150) (~200k cells, ~400 rays x ~500 radial cells), the
+in HBM.  Default workload: the reference's rail grid Setka(480,240,100,220,
+200,200,300,300) (938,010 cells, ~1000 rays x ~1000 radial cells: the
+1M-cell moving-grid configuration, whose inputs exceed the 126 MB L2), the
 reference's initial field and seeded Monte-Carlo moments.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload mk2_200k|mk2_1m|plain]
+                    [--workload mk2_1m|mk2_200k|plain|...]
 
 N>1 runs N independent replicas (one process per GPU, torchrun); value is
 the whole-job rate, the time is the max over ranks.  --impl reference times
 the reference's own CPU step (compiled from its sources, all host threads)
-on the same grid and prints its line; under torchrun only rank 0 does.
+on the same workload and prints its line; under torchrun only rank 0 does.
+For the rail-grid workloads the reference arm builds everything with the
+reference itself (its constructor, TVD_prepare and Init_conditions; seeded
+inputs from numpy) and loads no library of this package.
 """
 from __future__ import annotations
 
@@ -85,6 +89,17 @@ def _env_int(k, d):
         return int(os.environ.get(k, d))
     except ValueError:
         return d
+
+
+def workload_config(name: str, cells: int, counted: int, faces: int, points: int, world: int) -> dict:
+    desc, form, _ = WORKLOADS[name]
+    return {"workload": desc, "cells": int(cells), "cells_updated_per_step": int(counted), "faces": int(faces),
+            "points": int(points),
+            "l2": ("inputs larger than L2 (126 MB), not flushed" if name.endswith("_1m") else
+                   "flushed (256 MiB write) before each timed call of 100 steps; the few-MB state stays "
+                   "L2-resident within a call" if form in ("plain", "inner") else
+                   "flushed between timed steps (256 MiB write)"),
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
 
 
 def build_workload(name: str):
@@ -230,26 +245,41 @@ def cpu_oracle_mhd_rate(mesh, params, st0, mc, counted, budget_s=12.0, max_steps
     return counted * steps / el, steps, 1, el
 
 
-def cpu_reference_rate(mesh, params, st0, mc, counted, form, budget_s=12.0, max_steps=200, threads=None):
+RAIL_FORMS = ("mk2", "inner", "k5")
+
+
+def reference_workload(name: str):
+    """The rail-grid workload `name` built by the reference alone (its own
+    constructor, TVD_prepare and Init_conditions in oracle/_ref; seeded
+    inputs from numpy): nothing of this package is imported or loaded."""
+    from oracle import ref_workload as RW
+
+    _, form, dims = WORKLOADS[name]
+    return RW.build(dims, form)
+
+
+def cpu_reference_rate(mesh, params, st0, mc, counted, form, budget_s=12.0, max_steps=200, threads=None,
+                       rw=None):
     """The reference's own step (compiled from its sources, all host threads)
-    on the same grid: cell-updates/s over a bounded number of steps."""
+    on the same workload: cell-updates/s over a bounded number of steps.
+    Rail-grid forms run on `rw` (a reference_workload); the plain form on
+    reference objects made from `mesh`; the MHD form, which has no
+    reference step, on the oracle's restatement."""
     if form == "mhd":
         return cpu_oracle_mhd_rate(mesh, params, st0, mc, counted, budget_s, max_steps)
     from oracle import ref
 
     threads = threads or os.cpu_count() or 1
     ref.set_threads(threads, fast=True)
-    S = ref.RefSetka.from_mesh(mesh, fast=True)
-    S.tvd_prepare()
-    S.set_state(0, st0)
-    S.set_state(1, st0)
-    if form == "k5":
-        S.set_hydrogen(0, mc)
-        S.set_hydrogen(1, mc)
-    elif mc is not None:
-        S.set_mc(*mc)
-    if form == "inner":
-        S.build_inner_list()
+    if form in RAIL_FORMS:
+        if rw is None:
+            raise ValueError("rail-grid forms run on a reference_workload")
+        S, counted = rw.S, rw.counted
+    else:
+        S = ref.RefSetka.from_mesh(mesh, fast=True)
+        S.tvd_prepare()
+        S.set_state(0, st0)
+        S.set_state(1, st0)
     run = {"mk2": S.go_mk2, "k5": S.go_5_komponent, "inner": S.go_inner_mk2}.get(form, S.go_stationary)
     # keep the reference's printf diagnostics off our stdout
     saved = os.dup(1)
@@ -325,7 +355,7 @@ def fp32_flux_errors(mesh, params32, st0, mc, fcode, device, counts=(1, 100, 200
     return out
 
 
-def time_to_residual(mesh, params, st0, mc, form, fcode, device, tol, counted, max_steps=5_000_000,
+def time_to_residual(workload, mesh, params, st0, mc, form, fcode, device, tol, counted, max_steps=5_000_000,
                      check_every=10_000) -> dict:
     """Wall time from the seeded (cold) initial field until the density's L1
     residual per unit time, sum|ro(n+1) - ro(n)| / (dt sum|ro(n+1)|), is at
@@ -344,7 +374,8 @@ def time_to_residual(mesh, params, st0, mc, form, fcode, device, tol, counted, m
                                       f"{check_every} steps", "start": "cold (the workload's seeded initial field)",
            "reached": r <= tol, "steps": steps, "residual": r, "dt": dt, "gpu_s": gpu_s}
     try:
-        rate, n, threads, el = cpu_reference_rate(mesh, params, st0, mc, counted, form, budget_s=10.0)
+        rw = reference_workload(workload) if form in RAIL_FORMS else None
+        rate, n, threads, el = cpu_reference_rate(mesh, params, st0, mc, counted, form, budget_s=10.0, rw=rw)
         out["reference_cpu_s_projected"] = steps * counted / rate
         out["reference_cpu_sample"] = f"{n} steps on {threads} host threads ({el:.1f} s)"
     except Exception as e:  # the reference library must be prebuilt
@@ -528,7 +559,7 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mk2_200k", choices=sorted(WORKLOADS) + ["warm_start"])
+    ap.add_argument("--workload", default="mk2_1m", choices=sorted(WORKLOADS) + ["warm_start"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32flux"])
     # sweep64 only: one context and captured step graph per instance, autotuned and enqueued together
@@ -566,18 +597,18 @@ def main():
             return
         run_sweep(args, rank, world, local)
         return
-    desc, form, dims, mesh, params, st0, mc, counted = build_workload(args.workload)
-    config = {"workload": desc, "cells": int(mesh.n_cells), "cells_updated_per_step": int(counted),
-              "faces": int(mesh.n_faces), "points": int(mesh.n_points),
-              "l2": ("inputs larger than L2" if args.workload.endswith("_1m") else
-                     "flushed (256 MiB write) before each timed call of 100 steps; the few-MB state stays "
-                     "L2-resident within a call" if form in ("plain", "inner") else
-                     "flushed between timed steps (256 MiB write)"), "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
-
+    _, form, _ = WORKLOADS[args.workload]
     cpu_kind = "port" if form == "mhd" else "reference"
     cpu_what = "the oracle's restatement (no reference step exists)" if form == "mhd" else "the reference step"
     if args.impl == "reference":
-        rate, steps, threads, el = cpu_reference_rate(mesh, params, st0, mc, counted, form)
+        if form in RAIL_FORMS:  # built and stepped by the reference alone
+            rw = reference_workload(args.workload)
+            config = workload_config(args.workload, rw.n_cells, rw.counted, rw.n_faces, rw.n_points, world)
+            rate, steps, threads, el = cpu_reference_rate(None, None, None, None, rw.counted, form, rw=rw)
+        else:
+            desc, form, dims, mesh, params, st0, mc, counted = build_workload(args.workload)
+            config = workload_config(args.workload, mesh.n_cells, counted, mesh.n_faces, mesh.n_points, world)
+            rate, steps, threads, el = cpu_reference_rate(mesh, params, st0, mc, counted, form)
         line = {"metric": METRIC, "value": rate, "unit": "cell-updates/s", "impl": "reference",
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": 1000.0 * el / steps, "higher_is_better": True, "scaling": "weak",
@@ -587,6 +618,9 @@ def main():
                 "e2e": {"value": rate, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
+
+    desc, form, dims, mesh, params, st0, mc, counted = build_workload(args.workload)
+    config = workload_config(args.workload, mesh.n_cells, counted, mesh.n_faces, mesh.n_points, world)
 
     import torch
 
@@ -713,11 +747,12 @@ def main():
     if args.precision == "fp32flux" and rank == 0:
         line["fp32_flux_errors"] = fp32_flux_errors(mesh, params, st0, mc, fcode, device, form=form)
     if args.residual is not None and rank == 0:
-        line["time_to_residual"] = time_to_residual(mesh, params, st0, mc, form, fcode, device, args.residual,
-                                                    counted)
+        line["time_to_residual"] = time_to_residual(args.workload, mesh, params, st0, mc, form, fcode, device,
+                                                    args.residual, counted)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            rate, steps, threads, el = cpu_reference_rate(mesh, params, st0, mc, counted, form)
+            rw = reference_workload(args.workload) if form in RAIL_FORMS else None
+            rate, steps, threads, el = cpu_reference_rate(mesh, params, st0, mc, counted, form, rw=rw)
             line["cpu_baseline"] = {"value": rate, "unit": "cell-updates/s", "cores": threads, "kind": cpu_kind,
                                     "sample": f"{steps} steps of {cpu_what} on the full grid ({el:.1f} s)"}
         except Exception as e:  # the reference library must be prebuilt

@@ -54,6 +54,15 @@ __global__ void noalloc_words_init(unsigned long long* acc, unsigned long long* 
     *status = 0;
 }
 
+// Go_stationary leaves C_centr cells as they are (Setka.cpp:5239); the
+// context path keeps both state buffers equal there.  Here state_out may be a
+// fresh array, so those cells are copied through from state_in.
+__global__ void noalloc_copy_centr(const uint32_t* __restrict__ flags, int n, StepBuffers b) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n || !(flags[c] & CF_CENTR)) return;
+    for (int k = 0; k < 5; k++) b.nxt[k][c] = b.cur[k][c];
+}
+
 }  // namespace
 
 extern "C" int gelios_stationary_step_noalloc(const gelios_params* prm, const gelios_device_grid* g,
@@ -148,6 +157,7 @@ extern "C" int gelios_stationary_step_noalloc(const gelios_params* prm, const ge
                     s);
     launch_stationary_units(d, *prm, b, flux, s);
     launch_stationary_update(d, *prm, b, flux, s);
+    noalloc_copy_centr<<<(d.n_cells + 127) / 128, 128, 0, s>>>(d.cflags, d.n_cells, b);
     launch_dt_finalize(b, s);
     e = cudaGetLastError();
     if (e != cudaSuccess) {

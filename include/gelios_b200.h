@@ -6,7 +6,9 @@
  * sizes and POD structs: a C++ driver that holds a reference Setka converts
  * its Point/Cell/Gran/Rail pointers to indices (Point::number, Cell::number,
  * All_Gran / All_Gran_copy order) and calls these functions in place of the
- * member functions (see INTEGRATION.md for the shim).
+ * member functions (a thin C++ shim over these entry points replaces the
+ * bodies of Setka::Go_5_komponent__MK2, Go_stationary and
+ * Go_stationary_5_komponent_inner_MK2).
  *
  * Conventions
  *   - return 0 on success, a negative GELIOS_E_* code on error; the message
@@ -387,12 +389,20 @@ int gelios_hlld_batch(const gelios_params *prm, int n, const double *in, double 
  * one fixed file-scope device array of about 6.0 MB that every GPU loading
  * the library holds until exit, so grids are limited to
  * GELIOS_NOALLOC_MAX_CELLS cells and GELIOS_NOALLOC_MAX_SLOTS face slots
- * (GELIOS_E_LIMIT beyond).  The first call on a device resolves that array's
- * device address and should come before any stream capture.  All calls share
- * the array: calls that overlap on the GPU (other streams, other threads)
- * race.  Inputs: the grid arrays below, state_in[5] (ro, p, u, v, Q per cell)
- * and dt_in (one device double, the dt of this step); outputs: state_out[5]
- * and dt_out (the dt the next step would use).  Runs on `stream`
+ * (GELIOS_E_LIMIT beyond).  The array is reserved when the CUDA module of the
+ * library loads on a device, which under lazy module loading (the default
+ * since CUDA 12.2) is the first call on that device; the first call on a
+ * device also resolves the array's device address (cached per device ordinal
+ * for the life of the process, so it goes stale after cudaDeviceReset or a
+ * different driver context on that device).  Make one call before any stream
+ * capture and before handing the rest of the device memory to a pool.  All
+ * calls share the array: calls that overlap on the GPU (other streams, other
+ * threads) race.  Inputs: the grid arrays below, state_in[5] (ro, p, u, v, Q
+ * per cell) and dt_in (one device double, the dt of this step); outputs:
+ * state_out[5] (every cell: C_centr cells, which the step leaves unchanged,
+ * are copied from state_in) and dt_out (the dt the next step would use).
+ * Density / pressure floor counts and status flags are not reported (the
+ * context path returns them in gelios_status).  Runs on `stream`
  * (cudaStream_t as void*, may be NULL) and returns without synchronising. */
 #define GELIOS_NOALLOC_MAX_CELLS 32768
 #define GELIOS_NOALLOC_MAX_SLOTS 131072

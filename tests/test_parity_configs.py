@@ -1,0 +1,148 @@
+"""Parity at the configurations themselves, in the conserved variables.
+
+The FP64 device path must agree with the oracle (the C restatement pinned bit
+for bit to the compiled reference) to <= 1e-12 relative after one or two
+steps and to <= 1e-9 after 1000 steps in every conserved variable:
+
+* gas dynamics (Go_5_komponent__MK2, Setka.cpp:10121-10482; the update of
+  Setka.cpp:10425-10460 advances exactly these): rho, rho u, rho v,
+  E = p / (gamma - 1) + rho (u^2 + v^2) / 2, and the tracer Q (updated in
+  conservative form by the reference itself);
+* MHD + pickup protons (no reference step; the project's step checked against
+  the oracle's go_mhd): ion rho, rho u, rho v, rho w,
+  E = p / (gamma - 1) + rho |v|^2 / 2 + |B|^2 / (8 pi), Bx, By, Bz, Q; pickup
+  rho, rho u, rho v, E.
+
+Error of a variable = max |device - oracle| / max |oracle| over the cells; a
+vector's components (momentum, field) are measured against the largest
+magnitude of the vector, since a component alone can be near zero where its
+vector is not.  The rail grids: Setka(30,7,11,20,60,20,40,40) (8,808 cells)
+for the long runs; Setka(200,100,50,100,100,100,150,150) (200,010 cells) and
+Setka(480,240,100,220,200,200,300,300) (938,010 cells), the two benchmarked
+grids, for two steps.  Point coordinates after the motion: <= 1e-13
+relative per step, <= 1e-11 after 1000 steps (libdevice cos / sin / pow
+against glibc, ~1 ulp per step, carried by the moving surfaces).
+"""
+import numpy as np
+import pytest
+
+import gelios_2d_b200 as g
+from gelios_2d_b200 import _native as N
+from gelios_2d_b200 import workloads as W
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+MEDIUM = W.SETKA_SMALL
+GAMMA = 5.0 / 3.0
+
+
+def go_params(p: N.GeliosParams) -> O.GoParams:
+    return O.GoParams(**{n: getattr(p, n) for n, _ in O.GoParams._fields_ if n != "pad_"}, pad_=0)
+
+
+def conserved_gas(st, gamma=GAMMA):
+    ro, p, u, v, Q = st
+    return {"rho": ro, "mom": np.stack([ro * u, ro * v]), "E": p / (gamma - 1) + 0.5 * ro * (u * u + v * v),
+            "Q": Q}
+
+
+def conserved_mhd(st, x8, gamma=GAMMA):
+    ro, p, u, v, Q = st
+    w, bx, by, bz, pr, pp, pu, pv = x8
+    b2 = bx * bx + by * by + bz * bz
+    return {"rho": ro, "mom": np.stack([ro * u, ro * v, ro * w]),
+            "E": p / (gamma - 1) + 0.5 * ro * (u * u + v * v + w * w) + b2 / (8.0 * np.pi),
+            "B": np.stack([bx, by, bz]), "Q": Q, "pui_rho": pr, "pui_mom": np.stack([pr * pu, pr * pv]),
+            "pui_E": pp / (gamma - 1) + 0.5 * pr * (pu * pu + pv * pv)}
+
+
+def errors(dev: dict, ora: dict) -> dict:
+    out = {}
+    for k, b in ora.items():
+        a = dev[k]
+        if b.ndim == 2:  # a vector: its components against the largest magnitude
+            scale = float(np.max(np.sqrt(np.sum(b * b, axis=0))))
+        else:
+            scale = float(np.max(np.abs(b)))
+        out[k] = float(np.max(np.abs(a - b))) / scale if scale > 0 else float(np.max(np.abs(a - b)))
+    return out
+
+
+def point_err(dev, ora):
+    x, y = dev.points()
+    pts = ora.points()
+    return max(float(np.max(np.abs(x - pts["x"]) / np.maximum(np.abs(pts["x"]), 1e-3))),
+               float(np.max(np.abs(y - pts["y"]) / np.maximum(np.abs(pts["y"]), 1e-3))))
+
+
+def mk2_pair(dims, steps, seed=9):
+    mesh = g.Mesh.setka(*dims)
+    P = N.reference_params()
+    st0 = W.init_conditions_reference(mesh)
+    mc = W.mc_fields(mesh, seed=seed)
+    dev = g.Setka(mesh, P)
+    ora = O.Oracle(go_params(P), mesh)
+    for b in (0, 1):
+        dev.set_par(b, st0)
+        ora.set_state(b, st0)
+    dev.set_mc(*mc)
+    ora.set_mc(*mc)
+    s = dev.Go_5_komponent__MK2(steps)
+    ora.mk2(steps)
+    return dev, ora, s
+
+
+@pytest.mark.parametrize("dims", [W.SETKA_200K, W.SETKA_1M], ids=["setka200k", "setka938k"])
+def test_mk2_two_steps_on_the_benchmarked_grids(dims):
+    dev, ora, s = mk2_pair(dims, 2)
+    assert s.result_buf == 0
+    for b in (0, 1):
+        e = errors(conserved_gas(dev.par(b)), conserved_gas(ora.get_state(b)))
+        assert max(e.values()) <= 1e-12, (b, e)
+    assert point_err(dev, ora) <= 1e-13
+    assert abs(s.dt - ora.last_dt()) <= 1e-12 * ora.last_dt()
+
+
+def test_mk2_1000_steps_conserved():
+    """One call of 1000 moving-grid steps (dt restarts at 1e-8 with the call,
+    as the reference's Go_5_komponent__MK2(step) does)."""
+    dev, ora, s = mk2_pair(MEDIUM, 1000)
+    assert s.result_buf == 0 and s.steps_done == 1000
+    e = errors(conserved_gas(dev.par(0)), conserved_gas(ora.get_state(0)))
+    assert max(e.values()) <= 1e-9, e
+    e1 = errors(conserved_gas(dev.par(1)), conserved_gas(ora.get_state(1)))
+    assert max(e1.values()) <= 1e-9, e1
+    assert point_err(dev, ora) <= 1e-11
+    assert abs(s.dt - ora.last_dt()) <= 1e-9 * ora.last_dt()
+
+
+def mhd_pair(dims, steps, seed=17):
+    mesh = g.Mesh.setka(*dims)
+    P = N.reference_params()
+    mp = W.mhd_params()
+    st0 = W.init_conditions_reference(mesh)
+    x0 = W.mhd_initial(mesh, st0, mp)
+    src = W.mhd_sources(mesh, seed=seed)
+    ora = O.Oracle(go_params(P), mesh)
+    dev = g.Setka(mesh, P)
+    dev.set_mhd_params(mp)
+    for b in (0, 1):
+        ora.set_state(b, st0)
+        ora.set_mhd(b, x0)
+        dev.set_par(b, st0)
+        dev.set_mhd(b, x0)
+    ora.set_sources(*src)
+    dev.set_sources(*src)
+    ora.mhd(mp.as_dict(), steps)
+    s = dev.Go_MHD_pickup(steps)
+    return dev, ora, s
+
+
+@pytest.mark.parametrize("steps,tol", [(1, 1e-12), (2, 1e-12), (1000, 1e-9)])
+def test_mhd_conserved(steps, tol):
+    dev, ora, s = mhd_pair(MEDIUM, steps)
+    b = steps % 2
+    assert s.result_buf == b
+    e = errors(conserved_mhd(dev.par(b), dev.mhd(b)), conserved_mhd(ora.get_state(b), ora.get_mhd(b)))
+    assert max(e.values()) <= tol, e
+    assert point_err(dev, ora) <= (1e-13 if steps <= 2 else 1e-11)

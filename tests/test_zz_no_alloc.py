@@ -60,12 +60,24 @@ def device_grid_arrays(m: g.Mesh) -> dict:
                 unit_slot=np.array(us, np.int32), unit_cell=np.array(uc, np.int32), unit_twin=np.array(ut, np.int32))
 
 
-def test_noalloc_step_matches_context_step_twice():
+def _case(name):
+    """(mesh, params, initial state): the polar plain grid, or the
+    reference's rail grid, whose central fan (C_centr cells) the step leaves
+    unchanged."""
+    if name == "polar":
+        mesh = W.plain_mesh(48, 32)
+        P = W.plain_params()
+        return mesh, P, W.plain_initial(mesh, P, seed=11)
+    mesh = g.Mesh.setka(*W.SETKA_SMALL)
+    assert np.count_nonzero(mesh["cell_type"] == 5) > 0
+    return mesh, N.reference_params(), W.init_conditions_reference(mesh)
+
+
+@pytest.mark.parametrize("case", ["polar", "setka_with_central_fan"])
+def test_noalloc_step_matches_context_step_twice(case):
     import torch
 
-    mesh = W.plain_mesh(48, 32)
-    P = W.plain_params()
-    st0 = W.plain_initial(mesh, P, seed=11)
+    mesh, P, st0 = _case(case)
     # the existing entry point: one and two steps through a context
     ctx = g.Setka(mesh, P)
     ctx.set_par(0, st0)
@@ -94,8 +106,9 @@ def test_noalloc_step_matches_context_step_twice():
     for k in t:
         setattr(grid, k, t[k].data_ptr())
     st_a = torch.from_numpy(np.ascontiguousarray(st0)).to(dev)
-    st_b = torch.zeros_like(st_a)
-    st_c = torch.zeros_like(st_a)
+    # fresh outputs (NaN): every cell must be written, C_centr cells included
+    st_b = torch.full_like(st_a, float("nan"))
+    st_c = torch.full_like(st_a, float("nan"))
     dt = torch.tensor([P.dt0, 0.0, 0.0], dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream(dev).cuda_stream
     L = N.lib()
@@ -114,6 +127,7 @@ def test_noalloc_step_matches_context_step_twice():
     torch.cuda.synchronize(dev)
     out1 = st_b.cpu().numpy()
     out2 = st_c.cpu().numpy()
+    assert np.isfinite(out1).all() and np.isfinite(out2).all()
     assert rel_err(out1, ref1) <= 1e-12
     assert rel_err(out2, ref2) <= 1e-12
     assert abs(dt[1].item() - s1.dt) <= 1e-12 * s1.dt
