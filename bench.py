@@ -74,8 +74,8 @@ WORKLOADS = {
 #             grid) + 4*4 neighbour indices = 264 B
 BYTES_PER_CELL = {"mk2": 288, "plain": 112, "k5": 392, "mhd": 288, "inner": 264}
 STEP_KERNELS = {
-    "mk2": "whole moving-grid step: recon, tracked_solve, source, surface_faces, rails, flux x2, update, commit "
-           "(one CUDA graph, 3 streams)",
+    "mk2": "whole moving-grid step: tracked recon + solve, source, surface_faces, rails, tracked flux, "
+           "face (reconstruction + flux), update, commit (one CUDA graph, 2 streams)",
     "plain": "whole plain step: stationary_persistent_kernel (face units, cell update, dt; all steps of a call "
              "in one cooperative launch)",
     "k5": "whole four-fluid step: centroid, surface_faces, rails, k5_cell, commit",
@@ -643,11 +643,11 @@ def main():
     S = g.Setka(mesh, params, device=device)
     load_inputs(S, form, st0, mc)
     tuned = None
-    if form == "mhd":  # launch shape of the face kernel picked on this grid (the library's autotuner)
-        v, tms = S.autotune(N.FORM_MHD_PUI, reps=3)
-        tuned = {"variant": v, "face_kernel_ms": tms}
     fcode = {"mk2": N.FORM_MK2, "k5": N.FORM_5_KOMPONENT, "mhd": N.FORM_MHD_PUI,
              "inner": N.FORM_INNER_MK2}.get(form, N.FORM_STATIONARY)
+    if form in ("mhd", "mk2"):  # launch shape of the face kernel picked on this grid (the library's autotuner)
+        v, tms = S.autotune(fcode, reps=3)
+        tuned = {"variant": v, "face_kernel_ms": tms}
     stream = torch.cuda.ExternalStream(S.stream_handle(), device=device)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")
     do_flush = not args.workload.endswith("_1m")

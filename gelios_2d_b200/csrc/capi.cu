@@ -106,6 +106,7 @@ struct gelios_ctx {
     DBuf src_fixed;  // MHD form: fixed charge-exchange sources (3 rows)
     DBuf flux_mhd;   // multi-fluid forms: 13 (MHD) or 21 (Go_5_komponent) flux rows per face slot, on first use
     int mhd_face_variant = 0;  // launch shape of the MHD face kernel (gelios_autotune)
+    int mk2_face_variant = 0;  // launch shape of the moving-grid face kernel (gelios_autotune)
     DBuf resid;                // residual partial sums (gelios_residual)
     // streamed host I/O (gelios_run_streamed): copy streams, staging
     // buffers and their events, created on first use
@@ -605,7 +606,7 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     rc |= upload<double>(ctx->flux, nullptr, 5 * static_cast<size_t>(ng), s);
     rc |= upload<double>(ctx->upf, nullptr, static_cast<size_t>(kUnitGeoRows) * u_slot.size(), s);
     rc |= upload<double>(ctx->aux, nullptr, 3 * static_cast<size_t>(nc), s);
-    rc |= upload<double>(ctx->rec, nullptr, static_cast<size_t>(kRecRows) * u_slot.size(), s);
+    rc |= upload<double>(ctx->rec, nullptr, static_cast<size_t>(kRecRows) * (u_tr1 - u_tr0 + 1), s);
     rc |= upload<double>(ctx->pstar, nullptr, static_cast<size_t>(u_tr1 - u_tr0) + 1, s);
     rc |= upload(ctx->sp_point, sp_point.data(), sp_point.size(), s);
     rc |= upload(ctx->sp_line, sp_line.data(), sp_line.size(), s);
@@ -865,18 +866,17 @@ int enqueue_mk2(gelios_ctx* ctx, const StepBuffers& b) {
     const gelios_params& P = ctx->prm;
     cudaStream_t s = ctx->stream;
     // Two streams per step.
-    //   side: face reconstructions, the star pressures of the tracked faces
-    //         and the charge-exchange source terms (none depends on the
-    //         motion), then, once the rails have moved, the tracked-face
-    //         fluxes (sampling of the solved Riemann problems at the face
-    //         speed);
-    //   main: surface tracking + rails, the other face fluxes, the cell
-    //         update, the commit.
+    //   side: the tracked face units' reconstructions and the star pressures
+    //         of their exact Riemann problems, the charge-exchange source
+    //         terms (none depends on the motion), then, once the rails have
+    //         moved, the tracked-face fluxes (sampling of the solved Riemann
+    //         problems at the face speed);
+    //   main: surface tracking + rails, reconstruction and flux of every
+    //         other face unit in one kernel, the cell update, the commit.
     cudaStream_t sd = ctx->side;
     GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_fork, s));
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_fork, 0));
     launch_mk2_recon(d, P, b, ctx->rec.as<double>(), sd);
-    GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_recon, sd));
     const int nsv = launch_mk2_tracked_solve(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(), sd);
     launch_mk2_source(d, P, b, ctx->aux.as<double>(), sd);
     cudaEvent_t e1 = ctx->phase_begin();
@@ -887,9 +887,8 @@ int enqueue_mk2(gelios_ctx* ctx, const StepBuffers& b) {
     const int nft = launch_mk2_flux_tracked(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(),
                                             ctx->flux.as<double>(), sd);
     GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_tracked, sd));
-    GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_recon, 0));
     cudaEvent_t e3 = ctx->phase_begin();
-    const int nfl = launch_mk2_flux_plain(d, P, b, ctx->rec.as<double>(), ctx->flux.as<double>(), s) + nft;
+    const int nfl = launch_mk2_faces(d, P, b, ctx->flux.as<double>(), s, ctx->mk2_face_variant) + nft;
     ctx->phase_end(1, e3, nfl);
     // the update reads the tracked-face fluxes and the source terms
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_tracked, 0));
@@ -900,7 +899,7 @@ int enqueue_mk2(gelios_ctx* ctx, const StepBuffers& b) {
     launch_commit(d, b, s);
     ctx->phase_end(4, e4, 1);
     GELIOS_CUDA_TRY(cudaGetLastError());
-    return nm + 4 + nfl + nsv;
+    return nm + 4 + nfl + nsv - 1 + (d.u_tr1 > d.u_tr0 ? 1 : 0);
 }
 
 // Enqueues one step of the MHD + pickup form on the main stream: Move_surface
@@ -1326,20 +1325,26 @@ extern "C" int gelios_run_streamed(gelios_ctx* ctx, int form, int nsteps, const 
     return GELIOS_OK;
 }
 
-extern "C" int gelios_variant_count(int form) { return form == GELIOS_FORM_MHD_PUI ? kMhdFaceVariants : 1; }
+extern "C" int gelios_variant_count(int form) {
+    return form == GELIOS_FORM_MHD_PUI ? kMhdFaceVariants : form == GELIOS_FORM_MK2 ? kMk2FaceVariants : 1;
+}
 
 extern "C" int gelios_set_variant(gelios_ctx* ctx, int form, int32_t variant) {
     if (!ctx || variant < 0 || variant >= gelios_variant_count(form)) return GELIOS_E_ARG;
     if (form == GELIOS_FORM_MHD_PUI) {
         ctx->mhd_face_variant = variant;
         ctx->drop_graphs();  // the captured steps hold the old launch shape
+    } else if (form == GELIOS_FORM_MK2) {
+        ctx->mk2_face_variant = variant;
+        ctx->drop_graphs();
     }
     return GELIOS_OK;
 }
 
 extern "C" int gelios_autotune(gelios_ctx* ctx, int form, int reps, int32_t* variant, double* ms) {
     if (!ctx || reps < 1) return GELIOS_E_ARG;
-    if (form != GELIOS_FORM_MHD_PUI) {
+    const bool mhd = form == GELIOS_FORM_MHD_PUI;
+    if (!mhd && form != GELIOS_FORM_MK2) {
         if (variant) *variant = 0;
         if (ms) *ms = 0.0;
         return GELIOS_OK;
@@ -1348,10 +1353,12 @@ extern "C" int gelios_autotune(gelios_ctx* ctx, int form, int reps, int32_t* var
     const DevMesh& d = ctx->d;
     GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
     cudaStream_t s = ctx->stream;
-    const size_t fb = static_cast<size_t>(kMhdFluxRows) * d.n_slots * sizeof(double);
-    if (ctx->flux_mhd.bytes != fb) {
-        ctx->drop_graphs();
-        if (ctx->flux_mhd.alloc(fb)) return GELIOS_E_CUDA;
+    if (mhd) {
+        const size_t fb = static_cast<size_t>(kMhdFluxRows) * d.n_slots * sizeof(double);
+        if (ctx->flux_mhd.bytes != fb) {
+            ctx->drop_graphs();
+            if (ctx->flux_mhd.alloc(fb)) return GELIOS_E_CUDA;
+        }
     }
     // the words a step starts from (dt0, empty accumulator); reset again below
     struct Words {
@@ -1391,12 +1398,20 @@ extern "C" int gelios_autotune(gelios_ctx* ctx, int form, int reps, int32_t* var
     GELIOS_CUDA_TRY(cudaEventCreate(&e1));
     int best = 0;
     double best_ms = 0.0;
-    for (int v = 0; v < kMhdFaceVariants; v++) {
-        launch_mhd_faces(d, ctx->prm, ctx->mprm, b, ctx->hstate[0].as<double>(), ctx->flux_mhd.as<double>(), s, v);
-        cudaEventRecord(e0, s);
-        for (int r = 0; r < reps; r++)
+    // the face kernel of the form (only scratch and the dt / status words,
+    // reset below, are written)
+    auto faces = [&](int v) {
+        if (mhd)
             launch_mhd_faces(d, ctx->prm, ctx->mprm, b, ctx->hstate[0].as<double>(), ctx->flux_mhd.as<double>(), s,
                              v);
+        else
+            launch_mk2_faces(d, ctx->prm, b, ctx->flux.as<double>(), s, v);
+    };
+    const int nv = mhd ? kMhdFaceVariants : kMk2FaceVariants;
+    for (int v = 0; v < nv; v++) {
+        faces(v);
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < reps; r++) faces(v);
         cudaEventRecord(e1, s);
         cudaError_t err = cudaEventSynchronize(e1);
         float t = 0.f;
@@ -1417,8 +1432,9 @@ extern "C" int gelios_autotune(gelios_ctx* ctx, int form, int reps, int32_t* var
     cudaEventDestroy(e1);
     GELIOS_CUDA_TRY(cudaMemcpyAsync(ctx->words.p, &w, sizeof(w), cudaMemcpyHostToDevice, s));
     GELIOS_CUDA_TRY(cudaStreamSynchronize(s));
-    if (best != ctx->mhd_face_variant) {
-        ctx->mhd_face_variant = best;
+    int& current = mhd ? ctx->mhd_face_variant : ctx->mk2_face_variant;
+    if (best != current) {
+        current = best;
         ctx->drop_graphs();
     }
     if (variant) *variant = best;

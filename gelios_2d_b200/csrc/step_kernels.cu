@@ -39,12 +39,6 @@ namespace cg = cooperative_groups;
 
 // Minimum resident blocks per SM of the grid-wide moving-grid kernels
 // (register caps: 128 threads x 65536/(128 x minBlocks) registers).
-#ifndef GELIOS_RECON_MINB
-#define GELIOS_RECON_MINB 8
-#endif
-#ifndef GELIOS_FLUX_MINB
-#define GELIOS_FLUX_MINB 8
-#endif
 #ifndef GELIOS_UPDATE_MINB
 #define GELIOS_UPDATE_MINB 6
 #endif
@@ -873,191 +867,227 @@ __device__ __forceinline__ St5 mk2_usualy_side(const double* const* st, const do
     return tvd_usualy(st, cx, cy, fx, fy, Ms, Mx, My, So, Sd, (mf & CF_AXIS) != 0, tracked, status);
 }
 
-// The MK2 face units in two kernels:
-//  * mk2_recon_kernel: the two reconstructed face states of every unit
-//    (Setka.cpp:10204-10276: TVD / radial TVD / boundary states).  They use
-//    the points before the motion only, so this kernel runs on the side
-//    stream while surface tracking and the rails move the grid;
-//  * mk2_flux_kernel: face speed W from the moved points, HLL / HLLC, exact
-//    Godunov on tracked faces (Setka.cpp:10198-10209, 10335-10380), slot
-//    fluxes and CFL candidates.
-// rec rows: ro, p, u, v, Q of the owner side, then of the other side.
-// LANES = 2: two lanes per unit; on interior faces lane 0 reconstructs the
-// owner side and lane 1 the other side.  LANES = 1: one thread does both.
-template <int LANES>
-__global__ void __launch_bounds__(128, GELIOS_RECON_MINB) mk2_recon_kernel(DevMesh d, gelios_params P, StepBuffers b,
-                                                        double* __restrict__ rec) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int u = t / LANES, side = LANES == 2 ? (t & 1) : 0;
+// One MK2 face unit before the grid moves (Setka.cpp:10204-10276): the two
+// reconstructed face states (TVD / radial TVD / boundary states), the face
+// normal, S = |AB| (yA + yB) / 2, the face centre and the two CFL distances
+// (negative: that side is not updated this step).  Everything here reads the
+// points before the motion (X, Y) and the cached centroids, never the moved
+// points, so it may run before or after the rails.
+struct RecUnit {
+    St5 a, o;                  // owner side, other side
+    double n1, n2, S, x2, y2;  // face normal, S, face centre
+    double dist, distn;        // owner / other centroid to the face centre, -1 if not updated
+};
+
+__device__ __forceinline__ void mk2_recon_unit(const DevMesh& d, const gelios_params& P, const StepBuffers& b, int u,
+                                               RecUnit& r, int* status) {
+    const int K = d.u_cell[u], nb = d.u_nb[u];
+    const uint32_t info = d.u_info[u];
+    const double x = b.cx[K], y = b.cy[K];
+    const bool procK = !(sqrt(sq(x) + sq(y)) < P.R11);
+    double x3 = 0.0, y3 = 0.0;
+    bool procN = false;
+    if (nb >= 0) {
+        x3 = b.cx[nb];
+        y3 = b.cy[nb];
+        procN = !(sqrt(sq(x3) + sq(y3)) < P.R11);
+    }
+    const int A = d.u_A[u], B = d.u_B[u];
+    const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
+    const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
+    {
+        double t1 = xb - xa, t2 = yb - ya;
+        const double nn = sqrt(sq(t1) + sq(t2));
+        t1 = t1 / nn;
+        t2 = t2 / nn;
+        r.n1 = t2;
+        r.n2 = -t1;
+        r.S = sqrt(sq(xb - xa) + sq(yb - ya)) * (ya + yb) * 0.5;
+        r.x2 = x2;
+        r.y2 = y2;
+        r.dist = procK ? sqrt(sq(x - x2) + sq(y - y2)) : -1.0;
+        r.distn = procN ? sqrt(sq(x3 - x2) + sq(y3 - y2)) : -1.0;
+    }
+    if (!(procK || procN)) return;
+    const int ft = info & SI_TYPE_MASK;
+    const uint32_t cf = (info >> UI_CF_OWN) & 15u;
+    const double g2 = 2 * P.gamma;
+    const St5 par1 = load_state(b.cur, K);
+    St5 par11 = par1;
+    St5 par2 = get_par(P, ft, par1, b.cur, nb, x2, y2);
+    const double dis = sqrt(sq(x2) + sq(y2));
+    const bool tracked = (info & SI_GOD) != 0;
+    const uint32_t nbf = (info >> UI_CF_NB) & 15u;
+    const bool radial = ((cf & CF_C1) && (ft == G_USUALY || ft == G_AXIS)) || ft == G_INNER_SPHERE ||
+                        (ft == G_USUALY && (nbf & CF_C1));
+    const double pdis = radial ? pow2g(dis, g2) : 1.0;
+    if (ft == G_USUALY) {
+        r.a = mk2_usualy_side(b.cur, b.cx, b.cy, b.rp, x2, y2, dis, pdis, par1, x, y, b.rp[K], cf, nb, d.u_sd[u],
+                              tracked, status);
+        r.o = mk2_usualy_side(b.cur, b.cx, b.cy, b.rp, x2, y2, dis, pdis, par2, x3, y3, b.rp[nb], nbf, K, d.u_sd2[u],
+                              tracked, status);
+        return;
+    }
+    if (ft == G_INNER_SPHERE) {
+        const double radius = sqrt(sq(x) + sq(y));
+        par11.ro = par11.ro * sq(radius) / sq(dis);
+        par11.Q = par11.Q * sq(radius) / sq(dis);
+        par11.p = par11.p * (b.rp[K] / pdis);
+    } else if (ft == G_AXIS) {
+        if (cf & CF_C1) {
+            const double radius = sqrt(sq(x) + sq(y));
+            par11.ro = par11.ro * sq(radius) / sq(dis);
+            par11.Q = par11.Q * sq(radius) / sq(dis);
+            par11.p = par11.p * (b.rp[K] / pdis);
+            polar_perenos(x, y, x2, y2, par11.u, par11.v);
+        } else {
+            par11 = tvd_axis(b.cur, b.cx, b.cy, x2, y2, par1, x, y, d.u_sd[u]);
+        }
+        par2 = par11;
+        par2.v = -par2.v;
+    }
+    r.a = par11;
+    r.o = par2;
+}
+
+// The flux of one MK2 face unit once the grid has moved (Setka.cpp:10198-10209,
+// 10335-10393): face speed W from the moved points, HLL (`metod 0`), exact
+// Godunov sampled at W on tracked faces (star pressure pstar solved before the
+// motion), F.S to the owner slot and -F.S to the twin slot, CFL candidates.
+template <typename TF, bool TRACKED>
+__device__ __forceinline__ void mk2_flux_unit(const DevMesh& d, const gelios_params& P, const StepBuffers& b, int u,
+                                              const RecUnit& r, double* __restrict__ fl, const double* pstar,
+                                              double& tmin_u, int* status) {
+    const bool procK = !(r.dist < 0.0), procN = !(r.distn < 0.0);
+    if (!(procK || procN)) return;
+    const size_t ng = d.n_slots;
+    const double dt = *b.dt_cur;
+    const uint32_t info = d.u_info[u];
+    const int A = d.u_A[u], B = d.u_B[u];
+    const double x4 = (d.X2[A] + d.X2[B]) / 2.0, y4 = (d.Y2[A] + d.Y2[B]) / 2.0;
+    const double W = ((x4 - r.x2) * r.n1 + (y4 - r.y2) * r.n2) / dt;
+    const int g = d.u_slot[u], gt = d.u_twin[u];
+    const bool np = (info & SI_NP) != 0;
+    FluxOut<double> F;
+    const double UU = hllc_flux<TF>(P.gamma, P.kurant, r.a, r.o, W, r.n1, r.n2, 1.0, 0, np, F);
+    const double S = r.S;
+    double fm0 = F.P0 * S, fm1 = F.P1 * S, fm2 = F.P2 * S, fm3 = F.P3 * S;
+    double UG = 1.0;
+    if (TRACKED) {
+        double q1[5] = {r.a.ro, r.a.p, r.a.u, r.a.v, 0.0};
+        double q2[5] = {r.o.ro, r.o.p, r.o.u, r.o.v, 0.0};
+        double nv[3] = {r.n1, r.n2, 0.0};
+        double qq[5], ds[3];
+        UG = godunov_dev<false>(P.gamma, P.kurant, q1, q2, nv, qq, ds, W, 1.0, P.godunov_max_iter, status, pstar);
+        fm0 = qq[0] * S;
+        fm1 = qq[1] * S;
+        fm2 = qq[2] * S;
+        fm3 = qq[4] * S;
+    }
+    const double fq = F.PQ * S;
+    fl[0 * ng + g] = fm0;
+    fl[1 * ng + g] = fm1;
+    fl[2 * ng + g] = fm2;
+    fl[3 * ng + g] = fm3;
+    fl[4 * ng + g] = fq;
+    if (procK) {
+        // reference order: Godunov candidate first, then HLL (Setka.cpp:10359, 10366)
+        if (TRACKED) tmin_u = dmin_ref(tmin_u, P.kurant * r.dist / UG);
+        tmin_u = dmin_ref(tmin_u, P.kurant * r.dist / UU);
+    }
+    if (gt >= 0) {
+        fl[0 * ng + gt] = -fm0;
+        fl[1 * ng + gt] = -fm1;
+        fl[2 * ng + gt] = -fm2;
+        fl[3 * ng + gt] = -fm3;
+        fl[4 * ng + gt] = -fq;
+        if (procN) {
+            if (TRACKED) tmin_u = dmin_ref(tmin_u, P.kurant * r.distn / UG);
+            tmin_u = dmin_ref(tmin_u, P.kurant * r.distn / UU);
+        }
+    }
+}
+
+// Rows of the tracked units' reconstruction (kRecRows rows of n_tracked
+// doubles; row r of tracked unit i at rec[r * n_tracked + i]).
+__device__ __forceinline__ void rec_store(double* __restrict__ rec, size_t n, int i, const RecUnit& r) {
+    const double v[kRecRows] = {r.a.ro, r.a.p, r.a.u, r.a.v, r.a.Q, r.o.ro, r.o.p, r.o.u, r.o.v,
+                                r.o.Q, r.n1,  r.n2,  r.S,   r.x2,  r.y2,  r.dist, r.distn};
+#pragma unroll
+    for (int k = 0; k < kRecRows; k++) rec[k * n + i] = v[k];
+}
+__device__ __forceinline__ RecUnit rec_load(const double* __restrict__ rec, size_t n, int i) {
+    RecUnit r;
+    r.a.ro = rec[0 * n + i];
+    r.a.p = rec[1 * n + i];
+    r.a.u = rec[2 * n + i];
+    r.a.v = rec[3 * n + i];
+    r.a.Q = rec[4 * n + i];
+    r.o.ro = rec[5 * n + i];
+    r.o.p = rec[6 * n + i];
+    r.o.u = rec[7 * n + i];
+    r.o.v = rec[8 * n + i];
+    r.o.Q = rec[9 * n + i];
+    r.n1 = rec[10 * n + i];
+    r.n2 = rec[11 * n + i];
+    r.S = rec[12 * n + i];
+    r.x2 = rec[13 * n + i];
+    r.y2 = rec[14 * n + i];
+    r.dist = rec[15 * n + i];
+    r.distn = rec[16 * n + i];
+    return r;
+}
+
+// The tracked face units (grouped in [u_tr0, u_tr1)) are reconstructed before
+// the motion: their exact Riemann problems are solved while the grid moves.
+__global__ void __launch_bounds__(128) mk2_recon_tracked_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                                double* __restrict__ rec) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nt = d.u_tr1 - d.u_tr0;
     int status = 0;
-    if (u < d.n_units) {
-        const size_t n = d.n_units;
-        const int K = d.u_cell[u], nb = d.u_nb[u];
-        const uint32_t info = d.u_info[u];
-        const double x = b.cx[K], y = b.cy[K];
-        const bool procK = !(sqrt(sq(x) + sq(y)) < P.R11);
-        double x3 = 0.0, y3 = 0.0;
-        bool procN = false;
-        if (nb >= 0) {
-            x3 = b.cx[nb];
-            y3 = b.cy[nb];
-            procN = !(sqrt(sq(x3) + sq(y3)) < P.R11);
-        }
-        const int A = d.u_A[u], B = d.u_B[u];
-        const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
-        const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
-        if (side == 0) {
-            double t1 = xb - xa, t2 = yb - ya;
-            const double nn = sqrt(sq(t1) + sq(t2));
-            t1 = t1 / nn;
-            t2 = t2 / nn;
-            rec[10 * n + u] = t2;
-            rec[11 * n + u] = -t1;
-            rec[12 * n + u] = sqrt(sq(xb - xa) + sq(yb - ya)) * (ya + yb) * 0.5;
-            rec[13 * n + u] = x2;
-            rec[14 * n + u] = y2;
-            rec[15 * n + u] = procK ? sqrt(sq(x - x2) + sq(y - y2)) : -1.0;
-            rec[16 * n + u] = procN ? sqrt(sq(x3 - x2) + sq(y3 - y2)) : -1.0;
-        }
-        if (procK || procN) {
-            const int ft = info & SI_TYPE_MASK;
-            const uint32_t cf = (info >> UI_CF_OWN) & 15u;
-            const double g2 = 2 * P.gamma;
-            const St5 par1 = load_state(b.cur, K);
-            St5 par11 = par1;
-            St5 par2 = get_par(P, ft, par1, b.cur, nb, x2, y2);
-            const double dis = sqrt(sq(x2) + sq(y2));
-            const bool tracked = (info & SI_GOD) != 0;
-            const uint32_t nbf = (info >> UI_CF_NB) & 15u;
-            const bool radial = ((cf & CF_C1) && (ft == G_USUALY || ft == G_AXIS)) || ft == G_INNER_SPHERE ||
-                                (ft == G_USUALY && (nbf & CF_C1));
-            const double pdis = radial ? pow2g(dis, g2) : 1.0;
-            if (ft == G_USUALY) {
-                for (int sd = side; sd < 2; sd += LANES) {
-                    const bool s1 = sd == 1;
-                    const St5 r = mk2_usualy_side(b.cur, b.cx, b.cy, b.rp, x2, y2, dis, pdis, s1 ? par2 : par1,
-                                                  s1 ? x3 : x, s1 ? y3 : y, b.rp[s1 ? nb : K], s1 ? nbf : cf,
-                                                  s1 ? K : nb, s1 ? d.u_sd2[u] : d.u_sd[u], tracked, &status);
-                    const int r0 = s1 ? 5 : 0;
-                    rec[(r0 + 0) * n + u] = r.ro;
-                    rec[(r0 + 1) * n + u] = r.p;
-                    rec[(r0 + 2) * n + u] = r.u;
-                    rec[(r0 + 3) * n + u] = r.v;
-                    rec[(r0 + 4) * n + u] = r.Q;
-                }
-            } else if (side == 0) {
-                if (ft == G_INNER_SPHERE) {
-                    const double radius = sqrt(sq(x) + sq(y));
-                    par11.ro = par11.ro * sq(radius) / sq(dis);
-                    par11.Q = par11.Q * sq(radius) / sq(dis);
-                    par11.p = par11.p * (b.rp[K] / pdis);
-                } else if (ft == G_AXIS) {
-                    if (cf & CF_C1) {
-                        const double radius = sqrt(sq(x) + sq(y));
-                        par11.ro = par11.ro * sq(radius) / sq(dis);
-                        par11.Q = par11.Q * sq(radius) / sq(dis);
-                        par11.p = par11.p * (b.rp[K] / pdis);
-                        polar_perenos(x, y, x2, y2, par11.u, par11.v);
-                    } else {
-                        par11 = tvd_axis(b.cur, b.cx, b.cy, x2, y2, par1, x, y, d.u_sd[u]);
-                    }
-                    par2 = par11;
-                    par2.v = -par2.v;
-                }
-                rec[0 * n + u] = par11.ro;
-                rec[1 * n + u] = par11.p;
-                rec[2 * n + u] = par11.u;
-                rec[3 * n + u] = par11.v;
-                rec[4 * n + u] = par11.Q;
-                rec[5 * n + u] = par2.ro;
-                rec[6 * n + u] = par2.p;
-                rec[7 * n + u] = par2.u;
-                rec[8 * n + u] = par2.v;
-                rec[9 * n + u] = par2.Q;
-            }
-        }
+    if (i < nt) {
+        RecUnit r;
+        r.a = St5{};
+        r.o = St5{};
+        mk2_recon_unit(d, P, b, d.u_tr0 + i, r, &status);
+        rec_store(rec, nt, i, r);
     }
     if (status) atomicOr(b.status, status);
 }
 
-// Units are grouped by kind with the tracked ones in [u_tr0, u_tr1): the
-// kernel without the exact Godunov solver covers the rest (index i is
-// remapped around the tracked range), a second launch covers that range.
-template <typename TF, bool TRACKED>
-__global__ void __launch_bounds__(128, GELIOS_FLUX_MINB) mk2_flux_kernel(DevMesh d, gelios_params P, StepBuffers b,
-                                                       const double* __restrict__ rec, double* __restrict__ fl,
-                                                       const double* __restrict__ pstar, int n_launch) {
+// Tracked units after the motion: sampling of the solved Riemann problems
+// at the face speed (one thread per unit).
+template <typename TF>
+__global__ void __launch_bounds__(32) mk2_flux_tracked_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                              const double* __restrict__ rec, double* __restrict__ fl,
+                                                              const double* __restrict__ pstar) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nt = d.u_tr1 - d.u_tr0;
+    double tmin_u = __longlong_as_double(0x7ff0000000000000LL);
+    int status = 0;
+    if (i < nt) {
+        const RecUnit r = rec_load(rec, nt, i);
+        mk2_flux_unit<TF, true>(d, P, b, d.u_tr0 + i, r, fl, pstar + i, tmin_u, &status);
+    }
+    block_reduce_commit(tmin_u, 0, 0, status, b.dt_acc, b.counters, b.status);
+}
+
+// Every other face unit after the motion, reconstruction and flux in one
+// pass: the reconstructed states stay in registers (no per-unit scratch).
+// Index i is remapped around the tracked range [u_tr0, u_tr1).
+template <typename TF, int MINB>
+__global__ void __launch_bounds__(128, MINB) mk2_face_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                           double* __restrict__ fl, int n_launch) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double tmin_u = __longlong_as_double(0x7ff0000000000000LL);
     int status = 0;
-    const size_t ng = d.n_slots;
-    const int u = TRACKED ? d.u_tr0 + i : (i < d.u_tr0 ? i : i + (d.u_tr1 - d.u_tr0));
     if (i < n_launch) {
-        const size_t n = d.n_units;
-        const double dist = rec[15 * n + u], distn = rec[16 * n + u];
-        const bool procK = !(dist < 0.0), procN = !(distn < 0.0);
-        if (procK || procN) {
-            const double dt = *b.dt_cur;
-            const uint32_t info = d.u_info[u];
-            const int A = d.u_A[u], B = d.u_B[u];
-            const double n1 = rec[10 * n + u], n2 = rec[11 * n + u];
-            const double S = rec[12 * n + u], x2 = rec[13 * n + u], y2 = rec[14 * n + u];
-            const double x4 = (d.X2[A] + d.X2[B]) / 2.0, y4 = (d.Y2[A] + d.Y2[B]) / 2.0;
-            const double W = ((x4 - x2) * n1 + (y4 - y2) * n2) / dt;
-            St5 par11, par2;
-            par11.ro = rec[0 * n + u];
-            par11.p = rec[1 * n + u];
-            par11.u = rec[2 * n + u];
-            par11.v = rec[3 * n + u];
-            par11.Q = rec[4 * n + u];
-            par2.ro = rec[5 * n + u];
-            par2.p = rec[6 * n + u];
-            par2.u = rec[7 * n + u];
-            par2.v = rec[8 * n + u];
-            par2.Q = rec[9 * n + u];
-            const int g = d.u_slot[u], gt = d.u_twin[u];
-            const bool tracked = TRACKED;
-            const bool np = (info & SI_NP) != 0;
-            FluxOut<double> F;
-            const double UU = hllc_flux<TF>(P.gamma, P.kurant, par11, par2, W, n1, n2, 1.0, 0, np, F);
-            double fm0 = F.P0 * S, fm1 = F.P1 * S, fm2 = F.P2 * S, fm3 = F.P3 * S;
-            double UG = 1.0;
-            if (TRACKED) {
-                double q1[5] = {par11.ro, par11.p, par11.u, par11.v, 0.0};
-                double q2[5] = {par2.ro, par2.p, par2.u, par2.v, 0.0};
-                double nv[3] = {n1, n2, 0.0};
-                double qq[5], ds[3];
-                // star pressure from mk2_tracked_solve_kernel (solved before the motion)
-                UG = godunov_dev<false>(P.gamma, P.kurant, q1, q2, nv, qq, ds, W, 1.0, P.godunov_max_iter, &status,
-                                        pstar + i);
-                fm0 = qq[0] * S;
-                fm1 = qq[1] * S;
-                fm2 = qq[2] * S;
-                fm3 = qq[4] * S;
-            }
-            const double fq = F.PQ * S;
-            fl[0 * ng + g] = fm0;
-            fl[1 * ng + g] = fm1;
-            fl[2 * ng + g] = fm2;
-            fl[3 * ng + g] = fm3;
-            fl[4 * ng + g] = fq;
-            if (procK) {
-                // reference order: Godunov candidate first, then HLL (Setka.cpp:10359, 10366)
-                if (tracked) tmin_u = dmin_ref(tmin_u, P.kurant * dist / UG);
-                tmin_u = dmin_ref(tmin_u, P.kurant * dist / UU);
-            }
-            if (gt >= 0) {
-                fl[0 * ng + gt] = -fm0;
-                fl[1 * ng + gt] = -fm1;
-                fl[2 * ng + gt] = -fm2;
-                fl[3 * ng + gt] = -fm3;
-                fl[4 * ng + gt] = -fq;
-                if (procN) {
-                    if (tracked) tmin_u = dmin_ref(tmin_u, P.kurant * distn / UG);
-                    tmin_u = dmin_ref(tmin_u, P.kurant * distn / UU);
-                }
-            }
-        }
+        const int u = i < d.u_tr0 ? i : i + (d.u_tr1 - d.u_tr0);
+        RecUnit r;
+        r.a = St5{};
+        r.o = St5{};
+        mk2_recon_unit(d, P, b, u, r, &status);
+        mk2_flux_unit<TF, false>(d, P, b, u, r, fl, nullptr, tmin_u, &status);
     }
     block_reduce_commit(tmin_u, 0, 0, status, b.dt_acc, b.counters, b.status);
 }
@@ -1065,22 +1095,22 @@ __global__ void __launch_bounds__(128, GELIOS_FLUX_MINB) mk2_flux_kernel(DevMesh
 // Star pressure of the exact Godunov problem of every tracked-face unit
 // (Solvers.cpp:1174-1305).  It depends on the reconstructed states and on
 // the face normal before the motion, not on the face speed, so it runs on a
-// side stream while the grid moves; mk2_flux_kernel<TRACKED> samples the
+// side stream while the grid moves; mk2_flux_tracked_kernel samples the
 // solution at the face speed afterwards.  One warp per unit (warp-cooperative
 // bisection); pstar[i] belongs to unit u_tr0 + i.
 __global__ void __launch_bounds__(64) mk2_tracked_solve_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                                const double* __restrict__ rec,
                                                                double* __restrict__ pstar) {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= d.u_tr1 - d.u_tr0) return;
-    const int u = d.u_tr0 + i;
+    const int nt = d.u_tr1 - d.u_tr0;
+    if (i >= nt) return;
     int status = 0;
-    const size_t n = d.n_units;
+    const size_t n = nt;
     // a unit with neither side updated has no flux (rows 15 and 16)
-    if (rec[15 * n + u] < 0.0 && rec[16 * n + u] < 0.0) return;
-    double q1[5] = {rec[0 * n + u], rec[1 * n + u], rec[2 * n + u], rec[3 * n + u], 0.0};
-    double q2[5] = {rec[5 * n + u], rec[6 * n + u], rec[7 * n + u], rec[8 * n + u], 0.0};
-    double nv[3] = {rec[10 * n + u], rec[11 * n + u], 0.0};
+    if (rec[15 * n + i] < 0.0 && rec[16 * n + i] < 0.0) return;
+    double q1[5] = {rec[0 * n + i], rec[1 * n + i], rec[2 * n + i], rec[3 * n + i], 0.0};
+    double q2[5] = {rec[5 * n + i], rec[6 * n + i], rec[7 * n + i], rec[8 * n + i], 0.0};
+    double nv[3] = {rec[10 * n + i], rec[11 * n + i], 0.0};
     double qq[5], ds[3], p = 0.0;
     godunov_dev<true>(P.gamma, P.kurant, q1, q2, nv, qq, ds, 0.0, 1.0, P.godunov_max_iter, &status, nullptr, &p);
     if ((threadIdx.x & 31) == 0) {
@@ -3192,17 +3222,33 @@ void launch_plain_batch_words_init(const PlainInstance* inst, const int* active,
     if (n > 0) plain_batch_words_init_kernel<<<blocks_for(n, 128), 128, 0, s>>>(inst, active, n);
 }
 void launch_mk2_recon(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* rec, cudaStream_t s) {
-    constexpr int kLanes = 1;
-    mk2_recon_kernel<kLanes><<<blocks_for(kLanes * d.n_units, 128), 128, 0, s>>>(d, P, b, rec);
+    const int nt = d.u_tr1 - d.u_tr0;
+    if (nt > 0) mk2_recon_tracked_kernel<<<blocks_for(nt, 128), 128, 0, s>>>(d, P, b, rec);
 }
-int launch_mk2_flux_plain(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
-                          double* fl, cudaStream_t s) {
+template <int MINB>
+static void launch_mk2_faces_v(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl, int nr,
+                               cudaStream_t s) {
+    if (P.precision == GELIOS_PREC_FP32_FLUX)
+        mk2_face_kernel<float, MINB><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, b, fl, nr);
+    else
+        mk2_face_kernel<double, MINB><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, b, fl, nr);
+}
+// variant v: minimum resident blocks of 128 threads per SM (a register cap):
+// 5, 4, 6, 8
+const char* mk2_face_variant_name(int v) {
+    static const char* names[kMk2FaceVariants] = {"128x5", "128x4", "128x6", "128x8"};
+    return (v >= 0 && v < kMk2FaceVariants) ? names[v] : "?";
+}
+int launch_mk2_faces(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl, cudaStream_t s,
+                     int variant) {
     const int nr = d.n_units - (d.u_tr1 - d.u_tr0);
     if (nr <= 0) return 0;
-    if (P.precision == GELIOS_PREC_FP32_FLUX)
-        mk2_flux_kernel<float, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, b, rec, fl, nullptr, nr);
-    else
-        mk2_flux_kernel<double, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, b, rec, fl, nullptr, nr);
+    switch (variant) {
+        case 1: launch_mk2_faces_v<4>(d, P, b, fl, nr, s); break;
+        case 2: launch_mk2_faces_v<6>(d, P, b, fl, nr, s); break;
+        case 3: launch_mk2_faces_v<8>(d, P, b, fl, nr, s); break;
+        default: launch_mk2_faces_v<5>(d, P, b, fl, nr, s); break;
+    }
     return 1;
 }
 int launch_mk2_tracked_solve(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
@@ -3217,9 +3263,9 @@ int launch_mk2_flux_tracked(const DevMesh& d, const gelios_params& P, const Step
     const int nt = d.u_tr1 - d.u_tr0;
     if (nt <= 0) return 0;
     if (P.precision == GELIOS_PREC_FP32_FLUX)
-        mk2_flux_kernel<float, true><<<blocks_for(nt, 32), 32, 0, s>>>(d, P, b, rec, fl, pstar, nt);
+        mk2_flux_tracked_kernel<float><<<blocks_for(nt, 32), 32, 0, s>>>(d, P, b, rec, fl, pstar);
     else
-        mk2_flux_kernel<double, true><<<blocks_for(nt, 32), 32, 0, s>>>(d, P, b, rec, fl, pstar, nt);
+        mk2_flux_tracked_kernel<double><<<blocks_for(nt, 32), 32, 0, s>>>(d, P, b, rec, fl, pstar);
     return 1;
 }
 void launch_mk2_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,

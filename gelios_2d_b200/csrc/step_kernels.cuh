@@ -66,8 +66,9 @@ struct DevMesh {
 
 // Buffers of one time step (double buffering of the state like par[now1] ->
 // par[now2]; centroids of the current/next point positions; dt words).
-// Rows of the per-unit reconstruction array of the moving-grid step
-// (unit-major, n_units doubles per row), written before the grid moves:
+// Rows of the tracked units' reconstruction array of the moving-grid step
+// (unit-major, n_tracked = u_tr1 - u_tr0 doubles per row), written before the
+// grid moves (the other units reconstruct in registers after the motion):
 //   0-4   owner side TVD state ro, p, u, v, Q
 //   5-9   other side TVD state
 //   10,11 face normal n1, n2 (pre-motion points)
@@ -136,9 +137,17 @@ struct PlainInstance {
 cudaError_t launch_stationary_batch(const DevMesh& d, const PlainInstance* inst, const int* active, int n_active,
                                     int nsteps, bool fp32, cudaStream_t s);
 void launch_plain_batch_words_init(const PlainInstance* inst, const int* active, int n, cudaStream_t s);
+// Moving-grid step: reconstruction of the tracked units before the motion
+// (rec: kRecRows x n_tracked), reconstruction + flux of every other unit after
+// it (mk2_face_kernel, no scratch but the flux slots).
 void launch_mk2_recon(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* rec, cudaStream_t s);
-int launch_mk2_flux_plain(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
-                          double* fl, cudaStream_t s);
+// The face kernel has kMk2FaceVariants launch shapes (resident blocks of 128
+// threads per SM); variant 0 is the default, gelios_autotune picks the
+// fastest for a grid.  All shapes give the same bits.
+constexpr int kMk2FaceVariants = 4;
+const char* mk2_face_variant_name(int v);
+int launch_mk2_faces(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl, cudaStream_t s,
+                     int variant = 0);
 int launch_mk2_tracked_solve(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
                              double* pstar, cudaStream_t s);
 int launch_mk2_flux_tracked(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,

@@ -39,7 +39,29 @@ def lib(fast: bool = False) -> C.CDLL:
     name = "libgelios_ref_fast.so" if fast else "libgelios_ref.so"
     if name in _LIBS:
         return _LIBS[name]
-    L = _load(name)
+    L = _configure(_load(name))
+    _LIBS[name] = L
+    return L
+
+
+def shim_lib() -> C.CDLL:
+    """The parity build of the reference plus include/gelios_setka_shim.hpp
+    (oracle/shim_harness.cpp), linked against the product library: loads
+    gelios_2d_b200/_lib/libgelios_b200.so.  Tests only."""
+    name = "libgelios_shim.so"
+    if name in _LIBS:
+        return _LIBS[name]
+    L = _configure(_load(name))
+    vp = C.c_void_p
+    L.gshim_mirror_check.argtypes = [vp, C.c_char_p, C.c_int]
+    L.gshim_new.restype = vp
+    L.gshim_free.argtypes = [vp]
+    L.gshim_step.argtypes = [vp, vp, C.c_int, C.c_int]
+    _LIBS[name] = L
+    return L
+
+
+def _configure(L: C.CDLL) -> C.CDLL:
     vp = C.c_void_p
     L.gref_setka_new.restype = vp
     L.gref_setka_new.argtypes = [C.c_int] * 8
@@ -92,7 +114,6 @@ def lib(fast: bool = False) -> C.CDLL:
     L.gref_set_threads.argtypes = [C.c_int]
     L.gref_max_threads.restype = C.c_int
     L.gref_set_threads(1)
-    _LIBS[name] = L
     return L
 
 
@@ -127,8 +148,8 @@ class RefSetka:
 
     # ------------------------------------------------------------ construction
     @classmethod
-    def constructor(cls, N1, N2, N3, N4, M1, M2, M3, M4, fast=False) -> "RefSetka":
-        L = lib(fast)
+    def constructor(cls, N1, N2, N3, N4, M1, M2, M3, M4, fast=False, L=None) -> "RefSetka":
+        L = L or lib(fast)
         return cls(L.gref_setka_new(N1, N2, N3, N4, M1, M2, M3, M4), L, (N1, N2, N3, N4, M1, M2, M3, M4))
 
     @classmethod

@@ -568,3 +568,8 @@ void gref_constants(double* out) {
 }
 
 }  // extern "C"
+
+extern "C" {
+// The reference Setka behind a handle (for the shim test harness).
+Setka* gref_setka_ptr(void* hv) { return static_cast<Handle*>(hv)->S; }
+}

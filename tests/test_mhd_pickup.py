@@ -188,7 +188,8 @@ def test_mhd_graph_matches_direct_launches():
 def test_variant_counts():
     L = N.lib()
     assert L.gelios_variant_count(N.FORM_MHD_PUI) == 6
-    for f in (N.FORM_STATIONARY, N.FORM_MK2, N.FORM_INNER_MK2, N.FORM_5_KOMPONENT):
+    assert L.gelios_variant_count(N.FORM_MK2) == 4
+    for f in (N.FORM_STATIONARY, N.FORM_INNER_MK2, N.FORM_5_KOMPONENT):
         assert L.gelios_variant_count(f) == 1
 
 
@@ -261,3 +262,34 @@ def test_batched_instances_match_one_context_steps():
         assert abs(st[i].dt - sa[i].dt) <= 1e-12 * sa[i].dt
     together.close()
     alone.close()
+
+
+@pytest.mark.gpu
+def test_mk2_launch_shapes_give_same_bits_and_autotune_keeps_state():
+    """The moving-grid face kernel's launch shapes (register caps) give the
+    same bits; autotuning writes only scratch."""
+    mesh = g.Mesh.setka(*MEDIUM)
+    P = N.reference_params()
+    st0 = W.init_conditions_reference(mesh)
+    mc = W.mc_fields(mesh, seed=9)
+
+    def fresh():
+        d = g.Setka(mesh, P)
+        for b in (0, 1):
+            d.set_par(b, st0)
+        d.set_mc(*mc)
+        return d
+
+    ref = fresh()
+    ref.Go_5_komponent__MK2(3)
+    n = N.lib().gelios_variant_count(N.FORM_MK2)
+    for v in range(1, n):
+        d = fresh()
+        d.set_variant(N.FORM_MK2, v)
+        d.Go_5_komponent__MK2(3)
+        assert np.array_equal(d.par(1), ref.par(1)) and np.array_equal(d.points()[0], ref.points()[0]), v
+    d = fresh()
+    v, ms = d.autotune(N.FORM_MK2, reps=2)
+    assert 0 <= v < n and ms > 0.0
+    d.Go_5_komponent__MK2(3)
+    assert np.array_equal(d.par(1), ref.par(1)) and np.array_equal(d.par(0), ref.par(0))
