@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <memory>
@@ -106,7 +107,10 @@ struct gelios_ctx {
     DBuf src_fixed;  // MHD form: fixed charge-exchange sources (3 rows)
     DBuf flux_mhd;   // multi-fluid forms: 13 (MHD) or 21 (Go_5_komponent) flux rows per face slot, on first use
     int mhd_face_variant = 0;  // launch shape of the MHD face kernel (gelios_autotune)
-    int mk2_face_variant = 0;  // launch shape of the moving-grid face kernel (gelios_autotune)
+    int mk2_tile_variant = 0;  // launch shape of the moving-grid tile kernel (gelios_autotune)
+    // tiles of the moving-grid step (see TileView)
+    DBuf t_cstart, t_cells, t_lbase, t_fstart, t_faces;
+    TileView tiles;
     DBuf resid;                // residual partial sums (gelios_residual)
     // streamed host I/O (gelios_run_streamed): copy streams, staging
     // buffers and their events, created on first use
@@ -303,6 +307,146 @@ extern "C" void gelios_destroy(gelios_ctx* ctx) {
     delete ctx;
 }
 
+namespace {
+
+// Tiles of the moving-grid step (TileView): recursive coordinate bisection of
+// the cell centroids in (polar angle, log radius), each axis scaled by the
+// median spacing of face neighbours along it so that a tile spans about as
+// many cells in both directions; splits at multiples of kTileCells so that
+// every tile but the last of a branch is full.  Then, per tile, its cells in
+// index order with their local slot bases, and the face units that touch
+// them (owner side, other side or both).
+struct TileBuild {
+    std::vector<int32_t> cstart, cells, lbase, fstart;
+    std::vector<int2> faces;
+    int max_slots = 0;
+};
+
+int build_tiles(const gelios_mesh_view* v, const std::vector<int32_t>& u_slot, const std::vector<int32_t>& u_cell,
+                const std::vector<int32_t>& u_twin, const std::vector<int32_t>& snb, TileBuild& tb) {
+    const int nc = v->n_cells;
+    std::vector<double> kx(nc), ky(nc);
+    for (int c = 0; c < nc; c++) {
+        // polygon centroid (the tiling needs no exact geometry)
+        double A = 0.0, gx = 0.0, gy = 0.0;
+        const int s0 = v->contour_start[c], n = v->contour_start[c + 1] - s0;
+        for (int i = 0; i < n; i++) {
+            const int a = v->contour[s0 + i], b = v->contour[s0 + (i + 1) % n];
+            const double cr = v->x[a] * v->y[b] - v->y[a] * v->x[b];
+            A += cr;
+            gx += (v->x[a] + v->x[b]) * cr;
+            gy += (v->y[a] + v->y[b]) * cr;
+        }
+        double x = 0.0, y = 0.0;
+        if (A != 0.0) {
+            x = gx / (3.0 * A);
+            y = gy / (3.0 * A);
+        }
+        const double r = std::sqrt(x * x + y * y);
+        kx[c] = std::atan2(y, x);
+        ky[c] = std::log(r > 1e-300 ? r : 1e-300);
+    }
+    // median neighbour spacing along each axis
+    std::vector<double> dth, dlr;
+    for (size_t u = 0; u < u_slot.size(); u++) {
+        if (u_twin[u] < 0) continue;
+        const int a = u_cell[u], b = snb[u_slot[u]];
+        const double t = std::fabs(kx[a] - kx[b]), l = std::fabs(ky[a] - ky[b]);
+        if (t > l)
+            dth.push_back(t);
+        else
+            dlr.push_back(l);
+    }
+    auto median = [](std::vector<double>& w) {
+        if (w.empty()) return 1.0;
+        std::nth_element(w.begin(), w.begin() + w.size() / 2, w.end());
+        const double m = w[w.size() / 2];
+        return m > 0.0 ? m : 1.0;
+    };
+    const double sx = 1.0 / median(dth), sy = 1.0 / median(dlr);
+    for (int c = 0; c < nc; c++) {
+        kx[c] *= sx;
+        ky[c] *= sy;
+    }
+    std::vector<int32_t> perm(nc);
+    for (int c = 0; c < nc; c++) perm[c] = c;
+    std::vector<std::pair<int, int>> stack{{0, nc}}, leaves;
+    while (!stack.empty()) {
+        const std::pair<int, int> range = stack.back();
+        stack.pop_back();
+        const int lo = range.first, hi = range.second, n = hi - lo;
+        if (n <= kTileCells) {
+            if (n > 0) leaves.push_back(range);
+            continue;
+        }
+        double x0 = 1e300, x1 = -1e300, y0 = 1e300, y1 = -1e300;
+        for (int i = lo; i < hi; i++) {
+            const int c = perm[i];
+            x0 = std::min(x0, kx[c]);
+            x1 = std::max(x1, kx[c]);
+            y0 = std::min(y0, ky[c]);
+            y1 = std::max(y1, ky[c]);
+        }
+        const std::vector<double>& key = (x1 - x0 >= y1 - y0) ? kx : ky;
+        const int nt = (n + kTileCells - 1) / kTileCells;
+        const int left = (nt / 2) * kTileCells;
+        std::nth_element(perm.begin() + lo, perm.begin() + lo + left, perm.begin() + hi, [&](int a, int b) {
+            return key[a] < key[b] || (key[a] == key[b] && a < b);
+        });
+        stack.push_back({lo + left, hi});
+        stack.push_back({lo, lo + left});
+    }
+    std::sort(leaves.begin(), leaves.end());
+    const int nt = static_cast<int>(leaves.size());
+    std::vector<int32_t> tile_of(nc), local_of(nc);
+    tb.cstart.assign(1, 0);
+    tb.cells.clear();
+    tb.lbase.clear();
+    tb.max_slots = 0;
+    for (int t = 0; t < nt; t++) {
+        std::sort(perm.begin() + leaves[t].first, perm.begin() + leaves[t].second);
+        int slots = 0;
+        for (int i = leaves[t].first; i < leaves[t].second; i++) {
+            const int c = perm[i];
+            tile_of[c] = t;
+            local_of[c] = slots;
+            tb.cells.push_back(c);
+            tb.lbase.push_back(slots);
+            slots += v->gran_start[c + 1] - v->gran_start[c];
+        }
+        if (slots >= kTileNone) return GELIOS_E_LIMIT;
+        tb.max_slots = std::max(tb.max_slots, slots);
+        tb.cstart.push_back(static_cast<int32_t>(tb.cells.size()));
+    }
+    // face units per tile: by the owner cell's tile, and by the other side's
+    // tile when that differs
+    std::vector<std::vector<int2>> per(nt);
+    for (size_t u = 0; u < u_slot.size(); u++) {
+        const int K = u_cell[u], g = u_slot[u];
+        const int tK = tile_of[K];
+        const int own = local_of[K] + (g - v->gran_start[K]);
+        int tw = kTileNone, tN = -1, other = kTileNone;
+        if (u_twin[u] >= 0) {
+            const int N = snb[g], gt = u_twin[u];
+            tN = tile_of[N];
+            other = local_of[N] + (gt - v->gran_start[N]);
+            if (tN == tK) tw = other;
+        }
+        per[tK].push_back(make_int2(static_cast<int>(u), own | (tw << 16)));
+        if (tN >= 0 && tN != tK) per[tN].push_back(make_int2(static_cast<int>(u), kTileNone | (other << 16)));
+    }
+    tb.fstart.assign(1, 0);
+    tb.faces.clear();
+    for (int t = 0; t < nt; t++) {
+        std::sort(per[t].begin(), per[t].end(), [](const int2& a, const int2& b) { return a.x < b.x; });
+        tb.faces.insert(tb.faces.end(), per[t].begin(), per[t].end());
+        tb.fstart.push_back(static_cast<int32_t>(tb.faces.size()));
+    }
+    return GELIOS_OK;
+}
+
+}  // namespace
+
 extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v) {
     if (!ctx || !v) return GELIOS_E_ARG;
     ctx->drop_graphs();  // they hold the buffers about to be replaced
@@ -462,7 +606,7 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     }
     // CF_RP: cells whose |centroid|^(2 gamma) a moving-grid step reads: the
     // cells of every radially reconstructed unit (its two cells and both
-    // Sosed_down cells, see mk2_recon_kernel) and the masters of the inner
+    // Sosed_down cells, see mk2_recon_unit) and the masters of the inner
     // shock's faces (surface_faces_kernel)
     for (size_t u = 0; u < u_slot.size(); u++) {
         const int g = u_slot[u], K = u_cell[u];
@@ -603,6 +747,16 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     }
     rc |= upload(ctx->u_cell, u_cell.data(), u_cell.size(), s);
     rc |= upload(ctx->u_twin, u_twin.data(), u_twin.size(), s);
+    TileBuild tb;
+    if (build_tiles(v, u_slot, u_cell, u_twin, snb, tb) != GELIOS_OK) {
+        set_error("gelios_upload_topology: a tile of the moving-grid step has too many face slots");
+        return GELIOS_E_LIMIT;
+    }
+    rc |= upload(ctx->t_cstart, tb.cstart.data(), tb.cstart.size(), s);
+    rc |= upload(ctx->t_cells, tb.cells.data(), tb.cells.size(), s);
+    rc |= upload(ctx->t_lbase, tb.lbase.data(), tb.lbase.size(), s);
+    rc |= upload(ctx->t_fstart, tb.fstart.data(), tb.fstart.size(), s);
+    rc |= upload(ctx->t_faces, tb.faces.data(), tb.faces.size(), s);
     rc |= upload<double>(ctx->flux, nullptr, 5 * static_cast<size_t>(ng), s);
     rc |= upload<double>(ctx->upf, nullptr, static_cast<size_t>(kUnitGeoRows) * u_slot.size(), s);
     rc |= upload<double>(ctx->aux, nullptr, 3 * static_cast<size_t>(nc), s);
@@ -723,6 +877,14 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     d.cnext = ctx->cnext.as<int32_t>();
     d.src_lo = chains_ok ? ctx->src_lo.as<int32_t>() : nullptr;
     d.src_lo_out = chains_ok ? ctx->src_lo.as<int32_t>() : nullptr;
+    ctx->tiles = TileView();
+    ctx->tiles.n_tiles = static_cast<int>(tb.cstart.size()) - 1;
+    ctx->tiles.max_slots = tb.max_slots;
+    ctx->tiles.cstart = ctx->t_cstart.as<int32_t>();
+    ctx->tiles.cells = ctx->t_cells.as<int32_t>();
+    ctx->tiles.lbase = ctx->t_lbase.as<int32_t>();
+    ctx->tiles.fstart = ctx->t_fstart.as<int32_t>();
+    ctx->tiles.faces = ctx->t_faces.as<int2>();
     ctx->have_mesh = true;
     ctx->n_inner = 0;
     ctx->cen_valid = false;
@@ -871,8 +1033,9 @@ int enqueue_mk2(gelios_ctx* ctx, const StepBuffers& b) {
     //         terms (none depends on the motion), then, once the rails have
     //         moved, the tracked-face fluxes (sampling of the solved Riemann
     //         problems at the face speed);
-    //   main: surface tracking + rails, reconstruction and flux of every
-    //         other face unit in one kernel, the cell update, the commit.
+    //   main: surface tracking + rails, then (once the side stream is done)
+    //         the tile kernel: reconstruction and flux of every other face
+    //         unit and the cell update; the commit.
     cudaStream_t sd = ctx->side;
     GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_fork, s));
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_fork, 0));
@@ -887,19 +1050,17 @@ int enqueue_mk2(gelios_ctx* ctx, const StepBuffers& b) {
     const int nft = launch_mk2_flux_tracked(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(),
                                             ctx->flux.as<double>(), sd);
     GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_tracked, sd));
-    cudaEvent_t e3 = ctx->phase_begin();
-    const int nfl = launch_mk2_faces(d, P, b, ctx->flux.as<double>(), s, ctx->mk2_face_variant) + nft;
-    ctx->phase_end(1, e3, nfl);
-    // the update reads the tracked-face fluxes and the source terms
+    // the tiles read the tracked-face fluxes and the source terms
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_tracked, 0));
-    cudaEvent_t e5 = ctx->phase_begin();
-    launch_mk2_update(d, P, b, ctx->flux.as<double>(), ctx->aux.as<double>(), s);
-    ctx->phase_end(3, e5, 1);
+    cudaEvent_t e3 = ctx->phase_begin();
+    GELIOS_CUDA_TRY(
+        launch_mk2_tiles(d, P, b, ctx->tiles, ctx->flux.as<double>(), ctx->aux.as<double>(), s, ctx->mk2_tile_variant));
+    ctx->phase_end(1, e3, 1 + nft);  // face units + cell update
     cudaEvent_t e4 = ctx->phase_begin();
     launch_commit(d, b, s);
     ctx->phase_end(4, e4, 1);
     GELIOS_CUDA_TRY(cudaGetLastError());
-    return nm + 4 + nfl + nsv - 1 + (d.u_tr1 > d.u_tr0 ? 1 : 0);
+    return (d.u_tr1 > d.u_tr0 ? 1 : 0) + nsv + 1 + nm + nft + 1 + 1;
 }
 
 // Enqueues one step of the MHD + pickup form on the main stream: Move_surface
@@ -1326,7 +1487,7 @@ extern "C" int gelios_run_streamed(gelios_ctx* ctx, int form, int nsteps, const 
 }
 
 extern "C" int gelios_variant_count(int form) {
-    return form == GELIOS_FORM_MHD_PUI ? kMhdFaceVariants : form == GELIOS_FORM_MK2 ? kMk2FaceVariants : 1;
+    return form == GELIOS_FORM_MHD_PUI ? kMhdFaceVariants : form == GELIOS_FORM_MK2 ? kMk2TileVariants : 1;
 }
 
 extern "C" int gelios_set_variant(gelios_ctx* ctx, int form, int32_t variant) {
@@ -1335,7 +1496,7 @@ extern "C" int gelios_set_variant(gelios_ctx* ctx, int form, int32_t variant) {
         ctx->mhd_face_variant = variant;
         ctx->drop_graphs();  // the captured steps hold the old launch shape
     } else if (form == GELIOS_FORM_MK2) {
-        ctx->mk2_face_variant = variant;
+        ctx->mk2_tile_variant = variant;
         ctx->drop_graphs();
     }
     return GELIOS_OK;
@@ -1398,16 +1559,29 @@ extern "C" int gelios_autotune(gelios_ctx* ctx, int form, int reps, int32_t* var
     GELIOS_CUDA_TRY(cudaEventCreate(&e1));
     int best = 0;
     double best_ms = 0.0;
-    // the face kernel of the form (only scratch and the dt / status words,
-    // reset below, are written)
+    // the moving-grid tile kernel writes a next state and a next geometry
+    // cache: give it scratch (the second cache buffer is free between calls)
+    DBuf scratch;
+    if (!mhd) {
+        if (scratch.alloc(5 * nc * sizeof(double))) return GELIOS_E_CUDA;
+        double* cen1 = ctx->cen[1].as<double>();
+        for (int k = 0; k < 5; k++) b.nxt[k] = scratch.as<double>() + k * nc;
+        b.cx_next = cen1;
+        b.cy_next = cen1 + nc;
+        b.rp_next = cen1 + 2 * nc;
+        b.vs_next = cen1 + 3 * nc;
+        b.vol_next = cen1 + 4 * nc;
+    }
+    // the dominant kernel of the form (only scratch and the dt / status
+    // words, reset below, are written)
     auto faces = [&](int v) {
         if (mhd)
             launch_mhd_faces(d, ctx->prm, ctx->mprm, b, ctx->hstate[0].as<double>(), ctx->flux_mhd.as<double>(), s,
                              v);
         else
-            launch_mk2_faces(d, ctx->prm, b, ctx->flux.as<double>(), s, v);
+            launch_mk2_tiles(d, ctx->prm, b, ctx->tiles, ctx->flux.as<double>(), ctx->aux.as<double>(), s, v);
     };
-    const int nv = mhd ? kMhdFaceVariants : kMk2FaceVariants;
+    const int nv = mhd ? kMhdFaceVariants : kMk2TileVariants;
     for (int v = 0; v < nv; v++) {
         faces(v);
         cudaEventRecord(e0, s);
@@ -1432,7 +1606,7 @@ extern "C" int gelios_autotune(gelios_ctx* ctx, int form, int reps, int32_t* var
     cudaEventDestroy(e1);
     GELIOS_CUDA_TRY(cudaMemcpyAsync(ctx->words.p, &w, sizeof(w), cudaMemcpyHostToDevice, s));
     GELIOS_CUDA_TRY(cudaStreamSynchronize(s));
-    int& current = mhd ? ctx->mhd_face_variant : ctx->mk2_face_variant;
+    int& current = mhd ? ctx->mhd_face_variant : ctx->mk2_tile_variant;
     if (best != current) {
         current = best;
         ctx->drop_graphs();

@@ -1,22 +1,26 @@
 // sm_100a kernels of the Gelios_2D plasma time step.
 //
 // One time step of Setka::Go_5_komponent__MK2 (Setka.cpp:10121-10482) is,
-// on three streams:
-//   mk2_recon_kernel          TVD states of every face unit (pre-motion)
+// on two streams:
+//   mk2_recon_tracked_kernel  TVD states of the tracked face units (pre-motion)
 //   mk2_tracked_solve_kernel  star pressures of the tracked faces' exact
 //                             Riemann problems (warp per face)
 //   mk2_source_kernel         charge-exchange source (Get_Sourse_MK1), four
-//                             lanes per cell; pre-motion areas and volumes
+//                             lanes per cell
 //   surface_faces_kernel      Move_surface (Setka.cpp:3378-3844): exact
 //                             Godunov speeds of the tracked faces (warp per
 //                             face)
 //   rails_kernel              node velocities of the key points, then
 //                             Move_Setka_Calculate_2 (Setka.cpp:4324-4759):
 //                             one CTA per rail
-//   mk2_flux_kernel           face speed from the moved points, HLL fluxes;
-//                             tracked faces sample their Riemann solution
-//   mk2_update_kernel         per-cell flux sums in Grans order, conservative
-//                             ALE update, next-step centroid, CFL block-min
+//   mk2_flux_tracked_kernel   tracked faces: HLL + the Riemann solution
+//                             sampled at the moved face speed
+//   mk2_tile_kernel           one tile of cells per block: reconstruction and
+//                             HLL flux of every other face unit touching the
+//                             tile (face speed from the moved points), slot
+//                             fluxes in shared memory, then the per-cell sums
+//                             in Grans order, the conservative ALE update,
+//                             the next step's geometry cache, CFL block-min
 //   commit_kernel             x = x2; dt of the next step
 // Go_stationary (Setka.cpp:5205-5343) and
 // Go_stationary_5_komponent_inner_MK2 (Setka.cpp:6999-7212) are
@@ -39,9 +43,6 @@ namespace cg = cooperative_groups;
 
 // Minimum resident blocks per SM of the grid-wide moving-grid kernels
 // (register caps: 128 threads x 65536/(128 x minBlocks) registers).
-#ifndef GELIOS_UPDATE_MINB
-#define GELIOS_UPDATE_MINB 6
-#endif
 #ifndef GELIOS_SOURCE_MINB
 #define GELIOS_SOURCE_MINB 1
 #endif
@@ -1072,26 +1073,6 @@ __global__ void __launch_bounds__(32) mk2_flux_tracked_kernel(DevMesh d, gelios_
     block_reduce_commit(tmin_u, 0, 0, status, b.dt_acc, b.counters, b.status);
 }
 
-// Every other face unit after the motion, reconstruction and flux in one
-// pass: the reconstructed states stay in registers (no per-unit scratch).
-// Index i is remapped around the tracked range [u_tr0, u_tr1).
-template <typename TF, int MINB>
-__global__ void __launch_bounds__(128, MINB) mk2_face_kernel(DevMesh d, gelios_params P, StepBuffers b,
-                                                           double* __restrict__ fl, int n_launch) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double tmin_u = __longlong_as_double(0x7ff0000000000000LL);
-    int status = 0;
-    if (i < n_launch) {
-        const int u = i < d.u_tr0 ? i : i + (d.u_tr1 - d.u_tr0);
-        RecUnit r;
-        r.a = St5{};
-        r.o = St5{};
-        mk2_recon_unit(d, P, b, u, r, &status);
-        mk2_flux_unit<TF, false>(d, P, b, u, r, fl, nullptr, tmin_u, &status);
-    }
-    block_reduce_commit(tmin_u, 0, 0, status, b.dt_acc, b.counters, b.status);
-}
-
 // Star pressure of the exact Godunov problem of every tracked-face unit
 // (Solvers.cpp:1174-1305).  It depends on the reconstructed states and on
 // the face normal before the motion, not on the face speed, so it runs on a
@@ -1179,103 +1160,168 @@ __global__ void __launch_bounds__(128, GELIOS_SOURCE_MINB) mk2_source_kernel(Dev
     if (status) atomicOr(b.status, status);
 }
 
-// Go_5_komponent__MK2 cell update (Setka.cpp:10386-10468) from the summed
-// slots.  The area and rotated volume before the motion come from the cache
-// (b.vs, b.vol); the kernel refills the cache for the next step from the
-// moved points: centroid, and area and rotated volume of every cell but the
-// C_centr ones (the points after the commit are these moved points, bit for bit),
+// Go_5_komponent__MK2 cell update (Setka.cpp:10386-10468) of cell c from its
+// face slots' fluxes (fetch(k, j): row k of the cell's j-th slot, Grans
+// order).  The area and rotated volume before the motion come from the cache
+// (b.vs, b.vol); the cache is refilled for the next step from the moved
+// points: centroid, and area and rotated volume of every cell but the C_centr
+// ones (the points after the commit are these moved points, bit for bit),
 // |centroid|^(2 gamma) of the cells flagged CF_RP.  For a quadrilateral
 // Get_Volume and Get_Volume_posle are the same formula; other cells get the
 // Get_Volume form for the cache.
-__global__ void __launch_bounds__(128, GELIOS_UPDATE_MINB) mk2_update_kernel(DevMesh d, gelios_params P, StepBuffers b,
-                                                         const double* __restrict__ fl,
-                                                         const double* __restrict__ aux) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    double tmark = __longlong_as_double(0x7ff0000000000000LL);
-    int nro = 0, npc = 0, status = 0;
-    const size_t ng = d.n_slots;
-    if (c < d.n_cells) {
-        const int s0 = d.cstart[c], n = d.cstart[c + 1] - s0;
-        const int32_t* con = d.contour + s0;
-        double xn, yn;
-        centroid(con, n, d.X2, d.Y2, xn, yn);
-        b.cx_next[c] = xn;
-        b.cy_next[c] = yn;
-        const uint32_t cfl = d.cflags[c];
-        if (cfl & CF_RP) b.rp_next[c] = pow2g(sqrt(sq(xn) + sq(yn)), 2 * P.gamma);
-        const double x = b.cx[c], y = b.cy[c];
-        double vs2 = 0.0, Volume2 = 0.0;
-        if (!(cfl & CF_CENTR)) {
-            vs2 = area(con, n, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X2, d.Y2, true);
-            Volume2 = volume_rotate(con, n, d.X2, d.Y2);
-            b.vs_next[c] = n == 4 ? vs2 : area(con, n, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X2, d.Y2, false);
-            b.vol_next[c] = Volume2;
-        }
-        if (!(sqrt(sq(x) + sq(y)) < P.R11)) {
-            tmark = 10000000.0;  // `time` starts at 1e7 in every step (Setka.cpp:10141)
-            const double dt = *b.dt_cur;
-            const int g0 = d.gstart[c], g1 = d.gstart[c + 1];
-            double Pt0 = 0.0, Pt1 = 0.0, Pt2 = 0.0, Pt3 = 0.0, Pt4 = 0.0;
-            if (g1 - g0 == 4) {  // quadrilaterals: all slot loads in flight together
-                double a[5][4];
+template <typename Fetch>
+__device__ __forceinline__ void mk2_update_cell(const DevMesh& d, const gelios_params& P, const StepBuffers& b, int c,
+                                                Fetch fetch, const double* __restrict__ aux, double& tmark, int& nro,
+                                                int& npc) {
+    const int s0 = d.cstart[c], n = d.cstart[c + 1] - s0;
+    const int32_t* con = d.contour + s0;
+    double xn, yn;
+    centroid(con, n, d.X2, d.Y2, xn, yn);
+    b.cx_next[c] = xn;
+    b.cy_next[c] = yn;
+    const uint32_t cfl = d.cflags[c];
+    if (cfl & CF_RP) b.rp_next[c] = pow2g(sqrt(sq(xn) + sq(yn)), 2 * P.gamma);
+    const double x = b.cx[c], y = b.cy[c];
+    double vs2 = 0.0, Volume2 = 0.0;
+    if (!(cfl & CF_CENTR)) {
+        vs2 = area(con, n, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X2, d.Y2, true);
+        Volume2 = volume_rotate(con, n, d.X2, d.Y2);
+        b.vs_next[c] = n == 4 ? vs2 : area(con, n, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X2, d.Y2, false);
+        b.vol_next[c] = Volume2;
+    }
+    if (sqrt(sq(x) + sq(y)) < P.R11) return;
+    tmark = dmin_ref(tmark, 10000000.0);  // `time` starts at 1e7 in every step (Setka.cpp:10141)
+    const double dt = *b.dt_cur;
+    const int nf = d.gstart[c + 1] - d.gstart[c];
+    double Pt0 = 0.0, Pt1 = 0.0, Pt2 = 0.0, Pt3 = 0.0, Pt4 = 0.0;
+    if (nf == 4) {  // quadrilaterals: all slot loads in flight together
+        double a[5][4];
 #pragma unroll
-                for (int k = 0; k < 5; k++)
+        for (int k = 0; k < 5; k++)
 #pragma unroll
-                    for (int j = 0; j < 4; j++) a[k][j] = fl[k * ng + g0 + j];
-                Pt0 = (((Pt0 + a[0][0]) + a[0][1]) + a[0][2]) + a[0][3];
-                Pt1 = (((Pt1 + a[1][0]) + a[1][1]) + a[1][2]) + a[1][3];
-                Pt2 = (((Pt2 + a[2][0]) + a[2][1]) + a[2][2]) + a[2][3];
-                Pt3 = (((Pt3 + a[3][0]) + a[3][1]) + a[3][2]) + a[3][3];
-                Pt4 = (((Pt4 + a[4][0]) + a[4][1]) + a[4][2]) + a[4][3];
-            } else {
-                for (int g = g0; g < g1; g++) {
-                    Pt0 = Pt0 + fl[0 * ng + g];
-                    Pt1 = Pt1 + fl[1 * ng + g];
-                    Pt2 = Pt2 + fl[2 * ng + g];
-                    Pt3 = Pt3 + fl[3 * ng + g];
-                    Pt4 = Pt4 + fl[4 * ng + g];
-                }
-            }
-            const St5 par1 = load_state(b.cur, c);
-            const size_t nc = d.n_cells;
-            const double q2_1 = aux[0 * nc + c], q2_2 = aux[1 * nc + c], q3 = aux[2 * nc + c];
-            if (!(cfl & CF_CENTR)) {
-                const double vs1 = b.vs[c];
-                const double Volume = b.vol[c];
-                const double ro = par1.ro, u = par1.u, v = par1.v, p = par1.p, Q = par1.Q;
-                const double gm1 = P.gamma - 1;
-                const double rV2 = 1.0 / Volume2, VV = Volume * rV2;
-                double ro3 = ro * VV - dt * (Pt0 * rV2);
-                const double Q33 = Q * VV - (dt * rV2) * Pt4;
-                if (ro3 <= 0.0) {
-                    ro3 = P.ro_floor;
-                    nro = 1;
-                }
-                const double rro3 = 1.0 / ro3;
-                const double u3 = (ro * u * VV - dt * (Pt1 * rV2 - q2_1)) * rro3;
-                const double v3 = (ro * v * VV - dt * ((Pt2 - p * 0.5 * (vs1 + vs2)) * rV2 - q2_2)) * rro3;
-                double p3 = (((p / gm1 + ro * (u * u + v * v) * 0.5) * VV - dt * (Pt3 * rV2 - q3)) -
-                             0.5 * ro3 * (u3 * u3 + v3 * v3)) *
-                            gm1;
-                if (p3 <= 0) {
-                    p3 = P.p_floor;
-                    npc = 1;
-                }
-                b.nxt[0][c] = ro3;
-                b.nxt[1][c] = p3;
-                b.nxt[2][c] = u3;
-                b.nxt[3][c] = v3;
-                b.nxt[4][c] = Q33;
-            } else {
-                b.nxt[0][c] = par1.ro;
-                b.nxt[1][c] = par1.p;
-                b.nxt[2][c] = par1.u;
-                b.nxt[3][c] = par1.v;
-                b.nxt[4][c] = par1.Q;
-            }
+            for (int j = 0; j < 4; j++) a[k][j] = fetch(k, j);
+        Pt0 = (((Pt0 + a[0][0]) + a[0][1]) + a[0][2]) + a[0][3];
+        Pt1 = (((Pt1 + a[1][0]) + a[1][1]) + a[1][2]) + a[1][3];
+        Pt2 = (((Pt2 + a[2][0]) + a[2][1]) + a[2][2]) + a[2][3];
+        Pt3 = (((Pt3 + a[3][0]) + a[3][1]) + a[3][2]) + a[3][3];
+        Pt4 = (((Pt4 + a[4][0]) + a[4][1]) + a[4][2]) + a[4][3];
+    } else {
+        for (int j = 0; j < nf; j++) {
+            Pt0 = Pt0 + fetch(0, j);
+            Pt1 = Pt1 + fetch(1, j);
+            Pt2 = Pt2 + fetch(2, j);
+            Pt3 = Pt3 + fetch(3, j);
+            Pt4 = Pt4 + fetch(4, j);
         }
     }
-    block_reduce_commit(tmark, nro, npc, status, b.dt_acc, b.counters, b.status);
+    const St5 par1 = load_state(b.cur, c);
+    const size_t nc = d.n_cells;
+    const double q2_1 = aux[0 * nc + c], q2_2 = aux[1 * nc + c], q3 = aux[2 * nc + c];
+    if (!(cfl & CF_CENTR)) {
+        const double vs1 = b.vs[c];
+        const double Volume = b.vol[c];
+        const double ro = par1.ro, u = par1.u, v = par1.v, p = par1.p, Q = par1.Q;
+        const double gm1 = P.gamma - 1;
+        const double rV2 = 1.0 / Volume2, VV = Volume * rV2;
+        double ro3 = ro * VV - dt * (Pt0 * rV2);
+        const double Q33 = Q * VV - (dt * rV2) * Pt4;
+        if (ro3 <= 0.0) {
+            ro3 = P.ro_floor;
+            nro++;
+        }
+        const double rro3 = 1.0 / ro3;
+        const double u3 = (ro * u * VV - dt * (Pt1 * rV2 - q2_1)) * rro3;
+        const double v3 = (ro * v * VV - dt * ((Pt2 - p * 0.5 * (vs1 + vs2)) * rV2 - q2_2)) * rro3;
+        double p3 =
+            (((p / gm1 + ro * (u * u + v * v) * 0.5) * VV - dt * (Pt3 * rV2 - q3)) - 0.5 * ro3 * (u3 * u3 + v3 * v3)) *
+            gm1;
+        if (p3 <= 0) {
+            p3 = P.p_floor;
+            npc++;
+        }
+        b.nxt[0][c] = ro3;
+        b.nxt[1][c] = p3;
+        b.nxt[2][c] = u3;
+        b.nxt[3][c] = v3;
+        b.nxt[4][c] = Q33;
+    } else {
+        b.nxt[0][c] = par1.ro;
+        b.nxt[1][c] = par1.p;
+        b.nxt[2][c] = par1.u;
+        b.nxt[3][c] = par1.v;
+        b.nxt[4][c] = par1.Q;
+    }
+}
+
+// The face units and the cell update of the moving-grid step, one tile of
+// cells per block (tiles: spatially compact groups built at upload).  Phase
+// 1: every face unit that touches the tile's cells, reconstruction and flux
+// in registers, F.S (owner side) / -F.S (other side) into the tile-local
+// slots in shared memory; a unit whose two cells lie in different tiles is
+// evaluated by both (same inputs, same code: the same bits on both sides).
+// Tracked units take the fluxes the tracked-face kernel left in `fl`.
+// Phase 2: the update of every cell of the tile from its slots.  No flux
+// leaves the SM.  The CFL candidate of a side is taken by the tile that holds
+// that side's cell, so each is taken once.
+template <typename TF, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) mk2_tile_kernel(DevMesh d, gelios_params P, StepBuffers b, TileView t,
+                                                           const double* __restrict__ fl,
+                                                           const double* __restrict__ aux) {
+    extern __shared__ double sfl[];  // 5 rows of t.max_slots
+    const int tile = blockIdx.x;
+    const int ms = t.max_slots;
+    const size_t ng = d.n_slots;
+    double tmin = __longlong_as_double(0x7ff0000000000000LL);
+    int nro = 0, npc = 0, status = 0;
+    const int f0 = t.fstart[tile], f1 = t.fstart[tile + 1];
+    for (int j = f0 + threadIdx.x; j < f1; j += NT) {
+        const int2 rec = t.faces[j];
+        const int u = rec.x;
+        const int own = rec.y & 0xffff, tw = (rec.y >> 16) & 0xffff;
+        if (u >= d.u_tr0 && u < d.u_tr1) {
+            const int g = d.u_slot[u], gt = d.u_twin[u];
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+                if (own != kTileNone) sfl[k * ms + own] = fl[k * ng + g];
+                if (tw != kTileNone) sfl[k * ms + tw] = fl[k * ng + gt];
+            }
+            continue;
+        }
+        RecUnit r;
+        r.a = St5{};
+        r.o = St5{};
+        mk2_recon_unit(d, P, b, u, r, &status);
+        const bool procK = !(r.dist < 0.0), procN = !(r.distn < 0.0);
+        if (!(procK || procN)) continue;
+        const double dt = *b.dt_cur;
+        const uint32_t info = d.u_info[u];
+        const int A = d.u_A[u], B = d.u_B[u];
+        const double x4 = (d.X2[A] + d.X2[B]) / 2.0, y4 = (d.Y2[A] + d.Y2[B]) / 2.0;
+        const double W = ((x4 - r.x2) * r.n1 + (y4 - r.y2) * r.n2) / dt;
+        const bool np = (info & SI_NP) != 0;
+        FluxOut<double> F;
+        const double UU = hllc_flux<TF>(P.gamma, P.kurant, r.a, r.o, W, r.n1, r.n2, 1.0, 0, np, F);
+        const double S = r.S;
+        const double fm[5] = {F.P0 * S, F.P1 * S, F.P2 * S, F.P3 * S, F.PQ * S};
+        if (own != kTileNone) {
+#pragma unroll
+            for (int k = 0; k < 5; k++) sfl[k * ms + own] = fm[k];
+            if (procK) tmin = dmin_ref(tmin, P.kurant * r.dist / UU);
+        }
+        if (tw != kTileNone) {
+#pragma unroll
+            for (int k = 0; k < 5; k++) sfl[k * ms + tw] = -fm[k];
+            if (procN) tmin = dmin_ref(tmin, P.kurant * r.distn / UU);
+        }
+    }
+    __syncthreads();
+    const int c0 = t.cstart[tile], c1 = t.cstart[tile + 1];
+    for (int i = c0 + threadIdx.x; i < c1; i += NT) {
+        const int c = t.cells[i];
+        const int base = t.lbase[i];
+        mk2_update_cell(d, P, b, c, [&](int k, int jj) { return sfl[k * ms + base + jj]; }, aux, tmin, nro, npc);
+    }
+    block_reduce_commit(tmin, nro, npc, status, b.dt_acc, b.counters, b.status);
 }
 
 // Go_stationary_5_komponent_inner_MK2 cell update (Setka.cpp:7021-7210).
@@ -2405,7 +2451,7 @@ __global__ void __launch_bounds__(128) k5_update_kernel(DevMesh d, gelios_params
     int nro = 0, npc = 0, status = 0;
     const size_t nc = d.n_cells;
     if (c < d.n_cells) {
-        {  // the next step's geometry cache from the moved points (see mk2_update_kernel)
+        {  // the next step's geometry cache from the moved points (see mk2_update_cell)
             const int s0 = d.cstart[c], n = d.cstart[c + 1] - s0;
             const int32_t* con = d.contour + s0;
             double xn, yn;
@@ -2838,7 +2884,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) mhd_face_kernel(DevMesh d, gelios
 // Cell update of the MHD form: the MK2 update (Setka.cpp:10386-10468) for
 // both fluids with their axisymmetric terms (area-weighted like the
 // reference's p (vs1 + vs2)/2) and the fixed charge-exchange sources of the
-// ion momentum and energy; refills the geometry cache like mk2_update_kernel.
+// ion momentum and energy; refills the geometry cache like mk2_update_cell.
 __device__ __forceinline__ void mhd_update_body(const DevMesh& d, const gelios_params& P, const StepBuffers& b,
                                                 const double* __restrict__ fl, const double* __restrict__ src,
                                                 const double* __restrict__ hcur, double* __restrict__ hnxt, int c,
@@ -3225,31 +3271,39 @@ void launch_mk2_recon(const DevMesh& d, const gelios_params& P, const StepBuffer
     const int nt = d.u_tr1 - d.u_tr0;
     if (nt > 0) mk2_recon_tracked_kernel<<<blocks_for(nt, 128), 128, 0, s>>>(d, P, b, rec);
 }
-template <int MINB>
-static void launch_mk2_faces_v(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl, int nr,
-                               cudaStream_t s) {
-    if (P.precision == GELIOS_PREC_FP32_FLUX)
-        mk2_face_kernel<float, MINB><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, b, fl, nr);
-    else
-        mk2_face_kernel<double, MINB><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, b, fl, nr);
-}
-// variant v: minimum resident blocks of 128 threads per SM (a register cap):
-// 5, 4, 6, 8
-const char* mk2_face_variant_name(int v) {
-    static const char* names[kMk2FaceVariants] = {"128x5", "128x4", "128x6", "128x8"};
-    return (v >= 0 && v < kMk2FaceVariants) ? names[v] : "?";
-}
-int launch_mk2_faces(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl, cudaStream_t s,
-                     int variant) {
-    const int nr = d.n_units - (d.u_tr1 - d.u_tr0);
-    if (nr <= 0) return 0;
-    switch (variant) {
-        case 1: launch_mk2_faces_v<4>(d, P, b, fl, nr, s); break;
-        case 2: launch_mk2_faces_v<6>(d, P, b, fl, nr, s); break;
-        case 3: launch_mk2_faces_v<8>(d, P, b, fl, nr, s); break;
-        default: launch_mk2_faces_v<5>(d, P, b, fl, nr, s); break;
+// variant v of the tile kernel: threads per block x minimum resident blocks
+// per SM (a register cap)
+template <typename TF, int NT, int MINB>
+static cudaError_t launch_tiles_v(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const TileView& t,
+                                  const double* fl, const double* aux, cudaStream_t s) {
+    const size_t smem = 5ull * static_cast<size_t>(t.max_slots) * sizeof(double);
+    if (smem > 48 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(mk2_tile_kernel<TF, NT, MINB>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
     }
-    return 1;
+    mk2_tile_kernel<TF, NT, MINB><<<t.n_tiles, NT, smem, s>>>(d, P, b, t, fl, aux);
+    return cudaGetLastError();
+}
+template <typename TF>
+static cudaError_t launch_tiles_p(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const TileView& t,
+                                  const double* fl, const double* aux, cudaStream_t s, int variant) {
+    switch (variant) {
+        case 1: return launch_tiles_v<TF, 128, 4>(d, P, b, t, fl, aux, s);
+        case 2: return launch_tiles_v<TF, 256, 3>(d, P, b, t, fl, aux, s);
+        case 3: return launch_tiles_v<TF, 128, 5>(d, P, b, t, fl, aux, s);
+        default: return launch_tiles_v<TF, 256, 2>(d, P, b, t, fl, aux, s);
+    }
+}
+const char* mk2_tile_variant_name(int v) {
+    static const char* names[kMk2TileVariants] = {"256x2", "128x4", "256x3", "128x5"};
+    return (v >= 0 && v < kMk2TileVariants) ? names[v] : "?";
+}
+cudaError_t launch_mk2_tiles(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const TileView& t,
+                             const double* fl, const double* aux, cudaStream_t s, int variant) {
+    if (t.n_tiles <= 0) return cudaSuccess;
+    if (P.precision == GELIOS_PREC_FP32_FLUX) return launch_tiles_p<float>(d, P, b, t, fl, aux, s, variant);
+    return launch_tiles_p<double>(d, P, b, t, fl, aux, s, variant);
 }
 int launch_mk2_tracked_solve(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
                              double* pstar, cudaStream_t s) {
@@ -3267,10 +3321,6 @@ int launch_mk2_flux_tracked(const DevMesh& d, const gelios_params& P, const Step
     else
         mk2_flux_tracked_kernel<double><<<blocks_for(nt, 32), 32, 0, s>>>(d, P, b, rec, fl, pstar);
     return 1;
-}
-void launch_mk2_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
-                       const double* aux, cudaStream_t s) {
-    mk2_update_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, fl, aux);
 }
 void launch_mk2_source(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* aux, cudaStream_t s) {
     mk2_source_kernel<<<blocks_for(4 * d.n_cells, 128), 128, 0, s>>>(d, P, b, aux);

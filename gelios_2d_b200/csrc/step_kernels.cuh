@@ -137,23 +137,39 @@ struct PlainInstance {
 cudaError_t launch_stationary_batch(const DevMesh& d, const PlainInstance* inst, const int* active, int n_active,
                                     int nsteps, bool fp32, cudaStream_t s);
 void launch_plain_batch_words_init(const PlainInstance* inst, const int* active, int n, cudaStream_t s);
+// Tiles of the moving-grid step, built at topology upload: spatially compact
+// groups of at most kTileCells cells.  Cells of tile t are
+// cells[cstart[t] .. cstart[t+1]); the j-th face slot (Grans order) of
+// cells[i] is tile-local slot lbase[i] + j.  faces[fstart[t] .. fstart[t+1])
+// are the face units that touch the tile's cells, in unit order: (unit,
+// owner's local slot | other side's local slot << 16), kTileNone where that
+// side's cell lies in another tile (or there is no other side).
+constexpr int kTileCells = 256;
+constexpr int kTileNone = 0xffff;
+struct TileView {
+    int n_tiles = 0, max_slots = 0;
+    const int32_t* cstart = nullptr;
+    const int32_t* cells = nullptr;
+    const int32_t* lbase = nullptr;
+    const int32_t* fstart = nullptr;
+    const int2* faces = nullptr;
+};
 // Moving-grid step: reconstruction of the tracked units before the motion
-// (rec: kRecRows x n_tracked), reconstruction + flux of every other unit after
-// it (mk2_face_kernel, no scratch but the flux slots).
+// (rec: kRecRows x n_tracked), then one kernel for every other unit and the
+// cell update (mk2_tile_kernel: reconstruction and flux in registers, slot
+// fluxes in shared memory).  The tile kernel has kMk2TileVariants launch
+// shapes (threads per block x resident blocks per SM); variant 0 is the
+// default, gelios_autotune picks the fastest for a grid.  All shapes give the
+// same bits.
 void launch_mk2_recon(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* rec, cudaStream_t s);
-// The face kernel has kMk2FaceVariants launch shapes (resident blocks of 128
-// threads per SM); variant 0 is the default, gelios_autotune picks the
-// fastest for a grid.  All shapes give the same bits.
-constexpr int kMk2FaceVariants = 4;
-const char* mk2_face_variant_name(int v);
-int launch_mk2_faces(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl, cudaStream_t s,
-                     int variant = 0);
+constexpr int kMk2TileVariants = 4;
+const char* mk2_tile_variant_name(int v);
+cudaError_t launch_mk2_tiles(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const TileView& t,
+                             const double* fl, const double* aux, cudaStream_t s, int variant = 0);
 int launch_mk2_tracked_solve(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
                              double* pstar, cudaStream_t s);
 int launch_mk2_flux_tracked(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
                             const double* pstar, double* fl, cudaStream_t s);
-void launch_mk2_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
-                       const double* aux, cudaStream_t s);
 void launch_mk2_source(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* aux, cudaStream_t s);
 void launch_inner(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const int32_t* list, int n,
                   cudaStream_t s);
