@@ -107,7 +107,8 @@ struct gelios_ctx {
     DBuf src_fixed;  // MHD form: fixed charge-exchange sources (3 rows)
     DBuf flux_mhd;   // multi-fluid forms: 13 (MHD) or 21 (Go_5_komponent) flux rows per face slot, on first use
     int mhd_face_variant = 0;  // launch shape of the MHD face kernel (gelios_autotune)
-    int mk2_tile_variant = 0;  // launch shape of the moving-grid tile kernel (gelios_autotune)
+    int mk2_variant = 0;  // arrangement / launch shape of the moving-grid face units + update (gelios_autotune)
+    int mk2_source_variant = 0;  // arrangement of the moving-grid source kernel (gelios_autotune)
     // tiles of the moving-grid step (see TileView)
     DBuf t_cstart, t_cells, t_lbase, t_fstart, t_faces;
     TileView tiles;
@@ -1041,7 +1042,7 @@ int enqueue_mk2(gelios_ctx* ctx, const StepBuffers& b) {
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_fork, 0));
     launch_mk2_recon(d, P, b, ctx->rec.as<double>(), sd);
     const int nsv = launch_mk2_tracked_solve(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(), sd);
-    launch_mk2_source(d, P, b, ctx->aux.as<double>(), sd);
+    launch_mk2_source(d, P, b, ctx->aux.as<double>(), sd, ctx->mk2_source_variant);
     cudaEvent_t e1 = ctx->phase_begin();
     const int nm = launch_motion(d, P, b, ctx->surface.as<double>(), s);
     ctx->phase_end(2, e1, nm);  // Move_surface + rails
@@ -1054,13 +1055,14 @@ int enqueue_mk2(gelios_ctx* ctx, const StepBuffers& b) {
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_tracked, 0));
     cudaEvent_t e3 = ctx->phase_begin();
     GELIOS_CUDA_TRY(
-        launch_mk2_tiles(d, P, b, ctx->tiles, ctx->flux.as<double>(), ctx->aux.as<double>(), s, ctx->mk2_tile_variant));
-    ctx->phase_end(1, e3, 1 + nft);  // face units + cell update
+        launch_mk2_cells(d, P, b, ctx->tiles, ctx->flux.as<double>(), ctx->aux.as<double>(), s, ctx->mk2_variant));
+    const int ncl = mk2_variant_launches(ctx->mk2_variant);
+    ctx->phase_end(1, e3, ncl + nft);  // face units + cell update
     cudaEvent_t e4 = ctx->phase_begin();
     launch_commit(d, b, s);
     ctx->phase_end(4, e4, 1);
     GELIOS_CUDA_TRY(cudaGetLastError());
-    return (d.u_tr1 > d.u_tr0 ? 1 : 0) + nsv + 1 + nm + nft + 1 + 1;
+    return (d.u_tr1 > d.u_tr0 ? 1 : 0) + nsv + 1 + nm + nft + ncl + 1;
 }
 
 // Enqueues one step of the MHD + pickup form on the main stream: Move_surface
@@ -1487,7 +1489,7 @@ extern "C" int gelios_run_streamed(gelios_ctx* ctx, int form, int nsteps, const 
 }
 
 extern "C" int gelios_variant_count(int form) {
-    return form == GELIOS_FORM_MHD_PUI ? kMhdFaceVariants : form == GELIOS_FORM_MK2 ? kMk2TileVariants : 1;
+    return form == GELIOS_FORM_MHD_PUI ? kMhdFaceVariants : form == GELIOS_FORM_MK2 ? kMk2Variants : 1;
 }
 
 extern "C" int gelios_set_variant(gelios_ctx* ctx, int form, int32_t variant) {
@@ -1496,7 +1498,7 @@ extern "C" int gelios_set_variant(gelios_ctx* ctx, int form, int32_t variant) {
         ctx->mhd_face_variant = variant;
         ctx->drop_graphs();  // the captured steps hold the old launch shape
     } else if (form == GELIOS_FORM_MK2) {
-        ctx->mk2_tile_variant = variant;
+        ctx->mk2_variant = variant;
         ctx->drop_graphs();
     }
     return GELIOS_OK;
@@ -1559,8 +1561,8 @@ extern "C" int gelios_autotune(gelios_ctx* ctx, int form, int reps, int32_t* var
     GELIOS_CUDA_TRY(cudaEventCreate(&e1));
     int best = 0;
     double best_ms = 0.0;
-    // the moving-grid tile kernel writes a next state and a next geometry
-    // cache: give it scratch (the second cache buffer is free between calls)
+    // the moving-grid update writes a next state and a next geometry cache:
+    // give it scratch (the second cache buffer is free between calls)
     DBuf scratch;
     if (!mhd) {
         if (scratch.alloc(5 * nc * sizeof(double))) return GELIOS_E_CUDA;
@@ -1579,34 +1581,60 @@ extern "C" int gelios_autotune(gelios_ctx* ctx, int form, int reps, int32_t* var
             launch_mhd_faces(d, ctx->prm, ctx->mprm, b, ctx->hstate[0].as<double>(), ctx->flux_mhd.as<double>(), s,
                              v);
         else
-            launch_mk2_tiles(d, ctx->prm, b, ctx->tiles, ctx->flux.as<double>(), ctx->aux.as<double>(), s, v);
+            launch_mk2_cells(d, ctx->prm, b, ctx->tiles, ctx->flux.as<double>(), ctx->aux.as<double>(), s, v);
     };
-    const int nv = mhd ? kMhdFaceVariants : kMk2TileVariants;
-    for (int v = 0; v < nv; v++) {
-        faces(v);
+    // mean ms of `reps` launches of fn(v) after one untimed launch
+    auto time_ms = [&](auto fn, int v, double& out) -> cudaError_t {
+        fn(v);
         cudaEventRecord(e0, s);
-        for (int r = 0; r < reps; r++) faces(v);
+        for (int r = 0; r < reps; r++) fn(v);
         cudaEventRecord(e1, s);
         cudaError_t err = cudaEventSynchronize(e1);
         float t = 0.f;
         if (err == cudaSuccess) err = cudaEventElapsedTime(&t, e0, e1);
-        if (err != cudaSuccess) {
-            cudaEventDestroy(e0);
-            cudaEventDestroy(e1);
-            set_error(std::string("gelios_autotune: ") + cudaGetErrorString(err));
-            return GELIOS_E_CUDA;
-        }
-        const double m = static_cast<double>(t) / reps;
+        out = static_cast<double>(t) / reps;
+        return err;
+    };
+    const int nv = mhd ? kMhdFaceVariants : kMk2Variants;
+    cudaError_t err = cudaSuccess;
+    for (int v = 0; v < nv && err == cudaSuccess; v++) {
+        double m = 0.0;
+        err = time_ms(faces, v, m);
         if (v == 0 || m < best_ms) {
             best = v;
             best_ms = m;
         }
     }
+    // the moving-grid form also picks the arrangement of its source kernel
+    // (writes only the source rows and the bracket hints)
+    int best_src = 0;
+    if (!mhd) {
+        double src_best = 0.0;
+        auto src = [&](int v) { launch_mk2_source(d, ctx->prm, b, ctx->aux.as<double>(), s, v); };
+        for (int v = 0; v < kMk2SourceVariants && err == cudaSuccess; v++) {
+            double m = 0.0;
+            err = time_ms(src, v, m);
+            if (v == 0 || m < src_best) {
+                best_src = v;
+                src_best = m;
+            }
+        }
+    }
+    if (err != cudaSuccess) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        set_error(std::string("gelios_autotune: ") + cudaGetErrorString(err));
+        return GELIOS_E_CUDA;
+    }
+    if (!mhd && best_src != ctx->mk2_source_variant) {
+        ctx->mk2_source_variant = best_src;
+        ctx->drop_graphs();
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     GELIOS_CUDA_TRY(cudaMemcpyAsync(ctx->words.p, &w, sizeof(w), cudaMemcpyHostToDevice, s));
     GELIOS_CUDA_TRY(cudaStreamSynchronize(s));
-    int& current = mhd ? ctx->mhd_face_variant : ctx->mk2_tile_variant;
+    int& current = mhd ? ctx->mhd_face_variant : ctx->mk2_variant;
     if (best != current) {
         current = best;
         ctx->drop_graphs();

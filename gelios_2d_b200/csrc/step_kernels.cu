@@ -1073,6 +1073,27 @@ __global__ void __launch_bounds__(32) mk2_flux_tracked_kernel(DevMesh d, gelios_
     block_reduce_commit(tmin_u, 0, 0, status, b.dt_acc, b.counters, b.status);
 }
 
+// Every other face unit after the motion, reconstruction and flux in one
+// pass: the reconstructed states stay in registers (no per-unit scratch);
+// F.S to the owner's flux slot and -F.S to the twin's.  Index i is remapped
+// around the tracked range [u_tr0, u_tr1).
+template <typename TF, int MINB>
+__global__ void __launch_bounds__(128, MINB) mk2_face_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                           double* __restrict__ fl, int n_launch) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double tmin_u = __longlong_as_double(0x7ff0000000000000LL);
+    int status = 0;
+    if (i < n_launch) {
+        const int u = i < d.u_tr0 ? i : i + (d.u_tr1 - d.u_tr0);
+        RecUnit r;
+        r.a = St5{};
+        r.o = St5{};
+        mk2_recon_unit(d, P, b, u, r, &status);
+        mk2_flux_unit<TF, false>(d, P, b, u, r, fl, nullptr, tmin_u, &status);
+    }
+    block_reduce_commit(tmin_u, 0, 0, status, b.dt_acc, b.counters, b.status);
+}
+
 // Star pressure of the exact Godunov problem of every tracked-face unit
 // (Solvers.cpp:1174-1305).  It depends on the reconstructed states and on
 // the face normal before the motion, not on the face speed, so it runs on a
@@ -1156,6 +1177,29 @@ __global__ void __launch_bounds__(128, GELIOS_SOURCE_MINB) mk2_source_kernel(Dev
         aux[0 * n + c] = q1;
         aux[1 * n + c] = q2;
         aux[2 * n + c] = q3;
+    }
+    if (status) atomicOr(b.status, status);
+}
+
+// The same source terms with one thread per cell and the four species in turn
+// (source_mk1, as the inner form evaluates them): one bracket search and one
+// set of k_u, k_v, k_T per cell instead of four, more independent loads per
+// thread, a quarter of the threads.  Same sums in the same order, same bits.
+__global__ void __launch_bounds__(128) mk2_source_cell_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                              double* __restrict__ aux) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    int status = 0;
+    if (c < d.n_cells) {
+        const double x = b.cx[c], y = b.cy[c];
+        if (!(sqrt(sq(x) + sq(y)) < P.R11)) {
+            const St5 par1 = load_state(b.cur, c);
+            double q1 = 0.0, q2 = 0.0, q3 = 0.0;
+            source_mk1(d, P, c, x, y, par1.u, par1.v, par1.ro, par1.p, q1, q2, q3, &status);
+            const size_t n = d.n_cells;
+            aux[0 * n + c] = q1;
+            aux[1 * n + c] = q2;
+            aux[2 * n + c] = q3;
+        }
     }
     if (status) atomicOr(b.status, status);
 }
@@ -1322,6 +1366,22 @@ __global__ void __launch_bounds__(NT, MINB) mk2_tile_kernel(DevMesh d, gelios_pa
         mk2_update_cell(d, P, b, c, [&](int k, int jj) { return sfl[k * ms + base + jj]; }, aux, tmin, nro, npc);
     }
     block_reduce_commit(tmin, nro, npc, status, b.dt_acc, b.counters, b.status);
+}
+
+// The cell update alone, from the flux slots in global memory (the update
+// phase of the tile kernel for the face-kernel arrangement).
+__global__ void __launch_bounds__(128, 6) mk2_update_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                          const double* __restrict__ fl,
+                                                          const double* __restrict__ aux) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double tmark = __longlong_as_double(0x7ff0000000000000LL);
+    int nro = 0, npc = 0;
+    const size_t ng = d.n_slots;
+    if (c < d.n_cells) {
+        const int g0 = d.gstart[c];
+        mk2_update_cell(d, P, b, c, [&](int k, int j) { return fl[k * ng + g0 + j]; }, aux, tmark, nro, npc);
+    }
+    block_reduce_commit(tmark, nro, npc, 0, b.dt_acc, b.counters, b.status);
 }
 
 // Go_stationary_5_komponent_inner_MK2 cell update (Setka.cpp:7021-7210).
@@ -3285,25 +3345,40 @@ static cudaError_t launch_tiles_v(const DevMesh& d, const gelios_params& P, cons
     mk2_tile_kernel<TF, NT, MINB><<<t.n_tiles, NT, smem, s>>>(d, P, b, t, fl, aux);
     return cudaGetLastError();
 }
+template <typename TF, int MINB>
+static cudaError_t launch_faces_v(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
+                                  const double* aux, cudaStream_t s) {
+    const int nr = d.n_units - (d.u_tr1 - d.u_tr0);
+    if (nr > 0) mk2_face_kernel<TF, MINB><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, b, fl, nr);
+    mk2_update_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, fl, aux);
+    return cudaGetLastError();
+}
 template <typename TF>
-static cudaError_t launch_tiles_p(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const TileView& t,
-                                  const double* fl, const double* aux, cudaStream_t s, int variant) {
+static cudaError_t launch_cells_p(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const TileView& t,
+                                  double* fl, const double* aux, cudaStream_t s, int variant) {
     switch (variant) {
-        case 1: return launch_tiles_v<TF, 128, 4>(d, P, b, t, fl, aux, s);
-        case 2: return launch_tiles_v<TF, 256, 3>(d, P, b, t, fl, aux, s);
-        case 3: return launch_tiles_v<TF, 128, 5>(d, P, b, t, fl, aux, s);
-        default: return launch_tiles_v<TF, 256, 2>(d, P, b, t, fl, aux, s);
+        case 1: return launch_faces_v<TF, 5>(d, P, b, fl, aux, s);
+        case 2: return launch_faces_v<TF, 6>(d, P, b, fl, aux, s);
+        case 3: return launch_faces_v<TF, 4>(d, P, b, fl, aux, s);
+        case 4: return launch_tiles_v<TF, 256, 3>(d, P, b, t, fl, aux, s);
+        case 5: return launch_tiles_v<TF, 256, 2>(d, P, b, t, fl, aux, s);
+        case 6: return launch_tiles_v<TF, 128, 5>(d, P, b, t, fl, aux, s);
+        case 7: return launch_tiles_v<TF, 128, 4>(d, P, b, t, fl, aux, s);
+        default: return launch_faces_v<TF, 8>(d, P, b, fl, aux, s);
     }
 }
-const char* mk2_tile_variant_name(int v) {
-    static const char* names[kMk2TileVariants] = {"256x2", "128x4", "256x3", "128x5"};
-    return (v >= 0 && v < kMk2TileVariants) ? names[v] : "?";
+const char* mk2_variant_name(int v) {
+    static const char* names[kMk2Variants] = {"faces 128x8 + update", "faces 128x5 + update",
+                                              "faces 128x6 + update", "faces 128x4 + update",
+                                              "tiles 256x3",          "tiles 256x2",
+                                              "tiles 128x5",          "tiles 128x4"};
+    return (v >= 0 && v < kMk2Variants) ? names[v] : "?";
 }
-cudaError_t launch_mk2_tiles(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const TileView& t,
-                             const double* fl, const double* aux, cudaStream_t s, int variant) {
-    if (t.n_tiles <= 0) return cudaSuccess;
-    if (P.precision == GELIOS_PREC_FP32_FLUX) return launch_tiles_p<float>(d, P, b, t, fl, aux, s, variant);
-    return launch_tiles_p<double>(d, P, b, t, fl, aux, s, variant);
+int mk2_variant_launches(int v) { return v >= 4 ? 1 : 2; }
+cudaError_t launch_mk2_cells(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const TileView& t,
+                             double* fl, const double* aux, cudaStream_t s, int variant) {
+    if (P.precision == GELIOS_PREC_FP32_FLUX) return launch_cells_p<float>(d, P, b, t, fl, aux, s, variant);
+    return launch_cells_p<double>(d, P, b, t, fl, aux, s, variant);
 }
 int launch_mk2_tracked_solve(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
                              double* pstar, cudaStream_t s) {
@@ -3322,8 +3397,12 @@ int launch_mk2_flux_tracked(const DevMesh& d, const gelios_params& P, const Step
         mk2_flux_tracked_kernel<double><<<blocks_for(nt, 32), 32, 0, s>>>(d, P, b, rec, fl, pstar);
     return 1;
 }
-void launch_mk2_source(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* aux, cudaStream_t s) {
-    mk2_source_kernel<<<blocks_for(4 * d.n_cells, 128), 128, 0, s>>>(d, P, b, aux);
+void launch_mk2_source(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* aux, cudaStream_t s,
+                       int variant) {
+    if (variant == 1)
+        mk2_source_cell_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, aux);
+    else
+        mk2_source_kernel<<<blocks_for(4 * d.n_cells, 128), 128, 0, s>>>(d, P, b, aux);
 }
 void launch_inner(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const int32_t* list, int n,
                   cudaStream_t s) {

@@ -155,22 +155,31 @@ struct TileView {
     const int2* faces = nullptr;
 };
 // Moving-grid step: reconstruction of the tracked units before the motion
-// (rec: kRecRows x n_tracked), then one kernel for every other unit and the
-// cell update (mk2_tile_kernel: reconstruction and flux in registers, slot
-// fluxes in shared memory).  The tile kernel has kMk2TileVariants launch
-// shapes (threads per block x resident blocks per SM); variant 0 is the
-// default, gelios_autotune picks the fastest for a grid.  All shapes give the
-// same bits.
+// (rec: kRecRows x n_tracked); after it, every other face unit and the cell
+// update in one of two arrangements, kMk2Variants launch shapes in all:
+//   variants 0-3  mk2_face_kernel (reconstruction and flux in registers, F.S
+//                 to the flux slots in global memory; 128 threads x 8, 5, 6,
+//                 4 resident blocks) + mk2_update_kernel (slot sums, update);
+//   variants 4-7  mk2_tile_kernel, one tile of cells per block, slot fluxes
+//                 in shared memory (256 x 3, 256 x 2, 128 x 5, 128 x 4).
+// Variant 0 is the default; gelios_autotune picks the fastest for a grid.
+// All give the same bits.
 void launch_mk2_recon(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* rec, cudaStream_t s);
-constexpr int kMk2TileVariants = 4;
-const char* mk2_tile_variant_name(int v);
-cudaError_t launch_mk2_tiles(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const TileView& t,
-                             const double* fl, const double* aux, cudaStream_t s, int variant = 0);
+constexpr int kMk2Variants = 8;
+const char* mk2_variant_name(int v);
+int mk2_variant_launches(int v);
+cudaError_t launch_mk2_cells(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const TileView& t,
+                             double* fl, const double* aux, cudaStream_t s, int variant = 0);
 int launch_mk2_tracked_solve(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
                              double* pstar, cudaStream_t s);
 int launch_mk2_flux_tracked(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
                             const double* pstar, double* fl, cudaStream_t s);
-void launch_mk2_source(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* aux, cudaStream_t s);
+// Charge-exchange source terms of the moving-grid step (aux rows q1, q2, q3):
+// variant 0 four lanes per cell (one hydrogen species each), variant 1 one
+// thread per cell; same bits.  gelios_autotune picks the faster for a grid.
+constexpr int kMk2SourceVariants = 2;
+void launch_mk2_source(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* aux, cudaStream_t s,
+                       int variant = 0);
 void launch_inner(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const int32_t* list, int n,
                   cudaStream_t s);
 void launch_dt_finalize(const StepBuffers& b, cudaStream_t s);

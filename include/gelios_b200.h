@@ -345,10 +345,16 @@ int gelios_mlp_gemm_bf16(int M, int N, int K, const void *A, int64_t lda, const 
                          int64_t ldc, void *stream);
 
 /* ---- autotuning of launch shapes (no counterpart in the reference) ---------
- * The dominant kernel of the MHD form and of the moving-grid form
- * (GELIOS_FORM_MK2; their face kernels) has gelios_variant_count(form)
- * launch shapes (threads per block x resident blocks per SM, i.e. a register
- * cap); all give the same bits.
+ * The dominant kernel of the MHD form (its face kernel) has
+ * gelios_variant_count(form) launch shapes (threads per block x resident
+ * blocks per SM, i.e. a register cap); the moving-grid form
+ * (GELIOS_FORM_MK2) has as many variants of its face units + cell update:
+ * a face kernel writing flux slots in global memory followed by an update
+ * kernel, or one kernel per tile of cells with the slots in shared memory,
+ * each in several launch shapes.  All give the same bits.  For
+ * the moving-grid form gelios_autotune also picks the faster of two
+ * arrangements of the source-term kernel (four lanes or one thread per cell;
+ * same bits).
  * gelios_autotune times each shape on the context's grid and current state
  * (`reps` launches each, CUDA events on the context stream; only scratch
  * buffers are written, the state and the points are not touched), keeps the

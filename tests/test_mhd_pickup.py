@@ -188,7 +188,7 @@ def test_mhd_graph_matches_direct_launches():
 def test_variant_counts():
     L = N.lib()
     assert L.gelios_variant_count(N.FORM_MHD_PUI) == 6
-    assert L.gelios_variant_count(N.FORM_MK2) == 4
+    assert L.gelios_variant_count(N.FORM_MK2) == 8
     for f in (N.FORM_STATIONARY, N.FORM_INNER_MK2, N.FORM_5_KOMPONENT):
         assert L.gelios_variant_count(f) == 1
 
@@ -266,8 +266,9 @@ def test_batched_instances_match_one_context_steps():
 
 @pytest.mark.gpu
 def test_mk2_launch_shapes_give_same_bits_and_autotune_keeps_state():
-    """The moving-grid face kernel's launch shapes (register caps) give the
-    same bits; autotuning writes only scratch."""
+    """The moving-grid step's arrangements (face kernel + update kernel, or
+    one tile kernel) and launch shapes give the same bits; autotuning writes
+    only scratch."""
     mesh = g.Mesh.setka(*MEDIUM)
     P = N.reference_params()
     st0 = W.init_conditions_reference(mesh)
