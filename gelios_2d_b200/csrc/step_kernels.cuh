@@ -161,11 +161,13 @@ struct TileView {
 //                 to the flux slots in global memory; 128 threads x 8, 5, 6,
 //                 4 resident blocks) + mk2_update_kernel (slot sums, update);
 //   variants 4-7  mk2_tile_kernel, one tile of cells per block, slot fluxes
-//                 in shared memory (256 x 3, 256 x 2, 128 x 5, 128 x 4).
+//                 in shared memory (256 x 3, 256 x 2, 128 x 5, 128 x 4);
+//   variants 8-10 mk2_face2_kernel (two lanes per face unit, one side each;
+//                 128 threads x 8, 6, 10 resident blocks) + mk2_update_kernel.
 // Variant 0 is the default; gelios_autotune picks the fastest for a grid.
 // All give the same bits.
 void launch_mk2_recon(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* rec, cudaStream_t s);
-constexpr int kMk2Variants = 8;
+constexpr int kMk2Variants = 11;
 const char* mk2_variant_name(int v);
 int mk2_variant_launches(int v);
 cudaError_t launch_mk2_cells(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const TileView& t,
