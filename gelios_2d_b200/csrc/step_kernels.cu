@@ -158,6 +158,39 @@ __device__ double area(const int32_t* contour, int n, const int32_t* sA, const i
     return S;
 }
 
+// centroid, area (Get_Volume) and rotated volume of a quadrilateral whose
+// corners (contour order) are in registers: the operations of centroid(),
+// area() (n == 4) and volume_rotate() in the same order.
+__device__ __forceinline__ void quad_geometry(const double (&X)[4], const double (&Y)[4], double& ox, double& oy,
+                                              double& vs, double& vol) {
+    double A = 0.0, Gx = 0.0, Gy = 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const double xa = X[i], ya = Y[i], xb = X[(i + 1) & 3], yb = Y[(i + 1) & 3];
+        const double cr = xa * yb - ya * xb;
+        A = A + cr;
+        Gx = Gx + (xa + xb) * cr;
+        Gy = Gy + (ya + yb) * cr;
+    }
+    A = A * 0.5;
+    ox = Gx / (6.0 * A);
+    oy = Gy / (6.0 * A);
+    vol = fabs(A) * (1.0 / (6.0 * A)) * Gy * kPi * 360.0 / 180.0 / (2.0 * kPi);
+    double a1 = X[0] - X[2];
+    double a2 = Y[0] - Y[2];
+    const double a = sqrt(sq(a1) + sq(a2));
+    double b1 = X[1] - X[3];
+    double b2 = Y[1] - Y[3];
+    const double bb = sqrt(sq(b1) + sq(b2));
+    a1 = a1 / a;
+    a2 = a2 / a;
+    b1 = b1 / bb;
+    b2 = b2 / bb;
+    const double cc = a1 * b1 + a2 * b2;
+    const double sn = sqrt(1 - sq(cc));
+    vs = 0.5 * a * bb * sn;
+}
+
 // Inner_sphere BC state (Gran.cpp:234-265, 520-534) at face centre (x, y).
 __device__ __forceinline__ St5 inner_sphere_state(const gelios_params& P, double x, double y) {
     const double dist = sqrt(x * x + y * y);
@@ -1354,20 +1387,32 @@ __device__ __forceinline__ void mk2_update_cell(const DevMesh& d, const gelios_p
                                                 int& npc) {
     const int s0 = d.cstart[c], n = d.cstart[c + 1] - s0;
     const int32_t* con = d.contour + s0;
-    double xn, yn;
-    centroid(con, n, d.X2, d.Y2, xn, yn);
+    const uint32_t cfl = d.cflags[c];
+    const double x = b.cx[c], y = b.cy[c];
+    double xn, yn, vs2 = 0.0, Volume2 = 0.0;
+    if (n == 4) {
+        // quadrilateral: the four moved points once, in registers (the same
+        // operations as centroid / area / volume_rotate)
+        const int p0 = con[0], p1 = con[1], p2 = con[2], p3 = con[3];
+        const double qx[4] = {d.X2[p0], d.X2[p1], d.X2[p2], d.X2[p3]};
+        const double qy[4] = {d.Y2[p0], d.Y2[p1], d.Y2[p2], d.Y2[p3]};
+        quad_geometry(qx, qy, xn, yn, vs2, Volume2);
+        if (!(cfl & CF_CENTR)) {
+            b.vs_next[c] = vs2;
+            b.vol_next[c] = Volume2;
+        }
+    } else {
+        centroid(con, n, d.X2, d.Y2, xn, yn);
+        if (!(cfl & CF_CENTR)) {
+            vs2 = area(con, n, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X2, d.Y2, true);
+            Volume2 = volume_rotate(con, n, d.X2, d.Y2);
+            b.vs_next[c] = area(con, n, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X2, d.Y2, false);
+            b.vol_next[c] = Volume2;
+        }
+    }
     b.cx_next[c] = xn;
     b.cy_next[c] = yn;
-    const uint32_t cfl = d.cflags[c];
     if (cfl & CF_RP) b.rp_next[c] = pow2g(sqrt(sq(xn) + sq(yn)), 2 * P.gamma);
-    const double x = b.cx[c], y = b.cy[c];
-    double vs2 = 0.0, Volume2 = 0.0;
-    if (!(cfl & CF_CENTR)) {
-        vs2 = area(con, n, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X2, d.Y2, true);
-        Volume2 = volume_rotate(con, n, d.X2, d.Y2);
-        b.vs_next[c] = n == 4 ? vs2 : area(con, n, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X2, d.Y2, false);
-        b.vol_next[c] = Volume2;
-    }
     if (sqrt(sq(x) + sq(y)) < P.R11) return;
     tmark = dmin_ref(tmark, 10000000.0);  // `time` starts at 1e7 in every step (Setka.cpp:10141)
     const double dt = *b.dt_cur;
