@@ -75,7 +75,8 @@ WORKLOADS = {
 BYTES_PER_CELL = {"mk2": 288, "plain": 112, "k5": 392, "mhd": 288, "inner": 264}
 STEP_KERNELS = {
     "mk2": "whole moving-grid step: tracked recon + solve, source, surface_faces, rails, tracked flux, "
-           "face (reconstruction + flux), update, commit (one CUDA graph, 2 streams)",
+           "face units (reconstruction + flux) and cell update in the autotuned arrangement, commit "
+           "(one CUDA graph, 2 streams)",
     "plain": "whole plain step: stationary_persistent_kernel (face units, cell update, dt; all steps of a call "
              "in one cooperative launch)",
     "k5": "whole four-fluid step: centroid, surface_faces, rails, k5_cell, commit",
@@ -734,7 +735,12 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64 (fp32 flux)",
         "data": "synthetic (seeded initial field and Monte-Carlo moments)", "config": config,
         "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": e2e_bytes,
-                "d2h_bytes_per_step": e2e_bytes},
+                "d2h_bytes_per_step": e2e_bytes,
+                "moved_per_step": "the step's full state rows in from pinned host memory and out again "
+                                  f"({block.shape[0]} rows x {block.shape[1]} cells, gelios_run_streamed)" +
+                                  ("; the Monte-Carlo moments (19 doubles per cell) stay resident: the coupled "
+                                   "host code refreshes them once per global iteration, not per step"
+                                   if form in ("mk2", "inner") else "")},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
