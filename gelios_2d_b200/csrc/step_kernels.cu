@@ -504,6 +504,89 @@ __device__ void source_mk1(const DevMesh& d, const gelios_params& P, int k, doub
     q3 = MT * m.kT;
 }
 
+// source_mk1 with the four species' moments of a cell read as two 16-byte
+// loads per row (rows [cell][4] are 32-byte aligned), all issued before the
+// rates are evaluated; the same operations in the same order.
+__device__ __forceinline__ void load_sorts(const double* __restrict__ a, int K, double (&o)[4]) {
+    const double2* q = reinterpret_cast<const double2*>(a + 4 * static_cast<size_t>(K));
+    const double2 lo = q[0], hi = q[1];
+    o[0] = lo.x;
+    o[1] = lo.y;
+    o[2] = hi.x;
+    o[3] = hi.y;
+}
+__device__ void source_cell(const DevMesh& d, const gelios_params& P, int k, double xx, double yy, double u, double v,
+                            double ro, double p, double& q1, double& q2, double& q3, int* status) {
+    const double rr = sqrt(sq(xx) + sq(yy));
+    const bool interp = rr > P.src_rmin && rr < P.src_rmax && xx >= 0.0;
+    int K_do = k, K_posle = k;
+    if (interp) {
+        if (!source_bracket(d, k, rr, K_do, K_posle, status)) {
+            q1 = q2 = q3 = 0.0;
+            return;
+        }
+        if (d.src_lo_out) d.src_lo_out[k] = K_do;
+    }
+    double uH[4], vH[4], roH[4], pH[4], ku, kv, kT;
+    if (interp) {
+        double u1[4], u2[4], v1[4], v2[4], n1[4], n2[4], T1[4], T2[4];
+        load_sorts(d.Hu, K_do, u1);
+        load_sorts(d.Hu, K_posle, u2);
+        load_sorts(d.Hv, K_do, v1);
+        load_sorts(d.Hv, K_posle, v2);
+        load_sorts(d.Hn, K_do, n1);
+        load_sorts(d.Hn, K_posle, n2);
+        load_sorts(d.HT, K_do, T1);
+        load_sorts(d.HT, K_posle, T2);
+        const double r1 = d.r_istoch[K_do];
+        const double r2 = d.r_istoch[K_posle];
+        const double ir = 1.0 / (r1 - r2), dr = rr - r2;
+        auto lin = [&](double t1, double t2) { return (t1 - t2) * ir * dr + t2; };
+#pragma unroll
+        for (int s = 0; s < 4; s++) {
+            uH[s] = lin(u1[s], u2[s]);
+            vH[s] = lin(v1[s], v2[s]);
+            roH[s] = lin(n1[s], n2[s]);
+            pH[s] = 0.5 * lin(T1[s], T2[s]) * roH[s];
+        }
+        ku = lin(d.ku[K_do], d.ku[K_posle]);
+        kv = lin(d.kv[K_do], d.kv[K_posle]);
+        kT = lin(d.kT[K_do], d.kT[K_posle]);
+    } else {
+        double T[4];
+        load_sorts(d.Hu, k, uH);
+        load_sorts(d.Hv, k, vH);
+        load_sorts(d.Hn, k, roH);
+        load_sorts(d.HT, k, T);
+#pragma unroll
+        for (int s = 0; s < 4; s++) pH[s] = 0.5 * T[s] * roH[s];
+        ku = d.ku[k];
+        kv = d.kv[k];
+        kT = d.kT[k];
+    }
+    const double pro = p / ro;
+    const double kin = sq(u) + sq(v);
+    double nuu[4], nuv[4], nue[4];
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+        SrcMoments m;
+        m.uH = uH[s];
+        m.vH = vH[s];
+        m.roH = roH[s];
+        m.pH = pH[s];
+        m.ku = ku;
+        m.kv = kv;
+        m.kT = kT;
+        source_rates(P, m, u, v, ro, pro, kin, nuu[s], nuv[s], nue[s]);
+    }
+    const double Mu = P.src_coef * (nuu[0] + nuu[1] + nuu[2] + nuu[3]);
+    const double Mv = P.src_coef * (nuv[0] + nuv[1] + nuv[2] + nuv[3]);
+    const double MT = P.src_coef * (nue[0] + nue[1] + nue[2] + nue[3]);
+    q1 = Mu * ku;
+    q2 = Mv * kv;
+    q3 = MT * kT;
+}
+
 // Block-level minimum of `t` (non-negative doubles; NaN ignored) folded into
 // the device word acc with one atomicMin per block; clamp counters likewise.
 __device__ __forceinline__ void block_reduce_commit(double t, int nro, int np_, int status, unsigned long long* acc,
@@ -1350,9 +1433,9 @@ __global__ void __launch_bounds__(128, GELIOS_SOURCE_MINB) mk2_source_kernel(Dev
 }
 
 // The same source terms with one thread per cell and the four species in turn
-// (source_mk1, as the inner form evaluates them): one bracket search and one
-// set of k_u, k_v, k_T per cell instead of four, more independent loads per
-// thread, a quarter of the threads.  Same sums in the same order, same bits.
+// (source_cell): one bracket search and one set of k_u, k_v, k_T per cell
+// instead of four, the moments as 16-byte loads all in flight together, a
+// quarter of the threads.  Same sums in the same order, same bits.
 __global__ void __launch_bounds__(128) mk2_source_cell_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                               double* __restrict__ aux) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1362,7 +1445,7 @@ __global__ void __launch_bounds__(128) mk2_source_cell_kernel(DevMesh d, gelios_
         if (!(sqrt(sq(x) + sq(y)) < P.R11)) {
             const St5 par1 = load_state(b.cur, c);
             double q1 = 0.0, q2 = 0.0, q3 = 0.0;
-            source_mk1(d, P, c, x, y, par1.u, par1.v, par1.ro, par1.p, q1, q2, q3, &status);
+            source_cell(d, P, c, x, y, par1.u, par1.v, par1.ro, par1.p, q1, q2, q3, &status);
             const size_t n = d.n_cells;
             aux[0 * n + c] = q1;
             aux[1 * n + c] = q2;
