@@ -1436,7 +1436,7 @@ __global__ void __launch_bounds__(128, GELIOS_SOURCE_MINB) mk2_source_kernel(Dev
 // (source_cell): one bracket search and one set of k_u, k_v, k_T per cell
 // instead of four, the moments as 16-byte loads all in flight together, a
 // quarter of the threads.  Same sums in the same order, same bits.
-__global__ void __launch_bounds__(128) mk2_source_cell_kernel(DevMesh d, gelios_params P, StepBuffers b,
+__global__ void __launch_bounds__(128, 6) mk2_source_cell_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                               double* __restrict__ aux) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     int status = 0;
@@ -3608,38 +3608,48 @@ static cudaError_t launch_tiles_v(const DevMesh& d, const gelios_params& P, cons
     mk2_tile_kernel<TF, NT, MINB><<<t.n_tiles, NT, smem, s>>>(d, P, b, t, fl, aux);
     return cudaGetLastError();
 }
+// Part 1 of a variant: the face units (none for the tile variants); part 2:
+// the cell update (the whole tile kernel for the tile variants).  Part 1
+// needs only the moved points; part 2 also the tracked-face fluxes and the
+// source terms of the side stream.
 template <typename TF, int MINB>
-static cudaError_t launch_faces_v(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
-                                  const double* aux, cudaStream_t s) {
+static void launch_faces_v(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
+                           cudaStream_t s) {
     const int nr = d.n_units - (d.u_tr1 - d.u_tr0);
     if (nr > 0) mk2_face_kernel<TF, MINB><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, b, fl, nr);
-    mk2_update_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, fl, aux);
-    return cudaGetLastError();
 }
 template <typename TF, int MINB>
-static cudaError_t launch_faces2_v(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
-                                   const double* aux, cudaStream_t s) {
+static void launch_faces2_v(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
+                            cudaStream_t s) {
     const int nr = d.n_units - (d.u_tr1 - d.u_tr0);
     if (nr > 0) mk2_face2_kernel<TF, MINB><<<blocks_for(2 * nr, 128), 128, 0, s>>>(d, P, b, fl, nr);
-    mk2_update_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, fl, aux);
-    return cudaGetLastError();
 }
 template <typename TF>
 static cudaError_t launch_cells_p(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const TileView& t,
-                                  double* fl, const double* aux, cudaStream_t s, int variant) {
-    switch (variant) {
-        case 1: return launch_faces_v<TF, 5>(d, P, b, fl, aux, s);
-        case 2: return launch_faces_v<TF, 6>(d, P, b, fl, aux, s);
-        case 3: return launch_faces_v<TF, 4>(d, P, b, fl, aux, s);
-        case 4: return launch_tiles_v<TF, 256, 3>(d, P, b, t, fl, aux, s);
-        case 5: return launch_tiles_v<TF, 256, 2>(d, P, b, t, fl, aux, s);
-        case 6: return launch_tiles_v<TF, 128, 5>(d, P, b, t, fl, aux, s);
-        case 7: return launch_tiles_v<TF, 128, 4>(d, P, b, t, fl, aux, s);
-        case 8: return launch_faces2_v<TF, 8>(d, P, b, fl, aux, s);
-        case 9: return launch_faces2_v<TF, 6>(d, P, b, fl, aux, s);
-        case 10: return launch_faces2_v<TF, 10>(d, P, b, fl, aux, s);
-        default: return launch_faces_v<TF, 8>(d, P, b, fl, aux, s);
+                                  double* fl, const double* aux, cudaStream_t s, int variant, int part) {
+    if (variant >= 4 && variant < 8) {
+        if (part == 1) return cudaSuccess;
+        switch (variant) {
+            case 4: return launch_tiles_v<TF, 256, 3>(d, P, b, t, fl, aux, s);
+            case 5: return launch_tiles_v<TF, 256, 2>(d, P, b, t, fl, aux, s);
+            case 6: return launch_tiles_v<TF, 128, 5>(d, P, b, t, fl, aux, s);
+            default: return launch_tiles_v<TF, 128, 4>(d, P, b, t, fl, aux, s);
+        }
     }
+    if (part == 2) {
+        mk2_update_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, fl, aux);
+        return cudaGetLastError();
+    }
+    switch (variant) {
+        case 1: launch_faces_v<TF, 5>(d, P, b, fl, s); break;
+        case 2: launch_faces_v<TF, 6>(d, P, b, fl, s); break;
+        case 3: launch_faces_v<TF, 4>(d, P, b, fl, s); break;
+        case 8: launch_faces2_v<TF, 8>(d, P, b, fl, s); break;
+        case 9: launch_faces2_v<TF, 6>(d, P, b, fl, s); break;
+        case 10: launch_faces2_v<TF, 10>(d, P, b, fl, s); break;
+        default: launch_faces_v<TF, 8>(d, P, b, fl, s); break;
+    }
+    return cudaGetLastError();
 }
 const char* mk2_variant_name(int v) {
     static const char* names[kMk2Variants] = {"faces 128x8 + update", "faces 128x5 + update",
@@ -3650,11 +3660,14 @@ const char* mk2_variant_name(int v) {
                                               "faces2 128x10 + update"};
     return (v >= 0 && v < kMk2Variants) ? names[v] : "?";
 }
-int mk2_variant_launches(int v) { return (v >= 4 && v < 8) ? 1 : 2; }
+int mk2_variant_launches(int v, int part) {
+    const bool tiles = v >= 4 && v < 8;
+    return part == 1 ? (tiles ? 0 : 1) : 1;
+}
 cudaError_t launch_mk2_cells(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const TileView& t,
-                             double* fl, const double* aux, cudaStream_t s, int variant) {
-    if (P.precision == GELIOS_PREC_FP32_FLUX) return launch_cells_p<float>(d, P, b, t, fl, aux, s, variant);
-    return launch_cells_p<double>(d, P, b, t, fl, aux, s, variant);
+                             double* fl, const double* aux, cudaStream_t s, int variant, int part) {
+    if (P.precision == GELIOS_PREC_FP32_FLUX) return launch_cells_p<float>(d, P, b, t, fl, aux, s, variant, part);
+    return launch_cells_p<double>(d, P, b, t, fl, aux, s, variant, part);
 }
 int launch_mk2_tracked_solve(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
                              double* pstar, cudaStream_t s) {

@@ -169,9 +169,12 @@ struct TileView {
 void launch_mk2_recon(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* rec, cudaStream_t s);
 constexpr int kMk2Variants = 11;
 const char* mk2_variant_name(int v);
-int mk2_variant_launches(int v);
+// part 1: the face units of the face-kernel variants (reads the moved points
+// only); part 2: the cell update, or the whole tile kernel (also reads the
+// tracked-face fluxes and the source terms).  Returns the launch's error.
+int mk2_variant_launches(int v, int part);
 cudaError_t launch_mk2_cells(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const TileView& t,
-                             double* fl, const double* aux, cudaStream_t s, int variant = 0);
+                             double* fl, const double* aux, cudaStream_t s, int variant, int part);
 int launch_mk2_tracked_solve(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
                              double* pstar, cudaStream_t s);
 int launch_mk2_flux_tracked(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
