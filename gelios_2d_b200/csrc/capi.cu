@@ -539,7 +539,7 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     // face units: every slot of a cell except the twins of interior faces,
     // whose flux comes from the unit of the main face (see step_kernels.cu)
     std::vector<int32_t> u_slot, u_cell, u_twin;
-    int u_tr0 = 0, u_tr1 = 0;
+    int u_c1 = 0, u_tr0 = 0, u_tr1 = 0;
     {
         std::vector<int32_t> slot_of_face(nf, -1);
         for (int c = 0; c < nc; c++)
@@ -588,6 +588,8 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
             u_slot.swap(s2);
             u_cell.swap(c2);
             u_twin.swap(t2);
+            u_c1 = 0;
+            while (u_c1 < static_cast<int>(nu) && cls[order[u_c1]] < 1) u_c1++;
             u_tr0 = 0;
             while (u_tr0 < static_cast<int>(nu) && cls[order[u_tr0]] < 2) u_tr0++;
             u_tr1 = u_tr0;
@@ -833,6 +835,7 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     d.u_sd2 = ctx->u_sd2.as<int32_t>();
     d.u_cell = ctx->u_cell.as<int32_t>();
     d.u_twin = ctx->u_twin.as<int32_t>();
+    d.u_c1 = u_c1;
     d.u_tr0 = u_tr0;
     d.u_tr1 = u_tr1;
     d.fA = ctx->fA.as<int32_t>();

@@ -996,6 +996,10 @@ struct RecUnit {
     double dist, distn;        // owner / other centroid to the face centre, -1 if not updated
 };
 
+// PLAIN: a unit of the plain interior group [0, u_c1) (a Usualy face, neither
+// cell C_1, not tracked): the boundary, radial and tracked branches drop out
+// at compile time.
+template <bool PLAIN = false>
 __device__ __forceinline__ void mk2_recon_unit(const DevMesh& d, const gelios_params& P, const StepBuffers& b, int u,
                                                RecUnit& r, int* status) {
     const int K = d.u_cell[u], nb = d.u_nb[u];
@@ -1026,15 +1030,15 @@ __device__ __forceinline__ void mk2_recon_unit(const DevMesh& d, const gelios_pa
         r.distn = procN ? sqrt(sq(x3 - x2) + sq(y3 - y2)) : -1.0;
     }
     if (!(procK || procN)) return;
-    const int ft = info & SI_TYPE_MASK;
-    const uint32_t cf = (info >> UI_CF_OWN) & 15u;
+    const int ft = PLAIN ? static_cast<int>(G_USUALY) : static_cast<int>(info & SI_TYPE_MASK);
+    const uint32_t cf = (info >> UI_CF_OWN) & (PLAIN ? (15u & ~CF_C1) : 15u);
     const double g2 = 2 * P.gamma;
     const St5 par1 = load_state(b.cur, K);
     St5 par11 = par1;
     St5 par2 = get_par(P, ft, par1, b.cur, nb, x2, y2);
     const double dis = sqrt(sq(x2) + sq(y2));
-    const bool tracked = (info & SI_GOD) != 0;
-    const uint32_t nbf = (info >> UI_CF_NB) & 15u;
+    const bool tracked = !PLAIN && (info & SI_GOD) != 0;
+    const uint32_t nbf = (info >> UI_CF_NB) & (PLAIN ? (15u & ~CF_C1) : 15u);
     const bool radial = ((cf & CF_C1) && (ft == G_USUALY || ft == G_AXIS)) || ft == G_INNER_SPHERE ||
                         (ft == G_USUALY && (nbf & CF_C1));
     const double pdis = radial ? pow2g(dis, g2) : 1.0;
@@ -1193,18 +1197,22 @@ __global__ void __launch_bounds__(32) mk2_flux_tracked_kernel(DevMesh d, gelios_
 // pass: the reconstructed states stay in registers (no per-unit scratch);
 // F.S to the owner's flux slot and -F.S to the twin's.  Index i is remapped
 // around the tracked range [u_tr0, u_tr1).
-template <typename TF, int MINB>
+// PLAIN: the plain interior group [0, u_c1) only (compiled without the
+// boundary, radial and tracked branches); otherwise the units [u_c1, u_tr0)
+// and [u_tr1, n_units).
+template <typename TF, int MINB, bool PLAIN>
 __global__ void __launch_bounds__(128, MINB) mk2_face_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                            double* __restrict__ fl, int n_launch) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double tmin_u = __longlong_as_double(0x7ff0000000000000LL);
     int status = 0;
     if (i < n_launch) {
-        const int u = i < d.u_tr0 ? i : i + (d.u_tr1 - d.u_tr0);
+        const int j = PLAIN ? i : d.u_c1 + i;
+        const int u = (PLAIN || j < d.u_tr0) ? j : j + (d.u_tr1 - d.u_tr0);
         RecUnit r;
         r.a = St5{};
         r.o = St5{};
-        mk2_recon_unit(d, P, b, u, r, &status);
+        mk2_recon_unit<PLAIN>(d, P, b, u, r, &status);
         mk2_flux_unit<TF, false>(d, P, b, u, r, fl, nullptr, tmin_u, &status);
     }
     block_reduce_commit(tmin_u, 0, 0, status, b.dt_acc, b.counters, b.status);
@@ -3615,8 +3623,11 @@ static cudaError_t launch_tiles_v(const DevMesh& d, const gelios_params& P, cons
 template <typename TF, int MINB>
 static void launch_faces_v(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
                            cudaStream_t s) {
-    const int nr = d.n_units - (d.u_tr1 - d.u_tr0);
-    if (nr > 0) mk2_face_kernel<TF, MINB><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, b, fl, nr);
+    // the plain interior group with the lean kernel, the other groups after it
+    const int n0 = d.u_c1;
+    const int nr = d.n_units - (d.u_tr1 - d.u_tr0) - n0;
+    if (n0 > 0) mk2_face_kernel<TF, MINB, true><<<blocks_for(n0, 128), 128, 0, s>>>(d, P, b, fl, n0);
+    if (nr > 0) mk2_face_kernel<TF, 4, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, b, fl, nr);
 }
 template <typename TF, int MINB>
 static void launch_faces2_v(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
@@ -3661,8 +3672,8 @@ const char* mk2_variant_name(int v) {
     return (v >= 0 && v < kMk2Variants) ? names[v] : "?";
 }
 int mk2_variant_launches(int v, int part) {
-    const bool tiles = v >= 4 && v < 8;
-    return part == 1 ? (tiles ? 0 : 1) : 1;
+    const bool tiles = v >= 4 && v < 8, two = v < 4;  // face variants 0-3: plain group + the rest
+    return part == 1 ? (tiles ? 0 : (two ? 2 : 1)) : 1;
 }
 cudaError_t launch_mk2_cells(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const TileView& t,
                              double* fl, const double* aux, cudaStream_t s, int variant, int part) {

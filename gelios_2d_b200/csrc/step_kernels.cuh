@@ -31,7 +31,9 @@ struct DevMesh {
     // face units (one flux evaluation each, see step_kernels.cu): owner slot,
     // owner cell, slot of the twin face in the neighbour (-1: one-sided)
     int n_slots = 0, n_units = 0;
-    int u_tr0 = 0, u_tr1 = 0;  // range of the tracked-face units (grouped together)
+    // units are grouped: plain interior [0, u_c1), interior with a C_1 side
+    // [u_c1, u_tr0), tracked [u_tr0, u_tr1), one-sided [u_tr1, n_units)
+    int u_c1 = 0, u_tr0 = 0, u_tr1 = 0;
     const int32_t *u_slot = nullptr, *u_cell = nullptr, *u_twin = nullptr;
     const int32_t *u_A = nullptr, *u_B = nullptr;  // end points of the unit's face
     // slot info of the unit's face | owner flags << UI_CF_OWN | neighbour flags << UI_CF_NB
@@ -159,7 +161,9 @@ struct TileView {
 // update in one of two arrangements, kMk2Variants launch shapes in all:
 //   variants 0-3  mk2_face_kernel (reconstruction and flux in registers, F.S
 //                 to the flux slots in global memory; 128 threads x 8, 5, 6,
-//                 4 resident blocks) + mk2_update_kernel (slot sums, update);
+//                 4 resident blocks; the plain interior group in its own
+//                 launch of a lean instance) + mk2_update_kernel (slot sums,
+//                 update);
 //   variants 4-7  mk2_tile_kernel, one tile of cells per block, slot fluxes
 //                 in shared memory (256 x 3, 256 x 2, 128 x 5, 128 x 4);
 //   variants 8-10 mk2_face2_kernel (two lanes per face unit, one side each;
