@@ -1641,7 +1641,7 @@ __global__ void __launch_bounds__(NT, MINB) mk2_tile_kernel(DevMesh d, gelios_pa
 
 // The cell update alone, from the flux slots in global memory (the update
 // phase of the tile kernel for the face-kernel arrangement).
-__global__ void __launch_bounds__(128, 6) mk2_update_kernel(DevMesh d, gelios_params P, StepBuffers b,
+__global__ void __launch_bounds__(128, 8) mk2_update_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                           const double* __restrict__ fl,
                                                           const double* __restrict__ aux) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
