@@ -1509,6 +1509,14 @@ extern "C" int gelios_set_variant(gelios_ctx* ctx, int form, int32_t variant) {
     return GELIOS_OK;
 }
 
+extern "C" int gelios_get_variant(gelios_ctx* ctx, int form, int32_t* variant, int32_t* source_variant) {
+    if (!ctx) return GELIOS_E_ARG;
+    const bool mk2 = form == GELIOS_FORM_MK2;
+    if (variant) *variant = form == GELIOS_FORM_MHD_PUI ? ctx->mhd_face_variant : mk2 ? ctx->mk2_variant : 0;
+    if (source_variant) *source_variant = mk2 ? ctx->mk2_source_variant : 0;
+    return GELIOS_OK;
+}
+
 extern "C" int gelios_autotune(gelios_ctx* ctx, int form, int reps, int32_t* variant, double* ms) {
     if (!ctx || reps < 1) return GELIOS_E_ARG;
     const bool mhd = form == GELIOS_FORM_MHD_PUI;

@@ -365,6 +365,11 @@ int gelios_mlp_gemm_bf16(int M, int N, int K, const void *A, int64_t lda, const 
 int gelios_variant_count(int form);
 int gelios_autotune(gelios_ctx *ctx, int form, int reps, int32_t *variant, double *ms);
 int gelios_set_variant(gelios_ctx *ctx, int form, int32_t variant);
+/* The variant a context uses for `form` (set by hand or by gelios_autotune)
+ * and, for GELIOS_FORM_MK2, the arrangement of its source-term kernel (0: four
+ * lanes per cell, 1: one thread per cell; 0 for the other forms); either
+ * pointer may be NULL. */
+int gelios_get_variant(gelios_ctx *ctx, int form, int32_t *variant, int32_t *source_variant);
 
 /* ---- per-face solvers on the device (known-answer checks) ------------------
  * Batched HLLC_2d_Korolkov_b_s (Setka.cpp:10484-10700): in[n*16] =
