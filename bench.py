@@ -649,8 +649,6 @@ def main():
     if form in ("mhd", "mk2"):  # launch shape of the face kernel picked on this grid (the library's autotuner)
         v, tms = S.autotune(fcode, reps=3)
         tuned = {"variant": v, "face_kernel_ms": tms}
-        if form == "mk2":
-            tuned["source_variant"] = S.get_variant(fcode)[1]
     stream = torch.cuda.ExternalStream(S.stream_handle(), device=device)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")
     do_flush = not args.workload.endswith("_1m")

@@ -108,7 +108,6 @@ struct gelios_ctx {
     DBuf flux_mhd;   // multi-fluid forms: 13 (MHD) or 21 (Go_5_komponent) flux rows per face slot, on first use
     int mhd_face_variant = 0;  // launch shape of the MHD face kernel (gelios_autotune)
     int mk2_variant = 0;  // arrangement / launch shape of the moving-grid face units + update (gelios_autotune)
-    int mk2_source_variant = 0;  // arrangement of the moving-grid source kernel (gelios_autotune)
     // tiles of the moving-grid step (see TileView)
     DBuf t_cstart, t_cells, t_lbase, t_fstart, t_faces;
     TileView tiles;
@@ -1045,7 +1044,7 @@ int enqueue_mk2(gelios_ctx* ctx, const StepBuffers& b) {
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_fork, 0));
     launch_mk2_recon(d, P, b, ctx->rec.as<double>(), sd);
     const int nsv = launch_mk2_tracked_solve(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(), sd);
-    launch_mk2_source(d, P, b, ctx->aux.as<double>(), sd, ctx->mk2_source_variant);
+    launch_mk2_source(d, P, b, ctx->aux.as<double>(), sd);
     cudaEvent_t e1 = ctx->phase_begin();
     const int nm = launch_motion(d, P, b, ctx->surface.as<double>(), s);
     ctx->phase_end(2, e1, nm);  // Move_surface + rails
@@ -1509,11 +1508,9 @@ extern "C" int gelios_set_variant(gelios_ctx* ctx, int form, int32_t variant) {
     return GELIOS_OK;
 }
 
-extern "C" int gelios_get_variant(gelios_ctx* ctx, int form, int32_t* variant, int32_t* source_variant) {
-    if (!ctx) return GELIOS_E_ARG;
-    const bool mk2 = form == GELIOS_FORM_MK2;
-    if (variant) *variant = form == GELIOS_FORM_MHD_PUI ? ctx->mhd_face_variant : mk2 ? ctx->mk2_variant : 0;
-    if (source_variant) *source_variant = mk2 ? ctx->mk2_source_variant : 0;
+extern "C" int gelios_get_variant(gelios_ctx* ctx, int form, int32_t* variant) {
+    if (!ctx || !variant) return GELIOS_E_ARG;
+    *variant = form == GELIOS_FORM_MHD_PUI ? ctx->mhd_face_variant : form == GELIOS_FORM_MK2 ? ctx->mk2_variant : 0;
     return GELIOS_OK;
 }
 
@@ -1620,30 +1617,11 @@ extern "C" int gelios_autotune(gelios_ctx* ctx, int form, int reps, int32_t* var
             best_ms = m;
         }
     }
-    // the moving-grid form also picks the arrangement of its source kernel
-    // (writes only the source rows and the bracket hints)
-    int best_src = 0;
-    if (!mhd) {
-        double src_best = 0.0;
-        auto src = [&](int v) { launch_mk2_source(d, ctx->prm, b, ctx->aux.as<double>(), s, v); };
-        for (int v = 0; v < kMk2SourceVariants && err == cudaSuccess; v++) {
-            double m = 0.0;
-            err = time_ms(src, v, m);
-            if (v == 0 || m < src_best) {
-                best_src = v;
-                src_best = m;
-            }
-        }
-    }
     if (err != cudaSuccess) {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         set_error(std::string("gelios_autotune: ") + cudaGetErrorString(err));
         return GELIOS_E_CUDA;
-    }
-    if (!mhd && best_src != ctx->mk2_source_variant) {
-        ctx->mk2_source_variant = best_src;
-        ctx->drop_graphs();
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -6,7 +6,7 @@
 //   mk2_tracked_solve_kernel  star pressures of the tracked faces' exact
 //                             Riemann problems (warp per face)
 //   mk2_source_kernel         charge-exchange source (Get_Sourse_MK1), four
-//                             lanes per cell
+//                             lanes per cell (one hydrogen species each)
 //   surface_faces_kernel      Move_surface (Setka.cpp:3378-3844): exact
 //                             Godunov speeds of the tracked faces (warp per
 //                             face)
@@ -427,7 +427,7 @@ struct SrcMoments {
     double uH, vH, roH, pH, ku, kv, kT;
 };
 __device__ __forceinline__ SrcMoments source_moments(const DevMesh& d, int k, int s, bool interp, int K_do, int K_posle,
-                                                     double rr) {
+                                                     double rr, bool with_k = true) {
     SrcMoments m;
     if (interp) {
         const double r1 = d.r_istoch[K_do];
@@ -439,18 +439,21 @@ __device__ __forceinline__ SrcMoments source_moments(const DevMesh& d, int k, in
         m.vH = lin(d.Hv[4 * K_do + s], d.Hv[4 * K_posle + s]);
         m.roH = lin(d.Hn[4 * K_do + s], d.Hn[4 * K_posle + s]);
         const double TH = lin(d.HT[4 * K_do + s], d.HT[4 * K_posle + s]);
-        m.ku = lin(d.ku[K_do], d.ku[K_posle]);
-        m.kv = lin(d.kv[K_do], d.kv[K_posle]);
-        m.kT = lin(d.kT[K_do], d.kT[K_posle]);
+        m.ku = m.kv = m.kT = 0.0;
+        if (with_k) {
+            m.ku = lin(d.ku[K_do], d.ku[K_posle]);
+            m.kv = lin(d.kv[K_do], d.kv[K_posle]);
+            m.kT = lin(d.kT[K_do], d.kT[K_posle]);
+        }
         m.pH = 0.5 * TH * m.roH;
     } else {
         m.uH = d.Hu[4 * k + s];
         m.vH = d.Hv[4 * k + s];
         m.roH = d.Hn[4 * k + s];
         m.pH = 0.5 * d.HT[4 * k + s] * d.Hn[4 * k + s];
-        m.ku = d.ku[k];
-        m.kv = d.kv[k];
-        m.kT = d.kT[k];
+        m.ku = with_k ? d.ku[k] : 0.0;
+        m.kv = with_k ? d.kv[k] : 0.0;
+        m.kT = with_k ? d.kT[k] : 0.0;
     }
     return m;
 }
@@ -502,89 +505,6 @@ __device__ void source_mk1(const DevMesh& d, const gelios_params& P, int k, doub
     q1 = Mu * m.ku;
     q2 = Mv * m.kv;
     q3 = MT * m.kT;
-}
-
-// source_mk1 with the four species' moments of a cell read as two 16-byte
-// loads per row (rows [cell][4] are 32-byte aligned), all issued before the
-// rates are evaluated; the same operations in the same order.
-__device__ __forceinline__ void load_sorts(const double* __restrict__ a, int K, double (&o)[4]) {
-    const double2* q = reinterpret_cast<const double2*>(a + 4 * static_cast<size_t>(K));
-    const double2 lo = q[0], hi = q[1];
-    o[0] = lo.x;
-    o[1] = lo.y;
-    o[2] = hi.x;
-    o[3] = hi.y;
-}
-__device__ void source_cell(const DevMesh& d, const gelios_params& P, int k, double xx, double yy, double u, double v,
-                            double ro, double p, double& q1, double& q2, double& q3, int* status) {
-    const double rr = sqrt(sq(xx) + sq(yy));
-    const bool interp = rr > P.src_rmin && rr < P.src_rmax && xx >= 0.0;
-    int K_do = k, K_posle = k;
-    if (interp) {
-        if (!source_bracket(d, k, rr, K_do, K_posle, status)) {
-            q1 = q2 = q3 = 0.0;
-            return;
-        }
-        if (d.src_lo_out) d.src_lo_out[k] = K_do;
-    }
-    double uH[4], vH[4], roH[4], pH[4], ku, kv, kT;
-    if (interp) {
-        double u1[4], u2[4], v1[4], v2[4], n1[4], n2[4], T1[4], T2[4];
-        load_sorts(d.Hu, K_do, u1);
-        load_sorts(d.Hu, K_posle, u2);
-        load_sorts(d.Hv, K_do, v1);
-        load_sorts(d.Hv, K_posle, v2);
-        load_sorts(d.Hn, K_do, n1);
-        load_sorts(d.Hn, K_posle, n2);
-        load_sorts(d.HT, K_do, T1);
-        load_sorts(d.HT, K_posle, T2);
-        const double r1 = d.r_istoch[K_do];
-        const double r2 = d.r_istoch[K_posle];
-        const double ir = 1.0 / (r1 - r2), dr = rr - r2;
-        auto lin = [&](double t1, double t2) { return (t1 - t2) * ir * dr + t2; };
-#pragma unroll
-        for (int s = 0; s < 4; s++) {
-            uH[s] = lin(u1[s], u2[s]);
-            vH[s] = lin(v1[s], v2[s]);
-            roH[s] = lin(n1[s], n2[s]);
-            pH[s] = 0.5 * lin(T1[s], T2[s]) * roH[s];
-        }
-        ku = lin(d.ku[K_do], d.ku[K_posle]);
-        kv = lin(d.kv[K_do], d.kv[K_posle]);
-        kT = lin(d.kT[K_do], d.kT[K_posle]);
-    } else {
-        double T[4];
-        load_sorts(d.Hu, k, uH);
-        load_sorts(d.Hv, k, vH);
-        load_sorts(d.Hn, k, roH);
-        load_sorts(d.HT, k, T);
-#pragma unroll
-        for (int s = 0; s < 4; s++) pH[s] = 0.5 * T[s] * roH[s];
-        ku = d.ku[k];
-        kv = d.kv[k];
-        kT = d.kT[k];
-    }
-    const double pro = p / ro;
-    const double kin = sq(u) + sq(v);
-    double nuu[4], nuv[4], nue[4];
-#pragma unroll
-    for (int s = 0; s < 4; s++) {
-        SrcMoments m;
-        m.uH = uH[s];
-        m.vH = vH[s];
-        m.roH = roH[s];
-        m.pH = pH[s];
-        m.ku = ku;
-        m.kv = kv;
-        m.kT = kT;
-        source_rates(P, m, u, v, ro, pro, kin, nuu[s], nuv[s], nue[s]);
-    }
-    const double Mu = P.src_coef * (nuu[0] + nuu[1] + nuu[2] + nuu[3]);
-    const double Mv = P.src_coef * (nuv[0] + nuv[1] + nuv[2] + nuv[3]);
-    const double MT = P.src_coef * (nue[0] + nue[1] + nue[2] + nue[3]);
-    q1 = Mu * ku;
-    q2 = Mv * kv;
-    q3 = MT * kT;
 }
 
 // Block-level minimum of `t` (non-negative doubles; NaN ignored) folded into
@@ -1386,35 +1306,38 @@ __global__ void __launch_bounds__(64) mk2_tracked_solve_kernel(DevMesh d, gelios
 // aux rows: q1, q2, q3
 __global__ void __launch_bounds__(128, GELIOS_SOURCE_MINB) mk2_source_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                          double* __restrict__ aux) {
-    // four lanes per cell, one hydrogen species per lane; the four rates
-    // are summed on the cell's first lane in the reference's order
+    // four lanes per cell, one hydrogen species per lane; the cell's first
+    // lane finds the bracket of the radial interpolation and hands it to the
+    // others; the four rates are summed on it in the reference's order
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int c = t >> 2, sp = t & 3;
+    const unsigned full = 0xffffffffu;
+    const int q0 = (threadIdx.x & 31) & ~3;
     int status = 0;
-    bool proc = false, ok = false;
-    double nuu = 0.0, nuv = 0.0, nue = 0.0;
-    SrcMoments m{};
-    double x = 0.0, y = 0.0;
+    bool proc = false, interp = false;
+    double x = 0.0, y = 0.0, rr = 0.0;
     if (c < d.n_cells) {
         x = b.cx[c];
         y = b.cy[c];
-        proc = !(sqrt(sq(x) + sq(y)) < P.R11);
-        if (proc) {
-            const St5 par1 = load_state(b.cur, c);
-            const double rr = sqrt(sq(x) + sq(y));
-            const bool interp = rr > P.src_rmin && rr < P.src_rmax && x >= 0.0;
-            int K_do = -1, K_posle = -1;
-            ok = !interp || source_bracket(d, c, rr, K_do, K_posle, &status);
-            if (ok) {
-                if (interp && sp == 0 && d.src_lo_out) d.src_lo_out[c] = K_do;
-                m = source_moments(d, c, sp, interp, K_do, K_posle, rr);
-                source_rates(P, m, par1.u, par1.v, par1.ro, par1.p / par1.ro, sq(par1.u) + sq(par1.v), nuu, nuv,
-                             nue);
-            }
-        }
+        rr = sqrt(sq(x) + sq(y));
+        proc = !(rr < P.R11);
+        interp = proc && rr > P.src_rmin && rr < P.src_rmax && x >= 0.0;
     }
-    const unsigned full = 0xffffffffu;
-    const int q0 = (threadIdx.x & 31) & ~3;
+    int K_do = -1, K_posle = -1, ok = 1;
+    if (interp && sp == 0) {
+        ok = source_bracket(d, c, rr, K_do, K_posle, &status) ? 1 : 0;
+        if (ok && d.src_lo_out) d.src_lo_out[c] = K_do;
+    }
+    K_do = __shfl_sync(full, K_do, q0);
+    K_posle = __shfl_sync(full, K_posle, q0);
+    ok = __shfl_sync(full, ok, q0);
+    double nuu = 0.0, nuv = 0.0, nue = 0.0;
+    SrcMoments m{};
+    if (proc && ok) {
+        const St5 par1 = load_state(b.cur, c);
+        m = source_moments(d, c, sp, interp, K_do, K_posle, rr, sp == 0);
+        source_rates(P, m, par1.u, par1.v, par1.ro, par1.p / par1.ro, sq(par1.u) + sq(par1.v), nuu, nuv, nue);
+    }
     double su[3], sv[3], se[3];
 #pragma unroll
     for (int j = 0; j < 3; j++) {
@@ -1436,29 +1359,6 @@ __global__ void __launch_bounds__(128, GELIOS_SOURCE_MINB) mk2_source_kernel(Dev
         aux[0 * n + c] = q1;
         aux[1 * n + c] = q2;
         aux[2 * n + c] = q3;
-    }
-    if (status) atomicOr(b.status, status);
-}
-
-// The same source terms with one thread per cell and the four species in turn
-// (source_cell): one bracket search and one set of k_u, k_v, k_T per cell
-// instead of four, the moments as 16-byte loads all in flight together, a
-// quarter of the threads.  Same sums in the same order, same bits.
-__global__ void __launch_bounds__(128, 6) mk2_source_cell_kernel(DevMesh d, gelios_params P, StepBuffers b,
-                                                              double* __restrict__ aux) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    int status = 0;
-    if (c < d.n_cells) {
-        const double x = b.cx[c], y = b.cy[c];
-        if (!(sqrt(sq(x) + sq(y)) < P.R11)) {
-            const St5 par1 = load_state(b.cur, c);
-            double q1 = 0.0, q2 = 0.0, q3 = 0.0;
-            source_cell(d, P, c, x, y, par1.u, par1.v, par1.ro, par1.p, q1, q2, q3, &status);
-            const size_t n = d.n_cells;
-            aux[0 * n + c] = q1;
-            aux[1 * n + c] = q2;
-            aux[2 * n + c] = q3;
-        }
     }
     if (status) atomicOr(b.status, status);
 }
@@ -3697,12 +3597,8 @@ int launch_mk2_flux_tracked(const DevMesh& d, const gelios_params& P, const Step
         mk2_flux_tracked_kernel<double><<<blocks_for(nt, 32), 32, 0, s>>>(d, P, b, rec, fl, pstar);
     return 1;
 }
-void launch_mk2_source(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* aux, cudaStream_t s,
-                       int variant) {
-    if (variant == 1)
-        mk2_source_cell_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, aux);
-    else
-        mk2_source_kernel<<<blocks_for(4 * d.n_cells, 128), 128, 0, s>>>(d, P, b, aux);
+void launch_mk2_source(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* aux, cudaStream_t s) {
+    mk2_source_kernel<<<blocks_for(4 * d.n_cells, 128), 128, 0, s>>>(d, P, b, aux);
 }
 void launch_inner(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const int32_t* list, int n,
                   cudaStream_t s) {

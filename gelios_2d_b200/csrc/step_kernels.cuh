@@ -183,12 +183,9 @@ int launch_mk2_tracked_solve(const DevMesh& d, const gelios_params& P, const Ste
                              double* pstar, cudaStream_t s);
 int launch_mk2_flux_tracked(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
                             const double* pstar, double* fl, cudaStream_t s);
-// Charge-exchange source terms of the moving-grid step (aux rows q1, q2, q3):
-// variant 0 four lanes per cell (one hydrogen species each), variant 1 one
-// thread per cell; same bits.  gelios_autotune picks the faster for a grid.
-constexpr int kMk2SourceVariants = 2;
-void launch_mk2_source(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* aux, cudaStream_t s,
-                       int variant = 0);
+// Charge-exchange source terms of the moving-grid step (aux rows q1, q2, q3),
+// four lanes per cell.
+void launch_mk2_source(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* aux, cudaStream_t s);
 void launch_inner(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const int32_t* list, int n,
                   cudaStream_t s);
 void launch_dt_finalize(const StepBuffers& b, cudaStream_t s);

@@ -227,11 +227,11 @@ class Setka:
     def set_variant(self, form: int, variant: int):
         N.check(self._L.gelios_set_variant(self._h, int(form), int(variant)), "gelios_set_variant")
 
-    def get_variant(self, form: int) -> tuple[int, int]:
-        """(variant of the form's dominant kernels, source-kernel arrangement)."""
-        v, sv = C.c_int32(), C.c_int32()
-        N.check(self._L.gelios_get_variant(self._h, int(form), C.byref(v), C.byref(sv)), "gelios_get_variant")
-        return int(v.value), int(sv.value)
+    def get_variant(self, form: int) -> int:
+        """The variant of the form's dominant kernels this context uses."""
+        v = C.c_int32()
+        N.check(self._L.gelios_get_variant(self._h, int(form), C.byref(v)), "gelios_get_variant")
+        return int(v.value)
     def set_hydrogen(self, buf: int, h16: np.ndarray):
         """ro, p, u, v of the hydrogen fluids H1..H4 of Cell::par[buf]
         (shape (16, n_cells))."""

