@@ -1026,22 +1026,24 @@ __device__ __forceinline__ void mk2_flux_unit(const DevMesh& d, const gelios_par
         fm3 = qq[4] * S;
     }
     const double fq = F.PQ * S;
-    fl[0 * ng + g] = fm0;
-    fl[1 * ng + g] = fm1;
-    fl[2 * ng + g] = fm2;
-    fl[3 * ng + g] = fm3;
-    fl[4 * ng + g] = fq;
+    // the slots are read once, by the update: streaming stores keep the
+    // gathered cell data in L2
+    __stcs(fl + 0 * ng + g, fm0);
+    __stcs(fl + 1 * ng + g, fm1);
+    __stcs(fl + 2 * ng + g, fm2);
+    __stcs(fl + 3 * ng + g, fm3);
+    __stcs(fl + 4 * ng + g, fq);
     if (procK) {
         // reference order: Godunov candidate first, then HLL (Setka.cpp:10359, 10366)
         if (TRACKED) tmin_u = dmin_ref(tmin_u, P.kurant * r.dist / UG);
         tmin_u = dmin_ref(tmin_u, P.kurant * r.dist / UU);
     }
     if (gt >= 0) {
-        fl[0 * ng + gt] = -fm0;
-        fl[1 * ng + gt] = -fm1;
-        fl[2 * ng + gt] = -fm2;
-        fl[3 * ng + gt] = -fm3;
-        fl[4 * ng + gt] = -fq;
+        __stcs(fl + 0 * ng + gt, -fm0);
+        __stcs(fl + 1 * ng + gt, -fm1);
+        __stcs(fl + 2 * ng + gt, -fm2);
+        __stcs(fl + 3 * ng + gt, -fm3);
+        __stcs(fl + 4 * ng + gt, -fq);
         if (procN) {
             if (TRACKED) tmin_u = dmin_ref(tmin_u, P.kurant * r.distn / UG);
             tmin_u = dmin_ref(tmin_u, P.kurant * r.distn / UU);
@@ -1262,11 +1264,11 @@ __global__ void __launch_bounds__(128, MINB) mk2_face2_kernel(DevMesh d, gelios_
         const double sg = side ? -1.0 : 1.0;
         const int g = side ? d.u_twin[u] : d.u_slot[u];
         if (g >= 0) {
-            fl[0 * ng + g] = sg * (F.P0 * S);
-            fl[1 * ng + g] = sg * (F.P1 * S);
-            fl[2 * ng + g] = sg * (F.P2 * S);
-            fl[3 * ng + g] = sg * (F.P3 * S);
-            fl[4 * ng + g] = sg * (F.PQ * S);
+            __stcs(fl + 0 * ng + g, sg * (F.P0 * S));
+            __stcs(fl + 1 * ng + g, sg * (F.P1 * S));
+            __stcs(fl + 2 * ng + g, sg * (F.P2 * S));
+            __stcs(fl + 3 * ng + g, sg * (F.P3 * S));
+            __stcs(fl + 4 * ng + g, sg * (F.PQ * S));
             if (side == 0 ? procK : procN) tmin_u = dmin_ref(tmin_u, P.kurant * (side ? r.distn : r.dist) / UU);
         }
     }
@@ -1550,7 +1552,7 @@ __global__ void __launch_bounds__(128, 8) mk2_update_kernel(DevMesh d, gelios_pa
     const size_t ng = d.n_slots;
     if (c < d.n_cells) {
         const int g0 = d.gstart[c];
-        mk2_update_cell(d, P, b, c, [&](int k, int j) { return fl[k * ng + g0 + j]; }, aux, tmark, nro, npc);
+        mk2_update_cell(d, P, b, c, [&](int k, int j) { return __ldcs(fl + k * ng + g0 + j); }, aux, tmark, nro, npc);
     }
     block_reduce_commit(tmark, nro, npc, 0, b.dt_acc, b.counters, b.status);
 }
