@@ -1080,9 +1080,9 @@ int enqueue_mhd(gelios_ctx* ctx, const StepBuffers& b) {
     const int nm = launch_motion(d, P, b, ctx->surface.as<double>(), s);
     ctx->phase_end(2, e1, nm);
     cudaEvent_t e3 = ctx->phase_begin();
-    launch_mhd_faces(d, P, ctx->mprm, b, ctx->hstate[cur].as<double>(), ctx->flux_mhd.as<double>(), s,
-                     ctx->mhd_face_variant);
-    ctx->phase_end(1, e3, 1);
+    const int nfc = launch_mhd_faces(d, P, ctx->mprm, b, ctx->hstate[cur].as<double>(), ctx->flux_mhd.as<double>(),
+                                     s, ctx->mhd_face_variant);
+    ctx->phase_end(1, e3, nfc);
     cudaEvent_t e5 = ctx->phase_begin();
     launch_mhd_update(d, P, b, ctx->flux_mhd.as<double>(), ctx->src_fixed.as<double>(), ctx->hstate[cur].as<double>(),
                       ctx->hstate[nxt].as<double>(), s);
@@ -1091,7 +1091,7 @@ int enqueue_mhd(gelios_ctx* ctx, const StepBuffers& b) {
     launch_commit(d, b, s);
     ctx->phase_end(4, e4, 1);
     GELIOS_CUDA_TRY(cudaGetLastError());
-    return nm + 3;
+    return nm + nfc + 2;
 }
 
 int enqueue_form(gelios_ctx* ctx, const StepBuffers& b, int form) {

@@ -2994,7 +2994,8 @@ __device__ __forceinline__ double mhd_face_flux(double ga, const St5& iL, const 
 // 13 flux rows times S to the owner slot and their negatives to the twin,
 // CFL candidates of both fluids.  BLOCK x MINB: the launch shape (threads
 // per block, minimum resident blocks per SM, which caps the registers).
-template <typename TF>
+// PLAIN: a unit of the plain interior group [0, u_c1) (see mk2_recon_unit).
+template <typename TF, bool PLAIN = false>
 __device__ __forceinline__ double mhd_face_body(const DevMesh& d, const gelios_params& P, const gelios_mhd_params& M,
                                                 const StepBuffers& b, const double* __restrict__ hs,
                                                 double* __restrict__ fl, int u, int& status) {
@@ -3025,15 +3026,16 @@ __device__ __forceinline__ double mhd_face_body(const DevMesh& d, const gelios_p
             const double x4 = (d.X2[A] + d.X2[B]) / 2.0, y4 = (d.Y2[A] + d.Y2[B]) / 2.0;
             const double dt = *b.dt_cur;
             const double W = ((x4 - x2) * n1 + (y4 - y2) * n2) / dt;
-            const int ft = info & SI_TYPE_MASK;
-            const uint32_t cf = (info >> UI_CF_OWN) & 15u, nbf = (info >> UI_CF_NB) & 15u;
+            const int ft = PLAIN ? static_cast<int>(G_USUALY) : static_cast<int>(info & SI_TYPE_MASK);
+            const uint32_t cmask = PLAIN ? (15u & ~CF_C1) : 15u;
+            const uint32_t cf = (info >> UI_CF_OWN) & cmask, nbf = (info >> UI_CF_NB) & cmask;
             const double g2 = 2 * P.gamma;
             const St5 par1 = load_state(b.cur, K);
             const Ext8 ex1 = load_ext(hs, nc, K);
             St5 par11 = par1, par2 = get_par(P, ft, par1, b.cur, nb, x2, y2);
             Ext8 e11 = ex1, e2 = get_par_ext(P, M, ft, ex1, hs, nc, nb, x2, y2, par2);
             const double dis = sqrt(sq(x2) + sq(y2));
-            const bool tracked = (info & SI_GOD) != 0;
+            const bool tracked = !PLAIN && (info & SI_GOD) != 0;
             const bool radial = ((cf & CF_C1) && (ft == G_USUALY || ft == G_AXIS)) || ft == G_INNER_SPHERE ||
                                 (ft == G_USUALY && (nbf & CF_C1));
             const double pdis = radial ? pow2g(dis, g2) : 1.0;
@@ -3082,11 +3084,12 @@ __device__ __forceinline__ double mhd_face_body(const DevMesh& d, const gelios_p
             F[11] = G.P2;
             F[12] = G.P3;
             const int g = d.u_slot[u], gt = d.u_twin[u];
+            // slots are read once, by the update: streaming stores
 #pragma unroll
-            for (int k = 0; k < kMhdFlux; k++) fl[k * ng + g] = F[k] * S;
+            for (int k = 0; k < kMhdFlux; k++) __stcs(fl + k * ng + g, F[k] * S);
             if (gt >= 0) {
 #pragma unroll
-                for (int k = 0; k < kMhdFlux; k++) fl[k * ng + gt] = -(F[k] * S);
+                for (int k = 0; k < kMhdFlux; k++) __stcs(fl + k * ng + gt, -(F[k] * S));
             }
             if (procK) {
                 const double dist = sqrt(sq(x - x2) + sq(y - y2));
@@ -3103,14 +3106,17 @@ __device__ __forceinline__ double mhd_face_body(const DevMesh& d, const gelios_p
     return tmin_u;
 }
 
-template <typename TF, int BLOCK, int MINB>
+// PLAIN: the plain interior group [0, u_c1) (lean instance); otherwise the
+// units [u_c1, n_units).
+template <typename TF, int BLOCK, int MINB, bool PLAIN>
 __global__ void __launch_bounds__(BLOCK, MINB) mhd_face_kernel(DevMesh d, gelios_params P, gelios_mhd_params M,
                                                                StepBuffers b, const double* __restrict__ hs,
                                                                double* __restrict__ fl) {
-    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int u = PLAIN ? i : d.u_c1 + i;
     double tmin_u = __longlong_as_double(0x7ff0000000000000LL);
     int status = 0;
-    if (u < d.n_units) tmin_u = mhd_face_body<TF>(d, P, M, b, hs, fl, u, status);
+    if (PLAIN ? u < d.u_c1 : u < d.n_units) tmin_u = mhd_face_body<TF, PLAIN>(d, P, M, b, hs, fl, u, status);
     block_reduce_commit(tmin_u, 0, 0, status, b.dt_acc, b.counters, b.status);
 }
 
@@ -3154,7 +3160,7 @@ __device__ __forceinline__ void mhd_update_body(const DevMesh& d, const gelios_p
 #pragma unroll
                     for (int k = 0; k < kMhdFlux; k++) {
                         const double* f = fl + k * ng + g0;
-                        const double a0 = f[0], a1 = f[1], a2 = f[2], a3 = f[3];
+                        const double a0 = __ldcs(f), a1 = __ldcs(f + 1), a2 = __ldcs(f + 2), a3 = __ldcs(f + 3);
                         Pt[k] = (((Pt[k] + a0) + a1) + a2) + a3;
                     }
                 } else {
@@ -3647,14 +3653,25 @@ void launch_godunov_batch(const gelios_params& P, int n, const double* in, doubl
     godunov_batch_kernel<<<blocks_for(n, 2), 64, 0, s>>>(P, n, in, out);
 }
 namespace {
+// The plain interior group in the variant's shape, the other groups (a few
+// percent of the units, every branch) in one fixed shape after it.
 template <int BLOCK, int MINB>
 void mhd_faces_shape(const DevMesh& d, const gelios_params& P, const gelios_mhd_params& M, const StepBuffers& b,
                      const double* hcur, double* fl, cudaStream_t s) {
-    const int nb = blocks_for(d.n_units, BLOCK);
-    if (P.precision == GELIOS_PREC_FP32_FLUX)
-        mhd_face_kernel<float, BLOCK, MINB><<<nb, BLOCK, 0, s>>>(d, P, M, b, hcur, fl);
-    else
-        mhd_face_kernel<double, BLOCK, MINB><<<nb, BLOCK, 0, s>>>(d, P, M, b, hcur, fl);
+    const int n0 = d.u_c1, nr = d.n_units - d.u_c1;
+    const bool f32 = P.precision == GELIOS_PREC_FP32_FLUX;
+    if (n0 > 0) {
+        if (f32)
+            mhd_face_kernel<float, BLOCK, MINB, true><<<blocks_for(n0, BLOCK), BLOCK, 0, s>>>(d, P, M, b, hcur, fl);
+        else
+            mhd_face_kernel<double, BLOCK, MINB, true><<<blocks_for(n0, BLOCK), BLOCK, 0, s>>>(d, P, M, b, hcur, fl);
+    }
+    if (nr > 0) {
+        if (f32)
+            mhd_face_kernel<float, 128, 1, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, M, b, hcur, fl);
+        else
+            mhd_face_kernel<double, 128, 1, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, M, b, hcur, fl);
+    }
 }
 }  // namespace
 
@@ -3662,9 +3679,9 @@ const char* mhd_face_variant_name(int v) {
     static const char* names[kMhdFaceVariants] = {"128x3", "128x1", "128x4", "64x6", "64x3", "256x1"};
     return (v >= 0 && v < kMhdFaceVariants) ? names[v] : "?";
 }
-void launch_mhd_faces(const DevMesh& d, const gelios_params& P, const gelios_mhd_params& M, const StepBuffers& b,
-                      const double* hcur, double* fl, cudaStream_t s, int variant) {
-    if (d.n_units <= 0) return;
+int launch_mhd_faces(const DevMesh& d, const gelios_params& P, const gelios_mhd_params& M, const StepBuffers& b,
+                     const double* hcur, double* fl, cudaStream_t s, int variant) {
+    if (d.n_units <= 0) return 0;
     switch (variant) {
         case 1: mhd_faces_shape<128, 1>(d, P, M, b, hcur, fl, s); break;
         case 2: mhd_faces_shape<128, 4>(d, P, M, b, hcur, fl, s); break;
@@ -3673,6 +3690,7 @@ void launch_mhd_faces(const DevMesh& d, const gelios_params& P, const gelios_mhd
         case 5: mhd_faces_shape<256, 1>(d, P, M, b, hcur, fl, s); break;
         default: mhd_faces_shape<128, 3>(d, P, M, b, hcur, fl, s); break;
     }
+    return (d.u_c1 > 0 ? 1 : 0) + (d.n_units > d.u_c1 ? 1 : 0);
 }
 int launch_residual(const double* a, const double* b, int n, double* scratch, cudaStream_t s) {
     const int nb = n > 0 ? (blocks_for(n, 256) < 296 ? blocks_for(n, 256) : 296) : 1;

@@ -206,8 +206,9 @@ constexpr int kMhdFluxRows = 13;
 // the fastest for a grid.  All shapes give the same bits.
 constexpr int kMhdFaceVariants = 6;
 const char* mhd_face_variant_name(int v);
-void launch_mhd_faces(const DevMesh& d, const gelios_params& P, const gelios_mhd_params& M, const StepBuffers& b,
-                      const double* hcur, double* fl, cudaStream_t s, int variant = 0);
+// Returns the number of launches (the plain interior group, then the rest).
+int launch_mhd_faces(const DevMesh& d, const gelios_params& P, const gelios_mhd_params& M, const StepBuffers& b,
+                     const double* hcur, double* fl, cudaStream_t s, int variant = 0);
 void launch_mhd_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
                        const double* src, const double* hcur, double* hnxt, cudaStream_t s);
 // ---- batched MHD step: many instances, one launch per phase
