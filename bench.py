@@ -563,6 +563,9 @@ def main():
     ap.add_argument("--workload", default="mk2_1m", choices=sorted(WORKLOADS) + ["warm_start"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32flux"])
+    # moving-grid / MHD forms: use this variant of the face units + update instead of autotuning
+    # (the autotuner times kernels alone; under a profiler its choice would differ from the plain run's)
+    ap.add_argument("--variant", type=int, default=None)
     # sweep64 only: one context and captured step graph per instance, autotuned and enqueued together
     # (default), or gelios_batch: one launch per phase over the instances of each of --sweep-groups groups
     ap.add_argument("--sweep-mode", default="contexts", choices=["contexts", "batched"])
@@ -646,7 +649,10 @@ def main():
     tuned = None
     fcode = {"mk2": N.FORM_MK2, "k5": N.FORM_5_KOMPONENT, "mhd": N.FORM_MHD_PUI,
              "inner": N.FORM_INNER_MK2}.get(form, N.FORM_STATIONARY)
-    if form in ("mhd", "mk2"):  # launch shape of the face kernel picked on this grid (the library's autotuner)
+    if form in ("mhd", "mk2") and args.variant is not None:  # a fixed arrangement (profiling runs)
+        S.set_variant(fcode, args.variant)
+        tuned = {"variant": args.variant, "fixed": True}
+    elif form in ("mhd", "mk2"):  # launch shape of the face kernel picked on this grid (the library's autotuner)
         v, tms = S.autotune(fcode, reps=3)
         tuned = {"variant": v, "face_kernel_ms": tms}
     stream = torch.cuda.ExternalStream(S.stream_handle(), device=device)
