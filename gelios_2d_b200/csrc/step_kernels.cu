@@ -916,12 +916,15 @@ struct RecUnit {
     double dist, distn;        // owner / other centroid to the face centre, -1 if not updated
 };
 
-// PLAIN: a unit of the plain interior group [0, u_c1) (a Usualy face, neither
-// cell C_1, not tracked): the boundary, radial and tracked branches drop out
-// at compile time.
-template <bool PLAIN = false>
+// GROUP: the unit group the caller knows the unit to be in, so that branches
+// drop out at compile time: kPlainGroup [0, u_c1) (a Usualy face, neither
+// cell C_1, not tracked), kC1Group [u_c1, u_tr0) (a Usualy face with a C_1
+// side, not tracked), kAnyGroup (no assumption).
+constexpr int kPlainGroup = 0, kC1Group = 1, kAnyGroup = 2;
+template <int GROUP = kAnyGroup>
 __device__ __forceinline__ void mk2_recon_unit(const DevMesh& d, const gelios_params& P, const StepBuffers& b, int u,
                                                RecUnit& r, int* status) {
+    constexpr bool PLAIN = GROUP == kPlainGroup, USUALY = GROUP != kAnyGroup;
     const int K = d.u_cell[u], nb = d.u_nb[u];
     const uint32_t info = d.u_info[u];
     const double x = b.cx[K], y = b.cy[K];
@@ -950,14 +953,14 @@ __device__ __forceinline__ void mk2_recon_unit(const DevMesh& d, const gelios_pa
         r.distn = procN ? sqrt(sq(x3 - x2) + sq(y3 - y2)) : -1.0;
     }
     if (!(procK || procN)) return;
-    const int ft = PLAIN ? static_cast<int>(G_USUALY) : static_cast<int>(info & SI_TYPE_MASK);
+    const int ft = USUALY ? static_cast<int>(G_USUALY) : static_cast<int>(info & SI_TYPE_MASK);
     const uint32_t cf = (info >> UI_CF_OWN) & (PLAIN ? (15u & ~CF_C1) : 15u);
     const double g2 = 2 * P.gamma;
     const St5 par1 = load_state(b.cur, K);
     St5 par11 = par1;
     St5 par2 = get_par(P, ft, par1, b.cur, nb, x2, y2);
     const double dis = sqrt(sq(x2) + sq(y2));
-    const bool tracked = !PLAIN && (info & SI_GOD) != 0;
+    const bool tracked = !USUALY && (info & SI_GOD) != 0;
     const uint32_t nbf = (info >> UI_CF_NB) & (PLAIN ? (15u & ~CF_C1) : 15u);
     const bool radial = ((cf & CF_C1) && (ft == G_USUALY || ft == G_AXIS)) || ft == G_INNER_SPHERE ||
                         (ft == G_USUALY && (nbf & CF_C1));
@@ -1119,22 +1122,21 @@ __global__ void __launch_bounds__(32) mk2_flux_tracked_kernel(DevMesh d, gelios_
 // pass: the reconstructed states stay in registers (no per-unit scratch);
 // F.S to the owner's flux slot and -F.S to the twin's.  Index i is remapped
 // around the tracked range [u_tr0, u_tr1).
-// PLAIN: the plain interior group [0, u_c1) only (compiled without the
-// boundary, radial and tracked branches); otherwise the units [u_c1, u_tr0)
-// and [u_tr1, n_units).
-template <typename TF, int MINB, bool PLAIN>
+// One launch per unit group (compiled without the branches the group cannot
+// take): kPlainGroup [0, u_c1), kC1Group [u_c1, u_tr0), kAnyGroup the
+// one-sided units [u_tr1, n_units).
+template <typename TF, int MINB, int GROUP>
 __global__ void __launch_bounds__(128, MINB) mk2_face_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                            double* __restrict__ fl, int n_launch) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double tmin_u = __longlong_as_double(0x7ff0000000000000LL);
     int status = 0;
     if (i < n_launch) {
-        const int j = PLAIN ? i : d.u_c1 + i;
-        const int u = (PLAIN || j < d.u_tr0) ? j : j + (d.u_tr1 - d.u_tr0);
+        const int u = GROUP == kPlainGroup ? i : GROUP == kC1Group ? d.u_c1 + i : d.u_tr1 + i;
         RecUnit r;
         r.a = St5{};
         r.o = St5{};
-        mk2_recon_unit<PLAIN>(d, P, b, u, r, &status);
+        mk2_recon_unit<GROUP>(d, P, b, u, r, &status);
         mk2_flux_unit<TF, false>(d, P, b, u, r, fl, nullptr, tmin_u, &status);
     }
     block_reduce_commit(tmin_u, 0, 0, status, b.dt_acc, b.counters, b.status);
@@ -3531,11 +3533,12 @@ static cudaError_t launch_tiles_v(const DevMesh& d, const gelios_params& P, cons
 template <typename TF, int MINB>
 static void launch_faces_v(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
                            cudaStream_t s) {
-    // the plain interior group with the lean kernel, the other groups after it
-    const int n0 = d.u_c1;
-    const int nr = d.n_units - (d.u_tr1 - d.u_tr0) - n0;
-    if (n0 > 0) mk2_face_kernel<TF, MINB, true><<<blocks_for(n0, 128), 128, 0, s>>>(d, P, b, fl, n0);
-    if (nr > 0) mk2_face_kernel<TF, 4, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, b, fl, nr);
+    // one launch per unit group, each compiled for its group; the plain
+    // interior group in the variant's shape
+    const int n0 = d.u_c1, n1 = d.u_tr0 - d.u_c1, n3 = d.n_units - d.u_tr1;
+    if (n0 > 0) mk2_face_kernel<TF, MINB, kPlainGroup><<<blocks_for(n0, 128), 128, 0, s>>>(d, P, b, fl, n0);
+    if (n1 > 0) mk2_face_kernel<TF, 6, kC1Group><<<blocks_for(n1, 128), 128, 0, s>>>(d, P, b, fl, n1);
+    if (n3 > 0) mk2_face_kernel<TF, 4, kAnyGroup><<<blocks_for(n3, 128), 128, 0, s>>>(d, P, b, fl, n3);
 }
 template <typename TF, int MINB>
 static void launch_faces2_v(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
@@ -3580,8 +3583,8 @@ const char* mk2_variant_name(int v) {
     return (v >= 0 && v < kMk2Variants) ? names[v] : "?";
 }
 int mk2_variant_launches(int v, int part) {
-    const bool tiles = v >= 4 && v < 8, two = v < 4;  // face variants 0-3: plain group + the rest
-    return part == 1 ? (tiles ? 0 : (two ? 2 : 1)) : 1;
+    const bool tiles = v >= 4 && v < 8, groups = v < 4;  // face variants 0-3: one launch per unit group
+    return part == 1 ? (tiles ? 0 : (groups ? 3 : 1)) : 1;
 }
 cudaError_t launch_mk2_cells(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const TileView& t,
                              double* fl, const double* aux, cudaStream_t s, int variant, int part) {
