@@ -9,6 +9,13 @@
 //                         (backward, data) and (dZ^T).(H^T)^T (backward,
 //                         weights; split over K into partial tiles that
 //                         splitk_reduce_kernel adds in a fixed order)
+//   gemm_tma_kernel       the same GEMM with the operand tiles brought in by
+//                         the tensor memory accelerator (one thread issues
+//                         cp.async.bulk.tensor per tile; no cluster
+//                         multicast) and, for the forward layers, bias +
+//                         GELU applied to the accumulator as it leaves
+//                         tensor memory; used whenever both operands' rows
+//                         are 16-byte aligned
 //   transpose_bf16_kernel the transposed operands of the backward GEMMs
 //   features_kernel       network inputs: the raw inputs, then sin / cos of
 //                         2^f pi s of the last two (the cell position), bf16
@@ -22,6 +29,7 @@
 //   adam_kernel           Adam on the fp32 master weights, bf16 copy refreshed
 // GELU(x) = x Phi(x) = x/2 (1 + erf(x / sqrt 2)) through CUDA's erff; its
 // derivative Phi(x) + x phi(x) through erff and expf.
+#include <cuda.h>  // CUtensorMap and its enums (the encoder is looked up at run time)
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -280,6 +288,193 @@ __device__ __forceinline__ float gelu_grad(float x) {
     return cdf + x * pdf;
 }
 
+// ---- the GEMM with TMA staging
+// Per stage and operand, eight boxes of 8 k x 128 rows (16 bytes x 128
+// rows), one per 8-wide k chunk; a box lands as 128 rows of 16 bytes, so the
+// stage is the canonical K-major layout without swizzle with the k-chunk
+// stride (leading byte offset) 2048 and the 8-row stride (stride byte offset)
+// 128.  Thread 0 issues the loads (mbarrier expect_tx / complete_tx per
+// stage), waits for each stage, issues its four MMAs and commits them to the
+// stage's "empty" mbarrier before refilling it.  Out-of-range rows and k are
+// zero-filled by the TMA unit.  EPI 0: C (fp32) as gemm_tc_kernel writes it;
+// EPI 1: z = C + bias per column, then Z = z, H = bf16(act(z)), Hf = act(z)
+// (each output optional, rows of N).
+constexpr uint32_t TM_LBO = 2048, TM_SBO = 128;
+__device__ __forceinline__ uint64_t tm_desc(uint32_t saddr) {
+    return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (static_cast<uint64_t>((TM_LBO >> 4) & 0x3FFFu) << 16) |
+           (static_cast<uint64_t>((TM_SBO >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::
+            "r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+struct GemmEpilogue {
+    const float* bias = nullptr;
+    float* Z = nullptr;
+    __nv_bfloat16* H = nullptr;
+    float* Hf = nullptr;
+    int act = 0;
+};
+
+template <int EPI>
+__global__ void __launch_bounds__(TC_THREADS) gemm_tma_kernel(const __grid_constant__ CUtensorMap tmA,
+                                                            const __grid_constant__ CUtensorMap tmB, int M, int N,
+                                                            int K, int kc, float* __restrict__ C, int64_t ldc,
+                                                            int64_t c_split, GemmEpilogue ep, int* __restrict__ status) {
+    extern __shared__ __align__(1024) uint8_t tc_smem[];
+    __shared__ uint64_t full[TC_STAGES], empty[TC_STAGES];
+    __shared__ uint32_t tmem_slot;
+    uint8_t* sA0 = tc_smem;
+    uint8_t* sB0 = tc_smem + TC_STAGES * TC_TILE;
+    const int m0 = blockIdx.y * TC_BM, n0 = blockIdx.x * TC_BN;
+    const int kb = blockIdx.z * kc, ke = min(K, kb + kc);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(TC_BN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < TC_STAGES; i++) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+    const int nk = ke > kb ? (ke - kb + TC_BK - 1) / TC_BK : 0;
+    bool ok = true;
+    if (threadIdx.x == 0 && nk > 0) {
+        auto load = [&](int j) {
+            const int st = j % TC_STAGES;
+            mbar_expect_tx(&full[st], 2u * TC_TILE);
+            const uint32_t a = smem_u32(sA0 + st * TC_TILE), b = smem_u32(sB0 + st * TC_TILE);
+            const int k0 = kb + j * TC_BK;
+#pragma unroll
+            for (int q = 0; q < TC_BK / 8; q++) {
+                tma_load_2d(a + q * TM_LBO, &tmA, k0 + 8 * q, m0, &full[st]);
+                tma_load_2d(b + q * TM_LBO, &tmB, k0 + 8 * q, n0, &full[st]);
+            }
+        };
+        for (int j = 0; j < TC_STAGES && j < nk; j++) load(j);
+        for (int it = 0; it < nk; it++) {
+            const int st = it % TC_STAGES;
+            const unsigned ph = (it / TC_STAGES) & 1;
+            if (!mbar_wait(&full[st], ph)) ok = false;
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(sA0 + st * TC_TILE), b0 = smem_u32(sB0 + st * TC_TILE);
+#pragma unroll
+            for (int k = 0; k < TC_BK / 16; k++) {
+                const uint64_t ad = tm_desc(a0 + k * 2 * TM_LBO), bd = tm_desc(b0 + k * 2 * TM_LBO);
+                const uint32_t acc = (it > 0 || k > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(tmem),
+                    "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             smem_u32(&empty[st]))
+                         : "memory");
+            if (it + TC_STAGES < nk) {
+                // the stage is free once its MMAs have read it
+                if (!mbar_wait(&empty[st], ph)) ok = false;
+                load(it + TC_STAGES);
+            }
+        }
+    }
+    __syncwarp();
+    if (nk > 0 && !mbar_wait(&empty[(nk - 1) % TC_STAGES], ((nk - 1) / TC_STAGES) & 1)) ok = false;
+    tc_fence_after();
+    const int64_t row = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < TC_BN; c0 += 16) {
+        uint32_t v[16];
+        if (nk > 0) {
+            const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0);
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];\n"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                  "=r"(v[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        } else {
+#pragma unroll
+            for (int j = 0; j < 16; j++) v[j] = 0u;
+        }
+        if (row >= M) continue;
+        const int col0 = n0 + c0;
+        if (EPI == 0) {
+            float* dst = C + blockIdx.z * c_split + row * ldc + col0;
+            if (col0 + 16 <= N && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+#pragma unroll
+                for (int j = 0; j < 16; j += 4)
+                    *reinterpret_cast<float4*>(dst + j) = make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]),
+                                                                      __uint_as_float(v[j + 2]), __uint_as_float(v[j + 3]));
+            } else {
+#pragma unroll
+                for (int j = 0; j < 16; j++)
+                    if (col0 + j < N) dst[j] = __uint_as_float(v[j]);
+            }
+        } else {
+            float z[16], h[16];
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+                z[j] = col0 + j < N ? __uint_as_float(v[j]) + ep.bias[col0 + j] : 0.f;
+                h[j] = ep.act ? gelu(z[j]) : z[j];
+            }
+            const int64_t o = row * N + col0;
+            const bool full16 = col0 + 16 <= N && (N & 7) == 0;
+            if (ep.Z) {
+                if (full16 && (N & 3) == 0) {
+#pragma unroll
+                    for (int j = 0; j < 16; j += 4)
+                        *reinterpret_cast<float4*>(ep.Z + o + j) = make_float4(z[j], z[j + 1], z[j + 2], z[j + 3]);
+                } else {
+                    for (int j = 0; j < 16; j++)
+                        if (col0 + j < N) ep.Z[o + j] = z[j];
+                }
+            }
+            if (ep.Hf) {
+                for (int j = 0; j < 16; j++)
+                    if (col0 + j < N) ep.Hf[o + j] = h[j];
+            }
+            if (ep.H) {
+                if (full16) {
+                    __align__(16) __nv_bfloat16 hb[16];
+#pragma unroll
+                    for (int j = 0; j < 16; j++) hb[j] = __float2bfloat16(h[j]);
+                    *reinterpret_cast<uint4*>(ep.H + o) = *reinterpret_cast<const uint4*>(hb);
+                    *reinterpret_cast<uint4*>(ep.H + o + 8) = *reinterpret_cast<const uint4*>(hb + 8);
+                } else {
+                    for (int j = 0; j < 16; j++)
+                        if (col0 + j < N) ep.H[o + j] = __float2bfloat16(h[j]);
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TC_BN) : "memory");
+    }
+    if (!ok) atomicOr(status, 1);
+}
+
 __device__ __forceinline__ uint64_t mix64(uint64_t z) {
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
     z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
@@ -459,6 +654,63 @@ void launch_tc(dim3 grid, int M, int N, int K, int kc, const __nv_bfloat16* A, i
     gemm_tc_kernel<AV, BV><<<grid, TC_THREADS, TC_SMEM, s>>>(M, N, K, kc, A, lda, B, ldb, C, ldc, c_split, st);
 }
 
+// cuTensorMapEncodeTiled, looked up in the driver once (no link against the
+// driver library); null where the driver does not offer it
+using TensorMapEncode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                     const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                     CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+TensorMapEncode tensor_map_encoder() {
+    static TensorMapEncode fn = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        looked = true;
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<TensorMapEncode>(f);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// The tensor map of a k-contiguous bf16 operand of `rows` rows of `ld`
+// elements, K of them used: boxes of 8 k x 128 rows, zero fill outside.
+bool operand_map(CUtensorMap* map, const __nv_bfloat16* X, int64_t ld, int rows, int K) {
+    const TensorMapEncode enc = tensor_map_encoder();
+    if (!enc || rows <= 0 || K <= 0) return false;
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(K), static_cast<cuuint64_t>(rows)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld) * 2};
+    const cuuint32_t box[2] = {8, TC_BM};
+    const cuuint32_t estr[2] = {1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(X), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The TMA GEMM; false (nothing launched) where an operand cannot be
+// described by a tensor map (rows not 16-byte aligned) or the driver offers
+// no encoder: the caller then uses gemm_tc_kernel.
+template <int EPI>
+bool launch_tma(dim3 grid, int M, int N, int K, int kc, const __nv_bfloat16* A, int64_t lda, const __nv_bfloat16* B,
+                int64_t ldb, float* C, int64_t ldc, int64_t c_split, const GemmEpilogue& ep, cudaStream_t s) {
+    if (!vec_ok(A, lda) || !vec_ok(B, ldb)) return false;
+    CUtensorMap ma, mb;
+    if (!operand_map(&ma, A, lda, M, K) || !operand_map(&mb, B, ldb, N, K)) return false;
+    static bool attr[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !attr[dev]) {
+        cudaFuncSetAttribute(gemm_tma_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+        if (dev >= 0 && dev < 64) attr[dev] = true;
+    }
+    int* st = nullptr;
+    cudaGetSymbolAddress(reinterpret_cast<void**>(&st), g_gemm_status);
+    gemm_tma_kernel<EPI><<<grid, TC_THREADS, TC_SMEM, s>>>(ma, mb, M, N, K, kc, C, ldc, c_split, ep, st);
+    return true;
+}
+
 // K slice of a GEMM split `splits` ways (a multiple of the K stage)
 inline int tc_split_len(int K, int splits) {
     int kc = (K + splits - 1) / splits;
@@ -471,6 +723,7 @@ void gemm(int M, int N, int K, const __nv_bfloat16* A, int64_t lda, const __nv_b
     if (M <= 0 || N <= 0) return;
     const int kc = tc_split_len(K, splits);
     dim3 grid(blocks(N, TC_BN), blocks(M, TC_BM), split_count(K, kc));
+    if (launch_tma<0>(grid, M, N, K, kc, A, lda, B, ldb, C, ldc, c_split, GemmEpilogue{}, s)) return;
     const bool av = vec_ok(A, lda), bv = vec_ok(B, ldb);
     if (av && bv)
         launch_tc<true, true>(grid, M, N, K, kc, A, lda, B, ldb, C, ldc, c_split, s);
@@ -548,12 +801,23 @@ void forward(gelios_mlp* n, int M) {
     const __nv_bfloat16* wb = n->wb.as<__nv_bfloat16>();
     for (int l = 0; l < n->layers(); l++) {
         const int di = n->din[l], dO = n->dout[l];
-        gemm(M, dO, di, n->h[l].as<__nv_bfloat16>(), di, wb + n->w_off[l], di, n->c.as<float>(), dO, s);
-        const int64_t e = static_cast<int64_t>(M) * dO;
         const bool last = l == n->layers() - 1;
-        bias_act_kernel<<<blocks(e, 256), 256, 0, s>>>(
-            M, dO, n->c.as<float>(), n->w32.as<float>() + n->b_off[l], last ? nullptr : n->z[l].as<float>(),
-            last ? nullptr : n->h[l + 1].as<__nv_bfloat16>(), last ? n->y.as<float>() : nullptr, last ? 0 : 1);
+        GemmEpilogue ep;
+        ep.bias = n->w32.as<float>() + n->b_off[l];
+        ep.Z = last ? nullptr : n->z[l].as<float>();
+        ep.H = last ? nullptr : n->h[l + 1].as<__nv_bfloat16>();
+        ep.Hf = last ? n->y.as<float>() : nullptr;
+        ep.act = last ? 0 : 1;
+        // bias and activation applied as the accumulator leaves tensor memory
+        // (TMA path), or by bias_act_kernel after the GEMM
+        const __nv_bfloat16* A = n->h[l].as<__nv_bfloat16>();
+        dim3 grid(blocks(dO, TC_BN), blocks(M, TC_BM), 1);
+        if (M > 0 && launch_tma<1>(grid, M, dO, di, tc_split_len(di, 1), A, di, wb + n->w_off[l], di, nullptr, 0, 0,
+                                   ep, s))
+            continue;
+        gemm(M, dO, di, A, di, wb + n->w_off[l], di, n->c.as<float>(), dO, s);
+        const int64_t e = static_cast<int64_t>(M) * dO;
+        bias_act_kernel<<<blocks(e, 256), 256, 0, s>>>(M, dO, n->c.as<float>(), ep.bias, ep.Z, ep.H, ep.Hf, ep.act);
     }
 }
 
@@ -792,5 +1056,61 @@ extern "C" int gelios_mlp_gemm_bf16(int M, int N, int K, const void* A, int64_t 
     MLP_TRY(cudaGetLastError());
     MLP_TRY(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
     if (!gemm_status_ok()) return cuda_fail(cudaErrorLaunchTimeout);
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_mlp_time_layer(int M, int N, int K, int reps, double* ms) {
+    if (M <= 0 || N <= 0 || K <= 0 || reps < 1 || !ms) return fail("gelios_mlp_time_layer: bad arguments");
+    const int64_t lda = pad8(K);
+    Buf A, B, bias, Z, H;
+    if (!A.alloc(static_cast<size_t>(M) * lda * 2) || !B.alloc(static_cast<size_t>(N) * lda * 2) ||
+        !bias.alloc(static_cast<size_t>(N) * 4) || !Z.alloc(static_cast<size_t>(M) * N * 4) ||
+        !H.alloc(static_cast<size_t>(M) * N * 2))
+        return cuda_fail(cudaErrorMemoryAllocation);
+    cudaStream_t s = nullptr;
+    MLP_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    std::unique_ptr<CUstream_st, void (*)(cudaStream_t)> guard(s, [](cudaStream_t x) { cudaStreamDestroy(x); });
+    // seeded operands (a fixed hash of the index, scaled like a trained layer)
+    {
+        std::vector<__nv_bfloat16> ha(static_cast<size_t>(M) * lda), hb(static_cast<size_t>(N) * lda);
+        std::vector<float> hbias(N);
+        auto val = [](uint64_t i) {
+            uint64_t z = i * 0x9E3779B97F4A7C15ULL;
+            z = (z ^ (z >> 31)) * 0xBF58476D1CE4E5B9ULL;
+            return static_cast<float>((z >> 40) & 0xFFFF) / 65536.f - 0.5f;
+        };
+        for (size_t i = 0; i < ha.size(); i++) ha[i] = __float2bfloat16(val(i));
+        for (size_t i = 0; i < hb.size(); i++) hb[i] = __float2bfloat16(0.1f * val(i + ha.size()));
+        for (int i = 0; i < N; i++) hbias[i] = 0.01f * val(i + 7);
+        MLP_TRY(cudaMemcpyAsync(A.p, ha.data(), ha.size() * 2, cudaMemcpyHostToDevice, s));
+        MLP_TRY(cudaMemcpyAsync(B.p, hb.data(), hb.size() * 2, cudaMemcpyHostToDevice, s));
+        MLP_TRY(cudaMemcpyAsync(bias.p, hbias.data(), hbias.size() * 4, cudaMemcpyHostToDevice, s));
+    }
+    GemmEpilogue ep;
+    ep.bias = bias.as<float>();
+    ep.Z = Z.as<float>();
+    ep.H = H.as<__nv_bfloat16>();
+    ep.act = 1;
+    const dim3 grid(blocks(N, TC_BN), blocks(M, TC_BM), 1);
+    const int kc = tc_split_len(K, 1);
+    auto layer = [&]() {
+        return launch_tma<1>(grid, M, N, K, kc, A.as<__nv_bfloat16>(), lda, B.as<__nv_bfloat16>(), lda, nullptr, 0, 0,
+                             ep, s);
+    };
+    if (!layer()) return fail("gelios_mlp_time_layer: no tensor-map encoder in this driver");
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    MLP_TRY(cudaEventCreate(&e0));
+    MLP_TRY(cudaEventCreate(&e1));
+    MLP_TRY(cudaEventRecord(e0, s));
+    for (int r = 0; r < reps; r++) layer();
+    MLP_TRY(cudaEventRecord(e1, s));
+    MLP_TRY(cudaEventSynchronize(e1));
+    float t = 0.f;
+    MLP_TRY(cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    MLP_TRY(cudaGetLastError());
+    if (!gemm_status_ok()) return cuda_fail(cudaErrorLaunchTimeout);
+    *ms = static_cast<double>(t) / reps;
     return GELIOS_OK;
 }

@@ -111,6 +111,21 @@ def test_gemm_bf16_against_float64(shape):
 
 
 @pytest.mark.gpu
+def test_hidden_layer_timing_runs():
+    """gelios_mlp_time_layer: the TMA-staged GEMM with its bias + GELU
+    epilogue on the 8192 x 256 x 256 hidden layer of the warm-start network."""
+    import ctypes as C
+
+    from gelios_2d_b200 import _native as N
+
+    ms = C.c_double()
+    N.check(N.lib().gelios_mlp_time_layer(8192, 256, 256, 20, C.byref(ms)), "gelios_mlp_time_layer")
+    assert 0.0 < ms.value < 1.0
+    print(f"hidden layer 8192x256x256: {ms.value * 1e3:.2f} us, "
+          f"{2 * 8192 * 256 * 256 / (ms.value * 1e-3) / 1e12:.1f} TFLOP/s")
+
+
+@pytest.mark.gpu
 def test_device_gradients_match_the_float64_restatement():
     net = W.Mlp(7, 6, 64, 3, 5, 2048)
     try:
