@@ -1607,7 +1607,7 @@ extern "C" int gelios_autotune(gelios_ctx* ctx, int form, int reps, int32_t* var
         out = static_cast<double>(t) / reps;
         return err;
     };
-    const int nv = mhd ? kMhdFaceVariants : kMk2Variants;
+    const int nv = mhd ? kMhdFaceVariants : kMk2TunedVariants;
     cudaError_t err = cudaSuccess;
     for (int v = 0; v < nv && err == cudaSuccess; v++) {
         double m = 0.0;

@@ -1142,141 +1142,6 @@ __global__ void __launch_bounds__(128, MINB) mk2_face_kernel(DevMesh d, gelios_p
     block_reduce_commit(tmin_u, 0, 0, status, b.dt_acc, b.counters, b.status);
 }
 
-// Two lanes per face unit (lanes 2j, 2j+1 of a warp): on an interior
-// (Usualy) face each lane reconstructs one side (lane 0 the owner's, lane 1
-// the neighbour's: the same calls as mk2_recon_unit), the lanes swap their
-// states, both evaluate the same HLL flux and each writes its own side's slot
-// and CFL candidate.  Boundary faces (one side only) run on the even lane.
-// Half the gathers and registers of a reconstruction per thread, twice the
-// threads in flight.
-template <typename TF, int MINB>
-__global__ void __launch_bounds__(128, MINB) mk2_face2_kernel(DevMesh d, gelios_params P, StepBuffers b,
-                                                            double* __restrict__ fl, int n_launch) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = t >> 1, side = t & 1;
-    double tmin_u = __longlong_as_double(0x7ff0000000000000LL);
-    int status = 0;
-    const bool active = i < n_launch;
-    RecUnit r;
-    r.a = St5{};
-    r.o = St5{};
-    r.dist = r.distn = -1.0;
-    bool usualy = false;
-    int u = 0;
-    if (active) {
-        u = i < d.u_tr0 ? i : i + (d.u_tr1 - d.u_tr0);
-        const int K = d.u_cell[u], nb = d.u_nb[u];
-        const uint32_t info = d.u_info[u];
-        const double x = b.cx[K], y = b.cy[K];
-        const bool procK = !(sqrt(sq(x) + sq(y)) < P.R11);
-        double x3 = 0.0, y3 = 0.0;
-        bool procN = false;
-        if (nb >= 0) {
-            x3 = b.cx[nb];
-            y3 = b.cy[nb];
-            procN = !(sqrt(sq(x3) + sq(y3)) < P.R11);
-        }
-        const int A = d.u_A[u], B = d.u_B[u];
-        const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
-        const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
-        {
-            double t1 = xb - xa, t2 = yb - ya;
-            const double nn = sqrt(sq(t1) + sq(t2));
-            t1 = t1 / nn;
-            t2 = t2 / nn;
-            r.n1 = t2;
-            r.n2 = -t1;
-            r.S = sqrt(sq(xb - xa) + sq(yb - ya)) * (ya + yb) * 0.5;
-            r.x2 = x2;
-            r.y2 = y2;
-            r.dist = procK ? sqrt(sq(x - x2) + sq(y - y2)) : -1.0;
-            r.distn = procN ? sqrt(sq(x3 - x2) + sq(y3 - y2)) : -1.0;
-        }
-        const int ft = info & SI_TYPE_MASK;
-        usualy = ft == G_USUALY;
-        if (procK || procN) {
-            const uint32_t cf = (info >> UI_CF_OWN) & 15u;
-            const uint32_t nbf = (info >> UI_CF_NB) & 15u;
-            const double g2 = 2 * P.gamma;
-            const double dis = sqrt(sq(x2) + sq(y2));
-            const bool tracked = (info & SI_GOD) != 0;
-            const bool radial = ((cf & CF_C1) && (ft == G_USUALY || ft == G_AXIS)) || ft == G_INNER_SPHERE ||
-                                (ft == G_USUALY && (nbf & CF_C1));
-            const double pdis = radial ? pow2g(dis, g2) : 1.0;
-            if (usualy) {
-                if (side == 0)
-                    r.a = mk2_usualy_side(b.cur, b.cx, b.cy, b.rp, x2, y2, dis, pdis, load_state(b.cur, K), x, y,
-                                          b.rp[K], cf, nb, d.u_sd[u], tracked, &status);
-                else
-                    r.o = mk2_usualy_side(b.cur, b.cx, b.cy, b.rp, x2, y2, dis, pdis, load_state(b.cur, nb), x3, y3,
-                                          b.rp[nb], nbf, K, d.u_sd2[u], tracked, &status);
-            } else if (side == 0) {
-                const St5 par1 = load_state(b.cur, K);
-                St5 par11 = par1;
-                St5 par2 = get_par(P, ft, par1, b.cur, nb, x2, y2);
-                if (ft == G_INNER_SPHERE) {
-                    const double radius = sqrt(sq(x) + sq(y));
-                    par11.ro = par11.ro * sq(radius) / sq(dis);
-                    par11.Q = par11.Q * sq(radius) / sq(dis);
-                    par11.p = par11.p * (b.rp[K] / pdis);
-                } else if (ft == G_AXIS) {
-                    if (cf & CF_C1) {
-                        const double radius = sqrt(sq(x) + sq(y));
-                        par11.ro = par11.ro * sq(radius) / sq(dis);
-                        par11.Q = par11.Q * sq(radius) / sq(dis);
-                        par11.p = par11.p * (b.rp[K] / pdis);
-                        polar_perenos(x, y, x2, y2, par11.u, par11.v);
-                    } else {
-                        par11 = tvd_axis(b.cur, b.cx, b.cy, x2, y2, par1, x, y, d.u_sd[u]);
-                    }
-                    par2 = par11;
-                    par2.v = -par2.v;
-                }
-                r.a = par11;
-                r.o = par2;
-            }
-        }
-    }
-    // swap the reconstructed sides of an interior face between the two lanes
-    const St5 mine = side ? r.o : r.a;
-    St5 other;
-    other.ro = __shfl_xor_sync(0xffffffffu, mine.ro, 1);
-    other.p = __shfl_xor_sync(0xffffffffu, mine.p, 1);
-    other.u = __shfl_xor_sync(0xffffffffu, mine.u, 1);
-    other.v = __shfl_xor_sync(0xffffffffu, mine.v, 1);
-    other.Q = __shfl_xor_sync(0xffffffffu, mine.Q, 1);
-    if (active && usualy) {
-        if (side)
-            r.a = other;
-        else
-            r.o = other;
-    }
-    const bool procK = !(r.dist < 0.0), procN = !(r.distn < 0.0);
-    if (active && (procK || procN) && (side == 0 || usualy)) {
-        const size_t ng = d.n_slots;
-        const double dt = *b.dt_cur;
-        const uint32_t info = d.u_info[u];
-        const int A = d.u_A[u], B = d.u_B[u];
-        const double x4 = (d.X2[A] + d.X2[B]) / 2.0, y4 = (d.Y2[A] + d.Y2[B]) / 2.0;
-        const double W = ((x4 - r.x2) * r.n1 + (y4 - r.y2) * r.n2) / dt;
-        const bool np = (info & SI_NP) != 0;
-        FluxOut<double> F;
-        const double UU = hllc_flux<TF>(P.gamma, P.kurant, r.a, r.o, W, r.n1, r.n2, 1.0, 0, np, F);
-        const double S = r.S;
-        const double sg = side ? -1.0 : 1.0;
-        const int g = side ? d.u_twin[u] : d.u_slot[u];
-        if (g >= 0) {
-            __stcs(fl + 0 * ng + g, sg * (F.P0 * S));
-            __stcs(fl + 1 * ng + g, sg * (F.P1 * S));
-            __stcs(fl + 2 * ng + g, sg * (F.P2 * S));
-            __stcs(fl + 3 * ng + g, sg * (F.P3 * S));
-            __stcs(fl + 4 * ng + g, sg * (F.PQ * S));
-            if (side == 0 ? procK : procN) tmin_u = dmin_ref(tmin_u, P.kurant * (side ? r.distn : r.dist) / UU);
-        }
-    }
-    block_reduce_commit(tmin_u, 0, 0, status, b.dt_acc, b.counters, b.status);
-}
-
 // Star pressure of the exact Godunov problem of every tracked-face unit
 // (Solvers.cpp:1174-1305).  It depends on the reconstructed states and on
 // the face normal before the motion, not on the face speed, so it runs on a
@@ -3540,12 +3405,6 @@ static void launch_faces_v(const DevMesh& d, const gelios_params& P, const StepB
     if (n1 > 0) mk2_face_kernel<TF, 6, kC1Group><<<blocks_for(n1, 128), 128, 0, s>>>(d, P, b, fl, n1);
     if (n3 > 0) mk2_face_kernel<TF, 4, kAnyGroup><<<blocks_for(n3, 128), 128, 0, s>>>(d, P, b, fl, n3);
 }
-template <typename TF, int MINB>
-static void launch_faces2_v(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
-                            cudaStream_t s) {
-    const int nr = d.n_units - (d.u_tr1 - d.u_tr0);
-    if (nr > 0) mk2_face2_kernel<TF, MINB><<<blocks_for(2 * nr, 128), 128, 0, s>>>(d, P, b, fl, nr);
-}
 template <typename TF>
 static cudaError_t launch_cells_p(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const TileView& t,
                                   double* fl, const double* aux, cudaStream_t s, int variant, int part) {
@@ -3566,9 +3425,6 @@ static cudaError_t launch_cells_p(const DevMesh& d, const gelios_params& P, cons
         case 1: launch_faces_v<TF, 5>(d, P, b, fl, s); break;
         case 2: launch_faces_v<TF, 6>(d, P, b, fl, s); break;
         case 3: launch_faces_v<TF, 4>(d, P, b, fl, s); break;
-        case 8: launch_faces2_v<TF, 8>(d, P, b, fl, s); break;
-        case 9: launch_faces2_v<TF, 6>(d, P, b, fl, s); break;
-        case 10: launch_faces2_v<TF, 10>(d, P, b, fl, s); break;
         default: launch_faces_v<TF, 8>(d, P, b, fl, s); break;
     }
     return cudaGetLastError();
@@ -3577,9 +3433,7 @@ const char* mk2_variant_name(int v) {
     static const char* names[kMk2Variants] = {"faces 128x8 + update", "faces 128x5 + update",
                                               "faces 128x6 + update", "faces 128x4 + update",
                                               "tiles 256x3",          "tiles 256x2",
-                                              "tiles 128x5",          "tiles 128x4",
-                                              "faces2 128x8 + update", "faces2 128x6 + update",
-                                              "faces2 128x10 + update"};
+                                              "tiles 128x5",          "tiles 128x4"};
     return (v >= 0 && v < kMk2Variants) ? names[v] : "?";
 }
 int mk2_variant_launches(int v, int part) {

@@ -165,13 +165,14 @@ struct TileView {
 //                 launch of a lean instance) + mk2_update_kernel (slot sums,
 //                 update);
 //   variants 4-7  mk2_tile_kernel, one tile of cells per block, slot fluxes
-//                 in shared memory (256 x 3, 256 x 2, 128 x 5, 128 x 4);
-//   variants 8-10 mk2_face2_kernel (two lanes per face unit, one side each;
-//                 128 threads x 8, 6, 10 resident blocks) + mk2_update_kernel.
-// Variant 0 is the default; gelios_autotune picks the fastest for a grid.
-// All give the same bits.
+//                 in shared memory (256 x 3, 256 x 2, 128 x 5, 128 x 4).
+// Variant 0 is the default; gelios_autotune picks the fastest of the face-
+// kernel variants for a grid (kMk2TunedVariants; the tile kernel is slower in
+// the whole step, where the face kernel overlaps the side stream and the tile
+// kernel cannot, and is chosen only by hand).  All give the same bits.
 void launch_mk2_recon(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* rec, cudaStream_t s);
-constexpr int kMk2Variants = 11;
+constexpr int kMk2Variants = 8;
+constexpr int kMk2TunedVariants = 4;
 const char* mk2_variant_name(int v);
 // part 1: the face units of the face-kernel variants (reads the moved points
 // only); part 2: the cell update, or the whole tile kernel (also reads the

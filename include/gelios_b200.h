@@ -356,8 +356,9 @@ int gelios_mlp_time_layer(int M, int N, int K, int reps, double *ms);
  * blocks per SM, i.e. a register cap); the moving-grid form
  * (GELIOS_FORM_MK2) has as many variants of its face units + cell update:
  * a face kernel writing flux slots in global memory followed by an update
- * kernel, or one kernel per tile of cells with the slots in shared memory,
- * each in several launch shapes.  All give the same bits.
+ * kernel (variants 0-3), or one kernel per tile of cells with the slots in
+ * shared memory (4-7, slower in the whole step; gelios_autotune for this
+ * form times variants 0-3 only).  All give the same bits.
  * gelios_autotune times each shape on the context's grid and current state
  * (`reps` launches each, CUDA events on the context stream; only scratch
  * buffers are written, the state and the points are not touched), keeps the
