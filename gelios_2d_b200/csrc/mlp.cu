@@ -323,8 +323,12 @@ struct GemmEpilogue {
     int act = 0;
 };
 
+// 16 warps: warp w reads TMEM lanes 32 (w % 4) .. (its rows) and the
+// columns 32 (w / 4) .. +32 of the tile, so the epilogue runs on four times
+// the threads of the staging kernel.
+constexpr int TM_THREADS = 512;
 template <int EPI>
-__global__ void __launch_bounds__(TC_THREADS) gemm_tma_kernel(const __grid_constant__ CUtensorMap tmA,
+__global__ void __launch_bounds__(TM_THREADS) gemm_tma_kernel(const __grid_constant__ CUtensorMap tmA,
                                                             const __grid_constant__ CUtensorMap tmB, int M, int N,
                                                             int K, int kc, float* __restrict__ C, int64_t ldc,
                                                             int64_t c_split, GemmEpilogue ep, int* __restrict__ status) {
@@ -397,12 +401,13 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tma_kernel(const __grid_const
     __syncwarp();
     if (nk > 0 && !mbar_wait(&empty[(nk - 1) % TC_STAGES], ((nk - 1) / TC_STAGES) & 1)) ok = false;
     tc_fence_after();
-    const int64_t row = m0 + warp * 32 + lane;
+    const int wl = warp & 3, wc = warp >> 2;
+    const int64_t row = m0 + wl * 32 + lane;
 #pragma unroll 1
-    for (int c0 = 0; c0 < TC_BN; c0 += 16) {
+    for (int c0 = wc * 32; c0 < wc * 32 + 32; c0 += 16) {
         uint32_t v[16];
         if (nk > 0) {
-            const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0);
+            const uint32_t taddr = tmem + (static_cast<uint32_t>(wl * 32) << 16) + static_cast<uint32_t>(c0);
             asm volatile(
                 "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
                 "[%16];\n"
@@ -707,7 +712,7 @@ bool launch_tma(dim3 grid, int M, int N, int K, int kc, const __nv_bfloat16* A, 
     }
     int* st = nullptr;
     cudaGetSymbolAddress(reinterpret_cast<void**>(&st), g_gemm_status);
-    gemm_tma_kernel<EPI><<<grid, TC_THREADS, TC_SMEM, s>>>(ma, mb, M, N, K, kc, C, ldc, c_split, ep, st);
+    gemm_tma_kernel<EPI><<<grid, TM_THREADS, TC_SMEM, s>>>(ma, mb, M, N, K, kc, C, ldc, c_split, ep, st);
     return true;
 }
 
