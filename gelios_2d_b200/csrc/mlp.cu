@@ -299,9 +299,17 @@ __device__ __forceinline__ float gelu_grad(float x) {
 // zero-filled by the TMA unit.  EPI 0: C (fp32) as gemm_tc_kernel writes it;
 // EPI 1: z = C + bias per column, then Z = z, H = bf16(act(z)), Hf = act(z)
 // (each output optional, rows of N).
-constexpr uint32_t TM_LBO = 2048, TM_SBO = 128;
-__device__ __forceinline__ uint64_t tm_desc(uint32_t saddr) {
-    return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (static_cast<uint64_t>((TM_LBO >> 4) & 0x3FFFu) << 16) |
+// tile: TM_BN = 64 columns per CTA (256 CTAs for a 8192 x 256 layer, two
+// resident per SM: one's epilogue overlaps the other's loads); k-chunk
+// stride of the A stage 128 rows x 16 bytes, of the B stage 64 x 16 bytes
+constexpr int TM_BN = 64;
+constexpr uint32_t TM_LBO_A = TC_BM * 16, TM_LBO_B = TM_BN * 16, TM_SBO = 128;
+constexpr int TM_TILE_B = TM_BN * TC_BK * 2;
+constexpr int TM_SMEM = TC_STAGES * (TC_TILE + TM_TILE_B);
+constexpr uint32_t TM_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TM_BN >> 3) << 17) |
+                              ((uint32_t)(TC_BM >> 4) << 24);
+__device__ __forceinline__ uint64_t tm_desc(uint32_t saddr, uint32_t lbo) {
+    return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16) |
            (static_cast<uint64_t>((TM_SBO >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
@@ -324,11 +332,10 @@ struct GemmEpilogue {
 };
 
 // 16 warps: warp w reads TMEM lanes 32 (w % 4) .. (its rows) and the
-// columns 32 (w / 4) .. +32 of the tile, so the epilogue runs on four times
-// the threads of the staging kernel.
+// columns 16 (w / 4) .. +16 of the tile.
 constexpr int TM_THREADS = 512;
 template <int EPI>
-__global__ void __launch_bounds__(TM_THREADS) gemm_tma_kernel(const __grid_constant__ CUtensorMap tmA,
+__global__ void __launch_bounds__(TM_THREADS, 2) gemm_tma_kernel(const __grid_constant__ CUtensorMap tmA,
                                                             const __grid_constant__ CUtensorMap tmB, int M, int N,
                                                             int K, int kc, float* __restrict__ C, int64_t ldc,
                                                             int64_t c_split, GemmEpilogue ep, int* __restrict__ status) {
@@ -337,12 +344,12 @@ __global__ void __launch_bounds__(TM_THREADS) gemm_tma_kernel(const __grid_const
     __shared__ uint32_t tmem_slot;
     uint8_t* sA0 = tc_smem;
     uint8_t* sB0 = tc_smem + TC_STAGES * TC_TILE;
-    const int m0 = blockIdx.y * TC_BM, n0 = blockIdx.x * TC_BN;
+    const int m0 = blockIdx.y * TC_BM, n0 = blockIdx.x * TM_BN;
     const int kb = blockIdx.z * kc, ke = min(K, kb + kc);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_slot)),
-                     "r"(TC_BN)
+                     "r"(TM_BN)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
     }
@@ -362,13 +369,13 @@ __global__ void __launch_bounds__(TM_THREADS) gemm_tma_kernel(const __grid_const
     if (threadIdx.x == 0 && nk > 0) {
         auto load = [&](int j) {
             const int st = j % TC_STAGES;
-            mbar_expect_tx(&full[st], 2u * TC_TILE);
-            const uint32_t a = smem_u32(sA0 + st * TC_TILE), b = smem_u32(sB0 + st * TC_TILE);
+            mbar_expect_tx(&full[st], static_cast<uint32_t>(TC_TILE + TM_TILE_B));
+            const uint32_t a = smem_u32(sA0 + st * TC_TILE), b = smem_u32(sB0 + st * TM_TILE_B);
             const int k0 = kb + j * TC_BK;
 #pragma unroll
             for (int q = 0; q < TC_BK / 8; q++) {
-                tma_load_2d(a + q * TM_LBO, &tmA, k0 + 8 * q, m0, &full[st]);
-                tma_load_2d(b + q * TM_LBO, &tmB, k0 + 8 * q, n0, &full[st]);
+                tma_load_2d(a + q * TM_LBO_A, &tmA, k0 + 8 * q, m0, &full[st]);
+                tma_load_2d(b + q * TM_LBO_B, &tmB, k0 + 8 * q, n0, &full[st]);
             }
         };
         for (int j = 0; j < TC_STAGES && j < nk; j++) load(j);
@@ -377,15 +384,16 @@ __global__ void __launch_bounds__(TM_THREADS) gemm_tma_kernel(const __grid_const
             const unsigned ph = (it / TC_STAGES) & 1;
             if (!mbar_wait(&full[st], ph)) ok = false;
             tc_fence_after();
-            const uint32_t a0 = smem_u32(sA0 + st * TC_TILE), b0 = smem_u32(sB0 + st * TC_TILE);
+            const uint32_t a0 = smem_u32(sA0 + st * TC_TILE), b0 = smem_u32(sB0 + st * TM_TILE_B);
 #pragma unroll
             for (int k = 0; k < TC_BK / 16; k++) {
-                const uint64_t ad = tm_desc(a0 + k * 2 * TM_LBO), bd = tm_desc(b0 + k * 2 * TM_LBO);
+                const uint64_t ad = tm_desc(a0 + k * 2 * TM_LBO_A, TM_LBO_A);
+                const uint64_t bd = tm_desc(b0 + k * 2 * TM_LBO_B, TM_LBO_B);
                 const uint32_t acc = (it > 0 || k > 0) ? 1u : 0u;
                 asm volatile(
                     "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
                     " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(tmem),
-                    "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                    "l"(ad), "l"(bd), "r"(TM_IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
                     : "memory");
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
@@ -403,8 +411,8 @@ __global__ void __launch_bounds__(TM_THREADS) gemm_tma_kernel(const __grid_const
     tc_fence_after();
     const int wl = warp & 3, wc = warp >> 2;
     const int64_t row = m0 + wl * 32 + lane;
-#pragma unroll 1
-    for (int c0 = wc * 32; c0 < wc * 32 + 32; c0 += 16) {
+    {
+        const int c0 = wc * 16;
         uint32_t v[16];
         if (nk > 0) {
             const uint32_t taddr = tmem + (static_cast<uint32_t>(wl * 32) << 16) + static_cast<uint32_t>(c0);
@@ -420,9 +428,9 @@ __global__ void __launch_bounds__(TM_THREADS) gemm_tma_kernel(const __grid_const
 #pragma unroll
             for (int j = 0; j < 16; j++) v[j] = 0u;
         }
-        if (row >= M) continue;
         const int col0 = n0 + c0;
-        if (EPI == 0) {
+        if (row >= M) {
+        } else if (EPI == 0) {
             float* dst = C + blockIdx.z * c_split + row * ldc + col0;
             if (col0 + 16 <= N && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
 #pragma unroll
@@ -475,7 +483,7 @@ __global__ void __launch_bounds__(TM_THREADS) gemm_tma_kernel(const __grid_const
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TC_BN) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TM_BN) : "memory");
     }
     if (!ok) atomicOr(status, 1);
 }
@@ -681,13 +689,13 @@ TensorMapEncode tensor_map_encoder() {
 }
 
 // The tensor map of a k-contiguous bf16 operand of `rows` rows of `ld`
-// elements, K of them used: boxes of 8 k x 128 rows, zero fill outside.
-bool operand_map(CUtensorMap* map, const __nv_bfloat16* X, int64_t ld, int rows, int K) {
+// elements, K of them used: boxes of 8 k x box_rows rows, zero fill outside.
+bool operand_map(CUtensorMap* map, const __nv_bfloat16* X, int64_t ld, int rows, int K, int box_rows) {
     const TensorMapEncode enc = tensor_map_encoder();
     if (!enc || rows <= 0 || K <= 0) return false;
     const cuuint64_t dims[2] = {static_cast<cuuint64_t>(K), static_cast<cuuint64_t>(rows)};
     const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld) * 2};
-    const cuuint32_t box[2] = {8, TC_BM};
+    const cuuint32_t box[2] = {8, static_cast<cuuint32_t>(box_rows)};
     const cuuint32_t estr[2] = {1, 1};
     return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(X), dims, strides, box, estr,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -702,17 +710,18 @@ bool launch_tma(dim3 grid, int M, int N, int K, int kc, const __nv_bfloat16* A, 
                 int64_t ldb, float* C, int64_t ldc, int64_t c_split, const GemmEpilogue& ep, cudaStream_t s) {
     if (!vec_ok(A, lda) || !vec_ok(B, ldb)) return false;
     CUtensorMap ma, mb;
-    if (!operand_map(&ma, A, lda, M, K) || !operand_map(&mb, B, ldb, N, K)) return false;
+    if (!operand_map(&ma, A, lda, M, K, TC_BM) || !operand_map(&mb, B, ldb, N, K, TM_BN)) return false;
+    grid.x = blocks(N, TM_BN);
     static bool attr[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64 || !attr[dev]) {
-        cudaFuncSetAttribute(gemm_tma_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+        cudaFuncSetAttribute(gemm_tma_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, TM_SMEM);
         if (dev >= 0 && dev < 64) attr[dev] = true;
     }
     int* st = nullptr;
     cudaGetSymbolAddress(reinterpret_cast<void**>(&st), g_gemm_status);
-    gemm_tma_kernel<EPI><<<grid, TM_THREADS, TC_SMEM, s>>>(ma, mb, M, N, K, kc, C, ldc, c_split, ep, st);
+    gemm_tma_kernel<EPI><<<grid, TM_THREADS, TM_SMEM, s>>>(ma, mb, M, N, K, kc, C, ldc, c_split, ep, st);
     return true;
 }
 
