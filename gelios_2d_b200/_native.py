@@ -177,7 +177,7 @@ def lib() -> C.CDLL:
     L.gelios_mlp_train.argtypes = [vp, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, C.c_uint64, C.c_void_p]
     L.gelios_mlp_predict.argtypes = [vp, fp, C.c_int64, fp]
     L.gelios_mlp_gemm_bf16.argtypes = [C.c_int, C.c_int, C.c_int, vp, C.c_int64, vp, C.c_int64, vp, C.c_int64, vp]
-    L.gelios_mlp_time_layer.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]
+    L.gelios_mlp_time_layer.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]
     L.gelios_run_streamed.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
     L.gelios_autotune.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
     L.gelios_set_variant.argtypes = [vp, C.c_int, C.c_int32]

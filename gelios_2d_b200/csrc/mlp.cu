@@ -1073,11 +1073,12 @@ extern "C" int gelios_mlp_gemm_bf16(int M, int N, int K, const void* A, int64_t 
     return GELIOS_OK;
 }
 
-extern "C" int gelios_mlp_time_layer(int M, int N, int K, int reps, double* ms) {
+extern "C" int gelios_mlp_time_layer(int M, int N, int K, int reps, int tma, double* ms) {
     if (M <= 0 || N <= 0 || K <= 0 || reps < 1 || !ms) return fail("gelios_mlp_time_layer: bad arguments");
     const int64_t lda = pad8(K);
-    Buf A, B, bias, Z, H;
+    Buf A, B, bias, Z, H, Cf;
     if (!A.alloc(static_cast<size_t>(M) * lda * 2) || !B.alloc(static_cast<size_t>(N) * lda * 2) ||
+        !Cf.alloc(tma ? 16 : static_cast<size_t>(M) * N * 4) ||
         !bias.alloc(static_cast<size_t>(N) * 4) || !Z.alloc(static_cast<size_t>(M) * N * 4) ||
         !H.alloc(static_cast<size_t>(M) * N * 2))
         return cuda_fail(cudaErrorMemoryAllocation);
@@ -1108,8 +1109,16 @@ extern "C" int gelios_mlp_time_layer(int M, int N, int K, int reps, double* ms) 
     const dim3 grid(blocks(N, TC_BN), blocks(M, TC_BM), 1);
     const int kc = tc_split_len(K, 1);
     auto layer = [&]() {
-        return launch_tma<1>(grid, M, N, K, kc, A.as<__nv_bfloat16>(), lda, B.as<__nv_bfloat16>(), lda, nullptr, 0, 0,
-                             ep, s);
+        if (tma)
+            return launch_tma<1>(grid, M, N, K, kc, A.as<__nv_bfloat16>(), lda, B.as<__nv_bfloat16>(), lda, nullptr, 0,
+                                 0, ep, s);
+        // the cp.async-staged GEMM, then the bias + activation kernel
+        const dim3 g2(blocks(N, TC_BN), blocks(M, TC_BM), 1);
+        launch_tc<true, true>(g2, M, N, K, kc, A.as<__nv_bfloat16>(), lda, B.as<__nv_bfloat16>(), lda, Cf.as<float>(),
+                              N, 0, s);
+        const int64_t e = static_cast<int64_t>(M) * N;
+        bias_act_kernel<<<blocks(e, 256), 256, 0, s>>>(M, N, Cf.as<float>(), ep.bias, ep.Z, ep.H, nullptr, 1);
+        return true;
     };
     if (!layer()) return fail("gelios_mlp_time_layer: no tensor-map encoder in this driver");
     cudaEvent_t e0 = nullptr, e1 = nullptr;

@@ -118,11 +118,12 @@ def test_hidden_layer_timing_runs():
 
     from gelios_2d_b200 import _native as N
 
-    ms = C.c_double()
-    N.check(N.lib().gelios_mlp_time_layer(8192, 256, 256, 20, C.byref(ms)), "gelios_mlp_time_layer")
-    assert ms.value > 0.0
-    print(f"hidden layer 8192x256x256: {ms.value * 1e3:.2f} us, "
-          f"{2 * 8192 * 256 * 256 / (ms.value * 1e-3) / 1e12:.1f} TFLOP/s")
+    for tma in (1, 0):
+        ms = C.c_double()
+        N.check(N.lib().gelios_mlp_time_layer(8192, 256, 256, 20, tma, C.byref(ms)), "gelios_mlp_time_layer")
+        assert ms.value > 0.0
+        print(f"hidden layer 8192x256x256 ({'TMA, fused epilogue' if tma else 'cp.async + bias/GELU kernel'}): "
+              f"{ms.value * 1e3:.2f} us, {2 * 8192 * 256 * 256 / (ms.value * 1e-3) / 1e12:.1f} TFLOP/s")
 
 
 @pytest.mark.gpu
