@@ -44,7 +44,7 @@ namespace cg = cooperative_groups;
 // Minimum resident blocks per SM of the grid-wide moving-grid kernels
 // (register caps: 128 threads x 65536/(128 x minBlocks) registers).
 #ifndef GELIOS_SOURCE_MINB
-#define GELIOS_SOURCE_MINB 1
+#define GELIOS_SOURCE_MINB 10
 #endif
 
 namespace gelios {
