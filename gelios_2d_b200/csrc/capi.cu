@@ -1035,10 +1035,11 @@ int enqueue_mk2(gelios_ctx* ctx, const StepBuffers& b) {
     //         of their exact Riemann problems, the charge-exchange source
     //         terms (none depends on the motion), then, once the rails have
     //         moved, the tracked-face fluxes (sampling of the solved Riemann
-    //         problems at the face speed);
-    //   main: surface tracking + rails, then (once the side stream is done)
-    //         the tile kernel: reconstruction and flux of every other face
-    //         unit and the cell update; the commit.
+    //         problems at the face speed) and the C_1 interior and one-sided
+    //         face units;
+    //   main: surface tracking + rails, the plain interior face units, then
+    //         (once the side stream is done) the cell update; the commit.
+    //         The tile variants do the plain units' work inside the update.
     cudaStream_t sd = ctx->side;
     GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_fork, s));
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_fork, 0));
@@ -1052,15 +1053,19 @@ int enqueue_mk2(gelios_ctx* ctx, const StepBuffers& b) {
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_rails, 0));
     const int nft = launch_mk2_flux_tracked(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(),
                                             ctx->flux.as<double>(), sd);
+    // the smaller unit groups (C_1 interior, one-sided) beside the plain group
+    GELIOS_CUDA_TRY(
+        launch_mk2_cells(d, P, b, ctx->tiles, ctx->flux.as<double>(), ctx->aux.as<double>(), sd, ctx->mk2_variant, 3));
     GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_tracked, sd));
     cudaEvent_t e3 = ctx->phase_begin();
     GELIOS_CUDA_TRY(
         launch_mk2_cells(d, P, b, ctx->tiles, ctx->flux.as<double>(), ctx->aux.as<double>(), s, ctx->mk2_variant, 1));
-    // the cell update reads the tracked-face fluxes and the source terms
+    // the cell update reads every face's flux and the source terms
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_tracked, 0));
     GELIOS_CUDA_TRY(
         launch_mk2_cells(d, P, b, ctx->tiles, ctx->flux.as<double>(), ctx->aux.as<double>(), s, ctx->mk2_variant, 2));
-    const int ncl = mk2_variant_launches(ctx->mk2_variant, 1) + mk2_variant_launches(ctx->mk2_variant, 2);
+    const int ncl = mk2_variant_launches(d, ctx->mk2_variant, 1) + mk2_variant_launches(d, ctx->mk2_variant, 2) +
+                    mk2_variant_launches(d, ctx->mk2_variant, 3);
     ctx->phase_end(1, e3, ncl + nft);  // face units + cell update
     cudaEvent_t e4 = ctx->phase_begin();
     launch_commit(d, b, s);
@@ -1592,6 +1597,7 @@ extern "C" int gelios_autotune(gelios_ctx* ctx, int form, int reps, int32_t* var
                              v);
         } else {
             launch_mk2_cells(d, ctx->prm, b, ctx->tiles, ctx->flux.as<double>(), ctx->aux.as<double>(), s, v, 1);
+            launch_mk2_cells(d, ctx->prm, b, ctx->tiles, ctx->flux.as<double>(), ctx->aux.as<double>(), s, v, 3);
             launch_mk2_cells(d, ctx->prm, b, ctx->tiles, ctx->flux.as<double>(), ctx->aux.as<double>(), s, v, 2);
         }
     };

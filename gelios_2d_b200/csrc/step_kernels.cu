@@ -3398,10 +3398,15 @@ static cudaError_t launch_tiles_v(const DevMesh& d, const gelios_params& P, cons
 template <typename TF, int MINB>
 static void launch_faces_v(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
                            cudaStream_t s) {
-    // one launch per unit group, each compiled for its group; the plain
-    // interior group in the variant's shape
-    const int n0 = d.u_c1, n1 = d.u_tr0 - d.u_c1, n3 = d.n_units - d.u_tr1;
+    // the plain interior group in the variant's shape
+    const int n0 = d.u_c1;
     if (n0 > 0) mk2_face_kernel<TF, MINB, kPlainGroup><<<blocks_for(n0, 128), 128, 0, s>>>(d, P, b, fl, n0);
+}
+// the C_1 interior and one-sided groups, each in an instance compiled for it
+template <typename TF>
+static void launch_faces_rest(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
+                              cudaStream_t s) {
+    const int n1 = d.u_tr0 - d.u_c1, n3 = d.n_units - d.u_tr1;
     if (n1 > 0) mk2_face_kernel<TF, 6, kC1Group><<<blocks_for(n1, 128), 128, 0, s>>>(d, P, b, fl, n1);
     if (n3 > 0) mk2_face_kernel<TF, 4, kAnyGroup><<<blocks_for(n3, 128), 128, 0, s>>>(d, P, b, fl, n3);
 }
@@ -3409,7 +3414,7 @@ template <typename TF>
 static cudaError_t launch_cells_p(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const TileView& t,
                                   double* fl, const double* aux, cudaStream_t s, int variant, int part) {
     if (variant >= 4 && variant < 8) {
-        if (part == 1) return cudaSuccess;
+        if (part != 2) return cudaSuccess;
         switch (variant) {
             case 4: return launch_tiles_v<TF, 256, 3>(d, P, b, t, fl, aux, s);
             case 5: return launch_tiles_v<TF, 256, 2>(d, P, b, t, fl, aux, s);
@@ -3419,6 +3424,10 @@ static cudaError_t launch_cells_p(const DevMesh& d, const gelios_params& P, cons
     }
     if (part == 2) {
         mk2_update_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, fl, aux);
+        return cudaGetLastError();
+    }
+    if (part == 3) {
+        launch_faces_rest<TF>(d, P, b, fl, s);
         return cudaGetLastError();
     }
     switch (variant) {
@@ -3436,9 +3445,12 @@ const char* mk2_variant_name(int v) {
                                               "tiles 128x5",          "tiles 128x4"};
     return (v >= 0 && v < kMk2Variants) ? names[v] : "?";
 }
-int mk2_variant_launches(int v, int part) {
-    const bool tiles = v >= 4 && v < 8, groups = v < 4;  // face variants 0-3: one launch per unit group
-    return part == 1 ? (tiles ? 0 : (groups ? 3 : 1)) : 1;
+int mk2_variant_launches(const DevMesh& d, int v, int part) {
+    const bool tiles = v >= 4 && v < 8;
+    if (part == 2) return 1;
+    if (tiles) return 0;
+    if (part == 1) return d.u_c1 > 0 ? 1 : 0;
+    return (d.u_tr0 > d.u_c1 ? 1 : 0) + (d.n_units > d.u_tr1 ? 1 : 0);
 }
 cudaError_t launch_mk2_cells(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const TileView& t,
                              double* fl, const double* aux, cudaStream_t s, int variant, int part) {
@@ -3525,9 +3537,9 @@ void mhd_faces_shape(const DevMesh& d, const gelios_params& P, const gelios_mhd_
     }
     if (nr > 0) {
         if (f32)
-            mhd_face_kernel<float, 128, 1, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, M, b, hcur, fl);
+            mhd_face_kernel<float, 128, 3, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, M, b, hcur, fl);
         else
-            mhd_face_kernel<double, 128, 1, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, M, b, hcur, fl);
+            mhd_face_kernel<double, 128, 3, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, M, b, hcur, fl);
     }
 }
 }  // namespace

@@ -174,10 +174,12 @@ void launch_mk2_recon(const DevMesh& d, const gelios_params& P, const StepBuffer
 constexpr int kMk2Variants = 8;
 constexpr int kMk2TunedVariants = 4;
 const char* mk2_variant_name(int v);
-// part 1: the face units of the face-kernel variants (reads the moved points
-// only); part 2: the cell update, or the whole tile kernel (also reads the
-// tracked-face fluxes and the source terms).  Returns the launch's error.
-int mk2_variant_launches(int v, int part);
+// part 1: the plain interior face units of the face-kernel variants (reads
+// the moved points only); part 3: their other untracked units (C_1 interior,
+// one-sided), launched on the side stream; part 2: the cell update, or the
+// whole tile kernel (also reads the tracked-face fluxes and the source
+// terms).  Returns the launch's error.
+int mk2_variant_launches(const DevMesh& d, int v, int part);
 cudaError_t launch_mk2_cells(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const TileView& t,
                              double* fl, const double* aux, cudaStream_t s, int variant, int part);
 int launch_mk2_tracked_solve(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
