@@ -43,6 +43,8 @@ WORKLOADS = {
                  "mk2", (200, 100, 50, 100, 100, 100, 150, 150)),
     "mk2_1m": ("moving-grid plasma step (Go_5_komponent__MK2 form) on Setka(480,240,100,220,200,200,300,300)",
                "mk2", (480, 240, 100, 220, 200, 200, 300, 300)),
+    "mk2_8k": ("moving-grid plasma step (Go_5_komponent__MK2 form) on Setka(30,7,11,20,60,20,40,40)",
+               "mk2", (30, 7, 11, 20, 60, 20, 40, 40)),
     "plain": ("plain single-fluid step (Go_stationary form), polar 180x120, r=1..600", "plain", None),
     "k5_200k": ("plasma + four hydrogen fluids (Go_5_komponent form) on Setka(200,100,50,100,100,100,150,150)",
                 "k5", (200, 100, 50, 100, 100, 100, 150, 150)),
@@ -385,6 +387,41 @@ def time_to_residual(workload, mesh, params, st0, mc, form, fcode, device, tol, 
     return out
 
 
+def march_record(mesh, params, st0, mc, fcode, device, total, every) -> list:
+    """The moving-grid step marched from the workload's initial field in
+    calls of `every` steps (each call restarts dt at dt0, as the reference's
+    time loop does), recording after each call: the step residual per unit
+    time (sum|ro(n+1)-ro(n)| / (dt sum|ro(n+1)|), which contains the volume
+    change of moving cells), the operator residual with the grid held still
+    (gelios_operator_residual: flux balance per unit volume, face speeds 0),
+    the largest and the mean point displacement per step over the call, dt
+    and the status flags."""
+    import gelios_2d_b200 as g
+
+    S = g.Setka(mesh, params, device=device)
+    load_inputs(S, "mk2", st0, mc)
+    x0, y0 = S.points()
+    out = []
+    done = 0
+    while done < total:
+        n = min(every, total - done)
+        st = S.Go_5_komponent__MK2(n)
+        done += n
+        x1, y1 = S.points()
+        mv = np.hypot(x1 - x0, y1 - y0)
+        x0, y0 = x1, y1
+        rb = int(st.result_buf)
+        r_step = S.residual(rb) / st.dt if st.dt > 0 else float("nan")
+        rec = {"steps": done, "dt": float(st.dt), "flags": int(st.flags), "step_residual_per_time": float(r_step),
+               "operator_residual_per_time": float(S.operator_residual(rb)),
+               "point_move_per_step_max": float(np.max(mv) / n), "point_move_per_step_mean": float(np.mean(mv) / n)}
+        out.append(rec)
+        if st.flags or not np.isfinite(r_step):
+            break
+    S.close()
+    return out
+
+
 def run_sweep(args, rank: int, world: int, local: int) -> None:
     """The sweep workload: instances partitioned over the ranks by cell count,
     each rank steps its instances together (one context and graph per
@@ -572,6 +609,10 @@ def main():
     ap.add_argument("--sweep-groups", type=int, default=1)
     # wall time to an L1 residual per unit time (cold start), reported beside the rate
     ap.add_argument("--residual", type=float, default=None)
+    # moving-grid workloads: march this many steps from the initial field, recording the step residual, the
+    # operator residual (grid held still) and the point motion after every call of --march-every steps
+    ap.add_argument("--march", type=int, default=None)
+    ap.add_argument("--march-every", type=int, default=10000)
     # warm_start only: polar grid, training / held-out parameter sets, residual tolerance, training steps
     ap.add_argument("--ws-grid", default="90x60")
     ap.add_argument("--ws-train", type=int, default=256)
@@ -758,6 +799,8 @@ def main():
     }
     if args.precision == "fp32flux" and rank == 0:
         line["fp32_flux_errors"] = fp32_flux_errors(mesh, params, st0, mc, fcode, device, form=form)
+    if args.march is not None and rank == 0 and form == "mk2":
+        line["march"] = march_record(mesh, params, st0, mc, fcode, device, args.march, args.march_every)
     if args.residual is not None and rank == 0:
         line["time_to_residual"] = time_to_residual(args.workload, mesh, params, st0, mc, form, fcode, device,
                                                     args.residual, counted)

@@ -88,11 +88,19 @@ struct gelios_ctx {
     // through contention for the SMs)
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_recon = nullptr, ev_rails = nullptr, ev_tracked = nullptr;
+    // pipelined moving-grid step: the next step's surface tracking and rails
+    // run on `motion` while the main stream updates the cells nobody of the
+    // next step's motion reads (see mk2_pipelined)
+    cudaStream_t motion = nullptr;
+    cudaEvent_t ev_early = nullptr, ev_motion = nullptr, ev_side2 = nullptr;
+    DBuf early;       // cells flagged CF_EARLY, updated first
+    int n_early = 0;
+    bool pipelined = true;  // gelios_set_pipelined
     gelios_params prm{};
     bool have_mesh = false;
     DevMesh d;
     // topology / geometry
-    DBuf X, Y, X2, Y2, ptype, cstart, contour, gstart, cflags, ctype, sA, sB, snb, ssd, ssd2, sinfo;
+    DBuf X, Y, X2, Y2, ptype, cstart, contour, gstart, cflags, ctype, sA, sB, snb, ssd, ssd2, sinfo, qcorner;
     DBuf fA, fB, ftype, fmaster, fsosed, fcopy, fsdown;
     DBuf rtype, rM, rpstart, rpts, rkstart, rkeys, rs;
     DBuf lc, li, lo, sp_point, sp_line, sp_inc, sp_ainc, sp_fix, sp_of_point;
@@ -138,6 +146,7 @@ struct gelios_ctx {
     // topology or the parameters change.
     struct StepGraph {
         int form = -1;
+        int kind = 0;   // 0: one whole step; 1-3: head / body / last part of a pipelined moving-grid call
         int first = 0;  // the first step of a call: the graph starts with the words' initialisation
         int parity = -1;
         const void* cen = nullptr;
@@ -272,15 +281,23 @@ extern "C" int gelios_create(gelios_ctx** out, const gelios_params* prm, int dev
     GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_recon, cudaEventDisableTiming));
     GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_rails, cudaEventDisableTiming));
     GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_tracked, cudaEventDisableTiming));
+    GELIOS_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->motion, cudaStreamNonBlocking, prio_greatest));
+    for (cudaEvent_t* e : {&ctx->ev_early, &ctx->ev_motion, &ctx->ev_side2})
+        GELIOS_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     if (ctx->words.alloc(64)) return GELIOS_E_CUDA;
     GELIOS_CUDA_TRY(cudaMemsetAsync(ctx->words.p, 0, 64, ctx->stream));
     *out = ctx.release();
     return GELIOS_OK;
 }
 
+namespace {
+double sqrt_threshold(double R);
+}
+
 extern "C" int gelios_set_params(gelios_ctx* ctx, const gelios_params* prm) {
     if (!ctx || !prm) return GELIOS_E_ARG;
     ctx->prm = *prm;
+    ctx->d.r11_sq = sqrt_threshold(prm->R11);
     ctx->cen_valid = false;  // the cached |centroid|^(2 gamma) depends on gamma
     ctx->upf_valid = false;
     ctx->drop_graphs();      // the parameters are kernel arguments
@@ -294,12 +311,13 @@ extern "C" void gelios_destroy(gelios_ctx* ctx) {
         cudaStreamSynchronize(ctx->stream);
         cudaStreamDestroy(ctx->stream);
     }
-    for (cudaStream_t* sp : {&ctx->side, &ctx->io_h2d, &ctx->io_d2h})
+    for (cudaStream_t* sp : {&ctx->side, &ctx->motion, &ctx->io_h2d, &ctx->io_d2h})
         if (*sp) {
             cudaStreamSynchronize(*sp);
             cudaStreamDestroy(*sp);
         }
-    for (cudaEvent_t e : {ctx->ev_fork, ctx->ev_recon, ctx->ev_rails, ctx->ev_tracked})
+    for (cudaEvent_t e : {ctx->ev_fork, ctx->ev_recon, ctx->ev_rails, ctx->ev_tracked, ctx->ev_early,
+                          ctx->ev_motion, ctx->ev_side2})
         if (e) cudaEventDestroy(e);
     for (int j = 0; j < 2; j++)
         for (cudaEvent_t e : {ctx->ev_in_ready[j], ctx->ev_in_free[j], ctx->ev_out_ready[j], ctx->ev_out_free[j]})
@@ -308,6 +326,16 @@ extern "C" void gelios_destroy(gelios_ctx* ctx) {
 }
 
 namespace {
+
+// Smallest a >= 0 with sqrt(a) >= R (sqrt correctly rounded, as on the
+// device): !(sqrt(a) < R) holds exactly when !(a < threshold).
+double sqrt_threshold(double R) {
+    if (!(R > 0.0)) return 0.0;
+    double t = R * R;
+    while (t > 0.0 && std::sqrt(std::nextafter(t, 0.0)) >= R) t = std::nextafter(t, 0.0);
+    while (std::sqrt(t) < R) t = std::nextafter(t, HUGE_VAL);
+    return t;
+}
 
 // Tiles of the moving-grid step (TileView): recursive coordinate bisection of
 // the cell centroids in (polar angle, log radius), each axis scaled by the
@@ -624,6 +652,41 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
         const int f = v->line_inner[j];
         if (f >= 0 && f < nf && v->face_master[f] >= 0) cflags[v->face_master[f]] |= CF_RP;
     }
+    // CF_EARLY: cells whose new state and geometry cache the next
+    // moving-grid step reads before its face units: the four cells of every
+    // tracked unit (both cells and both Sosed_down cells, mk2_recon_unit)
+    // and, for every face of the three tracked lines and for its copy, the
+    // master, the Sosed and the Sosed_down (face_tvd, surface_faces_kernel).
+    // The pipelined step updates them first and moves the grid of the next
+    // step while the other cells are updated.
+    std::vector<int32_t> early;
+    {
+        auto mark = [&](int c) {
+            if (c >= 0 && c < nc) cflags[c] |= CF_EARLY;
+        };
+        for (int u = u_tr0; u < u_tr1; u++) {
+            const int g = u_slot[u];
+            mark(u_cell[u]);
+            mark(u_twin[u] >= 0 ? snb[g] : -1);
+            mark(ssd[g]);
+            mark(ssd2[g]);
+        }
+        const int32_t* lines[3] = {v->line_contact, v->line_inner, v->line_outer};
+        const int nl[3] = {v->n_contact, v->n_inner_line, v->n_outer_line};
+        for (int l = 0; l < 3; l++)
+            for (int j = 0; j < nl[l]; j++) {
+                const int f = lines[l][j];
+                if (f < 0 || f >= nf) continue;
+                for (const int ff : {f, v->face_copy[f]}) {
+                    if (ff < 0 || ff >= nf) continue;
+                    mark(v->face_master[ff]);
+                    mark(v->face_sosed[ff]);
+                    mark(fsdown[ff]);
+                }
+            }
+        for (int c = 0; c < nc; c++)
+            if (cflags[c] & CF_EARLY) early.push_back(c);
+    }
     // surface-tracking nodes (see point_velocity)
     std::vector<int32_t> sp_point, sp_line, sp_inc, sp_ainc, sp_fix(12, 0);
     std::vector<int32_t> local(np, -1);
@@ -691,8 +754,19 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     rc |= upload(ctx->ptype, v->point_type, np, s);
     rc |= upload(ctx->cstart, v->contour_start, nc + 1, s);
     rc |= upload(ctx->contour, v->contour, v->contour_start[nc], s);
+    {
+        std::vector<int32_t> q(4 * static_cast<size_t>(nc), -1);
+        for (int c = 0; c < nc; c++) {
+            const int32_t s0 = v->contour_start[c];
+            if (v->contour_start[c + 1] - s0 == 4)
+                for (int k = 0; k < 4; k++) q[4 * static_cast<size_t>(c) + k] = v->contour[s0 + k];
+        }
+        rc |= upload(ctx->qcorner, q.data(), q.size(), s);
+    }
     rc |= upload(ctx->gstart, v->gran_start, nc + 1, s);
     rc |= upload(ctx->cflags, cflags.data(), nc, s);
+    rc |= upload(ctx->early, early.data(), early.size(), s);
+    ctx->n_early = static_cast<int>(early.size());
     rc |= upload(ctx->ctype, v->cell_type, nc, s);
     rc |= upload<double>(ctx->hstate[0], nullptr, 16 * static_cast<size_t>(nc), s);
     rc |= upload<double>(ctx->hstate[1], nullptr, 16 * static_cast<size_t>(nc), s);
@@ -812,7 +886,9 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     d.X2 = ctx->X2.as<double>();
     d.Y2 = ctx->Y2.as<double>();
     d.ptype = ctx->ptype.as<int32_t>();
+    d.r11_sq = sqrt_threshold(ctx->prm.R11);
     d.cstart = ctx->cstart.as<int32_t>();
+    d.qcorner = reinterpret_cast<const int4*>(ctx->qcorner.as<int32_t>());
     d.contour = ctx->contour.as<int32_t>();
     d.gstart = ctx->gstart.as<int32_t>();
     d.cflags = ctx->cflags.as<uint32_t>();
@@ -1103,21 +1179,17 @@ int enqueue_form(gelios_ctx* ctx, const StepBuffers& b, int form) {
     return form == GELIOS_FORM_MHD_PUI ? enqueue_mhd(ctx, b) : enqueue_mk2(ctx, b);
 }
 
-// One moving-grid step (MK2 or MHD form): replays the instantiated graph of
-// this form and these buffers (captured on first use), or launches directly
-// while phase timing is on or if capture is unavailable.  Returns the kernel
-// count or a negative error code.
-// first: the first step of a call, whose graph begins with the initialisation
-// of the dt / status words (one launch per step, not two).
-int step_graph(gelios_ctx* ctx, const StepBuffers& b, int form, bool first) {
-    if (ctx->timing || ctx->graphs_off) {
-        if (first) launch_words_init(ctx->words.p, ctx->prm.dt0, ctx->stream);
-        const int m = enqueue_form(ctx, b, form);
-        return m < 0 ? m : m + (first ? 1 : 0);
-    }
-    const int parity = b.cur[0] == ctx->field(0, 0) ? 0 : 1;
+// Replays the instantiated graph keyed by (form, kind, first, parity,
+// centroid buffer), or captures `enqueue` (which enqueues on ctx->stream,
+// may fork to the other streams and join them back, and returns its kernel
+// count or a negative error code) into a new one and launches it.  Launches
+// directly while phase timing is on or once a capture has failed.
+template <class F>
+int graph_or_direct(gelios_ctx* ctx, int form, int kind, bool first, int parity, const void* cen, F&& enqueue) {
+    if (ctx->timing || ctx->graphs_off) return enqueue();
     for (auto& g : ctx->graphs)
-        if (g.exec && g.form == form && g.first == static_cast<int>(first) && g.parity == parity && g.cen == b.cx) {
+        if (g.exec && g.form == form && g.kind == kind && g.first == static_cast<int>(first) && g.parity == parity &&
+            g.cen == cen) {
             GELIOS_CUDA_TRY(cudaGraphLaunch(g.exec, ctx->stream));
             return g.launches;
         }
@@ -1125,12 +1197,9 @@ int step_graph(gelios_ctx* ctx, const StepBuffers& b, int form, bool first) {
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         cudaGetLastError();
         ctx->graphs_off = true;
-        if (first) launch_words_init(ctx->words.p, ctx->prm.dt0, s);
-        const int m = enqueue_form(ctx, b, form);
-        return m < 0 ? m : m + (first ? 1 : 0);
+        return enqueue();
     }
-    if (first) launch_words_init(ctx->words.p, ctx->prm.dt0, s);
-    const int n = enqueue_form(ctx, b, form) + (first ? 1 : 0);
+    const int n = enqueue();
     cudaGraph_t graph = nullptr;
     const cudaError_t e = cudaStreamEndCapture(s, &graph);
     cudaGraphExec_t exec = nullptr;
@@ -1138,9 +1207,7 @@ int step_graph(gelios_ctx* ctx, const StepBuffers& b, int form, bool first) {
         if (graph) cudaGraphDestroy(graph);
         cudaGetLastError();
         ctx->graphs_off = true;
-        if (first) launch_words_init(ctx->words.p, ctx->prm.dt0, s);
-        const int m = enqueue_form(ctx, b, form);
-        return m < 0 ? m : m + (first ? 1 : 0);
+        return enqueue();
     }
     cudaGraphDestroy(graph);
     gelios_ctx::StepGraph* slot = &ctx->graphs[0];
@@ -1151,13 +1218,196 @@ int step_graph(gelios_ctx* ctx, const StepBuffers& b, int form, bool first) {
         }
     if (slot->exec) cudaGraphExecDestroy(slot->exec);
     slot->form = form;
+    slot->kind = kind;
     slot->first = first;
     slot->parity = parity;
-    slot->cen = b.cx;
+    slot->cen = cen;
     slot->exec = exec;
     slot->launches = n;
     GELIOS_CUDA_TRY(cudaGraphLaunch(exec, s));
     return n;
+}
+
+// One moving-grid step (MK2 or MHD form) as one graph: the instantiated graph
+// of this form and these buffers (captured on first use), or direct launches
+// while phase timing is on or if capture is unavailable.  Returns the kernel
+// count or a negative error code.
+// first: the first step of a call, whose graph begins with the initialisation
+// of the dt / status words (one launch per step, not two).
+int step_graph(gelios_ctx* ctx, const StepBuffers& b, int form, bool first) {
+    const int parity = b.cur[0] == ctx->field(0, 0) ? 0 : 1;
+    return graph_or_direct(ctx, form, 0, first, parity, b.cx, [&]() {
+        if (first) launch_words_init(ctx->words.p, ctx->prm.dt0, ctx->stream);
+        const int m = enqueue_form(ctx, b, form);
+        return m < 0 ? m : m + (first ? 1 : 0);
+    });
+}
+
+// ---- the pipelined moving-grid call
+// A call of N steps runs as head(0), body(0), ..., body(N-2), last(N-1),
+// each part one graph (or direct launches):
+//   head(n): the tracked-face reconstructions and star pressures of step n
+//            (side stream) and its motion: surface tracking + rails (motion
+//            stream);
+//   body(n): step n's source terms, tracked-face fluxes and C_1 / one-sided
+//            face units (side) beside its plain face units (main); the
+//            update of the CF_EARLY cells; then the dt of step n+1 and its
+//            motion (motion stream) and its tracked-face reconstructions and
+//            star pressures (side) while the main stream updates every other
+//            cell of step n;
+//   last(n): as body(n) without step n+1: one update of every cell, then the
+//            commit (x = x2) and the dt that follows.
+// The motion of a step is a chain of latency-bound kernels on few SMs; here
+// it runs beside the memory-bound update of the step before instead of in
+// front of the face units.  It reads only the CF_EARLY cells of that step
+// (state, centroids, |c|^(2 gamma)), the points the step before moved and
+// its dt.  The points are double-buffered: step n reads the points before
+// its motion from X (n even) or X2 (n odd) and moves them into the other
+// buffer, so step n+1's rails never overwrite points that step n's update
+// still reads; the commit of the last step leaves the final points in X.
+// The 1e7 start of the CFL minimum is folded in where dt is finalised
+// (dt_finalize_cap) instead of by the update, so step n+1's dt is final once
+// step n's face units are done.  The results are the bits of the
+// one-graph-per-step arrangement (tested).
+DevMesh pipe_mesh(const gelios_ctx* ctx, int st) {
+    DevMesh d = ctx->d;
+    if (st & 1) {
+        std::swap(d.X, d.X2);
+        std::swap(d.Y, d.Y2);
+    }
+    return d;
+}
+
+// Buffers of step st of a moving-grid call: state par[st & 1] -> par[st & 1
+// ^ 1], the geometry cache of the current points in cen0 (st even) or cen1.
+StepBuffers mk2_buffers(gelios_ctx* ctx, int st, double* cen0, double* cen1) {
+    const size_t nc = ctx->d.n_cells;
+    const int cur = st & 1, nxt = cur ^ 1;
+    StepBuffers b;
+    for (int k = 0; k < 5; k++) {
+        b.cur[k] = ctx->field(cur, k);
+        b.nxt[k] = ctx->field(nxt, k);
+    }
+    b.dt_cur = ctx->T() + cur;
+    b.dt_next = ctx->T() + nxt;
+    b.dt_acc = ctx->acc();
+    b.counters = ctx->counters();
+    b.status = ctx->status();
+    double* cc = cur ? cen1 : cen0;
+    double* cn = cur ? cen0 : cen1;
+    b.cx = cc;
+    b.cy = cc + nc;
+    b.rp = cc + 2 * nc;
+    b.vs = cc + 3 * nc;
+    b.vol = cc + 4 * nc;
+    b.cx_next = cn;
+    b.cy_next = cn + nc;
+    b.rp_next = cn + 2 * nc;
+    b.vs_next = cn + 3 * nc;
+    b.vol_next = cn + 4 * nc;
+    return b;
+}
+
+int enqueue_pipe_head(gelios_ctx* ctx, int st, const StepBuffers& b, bool first) {
+    const DevMesh d = pipe_mesh(ctx, st);
+    const gelios_params& P = ctx->prm;
+    cudaStream_t s = ctx->stream, sd = ctx->side, sm = ctx->motion;
+    int n = 0;
+    if (first) {
+        launch_words_init(ctx->words.p, P.dt0, s);
+        n++;
+    }
+    GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_fork, s));
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_fork, 0));
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(sm, ctx->ev_fork, 0));
+    launch_mk2_recon(d, P, b, ctx->rec.as<double>(), sd);
+    n += d.u_tr1 > d.u_tr0 ? 1 : 0;
+    n += launch_mk2_tracked_solve(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(), sd);
+    GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_side2, sd));
+    n += launch_motion(d, P, b, ctx->surface.as<double>(), sm);
+    GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_motion, sm));
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_side2, 0));
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_motion, 0));
+    GELIOS_CUDA_TRY(cudaGetLastError());
+    return n;
+}
+
+// body(st) when bn (the buffers of step st + 1) is given, last(st) otherwise
+int enqueue_pipe_step(gelios_ctx* ctx, int st, const StepBuffers& b, const StepBuffers* bn) {
+    const DevMesh d = pipe_mesh(ctx, st);
+    const gelios_params& P = ctx->prm;
+    const int v = ctx->mk2_variant;
+    cudaStream_t s = ctx->stream, sd = ctx->side, sm = ctx->motion;
+    double* fl = ctx->flux.as<double>();
+    double* aux = ctx->aux.as<double>();
+    int n = 0;
+    GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_fork, s));
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_fork, 0));
+    launch_mk2_source(d, P, b, aux, sd);
+    n++;
+    n += launch_mk2_flux_tracked(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(), fl, sd);
+    GELIOS_CUDA_TRY(launch_mk2_cells(d, P, b, ctx->tiles, fl, aux, sd, v, 3));
+    n += mk2_variant_launches(d, v, 3);
+    GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_tracked, sd));
+    GELIOS_CUDA_TRY(launch_mk2_cells(d, P, b, ctx->tiles, fl, aux, s, v, 1));
+    n += mk2_variant_launches(d, v, 1);
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_tracked, 0));
+    if (!bn) {
+        launch_mk2_update(d, P, b, fl, aux, s, 3, nullptr, 0);
+        launch_commit(d, b, s, true);
+        GELIOS_CUDA_TRY(cudaGetLastError());
+        return n + 2;
+    }
+    const DevMesh dn = pipe_mesh(ctx, st + 1);
+    const int32_t* early = ctx->early.as<int32_t>();
+    launch_mk2_update(d, P, b, fl, aux, s, 1, early, ctx->n_early);
+    n += ctx->n_early > 0 ? 1 : 0;
+    GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_early, s));
+    // step st + 1: dt, then surface tracking + rails
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(sm, ctx->ev_early, 0));
+    launch_dt_finalize_cap(b, sm);
+    n++;
+    n += launch_motion(dn, P, *bn, ctx->surface.as<double>(), sm);
+    GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_motion, sm));
+    // step st + 1: tracked-face reconstructions and star pressures
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_early, 0));
+    launch_mk2_recon(dn, P, *bn, ctx->rec.as<double>(), sd);
+    n += dn.u_tr1 > dn.u_tr0 ? 1 : 0;
+    n += launch_mk2_tracked_solve(dn, P, *bn, ctx->rec.as<double>(), ctx->pstar.as<double>(), sd);
+    GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_side2, sd));
+    // step st: the other cells
+    launch_mk2_update(d, P, b, fl, aux, s, 2, early, ctx->n_early);
+    n++;
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_motion, 0));
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_side2, 0));
+    GELIOS_CUDA_TRY(cudaGetLastError());
+    return n;
+}
+
+bool pipe_ok(const gelios_ctx* ctx) {
+    const int v = ctx->mk2_variant;
+    return ctx->pipelined && !ctx->timing && !(v >= 4 && v < 8);
+}
+
+// nsteps (> 0) moving-grid steps as one pipelined call; returns the kernel
+// count or a negative error code
+int mk2_pipelined(gelios_ctx* ctx, int nsteps, double* cen0, double* cen1) {
+    int launches = 0;
+    StepBuffers b = mk2_buffers(ctx, 0, cen0, cen1);
+    int n = graph_or_direct(ctx, GELIOS_FORM_MK2, 1, true, 0, b.cx,
+                            [&]() { return enqueue_pipe_head(ctx, 0, b, true); });
+    if (n < 0) return n;
+    launches += n;
+    for (int st = 0; st < nsteps; st++) {
+        const bool last = st + 1 == nsteps;
+        const StepBuffers bn = last ? b : mk2_buffers(ctx, st + 1, cen0, cen1);
+        n = graph_or_direct(ctx, GELIOS_FORM_MK2, last ? 3 : 2, false, st & 1, b.cx,
+                            [&]() { return enqueue_pipe_step(ctx, st, b, last ? nullptr : &bn); });
+        if (n < 0) return n;
+        launches += n;
+        b = bn;
+    }
+    return launches;
 }
 
 }  // namespace
@@ -1260,6 +1510,12 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             cudaGetLastError();
             ctx->coop_off = true;
         }
+    }
+    if (form == GELIOS_FORM_MK2 && nsteps > 0 && pipe_ok(ctx)) {
+        const int n = mk2_pipelined(ctx, nsteps, cen0, cen1);
+        if (n < 0) return n;
+        launches += n;
+        first = nsteps;
     }
     for (int st = first; st < nsteps; st++) {
         const int cur = st & 1, nxt = cur ^ 1;
@@ -1403,6 +1659,74 @@ extern "C" int gelios_residual(gelios_ctx* ctx, int result_buf, double* residual
     return GELIOS_OK;
 }
 
+extern "C" int gelios_operator_residual(gelios_ctx* ctx, int buf, double* residual) {
+    if (!ctx || !residual || buf < 0 || buf > 1) return GELIOS_E_ARG;
+    if (!ctx->have_mesh) return GELIOS_E_STATE;
+    const DevMesh& d = ctx->d;
+    if (d.n_rail_a + d.n_rail_b + d.n_rail_c + d.n_rail_d == 0 || d.n_lc == 0) {
+        set_error("gelios_operator_residual: the moving-grid form needs rails and tracked lines");
+        return GELIOS_E_MESH;
+    }
+    GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    const size_t need = (kResidualScratch + 8) * sizeof(double);
+    if (ctx->resid.bytes < need && ctx->resid.alloc(need)) return GELIOS_E_CUDA;
+    const gelios_params& P = ctx->prm;
+    const size_t nc = d.n_cells;
+    double* cen0 = ctx->cen[0].as<double>();
+    if (!ctx->cen_valid) {
+        launch_centroid(d, d.X, d.Y, cen0, cen0 + nc, cen0 + 2 * nc, P.gamma, s, cen0 + 3 * nc, cen0 + 4 * nc);
+        ctx->cen_valid = true;
+        ctx->cen_rp_partial = false;
+    }
+    // the grid held still: moved points = current points, so every face
+    // speed is 0; dt = 1 (it only divides the zero displacement) and CFL /
+    // status words in scratch, so the context's own words stay untouched
+    double* sc = ctx->resid.as<double>();
+    double* words = sc + kResidualScratch;
+    struct Words {
+        double dt;
+        unsigned long long acc;
+        unsigned long long counters[2];
+        int status;
+        int pad[7];
+    } w{};
+    w.dt = 1.0;
+    w.acc = 0x7ff0000000000000ULL;
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(words, &w, sizeof(w), cudaMemcpyHostToDevice, s));
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(d.X2, d.X, d.n_points * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(d.Y2, d.Y, d.n_points * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    StepBuffers b;
+    for (int k = 0; k < 5; k++) {
+        b.cur[k] = ctx->field(buf, k);
+        b.nxt[k] = ctx->field(buf ^ 1, k);
+    }
+    b.dt_cur = words;
+    b.dt_next = words;
+    b.dt_acc = reinterpret_cast<unsigned long long*>(words + 1);
+    b.counters = reinterpret_cast<unsigned long long*>(words + 2);
+    b.status = reinterpret_cast<int*>(words + 4);
+    b.cx = cen0;
+    b.cy = cen0 + nc;
+    b.rp = cen0 + 2 * nc;
+    b.vs = cen0 + 3 * nc;
+    b.vol = cen0 + 4 * nc;
+    const int v = (ctx->mk2_variant >= 4 && ctx->mk2_variant < 8) ? 0 : ctx->mk2_variant;
+    double* fl = ctx->flux.as<double>();
+    launch_mk2_recon(d, P, b, ctx->rec.as<double>(), s);
+    launch_mk2_tracked_solve(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(), s);
+    launch_mk2_flux_tracked(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(), fl, s);
+    GELIOS_CUDA_TRY(launch_mk2_cells(d, P, b, ctx->tiles, fl, ctx->aux.as<double>(), s, v, 1));
+    GELIOS_CUDA_TRY(launch_mk2_cells(d, P, b, ctx->tiles, fl, ctx->aux.as<double>(), s, v, 3));
+    launch_op_residual(d, P, b, fl, sc, s);
+    GELIOS_CUDA_TRY(cudaGetLastError());
+    double r[2] = {0.0, 0.0};
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(r, sc, sizeof(r), cudaMemcpyDeviceToHost, s));
+    GELIOS_CUDA_TRY(cudaStreamSynchronize(s));
+    *residual = r[1] > 0.0 ? r[0] / r[1] : 0.0;
+    return GELIOS_OK;
+}
+
 extern "C" int gelios_run_to_residual(gelios_ctx* ctx, int form, double tol, int64_t max_steps, int32_t check_every,
                                       int64_t* steps_done, double* residual_per_time, double* dt) {
     if (!ctx || check_every <= 0 || (check_every & 1) || max_steps < 0) return GELIOS_E_ARG;
@@ -1499,6 +1823,12 @@ extern "C" int gelios_run_streamed(gelios_ctx* ctx, int form, int nsteps, const 
 
 extern "C" int gelios_variant_count(int form) {
     return form == GELIOS_FORM_MHD_PUI ? kMhdFaceVariants : form == GELIOS_FORM_MK2 ? kMk2Variants : 1;
+}
+
+extern "C" int gelios_set_pipelined(gelios_ctx* ctx, int on) {
+    if (!ctx) return GELIOS_E_ARG;
+    ctx->pipelined = on != 0;
+    return GELIOS_OK;
 }
 
 extern "C" int gelios_set_variant(gelios_ctx* ctx, int form, int32_t variant) {
@@ -1615,10 +1945,11 @@ extern "C" int gelios_autotune(gelios_ctx* ctx, int form, int reps, int32_t* var
     };
     const int nv = mhd ? kMhdFaceVariants : kMk2TunedVariants;
     cudaError_t err = cudaSuccess;
-    for (int v = 0; v < nv && err == cudaSuccess; v++) {
+    for (int i = 0; i < nv && err == cudaSuccess; i++) {
+        const int v = mhd ? i : kMk2Tuned[i];
         double m = 0.0;
         err = time_ms(faces, v, m);
-        if (v == 0 || m < best_ms) {
+        if (i == 0 || m < best_ms) {
             best = v;
             best_ms = m;
         }

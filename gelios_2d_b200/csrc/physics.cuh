@@ -30,7 +30,9 @@ enum : uint32_t {
 // Cell flag bits.
 // cell flags; CF_RP marks the cells whose |centroid|^(2 gamma) a moving-grid
 // step reads (radial reconstructions, inner-shock masters)
-enum : uint32_t { CF_AXIS = 1u, CF_C1 = 2u, CF_CENTR = 4u, CF_RP = 8u };
+// CF_EARLY: updated first by the pipelined moving-grid step (the next step's
+// surface tracking and tracked-face reconstructions read the cell)
+enum : uint32_t { CF_AXIS = 1u, CF_C1 = 2u, CF_CENTR = 4u, CF_RP = 8u, CF_EARLY = 16u };
 // unit info: slot info (SI_*) in bits 0-7, the owner's cell flags from bit
 // 8, the neighbour's from bit 12
 enum : uint32_t { UI_CF_OWN = 8u, UI_CF_NB = 12u };

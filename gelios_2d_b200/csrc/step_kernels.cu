@@ -232,24 +232,24 @@ __device__ __forceinline__ St5 get_par(const gelios_params& P, int ft, const St5
     return s;
 }
 
-// Gran::Get_par_TVD (Gran.cpp:292-473) of a Usualy face seen from Master M
-// (state Ms, centre Mx,My) with Sosed So and Sosed_down Sd.
-__device__ St5 tvd_usualy(const double* const* st, const double* cx, const double* cy, double fx, double fy,
-                          const St5& Ms, double Mx, double My, int So, int Sd, bool m_has_axis, bool tracked,
-                          int* status) {
+// dM, dS: distances from the face centre to the centroids of M and So (the
+// face unit computes them for its CFL candidates; passed in, not recomputed).
+__device__ St5 tvd_usualy_d(const double* const* st, const double* cx, const double* cy, double fx, double fy,
+                            const St5& Ms, double Mx, double My, int So, int Sd, bool m_has_axis, bool tracked,
+                            double dM, double dS, int* status) {
     if (Sd < 0) {
         St5 par = Ms;
         if (m_has_axis) {  // Gran.cpp:308-338
             const St5 par3 = load_state(st, So);
-            const double dist2 = sqrt(sq(fx - Mx) + sq(fy - My));
-            const double dist3 = sqrt(sq(fx - cx[So]) + sq(fy - cy[So]));
+            const double dist2 = dM;
+            const double dist3 = dS;
             const double dist1 = sqrt(sq(fx - Mx) + sq(fy - (-My)));
             par.v = linear3(-dist1, -Ms.v, -dist2, Ms.v, dist3, par3.v, 0.0);
         }
         return par;
     }
     const St5 par1 = load_state(st, Sd);
-    const double dist2 = sqrt(sq(fx - Mx) + sq(fy - My));
+    const double dist2 = dM;
     if (tracked) {  // Gran.cpp:345-426
         const double dist1 = sqrt(sq(fx - cx[Sd]) + sq(fy - cy[Sd]));
         // linear(-dist1, t1, -dist2, t2, 0) with one reciprocal
@@ -265,7 +265,7 @@ __device__ St5 tvd_usualy(const double* const* st, const double* cx, const doubl
         return o;
     }
     const St5 par3 = load_state(st, So);
-    const double dist3 = sqrt(sq(fx - cx[So]) + sq(fy - cy[So]));
+    const double dist3 = dS;
     const double dist1 = sqrt(sq(fx - cx[Sd]) + sq(fy - cy[Sd]));
     // linear(-dist1, t1, -dist2, t2, dist3, t3, 0) for the five fields
     const double r12 = 1.0 / (-dist1 - (-dist2)), r23 = 1.0 / (-dist2 - dist3), x2 = -dist2;
@@ -277,6 +277,16 @@ __device__ St5 tvd_usualy(const double* const* st, const double* cx, const doubl
     o.Q = linear3r(par1.Q, Ms.Q, par3.Q, r12, r23, x2);
     if (o.ro <= 0.0 || o.p <= 0.0) *status |= ST_TVD_BAD;  // the reference exits (Gran.cpp:444-455)
     return o;
+}
+
+// Gran::Get_par_TVD (Gran.cpp:292-473) of a Usualy face seen from Master M
+// (state Ms, centre Mx,My) with Sosed So and Sosed_down Sd.
+__device__ St5 tvd_usualy(const double* const* st, const double* cx, const double* cy, double fx, double fy,
+                          const St5& Ms, double Mx, double My, int So, int Sd, bool m_has_axis, bool tracked,
+                          int* status) {
+    const double dM = sqrt(sq(fx - Mx) + sq(fy - My));
+    const double dS = (Sd < 0 && !m_has_axis) || (Sd >= 0 && tracked) ? 0.0 : sqrt(sq(fx - cx[So]) + sq(fy - cy[So]));
+    return tvd_usualy_d(st, cx, cy, fx, fy, Ms, Mx, My, So, Sd, m_has_axis, tracked, dM, dS, status);
 }
 
 // Gran::Get_par_TVD of an Axis face (Gran.cpp:486-519).
@@ -295,6 +305,39 @@ __device__ __forceinline__ St5 tvd_axis(const double* const* st, const double* c
 // use no other field).  rp[c] = |centroid of c|^(2 gamma) is computed once
 // per cell and step; pdis = |face centre|^(2 gamma) once per face (the
 // reference evaluates pow at every use).
+// r: |face centre|, r2 / r3: |centroid| of M / So, dM / dS: distances from
+// the face centre to those centroids (computed by the face unit, passed in).
+__device__ void tvd_radial_d(const double* const* st, const double* cx, const double* cy, const double* rp,
+                             double fx, double fy, const St5& Ms, double Mx, double My, double rpM, int So, int Sd,
+                             bool m_has_axis, double pdis, double r, double r2, double r3, double dM, double dS,
+                             double& oro, double& op) {
+    if (Sd < 0) {
+        if (!m_has_axis) {
+            oro = Ms.ro;
+            op = Ms.p;
+            return;
+        }
+        const St5 par3 = load_state(st, So);
+        const double dist2 = dM;
+        const double dist3 = dS;
+        const double dist1 = sqrt(sq(fx - Mx) + sq(fy - (-My)));
+        const double r12 = 1.0 / (-dist1 - (-dist2)), r23 = 1.0 / (-dist2 - dist3);
+        // the mirrored centre has the radius of M itself
+        oro = linear3r(Ms.ro * sq(r2), Ms.ro * sq(r2), par3.ro * sq(r3), r12, r23, -dist2) / sq(r);
+        op = linear3r(Ms.p * rpM, Ms.p * rpM, par3.p * rp[So], r12, r23, -dist2) / pdis;
+        return;
+    }
+    const St5 par1 = load_state(st, Sd);
+    const St5 par3 = load_state(st, So);
+    const double dist2 = dM;
+    const double dist3 = dS;
+    const double dx = cx[Sd], dy = cy[Sd];
+    const double r1 = sqrt(sq(dx) + sq(dy));
+    const double dist1 = sqrt(sq(fx - dx) + sq(fy - dy));
+    const double r12 = 1.0 / (-dist1 - (-dist2)), r23 = 1.0 / (-dist2 - dist3);
+    oro = linear3r(par1.ro * sq(r1), Ms.ro * sq(r2), par3.ro * sq(r3), r12, r23, -dist2) / sq(r);
+    op = linear3r(par1.p * rp[Sd], Ms.p * rpM, par3.p * rp[So], r12, r23, -dist2) / pdis;
+}
 __device__ void tvd_radial(const double* const* st, const double* cx, const double* cy, const double* rp, double fx,
                            double fy, const St5& Ms, double Mx, double My, double rpM, int So, int Sd,
                            bool m_has_axis, double pdis, double& oro, double& op) {
@@ -903,6 +946,26 @@ __device__ __forceinline__ St5 mk2_usualy_side(const double* const* st, const do
     }
     return tvd_usualy(st, cx, cy, fx, fy, Ms, Mx, My, So, Sd, (mf & CF_AXIS) != 0, tracked, status);
 }
+// The same for a face unit that has computed the distances already: rM, rS
+// = |centroid| of M and So, dM, dS = face centre to those centroids.
+__device__ __forceinline__ St5 mk2_usualy_side_d(const double* const* st, const double* cx, const double* cy,
+                                                 const double* rp, double fx, double fy, double dis, double pdis,
+                                                 const St5& Ms, double Mx, double My, double rpM, uint32_t mf, int So,
+                                                 int Sd, bool tracked, double rM, double rS, double dM, double dS,
+                                                 int* status) {
+    if (mf & CF_C1) {
+        const double radius = rM;
+        St5 o = Ms;
+        o.ro = o.ro * sq(radius) / sq(dis);
+        o.Q = o.Q * sq(radius) / sq(dis);
+        o.p = o.p * (rpM / pdis);
+        polar_perenos(Mx, My, fx, fy, o.u, o.v);
+        tvd_radial_d(st, cx, cy, rp, fx, fy, Ms, Mx, My, rpM, So, Sd, (mf & CF_AXIS) != 0, pdis, dis, rM, rS, dM, dS,
+                     o.ro, o.p);
+        return o;
+    }
+    return tvd_usualy_d(st, cx, cy, fx, fy, Ms, Mx, My, So, Sd, (mf & CF_AXIS) != 0, tracked, dM, dS, status);
+}
 
 // One MK2 face unit before the grid moves (Setka.cpp:10204-10276): the two
 // reconstructed face states (TVD / radial TVD / boundary states), the face
@@ -916,6 +979,38 @@ struct RecUnit {
     double dist, distn;        // owner / other centroid to the face centre, -1 if not updated
 };
 
+// L1 prefetch of one global address (no register, no wait).
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
+// Prefetch into L1 of everything mk2_recon_unit / mk2_flux_unit gather for
+// face unit u: state rows and centroids of the owner, the neighbour and both
+// Sosed_down cells (and |c|^(2 gamma) where RP: the radial reconstruction),
+// the end points before and after the motion.
+template <bool RP>
+__device__ __forceinline__ void mk2_prefetch_unit(const DevMesh& d, const StepBuffers& b, int u) {
+    const int K = d.u_cell[u], nb = d.u_nb[u], A = d.u_A[u], B = d.u_B[u];
+    const int sd = d.u_sd[u], sd2 = d.u_sd2[u];
+    auto cell = [&](int c) {
+#pragma unroll
+        for (int k = 0; k < 5; k++) prefetch_l1(b.cur[k] + c);
+        prefetch_l1(b.cx + c);
+        prefetch_l1(b.cy + c);
+        if (RP) prefetch_l1(b.rp + c);
+    };
+    cell(K);
+    if (nb >= 0) cell(nb);
+    if (sd >= 0) cell(sd);
+    if (sd2 >= 0) cell(sd2);
+    prefetch_l1(d.X + A);
+    prefetch_l1(d.Y + A);
+    prefetch_l1(d.X + B);
+    prefetch_l1(d.Y + B);
+    prefetch_l1(d.X2 + A);
+    prefetch_l1(d.Y2 + A);
+    prefetch_l1(d.X2 + B);
+    prefetch_l1(d.Y2 + B);
+}
+
 // GROUP: the unit group the caller knows the unit to be in, so that branches
 // drop out at compile time: kPlainGroup [0, u_c1) (a Usualy face, neither
 // cell C_1, not tracked), kC1Group [u_c1, u_tr0) (a Usualy face with a C_1
@@ -928,17 +1023,26 @@ __device__ __forceinline__ void mk2_recon_unit(const DevMesh& d, const gelios_pa
     const int K = d.u_cell[u], nb = d.u_nb[u];
     const uint32_t info = d.u_info[u];
     const double x = b.cx[K], y = b.cy[K];
-    const bool procK = !(sqrt(sq(x) + sq(y)) < P.R11);
-    double x3 = 0.0, y3 = 0.0;
+    // centroid radii (where a radial reconstruction needs them) and
+    // face-centre-to-centroid distances, computed once for the R11 test, the
+    // CFL candidates and both reconstructions
+    const double aK = sq(x) + sq(y);
+    const bool procK = !(aK < d.r11_sq);
+    const double rK = PLAIN ? 0.0 : sqrt(aK);
+    double x3 = 0.0, y3 = 0.0, rN = 0.0;
     bool procN = false;
     if (nb >= 0) {
         x3 = b.cx[nb];
         y3 = b.cy[nb];
-        procN = !(sqrt(sq(x3) + sq(y3)) < P.R11);
+        const double aN = sq(x3) + sq(y3);
+        procN = !(aN < d.r11_sq);
+        rN = PLAIN ? 0.0 : sqrt(aN);
     }
     const int A = d.u_A[u], B = d.u_B[u];
     const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
     const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
+    const double dK = sqrt(sq(x - x2) + sq(y - y2));
+    const double dN = sqrt(sq(x3 - x2) + sq(y3 - y2));
     {
         double t1 = xb - xa, t2 = yb - ya;
         const double nn = sqrt(sq(t1) + sq(t2));
@@ -949,8 +1053,8 @@ __device__ __forceinline__ void mk2_recon_unit(const DevMesh& d, const gelios_pa
         r.S = sqrt(sq(xb - xa) + sq(yb - ya)) * (ya + yb) * 0.5;
         r.x2 = x2;
         r.y2 = y2;
-        r.dist = procK ? sqrt(sq(x - x2) + sq(y - y2)) : -1.0;
-        r.distn = procN ? sqrt(sq(x3 - x2) + sq(y3 - y2)) : -1.0;
+        r.dist = procK ? dK : -1.0;
+        r.distn = procN ? dN : -1.0;
     }
     if (!(procK || procN)) return;
     const int ft = USUALY ? static_cast<int>(G_USUALY) : static_cast<int>(info & SI_TYPE_MASK);
@@ -966,20 +1070,20 @@ __device__ __forceinline__ void mk2_recon_unit(const DevMesh& d, const gelios_pa
                         (ft == G_USUALY && (nbf & CF_C1));
     const double pdis = radial ? pow2g(dis, g2) : 1.0;
     if (ft == G_USUALY) {
-        r.a = mk2_usualy_side(b.cur, b.cx, b.cy, b.rp, x2, y2, dis, pdis, par1, x, y, b.rp[K], cf, nb, d.u_sd[u],
-                              tracked, status);
-        r.o = mk2_usualy_side(b.cur, b.cx, b.cy, b.rp, x2, y2, dis, pdis, par2, x3, y3, b.rp[nb], nbf, K, d.u_sd2[u],
-                              tracked, status);
+        r.a = mk2_usualy_side_d(b.cur, b.cx, b.cy, b.rp, x2, y2, dis, pdis, par1, x, y, b.rp[K], cf, nb, d.u_sd[u],
+                                tracked, rK, rN, dK, dN, status);
+        r.o = mk2_usualy_side_d(b.cur, b.cx, b.cy, b.rp, x2, y2, dis, pdis, par2, x3, y3, b.rp[nb], nbf, K,
+                                d.u_sd2[u], tracked, rN, rK, dN, dK, status);
         return;
     }
     if (ft == G_INNER_SPHERE) {
-        const double radius = sqrt(sq(x) + sq(y));
+        const double radius = rK;
         par11.ro = par11.ro * sq(radius) / sq(dis);
         par11.Q = par11.Q * sq(radius) / sq(dis);
         par11.p = par11.p * (b.rp[K] / pdis);
     } else if (ft == G_AXIS) {
         if (cf & CF_C1) {
-            const double radius = sqrt(sq(x) + sq(y));
+            const double radius = rK;
             par11.ro = par11.ro * sq(radius) / sq(dis);
             par11.Q = par11.Q * sq(radius) / sq(dis);
             par11.p = par11.p * (b.rp[K] / pdis);
@@ -1125,7 +1229,11 @@ __global__ void __launch_bounds__(32) mk2_flux_tracked_kernel(DevMesh d, gelios_
 // One launch per unit group (compiled without the branches the group cannot
 // take): kPlainGroup [0, u_c1), kC1Group [u_c1, u_tr0), kAnyGroup the
 // one-sided units [u_tr1, n_units).
-template <typename TF, int MINB, int GROUP>
+// PF: every gathered address of the unit is prefetched into L1 as soon as
+// the unit's indices are in (mk2_prefetch_unit), so that the loads of the
+// reconstruction's later levels hit L1 instead of waiting for L2 / DRAM one
+// level at a time; the arithmetic is the same code.
+template <typename TF, int MINB, int GROUP, bool PF = false>
 __global__ void __launch_bounds__(128, MINB) mk2_face_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                            double* __restrict__ fl, int n_launch) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1133,6 +1241,7 @@ __global__ void __launch_bounds__(128, MINB) mk2_face_kernel(DevMesh d, gelios_p
     int status = 0;
     if (i < n_launch) {
         const int u = GROUP == kPlainGroup ? i : GROUP == kC1Group ? d.u_c1 + i : d.u_tr1 + i;
+        if (PF) mk2_prefetch_unit<GROUP != kPlainGroup>(d, b, u);
         RecUnit r;
         r.a = St5{};
         r.o = St5{};
@@ -1245,14 +1354,24 @@ template <typename Fetch>
 __device__ __forceinline__ void mk2_update_cell(const DevMesh& d, const gelios_params& P, const StepBuffers& b, int c,
                                                 Fetch fetch, const double* __restrict__ aux, double& tmark, int& nro,
                                                 int& npc) {
-    const int s0 = d.cstart[c], n = d.cstart[c + 1] - s0;
-    const int32_t* con = d.contour + s0;
     const uint32_t cfl = d.cflags[c];
     const double x = b.cx[c], y = b.cy[c];
     double xn, yn, vs2 = 0.0, Volume2 = 0.0;
-    if (n == 4) {
-        // quadrilateral: the four moved points once, in registers (the same
-        // operations as centroid / area / volume_rotate)
+    // quadrilaterals: the corner indices in one 16-byte load (qcorner), so
+    // the moved points are the second level of dependent loads, not the third
+    const int4 qc = d.qcorner ? d.qcorner[c] : make_int4(-1, -1, -1, -1);
+    if (qc.x >= 0) {
+        // the four moved points once, in registers (the same operations as
+        // centroid / area / volume_rotate)
+        const double qx[4] = {d.X2[qc.x], d.X2[qc.y], d.X2[qc.z], d.X2[qc.w]};
+        const double qy[4] = {d.Y2[qc.x], d.Y2[qc.y], d.Y2[qc.z], d.Y2[qc.w]};
+        quad_geometry(qx, qy, xn, yn, vs2, Volume2);
+        if (!(cfl & CF_CENTR)) {
+            b.vs_next[c] = vs2;
+            b.vol_next[c] = Volume2;
+        }
+    } else if (const int n4 = d.cstart[c + 1] - d.cstart[c]; n4 == 4) {
+        const int32_t* con = d.contour + d.cstart[c];
         const int p0 = con[0], p1 = con[1], p2 = con[2], p3 = con[3];
         const double qx[4] = {d.X2[p0], d.X2[p1], d.X2[p2], d.X2[p3]};
         const double qy[4] = {d.Y2[p0], d.Y2[p1], d.Y2[p2], d.Y2[p3]};
@@ -1262,6 +1381,8 @@ __device__ __forceinline__ void mk2_update_cell(const DevMesh& d, const gelios_p
             b.vol_next[c] = Volume2;
         }
     } else {
+        const int s0 = d.cstart[c], n = d.cstart[c + 1] - s0;
+        const int32_t* con = d.contour + s0;
         centroid(con, n, d.X2, d.Y2, xn, yn);
         if (!(cfl & CF_CENTR)) {
             vs2 = area(con, n, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X2, d.Y2, true);
@@ -1410,17 +1531,34 @@ __global__ void __launch_bounds__(NT, MINB) mk2_tile_kernel(DevMesh d, gelios_pa
 
 // The cell update alone, from the flux slots in global memory (the update
 // phase of the tile kernel for the face-kernel arrangement).
+// MODE kUpdAll: every cell, the 1e7 start of the CFL minimum folded into the
+// accumulator (the reference's `time`, Setka.cpp:10141) when a cell takes
+// part.  The pipelined step leaves that to its dt finalisation
+// (dt_finalize_cap_kernel, commit with cap) and updates in two parts:
+// kUpdEarly the listed cells (CF_EARLY), kUpdRest every other cell;
+// kUpdAllNoMark every cell (its last step).
+enum : int { kUpdAll = 0, kUpdEarly = 1, kUpdRest = 2, kUpdAllNoMark = 3 };
+template <int MODE>
 __global__ void __launch_bounds__(128, 8) mk2_update_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                           const double* __restrict__ fl,
-                                                          const double* __restrict__ aux) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+                                                          const double* __restrict__ aux,
+                                                          const int32_t* __restrict__ list, int n_list) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double tmark = __longlong_as_double(0x7ff0000000000000LL);
     int nro = 0, npc = 0;
     const size_t ng = d.n_slots;
-    if (c < d.n_cells) {
+    int c = -1;
+    if (MODE == kUpdEarly) {
+        if (i < n_list) c = list[i];
+    } else if (i < d.n_cells) {
+        c = i;
+        if (MODE == kUpdRest && (d.cflags[c] & CF_EARLY)) c = -1;
+    }
+    if (c >= 0) {
         const int g0 = d.gstart[c];
         mk2_update_cell(d, P, b, c, [&](int k, int j) { return __ldcs(fl + k * ng + g0 + j); }, aux, tmark, nro, npc);
     }
+    if (MODE != kUpdAll) tmark = __longlong_as_double(0x7ff0000000000000LL);
     block_reduce_commit(tmark, nro, npc, 0, b.dt_acc, b.counters, b.status);
 }
 
@@ -1543,15 +1681,35 @@ __global__ void dt_finalize_kernel(StepBuffers b) {
     *b.dt_acc = 0x7ff0000000000000ULL;
 }
 
+// T[now2] when the update did not fold the 1e7 start of the CFL minimum in
+// (the pipelined moving-grid step): a face candidate exists exactly when a
+// cell takes part (a cell that takes part gives its faces a candidate), so
+// min(1e7, candidates) if there is one, 1e8 otherwise; re-arm the
+// accumulator.
+__device__ __forceinline__ void dt_finalize_cap(const StepBuffers& b) {
+    const unsigned long long a = *b.dt_acc;
+    const double t = (a == 0x7ff0000000000000ULL)
+                         ? 100000000.0
+                         : dmin_ref(10000000.0, __longlong_as_double(static_cast<long long>(a)));
+    *b.dt_next = t;
+    *b.dt_acc = 0x7ff0000000000000ULL;
+}
+__global__ void dt_finalize_cap_kernel(StepBuffers b) { dt_finalize_cap(b); }
+
 // x = x2, y = y2 (Setka.cpp:10473-10480; the zeroed V and count are never
-// stored, see point_velocity) + dt finalisation.
+// stored, see point_velocity) + dt finalisation (CAP: dt_finalize_cap).
+template <bool CAP>
 __global__ void commit_kernel(DevMesh d, StepBuffers b) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
-        const unsigned long long a = *b.dt_acc;
-        double t = (a == 0x7ff0000000000000ULL) ? 100000000.0 : __longlong_as_double(static_cast<long long>(a));
-        *b.dt_next = t;
-        *b.dt_acc = 0x7ff0000000000000ULL;
+        if (CAP) {
+            dt_finalize_cap(b);
+        } else {
+            const unsigned long long a = *b.dt_acc;
+            double t = (a == 0x7ff0000000000000ULL) ? 100000000.0 : __longlong_as_double(static_cast<long long>(a));
+            *b.dt_next = t;
+            *b.dt_acc = 0x7ff0000000000000ULL;
+        }
     }
     if (i < d.n_points) {
         d.X[i] = d.X2[i];
@@ -3402,13 +3560,20 @@ static void launch_faces_v(const DevMesh& d, const gelios_params& P, const StepB
     const int n0 = d.u_c1;
     if (n0 > 0) mk2_face_kernel<TF, MINB, kPlainGroup><<<blocks_for(n0, 128), 128, 0, s>>>(d, P, b, fl, n0);
 }
+// the plain interior group with the unit's gathers prefetched into L1
+template <typename TF, int MINB>
+static void launch_faces_pf(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
+                            cudaStream_t s) {
+    const int n0 = d.u_c1;
+    if (n0 > 0) mk2_face_kernel<TF, MINB, kPlainGroup, true><<<blocks_for(n0, 128), 128, 0, s>>>(d, P, b, fl, n0);
+}
 // the C_1 interior and one-sided groups, each in an instance compiled for it
-template <typename TF>
+template <typename TF, bool PF>
 static void launch_faces_rest(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* fl,
                               cudaStream_t s) {
     const int n1 = d.u_tr0 - d.u_c1, n3 = d.n_units - d.u_tr1;
-    if (n1 > 0) mk2_face_kernel<TF, 6, kC1Group><<<blocks_for(n1, 128), 128, 0, s>>>(d, P, b, fl, n1);
-    if (n3 > 0) mk2_face_kernel<TF, 4, kAnyGroup><<<blocks_for(n3, 128), 128, 0, s>>>(d, P, b, fl, n3);
+    if (n1 > 0) mk2_face_kernel<TF, 6, kC1Group, PF><<<blocks_for(n1, 128), 128, 0, s>>>(d, P, b, fl, n1);
+    if (n3 > 0) mk2_face_kernel<TF, 4, kAnyGroup, PF><<<blocks_for(n3, 128), 128, 0, s>>>(d, P, b, fl, n3);
 }
 template <typename TF>
 static cudaError_t launch_cells_p(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const TileView& t,
@@ -3423,26 +3588,34 @@ static cudaError_t launch_cells_p(const DevMesh& d, const gelios_params& P, cons
         }
     }
     if (part == 2) {
-        mk2_update_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, fl, aux);
+        mk2_update_kernel<kUpdAll><<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, fl, aux, nullptr, 0);
         return cudaGetLastError();
     }
     if (part == 3) {
-        launch_faces_rest<TF>(d, P, b, fl, s);
+        if (variant >= 8)
+            launch_faces_rest<TF, true>(d, P, b, fl, s);
+        else
+            launch_faces_rest<TF, false>(d, P, b, fl, s);
         return cudaGetLastError();
     }
     switch (variant) {
         case 1: launch_faces_v<TF, 5>(d, P, b, fl, s); break;
         case 2: launch_faces_v<TF, 6>(d, P, b, fl, s); break;
         case 3: launch_faces_v<TF, 4>(d, P, b, fl, s); break;
+        case 8: launch_faces_pf<TF, 8>(d, P, b, fl, s); break;
+        case 9: launch_faces_pf<TF, 6>(d, P, b, fl, s); break;
+        case 10: launch_faces_pf<TF, 4>(d, P, b, fl, s); break;
         default: launch_faces_v<TF, 8>(d, P, b, fl, s); break;
     }
     return cudaGetLastError();
 }
 const char* mk2_variant_name(int v) {
-    static const char* names[kMk2Variants] = {"faces 128x8 + update", "faces 128x5 + update",
-                                              "faces 128x6 + update", "faces 128x4 + update",
-                                              "tiles 256x3",          "tiles 256x2",
-                                              "tiles 128x5",          "tiles 128x4"};
+    static const char* names[kMk2Variants] = {"faces 128x8 + update",         "faces 128x5 + update",
+                                              "faces 128x6 + update",         "faces 128x4 + update",
+                                              "tiles 256x3",                  "tiles 256x2",
+                                              "tiles 128x5",                  "tiles 128x4",
+                                              "faces prefetched 128x8 + update", "faces prefetched 128x6 + update",
+                                              "faces prefetched 128x4 + update"};
     return (v >= 0 && v < kMk2Variants) ? names[v] : "?";
 }
 int mk2_variant_launches(const DevMesh& d, int v, int part) {
@@ -3486,8 +3659,27 @@ void launch_inner(const DevMesh& d, const gelios_params& P, const StepBuffers& b
         inner_cell_kernel<double><<<nb, 128, 0, s>>>(d, P, b, list, n);
 }
 void launch_dt_finalize(const StepBuffers& b, cudaStream_t s) { dt_finalize_kernel<<<1, 1, 0, s>>>(b); }
-void launch_commit(const DevMesh& d, const StepBuffers& b, cudaStream_t s) {
-    commit_kernel<<<blocks_for(d.n_points > 0 ? d.n_points : 1, 256), 256, 0, s>>>(d, b);
+void launch_commit(const DevMesh& d, const StepBuffers& b, cudaStream_t s, bool cap) {
+    if (cap)
+        commit_kernel<true><<<blocks_for(d.n_points > 0 ? d.n_points : 1, 256), 256, 0, s>>>(d, b);
+    else
+        commit_kernel<false><<<blocks_for(d.n_points > 0 ? d.n_points : 1, 256), 256, 0, s>>>(d, b);
+}
+void launch_dt_finalize_cap(const StepBuffers& b, cudaStream_t s) { dt_finalize_cap_kernel<<<1, 1, 0, s>>>(b); }
+void launch_mk2_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
+                       const double* aux, cudaStream_t s, int mode, const int32_t* list, int n_list) {
+    if (mode == kUpdEarly) {
+        if (n_list > 0)
+            mk2_update_kernel<kUpdEarly><<<blocks_for(n_list, 128), 128, 0, s>>>(d, P, b, fl, aux, list, n_list);
+        return;
+    }
+    const int nb = blocks_for(d.n_cells, 128);
+    if (mode == kUpdRest)
+        mk2_update_kernel<kUpdRest><<<nb, 128, 0, s>>>(d, P, b, fl, aux, list, n_list);
+    else if (mode == kUpdAllNoMark)
+        mk2_update_kernel<kUpdAllNoMark><<<nb, 128, 0, s>>>(d, P, b, fl, aux, list, n_list);
+    else
+        mk2_update_kernel<kUpdAll><<<nb, 128, 0, s>>>(d, P, b, fl, aux, list, n_list);
 }
 int launch_motion(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* scratch, cudaStream_t s,
                   bool copy_outer_shock) {
@@ -3560,6 +3752,48 @@ int launch_mhd_faces(const DevMesh& d, const gelios_params& P, const gelios_mhd_
         default: mhd_faces_shape<128, 3>(d, P, M, b, hcur, fl, s); break;
     }
     return (d.u_c1 > 0 ? 1 : 0) + (d.n_units > d.u_c1 ? 1 : 0);
+}
+// Frozen-grid residual of the moving-grid operator, per block: over the
+// cells that take part in a step (centroid radius >= R11, not C_centr) the
+// sum of |sum of the mass fluxes F.S of the cell's face slots| / rotated
+// volume (the density change per unit time the step's flux balance gives
+// with the grid held still: d(rho V)/dt = -sum F.S, Setka.cpp:10425-10431),
+// and the sum of |rho| over every cell.  Fixed-order tree sums.
+__global__ void __launch_bounds__(256) op_residual_partial_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                                  const double* __restrict__ fl,
+                                                                  double* __restrict__ part) {
+    __shared__ double sd[256], sa[256];
+    double dsum = 0.0, asum = 0.0;
+    for (int c = blockIdx.x * 256 + threadIdx.x; c < d.n_cells; c += gridDim.x * 256) {
+        asum += fabs(b.cur[0][c]);
+        const double x = b.cx[c], y = b.cy[c];
+        if (sqrt(sq(x) + sq(y)) < P.R11 || (d.cflags[c] & CF_CENTR)) continue;
+        double pt = 0.0;
+        for (int g = d.gstart[c]; g < d.gstart[c + 1]; g++) pt = pt + fl[g];
+        dsum += fabs(pt) / b.vol[c];
+    }
+    sd[threadIdx.x] = dsum;
+    sa[threadIdx.x] = asum;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            sd[threadIdx.x] += sd[threadIdx.x + o];
+            sa[threadIdx.x] += sa[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = sd[0];
+        part[2 * blockIdx.x + 1] = sa[0];
+    }
+}
+int launch_op_residual(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
+                       double* scratch, cudaStream_t s) {
+    const int n = d.n_cells;
+    const int nb = n > 0 ? (blocks_for(n, 256) < 296 ? blocks_for(n, 256) : 296) : 1;
+    op_residual_partial_kernel<<<nb, 256, 0, s>>>(d, P, b, fl, scratch + 2);
+    residual_final_kernel<<<1, 1, 0, s>>>(scratch + 2, nb, scratch);
+    return 2;
 }
 int launch_residual(const double* a, const double* b, int n, double* scratch, cudaStream_t s) {
     const int nb = n > 0 ? (blocks_for(n, 256) < 296 ? blocks_for(n, 256) : 296) : 1;

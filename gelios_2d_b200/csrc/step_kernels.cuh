@@ -20,10 +20,17 @@ namespace gelios {
 //   sinfo   face type | SI_GOD | SI_NP
 struct DevMesh {
     int n_points = 0, n_cells = 0, n_faces = 0, n_main = 0;
+    // smallest a with sqrt(a) >= R11 (IEEE sqrt, host-computed): a cell takes
+    // part in a moving-grid step iff !(x^2 + y^2 < r11_sq), the same cells as
+    // !(sqrt(x^2 + y^2) < R11) without the square root
+    double r11_sq = 0.0;
     int dims[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     double *X = nullptr, *Y = nullptr, *X2 = nullptr, *Y2 = nullptr;
     const int32_t* ptype = nullptr;
     const int32_t *cstart = nullptr, *contour = nullptr, *gstart = nullptr;
+    // contour of every quadrilateral cell as one int4 ({-1, -1, -1, -1} for
+    // other cells); may be null (the contour arrays are read instead)
+    const int4* qcorner = nullptr;
     const uint32_t* cflags = nullptr;
     const int32_t* ctype = nullptr;  // Cell_type of every cell
     const int32_t *sA = nullptr, *sB = nullptr, *snb = nullptr, *ssd = nullptr, *ssd2 = nullptr;
@@ -165,14 +172,18 @@ struct TileView {
 //                 launch of a lean instance) + mk2_update_kernel (slot sums,
 //                 update);
 //   variants 4-7  mk2_tile_kernel, one tile of cells per block, slot fluxes
-//                 in shared memory (256 x 3, 256 x 2, 128 x 5, 128 x 4).
+//                 in shared memory (256 x 3, 256 x 2, 128 x 5, 128 x 4);
+//   variants 8-10 as 0-3 with every gather of a face unit prefetched into
+//                 L1 as soon as its indices are in (128 threads x 8, 6, 4
+//                 resident blocks for the plain interior group).
 // Variant 0 is the default; gelios_autotune picks the fastest of the face-
-// kernel variants for a grid (kMk2TunedVariants; the tile kernel is slower in
-// the whole step, where the face kernel overlaps the side stream and the tile
+// kernel variants for a grid (kMk2Tuned; the tile kernel is slower in the
+// whole step, where the face kernel overlaps the side stream and the tile
 // kernel cannot, and is chosen only by hand).  All give the same bits.
 void launch_mk2_recon(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* rec, cudaStream_t s);
-constexpr int kMk2Variants = 8;
-constexpr int kMk2TunedVariants = 4;
+constexpr int kMk2Variants = 11;
+constexpr int kMk2TunedVariants = 7;
+constexpr int kMk2Tuned[kMk2TunedVariants] = {0, 1, 2, 3, 8, 9, 10};
 const char* mk2_variant_name(int v);
 // part 1: the plain interior face units of the face-kernel variants (reads
 // the moved points only); part 3: their other untracked units (C_1 interior,
@@ -192,7 +203,15 @@ void launch_mk2_source(const DevMesh& d, const gelios_params& P, const StepBuffe
 void launch_inner(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const int32_t* list, int n,
                   cudaStream_t s);
 void launch_dt_finalize(const StepBuffers& b, cudaStream_t s);
-void launch_commit(const DevMesh& d, const StepBuffers& b, cudaStream_t s);
+void launch_commit(const DevMesh& d, const StepBuffers& b, cudaStream_t s, bool cap = false);
+// dt of the next step from the CFL accumulator when the update did not fold
+// the 1e7 start in (the pipelined moving-grid step); re-arms the accumulator
+void launch_dt_finalize_cap(const StepBuffers& b, cudaStream_t s);
+// the moving-grid cell update: mode 0 every cell (1e7 start of the CFL
+// minimum folded in), 1 the listed cells, 2 every cell not flagged CF_EARLY,
+// 3 every cell (modes 1-3 fold nothing into the CFL accumulator)
+void launch_mk2_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
+                       const double* aux, cudaStream_t s, int mode, const int32_t* list, int n_list);
 int launch_motion(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* scratch, cudaStream_t s,
                   bool copy_outer_shock = true);
 // Go_5_komponent: face units then the cell update.  Hydrogen state rows
@@ -242,6 +261,11 @@ struct BatchTables {
 // sum |a - b| and sum |a| over n doubles into scratch[0], scratch[1]
 // (scratch: 2 + 2 * 296 doubles); deterministic.  Returns the launch count.
 constexpr int kResidualScratch = 2 + 2 * 296;
+// frozen-grid operator residual of the moving-grid step from the mass-flux
+// row of the face slots fl (see op_residual_partial_kernel): scratch[0] =
+// sum over updated cells of |sum F.S| / volume, scratch[1] = sum |rho|
+int launch_op_residual(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
+                       double* scratch, cudaStream_t s);
 int launch_residual(const double* a, const double* b, int n, double* scratch, cudaStream_t s);
 // Words a call starts from (dt0, empty accumulator, zero counters/status),
 // on the stream: for one context / for every instance of a batch.

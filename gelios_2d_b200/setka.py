@@ -191,6 +191,14 @@ class Setka:
         N.check(self._L.gelios_residual(self._h, int(result_buf), C.byref(r)), "gelios_residual")
         return float(r.value)
 
+    def operator_residual(self, buf: int = 0) -> float:
+        """Residual per unit time of the moving-grid operator at par[buf]
+        with the grid held still (face speeds 0): sum over updated cells of
+        |sum of the mass fluxes F.S| / volume over sum |ro|."""
+        r = C.c_double()
+        N.check(self._L.gelios_operator_residual(self._h, int(buf), C.byref(r)), "gelios_operator_residual")
+        return float(r.value)
+
     def run_to_residual(self, form: int, tol: float, max_steps: int, check_every: int = 20000):
         """Calls of check_every steps until residual / dt <= tol; returns
         (steps run, residual per unit time, dt)."""
@@ -232,6 +240,12 @@ class Setka:
         v = C.c_int32()
         N.check(self._L.gelios_get_variant(self._h, int(form), C.byref(v)), "gelios_get_variant")
         return int(v.value)
+
+    def set_pipelined(self, on: bool):
+        """Moving-grid calls with the next step's motion overlapping the
+        update (default), or one step after the other (same bits)."""
+        N.check(self._L.gelios_set_pipelined(self._h, 1 if on else 0), "gelios_set_pipelined")
+
     def set_hydrogen(self, buf: int, h16: np.ndarray):
         """ro, p, u, v of the hydrogen fluids H1..H4 of Cell::par[buf]
         (shape (16, n_cells))."""

@@ -251,6 +251,16 @@ int gelios_upload_sources(gelios_ctx *ctx, const double *q1, const double *q2, c
 int gelios_residual(gelios_ctx *ctx, int result_buf, double *residual);
 int gelios_run_to_residual(gelios_ctx *ctx, int form, double tol, int64_t max_steps, int32_t check_every,
                            int64_t *steps_done, double *residual_per_time, double *dt);
+/* gelios_operator_residual: the residual of the moving-grid operator
+ * (GELIOS_FORM_MK2) at state par[buf] with the grid held still: every face
+ * flux of the step (the same reconstructions, HLL and exact Godunov fluxes)
+ * evaluated at face speed 0 on the current points, then
+ * sum over updated cells of |sum of the cell's mass fluxes F.S| / volume,
+ * divided by sum |ro|: the L1 density change per unit time of the flow
+ * alone, without the volume change of moving cells that the step residual
+ * above contains.  Writes only scratch (the moved-point buffer is set to
+ * the current points); the state, the points and the dt words stay. */
+int gelios_operator_residual(gelios_ctx *ctx, int buf, double *residual);
 
 /* ---- streamed host I/O (no counterpart in the reference) --------------------
  * For callers that feed a fresh state from host memory every step and read
@@ -359,9 +369,10 @@ int gelios_mlp_time_layer(int M, int N, int K, int reps, int tma, double *ms);
  * blocks per SM, i.e. a register cap); the moving-grid form
  * (GELIOS_FORM_MK2) has as many variants of its face units + cell update:
  * a face kernel writing flux slots in global memory followed by an update
- * kernel (variants 0-3), or one kernel per tile of cells with the slots in
+ * kernel (variants 0-3; 8-10 the same with every gather of a face unit
+ * prefetched into L1), or one kernel per tile of cells with the slots in
  * shared memory (4-7, slower in the whole step; gelios_autotune for this
- * form times variants 0-3 only).  All give the same bits.
+ * form times variants 0-3 and 8-10).  All give the same bits.
  * gelios_autotune times each shape on the context's grid and current state
  * (`reps` launches each, CUDA events on the context stream; only scratch
  * buffers are written, the state and the points are not touched), keeps the
@@ -375,6 +386,13 @@ int gelios_set_variant(gelios_ctx *ctx, int form, int32_t variant);
 /* The variant a context uses for `form` (set by hand or by gelios_autotune;
  * 0 for forms without variants). */
 int gelios_get_variant(gelios_ctx *ctx, int form, int32_t *variant);
+/* Pipelined moving-grid calls (on by default; no counterpart in the
+ * reference): within a call of GELIOS_FORM_MK2 steps, the next step's
+ * surface tracking and rail motion (Setka::Move_surface,
+ * Move_Setka_Calculate_2) run while the cells they do not read are still
+ * being updated.  Same results bit for bit as one step after the other
+ * (on = 0), which the tile variants (4-7) and phase timing always use. */
+int gelios_set_pipelined(gelios_ctx *ctx, int on);
 
 /* ---- per-face solvers on the device (known-answer checks) ------------------
  * Batched HLLC_2d_Korolkov_b_s (Setka.cpp:10484-10700): in[n*16] =

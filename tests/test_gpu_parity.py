@@ -237,6 +237,35 @@ def test_mk2_graph_matches_direct_launches():
     assert a[3] == b[3]
 
 
+@pytest.mark.parametrize("variant,precision", [(0, N.PREC_FP64), (8, N.PREC_FP64), (10, N.PREC_FP32_FLUX)])
+def test_mk2_pipelined_calls_match_step_by_step(variant, precision):
+    """A pipelined call (the next step's surface tracking and rails run while
+    the cells they do not read are updated; points double-buffered) leaves
+    the bits of one step after the other: states of both buffers, points, dt
+    and the clamp / status words, over calls of 1, 2, 3, 7 and 40 steps."""
+    mesh = g.Mesh.setka(*MEDIUM)
+    P = N.reference_params().copy(precision=precision)
+    st0 = W.init_conditions_reference(mesh)
+    mc = W.mc_fields(mesh, seed=9)
+    runs = []
+    for pipelined in (True, False):
+        dev = g.Setka(mesh, P)
+        dev.set_par(0, st0)
+        dev.set_par(1, st0)
+        dev.set_mc(*mc)
+        dev.set_variant(N.FORM_MK2, variant)
+        dev.set_pipelined(pipelined)
+        out = []
+        for n in (1, 2, 3, 7, 40):
+            s = dev.Go_5_komponent__MK2(n)
+            out.append((dev.par(0), dev.par(1), dev.points(), s.dt, s.flags, s.n_ro_clamp, s.n_p_clamp))
+        runs.append(out)
+    for a, b in zip(*runs):
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+        assert np.array_equal(a[2][0], b[2][0]) and np.array_equal(a[2][1], b[2][1])
+        assert a[3:] == b[3:]
+
+
 def test_deterministic_runs():
     mesh = g.Mesh.setka(*MEDIUM)
     P = N.reference_params()
@@ -341,3 +370,42 @@ def test_residual_matches_host_and_run_to_residual_stops():
     assert n == 100 and r <= 1e300 and dt > 0
     n, r, dt = dev.run_to_residual(N.FORM_STATIONARY, 0.0, 300, 100)
     assert n == 300 and r > 0.0
+
+
+def test_operator_residual_is_the_flux_balance_of_a_still_grid():
+    """gelios_operator_residual is the density change per unit time of a step
+    on a grid that does not move: with the surface speeds scaled by koef = 0
+    the first step snaps the points onto the rail formulas and the next step
+    leaves them in place bit for bit, so its density change over dt is the
+    flux balance the residual evaluates (each updated cell: V2 = V,
+    |ro' - ro| = dt |sum F.S| / V; relative 1e-6: ro' - ro is ~1e-8 of ro at
+    dt0).  The call changes no state, point or dt word (the following steps
+    give the same bits as without it)."""
+    mesh = g.Mesh.setka(*MEDIUM)
+    P = N.reference_params().copy(koef=0.0)
+    st0 = W.init_conditions_reference(mesh)
+    mc = W.mc_fields(mesh, seed=9)
+
+    def run(with_residual):
+        dev = g.Setka(mesh, P)
+        dev.set_par(0, st0)
+        dev.set_par(1, st0)
+        dev.set_mc(*mc)
+        dev.Go_5_komponent__MK2(1)
+        s1 = dev.par(1)
+        pts1 = dev.points()
+        dev.set_par(0, s1)
+        r = [dev.operator_residual(0), dev.operator_residual(0)] if with_residual else None
+        st = dev.Go_5_komponent__MK2(1)
+        return dev, s1, pts1, st, r
+
+    dev, s1, pts1, st, r = run(True)
+    assert r[0] == r[1] and np.isfinite(r[0]) and r[0] > 0.0
+    pts2 = dev.points()
+    assert np.array_equal(pts1[0], pts2[0]) and np.array_equal(pts1[1], pts2[1])
+    s2 = dev.par(1)
+    dt = N.reference_params().dt0
+    ref = float(np.abs(s2[0] - s1[0]).sum() / (dt * np.abs(s1[0]).sum()))
+    assert abs(r[0] - ref) <= 1e-6 * ref, (r[0], ref)
+    dev2, _, _, st_b, _ = run(False)
+    assert np.array_equal(dev2.par(1), s2) and np.array_equal(dev2.points()[0], pts2[0]) and st_b.dt == st.dt

@@ -188,7 +188,7 @@ def test_mhd_graph_matches_direct_launches():
 def test_variant_counts():
     L = N.lib()
     assert L.gelios_variant_count(N.FORM_MHD_PUI) == 6
-    assert L.gelios_variant_count(N.FORM_MK2) == 8
+    assert L.gelios_variant_count(N.FORM_MK2) == 11
     for f in (N.FORM_STATIONARY, N.FORM_INNER_MK2, N.FORM_5_KOMPONENT):
         assert L.gelios_variant_count(f) == 1
 
