@@ -76,9 +76,10 @@ WORKLOADS = {
 #             grid) + 4*4 neighbour indices = 264 B
 BYTES_PER_CELL = {"mk2": 288, "plain": 112, "k5": 392, "mhd": 288, "inner": 264}
 STEP_KERNELS = {
-    "mk2": "whole moving-grid step: tracked recon + solve, source, surface_faces, rails, tracked flux, "
-           "face units (reconstruction + flux) and cell update in the autotuned arrangement, commit "
-           "(one CUDA graph, 2 streams)",
+    "mk2": "whole moving-grid step, pipelined: source, tracked flux, face units (reconstruction + flux, "
+           "autotuned arrangement), update of the cells the next motion reads, then the next step's dt, "
+           "surface_faces, rails, tracked recon + solve beside the update of the other cells "
+           "(CUDA graphs, 3 streams; one commit per call)",
     "plain": "whole plain step: stationary_persistent_kernel (face units, cell update, dt; all steps of a call "
              "in one cooperative launch)",
     "k5": "whole four-fluid step: centroid, surface_faces, rails, k5_cell, commit",

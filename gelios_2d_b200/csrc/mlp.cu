@@ -289,28 +289,36 @@ __device__ __forceinline__ float gelu_grad(float x) {
 }
 
 // ---- the GEMM with TMA staging
-// Per stage and operand, eight boxes of 8 k x 128 rows (16 bytes x 128
-// rows), one per 8-wide k chunk; a box lands as 128 rows of 16 bytes, so the
-// stage is the canonical K-major layout without swizzle with the k-chunk
-// stride (leading byte offset) 2048 and the 8-row stride (stride byte offset)
-// 128.  Thread 0 issues the loads (mbarrier expect_tx / complete_tx per
-// stage), waits for each stage, issues its four MMAs and commits them to the
-// stage's "empty" mbarrier before refilling it.  Out-of-range rows and k are
-// zero-filled by the TMA unit.  EPI 0: C (fp32) as gemm_tc_kernel writes it;
+// Per stage and operand one box of 64 k x rows (128 bytes x 128 rows for A,
+// x 64 rows for B) loaded with the 128-byte swizzle: row r lands at r * 128
+// bytes with its 16-byte chunks permuted by (r mod 8), which is the
+// canonical K-major SWIZZLE_128B layout the MMA descriptor names (8-row
+// groups 1024 bytes apart; the k-th 16-deep slice of the stage starts 32 k
+// bytes into the rows).  Stage buffers are 1024-byte aligned.  Thread 0
+// issues the loads (mbarrier expect_tx / complete_tx per stage), waits for
+// each stage, issues its four MMAs and commits them to the stage's "empty"
+// mbarrier before refilling it.  Out-of-range rows and k are zero-filled by
+// the TMA unit.  EPI 0: C (fp32) as gemm_tc_kernel writes it;
 // EPI 1: z = C + bias per column, then Z = z, H = bf16(act(z)), Hf = act(z)
 // (each output optional, rows of N).
 // tile: TM_BN = 64 columns per CTA (256 CTAs for a 8192 x 256 layer, two
 // resident per SM: one's epilogue overlaps the other's loads); k-chunk
 // stride of the A stage 128 rows x 16 bytes, of the B stage 64 x 16 bytes
 constexpr int TM_BN = 64;
-constexpr uint32_t TM_LBO_A = TC_BM * 16, TM_LBO_B = TM_BN * 16, TM_SBO = 128;
+constexpr uint32_t TM_SBO = 1024;
 constexpr int TM_TILE_B = TM_BN * TC_BK * 2;
-constexpr int TM_SMEM = TC_STAGES * (TC_TILE + TM_TILE_B);
+// + 1024: the dynamic shared memory base is rounded up to 1024 bytes
+constexpr int TM_SMEM = TC_STAGES * (TC_TILE + TM_TILE_B) + 1024;
 constexpr uint32_t TM_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TM_BN >> 3) << 17) |
                               ((uint32_t)(TC_BM >> 4) << 24);
-__device__ __forceinline__ uint64_t tm_desc(uint32_t saddr, uint32_t lbo) {
-    return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16) |
-           (static_cast<uint64_t>((TM_SBO >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+// shared-memory matrix descriptor of a K-major SWIZZLE_128B operand: start
+// address >> 4 (bits 0-13), leading byte offset 16 (unused for swizzled
+// K-major layouts; bits 16-29), stride byte offset 1024 >> 4 (bits 32-45),
+// version 1 (bits 46-47), base offset 0 (1024-aligned buffers), layout type
+// 2 = SWIZZLE_128B (bits 61-63)
+__device__ __forceinline__ uint64_t tm_desc(uint32_t saddr) {
+    return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (1ull << 16) |
+           (static_cast<uint64_t>((TM_SBO >> 4) & 0x3FFFu) << 32) | (1ull << 46) | (2ull << 61);
 }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
@@ -342,8 +350,11 @@ __global__ void __launch_bounds__(TM_THREADS, 2) gemm_tma_kernel(const __grid_co
     extern __shared__ __align__(1024) uint8_t tc_smem[];
     __shared__ uint64_t full[TC_STAGES], empty[TC_STAGES];
     __shared__ uint32_t tmem_slot;
-    uint8_t* sA0 = tc_smem;
-    uint8_t* sB0 = tc_smem + TC_STAGES * TC_TILE;
+    // 1024-byte aligned stage buffers (the swizzle pattern repeats every
+    // 1024 bytes and the descriptors assume it starts at the buffer)
+    uint8_t* base = tc_smem + ((1024u - (smem_u32(tc_smem) & 1023u)) & 1023u);
+    uint8_t* sA0 = base;
+    uint8_t* sB0 = base + TC_STAGES * TC_TILE;
     const int m0 = blockIdx.y * TC_BM, n0 = blockIdx.x * TM_BN;
     const int kb = blockIdx.z * kc, ke = min(K, kb + kc);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -372,11 +383,8 @@ __global__ void __launch_bounds__(TM_THREADS, 2) gemm_tma_kernel(const __grid_co
             mbar_expect_tx(&full[st], static_cast<uint32_t>(TC_TILE + TM_TILE_B));
             const uint32_t a = smem_u32(sA0 + st * TC_TILE), b = smem_u32(sB0 + st * TM_TILE_B);
             const int k0 = kb + j * TC_BK;
-#pragma unroll
-            for (int q = 0; q < TC_BK / 8; q++) {
-                tma_load_2d(a + q * TM_LBO_A, &tmA, k0 + 8 * q, m0, &full[st]);
-                tma_load_2d(b + q * TM_LBO_B, &tmB, k0 + 8 * q, n0, &full[st]);
-            }
+            tma_load_2d(a, &tmA, k0, m0, &full[st]);
+            tma_load_2d(b, &tmB, k0, n0, &full[st]);
         };
         for (int j = 0; j < TC_STAGES && j < nk; j++) load(j);
         for (int it = 0; it < nk; it++) {
@@ -387,8 +395,8 @@ __global__ void __launch_bounds__(TM_THREADS, 2) gemm_tma_kernel(const __grid_co
             const uint32_t a0 = smem_u32(sA0 + st * TC_TILE), b0 = smem_u32(sB0 + st * TM_TILE_B);
 #pragma unroll
             for (int k = 0; k < TC_BK / 16; k++) {
-                const uint64_t ad = tm_desc(a0 + k * 2 * TM_LBO_A, TM_LBO_A);
-                const uint64_t bd = tm_desc(b0 + k * 2 * TM_LBO_B, TM_LBO_B);
+                const uint64_t ad = tm_desc(a0 + k * 32);
+                const uint64_t bd = tm_desc(b0 + k * 32);
                 const uint32_t acc = (it > 0 || k > 0) ? 1u : 0u;
                 asm volatile(
                     "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
@@ -689,16 +697,17 @@ TensorMapEncode tensor_map_encoder() {
 }
 
 // The tensor map of a k-contiguous bf16 operand of `rows` rows of `ld`
-// elements, K of them used: boxes of 8 k x box_rows rows, zero fill outside.
+// elements, K of them used: boxes of 64 k (128 bytes) x box_rows rows with
+// the 128-byte swizzle, zero fill outside.
 bool operand_map(CUtensorMap* map, const __nv_bfloat16* X, int64_t ld, int rows, int K, int box_rows) {
     const TensorMapEncode enc = tensor_map_encoder();
     if (!enc || rows <= 0 || K <= 0) return false;
     const cuuint64_t dims[2] = {static_cast<cuuint64_t>(K), static_cast<cuuint64_t>(rows)};
     const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld) * 2};
-    const cuuint32_t box[2] = {8, static_cast<cuuint32_t>(box_rows)};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(TC_BK), static_cast<cuuint32_t>(box_rows)};
     const cuuint32_t estr[2] = {1, 1};
     return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(X), dims, strides, box, estr,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 

@@ -2919,10 +2919,13 @@ __device__ __forceinline__ void mhd_usualy_side(const double* const* st, const d
                                                 const double* cx, const double* cy, const double* rp, double fx,
                                                 double fy, double dis, double pdis, const St5& Ms, const Ext8& Me,
                                                 double Mx, double My, double rpM, uint32_t mf, int So, const St5& Ss,
-                                                const Ext8& Se, double Sx, double Sy, int Sd, bool tracked, St5& oi,
-                                                Ext8& oe, int* status) {
+                                                const Ext8& Se, double Sx, double Sy, int Sd, bool tracked,
+                                                double rM, double rS, double dM, double dS, St5& oi, Ext8& oe,
+                                                int* status) {
+    // rM, rS: |centroid| of M and So; dM, dS: face centre to those centroids
     if (mf & CF_C1) {
-        oi = mk2_usualy_side(st, cx, cy, rp, fx, fy, dis, pdis, Ms, Mx, My, rpM, mf, So, Sd, tracked, status);
+        oi = mk2_usualy_side_d(st, cx, cy, rp, fx, fy, dis, pdis, Ms, Mx, My, rpM, mf, So, Sd, tracked, rM, rS, dM,
+                               dS, status);
         oe = Me;
         return;
     }
@@ -2930,8 +2933,8 @@ __device__ __forceinline__ void mhd_usualy_side(const double* const* st, const d
     oe = Me;
     if (Sd < 0) {
         if (mf & CF_AXIS) {  // Gran.cpp:308-338
-            const double dist2 = sqrt(sq(fx - Mx) + sq(fy - My));
-            const double dist3 = sqrt(sq(fx - Sx) + sq(fy - Sy));
+            const double dist2 = dM;
+            const double dist3 = dS;
             const double dist1 = sqrt(sq(fx - Mx) + sq(fy - (-My)));
             oi.v = linear3(-dist1, -Ms.v, -dist2, Ms.v, dist3, Ss.v, 0.0);
         }
@@ -2939,7 +2942,7 @@ __device__ __forceinline__ void mhd_usualy_side(const double* const* st, const d
     }
     const St5 s1 = load_state(st, Sd);
     const Ext8 e1 = load_ext(hs, nc, Sd);
-    const double dist2 = sqrt(sq(fx - Mx) + sq(fy - My));
+    const double dist2 = dM;
     const double dist1 = sqrt(sq(fx - cx[Sd]) + sq(fy - cy[Sd]));
     const double r12 = 1.0 / (-dist1 - (-dist2)), x2 = -dist2;
     if (tracked) {  // Gran.cpp:345-426
@@ -2953,7 +2956,7 @@ __device__ __forceinline__ void mhd_usualy_side(const double* const* st, const d
 #pragma unroll
         for (int k = 0; k < kMhdExtra; k++) oe.f[k] = (e1.f[k] - Me.f[k]) * r12 * (0.0 - x2) + Me.f[k];
     } else {
-        const double dist3 = sqrt(sq(fx - Sx) + sq(fy - Sy));
+        const double dist3 = dS;
         const double r23 = 1.0 / (-dist2 - dist3);
         oi.ro = linear3r(s1.ro, Ms.ro, Ss.ro, r12, r23, x2);
         oi.p = linear3r(s1.p, Ms.p, Ss.p, r12, r23, x2);
@@ -3030,18 +3033,25 @@ __device__ __forceinline__ double mhd_face_body(const DevMesh& d, const gelios_p
         const int K = d.u_cell[u], nb = d.u_nb[u];
         const uint32_t info = d.u_info[u];
         const double x = b.cx[K], y = b.cy[K];
-        const bool procK = !(sqrt(sq(x) + sq(y)) < P.R11);
-        double x3 = 0.0, y3 = 0.0;
+        // as mk2_recon_unit: the R11 test without a square root, the radii
+        // only where a radial reconstruction reads them, the distances once
+        const double aK = sq(x) + sq(y);
+        const bool procK = !(aK < d.r11_sq);
+        double x3 = 0.0, y3 = 0.0, aN = 0.0;
         bool procN = false;
         if (nb >= 0) {
             x3 = b.cx[nb];
             y3 = b.cy[nb];
-            procN = !(sqrt(sq(x3) + sq(y3)) < P.R11);
+            aN = sq(x3) + sq(y3);
+            procN = !(aN < d.r11_sq);
         }
         if (procK || procN) {
+            const double rK = PLAIN ? 0.0 : sqrt(aK), rN = PLAIN ? 0.0 : sqrt(aN);
             const int A = d.u_A[u], B = d.u_B[u];
             const double xa = d.X[A], ya = d.Y[A], xb = d.X[B], yb = d.Y[B];
             const double x2 = (xa + xb) / 2.0, y2 = (ya + yb) / 2.0;
+            const double dK = sqrt(sq(x - x2) + sq(y - y2));
+            const double dN = sqrt(sq(x3 - x2) + sq(y3 - y2));
             double t1 = xb - xa, t2 = yb - ya;
             const double nn = sqrt(sq(t1) + sq(t2));
             t1 = t1 / nn;
@@ -3068,11 +3078,11 @@ __device__ __forceinline__ double mhd_face_body(const DevMesh& d, const gelios_p
                 const St5 sN = par2;
                 const Ext8 eN = e2;
                 mhd_usualy_side(b.cur, hs, nc, b.cx, b.cy, b.rp, x2, y2, dis, pdis, par1, ex1, x, y, b.rp[K], cf, nb,
-                                sN, eN, x3, y3, d.u_sd[u], tracked, par11, e11, &status);
+                                sN, eN, x3, y3, d.u_sd[u], tracked, rK, rN, dK, dN, par11, e11, &status);
                 mhd_usualy_side(b.cur, hs, nc, b.cx, b.cy, b.rp, x2, y2, dis, pdis, sN, eN, x3, y3, b.rp[nb], nbf, K,
-                                par1, ex1, x, y, d.u_sd2[u], tracked, par2, e2, &status);
+                                par1, ex1, x, y, d.u_sd2[u], tracked, rN, rK, dN, dK, par2, e2, &status);
             } else if (ft == G_INNER_SPHERE) {
-                const double radius = sqrt(sq(x) + sq(y));
+                const double radius = rK;
                 par11.ro = par11.ro * sq(radius) / sq(dis);
                 par11.Q = par11.Q * sq(radius) / sq(dis);
                 par11.p = par11.p * (b.rp[K] / pdis);
@@ -3117,12 +3127,12 @@ __device__ __forceinline__ double mhd_face_body(const DevMesh& d, const gelios_p
                 for (int k = 0; k < kMhdFlux; k++) __stcs(fl + k * ng + gt, -(F[k] * S));
             }
             if (procK) {
-                const double dist = sqrt(sq(x - x2) + sq(y - y2));
+                const double dist = dK;
                 tmin_u = dmin_ref(tmin_u, P.kurant * dist * tI);
                 tmin_u = dmin_ref(tmin_u, P.kurant * dist / UUp);
             }
             if (gt >= 0 && procN) {
-                const double distn = sqrt(sq(x3 - x2) + sq(y3 - y2));
+                const double distn = dN;
                 tmin_u = dmin_ref(tmin_u, P.kurant * distn * tI);
                 tmin_u = dmin_ref(tmin_u, P.kurant * distn / UUp);
             }
@@ -3155,22 +3165,39 @@ __device__ __forceinline__ void mhd_update_body(const DevMesh& d, const gelios_p
                                                 double& tmark, int& nro, int& npc) {
     const size_t ng = d.n_slots, nc = d.n_cells;
     {
-        const int s0 = d.cstart[c], n = d.cstart[c + 1] - s0;
-        const int32_t* con = d.contour + s0;
+        const uint32_t cfl = d.cflags[c];
         double xn, yn;
-        centroid(con, n, d.X2, d.Y2, xn, yn);
+        double vs2 = 0.0, Volume2 = 0.0;
+        // quadrilaterals: the four moved corners from one int4 load, the
+        // operations of centroid / area / volume_rotate in registers
+        const int4 qc = d.qcorner ? d.qcorner[c] : make_int4(-1, -1, -1, -1);
+        if (qc.x >= 0) {
+            const double qx[4] = {d.X2[qc.x], d.X2[qc.y], d.X2[qc.z], d.X2[qc.w]};
+            const double qy[4] = {d.Y2[qc.x], d.Y2[qc.y], d.Y2[qc.z], d.Y2[qc.w]};
+            double vq, volq;
+            quad_geometry(qx, qy, xn, yn, vq, volq);
+            if (!(cfl & CF_CENTR)) {
+                vs2 = vq;
+                Volume2 = volq;
+                b.vs_next[c] = vq;
+                b.vol_next[c] = volq;
+            }
+        } else {
+            const int s0 = d.cstart[c], n = d.cstart[c + 1] - s0;
+            const int32_t* con = d.contour + s0;
+            centroid(con, n, d.X2, d.Y2, xn, yn);
+            if (!(cfl & CF_CENTR)) {
+                vs2 = area(con, n, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X2, d.Y2, true);
+                Volume2 = volume_rotate(con, n, d.X2, d.Y2);
+                b.vs_next[c] =
+                    n == 4 ? vs2 : area(con, n, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X2, d.Y2, false);
+                b.vol_next[c] = Volume2;
+            }
+        }
         b.cx_next[c] = xn;
         b.cy_next[c] = yn;
-        const uint32_t cfl = d.cflags[c];
         if (cfl & CF_RP) b.rp_next[c] = pow2g(sqrt(sq(xn) + sq(yn)), 2 * P.gamma);
         const double x = b.cx[c], y = b.cy[c];
-        double vs2 = 0.0, Volume2 = 0.0;
-        if (!(cfl & CF_CENTR)) {
-            vs2 = area(con, n, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X2, d.Y2, true);
-            Volume2 = volume_rotate(con, n, d.X2, d.Y2);
-            b.vs_next[c] = n == 4 ? vs2 : area(con, n, d.sA, d.sB, d.gstart[c], d.gstart[c + 1], d.X2, d.Y2, false);
-            b.vol_next[c] = Volume2;
-        }
         if (!(sqrt(sq(x) + sq(y)) < P.R11)) {
             tmark = 10000000.0;
             const St5 par1 = load_state(b.cur, c);
