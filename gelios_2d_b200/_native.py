@@ -31,6 +31,7 @@ FORM_5_KOMPONENT = 3
 FORM_MHD_PUI = 4
 PREC_FP64 = 0
 PREC_FP32_FLUX = 1
+PREC_FP32_WAVES = 2
 
 _DOUBLE_FIELDS = ("gamma", "kurant", "chi", "inner_mach", "in_ro", "in_p", "in_u", "in_v", "in_Q",
                   "extern_u_par", "extern_u_tvd", "R11", "rad_stat", "R1", "R111", "R5", "Left", "koef",

@@ -2316,7 +2316,7 @@ struct gelios_plain_batch {
     cudaStream_t stream = nullptr;
     std::vector<gelios_ctx*> ctxs;
     DBuf inst, active, resid;
-    bool fp32 = false;
+    int prec = GELIOS_PREC_FP64;  // flux precision of every instance
     ~gelios_plain_batch() {
         if (stream) cudaStreamDestroy(stream);
     }
@@ -2332,14 +2332,14 @@ extern "C" int gelios_plain_batch_create(gelios_plain_batch** out, gelios_ctx* c
         return GELIOS_E_STATE;
     }
     B->device = c0->device;
-    B->fp32 = c0->prm.precision == GELIOS_PREC_FP32_FLUX;
+    B->prec = c0->prm.precision;
     for (int i = 0; i < n; i++) {
         gelios_ctx* c = ctxs[i];
         if (!c || !c->have_mesh) {
             set_error("gelios_plain_batch_create: a context without topology");
             return GELIOS_E_STATE;
         }
-        if (c->device != B->device || (c->prm.precision == GELIOS_PREC_FP32_FLUX) != B->fp32) {
+        if (c->device != B->device || c->prm.precision != B->prec) {
             set_error("gelios_plain_batch_create: contexts on different devices or with different flux precisions");
             return GELIOS_E_ARG;
         }
@@ -2381,7 +2381,7 @@ int plain_batch_prepare(gelios_plain_batch* B, const std::vector<int>& list) {
     std::vector<PlainInstance> host(B->ctxs.size());
     for (size_t i = 0; i < B->ctxs.size(); i++) {
         gelios_ctx* c = B->ctxs[i];
-        if ((c->prm.precision == GELIOS_PREC_FP32_FLUX) != B->fp32) {
+        if (c->prm.precision != B->prec) {
             set_error("gelios_plain_batch: the instances' flux precisions differ");
             return GELIOS_E_ARG;
         }
@@ -2443,7 +2443,7 @@ extern "C" int gelios_plain_batch_step(gelios_plain_batch* B, int nsteps, gelios
     int rc = plain_batch_prepare(B, list);
     if (rc) return rc;
     GELIOS_CUDA_TRY(launch_stationary_batch(B->ctxs[0]->d, B->inst.as<PlainInstance>(), B->active.as<int>(), n, nsteps,
-                                            B->fp32, B->stream));
+                                            B->prec, B->stream));
     GELIOS_CUDA_TRY(cudaStreamSynchronize(B->stream));
     for (int i = 0; i < n; i++) {
         gelios_ctx* c = B->ctxs[i];
@@ -2486,7 +2486,7 @@ extern "C" int gelios_plain_batch_run_to_residual(gelios_plain_batch* B, double 
         int rc = plain_batch_prepare(B, list);
         if (rc) return rc;
         GELIOS_CUDA_TRY(launch_stationary_batch(B->ctxs[0]->d, B->inst.as<PlainInstance>(), B->active.as<int>(),
-                                                static_cast<int>(list.size()), chunk, B->fp32, B->stream));
+                                                static_cast<int>(list.size()), chunk, B->prec, B->stream));
         for (int i : list) {
             gelios_ctx* c = B->ctxs[i];
             double* sc = B->resid.as<double>() + static_cast<size_t>(kResidualScratch) * i;

@@ -123,10 +123,33 @@ __device__ __forceinline__ double tsqrt<double>(double a) { return sqrt(a); }
 template <>
 __device__ __forceinline__ float tsqrt<float>(float a) { return sqrtf(a); }
 
-template <typename T>
+// Flux arithmetic tags: double (the drop-in), float (the FP32-flux form),
+// WaveF32 (the wave-speed estimates SL, SR and the sound speeds behind them
+// in FP32, every flux and star state in FP64).
+struct WaveF32 {};
+template <typename TF>
+struct FluxArith {
+    using type = TF;
+};
+template <>
+struct FluxArith<WaveF32> {
+    using type = double;
+};
+template <typename TF>
+struct WaveArith {
+    using type = TF;
+};
+template <>
+struct WaveArith<WaveF32> {
+    using type = float;
+};
+
+template <typename TF>
 __device__ __forceinline__ double hllc_flux(double gamma, double kurant, const St5& L, const St5& R, double Wd,
                                             double n1d, double n2d, double rad, int metod, bool nul_potok,
                                             FluxOut<double>& out) {
+    using T = typename FluxArith<TF>::type;
+    using TW = typename WaveArith<TF>::type;
     const T ggg = (T)gamma, g1 = (T)(gamma - 1.0);
     const T n1 = (T)n1d, n2 = (T)n2d, W = (T)Wd;
     const T ro_L = (T)L.ro, Q_L = (T)L.Q, p_L = (T)L.p, v1_L = (T)L.u, v2_L = (T)L.v;
@@ -136,12 +159,14 @@ __device__ __forceinline__ double hllc_flux(double gamma, double kurant, const S
     const T v1 = v1_L * t1 + v2_L * t2;
     const T u2 = v1_R * n1 + v2_R * n2;
     const T v2 = v1_R * t1 + v2_R * t2;
-    const T cL = tsqrt<T>(ggg * p_L / ro_L);
-    const T cR = tsqrt<T>(ggg * p_R / ro_R);
+    // sound speeds and the HLL wave-speed estimates in the wave arithmetic
+    // (the flux arithmetic except for WaveF32)
+    const TW cL = tsqrt<TW>((TW)gamma * (TW)L.p / (TW)L.ro);
+    const TW cR = tsqrt<TW>((TW)gamma * (TW)R.p / (TW)R.ro);
     const T uu_L = (v1_L * v1_L + v2_L * v2_L) / (T)2;
     const T uu_R = (v1_R * v1_R + v2_R * v2_R) / (T)2;
-    const T SL = tmin<T>(u1, u2) - tmax<T>(cL, cR);
-    const T SR = tmax<T>(u1, u2) + tmax<T>(cL, cR);
+    const T SL = (T)((TW)tmin<T>(u1, u2) - tmax<TW>(cL, cR));
+    const T SR = (T)((TW)tmax<T>(u1, u2) + tmax<TW>(cL, cR));
     const T suR = (SR - u2);
     const T suL = (SL - u1);
     const T SM = (suR * ro_R * u2 - suL * ro_L * u1 - p_R + p_L) / (suR * ro_R - suL * ro_L);

@@ -1110,12 +1110,11 @@ __device__ __forceinline__ void mk2_flux_unit(const DevMesh& d, const gelios_par
     if (!(procK || procN)) return;
     const size_t ng = d.n_slots;
     const double dt = *b.dt_cur;
-    const uint32_t info = d.u_info[u];
     const int A = d.u_A[u], B = d.u_B[u];
     const double x4 = (d.X2[A] + d.X2[B]) / 2.0, y4 = (d.Y2[A] + d.Y2[B]) / 2.0;
     const double W = ((x4 - r.x2) * r.n1 + (y4 - r.y2) * r.n2) / dt;
     const int g = d.u_slot[u], gt = d.u_twin[u];
-    const bool np = (info & SI_NP) != 0;
+    const bool np = (d.u_info[u] & SI_NP) != 0;
     FluxOut<double> F;
     const double UU = hllc_flux<TF>(P.gamma, P.kurant, r.a, r.o, W, r.n1, r.n2, 1.0, 0, np, F);
     const double S = r.S;
@@ -1499,11 +1498,10 @@ __global__ void __launch_bounds__(NT, MINB) mk2_tile_kernel(DevMesh d, gelios_pa
         const bool procK = !(r.dist < 0.0), procN = !(r.distn < 0.0);
         if (!(procK || procN)) continue;
         const double dt = *b.dt_cur;
-        const uint32_t info = d.u_info[u];
         const int A = d.u_A[u], B = d.u_B[u];
         const double x4 = (d.X2[A] + d.X2[B]) / 2.0, y4 = (d.Y2[A] + d.Y2[B]) / 2.0;
         const double W = ((x4 - r.x2) * r.n1 + (y4 - r.y2) * r.n2) / dt;
-        const bool np = (info & SI_NP) != 0;
+        const bool np = (d.u_info[u] & SI_NP) != 0;
         FluxOut<double> F;
         const double UU = hllc_flux<TF>(P.gamma, P.kurant, r.a, r.o, W, r.n1, r.n2, 1.0, 0, np, F);
         const double S = r.S;
@@ -2208,6 +2206,8 @@ __global__ void hllc_batch_kernel(gelios_params P, int n, const double* __restri
     double t;
     if (P.precision == GELIOS_PREC_FP32_FLUX)
         t = hllc_flux<float>(P.gamma, P.kurant, L, R, a[10], a[11], a[12], a[13], (int)a[14], a[15] != 0.0, F);
+    else if (P.precision == GELIOS_PREC_FP32_WAVES)
+        t = hllc_flux<WaveF32>(P.gamma, P.kurant, L, R, a[10], a[11], a[12], a[13], (int)a[14], a[15] != 0.0, F);
     else
         t = hllc_flux<double>(P.gamma, P.kurant, L, R, a[10], a[11], a[12], a[13], (int)a[14], a[15] != 0.0, F);
     t = P.kurant * a[13] / t;
@@ -3470,6 +3470,8 @@ void launch_stationary_units(const DevMesh& d, const gelios_params& P, const Ste
                              cudaStream_t s) {
     if (P.precision == GELIOS_PREC_FP32_FLUX)
         stationary_unit_kernel<float><<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, b, fl);
+    else if (P.precision == GELIOS_PREC_FP32_WAVES)
+        stationary_unit_kernel<WaveF32><<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, b, fl);
     else
         stationary_unit_kernel<double><<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, P, b, fl);
 }
@@ -3479,8 +3481,10 @@ void launch_stationary_update(const DevMesh& d, const gelios_params& P, const St
 }
 cudaError_t launch_stationary_persistent(const DevMesh& d, const gelios_params& P, const StepBuffers& b0,
                                          const StepBuffers& b1, double* fl, int nsteps, cudaStream_t s) {
-    const bool f32 = P.precision == GELIOS_PREC_FP32_FLUX;
-    const void* fn = f32 ? reinterpret_cast<const void*>(&stationary_persistent_kernel<float>)
+    const void* fn = P.precision == GELIOS_PREC_FP32_FLUX
+                         ? reinterpret_cast<const void*>(&stationary_persistent_kernel<float>)
+                     : P.precision == GELIOS_PREC_FP32_WAVES
+                         ? reinterpret_cast<const void*>(&stationary_persistent_kernel<WaveF32>)
                          : reinterpret_cast<const void*>(&stationary_persistent_kernel<double>);
     int dev = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -3524,10 +3528,12 @@ void launch_unit_geometry(const DevMesh& d, double gamma, const double* cx, cons
     if (d.n_units > 0) unit_geometry_kernel<<<blocks_for(d.n_units, 128), 128, 0, s>>>(d, 2 * gamma, cx, cy, upf);
 }
 cudaError_t launch_stationary_batch(const DevMesh& d, const PlainInstance* inst, const int* active, int n_active,
-                                    int nsteps, bool fp32, cudaStream_t s) {
+                                    int nsteps, int prec, cudaStream_t s) {
     if (n_active <= 0 || nsteps <= 0) return cudaSuccess;
-    const void* fn = fp32 ? reinterpret_cast<const void*>(&stationary_batch_kernel<float>)
-                          : reinterpret_cast<const void*>(&stationary_batch_kernel<double>);
+    const void* fn = prec == GELIOS_PREC_FP32_FLUX ? reinterpret_cast<const void*>(&stationary_batch_kernel<float>)
+                     : prec == GELIOS_PREC_FP32_WAVES
+                         ? reinterpret_cast<const void*>(&stationary_batch_kernel<WaveF32>)
+                         : reinterpret_cast<const void*>(&stationary_batch_kernel<double>);
     int dev = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

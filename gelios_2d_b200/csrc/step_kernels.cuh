@@ -144,7 +144,7 @@ struct PlainInstance {
 // `nsteps` steps of the instances listed in `active` (device arrays) in one
 // cooperative launch; returns the launch's error code.
 cudaError_t launch_stationary_batch(const DevMesh& d, const PlainInstance* inst, const int* active, int n_active,
-                                    int nsteps, bool fp32, cudaStream_t s);
+                                    int nsteps, int prec, cudaStream_t s);
 void launch_plain_batch_words_init(const PlainInstance* inst, const int* active, int n, cudaStream_t s);
 // Tiles of the moving-grid step, built at topology upload: spatially compact
 // groups of at most kTileCells cells.  Cells of tile t are

@@ -43,8 +43,10 @@ def sample_inflows(n: int, seed: int) -> np.ndarray:
     return PARAM_LO + u * (PARAM_HI - PARAM_LO)
 
 
-def inflow_params(theta, fp32: bool = False) -> N.GeliosParams:
-    """gelios_params of the plain workload with the inflow of `theta`."""
+def inflow_params(theta, fp32: int = 0) -> N.GeliosParams:
+    """gelios_params of the plain workload with the inflow of `theta`;
+    fp32: 0 (or False) FP64 fluxes, 1 (or True) FP32 fluxes, 2 FP32 wave
+    speeds with the fluxes assembled in FP64 (N.PREC_*)."""
     ro, u, mach, chi, mach_in = (float(v) for v in theta)
     p = plain_params()
     g = p.gamma
@@ -54,7 +56,7 @@ def inflow_params(theta, fp32: bool = False) -> N.GeliosParams:
     p.in_v = 0.0
     p.chi = chi
     p.inner_mach = mach_in
-    p.precision = N.PREC_FP32_FLUX if fp32 else N.PREC_FP64
+    p.precision = int(fp32)
     return p
 
 
@@ -386,6 +388,7 @@ def experiment(mesh: Mesh, n_train=256, n_test=32, tol=1e-6, max_steps=3_000_000
     dl = solve_in_chunks(mesh, th_te, delta_te, tol, max_steps, check_every, chunk, False, device)
     w32 = (solve_in_chunks(mesh, th_te, warm_te, tol, fp32_max_steps, check_every, chunk, True, device)
            if fp32_max_steps > 0 else None)
+    w32w = solve_in_chunks(mesh, th_te, warm_te, tol, max_steps, check_every, chunk, N.PREC_FP32_WAVES, device)
     serial = [solve_single(mesh, th_te[i], cold_te[i], tol, max_steps, check_every, False, device)
               for i in range(min(n_serial, n_test))]
     ws.close()
@@ -413,6 +416,7 @@ def experiment(mesh: Mesh, n_train=256, n_test=32, tol=1e-6, max_steps=3_000_000
         "predict_s": predict_s, "fallbacks": int(sum(1 for _, ok in warm if not ok)),
         "cold_fp64": stats(cold), "nearest_fp64": stats(nn), "warm_fp64": stats(w64), "delta_fp64": stats(dl),
         "warm_fp32flux": stats(w32) | {"max_steps": fp32_max_steps} if w32 is not None else None,
+        "warm_fp32waves": stats(w32w),
         "serial_cold_fp64": {"instances": len(serial), "wall_s_per_instance": serial_per,
                              "wall_s_projected_all": serial_per * n_test if serial_per else None,
                              "steps": [int(s.steps[0]) for s in serial]},
@@ -420,6 +424,7 @@ def experiment(mesh: Mesh, n_train=256, n_test=32, tol=1e-6, max_steps=3_000_000
         "nearest_vs_converged": diff(Solve(None, None, None, np.stack(nn_te), 0.0), cold),
         "delta_vs_converged": diff(Solve(None, None, None, np.stack(delta_te), 0.0), cold),
         "converged_warm_vs_cold": diff(w64, cold), "converged_warm32_vs_cold": diff(w32, cold),
+        "converged_warm32waves_vs_cold": diff(w32w, cold),
         "converged_nearest_vs_cold": diff(nn, cold), "converged_delta_vs_cold": diff(dl, cold),
     }
     return out, gen.states

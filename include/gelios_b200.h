@@ -53,8 +53,14 @@ enum {
     GELIOS_FORM_MHD_PUI = 4     /* ion MHD fluid + pickup protons on the moving grid: no reference step (see below) */
 };
 
-/* Riemann-solver precision (geometry, accumulation and the dt reduction stay FP64). */
-enum { GELIOS_PREC_FP64 = 0, GELIOS_PREC_FP32_FLUX = 1 };
+/* Riemann-solver precision (geometry, accumulation and the dt reduction stay FP64).
+ * GELIOS_PREC_FP32_FLUX: the approximate Riemann solvers in FP32.
+ * GELIOS_PREC_FP32_WAVES: the plain form's HLLC (GELIOS_FORM_STATIONARY and
+ * plain batches) with its sound speeds and wave-speed estimates SL, SR in
+ * FP32 and every flux and star state in FP64, so that the FP32 rounding no
+ * longer sets a residual floor; the other forms run it as FP64.  No
+ * counterpart in the reference (FP64 throughout). */
+enum { GELIOS_PREC_FP64 = 0, GELIOS_PREC_FP32_FLUX = 1, GELIOS_PREC_FP32_WAVES = 2 };
 
 /* Runtime replacement of the reference's compile-time constants
  * (Help.h:39-114, Gran.cpp:216-281, Setka.cpp:3380/5256/10129/10169,

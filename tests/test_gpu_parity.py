@@ -74,6 +74,22 @@ def test_hllc_fp32_flux_form():
     assert np.max(err) <= 1e-5, np.max(err)
 
 
+def test_hllc_fp32_wave_speed_form():
+    """FP32 sound speeds and wave-speed estimates, fluxes assembled in FP64:
+    against the reference's HLLC / HLL golden vectors the fluxes move by the
+    wave speeds' float rounding only, well inside the full FP32 form's
+    error."""
+    d = np.load(GOLD / "kat_hllc.npz")
+    ref = d["outputs"]
+    rows = np.max(np.abs(ref[:, 1:6]), axis=1, keepdims=True)
+    errs = {}
+    for prec in (N.PREC_FP32_WAVES, N.PREC_FP32_FLUX):
+        dev = g.hllc_batch(N.reference_params(precision=prec), d["inputs"])
+        errs[prec] = float(np.max(np.abs(dev[:, 1:6] - ref[:, 1:6]) / rows))
+    assert errs[N.PREC_FP32_WAVES] <= 1e-6, errs
+    assert errs[N.PREC_FP32_WAVES] < errs[N.PREC_FP32_FLUX], errs
+
+
 def test_godunov_device_vs_oracle():
     d = np.load(GOLD / "kat_godunov.npz")
     P = N.reference_params()
@@ -330,7 +346,7 @@ def test_launch_count_reported():
     assert dev.launches() == 1 + 3 * 5  # words + (face units, cell update, dt) per step; geometry cached
 
 
-@pytest.mark.parametrize("precision", [N.PREC_FP64, N.PREC_FP32_FLUX])
+@pytest.mark.parametrize("precision", [N.PREC_FP64, N.PREC_FP32_FLUX, N.PREC_FP32_WAVES])
 def test_stationary_persistent_matches_three_kernel_steps(precision):
     """The cooperative multi-step launch and the three kernels per step
     (phase timing on) agree to rounding (the shared bodies are compiled into
@@ -349,7 +365,9 @@ def test_stationary_persistent_matches_three_kernel_steps(precision):
         out.append((dev.par(1), st.dt, st.n_ro_clamp, st.n_p_clamp, st.flags))
     # FP64: rounding of the last bits; FP32 fluxes: float rounding (1e-7 per
     # operation) compounds over the 25 steps
-    tol = 1e-13 if precision == N.PREC_FP64 else 1e-4
+    # FP32 wave speeds: a float rounding of a wave speed that flips between
+    # the two kernels moves one face's dissipation by ~1e-7 of itself
+    tol = {N.PREC_FP64: 1e-13, N.PREC_FP32_FLUX: 1e-4, N.PREC_FP32_WAVES: 1e-6}[precision]
     assert rel_err(out[0][0], out[1][0]) <= tol
     assert abs(out[0][1] - out[1][1]) <= tol * out[1][1]
     assert out[0][2:] == out[1][2:]
