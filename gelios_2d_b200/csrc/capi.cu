@@ -1511,7 +1511,8 @@ extern "C" int gelios_step(gelios_ctx* ctx, int form, int nsteps, gelios_status*
             ctx->coop_off = true;
         }
     }
-    if (form == GELIOS_FORM_MK2 && nsteps > 0 && pipe_ok(ctx)) {
+    // a one-step call has no next step to overlap: one graph per step
+    if (form == GELIOS_FORM_MK2 && nsteps > 1 && pipe_ok(ctx)) {
         const int n = mk2_pipelined(ctx, nsteps, cen0, cen1);
         if (n < 0) return n;
         launches += n;

@@ -393,11 +393,12 @@ int gelios_set_variant(gelios_ctx *ctx, int form, int32_t variant);
  * 0 for forms without variants). */
 int gelios_get_variant(gelios_ctx *ctx, int form, int32_t *variant);
 /* Pipelined moving-grid calls (on by default; no counterpart in the
- * reference): within a call of GELIOS_FORM_MK2 steps, the next step's
- * surface tracking and rail motion (Setka::Move_surface,
+ * reference): within a call of two or more GELIOS_FORM_MK2 steps, the next
+ * step's surface tracking and rail motion (Setka::Move_surface,
  * Move_Setka_Calculate_2) run while the cells they do not read are still
  * being updated.  Same results bit for bit as one step after the other
- * (on = 0), which the tile variants (4-7) and phase timing always use. */
+ * (on = 0), which one-step calls, the tile variants (4-7) and phase timing
+ * always use. */
 int gelios_set_pipelined(gelios_ctx *ctx, int on);
 
 /* ---- per-face solvers on the device (known-answer checks) ------------------
