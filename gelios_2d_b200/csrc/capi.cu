@@ -864,7 +864,8 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     }
     {
         std::vector<int32_t> minus1(nc, -1);
-        rc |= upload(ctx->src_lo, minus1.data(), nc, s);
+        std::vector<int32_t> minus1x2(2 * static_cast<size_t>(nc), -1);
+        rc |= upload(ctx->src_lo, minus1x2.data(), minus1x2.size(), s);
     }
     rc |= upload<double>(ctx->state[0], nullptr, 5 * static_cast<size_t>(nc), s);
     rc |= upload<double>(ctx->state[1], nullptr, 5 * static_cast<size_t>(nc), s);
@@ -954,8 +955,8 @@ extern "C" int gelios_upload_topology(gelios_ctx* ctx, const gelios_mesh_view* v
     d.r_istoch = ctx->r_istoch.as<double>();
     d.cback = ctx->cback.as<int32_t>();
     d.cnext = ctx->cnext.as<int32_t>();
-    d.src_lo = chains_ok ? ctx->src_lo.as<int32_t>() : nullptr;
-    d.src_lo_out = chains_ok ? ctx->src_lo.as<int32_t>() : nullptr;
+    d.src_lo = chains_ok ? reinterpret_cast<const int2*>(ctx->src_lo.as<int32_t>()) : nullptr;
+    d.src_lo_out = chains_ok ? reinterpret_cast<int2*>(ctx->src_lo.as<int32_t>()) : nullptr;
     ctx->tiles = TileView();
     ctx->tiles.n_tiles = static_cast<int>(tb.cstart.size()) - 1;
     ctx->tiles.max_slots = tb.max_slots;
@@ -1161,8 +1162,14 @@ int enqueue_mhd(gelios_ctx* ctx, const StepBuffers& b) {
     const int nm = launch_motion(d, P, b, ctx->surface.as<double>(), s);
     ctx->phase_end(2, e1, nm);
     cudaEvent_t e3 = ctx->phase_begin();
+    // the plain interior face units on the main stream, the other groups
+    // (C_1, tracked, one-sided units) beside them on the side stream
+    GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_fork, s));
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
     const int nfc = launch_mhd_faces(d, P, ctx->mprm, b, ctx->hstate[cur].as<double>(), ctx->flux_mhd.as<double>(),
-                                     s, ctx->mhd_face_variant);
+                                     s, ctx->mhd_face_variant, ctx->side);
+    GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_tracked, ctx->side));
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_tracked, 0));
     ctx->phase_end(1, e3, nfc);
     cudaEvent_t e5 = ctx->phase_begin();
     launch_mhd_update(d, P, b, ctx->flux_mhd.as<double>(), ctx->src_fixed.as<double>(), ctx->hstate[cur].as<double>(),
@@ -1341,9 +1348,14 @@ int enqueue_pipe_step(gelios_ctx* ctx, int st, const StepBuffers& b, const StepB
     double* fl = ctx->flux.as<double>();
     double* aux = ctx->aux.as<double>();
     int n = 0;
+    // the source terms on the motion stream (idle until step st's early
+    // update), the tracked-face fluxes and the small face-unit groups on the
+    // side stream, the plain face units on the main stream
     GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_fork, s));
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_fork, 0));
-    launch_mk2_source(d, P, b, aux, sd);
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(sm, ctx->ev_fork, 0));
+    launch_mk2_source(d, P, b, aux, sm);
+    GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_motion, sm));
     n++;
     n += launch_mk2_flux_tracked(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(), fl, sd);
     GELIOS_CUDA_TRY(launch_mk2_cells(d, P, b, ctx->tiles, fl, aux, sd, v, 3));
@@ -1352,6 +1364,7 @@ int enqueue_pipe_step(gelios_ctx* ctx, int st, const StepBuffers& b, const StepB
     GELIOS_CUDA_TRY(launch_mk2_cells(d, P, b, ctx->tiles, fl, aux, s, v, 1));
     n += mk2_variant_launches(d, v, 1);
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_tracked, 0));
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_motion, 0));
     if (!bn) {
         launch_mk2_update(d, P, b, fl, aux, s, 3, nullptr, 0);
         launch_commit(d, b, s, true);

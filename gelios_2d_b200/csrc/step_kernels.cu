@@ -380,11 +380,16 @@ __device__ void tvd_radial(const double* const* st, const double* cx, const doub
 // whose r_istoch bracket the centroid radius rr (K_posle = Next(K_do)).
 // Returns false (and raises ST_CHAIN) where the reference would follow a
 // missing Back/Next link.
-__device__ bool source_bracket(const DevMesh& d, int k, double rr, int& K_do, int& K_posle, int* status) {
+// `cached` (out): the cache entry read, so that the caller rewrites it only
+// where the bracket changed.
+__device__ bool source_bracket(const DevMesh& d, int k, double rr, int& K_do, int& K_posle, int* status,
+                               int2* cached_out = nullptr) {
     K_do = d.cback[k];
     K_posle = d.cnext[k];
     const double ri = d.r_istoch[k];
-    const int cached = d.src_lo ? d.src_lo[k] : -1;
+    const int2 cpair = d.src_lo ? d.src_lo[k] : make_int2(-1, -1);
+    if (cached_out) *cached_out = cpair;
+    const int cached = cpair.x;
     if (cached >= 0) {
         // The reference walks the radial chain from the cell itself.  Along
         // a chain r_istoch increases strictly (checked at upload), so the
@@ -393,6 +398,25 @@ __device__ bool source_bracket(const DevMesh& d, int k, double rr, int& K_do, in
         // Searching from last step's bracket finds the same pair in a step
         // or two.
         const bool caseA = rr < ri;
+        {
+            // the walk's first step, from the cached pair (hi = Next(lo)
+            // cached too): both radii and the link the reference
+            // dereferences are loaded together, one level of loads
+            const int hi = cpair.y;
+            const double rlo = d.r_istoch[cached], rhi = d.r_istoch[hi];
+            const int link = caseA ? d.cback[cached] : d.cnext[hi];
+            const bool below = caseA ? (rr < rlo) : !(rr > rlo);
+            const bool above = caseA ? !(rr < rhi) : (rr > rhi);
+            if (!below && !above) {
+                if (link < 0) {
+                    *status |= ST_CHAIN;
+                    return false;
+                }
+                K_do = cached;
+                K_posle = hi;
+                return true;
+            }
+        }
         int lo = cached;
         int guard = 0;
         for (;;) {
@@ -531,7 +555,7 @@ __device__ void source_mk1(const DevMesh& d, const gelios_params& P, int k, doub
             q1 = q2 = q3 = 0.0;
             return;
         }
-        if (d.src_lo_out) d.src_lo_out[k] = K_do;
+        if (d.src_lo_out) d.src_lo_out[k] = make_int2(K_do, K_posle);
     }
     const double pro = p / ro;
     const double kin = sq(u) + sq(v);
@@ -1302,8 +1326,9 @@ __global__ void __launch_bounds__(128, GELIOS_SOURCE_MINB) mk2_source_kernel(Dev
     }
     int K_do = -1, K_posle = -1, ok = 1;
     if (interp && sp == 0) {
-        ok = source_bracket(d, c, rr, K_do, K_posle, &status) ? 1 : 0;
-        if (ok && d.src_lo_out) d.src_lo_out[c] = K_do;
+        int2 cached;
+        ok = source_bracket(d, c, rr, K_do, K_posle, &status, &cached) ? 1 : 0;
+        if (ok && d.src_lo_out && cached.x != K_do) d.src_lo_out[c] = make_int2(K_do, K_posle);
     }
     K_do = __shfl_sync(full, K_do, q0);
     K_posle = __shfl_sync(full, K_posle, q0);
@@ -3747,11 +3772,12 @@ void launch_godunov_batch(const gelios_params& P, int n, const double* in, doubl
     godunov_batch_kernel<<<blocks_for(n, 2), 64, 0, s>>>(P, n, in, out);
 }
 namespace {
-// The plain interior group in the variant's shape, the other groups (a few
-// percent of the units, every branch) in one fixed shape after it.
+// The plain interior group in the variant's shape on stream s, the other
+// groups (a few percent of the units, every branch) in one fixed shape on
+// stream sr (s itself, or a stream the caller forks and joins).
 template <int BLOCK, int MINB>
 void mhd_faces_shape(const DevMesh& d, const gelios_params& P, const gelios_mhd_params& M, const StepBuffers& b,
-                     const double* hcur, double* fl, cudaStream_t s) {
+                     const double* hcur, double* fl, cudaStream_t s, cudaStream_t sr) {
     const int n0 = d.u_c1, nr = d.n_units - d.u_c1;
     const bool f32 = P.precision == GELIOS_PREC_FP32_FLUX;
     if (n0 > 0) {
@@ -3762,9 +3788,9 @@ void mhd_faces_shape(const DevMesh& d, const gelios_params& P, const gelios_mhd_
     }
     if (nr > 0) {
         if (f32)
-            mhd_face_kernel<float, 128, 3, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, M, b, hcur, fl);
+            mhd_face_kernel<float, 128, 3, false><<<blocks_for(nr, 128), 128, 0, sr>>>(d, P, M, b, hcur, fl);
         else
-            mhd_face_kernel<double, 128, 3, false><<<blocks_for(nr, 128), 128, 0, s>>>(d, P, M, b, hcur, fl);
+            mhd_face_kernel<double, 128, 3, false><<<blocks_for(nr, 128), 128, 0, sr>>>(d, P, M, b, hcur, fl);
     }
 }
 }  // namespace
@@ -3774,15 +3800,16 @@ const char* mhd_face_variant_name(int v) {
     return (v >= 0 && v < kMhdFaceVariants) ? names[v] : "?";
 }
 int launch_mhd_faces(const DevMesh& d, const gelios_params& P, const gelios_mhd_params& M, const StepBuffers& b,
-                     const double* hcur, double* fl, cudaStream_t s, int variant) {
+                     const double* hcur, double* fl, cudaStream_t s, int variant, cudaStream_t s_rest) {
     if (d.n_units <= 0) return 0;
+    cudaStream_t sr = s_rest ? s_rest : s;
     switch (variant) {
-        case 1: mhd_faces_shape<128, 1>(d, P, M, b, hcur, fl, s); break;
-        case 2: mhd_faces_shape<128, 4>(d, P, M, b, hcur, fl, s); break;
-        case 3: mhd_faces_shape<64, 6>(d, P, M, b, hcur, fl, s); break;
-        case 4: mhd_faces_shape<64, 3>(d, P, M, b, hcur, fl, s); break;
-        case 5: mhd_faces_shape<256, 1>(d, P, M, b, hcur, fl, s); break;
-        default: mhd_faces_shape<128, 3>(d, P, M, b, hcur, fl, s); break;
+        case 1: mhd_faces_shape<128, 1>(d, P, M, b, hcur, fl, s, sr); break;
+        case 2: mhd_faces_shape<128, 4>(d, P, M, b, hcur, fl, s, sr); break;
+        case 3: mhd_faces_shape<64, 6>(d, P, M, b, hcur, fl, s, sr); break;
+        case 4: mhd_faces_shape<64, 3>(d, P, M, b, hcur, fl, s, sr); break;
+        case 5: mhd_faces_shape<256, 1>(d, P, M, b, hcur, fl, s, sr); break;
+        default: mhd_faces_shape<128, 3>(d, P, M, b, hcur, fl, s, sr); break;
     }
     return (d.u_c1 > 0 ? 1 : 0) + (d.n_units > d.u_c1 ? 1 : 0);
 }

@@ -69,8 +69,9 @@ struct DevMesh {
     const int32_t *cback = nullptr, *cnext = nullptr;
     // bracket of the source interpolation found in the previous step (lower
     // cell, -1 = none); used when the chains are consistent (see source_mk1)
-    const int32_t* src_lo = nullptr;
-    int32_t* src_lo_out = nullptr;
+    // (lower cell, Next of it) of the previous step's bracket, {-1, -1} = none
+    const int2* src_lo = nullptr;
+    int2* src_lo_out = nullptr;
 };
 
 // Buffers of one time step (double buffering of the state like par[now1] ->
@@ -229,8 +230,9 @@ constexpr int kMhdFluxRows = 13;
 constexpr int kMhdFaceVariants = 6;
 const char* mhd_face_variant_name(int v);
 // Returns the number of launches (the plain interior group, then the rest).
+// s_rest: stream of the groups other than the plain interior one (null: s)
 int launch_mhd_faces(const DevMesh& d, const gelios_params& P, const gelios_mhd_params& M, const StepBuffers& b,
-                     const double* hcur, double* fl, cudaStream_t s, int variant = 0);
+                     const double* hcur, double* fl, cudaStream_t s, int variant = 0, cudaStream_t s_rest = nullptr);
 void launch_mhd_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
                        const double* src, const double* hcur, double* hnxt, cudaStream_t s);
 // ---- batched MHD step: many instances, one launch per phase
