@@ -79,7 +79,7 @@ STEP_KERNELS = {
     "mk2": "whole moving-grid step, pipelined: source, tracked flux, face units (reconstruction + flux, "
            "autotuned arrangement), update of the cells the next motion reads, then the next step's dt, "
            "surface_faces, rails, tracked recon + solve beside the update of the other cells "
-           "(CUDA graphs, 3 streams; one commit per call)",
+           "(CUDA graphs, 4 streams; one commit per call)",
     "plain": "whole plain step: stationary_persistent_kernel (face units, cell update, dt; all steps of a call "
              "in one cooperative launch)",
     "k5": "whole four-fluid step: centroid, surface_faces, rails, k5_cell, commit",

@@ -93,6 +93,10 @@ struct gelios_ctx {
     // next step's motion reads (see mk2_pipelined)
     cudaStream_t motion = nullptr;
     cudaEvent_t ev_early = nullptr, ev_motion = nullptr, ev_side2 = nullptr;
+    // the C_1 interior and one-sided face-unit groups beside the tracked-face
+    // fluxes in a pipelined call
+    cudaStream_t groups = nullptr;
+    cudaEvent_t ev_groups = nullptr;
     DBuf early;       // cells flagged CF_EARLY, updated first
     int n_early = 0;
     bool pipelined = true;  // gelios_set_pipelined
@@ -282,7 +286,8 @@ extern "C" int gelios_create(gelios_ctx** out, const gelios_params* prm, int dev
     GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_rails, cudaEventDisableTiming));
     GELIOS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_tracked, cudaEventDisableTiming));
     GELIOS_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->motion, cudaStreamNonBlocking, prio_greatest));
-    for (cudaEvent_t* e : {&ctx->ev_early, &ctx->ev_motion, &ctx->ev_side2})
+    GELIOS_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->groups, cudaStreamNonBlocking, prio_least));
+    for (cudaEvent_t* e : {&ctx->ev_early, &ctx->ev_motion, &ctx->ev_side2, &ctx->ev_groups})
         GELIOS_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     if (ctx->words.alloc(64)) return GELIOS_E_CUDA;
     GELIOS_CUDA_TRY(cudaMemsetAsync(ctx->words.p, 0, 64, ctx->stream));
@@ -311,13 +316,13 @@ extern "C" void gelios_destroy(gelios_ctx* ctx) {
         cudaStreamSynchronize(ctx->stream);
         cudaStreamDestroy(ctx->stream);
     }
-    for (cudaStream_t* sp : {&ctx->side, &ctx->motion, &ctx->io_h2d, &ctx->io_d2h})
+    for (cudaStream_t* sp : {&ctx->side, &ctx->motion, &ctx->groups, &ctx->io_h2d, &ctx->io_d2h})
         if (*sp) {
             cudaStreamSynchronize(*sp);
             cudaStreamDestroy(*sp);
         }
     for (cudaEvent_t e : {ctx->ev_fork, ctx->ev_recon, ctx->ev_rails, ctx->ev_tracked, ctx->ev_early,
-                          ctx->ev_motion, ctx->ev_side2})
+                          ctx->ev_motion, ctx->ev_side2, ctx->ev_groups})
         if (e) cudaEventDestroy(e);
     for (int j = 0; j < 2; j++)
         for (cudaEvent_t e : {ctx->ev_in_ready[j], ctx->ev_in_free[j], ctx->ev_out_ready[j], ctx->ev_out_free[j]})
@@ -1349,8 +1354,9 @@ int enqueue_pipe_step(gelios_ctx* ctx, int st, const StepBuffers& b, const StepB
     double* aux = ctx->aux.as<double>();
     int n = 0;
     // the source terms on the motion stream (idle until step st's early
-    // update), the tracked-face fluxes and the small face-unit groups on the
-    // side stream, the plain face units on the main stream
+    // update), the tracked-face fluxes on the side stream, the C_1 interior
+    // and one-sided face-unit groups on the groups stream, the plain face
+    // units on the main stream
     GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_fork, s));
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_fork, 0));
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(sm, ctx->ev_fork, 0));
@@ -1358,12 +1364,15 @@ int enqueue_pipe_step(gelios_ctx* ctx, int st, const StepBuffers& b, const StepB
     GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_motion, sm));
     n++;
     n += launch_mk2_flux_tracked(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(), fl, sd);
-    GELIOS_CUDA_TRY(launch_mk2_cells(d, P, b, ctx->tiles, fl, aux, sd, v, 3));
-    n += mk2_variant_launches(d, v, 3);
     GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_tracked, sd));
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(ctx->groups, ctx->ev_fork, 0));
+    GELIOS_CUDA_TRY(launch_mk2_cells(d, P, b, ctx->tiles, fl, aux, ctx->groups, v, 3));
+    n += mk2_variant_launches(d, v, 3);
+    GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_groups, ctx->groups));
     GELIOS_CUDA_TRY(launch_mk2_cells(d, P, b, ctx->tiles, fl, aux, s, v, 1));
     n += mk2_variant_launches(d, v, 1);
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_tracked, 0));
+    GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_groups, 0));
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_motion, 0));
     if (!bn) {
         launch_mk2_update(d, P, b, fl, aux, s, 3, nullptr, 0);
