@@ -54,6 +54,8 @@ WORKLOADS = {
     "mhd_200k": ("ion MHD fluid (HLLD) + pickup protons (HLLC) on the moving grid Setka(200,100,50,100,100,100,"
                  "150,150): LISM B=0.01 at 30 deg, seeded fixed charge-exchange sources", "mhd",
                  (200, 100, 50, 100, 100, 100, 150, 150)),
+    "mhd_8k": ("ion MHD fluid (HLLD) + pickup protons (HLLC) on the moving grid Setka(30,7,11,20,60,20,40,40): "
+               "LISM B=0.01 at 30 deg, seeded fixed charge-exchange sources", "mhd", (30, 7, 11, 20, 60, 20, 40, 40)),
     "mhd_1m": ("ion MHD fluid (HLLD) + pickup protons (HLLC) on the moving grid Setka(480,240,100,220,200,200,300,"
                "300): LISM B=0.01 at 30 deg, seeded fixed charge-exchange sources", "mhd",
                (480, 240, 100, 220, 200, 200, 300, 300)),
@@ -388,25 +390,26 @@ def time_to_residual(workload, mesh, params, st0, mc, form, fcode, device, tol, 
     return out
 
 
-def march_record(mesh, params, st0, mc, fcode, device, total, every) -> list:
-    """The moving-grid step marched from the workload's initial field in
-    calls of `every` steps (each call restarts dt at dt0, as the reference's
-    time loop does), recording after each call: the step residual per unit
-    time (sum|ro(n+1)-ro(n)| / (dt sum|ro(n+1)|), which contains the volume
-    change of moving cells), the operator residual with the grid held still
-    (gelios_operator_residual: flux balance per unit volume, face speeds 0),
-    the largest and the mean point displacement per step over the call, dt
-    and the status flags."""
+def march_record(mesh, params, st0, mc, fcode, device, total, every, form="mk2") -> list:
+    """A moving-grid step (the MK2 form, or the MHD + pickup form) marched
+    from the workload's initial field in calls of `every` steps (each call
+    restarts dt at dt0, as the reference's time loop does), recording after
+    each call: the step residual per unit time (sum|ro(n+1)-ro(n)| / (dt
+    sum|ro(n+1)|), which contains the volume change of moving cells), the
+    operator residual with the grid held still (gelios_operator_residual:
+    (ion) mass flux balance per unit volume, face speeds 0), the largest and
+    the mean point displacement per step over the call, dt and the status
+    flags."""
     import gelios_2d_b200 as g
 
     S = g.Setka(mesh, params, device=device)
-    load_inputs(S, "mk2", st0, mc)
+    load_inputs(S, form, st0, mc)
     x0, y0 = S.points()
     out = []
     done = 0
     while done < total:
         n = min(every, total - done)
-        st = S.Go_5_komponent__MK2(n)
+        st = S.step(fcode, n)
         done += n
         x1, y1 = S.points()
         mv = np.hypot(x1 - x0, y1 - y0)
@@ -414,7 +417,7 @@ def march_record(mesh, params, st0, mc, fcode, device, total, every) -> list:
         rb = int(st.result_buf)
         r_step = S.residual(rb) / st.dt if st.dt > 0 else float("nan")
         rec = {"steps": done, "dt": float(st.dt), "flags": int(st.flags), "step_residual_per_time": float(r_step),
-               "operator_residual_per_time": float(S.operator_residual(rb)),
+               "operator_residual_per_time": float(S.operator_residual(rb, fcode)),
                "point_move_per_step_max": float(np.max(mv) / n), "point_move_per_step_mean": float(np.mean(mv) / n)}
         out.append(rec)
         if st.flags or not np.isfinite(r_step):
@@ -800,8 +803,8 @@ def main():
     }
     if args.precision == "fp32flux" and rank == 0:
         line["fp32_flux_errors"] = fp32_flux_errors(mesh, params, st0, mc, fcode, device, form=form)
-    if args.march is not None and rank == 0 and form == "mk2":
-        line["march"] = march_record(mesh, params, st0, mc, fcode, device, args.march, args.march_every)
+    if args.march is not None and rank == 0 and form in ("mk2", "mhd"):
+        line["march"] = march_record(mesh, params, st0, mc, fcode, device, args.march, args.march_every, form)
     if args.residual is not None and rank == 0:
         line["time_to_residual"] = time_to_residual(args.workload, mesh, params, st0, mc, form, fcode, device,
                                                     args.residual, counted)

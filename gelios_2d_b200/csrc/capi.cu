@@ -1682,9 +1682,14 @@ extern "C" int gelios_residual(gelios_ctx* ctx, int result_buf, double* residual
     return GELIOS_OK;
 }
 
-extern "C" int gelios_operator_residual(gelios_ctx* ctx, int buf, double* residual) {
+extern "C" int gelios_operator_residual(gelios_ctx* ctx, int form, int buf, double* residual) {
     if (!ctx || !residual || buf < 0 || buf > 1) return GELIOS_E_ARG;
+    if (form != GELIOS_FORM_MK2 && form != GELIOS_FORM_MHD_PUI) {
+        set_error("gelios_operator_residual: the moving-grid forms only (MK2, MHD + pickup)");
+        return GELIOS_E_ARG;
+    }
     if (!ctx->have_mesh) return GELIOS_E_STATE;
+    const bool mhd = form == GELIOS_FORM_MHD_PUI;
     const DevMesh& d = ctx->d;
     if (d.n_rail_a + d.n_rail_b + d.n_rail_c + d.n_rail_d == 0 || d.n_lc == 0) {
         set_error("gelios_operator_residual: the moving-grid form needs rails and tracked lines");
@@ -1694,6 +1699,13 @@ extern "C" int gelios_operator_residual(gelios_ctx* ctx, int buf, double* residu
     cudaStream_t s = ctx->stream;
     const size_t need = (kResidualScratch + 8) * sizeof(double);
     if (ctx->resid.bytes < need && ctx->resid.alloc(need)) return GELIOS_E_CUDA;
+    if (mhd) {
+        const size_t fb = static_cast<size_t>(kMhdFluxRows) * d.n_slots * sizeof(double);
+        if (ctx->flux_mhd.bytes != fb) {
+            ctx->drop_graphs();  // they hold the buffer about to be replaced
+            if (ctx->flux_mhd.alloc(fb)) return GELIOS_E_CUDA;
+        }
+    }
     const gelios_params& P = ctx->prm;
     const size_t nc = d.n_cells;
     double* cen0 = ctx->cen[0].as<double>();
@@ -1734,13 +1746,21 @@ extern "C" int gelios_operator_residual(gelios_ctx* ctx, int buf, double* residu
     b.rp = cen0 + 2 * nc;
     b.vs = cen0 + 3 * nc;
     b.vol = cen0 + 4 * nc;
-    const int v = (ctx->mk2_variant >= 4 && ctx->mk2_variant < 8) ? 0 : ctx->mk2_variant;
-    double* fl = ctx->flux.as<double>();
-    launch_mk2_recon(d, P, b, ctx->rec.as<double>(), s);
-    launch_mk2_tracked_solve(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(), s);
-    launch_mk2_flux_tracked(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(), fl, s);
-    GELIOS_CUDA_TRY(launch_mk2_cells(d, P, b, ctx->tiles, fl, ctx->aux.as<double>(), s, v, 1));
-    GELIOS_CUDA_TRY(launch_mk2_cells(d, P, b, ctx->tiles, fl, ctx->aux.as<double>(), s, v, 3));
+    double* fl;
+    if (mhd) {
+        // the MHD form's face units (ion HLLD, pickup HLLC) into its 13 flux
+        // rows; row 0 is the ion mass flux, state row 0 the ion density
+        fl = ctx->flux_mhd.as<double>();
+        launch_mhd_faces(d, P, ctx->mprm, b, ctx->hstate[buf].as<double>(), fl, s, ctx->mhd_face_variant);
+    } else {
+        const int v = (ctx->mk2_variant >= 4 && ctx->mk2_variant < 8) ? 0 : ctx->mk2_variant;
+        fl = ctx->flux.as<double>();
+        launch_mk2_recon(d, P, b, ctx->rec.as<double>(), s);
+        launch_mk2_tracked_solve(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(), s);
+        launch_mk2_flux_tracked(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(), fl, s);
+        GELIOS_CUDA_TRY(launch_mk2_cells(d, P, b, ctx->tiles, fl, ctx->aux.as<double>(), s, v, 1));
+        GELIOS_CUDA_TRY(launch_mk2_cells(d, P, b, ctx->tiles, fl, ctx->aux.as<double>(), s, v, 3));
+    }
     launch_op_residual(d, P, b, fl, sc, s);
     GELIOS_CUDA_TRY(cudaGetLastError());
     double r[2] = {0.0, 0.0};

@@ -191,12 +191,14 @@ class Setka:
         N.check(self._L.gelios_residual(self._h, int(result_buf), C.byref(r)), "gelios_residual")
         return float(r.value)
 
-    def operator_residual(self, buf: int = 0) -> float:
-        """Residual per unit time of the moving-grid operator at par[buf]
-        with the grid held still (face speeds 0): sum over updated cells of
-        |sum of the mass fluxes F.S| / volume over sum |ro|."""
+    def operator_residual(self, buf: int = 0, form: int = N.FORM_MK2) -> float:
+        """Residual per unit time of the moving-grid operator of `form` (MK2
+        or MHD + pickup) at par[buf] with the grid held still (face speeds
+        0): sum over updated cells of |sum of the mass fluxes F.S| / volume
+        over sum |ro|."""
         r = C.c_double()
-        N.check(self._L.gelios_operator_residual(self._h, int(buf), C.byref(r)), "gelios_operator_residual")
+        N.check(self._L.gelios_operator_residual(self._h, int(form), int(buf), C.byref(r)),
+                "gelios_operator_residual")
         return float(r.value)
 
     def run_to_residual(self, form: int, tol: float, max_steps: int, check_every: int = 20000):

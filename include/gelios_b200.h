@@ -257,16 +257,17 @@ int gelios_upload_sources(gelios_ctx *ctx, const double *q1, const double *q2, c
 int gelios_residual(gelios_ctx *ctx, int result_buf, double *residual);
 int gelios_run_to_residual(gelios_ctx *ctx, int form, double tol, int64_t max_steps, int32_t check_every,
                            int64_t *steps_done, double *residual_per_time, double *dt);
-/* gelios_operator_residual: the residual of the moving-grid operator
- * (GELIOS_FORM_MK2) at state par[buf] with the grid held still: every face
- * flux of the step (the same reconstructions, HLL and exact Godunov fluxes)
- * evaluated at face speed 0 on the current points, then
- * sum over updated cells of |sum of the cell's mass fluxes F.S| / volume,
- * divided by sum |ro|: the L1 density change per unit time of the flow
- * alone, without the volume change of moving cells that the step residual
- * above contains.  Writes only scratch (the moved-point buffer is set to
- * the current points); the state, the points and the dt words stay. */
-int gelios_operator_residual(gelios_ctx *ctx, int buf, double *residual);
+/* gelios_operator_residual: the residual of a moving-grid operator
+ * (form GELIOS_FORM_MK2 or GELIOS_FORM_MHD_PUI) at state par[buf] (and the
+ * MHD form's extra rows of buffer buf) with the grid held still: every face
+ * flux of the step (the same reconstructions and Riemann solvers) evaluated
+ * at face speed 0 on the current points, then sum over updated cells of
+ * |sum of the cell's (ion) mass fluxes F.S| / volume, divided by sum |ro|:
+ * the L1 density change per unit time of the flow alone, without the volume
+ * change of moving cells that the step residual above contains.  Writes
+ * only scratch (the moved-point buffer is set to the current points); the
+ * state, the points and the dt words stay. */
+int gelios_operator_residual(gelios_ctx *ctx, int form, int buf, double *residual);
 
 /* ---- streamed host I/O (no counterpart in the reference) --------------------
  * For callers that feed a fresh state from host memory every step and read

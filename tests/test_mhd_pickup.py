@@ -294,3 +294,38 @@ def test_mk2_launch_shapes_give_same_bits_and_autotune_keeps_state():
     assert 0 <= v < n and ms > 0.0
     d.Go_5_komponent__MK2(3)
     assert np.array_equal(d.par(1), ref.par(1)) and np.array_equal(d.par(0), ref.par(0))
+
+
+@pytest.mark.gpu
+def test_mhd_operator_residual_is_the_ion_flux_balance_of_a_still_grid():
+    """gelios_operator_residual of the MHD + pickup form is the ion density
+    change per unit time of a step on a grid that does not move (koef = 0:
+    the first step snaps the points onto the rail formulas, the next leaves
+    them in place bit for bit; the ion mass update has no source term, so
+    |ro' - ro| = dt |sum F.S| / V in each updated cell; relative 1e-6).  The
+    call changes no state, point or dt word."""
+    mesh, P, mp, st0, x0, src = setup(MEDIUM)
+    P = P.copy(koef=0.0)
+
+    def run(with_residual):
+        dev, _ = device_run(mesh, P, mp, st0, x0, src, 1)
+        s1, h1 = dev.par(1), dev.mhd(1)
+        pts1 = dev.points()
+        dev.set_par(0, s1)
+        dev.set_mhd(0, h1)
+        r = None
+        if with_residual:
+            r = [dev.operator_residual(0, N.FORM_MHD_PUI), dev.operator_residual(0, N.FORM_MHD_PUI)]
+        st = dev.Go_MHD_pickup(1)
+        return dev, s1, pts1, st, r
+
+    dev, s1, pts1, st, r = run(True)
+    assert r[0] == r[1] and np.isfinite(r[0]) and r[0] > 0.0
+    pts2 = dev.points()
+    assert np.array_equal(pts1[0], pts2[0]) and np.array_equal(pts1[1], pts2[1])
+    s2 = dev.par(1)
+    ref = float(np.abs(s2[0] - s1[0]).sum() / (P.dt0 * np.abs(s1[0]).sum()))
+    assert abs(r[0] - ref) <= 1e-6 * ref, (r[0], ref)
+    dev2, _, _, st_b, _ = run(False)
+    assert np.array_equal(dev2.par(1), s2) and np.array_equal(dev2.mhd(1), dev.mhd(1)) and st_b.dt == st.dt
+    assert np.array_equal(dev2.points()[0], pts2[0])
