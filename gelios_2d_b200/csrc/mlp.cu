@@ -14,8 +14,10 @@
 //                         cp.async.bulk.tensor per tile; no cluster
 //                         multicast) and, for the forward layers, bias +
 //                         GELU applied to the accumulator as it leaves
-//                         tensor memory; used whenever both operands' rows
-//                         are 16-byte aligned
+//                         tensor memory, the hidden layers' Z and H tiles
+//                         staged in shared memory and stored by the TMA;
+//                         used whenever both operands' rows are 16-byte
+//                         aligned
 //   transpose_bf16_kernel the transposed operands of the backward GEMMs
 //   features_kernel       network inputs: the raw inputs, then sin / cos of
 //                         2^f pi s of the last two (the cell position), bf16
@@ -331,6 +333,15 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
         : "memory");
 }
 
+// the tile in shared memory -> global memory through the tensor map (rows
+// and columns outside the tensor are not written); one bulk group per CTA
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, uint32_t src, int x, int y) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];\n" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(src), "r"(x), "r"(y)
+                 : "memory");
+}
+
 struct GemmEpilogue {
     const float* bias = nullptr;
     float* Z = nullptr;
@@ -346,7 +357,9 @@ template <int EPI>
 __global__ void __launch_bounds__(TM_THREADS, 2) gemm_tma_kernel(const __grid_constant__ CUtensorMap tmA,
                                                             const __grid_constant__ CUtensorMap tmB, int M, int N,
                                                             int K, int kc, float* __restrict__ C, int64_t ldc,
-                                                            int64_t c_split, GemmEpilogue ep, int* __restrict__ status) {
+                                                            int64_t c_split, GemmEpilogue ep, int* __restrict__ status,
+                                                            const __grid_constant__ CUtensorMap tmZ,
+                                                            const __grid_constant__ CUtensorMap tmH, int tstore) {
     extern __shared__ __align__(1024) uint8_t tc_smem[];
     __shared__ uint64_t full[TC_STAGES], empty[TC_STAGES];
     __shared__ uint32_t tmem_slot;
@@ -437,7 +450,56 @@ __global__ void __launch_bounds__(TM_THREADS, 2) gemm_tma_kernel(const __grid_co
             for (int j = 0; j < 16; j++) v[j] = 0u;
         }
         const int col0 = n0 + c0;
-        if (row >= M) {
+        if (EPI == 1 && tstore) {
+            // Z and H of the tile into shared memory in the 128-byte-swizzled
+            // layout of the output tensor maps (16-byte chunk c of tile row r
+            // at r * 128 + ((c ^ (r & 7)) << 4), so the 8 rows of one store
+            // phase fall on 8 different bank groups): Z as two boxes of 32
+            // columns, H as one of 64; thread 0 stores them with the TMA
+            // below.  The stage buffers are free: the last commit covered
+            // every MMA, and every load had landed before its MMA.
+            float bv[16];
+            const float* bp = ep.bias + col0;
+            if (col0 + 16 <= N && (reinterpret_cast<uintptr_t>(bp) & 15) == 0) {
+#pragma unroll
+                for (int j = 0; j < 16; j += 4) {
+                    const float4 q = __ldg(reinterpret_cast<const float4*>(bp + j));
+                    bv[j] = q.x;
+                    bv[j + 1] = q.y;
+                    bv[j + 2] = q.z;
+                    bv[j + 3] = q.w;
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 16; j++) bv[j] = col0 + j < N ? bp[j] : 0.f;
+            }
+            float z[16], h[16];
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+                z[j] = __uint_as_float(v[j]) + bv[j];
+                h[j] = ep.act ? gelu(z[j]) : z[j];
+            }
+            const int r = wl * 32 + lane;
+            const uint32_t sw = static_cast<uint32_t>(r & 7);
+            uint8_t* zrow = base + (wc >> 1) * (TC_BM * 128) + r * 128;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const uint32_t ch = static_cast<uint32_t>(4 * (wc & 1) + q);
+                *reinterpret_cast<float4*>(zrow + ((ch ^ sw) << 4)) =
+                    make_float4(z[4 * q], z[4 * q + 1], z[4 * q + 2], z[4 * q + 3]);
+            }
+            uint8_t* hrow = base + 2 * (TC_BM * 128) + r * 128;
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                __align__(16) __nv_bfloat16 hb[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++) hb[j] = __float2bfloat16(h[8 * q + j]);
+                const uint32_t ch = static_cast<uint32_t>(2 * wc + q);
+                *reinterpret_cast<uint4*>(hrow + ((ch ^ sw) << 4)) = *reinterpret_cast<const uint4*>(hb);
+            }
+            // the generic-proxy writes, visible to the bulk copies
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        } else if (row >= M) {
         } else if (EPI == 0) {
             float* dst = C + blockIdx.z * c_split + row * ldc + col0;
             if (col0 + 16 <= N && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
@@ -492,6 +554,15 @@ __global__ void __launch_bounds__(TM_THREADS, 2) gemm_tma_kernel(const __grid_co
     if (warp == 0) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TM_BN) : "memory");
+    }
+    if (EPI == 1 && tstore && threadIdx.x == 0) {
+        // x = n0 and n0 + 32: multiples of 32 columns, 128-byte aligned
+        tma_store_2d(&tmZ, smem_u32(base), n0, m0);
+        if (n0 + 32 < N) tma_store_2d(&tmZ, smem_u32(base + TC_BM * 128), n0 + 32, m0);
+        tma_store_2d(&tmH, smem_u32(base + 2 * TC_BM * 128), n0, m0);
+        asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+        // the shared memory stays allocated until the copies are complete
+        asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
     }
     if (!ok) atomicOr(status, 1);
 }
@@ -711,6 +782,32 @@ bool operand_map(CUtensorMap* map, const __nv_bfloat16* X, int64_t ld, int rows,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// The tensor map of a row-major output [rows][N] (fp32 or bf16) for the
+// TMA stores of the fused epilogue: boxes of 128 bytes of a row (32 fp32 or
+// 64 bf16) x 128 rows, 128-byte swizzle.
+bool output_map(CUtensorMap* map, void* X, bool f32, int rows, int N) {
+    const TensorMapEncode enc = tensor_map_encoder();
+    if (!enc || rows <= 0 || N <= 0) return false;
+    const int es = f32 ? 4 : 2;
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(N), static_cast<cuuint64_t>(rows)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(N) * es};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(128 / es), static_cast<cuuint32_t>(TC_BM)};
+    const cuuint32_t estr[2] = {1, 1};
+    return enc(map, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, X, dims, strides, box,
+               estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// address of the GEMM status word on the current device (looked up once)
+int* gemm_status_ptr() {
+    static int* addr[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!addr[dev]) cudaGetSymbolAddress(reinterpret_cast<void**>(&addr[dev]), g_gemm_status);
+    return addr[dev];
+}
+
 // The TMA GEMM; false (nothing launched) where an operand cannot be
 // described by a tensor map (rows not 16-byte aligned) or the driver offers
 // no encoder: the caller then uses gemm_tc_kernel.
@@ -728,9 +825,15 @@ bool launch_tma(dim3 grid, int M, int N, int K, int kc, const __nv_bfloat16* A, 
         cudaFuncSetAttribute(gemm_tma_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, TM_SMEM);
         if (dev >= 0 && dev < 64) attr[dev] = true;
     }
-    int* st = nullptr;
-    cudaGetSymbolAddress(reinterpret_cast<void**>(&st), g_gemm_status);
-    gemm_tma_kernel<EPI><<<grid, TM_THREADS, TM_SMEM, s>>>(ma, mb, M, N, K, kc, C, ldc, c_split, ep, st);
+    // the fused epilogue of a hidden layer (Z and H, no fp32 activation)
+    // leaves the tile through shared memory and the TMA where both outputs
+    // can be described by tensor maps (16-byte aligned rows)
+    CUtensorMap mz{}, mh{};
+    const bool tstore = EPI == 1 && ep.Z && ep.H && !ep.Hf && N % 8 == 0 &&
+                        (reinterpret_cast<uintptr_t>(ep.Z) & 15) == 0 && (reinterpret_cast<uintptr_t>(ep.H) & 15) == 0 &&
+                        output_map(&mz, ep.Z, true, M, N) && output_map(&mh, ep.H, false, M, N);
+    gemm_tma_kernel<EPI><<<grid, TM_THREADS, TM_SMEM, s>>>(ma, mb, M, N, K, kc, C, ldc, c_split, ep,
+                                                           gemm_status_ptr(), mz, mh, tstore ? 1 : 0);
     return true;
 }
 
@@ -1130,11 +1233,23 @@ extern "C" int gelios_mlp_time_layer(int M, int N, int K, int reps, int tma, dou
         return true;
     };
     if (!layer()) return fail("gelios_mlp_time_layer: no tensor-map encoder in this driver");
+    // the reps launches captured in one CUDA graph, so that the device time
+    // per layer is not the host's launch rate
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    MLP_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+    for (int r = 0; r < reps; r++) layer();
+    MLP_TRY(cudaStreamEndCapture(s, &graph));
+    std::unique_ptr<CUgraph_st, void (*)(cudaGraph_t)> gguard(graph, [](cudaGraph_t g) { cudaGraphDestroy(g); });
+    MLP_TRY(cudaGraphInstantiate(&exec, graph, 0));
+    std::unique_ptr<CUgraphExec_st, void (*)(cudaGraphExec_t)> xguard(exec,
+                                                                      [](cudaGraphExec_t x) { cudaGraphExecDestroy(x); });
+    MLP_TRY(cudaGraphLaunch(exec, s));
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     MLP_TRY(cudaEventCreate(&e0));
     MLP_TRY(cudaEventCreate(&e1));
     MLP_TRY(cudaEventRecord(e0, s));
-    for (int r = 0; r < reps; r++) layer();
+    MLP_TRY(cudaGraphLaunch(exec, s));
     MLP_TRY(cudaEventRecord(e1, s));
     MLP_TRY(cudaEventSynchronize(e1));
     float t = 0.f;

@@ -363,11 +363,12 @@ int gelios_mlp_gemm_bf16(int M, int N, int K, const void *A, int64_t lda, const 
 /* gelios_mlp_time_layer: device time of one hidden layer of the network's
  * forward pass, an M x N x K bf16 GEMM with bias + GELU (seeded operands
  * allocated for the call): tma != 0 the TMA-staged GEMM applying bias + GELU
- * as the accumulator leaves tensor memory (what the forward pass uses),
- * tma == 0 the cp.async-staged GEMM followed by a separate bias + GELU
- * kernel.  `reps` layers back to back after one untimed one, CUDA events on
- * a private stream; mean ms per layer.  For measurements; no counterpart in
- * the reference. */
+ * as the accumulator leaves tensor memory and storing the Z / H tiles
+ * through shared memory with the TMA (what the forward pass uses), tma == 0
+ * the cp.async-staged GEMM followed by a separate bias + GELU kernel.
+ * `reps` layers back to back, captured in one CUDA graph and replayed once
+ * untimed, then timed with CUDA events on a private stream; mean ms per
+ * layer.  For measurements; no counterpart in the reference. */
 int gelios_mlp_time_layer(int M, int N, int K, int reps, int tma, double *ms);
 
 /* ---- autotuning of launch shapes (no counterpart in the reference) ---------
