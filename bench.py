@@ -357,6 +357,17 @@ def fp32_flux_errors(mesh, params32, st0, mc, fcode, device, counts=(1, 100, 200
             d = np.abs(a[k] - b[k])
             errs[name] = {"L1": float(d.sum() / max(np.abs(b[k]).sum(), 1e-300)),
                           "Linf": float(d.max() / max(np.abs(b[k]).max(), 1e-300))}
+        if form == "mhd":
+            # vector scales: w (zero at the start) against the ion speed, each
+            # field component against |B|
+            spd = np.sqrt(b[2] ** 2 + b[3] ** 2 + b[5] ** 2)
+            bm = np.sqrt(b[6] ** 2 + b[7] ** 2 + b[8] ** 2)
+            dw = np.abs(a[5] - b[5])
+            errs["w/|u|"] = {"L1": float(dw.sum() / max(spd.sum(), 1e-300)),
+                             "Linf": float(dw.max() / max(spd.max(), 1e-300))}
+            db = np.sqrt((a[6] - b[6]) ** 2 + (a[7] - b[7]) ** 2 + (a[8] - b[8]) ** 2)
+            errs["B/|B|"] = {"L1": float(db.sum() / max(bm.sum(), 1e-300)),
+                             "Linf": float(db.max() / max(bm.max(), 1e-300))}
         out[str(n)] = errs
     return out
 
@@ -463,7 +474,8 @@ def run_sweep(args, rank: int, world: int, local: int) -> None:
         inst = sw.instance_set(n_inst, seed=seed, scale=(0.5, 1.4), only=mine)
     counted = sum(W.counted_cells_mk2(m, p) for m, p, _, _ in inst)
     cells = sum(m.n_cells for m, _, _, _ in inst)
-    batched = mhd and args.sweep_mode == "batched"
+    batched = mhd and args.sweep_mode in ("batched", "persistent")
+    call_steps = max(1, int(args.sweep_call_steps))
     B = sw.Sweep(inst, device=local, form=N.FORM_MHD_PUI if mhd else N.FORM_MK2)
     tuned = None
     if mhd and not batched:  # per-instance launch shape and enqueue order (the sweep's autotuner)
@@ -471,8 +483,13 @@ def run_sweep(args, rank: int, world: int, local: int) -> None:
         tuned = {}
         for v, _ in res:
             tuned[str(v)] = tuned.get(str(v), 0) + 1
+    schedule = None
     if batched:  # one launch per phase over the instances of a group (gelios_batch)
         B.enable_batch(args.sweep_groups)
+        if args.sweep_mode == "persistent":
+            # the batch's autotuner: per-phase graph or one persistent kernel at
+            # each co-resident block count (its trial steps advance the instances)
+            schedule = B.autotune_batch(2)
     streams = [torch.cuda.ExternalStream(S.stream_handle(), device=local) for S in B.items]
     s0 = torch.cuda.current_stream(local)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
@@ -483,7 +500,7 @@ def run_sweep(args, rank: int, world: int, local: int) -> None:
         start.record(s0)
         for st in streams:
             st.wait_event(start)
-        B.step_async(1)
+        B.step_async(call_steps)
         for st in streams:
             e = torch.cuda.Event()
             e.record(st)
@@ -492,6 +509,8 @@ def run_sweep(args, rank: int, world: int, local: int) -> None:
         end.record(s0)
         if ev is not None:
             ev.append((start, end))
+        if batched:  # every context of a group reports the group's launches
+            return sum(B.items[p[0]].launches() for p in B._groups)
         return sum(S.launches() for S in B.items)
 
     for _ in range(args.warmup):
@@ -514,13 +533,13 @@ def run_sweep(args, rank: int, world: int, local: int) -> None:
         t = torch.tensor([float(counted)], device=f"cuda:{local}", dtype=torch.float64)
         dist.all_reduce(t)
         counted_all = float(t.item())
-    value = counted_all * args.steps / (total_ms / 1000.0)
+    value = counted_all * args.steps * call_steps / (total_ms / 1000.0)
     peak, peak_kind = measured_peaks()
     bpc = BYTES_PER_CELL["mhd" if mhd else "mk2"]
-    achieved = bpc * counted_all / world / (total_ms / args.steps / 1000.0) / 1e9
+    achieved = bpc * counted_all / world / (total_ms / args.steps / call_steps / 1000.0) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps / call_steps, "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "f64 (fp32 flux)" if mhd else "f64",
         "data": "synthetic (seeded instances: grid scale, inflow, initial field, " +
                 ("LISM field, charge-exchange sources)" if mhd else "Monte-Carlo moments)"),
@@ -528,17 +547,40 @@ def run_sweep(args, rank: int, world: int, local: int) -> None:
                    "cells_rank0": int(cells), "cells_updated_per_step": int(counted_all),
                    "l2": "flushed between timed steps (256 MiB write)",
                    "parallelism": f"instances partitioned over {world} GPU(s)",
-                   "autotune_variants_rank0": tuned,
-                   "mode": "batched: one launch per phase over all instances, one CUDA graph per step" if batched
+                   "autotune_variants_rank0": tuned, "steps_per_call": call_steps,
+                   "batch_schedule_rank0": schedule,
+                   "mode": ("persistent: autotuned per group between one launch per phase (schedule 0) and one "
+                            "cooperative kernel over all steps of a call (schedule k: k blocks per SM)")
+                           if args.sweep_mode == "persistent" and mhd else
+                           "batched: one launch per phase over all instances, one CUDA graph per step" if batched
                            else "one context and captured step graph per instance, enqueued together"},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "kernel": "batched moving-grid steps of all instances on a GPU",
-                     "bytes_per_cell": bpc, "avg_launch_us": total_ms / args.steps * 1000.0,
+                     "bytes_per_cell": bpc, "avg_launch_us": total_ms / args.steps / call_steps * 1000.0,
                      "peak_kind": f"{peak_kind} hbm_gbs (burst copy)"},
         "clocks": clocks,
     }
     B.close()
+    if mhd and rank == 0 and args.sweep_errors > 0:
+        # FP32-flux errors of the sweep's own instances against their FP64 steps
+        per = []
+        for mesh, p32, st0, extra in inst[: args.sweep_errors]:
+            e = fp32_flux_errors(mesh, p32, st0, extra, N.FORM_MHD_PUI, local, form="mhd")
+            e["cells"] = int(mesh.n_cells)
+            per.append(e)
+        worst = {}
+        for e in per:
+            for n, errs in e.items():
+                if not isinstance(errs, dict):
+                    continue
+                w = worst.setdefault(n, {})
+                for name, v in errs.items():
+                    o = w.setdefault(name, {"L1": 0.0, "Linf": 0.0})
+                    o["L1"] = max(o["L1"], v["L1"])
+                    o["Linf"] = max(o["Linf"], v["Linf"])
+        line["fp32_flux_errors"] = {"against": "FP64 device path, same instance and initial state",
+                                    "instances": len(per), "worst_over_instances": worst, "per_instance": per}
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -609,8 +651,11 @@ def main():
     ap.add_argument("--variant", type=int, default=None)
     # sweep64 only: one context and captured step graph per instance, autotuned and enqueued together
     # (default), or gelios_batch: one launch per phase over the instances of each of --sweep-groups groups
-    ap.add_argument("--sweep-mode", default="contexts", choices=["contexts", "batched"])
+    ap.add_argument("--sweep-mode", default="contexts", choices=["contexts", "batched", "persistent"])
     ap.add_argument("--sweep-groups", type=int, default=1)
+    ap.add_argument("--sweep-call-steps", type=int, default=1, help="steps per timed call of the sweep")
+    ap.add_argument("--sweep-errors", type=int, default=0,
+                    help="sweep64: FP32-flux L1/Linf errors of this many instances after 1, 100, 2000 steps")
     # wall time to an L1 residual per unit time (cold start), reported beside the rate
     ap.add_argument("--residual", type=float, default=None)
     # moving-grid workloads: march this many steps from the initial field, recording the step residual, the

@@ -161,6 +161,9 @@ def lib() -> C.CDLL:
     L.gelios_batch_create.argtypes = [C.POINTER(vp), C.POINTER(vp), C.c_int]
     L.gelios_batch_step.argtypes = [vp, C.c_int, C.c_int, C.POINTER(GeliosStatus)]
     L.gelios_batch_destroy.argtypes = [vp]
+    L.gelios_batch_set_schedule.argtypes = [vp, C.c_int32]
+    L.gelios_batch_get_schedule.argtypes = [vp, C.POINTER(C.c_int32)]
+    L.gelios_batch_autotune.argtypes = [vp, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_double), C.c_void_p, C.c_int]
     L.gelios_plain_batch_create.argtypes = [C.POINTER(vp), C.POINTER(vp), C.c_int]
     L.gelios_plain_batch_step.argtypes = [vp, C.c_int, C.POINTER(GeliosStatus)]
     L.gelios_plain_batch_run_to_residual.argtypes = [vp, C.c_double, C.c_int64, C.c_int32, C.c_void_p, C.c_void_p,

@@ -2029,6 +2029,9 @@ struct gelios_batch {
     bool table_pending = false;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool graphs_off = false;
+    // 0: one launch per phase, a captured graph per step; k > 0: all steps
+    // of a call in one cooperative launch of k blocks per SM
+    int schedule = 0;
     ~gelios_batch() {
         for (auto& g : graph)
             if (g) cudaGraphExecDestroy(g);
@@ -2198,7 +2201,11 @@ extern "C" int gelios_batch_step(gelios_batch* B, int form, int nsteps, gelios_s
     int64_t launches = 1;
     const int per_step = (B->tab.n_surf > 0) + (B->tab.n_rails > 0) + (B->tab.n_units > 0) + (B->tab.n_cells > 0) +
                          (B->tab.n_points > 0);
-    for (int st = 0; st < nsteps; st++) {
+    if (B->schedule > 0 && nsteps > 0) {
+        GELIOS_CUDA_TRY(launch_batch_mhd_persistent(B->tab, nsteps, B->schedule, s));
+        launches += 1;
+    }
+    for (int st = 0; st < (B->schedule > 0 ? 0 : nsteps); st++) {
         const int par = st & 1;
         if (!B->graphs_off && !B->graph[par]) {
             cudaGraph_t g = nullptr;
@@ -2253,6 +2260,73 @@ extern "C" int gelios_batch_step(gelios_batch* B, int form, int nsteps, gelios_s
             if (!(o.dt == o.dt)) o.flags |= ST_DT_BAD;
         }
     }
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_batch_set_schedule(gelios_batch* B, int32_t schedule) {
+    if (!B || schedule < 0) return GELIOS_E_ARG;
+    GELIOS_CUDA_TRY(cudaSetDevice(B->device));
+    if (schedule > 0) {
+        int max_per_sm = 0;
+        const cudaError_t e = launch_batch_mhd_persistent(B->tab, 0, schedule, B->ctxs[0]->stream, &max_per_sm);
+        if (e == cudaErrorCooperativeLaunchTooLarge) {
+            set_error("gelios_batch_set_schedule: " + std::to_string(schedule) + " blocks per SM do not fit (at most " +
+                      std::to_string(max_per_sm) + ")");
+            return GELIOS_E_ARG;
+        }
+        GELIOS_CUDA_TRY(e);
+    }
+    B->schedule = schedule;
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_batch_get_schedule(gelios_batch* B, int32_t* schedule) {
+    if (!B || !schedule) return GELIOS_E_ARG;
+    *schedule = B->schedule;
+    return GELIOS_OK;
+}
+
+extern "C" int gelios_batch_autotune(gelios_batch* B, int steps, int32_t* schedule, double* ms, double* each_ms,
+                                     int n_each) {
+    if (!B || steps < 1 || n_each < 0 || (n_each > 0 && !each_ms)) return GELIOS_E_ARG;
+    for (int k = 0; k < n_each; k++) each_ms[k] = -1.0;
+    GELIOS_CUDA_TRY(cudaSetDevice(B->device));
+    cudaStream_t s = B->ctxs[0]->stream;
+    int max_per_sm = 0;
+    GELIOS_CUDA_TRY(launch_batch_mhd_persistent(B->tab, 0, 0, s, &max_per_sm));
+    cudaEvent_t e0, e1;
+    GELIOS_CUDA_TRY(cudaEventCreate(&e0));
+    GELIOS_CUDA_TRY(cudaEventCreate(&e1));
+    int best = 0;
+    double best_ms = -1.0;
+    int rc = GELIOS_OK;
+    // every candidate once untimed (graph capture, first touch), then timed
+    for (int cand = 0; cand <= max_per_sm && rc == GELIOS_OK; cand++) {
+        B->schedule = cand;
+        for (int rep = 0; rep < 2 && rc == GELIOS_OK; rep++) {
+            if (rep == 1 && cudaEventRecord(e0, s) != cudaSuccess) rc = GELIOS_E_CUDA;
+            if (rc == GELIOS_OK) rc = gelios_batch_step(B, GELIOS_FORM_MHD_PUI, steps, nullptr);
+            if (rc == GELIOS_OK && rep == 1) {
+                float t = 0.f;
+                if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                    cudaEventElapsedTime(&t, e0, e1) != cudaSuccess) {
+                    rc = GELIOS_E_CUDA;
+                } else {
+                    if (cand < n_each) each_ms[cand] = t / steps;
+                    if (best_ms < 0.0 || t < best_ms) {
+                        best_ms = t;
+                        best = cand;
+                    }
+                }
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    B->schedule = best;
+    if (rc != GELIOS_OK) return rc;
+    if (schedule) *schedule = best;
+    if (ms) *ms = best_ms / steps;
     return GELIOS_OK;
 }
 

@@ -3416,6 +3416,85 @@ __global__ void __launch_bounds__(256) batch_commit_kernel(BatchTables t, int pa
     }
 }
 
+// `nsteps` batched MHD + pickup steps of every instance in ONE cooperative
+// launch: the five phases of launch_batch_mhd_step (tracked-face speeds,
+// rails, face units, cell update, commit) with a grid barrier where a kernel
+// boundary was.  The blocks deal each phase's table by grid stride (table
+// entries are equal-sized tiles of one instance each, so every CFL block
+// minimum still goes to one instance's dt word); the per-item work is the
+// bodies of the per-phase kernels, so a call leaves the same state as the
+// same number of per-phase steps.  The grid must be co-resident (launched
+// by cudaLaunchCooperativeKernel, which refuses a grid that is not).
+template <typename TF>
+__global__ void __launch_bounds__(128, GELIOS_BATCH_FACE_MINB) batch_mhd_persistent_kernel(BatchTables t, int nsteps) {
+    cg::grid_group grid = cg::this_grid();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int st = 0; st < nsteps; st++) {
+        const int parity = st & 1;
+        // tracked faces: a surf entry holds two faces (one warp each), so a
+        // 128-thread block takes two entries per round
+        for (int i = 2 * blockIdx.x + (warp >> 1); i < t.n_surf; i += 2 * gridDim.x) {
+            const int2 e = t.surf[i];
+            const BatchInstance& I = t.inst[e.x];
+            const int j = e.y + (warp & 1);
+            if (j < I.d.n_lc + I.d.n_li + I.d.n_lo) surface_face_body(I.d, I.P, I.b[parity], I.surface, j, lane);
+        }
+        grid.sync();
+        for (int i = blockIdx.x; i < t.n_rails; i += gridDim.x) {
+            const int2 e = t.rails[i];
+            const BatchInstance& I = t.inst[e.x];
+            rails_body(I.d, I.P, I.b[parity].dt_cur, I.surface, true, e.y);
+            __syncthreads();  // the next rail reuses the block's shared words
+        }
+        grid.sync();
+        for (int i = blockIdx.x; i < t.n_units; i += gridDim.x) {
+            const int2 e = t.units[i];
+            const BatchInstance& I = t.inst[e.x];
+            const int u = e.y + threadIdx.x;
+            const StepBuffers& b = I.b[parity];
+            double tmin = __longlong_as_double(0x7ff0000000000000LL);
+            int status = 0;
+            if (u < I.d.n_units) tmin = mhd_face_body<TF>(I.d, I.P, I.M, b, I.hs[parity], I.fl, u, status);
+            block_reduce_commit(tmin, 0, 0, status, b.dt_acc, b.counters, b.status);
+            __syncthreads();  // the next tile reuses the reduction's shared words
+        }
+        grid.sync();
+        for (int i = blockIdx.x; i < t.n_cells; i += gridDim.x) {
+            const int2 e = t.cells[i];
+            const BatchInstance& I = t.inst[e.x];
+            const int c = e.y + threadIdx.x;
+            const StepBuffers& b = I.b[parity];
+            double tmark = __longlong_as_double(0x7ff0000000000000LL);
+            int nro = 0, npc = 0;
+            if (c < I.d.n_cells)
+                mhd_update_body(I.d, I.P, b, I.fl, I.src, I.hs[parity], I.hn[parity], c, tmark, nro, npc);
+            block_reduce_commit(tmark, nro, npc, 0, b.dt_acc, b.counters, b.status);
+            __syncthreads();
+        }
+        grid.sync();
+        // commit: a points entry covers 256 points (two per thread here)
+        for (int i = blockIdx.x; i < t.n_points; i += gridDim.x) {
+            const int2 e = t.points[i];
+            const BatchInstance& I = t.inst[e.x];
+            const StepBuffers& b = I.b[parity];
+            if (e.y == 0 && threadIdx.x == 0) {
+                const unsigned long long a = *b.dt_acc;
+                *b.dt_next =
+                    (a == 0x7ff0000000000000ULL) ? 100000000.0 : __longlong_as_double(static_cast<long long>(a));
+                *b.dt_acc = 0x7ff0000000000000ULL;
+            }
+            for (int k = threadIdx.x; k < 256; k += blockDim.x) {
+                const int p = e.y + k;
+                if (p < I.d.n_points) {
+                    I.d.X[p] = I.d.X2[p];
+                    I.d.Y[p] = I.d.Y2[p];
+                }
+            }
+        }
+        grid.sync();
+    }
+}
+
 // The dt / status words a call starts from: T[0] = T[1] = dt0, an empty CFL
 // accumulator, zero clamp counters and status (layout: T[2], acc,
 // counters[2], status).  A kernel rather than a copy from host memory: a
@@ -3878,6 +3957,24 @@ void launch_batch_mhd_step(const BatchTables& t, int parity, cudaStream_t s) {
     }
     if (t.n_cells > 0) batch_mhd_update_kernel<<<t.n_cells, 128, 0, s>>>(t, parity);
     if (t.n_points > 0) batch_commit_kernel<<<t.n_points, 256, 0, s>>>(t, parity);
+}
+cudaError_t launch_batch_mhd_persistent(const BatchTables& t, int nsteps, int blocks_per_sm, cudaStream_t s,
+                                        int* max_per_sm) {
+    const void* fn = t.fp32 ? reinterpret_cast<const void*>(&batch_mhd_persistent_kernel<float>)
+                            : reinterpret_cast<const void*>(&batch_mhd_persistent_kernel<double>);
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 128, 0);
+    if (e != cudaSuccess) return e;
+    if (max_per_sm) *max_per_sm = per_sm;
+    if (per_sm < 1 || blocks_per_sm > per_sm) return cudaErrorCooperativeLaunchTooLarge;
+    if (nsteps <= 0) return cudaSuccess;
+    const int k = blocks_per_sm > 0 ? blocks_per_sm : per_sm;
+    BatchTables tt = t;
+    int n = nsteps;
+    void* args[] = {&tt, &n};
+    return cudaLaunchCooperativeKernel(fn, dim3(k * sms), dim3(128), args, 0, s);
 }
 void launch_mhd_update(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* fl,
                        const double* src, const double* hcur, double* hnxt, cudaStream_t s) {

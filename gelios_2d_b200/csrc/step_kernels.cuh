@@ -275,6 +275,12 @@ void launch_words_init(void* words, double dt0, cudaStream_t s);
 void launch_batch_words_init(const BatchTables& t, int n, cudaStream_t s);
 // The five launches of one batched MHD step (parity: even / odd step of the call).
 void launch_batch_mhd_step(const BatchTables& t, int parity, cudaStream_t s);
+// All phases of `nsteps` batched MHD steps in one cooperative launch of
+// blocks_per_sm 128-thread blocks per SM (0: as many as fit); *max_per_sm
+// (optional) receives how many fit.  Errors: cudaErrorCooperativeLaunchTooLarge
+// when blocks_per_sm exceeds what fits.
+cudaError_t launch_batch_mhd_persistent(const BatchTables& t, int nsteps, int blocks_per_sm, cudaStream_t s,
+                                        int* max_per_sm = nullptr);
 
 void launch_hllc_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s);
 void launch_hlldq_batch(const gelios_params& P, int n, const double* in, double* out, cudaStream_t s);

@@ -80,6 +80,44 @@ class Sweep:
             N.check(L.gelios_batch_create(C.byref(h), arr, len(p)), "gelios_batch_create")
             self._batch.append(h)
 
+    def set_batch_schedule(self, schedule: int):
+        """0: one launch per phase (a captured graph per step); k > 0: every
+        step of a call in one persistent cooperative kernel of k blocks per
+        SM (gelios_batch_set_schedule)."""
+        import ctypes as C
+
+        L = N.lib()
+        for h in self._batch:
+            N.check(L.gelios_batch_set_schedule(h, C.c_int32(int(schedule))), "gelios_batch_set_schedule")
+
+    def batch_schedules(self) -> list[int]:
+        import ctypes as C
+
+        L = N.lib()
+        out = []
+        for h in self._batch:
+            v = C.c_int32()
+            N.check(L.gelios_batch_get_schedule(h, C.byref(v)), "gelios_batch_get_schedule")
+            out.append(v.value)
+        return out
+
+    def autotune_batch(self, steps: int = 2) -> list[tuple[int, float, list[float]]]:
+        """Per batch: time the per-phase schedule and the persistent kernel
+        at every co-resident block count on `steps` real steps each (they
+        advance the instances) and keep the fastest.  Returns (schedule,
+        ms per step, ms per step of every schedule 0..15 that ran) per batch."""
+        import ctypes as C
+
+        L = N.lib()
+        res = []
+        for h in self._batch:
+            v, ms = C.c_int32(), C.c_double()
+            each = (C.c_double * 16)()
+            N.check(L.gelios_batch_autotune(h, int(steps), C.byref(v), C.byref(ms), C.cast(each, C.c_void_p), 16),
+                    "gelios_batch_autotune")
+            res.append((v.value, ms.value, [round(x, 4) for x in each if x >= 0.0]))
+        return res
+
     def batch_step(self, n: int = 1, statuses: bool = False):
         """n batched steps; with statuses=True waits and returns the
         instances' statuses (in instance order)."""

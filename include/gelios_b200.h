@@ -299,6 +299,21 @@ typedef struct gelios_batch gelios_batch;
 int gelios_batch_create(gelios_batch **out, gelios_ctx *const *ctxs, int n);
 int gelios_batch_step(gelios_batch *batch, int form, int nsteps, gelios_status *statuses);
 void gelios_batch_destroy(gelios_batch *batch);
+/* How a batch runs its steps.  schedule 0: one launch per phase, each step
+ * a captured CUDA graph (the default).  schedule k > 0: every step of a
+ * call in ONE persistent cooperative kernel of k 128-thread blocks per SM,
+ * the phases separated by grid barriers, the tiles of all instances dealt
+ * to the blocks by grid stride; both schedules compute the same per-face
+ * and per-cell bodies.  GELIOS_E_ARG if k blocks per SM cannot be
+ * co-resident.  gelios_batch_autotune runs `steps` real steps of the sweep
+ * for each schedule (0 and every k that fits; each advances every
+ * instance, once untimed and once timed), keeps the fastest and returns it
+ * with its time per step in ms (either pointer may be NULL); each_ms[k]
+ * (k < n_each; each_ms may be NULL when n_each is 0) receives schedule k's
+ * time per step, -1 where k blocks per SM do not fit. */
+int gelios_batch_set_schedule(gelios_batch *batch, int32_t schedule);
+int gelios_batch_get_schedule(gelios_batch *batch, int32_t *schedule);
+int gelios_batch_autotune(gelios_batch *batch, int steps, int32_t *schedule, double *ms, double *each_ms, int n_each);
 
 /* ---- batched plain-form instances (no counterpart in the reference) --------
  * Instances of GELIOS_FORM_STATIONARY that share one mesh (the contexts

@@ -265,6 +265,45 @@ def test_batched_instances_match_one_context_steps():
 
 
 @pytest.mark.gpu
+def test_persistent_batch_matches_per_phase_batch():
+    """The persistent schedule (every step of a call in one cooperative
+    kernel, grid barriers where the per-phase kernels end) against the
+    per-phase batch: same states, points, dt and flags to rounding, over two
+    calls (odd and even step counts); a block count that cannot be
+    co-resident is refused; the autotuner keeps a schedule that fits."""
+    from gelios_2d_b200 import sweep as sw
+
+    inst = sw.instance_set_mhd(3, seed=5, scale=(0.12, 0.2))
+    per_phase = sw.Sweep(inst, form=N.FORM_MHD_PUI, batched=True)
+    persistent = sw.Sweep(inst, form=N.FORM_MHD_PUI, batched=True)
+    persistent.set_batch_schedule(2)
+    assert persistent.batch_schedules() == [2]
+    for n, buf in ((5, 1), (2, 0)):
+        sa = per_phase.batch_step(n, statuses=True)
+        sp = persistent.batch_step(n, statuses=True)
+        for i in range(len(inst)):
+            a, b = per_phase.items[i], persistent.items[i]
+            assert rel_err(b.par(buf), a.par(buf)) <= 1e-12
+            assert ext_err(b.mhd(buf), a.mhd(buf), a.par(buf)) <= 1e-12
+            xa, ya = a.points()
+            xb, yb = b.points()
+            assert np.max(np.abs(xa - xb)) <= 1e-13 * np.max(np.abs(xa))
+            assert np.max(np.abs(ya - yb)) <= 1e-13 * np.max(np.abs(ya))
+            assert sp[i].result_buf == buf and sp[i].steps_done == n and sp[i].flags == sa[i].flags
+            assert abs(sp[i].dt - sa[i].dt) <= 1e-12 * sa[i].dt
+    with pytest.raises(N.GeliosError):
+        persistent.set_batch_schedule(4096)
+    assert persistent.batch_schedules() == [2]
+    (sched, ms, each), = persistent.autotune_batch(1)
+    assert sched >= 0 and ms > 0.0 and persistent.batch_schedules() == [sched]
+    assert len(each) >= 2 and min(each) == ms
+    st = persistent.batch_step(1, statuses=True)
+    assert all(s.flags == 0 and s.dt > 0.0 for s in st)
+    persistent.close()
+    per_phase.close()
+
+
+@pytest.mark.gpu
 def test_mk2_launch_shapes_give_same_bits_and_autotune_keeps_state():
     """The moving-grid step's arrangements (face kernel + update kernel, or
     one tile kernel) and launch shapes give the same bits; autotuning writes
