@@ -581,6 +581,17 @@ def run_sweep(args, rank: int, world: int, local: int) -> None:
                     o["Linf"] = max(o["Linf"], v["Linf"])
         line["fp32_flux_errors"] = {"against": "FP64 device path, same instance and initial state",
                                     "instances": len(per), "worst_over_instances": worst, "per_instance": per}
+    if mhd and rank == 0 and args.sweep_march:
+        # config-4 instances (FP32 fluxes) marched from their cold start: step
+        # and operator residuals per call of --march-every steps; the
+        # smallest, the median and the largest instance of this rank
+        order = sorted(range(len(inst)), key=lambda i: inst[i][0].n_cells)
+        pick = sorted({order[0], order[len(order) // 2], order[-1]})
+        line["march"] = []
+        for i in pick:
+            mesh, p32, st0, extra = inst[i]
+            rec = march_record(mesh, p32, st0, extra, N.FORM_MHD_PUI, local, args.sweep_march, args.march_every, "mhd")
+            line["march"].append({"instance_on_rank0": i, "cells": int(mesh.n_cells), "record": rec})
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -654,6 +665,8 @@ def main():
     ap.add_argument("--sweep-mode", default="contexts", choices=["contexts", "batched", "persistent"])
     ap.add_argument("--sweep-groups", type=int, default=1)
     ap.add_argument("--sweep-call-steps", type=int, default=1, help="steps per timed call of the sweep")
+    ap.add_argument("--sweep-march", type=int, default=0,
+                    help="sweep64: march three instances this many steps, recording their residuals")
     ap.add_argument("--sweep-errors", type=int, default=0,
                     help="sweep64: FP32-flux L1/Linf errors of this many instances after 1, 100, 2000 steps")
     # wall time to an L1 residual per unit time (cold start), reported beside the rate

@@ -115,7 +115,7 @@ class Sweep:
             each = (C.c_double * 16)()
             N.check(L.gelios_batch_autotune(h, int(steps), C.byref(v), C.byref(ms), C.cast(each, C.c_void_p), 16),
                     "gelios_batch_autotune")
-            res.append((v.value, ms.value, [round(x, 4) for x in each if x >= 0.0]))
+            res.append((v.value, ms.value, [x for x in each if x >= 0.0]))
         return res
 
     def batch_step(self, n: int = 1, statuses: bool = False):

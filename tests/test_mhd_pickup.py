@@ -296,7 +296,7 @@ def test_persistent_batch_matches_per_phase_batch():
     assert persistent.batch_schedules() == [2]
     (sched, ms, each), = persistent.autotune_batch(1)
     assert sched >= 0 and ms > 0.0 and persistent.batch_schedules() == [sched]
-    assert len(each) >= 2 and min(each) == ms
+    assert len(each) >= 2 and abs(min(each) - ms) <= 1e-9 * ms
     st = persistent.batch_step(1, statuses=True)
     assert all(s.flags == 0 and s.dt > 0.0 for s in st)
     persistent.close()
