@@ -46,6 +46,11 @@ namespace cg = cooperative_groups;
 #ifndef GELIOS_SOURCE_MINB
 #define GELIOS_SOURCE_MINB 10
 #endif
+// Source kernel arrangement: 32 cells per warp in a cell phase and a
+// species phase (1), or four lanes per cell throughout (0).
+#ifndef GELIOS_SOURCE_WARP
+#define GELIOS_SOURCE_WARP 1
+#endif
 
 namespace gelios {
 
@@ -1305,6 +1310,123 @@ __global__ void __launch_bounds__(64) mk2_tracked_solve_kernel(DevMesh d, gelios
 // the motion: the charge-exchange source Get_Sourse_MK1 (Cell.cpp:498-665).
 // Runs on a side stream while surface tracking and the rails move the grid.
 // aux rows: q1, q2, q3
+#if GELIOS_SOURCE_WARP
+// 32 cells per warp in two phases, every lane busy in both.  Cell phase: one
+// lane per cell decides whether the cell takes part, finds the bracket of
+// the radial interpolation, loads the cell's state and interpolates the
+// k_u, k_v, k_T factors; the per-cell values go to shared memory.  Species
+// phase: four rounds of eight cells x four hydrogen species, one (cell,
+// species) pair per lane: the species' moments at the cell and its exchange
+// rates; the four rates are summed on the cell's first species lane in the
+// reference's order (H1 + H2 + H3 + H4), which writes the cell's q1..q3.
+__global__ void __launch_bounds__(128, GELIOS_SOURCE_MINB) mk2_source_kernel(DevMesh d, gelios_params P, StepBuffers b,
+                                                                             double* __restrict__ aux) {
+    // per-cell values of the block's 128 cells, one row per quantity
+    __shared__ double sd[10][128];  // u, v, ro, p/ro, u^2+v^2, 1/(r1-r2), rr-r2, k_u, k_v, k_T
+    __shared__ int si[3][128];      // K_do, K_posle, flags (1 takes part, 2 bracket found, 4 interpolated)
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, wbase = threadIdx.x & ~31;
+    const int c0 = blockIdx.x * blockDim.x + wbase;  // the warp's first cell
+    int status = 0;
+    {
+        const int c = c0 + lane, t = threadIdx.x;
+        int flags = 0, K_do = -1, K_posle = -1;
+        double e[10] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        if (c < d.n_cells) {
+            const double x = b.cx[c], y = b.cy[c];
+            const double rr = sqrt(sq(x) + sq(y));
+            const bool proc = !(rr < P.R11);
+            const bool interp = proc && rr > P.src_rmin && rr < P.src_rmax && x >= 0.0;
+            bool ok = true;
+            if (interp) {
+                int2 cached;
+                ok = source_bracket(d, c, rr, K_do, K_posle, &status, &cached);
+                if (ok && d.src_lo_out && cached.x != K_do) d.src_lo_out[c] = make_int2(K_do, K_posle);
+            }
+            if (proc && ok) {
+                const St5 par1 = load_state(b.cur, c);
+                e[0] = par1.u;
+                e[1] = par1.v;
+                e[2] = par1.ro;
+                e[3] = par1.p / par1.ro;
+                e[4] = sq(par1.u) + sq(par1.v);
+                if (interp) {
+                    const double r1 = d.r_istoch[K_do], r2 = d.r_istoch[K_posle];
+                    const double ir = 1.0 / (r1 - r2), dr = rr - r2;
+                    auto lin = [&](double t1, double t2) { return (t1 - t2) * ir * dr + t2; };
+                    e[5] = ir;
+                    e[6] = dr;
+                    e[7] = lin(d.ku[K_do], d.ku[K_posle]);
+                    e[8] = lin(d.kv[K_do], d.kv[K_posle]);
+                    e[9] = lin(d.kT[K_do], d.kT[K_posle]);
+                } else {
+                    e[7] = d.ku[c];
+                    e[8] = d.kv[c];
+                    e[9] = d.kT[c];
+                }
+            }
+            flags = (proc ? 1 : 0) | (ok ? 2 : 0) | (interp ? 4 : 0);
+        }
+#pragma unroll
+        for (int k = 0; k < 10; k++) sd[k][t] = e[k];
+        si[0][t] = K_do;
+        si[1][t] = K_posle;
+        si[2][t] = flags;
+    }
+    __syncwarp();
+    const int sp = lane & 3, q0 = lane & ~3;
+#pragma unroll 1
+    for (int r = 0; r < 4; r++) {
+        const int t = wbase + 8 * r + (lane >> 2);  // the lane's cell, as a block slot
+        const int c = c0 + 8 * r + (lane >> 2);
+        const int flags = c < d.n_cells ? si[2][t] : 0;
+        double nuu = 0.0, nuv = 0.0, nue = 0.0;
+        if ((flags & 3) == 3) {
+            SrcMoments m;
+            if (flags & 4) {
+                const int K_do = si[0][t], K_posle = si[1][t];
+                const double ir = sd[5][t], dr = sd[6][t];
+                auto lin = [&](double t1, double t2) { return (t1 - t2) * ir * dr + t2; };
+                m.uH = lin(d.Hu[4 * K_do + sp], d.Hu[4 * K_posle + sp]);
+                m.vH = lin(d.Hv[4 * K_do + sp], d.Hv[4 * K_posle + sp]);
+                m.roH = lin(d.Hn[4 * K_do + sp], d.Hn[4 * K_posle + sp]);
+                const double TH = lin(d.HT[4 * K_do + sp], d.HT[4 * K_posle + sp]);
+                m.pH = 0.5 * TH * m.roH;
+            } else {
+                m.uH = d.Hu[4 * c + sp];
+                m.vH = d.Hv[4 * c + sp];
+                m.roH = d.Hn[4 * c + sp];
+                m.pH = 0.5 * d.HT[4 * c + sp] * d.Hn[4 * c + sp];
+            }
+            m.ku = m.kv = m.kT = 0.0;
+            source_rates(P, m, sd[0][t], sd[1][t], sd[2][t], sd[3][t], sd[4][t], nuu, nuv, nue);
+        }
+        double su[3], sv[3], se[3];
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            su[j] = __shfl_sync(full, nuu, q0 + 1 + j);
+            sv[j] = __shfl_sync(full, nuv, q0 + 1 + j);
+            se[j] = __shfl_sync(full, nue, q0 + 1 + j);
+        }
+        if (sp == 0 && (flags & 1)) {
+            const size_t n = d.n_cells;
+            double q1 = 0.0, q2 = 0.0, q3 = 0.0;
+            if (flags & 2) {
+                const double Mu = P.src_coef * (nuu + su[0] + su[1] + su[2]);
+                const double Mv = P.src_coef * (nuv + sv[0] + sv[1] + sv[2]);
+                const double MT = P.src_coef * (nue + se[0] + se[1] + se[2]);
+                q1 = Mu * sd[7][t];
+                q2 = Mv * sd[8][t];
+                q3 = MT * sd[9][t];
+            }
+            aux[0 * n + c] = q1;
+            aux[1 * n + c] = q2;
+            aux[2 * n + c] = q3;
+        }
+    }
+    if (status) atomicOr(b.status, status);
+}
+#else
 __global__ void __launch_bounds__(128, GELIOS_SOURCE_MINB) mk2_source_kernel(DevMesh d, gelios_params P, StepBuffers b,
                                                          double* __restrict__ aux) {
     // four lanes per cell, one hydrogen species per lane; the cell's first
@@ -1364,6 +1486,7 @@ __global__ void __launch_bounds__(128, GELIOS_SOURCE_MINB) mk2_source_kernel(Dev
     }
     if (status) atomicOr(b.status, status);
 }
+#endif
 
 // Go_5_komponent__MK2 cell update (Setka.cpp:10386-10468) of cell c from its
 // face slots' fluxes (fetch(k, j): row k of the cell's j-th slot, Grans
@@ -3785,7 +3908,11 @@ int launch_mk2_flux_tracked(const DevMesh& d, const gelios_params& P, const Step
     return 1;
 }
 void launch_mk2_source(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* aux, cudaStream_t s) {
+#if GELIOS_SOURCE_WARP
+    mk2_source_kernel<<<blocks_for(d.n_cells, 128), 128, 0, s>>>(d, P, b, aux);
+#else
     mk2_source_kernel<<<blocks_for(4 * d.n_cells, 128), 128, 0, s>>>(d, P, b, aux);
+#endif
 }
 void launch_inner(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const int32_t* list, int n,
                   cudaStream_t s) {
