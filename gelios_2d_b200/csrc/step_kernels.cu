@@ -5,8 +5,10 @@
 //   mk2_recon_tracked_kernel  TVD states of the tracked face units (pre-motion)
 //   mk2_tracked_solve_kernel  star pressures of the tracked faces' exact
 //                             Riemann problems (warp per face)
-//   mk2_source_kernel         charge-exchange source (Get_Sourse_MK1), four
-//                             lanes per cell (one hydrogen species each)
+//   mk2_source_kernel         charge-exchange source (Get_Sourse_MK1), 32
+//                             cells per warp: a cell phase (one lane per
+//                             cell), then a species phase (one lane per cell
+//                             and hydrogen species)
 //   surface_faces_kernel      Move_surface (Setka.cpp:3378-3844): exact
 //                             Godunov speeds of the tracked faces (warp per
 //                             face)

@@ -199,7 +199,7 @@ int launch_mk2_tracked_solve(const DevMesh& d, const gelios_params& P, const Ste
 int launch_mk2_flux_tracked(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const double* rec,
                             const double* pstar, double* fl, cudaStream_t s);
 // Charge-exchange source terms of the moving-grid step (aux rows q1, q2, q3),
-// four lanes per cell.
+// 128 cells per block (a cell phase, then a species phase).
 void launch_mk2_source(const DevMesh& d, const gelios_params& P, const StepBuffers& b, double* aux, cudaStream_t s);
 void launch_inner(const DevMesh& d, const gelios_params& P, const StepBuffers& b, const int32_t* list, int n,
                   cudaStream_t s);
