@@ -188,6 +188,7 @@ def lib() -> C.CDLL:
     L.gelios_get_variant.argtypes = [vp, C.c_int, C.POINTER(C.c_int32)]
     L.gelios_set_pipelined.argtypes = [vp, C.c_int]
     L.gelios_operator_residual.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_double)]
+    L.gelios_mk2_source_terms.argtypes = [vp, C.c_int, dp, dp, dp]
     L.gelios_set_inner_cells.argtypes = [vp, C.POINTER(C.c_int32), C.c_int32]
     L.gelios_step.argtypes = [vp, C.c_int, C.c_int, C.POINTER(GeliosStatus)]
     L.gelios_download_points.argtypes = [vp, dp, dp]

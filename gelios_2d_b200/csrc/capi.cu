@@ -1770,6 +1770,52 @@ extern "C" int gelios_operator_residual(gelios_ctx* ctx, int form, int buf, doub
     return GELIOS_OK;
 }
 
+extern "C" int gelios_mk2_source_terms(gelios_ctx* ctx, int buf, double* q1, double* q2, double* q3) {
+    if (!ctx || !q1 || !q2 || !q3 || buf < 0 || buf > 1) return GELIOS_E_ARG;
+    if (!ctx->have_mesh) return GELIOS_E_STATE;
+    GELIOS_CUDA_TRY(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    const DevMesh& d = ctx->d;
+    const gelios_params& P = ctx->prm;
+    const size_t nc = d.n_cells;
+    const size_t need = (kResidualScratch + 8) * sizeof(double);
+    if (ctx->resid.bytes < need && ctx->resid.alloc(need)) return GELIOS_E_CUDA;
+    double* cen0 = ctx->cen[0].as<double>();
+    if (!ctx->cen_valid) {
+        launch_centroid(d, d.X, d.Y, cen0, cen0 + nc, cen0 + 2 * nc, P.gamma, s, cen0 + 3 * nc, cen0 + 4 * nc);
+        ctx->cen_valid = true;
+        ctx->cen_rp_partial = false;
+    }
+    // the status word in scratch, so the context's own words stay untouched;
+    // rows of cells the step does not update stay 0
+    int* status = reinterpret_cast<int*>(ctx->resid.as<double>() + kResidualScratch);
+    GELIOS_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), s));
+    double* aux = ctx->aux.as<double>();
+    GELIOS_CUDA_TRY(cudaMemsetAsync(aux, 0, 3 * nc * sizeof(double), s));
+    StepBuffers b;
+    for (int k = 0; k < 5; k++) {
+        b.cur[k] = ctx->field(buf, k);
+        b.nxt[k] = ctx->field(buf ^ 1, k);
+    }
+    b.cx = cen0;
+    b.cy = cen0 + nc;
+    b.status = status;
+    launch_mk2_source(d, P, b, aux, s);
+    GELIOS_CUDA_TRY(cudaGetLastError());
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(q1, aux, nc * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(q2, aux + nc, nc * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(q3, aux + 2 * nc, nc * sizeof(double), cudaMemcpyDeviceToHost, s));
+    int st = 0;
+    GELIOS_CUDA_TRY(cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, s));
+    GELIOS_CUDA_TRY(cudaStreamSynchronize(s));
+    if (st) {
+        set_error("gelios_mk2_source_terms: a source chain link the reference would follow is missing (status " +
+                  std::to_string(st) + ")");
+        return GELIOS_E_STATE;
+    }
+    return GELIOS_OK;
+}
+
 extern "C" int gelios_run_to_residual(gelios_ctx* ctx, int form, double tol, int64_t max_steps, int32_t check_every,
                                       int64_t* steps_done, double* residual_per_time, double* dt) {
     if (!ctx || check_every <= 0 || (check_every & 1) || max_steps < 0) return GELIOS_E_ARG;

@@ -268,6 +268,16 @@ int gelios_run_to_residual(gelios_ctx *ctx, int form, double tol, int64_t max_st
  * only scratch (the moved-point buffer is set to the current points); the
  * state, the points and the dt words stay. */
 int gelios_operator_residual(gelios_ctx *ctx, int form, int buf, double *residual);
+/* gelios_mk2_source_terms: the charge-exchange source terms the moving-grid
+ * step adds per cell, Cell::Get_Sourse_MK1 (Cell.cpp:498-665) as
+ * Go_5_komponent__MK2 calls it (Setka.cpp:10414-10420), for the state
+ * par[buf], the current points' cell centres and the uploaded Monte-Carlo
+ * moments (gelios_upload_mc): q1, q2, q3 (n_cells each, host arrays) = the
+ * x-momentum, y-momentum and energy sources; 0 for the cells the step does
+ * not update (centre radius < R11).  The step's own kernel, run alone (for
+ * checking it and for callers that want the sources).  GELIOS_E_STATE where
+ * an interpolation chain link the reference would follow is missing. */
+int gelios_mk2_source_terms(gelios_ctx *ctx, int buf, double *q1, double *q2, double *q3);
 
 /* ---- streamed host I/O (no counterpart in the reference) --------------------
  * For callers that feed a fresh state from host memory every step and read

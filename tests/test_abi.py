@@ -68,3 +68,16 @@ def test_no_cpu_fallback_without_device():
             g.Setka(m)
     else:
         N.lib().gelios_destroy(h)
+
+
+def test_batch_schedule_and_source_entry_points_reject_null_handles():
+    """Argument checks that need no GPU: a missing batch or context handle
+    is refused before any CUDA call."""
+    import numpy as np
+
+    L = N.lib()
+    assert L.gelios_batch_set_schedule(None, 1) == N.GELIOS_E_ARG
+    assert L.gelios_batch_get_schedule(None, None) == N.GELIOS_E_ARG
+    assert L.gelios_batch_autotune(None, 1, None, None, None, 0) == N.GELIOS_E_ARG
+    q = np.zeros(1)
+    assert L.gelios_mk2_source_terms(None, 0, q, q, q) == N.GELIOS_E_ARG

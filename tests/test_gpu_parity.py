@@ -179,6 +179,38 @@ def test_mk2_moving_grid(steps):
     assert (s.flags & 1) == (st[0] & 1)
 
 
+def test_mk2_source_terms_match_the_oracle():
+    """The moving-grid step's charge-exchange source kernel run alone
+    (gelios_mk2_source_terms) against the oracle's Get_Sourse_MK1
+    (Cell.cpp:498-665) cell by cell on the medium rail grid with seeded
+    Monte-Carlo moments: every cell the step updates, inside the radial
+    re-interpolation window (bracket search along the cell chains) and
+    outside it (the cell's own moments); 0 for the cells it skips.
+    Tolerance: 1e-12 of each source row's largest magnitude."""
+    mesh = g.Mesh.setka(*MEDIUM)
+    P = N.reference_params()
+    st0 = W.init_conditions_reference(mesh)
+    mc = W.mc_fields(mesh, seed=9)
+    dev, ora = _pair(mesh, P, st0, mc)
+    n = mesh.n_cells
+    q = [np.zeros(n) for _ in range(3)]
+    for _ in range(2):  # the second call starts from the brackets the first one cached
+        N.check(N.lib().gelios_mk2_source_terms(dev._h, 0, *q), "gelios_mk2_source_terms")
+        x, y = mesh.centroids()
+        rr = np.hypot(x, y)
+        upd = ~(rr < P.R11)
+        ref = np.zeros((3, n))
+        for c in np.nonzero(upd)[0]:
+            ref[:, c] = ora.source_mk1(c, st0[2, c], st0[3, c], st0[0, c], st0[1, c])
+        for k in range(3):
+            scale = float(np.max(np.abs(ref[k])))
+            assert scale > 0.0
+            assert float(np.max(np.abs(q[k] - ref[k]))) <= 1e-12 * scale
+            assert np.all(q[k][~upd] == 0.0)
+    window = upd & (rr > P.src_rmin) & (rr < P.src_rmax) & (x >= 0.0)
+    assert window.any() and (upd & ~window).any() and (~upd).any()
+
+
 def test_inner_mk2():
     mesh = g.Mesh.setka(*MEDIUM)
     P = N.reference_params()
