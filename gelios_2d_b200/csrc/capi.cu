@@ -1353,25 +1353,24 @@ int enqueue_pipe_step(gelios_ctx* ctx, int st, const StepBuffers& b, const StepB
     double* fl = ctx->flux.as<double>();
     double* aux = ctx->aux.as<double>();
     int n = 0;
-    // the source terms on the motion stream (idle until step st's early
-    // update), the tracked-face fluxes on the side stream, the C_1 interior
+    // the tracked-face fluxes, then the source terms, on the (high-priority)
+    // motion stream, idle until step st's early update; the C_1 interior
     // and one-sided face-unit groups on the groups stream, the plain face
-    // units on the main stream
+    // units on the main stream.  The next step's tracked reconstructions
+    // (side stream) overwrite the rows the tracked fluxes read: they wait
+    // for the early update, which waits for the motion stream.
     GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_fork, s));
-    GELIOS_CUDA_TRY(cudaStreamWaitEvent(sd, ctx->ev_fork, 0));
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(sm, ctx->ev_fork, 0));
+    n += launch_mk2_flux_tracked(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(), fl, sm);
     launch_mk2_source(d, P, b, aux, sm);
     GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_motion, sm));
     n++;
-    n += launch_mk2_flux_tracked(d, P, b, ctx->rec.as<double>(), ctx->pstar.as<double>(), fl, sd);
-    GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_tracked, sd));
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(ctx->groups, ctx->ev_fork, 0));
     GELIOS_CUDA_TRY(launch_mk2_cells(d, P, b, ctx->tiles, fl, aux, ctx->groups, v, 3));
     n += mk2_variant_launches(d, v, 3);
     GELIOS_CUDA_TRY(cudaEventRecord(ctx->ev_groups, ctx->groups));
     GELIOS_CUDA_TRY(launch_mk2_cells(d, P, b, ctx->tiles, fl, aux, s, v, 1));
     n += mk2_variant_launches(d, v, 1);
-    GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_tracked, 0));
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_groups, 0));
     GELIOS_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev_motion, 0));
     if (!bn) {
