@@ -126,6 +126,37 @@ def test_steps_live_reference_medium(have_ref):
     assert np.array_equal(o.get_state(1), S.get_state(1))
 
 
+def test_source_mk1_bitexact_live_reference(have_ref):
+    """The oracle's Get_Sourse_MK1 (Cell.cpp:498-665) against the compiled
+    reference's own member function, cell by cell, for every cell the
+    moving-grid step updates (centroid radius >= R11), with seeded
+    Monte-Carlo moments: bit for bit, inside the radial re-interpolation
+    window (bracket search along the Back/Next chains of TVD_prepare) and
+    outside it."""
+    from oracle import ref
+
+    S = ref.RefSetka.constructor(*MEDIUM)
+    S.tvd_prepare()
+    S.init_conditions()
+    m = Mesh.from_arrays(S.export())
+    st0 = S.get_state(0)
+    mc = W.mc_fields(m, seed=5)
+    S.set_mc(*mc)
+    P = O.reference_params()
+    o = O.Oracle(P, m)
+    o.set_state(0, st0)
+    o.set_state(1, st0)
+    o.set_mc(*mc)
+    x, y = m.centroids()
+    rr = np.hypot(x, y)
+    upd = np.nonzero(~(rr < P.R11))[0]
+    window = (rr > P.src_rmin) & (rr < P.src_rmax) & (x >= 0.0)
+    assert window[upd].any() and (~window[upd]).any()
+    for c in upd:
+        args = (c, st0[2, c], st0[3, c], st0[0, c], st0[1, c])
+        assert np.array_equal(o.source_mk1(*args), S.source_mk1(*args)), c
+
+
 def test_polar_grid_through_reference_objects(have_ref):
     """The polar grid of the plain workload, instantiated as reference objects,
     stepped by the reference's own Go_stationary vs the restatement."""
