@@ -157,6 +157,22 @@ def test_source_mk1_bitexact_live_reference(have_ref):
         assert np.array_equal(o.source_mk1(*args), S.source_mk1(*args)), c
 
 
+def test_cell_geometry_bitexact_live_reference(have_ref):
+    """The oracle's cell geometry against the compiled reference's own
+    Cell methods, every cell of the medium rail grid, bit for bit: centre
+    and moved centre (Cell.cpp:66-111), area and moved area (146-254),
+    rotated volumes (188-206, 256-275)."""
+    from oracle import ref
+
+    S = ref.RefSetka.constructor(*MEDIUM)
+    S.tvd_prepare()
+    S.init_conditions()
+    m = Mesh.from_arrays(S.export())
+    o = O.Oracle(O.reference_params(), m)
+    for c in range(m.n_cells):
+        assert np.array_equal(o.cell_geom(c), S.cell_geom(c)), c
+
+
 def test_polar_grid_through_reference_objects(have_ref):
     """The polar grid of the plain workload, instantiated as reference objects,
     stepped by the reference's own Go_stationary vs the restatement."""
